@@ -1,0 +1,333 @@
+"""Benchmark of the CHAPSim periodic-channel time step on B200.
+
+Workload (one "step" = one RK3 time step: CFL/dt + 3 substeps, the CpuT
+boundary of src/SOLVE.f90:76,137): periodic plane channel at Re_tau ~ 180
+(REN = 2800), domain 4pi x 2 x 4pi/3, grid 128 x 128 x 128, tanh-stretched y
+(STR2 = 2), FP64 throughout, seeded perturbed-Poiseuille start projected by
+the NS = 0 substep, CFL 0.5.  Metric: grid-point * RK3-steps per second.
+
+  python bench.py [--gpus N --steps K --warmup W]        # B200 arm
+  python bench.py --impl reference [...]                 # CPU reference arm
+
+With N > 1 (launched by torch.distributed.run) every rank advances its own
+independent channel (replicas: the path has no data-parallel exchange) and
+the time is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "chapsim1.0_b200"))
+
+from chapsim.mesh import channel_setup  # noqa: E402
+from chapsim.fields import initial_field  # noqa: E402
+
+METRIC = "grid-pt·RK3-steps/s: mixed/learned vs plain FP64 on 1 B200 at stated error"
+UNIT = "grid-pt*RK3-steps/s"
+WORKLOADS = {
+    # name: (L, M, N, HX, HZ, STR2, REN, DT0, CFLGV)
+    "channel128_retau180_fp64": (128, 128, 128, 4 * math.pi, 4 * math.pi / 3, 2.0, 2800.0, 0.05, 0.5),
+    "channel64_retau180_fp64": (64, 64, 64, 2 * math.pi, math.pi, 2.0, 2800.0, 0.05, 0.5),
+    "channel384x256x384_retau395_fp64": (384, 256, 384, 2 * math.pi, math.pi, 2.0, 6875.0, 0.05, 0.5),
+}
+DEFAULT_WORKLOAD = "channel128_retau180_fp64"
+L2_BYTES = 126 * 1024 * 1024
+
+# algorithmic FP64 words per grid point moved by one launch of each kernel
+# (reads + writes of the arrays the reference's algorithm needs; the
+# spectral arrays hold (L/2+1)/L complex values per point)
+def kernel_words(L):
+    spec = 2.0 * (L // 2 + 1) / L  # complex spectrum, words per point
+    return {
+        "k_cfl": 3.0, "k_dt": 0.0,
+        "k_rhs_xsweep": 13.0,          # Q x3, PR, H0 x3 in; H0 x3, RHS x3 out
+        "k_zsweep": 6.0,               # RHS x3 in/out
+        "k_ysweep": 9.0,               # RHS x3, Q x3 in; Q x3 out
+        "k_div_fftx": 4.0 + spec,      # Q x3 in; RHSLLPHI, spectrum out
+        "k_fftz_fwd": 2.0 * spec, "k_fftz_inv": 2.0 * spec, "k_ysolve": 2.0 * spec,
+        "k_fftx_inv": spec + 1.0,      # spectrum in; DPH out
+        "k_correct": 10.0,             # DPH, Q x3, PR, RHSLLPHI in; Q x3, PR out
+    }
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(workload):
+    """Per-launch DRAM bytes of each kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", f"dram_traffic_{workload}.txt")
+    out = {}
+    if os.path.exists(p):
+        for line in open(p):
+            s = line.split()
+            if len(s) >= 2 and not line.startswith("#"):
+                try:
+                    out[s[0]] = float(s[1])
+                except ValueError:
+                    pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference_rate(wl, steps_cap, time_budget_s, threads):
+    """Timed CPU restatement of the step (oracle port, all host threads)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = WORKLOADS[wl]
+    s = channel_setup(L, M, N, HX, HZ, STR2, REN)
+    Q, PR = initial_field(s, 1973, 0.1)
+    o = Oracle(L, M, N, HX, HZ, STR2, REN, DT0=DT0, CFLGV=CFLGV, threads=threads)
+    o.set_fields(Q, PR)
+    o.substep(0)
+    o.run_steps(1)  # warm-up
+    t0 = time.perf_counter()
+    n = 0
+    while n < steps_cap:
+        o.run_steps(1)
+        n += 1
+        if time.perf_counter() - t0 > time_budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return L * M * N * n / dt, n, dt
+
+
+def run_reference(args):
+    ws, rank, local = dist_setup()
+    wl = args.workload
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    budget = float(os.environ.get("CHAPSIM_REF_BUDGET_S", "60"))
+    rate, n, dt = cpu_reference_rate(wl, max(args.steps, 1), budget, threads)
+    L, M, N = WORKLOADS[wl][:3]
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl, "grid": [L, M, N], "precision": "fp64", "parallelism": "replicas"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{n} of {args.steps} RK3 steps of {wl} (CPU FP64 restatement, OpenMP)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    from chapsim import gpu
+    ws, rank, local = dist_setup()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    import torch
+    torch.cuda.set_device(local)
+    wl = args.workload
+    L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = WORKLOADS[wl]
+    DTMIN = 1e-6
+    s = channel_setup(L, M, N, HX, HZ, STR2, REN)
+    Q0, PR0 = initial_field(s, 1973 + rank, 0.1)
+    ch = gpu.ChannelTG(s, device=local)
+    ch.upload(Q0, PR0)
+    ch.set_dt(DT0)
+    ch.SOLVERRK3_MOM_tg(0)
+    # warm-up (also captures the step graph)
+    ch.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)
+    stream = torch.cuda.ExternalStream(ch.stream_handle(), device=local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    launches0 = ch.launch_count()
+    barrier()
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        dt_last, cfl_last = ch.advance(args.steps, DT0, DTMIN, CFLGV)
+        ev1.record(stream)
+        torch.cuda.synchronize(local)
+    barrier()
+    launches = ch.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    pts = L * M * N
+    value = pts * args.steps * ws / (ms / 1000.0)
+    maxdiv = ch.DIVGCK_tg()
+
+    # ---- end to end through the public API with host buffers ----
+    try:
+        qh = torch.empty(Q0.shape, dtype=torch.float64, pin_memory=True).numpy()
+        ph = torch.empty(PR0.shape, dtype=torch.float64, pin_memory=True).numpy()
+    except Exception:
+        qh, ph = np.empty_like(Q0), np.empty_like(PR0)
+    qh[...], ph[...] = ch.download()
+    ne = max(1, min(args.steps, args.e2e_steps))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        ch.upload(qh, ph)                      # H2D: this step's input fields
+        ch.advance(1, DT0, DTMIN, CFLGV)
+        ch.lib.chapsim_download_fields(ch.h, gpu._ptr(qh), gpu._ptr(ph), None)  # D2H: the step's result
+    ch.sync()
+    te = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([te], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        te = float(t.item())
+    e2e = pts * ne * ws / te
+    hbytes = int(qh.nbytes + ph.nbytes)
+
+    # ---- per-kernel durations (CUDA events on the library stream) ----
+    prof_steps = max(1, min(20, args.steps))
+    kms = ch.profile_steps(prof_steps, DT0, DTMIN, CFLGV)
+    launches_per_step = {k: (1 if k in ("k_cfl", "k_dt") else 3) for k in kms}
+    words = kernel_words(L)
+    peak, peak_kind = load_peaks()
+    per_launch = {k: kms[k] / (prof_steps * launches_per_step[k]) for k in kms}
+    total_ms = sum(kms.values())
+    dom = max(kms, key=lambda k: kms[k])
+    dom_bytes = words[dom] * 8.0 * pts
+    achieved = dom_bytes / (per_launch[dom] / 1000.0) / 1e9
+    traffic = load_traffic(wl).get(dom)
+    step_bytes = sum(words[k] * 8.0 * pts * launches_per_step[k] for k in words)
+    step_ms = 1000.0 * 1.0 / (value / ws / pts)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl, "grid": [L, M, N], "domain": "4pi x 2 x 4pi/3" if L == 128 else None,
+                   "REN": REN, "STR2": STR2, "CFLGV": CFLGV, "precision": "fp64",
+                   "parallelism": "replicas" if ws > 1 else "single", "cuda_graph": True,
+                   "l2": "no flush: per-step working set %.0f MB > 126 MB L2" % (
+                       (12 * 8 * (M + 2) * L * N + 4 * 8 * L * M * N + 24 * (L // 2 + 1) * M * N) / 1e6),
+                   "final_dt": dt_last, "final_cfl": cfl_last, "max_div": maxdiv},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": hbytes, "d2h_bytes_per_step": hbytes,
+                "steps": ne, "api": "chapsim_upload_fields + chapsim_advance_tg(1) + chapsim_download_fields"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes,
+                     "share_of_step": kms[dom] / total_ms},
+        "step_roofline": {"bytes_per_point_step": step_bytes / pts, "achieved_gbs": step_bytes / (step_ms / 1000) / 1e9,
+                          "frac": step_bytes / (step_ms / 1000) / 1e9 / peak,
+                          "survey_model_1344B_frac": 1344.0 * pts / (step_ms / 1000) / 1e9 / peak},
+        "kernel_ms_per_step": {k: kms[k] / prof_steps for k in sorted(kms)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt = cpu_reference_rate(wl, 1000, float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n} RK3 steps of {wl} on the CPU FP64 restatement (OpenMP)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ch.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,292 @@
+"""ctypes binding of libchapsim_gpu.so and a host-side mirror of CHAPSim's
+subroutine interface for the periodic-channel time step.
+
+Method names follow the Fortran subroutines they replace; arguments keep the
+reference's meaning (NS = RK substep 0..3, DT0/DTMIN/CFLGV from readdata.ini)
+and a nonzero status raises :class:`ChapsimError`, the counterpart of
+``CALL ERRHDL`` (src/WRTHDL.f90:48-63, log + STOP).  There is no CPU
+fallback: if the CUDA library is missing, construction fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from .mesh import ChannelSetup, channel_setup
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libchapsim_gpu.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+ERR_NAMES = {0: "CHAPSIM_OK", -1: "CHAPSIM_ERR_CUDA", -2: "CHAPSIM_ERR_NAN", -3: "CHAPSIM_ERR_DT_COLLAPSE",
+             -4: "CHAPSIM_ERR_TABLE_RANGE", -5: "CHAPSIM_ERR_TIMEOUT", -6: "CHAPSIM_ERR_BADARG",
+             -7: "CHAPSIM_ERR_NOMEM"}
+
+EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_string", "chapsim_upload_fields",
+            "chapsim_download_fields", "chapsim_set_dt", "chapsim_get_dt", "chapsim_cfl_tg", "chapsim_step_begin",
+            "chapsim_rk_substep_tg", "chapsim_advance_tg", "chapsim_divgck_tg", "chapsim_fft99_pois3d",
+            "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_profile_steps", "chapsim_get_stream",
+            "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step"]
+
+KERNEL_SLOTS = ["k_cfl", "k_dt"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
+                                    "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
+
+
+class ChapsimError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("ncl1", ctypes.c_int32), ("ncl2", ctypes.c_int32), ("ncl3", ctypes.c_int32),
+                ("icase", ctypes.c_int32), ("idomain", ctypes.c_int32)]
+
+
+class Coefs(ctypes.Structure):
+    _fields_ = [("dxi", ctypes.c_double), ("dzi", ctypes.c_double), ("dxqi", ctypes.c_double),
+                ("dzqi", ctypes.c_double), ("cvisc", ctypes.c_double), ("volm", ctypes.c_double),
+                ("cf_given", ctypes.c_double), ("iflowdriven", ctypes.c_int32), ("pad0", ctypes.c_int32),
+                ("dyfi", _dp), ("dyci", _dp), ("ycl2nd_wff", _dp), ("ycl2nd_wfb", _dp), ("amph", _dp),
+                ("acph", _dp), ("apph", _dp), ("amvr", _dp), ("acvr", _dp), ("apvr", _dp), ("ak1", _dp),
+                ("ak3", _dp), ("tgam", ctypes.c_double * 4), ("troh", ctypes.c_double * 4),
+                ("talp", ctypes.c_double * 4)]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("fix_v_wall_row", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the CUDA library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libchapsim_gpu.so not built ({path}); run `make -C chapsim1.0_b200`")
+    L = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    L.chapsim_gpu_init.argtypes = [ctypes.POINTER(Grid), ctypes.POINTER(Coefs), ctypes.POINTER(Opts),
+                                   ctypes.POINTER(vp)]
+    L.chapsim_gpu_finalize.argtypes = [vp]
+    L.chapsim_last_error_string.argtypes = [vp]
+    L.chapsim_last_error_string.restype = ctypes.c_char_p
+    L.chapsim_upload_fields.argtypes = [vp, _dp, _dp, _dp]
+    L.chapsim_download_fields.argtypes = [vp, _dp, _dp, _dp]
+    L.chapsim_set_dt.argtypes = [vp, ctypes.c_double]
+    L.chapsim_get_dt.argtypes = [vp, _dp]
+    L.chapsim_cfl_tg.argtypes = [vp, _dp]
+    L.chapsim_step_begin.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp]
+    L.chapsim_rk_substep_tg.argtypes = [vp, ctypes.c_int32]
+    L.chapsim_advance_tg.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _dp]
+    L.chapsim_divgck_tg.argtypes = [vp, _dp]
+    L.chapsim_fft99_pois3d.argtypes = [vp, _dp, _dp]
+    L.chapsim_tdmaiji_cyc.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
+    L.chapsim_tdmaijj_noncyc.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
+    L.chapsim_profile_steps.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
+    L.chapsim_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.chapsim_sync.argtypes = [vp]
+    L.chapsim_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.chapsim_kernels_per_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int32)]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _fortran_cols(arr_idr_j: np.ndarray, M: int) -> np.ndarray:
+    """AMVR(1:NND2, 1:3) in Fortran order from a [IDR, j] 1-based table."""
+    return np.ascontiguousarray(np.concatenate([arr_idr_j[c, 1:M + 2] for c in (1, 2, 3)]))
+
+
+def _check_global(rc):
+    if rc != 0:
+        lib = load_library()
+        raise ChapsimError(rc, lib.chapsim_last_error_string(None).decode())
+
+
+def tdmaiji_cyc(A, B, C, R):
+    """TDMAIJI_CYC on (ISZ, JSZ) arrays given as numpy (JSZ, ISZ) C-order (lines along ISZ)."""
+    lib = load_library()
+    R = np.ascontiguousarray(R, np.float64).copy()
+    jsz, isz = R.shape
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (A, B, C)]
+    _check_global(lib.chapsim_tdmaiji_cyc(_ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(R), isz, jsz))
+    return R
+
+
+def tdmaijj_noncyc(A, B, C, R, BCJ=None):
+    """TDMAIJJ_nonCYC on (ISZ, JSZ) arrays given as numpy (JSZ, ISZ) C-order (lines along JSZ);
+    BCJ is (2, ISZ) or None."""
+    lib = load_library()
+    R = np.ascontiguousarray(R, np.float64).copy()
+    jsz, isz = R.shape
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (A, B, C)]
+    bc = None if BCJ is None else np.ascontiguousarray(BCJ, np.float64)
+    _check_global(lib.chapsim_tdmaijj_noncyc(_ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(R), _ptr(bc), jsz, isz))
+    return R
+
+
+class ChannelTG:
+    """Device-resident periodic plane channel (CHAPSim TG domain).
+
+    Fields use the reference layout: ``Q`` is numpy (3, N, M+2, L) C-order =
+    Fortran ``Q_tg(L, 0:M+1, N, 3)``; ``PR`` is (N, M+2, L); ``CONVH0`` is
+    (3, N, M, L) = ``CONVH0_tg(L, M, N, 3)``.
+    """
+
+    def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False):
+        self.lib = load_library()
+        self.s = setup
+        L, M, N = setup.L, setup.M, setup.N
+        self.L, self.M, self.N = L, M, N
+        self._keep = {
+            "dyfi": np.ascontiguousarray(setup.DYFI[1:M + 1]),
+            "dyci": np.ascontiguousarray(setup.DYCI[1:M + 2]),
+            "wff": np.ascontiguousarray(setup.WFF[1:M + 2]),
+            "wfb": np.ascontiguousarray(setup.WFB[1:M + 2]),
+            "amph": np.ascontiguousarray(setup.AMPH[1:M + 1]),
+            "acph": np.ascontiguousarray(setup.ACPH[1:M + 1]),
+            "apph": np.ascontiguousarray(setup.APPH[1:M + 1]),
+            "amvr": _fortran_cols(setup.AMVR, M),
+            "acvr": _fortran_cols(setup.ACVR, M),
+            "apvr": _fortran_cols(setup.APVR, M),
+            "ak1": np.ascontiguousarray(setup.AK1),
+            "ak3": np.ascontiguousarray(setup.AK3),
+        }
+        k = self._keep
+        cf = Coefs(setup.DXI, setup.DZI, setup.DXQI, setup.DZQI, setup.CVISC, setup.VOLM, setup.Cf_Given,
+                   setup.iFlowDriven, 0, _ptr(k["dyfi"]), _ptr(k["dyci"]), _ptr(k["wff"]), _ptr(k["wfb"]),
+                   _ptr(k["amph"]), _ptr(k["acph"]), _ptr(k["apph"]), _ptr(k["amvr"]), _ptr(k["acvr"]),
+                   _ptr(k["apvr"]), _ptr(k["ak1"]), _ptr(k["ak3"]), (ctypes.c_double * 4)(*setup.TGAM),
+                   (ctypes.c_double * 4)(*setup.TROH), (ctypes.c_double * 4)(*setup.TALP))
+        g = Grid(L, M, N, 1, 1)
+        o = Opts(device, int(bool(fix_v_wall_row)))
+        h = ctypes.c_void_p()
+        rc = self.lib.chapsim_gpu_init(ctypes.byref(g), ctypes.byref(cf), ctypes.byref(o), ctypes.byref(h))
+        if rc != 0:
+            raise ChapsimError(rc, self.lib.chapsim_last_error_string(None).decode())
+        self.h = h
+
+    @classmethod
+    def create(cls, L, M, N, HX, HZ, STR2, REN, iFlowDriven=1, Cf_Given=8.18e-3, **kw):
+        return cls(channel_setup(L, M, N, HX, HZ, STR2, REN, iFlowDriven, Cf_Given), **kw)
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, rc):
+        if rc != 0:
+            raise ChapsimError(rc, self.lib.chapsim_last_error_string(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chapsim_gpu_finalize(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def field_shape(self):
+        return (self.N, self.M + 2, self.L)
+
+    def upload(self, Q, PR, CONVH0=None):
+        Q = np.ascontiguousarray(Q, np.float64)
+        PR = np.ascontiguousarray(PR, np.float64)
+        if Q.shape != (3,) + self.field_shape() or PR.shape != self.field_shape():
+            raise ValueError("field shape mismatch")
+        H = None
+        if CONVH0 is not None:
+            H = np.ascontiguousarray(CONVH0, np.float64)
+            if H.shape != (3, self.N, self.M, self.L):
+                raise ValueError("CONVH0 shape mismatch")
+        self._check(self.lib.chapsim_upload_fields(self.h, _ptr(Q), _ptr(PR), _ptr(H)))
+
+    def download(self, want_h0=False):
+        Q = np.empty((3,) + self.field_shape())
+        PR = np.empty(self.field_shape())
+        H = np.empty((3, self.N, self.M, self.L)) if want_h0 else None
+        self._check(self.lib.chapsim_download_fields(self.h, _ptr(Q), _ptr(PR), _ptr(H)))
+        return (Q, PR, H) if want_h0 else (Q, PR)
+
+    def set_dt(self, dt):
+        self._check(self.lib.chapsim_set_dt(self.h, float(dt)))
+
+    def get_dt(self):
+        v = ctypes.c_double()
+        self._check(self.lib.chapsim_get_dt(self.h, ctypes.byref(v)))
+        return v.value
+
+    def sync(self):
+        self._check(self.lib.chapsim_sync(self.h))
+
+    def launch_count(self):
+        v = ctypes.c_uint64()
+        self._check(self.lib.chapsim_launch_count(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    def kernels_per_step(self):
+        v = ctypes.c_int32()
+        self._check(self.lib.chapsim_kernels_per_step(self.h, ctypes.byref(v)))
+        return int(v.value)
+
+    # -- reference interface ---------------------------------------------------
+    def CFL_tg(self):
+        v = ctypes.c_double()
+        self._check(self.lib.chapsim_cfl_tg(self.h, ctypes.byref(v)))
+        return v.value
+
+    def step_begin(self, DT0, DTMIN, CFLGV):
+        dt, cfl = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.chapsim_step_begin(self.h, DT0, DTMIN, CFLGV, ctypes.byref(dt), ctypes.byref(cfl)))
+        return dt.value, cfl.value
+
+    def SOLVERRK3_MOM_tg(self, NS):
+        self._check(self.lib.chapsim_rk_substep_tg(self.h, int(NS)))
+
+    def advance(self, nsteps, DT0, DTMIN, CFLGV):
+        dt, cfl = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.chapsim_advance_tg(self.h, int(nsteps), DT0, DTMIN, CFLGV, ctypes.byref(dt),
+                                                ctypes.byref(cfl)))
+        return dt.value, cfl.value
+
+    def profile_steps(self, nsteps, DT0, DTMIN, CFLGV):
+        """Per-kernel durations (ms, summed over nsteps) keyed by kernel name."""
+        n = len(KERNEL_SLOTS)
+        buf = (ctypes.c_float * n)()
+        self._check(self.lib.chapsim_profile_steps(self.h, int(nsteps), DT0, DTMIN, CFLGV, buf, n))
+        out = {}
+        for name, v in zip(KERNEL_SLOTS, buf):
+            out[name] = out.get(name, 0.0) + float(v)
+        return out
+
+    def stream_handle(self):
+        v = ctypes.c_void_p()
+        self._check(self.lib.chapsim_get_stream(self.h, ctypes.byref(v)))
+        return v.value or 0
+
+    def DIVGCK_tg(self):
+        v = ctypes.c_double()
+        self._check(self.lib.chapsim_divgck_tg(self.h, ctypes.byref(v)))
+        return v.value
+
+    def FFT99_POIS3D_periodicxz(self, rhs_nml):
+        rhs = np.ascontiguousarray(rhs_nml, np.float64)
+        if rhs.shape != (self.N, self.M, self.L):
+            raise ValueError("RHSLLPHI shape mismatch")
+        out = np.zeros(self.field_shape())
+        self._check(self.lib.chapsim_fft99_pois3d(self.h, _ptr(rhs), _ptr(out)))
+        return out

@@ -1,0 +1,720 @@
+// C ABI, device context and launch sequencing of the periodic-channel step.
+// Build: nvcc -gencode arch=compute_100a,code=sm_100a -O3 -shared (see Makefile).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/chapsim_gpu.h"
+#include "common.cuh"
+#include "diag.cuh"
+#include "fft.cuh"
+#include "momentum.cuh"
+#include "poisson.cuh"
+#include "tdma.cuh"
+
+// x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
+__global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
+    extern __shared__ double2 smc[];
+    const int L = g.L, M = g.M, LH = g.LH;
+    const int j0 = 1 + blockIdx.x * PX_TJ;
+    const int k = blockIdx.y;
+    const int nj = min(PX_TJ, M - j0 + 1);
+    const int np = (nj + 1) >> 1;
+    for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
+        const int jl = p / L, i = p - jl * L;
+        const int pair = jl >> 1, part = jl & 1;
+        const double val = jl < nj ? RHSLL[iidx(g, i, j0 + jl, k)] : 0.0;
+        double2* line = smc + pair * L;
+        const int pos = g.permx[i];
+        if (part == 0) line[pos].x = val; else line[pos].y = val;
+    }
+    block_fft<-1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    const double sc = 0.5 / (double)L;
+    for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
+        const int pair = p / LH, kx = p - pair * LH;
+        const double2* line = smc + pair * L;
+        const double2 z = line[kx];
+        const double2 zc = line[kx == 0 ? 0 : L - kx];
+        const int ja = j0 + 2 * pair;
+        SP[kx + (long long)LH * ((ja - 1) + (long long)M * k)] = make_double2((z.x + zc.x) * sc, (z.y - zc.y) * sc);
+        if (2 * pair + 1 < nj)
+            SP[kx + (long long)LH * ((ja) + (long long)M * k)] = make_double2((z.y + zc.y) * sc, (zc.x - z.x) * sc);
+    }
+}
+
+// ------------------------- general line solvers (ABI) ------------------------
+// Coefficients per point in global memory, element e of line l at off(l) + e*es.
+struct GlobalCoef {
+    const double *a, *b, *c;
+    long long off, es;
+    __device__ __forceinline__ double A(int r) const { return a[off + r * es]; }
+    __device__ __forceinline__ double B(int r) const { return b[off + r * es]; }
+    __device__ __forceinline__ double C(int r) const { return c[off + r * es]; }
+};
+
+template <int S, bool CYCLIC>
+__global__ void k_tdma_lines(const double* a, const double* b, const double* c, double* r, const double* bcj, int nlines,
+                             long long ls, long long es, int n) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= nlines) return;
+    GlobalCoef cf{a, b, c, (long long)warp * ls, es};
+    double d[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) d[k] = r[cf.off + (long long)(lane * S + k) * es];
+    if (!CYCLIC && bcj) {
+        if (lane == 0) d[0] -= cf.A(0) * bcj[warp];
+        if (lane == 31) d[S - 1] -= cf.C(n - 1) * bcj[nlines + warp];
+    }
+    warp_tdma<S, CYCLIC>(d, cf, lane);
+#pragma unroll
+    for (int k = 0; k < S; ++k) r[cf.off + (long long)(lane * S + k) * es] = d[k];
+}
+
+// sequential reference recurrences, one thread per line, for lengths that
+// are not 32*S (TDMAIJI_CYC :100-154 and TDMAIJJ_nonCYC :95-121)
+__global__ void k_tdma_seq(const double* A, const double* B, const double* C, double* R, const double* bcj, double* wk,
+                           int nlines, long long ls, long long es, int n, int cyclic) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines) return;
+    const long long o = (long long)l * ls;
+#define E(X, i) X[o + (long long)(i) * es]
+    double* H0 = wk + (long long)l * 3 * n;
+    double* G1 = H0 + n;
+    double* G2 = G1 + n;
+    if (cyclic) {
+        H0[0] = E(C, 0) / E(B, 0); G1[0] = E(R, 0) / E(B, 0); G2[0] = -E(A, 0) / E(B, 0);
+        for (int i = 1; i <= n - 3; ++i) {
+            double pp = 1.0 / (E(B, i) - H0[i - 1] * E(A, i));
+            double q1 = G1[i - 1] * E(A, i), q2 = G2[i - 1] * E(A, i);
+            H0[i] = E(C, i) * pp; G1[i] = (E(R, i) - q1) * pp; G2[i] = -q2 * pp;
+        }
+        {
+            int i = n - 2;
+            double pp = 1.0 / (E(B, i) - H0[i - 1] * E(A, i));
+            double q1 = G1[i - 1] * E(A, i), q2 = G2[i - 1] * E(A, i);
+            G1[i] = (E(R, i) - q1) * pp; G2[i] = (-E(C, i) - q2) * pp;
+        }
+        for (int i = n - 3; i >= 0; --i) { G1[i] = -H0[i] * G1[i + 1] + G1[i]; G2[i] = -H0[i] * G2[i + 1] + G2[i]; }
+        int i = n - 1;
+        double pp = E(R, i) - E(C, i) * G1[0] - E(A, i) * G1[i - 1];
+        double qq = E(B, i) + E(C, i) * G2[0] + E(A, i) * G2[i - 1];
+        E(R, i) = pp / qq;
+        for (int k = n - 2; k >= 0; --k) E(R, k) = G1[k] + G2[k] * E(R, n - 1);
+    } else {
+        double b1 = bcj ? bcj[l] : 0.0, b2 = bcj ? bcj[nlines + l] : 0.0;
+        H0[0] = E(C, 0) / E(B, 0);
+        G1[0] = (E(R, 0) - E(A, 0) * b1) / E(B, 0);
+        for (int j = 1; j <= n - 2; ++j) {
+            double pp = 1.0 / (E(B, j) - H0[j - 1] * E(A, j));
+            H0[j] = E(C, j) * pp;
+            G1[j] = (E(R, j) - E(A, j) * G1[j - 1]) * pp;
+        }
+        int j = n - 1;
+        double pp = 1.0 / (E(B, j) - H0[j - 1] * E(A, j));
+        G1[j] = (E(R, j) - E(C, j) * b2 - E(A, j) * G1[j - 1]) * pp;
+        E(R, j) = G1[j];
+        for (int k = n - 2; k >= 0; --k) E(R, k) = G1[k] - H0[k] * E(R, k + 1);
+    }
+#undef E
+}
+
+
+struct chapsim_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Geo g{};
+    double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr, *HS = nullptr;
+    double2* SP = nullptr;
+    double* part_rhs = nullptr;  // per-block bulk-flux partial sums
+    int npart_rhs = 0;
+    double* part_red = nullptr;  // per-block CFL / divergence maxima
+    int npart_red = 0;
+    DevState* st = nullptr;
+    DevState* st_host = nullptr;  // pinned mirror for readback
+    double* ybuf = nullptr;       // device copies of y-arrays and wavenumbers
+    double2* tw = nullptr;
+    int* perm = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    cudaEvent_t* prof_ev = nullptr;  // when set, an event is recorded after every kernel
+    int prof_n = 0;
+    int kernels_per_step = 0;
+    unsigned long long launches = 0;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_init_error;
+
+int fail(chapsim_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    else g_init_error = msg;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(ctx, CHAPSIM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+bool factor23(int n, std::vector<int>& rad) {
+    rad.clear();
+    int m = n;
+    while (m % 4 == 0) { rad.push_back(4); m /= 4; }
+    while (m % 2 == 0) { rad.push_back(2); m /= 2; }
+    while (m % 3 == 0) { rad.push_back(3); m /= 3; }
+    return m == 1 && rad.size() <= 8;
+}
+
+// position of input element j for the in-place DIT with pass order rad[0..]
+std::vector<int> dit_perm(int n, const std::vector<int>& rad) {
+    std::vector<int> perm(n);
+    for (int j = 0; j < n; ++j) {
+        int rem = j, mult = n, p = 0;
+        for (int i = (int)rad.size() - 1; i >= 0; --i) {
+            int t = rem % rad[i];
+            rem /= rad[i];
+            mult /= rad[i];
+            p += t * mult;
+        }
+        perm[j] = p;
+    }
+    return perm;
+}
+
+std::vector<double2> twiddles(int n) {
+    std::vector<double2> w(n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int e = 0; e < n; ++e) {
+        long double a = 2.0L * pi * (long double)e / (long double)n;
+        w[e].x = (double)cosl(a);
+        w[e].y = (double)(-sinl(a));
+    }
+    return w;
+}
+
+size_t smem_rhs(const Geo& g) { return (size_t)(3 * RHS_TJ * (g.L + 33) + 32) * sizeof(double); }
+size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(double); }
+size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33) + 3 * g.M + 64) * sizeof(double); }
+size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * g.L) * sizeof(double2); }
+size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * (g.N + 1)) * sizeof(double2); }
+
+template <typename F>
+cudaError_t set_smem(F* f, size_t bytes) {
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+#define DISPATCH_S(S_, KERNEL_CALL)                    \
+    switch (S_) {                                      \
+        case 1: { constexpr int S = 1; KERNEL_CALL; } break;  \
+        case 2: { constexpr int S = 2; KERNEL_CALL; } break;  \
+        case 3: { constexpr int S = 3; KERNEL_CALL; } break;  \
+        case 4: { constexpr int S = 4; KERNEL_CALL; } break;  \
+        case 6: { constexpr int S = 6; KERNEL_CALL; } break;  \
+        case 8: { constexpr int S = 8; KERNEL_CALL; } break;  \
+        case 12: { constexpr int S = 12; KERNEL_CALL; } break; \
+        default: break;                                \
+    }
+
+bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
+
+int configure_kernels(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S>, smem_rhs(g))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S>, smem_z(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S>, smem_y(g))));
+    CK(set_smem(k_div_fftx, smem_px(g)));
+    CK(set_smem(k_fftx_inv, smem_px(g)));
+    CK(set_smem(k_fftz<-1>, smem_fz(g)));
+    CK(set_smem(k_fftz<+1>, smem_fz(g)));
+    return CHAPSIM_OK;
+}
+
+// --------------------------- launch helpers ---------------------------------
+inline void prof_mark(chapsim_ctx* ctx) {
+    if (ctx->prof_ev) cudaEventRecord(ctx->prof_ev[ctx->prof_n++], ctx->stream);
+}
+
+void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
+    const Geo& g = ctx->g;
+    k_cfl<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
+    prof_mark(ctx);
+    k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, update_dt);
+    prof_mark(ctx);
+    ctx->launches += 2;
+}
+
+void launch_substep(chapsim_ctx* ctx, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    dim3 grx((g.M + RHS_TJ - 1) / RHS_TJ, g.N);
+    DISPATCH_S(g.L / 32, (k_rhs_xsweep<S><<<grx, RHS_NT, smem_rhs(g), s>>>(g, ctx->Q, ctx->PR, ctx->H0, ctx->RHS,
+                                                                             ctx->part_rhs, ctx->st, ns)));
+    prof_mark(ctx);
+    dim3 grz((g.L + 31) / 32, g.M, 3);
+    DISPATCH_S(g.N / 32, (k_zsweep<S><<<grz, SWEEP_NT, smem_z(g), s>>>(g, ctx->RHS, ctx->st, ns)));
+    prof_mark(ctx);
+    dim3 gry((g.L + 31) / 32, g.N);
+    DISPATCH_S(g.M / 32, (k_ysweep<S><<<gry, SWEEP_NT, smem_y(g), s>>>(g, ctx->Q, ctx->RHS, ctx->part_rhs,
+                                                                        ctx->npart_rhs, ctx->st, ns)));
+    prof_mark(ctx);
+    dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
+    k_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->Q, ctx->RHSLL, ctx->SP, ctx->st, ns);
+    prof_mark(ctx);
+    const long long nq = (long long)g.LH * g.M;
+    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
+    k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    prof_mark(ctx);
+    const long long nl = (long long)g.LH * g.N;
+    k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, s>>>(g, ctx->SP, ctx->HS);
+    prof_mark(ctx);
+    k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    prof_mark(ctx);
+    k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
+    prof_mark(ctx);
+    const long long tot = (long long)g.L * g.M * g.N;
+    k_correct<<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, ctx->Q, ctx->PR, ctx->DPH, ctx->RHSLL, ctx->st, ns);
+    prof_mark(ctx);
+    ctx->launches += 9;
+}
+
+int check_device_error(chapsim_ctx* ctx) {
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned int e = ctx->st_host->err;
+    if (e) {
+        unsigned int zero = 0;
+        CK(cudaMemcpyAsync(&ctx->st->err, &zero, sizeof(unsigned int), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (e & CHS_EBIT_NAN) return fail(ctx, CHAPSIM_ERR_NAN, "non-finite velocity or time step on the device");
+        if (e & CHS_EBIT_DT_COLLAPSE) return fail(ctx, CHAPSIM_ERR_DT_COLLAPSE, "DT/DT0 < 0.01 (time step collapse)");
+    }
+    return CHAPSIM_OK;
+}
+
+int build_step_graph(chapsim_ctx* ctx) {
+    if (ctx->step_exec) return CHAPSIM_OK;
+    cudaGraph_t graph;
+    unsigned long long before = ctx->launches;
+    CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    launch_cfl_dt(ctx, 1);
+    for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    ctx->kernels_per_step = (int)(ctx->launches - before);
+    ctx->launches = before;  // capture does not launch
+    if (e != cudaSuccess) return fail(ctx, CHAPSIM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ctx->step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, CHAPSIM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return CHAPSIM_OK;
+}
+
+}  // namespace
+
+// ============================== C ABI ========================================
+extern "C" {
+
+int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, const chapsim_opts_t* opts,
+                     chapsim_ctx_t** out) {
+    chapsim_ctx* ctx = nullptr;
+    if (!grid || !cf || !out) return fail(nullptr, CHAPSIM_ERR_BADARG, "null argument");
+    *out = nullptr;
+    const int L = grid->ncl1, M = grid->ncl2, N = grid->ncl3;
+    if (grid->icase != 1 || grid->idomain != 1)
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "only the periodic plane channel (iCase=1, iDomain=1) is supported");
+    if (L < 32 || M < 32 || N < 32 || L % 32 || M % 32 || N % 32 || !valid_S(L / 32) || !valid_S(M / 32) ||
+        !valid_S(N / 32))
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");
+    std::vector<int> radx, radz;
+    if (!factor23(L, radx) || !factor23(N, radz))
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1 and NCL3 must factor into 2s and 3s");
+    if (!cf->dyfi || !cf->dyci || !cf->ycl2nd_wff || !cf->ycl2nd_wfb || !cf->amph || !cf->acph || !cf->apph ||
+        !cf->amvr || !cf->acvr || !cf->apvr || !cf->ak1 || !cf->ak3)
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "missing coefficient array");
+    if (cf->iflowdriven < 0 || cf->iflowdriven > 2) return fail(nullptr, CHAPSIM_ERR_BADARG, "iFlowDriven must be 0, 1 or 2");
+
+    ctx = new chapsim_ctx();
+    ctx->device = opts ? opts->device : 0;
+    int rc;
+#define INIT_CK(call)                                  \
+    do {                                               \
+        cudaError_t e_ = (call);                       \
+        if (e_ != cudaSuccess) {                       \
+            g_init_error = std::string(#call) + ": " + cudaGetErrorString(e_); \
+            chapsim_gpu_finalize(ctx);                 \
+            return CHAPSIM_ERR_CUDA;                   \
+        }                                              \
+    } while (0)
+    INIT_CK(cudaSetDevice(ctx->device));
+    INIT_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    Geo& g = ctx->g;
+    g.L = L; g.M = M; g.N = N; g.LH = L / 2 + 1;
+    g.P = (long long)L * (M + 2);
+    g.FS = g.P * N;
+    g.PI_ = (long long)L * M;
+    g.FI = g.PI_ * N;
+    g.dxi = cf->dxi; g.dzi = cf->dzi; g.dxqi = cf->dxqi; g.dzqi = cf->dzqi;
+    g.cvisc = cf->cvisc; g.volm = cf->volm; g.cf_given = cf->cf_given; g.iflowdriven = cf->iflowdriven;
+    g.fix_v_wall_row = opts ? opts->fix_v_wall_row : 0;
+    for (int s = 0; s < 4; ++s) { g.tgam[s] = cf->tgam[s]; g.troh[s] = cf->troh[s]; g.talp[s] = cf->talp[s]; }
+    // y arrays with the reference's 1-based index (entry 0 unused)
+    const int YS = M + 2;
+    std::vector<double> yb((size_t)YS * 13 + L + N, 0.0);
+    double* y = yb.data();
+    for (int j = 1; j <= M; ++j) {
+        y[0 * YS + j] = cf->dyfi[j - 1];
+        y[4 * YS + j] = cf->amph[j - 1];
+        y[5 * YS + j] = cf->acph[j - 1];
+        y[6 * YS + j] = cf->apph[j - 1];
+    }
+    for (int j = 1; j <= M + 1; ++j) {
+        y[1 * YS + j] = cf->dyci[j - 1];
+        y[2 * YS + j] = cf->ycl2nd_wff[j - 1];
+        y[3 * YS + j] = cf->ycl2nd_wfb[j - 1];
+        for (int c = 0; c < 3; ++c) {
+            y[(7 + c) * YS + j] = cf->amvr[(size_t)c * (M + 1) + (j - 1)];
+            y[(10 + c) * YS + j] = cf->acvr[(size_t)c * (M + 1) + (j - 1)];
+        }
+    }
+    // apvr occupies its own block after the 13 y arrays: reuse slots via a second vector
+    std::vector<double> ap((size_t)3 * YS, 0.0);
+    for (int j = 1; j <= M + 1; ++j)
+        for (int c = 0; c < 3; ++c) ap[(size_t)c * YS + j] = cf->apvr[(size_t)c * (M + 1) + (j - 1)];
+    double* ak = y + 13 * YS;
+    for (int i = 0; i < L; ++i) ak[i] = cf->ak1[i];
+    for (int k = 0; k < N; ++k) ak[L + k] = cf->ak3[k];
+    const size_t nyb = yb.size() + ap.size();
+    INIT_CK(cudaMalloc(&ctx->ybuf, nyb * sizeof(double)));
+    INIT_CK(cudaMemcpy(ctx->ybuf, yb.data(), yb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    INIT_CK(cudaMemcpy(ctx->ybuf + yb.size(), ap.data(), ap.size() * sizeof(double), cudaMemcpyHostToDevice));
+    double* yd = ctx->ybuf;
+    g.dyfi = yd + 0 * YS; g.dyci = yd + 1 * YS; g.wff = yd + 2 * YS; g.wfb = yd + 3 * YS;
+    g.amph = yd + 4 * YS; g.acph = yd + 5 * YS; g.apph = yd + 6 * YS;
+    g.amvr = yd + 7 * YS; g.acvr = yd + 10 * YS; g.apvr = yd + yb.size();
+    g.ak1 = yd + 13 * YS; g.ak3 = yd + 13 * YS + L;
+    // FFT plans
+    std::vector<double2> twx = twiddles(L), twz = twiddles(N);
+    std::vector<int> px = dit_perm(L, radx), pz = dit_perm(N, radz);
+    INIT_CK(cudaMalloc(&ctx->tw, (size_t)(L + N) * sizeof(double2)));
+    INIT_CK(cudaMemcpy(ctx->tw, twx.data(), L * sizeof(double2), cudaMemcpyHostToDevice));
+    INIT_CK(cudaMemcpy(ctx->tw + L, twz.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
+    INIT_CK(cudaMalloc(&ctx->perm, (size_t)(L + N) * sizeof(int)));
+    INIT_CK(cudaMemcpy(ctx->perm, px.data(), L * sizeof(int), cudaMemcpyHostToDevice));
+    INIT_CK(cudaMemcpy(ctx->perm + L, pz.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    g.twx = ctx->tw; g.twz = ctx->tw + L; g.permx = ctx->perm; g.permz = ctx->perm + L;
+    g.nradx = (int)radx.size(); g.nradz = (int)radz.size();
+    for (int i = 0; i < 8; ++i) {
+        g.radx[i] = i < g.nradx ? radx[i] : 0;
+        g.radz[i] = i < g.nradz ? radz[i] : 0;
+    }
+    // fields
+    INIT_CK(cudaMalloc(&ctx->Q, (size_t)(3 * g.FS) * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->PR, (size_t)g.FS * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->DPH, (size_t)g.FS * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->H0, (size_t)(3 * g.FI) * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->RHS, (size_t)(3 * g.FI) * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->RHSLL, (size_t)g.FI * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->SP, (size_t)g.LH * M * N * sizeof(double2)));
+    INIT_CK(cudaMalloc(&ctx->HS, (size_t)g.LH * M * N * sizeof(double)));
+    ctx->npart_rhs = ((M + RHS_TJ - 1) / RHS_TJ) * N;
+    INIT_CK(cudaMalloc(&ctx->part_rhs, (size_t)ctx->npart_rhs * sizeof(double)));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    ctx->npart_red = 4 * nsm;
+    INIT_CK(cudaMalloc(&ctx->part_red, (size_t)ctx->npart_red * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->st, sizeof(DevState)));
+    INIT_CK(cudaMallocHost(&ctx->st_host, sizeof(DevState)));
+    INIT_CK(cudaMemset(ctx->Q, 0, (size_t)(3 * g.FS) * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->PR, 0, (size_t)g.FS * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->DPH, 0, (size_t)g.FS * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->H0, 0, (size_t)(3 * g.FI) * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->RHS, 0, (size_t)(3 * g.FI) * sizeof(double)));
+    DevState s0{};
+    s0.dt = 1e-3; s0.dt0 = 1e-3; s0.dtmin = 1e-6; s0.cflgv = 0.5;
+    INIT_CK(cudaMemcpy(ctx->st, &s0, sizeof(DevState), cudaMemcpyHostToDevice));
+    rc = configure_kernels(ctx);
+    if (rc != CHAPSIM_OK) {
+        g_init_error = ctx->err;
+        chapsim_gpu_finalize(ctx);
+        return rc;
+    }
+#undef INIT_CK
+    *out = ctx;
+    return CHAPSIM_OK;
+}
+
+void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
+    cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
+    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red);
+    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
+    if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* chapsim_last_error_string(const chapsim_ctx_t* ctx) {
+    return ctx ? ctx->err.c_str() : g_init_error.c_str();
+}
+
+int chapsim_upload_fields(chapsim_ctx_t* ctx, const double* q, const double* pr, const double* convh0) {
+    if (!ctx || !q || !pr) return fail(ctx, CHAPSIM_ERR_BADARG, "null field");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    CK(cudaMemcpyAsync(ctx->Q, q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->PR, pr, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (convh0)
+        CK(cudaMemcpyAsync(ctx->H0, convh0, (size_t)(3 * g.FI) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    else
+        CK(cudaMemsetAsync(ctx->H0, 0, (size_t)(3 * g.FI) * sizeof(double), ctx->stream));
+    k_bc_fields<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->PR);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_download_fields(chapsim_ctx_t* ctx, double* q, double* pr, double* convh0) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    if (q) CK(cudaMemcpyAsync(q, ctx->Q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (pr) CK(cudaMemcpyAsync(pr, ctx->PR, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (convh0)
+        CK(cudaMemcpyAsync(convh0, ctx->H0, (size_t)(3 * g.FI) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_set_dt(chapsim_ctx_t* ctx, double dt) {
+    if (!ctx || !(dt > 0.0)) return fail(ctx, CHAPSIM_ERR_BADARG, "dt must be positive");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(&ctx->st->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_get_dt(chapsim_ctx_t* ctx, double* dt) {
+    if (!ctx || !dt) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *dt = ctx->st_host->dt;
+    return CHAPSIM_OK;
+}
+
+int chapsim_cfl_tg(chapsim_ctx_t* ctx, double* cflmm) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    launch_cfl_dt(ctx, 0);
+    CK(cudaGetLastError());
+    int rc = check_device_error(ctx);
+    if (cflmm) *cflmm = ctx->st_host->cflmm;
+    return rc;
+}
+
+static int set_step_params(chapsim_ctx_t* ctx, double dt0, double dtmin, double cflgv) {
+    if (!(dt0 > 0.0) || !(dtmin > 0.0) || !(cflgv > 0.0)) return fail(ctx, CHAPSIM_ERR_BADARG, "dt0, dtmin, cflgv must be positive");
+    double p[3] = {dt0, dtmin, cflgv};
+    CK(cudaMemcpyAsync(&ctx->st->dt0, p, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_step_begin(chapsim_ctx_t* ctx, double dt0, double dtmin, double cflgv, double* dt_out, double* cfl_out) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = set_step_params(ctx, dt0, dtmin, cflgv);
+    if (rc) return rc;
+    launch_cfl_dt(ctx, 1);
+    CK(cudaGetLastError());
+    rc = check_device_error(ctx);
+    if (dt_out) *dt_out = ctx->st_host->dt;
+    if (cfl_out) *cfl_out = ctx->st_host->cflmm;
+    return rc;
+}
+
+int chapsim_rk_substep_tg(chapsim_ctx_t* ctx, int32_t ns) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (ns < 0 || ns > 3) return fail(ctx, CHAPSIM_ERR_BADARG, "NS must be 0..3");
+    CK(cudaSetDevice(ctx->device));
+    launch_substep(ctx, ns);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_advance_tg(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, double* dt_out,
+                       double* cfl_out) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (nsteps < 0) return fail(ctx, CHAPSIM_ERR_BADARG, "nsteps < 0");
+    CK(cudaSetDevice(ctx->device));
+    int rc = set_step_params(ctx, dt0, dtmin, cflgv);
+    if (rc) return rc;
+    rc = build_step_graph(ctx);
+    if (rc) return rc;
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaGraphLaunch(ctx->step_exec, ctx->stream));
+        ctx->launches += (unsigned long long)ctx->kernels_per_step;
+    }
+    CK(cudaGetLastError());
+    rc = check_device_error(ctx);
+    if (dt_out) *dt_out = ctx->st_host->dt;
+    if (cfl_out) *cfl_out = ctx->st_host->cflmm;
+    return rc;
+}
+
+int chapsim_divgck_tg(chapsim_ctx_t* ctx, double* maxdiv) {
+    if (!ctx || !maxdiv) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    k_divgck<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(ctx->g, ctx->Q, ctx->part_red);
+    k_maxdiv_final<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *maxdiv = ctx->st_host->maxdiv;
+    return CHAPSIM_OK;
+}
+
+int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph) {
+    if (!ctx || !rhs || !dph) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    // the divergence kernel is bypassed: RHSLLPHI is uploaded and packed by a
+    // copy of the x-transform path that reads it instead of Q
+    CK(cudaMemcpyAsync(ctx->RHSLL, rhs, (size_t)g.FI * sizeof(double), cudaMemcpyHostToDevice, s));
+    dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
+    k_fftx_from_rhs<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->RHSLL, ctx->SP);
+    const long long nq = (long long)g.LH * g.M;
+    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
+    k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    const long long nl = (long long)g.LH * g.N;
+    k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, s>>>(g, ctx->SP, ctx->HS);
+    k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
+    ctx->launches += 5;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dph, ctx->DPH, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return CHAPSIM_OK;
+}
+
+int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, float* ms,
+                          int32_t nslots) {
+    // One step = 2 + 3*9 kernels launched individually with an event after
+    // each; ms[slot] accumulates the duration of kernel slot `slot` over the
+    // nsteps steps (slot 0 is timed from an event recorded before it).
+    const int per = 2 + 3 * 9;
+    if (!ctx || !ms || nslots < per || nsteps < 1) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = set_step_params(ctx, dt0, dtmin, cflgv);
+    if (rc) return rc;
+    std::vector<cudaEvent_t> ev(per + 1);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    for (int i = 0; i < per; ++i) ms[i] = 0.0f;
+    for (int s = 0; s < nsteps; ++s) {
+        CK(cudaEventRecord(ev[0], ctx->stream));
+        ctx->prof_ev = ev.data() + 1;
+        ctx->prof_n = 0;
+        launch_cfl_dt(ctx, 1);
+        for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns);
+        ctx->prof_ev = nullptr;
+        CK(cudaGetLastError());
+        CK(cudaEventSynchronize(ev[per]));
+        for (int i = 0; i < per; ++i) {
+            float t = 0.0f;
+            CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+            ms[i] += t;
+        }
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return check_device_error(ctx);
+}
+
+int chapsim_get_stream(chapsim_ctx_t* ctx, void** stream) {
+    if (!ctx || !stream) return CHAPSIM_ERR_BADARG;
+    *stream = (void*)ctx->stream;
+    return CHAPSIM_OK;
+}
+
+int chapsim_sync(chapsim_ctx_t* ctx) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count) {
+    if (!ctx || !count) return CHAPSIM_ERR_BADARG;
+    *count = ctx->launches;
+    return CHAPSIM_OK;
+}
+
+int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count) {
+    if (!ctx || !count) return CHAPSIM_ERR_BADARG;
+    int per = 2 + 3 * 9;
+    *count = per;
+    return CHAPSIM_OK;
+}
+
+}  // extern "C"
+
+static int run_lines(const double* a, const double* b, const double* c, double* r, const double* bcj, int nlines,
+                     long long ls, long long es, int n, bool cyclic) {
+    chapsim_ctx* ctx = nullptr;
+    if (!a || !b || !c || !r || nlines <= 0 || n < 3) return fail(nullptr, CHAPSIM_ERR_BADARG, "bad tridiagonal arguments");
+    const size_t tot = (size_t)nlines * (size_t)n;
+    double *da = nullptr, *db = nullptr, *dc = nullptr, *dr = nullptr, *dbc = nullptr, *wk = nullptr;
+    auto cleanup = [&]() { cudaFree(da); cudaFree(db); cudaFree(dc); cudaFree(dr); cudaFree(dbc); cudaFree(wk); };
+#define LCK(call)                                                                   \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) { cleanup(); return fail(nullptr, CHAPSIM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); } \
+    } while (0)
+    LCK(cudaMalloc(&da, tot * 8)); LCK(cudaMalloc(&db, tot * 8)); LCK(cudaMalloc(&dc, tot * 8)); LCK(cudaMalloc(&dr, tot * 8));
+    LCK(cudaMemcpy(da, a, tot * 8, cudaMemcpyHostToDevice));
+    LCK(cudaMemcpy(db, b, tot * 8, cudaMemcpyHostToDevice));
+    LCK(cudaMemcpy(dc, c, tot * 8, cudaMemcpyHostToDevice));
+    LCK(cudaMemcpy(dr, r, tot * 8, cudaMemcpyHostToDevice));
+    if (bcj) {
+        LCK(cudaMalloc(&dbc, (size_t)2 * nlines * 8));
+        LCK(cudaMemcpy(dbc, bcj, (size_t)2 * nlines * 8, cudaMemcpyHostToDevice));
+    }
+    const int S = n / 32;
+    if (n % 32 == 0 && valid_S(S)) {
+        const int nt = 256, nb = (int)(((long long)nlines * 32 + nt - 1) / nt);
+        if (cyclic) { DISPATCH_S(S, (k_tdma_lines<S, true><<<nb, nt>>>(da, db, dc, dr, dbc, nlines, ls, es, n))); }
+        else { DISPATCH_S(S, (k_tdma_lines<S, false><<<nb, nt>>>(da, db, dc, dr, dbc, nlines, ls, es, n))); }
+    } else {
+        LCK(cudaMalloc(&wk, (size_t)nlines * 3 * n * 8));
+        k_tdma_seq<<<(nlines + 127) / 128, 128>>>(da, db, dc, dr, dbc, wk, nlines, ls, es, n, cyclic ? 1 : 0);
+    }
+    LCK(cudaGetLastError());
+    LCK(cudaMemcpy(r, dr, tot * 8, cudaMemcpyDeviceToHost));
+    cleanup();
+#undef LCK
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_tdmaiji_cyc(const double* a, const double* b, const double* c, double* r, int32_t isz, int32_t jsz) {
+    // lines along I (contiguous), one per J
+    return run_lines(a, b, c, r, nullptr, jsz, isz, 1, isz, true);
+}
+
+extern "C" int chapsim_tdmaijj_noncyc(const double* a, const double* b, const double* c, double* r, const double* bcj,
+                                      int32_t jsz, int32_t isz) {
+    // lines along J (stride ISZ), one per I
+    return run_lines(a, b, c, r, bcj, isz, 1, isz, jsz, false);
+}

@@ -1,0 +1,103 @@
+// Common definitions for the CHAPSim periodic-channel (TG) step on sm_100a.
+//
+// Field layout in HBM is the reference's Fortran layout, so that the C ABI
+// uploads and downloads the host arrays with one contiguous copy each:
+//   F(i, j, k): i = 0..L-1 (x, fastest), j = 0..M+1 (y; 0 and M+1 are the
+//   wall ghost planes, 1..M interior), k = 0..N-1 (z).
+//   offset = i + L * (j + (M + 2) * k)      ("padded" fields: Q, PR, DPH)
+// Work arrays without ghosts (RHS, CONVH0, RHSLLPHI) use
+//   offset = i + L * ((j - 1) + M * k)      ("interior" fields).
+// Spectral array of the Poisson solve (kx = 0..L/2, y row j, kz):
+//   offset = kx + LH * ((j - 1) + M * kz),  LH = L/2 + 1, complex double2.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CHS_WARP 32
+
+// error bits written by kernels into DevState::err
+#define CHS_EBIT_NAN 1u
+#define CHS_EBIT_DT_COLLAPSE 2u
+
+struct DevState {
+    double dt;       // current DT (BCAST_COMM_STEP)
+    double dt0;      // DT0
+    double dtmin;    // DTMIN
+    double cflgv;    // CFLGV
+    double cflmm;    // last CFL maximum
+    double maxdiv;   // last DIVGCK result
+    unsigned int err;
+    unsigned int pad;
+};
+
+// Geometry and constant coefficients of one channel (passed by value).
+struct Geo {
+    int L, M, N, LH;
+    long long P;    // L*(M+2): k-plane stride of padded fields
+    long long FS;   // P*N: size of one padded field
+    long long PI_;  // L*M: k-plane stride of interior fields
+    long long FI;   // L*M*N: size of one interior field
+    double dxi, dzi, dxqi, dzqi, cvisc, volm, cf_given;
+    int iflowdriven;
+    int fix_v_wall_row;
+    // y-direction arrays, indexed by the reference's 1-based j (entry 0 unused)
+    const double* dyfi;  // [M+2]
+    const double* dyci;  // [M+2]
+    const double* wff;   // [M+2]
+    const double* wfb;   // [M+2]
+    const double* amph;  // [M+2]
+    const double* acph;
+    const double* apph;
+    const double* amvr;  // [3][M+2]
+    const double* acvr;
+    const double* apvr;
+    const double* ak1;   // [L]  modified wavenumbers in x, 0-based kx
+    const double* ak3;   // [N]  modified wavenumbers in z, 0-based kz
+    double tgam[4], troh[4], talp[4];
+    // FFT plans
+    const double2* twx;  // [L] exp(-2 pi i e / L)
+    const double2* twz;  // [N]
+    const int* permx;    // [L] digit-reversal permutation for the in-place DIT
+    const int* permz;    // [N]
+    int radx[8], nradx;
+    int radz[8], nradz;
+};
+
+__device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {
+    return (long long)i + (long long)g.L * ((long long)j + (long long)(g.M + 2) * (long long)k);
+}
+__device__ __forceinline__ long long iidx(const Geo& g, int i, int j, int k) {
+    return (long long)i + (long long)g.L * ((long long)(j - 1) + (long long)g.M * (long long)k);
+}
+__device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
+__device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
+
+// Deterministic block reduction (fixed tree order) of one double per thread.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sbuf) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sbuf[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x < 32) {
+        r = (l < NT / 32) ? sbuf[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    return r;  // valid in thread 0
+}
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* sbuf) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sbuf[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x < 32) {
+        r = (l < NT / 32) ? sbuf[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
+    }
+    return r;
+}

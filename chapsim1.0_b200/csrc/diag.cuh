@@ -1,0 +1,95 @@
+// Step control and diagnostics:
+//   k_cfl        CFL_tg (src/CFL.f90:13-52): per-block maxima of
+//                0.5*(|(u_i+u_i+1) DXI| + |(v_j+v_j+1) DYFI| + |(w_k+w_k+1) DZI|)
+//   k_dt         BCAST_COMM_STEP (src/SOLVE.f90:154-211):
+//                DT = max(min(DT0, 5 DT, CFLGV/CFLMM), DTMIN); flags DT/DT0 < 0.01
+//   k_divgck     DIVGCK_tg (src/DIVGCK.f90:15-55): max |div u|
+//   k_bc_fields  BC_WALL_Q_tg / BC_WALL_PR_tg ghost planes (src/BC_WALL.f90:212-361)
+#pragma once
+#include "common.cuh"
+
+#define DG_NT 256
+
+__global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const double* __restrict__ Q, double* __restrict__ partial,
+                                               DevState* __restrict__ st) {
+    __shared__ double sred[32];
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * M * N;
+    double mx = 0.0;
+    bool bad = false;
+    for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
+        const int i = (int)(t % L);
+        const long long r = t / L;
+        const int j = 1 + (int)(r % M);
+        const int k = (int)(r / M);
+        const long long c = pidx(g, i, j, k);
+        const double q = (fabs((Q[c] + Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
+                          fabs((Q[c + g.FS] + Q[c + g.FS + g.L]) * g.dyfi[j] * 1.0) +
+                          fabs((Q[c + 2 * g.FS] + Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
+        if (!(q == q)) bad = true;
+        mx = fmax(mx, q);
+    }
+    if (bad) atomicOr(&st->err, CHS_EBIT_NAN);
+    double r = block_max<DG_NT>(mx, sred);
+    if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+__global__ void __launch_bounds__(DG_NT) k_dt(const double* __restrict__ partial, int np, DevState* __restrict__ st,
+                                              int update_dt) {
+    __shared__ double sred[32];
+    double mx = 0.0;
+    for (int t = threadIdx.x; t < np; t += DG_NT) mx = fmax(mx, partial[t]);
+    double c = block_max<DG_NT>(mx, sred);
+    if (threadIdx.x == 0) {
+        st->cflmm = c;
+        if (update_dt) {
+            double dt = fmin(fmin(st->dt0, 5.0 * st->dt), st->cflgv / c);
+            dt = fmax(dt, st->dtmin);
+            st->dt = dt;
+            if ((dt / st->dt0) < 0.01) atomicOr(&st->err, CHS_EBIT_DT_COLLAPSE);
+            if (!(dt == dt)) atomicOr(&st->err, CHS_EBIT_NAN);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(DG_NT) k_divgck(Geo g, const double* __restrict__ Q, double* __restrict__ partial) {
+    __shared__ double sred[32];
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * M * N;
+    double mx = 0.0;
+    for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
+        const int i = (int)(t % L);
+        const long long r = t / L;
+        const int j = 1 + (int)(r % M);
+        const int k = (int)(r / M);
+        const long long c = pidx(g, i, j, k);
+        const double d = (Q[pidx(g, wrapp(i, L), j, k)] - Q[c]) * g.dxi + (Q[c + g.FS + g.L] - Q[c + g.FS]) * g.dyfi[j] * 1.0 +
+                         (Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - Q[c + 2 * g.FS]) * g.dzi * 1.0;
+        mx = fmax(fabs(d), mx);
+    }
+    double r = block_max<DG_NT>(mx, sred);
+    if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}
+
+__global__ void k_maxdiv_final(const double* __restrict__ partial, int np, DevState* __restrict__ st) {
+    __shared__ double sred[32];
+    double mx = 0.0;
+    for (int t = threadIdx.x; t < np; t += DG_NT) mx = fmax(mx, partial[t]);
+    double c = block_max<DG_NT>(mx, sred);
+    if (threadIdx.x == 0) st->maxdiv = c;
+}
+
+// Wall ghost planes after an upload: u = w = 0 at j = 0, M+1; v = 0 at
+// j = 0, 1, M+1; PR zero-gradient.
+__global__ void __launch_bounds__(DG_NT) k_bc_fields(Geo g, double* __restrict__ Q, double* __restrict__ PR) {
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * N;
+    for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
+        const int i = (int)(t % L), k = (int)(t / L);
+        const long long b0 = pidx(g, i, 0, k), b1 = pidx(g, i, 1, k), bm = pidx(g, i, M, k), bt = pidx(g, i, M + 1, k);
+        Q[bt] = 0.0; Q[bt + 2 * g.FS] = 0.0; Q[bt + g.FS] = 0.0;
+        Q[b0] = 0.0; Q[b0 + 2 * g.FS] = 0.0; Q[b1 + g.FS] = 0.0; Q[b0 + g.FS] = 0.0;
+        PR[bt] = PR[bm];
+        PR[b0] = PR[b1];
+    }
+}

@@ -1,0 +1,203 @@
+// Pressure Poisson solve and projection of one RK3 substep:
+//   DIVG_tg (src/DIVG.f90:15-51), FFT99_POIS3D_periodicxz
+//   (src/possion3d_FFT99.f90:271-505), VELOUPDT_tg
+//   (src/VELO_CORRECTION.f90:14-100), PRCALC_tg
+//   (src/PRESSURE_CORRECTION.f90:15-99) and the wall ghosts of
+//   BC_WALL_PR_tg (src/BC_WALL.f90:293-361).
+//
+// Kernels:
+//   k_div_fftx   divergence of u* / (alpha dt) -> RHSLLPHI, then the real
+//                x transform of every (j, k) line (two real lines packed in
+//                one complex FFT), times 1/L, into the spectral array
+//   k_fftz<S>    complex z transform of every (kx, j) line; forward pass
+//                multiplies by 1/N (UN3M)
+//   k_ysolve     per (kx, kz) tridiagonal solve in y with diagonal
+//                ACPH(j) - AK1(kx) - AK3(kz), the reference's Thomas
+//                recurrence, zero mode pinned as in TDMA_PHI_COEF (:225-231)
+//                and :341-344, :387-389 (phi_hat(0,y_1,0) = 0)
+//   k_fftx_inv   inverse x transform -> DPH
+//   k_correct    velocity correction, pressure update, PR wall ghosts
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+
+#define PX_TJ 8   // x-lines per block (4 packed pairs)
+#define PX_NT 256
+#define FZ_TQ 16  // z-lines per block
+#define FZ_NT 256
+#define YS_NT 128
+#define CR_NT 256
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const double* __restrict__ Q, double* __restrict__ RHSLL,
+                                                    double2* __restrict__ SP, const DevState* __restrict__ st, int ns) {
+    extern __shared__ double2 smc[];
+    const int L = g.L, M = g.M, N = g.N, LH = g.LH;
+    const int j0 = 1 + blockIdx.x * PX_TJ;
+    const int k = blockIdx.y;
+    const int nj = min(PX_TJ, M - j0 + 1);
+    const int np = (nj + 1) >> 1;
+    const int kp = wrapp(k, N);
+    const double coe0 = 1.0 / (st->dt * g.talp[ns]);
+    const double* U = Q;
+    const double* V = Q + g.FS;
+    const double* W = Q + 2 * g.FS;
+    for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
+        const int jl = p / L, i = p - jl * L;
+        const int pair = jl >> 1, part = jl & 1;
+        double val = 0.0;
+        if (jl < nj) {
+            const int j = j0 + jl;
+            const int ip = wrapp(i, L);
+            const double coe1 = g.dxi / 1.0;
+            const double coe2 = g.dyfi[j] / 1.0;
+            const long long c = pidx(g, i, j, k);
+            const double dv = (U[pidx(g, ip, j, k)] - U[c]) * coe1 + (V[pidx(g, i, j + 1, k)] - V[c]) * coe2 +
+                              (W[pidx(g, i, j, kp)] - W[c]) * g.dzi;
+            val = dv * coe0;
+            RHSLL[iidx(g, i, j, k)] = val;
+        }
+        double2* line = smc + pair * L;
+        const int pos = g.permx[i];
+        if (part == 0) line[pos].x = val; else line[pos].y = val;
+    }
+    block_fft<-1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    // unpack: A_k = (Z_k + conj Z_{L-k}) / 2, B_k = (Z_k - conj Z_{L-k}) / (2i), both times 1/L
+    const double sc = 0.5 / (double)L;
+    for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
+        const int pair = p / LH, kx = p - pair * LH;
+        const double2* line = smc + pair * L;
+        const double2 z = line[kx];
+        const double2 zc = line[kx == 0 ? 0 : L - kx];
+        const double2 a = make_double2((z.x + zc.x) * sc, (z.y - zc.y) * sc);
+        const double2 b = make_double2((z.y + zc.y) * sc, (zc.x - z.x) * sc);
+        const int ja = j0 + 2 * pair;
+        SP[kx + (long long)LH * ((ja - 1) + (long long)M * k)] = a;
+        if (2 * pair + 1 < nj) SP[kx + (long long)LH * ((ja) + (long long)M * k)] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// complex z transform of FZ_TQ consecutive (kx, j) lines (index q = kx + LH*(j-1))
+template <int SIGN>
+__global__ void __launch_bounds__(FZ_NT) k_fftz(Geo g, double2* __restrict__ SP) {
+    extern __shared__ double2 smc[];
+    const int N = g.N;
+    const long long Q = (long long)g.LH * g.M;
+    const long long q0 = (long long)blockIdx.x * FZ_TQ;
+    const int nq = (int)min((long long)FZ_TQ, Q - q0);
+    for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
+        const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
+        if (ql < nq) smc[ql * (N + 1) + g.permz[kz]] = SP[q0 + ql + Q * kz];
+    }
+    block_fft<SIGN>(smc, N, nq, N + 1, g.twz, g.radz, g.nradz);
+    const double sc = SIGN < 0 ? 1.0 / (double)N : 1.0;
+    for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
+        const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
+        if (ql < nq) {
+            double2 v = smc[ql * (N + 1) + kz];
+            if (SIGN < 0) { v.x = v.x * sc; v.y = v.y * sc; }
+            SP[q0 + ql + Q * kz] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// y solve per (kx, kz): TDMAIJJ_nonCYC with AMPH, ACPH - AK1 - AK3, APPH.
+// HS is scratch of LH*M*N doubles for the forward-elimination factors.
+__global__ void __launch_bounds__(YS_NT) k_ysolve(Geo g, double2* __restrict__ SP, double* __restrict__ HS) {
+    const int M = g.M, LH = g.LH;
+    const long long nl = (long long)LH * g.N;
+    const long long t = (long long)blockIdx.x * YS_NT + threadIdx.x;
+    if (t >= nl) return;
+    const int kz = (int)(t / LH), kx = (int)(t - (long long)kz * LH);
+    const long long js = LH;  // stride between y rows
+    double2* s = SP + kx + (long long)LH * (long long)M * kz;
+    double* h = HS + kx + (long long)LH * (long long)M * kz;
+    const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+    const bool zero = (kx == 0 && kz == 0);
+    // row 1 (j = 1)
+    double b = g.acph[1] + shift;
+    double c = zero ? 0.0 : g.apph[1];
+    double2 r = s[0];
+    if (zero) r = make_double2(0.0, 0.0);
+    double hp = c / b;
+    double2 gp = make_double2(r.x / b, r.y / b);
+    h[0] = hp;
+    s[0] = gp;
+    for (int j = 2; j <= M; ++j) {
+        const double a = g.amph[j];
+        const double bj = g.acph[j] + shift;
+        const double pp = 1.0 / (bj - hp * a);
+        const double2 rj = s[(j - 1) * js];
+        gp = make_double2((rj.x - a * gp.x) * pp, (rj.y - a * gp.y) * pp);
+        if (j < M) {
+            hp = g.apph[j] * pp;
+            h[(j - 1) * js] = hp;
+        }
+        s[(j - 1) * js] = gp;
+    }
+    double2 xn = gp;
+    for (int j = M - 1; j >= 1; --j) {
+        const double hj = h[(j - 1) * js];
+        const double2 gj = s[(j - 1) * js];
+        xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
+        s[(j - 1) * js] = xn;
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(PX_NT) k_fftx_inv(Geo g, const double2* __restrict__ SP, double* __restrict__ DPH) {
+    extern __shared__ double2 smc[];
+    const int L = g.L, M = g.M, LH = g.LH;
+    const int j0 = 1 + blockIdx.x * PX_TJ;
+    const int k = blockIdx.y;
+    const int nj = min(PX_TJ, M - j0 + 1);
+    const int np = (nj + 1) >> 1;
+    // Z_k = A_k + i B_k with A_{L-k} = conj A_k; imaginary parts of the k = 0 and
+    // k = L/2 coefficients are dropped, as FFT99 does for ISIGN = +1.
+    for (int p = threadIdx.x; p < np * L; p += PX_NT) {
+        const int pair = p / L, kk = p - pair * L;
+        const int ja = j0 + 2 * pair;
+        const bool hasb = 2 * pair + 1 < nj;
+        const int ks = kk <= L / 2 ? kk : L - kk;
+        double2 a = SP[ks + (long long)LH * ((ja - 1) + (long long)M * k)];
+        double2 b = hasb ? SP[ks + (long long)LH * ((ja) + (long long)M * k)] : make_double2(0.0, 0.0);
+        if (ks == 0 || 2 * ks == L) { a.y = 0.0; b.y = 0.0; }
+        if (kk > L / 2) { a.y = -a.y; b.y = -b.y; }
+        smc[pair * L + g.permx[kk]] = make_double2(a.x - b.y, a.y + b.x);
+    }
+    block_fft<+1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
+        const int jl = p / L, i = p - jl * L;
+        if (jl >= nj) continue;
+        const double2 z = smc[(jl >> 1) * L + i];
+        DPH[pidx(g, i, j0 + jl, k)] = (jl & 1) ? z.y : z.x;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// VELOUPDT_tg + PRCALC_tg + BC_WALL_PR_tg (Q walls are never written)
+__global__ void __launch_bounds__(CR_NT) k_correct(Geo g, double* __restrict__ Q, double* __restrict__ PR,
+                                                   const double* __restrict__ DPH, const double* __restrict__ RHSLL,
+                                                   const DevState* __restrict__ st, int ns) {
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * M * N;
+    const long long t = (long long)blockIdx.x * CR_NT + threadIdx.x;
+    if (t >= tot) return;
+    const int i = (int)(t % L);
+    const long long r = t / L;
+    const int j = 1 + (int)(r % M);
+    const int k = (int)(r / M);
+    const double dt = st->dt, ta = g.talp[ns];
+    const long long c = pidx(g, i, j, k);
+    const double ph = DPH[c];
+    Q[c] = Q[c] - (ph - DPH[pidx(g, wrapm(i, L), j, k)]) * (dt * ta * g.dxi);
+    Q[c + 2 * g.FS] = Q[c + 2 * g.FS] - (ph - DPH[pidx(g, i, j, wrapm(k, N))]) * (dt * ta * g.dzi);
+    if (j >= 2) Q[c + g.FS] = Q[c + g.FS] - (ph - DPH[pidx(g, i, j - 1, k)]) * (dt * ta * g.dyci[j] / 1.0);
+    const double be = 0.5 * ta * dt * g.cvisc * 1.0 / 1.0;
+    const double pn = PR[c] + ph - be * RHSLL[iidx(g, i, j, k)];
+    PR[c] = pn;
+    if (j == 1) PR[pidx(g, i, 0, k)] = pn;
+    if (j == M) PR[pidx(g, i, M + 1, k)] = pn;
+}

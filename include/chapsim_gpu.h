@@ -1,0 +1,160 @@
+/*
+ * chapsim_gpu.h -- C ABI of the B200 implementation of CHAPSim's
+ * fractional-step time step for the periodic plane channel (TG domain).
+ *
+ * The Fortran host (CHAPSim's driver, readdata.ini parser and file I/O)
+ * stays unchanged; its subroutine bodies call these entry points through an
+ * ISO_C_BINDING shim.  All arguments are plain C types:
+ * array arguments are host pointers to Fortran-ordered FP64 arrays with the
+ * reference's shapes, copied with one contiguous transfer each.
+ *
+ * Every entry point returns CHAPSIM_OK (0) or a negative error code; the
+ * shim maps a nonzero code to CALL ERRHDL(msg, MYID) (src/WRTHDL.f90:48-63),
+ * which keeps the reference's "log + STOP" behaviour.
+ */
+#ifndef CHAPSIM_GPU_H
+#define CHAPSIM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHAPSIM_OK 0
+#define CHAPSIM_ERR_CUDA (-1)        /* a CUDA call failed */
+#define CHAPSIM_ERR_NAN (-2)         /* non-finite velocity or dt */
+#define CHAPSIM_ERR_DT_COLLAPSE (-3) /* DT/DT0 < 0.01: src/SOLVE.f90:199-207 dumps and STOPs */
+#define CHAPSIM_ERR_TABLE_RANGE (-4) /* reserved: property table out of range */
+#define CHAPSIM_ERR_TIMEOUT (-5)     /* reserved: bounded device wait expired */
+#define CHAPSIM_ERR_BADARG (-6)      /* invalid argument or unsupported grid */
+#define CHAPSIM_ERR_NOMEM (-7)       /* device allocation failed */
+
+typedef struct chapsim_ctx chapsim_ctx_t;
+
+/* Grid: NCL1_tg, NCL2, NCL3 of src/modules.f90 (mesh_info).  Only the plane
+ * channel (iCase = 1) in the periodic TG domain (iDomain = 1) is accepted.
+ * L and N must factor into 2s and 3s (FFT lengths), L, M, N must be
+ * multiples of 32 between 32 and 384. */
+typedef struct {
+    int32_t ncl1;   /* L */
+    int32_t ncl2;   /* M */
+    int32_t ncl3;   /* N */
+    int32_t icase;  /* must be 1 (ICHANL) */
+    int32_t idomain;/* must be 1 (ITG)    */
+} chapsim_grid_t;
+
+/* Coefficients computed by the host's set-up routines, passed unchanged.
+ * y-arrays are 1-based in Fortran; here element [j-1] holds A(j). */
+typedef struct {
+    double dxi, dzi, dxqi, dzqi; /* CONSPARA (src/CONSPARA.f90:54-73)            */
+    double cvisc;                /* CVISC = 1/REN (src/SOLVE.f90:168)            */
+    double volm;                 /* VOLM_tg (src/COORDJR.f90:372-381)            */
+    double cf_given;             /* Cf_Given (readdata.ini [fluid])              */
+    int32_t iflowdriven;         /* 1 constant mass flux, 2 constant Cf          */
+    int32_t pad0;
+    const double* dyfi;          /* DYFI(1:NCL2)                                 */
+    const double* dyci;          /* DYCI(1:NND2)                                 */
+    const double* ycl2nd_wff;    /* YCL2ND_WFF(1:NND2)                           */
+    const double* ycl2nd_wfb;    /* YCL2ND_WFB(1:NND2)                           */
+    const double* amph;          /* AMPH(1:NCL2) (src/TDMA_COEF.f90:44-65)       */
+    const double* acph;          /* ACPH(1:NCL2)                                 */
+    const double* apph;          /* APPH(1:NCL2)                                 */
+    const double* amvr;          /* AMVR(1:NND2, 1:3), Fortran order             */
+    const double* acvr;          /* ACVR(1:NND2, 1:3)                            */
+    const double* apvr;          /* APVR(1:NND2, 1:3)                            */
+    const double* ak1;           /* AK1(1:NCL1) (src/possion3d_FFT99.f90:180-198)*/
+    const double* ak3;           /* AK3(1:NCL3)                                  */
+    double tgam[4], troh[4], talp[4]; /* CONS_RKCOEF (src/CONS_RKCOEF.f90:25-51) */
+} chapsim_coefs_t;
+
+typedef struct {
+    int32_t device;          /* CUDA device ordinal                            */
+    int32_t fix_v_wall_row;  /* 0: reproduce the reference (default), see DESIGN */
+    int32_t reserved[6];
+} chapsim_opts_t;
+
+/* Allocates the device fields and uploads coefficients.  Hooks in after
+ * FFT99_POIS3D_INIT (src/DNS_THERMAL.f90:118-130). */
+int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* coefs, const chapsim_opts_t* opts,
+                     chapsim_ctx_t** out);
+void chapsim_gpu_finalize(chapsim_ctx_t* ctx);
+const char* chapsim_last_error_string(const chapsim_ctx_t* ctx);
+
+/* Field transfer.  q: Q_tg(NCL1, 0:NCL2+1, NCL3, 3); pr: PR_tg(NCL1, 0:NCL2+1, NCL3);
+ * convh0: CONVH0_tg(NCL1, NCL2, NCL3, 3) or NULL (upload: zero; download: skipped).
+ * Upload also applies BC_WALL_Q_tg / BC_WALL_PR_tg to the ghost planes
+ * (src/BC_WALL.f90:212-361).  Called after the host writes a restart or
+ * initial field, and before any host consumer of the fields. */
+int chapsim_upload_fields(chapsim_ctx_t* ctx, const double* q, const double* pr, const double* convh0);
+int chapsim_download_fields(chapsim_ctx_t* ctx, double* q, double* pr, double* convh0);
+
+/* The module variable DT (src/modules.f90 init_info) as seen by the device. */
+int chapsim_set_dt(chapsim_ctx_t* ctx, double dt);
+int chapsim_get_dt(chapsim_ctx_t* ctx, double* dt);
+
+/* CFL_tg (src/CFL.f90:13-52): CFLMM_tg of the resident velocity. */
+int chapsim_cfl_tg(chapsim_ctx_t* ctx, double* cflmm);
+
+/* CFL_tg + the dt rule of BCAST_COMM_STEP (src/SOLVE.f90:79-94,154-211):
+ * DT = max(min(DT0, 5*DT, CFLGV/CFLMM), DTMIN) on the device; returns
+ * CHAPSIM_ERR_DT_COLLAPSE when DT/DT0 < 0.01. */
+int chapsim_step_begin(chapsim_ctx_t* ctx, double dt0, double dtmin, double cflgv, double* dt_out,
+                       double* cfl_out);
+
+/* SOLVERRK3_MOM_tg(NS) (src/SOLVERRK3_MOM_tg.f90:13-56), NS = 0..3, with
+ * the device-resident DT.  NS = 0 is the initial projection step of
+ * CALC_INITIALIZATION_tg (src/INITIAL_FL_FLD_TG.f90:109-139). */
+int chapsim_rk_substep_tg(chapsim_ctx_t* ctx, int32_t ns);
+
+/* nsteps iterations of the SOLVE loop body (src/SOLVE.f90:75-134) without
+ * post-processing: CFL, dt rule and the three RK substeps, replayed as one
+ * captured CUDA graph per step with dt kept on the device.  dt_out and
+ * cfl_out (may be NULL) receive the values of the last step. */
+int chapsim_advance_tg(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, double* dt_out,
+                       double* cfl_out);
+
+/* DIVGCK_tg (src/DIVGCK.f90:15-55): max |div u| of the resident velocity. */
+int chapsim_divgck_tg(chapsim_ctx_t* ctx, double* maxdiv);
+
+/* FFT99_POIS3D_periodicxz(ITG) (src/possion3d_FFT99.f90:271-505) on host
+ * arrays: rhs = RHSLLPHI_tg(NCL1, NCL2, NCL3), dph = DPH_tg(NCL1, 0:NCL2+1,
+ * NCL3) (rows 1..NCL2 written). */
+int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph);
+
+/* TDMAIJI_CYC(A,B,C,R,1,ISZ,1,JSZ) (src/TDMAIJI_CYC.f90:67): cyclic
+ * tridiagonal systems along the first index of (ISZ, JSZ) arrays; R is
+ * overwritten with the solution.  Host arrays. */
+int chapsim_tdmaiji_cyc(const double* a, const double* b, const double* c, double* r, int32_t isz, int32_t jsz);
+
+/* TDMAIJJ_nonCYC(A,B,C,R,BCJ,1,JSZ,1,ISZ) (src/TDMAIJJ_nonCYC.f90:67):
+ * systems along the second index of (ISZ, JSZ) arrays with Dirichlet values
+ * BCJ(ISZ, 2) (may be NULL for zero).  Host arrays. */
+int chapsim_tdmaijj_noncyc(const double* a, const double* b, const double* c, double* r, const double* bcj,
+                           int32_t jsz, int32_t isz);
+
+/* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
+ * with a CUDA event after every kernel; ms[slot] receives the summed
+ * duration of kernel slot `slot` of a step.  Slot order: k_cfl, k_dt, then
+ * for each substep k_rhs_xsweep, k_zsweep, k_ysweep, k_div_fftx, k_fftz_fwd,
+ * k_ysolve, k_fftz_inv, k_fftx_inv, k_correct (nslots >= 29). */
+int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, float* ms,
+                          int32_t nslots);
+
+/* The cudaStream_t (as void*) all of the context's work is queued on. */
+int chapsim_get_stream(chapsim_ctx_t* ctx, void** stream);
+
+/* Waits for all work queued on the context's stream. */
+int chapsim_sync(chapsim_ctx_t* ctx);
+
+/* Number of kernels this context has launched so far (graph replays count
+ * each kernel node). */
+int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count);
+
+/* Kernels launched per call of chapsim_advance_tg per step (for accounting). */
+int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHAPSIM_GPU_H */

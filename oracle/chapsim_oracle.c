@@ -1,0 +1,942 @@
+/*
+ * chapsim_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * FP64 CPU restatement of CHAPSim's fractional-step time step for the
+ * periodic ("TG", iDomain=1) plane channel (iCase=1).  It exists to check
+ * the CUDA path and to provide the timed CPU baseline; nothing in the product
+ * library links, loads or calls it.  Only tests/, the smoke check and the
+ * CPU-baseline leg of bench.py may use it.
+ *
+ * Every routine follows the Fortran subroutine named in its comment,
+ * statement by statement and in the same floating-point operation order,
+ * so that results agree with the reference to round-off.  Pinning: the
+ * setup stage (mesh, metrics, TDMA/Poisson coefficients, Poiseuille
+ * profile) is checked against the reference's own CHK_*.dat dumps of
+ * test_cases_template/TC8_Channel_IO_thermal_LiquidWater/0_log_monitors.
+ *
+ * Layout (identical to the reference and to the CUDA path):
+ *   field F(i, j, k), i = 1..L, j = 0..M+1 (ghosts at 0 and M+1), k = 1..N,
+ *   column-major, x fastest:  off = (i-1) + L*(j + (M+2)*(k-1)).
+ *   Q holds u, v, w as three consecutive such fields.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+    int L, M, N, NND2;
+    double HX, HZ, STR2, REN, CVISC;
+    int iFlowDriven;
+    double Cf_Given;
+    double DT, DT0, DTMIN, CFLGV, CFLMM;
+    /* CONSPARA */
+    double DX, DZ, DXI, DZI, DXQI, DZQI;
+    /* COORDJR (1-based, index 0 unused) */
+    double *YND, *YCC, *DYFI, *DYCI, *WFF, *WFB;
+    double Area_inlet, VOLM;
+    /* TDMA_COEF */
+    double *AMPH, *ACPH, *APPH;
+    double *AMVR[4], *ACVR[4], *APVR[4];
+    double AMVR1, APVRN;
+    /* LAMPOISLPROF */
+    double *Vini;
+    /* CONS_RKCOEF */
+    double TGAM[4], TROH[4], TALP[4];
+    /* FFT99_ROOT */
+    double *AK1, *AK3;
+    /* fields */
+    double *Q, *PR, *CONVH0;
+    double *QTMP, *DPH, *RHSLLPHI, *RHS;
+    /* Poisson spectral work (LH, M, N) */
+    double *SRe, *SIm;
+    int nthreads;
+    int fix_v_wall_row; /* 0: reproduce the reference (default) */
+} orc_t;
+
+#define FOFF(o, i, j, k) ((size_t)((i) - 1) + (size_t)(o)->L * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
+#define FSZ(o) ((size_t)(o)->L * (size_t)((o)->M + 2) * (size_t)(o)->N)
+#define QV(o, i, j, k, c) ((o)->Q[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+#define F3(a, o, i, j, k) ((a)[FOFF(o, i, j, k)])
+#define H0V(o, i, j, k, c) ((o)->CONVH0[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+
+static inline int IPV(const orc_t* o, int i) { return i == o->L ? 1 : i + 1; }
+static inline int IMV(const orc_t* o, int i) { return i == 1 ? o->L : i - 1; }
+static inline int KPV(const orc_t* o, int k) { return k == o->N ? 1 : k + 1; }
+static inline int KMV(const orc_t* o, int k) { return k == 1 ? o->N : k - 1; }
+
+static double* dalloc(size_t n) { return (double*)calloc(n ? n : 1, sizeof(double)); }
+
+/* ------------------------------------------------------------------ */
+/* Complex FFT (mixed radix, recursive).  Unnormalised:                  */
+/*   X[k] = sum_j x[j] exp(sign * 2*pi*i*j*k/n).                        */
+/* Only the discrete transform has to be reproduced to round-off; the   */
+/* Temperton FFT99/CFFT99 factorisation itself is not restated.         */
+/* ------------------------------------------------------------------ */
+typedef struct { double re, im; } cplx;
+
+static void fft_rec(int n, const cplx* in, int stride, cplx* out, int sign, const cplx* wtab, int wstride) {
+    if (n == 1) { out[0] = in[0]; return; }
+    int p;
+    if (n % 4 == 0 && n > 4) p = 4;
+    else if (n % 2 == 0) p = 2;
+    else if (n % 3 == 0) p = 3;
+    else if (n % 5 == 0) p = 5;
+    else p = n;
+    int m = n / p;
+    if (p == n) {
+        /* direct DFT */
+        for (int k = 0; k < n; ++k) {
+            double sr = 0, si = 0;
+            for (int j = 0; j < n; ++j) {
+                int e = (int)(((long)j * k) % n);
+                cplx w = wtab[(size_t)e * wstride];
+                double xr = in[(size_t)j * stride].re, xi = in[(size_t)j * stride].im;
+                sr += xr * w.re - xi * w.im;
+                si += xr * w.im + xi * w.re;
+            }
+            out[k].re = sr; out[k].im = si;
+        }
+        return;
+    }
+    for (int q = 0; q < p; ++q)
+        fft_rec(m, in + (size_t)q * stride, stride * p, out + (size_t)q * m, sign, wtab, wstride * p);
+    cplx tmp[8];
+    for (int k = 0; k < m; ++k) {
+        cplx t[8];
+        for (int q = 0; q < p; ++q) {
+            cplx a = out[(size_t)q * m + k];
+            cplx w = wtab[(size_t)((q * k) % n) * wstride];
+            t[q].re = a.re * w.re - a.im * w.im;
+            t[q].im = a.re * w.im + a.im * w.re;
+        }
+        for (int r = 0; r < p; ++r) {
+            double sr = 0, si = 0;
+            for (int q = 0; q < p; ++q) {
+                cplx w = wtab[(size_t)(((q * r * m) % n)) * wstride];
+                sr += t[q].re * w.re - t[q].im * w.im;
+                si += t[q].re * w.im + t[q].im * w.re;
+            }
+            tmp[r].re = sr; tmp[r].im = si;
+        }
+        for (int r = 0; r < p; ++r) out[(size_t)r * m + k] = tmp[r];
+    }
+}
+
+static cplx* fft_table(int n, int sign) {
+    cplx* w = (cplx*)malloc(sizeof(cplx) * (size_t)n);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < n; ++k) {
+        long double a = 2.0L * pi * (long double)k / (long double)n;
+        w[k].re = (double)cosl(a);
+        w[k].im = (double)(sign * sinl(a));
+    }
+    return w;
+}
+
+/* Exported for tests: in-place complex FFT of one line. */
+void orc_fft_complex(int n, double* re, double* im, int sign) {
+    cplx* in = (cplx*)malloc(sizeof(cplx) * (size_t)n);
+    cplx* out = (cplx*)malloc(sizeof(cplx) * (size_t)n);
+    cplx* w = fft_table(n, sign);
+    for (int j = 0; j < n; ++j) { in[j].re = re[j]; in[j].im = im[j]; }
+    fft_rec(n, in, 1, out, sign, w, 1);
+    for (int j = 0; j < n; ++j) { re[j] = out[j].re; im[j] = out[j].im; }
+    free(in); free(out); free(w);
+}
+
+/* ------------------------------------------------------------------ */
+/* Setup: CONSPARA (src/CONSPARA.f90:54-73), COORDJR (src/COORDJR.f90:  */
+/* 38-145), AREA_INOUTLET (:345-395), MESH_YWEIGHT_FACTORS (:416-442), */
+/* TDMA_COEF (src/TDMA_COEF.f90:44-110), LAMPOISLPROF                   */
+/* (src/LAMPOISLPROF.f90:17-60), CONS_RKCOEF (src/CONS_RKCOEF.f90:     */
+/* 25-51), FFT99_ROOT (src/possion3d_FFT99.f90:140-202).                */
+/* ------------------------------------------------------------------ */
+static void setup(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N, NND2 = M + 1;
+    const double PI = 2.0 * asin(1.0);
+    /* CONSPARA */
+    o->DX = o->HX / (double)L;
+    o->DXI = 1.0 / o->DX;
+    o->DXQI = o->DXI * o->DXI;
+    o->DZ = o->HZ / (double)N;
+    o->DZI = 1.0 / o->DZ;
+    o->DZQI = o->DZI * o->DZI;
+    o->CVISC = 1.0 / o->REN;
+    /* COORDJR, channel */
+    double COE1 = 0.5;
+    for (int J = 1; J <= NND2; ++J) {
+        double X2 = (double)(J - 1) / (double)(NND2 - 1);
+        o->YND[J] = tanh(o->STR2 * (X2 - COE1)) / tanh(o->STR2 * COE1);
+    }
+    for (int J = 1; J <= M; ++J) o->YCC[J] = (o->YND[J] + o->YND[J + 1]) * 0.5;
+    for (int J = 1; J <= M; ++J) o->DYFI[J] = 1.0 / (o->YND[J + 1] - o->YND[J]);
+    for (int J = 2; J <= NND2 - 1; ++J) o->DYCI[J] = 1.0 / ((o->YND[J + 1] - o->YND[J - 1]) * 0.5);
+    o->DYCI[1] = 2.0 / (o->YND[2] - o->YND[1]);
+    o->DYCI[NND2] = 2.0 / (o->YND[NND2] - o->YND[M]);
+    /* AREA_INOUTLET (RCCI1 = 1 for the channel) */
+    o->Area_inlet = 0.0;
+    for (int JC = 1; JC <= M; ++JC)
+        for (int KC = 1; KC <= N; ++KC) o->Area_inlet = o->Area_inlet + 1.0 / 1.0 / o->DYFI[JC] / o->DZI;
+    o->VOLM = 0.0;
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) o->VOLM = o->VOLM + 1.0 / 1.0 / o->DYFI[JC];
+    /* MESH_YWEIGHT_FACTORS */
+    for (int JC = 2; JC <= M; ++JC) {
+        int JM = JC - 1;
+        o->WFF[JC] = (o->YND[JC] - o->YCC[JM]) / (o->YCC[JC] - o->YCC[JM]);
+        o->WFB[JC] = (o->YCC[JC] - o->YND[JC]) / (o->YCC[JC] - o->YCC[JM]);
+    }
+    o->WFB[1] = 1.0; o->WFF[1] = 0.0;
+    o->WFB[NND2] = 0.0; o->WFF[NND2] = 1.0;
+    /* TDMA_COEF, channel */
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1;
+        o->AMPH[JC] = o->DYFI[JC] * o->DYCI[JC];
+        o->APPH[JC] = o->DYFI[JC] * o->DYCI[JP];
+        if (JC == 1) o->AMPH[JC] = o->DYFI[JC] * o->DYCI[JC] * 0.5;
+        if (JP == NND2) o->APPH[JC] = o->DYFI[JC] * o->DYCI[JP] * 0.5;
+    }
+    for (int JC = 1; JC <= M; ++JC) o->ACPH[JC] = -(o->AMPH[JC] + o->APPH[JC]);
+    o->ACPH[1] = o->AMPH[1] + o->ACPH[1];
+    o->AMPH[1] = 0.0;
+    o->ACPH[M] = o->APPH[M] + o->ACPH[M];
+    o->APPH[M] = 0.0;
+    for (int IDR = 1; IDR <= 3; ++IDR) {
+        double *AM = o->AMVR[IDR], *AC = o->ACVR[IDR], *AP = o->APVR[IDR];
+        if (IDR == 1 || IDR == 3) {
+            for (int JC = 2; JC <= M - 1; ++JC) {
+                int JP = JC + 1;
+                AM[JC] = o->DYFI[JC] * o->DYCI[JC];
+                AP[JC] = o->DYFI[JC] * o->DYCI[JP];
+                AC[JC] = -(AM[JC] + AP[JC]);
+            }
+            double UCAJ = 4.0 / (2.0 / o->DYCI[2] + 1.0 / o->DYFI[1]);
+            AM[1] = 0.0;
+            AP[1] = UCAJ * o->DYCI[2];
+            AC[1] = -UCAJ * (o->DYCI[2] + 2.0 * o->DYFI[1]);
+            o->AMVR1 = UCAJ * (2.0 * o->DYFI[1]);
+            UCAJ = 4.0 / (2.0 / o->DYCI[M] + 1.0 / o->DYFI[M]);
+            AM[M] = UCAJ * o->DYCI[M];
+            AP[M] = 0.0;
+            AC[M] = -UCAJ * (2.0 * o->DYFI[M] + o->DYCI[M]);
+            o->APVRN = UCAJ * (2.0 * o->DYFI[M]);
+        } else {
+            for (int JC = 2; JC <= M; ++JC) {
+                int JM = JC - 1;
+                AM[JC] = o->DYFI[JM] * o->DYCI[JC];
+                AP[JC] = o->DYFI[JC] * o->DYCI[JC];
+                AC[JC] = -(AM[JC] + AP[JC]);
+            }
+            AM[1] = 0.0; AP[1] = 0.0; AC[1] = 1.0;
+            AM[NND2] = 0.0; AP[NND2] = 0.0; AC[NND2] = 1.0;
+        }
+    }
+    /* LAMPOISLPROF, channel: a = 1, b = 0, PCOE = 3/2 */
+    {
+        double Y1 = -1.0, Y2 = 1.0, a = (1.0 - (-1.0)) / 2.0, b = 0.0, PCOE = 3.0 / 2.0;
+        for (int J = 1; J <= M; ++J) {
+            if (o->YCC[J] < Y2 && o->YCC[J] > Y1)
+                o->Vini[J] = (1.0 - ((o->YCC[J] - b) * (o->YCC[J] - b)) / a / a) * PCOE;
+            else
+                o->Vini[J] = 0.0;
+        }
+    }
+    /* CONS_RKCOEF */
+    o->TGAM[0] = 1.0; o->TGAM[1] = 8.0 / 15.0; o->TGAM[2] = 5.0 / 12.0; o->TGAM[3] = 3.0 / 4.0;
+    o->TROH[0] = 0.0; o->TROH[1] = 0.0; o->TROH[2] = -17.0 / 60.0; o->TROH[3] = -5.0 / 12.0;
+    for (int s = 0; s < 4; ++s) o->TALP[s] = o->TGAM[s] + o->TROH[s];
+    /* FFT99_ROOT modified wavenumbers */
+    {
+        int N1MH = L / 2, N3MH = N / 2, N1MP = N1MH + 1, N3MP = N3MH + 1;
+        for (int K = 1; K <= N; ++K) {
+            double AN = (K <= N3MH) ? (double)(K - 1) * 2.0 * PI : -(double)(N - K + 1) * 2.0 * PI;
+            (void)N3MP;
+            o->AK3[K] = 2.0 * (1.0 - cos(AN / (double)N)) * o->DZQI;
+        }
+        for (int I = 1; I <= L; ++I) {
+            double AP = (I <= N1MH) ? (double)(I - 1) * 2.0 * PI : -(double)(L - I + 1) * 2.0 * PI;
+            (void)N1MP;
+            o->AK1[I] = 2.0 * (1.0 - cos(AP / (double)L)) * o->DXQI;
+        }
+    }
+}
+
+orc_t* orc_create(int L, int M, int N, double HX, double HZ, double STR2, double REN, int iFlowDriven,
+                  double Cf_Given, double DT0, double DTMIN, double CFLGV) {
+    if (L < 4 || M < 4 || N < 4 || (L % 2) || (N % 2)) return NULL;
+    orc_t* o = (orc_t*)calloc(1, sizeof(orc_t));
+    o->L = L; o->M = M; o->N = N; o->NND2 = M + 1;
+    o->HX = HX; o->HZ = HZ; o->STR2 = STR2; o->REN = REN;
+    o->iFlowDriven = iFlowDriven; o->Cf_Given = Cf_Given;
+    o->DT0 = DT0; o->DT = DT0; o->DTMIN = DTMIN; o->CFLGV = CFLGV;
+    o->nthreads = 1;
+    size_t ny = (size_t)M + 3;
+    o->YND = dalloc(ny); o->YCC = dalloc(ny); o->DYFI = dalloc(ny); o->DYCI = dalloc(ny);
+    o->WFF = dalloc(ny); o->WFB = dalloc(ny);
+    o->AMPH = dalloc(ny); o->ACPH = dalloc(ny); o->APPH = dalloc(ny);
+    for (int c = 1; c <= 3; ++c) { o->AMVR[c] = dalloc(ny); o->ACVR[c] = dalloc(ny); o->APVR[c] = dalloc(ny); }
+    o->Vini = dalloc(ny);
+    o->AK1 = dalloc((size_t)L + 1); o->AK3 = dalloc((size_t)N + 1);
+    size_t fs = FSZ(o);
+    o->Q = dalloc(3 * fs); o->PR = dalloc(fs); o->CONVH0 = dalloc(3 * fs);
+    o->QTMP = dalloc(fs); o->DPH = dalloc(fs); o->RHSLLPHI = dalloc(fs); o->RHS = dalloc(fs);
+    size_t LH = (size_t)L / 2 + 1;
+    o->SRe = dalloc(LH * (size_t)M * (size_t)N); o->SIm = dalloc(LH * (size_t)M * (size_t)N);
+    setup(o);
+    return o;
+}
+
+void orc_destroy(orc_t* o) {
+    if (!o) return;
+    free(o->YND); free(o->YCC); free(o->DYFI); free(o->DYCI); free(o->WFF); free(o->WFB);
+    free(o->AMPH); free(o->ACPH); free(o->APPH);
+    for (int c = 1; c <= 3; ++c) { free(o->AMVR[c]); free(o->ACVR[c]); free(o->APVR[c]); }
+    free(o->Vini); free(o->AK1); free(o->AK3);
+    free(o->Q); free(o->PR); free(o->CONVH0); free(o->QTMP); free(o->DPH); free(o->RHSLLPHI); free(o->RHS);
+    free(o->SRe); free(o->SIm);
+    free(o);
+}
+
+void orc_set_threads(orc_t* o, int n) {
+    o->nthreads = n < 1 ? 1 : n;
+#ifdef _OPENMP
+    omp_set_num_threads(o->nthreads);
+#endif
+}
+void orc_set_fix_v_wall_row(orc_t* o, int f) { o->fix_v_wall_row = f; }
+
+/* Setup export.  y-arrays are written 1-based into out[0..]: out[j-1] = A(j). */
+void orc_get_y(const orc_t* o, int which, int idr, double* out) {
+    int M = o->M, n = (which == 0 || which == 3 || which == 4 || which == 5) ? M + 1 : M;
+    const double* a = NULL;
+    switch (which) {
+        case 0: a = o->YND; break;
+        case 1: a = o->YCC; break;
+        case 2: a = o->DYFI; break;
+        case 3: a = o->DYCI; break;
+        case 4: a = o->WFF; break;
+        case 5: a = o->WFB; break;
+        case 6: a = o->AMPH; break;
+        case 7: a = o->ACPH; break;
+        case 8: a = o->APPH; break;
+        case 9: a = o->AMVR[idr]; n = M + 1; break;
+        case 10: a = o->ACVR[idr]; n = M + 1; break;
+        case 11: a = o->APVR[idr]; n = M + 1; break;
+        case 12: a = o->Vini; break;
+        default: return;
+    }
+    for (int j = 1; j <= n; ++j) out[j - 1] = a[j];
+}
+/* scalars: DX, DZ, DXI, DZI, DXQI, DZQI, VOLM, Area_inlet, AMVR1, APVRN, CVISC, DT */
+void orc_get_scalars(const orc_t* o, double* s) {
+    s[0] = o->DX; s[1] = o->DZ; s[2] = o->DXI; s[3] = o->DZI; s[4] = o->DXQI; s[5] = o->DZQI;
+    s[6] = o->VOLM; s[7] = o->Area_inlet; s[8] = o->AMVR1; s[9] = o->APVRN; s[10] = o->CVISC; s[11] = o->DT;
+}
+
+void orc_set_fields(orc_t* o, const double* Q, const double* PR, const double* H0) {
+    size_t fs = FSZ(o);
+    if (Q) memcpy(o->Q, Q, 3 * fs * sizeof(double));
+    if (PR) memcpy(o->PR, PR, fs * sizeof(double));
+    if (H0) memcpy(o->CONVH0, H0, 3 * fs * sizeof(double));
+    else memset(o->CONVH0, 0, 3 * fs * sizeof(double));
+}
+void orc_get_fields(const orc_t* o, double* Q, double* PR, double* H0) {
+    size_t fs = FSZ(o);
+    if (Q) memcpy(Q, o->Q, 3 * fs * sizeof(double));
+    if (PR) memcpy(PR, o->PR, fs * sizeof(double));
+    if (H0) memcpy(H0, o->CONVH0, 3 * fs * sizeof(double));
+}
+void orc_get_work(const orc_t* o, int which, double* out) {
+    size_t fs = FSZ(o);
+    const double* a = which == 0 ? o->DPH : which == 1 ? o->RHSLLPHI : which == 2 ? o->RHS : o->QTMP;
+    memcpy(out, a, fs * sizeof(double));
+}
+void orc_set_dt(orc_t* o, double dt) { o->DT = dt; }
+double orc_get_dt(const orc_t* o) { return o->DT; }
+
+/* ------------------------------------------------------------------ */
+/* Line solvers                                                         */
+/* ------------------------------------------------------------------ */
+/* TDMAIJI_CYC (src/TDMAIJI_CYC.f90:67-157), one line of length n with  */
+/* coefficient arrays a, b, c and rhs r (0-based); w is scratch 3*n.    */
+static void tdma_cyc_line(int n, const double* A, const double* B, const double* C, double* R, double* w) {
+    double *H0 = w, *G1 = w + n, *G2 = w + 2 * n;
+    int IS = 0, IEND = n - 1;
+    H0[IS] = C[IS] / B[IS];
+    G1[IS] = R[IS] / B[IS];
+    G2[IS] = -A[IS] / B[IS];
+    for (int I = IS + 1; I <= IEND - 2; ++I) {
+        double PP = 1.0 / (B[I] - H0[I - 1] * A[I]);
+        double QQ1 = G1[I - 1] * A[I];
+        double QQ2 = G2[I - 1] * A[I];
+        H0[I] = C[I] * PP;
+        G1[I] = (R[I] - QQ1) * PP;
+        G2[I] = -QQ2 * PP;
+    }
+    {
+        int I = IEND - 1;
+        double PP = 1.0 / (B[I] - H0[I - 1] * A[I]);
+        double QQ1 = G1[I - 1] * A[I];
+        double QQ2 = G2[I - 1] * A[I];
+        G1[I] = (R[I] - QQ1) * PP;
+        G2[I] = (-C[I] - QQ2) * PP;
+    }
+    for (int I = IEND - 2; I >= IS; --I) {
+        G1[I] = -H0[I] * G1[I + 1] + G1[I];
+        G2[I] = -H0[I] * G2[I + 1] + G2[I];
+    }
+    {
+        int I = IEND;
+        double PP = R[I] - C[I] * G1[IS] - A[I] * G1[I - 1];
+        double QQ1 = B[I] + C[I] * G2[IS] + A[I] * G2[I - 1];
+        R[I] = PP / QQ1;
+    }
+    for (int I = IEND - 1; I >= IS; --I) R[I] = G1[I] + G2[I] * R[IEND];
+}
+
+/* TDMAIJJ_nonCYC (src/TDMAIJJ_nonCYC.f90:67-123), zero Dirichlet BC.  */
+static void tdma_noncyc_line(int n, const double* A, const double* B, const double* C, double* R, double* w) {
+    double *H = w, *G = w + n;
+    const double BC1 = 0.0, BC2 = 0.0;
+    H[0] = C[0] / B[0];
+    G[0] = (R[0] - A[0] * BC1) / B[0];
+    for (int J = 1; J <= n - 2; ++J) {
+        double PP = 1.0 / (B[J] - H[J - 1] * A[J]);
+        H[J] = C[J] * PP;
+        G[J] = (R[J] - A[J] * G[J - 1]) * PP;
+    }
+    {
+        int J = n - 1;
+        double PP = 1.0 / (B[J] - H[J - 1] * A[J]);
+        G[J] = (R[J] - C[J] * BC2 - A[J] * G[J - 1]) * PP;
+        R[J] = G[J];
+    }
+    for (int J = n - 2; J >= 0; --J) R[J] = G[J] - H[J] * R[J + 1];
+}
+
+/* Exported single-line solvers for unit tests. */
+void orc_tdma_cyc(int n, const double* A, const double* B, const double* C, double* R) {
+    double* w = dalloc(3 * (size_t)n);
+    tdma_cyc_line(n, A, B, C, R, w);
+    free(w);
+}
+void orc_tdma_noncyc(int n, const double* A, const double* B, const double* C, double* R) {
+    double* w = dalloc(2 * (size_t)n);
+    tdma_noncyc_line(n, A, B, C, R, w);
+    free(w);
+}
+
+/* ------------------------------------------------------------------ */
+/* CONVECTION_X_tg (src/CONVECTION_X.f90:13-64)                        */
+/* ------------------------------------------------------------------ */
+static void convection_x(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    const double XND2CL = 0.5, ZND2CL = 0.5;
+    memset(o->QTMP, 0, FSZ(o) * sizeof(double));
+    double COE1 = XND2CL * XND2CL * o->DXI;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * XND2CL * 1.0;
+        double COE3 = XND2CL * ZND2CL * o->DZI * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double H11 = ((QV(o, IP, JC, KC, 1) + QV(o, IC, JC, KC, 1)) * (QV(o, IP, JC, KC, 1) + QV(o, IC, JC, KC, 1)) -
+                              (QV(o, IM, JC, KC, 1) + QV(o, IC, JC, KC, 1)) * (QV(o, IM, JC, KC, 1) + QV(o, IC, JC, KC, 1))) * COE1;
+                double H12 = ((QV(o, IC, JP, KC, 2) + QV(o, IM, JP, KC, 2)) *
+                                  (o->WFF[JJP] * QV(o, IC, JP, KC, 1) + o->WFB[JJP] * QV(o, IC, JC, KC, 1)) -
+                              (QV(o, IC, JC, KC, 2) + QV(o, IM, JC, KC, 2)) *
+                                  (o->WFF[JJ] * QV(o, IC, JC, KC, 1) + o->WFB[JJ] * QV(o, IC, JM, KC, 1))) * COE2;
+                double H13 = ((QV(o, IC, JC, KP, 3) + QV(o, IM, JC, KP, 3)) * (QV(o, IC, JC, KP, 1) + QV(o, IC, JC, KC, 1)) -
+                              (QV(o, IC, JC, KC, 3) + QV(o, IM, JC, KC, 3)) * (QV(o, IC, JC, KC, 1) + QV(o, IC, JC, KM, 1))) * COE3;
+                F3(o->QTMP, o, IC, JC, KC) = -(H11 + H12 + H13);
+            }
+        }
+    }
+}
+
+/* CONVECTION_Y_tg (src/CONVECTION_Y.f90:13-114), channel branch.  The  */
+/* v-equation skips the wall face j = 1 (NYI = 2).                      */
+static void convection_y(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    const double XND2CL = 0.5, YND2CL = 0.5, ZND2CL = 0.5;
+    memset(o->DPH, 0, FSZ(o) * sizeof(double));
+    double COE1 = o->DXI * XND2CL;
+    double COE30 = o->DZI * ZND2CL;
+#pragma omp parallel for schedule(static)
+    for (int JC = 2; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC;
+        double COE2 = o->DYCI[JJ] * YND2CL * YND2CL;
+        double COE31 = COE30 * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double H21 = ((o->WFF[JJ] * QV(o, IP, JC, KC, 1) + o->WFB[JJ] * QV(o, IP, JM, KC, 1)) *
+                                  (QV(o, IP, JC, KC, 2) + QV(o, IC, JC, KC, 2)) -
+                              (o->WFF[JJ] * QV(o, IC, JC, KC, 1) + o->WFB[JJ] * QV(o, IC, JM, KC, 1)) *
+                                  (QV(o, IC, JC, KC, 2) + QV(o, IM, JC, KC, 2))) * COE1;
+                double H22 = ((QV(o, IC, JP, KC, 2) * 1.0 + QV(o, IC, JC, KC, 2) * 1.0) * (QV(o, IC, JP, KC, 2) + QV(o, IC, JC, KC, 2)) -
+                              (QV(o, IC, JC, KC, 2) * 1.0 + QV(o, IC, JM, KC, 2) * 1.0) * (QV(o, IC, JC, KC, 2) + QV(o, IC, JM, KC, 2))) * COE2;
+                double H23 = ((o->WFF[JJ] * QV(o, IC, JC, KP, 3) * 1.0 + o->WFB[JJ] * QV(o, IC, JM, KP, 3) * 1.0) *
+                                  (QV(o, IC, JC, KP, 2) + QV(o, IC, JC, KC, 2)) -
+                              (o->WFF[JJ] * QV(o, IC, JC, KC, 3) * 1.0 + o->WFB[JJ] * QV(o, IC, JM, KC, 3) * 1.0) *
+                                  (QV(o, IC, JC, KC, 2) + QV(o, IC, JC, KM, 2))) * COE31;
+                F3(o->DPH, o, IC, JC, KC) = -(H21 + H22 + H23);
+            }
+        }
+    }
+}
+
+/* CONVECTION_Z_tg (src/CONVECTION_Z.f90:13-103), channel branch.       */
+static void convection_z(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    const double XND2CL = 0.5, ZND2CL = 0.5;
+    memset(o->RHSLLPHI, 0, FSZ(o) * sizeof(double));
+    double COE1 = XND2CL * ZND2CL * o->DXI;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * ZND2CL;
+        double COE3 = ZND2CL * ZND2CL * o->DZI * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double H31 = ((QV(o, IP, JC, KC, 1) + QV(o, IP, JC, KM, 1)) * (QV(o, IP, JC, KC, 3) + QV(o, IC, JC, KC, 3)) -
+                              (QV(o, IC, JC, KC, 1) + QV(o, IC, JC, KM, 1)) * (QV(o, IC, JC, KC, 3) + QV(o, IM, JC, KC, 3))) * COE1;
+                double H32 = ((QV(o, IC, JP, KC, 2) + QV(o, IC, JP, KM, 2)) *
+                                  (o->WFF[JJP] * QV(o, IC, JP, KC, 3) * 1.0 + o->WFB[JJP] * QV(o, IC, JC, KC, 3) * 1.0) -
+                              (QV(o, IC, JC, KC, 2) + QV(o, IC, JC, KM, 2)) *
+                                  (o->WFF[JJ] * QV(o, IC, JC, KC, 3) * 1.0 + o->WFB[JJ] * QV(o, IC, JM, KC, 3) * 1.0)) * COE2;
+                double H33 = ((QV(o, IC, JC, KP, 3) + QV(o, IC, JC, KC, 3)) * (QV(o, IC, JC, KP, 3) + QV(o, IC, JC, KC, 3)) -
+                              (QV(o, IC, JC, KC, 3) + QV(o, IC, JC, KM, 3)) * (QV(o, IC, JC, KC, 3) + QV(o, IC, JC, KM, 3))) * COE3;
+                F3(o->RHSLLPHI, o, IC, JC, KC) = -(H31 + H32 + H33);
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* RHS_CvLpGpS_tg (src/RHS_CvLpGpS_tg.f90:12-204).  RHS rows j < NII     */
+/* are left untouched, exactly as in the reference (the module array    */
+/* keeps its previous contents there).                                  */
+/* ------------------------------------------------------------------ */
+static void rhs_cvlpgps(orc_t* o, int NS, int IDR) {
+    int L = o->L, M = o->M, N = o->N;
+    int NII = (IDR == 2) ? 2 : 1;
+    const double* CONVH = IDR == 1 ? o->QTMP : IDR == 2 ? o->DPH : o->RHSLLPHI;
+    const double RMC2 = 1.0; /* RCCI2 / RNDI2 = 1 in the channel */
+    double COE1 = o->TALP[NS] * o->CVISC * 1.0 / 1.0;
+    double DT = o->DT;
+    const double *APVR = o->APVR[IDR], *ACVR = o->ACVR[IDR], *AMVR = o->AMVR[IDR];
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC) {
+        int KM = KMV(o, KC), KP = KPV(o, KC);
+        for (int JC = NII; JC <= M; ++JC) {
+            int JM = JC - 1, JP = JC + 1, JJ = JC;
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double CV = F3(CONVH, o, IC, JC, KC);
+                double RHSC = o->TGAM[NS] * CV + o->TROH[NS] * H0V(o, IC, JC, KC, IDR);
+                double RHSL = COE1 * ((QV(o, IP, JC, KC, IDR) - 2.0 * QV(o, IC, JC, KC, IDR) + QV(o, IM, JC, KC, IDR)) * o->DXQI +
+                                      (QV(o, IC, JC, KP, IDR) - 2.0 * QV(o, IC, JC, KC, IDR) + QV(o, IC, JC, KM, IDR)) * o->DZQI * RMC2 +
+                                      (QV(o, IC, JP, KC, IDR) * APVR[JJ] + QV(o, IC, JC, KC, IDR) * ACVR[JJ] +
+                                       QV(o, IC, JM, KC, IDR) * AMVR[JJ]));
+                H0V(o, IC, JC, KC, IDR) = CV;
+                F3(o->RHS, o, IC, JC, KC) = (RHSC + RHSL) * DT;
+            }
+        }
+    }
+    double COE2 = o->TALP[NS] * DT / 1.0;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC) {
+        int KM = KMV(o, KC);
+        for (int JC = NII; JC <= M; ++JC) {
+            int JM = JC - 1, JJ = JC;
+            double SUCACJ = o->DYCI[JJ] / 1.0;
+            for (int IC = 1; IC <= L; ++IC) {
+                int IM = IMV(o, IC);
+                double PGM;
+                if (IDR == 1) PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IM, JC, KC)) * o->DXI * COE2;
+                else if (IDR == 2) PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IC, JM, KC)) * SUCACJ * COE2;
+                else PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IC, JC, KM)) * o->DZI * COE2;
+                F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
+            }
+        }
+    }
+    if (IDR == 1) {
+        double DPGRNS = 0.0;
+        if (o->iFlowDriven == 1) {
+            /* naive sum in the reference's loop order: IC, JC, KC */
+            double INTGRHSY = 0.0;
+            for (int IC = 1; IC <= L; ++IC)
+                for (int JC = 1; JC <= M; ++JC)
+                    for (int KC = 1; KC <= N; ++KC)
+                        INTGRHSY = INTGRHSY + F3(o->RHS, o, IC, JC, KC) / o->DYFI[JC] / 1.0;
+            DPGRNS = INTGRHSY / o->VOLM;
+        } else if (o->iFlowDriven == 2) {
+            DPGRNS = -0.5 * o->Cf_Given * COE2;
+        }
+#pragma omp parallel for schedule(static)
+        for (int K = 1; K <= N; ++K)
+            for (int J = NII; J <= M; ++J)
+                for (int I = 1; I <= L; ++I) F3(o->RHS, o, I, J, K) = F3(o->RHS, o, I, J, K) - DPGRNS;
+    }
+}
+
+/* MOMFA_tg + MOMFA1_X_tg + MOMFA2_Z_tg + MOMFA3_Y_tg                   */
+/* (src/MOMFA_tg.f90:15-238).                                           */
+static void momfa(orc_t* o, int NS, int IDR) {
+    int L = o->L, M = o->M, N = o->N;
+    double FACOE = 0.5 * o->TALP[NS] * o->DT * o->CVISC * 1.0 / 1.0;
+    int N2I = (IDR == 2) ? 2 : 1;
+    /* x sweep: cyclic, constant coefficients */
+    {
+        double COE = -FACOE * o->DXQI;
+#pragma omp parallel
+        {
+            double* A = dalloc((size_t)L); double* B = dalloc((size_t)L); double* C = dalloc((size_t)L);
+            double* R = dalloc((size_t)L); double* w = dalloc(3 * (size_t)L);
+#pragma omp for schedule(static)
+            for (int K = 1; K <= N; ++K)
+                for (int J = N2I; J <= M; ++J) {
+                    for (int I = 1; I <= L; ++I) {
+                        C[I - 1] = COE; A[I - 1] = COE; B[I - 1] = 1.0 - C[I - 1] - A[I - 1];
+                        R[I - 1] = F3(o->RHS, o, I, J, K);
+                    }
+                    tdma_cyc_line(L, A, B, C, R, w);
+                    for (int I = 1; I <= L; ++I) F3(o->RHS, o, I, J, K) = R[I - 1];
+                }
+            free(A); free(B); free(C); free(R); free(w);
+        }
+    }
+    /* z sweep: cyclic, constant coefficients */
+    {
+        double RMC2 = 1.0 * (-FACOE * o->DZQI);
+#pragma omp parallel
+        {
+            double* A = dalloc((size_t)N); double* B = dalloc((size_t)N); double* C = dalloc((size_t)N);
+            double* R = dalloc((size_t)N); double* w = dalloc(3 * (size_t)N);
+#pragma omp for schedule(static)
+            for (int I = 1; I <= L; ++I)
+                for (int J = N2I; J <= M; ++J) {
+                    for (int K = 1; K <= N; ++K) {
+                        C[K - 1] = RMC2; A[K - 1] = RMC2; B[K - 1] = 1.0 - C[K - 1] - A[K - 1];
+                        R[K - 1] = F3(o->RHS, o, I, J, K);
+                    }
+                    tdma_cyc_line(N, A, B, C, R, w);
+                    for (int K = 1; K <= N; ++K) F3(o->RHS, o, I, J, K) = R[K - 1];
+                }
+            free(A); free(B); free(C); free(R); free(w);
+        }
+    }
+    /* y sweep: non-cyclic over J = 1..M for every component */
+    {
+        const double *AMVR = o->AMVR[IDR], *ACVR = o->ACVR[IDR], *APVR = o->APVR[IDR];
+#pragma omp parallel
+        {
+            double* A = dalloc((size_t)M); double* B = dalloc((size_t)M); double* C = dalloc((size_t)M);
+            double* R = dalloc((size_t)M); double* w = dalloc(2 * (size_t)M);
+#pragma omp for schedule(static)
+            for (int K = 1; K <= N; ++K)
+                for (int I = 1; I <= L; ++I) {
+                    for (int J = 1; J <= M; ++J) {
+                        R[J - 1] = F3(o->RHS, o, I, J, K);
+                        B[J - 1] = 1.0 - FACOE * ACVR[J];
+                        C[J - 1] = -FACOE * APVR[J];
+                        A[J - 1] = -FACOE * AMVR[J];
+                    }
+                    if (IDR == 2 && o->fix_v_wall_row) R[0] = 0.0;
+                    tdma_noncyc_line(M, A, B, C, R, w);
+                    for (int J = 1; J <= M; ++J) F3(o->RHS, o, I, J, K) = R[J - 1];
+                }
+            free(A); free(B); free(C); free(R); free(w);
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int K = 1; K <= N; ++K)
+        for (int J = N2I; J <= M; ++J)
+            for (int I = 1; I <= L; ++I) QV(o, I, J, K, IDR) = F3(o->RHS, o, I, J, K) + QV(o, I, J, K, IDR);
+}
+
+/* BC_WALL_Q_tg / BC_WALL_PR_tg / BC_WALL_DPH_tg (src/BC_WALL.f90:212-432) */
+static void bc_wall_q(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int K = 1; K <= N; ++K)
+        for (int I = 1; I <= L; ++I) {
+            QV(o, I, M + 1, K, 1) = 0.0; QV(o, I, M + 1, K, 3) = 0.0; QV(o, I, M + 1, K, 2) = 0.0;
+            QV(o, I, 0, K, 1) = 0.0; QV(o, I, 0, K, 3) = 0.0; QV(o, I, 1, K, 2) = 0.0; QV(o, I, 0, K, 2) = 0.0;
+        }
+}
+static void bc_wall_scalar(orc_t* o, double* F) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int K = 1; K <= N; ++K)
+        for (int I = 1; I <= L; ++I) {
+            F3(F, o, I, M + 1, K) = F3(F, o, I, M, K);
+            F3(F, o, I, 0, K) = F3(F, o, I, 1, K);
+        }
+}
+
+/* DIVG_tg (src/DIVG.f90:15-51) */
+static void divg(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+    double COE0 = 1.0 / (o->DT * o->TALP[NS]);
+    memset(o->RHSLLPHI, 0, FSZ(o) * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1, JJ = JC;
+        double COE1 = o->DXI / 1.0;
+        double COE2 = o->DYFI[JJ] / 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC);
+                double DV = (QV(o, IP, JC, KC, 1) - QV(o, IC, JC, KC, 1)) * COE1 + (QV(o, IC, JP, KC, 2) - QV(o, IC, JC, KC, 2)) * COE2 +
+                            (QV(o, IC, JC, KP, 3) - QV(o, IC, JC, KC, 3)) * o->DZI;
+                F3(o->RHSLLPHI, o, IC, JC, KC) = DV * COE0;
+            }
+        }
+    }
+}
+
+/* FFT99_POIS3D_periodicxz (src/possion3d_FFT99.f90:271-505) with the    */
+/* coefficients of TDMA_PHI_COEF (:204-239).  Forward: x transform with */
+/* 1/L (FFT99, ISIGN=-1), z transform (CFFT99, ISIGN=-1) times 1/N.     */
+/* Zero mode: RHS(1,1,1) = 0 and row 1 decoupled (phi(y_1) = 0).        */
+/* src: (L, 0:M+1, N) field; dst: (L, 0:M+1, N) field (rows 1..M).       */
+static void poisson(orc_t* o, const double* src, double* dst) {
+    int L = o->L, M = o->M, N = o->N, LH = L / 2 + 1;
+    double UN3M = 1.0 / (double)N;
+    cplx* wfx = fft_table(L, -1);
+    cplx* wbx = fft_table(L, +1);
+    cplx* wfz = fft_table(N, -1);
+    cplx* wbz = fft_table(N, +1);
+    double* SRe = o->SRe;
+    double* SIm = o->SIm;
+#define SIX(I, J, K) ((size_t)((I) - 1) + (size_t)LH * ((size_t)((J) - 1) + (size_t)M * (size_t)((K) - 1)))
+#pragma omp parallel
+    {
+        int nmax = L > N ? L : N;
+        cplx* a = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+        cplx* b = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+#pragma omp for schedule(static)
+        for (int J = 1; J <= M; ++J) {
+            for (int K = 1; K <= N; ++K) {
+                for (int I = 1; I <= L; ++I) { a[I - 1].re = F3(src, o, I, J, K); a[I - 1].im = 0.0; }
+                fft_rec(L, a, 1, b, -1, wfx, 1);
+                for (int I = 1; I <= LH; ++I) {
+                    SRe[SIX(I, J, K)] = b[I - 1].re / (double)L;
+                    SIm[SIX(I, J, K)] = b[I - 1].im / (double)L;
+                }
+            }
+            for (int I = 1; I <= LH; ++I) {
+                for (int K = 1; K <= N; ++K) { a[K - 1].re = SRe[SIX(I, J, K)]; a[K - 1].im = SIm[SIX(I, J, K)]; }
+                fft_rec(N, a, 1, b, -1, wfz, 1);
+                for (int K = 1; K <= N; ++K) {
+                    SRe[SIX(I, J, K)] = b[K - 1].re * UN3M;
+                    SIm[SIX(I, J, K)] = b[K - 1].im * UN3M;
+                }
+            }
+        }
+        free(a); free(b);
+    }
+    SRe[SIX(1, 1, 1)] = 0.0;
+    SIm[SIX(1, 1, 1)] = 0.0;
+#pragma omp parallel
+    {
+        double* A = dalloc((size_t)M); double* B = dalloc((size_t)M); double* C = dalloc((size_t)M);
+        double* R = dalloc((size_t)M); double* w = dalloc(2 * (size_t)M);
+#pragma omp for schedule(static)
+        for (int K = 1; K <= N; ++K)
+            for (int I = 1; I <= LH; ++I) {
+                for (int J = 1; J <= M; ++J) {
+                    C[J - 1] = o->APPH[J];
+                    A[J - 1] = o->AMPH[J];
+                    B[J - 1] = o->ACPH[J] + (-o->AK1[I] / 1.0 - o->AK3[K]);
+                }
+                if (I == 1 && K == 1) {
+                    B[0] = o->ACPH[1] + (-o->AK1[1] / 1.0 - o->AK3[1]);
+                    C[0] = 0.0;
+                    A[0] = 0.0;
+                }
+                for (int part = 0; part < 2; ++part) {
+                    double* S = part ? SIm : SRe;
+                    for (int J = 1; J <= M; ++J) R[J - 1] = S[SIX(I, J, K)];
+                    if (K == 1 && I == 1) R[0] = 0.0;
+                    tdma_noncyc_line(M, A, B, C, R, w);
+                    for (int J = 1; J <= M; ++J) S[SIX(I, J, K)] = R[J - 1];
+                }
+            }
+        free(A); free(B); free(C); free(R); free(w);
+    }
+#pragma omp parallel
+    {
+        int nmax = L > N ? L : N;
+        cplx* a = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+        cplx* b = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+#pragma omp for schedule(static)
+        for (int J = 1; J <= M; ++J) {
+            for (int I = 1; I <= LH; ++I) {
+                for (int K = 1; K <= N; ++K) { a[K - 1].re = SRe[SIX(I, J, K)]; a[K - 1].im = SIm[SIX(I, J, K)]; }
+                fft_rec(N, a, 1, b, +1, wbz, 1);
+                for (int K = 1; K <= N; ++K) { SRe[SIX(I, J, K)] = b[K - 1].re; SIm[SIX(I, J, K)] = b[K - 1].im; }
+            }
+            for (int K = 1; K <= N; ++K) {
+                /* FFT99 ISIGN=+1: x(j) = sum_k c(k) exp(+2 pi i j k / L), c(L-k) = conj(c(k));
+                   the imaginary parts of the k = 0 and k = L/2 coefficients do not enter. */
+                for (int I = 1; I <= LH; ++I) { a[I - 1].re = SRe[SIX(I, J, K)]; a[I - 1].im = SIm[SIX(I, J, K)]; }
+                a[0].im = 0.0;
+                a[L / 2].im = 0.0;
+                for (int I = LH + 1; I <= L; ++I) { a[I - 1].re = a[L - I + 1].re; a[I - 1].im = -a[L - I + 1].im; }
+                fft_rec(L, a, 1, b, +1, wbx, 1);
+                for (int I = 1; I <= L; ++I) F3(dst, o, I, J, K) = b[I - 1].re;
+            }
+        }
+        free(a); free(b);
+    }
+#undef SIX
+    free(wfx); free(wbx); free(wfz); free(wbz);
+}
+
+/* Exported Poisson solve on caller arrays in the (L, 0:M+1, N) layout. */
+void orc_poisson(orc_t* o, const double* rhs, double* dph) { poisson(o, rhs, dph); }
+
+/* VELOUPDT_tg (src/VELO_CORRECTION.f90:14-100) */
+static void veloupdt(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+    double COE1 = o->DT * o->TALP[NS] * o->DXI;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                int IM = IMV(o, IC);
+                double DFX11 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IM, JC, KC);
+                QV(o, IC, JC, KC, 1) = QV(o, IC, JC, KC, 1) - DFX11 * COE1;
+            }
+    COE1 = o->DT * o->TALP[NS] * o->DZI;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC) {
+        int KM = KMV(o, KC);
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double DFX33 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IC, JC, KM);
+                QV(o, IC, JC, KC, 3) = QV(o, IC, JC, KC, 3) - DFX33 * COE1;
+            }
+    }
+#pragma omp parallel for schedule(static)
+    for (int JC = 2; JC <= M; ++JC) {
+        int JJ = JC, JM = JC - 1;
+        double C1 = o->DT * o->TALP[NS] * o->DYCI[JJ] / 1.0;
+        for (int KC = 1; KC <= N; ++KC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double DFX22 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IC, JM, KC);
+                QV(o, IC, JC, KC, 2) = QV(o, IC, JC, KC, 2) - DFX22 * C1;
+            }
+    }
+}
+
+/* PRCALC_tg (src/PRESSURE_CORRECTION.f90:15-99) */
+static void prcalc(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+    double BE = 0.5 * o->TALP[NS] * o->DT * o->CVISC * 1.0 / 1.0;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double LLPHI = F3(o->RHSLLPHI, o, IC, JC, KC);
+                F3(o->PR, o, IC, JC, KC) = F3(o->PR, o, IC, JC, KC) + F3(o->DPH, o, IC, JC, KC) - BE * LLPHI;
+            }
+}
+
+/* SOLVERRK3_MOM_tg(NS) (src/SOLVERRK3_MOM_tg.f90:13-56) */
+int orc_substep(orc_t* o, int NS) {
+    if (NS < 0 || NS > 3) return -1;
+    convection_x(o);
+    convection_y(o);
+    convection_z(o);
+    for (int IDR = 1; IDR <= 3; ++IDR) {
+        rhs_cvlpgps(o, NS, IDR);
+        momfa(o, NS, IDR);
+    }
+    bc_wall_q(o);
+    divg(o, NS);
+    memset(o->DPH, 0, FSZ(o) * sizeof(double));
+    poisson(o, o->RHSLLPHI, o->DPH);
+    bc_wall_scalar(o, o->DPH);
+    veloupdt(o, NS);
+    bc_wall_q(o);
+    prcalc(o, NS);
+    bc_wall_scalar(o, o->PR);
+    return 0;
+}
+
+/* CFL_tg (src/CFL.f90:13-52) */
+double orc_cfl(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double CFLMA = 0.0;
+    for (int K = 1; K <= N; ++K) {
+        int KP = KPV(o, K);
+        for (int J = 1; J <= M; ++J) {
+            int JP = J + 1, JC = J;
+            for (int I = 1; I <= L; ++I) {
+                int IP = IPV(o, I);
+                double QCF = (fabs((QV(o, I, J, K, 1) + QV(o, IP, J, K, 1)) * o->DXI) +
+                              fabs((QV(o, I, J, K, 2) + QV(o, I, JP, K, 2)) * o->DYFI[JC] * 1.0) +
+                              fabs((QV(o, I, J, K, 3) + QV(o, I, J, KP, 3)) * o->DZI * 1.0)) * 0.5;
+                CFLMA = fmax(CFLMA, QCF);
+            }
+        }
+    }
+    o->CFLMM = CFLMA;
+    return CFLMA;
+}
+
+/* dt rule of BCAST_COMM_STEP (src/SOLVE.f90:177-178); returns 1 when   */
+/* DT/DT0 < 0.01 (the reference dumps and STOPs, :199-207).             */
+int orc_step_dt(orc_t* o, double* dt_out) {
+    double c = orc_cfl(o);
+    double dt = fmin(fmin(o->DT0, 5.0 * o->DT), o->CFLGV / c);
+    dt = fmax(dt, o->DTMIN);
+    o->DT = dt;
+    if (dt_out) *dt_out = dt;
+    return (dt / o->DT0) < 0.01 ? 1 : 0;
+}
+
+/* One time step of SOLVE (src/SOLVE.f90:75-134): CFL/dt + 3 substeps. */
+int orc_run_steps(orc_t* o, int nsteps, double* dts) {
+    for (int s = 0; s < nsteps; ++s) {
+        double dt;
+        if (orc_step_dt(o, &dt)) return 1;
+        if (dts) dts[s] = dt;
+        for (int NS = 1; NS <= 3; ++NS) orc_substep(o, NS);
+    }
+    return 0;
+}
+
+/* DIVGCK_tg (src/DIVGCK.f90:15-55) */
+double orc_divgck(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double DIVX = 0.0;
+    for (int K = 1; K <= N; ++K) {
+        int KP = KPV(o, K);
+        for (int J = 1; J <= M; ++J) {
+            int JP = J + 1, JJ = J;
+            for (int I = 1; I <= L; ++I) {
+                int IP = IPV(o, I);
+                double DQCAP = (QV(o, IP, J, K, 1) - QV(o, I, J, K, 1)) * o->DXI +
+                               (QV(o, I, JP, K, 2) - QV(o, I, J, K, 2)) * o->DYFI[JJ] * 1.0 +
+                               (QV(o, I, J, KP, 3) - QV(o, I, J, K, 3)) * o->DZI * 1.0;
+                DIVX = fmax(fabs(DQCAP), DIVX);
+            }
+        }
+    }
+    return DIVX;
+}

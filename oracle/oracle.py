@@ -1,0 +1,192 @@
+"""ctypes binding of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+The oracle (``chapsim_oracle.c``) is an FP64 restatement of CHAPSim's
+periodic-channel time step (``src/SOLVERRK3_MOM_tg.f90`` and the routines it
+calls).  It is used by ``tests/`` as the checker, by the smoke check, and by
+the CPU-baseline leg of ``bench.py``.  The product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle_chapsim.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc, OpenMP)."""
+    if force or not os.path.exists(_LIB_PATH) or (
+        os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "chapsim_oracle.c"))
+    ):
+        subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 4 + [ctypes.c_int] + [ctypes.c_double] * 4
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_set_fix_v_wall_row.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_get_y.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_get_scalars.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_set_fields.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.orc_get_fields.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.orc_get_work.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_set_dt.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.orc_get_dt.argtypes = [ctypes.c_void_p]
+        L.orc_get_dt.restype = ctypes.c_double
+        L.orc_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_substep.restype = ctypes.c_int
+        L.orc_cfl.argtypes = [ctypes.c_void_p]
+        L.orc_cfl.restype = ctypes.c_double
+        L.orc_step_dt.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_step_dt.restype = ctypes.c_int
+        L.orc_run_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_run_steps.restype = ctypes.c_int
+        L.orc_divgck.argtypes = [ctypes.c_void_p]
+        L.orc_divgck.restype = ctypes.c_double
+        L.orc_poisson.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_fft_complex.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
+        L.orc_tdma_cyc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.orc_tdma_noncyc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+class Oracle:
+    """CPU FP64 periodic-channel solver (test checker).
+
+    Fields use the reference layout: ``Q`` has shape (3, N, M+2, L) in C order,
+    i.e. Fortran ``Q_tg(L, 0:M+1, N, 3)``; ``PR`` is (N, M+2, L).
+    """
+
+    Y_NAMES = {"YND": 0, "YCC": 1, "DYFI": 2, "DYCI": 3, "WFF": 4, "WFB": 5, "AMPH": 6, "ACPH": 7,
+               "APPH": 8, "AMVR": 9, "ACVR": 10, "APVR": 11, "Vini": 12}
+
+    def __init__(self, L, M, N, HX, HZ, STR2, REN, iFlowDriven=1, Cf_Given=8.18e-3, DT0=1e-3, DTMIN=1e-6,
+                 CFLGV=0.5, threads=1):
+        self.L, self.M, self.N = L, M, N
+        self._lib = lib()
+        self._h = self._lib.orc_create(L, M, N, HX, HZ, STR2, REN, iFlowDriven, Cf_Given, DT0, DTMIN, CFLGV)
+        if not self._h:
+            raise ValueError("invalid oracle grid")
+        self._lib.orc_set_threads(self._h, int(threads))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.orc_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_fix_v_wall_row(self, flag: bool):
+        self._lib.orc_set_fix_v_wall_row(self._h, int(bool(flag)))
+
+    def y(self, name, idr=1):
+        n = self.M + 1
+        out = np.zeros(n, np.float64)
+        self._lib.orc_get_y(self._h, self.Y_NAMES[name], idr, _p(out))
+        if name in ("YCC", "DYFI", "AMPH", "ACPH", "APPH", "Vini"):
+            return out[: self.M]
+        return out
+
+    def scalars(self):
+        s = np.zeros(12, np.float64)
+        self._lib.orc_get_scalars(self._h, _p(s))
+        keys = ["DX", "DZ", "DXI", "DZI", "DXQI", "DZQI", "VOLM", "Area_inlet", "AMVR1", "APVRN", "CVISC", "DT"]
+        return dict(zip(keys, s.tolist()))
+
+    def field_shape(self):
+        return (self.N, self.M + 2, self.L)
+
+    def set_fields(self, Q, PR, H0=None):
+        Q = np.ascontiguousarray(Q, np.float64)
+        PR = np.ascontiguousarray(PR, np.float64)
+        assert Q.shape == (3,) + self.field_shape() and PR.shape == self.field_shape()
+        if H0 is None:
+            self._lib.orc_set_fields(self._h, _p(Q), _p(PR), None)
+        else:
+            H0 = np.ascontiguousarray(H0, np.float64)
+            self._lib.orc_set_fields(self._h, _p(Q), _p(PR), _p(H0))
+
+    def get_fields(self):
+        Q = np.zeros((3,) + self.field_shape())
+        PR = np.zeros(self.field_shape())
+        H0 = np.zeros((3,) + self.field_shape())
+        self._lib.orc_get_fields(self._h, _p(Q), _p(PR), _p(H0))
+        return Q, PR, H0
+
+    def work(self, which):
+        out = np.zeros(self.field_shape())
+        self._lib.orc_get_work(self._h, {"DPH": 0, "RHSLLPHI": 1, "RHS": 2, "QTMP": 3}[which], _p(out))
+        return out
+
+    def set_dt(self, dt):
+        self._lib.orc_set_dt(self._h, float(dt))
+
+    def dt(self):
+        return self._lib.orc_get_dt(self._h)
+
+    def substep(self, ns):
+        if self._lib.orc_substep(self._h, int(ns)) != 0:
+            raise ValueError("bad substep index")
+
+    def cfl(self):
+        return self._lib.orc_cfl(self._h)
+
+    def step_dt(self):
+        dt = ctypes.c_double()
+        rc = self._lib.orc_step_dt(self._h, ctypes.byref(dt))
+        return dt.value, rc
+
+    def run_steps(self, n):
+        dts = np.zeros(max(n, 1))
+        rc = self._lib.orc_run_steps(self._h, int(n), _p(dts))
+        return rc, dts[:n]
+
+    def divgck(self):
+        return self._lib.orc_divgck(self._h)
+
+    def poisson(self, rhs):
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        out = np.zeros(self.field_shape())
+        self._lib.orc_poisson(self._h, _p(rhs), _p(out))
+        return out
+
+
+def fft_complex(x: np.ndarray, sign: int) -> np.ndarray:
+    re = np.ascontiguousarray(x.real, np.float64).copy()
+    im = np.ascontiguousarray(x.imag, np.float64).copy()
+    lib().orc_fft_complex(len(x), _p(re), _p(im), int(sign))
+    return re + 1j * im
+
+
+def tdma_cyc(A, B, C, R):
+    R = np.array(R, np.float64)
+    lib().orc_tdma_cyc(len(R), _p(np.ascontiguousarray(A, np.float64)), _p(np.ascontiguousarray(B, np.float64)),
+                       _p(np.ascontiguousarray(C, np.float64)), _p(R))
+    return R
+
+
+def tdma_noncyc(A, B, C, R):
+    R = np.array(R, np.float64)
+    lib().orc_tdma_noncyc(len(R), _p(np.ascontiguousarray(A, np.float64)), _p(np.ascontiguousarray(B, np.float64)),
+                          _p(np.ascontiguousarray(C, np.float64)), _p(R))
+    return R
