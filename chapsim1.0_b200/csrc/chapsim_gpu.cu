@@ -131,6 +131,7 @@ struct chapsim_ctx {
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr, *HS = nullptr;
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
+    double* fac = nullptr;       // factor tables of the x, z, y sweeps
     int npart_rhs = 0;
     double* part_red = nullptr;  // per-block CFL / divergence maxima
     int npart_red = 0;
@@ -200,11 +201,22 @@ std::vector<double2> twiddles(int n) {
     return w;
 }
 
-size_t smem_rhs(const Geo& g) { return (size_t)(3 * RHS_TJ * (g.L + 33) + 32) * sizeof(double); }
+size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(double); }
 size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(double); }
-size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33) + 3 * g.M + 64) * sizeof(double); }
+size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(double); }
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * g.L) * sizeof(double2); }
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * (g.N + 1)) * sizeof(double2); }
+size_t smem_ys(const Geo& g) { return (size_t)(32 * g.M) * (sizeof(double2) + sizeof(double)); }
+bool use_ys_tile(const Geo& g) { return g.M <= 256; }
+
+void launch_ysolve(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    const long long nl = (long long)g.LH * g.N;
+    if (use_ys_tile(g))
+        k_ysolve_tile<<<(int)((nl + 31) / 32), YS2_NT, smem_ys(g), ctx->stream>>>(g, ctx->SP);
+    else
+        k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, ctx->stream>>>(g, ctx->SP, ctx->HS);
+}
 
 template <typename F>
 cudaError_t set_smem(F* f, size_t bytes) {
@@ -232,6 +244,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S>, smem_y(g))));
     CK(set_smem(k_div_fftx, smem_px(g)));
     CK(set_smem(k_fftx_inv, smem_px(g)));
+    if (use_ys_tile(g)) CK(set_smem(k_ysolve_tile, smem_ys(g)));
     CK(set_smem(k_fftz<-1>, smem_fz(g)));
     CK(set_smem(k_fftz<+1>, smem_fz(g)));
     return CHAPSIM_OK;
@@ -254,16 +267,17 @@ void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
 void launch_substep(chapsim_ctx* ctx, int ns) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    dim3 grx((g.M + RHS_TJ - 1) / RHS_TJ, g.N);
-    DISPATCH_S(g.L / 32, (k_rhs_xsweep<S><<<grx, RHS_NT, smem_rhs(g), s>>>(g, ctx->Q, ctx->PR, ctx->H0, ctx->RHS,
-                                                                             ctx->part_rhs, ctx->st, ns)));
+    k_factors<<<5, 32, 0, s>>>(g, ctx->fac, ctx->st, ns);
     prof_mark(ctx);
-    dim3 grz((g.L + 31) / 32, g.M, 3);
-    DISPATCH_S(g.N / 32, (k_zsweep<S><<<grz, SWEEP_NT, smem_z(g), s>>>(g, ctx->RHS, ctx->st, ns)));
+    const int grx = g.M * g.N / RHS_WPB;
+    DISPATCH_S(g.L / 32, (k_rhs_xsweep<S><<<grx, RHS_WPB * 32, smem_rhs(g), s>>>(g, ctx->Q, ctx->PR, ctx->H0, ctx->RHS,
+                                                                                   ctx->part_rhs, ctx->st, ctx->fac, ns)));
     prof_mark(ctx);
-    dim3 gry((g.L + 31) / 32, g.N);
-    DISPATCH_S(g.M / 32, (k_ysweep<S><<<gry, SWEEP_NT, smem_y(g), s>>>(g, ctx->Q, ctx->RHS, ctx->part_rhs,
-                                                                        ctx->npart_rhs, ctx->st, ns)));
+    dim3 grz(g.L / 32, g.M, 3);
+    DISPATCH_S(g.N / 32, (k_zsweep<S><<<grz, SWEEP_NT, smem_z(g), s>>>(g, ctx->RHS, ctx->fac)));
+    prof_mark(ctx);
+    dim3 gry(g.L / 32, g.N);
+    DISPATCH_S(g.M / 32, (k_ysweep<S><<<gry, SWEEP_NT, smem_y(g), s>>>(g, ctx->Q, ctx->RHS, ctx->st, ctx->fac, ns)));
     prof_mark(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
     k_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->Q, ctx->RHSLL, ctx->SP, ctx->st, ns);
@@ -272,8 +286,7 @@ void launch_substep(chapsim_ctx* ctx, int ns) {
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
     k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
     prof_mark(ctx);
-    const long long nl = (long long)g.LH * g.N;
-    k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, s>>>(g, ctx->SP, ctx->HS);
+    launch_ysolve(ctx);
     prof_mark(ctx);
     k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
     prof_mark(ctx);
@@ -282,7 +295,7 @@ void launch_substep(chapsim_ctx* ctx, int ns) {
     const long long tot = (long long)g.L * g.M * g.N;
     k_correct<<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, ctx->Q, ctx->PR, ctx->DPH, ctx->RHSLL, ctx->st, ns);
     prof_mark(ctx);
-    ctx->launches += 9;
+    ctx->launches += 10;
 }
 
 int check_device_error(chapsim_ctx* ctx) {
@@ -423,8 +436,10 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaMalloc(&ctx->RHSLL, (size_t)g.FI * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->SP, (size_t)g.LH * M * N * sizeof(double2)));
     INIT_CK(cudaMalloc(&ctx->HS, (size_t)g.LH * M * N * sizeof(double)));
-    ctx->npart_rhs = ((M + RHS_TJ - 1) / RHS_TJ) * N;
+    ctx->npart_rhs = M * N / RHS_WPB;
     INIT_CK(cudaMalloc(&ctx->part_rhs, (size_t)ctx->npart_rhs * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->fac, (size_t)5 * FAC_SET * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->fac, 0, (size_t)5 * FAC_SET * sizeof(double)));
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
     ctx->npart_red = 4 * nsm;
@@ -456,7 +471,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red);
+    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -600,8 +615,7 @@ int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph) {
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
     k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
-    const long long nl = (long long)g.LH * g.N;
-    k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, s>>>(g, ctx->SP, ctx->HS);
+    launch_ysolve(ctx);
     k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
     k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
     ctx->launches += 5;
@@ -616,7 +630,7 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
     // One step = 2 + 3*9 kernels launched individually with an event after
     // each; ms[slot] accumulates the duration of kernel slot `slot` over the
     // nsteps steps (slot 0 is timed from an event recorded before it).
-    const int per = 2 + 3 * 9;
+    const int per = 2 + 3 * 10;
     if (!ctx || !ms || nslots < per || nsteps < 1) return CHAPSIM_ERR_BADARG;
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
@@ -664,7 +678,7 @@ int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count) {
 
 int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count) {
     if (!ctx || !count) return CHAPSIM_ERR_BADARG;
-    int per = 2 + 3 * 9;
+    int per = 2 + 3 * 10;
     *count = per;
     return CHAPSIM_OK;
 }

@@ -26,8 +26,9 @@ struct DevState {
     double cflgv;    // CFLGV
     double cflmm;    // last CFL maximum
     double maxdiv;   // last DIVGCK result
+    double bulksum;  // sum of RHS_u / DYFI over the grid (RHS_CvLpGpS_tg :168-181)
     unsigned int err;
-    unsigned int pad;
+    unsigned int ctr; // block-completion counter of the bulk-flux reduction
 };
 
 // Geometry and constant coefficients of one channel (passed by value).
@@ -100,4 +101,18 @@ __device__ __forceinline__ double block_max(double v, double* sbuf) {
         for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
     }
     return r;
+}
+
+// 8-byte asynchronous global -> shared copy (no register staging).
+__device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gsrc) : "memory");
 }

@@ -147,6 +147,75 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve(Geo g, double2* __restrict__ S
 }
 
 // ---------------------------------------------------------------------------
+// Same solve with 32 lines (consecutive q = kx + LH*kz) staged in shared
+// memory: the tile is brought in with asynchronous copies, one thread per
+// line runs the recurrence out of shared memory (Re and Im together), and
+// the forward-elimination factors stay in shared memory too.  For M <= 256.
+#define YS2_NT 128
+__global__ void __launch_bounds__(YS2_NT) k_ysolve_tile(Geo g, double2* __restrict__ SP) {
+    extern __shared__ double2 smc[];
+    const int M = g.M, LH = g.LH;
+    const long long nl = (long long)LH * g.N;
+    const long long q0 = (long long)blockIdx.x * 32;
+    const int nq = (int)min((long long)32, nl - q0);
+    double2* tile = smc;                       // [M][32]
+    double* hs = (double*)(smc + 32 * M);      // [M][32]
+    for (int p = threadIdx.x; p < 32 * M; p += YS2_NT) {
+        const int l = p & 31, j = p >> 5;
+        if (l < nq) {
+            const long long q = q0 + l;
+            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+            cp_async16(tile + p, SP + kx + (long long)LH * (j + (long long)M * kz));
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (threadIdx.x < nq) {
+        const int l = threadIdx.x;
+        const long long q = q0 + l;
+        const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+        const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+        const bool zero = (kx == 0 && kz == 0);
+        double b = g.acph[1] + shift;
+        double c = zero ? 0.0 : g.apph[1];
+        double2 r = tile[l];
+        if (zero) r = make_double2(0.0, 0.0);
+        double hp = c / b;
+        double2 gp = make_double2(r.x / b, r.y / b);
+        hs[l] = hp;
+        tile[l] = gp;
+        for (int j = 2; j <= M; ++j) {
+            const double a = g.amph[j];
+            const double bj = g.acph[j] + shift;
+            const double pp = 1.0 / (bj - hp * a);
+            const double2 rj = tile[(j - 1) * 32 + l];
+            gp = make_double2((rj.x - a * gp.x) * pp, (rj.y - a * gp.y) * pp);
+            if (j < M) {
+                hp = g.apph[j] * pp;
+                hs[(j - 1) * 32 + l] = hp;
+            }
+            tile[(j - 1) * 32 + l] = gp;
+        }
+        double2 xn = gp;
+        for (int j = M - 1; j >= 1; --j) {
+            const double hj = hs[(j - 1) * 32 + l];
+            const double2 gj = tile[(j - 1) * 32 + l];
+            xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
+            tile[(j - 1) * 32 + l] = xn;
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < 32 * M; p += YS2_NT) {
+        const int l = p & 31, j = p >> 5;
+        if (l < nq) {
+            const long long q = q0 + l;
+            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+            SP[kx + (long long)LH * (j + (long long)M * kz)] = tile[p];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(PX_NT) k_fftx_inv(Geo g, const double2* __restrict__ SP, double* __restrict__ DPH) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, LH = g.LH;
@@ -191,12 +260,18 @@ __global__ void __launch_bounds__(CR_NT) k_correct(Geo g, double* __restrict__ Q
     const int k = (int)(r / M);
     const double dt = st->dt, ta = g.talp[ns];
     const long long c = pidx(g, i, j, k);
+    // all loads first: Q is read and written through one pointer
     const double ph = DPH[c];
-    Q[c] = Q[c] - (ph - DPH[pidx(g, wrapm(i, L), j, k)]) * (dt * ta * g.dxi);
-    Q[c + 2 * g.FS] = Q[c + 2 * g.FS] - (ph - DPH[pidx(g, i, j, wrapm(k, N))]) * (dt * ta * g.dzi);
-    if (j >= 2) Q[c + g.FS] = Q[c + g.FS] - (ph - DPH[pidx(g, i, j - 1, k)]) * (dt * ta * g.dyci[j] / 1.0);
+    const double phim = DPH[pidx(g, wrapm(i, L), j, k)];
+    const double phkm = DPH[pidx(g, i, j, wrapm(k, N))];
+    const double phjm = j >= 2 ? DPH[pidx(g, i, j - 1, k)] : 0.0;
+    const double u = Q[c], v = Q[c + g.FS], w = Q[c + 2 * g.FS];
+    const double pr = PR[c], ll = RHSLL[iidx(g, i, j, k)];
+    Q[c] = u - (ph - phim) * (dt * ta * g.dxi);
+    Q[c + 2 * g.FS] = w - (ph - phkm) * (dt * ta * g.dzi);
+    if (j >= 2) Q[c + g.FS] = v - (ph - phjm) * (dt * ta * g.dyci[j] / 1.0);
     const double be = 0.5 * ta * dt * g.cvisc * 1.0 / 1.0;
-    const double pn = PR[c] + ph - be * RHSLL[iidx(g, i, j, k)];
+    const double pn = pr + ph - be * ll;
     PR[c] = pn;
     if (j == 1) PR[pidx(g, i, 0, k)] = pn;
     if (j == M) PR[pidx(g, i, M + 1, k)] = pn;

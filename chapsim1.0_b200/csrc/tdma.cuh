@@ -177,3 +177,202 @@ __device__ __forceinline__ void warp_tdma_smem(double* base, const Coef& cf, int
 #pragma unroll
     for (int k = 0; k < S; ++k) base[lane * (S + 1) + k] = d[k];
 }
+
+// ---------------------------------------------------------------------------
+// Factorised form of warp_tdma for systems whose coefficients are the same
+// for every line of a batch (the constant-coefficient x and z sweeps, and
+// the y sweep whose coefficients depend on the row only).  warp_tdma_factor
+// runs the coefficient part of the algorithm once and stores, per lane, the
+// multipliers it produces; warp_tdma_apply then performs only the
+// right-hand-side part: a few FMAs per row and one shuffle per reduction
+// step.  The factor table of one system is TF_NF(S) x 32 doubles, laid out
+// [item][lane] so that a warp reads it with coalesced accesses.
+#define TF_NF(S) (5 * (S) + 20)
+
+template <int S, bool CYCLIC, class Coef>
+__device__ void warp_tdma_factor(const Coef& cf, int lane, double* __restrict__ fac) {
+    const int r0 = lane * S;
+    // item layout: [0,S) r, [S,2S) a, [2S,3S) cq(fwd), [3S,4S) ap(final), [4S,5S) cq(final),
+    //   5S+0 c0, +1 aL, +2 A0, +3 C0, +4 iB0, +5 ra, +6 rb, +7..+11 k1[5], +12..+16 k2[5], +17 f1, +18 f2, +19 unused
+    double rr[S > 2 ? S : 1], aa[S > 2 ? S : 1], cqf[S > 2 ? S : 1], ap[S > 2 ? S : 1], cq[S > 2 ? S : 1];
+    double A0, B0, C0, A1, B1, C1, c0 = 0.0, aL = 0.0;
+#pragma unroll
+    for (int k = 0; k < (S > 2 ? S : 1); ++k) { rr[k] = aa[k] = cqf[k] = ap[k] = cq[k] = 0.0; }
+    if constexpr (S == 1) {
+        A0 = cf.A(r0); B0 = cf.B(r0); C0 = cf.C(r0);
+        A1 = B1 = C1 = 0.0;
+    } else if constexpr (S == 2) {
+        A0 = cf.A(r0); B0 = cf.B(r0); C0 = cf.C(r0);
+        A1 = cf.A(r0 + 1); B1 = cf.B(r0 + 1); C1 = cf.C(r0 + 1);
+    } else {
+        rr[1] = 1.0 / cf.B(r0 + 1);
+        ap[1] = cf.A(r0 + 1) * rr[1];
+        cq[1] = cf.C(r0 + 1) * rr[1];
+#pragma unroll
+        for (int k = 2; k <= S - 2; ++k) {
+            aa[k] = cf.A(r0 + k);
+            rr[k] = 1.0 / (cf.B(r0 + k) - aa[k] * cq[k - 1]);
+            ap[k] = -aa[k] * ap[k - 1] * rr[k];
+            cq[k] = cf.C(r0 + k) * rr[k];
+        }
+#pragma unroll
+        for (int k = 0; k < S; ++k) cqf[k] = cq[k];
+#pragma unroll
+        for (int k = S - 3; k >= 1; --k) {
+            ap[k] = ap[k] - cq[k] * ap[k + 1];
+            cq[k] = -cq[k] * cq[k + 1];
+        }
+        c0 = cf.C(r0);
+        A0 = cf.A(r0);
+        B0 = cf.B(r0) - c0 * ap[1];
+        C0 = -c0 * cq[1];
+        aL = cf.A(r0 + S - 1);
+        A1 = -aL * ap[S - 2];
+        B1 = cf.B(r0 + S - 1) - aL * cq[S - 2];
+        C1 = cf.C(r0 + S - 1);
+    }
+    if constexpr (!CYCLIC) {
+        if (lane == 0) A0 = 0.0;
+        if (lane == 31) { if constexpr (S == 1) C0 = 0.0; else C1 = 0.0; }
+    }
+    double al, be, ga, iB0 = 1.0, ra = 0.0, rb = 0.0;
+    if constexpr (S == 1) {
+        al = A0; be = B0; ga = C0;
+    } else {
+        const int nx = (lane + 1) & 31;
+        double A0n = __shfl_sync(0xffffffffu, A0, nx);
+        double B0n = __shfl_sync(0xffffffffu, B0, nx);
+        double C0n = __shfl_sync(0xffffffffu, C0, nx);
+        iB0 = 1.0 / B0;
+        double iB0n = 1.0 / B0n;
+        al = -A1 * A0 * iB0;
+        be = B1 - A1 * C0 * iB0 - C1 * A0n * iB0n;
+        ga = -C1 * C0n * iB0n;
+        ra = A1 * iB0;
+        rb = C1 * iB0n;
+    }
+    double k1s[5] = {0, 0, 0, 0, 0}, k2s[5] = {0, 0, 0, 0, 0};
+    double f1, f2 = 0.0;
+    const int nsteps = CYCLIC ? 4 : 5;
+#pragma unroll
+    for (int st = 0; st < 5; ++st) {
+        if (st >= nsteps) break;
+        const int s = 1 << st;
+        const double lal = __shfl_sync(0xffffffffu, al, (lane - s) & 31);
+        const double lbe = __shfl_sync(0xffffffffu, be, (lane - s) & 31);
+        const double lga = __shfl_sync(0xffffffffu, ga, (lane - s) & 31);
+        const double hal = __shfl_sync(0xffffffffu, al, (lane + s) & 31);
+        const double hbe = __shfl_sync(0xffffffffu, be, (lane + s) & 31);
+        const double hga = __shfl_sync(0xffffffffu, ga, (lane + s) & 31);
+        bool hasl = CYCLIC || lane - s >= 0, hash = CYCLIC || lane + s <= 31;
+        double k1 = hasl ? al / lbe : 0.0;
+        double k2 = hash ? ga / hbe : 0.0;
+        double nal = hasl ? -k1 * lal : 0.0;
+        double nga = hash ? -k2 * hga : 0.0;
+        double nbe = be - (hasl ? k1 * lga : 0.0) - (hash ? k2 * hal : 0.0);
+        k1s[st] = k1; k2s[st] = k2;
+        al = nal; be = nbe; ga = nga;
+    }
+    if constexpr (CYCLIC) {
+        const double pal = __shfl_sync(0xffffffffu, al, lane ^ 16);
+        const double pbe = __shfl_sync(0xffffffffu, be, lane ^ 16);
+        const double pga = __shfl_sync(0xffffffffu, ga, lane ^ 16);
+        const double ci = al + ga, cm = pal + pga;
+        const double inv = 1.0 / (be * pbe - ci * cm);
+        f1 = pbe * inv;
+        f2 = -ci * inv;
+    } else {
+        f1 = 1.0 / be;
+    }
+    double* f = fac + lane;
+#pragma unroll
+    for (int k = 0; k < S; ++k) {
+        if constexpr (S > 2) {
+            f[(0 * S + k) * 32] = rr[k];
+            f[(1 * S + k) * 32] = aa[k];
+            f[(2 * S + k) * 32] = cqf[k];
+            f[(3 * S + k) * 32] = ap[k];
+            f[(4 * S + k) * 32] = cq[k];
+        } else {
+            f[(0 * S + k) * 32] = 0.0;
+            f[(1 * S + k) * 32] = 0.0;
+            f[(2 * S + k) * 32] = 0.0;
+            f[(3 * S + k) * 32] = 0.0;
+            f[(4 * S + k) * 32] = 0.0;
+        }
+    }
+    const int b = 5 * S;
+    f[(b + 0) * 32] = c0; f[(b + 1) * 32] = aL; f[(b + 2) * 32] = A0; f[(b + 3) * 32] = C0;
+    f[(b + 4) * 32] = iB0; f[(b + 5) * 32] = ra; f[(b + 6) * 32] = rb;
+#pragma unroll
+    for (int st = 0; st < 5; ++st) { f[(b + 7 + st) * 32] = k1s[st]; f[(b + 12 + st) * 32] = k2s[st]; }
+    f[(b + 17) * 32] = f1; f[(b + 18) * 32] = f2;
+}
+
+// Right-hand-side part of the solve; d[k] = rhs of row lane*S+k in, solution out.
+template <int S, bool CYCLIC>
+__device__ __forceinline__ void warp_tdma_apply(double (&d)[S], const double* __restrict__ fac, int lane) {
+    const double* f = fac + lane;
+    const int b = 5 * S;
+    double D0, D1;
+    if constexpr (S >= 3) {
+        d[1] *= f[(0 * S + 1) * 32];
+#pragma unroll
+        for (int k = 2; k <= S - 2; ++k) d[k] = (d[k] - f[(1 * S + k) * 32] * d[k - 1]) * f[(0 * S + k) * 32];
+#pragma unroll
+        for (int k = S - 3; k >= 1; --k) d[k] = d[k] - f[(2 * S + k) * 32] * d[k + 1];
+        D0 = d[0] - f[(b + 0) * 32] * d[1];
+        D1 = d[S - 1] - f[(b + 1) * 32] * d[S - 2];
+    } else if constexpr (S == 2) {
+        D0 = d[0];
+        D1 = d[1];
+    } else {
+        D0 = d[0];
+        D1 = 0.0;
+    }
+    double de;
+    if constexpr (S == 1) {
+        de = D0;
+    } else {
+        const double D0n = __shfl_sync(0xffffffffu, D0, (lane + 1) & 31);
+        de = D1 - f[(b + 5) * 32] * D0 - f[(b + 6) * 32] * D0n;
+    }
+    const int nsteps = CYCLIC ? 4 : 5;
+#pragma unroll
+    for (int st = 0; st < 5; ++st) {
+        if (st >= nsteps) break;
+        const int s = 1 << st;
+        const double lo = __shfl_sync(0xffffffffu, de, (lane - s) & 31);
+        const double hi = __shfl_sync(0xffffffffu, de, (lane + s) & 31);
+        de = de - f[(b + 7 + st) * 32] * lo - f[(b + 12 + st) * 32] * hi;
+    }
+    double u;
+    if constexpr (CYCLIC) {
+        const double pd = __shfl_sync(0xffffffffu, de, lane ^ 16);
+        u = de * f[(b + 17) * 32] + pd * f[(b + 18) * 32];
+    } else {
+        u = de * f[(b + 17) * 32];
+    }
+    if constexpr (S == 1) {
+        d[0] = u;
+    } else {
+        const double up = __shfl_sync(0xffffffffu, u, (lane - 1) & 31);
+        const double y0 = (D0 - f[(b + 2) * 32] * up - f[(b + 3) * 32] * u) * f[(b + 4) * 32];
+        d[0] = y0;
+        d[S - 1] = u;
+        if constexpr (S > 2) {
+#pragma unroll
+            for (int k = 1; k <= S - 2; ++k) d[k] = d[k] - f[(3 * S + k) * 32] * y0 - f[(4 * S + k) * 32] * u;
+        }
+    }
+}
+
+template <int S, bool CYCLIC>
+__device__ __forceinline__ void warp_tdma_apply_smem(double* base, const double* __restrict__ fac, int lane) {
+    double d[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) d[k] = base[lane * (S + 1) + k];
+    warp_tdma_apply<S, CYCLIC>(d, fac, lane);
+#pragma unroll
+    for (int k = 0; k < S; ++k) base[lane * (S + 1) + k] = d[k];
+}
