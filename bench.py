@@ -48,7 +48,7 @@ L2_BYTES = 126 * 1024 * 1024
 def kernel_words(L):
     spec = 2.0 * (L // 2 + 1) / L  # complex spectrum, words per point
     return {
-        "k_cfl": 3.0, "k_dt": 0.0, "k_factors": 0.0,
+        "k_cfl": 3.0, "k_dt_factors": 0.0,
         "k_rhs_xsweep": 13.0,          # Q x3, PR, H0 x3 in; H0 x3, RHS x3 out
         "k_zsweep": 6.0,               # RHS x3 in/out
         "k_ysweep": 9.0,               # RHS x3, Q x3 in; Q x3 out
@@ -263,7 +263,7 @@ def run_b200(args):
     # ---- per-kernel durations (CUDA events on the library stream) ----
     prof_steps = max(1, min(20, args.steps))
     kms = ch.profile_steps(prof_steps, DT0, DTMIN, CFLGV)
-    launches_per_step = {k: (1 if k in ("k_cfl", "k_dt") else 3) for k in kms}
+    launches_per_step = {k: (1 if k in ("k_cfl", "k_dt_factors") else 3) for k in kms}
     words = kernel_words(L)
     peak, peak_kind = load_peaks()
     per_launch = {k: kms[k] / (prof_steps * launches_per_step[k]) for k in kms}

@@ -17,7 +17,7 @@ import numpy as np
 from .mesh import ChannelSetup, channel_setup
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libchapsim_gpu.so")
+LIB_PATH = os.environ.get("CHAPSIM_GPU_LIB", os.path.join(_HERE, "libchapsim_gpu.so"))
 
 _dp = ctypes.POINTER(ctypes.c_double)
 
@@ -31,7 +31,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_profile_steps", "chapsim_get_stream",
             "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step"]
 
-KERNEL_SLOTS = ["k_cfl", "k_dt"] + ["k_factors", "k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
+KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
 
 

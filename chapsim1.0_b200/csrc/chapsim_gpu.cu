@@ -131,7 +131,8 @@ struct chapsim_ctx {
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr, *HS = nullptr;
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
-    double* fac = nullptr;       // factor tables of the x, z, y sweeps
+    double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
+    double *ppt = nullptr, *ht = nullptr;  // Poisson y-solve elimination factors
     int npart_rhs = 0;
     double* part_red = nullptr;  // per-block CFL / divergence maxima
     int npart_red = 0;
@@ -206,14 +207,14 @@ size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(double);
 size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(double); }
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * g.L) * sizeof(double2); }
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * (g.N + 1)) * sizeof(double2); }
-size_t smem_ys(const Geo& g) { return (size_t)(32 * g.M) * (sizeof(double2) + sizeof(double)); }
-bool use_ys_tile(const Geo& g) { return g.M <= 256; }
+size_t smem_ys(const Geo& g) { return (size_t)(YS_L * g.M) * (sizeof(double2) + 2 * sizeof(double)); }
+bool use_ys_tile(const Geo& g) { return true; }
 
 void launch_ysolve(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
     if (use_ys_tile(g))
-        k_ysolve_tile<<<(int)((nl + 31) / 32), YS2_NT, smem_ys(g), ctx->stream>>>(g, ctx->SP);
+        k_ysolve_tile<<<(int)((nl + YS_L - 1) / YS_L), YS2_NT, smem_ys(g), ctx->stream>>>(g, ctx->SP, ctx->ppt, ctx->ht);
     else
         k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, ctx->stream>>>(g, ctx->SP, ctx->HS);
 }
@@ -255,6 +256,16 @@ inline void prof_mark(chapsim_ctx* ctx) {
     if (ctx->prof_ev) cudaEventRecord(ctx->prof_ev[ctx->prof_n++], ctx->stream);
 }
 
+// CFL partials, then the dt rule fused with the factor tables of all three substeps
+void launch_step_start(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    k_cfl<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
+    prof_mark(ctx);
+    k_dt_factors<<<15, 32, 0, ctx->stream>>>(g, ctx->part_red, ctx->npart_red, ctx->st, ctx->fac);
+    prof_mark(ctx);
+    ctx->launches += 2;
+}
+
 void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
     const Geo& g = ctx->g;
     k_cfl<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
@@ -264,20 +275,24 @@ void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
     ctx->launches += 2;
 }
 
-void launch_substep(chapsim_ctx* ctx, int ns) {
+void launch_substep(chapsim_ctx* ctx, int ns, bool factors = true) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    k_factors<<<5, 32, 0, s>>>(g, ctx->fac, ctx->st, ns);
-    prof_mark(ctx);
+    double* fac = ctx->fac + (long long)ns * 5 * FAC_SET;
+    if (factors) {
+        k_factors<<<5, 32, 0, s>>>(g, fac, ctx->st, ns);
+        prof_mark(ctx);
+        ctx->launches += 1;
+    }
     const int grx = g.M * g.N / RHS_WPB;
     DISPATCH_S(g.L / 32, (k_rhs_xsweep<S><<<grx, RHS_WPB * 32, smem_rhs(g), s>>>(g, ctx->Q, ctx->PR, ctx->H0, ctx->RHS,
-                                                                                   ctx->part_rhs, ctx->st, ctx->fac, ns)));
+                                                                                   ctx->part_rhs, ctx->st, fac, ns)));
     prof_mark(ctx);
     dim3 grz(g.L / 32, g.M, 3);
-    DISPATCH_S(g.N / 32, (k_zsweep<S><<<grz, SWEEP_NT, smem_z(g), s>>>(g, ctx->RHS, ctx->fac)));
+    DISPATCH_S(g.N / 32, (k_zsweep<S><<<grz, SWEEP_NT, smem_z(g), s>>>(g, ctx->RHS, fac)));
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N);
-    DISPATCH_S(g.M / 32, (k_ysweep<S><<<gry, SWEEP_NT, smem_y(g), s>>>(g, ctx->Q, ctx->RHS, ctx->st, ctx->fac, ns)));
+    DISPATCH_S(g.M / 32, (k_ysweep<S><<<gry, SWEEP_NT, smem_y(g), s>>>(g, ctx->Q, ctx->RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
     k_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->Q, ctx->RHSLL, ctx->SP, ctx->st, ns);
@@ -295,7 +310,7 @@ void launch_substep(chapsim_ctx* ctx, int ns) {
     const long long tot = (long long)g.L * g.M * g.N;
     k_correct<<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, ctx->Q, ctx->PR, ctx->DPH, ctx->RHSLL, ctx->st, ns);
     prof_mark(ctx);
-    ctx->launches += 10;
+    ctx->launches += 9;
 }
 
 int check_device_error(chapsim_ctx* ctx) {
@@ -317,8 +332,8 @@ int build_step_graph(chapsim_ctx* ctx) {
     cudaGraph_t graph;
     unsigned long long before = ctx->launches;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    launch_cfl_dt(ctx, 1);
-    for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns);
+    launch_step_start(ctx);
+    for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns, false);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     ctx->kernels_per_step = (int)(ctx->launches - before);
     ctx->launches = before;  // capture does not launch
@@ -438,8 +453,11 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaMalloc(&ctx->HS, (size_t)g.LH * M * N * sizeof(double)));
     ctx->npart_rhs = M * N / RHS_WPB;
     INIT_CK(cudaMalloc(&ctx->part_rhs, (size_t)ctx->npart_rhs * sizeof(double)));
-    INIT_CK(cudaMalloc(&ctx->fac, (size_t)5 * FAC_SET * sizeof(double)));
-    INIT_CK(cudaMemset(ctx->fac, 0, (size_t)5 * FAC_SET * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->fac, (size_t)4 * 5 * FAC_SET * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->fac, 0, (size_t)4 * 5 * FAC_SET * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->ppt, (size_t)g.LH * M * N * sizeof(double)));
+    INIT_CK(cudaMalloc(&ctx->ht, (size_t)g.LH * M * N * sizeof(double)));
+
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
     ctx->npart_red = 4 * nsm;
@@ -460,6 +478,13 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         chapsim_gpu_finalize(ctx);
         return rc;
     }
+    {
+        const long long nl = (long long)g.LH * N;
+        k_ysolve_factors<<<(int)((nl + 127) / 128), 128, 0, ctx->stream>>>(g, ctx->ppt, ctx->ht);
+        INIT_CK(cudaGetLastError());
+        INIT_CK(cudaStreamSynchronize(ctx->stream));
+    }
+
 #undef INIT_CK
     *out = ctx;
     return CHAPSIM_OK;
@@ -471,7 +496,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
+    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac); cudaFree(ctx->ppt); cudaFree(ctx->ht);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -630,7 +655,7 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
     // One step = 2 + 3*9 kernels launched individually with an event after
     // each; ms[slot] accumulates the duration of kernel slot `slot` over the
     // nsteps steps (slot 0 is timed from an event recorded before it).
-    const int per = 2 + 3 * 10;
+    const int per = 2 + 3 * 9;
     if (!ctx || !ms || nslots < per || nsteps < 1) return CHAPSIM_ERR_BADARG;
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
@@ -642,8 +667,8 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
         CK(cudaEventRecord(ev[0], ctx->stream));
         ctx->prof_ev = ev.data() + 1;
         ctx->prof_n = 0;
-        launch_cfl_dt(ctx, 1);
-        for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns);
+        launch_step_start(ctx);
+        for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns, false);
         ctx->prof_ev = nullptr;
         CK(cudaGetLastError());
         CK(cudaEventSynchronize(ev[per]));
@@ -678,7 +703,7 @@ int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count) {
 
 int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count) {
     if (!ctx || !count) return CHAPSIM_ERR_BADARG;
-    int per = 2 + 3 * 10;
+    int per = 2 + 3 * 9;
     *count = per;
     return CHAPSIM_OK;
 }

@@ -27,6 +27,7 @@ struct DevState {
     double cflmm;    // last CFL maximum
     double maxdiv;   // last DIVGCK result
     double bulksum;  // sum of RHS_u / DYFI over the grid (RHS_CvLpGpS_tg :168-181)
+    double dtprev;   // DT of the previous step, read by the fused dt/factor kernel
     unsigned int err;
     unsigned int ctr; // block-completion counter of the bulk-flux reduction
 };

@@ -7,6 +7,7 @@
 //   k_bc_fields  BC_WALL_Q_tg / BC_WALL_PR_tg ghost planes (src/BC_WALL.f90:212-361)
 #pragma once
 #include "common.cuh"
+#include "momentum.cuh"
 
 #define DG_NT 256
 
@@ -30,6 +31,7 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const double* __restrict__
         mx = fmax(mx, q);
     }
     if (bad) atomicOr(&st->err, CHS_EBIT_NAN);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->dtprev = st->dt;
     double r = block_max<DG_NT>(mx, sred);
     if (threadIdx.x == 0) partial[blockIdx.x] = r;
 }
@@ -91,5 +93,29 @@ __global__ void __launch_bounds__(DG_NT) k_bc_fields(Geo g, double* __restrict__
         Q[b0] = 0.0; Q[b0 + 2 * g.FS] = 0.0; Q[b1 + g.FS] = 0.0; Q[b0 + g.FS] = 0.0;
         PR[bt] = PR[bm];
         PR[b0] = PR[b1];
+    }
+}
+
+// Step start of the captured graph: every block reduces the CFL partials
+// (order-independent maximum), applies the dt rule of BCAST_COMM_STEP, and
+// computes one factor table of one substep (block b: substep 1 + b / 5,
+// set b % 5).  Block 0 publishes CFLMM and DT.
+__global__ void __launch_bounds__(32) k_dt_factors(Geo g, const double* __restrict__ partial, int np,
+                                                   DevState* __restrict__ st, double* __restrict__ fac) {
+    const int lane = threadIdx.x;
+    double mx = 0.0;
+    for (int t = lane; t < np; t += 32) mx = fmax(mx, partial[t]);
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    const double c = mx;
+    double dt = fmin(fmin(st->dt0, 5.0 * st->dtprev), st->cflgv / c);
+    dt = fmax(dt, st->dtmin);
+    const int ns = 1 + blockIdx.x / 5, set = blockIdx.x % 5;
+    factor_set(g, dt, ns, set, fac + (long long)(ns * 5 + set) * FAC_SET, lane);
+    __syncwarp();
+    if (blockIdx.x == 0 && lane == 0) {
+        st->cflmm = c;
+        st->dt = dt;
+        if ((dt / st->dt0) < 0.01) atomicOr(&st->err, CHS_EBIT_DT_COLLAPSE);
+        if (!(dt == dt)) atomicOr(&st->err, CHS_EBIT_NAN);
     }
 }

@@ -29,6 +29,9 @@
 #include "tdma.cuh"
 
 #define RHS_WPB 4       // x lines (warps) per block
+#ifndef RHS_MINB
+#define RHS_MINB 4      // resident blocks per SM the register budget is sized for
+#endif
 #define SWEEP_NT 256
 #define FAC_SET (TF_NF(12) * 32)   // doubles per factor table
 
@@ -59,33 +62,36 @@ __device__ void factor_dispatch(int S, const C& cf, int lane, double* fac) {
     }
 }
 
-// block b computes set b: 0 x sweep, 1 z sweep, 2..4 y sweep of u, v, w
-__global__ void __launch_bounds__(32) k_factors(Geo g, double* __restrict__ fac, const DevState* __restrict__ st, int ns) {
-    const int lane = threadIdx.x;
-    const double facoe = 0.5 * g.talp[ns] * st->dt * g.cvisc * 1.0 / 1.0;
-    double* f = fac + (long long)blockIdx.x * FAC_SET;
-    if (blockIdx.x == FSET_X) {
+__device__ __forceinline__ void factor_set(const Geo& g, double dt, int ns, int set, double* f, int lane) {
+    const double facoe = 0.5 * g.talp[ns] * dt * g.cvisc * 1.0 / 1.0;
+    if (set == FSET_X) {
         ConstCoef cf;
         cf.a = -facoe * g.dxqi;  // MOMFA1_X_tg :72-78
         cf.c = cf.a;
         cf.b = 1.0 - cf.c - cf.a;
         factor_dispatch<true>(g.L / 32, cf, lane, f);
-    } else if (blockIdx.x == FSET_Z) {
+    } else if (set == FSET_Z) {
         ConstCoef cf;
         cf.a = 1.0 * (-facoe * g.dzqi);  // MOMFA2_Z_tg :133-155
         cf.c = cf.a;
         cf.b = 1.0 - cf.c - cf.a;
         factor_dispatch<true>(g.N / 32, cf, lane, f);
     } else {
-        const int comp = blockIdx.x - FSET_Y;
+        const int comp = set - FSET_Y;
         YCoef cf{g.amvr + comp * (g.M + 2), g.acvr + comp * (g.M + 2), g.apvr + comp * (g.M + 2), facoe};
         factor_dispatch<false>(g.M / 32, cf, lane, f);
     }
 }
 
+// Factor tables of one substep (block b computes set b: 0 x sweep, 1 z
+// sweep, 2..4 y sweep of u, v, w) for the device-resident DT.
+__global__ void __launch_bounds__(32) k_factors(Geo g, double* __restrict__ fac, const DevState* __restrict__ st, int ns) {
+    factor_set(g, st->dt, ns, blockIdx.x, fac + (long long)blockIdx.x * FAC_SET, threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 template <int S>
-__global__ void __launch_bounds__(RHS_WPB * 32, 4) k_rhs_xsweep(Geo g, const double* __restrict__ Q, const double* __restrict__ PR,
+__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB) k_rhs_xsweep(Geo g, const double* __restrict__ Q, const double* __restrict__ PR,
                                                              double* __restrict__ H0, double* __restrict__ RHS,
                                                              double* __restrict__ partial, DevState* __restrict__ st,
                                                              const double* __restrict__ fac, int ns) {
@@ -111,6 +117,7 @@ __global__ void __launch_bounds__(RHS_WPB * 32, 4) k_rhs_xsweep(Geo g, const dou
     const double c3x = 0.5 * 0.5 * g.dzi;
     const double wffj = g.wff[j], wfbj = g.wfb[j], wffp = g.wff[jp], wfbp = g.wfb[jp];
     const double dyfij = g.dyfi[j], dycij = g.dyci[j];
+    const double dyj = 1.0 / dyfij / 1.0;  // cell height in the bulk-flux integrand
     const double amu = g.amvr[j], acu = g.acvr[j], apu = g.apvr[j];
     const double amv = g.amvr[(M + 2) + j], acv = g.acvr[(M + 2) + j], apv = g.apvr[(M + 2) + j];
     const double amw = g.amvr[2 * (M + 2) + j], acw = g.acvr[2 * (M + 2) + j], apw = g.apvr[2 * (M + 2) + j];
@@ -156,7 +163,7 @@ __global__ void __launch_bounds__(RHS_WPB * 32, 4) k_rhs_xsweep(Geo g, const dou
                                         (ujp * apu + u * acu + ujm * amu));
             double r = (rhsc + rhsl) * dt;
             ru = r - (pc - pim) * g.dxi * coep;
-            bulk += ru / dyfij / 1.0;
+            bulk += ru * dyj;
         }
         // ---------------- v (CONVECTION_Y_tg), j >= 2 ----------------
         if (j >= 2) {

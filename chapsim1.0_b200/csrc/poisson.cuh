@@ -21,7 +21,7 @@
 #include "common.cuh"
 #include "fft.cuh"
 
-#define PX_TJ 8   // x-lines per block (4 packed pairs)
+#define PX_TJ 32  // x-lines per block (16 packed pairs)
 #define PX_NT 256
 #define FZ_TQ 16  // z-lines per block
 #define FZ_NT 256
@@ -42,18 +42,20 @@ __global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const double* __restr
     const double* U = Q;
     const double* V = Q + g.FS;
     const double* W = Q + 2 * g.FS;
+    const double coe1 = g.dxi / 1.0;
+#pragma unroll 4
     for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
         const int jl = p / L, i = p - jl * L;
         const int pair = jl >> 1, part = jl & 1;
         double val = 0.0;
         if (jl < nj) {
             const int j = j0 + jl;
-            const int ip = wrapp(i, L);
-            const double coe1 = g.dxi / 1.0;
-            const double coe2 = g.dyfi[j] / 1.0;
             const long long c = pidx(g, i, j, k);
-            const double dv = (U[pidx(g, ip, j, k)] - U[c]) * coe1 + (V[pidx(g, i, j + 1, k)] - V[c]) * coe2 +
-                              (W[pidx(g, i, j, kp)] - W[c]) * g.dzi;
+            const double u = U[c], up = U[pidx(g, wrapp(i, L), j, k)];
+            const double v = V[c], vp = V[c + L];
+            const double w = W[c], wp = W[pidx(g, i, j, kp)];
+            const double coe2 = g.dyfi[j] / 1.0;
+            const double dv = (up - u) * coe1 + (vp - v) * coe2 + (wp - w) * g.dzi;
             val = dv * coe0;
             RHSLL[iidx(g, i, j, k)] = val;
         }
@@ -88,8 +90,9 @@ __global__ void __launch_bounds__(FZ_NT) k_fftz(Geo g, double2* __restrict__ SP)
     const int nq = (int)min((long long)FZ_TQ, Q - q0);
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
         const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
-        if (ql < nq) smc[ql * (N + 1) + g.permz[kz]] = SP[q0 + ql + Q * kz];
+        if (ql < nq) cp_async16(smc + ql * (N + 1) + g.permz[kz], SP + q0 + ql + Q * kz);
     }
+    cp_async_wait_all();
     block_fft<SIGN>(smc, N, nq, N + 1, g.twz, g.radz, g.nradz);
     const double sc = SIGN < 0 ? 1.0 / (double)N : 1.0;
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
@@ -147,66 +150,89 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve(Geo g, double2* __restrict__ S
 }
 
 // ---------------------------------------------------------------------------
-// Same solve with 32 lines (consecutive q = kx + LH*kz) staged in shared
-// memory: the tile is brought in with asynchronous copies, one thread per
-// line runs the recurrence out of shared memory (Re and Im together), and
-// the forward-elimination factors stay in shared memory too.  For M <= 256.
-#define YS2_NT 128
-__global__ void __launch_bounds__(YS2_NT) k_ysolve_tile(Geo g, double2* __restrict__ SP) {
+// The coefficients of the per-(kx, kz) systems do not change during a run
+// (TDMA_PHI_COEF, src/possion3d_FFT99.f90:204-239), so the elimination
+// factors of the reference's Thomas recurrence (TDMAIJJ_nonCYC :95-121) are
+// computed once at initialisation, one thread per line, in the layout of the
+// spectral array: PPT(j) = 1/(B_j - H_{j-1} A_j) (row 1 holds B_1 itself: the
+// reference divides there) and HT(j) = C_j PPT(j).
+__global__ void k_ysolve_factors(Geo g, double* __restrict__ PPT, double* __restrict__ HT) {
+    const int M = g.M, LH = g.LH;
+    const long long nl = (long long)LH * g.N;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nl) return;
+    const int kz = (int)(t / LH), kx = (int)(t - (long long)kz * LH);
+    const long long base = kx + (long long)LH * (long long)M * kz;
+    const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+    const bool zero = (kx == 0 && kz == 0);
+    const double b = g.acph[1] + shift;
+    const double c = zero ? 0.0 : g.apph[1];
+    double hp = c / b;
+    PPT[base] = b;
+    HT[base] = hp;
+    for (int j = 2; j <= M; ++j) {
+        const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
+        PPT[base + (long long)(j - 1) * LH] = pp;
+        hp = j < M ? g.apph[j] * pp : 0.0;
+        HT[base + (long long)(j - 1) * LH] = hp;
+    }
+}
+
+// y solve of YS_L lines (consecutive q = kx + LH*kz) per block.  The data
+// tile and the factor columns are brought into shared memory with
+// asynchronous copies; lane l of warp 0 then runs the recurrence of line
+// l % YS_L for the real (l < YS_L) or imaginary part out of shared memory.
+#define YS_L 16
+#define YS2_NT 64
+__global__ void __launch_bounds__(YS2_NT) k_ysolve_tile(Geo g, double2* __restrict__ SP, const double* __restrict__ PPT,
+                                                        const double* __restrict__ HT) {
     extern __shared__ double2 smc[];
     const int M = g.M, LH = g.LH;
     const long long nl = (long long)LH * g.N;
-    const long long q0 = (long long)blockIdx.x * 32;
-    const int nq = (int)min((long long)32, nl - q0);
-    double2* tile = smc;                       // [M][32]
-    double* hs = (double*)(smc + 32 * M);      // [M][32]
-    for (int p = threadIdx.x; p < 32 * M; p += YS2_NT) {
-        const int l = p & 31, j = p >> 5;
+    const long long q0 = (long long)blockIdx.x * YS_L;
+    const int nq = (int)min((long long)YS_L, nl - q0);
+    double2* tile = smc;                        // [M][YS_L] complex
+    double* pt = (double*)(smc + YS_L * M);     // [M][YS_L]
+    double* ht = pt + YS_L * M;                 // [M][YS_L]
+    for (int p = threadIdx.x; p < YS_L * M; p += YS2_NT) {
+        const int l = p % YS_L, j = p / YS_L;
         if (l < nq) {
             const long long q = q0 + l;
             const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-            cp_async16(tile + p, SP + kx + (long long)LH * (j + (long long)M * kz));
+            const long long o = kx + (long long)LH * (j + (long long)M * kz);
+            cp_async16(tile + p, SP + o);
+            cp_async8(pt + p, PPT + o);
+            cp_async8(ht + p, HT + o);
         }
     }
     cp_async_wait_all();
     __syncthreads();
-    if (threadIdx.x < nq) {
-        const int l = threadIdx.x;
-        const long long q = q0 + l;
-        const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-        const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-        const bool zero = (kx == 0 && kz == 0);
-        double b = g.acph[1] + shift;
-        double c = zero ? 0.0 : g.apph[1];
-        double2 r = tile[l];
-        if (zero) r = make_double2(0.0, 0.0);
-        double hp = c / b;
-        double2 gp = make_double2(r.x / b, r.y / b);
-        hs[l] = hp;
-        tile[l] = gp;
-        for (int j = 2; j <= M; ++j) {
-            const double a = g.amph[j];
-            const double bj = g.acph[j] + shift;
-            const double pp = 1.0 / (bj - hp * a);
-            const double2 rj = tile[(j - 1) * 32 + l];
-            gp = make_double2((rj.x - a * gp.x) * pp, (rj.y - a * gp.y) * pp);
-            if (j < M) {
-                hp = g.apph[j] * pp;
-                hs[(j - 1) * 32 + l] = hp;
+    if (threadIdx.x < 2 * YS_L) {
+        const int l = threadIdx.x % YS_L, part = threadIdx.x / YS_L;
+        if (l < nq) {
+            double* d = (double*)tile + part;  // element (j, l) at d[2*(j*YS_L + l)]
+            const bool zero = (q0 + l == 0);
+            double r = zero ? 0.0 : d[2 * l];
+            double gp = r / pt[l];
+            d[2 * l] = gp;
+#pragma unroll 4
+            for (int j = 2; j <= M; ++j) {
+                const int e = (j - 1) * YS_L + l;
+                gp = (d[2 * e] - g.amph[j] * gp) * pt[e];
+                d[2 * e] = gp;
             }
-            tile[(j - 1) * 32 + l] = gp;
-        }
-        double2 xn = gp;
-        for (int j = M - 1; j >= 1; --j) {
-            const double hj = hs[(j - 1) * 32 + l];
-            const double2 gj = tile[(j - 1) * 32 + l];
-            xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
-            tile[(j - 1) * 32 + l] = xn;
+            double xn = gp;
+#pragma unroll 4
+            for (int j = M - 1; j >= 1; --j) {
+                const int e = (j - 1) * YS_L + l;
+                xn = d[2 * e] - ht[e] * xn;
+                d[2 * e] = xn;
+            }
         }
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < 32 * M; p += YS2_NT) {
-        const int l = p & 31, j = p >> 5;
+    for (int p = threadIdx.x; p < YS_L * M; p += YS2_NT) {
+        const int l = p % YS_L, j = p / YS_L;
         if (l < nq) {
             const long long q = q0 + l;
             const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);

@@ -135,9 +135,10 @@ int chapsim_tdmaijj_noncyc(const double* a, const double* b, const double* c, do
 
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
  * with a CUDA event after every kernel; ms[slot] receives the summed
- * duration of kernel slot `slot` of a step.  Slot order: k_cfl, k_dt, then
- * for each substep k_factors, k_rhs_xsweep, k_zsweep, k_ysweep, k_div_fftx,
- * k_fftz_fwd, k_ysolve, k_fftz_inv, k_fftx_inv, k_correct (nslots >= 32). */
+ * duration of kernel slot `slot` of a step.  Slot order: k_cfl,
+ * k_dt_factors, then for each substep k_rhs_xsweep, k_zsweep, k_ysweep,
+ * k_div_fftx, k_fftz_fwd, k_ysolve, k_fftz_inv, k_fftx_inv, k_correct
+ * (nslots >= 29). */
 int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, float* ms,
                           int32_t nslots);
 
