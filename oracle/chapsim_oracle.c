@@ -55,6 +55,10 @@ typedef struct {
     double *SRe, *SIm;
     int nthreads;
     int fix_v_wall_row; /* 0: reproduce the reference (default) */
+    /* IO (main-domain) path, allocated by orc_io_enable */
+    int io;
+    double *G, *EXPLT0, *RHO, *MU0, *MU, *DSTG, *MUSTG, *DIVU, *DRHODT;
+    double CFLMM_IO;
 } orc_t;
 
 #define FOFF(o, i, j, k) ((size_t)((i) - 1) + (size_t)(o)->L * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
@@ -62,6 +66,10 @@ typedef struct {
 #define QV(o, i, j, k, c) ((o)->Q[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
 #define F3(a, o, i, j, k) ((a)[FOFF(o, i, j, k)])
 #define H0V(o, i, j, k, c) ((o)->CONVH0[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+#define GV(o, i, j, k, c) ((o)->G[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+#define E0V(o, i, j, k, c) ((o)->EXPLT0[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+#define DSV(o, i, j, k, c) ((o)->DSTG[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+#define MSV(o, i, j, k, c) ((o)->MUSTG[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
 
 static inline int IPV(const orc_t* o, int i) { return i == o->L ? 1 : i + 1; }
 static inline int IMV(const orc_t* o, int i) { return i == 1 ? o->L : i - 1; }
@@ -299,6 +307,8 @@ void orc_destroy(orc_t* o) {
     free(o->Vini); free(o->AK1); free(o->AK3);
     free(o->Q); free(o->PR); free(o->CONVH0); free(o->QTMP); free(o->DPH); free(o->RHSLLPHI); free(o->RHS);
     free(o->SRe); free(o->SIm);
+    free(o->G); free(o->EXPLT0); free(o->RHO); free(o->MU0); free(o->MU); free(o->DSTG); free(o->MUSTG);
+    free(o->DIVU); free(o->DRHODT);
     free(o);
 }
 
@@ -939,4 +949,592 @@ double orc_divgck(orc_t* o) {
         }
     }
     return DIVX;
+}
+
+
+/* ====================================================================== */
+/* IO (main-domain, x-periodic) path with explicit viscous terms:         */
+/* SOLVERRK3_MOM_io (src/SOLVERRK3_MOM_IO.f90:11-120, iVisScheme = 0)      */
+/* for a flow whose thermodynamics is not yet active (the property fields */
+/* DENSITY0 / Viscousity0 are given and fixed; DrhoDtP = 0).               */
+/* ====================================================================== */
+
+void orc_io_enable(orc_t* o) {
+    if (o->io) return;
+    size_t fs = FSZ(o);
+    o->G = dalloc(3 * fs); o->EXPLT0 = dalloc(3 * fs); o->RHO = dalloc(fs); o->MU0 = dalloc(fs); o->MU = dalloc(fs);
+    o->DSTG = dalloc(3 * fs); o->MUSTG = dalloc(3 * fs); o->DIVU = dalloc(fs); o->DRHODT = dalloc(fs);
+    o->io = 1;
+}
+
+/* DENSITY_Staggered (src/MASSFLUX_CALC_IO.f90:262-329) and MU_Staggered   */
+/* (:155-259) from the cell-centred DENSITY0 (RHO) and Viscousity0 (MU0). */
+static void io_staggered_props(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int K = 1; K <= N; ++K) {
+        int KM = KMV(o, K);
+        for (int J = 1; J <= M; ++J)
+            for (int I = 1; I <= L; ++I) {
+                int IM = IMV(o, I);
+                DSV(o, I, J, K, 1) = (F3(o->RHO, o, I, J, K) + F3(o->RHO, o, IM, J, K)) * 0.5;
+                DSV(o, I, J, K, 3) = (F3(o->RHO, o, I, J, K) + F3(o->RHO, o, I, J, KM)) * 0.5;
+                if (J >= 2) DSV(o, I, J, K, 2) = o->WFF[J] * F3(o->RHO, o, I, J, K) + o->WFB[J] * F3(o->RHO, o, I, J - 1, K);
+                if (J >= 2)
+                    MSV(o, I, J, K, 1) = ((F3(o->MU0, o, I, J, K) + F3(o->MU0, o, IM, J, K)) * o->WFF[J] +
+                                          (F3(o->MU0, o, I, J - 1, K) + F3(o->MU0, o, IM, J - 1, K)) * o->WFB[J]) * 0.5;
+                MSV(o, I, J, K, 2) = (F3(o->MU0, o, I, J, K) + F3(o->MU0, o, IM, J, K) + F3(o->MU0, o, I, J, KM) +
+                                      F3(o->MU0, o, IM, J, KM)) * 0.5 * 0.5;
+                if (J >= 2)
+                    MSV(o, I, J, K, 3) = ((F3(o->MU0, o, I, J, KM) + F3(o->MU0, o, I, J, K)) * o->WFF[J] +
+                                          (F3(o->MU0, o, I, J - 1, KM) + F3(o->MU0, o, I, J - 1, K)) * o->WFB[J]) * 0.5;
+            }
+        for (int I = 1; I <= L; ++I) {
+            DSV(o, I, 1, K, 2) = F3(o->RHO, o, I, 0, K);
+            DSV(o, I, M + 1, K, 2) = F3(o->RHO, o, I, M + 1, K);
+            MSV(o, I, 1, K, 1) = F3(o->MU0, o, I, 0, K);
+            MSV(o, I, 1, K, 3) = F3(o->MU0, o, I, 0, K);
+            MSV(o, I, M + 1, K, 1) = F3(o->MU0, o, I, M + 1, K);
+            MSV(o, I, M + 1, K, 3) = F3(o->MU0, o, I, M + 1, K);
+        }
+    }
+}
+
+/* BC_WALL_G_io (src/BC_WALL.f90:435-481) */
+static void io_bc_wall_g(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int K = 1; K <= N; ++K)
+        for (int I = 1; I <= L; ++I) {
+            GV(o, I, 0, K, 1) = 0.0; GV(o, I, 0, K, 3) = 0.0; GV(o, I, 1, K, 2) = 0.0; GV(o, I, 0, K, 2) = 0.0;
+            GV(o, I, M + 1, K, 1) = 0.0; GV(o, I, M + 1, K, 3) = 0.0; GV(o, I, M + 1, K, 2) = 0.0;
+        }
+}
+
+/* VELOCITY_CALC_io (src/MASSFLUX_CALC_IO.f90:96-152) + BC_WALL_Q_io */
+static void io_velocity_calc(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+#pragma omp parallel for schedule(static)
+    for (int K = 1; K <= N; ++K)
+        for (int J = 1; J <= M; ++J)
+            for (int I = 1; I <= L; ++I) {
+                QV(o, I, J, K, 1) = GV(o, I, J, K, 1) / DSV(o, I, J, K, 1);
+                QV(o, I, J, K, 3) = GV(o, I, J, K, 3) / DSV(o, I, J, K, 3);
+                if (J >= 2) QV(o, I, J, K, 2) = GV(o, I, J, K, 2) / DSV(o, I, J, K, 2);
+            }
+    bc_wall_q(o);
+}
+
+/* Field set-up of ReStart_INSTANT_VARS_io (src/processing/RESTART_io.f90:
+ * 16-200) for a restart with the thermal solver not yet active: G, PR and the
+ * property fields are given (padded layout); ghosts, D_STG, MU_STG, Q follow. */
+void orc_io_set_fields(orc_t* o, const double* G, const double* PR, const double* RHO, const double* MU0,
+                       const double* MU) {
+    orc_io_enable(o);
+    size_t fs = FSZ(o);
+    memcpy(o->G, G, 3 * fs * sizeof(double));
+    memcpy(o->PR, PR, fs * sizeof(double));
+    memcpy(o->RHO, RHO, fs * sizeof(double));
+    memcpy(o->MU0, MU0, fs * sizeof(double));
+    memcpy(o->MU, MU, fs * sizeof(double));
+    memset(o->EXPLT0, 0, 3 * fs * sizeof(double));
+    memset(o->DRHODT, 0, fs * sizeof(double));
+    io_bc_wall_g(o);
+    bc_wall_scalar(o, o->PR);
+    io_staggered_props(o);
+    io_velocity_calc(o);
+}
+
+void orc_io_get_fields(const orc_t* o, double* G, double* Q, double* PR) {
+    size_t fs = FSZ(o);
+    if (G) memcpy(G, o->G, 3 * fs * sizeof(double));
+    if (Q) memcpy(Q, o->Q, 3 * fs * sizeof(double));
+    if (PR) memcpy(PR, o->PR, fs * sizeof(double));
+}
+
+/* CONVECTION_X_io (src/CONVECTION_X.f90:67-156) */
+static void io_convection_x(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->QTMP, 0, FSZ(o) * sizeof(double));
+    double COE1 = o->DXI * 0.5 * 0.5, COE3 = o->DZI * 0.5 * 0.5;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * 0.5 * 1.0, COE32 = COE3 * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double H11F = (GV(o, IP, JC, KC, 1) + GV(o, IC, JC, KC, 1)) * (QV(o, IP, JC, KC, 1) + QV(o, IC, JC, KC, 1));
+                double H11B = (GV(o, IC, JC, KC, 1) + GV(o, IM, JC, KC, 1)) * (QV(o, IC, JC, KC, 1) + QV(o, IM, JC, KC, 1));
+                double H11 = (H11F - H11B) * COE1;
+                double H12F = (GV(o, IC, JP, KC, 2) + GV(o, IM, JP, KC, 2)) *
+                              (o->WFF[JJP] * QV(o, IC, JP, KC, 1) + o->WFB[JJP] * QV(o, IC, JC, KC, 1));
+                double H12B = (GV(o, IC, JC, KC, 2) + GV(o, IM, JC, KC, 2)) *
+                              (o->WFF[JJ] * QV(o, IC, JC, KC, 1) + o->WFB[JJ] * QV(o, IC, JM, KC, 1));
+                double H12 = (H12F - H12B) * COE2;
+                double H13F = (GV(o, IC, JC, KP, 3) + GV(o, IM, JC, KP, 3)) * (QV(o, IC, JC, KP, 1) + QV(o, IC, JC, KC, 1));
+                double H13B = (GV(o, IC, JC, KC, 3) + GV(o, IM, JC, KC, 3)) * (QV(o, IC, JC, KC, 1) + QV(o, IC, JC, KM, 1));
+                double H13 = (H13F - H13B) * COE32;
+                F3(o->QTMP, o, IC, JC, KC) = -(H11 + H12 + H13);
+            }
+        }
+    }
+}
+
+/* CONVECTION_Y_io (src/CONVECTION_Y.f90:117-272), channel */
+static void io_convection_y(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->DPH, 0, FSZ(o) * sizeof(double));
+    double COE1 = o->DXI * 0.5, COE30 = o->DZI * 0.5;
+#pragma omp parallel for schedule(static)
+    for (int JC = 2; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC;
+        double COE2 = o->DYCI[JJ] * 0.5 * 0.5, COE31 = COE30 * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double H21F = (o->WFF[JJ] * GV(o, IP, JC, KC, 1) + o->WFB[JJ] * GV(o, IP, JM, KC, 1)) *
+                              (QV(o, IP, JC, KC, 2) + QV(o, IC, JC, KC, 2));
+                double H21B = (o->WFF[JJ] * GV(o, IC, JC, KC, 1) + o->WFB[JJ] * GV(o, IC, JM, KC, 1)) *
+                              (QV(o, IC, JC, KC, 2) + QV(o, IM, JC, KC, 2));
+                double H21 = (H21F - H21B) * COE1;
+                double H22F = (GV(o, IC, JP, KC, 2) + GV(o, IC, JC, KC, 2)) * (QV(o, IC, JP, KC, 2) * 1.0 + QV(o, IC, JC, KC, 2) * 1.0);
+                double H22B = (GV(o, IC, JC, KC, 2) + GV(o, IC, JM, KC, 2)) * (QV(o, IC, JC, KC, 2) * 1.0 + QV(o, IC, JM, KC, 2) * 1.0);
+                double H22 = (H22F - H22B) * COE2;
+                double H23F = (o->WFF[JJ] * GV(o, IC, JC, KP, 3) * 1.0 + o->WFB[JJ] * GV(o, IC, JM, KP, 3) * 1.0) *
+                              (QV(o, IC, JC, KP, 2) + QV(o, IC, JC, KC, 2));
+                double H23B = (o->WFF[JJ] * GV(o, IC, JC, KC, 3) * 1.0 + o->WFB[JJ] * GV(o, IC, JM, KC, 3) * 1.0) *
+                              (QV(o, IC, JC, KC, 2) + QV(o, IC, JC, KM, 2));
+                double H23 = (H23F - H23B) * COE31;
+                F3(o->DPH, o, IC, JC, KC) = -(H21 + H22 + H23);
+            }
+        }
+    }
+}
+
+/* CONVECTION_Z_io (src/CONVECTION_Z.f90:106-303), channel */
+static void io_convection_z(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->RHSLLPHI, 0, FSZ(o) * sizeof(double));
+    double COE1 = o->DXI * 0.5 * 0.5, COE30 = o->DZI * 0.5 * 0.5;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * 0.5, COE31 = COE30 * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double H31F = (GV(o, IP, JC, KC, 1) + GV(o, IP, JC, KM, 1)) * (QV(o, IP, JC, KC, 3) + QV(o, IC, JC, KC, 3));
+                double H31B = (GV(o, IC, JC, KC, 1) + GV(o, IC, JC, KM, 1)) * (QV(o, IC, JC, KC, 3) + QV(o, IM, JC, KC, 3));
+                double H31 = (H31F - H31B) * COE1;
+                double H32F = (GV(o, IC, JP, KC, 2) + GV(o, IC, JP, KM, 2)) *
+                              (o->WFF[JJP] * QV(o, IC, JP, KC, 3) * 1.0 + o->WFB[JJP] * QV(o, IC, JC, KC, 3) * 1.0);
+                double H32B = (GV(o, IC, JC, KC, 2) + GV(o, IC, JC, KM, 2)) *
+                              (o->WFF[JJ] * QV(o, IC, JC, KC, 3) * 1.0 + o->WFB[JJ] * QV(o, IC, JM, KC, 3) * 1.0);
+                double H32 = (H32F - H32B) * COE2;
+                double H33F = (GV(o, IC, JC, KP, 3) + GV(o, IC, JC, KC, 3)) * (QV(o, IC, JC, KP, 3) + QV(o, IC, JC, KC, 3));
+                double H33B = (GV(o, IC, JC, KC, 3) + GV(o, IC, JC, KM, 3)) * (QV(o, IC, JC, KC, 3) + QV(o, IC, JC, KM, 3));
+                double H33 = (H33F - H33B) * COE31;
+                F3(o->RHSLLPHI, o, IC, JC, KC) = -(H31 + H32 + H33);
+            }
+        }
+    }
+}
+
+/* DIVG_U_io (src/DIVG.f90:140-246): DivU = div(u) / 3 */
+static void io_divg_u(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->DIVU, 0, FSZ(o) * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1, JJ = JC;
+        double COE2 = o->DYFI[JJ] * 1.0, COE3 = o->DZI * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC);
+                double DIVX = (QV(o, IP, JC, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DXI;
+                double DIVY = (QV(o, IC, JP, KC, 2) - QV(o, IC, JC, KC, 2)) * COE2;
+                double DIVZ = (QV(o, IC, JC, KP, 3) - QV(o, IC, JC, KC, 3)) * COE3;
+                F3(o->DIVU, o, IC, JC, KC) = (DIVX + DIVY + DIVZ) / 3.0;
+            }
+        }
+    }
+}
+
+/* VISCOUS_ALL_EXPLT_X_io (src/VISCOUS_X_EXPLICIT_io.f90:13-128) */
+static void io_viscous_x(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double COE1 = 2.0 * o->DXI * o->CVISC, COE3 = o->DZI * o->CVISC;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * o->CVISC * 1.0, COE32 = COE3 * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double DUDX = (QV(o, IP, JC, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DXI;
+                double TAU11F = 0.5 * (F3(o->MU0, o, IC, JC, KC) + F3(o->MU0, o, IC, JC, KC)) * (DUDX - F3(o->DIVU, o, IC, JC, KC));
+                DUDX = (QV(o, IC, JC, KC, 1) - QV(o, IM, JC, KC, 1)) * o->DXI;
+                double TAU11B = 0.5 * (F3(o->MU0, o, IM, JC, KC) + F3(o->MU0, o, IM, JC, KC)) * (DUDX - F3(o->DIVU, o, IM, JC, KC));
+                double DTAU11DX = (TAU11F - TAU11B) * COE1;
+                double VIS12P = MSV(o, IC, JP, KC, 1);
+                double DUDY = (QV(o, IC, JP, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DYCI[JJP] / 1.0;
+                double DVDX = (QV(o, IC, JP, KC, 2) - QV(o, IM, JP, KC, 2)) * o->DXI;
+                double TAU12F = VIS12P * (DUDY + DVDX);
+                double VIS12C = MSV(o, IC, JC, KC, 1);
+                DUDY = (QV(o, IC, JC, KC, 1) - QV(o, IC, JM, KC, 1)) * o->DYCI[JJ] / 1.0;
+                DVDX = (QV(o, IC, JC, KC, 2) - QV(o, IM, JC, KC, 2)) * o->DXI;
+                double TAU12B = VIS12C * (DUDY + DVDX);
+                double DTAU12DY = (TAU12F - TAU12B) * COE2;
+                double VIS13P = MSV(o, IC, JC, KP, 2);
+                double DUDZ = (QV(o, IC, JC, KP, 1) - QV(o, IC, JC, KC, 1)) * o->DZI;
+                double DWDX = (QV(o, IC, JC, KP, 3) - QV(o, IM, JC, KP, 3)) * o->DXI;
+                double TAU13F = VIS13P * (DUDZ + DWDX);
+                double VIS13C = MSV(o, IC, JC, KC, 2);
+                DUDZ = (QV(o, IC, JC, KC, 1) - QV(o, IC, JC, KM, 1)) * o->DZI;
+                DWDX = (QV(o, IC, JC, KC, 3) - QV(o, IM, JC, KC, 3)) * o->DXI;
+                double TAU13B = VIS13C * (DUDZ + DWDX);
+                double DTAU13DZ = (TAU13F - TAU13B) * COE32;
+                F3(o->QTMP, o, IC, JC, KC) = F3(o->QTMP, o, IC, JC, KC) + DTAU11DX + DTAU12DY + DTAU13DZ;
+            }
+        }
+    }
+}
+
+/* VISCOUS_ALL_EXPLT_Y_io (src/VISCOUS_Y_EXPLICIT_io.f90:14-120), channel */
+static void io_viscous_y(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double COE1 = o->DXI * o->CVISC, COE3 = o->DZI * o->CVISC;
+#pragma omp parallel for schedule(static)
+    for (int JC = 2; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJM = JJ - 1;
+        double COE2 = 2.0 * o->DYCI[JJ] * o->CVISC;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double DVDY = (QV(o, IC, JP, KC, 2) - QV(o, IC, JC, KC, 2)) * o->DYFI[JJ];
+                double TAU22F = 0.5 * (F3(o->MU0, o, IC, JC, KC) + F3(o->MU0, o, IC, JC, KC)) * (DVDY - F3(o->DIVU, o, IC, JC, KC));
+                DVDY = (QV(o, IC, JC, KC, 2) - QV(o, IC, JM, KC, 2)) * o->DYFI[JJM];
+                double TAU22B = 0.5 * (F3(o->MU0, o, IC, JM, KC) + F3(o->MU0, o, IC, JM, KC)) * (DVDY - F3(o->DIVU, o, IC, JM, KC));
+                double DTAU22DY = (TAU22F - TAU22B) * COE2;
+                double VIS21P = MSV(o, IP, JC, KC, 1);
+                double DVDX = (QV(o, IP, JC, KC, 2) - QV(o, IC, JC, KC, 2)) * o->DXI;
+                double DUDY = (QV(o, IP, JC, KC, 1) - QV(o, IP, JM, KC, 1)) * o->DYCI[JJ];
+                double TAU21F = VIS21P * (DVDX + DUDY);
+                double VIS21C = MSV(o, IC, JC, KC, 1);
+                DVDX = (QV(o, IC, JC, KC, 2) - QV(o, IM, JC, KC, 2)) * o->DXI;
+                DUDY = (QV(o, IC, JC, KC, 1) - QV(o, IC, JM, KC, 1)) * o->DYCI[JJ];
+                double TAU21B = VIS21C * (DVDX + DUDY);
+                double DTAU21DX = (TAU21F - TAU21B) * COE1;
+                double VIS23P = MSV(o, IC, JC, KP, 3);
+                double DVDZ = (QV(o, IC, JC, KP, 2) - QV(o, IC, JC, KC, 2)) * o->DZI;
+                double DWDY = (QV(o, IC, JC, KP, 3) - QV(o, IC, JM, KP, 3)) * o->DYCI[JJ];
+                double TAU23F = VIS23P * (DVDZ + DWDY);
+                double VIS23C = MSV(o, IC, JC, KC, 3);
+                DVDZ = (QV(o, IC, JC, KC, 2) - QV(o, IC, JC, KM, 2)) * o->DZI;
+                DWDY = (QV(o, IC, JC, KC, 3) - QV(o, IC, JM, KC, 3)) * o->DYCI[JJ];
+                double TAU23B = VIS23C * (DVDZ + DWDY);
+                double DTAU23DZ = (TAU23F - TAU23B) * COE3;
+                F3(o->DPH, o, IC, JC, KC) = F3(o->DPH, o, IC, JC, KC) + DTAU21DX + DTAU22DY + DTAU23DZ;
+            }
+        }
+    }
+}
+
+/* VISCOUS_ALL_EXPLT_Z_io (src/VISCOUS_Z_EXPLICIT_io.f90:13-100), channel */
+static void io_viscous_z(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double COE1 = o->DXI * o->CVISC, COE3 = 2.0 * o->DZI * o->CVISC;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * o->CVISC;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double DWDZ = (QV(o, IC, JC, KP, 3) - QV(o, IC, JC, KC, 3)) * o->DZI;
+                double TAU33F = 0.5 * (F3(o->MU0, o, IC, JC, KC) + F3(o->MU0, o, IC, JC, KC)) * (DWDZ - F3(o->DIVU, o, IC, JC, KC));
+                DWDZ = (QV(o, IC, JC, KC, 3) - QV(o, IC, JC, KM, 3)) * o->DZI;
+                double TAU33B = 0.5 * (F3(o->MU0, o, IC, JC, KM) + F3(o->MU0, o, IC, JC, KM)) * (DWDZ - F3(o->DIVU, o, IC, JC, KM));
+                double DTAU33DZ = (TAU33F - TAU33B) * COE3;
+                double VIS31P = MSV(o, IP, JC, KC, 2);
+                double DWDX = (QV(o, IP, JC, KC, 3) - QV(o, IC, JC, KC, 3)) * o->DXI;
+                double DUDZ = (QV(o, IP, JC, KC, 1) - QV(o, IP, JC, KM, 1)) * o->DZI;
+                double TAU31F = VIS31P * (DWDX + DUDZ);
+                double VIS31C = MSV(o, IC, JC, KC, 2);
+                DWDX = (QV(o, IC, JC, KC, 3) - QV(o, IM, JC, KC, 3)) * o->DXI;
+                DUDZ = (QV(o, IC, JC, KC, 1) - QV(o, IC, JC, KM, 1)) * o->DZI;
+                double TAU31B = VIS31C * (DWDX + DUDZ);
+                double DTAU31DX = (TAU31F - TAU31B) * COE1;
+                double VIS32P = MSV(o, IC, JP, KC, 3);
+                double DWDY = (QV(o, IC, JP, KC, 3) - QV(o, IC, JC, KC, 3)) * o->DYCI[JJP];
+                double DVDZ = (QV(o, IC, JP, KC, 2) - QV(o, IC, JP, KM, 2)) * o->DZI;
+                double TAU32F = VIS32P * (DWDY + DVDZ);
+                double VIS32C = MSV(o, IC, JC, KC, 3);
+                DWDY = (QV(o, IC, JC, KC, 3) - QV(o, IC, JM, KC, 3)) * o->DYCI[JJ];
+                DVDZ = (QV(o, IC, JC, KC, 2) - QV(o, IC, JC, KM, 2)) * o->DZI;
+                double TAU32B = VIS32C * (DWDY + DVDZ);
+                double DTAU32DY = (TAU32F - TAU32B) * COE2;
+                F3(o->RHSLLPHI, o, IC, JC, KC) = F3(o->RHSLLPHI, o, IC, JC, KC) + DTAU31DX + DTAU32DY + DTAU33DZ;
+            }
+        }
+    }
+}
+
+/* RHS_MOM_EXPLICIT_io(NS, IDR) (src/RHS_MOM_EXPLICIT_io.f90:11-304),      */
+/* explicit scheme, no gravity, no weighted pressure.                     */
+static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
+    int L = o->L, M = o->M, N = o->N;
+    int NYI = (IDR == 2) ? 2 : 1;
+    double* EX = IDR == 1 ? o->QTMP : IDR == 2 ? o->DPH : o->RHSLLPHI;
+    double DT = o->DT;
+    memset(o->RHS, 0, FSZ(o) * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = NYI; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double RHSC = F3(EX, o, IC, JC, KC);
+                double RHSL = E0V(o, IC, JC, KC, IDR);
+                F3(o->RHS, o, IC, JC, KC) = (o->TGAM[NS] * RHSC + o->TROH[NS] * RHSL) * DT;
+                E0V(o, IC, JC, KC, IDR) = RHSC;
+            }
+    if (IDR == 1) {
+        double COE2 = o->TALP[NS] * DT * o->DXI;
+#pragma omp parallel for schedule(static)
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = 1; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    double PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IMV(o, IC), JC, KC)) * COE2;
+                    F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
+                }
+    } else if (IDR == 2) {
+#pragma omp parallel for schedule(static)
+        for (int JC = 2; JC <= M; ++JC) {
+            double COE2 = o->TALP[NS] * DT * o->DYCI[JC] / 1.0;
+            for (int KC = 1; KC <= N; ++KC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    double PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IC, JC - 1, KC)) * COE2;
+                    F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
+                }
+        }
+    } else {
+        double COE2 = o->TALP[NS] * DT * o->DZI;
+#pragma omp parallel for schedule(static)
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC);
+            for (int JC = 1; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    double PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IC, JC, KM)) * COE2;
+                    F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
+                }
+        }
+    }
+    if (IDR == 1) {
+        double DPGRNS = 0.0;
+        if (o->iFlowDriven == 1) {
+            double INTGRHSY = 0.0;  /* loop order JC, IC, KC */
+            for (int JC = 1; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC)
+                    for (int KC = 1; KC <= N; ++KC) INTGRHSY = INTGRHSY + F3(o->RHS, o, IC, JC, KC) / o->DYFI[JC] / 1.0;
+            DPGRNS = INTGRHSY / o->VOLM;
+        } else if (o->iFlowDriven == 2) {
+            DPGRNS = -0.5 * o->Cf_Given * (o->TALP[NS] * DT);
+        }
+#pragma omp parallel for schedule(static)
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = 1; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - DPGRNS;
+    }
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = NYI; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) F3(EX, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC);
+}
+
+/* MASSFLUX_CALC_io (src/MASSFLUX_CALC_IO.f90:15-93): G += explicit RHS */
+static void io_massflux_calc(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                GV(o, IC, JC, KC, 1) = GV(o, IC, JC, KC, 1) + F3(o->QTMP, o, IC, JC, KC);
+                GV(o, IC, JC, KC, 3) = GV(o, IC, JC, KC, 3) + F3(o->RHSLLPHI, o, IC, JC, KC);
+                if (JC >= 2) GV(o, IC, JC, KC, 2) = GV(o, IC, JC, KC, 2) + F3(o->DPH, o, IC, JC, KC);
+            }
+}
+
+/* DIVG_io (src/DIVG.f90:54-137), iWeightedPre = 0 */
+static void io_divg(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+    double COE0 = 1.0 / o->DT / o->TALP[NS];
+    memset(o->RHSLLPHI, 0, FSZ(o) * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1, JJ = JC;
+        double COE1 = o->DXI / 1.0, COE2 = o->DYFI[JJ] / 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC);
+                double DIVX = (GV(o, IP, JC, KC, 1) - GV(o, IC, JC, KC, 1)) * COE1;
+                double DIVY = (GV(o, IC, JP, KC, 2) - GV(o, IC, JC, KC, 2)) * COE2;
+                double DIVZ = (GV(o, IC, JC, KP, 3) - GV(o, IC, JC, KC, 3)) * o->DZI;
+                double DTRHO = F3(o->DRHODT, o, IC, JC, KC) / 1.0;
+                double DQCAP = DIVX + DIVY + DIVZ + DTRHO;
+                F3(o->RHSLLPHI, o, IC, JC, KC) = DQCAP * COE0;
+            }
+        }
+    }
+}
+
+/* PRCALC_io explicit (src/PRESSURE_CORRECTION.f90:102-170) and           */
+/* MASSFLUX_UPDATE_io (src/VELO_CORRECTION.f90:103-179)                   */
+static void io_prcalc_massflux_update(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) F3(o->PR, o, IC, JC, KC) = F3(o->PR, o, IC, JC, KC) + F3(o->DPH, o, IC, JC, KC);
+    bc_wall_scalar(o, o->PR);
+    double COE1 = o->DT * o->TALP[NS] * o->DXI;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC)
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double DFX11 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IMV(o, IC), JC, KC);
+                GV(o, IC, JC, KC, 1) = GV(o, IC, JC, KC, 1) - DFX11 * COE1;
+            }
+    COE1 = o->DT * o->TALP[NS] * o->DZI;
+#pragma omp parallel for schedule(static)
+    for (int KC = 1; KC <= N; ++KC) {
+        int KM = KMV(o, KC);
+        for (int JC = 1; JC <= M; ++JC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double DFX33 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IC, JC, KM);
+                GV(o, IC, JC, KC, 3) = GV(o, IC, JC, KC, 3) - DFX33 * COE1;
+            }
+    }
+#pragma omp parallel for schedule(static)
+    for (int JC = 2; JC <= M; ++JC) {
+        double C1 = o->DT * o->TALP[NS] * o->DYCI[JC] / 1.0;
+        for (int KC = 1; KC <= N; ++KC)
+            for (int IC = 1; IC <= L; ++IC) {
+                double DFX22 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IC, JC - 1, KC);
+                GV(o, IC, JC, KC, 2) = GV(o, IC, JC, KC, 2) - DFX22 * C1;
+            }
+    }
+    io_bc_wall_g(o);
+}
+
+/* SOLVERRK3_MOM_io(NS) (src/SOLVERRK3_MOM_IO.f90:11-120), explicit scheme. */
+/* The pressure Poisson equation is the one FISHPACK_POIS3D_SIMPLE solves */
+/* (same AMPH/ACPH/APPH operator and x/z eigenvalues); its singular       */
+/* kx = kz = 0 mode is fixed here as in FFT99 (phi_hat(y_1) = 0), which    */
+/* changes DPH and PR by an x-z-y constant only.                           */
+int orc_io_substep(orc_t* o, int NS) {
+    if (!o->io || NS < 0 || NS > 3) return -1;
+    io_velocity_calc(o);
+    io_convection_x(o);
+    io_convection_y(o);
+    io_convection_z(o);
+    io_divg_u(o);
+    io_viscous_x(o);
+    io_rhs_mom_explicit(o, NS, 1);
+    io_viscous_y(o);
+    io_rhs_mom_explicit(o, NS, 2);
+    io_viscous_z(o);
+    io_rhs_mom_explicit(o, NS, 3);
+    io_massflux_calc(o);
+    io_bc_wall_g(o);
+    io_divg(o, NS);
+    memset(o->DPH, 0, FSZ(o) * sizeof(double));
+    poisson(o, o->RHSLLPHI, o->DPH);
+    bc_wall_scalar(o, o->DPH);
+    io_prcalc_massflux_update(o, NS);
+    io_velocity_calc(o);
+    return 0;
+}
+
+/* CFL_io (src/CFL.f90:55-107), including the viscous number */
+double orc_io_cfl(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double CFLMA = 0.0;
+    for (int K = 1; K <= N; ++K) {
+        int KP = KPV(o, K);
+        for (int J = 1; J <= M; ++J) {
+            int JP = J + 1, JJ = J;
+            for (int I = 1; I <= L; ++I) {
+                int IP = IPV(o, I);
+                double QCF = (fabs((QV(o, I, J, K, 1) + QV(o, IP, J, K, 1)) * o->DXI) +
+                              fabs((QV(o, I, J, K, 2) + QV(o, I, JP, K, 2)) * o->DYFI[JJ] * 1.0) +
+                              fabs((QV(o, I, J, K, 3) + QV(o, I, J, KP, 3)) * o->DZI * 1.0)) * 0.5;
+                double VCF = 2.0 * o->CVISC * (o->DXQI + o->DZQI * 1.0 + o->DYFI[JJ] * o->DYFI[JJ]) * F3(o->MU, o, I, J, K) /
+                             F3(o->RHO, o, I, J, K);
+                QCF = fmax(QCF, VCF);
+                CFLMA = fmax(CFLMA, QCF);
+            }
+        }
+    }
+    o->CFLMM_IO = CFLMA;
+    return CFLMA;
+}
+
+/* One step of SOLVE for the IO domain: CFL_io, dt rule, three substeps. */
+int orc_io_run_steps(orc_t* o, int nsteps, double* cfl_dt) {
+    for (int s = 0; s < nsteps; ++s) {
+        double c = orc_io_cfl(o);
+        double dt = fmin(fmin(o->DT0, 5.0 * o->DT), o->CFLGV / c);
+        dt = fmax(dt, o->DTMIN);
+        o->DT = dt;
+        if (cfl_dt) cfl_dt[s] = c * dt;
+        if ((dt / o->DT0) < 0.01) return 1;
+        for (int NS = 1; NS <= 3; ++NS) orc_io_substep(o, NS);
+    }
+    return 0;
+}
+
+/* Monitor quantities of PP_MONITOR_Xperiodic_io (src/processing/
+ * PP_SCN_MONITOR.f90:255-625) that follow from the instantaneous x-z means
+ * of PP_MEAN_ZX_FLOW_Xperiodic_io (src/processing/PP_MEAN_ZX.f90:311-883):
+ * out[0] Uc = <G1>/<D> at j = M/2, out[1] u'u'_c, out[2] u'v'_c,
+ * out[3] Gmaxx = max_j |<G1>|, out[4] bulk G (G1BULK). Cell-centred values:
+ * G_CCT(1) = (G1(i) + G1(i+1))/2, G_CCT(2) = (G2(j) + G2(j+1))/2, likewise U. */
+void orc_io_monitor(orc_t* o, double* out) {
+    int L = o->L, M = o->M, N = o->N;
+    double VL1313 = 1.0 / (double)(L * N);
+    double gmax = 0.0, uc = 0, uu = 0, uv = 0, g1c = 0, dc = 0;
+    double rate = 0.0;
+    for (int J = 1; J <= M; ++J) {
+        double G1 = 0, G2 = 0, UG1 = 0, UG2 = 0, D1 = 0;
+        for (int I = 1; I <= L; ++I) {
+            int IP = IPV(o, I);
+            for (int K = 1; K <= N; ++K) {
+                double gc1 = (GV(o, I, J, K, 1) + GV(o, IP, J, K, 1)) * 0.5;
+                double uc1 = (QV(o, I, J, K, 1) + QV(o, IP, J, K, 1)) * 0.5;
+                double gc2 = ((GV(o, I, J, K, 2) + GV(o, I, J + 1, K, 2)) * 1.0) * 0.5;
+                G1 += gc1;
+                G2 += gc2;
+                UG1 += uc1 * gc1;
+                UG2 += uc1 * gc2;
+                D1 += F3(o->RHO, o, I, J, K);
+            }
+        }
+        G1 *= VL1313; G2 *= VL1313; UG1 *= VL1313; UG2 *= VL1313; D1 *= VL1313;
+        gmax = fmax(gmax, fabs(G1));
+        rate += G1 / o->DYFI[J];
+        if (J == M / 2) {
+            g1c = G1; dc = D1;
+            uc = G1 / D1;
+            uu = UG1 - G1 * G1 / D1;
+            uv = UG2 - G1 * G2 / D1;
+        }
+    }
+    (void)g1c; (void)dc;
+    out[0] = uc; out[1] = uu; out[2] = uv; out[3] = gmax; out[4] = rate / 2.0;
 }

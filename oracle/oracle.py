@@ -61,6 +61,16 @@ def lib():
         L.orc_fft_complex.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_tdma_cyc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
         L.orc_tdma_noncyc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.orc_io_enable.argtypes = [ctypes.c_void_p]
+        L.orc_io_set_fields.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp]
+        L.orc_io_get_fields.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.orc_io_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_io_substep.restype = ctypes.c_int
+        L.orc_io_cfl.argtypes = [ctypes.c_void_p]
+        L.orc_io_cfl.restype = ctypes.c_double
+        L.orc_io_run_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_io_run_steps.restype = ctypes.c_int
+        L.orc_io_monitor.argtypes = [ctypes.c_void_p, _dp]
         _lib = L
     return _lib
 
@@ -163,6 +173,36 @@ class Oracle:
 
     def divgck(self):
         return self._lib.orc_divgck(self._h)
+
+    # ---- IO (main-domain) path, explicit viscous terms ----
+    def io_set_fields(self, G, PR, RHO, MU0, MU):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (G, PR, RHO, MU0, MU)]
+        assert arrs[0].shape == (3,) + self.field_shape()
+        self._lib.orc_io_set_fields(self._h, *[_p(a) for a in arrs])
+
+    def io_get_fields(self):
+        G = np.zeros((3,) + self.field_shape())
+        Q = np.zeros((3,) + self.field_shape())
+        PR = np.zeros(self.field_shape())
+        self._lib.orc_io_get_fields(self._h, _p(G), _p(Q), _p(PR))
+        return G, Q, PR
+
+    def io_substep(self, ns):
+        if self._lib.orc_io_substep(self._h, int(ns)) != 0:
+            raise ValueError("bad substep or IO path not enabled")
+
+    def io_cfl(self):
+        return self._lib.orc_io_cfl(self._h)
+
+    def io_run_steps(self, n):
+        cdt = np.zeros(max(n, 1))
+        rc = self._lib.orc_io_run_steps(self._h, int(n), _p(cdt))
+        return rc, cdt[:n]
+
+    def io_monitor(self):
+        out = np.zeros(5)
+        self._lib.orc_io_monitor(self._h, _p(out))
+        return dict(zip(["Uc", "UUc", "UVc", "Gmaxx", "Gbulk"], out.tolist()))
 
     def poisson(self, rhs):
         rhs = np.ascontiguousarray(rhs, np.float64)

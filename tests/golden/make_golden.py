@@ -100,7 +100,27 @@ def main():
             rows.append([float(v) for v in s[: len(cols)]])
     with open(os.path.join(OUT, "tc8_monitor.json"), "w") as f:
         json.dump({"columns": cols, "rows": rows}, f)
-    print("wrote", os.path.join(OUT, "tc8_setup.json"), "and tc8_monitor.json")
+    # step-100 restart fields of the same run (rho*u, rho*v, rho*w and p; the
+    # thermal solver is not active yet, so D and M are uniform and stored as
+    # scalars).  float32 keeps the fixture small; the monitor columns are
+    # printed to 5-6 digits, far above the 1e-8 perturbation this introduces.
+    raw = os.path.join(TC8, "1_instant_rawdata")
+    fields = {}
+    hdr = None
+    for name in ("U", "V", "W", "P", "D", "M"):
+        b = open(os.path.join(raw, f"DNS_perixz_INSTANT_T1.000000000E-01_{name}.D"), "rb").read()
+        h = np.frombuffer(b[:16], "<i4")
+        hdr = (h.tolist(), np.frombuffer(b[16:40], "<f8").tolist())
+        L, M, N = (int(x) for x in h[:3])
+        f = np.frombuffer(b[40:], "<f8").reshape(N, M, L)
+        fields[name] = f
+    np.savez_compressed(os.path.join(OUT, "tc8_step100_fields.npz"),
+                        G1=fields["U"].astype(np.float32), G2=fields["V"].astype(np.float32),
+                        G3=fields["W"].astype(np.float32), P=fields["P"].astype(np.float32),
+                        D=np.float64(fields["D"].mean()), M=np.float64(fields["M"].mean()),
+                        D_ptp=np.float64(np.ptp(fields["D"])), M_ptp=np.float64(np.ptp(fields["M"])),
+                        header_int=np.array(hdr[0]), header_real=np.array(hdr[1]))
+    print("wrote", os.path.join(OUT, "tc8_setup.json"), "tc8_monitor.json and tc8_step100_fields.npz")
 
 
 def _rows_text(text):
