@@ -28,7 +28,9 @@ ERR_NAMES = {0: "CHAPSIM_OK", -1: "CHAPSIM_ERR_CUDA", -2: "CHAPSIM_ERR_NAN", -3:
 EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_string", "chapsim_upload_fields",
             "chapsim_download_fields", "chapsim_set_dt", "chapsim_get_dt", "chapsim_cfl_tg", "chapsim_step_begin",
             "chapsim_rk_substep_tg", "chapsim_advance_tg", "chapsim_divgck_tg", "chapsim_fft99_pois3d",
-            "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_profile_steps", "chapsim_get_stream",
+            "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_upload_io_fields",
+            "chapsim_download_io_fields", "chapsim_rk_substep_io", "chapsim_cfl_io", "chapsim_profile_steps",
+            "chapsim_get_stream",
             "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
@@ -89,6 +91,10 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_fft99_pois3d.argtypes = [vp, _dp, _dp]
     L.chapsim_tdmaiji_cyc.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
     L.chapsim_tdmaijj_noncyc.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
+    L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
+    L.chapsim_download_io_fields.argtypes = [vp, _dp, _dp, _dp]
+    L.chapsim_rk_substep_io.argtypes = [vp, ctypes.c_int32]
+    L.chapsim_cfl_io.argtypes = [vp, _dp]
     L.chapsim_profile_steps.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
     L.chapsim_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
@@ -147,6 +153,8 @@ class ChannelTG:
     (3, N, M, L) = ``CONVH0_tg(L, M, N, 3)``.
     """
 
+    IDOMAIN = 1
+
     def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False):
         self.lib = load_library()
         self.s = setup
@@ -172,7 +180,7 @@ class ChannelTG:
                    _ptr(k["amph"]), _ptr(k["acph"]), _ptr(k["apph"]), _ptr(k["amvr"]), _ptr(k["acvr"]),
                    _ptr(k["apvr"]), _ptr(k["ak1"]), _ptr(k["ak3"]), (ctypes.c_double * 4)(*setup.TGAM),
                    (ctypes.c_double * 4)(*setup.TROH), (ctypes.c_double * 4)(*setup.TALP))
-        g = Grid(L, M, N, 1, 1)
+        g = Grid(L, M, N, 1, self.IDOMAIN)
         o = Opts(device, int(bool(fix_v_wall_row)))
         h = ctypes.c_void_p()
         rc = self.lib.chapsim_gpu_init(ctypes.byref(g), ctypes.byref(cf), ctypes.byref(o), ctypes.byref(h))
@@ -290,3 +298,37 @@ class ChannelTG:
         out = np.zeros(self.field_shape())
         self._check(self.lib.chapsim_fft99_pois3d(self.h, _ptr(rhs), _ptr(out)))
         return out
+
+
+class ChannelIO(ChannelTG):
+    """Device-resident x-periodic main-domain channel (CHAPSim IO domain) with
+    explicit viscous terms and fixed property fields.
+
+    ``G`` is numpy (3, N, M+2, L) = Fortran ``G_io(L, 0:M+1, N, 3)`` (rho*u);
+    ``RHO``, ``MU0``, ``MU`` are (N, M+2, L) = ``DENSITY0``, ``Viscousity0``,
+    ``Viscousity``.  ``advance`` runs CFL_io, the dt rule and three
+    SOLVERRK3_MOM_io substeps per step.
+    """
+
+    IDOMAIN = 2
+
+    def upload_io(self, G, PR, RHO, MU0, MU):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (G, PR, RHO, MU0, MU)]
+        if arrs[0].shape != (3,) + self.field_shape() or any(a.shape != self.field_shape() for a in arrs[1:]):
+            raise ValueError("field shape mismatch")
+        self._check(self.lib.chapsim_upload_io_fields(self.h, *[_ptr(a) for a in arrs]))
+
+    def download_io(self):
+        G = np.empty((3,) + self.field_shape())
+        Q = np.empty((3,) + self.field_shape())
+        PR = np.empty(self.field_shape())
+        self._check(self.lib.chapsim_download_io_fields(self.h, _ptr(G), _ptr(Q), _ptr(PR)))
+        return G, Q, PR
+
+    def SOLVERRK3_MOM_io(self, NS):
+        self._check(self.lib.chapsim_rk_substep_io(self.h, int(NS)))
+
+    def CFL_io(self):
+        v = ctypes.c_double()
+        self._check(self.lib.chapsim_cfl_io(self.h, ctypes.byref(v)))
+        return v.value

@@ -15,6 +15,7 @@
 #include "momentum.cuh"
 #include "poisson.cuh"
 #include "tdma.cuh"
+#include "io.cuh"
 
 // x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
 __global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
@@ -141,6 +142,9 @@ struct chapsim_ctx {
     double* ybuf = nullptr;       // device copies of y-arrays and wavenumbers
     double2* tw = nullptr;
     int* perm = nullptr;
+    int domain = 1;               // 1: periodic TG channel, 2: main domain (IO)
+    IoFields io{};                // IO-path arrays (domain 2)
+    int io_grid = 0;              // blocks of the IO point-wise kernels
     cudaGraphExec_t step_exec = nullptr;
     cudaEvent_t* prof_ev = nullptr;  // when set, an event is recorded after every kernel
     int prof_n = 0;
@@ -313,6 +317,49 @@ void launch_substep(chapsim_ctx* ctx, int ns, bool factors = true) {
     ctx->launches += 9;
 }
 
+// ----------------------------- IO path -----------------------------------
+IoFields io_fields(chapsim_ctx* ctx) {
+    IoFields f = ctx->io;
+    f.Q = ctx->Q; f.PR = ctx->PR; f.RHS = ctx->RHS;
+    return f;
+}
+
+void launch_io_step_start(chapsim_ctx* ctx) {
+    k_io_cfl<<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields(ctx), ctx->part_red, ctx->st);
+    prof_mark(ctx);
+    k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, 1);
+    prof_mark(ctx);
+    ctx->launches += 2;
+}
+
+void launch_io_substep(chapsim_ctx* ctx, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    IoFields f = io_fields(ctx);
+    k_io_divu<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    prof_mark(ctx);
+    k_io_rhs<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
+    prof_mark(ctx);
+    k_io_massflux<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
+    prof_mark(ctx);
+    dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
+    k_io_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP, ctx->st, ns);
+    prof_mark(ctx);
+    const long long nq = (long long)g.LH * g.M;
+    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
+    k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    prof_mark(ctx);
+    launch_ysolve(ctx);
+    prof_mark(ctx);
+    k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    prof_mark(ctx);
+    k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
+    prof_mark(ctx);
+    k_io_correct<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns);
+    prof_mark(ctx);
+    ctx->launches += 9;
+}
+
 int check_device_error(chapsim_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -332,8 +379,13 @@ int build_step_graph(chapsim_ctx* ctx) {
     cudaGraph_t graph;
     unsigned long long before = ctx->launches;
     CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-    launch_step_start(ctx);
-    for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns, false);
+    if (ctx->domain == 2) {
+        launch_io_step_start(ctx);
+        for (int ns = 1; ns <= 3; ++ns) launch_io_substep(ctx, ns);
+    } else {
+        launch_step_start(ctx);
+        for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns, false);
+    }
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
     ctx->kernels_per_step = (int)(ctx->launches - before);
     ctx->launches = before;  // capture does not launch
@@ -355,8 +407,9 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     if (!grid || !cf || !out) return fail(nullptr, CHAPSIM_ERR_BADARG, "null argument");
     *out = nullptr;
     const int L = grid->ncl1, M = grid->ncl2, N = grid->ncl3;
-    if (grid->icase != 1 || grid->idomain != 1)
-        return fail(nullptr, CHAPSIM_ERR_BADARG, "only the periodic plane channel (iCase=1, iDomain=1) is supported");
+    if (grid->icase != 1 || (grid->idomain != 1 && grid->idomain != 2))
+        return fail(nullptr, CHAPSIM_ERR_BADARG,
+                    "only the plane channel (iCase=1) with a periodic TG (iDomain=1) or main (iDomain=2) domain is supported");
     if (L < 32 || M < 32 || N < 32 || L % 32 || M % 32 || N % 32 || !valid_S(L / 32) || !valid_S(M / 32) ||
         !valid_S(N / 32))
         return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");
@@ -370,6 +423,7 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
 
     ctx = new chapsim_ctx();
     ctx->device = opts ? opts->device : 0;
+    ctx->domain = grid->idomain;
     int rc;
 #define INIT_CK(call)                                  \
     do {                                               \
@@ -462,6 +516,21 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
     ctx->npart_red = 4 * nsm;
     INIT_CK(cudaMalloc(&ctx->part_red, (size_t)ctx->npart_red * sizeof(double)));
+    if (ctx->domain == 2) {
+        IoFields& f = ctx->io;
+        INIT_CK(cudaMalloc(&f.G, (size_t)(3 * g.FS) * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.EX0, (size_t)(3 * g.FI) * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.RHO, (size_t)g.FS * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.MU0, (size_t)g.FS * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.MU, (size_t)g.FS * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.DST, (size_t)(3 * g.FS) * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.MST, (size_t)(3 * g.FS) * sizeof(double)));
+        INIT_CK(cudaMalloc(&f.DIVU, (size_t)g.FS * sizeof(double)));
+        INIT_CK(cudaMemset(f.G, 0, (size_t)(3 * g.FS) * sizeof(double)));
+        INIT_CK(cudaMemset(f.EX0, 0, (size_t)(3 * g.FI) * sizeof(double)));
+        INIT_CK(cudaMemset(f.DIVU, 0, (size_t)g.FS * sizeof(double)));
+        ctx->io_grid = ctx->npart_rhs < 8 * nsm ? ctx->npart_rhs : 8 * nsm;
+    }
     INIT_CK(cudaMalloc(&ctx->st, sizeof(DevState)));
     INIT_CK(cudaMallocHost(&ctx->st_host, sizeof(DevState)));
     INIT_CK(cudaMemset(ctx->Q, 0, (size_t)(3 * g.FS) * sizeof(double)));
@@ -498,6 +567,8 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
     cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac); cudaFree(ctx->ppt); cudaFree(ctx->ht);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
+    cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
+    cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -555,6 +626,7 @@ int chapsim_get_dt(chapsim_ctx_t* ctx, double* dt) {
 
 int chapsim_cfl_tg(chapsim_ctx_t* ctx, double* cflmm) {
     if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 1) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the periodic TG domain");
     CK(cudaSetDevice(ctx->device));
     launch_cfl_dt(ctx, 0);
     CK(cudaGetLastError());
@@ -576,7 +648,8 @@ int chapsim_step_begin(chapsim_ctx_t* ctx, double dt0, double dtmin, double cflg
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
     if (rc) return rc;
-    launch_cfl_dt(ctx, 1);
+    if (ctx->domain == 2) launch_io_step_start(ctx);
+    else launch_cfl_dt(ctx, 1);
     CK(cudaGetLastError());
     rc = check_device_error(ctx);
     if (dt_out) *dt_out = ctx->st_host->dt;
@@ -586,6 +659,7 @@ int chapsim_step_begin(chapsim_ctx_t* ctx, double dt0, double dtmin, double cflg
 
 int chapsim_rk_substep_tg(chapsim_ctx_t* ctx, int32_t ns) {
     if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 1) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the periodic TG domain");
     if (ns < 0 || ns > 3) return fail(ctx, CHAPSIM_ERR_BADARG, "NS must be 0..3");
     CK(cudaSetDevice(ctx->device));
     launch_substep(ctx, ns);
@@ -667,8 +741,13 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
         CK(cudaEventRecord(ev[0], ctx->stream));
         ctx->prof_ev = ev.data() + 1;
         ctx->prof_n = 0;
-        launch_step_start(ctx);
-        for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns, false);
+        if (ctx->domain == 2) {
+            launch_io_step_start(ctx);
+            for (int ns = 1; ns <= 3; ++ns) launch_io_substep(ctx, ns);
+        } else {
+            launch_step_start(ctx);
+            for (int ns = 1; ns <= 3; ++ns) launch_substep(ctx, ns, false);
+        }
         ctx->prof_ev = nullptr;
         CK(cudaGetLastError());
         CK(cudaEventSynchronize(ev[per]));
@@ -680,6 +759,63 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
     }
     for (auto& e : ev) cudaEventDestroy(e);
     return check_device_error(ctx);
+}
+
+int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* gq, const double* pr, const double* rho,
+                             const double* mu0, const double* mu) {
+    if (!ctx || !gq || !pr || !rho || !mu0 || !mu) return fail(ctx, CHAPSIM_ERR_BADARG, "null field");
+    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    IoFields& f = ctx->io;
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(f.G, gq, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->PR, pr, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(f.RHO, rho, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(f.MU0, mu0, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(f.MU, mu, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(f.EX0, 0, (size_t)(3 * g.FI) * sizeof(double), s));
+    k_bc_fields<<<ctx->npart_red, DG_NT, 0, s>>>(g, f.G, ctx->PR);     // BC_WALL_G_io, BC_WALL_PR_io
+    k_io_props<<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));       // DENSITY_Staggered, MU_Staggered
+    k_io_velocity<<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));    // VELOCITY_CALC_io
+    k_bc_fields<<<ctx->npart_red, DG_NT, 0, s>>>(g, ctx->Q, ctx->PR);   // BC_WALL_Q_io
+    ctx->launches += 4;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s));
+    return CHAPSIM_OK;
+}
+
+int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* gq, double* q, double* pr) {
+    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    if (gq) CK(cudaMemcpyAsync(gq, ctx->io.G, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (q) CK(cudaMemcpyAsync(q, ctx->Q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (pr) CK(cudaMemcpyAsync(pr, ctx->PR, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns) {
+    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (ns < 0 || ns > 3) return fail(ctx, CHAPSIM_ERR_BADARG, "NS must be 0..3");
+    CK(cudaSetDevice(ctx->device));
+    launch_io_substep(ctx, ns);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {
+    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    CK(cudaSetDevice(ctx->device));
+    k_io_cfl<<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields(ctx), ctx->part_red, ctx->st);
+    k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, 0);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    int rc = check_device_error(ctx);
+    if (cflmm) *cflmm = ctx->st_host->cflmm;
+    return rc;
 }
 
 int chapsim_get_stream(chapsim_ctx_t* ctx, void** stream) {

@@ -1,0 +1,392 @@
+// Main-domain (IO, x-periodic) substep with explicit viscous terms:
+// SOLVERRK3_MOM_io (src/SOLVERRK3_MOM_IO.f90:11-120, iVisScheme = 0) for a
+// flow whose property fields (DENSITY0, Viscousity0, Viscousity) are given
+// and held fixed (thermal solver not active; DrhoDtP = 0).
+//
+//   k_io_props     DENSITY_Staggered + MU_Staggered (src/MASSFLUX_CALC_IO.f90:155-329), once per upload
+//   k_io_divu      DIVG_U_io (src/DIVG.f90:140-246): DivU = div(u)/3
+//   k_io_rhs       CONVECTION_X/Y/Z_io, VISCOUS_ALL_EXPLT_X/Y/Z_io, RHS_MOM_EXPLICIT_io
+//                  (RK combination, EXPLT0 update, pressure gradient, grid sum of the
+//                  bulk-forcing integrand), one thread per point and all components
+//   k_io_massflux  bulk forcing subtraction + MASSFLUX_CALC_io (G += RHS)
+//   k_io_div_fftx  DIVG_io (src/DIVG.f90:54-137) + forward x transform
+//   (shared)       k_fftz / k_ysolve_tile / k_fftz / k_fftx_inv of poisson.cuh: the
+//                  discrete problem of FISHPACK_POIS3D_SIMPLE (same AMPH/ACPH/APPH operator
+//                  and x/z eigenvalues); its singular kx = kz = 0 mode is fixed at
+//                  phi_hat(y_1) = 0, which shifts DPH and PR by a constant only
+//   k_io_correct   PRCALC_io (explicit: PR += DPH), MASSFLUX_UPDATE_io
+//                  (src/VELO_CORRECTION.f90:103-179), VELOCITY_CALC_io (Q = G/D_STG)
+//   k_io_cfl       CFL_io (src/CFL.f90:55-107), including the viscous number
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+#include "poisson.cuh"
+
+#define IO_NT 256
+
+struct IoFields {
+    double *G, *Q, *PR, *EX0, *RHS, *RHO, *MU0, *MU, *DST, *MST, *DIVU;
+};
+
+__device__ __forceinline__ void io_decode(const Geo& g, long long t, int& i, int& j, int& k) {
+    i = (int)(t % g.L);
+    const long long r = t / g.L;
+    j = 1 + (int)(r % g.M);
+    k = (int)(r / g.M);
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFields f) {
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * M * N;
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const int im = wrapm(i, L), km = wrapm(k, N);
+        const long long c = pidx(g, i, j, k);
+        const double* R = f.RHO;
+        const double* U0 = f.MU0;
+        f.DST[c] = (R[c] + R[pidx(g, im, j, k)]) * 0.5;
+        f.DST[c + 2 * g.FS] = (R[c] + R[pidx(g, i, j, km)]) * 0.5;
+        f.DST[c + g.FS] = j >= 2 ? g.wff[j] * R[c] + g.wfb[j] * R[pidx(g, i, j - 1, k)] : R[pidx(g, i, 0, k)];
+        if (j >= 2) {
+            f.MST[c] = ((U0[c] + U0[pidx(g, im, j, k)]) * g.wff[j] + (U0[pidx(g, i, j - 1, k)] + U0[pidx(g, im, j - 1, k)]) * g.wfb[j]) * 0.5;
+            f.MST[c + 2 * g.FS] = ((U0[pidx(g, i, j, km)] + U0[c]) * g.wff[j] +
+                                   (U0[pidx(g, i, j - 1, km)] + U0[pidx(g, i, j - 1, k)]) * g.wfb[j]) * 0.5;
+        } else {
+            f.MST[c] = U0[pidx(g, i, 0, k)];
+            f.MST[c + 2 * g.FS] = U0[pidx(g, i, 0, k)];
+        }
+        f.MST[c + g.FS] = (U0[c] + U0[pidx(g, im, j, k)] + U0[pidx(g, i, j, km)] + U0[pidx(g, im, j, km)]) * 0.5 * 0.5;
+        if (j == M) {
+            const long long ct = pidx(g, i, M + 1, k);
+            f.DST[ct + g.FS] = R[ct];
+            f.MST[ct] = U0[ct];
+            f.MST[ct + 2 * g.FS] = U0[ct];
+        }
+    }
+}
+
+// DIVG_U_io; also VELOCITY_CALC_io of the upload (Q = G / D_STG) when vel != 0
+__global__ void __launch_bounds__(IO_NT) k_io_velocity(Geo g, IoFields f) {
+    const long long tot = (long long)g.L * g.M * g.N;
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const long long c = pidx(g, i, j, k);
+        const double g1 = f.G[c], g3 = f.G[c + 2 * g.FS], d1 = f.DST[c], d3 = f.DST[c + 2 * g.FS];
+        f.Q[c] = g1 / d1;
+        f.Q[c + 2 * g.FS] = g3 / d3;
+        if (j >= 2) f.Q[c + g.FS] = f.G[c + g.FS] / f.DST[c + g.FS];
+    }
+}
+
+__global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFields f) {
+    const int L = g.L, N = g.N;
+    const long long tot = (long long)L * g.M * N;
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const long long c = pidx(g, i, j, k);
+        const double* Q = f.Q;
+        const double u = Q[c], up = Q[pidx(g, wrapp(i, L), j, k)];
+        const double v = Q[c + g.FS], vp = Q[c + g.FS + L];
+        const double w = Q[c + 2 * g.FS], wp = Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS];
+        const double DIVX = (up - u) * g.dxi;
+        const double DIVY = (vp - v) * (g.dyfi[j] * 1.0);
+        const double DIVZ = (wp - w) * (g.dzi * 1.0);
+        f.DIVU[c] = (DIVX + DIVY + DIVZ) / 3.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st,
+                                                  int ns) {
+    __shared__ double sred[32];
+    __shared__ int is_last;
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * M * N;
+    const long long FS = g.FS;
+    const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns], ta = g.talp[ns];
+    const double cv = g.cvisc;
+    const double* G = f.G;
+    const double* Q = f.Q;
+    const double* U0 = f.MU0;
+    const double* MS = f.MST;
+    const double* DV = f.DIVU;
+    const double* PR = f.PR;
+    double bulk = 0.0;
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const int ip = wrapp(i, L), im = wrapm(i, L), kp = wrapp(k, N), km = wrapm(k, N);
+        const int jp = j + 1, jm = j - 1;
+        const long long c = pidx(g, i, j, k);
+        const long long cip = pidx(g, ip, j, k), cim = pidx(g, im, j, k);
+        const long long cjp = pidx(g, i, jp, k), cjm = pidx(g, i, jm, k);
+        const long long ckp = pidx(g, i, j, kp), ckm = pidx(g, i, j, km);
+        const double wffj = g.wff[j], wfbj = g.wfb[j], wffp = g.wff[jp], wfbp = g.wfb[jp];
+        const double dyfij = g.dyfi[j], dycij = g.dyci[j], dycip = g.dyci[jp];
+        // -------- x momentum: CONVECTION_X_io + VISCOUS_ALL_EXPLT_X_io --------
+        double ex1, ex2 = 0.0, ex3;
+        {
+            const double H11F = (G[cip] + G[c]) * (Q[cip] + Q[c]);
+            const double H11B = (G[c] + G[cim]) * (Q[c] + Q[cim]);
+            const double H11 = (H11F - H11B) * (g.dxi * 0.5 * 0.5);
+            const double H12F = (G[cjp + FS] + G[pidx(g, im, jp, k) + FS]) * (wffp * Q[cjp] + wfbp * Q[c]);
+            const double H12B = (G[c + FS] + G[cim + FS]) * (wffj * Q[c] + wfbj * Q[cjm]);
+            const double H12 = (H12F - H12B) * (dyfij * 0.5 * 1.0);
+            const double H13F = (G[ckp + 2 * FS] + G[pidx(g, im, j, kp) + 2 * FS]) * (Q[ckp] + Q[c]);
+            const double H13B = (G[c + 2 * FS] + G[cim + 2 * FS]) * (Q[c] + Q[ckm]);
+            const double H13 = (H13F - H13B) * ((g.dzi * 0.5 * 0.5) * 1.0);
+            double DUDX = (Q[cip] - Q[c]) * g.dxi;
+            const double T11F = 0.5 * (U0[c] + U0[c]) * (DUDX - DV[c]);
+            DUDX = (Q[c] - Q[cim]) * g.dxi;
+            const double T11B = 0.5 * (U0[cim] + U0[cim]) * (DUDX - DV[cim]);
+            const double D11 = (T11F - T11B) * (2.0 * g.dxi * cv);
+            double DUDY = (Q[cjp] - Q[c]) * dycip / 1.0;
+            double DVDX = (Q[cjp + FS] - Q[pidx(g, im, jp, k) + FS]) * g.dxi;
+            const double T12F = MS[cjp] * (DUDY + DVDX);
+            DUDY = (Q[c] - Q[cjm]) * dycij / 1.0;
+            DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
+            const double T12B = MS[c] * (DUDY + DVDX);
+            const double D12 = (T12F - T12B) * (dyfij * cv * 1.0);
+            double DUDZ = (Q[ckp] - Q[c]) * g.dzi;
+            double DWDX = (Q[ckp + 2 * FS] - Q[pidx(g, im, j, kp) + 2 * FS]) * g.dxi;
+            const double T13F = MS[ckp + FS] * (DUDZ + DWDX);
+            DUDZ = (Q[c] - Q[ckm]) * g.dzi;
+            DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
+            const double T13B = MS[c + FS] * (DUDZ + DWDX);
+            const double D13 = (T13F - T13B) * ((g.dzi * cv) * 1.0);
+            ex1 = -(H11 + H12 + H13);
+            ex1 = ex1 + D11 + D12 + D13;
+        }
+        // -------- y momentum (j >= 2) --------
+        if (j >= 2) {
+            const double H21F = (wffj * G[cip] + wfbj * G[pidx(g, ip, jm, k)]) * (Q[cip + FS] + Q[c + FS]);
+            const double H21B = (wffj * G[c] + wfbj * G[cjm]) * (Q[c + FS] + Q[cim + FS]);
+            const double H21 = (H21F - H21B) * (g.dxi * 0.5);
+            const double H22F = (G[cjp + FS] + G[c + FS]) * (Q[cjp + FS] * 1.0 + Q[c + FS] * 1.0);
+            const double H22B = (G[c + FS] + G[cjm + FS]) * (Q[c + FS] * 1.0 + Q[cjm + FS] * 1.0);
+            const double H22 = (H22F - H22B) * (dycij * 0.5 * 0.5);
+            const double H23F = (wffj * G[ckp + 2 * FS] * 1.0 + wfbj * G[pidx(g, i, jm, kp) + 2 * FS] * 1.0) * (Q[ckp + FS] + Q[c + FS]);
+            const double H23B = (wffj * G[c + 2 * FS] * 1.0 + wfbj * G[cjm + 2 * FS] * 1.0) * (Q[c + FS] + Q[ckm + FS]);
+            const double H23 = (H23F - H23B) * ((g.dzi * 0.5) * 1.0);
+            double DVDY = (Q[cjp + FS] - Q[c + FS]) * dyfij;
+            const double T22F = 0.5 * (U0[c] + U0[c]) * (DVDY - DV[c]);
+            DVDY = (Q[c + FS] - Q[cjm + FS]) * g.dyfi[jm];
+            const double T22B = 0.5 * (U0[cjm] + U0[cjm]) * (DVDY - DV[cjm]);
+            const double D22 = (T22F - T22B) * (2.0 * dycij * cv);
+            double DVDX = (Q[cip + FS] - Q[c + FS]) * g.dxi;
+            double DUDY = (Q[cip] - Q[pidx(g, ip, jm, k)]) * dycij;
+            const double T21F = MS[cip] * (DVDX + DUDY);
+            DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
+            DUDY = (Q[c] - Q[cjm]) * dycij;
+            const double T21B = MS[c] * (DVDX + DUDY);
+            const double D21 = (T21F - T21B) * (g.dxi * cv);
+            double DVDZ = (Q[ckp + FS] - Q[c + FS]) * g.dzi;
+            double DWDY = (Q[ckp + 2 * FS] - Q[pidx(g, i, jm, kp) + 2 * FS]) * dycij;
+            const double T23F = MS[ckp + 2 * FS] * (DVDZ + DWDY);
+            DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
+            DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
+            const double T23B = MS[c + 2 * FS] * (DVDZ + DWDY);
+            const double D23 = (T23F - T23B) * (g.dzi * cv);
+            ex2 = -(H21 + H22 + H23);
+            ex2 = ex2 + D21 + D22 + D23;
+        }
+        // -------- z momentum --------
+        {
+            const double H31F = (G[cip] + G[pidx(g, ip, j, km)]) * (Q[cip + 2 * FS] + Q[c + 2 * FS]);
+            const double H31B = (G[c] + G[ckm]) * (Q[c + 2 * FS] + Q[cim + 2 * FS]);
+            const double H31 = (H31F - H31B) * (g.dxi * 0.5 * 0.5);
+            const double H32F = (G[cjp + FS] + G[pidx(g, i, jp, km) + FS]) * (wffp * Q[cjp + 2 * FS] * 1.0 + wfbp * Q[c + 2 * FS] * 1.0);
+            const double H32B = (G[c + FS] + G[ckm + FS]) * (wffj * Q[c + 2 * FS] * 1.0 + wfbj * Q[cjm + 2 * FS] * 1.0);
+            const double H32 = (H32F - H32B) * (dyfij * 0.5);
+            const double H33F = (G[ckp + 2 * FS] + G[c + 2 * FS]) * (Q[ckp + 2 * FS] + Q[c + 2 * FS]);
+            const double H33B = (G[c + 2 * FS] + G[ckm + 2 * FS]) * (Q[c + 2 * FS] + Q[ckm + 2 * FS]);
+            const double H33 = (H33F - H33B) * ((g.dzi * 0.5 * 0.5) * 1.0);
+            double DWDZ = (Q[ckp + 2 * FS] - Q[c + 2 * FS]) * g.dzi;
+            const double T33F = 0.5 * (U0[c] + U0[c]) * (DWDZ - DV[c]);
+            DWDZ = (Q[c + 2 * FS] - Q[ckm + 2 * FS]) * g.dzi;
+            const double T33B = 0.5 * (U0[ckm] + U0[ckm]) * (DWDZ - DV[ckm]);
+            const double D33 = (T33F - T33B) * (2.0 * g.dzi * cv);
+            double DWDX = (Q[cip + 2 * FS] - Q[c + 2 * FS]) * g.dxi;
+            double DUDZ = (Q[cip] - Q[pidx(g, ip, j, km)]) * g.dzi;
+            const double T31F = MS[cip + FS] * (DWDX + DUDZ);
+            DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
+            DUDZ = (Q[c] - Q[ckm]) * g.dzi;
+            const double T31B = MS[c + FS] * (DWDX + DUDZ);
+            const double D31 = (T31F - T31B) * (g.dxi * cv);
+            double DWDY = (Q[cjp + 2 * FS] - Q[c + 2 * FS]) * dycip;
+            double DVDZ = (Q[cjp + FS] - Q[pidx(g, i, jp, km) + FS]) * g.dzi;
+            const double T32F = MS[cjp + 2 * FS] * (DWDY + DVDZ);
+            DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
+            DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
+            const double T32B = MS[c + 2 * FS] * (DWDY + DVDZ);
+            const double D32 = (T32F - T32B) * (dyfij * cv);
+            ex3 = -(H31 + H32 + H33);
+            ex3 = ex3 + D31 + D32 + D33;
+        }
+        // -------- RHS_MOM_EXPLICIT_io --------
+        const long long ii = iidx(g, i, j, k);
+        const double e01 = f.EX0[ii], e02 = f.EX0[ii + g.FI], e03 = f.EX0[ii + 2 * g.FI];
+        const double pc = PR[c], pim = PR[cim], pjm = PR[cjm], pkm = PR[ckm];
+        double r1 = (tg * ex1 + tr * e01) * dt;
+        r1 = r1 - (pc - pim) * (ta * dt * g.dxi);
+        double r3 = (tg * ex3 + tr * e03) * dt;
+        r3 = r3 - (pc - pkm) * (ta * dt * g.dzi);
+        f.EX0[ii] = ex1;
+        f.EX0[ii + 2 * g.FI] = ex3;
+        f.RHS[ii] = r1;
+        f.RHS[ii + 2 * g.FI] = r3;
+        if (j >= 2) {
+            double r2 = (tg * ex2 + tr * e02) * dt;
+            r2 = r2 - (pc - pjm) * (ta * dt * dycij / 1.0);
+            f.EX0[ii + g.FI] = ex2;
+            f.RHS[ii + g.FI] = r2;
+        }
+        bulk += r1 / dyfij / 1.0;
+    }
+    double s = block_sum<IO_NT>(bulk, sred);
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = s;
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->ctr, 1u);
+        is_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        double a = 0.0;
+        for (int t = threadIdx.x; t < (int)gridDim.x; t += IO_NT) a += __ldcg(partial + t);
+        a = block_sum<IO_NT>(a, sred);
+        if (threadIdx.x == 0) {
+            st->bulksum = a;
+            st->ctr = 0u;
+        }
+    }
+}
+
+// bulk forcing (RHS_MOM_EXPLICIT_io :228-265) + MASSFLUX_CALC_io
+__global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+    const long long tot = (long long)g.L * g.M * g.N;
+    double dpg = 0.0;
+    if (g.iflowdriven == 1) dpg = st->bulksum / g.volm;
+    else if (g.iflowdriven == 2) dpg = -0.5 * g.cf_given * (g.talp[ns] * st->dt);
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const long long c = pidx(g, i, j, k), ii = iidx(g, i, j, k);
+        const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS];
+        const double r1 = f.RHS[ii] - dpg, r3 = f.RHS[ii + 2 * g.FI];
+        f.G[c] = g1 + r1;
+        f.G[c + 2 * g.FS] = g3 + r3;
+        if (j >= 2) f.G[c + g.FS] = g2 + f.RHS[ii + g.FI];
+    }
+}
+
+// DIVG_io + forward x transform (same tiling as k_div_fftx)
+__global__ void __launch_bounds__(PX_NT) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
+                                                       double2* __restrict__ SP, const DevState* __restrict__ st, int ns) {
+    extern __shared__ double2 smc[];
+    const int L = g.L, M = g.M, N = g.N, LH = g.LH;
+    const int j0 = 1 + blockIdx.x * PX_TJ;
+    const int k = blockIdx.y;
+    const int nj = min(PX_TJ, M - j0 + 1);
+    const int np = (nj + 1) >> 1;
+    const int kp = wrapp(k, N);
+    const double coe0 = 1.0 / st->dt / g.talp[ns];
+    const double coe1 = g.dxi / 1.0;
+#pragma unroll 4
+    for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
+        const int jl = p / L, i = p - jl * L;
+        const int pair = jl >> 1, part = jl & 1;
+        double val = 0.0;
+        if (jl < nj) {
+            const int j = j0 + jl;
+            const long long c = pidx(g, i, j, k);
+            const double u = G[c], up = G[pidx(g, wrapp(i, L), j, k)];
+            const double v = G[c + g.FS], vp = G[c + g.FS + L];
+            const double w = G[c + 2 * g.FS], wp = G[pidx(g, i, j, kp) + 2 * g.FS];
+            const double coe2 = g.dyfi[j] / 1.0;
+            const double DIVX = (up - u) * coe1, DIVY = (vp - v) * coe2, DIVZ = (wp - w) * g.dzi;
+            const double DQ = DIVX + DIVY + DIVZ + 0.0;  // + DrhoDtP (zero while the thermal solver is off)
+            val = DQ * coe0;
+            RHSLL[iidx(g, i, j, k)] = val;
+        }
+        double2* line = smc + pair * L;
+        const int pos = g.permx[i];
+        if (part == 0) line[pos].x = val; else line[pos].y = val;
+    }
+    block_fft<-1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    const double sc = 0.5 / (double)L;
+    for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
+        const int pair = p / LH, kx = p - pair * LH;
+        const double2* line = smc + pair * L;
+        const double2 z = line[kx];
+        const double2 zc = line[kx == 0 ? 0 : L - kx];
+        const int ja = j0 + 2 * pair;
+        SP[kx + (long long)LH * ((ja - 1) + (long long)M * k)] = make_double2((z.x + zc.x) * sc, (z.y - zc.y) * sc);
+        if (2 * pair + 1 < nj)
+            SP[kx + (long long)LH * ((ja) + (long long)M * k)] = make_double2((z.y + zc.y) * sc, (zc.x - z.x) * sc);
+    }
+}
+
+// PRCALC_io (explicit) + MASSFLUX_UPDATE_io + VELOCITY_CALC_io
+__global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFields f, const double* __restrict__ DPH,
+                                                      const DevState* __restrict__ st, int ns) {
+    const int L = g.L, M = g.M, N = g.N;
+    const long long tot = (long long)L * M * N;
+    const double dt = st->dt, ta = g.talp[ns];
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const long long c = pidx(g, i, j, k);
+        const double ph = DPH[c];
+        const double phim = DPH[pidx(g, wrapm(i, L), j, k)];
+        const double phkm = DPH[pidx(g, i, j, wrapm(k, N))];
+        const double phjm = j >= 2 ? DPH[pidx(g, i, j - 1, k)] : 0.0;
+        const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS], pr = f.PR[c];
+        const double d1 = f.DST[c], d2 = f.DST[c + g.FS], d3 = f.DST[c + 2 * g.FS];
+        const double pn = pr + ph;
+        f.PR[c] = pn;
+        if (j == 1) f.PR[pidx(g, i, 0, k)] = pn;
+        if (j == M) f.PR[pidx(g, i, M + 1, k)] = pn;
+        const double n1 = g1 - (ph - phim) * (dt * ta * g.dxi);
+        const double n3 = g3 - (ph - phkm) * (dt * ta * g.dzi);
+        f.G[c] = n1;
+        f.G[c + 2 * g.FS] = n3;
+        f.Q[c] = n1 / d1;
+        f.Q[c + 2 * g.FS] = n3 / d3;
+        if (j >= 2) {
+            const double n2 = g2 - (ph - phjm) * (dt * ta * g.dyci[j] / 1.0);
+            f.G[c + g.FS] = n2;
+            f.Q[c + g.FS] = n2 / d2;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st) {
+    __shared__ double sred[32];
+    const int L = g.L, N = g.N;
+    const long long tot = (long long)L * g.M * N;
+    double mx = 0.0;
+    bool bad = false;
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const long long c = pidx(g, i, j, k);
+        const double* Q = f.Q;
+        double q = (fabs((Q[c] + Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
+                    fabs((Q[c + g.FS] + Q[c + g.FS + L]) * g.dyfi[j] * 1.0) +
+                    fabs((Q[c + 2 * g.FS] + Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
+        const double vcf = 2.0 * g.cvisc * (g.dxqi + g.dzqi * 1.0 + g.dyfi[j] * g.dyfi[j]) * f.MU[c] / f.RHO[c];
+        if (!(q == q) || !(vcf == vcf)) bad = true;
+        q = fmax(q, vcf);
+        mx = fmax(mx, q);
+    }
+    if (bad) atomicOr(&st->err, CHS_EBIT_NAN);
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->dtprev = st->dt;
+    double r = block_max<IO_NT>(mx, sred);
+    if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}

@@ -32,8 +32,9 @@ extern "C" {
 
 typedef struct chapsim_ctx chapsim_ctx_t;
 
-/* Grid: NCL1_tg, NCL2, NCL3 of src/modules.f90 (mesh_info).  Only the plane
- * channel (iCase = 1) in the periodic TG domain (iDomain = 1) is accepted.
+/* Grid: NCL1 (NCL1_tg or NCL1_io), NCL2, NCL3 of src/modules.f90 (mesh_info).
+ * Only the plane channel (iCase = 1) is accepted, in the periodic TG domain
+ * (iDomain = 1) or the x-periodic main domain (iDomain = 2).
  * L and N must factor into 2s and 3s (FFT lengths), L, M, N must be
  * multiples of 32 between 32 and 384. */
 typedef struct {
@@ -41,7 +42,7 @@ typedef struct {
     int32_t ncl2;   /* M */
     int32_t ncl3;   /* N */
     int32_t icase;  /* must be 1 (ICHANL) */
-    int32_t idomain;/* must be 1 (ITG)    */
+    int32_t idomain;/* 1 (ITG) or 2 (IIO, x-periodic main domain) */
 } chapsim_grid_t;
 
 /* Coefficients computed by the host's set-up routines, passed unchanged.
@@ -132,6 +133,26 @@ int chapsim_tdmaiji_cyc(const double* a, const double* b, const double* c, doubl
  * BCJ(ISZ, 2) (may be NULL for zero).  Host arrays. */
 int chapsim_tdmaijj_noncyc(const double* a, const double* b, const double* c, double* r, const double* bcj,
                            int32_t jsz, int32_t isz);
+
+/* ---- Main (IO) domain, explicit viscous terms (context created with
+ * grid.idomain = 2).  SOLVERRK3_MOM_io(NS) (src/SOLVERRK3_MOM_IO.f90:11-120,
+ * iVisScheme = 0) for a flow whose property fields are fixed (thermal solver
+ * not yet active).  chapsim_advance_tg runs the IO step (CFL_io, dt rule, three
+ * substeps) for such a context. */
+
+/* ReStart_INSTANT_VARS_io (src/processing/RESTART_io.f90:16-200) field set-up:
+ * g = G_io(NCL1, 0:NCL2+1, NCL3, 3) (rho*u), pr = PR_io, rho = DENSITY0,
+ * mu0 = Viscousity0, mu = Viscousity (each (NCL1, 0:NCL2+1, NCL3)).  Applies
+ * BC_WALL_G_io/BC_WALL_PR_io, DENSITY_Staggered, MU_Staggered and
+ * VELOCITY_CALC_io; EXPLT0_io is zeroed. */
+int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* g, const double* pr, const double* rho,
+                             const double* mu0, const double* mu);
+/* g = G_io, q = Q_io (velocity), pr = PR_io; any may be NULL. */
+int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* g, double* q, double* pr);
+/* SOLVERRK3_MOM_io(NS) with the device-resident DT. */
+int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns);
+/* CFL_io (src/CFL.f90:55-107): CFLMM_io including the viscous number. */
+int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm);
 
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
  * with a CUDA event after every kernel; ms[slot] receives the summed
