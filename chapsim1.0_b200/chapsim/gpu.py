@@ -31,7 +31,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_upload_io_fields",
             "chapsim_download_io_fields", "chapsim_rk_substep_io", "chapsim_cfl_io", "chapsim_profile_steps",
             "chapsim_get_stream",
-            "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step"]
+            "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step", "chapsim_tdma_lines_noalloc"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
@@ -91,6 +91,8 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_fft99_pois3d.argtypes = [vp, _dp, _dp]
     L.chapsim_tdmaiji_cyc.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
     L.chapsim_tdmaijj_noncyc.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
+    L.chapsim_tdma_lines_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_int32, ctypes.c_int32, vp]
     L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
     L.chapsim_download_io_fields.argtypes = [vp, _dp, _dp, _dp]
     L.chapsim_rk_substep_io.argtypes = [vp, ctypes.c_int32]

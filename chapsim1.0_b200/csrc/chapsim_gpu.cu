@@ -893,3 +893,106 @@ extern "C" int chapsim_tdmaijj_noncyc(const double* a, const double* b, const do
     // lines along J (stride ISZ), one per I
     return run_lines(a, b, c, r, bcj, isz, 1, isz, jsz, false);
 }
+
+// ------------- line solver on caller-owned device memory, no allocation -------------
+// For callers that cannot let a library allocate device memory.  Examples: a host
+// whose HBM is already reserved by its own caching allocator or OpenACC / CUDA Fortran
+// data regions, where cudaMalloc may fail; or a time loop that must not stall, because
+// cudaFree waits for the whole device.  The per-line elimination vectors of the
+// sequential recurrence (k_tdma_seq) live in one fixed module-scope array instead.
+//   words [0, 32)  : status block; word 0 counts lines whose solution is not finite
+//   words [32, ...): 3*n doubles per line (the H, G1, G2 recurrences)
+#include <mutex>
+
+static_assert(CHAPSIM_NOALLOC_SCRATCH_BYTES % 256 == 0, "scratch size must be a multiple of 256 bytes");
+constexpr long long NOALLOC_STATUS_WORDS = 32;
+constexpr long long NOALLOC_TOTAL_WORDS = CHAPSIM_NOALLOC_SCRATCH_BYTES / sizeof(double);
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_TOTAL_WORDS];
+
+// one thread per line: counts lines with a non-finite entry
+__global__ void k_count_nonfinite_lines(const double* r, int nlines, long long ls, long long es, int n,
+                                        unsigned int* count) {
+    const int l = blockIdx.x * blockDim.x + threadIdx.x;
+    if (l >= nlines) return;
+    const long long o = (long long)l * ls;
+    bool bad = false;
+    for (int i = 0; i < n; ++i) bad |= !isfinite(r[o + (long long)i * es]);
+    if (bad) atomicAdd(count, 1u);
+}
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Address of the scratch array on the current device, looked up once per device.
+int noalloc_scratch(int dev, double** out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(nullptr, CHAPSIM_ERR_CUDA,
+                        std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return CHAPSIM_OK;
+}
+
+// true when p is device (or managed) memory of device dev
+bool on_device(const void* p, int dev) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) { cudaGetLastError(); return false; }
+    return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == dev;
+}
+}  // namespace
+
+extern "C" int chapsim_tdma_lines_noalloc(const double* a, const double* b, const double* c, double* r,
+                                          const double* bcj, int32_t nlines, int64_t line_stride,
+                                          int64_t elem_stride, int32_t n, int32_t cyclic, void* stream) {
+    if (!a || !b || !c || !r || nlines <= 0 || n < 3 || line_stride < 1 || elem_stride < 1)
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "bad tridiagonal arguments (need nlines >= 1, n >= 3, strides >= 1)");
+    if (cyclic && bcj) return fail(nullptr, CHAPSIM_ERR_BADARG, "cyclic systems take no Dirichlet values (bcj must be NULL)");
+    const long long need = 3LL * n * nlines;
+    const long long avail = NOALLOC_TOTAL_WORDS - NOALLOC_STATUS_WORDS;
+    if (need > avail)
+        return fail(nullptr, CHAPSIM_ERR_BADARG,
+                    "chapsim_tdma_lines_noalloc: 3*n*nlines = " + std::to_string(need) +
+                        " doubles of scratch exceeds the fixed limit of " + std::to_string(avail) +
+                        " (CHAPSIM_NOALLOC_SCRATCH_BYTES); split the lines over several calls");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(nullptr, CHAPSIM_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return fail(nullptr, CHAPSIM_ERR_BADARG, "device ordinal out of range");
+    for (const void* p : {(const void*)a, (const void*)b, (const void*)c, (const void*)r})
+        if (!on_device(p, dev))
+            return fail(nullptr, CHAPSIM_ERR_BADARG, "a, b, c and r must be device memory of the current device");
+    if (bcj && !on_device(bcj, dev))
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "bcj must be device memory of the current device");
+    double* scratch = nullptr;
+    if (int rc = noalloc_scratch(dev, &scratch)) return rc;
+    unsigned int* status = reinterpret_cast<unsigned int*>(scratch);
+    double* wk = scratch + NOALLOC_STATUS_WORDS;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+#define NCK(call)                                                                                    \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess) return fail(nullptr, CHAPSIM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+    // the array keeps the previous call's contents: the counter must start at zero
+    NCK(cudaMemsetAsync(status, 0, sizeof(unsigned int), s));
+    k_tdma_seq<<<(nlines + 127) / 128, 128, 0, s>>>(a, b, c, r, bcj, wk, nlines, line_stride, elem_stride, n,
+                                                     cyclic ? 1 : 0);
+    NCK(cudaGetLastError());
+    k_count_nonfinite_lines<<<(nlines + 127) / 128, 128, 0, s>>>(r, nlines, line_stride, elem_stride, n, status);
+    NCK(cudaGetLastError());
+    unsigned int nbad = 0;
+    NCK(cudaMemcpyAsync(&nbad, status, sizeof(nbad), cudaMemcpyDeviceToHost, s));
+    NCK(cudaStreamSynchronize(s));
+#undef NCK
+    if (nbad)
+        return fail(nullptr, CHAPSIM_ERR_NAN, std::to_string(nbad) + " of " + std::to_string(nlines) +
+                                                  " lines have a non-finite solution");
+    return CHAPSIM_OK;
+}

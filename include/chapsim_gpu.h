@@ -134,6 +134,38 @@ int chapsim_tdmaiji_cyc(const double* a, const double* b, const double* c, doubl
 int chapsim_tdmaijj_noncyc(const double* a, const double* b, const double* c, double* r, const double* bcj,
                            int32_t jsz, int32_t isz);
 
+/* Fixed size of the device scratch array used by chapsim_tdma_lines_noalloc
+ * (16 MiB per device: a 256-byte status block, then 2,097,120 doubles). */
+#define CHAPSIM_NOALLOC_SCRATCH_BYTES (16u * 1024u * 1024u)
+
+/* No counterpart in the reference.  The same tridiagonal line solves as
+ * chapsim_tdmaiji_cyc (cyclic != 0) and chapsim_tdmaijj_noncyc (cyclic == 0),
+ * for a caller that keeps its arrays on the device and cannot let the library
+ * allocate: a host whose HBM is already held by its own pool or data regions,
+ * or a time loop that must not stall on the device-wide wait of cudaFree.
+ * The call allocates nothing: its work vectors live in one module-scope
+ * device array of CHAPSIM_NOALLOC_SCRATCH_BYTES.
+ *   a, b, c, r: device memory of the current device; element e of line l is
+ *     at l*line_stride + e*elem_stride, e < n; r is overwritten.
+ *   bcj: NULL (zero) or 2*nlines device doubles, the Dirichlet values before
+ *     the first and after the last row of each line (non-cyclic only).
+ *   stream: cudaStream_t as void* (NULL = default stream); the call waits for
+ *     it before returning.
+ * Limits and errors: n >= 3; 3*n*nlines must not exceed 2,097,120, else
+ * CHAPSIM_ERR_BADARG with the sizes in chapsim_last_error_string(NULL);
+ * host pointers give CHAPSIM_ERR_BADARG; a non-finite solution on any line
+ * gives CHAPSIM_ERR_NAN.
+ * Set-up: the first call on each device (the one current in the calling
+ * thread) looks up the array's address with cudaGetSymbolAddress and keeps
+ * it; make that first call before any stream capture begins.
+ * Sharing: all calls on a device use the same array, which keeps the last
+ * call's contents (the call clears its status counter itself).  Calls that
+ * overlap in time on one device, e.g. from two host threads, race on it and
+ * must be serialised by the caller. */
+int chapsim_tdma_lines_noalloc(const double* a, const double* b, const double* c, double* r, const double* bcj,
+                               int32_t nlines, int64_t line_stride, int64_t elem_stride, int32_t n, int32_t cyclic,
+                               void* stream);
+
 /* ---- Main (IO) domain, explicit viscous terms (context created with
  * grid.idomain = 2).  SOLVERRK3_MOM_io(NS) (src/SOLVERRK3_MOM_IO.f90:11-120,
  * iVisScheme = 0) for a flow whose property fields are fixed (thermal solver
