@@ -31,7 +31,8 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_upload_io_fields",
             "chapsim_download_io_fields", "chapsim_rk_substep_io", "chapsim_cfl_io", "chapsim_profile_steps",
             "chapsim_get_stream",
-            "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step", "chapsim_tdma_lines_noalloc"]
+            "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step", "chapsim_tdma_lines_noalloc",
+            "chapsim_prop_table_init", "chapsim_therm_prop_update_points"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
@@ -56,6 +57,12 @@ class Coefs(ctypes.Structure):
                 ("acph", _dp), ("apph", _dp), ("amvr", _dp), ("acvr", _dp), ("apvr", _dp), ("ak1", _dp),
                 ("ak3", _dp), ("tgam", ctypes.c_double * 4), ("troh", ctypes.c_double * 4),
                 ("talp", ctypes.c_double * 4)]
+
+
+class PropTableC(ctypes.Structure):
+    _fields_ = ([("n_list", ctypes.c_int32), ("fix_swap", ctypes.c_int32)] +
+                [(f"list_{n}", _dp) for n in ("h", "t", "d", "m", "k", "cp", "dh")] +
+                [(f"{s}_{c}", _dp) for s in ("dhh", "ht", "hd", "hm", "hk", "hcp") for c in ("b", "c", "d")])
 
 
 class Opts(ctypes.Structure):
@@ -91,6 +98,8 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_fft99_pois3d.argtypes = [vp, _dp, _dp]
     L.chapsim_tdmaiji_cyc.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
     L.chapsim_tdmaijj_noncyc.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
+    L.chapsim_prop_table_init.argtypes = [vp, ctypes.POINTER(PropTableC)]
+    L.chapsim_therm_prop_update_points.argtypes = [vp, ctypes.c_int64] + [_dp] * 7
     L.chapsim_tdma_lines_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_int32, vp]
     L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
@@ -300,6 +309,29 @@ class ChannelTG:
         out = np.zeros(self.field_shape())
         self._check(self.lib.chapsim_fft99_pois3d(self.h, _ptr(rhs), _ptr(out)))
         return out
+
+
+    # -- thermophysical properties (table search) --------------------------------
+    def prop_table_init(self, table, fix_swap=False):
+        """Uploads a ``chapsim.thermo.SplineTable`` (nondimensional lists and coefficients)."""
+        li, co = table.lists, table.coef
+        keep = {f"list_{n.lower()}": np.ascontiguousarray(li[n], np.float64)
+                for n in ("H", "T", "D", "M", "K", "CP", "DH")}
+        for s, key in (("dhh", "DHH"), ("ht", "HT"), ("hd", "HD"), ("hm", "HM"), ("hk", "HK"), ("hcp", "HCP")):
+            for c, arr in zip("bcd", co[key]):
+                keep[f"{s}_{c}"] = np.ascontiguousarray(arr, np.float64)
+        t = PropTableC(n_list=table.n, fix_swap=int(bool(fix_swap)), **{k: _ptr(v) for k, v in keep.items()})
+        self._check(self.lib.chapsim_prop_table_init(self.h, ctypes.byref(t)))
+        self._prop_keep = keep
+
+    def THERM_PROP_UPDATE_points(self, dh):
+        """Table-search property update of host points; returns dict H, T, D, M, K, CP shaped like dh."""
+        dh = np.ascontiguousarray(dh, np.float64)
+        n = dh.size
+        outs = {k: np.empty(dh.shape) for k in ("H", "T", "D", "M", "K", "CP")}
+        self._check(self.lib.chapsim_therm_prop_update_points(self.h, n, _ptr(dh), *[_ptr(outs[k]) for k in
+                                                                                      ("H", "T", "D", "M", "K", "CP")]))
+        return outs
 
 
 class ChannelIO(ChannelTG):

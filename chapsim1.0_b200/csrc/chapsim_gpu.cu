@@ -16,6 +16,7 @@
 #include "poisson.cuh"
 #include "tdma.cuh"
 #include "io.cuh"
+#include "thermo.cuh"
 
 // x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
 __global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
@@ -150,6 +151,13 @@ struct chapsim_ctx {
     int prof_n = 0;
     int kernels_per_step = 0;
     unsigned long long launches = 0;
+    int nsm = 148;
+    // property table for THERM_PROP_UPDATE (table search)
+    void* ptab = nullptr;         // packed rows and keys, one allocation
+    PropTab tab{};
+    PropStatus* pstat = nullptr;
+    double* pbuf = nullptr;       // staging of the host-array entry (7 doubles per point)
+    long long pbuf_pts = 0;
     std::string err;
 };
 
@@ -514,6 +522,7 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
 
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    ctx->nsm = nsm;
     ctx->npart_red = 4 * nsm;
     INIT_CK(cudaMalloc(&ctx->part_red, (size_t)ctx->npart_red * sizeof(double)));
     if (ctx->domain == 2) {
@@ -569,6 +578,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
+    cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -892,6 +902,152 @@ extern "C" int chapsim_tdmaijj_noncyc(const double* a, const double* b, const do
                                       int32_t jsz, int32_t isz) {
     // lines along J (stride ISZ), one per I
     return run_lines(a, b, c, r, bcj, isz, 1, isz, jsz, false);
+}
+
+// ----------------------- property update by table search -----------------------
+namespace {
+int first_min(int n, const double* a) {
+    int k = 0;
+    for (int i = 1; i < n; ++i) if (a[i] < a[k]) k = i;
+    return k;
+}
+int first_max(int n, const double* a) {
+    int k = 0;
+    for (int i = 1; i < n; ++i) if (a[i] > a[k]) k = i;
+    return k;
+}
+size_t prop_smem(int n) { return n <= PROP_SMEM_MAX_ROWS ? (size_t)2 * n * sizeof(double) : 0; }
+
+int prop_grid(const chapsim_ctx* ctx, long long npts) {
+    const long long want = (npts + PROP_NT - 1) / PROP_NT;
+    const long long cap = 8LL * ctx->nsm;
+    return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+int prop_reset_status(chapsim_ctx* ctx) {
+    CK(cudaMemsetAsync(&ctx->pstat->first_bad, 0xff, sizeof(unsigned long long), ctx->stream));
+    CK(cudaMemsetAsync(&ctx->pstat->nbad, 0, 2 * sizeof(unsigned int), ctx->stream));
+    return CHAPSIM_OK;
+}
+}  // namespace
+
+extern "C" int chapsim_prop_table_init(chapsim_ctx_t* ctx, const chapsim_prop_table_t* t) {
+    if (!ctx || !t) return fail(ctx, CHAPSIM_ERR_BADARG, "null context or table");
+    const int n = t->n_list;
+    if (n < 4) return fail(ctx, CHAPSIM_ERR_BADARG, "the property table needs N_LIST >= 4 rows");
+    const double* need[] = {t->list_h, t->list_t, t->list_d, t->list_m, t->list_k, t->list_cp, t->list_dh,
+                            t->dhh_b, t->dhh_c, t->dhh_d, t->ht_b, t->ht_c, t->ht_d, t->hd_b, t->hd_c, t->hd_d,
+                            t->hm_b, t->hm_c, t->hm_d, t->hk_b, t->hk_c, t->hk_d, t->hcp_b, t->hcp_c, t->hcp_d};
+    for (const double* p : need)
+        if (!p) return fail(ctx, CHAPSIM_ERR_BADARG, "null property-table array");
+    const double *H = t->list_h, *T = t->list_t, *DH = t->list_dh;
+    // the reference's monotonicity checks (SPLINE_COEFFICIENTS_FOR_DH)
+    for (int i = 1; i < n - 1; ++i) {
+        if (((DH[i] - DH[i - 1]) / (T[i] - T[i - 1])) * ((DH[i + 1] - DH[i]) / (T[i + 1] - T[i])) < 0.0)
+            return fail(ctx, CHAPSIM_ERR_BADARG, "the relation (rho * h) = FUNCTION (T) is not monotone");
+        if (((DH[i] - DH[i - 1]) / (H[i] - H[i - 1])) * ((DH[i + 1] - DH[i]) / (H[i + 1] - H[i])) < 0.0)
+            return fail(ctx, CHAPSIM_ERR_BADARG, "the relation (rho * h) = FUNCTION (h) is not monotone");
+    }
+    // the binary search assumes ascending abscissae
+    for (int i = 1; i < n; ++i)
+        if (!(H[i] > H[i - 1]) || !(DH[i] > DH[i - 1]))
+            return fail(ctx, CHAPSIM_ERR_BADARG, "LIST_H and LIST_DH must increase strictly along the table");
+    // pack: DH->H rows, 5 H-spline rows per table row in output order, then keys
+    std::vector<SplineRow> rows((size_t)6 * n);
+    const double* ys[5];
+    const double* bs[5];
+    const double* cs[5];
+    const double* ds[5];
+    auto put = [&](int s, const double* y, const double* b, const double* c, const double* d) {
+        ys[s] = y; bs[s] = b; cs[s] = c; ds[s] = d;
+    };
+    put(0, t->list_t, t->ht_b, t->ht_c, t->ht_d);
+    if (t->fix_swap) {
+        put(1, t->list_d, t->hd_b, t->hd_c, t->hd_d);
+        put(2, t->list_m, t->hm_b, t->hm_c, t->hm_d);
+        put(3, t->list_k, t->hk_b, t->hk_c, t->hk_d);
+    } else {  // THERM_PROP_UPDATE_FROM_DH: D <- HM, M <- HK, K <- HD
+        put(1, t->list_m, t->hm_b, t->hm_c, t->hm_d);
+        put(2, t->list_k, t->hk_b, t->hk_c, t->hk_d);
+        put(3, t->list_d, t->hd_b, t->hd_c, t->hd_d);
+    }
+    put(4, t->list_cp, t->hcp_b, t->hcp_c, t->hcp_d);
+    for (int i = 0; i < n; ++i) {
+        rows[i] = SplineRow{t->list_h[i], t->dhh_b[i], t->dhh_c[i], t->dhh_d[i]};
+        for (int s = 0; s < 5; ++s) rows[(size_t)n + 5 * (size_t)i + s] = SplineRow{ys[s][i], bs[s][i], cs[s][i], ds[s][i]};
+    }
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->ptab);
+    ctx->ptab = nullptr;
+    const size_t rbytes = rows.size() * sizeof(SplineRow);
+    const size_t kbytes = (size_t)2 * n * sizeof(double);
+    CK(cudaMalloc(&ctx->ptab, rbytes + kbytes));
+    if (!ctx->pstat) CK(cudaMalloc(&ctx->pstat, sizeof(PropStatus)));
+    char* base = static_cast<char*>(ctx->ptab);
+    double* keys = reinterpret_cast<double*>(base + rbytes);
+    CK(cudaMemcpy(base, rows.data(), rbytes, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(keys, DH, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(keys + n, H, (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    PropTab& tb = ctx->tab;
+    tb.n = n;
+    tb.imin_h = first_min(n, H);
+    tb.imax_h = first_max(n, H);
+    tb.imin_dh = first_min(n, DH);
+    tb.imax_dh = first_max(n, DH);
+    tb.xdh = keys;
+    tb.xh = keys + n;
+    tb.dhh = reinterpret_cast<const SplineRow*>(base);
+    tb.hs = reinterpret_cast<const SplineRow*>(base) + n;
+    const size_t sm = prop_smem(n);
+    if (sm) {
+        CK(set_smem(k_prop_points<true>, sm));
+        CK(set_smem(k_prop_fields<true>, sm));
+    }
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_therm_prop_update_points(chapsim_ctx_t* ctx, int64_t npts, const double* dh, double* h,
+                                                double* t, double* d, double* m, double* k, double* cp) {
+    if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
+    if (!ctx->ptab) return fail(ctx, CHAPSIM_ERR_BADARG, "no property table (call chapsim_prop_table_init first)");
+    if (npts <= 0 || !dh || !h || !t || !d || !m || !k || !cp) return fail(ctx, CHAPSIM_ERR_BADARG, "bad point arrays");
+    CK(cudaSetDevice(ctx->device));
+    if (npts > ctx->pbuf_pts) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->pbuf);
+        ctx->pbuf = nullptr;
+        ctx->pbuf_pts = 0;
+        CK(cudaMalloc(&ctx->pbuf, (size_t)7 * npts * sizeof(double)));
+        ctx->pbuf_pts = npts;
+    }
+    double* dd = ctx->pbuf;
+    double* o = dd + npts;
+    const size_t b = (size_t)npts * sizeof(double);
+    CK(cudaMemcpyAsync(dd, dh, b, cudaMemcpyHostToDevice, ctx->stream));
+    if (int rc = prop_reset_status(ctx)) return rc;
+    const size_t sm = prop_smem(ctx->tab.n);
+    const int grid = prop_grid(ctx, npts);
+    if (sm)
+        k_prop_points<true><<<grid, PROP_NT, sm, ctx->stream>>>(ctx->tab, npts, dd, o, o + npts, o + 2 * npts,
+                                                                o + 3 * npts, o + 4 * npts, o + 5 * npts, ctx->pstat);
+    else
+        k_prop_points<false><<<grid, PROP_NT, 0, ctx->stream>>>(ctx->tab, npts, dd, o, o + npts, o + 2 * npts,
+                                                                o + 3 * npts, o + 4 * npts, o + 5 * npts, ctx->pstat);
+    CK(cudaGetLastError());
+    ctx->launches += 1;
+    double* outs[6] = {h, t, d, m, k, cp};
+    for (int s = 0; s < 6; ++s) CK(cudaMemcpyAsync(outs[s], o + (size_t)s * npts, b, cudaMemcpyDeviceToHost, ctx->stream));
+    PropStatus ps{};
+    CK(cudaMemcpyAsync(&ps, ctx->pstat, sizeof(ps), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ps.nbad) {
+        char msg[256];
+        snprintf(msg, sizeof msg, "%u of %lld points outside the property table; first at index %llu (DH = %.17g)",
+                 ps.nbad, (long long)npts, ps.first_bad, dh[ps.first_bad]);
+        return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, msg);
+    }
+    return CHAPSIM_OK;
 }
 
 // ------------- line solver on caller-owned device memory, no allocation -------------

@@ -186,6 +186,45 @@ int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns);
 /* CFL_io (src/CFL.f90:55-107): CFLMM_io including the viscous number. */
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm);
 
+/* ---- Thermophysical properties by table search ----
+ * The nondimensional table and spline coefficients of the thermal_info module
+ * after Property_Table_Nondimensionalization
+ * (src/thermo_properties_table_searching.f90:1226-1346) and
+ * SPLINE_COEFFICIENTS_FOR_DH / _FOR_H (:972-1128): LIST_H, LIST_T, LIST_D,
+ * LIST_M, LIST_K, LIST_CP, LIST_DH and SplineCoeff_{DHH,HT,HD,HM,HK,HCp}_{B,C,D},
+ * each N_LIST doubles.  LIST_B and the HB spline are not needed: the
+ * reference discards the beta it interpolates. */
+typedef struct {
+    int32_t n_list;   /* N_LIST (>= 4) */
+    int32_t fix_swap; /* 0: the reference's assignment in THERM_PROP_UPDATE_FROM_DH
+                         (DENSITY <- HM spline, Viscousity <- HK, THERMCONDT <- HD);
+                         1: DENSITY <- HD, Viscousity <- HM, THERMCONDT <- HK */
+    const double *list_h, *list_t, *list_d, *list_m, *list_k, *list_cp, *list_dh;
+    const double *dhh_b, *dhh_c, *dhh_d;
+    const double *ht_b, *ht_c, *ht_d;
+    const double *hd_b, *hd_c, *hd_d;
+    const double *hm_b, *hm_c, *hm_d;
+    const double *hk_b, *hk_c, *hk_d;
+    const double *hcp_b, *hcp_c, *hcp_d;
+} chapsim_prop_table_t;
+
+/* Copies the table to the device (replacing any earlier one).  Applies the
+ * reference's monotonicity checks of rho*h against T and h
+ * (SPLINE_COEFFICIENTS_FOR_DH, :1016-1023) and, because the binary search
+ * needs it, requires LIST_H and LIST_DH to increase strictly:
+ * CHAPSIM_ERR_BADARG otherwise. */
+int chapsim_prop_table_init(chapsim_ctx_t* ctx, const chapsim_prop_table_t* table);
+
+/* THERM_PROP_UPDATE_FROM_DH, table arm (src/THERM_PROP_UPDATE.f90:14-67), on
+ * npts host points: dh = DH in, h, t, d, m, k, cp = ENTHALPY, TEMPERATURE,
+ * DENSITY, Viscousity, THERMCONDT, HEATCAP out.  Bitwise the reference's
+ * spline evaluation.  A point (or its h) more than 1e-8 outside the table
+ * gives CHAPSIM_ERR_TABLE_RANGE, where the reference STOPs
+ * (spline_interpolation_*, :404-417); the message names the first such
+ * point.  The other points are still written. */
+int chapsim_therm_prop_update_points(chapsim_ctx_t* ctx, int64_t npts, const double* dh, double* h, double* t,
+                                     double* d, double* m, double* k, double* cp);
+
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
  * with a CUDA event after every kernel; ms[slot] receives the summed
  * duration of kernel slot `slot` of a step.  Slot order: k_cfl,

@@ -22,8 +22,9 @@ _dp = ctypes.POINTER(ctypes.c_double)
 
 def build(force: bool = False) -> str:
     """Compile the oracle with its Makefile (gcc, OpenMP)."""
+    srcs = [os.path.join(_HERE, f) for f in ("chapsim_oracle.c", "thermo_oracle.c")]
     if force or not os.path.exists(_LIB_PATH) or (
-        os.path.getmtime(_LIB_PATH) < os.path.getmtime(os.path.join(_HERE, "chapsim_oracle.c"))
+        os.path.getmtime(_LIB_PATH) < max(os.path.getmtime(f) for f in srcs)
     ):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
@@ -71,6 +72,21 @@ def lib():
         L.orc_io_run_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.orc_io_run_steps.restype = ctypes.c_int
         L.orc_io_monitor.argtypes = [ctypes.c_void_p, _dp]
+        _ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_cubic_spline.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.orc_spline_index.argtypes = [ctypes.c_int, _dp, ctypes.c_double]
+        L.orc_spline_index.restype = ctypes.c_int
+        L.orc_spline_eval.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_double, _dp]
+        L.orc_spline_eval.restype = ctypes.c_int
+        L.orc_table_nondim.argtypes = [ctypes.c_int, _dp, ctypes.c_double, _dp, _dp]
+        L.orc_table_create.argtypes = [ctypes.c_int, _dp, ctypes.c_int]
+        L.orc_table_create.restype = ctypes.c_void_p
+        L.orc_table_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_table_coefs.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_table_extrema.argtypes = [ctypes.c_void_p, _ip]
+        L.orc_prop_update.argtypes = [ctypes.c_void_p, ctypes.c_long, _dp, _dp, ctypes.POINTER(ctypes.c_long)]
+        L.orc_prop_update.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -230,3 +246,70 @@ def tdma_noncyc(A, B, C, R):
     lib().orc_tdma_noncyc(len(R), _p(np.ascontiguousarray(A, np.float64)), _p(np.ascontiguousarray(B, np.float64)),
                           _p(np.ascontiguousarray(C, np.float64)), _p(R))
     return R
+
+
+# ---- property update by table search (thermo_oracle.c) ----
+SPLINES = ["DHH", "HT", "HD", "HM", "HK", "HCP", "HB"]
+LIST_NAMES = ["H", "T", "D", "M", "K", "CP", "B", "DH"]
+
+
+def cubic_spline(x, y):
+    """CUBIC_SPLINE(N, X, Y, B, C, D); returns (B, C, D)."""
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.ascontiguousarray(y, np.float64)
+    n = len(x)
+    b, c, d = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().orc_cubic_spline(n, _p(x), _p(y), _p(b), _p(c), _p(d))
+    return b, c, d
+
+
+def table_nondim(raw, T0):
+    """Property_Table_Nondimensionalization of raw (n, 8) rows; returns
+    (lists dict H..DH, reference state dict H0, D0, K0, M0, CP0, B0)."""
+    raw = np.ascontiguousarray(raw, np.float64)
+    n = raw.shape[0]
+    lists = np.zeros(8 * n)
+    ref = np.zeros(6)
+    lib().orc_table_nondim(n, _p(raw), float(T0), _p(lists), _p(ref))
+    return ({k: lists[i * n:(i + 1) * n].copy() for i, k in enumerate(LIST_NAMES)},
+            dict(zip(["H0", "D0", "K0", "M0", "CP0", "B0"], ref.tolist())))
+
+
+class PropTable:
+    """Table with its spline coefficients; update() is THERM_PROP_UPDATE_FROM_DH (table arm)."""
+
+    def __init__(self, lists, fix_swap=False):
+        self.n = len(lists["H"])
+        self._buf = np.ascontiguousarray(np.concatenate([lists[k] for k in LIST_NAMES]), np.float64)
+        self._h = lib().orc_table_create(self.n, _p(self._buf), int(bool(fix_swap)))
+        if not self._h:
+            raise ValueError("table needs at least 4 rows")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().orc_table_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def coefs(self, name):
+        out = np.zeros(3 * self.n)
+        lib().orc_table_coefs(self._h, SPLINES.index(name), _p(out))
+        return out.reshape(3, self.n)
+
+    def extrema(self):
+        out = (ctypes.c_int * 4)()
+        lib().orc_table_extrema(self._h, out)
+        return dict(zip(["imin_h", "imax_h", "imin_dh", "imax_dh"], list(out)))
+
+    def update(self, dh):
+        """Returns (dict of H, T, D, M, K, CP arrays shaped like dh, number of
+        out-of-range points, first out-of-range flat index or -1)."""
+        dh = np.ascontiguousarray(dh, np.float64)
+        flat = dh.reshape(-1)
+        out = np.zeros(6 * flat.size)
+        fb = ctypes.c_long(-1)
+        nbad = lib().orc_prop_update(self._h, flat.size, _p(flat), _p(out), ctypes.byref(fb))
+        res = {k: out[i * flat.size:(i + 1) * flat.size].reshape(dh.shape) for i, k in
+               enumerate(["H", "T", "D", "M", "K", "CP"])}
+        return res, nbad, fb.value
