@@ -65,8 +65,13 @@ class PropTableC(ctypes.Structure):
                 [(f"{s}_{c}", _dp) for s in ("dhh", "ht", "hd", "hm", "hk", "hcp") for c in ("b", "c", "d")])
 
 
+PREC_FP64, PREC_MIXED = 0, 1
+PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
+
+
 class Opts(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int32), ("fix_v_wall_row", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6)]
+    _fields_ = [("device", ctypes.c_int32), ("fix_v_wall_row", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 5)]
 
 
 _lib = None
@@ -166,8 +171,14 @@ class ChannelTG:
 
     IDOMAIN = 1
 
-    def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False):
+    def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False, precision: str = "fp64"):
+        """precision: "fp64" (every field and operation in FP64) or "mixed" (FP32
+        velocity/pressure storage, stencils and CN sweeps; FP64 Poisson solve,
+        projection and bulk-flux sums)."""
         self.lib = load_library()
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self.precision = precision
         self.s = setup
         L, M, N = setup.L, setup.M, setup.N
         self.L, self.M, self.N = L, M, N
@@ -192,7 +203,7 @@ class ChannelTG:
                    _ptr(k["apvr"]), _ptr(k["ak1"]), _ptr(k["ak3"]), (ctypes.c_double * 4)(*setup.TGAM),
                    (ctypes.c_double * 4)(*setup.TROH), (ctypes.c_double * 4)(*setup.TALP))
         g = Grid(L, M, N, 1, self.IDOMAIN)
-        o = Opts(device, int(bool(fix_v_wall_row)))
+        o = Opts(device, int(bool(fix_v_wall_row)), PRECISIONS[precision])
         h = ctypes.c_void_p()
         rc = self.lib.chapsim_gpu_init(ctypes.byref(g), ctypes.byref(cf), ctypes.byref(o), ctypes.byref(h))
         if rc != 0:

@@ -134,6 +134,10 @@ struct chapsim_ctx {
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
+    // mixed precision (CHAPSIM_PREC_MIXED): FP32 copies of the momentum-stage
+    // fields; the FP64 arrays above then serve as host-transfer staging
+    int prec = CHAPSIM_PREC_FP64;
+    float *Qf = nullptr, *PRf = nullptr, *H0f = nullptr, *RHSf = nullptr, *RHSLLf = nullptr, *facf = nullptr;
     double *ppt = nullptr, *ht = nullptr;  // Poisson y-solve elimination factors
     int npart_rhs = 0;
     double* part_red = nullptr;  // per-block CFL / divergence maxima
@@ -214,9 +218,9 @@ std::vector<double2> twiddles(int n) {
     return w;
 }
 
-size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(double); }
-size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(double); }
-size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(double); }
+template <typename R> size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(R); }
+template <typename R> size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(R); }
+template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * g.L) * sizeof(double2); }
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * (g.N + 1)) * sizeof(double2); }
 size_t smem_ys(const Geo& g) { return (size_t)(YS_L * g.M) * (sizeof(double2) + 2 * sizeof(double)); }
@@ -250,12 +254,29 @@ cudaError_t set_smem(F* f, size_t bytes) {
 
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
 
+// Momentum-stage arrays of the context in the real type R of its precision.
+template <typename R>
+struct StepFields {
+    R *Q, *PR, *H0, *RHS, *RHSLL, *fac;
+};
+template <typename R> StepFields<R> step_fields(chapsim_ctx* c);
+template <> StepFields<double> step_fields<double>(chapsim_ctx* c) { return {c->Q, c->PR, c->H0, c->RHS, c->RHSLL, c->fac}; }
+template <> StepFields<float> step_fields<float>(chapsim_ctx* c) { return {c->Qf, c->PRf, c->H0f, c->RHSf, c->RHSLLf, c->facf}; }
+
+template <typename R>
+int configure_momentum(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R>, smem_rhs<R>(g))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R>, smem_z<R>(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
+    CK(set_smem(k_div_fftx<R>, smem_px(g)));
+    return CHAPSIM_OK;
+}
+
 int configure_kernels(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
-    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S>, smem_rhs(g))));
-    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S>, smem_z(g))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S>, smem_y(g))));
-    CK(set_smem(k_div_fftx, smem_px(g)));
+    int rc = ctx->prec == CHAPSIM_PREC_MIXED ? configure_momentum<float>(ctx) : configure_momentum<double>(ctx);
+    if (rc) return rc;
     CK(set_smem(k_fftx_inv, smem_px(g)));
     if (use_ys_tile(g)) CK(set_smem(k_ysolve_tile, smem_ys(g)));
     CK(set_smem(k_fftz<-1>, smem_fz(g)));
@@ -269,45 +290,54 @@ inline void prof_mark(chapsim_ctx* ctx) {
 }
 
 // CFL partials, then the dt rule fused with the factor tables of all three substeps
-void launch_step_start(chapsim_ctx* ctx) {
+template <typename R>
+void launch_step_start_t(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
-    k_cfl<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
+    StepFields<R> f = step_fields<R>(ctx);
+    k_cfl<R><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, f.Q, ctx->part_red, ctx->st);
     prof_mark(ctx);
-    k_dt_factors<<<15, 32, 0, ctx->stream>>>(g, ctx->part_red, ctx->npart_red, ctx->st, ctx->fac);
+    k_dt_factors<R><<<15, 32, 0, ctx->stream>>>(g, ctx->part_red, ctx->npart_red, ctx->st, f.fac);
     prof_mark(ctx);
     ctx->launches += 2;
+}
+void launch_step_start(chapsim_ctx* ctx) {
+    if (ctx->prec == CHAPSIM_PREC_MIXED) launch_step_start_t<float>(ctx);
+    else launch_step_start_t<double>(ctx);
 }
 
 void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
     const Geo& g = ctx->g;
-    k_cfl<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
+    if (ctx->prec == CHAPSIM_PREC_MIXED) k_cfl<float><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Qf, ctx->part_red, ctx->st);
+    else k_cfl<double><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
     prof_mark(ctx);
     k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, update_dt);
     prof_mark(ctx);
     ctx->launches += 2;
 }
 
-void launch_substep(chapsim_ctx* ctx, int ns, bool factors = true) {
+template <typename R>
+void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    double* fac = ctx->fac + (long long)ns * 5 * FAC_SET;
+    StepFields<R> f = step_fields<R>(ctx);
+    R* fac = f.fac + (long long)ns * 5 * FAC_SET;
     if (factors) {
-        k_factors<<<5, 32, 0, s>>>(g, fac, ctx->st, ns);
+        k_factors<R><<<5, 32, 0, s>>>(g, fac, ctx->st, ns);
         prof_mark(ctx);
         ctx->launches += 1;
     }
     const int grx = g.M * g.N / RHS_WPB;
-    DISPATCH_S(g.L / 32, (k_rhs_xsweep<S><<<grx, RHS_WPB * 32, smem_rhs(g), s>>>(g, ctx->Q, ctx->PR, ctx->H0, ctx->RHS,
-                                                                                   ctx->part_rhs, ctx->st, fac, ns)));
+    DISPATCH_S(g.L / 32, (k_rhs_xsweep<S, R><<<grx, RHS_WPB * 32, smem_rhs<R>(g), s>>>(g, f.Q, f.PR, f.H0, f.RHS,
+                                                                                         ctx->part_rhs, ctx->st, fac, ns)));
     prof_mark(ctx);
     dim3 grz(g.L / 32, g.M, 3);
-    DISPATCH_S(g.N / 32, (k_zsweep<S><<<grz, SWEEP_NT, smem_z(g), s>>>(g, ctx->RHS, fac)));
+    DISPATCH_S(g.N / 32, (k_zsweep<S, R><<<grz, SWEEP_NT, smem_z<R>(g), s>>>(g, f.RHS, fac)));
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N);
-    DISPATCH_S(g.M / 32, (k_ysweep<S><<<gry, SWEEP_NT, smem_y(g), s>>>(g, ctx->Q, ctx->RHS, ctx->st, fac, ns)));
+    DISPATCH_S(g.M / 32, (k_ysweep<S, R><<<gry, SWEEP_NT, smem_y<R>(g), s>>>(g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    k_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->Q, ctx->RHSLL, ctx->SP, ctx->st, ns);
+    k_div_fftx<R><<<grp, PX_NT, smem_px(g), s>>>(g, f.Q, f.RHSLL, ctx->SP, ctx->st, ns);
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
@@ -320,9 +350,36 @@ void launch_substep(chapsim_ctx* ctx, int ns, bool factors = true) {
     k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
     prof_mark(ctx);
     const long long tot = (long long)g.L * g.M * g.N;
-    k_correct<<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, ctx->Q, ctx->PR, ctx->DPH, ctx->RHSLL, ctx->st, ns);
+    k_correct<R><<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
     prof_mark(ctx);
     ctx->launches += 9;
+}
+void launch_substep(chapsim_ctx* ctx, int ns, bool factors = true) {
+    if (ctx->prec == CHAPSIM_PREC_MIXED) launch_substep_t<float>(ctx, ns, factors);
+    else launch_substep_t<double>(ctx, ns, factors);
+}
+
+// FP64 staging arrays <-> FP32 fields of the mixed-precision step
+int mixed_from_staging(chapsim_ctx* ctx, bool with_h0) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    const int nb = 4 * ctx->nsm;
+    k_convert<float, double><<<nb, DG_NT, 0, s>>>(ctx->Qf, ctx->Q, 3 * g.FS);
+    k_convert<float, double><<<nb, DG_NT, 0, s>>>(ctx->PRf, ctx->PR, g.FS);
+    if (with_h0) k_convert<float, double><<<nb, DG_NT, 0, s>>>(ctx->H0f, ctx->H0, 3 * g.FI);
+    ctx->launches += with_h0 ? 3 : 2;
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+int mixed_to_staging(chapsim_ctx* ctx, bool q, bool pr, bool h0) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    const int nb = 4 * ctx->nsm;
+    if (q) { k_convert<double, float><<<nb, DG_NT, 0, s>>>(ctx->Q, ctx->Qf, 3 * g.FS); ctx->launches += 1; }
+    if (pr) { k_convert<double, float><<<nb, DG_NT, 0, s>>>(ctx->PR, ctx->PRf, g.FS); ctx->launches += 1; }
+    if (h0) { k_convert<double, float><<<nb, DG_NT, 0, s>>>(ctx->H0, ctx->H0f, 3 * g.FI); ctx->launches += 1; }
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
 }
 
 // ----------------------------- IO path -----------------------------------
@@ -429,9 +486,15 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         return fail(nullptr, CHAPSIM_ERR_BADARG, "missing coefficient array");
     if (cf->iflowdriven < 0 || cf->iflowdriven > 2) return fail(nullptr, CHAPSIM_ERR_BADARG, "iFlowDriven must be 0, 1 or 2");
 
+    const int prec = opts ? opts->precision : CHAPSIM_PREC_FP64;
+    if (prec != CHAPSIM_PREC_FP64 && prec != CHAPSIM_PREC_MIXED)
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "precision must be CHAPSIM_PREC_FP64 or CHAPSIM_PREC_MIXED");
+    if (prec == CHAPSIM_PREC_MIXED && grid->idomain != 1)
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "the mixed-precision step is available for the periodic TG domain only");
     ctx = new chapsim_ctx();
     ctx->device = opts ? opts->device : 0;
     ctx->domain = grid->idomain;
+    ctx->prec = prec;
     int rc;
 #define INIT_CK(call)                                  \
     do {                                               \
@@ -540,6 +603,20 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         INIT_CK(cudaMemset(f.DIVU, 0, (size_t)g.FS * sizeof(double)));
         ctx->io_grid = ctx->npart_rhs < 8 * nsm ? ctx->npart_rhs : 8 * nsm;
     }
+    if (ctx->prec == CHAPSIM_PREC_MIXED) {
+        INIT_CK(cudaMalloc(&ctx->Qf, (size_t)(3 * g.FS) * sizeof(float)));
+        INIT_CK(cudaMalloc(&ctx->PRf, (size_t)g.FS * sizeof(float)));
+        INIT_CK(cudaMalloc(&ctx->H0f, (size_t)(3 * g.FI) * sizeof(float)));
+        INIT_CK(cudaMalloc(&ctx->RHSf, (size_t)(3 * g.FI) * sizeof(float)));
+        INIT_CK(cudaMalloc(&ctx->RHSLLf, (size_t)g.FI * sizeof(float)));
+        INIT_CK(cudaMalloc(&ctx->facf, (size_t)4 * 5 * FAC_SET * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->Qf, 0, (size_t)(3 * g.FS) * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->PRf, 0, (size_t)g.FS * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->H0f, 0, (size_t)(3 * g.FI) * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->RHSf, 0, (size_t)(3 * g.FI) * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->RHSLLf, 0, (size_t)g.FI * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->facf, 0, (size_t)4 * 5 * FAC_SET * sizeof(float)));
+    }
     INIT_CK(cudaMalloc(&ctx->st, sizeof(DevState)));
     INIT_CK(cudaMallocHost(&ctx->st_host, sizeof(DevState)));
     INIT_CK(cudaMemset(ctx->Q, 0, (size_t)(3 * g.FS) * sizeof(double)));
@@ -579,6 +656,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
+    cudaFree(ctx->Qf); cudaFree(ctx->PRf); cudaFree(ctx->H0f); cudaFree(ctx->RHSf); cudaFree(ctx->RHSLLf); cudaFree(ctx->facf);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -598,9 +676,13 @@ int chapsim_upload_fields(chapsim_ctx_t* ctx, const double* q, const double* pr,
         CK(cudaMemcpyAsync(ctx->H0, convh0, (size_t)(3 * g.FI) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     else
         CK(cudaMemsetAsync(ctx->H0, 0, (size_t)(3 * g.FI) * sizeof(double), ctx->stream));
-    k_bc_fields<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->PR);
+    k_bc_fields<double><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->PR);
     ctx->launches += 1;
     CK(cudaGetLastError());
+    if (ctx->prec == CHAPSIM_PREC_MIXED) {
+        int rc = mixed_from_staging(ctx, true);
+        if (rc) return rc;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     return CHAPSIM_OK;
 }
@@ -609,6 +691,10 @@ int chapsim_download_fields(chapsim_ctx_t* ctx, double* q, double* pr, double* c
     if (!ctx) return CHAPSIM_ERR_BADARG;
     CK(cudaSetDevice(ctx->device));
     const Geo& g = ctx->g;
+    if (ctx->prec == CHAPSIM_PREC_MIXED) {
+        int rc = mixed_to_staging(ctx, q != nullptr, pr != nullptr, convh0 != nullptr);
+        if (rc) return rc;
+    }
     if (q) CK(cudaMemcpyAsync(q, ctx->Q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (pr) CK(cudaMemcpyAsync(pr, ctx->PR, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (convh0)
@@ -701,7 +787,8 @@ int chapsim_advance_tg(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dt
 int chapsim_divgck_tg(chapsim_ctx_t* ctx, double* maxdiv) {
     if (!ctx || !maxdiv) return CHAPSIM_ERR_BADARG;
     CK(cudaSetDevice(ctx->device));
-    k_divgck<<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(ctx->g, ctx->Q, ctx->part_red);
+    if (ctx->prec == CHAPSIM_PREC_MIXED) k_divgck<float><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(ctx->g, ctx->Qf, ctx->part_red);
+    else k_divgck<double><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(ctx->g, ctx->Q, ctx->part_red);
     k_maxdiv_final<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st);
     ctx->launches += 2;
     CK(cudaGetLastError());

@@ -11,7 +11,10 @@
 
 #define DG_NT 256
 
-__global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const double* __restrict__ Q, double* __restrict__ partial,
+// The field kernels take the stored type R of Q and PR (double, or float in
+// the mixed-precision step) and evaluate in FP64.
+template <typename R>
+__global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, double* __restrict__ partial,
                                                DevState* __restrict__ st) {
     __shared__ double sred[32];
     const int L = g.L, M = g.M, N = g.N;
@@ -24,9 +27,9 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const double* __restrict__
         const int j = 1 + (int)(r % M);
         const int k = (int)(r / M);
         const long long c = pidx(g, i, j, k);
-        const double q = (fabs((Q[c] + Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
-                          fabs((Q[c + g.FS] + Q[c + g.FS + g.L]) * g.dyfi[j] * 1.0) +
-                          fabs((Q[c + 2 * g.FS] + Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
+        const double q = (fabs(((double)Q[c] + (double)Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
+                          fabs(((double)Q[c + g.FS] + (double)Q[c + g.FS + g.L]) * g.dyfi[j] * 1.0) +
+                          fabs(((double)Q[c + 2 * g.FS] + (double)Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
         if (!(q == q)) bad = true;
         mx = fmax(mx, q);
     }
@@ -54,7 +57,8 @@ __global__ void __launch_bounds__(DG_NT) k_dt(const double* __restrict__ partial
     }
 }
 
-__global__ void __launch_bounds__(DG_NT) k_divgck(Geo g, const double* __restrict__ Q, double* __restrict__ partial) {
+template <typename R>
+__global__ void __launch_bounds__(DG_NT) k_divgck(Geo g, const R* __restrict__ Q, double* __restrict__ partial) {
     __shared__ double sred[32];
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
@@ -65,8 +69,9 @@ __global__ void __launch_bounds__(DG_NT) k_divgck(Geo g, const double* __restric
         const int j = 1 + (int)(r % M);
         const int k = (int)(r / M);
         const long long c = pidx(g, i, j, k);
-        const double d = (Q[pidx(g, wrapp(i, L), j, k)] - Q[c]) * g.dxi + (Q[c + g.FS + g.L] - Q[c + g.FS]) * g.dyfi[j] * 1.0 +
-                         (Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - Q[c + 2 * g.FS]) * g.dzi * 1.0;
+        const double d = ((double)Q[pidx(g, wrapp(i, L), j, k)] - (double)Q[c]) * g.dxi +
+                         ((double)Q[c + g.FS + g.L] - (double)Q[c + g.FS]) * g.dyfi[j] * 1.0 +
+                         ((double)Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - (double)Q[c + 2 * g.FS]) * g.dzi * 1.0;
         mx = fmax(fabs(d), mx);
     }
     double r = block_max<DG_NT>(mx, sred);
@@ -83,14 +88,15 @@ __global__ void k_maxdiv_final(const double* __restrict__ partial, int np, DevSt
 
 // Wall ghost planes after an upload: u = w = 0 at j = 0, M+1; v = 0 at
 // j = 0, 1, M+1; PR zero-gradient.
-__global__ void __launch_bounds__(DG_NT) k_bc_fields(Geo g, double* __restrict__ Q, double* __restrict__ PR) {
+template <typename R>
+__global__ void __launch_bounds__(DG_NT) k_bc_fields(Geo g, R* __restrict__ Q, R* __restrict__ PR) {
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * N;
     for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
         const int i = (int)(t % L), k = (int)(t / L);
         const long long b0 = pidx(g, i, 0, k), b1 = pidx(g, i, 1, k), bm = pidx(g, i, M, k), bt = pidx(g, i, M + 1, k);
-        Q[bt] = 0.0; Q[bt + 2 * g.FS] = 0.0; Q[bt + g.FS] = 0.0;
-        Q[b0] = 0.0; Q[b0 + 2 * g.FS] = 0.0; Q[b1 + g.FS] = 0.0; Q[b0 + g.FS] = 0.0;
+        Q[bt] = R(0); Q[bt + 2 * g.FS] = R(0); Q[bt + g.FS] = R(0);
+        Q[b0] = R(0); Q[b0 + 2 * g.FS] = R(0); Q[b1 + g.FS] = R(0); Q[b0 + g.FS] = R(0);
         PR[bt] = PR[bm];
         PR[b0] = PR[b1];
     }
@@ -100,8 +106,9 @@ __global__ void __launch_bounds__(DG_NT) k_bc_fields(Geo g, double* __restrict__
 // (order-independent maximum), applies the dt rule of BCAST_COMM_STEP, and
 // computes one factor table of one substep (block b: substep 1 + b / 5,
 // set b % 5).  Block 0 publishes CFLMM and DT.
+template <typename T>
 __global__ void __launch_bounds__(32) k_dt_factors(Geo g, const double* __restrict__ partial, int np,
-                                                   DevState* __restrict__ st, double* __restrict__ fac) {
+                                                   DevState* __restrict__ st, T* __restrict__ fac) {
     const int lane = threadIdx.x;
     double mx = 0.0;
     for (int t = lane; t < np; t += 32) mx = fmax(mx, partial[t]);
@@ -118,4 +125,12 @@ __global__ void __launch_bounds__(32) k_dt_factors(Geo g, const double* __restri
         if ((dt / st->dt0) < 0.01) atomicOr(&st->err, CHS_EBIT_DT_COLLAPSE);
         if (!(dt == dt)) atomicOr(&st->err, CHS_EBIT_NAN);
     }
+}
+
+// Element-wise conversion between the FP64 host-facing copies and the FP32
+// fields of the mixed-precision step.
+template <typename TO, typename FROM>
+__global__ void __launch_bounds__(DG_NT) k_convert(TO* __restrict__ dst, const FROM* __restrict__ src, long long n) {
+    for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < n; t += (long long)gridDim.x * DG_NT)
+        dst[t] = (TO)src[t];
 }

@@ -29,7 +29,10 @@
 #define CR_NT 256
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const double* __restrict__ Q, double* __restrict__ RHSLL,
+// R is the stored type of Q, PR and RHSLLPHI (double, or float in the mixed-
+// precision step); divergence, transforms and correction are FP64 throughout.
+template <typename R>
+__global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                     double2* __restrict__ SP, const DevState* __restrict__ st, int ns) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, N = g.N, LH = g.LH;
@@ -39,9 +42,9 @@ __global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const double* __restr
     const int np = (nj + 1) >> 1;
     const int kp = wrapp(k, N);
     const double coe0 = 1.0 / (st->dt * g.talp[ns]);
-    const double* U = Q;
-    const double* V = Q + g.FS;
-    const double* W = Q + 2 * g.FS;
+    const R* U = Q;
+    const R* V = Q + g.FS;
+    const R* W = Q + 2 * g.FS;
     const double coe1 = g.dxi / 1.0;
 #pragma unroll 4
     for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
@@ -57,7 +60,7 @@ __global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const double* __restr
             const double coe2 = g.dyfi[j] / 1.0;
             const double dv = (up - u) * coe1 + (vp - v) * coe2 + (wp - w) * g.dzi;
             val = dv * coe0;
-            RHSLL[iidx(g, i, j, k)] = val;
+            RHSLL[iidx(g, i, j, k)] = (R)val;
         }
         double2* line = smc + pair * L;
         const int pos = g.permx[i];
@@ -273,8 +276,9 @@ __global__ void __launch_bounds__(PX_NT) k_fftx_inv(Geo g, const double2* __rest
 
 // ---------------------------------------------------------------------------
 // VELOUPDT_tg + PRCALC_tg + BC_WALL_PR_tg (Q walls are never written)
-__global__ void __launch_bounds__(CR_NT) k_correct(Geo g, double* __restrict__ Q, double* __restrict__ PR,
-                                                   const double* __restrict__ DPH, const double* __restrict__ RHSLL,
+template <typename R>
+__global__ void __launch_bounds__(CR_NT) k_correct(Geo g, R* __restrict__ Q, R* __restrict__ PR,
+                                                   const double* __restrict__ DPH, const R* __restrict__ RHSLL,
                                                    const DevState* __restrict__ st, int ns) {
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
@@ -293,11 +297,11 @@ __global__ void __launch_bounds__(CR_NT) k_correct(Geo g, double* __restrict__ Q
     const double phjm = j >= 2 ? DPH[pidx(g, i, j - 1, k)] : 0.0;
     const double u = Q[c], v = Q[c + g.FS], w = Q[c + 2 * g.FS];
     const double pr = PR[c], ll = RHSLL[iidx(g, i, j, k)];
-    Q[c] = u - (ph - phim) * (dt * ta * g.dxi);
-    Q[c + 2 * g.FS] = w - (ph - phkm) * (dt * ta * g.dzi);
-    if (j >= 2) Q[c + g.FS] = v - (ph - phjm) * (dt * ta * g.dyci[j] / 1.0);
+    Q[c] = (R)(u - (ph - phim) * (dt * ta * g.dxi));
+    Q[c + 2 * g.FS] = (R)(w - (ph - phkm) * (dt * ta * g.dzi));
+    if (j >= 2) Q[c + g.FS] = (R)(v - (ph - phjm) * (dt * ta * g.dyci[j] / 1.0));
     const double be = 0.5 * ta * dt * g.cvisc * 1.0 / 1.0;
-    const double pn = pr + ph - be * ll;
+    const R pn = (R)(pr + ph - be * ll);
     PR[c] = pn;
     if (j == 1) PR[pidx(g, i, 0, k)] = pn;
     if (j == M) PR[pidx(g, i, M + 1, k)] = pn;

@@ -189,8 +189,10 @@ __device__ __forceinline__ void warp_tdma_smem(double* base, const Coef& cf, int
 // [item][lane] so that a warp reads it with coalesced accesses.
 #define TF_NF(S) (5 * (S) + 20)
 
-template <int S, bool CYCLIC, class Coef>
-__device__ void warp_tdma_factor(const Coef& cf, int lane, double* __restrict__ fac) {
+// The factors are always computed in FP64; T is the type they are stored in
+// (float for the FP32 sweeps of the mixed-precision step).
+template <int S, bool CYCLIC, class Coef, typename T = double>
+__device__ void warp_tdma_factor(const Coef& cf, int lane, T* __restrict__ fac) {
     const int r0 = lane * S;
     // item layout: [0,S) r, [S,2S) a, [2S,3S) cq(fwd), [3S,4S) ap(final), [4S,5S) cq(final),
     //   5S+0 c0, +1 aL, +2 A0, +3 C0, +4 iB0, +5 ra, +6 rb, +7..+11 k1[5], +12..+16 k2[5], +17 f1, +18 f2, +19 unused
@@ -284,37 +286,37 @@ __device__ void warp_tdma_factor(const Coef& cf, int lane, double* __restrict__ 
     } else {
         f1 = 1.0 / be;
     }
-    double* f = fac + lane;
+    T* f = fac + lane;
 #pragma unroll
     for (int k = 0; k < S; ++k) {
         if constexpr (S > 2) {
-            f[(0 * S + k) * 32] = rr[k];
-            f[(1 * S + k) * 32] = aa[k];
-            f[(2 * S + k) * 32] = cqf[k];
-            f[(3 * S + k) * 32] = ap[k];
-            f[(4 * S + k) * 32] = cq[k];
+            f[(0 * S + k) * 32] = (T)rr[k];
+            f[(1 * S + k) * 32] = (T)aa[k];
+            f[(2 * S + k) * 32] = (T)cqf[k];
+            f[(3 * S + k) * 32] = (T)ap[k];
+            f[(4 * S + k) * 32] = (T)cq[k];
         } else {
-            f[(0 * S + k) * 32] = 0.0;
-            f[(1 * S + k) * 32] = 0.0;
-            f[(2 * S + k) * 32] = 0.0;
-            f[(3 * S + k) * 32] = 0.0;
-            f[(4 * S + k) * 32] = 0.0;
+            f[(0 * S + k) * 32] = T(0);
+            f[(1 * S + k) * 32] = T(0);
+            f[(2 * S + k) * 32] = T(0);
+            f[(3 * S + k) * 32] = T(0);
+            f[(4 * S + k) * 32] = T(0);
         }
     }
     const int b = 5 * S;
-    f[(b + 0) * 32] = c0; f[(b + 1) * 32] = aL; f[(b + 2) * 32] = A0; f[(b + 3) * 32] = C0;
-    f[(b + 4) * 32] = iB0; f[(b + 5) * 32] = ra; f[(b + 6) * 32] = rb;
+    f[(b + 0) * 32] = (T)c0; f[(b + 1) * 32] = (T)aL; f[(b + 2) * 32] = (T)A0; f[(b + 3) * 32] = (T)C0;
+    f[(b + 4) * 32] = (T)iB0; f[(b + 5) * 32] = (T)ra; f[(b + 6) * 32] = (T)rb;
 #pragma unroll
-    for (int st = 0; st < 5; ++st) { f[(b + 7 + st) * 32] = k1s[st]; f[(b + 12 + st) * 32] = k2s[st]; }
-    f[(b + 17) * 32] = f1; f[(b + 18) * 32] = f2;
+    for (int st = 0; st < 5; ++st) { f[(b + 7 + st) * 32] = (T)k1s[st]; f[(b + 12 + st) * 32] = (T)k2s[st]; }
+    f[(b + 17) * 32] = (T)f1; f[(b + 18) * 32] = (T)f2;
 }
 
 // Right-hand-side part of the solve; d[k] = rhs of row lane*S+k in, solution out.
-template <int S, bool CYCLIC>
-__device__ __forceinline__ void warp_tdma_apply(double (&d)[S], const double* __restrict__ fac, int lane) {
-    const double* f = fac + lane;
+template <int S, bool CYCLIC, typename R>
+__device__ __forceinline__ void warp_tdma_apply(R (&d)[S], const R* __restrict__ fac, int lane) {
+    const R* f = fac + lane;
     const int b = 5 * S;
-    double D0, D1;
+    R D0, D1;
     if constexpr (S >= 3) {
         d[1] *= f[(0 * S + 1) * 32];
 #pragma unroll
@@ -328,13 +330,13 @@ __device__ __forceinline__ void warp_tdma_apply(double (&d)[S], const double* __
         D1 = d[1];
     } else {
         D0 = d[0];
-        D1 = 0.0;
+        D1 = R(0);
     }
-    double de;
+    R de;
     if constexpr (S == 1) {
         de = D0;
     } else {
-        const double D0n = __shfl_sync(0xffffffffu, D0, (lane + 1) & 31);
+        const R D0n = __shfl_sync(0xffffffffu, D0, (lane + 1) & 31);
         de = D1 - f[(b + 5) * 32] * D0 - f[(b + 6) * 32] * D0n;
     }
     const int nsteps = CYCLIC ? 4 : 5;
@@ -342,13 +344,13 @@ __device__ __forceinline__ void warp_tdma_apply(double (&d)[S], const double* __
     for (int st = 0; st < 5; ++st) {
         if (st >= nsteps) break;
         const int s = 1 << st;
-        const double lo = __shfl_sync(0xffffffffu, de, (lane - s) & 31);
-        const double hi = __shfl_sync(0xffffffffu, de, (lane + s) & 31);
+        const R lo = __shfl_sync(0xffffffffu, de, (lane - s) & 31);
+        const R hi = __shfl_sync(0xffffffffu, de, (lane + s) & 31);
         de = de - f[(b + 7 + st) * 32] * lo - f[(b + 12 + st) * 32] * hi;
     }
-    double u;
+    R u;
     if constexpr (CYCLIC) {
-        const double pd = __shfl_sync(0xffffffffu, de, lane ^ 16);
+        const R pd = __shfl_sync(0xffffffffu, de, lane ^ 16);
         u = de * f[(b + 17) * 32] + pd * f[(b + 18) * 32];
     } else {
         u = de * f[(b + 17) * 32];
@@ -356,8 +358,8 @@ __device__ __forceinline__ void warp_tdma_apply(double (&d)[S], const double* __
     if constexpr (S == 1) {
         d[0] = u;
     } else {
-        const double up = __shfl_sync(0xffffffffu, u, (lane - 1) & 31);
-        const double y0 = (D0 - f[(b + 2) * 32] * up - f[(b + 3) * 32] * u) * f[(b + 4) * 32];
+        const R up = __shfl_sync(0xffffffffu, u, (lane - 1) & 31);
+        const R y0 = (D0 - f[(b + 2) * 32] * up - f[(b + 3) * 32] * u) * f[(b + 4) * 32];
         d[0] = y0;
         d[S - 1] = u;
         if constexpr (S > 2) {
@@ -367,9 +369,9 @@ __device__ __forceinline__ void warp_tdma_apply(double (&d)[S], const double* __
     }
 }
 
-template <int S, bool CYCLIC>
-__device__ __forceinline__ void warp_tdma_apply_smem(double* base, const double* __restrict__ fac, int lane) {
-    double d[S];
+template <int S, bool CYCLIC, typename R>
+__device__ __forceinline__ void warp_tdma_apply_smem(R* base, const R* __restrict__ fac, int lane) {
+    R d[S];
 #pragma unroll
     for (int k = 0; k < S; ++k) d[k] = base[lane * (S + 1) + k];
     warp_tdma_apply<S, CYCLIC>(d, fac, lane);

@@ -4,7 +4,7 @@
  *
  * The Fortran host (CHAPSim's driver, readdata.ini parser and file I/O)
  * stays unchanged; its subroutine bodies call these entry points through an
- * ISO_C_BINDING shim.  All arguments are plain C types:
+ * ISO_C_BINDING shim module.  All arguments are plain C types:
  * array arguments are host pointers to Fortran-ordered FP64 arrays with the
  * reference's shapes, copied with one contiguous transfer each.
  *
@@ -25,7 +25,7 @@ extern "C" {
 #define CHAPSIM_ERR_CUDA (-1)        /* a CUDA call failed */
 #define CHAPSIM_ERR_NAN (-2)         /* non-finite velocity or dt */
 #define CHAPSIM_ERR_DT_COLLAPSE (-3) /* DT/DT0 < 0.01: src/SOLVE.f90:199-207 dumps and STOPs */
-#define CHAPSIM_ERR_TABLE_RANGE (-4) /* reserved: property table out of range */
+#define CHAPSIM_ERR_TABLE_RANGE (-4) /* property table out of range: spline_interpolation_* STOP */
 #define CHAPSIM_ERR_TIMEOUT (-5)     /* reserved: bounded device wait expired */
 #define CHAPSIM_ERR_BADARG (-6)      /* invalid argument or unsupported grid */
 #define CHAPSIM_ERR_NOMEM (-7)       /* device allocation failed */
@@ -69,10 +69,17 @@ typedef struct {
     double tgam[4], troh[4], talp[4]; /* CONS_RKCOEF (src/CONS_RKCOEF.f90:25-51) */
 } chapsim_coefs_t;
 
+#define CHAPSIM_PREC_FP64 0  /* every field and operation in FP64 (the reference's precision) */
+#define CHAPSIM_PREC_MIXED 1 /* FP32 velocity, pressure, CONVH0 and RHS storage; FP32 stencils and
+                                Crank-Nicolson sweeps; FP64 Poisson spectrum, y-solve (with the
+                                kx = kz = 0 mode), DPH, divergence, projection and bulk-flux sums */
+
 typedef struct {
-    int32_t device;          /* CUDA device ordinal                            */
-    int32_t fix_v_wall_row;  /* 0: reproduce the reference (default), see DESIGN */
-    int32_t reserved[6];
+    int32_t device;          /* CUDA device ordinal                                            */
+    int32_t fix_v_wall_row;  /* 0: keep the reference's v-sweep row-1 input (the u increment of
+                                the same substep, MOMFA3_Y_tg); 1: zero it                      */
+    int32_t precision;       /* CHAPSIM_PREC_FP64 (default) or CHAPSIM_PREC_MIXED (TG domain)  */
+    int32_t reserved[5];
 } chapsim_opts_t;
 
 /* Allocates the device fields and uploads coefficients.  Hooks in after
