@@ -45,6 +45,25 @@ L2_BYTES = 126 * 1024 * 1024
 # algorithmic FP64 words per grid point moved by one launch of each kernel
 # (reads + writes of the arrays the reference's algorithm needs; the
 # spectral arrays hold (L/2+1)/L complex values per point)
+def kernel_bytes(L, precision="fp64"):
+    """Algorithmic bytes per grid point per launch.  FP64: 8 bytes per word of
+    kernel_words.  Mixed: Q, PR, CONVH0, RHS and RHSLLPHI are 4-byte words;
+    the spectrum and DPH stay FP64."""
+    if precision == "fp64":
+        return {k: 8.0 * v for k, v in kernel_words(L).items()}
+    spec = 2.0 * (L // 2 + 1) / L
+    return {
+        "k_cfl": 3 * 4.0, "k_dt_factors": 0.0,
+        "k_rhs_xsweep": 13 * 4.0,
+        "k_zsweep": 6 * 4.0,
+        "k_ysweep": 9 * 4.0,
+        "k_div_fftx": 4 * 4.0 + 8.0 * spec,
+        "k_fftz_fwd": 16.0 * spec, "k_fftz_inv": 16.0 * spec, "k_ysolve": 16.0 * spec,
+        "k_fftx_inv": 8.0 * spec + 8.0,
+        "k_correct": 8.0 + 6 * 4.0 + 2 * 4.0 + 4.0,   # DPH; Q x3 in/out; PR in/out; RHSLLPHI
+    }
+
+
 def kernel_words(L):
     spec = 2.0 * (L // 2 + 1) / L  # complex spectrum, words per point
     return {
@@ -204,7 +223,7 @@ def run_b200(args):
     DTMIN = 1e-6
     s = channel_setup(L, M, N, HX, HZ, STR2, REN)
     Q0, PR0 = initial_field(s, 1973 + rank, 0.1)
-    ch = gpu.ChannelTG(s, device=local)
+    ch = gpu.ChannelTG(s, device=local, precision=args.precision)
     ch.upload(Q0, PR0)
     ch.set_dt(DT0)
     ch.SOLVERRK3_MOM_tg(0)
@@ -264,23 +283,23 @@ def run_b200(args):
     prof_steps = max(1, min(20, args.steps))
     kms = ch.profile_steps(prof_steps, DT0, DTMIN, CFLGV)
     launches_per_step = {k: (1 if k in ("k_cfl", "k_dt_factors") else 3) for k in kms}
-    words = kernel_words(L)
+    kb = kernel_bytes(L, args.precision)
     peak, peak_kind = load_peaks()
     per_launch = {k: kms[k] / (prof_steps * launches_per_step[k]) for k in kms}
     total_ms = sum(kms.values())
     dom = max(kms, key=lambda k: kms[k])
-    dom_bytes = words[dom] * 8.0 * pts
+    dom_bytes = kb[dom] * pts
     achieved = dom_bytes / (per_launch[dom] / 1000.0) / 1e9
-    traffic = load_traffic(wl).get(dom)
-    step_bytes = sum(words[k] * 8.0 * pts * launches_per_step[k] for k in words)
+    traffic = load_traffic(wl if args.precision == "fp64" else wl + "_mixed").get(dom)
+    step_bytes = sum(kb[k] * pts * launches_per_step[k] for k in kb)
     step_ms = 1000.0 * 1.0 / (value / ws / pts)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": wl, "grid": [L, M, N], "domain": "4pi x 2 x 4pi/3" if L == 128 else None,
-                   "REN": REN, "STR2": STR2, "CFLGV": CFLGV, "precision": "fp64",
+                   "REN": REN, "STR2": STR2, "CFLGV": CFLGV, "precision": args.precision,
                    "parallelism": "replicas" if ws > 1 else "single", "cuda_graph": True,
                    "l2": "no flush: per-step working set %.0f MB > 126 MB L2" % (
                        (12 * 8 * (M + 2) * L * N + 4 * 8 * L * M * N + 24 * (L // 2 + 1) * M * N) / 1e6),
@@ -321,6 +340,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
