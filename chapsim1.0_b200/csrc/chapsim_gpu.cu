@@ -130,7 +130,7 @@ struct chapsim_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     Geo g{};
-    double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr, *HS = nullptr;
+    double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr;
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
@@ -138,7 +138,6 @@ struct chapsim_ctx {
     // fields; the FP64 arrays above then serve as host-transfer staging
     int prec = CHAPSIM_PREC_FP64;
     float *Qf = nullptr, *PRf = nullptr, *H0f = nullptr, *RHSf = nullptr, *RHSLLf = nullptr, *facf = nullptr;
-    double *ppt = nullptr, *ht = nullptr;  // Poisson y-solve elimination factors
     int npart_rhs = 0;
     double* part_red = nullptr;  // per-block CFL / divergence maxima
     int npart_red = 0;
@@ -223,17 +222,12 @@ template <typename R> size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 
 template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * g.L) * sizeof(double2); }
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * (g.N + 1)) * sizeof(double2); }
-size_t smem_ys(const Geo& g) { return (size_t)(YS_L * g.M) * (sizeof(double2) + 2 * sizeof(double)); }
-bool use_ys_tile(const Geo& g) { return true; }
+size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(double2) + (size_t)g.M * sizeof(double); }
 
-void launch_ysolve(chapsim_ctx* ctx) {
-    const Geo& g = ctx->g;
-    const long long nl = (long long)g.LH * g.N;
-    if (use_ys_tile(g))
-        k_ysolve_tile<<<(int)((nl + YS_L - 1) / YS_L), YS2_NT, smem_ys(g), ctx->stream>>>(g, ctx->SP, ctx->ppt, ctx->ht);
-    else
-        k_ysolve<<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, 0, ctx->stream>>>(g, ctx->SP, ctx->HS);
-}
+// forward declaration: DISPATCH_S is defined below
+void launch_ysolve_warp(chapsim_ctx* ctx);
+
+void launch_ysolve(chapsim_ctx* ctx) { launch_ysolve_warp(ctx); }
 
 template <typename F>
 cudaError_t set_smem(F* f, size_t bytes) {
@@ -253,6 +247,13 @@ cudaError_t set_smem(F* f, size_t bytes) {
     }
 
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
+
+void launch_ysolve_warp(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    const long long nl = (long long)g.LH * g.N;
+    const int nb = (int)((nl + YW_L - 1) / YW_L);
+    DISPATCH_S(g.M / 32, (k_ysolve_warp<S><<<nb, YW_NT, smem_yw(g), ctx->stream>>>(g, ctx->SP)));
+}
 
 // Momentum-stage arrays of the context in the real type R of its precision.
 template <typename R>
@@ -278,7 +279,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     int rc = ctx->prec == CHAPSIM_PREC_MIXED ? configure_momentum<float>(ctx) : configure_momentum<double>(ctx);
     if (rc) return rc;
     CK(set_smem(k_fftx_inv, smem_px(g)));
-    if (use_ys_tile(g)) CK(set_smem(k_ysolve_tile, smem_ys(g)));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S>, smem_yw(g))));
     CK(set_smem(k_fftz<-1>, smem_fz(g)));
     CK(set_smem(k_fftz<+1>, smem_fz(g)));
     return CHAPSIM_OK;
@@ -575,13 +576,10 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaMalloc(&ctx->RHS, (size_t)(3 * g.FI) * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->RHSLL, (size_t)g.FI * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->SP, (size_t)g.LH * M * N * sizeof(double2)));
-    INIT_CK(cudaMalloc(&ctx->HS, (size_t)g.LH * M * N * sizeof(double)));
     ctx->npart_rhs = M * N / RHS_WPB;
     INIT_CK(cudaMalloc(&ctx->part_rhs, (size_t)ctx->npart_rhs * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->fac, (size_t)4 * 5 * FAC_SET * sizeof(double)));
     INIT_CK(cudaMemset(ctx->fac, 0, (size_t)4 * 5 * FAC_SET * sizeof(double)));
-    INIT_CK(cudaMalloc(&ctx->ppt, (size_t)g.LH * M * N * sizeof(double)));
-    INIT_CK(cudaMalloc(&ctx->ht, (size_t)g.LH * M * N * sizeof(double)));
 
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
@@ -633,12 +631,6 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         chapsim_gpu_finalize(ctx);
         return rc;
     }
-    {
-        const long long nl = (long long)g.LH * N;
-        k_ysolve_factors<<<(int)((nl + 127) / 128), 128, 0, ctx->stream>>>(g, ctx->ppt, ctx->ht);
-        INIT_CK(cudaGetLastError());
-        INIT_CK(cudaStreamSynchronize(ctx->stream));
-    }
 
 #undef INIT_CK
     *out = ctx;
@@ -651,7 +643,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac); cudaFree(ctx->ppt); cudaFree(ctx->ht);
+    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);

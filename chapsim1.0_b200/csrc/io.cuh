@@ -10,7 +10,7 @@
 //                  bulk-forcing integrand), one thread per point and all components
 //   k_io_massflux  bulk forcing subtraction + MASSFLUX_CALC_io (G += RHS)
 //   k_io_div_fftx  DIVG_io (src/DIVG.f90:54-137) + forward x transform
-//   (shared)       k_fftz / k_ysolve_tile / k_fftz / k_fftx_inv of poisson.cuh: the
+//   (shared)       k_fftz / k_ysolve_warp / k_fftz / k_fftx_inv of poisson.cuh: the
 //                  discrete problem of FISHPACK_POIS3D_SIMPLE (same AMPH/ACPH/APPH operator
 //                  and x/z eigenvalues); its singular kx = kz = 0 mode is fixed at
 //                  phi_hat(y_1) = 0, which shifts DPH and PR by a constant only

@@ -11,21 +11,21 @@
 //                one complex FFT), times 1/L, into the spectral array
 //   k_fftz<S>    complex z transform of every (kx, j) line; forward pass
 //                multiplies by 1/N (UN3M)
-//   k_ysolve     per (kx, kz) tridiagonal solve in y with diagonal
-//                ACPH(j) - AK1(kx) - AK3(kz), the reference's Thomas
-//                recurrence, zero mode pinned as in TDMA_PHI_COEF (:225-231)
-//                and :341-344, :387-389 (phi_hat(0,y_1,0) = 0)
+//   k_ysolve_warp per (kx, kz) tridiagonal solve in y with diagonal
+//                ACPH(j) - AK1(kx) - AK3(kz); zero mode pinned as in
+//                TDMA_PHI_COEF (:225-231) and :341-344, :387-389
+//                (phi_hat(0,y_1,0) = 0)
 //   k_fftx_inv   inverse x transform -> DPH
 //   k_correct    velocity correction, pressure update, PR wall ghosts
 #pragma once
 #include "common.cuh"
 #include "fft.cuh"
+#include "tdma.cuh"
 
 #define PX_TJ 32  // x-lines per block (16 packed pairs)
 #define PX_NT 256
 #define FZ_TQ 16  // z-lines per block
 #define FZ_NT 256
-#define YS_NT 128
 #define CR_NT 256
 
 // ---------------------------------------------------------------------------
@@ -109,137 +109,93 @@ __global__ void __launch_bounds__(FZ_NT) k_fftz(Geo g, double2* __restrict__ SP)
 }
 
 // ---------------------------------------------------------------------------
-// y solve per (kx, kz): TDMAIJJ_nonCYC with AMPH, ACPH - AK1 - AK3, APPH.
-// HS is scratch of LH*M*N doubles for the forward-elimination factors.
-__global__ void __launch_bounds__(YS_NT) k_ysolve(Geo g, double2* __restrict__ SP, double* __restrict__ HS) {
-    const int M = g.M, LH = g.LH;
-    const long long nl = (long long)LH * g.N;
-    const long long t = (long long)blockIdx.x * YS_NT + threadIdx.x;
-    if (t >= nl) return;
-    const int kz = (int)(t / LH), kx = (int)(t - (long long)kz * LH);
-    const long long js = LH;  // stride between y rows
-    double2* s = SP + kx + (long long)LH * (long long)M * kz;
-    double* h = HS + kx + (long long)LH * (long long)M * kz;
-    const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-    const bool zero = (kx == 0 && kz == 0);
-    // row 1 (j = 1)
-    double b = g.acph[1] + shift;
-    double c = zero ? 0.0 : g.apph[1];
-    double2 r = s[0];
-    if (zero) r = make_double2(0.0, 0.0);
-    double hp = c / b;
-    double2 gp = make_double2(r.x / b, r.y / b);
-    h[0] = hp;
-    s[0] = gp;
-    for (int j = 2; j <= M; ++j) {
-        const double a = g.amph[j];
-        const double bj = g.acph[j] + shift;
-        const double pp = 1.0 / (bj - hp * a);
-        const double2 rj = s[(j - 1) * js];
-        gp = make_double2((rj.x - a * gp.x) * pp, (rj.y - a * gp.y) * pp);
-        if (j < M) {
-            hp = g.apph[j] * pp;
-            h[(j - 1) * js] = hp;
-        }
-        s[(j - 1) * js] = gp;
-    }
-    double2 xn = gp;
-    for (int j = M - 1; j >= 1; --j) {
-        const double hj = h[(j - 1) * js];
-        const double2 gj = s[(j - 1) * js];
-        xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
-        s[(j - 1) * js] = xn;
-    }
-}
+// y solve of YW_L consecutive lines q = kx + LH*kz per block, one warp per
+// line, by the warp Thomas/PCR hybrid with a complex right-hand side
+// (warp_tdma_c).  The coefficients (AMPH, ACPH - AK1 - AK3, APPH) are formed
+// on the fly, so no per-line factor arrays are read.  For kx != 0 or kz != 0
+// the systems are strictly diagonally dominant (AK1 + AK3 > 0 on top of the
+// weakly dominant Neumann operator), for which the reduction is stable.  The
+// singular kx = kz = 0 line keeps the reference's sequential recurrence with
+// its pinned first row (TDMA_PHI_COEF :225-231, :341-344, :387-389), run by
+// one lane.  Lines are staged in shared memory, line l at l*LS with row r at
+// seg_pos<S>(r), LS = M + 33: conflict-free both for the coalesced tile load
+// (16 lines per row) and for the per-lane segment access.
+#define YW_L 16
+#define YW_NT 256
 
-// ---------------------------------------------------------------------------
-// The coefficients of the per-(kx, kz) systems do not change during a run
-// (TDMA_PHI_COEF, src/possion3d_FFT99.f90:204-239), so the elimination
-// factors of the reference's Thomas recurrence (TDMAIJJ_nonCYC :95-121) are
-// computed once at initialisation, one thread per line, in the layout of the
-// spectral array: PPT(j) = 1/(B_j - H_{j-1} A_j) (row 1 holds B_1 itself: the
-// reference divides there) and HT(j) = C_j PPT(j).
-__global__ void k_ysolve_factors(Geo g, double* __restrict__ PPT, double* __restrict__ HT) {
-    const int M = g.M, LH = g.LH;
-    const long long nl = (long long)LH * g.N;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nl) return;
-    const int kz = (int)(t / LH), kx = (int)(t - (long long)kz * LH);
-    const long long base = kx + (long long)LH * (long long)M * kz;
-    const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-    const bool zero = (kx == 0 && kz == 0);
-    const double b = g.acph[1] + shift;
-    const double c = zero ? 0.0 : g.apph[1];
-    double hp = c / b;
-    PPT[base] = b;
-    HT[base] = hp;
-    for (int j = 2; j <= M; ++j) {
-        const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
-        PPT[base + (long long)(j - 1) * LH] = pp;
-        hp = j < M ? g.apph[j] * pp : 0.0;
-        HT[base + (long long)(j - 1) * LH] = hp;
-    }
-}
+struct PoisCoef {
+    const double *am, *ac, *ap;
+    double shift;
+    __device__ __forceinline__ double A(int r) const { return am[r + 1]; }
+    __device__ __forceinline__ double B(int r) const { return ac[r + 1] + shift; }
+    __device__ __forceinline__ double C(int r) const { return ap[r + 1]; }
+};
 
-// y solve of YS_L lines (consecutive q = kx + LH*kz) per block.  The data
-// tile and the factor columns are brought into shared memory with
-// asynchronous copies; lane l of warp 0 then runs the recurrence of line
-// l % YS_L for the real (l < YS_L) or imaginary part out of shared memory.
-#define YS_L 16
-#define YS2_NT 64
-__global__ void __launch_bounds__(YS2_NT) k_ysolve_tile(Geo g, double2* __restrict__ SP, const double* __restrict__ PPT,
-                                                        const double* __restrict__ HT) {
+template <int S>
+__global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __restrict__ SP) {
     extern __shared__ double2 smc[];
-    const int M = g.M, LH = g.LH;
+    const int M = 32 * S, LH = g.LH;
+    const int LS = M + 33;
     const long long nl = (long long)LH * g.N;
-    const long long q0 = (long long)blockIdx.x * YS_L;
-    const int nq = (int)min((long long)YS_L, nl - q0);
-    double2* tile = smc;                        // [M][YS_L] complex
-    double* pt = (double*)(smc + YS_L * M);     // [M][YS_L]
-    double* ht = pt + YS_L * M;                 // [M][YS_L]
-    for (int p = threadIdx.x; p < YS_L * M; p += YS2_NT) {
-        const int l = p % YS_L, j = p / YS_L;
+    const long long q0 = (long long)blockIdx.x * YW_L;
+    const int nq = (int)min((long long)YW_L, nl - q0);
+    for (int p = threadIdx.x; p < YW_L * M; p += YW_NT) {
+        const int l = p % YW_L, j = p / YW_L;
         if (l < nq) {
             const long long q = q0 + l;
             const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-            const long long o = kx + (long long)LH * (j + (long long)M * kz);
-            cp_async16(tile + p, SP + o);
-            cp_async8(pt + p, PPT + o);
-            cp_async8(ht + p, HT + o);
+            cp_async16(smc + l * LS + seg_pos<S>(j), SP + kx + (long long)LH * (j + (long long)M * kz));
         }
     }
     cp_async_wait_all();
     __syncthreads();
-    if (threadIdx.x < 2 * YS_L) {
-        const int l = threadIdx.x % YS_L, part = threadIdx.x / YS_L;
-        if (l < nq) {
-            double* d = (double*)tile + part;  // element (j, l) at d[2*(j*YS_L + l)]
-            const bool zero = (q0 + l == 0);
-            double r = zero ? 0.0 : d[2 * l];
-            double gp = r / pt[l];
-            d[2 * l] = gp;
-#pragma unroll 4
-            for (int j = 2; j <= M; ++j) {
-                const int e = (j - 1) * YS_L + l;
-                gp = (d[2 * e] - g.amph[j] * gp) * pt[e];
-                d[2 * e] = gp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int l = warp; l < nq; l += YW_NT / 32) {
+        const long long q = q0 + l;
+        const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+        double2* base = smc + l * LS;
+        if (q == 0) {
+            // zero mode: phi(y_1) = 0 and the reference's forward/backward recurrence
+            if (lane == 0) {
+                double* hz = reinterpret_cast<double*>(smc + YW_L * LS);  // M doubles
+                const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+                const double b = g.acph[1] + shift;
+                double hp = 0.0 / b;
+                double2 gp = make_double2(0.0 / b, 0.0 / b);
+                hz[0] = hp;
+                base[seg_pos<S>(0)] = gp;
+                for (int j = 2; j <= M; ++j) {
+                    const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
+                    const double2 rj = base[seg_pos<S>(j - 1)];
+                    gp = make_double2((rj.x - g.amph[j] * gp.x) * pp, (rj.y - g.amph[j] * gp.y) * pp);
+                    hp = j < M ? g.apph[j] * pp : 0.0;
+                    hz[j - 1] = hp;
+                    base[seg_pos<S>(j - 1)] = gp;
+                }
+                double2 xn = gp;
+                for (int j = M - 1; j >= 1; --j) {
+                    const double2 gj = base[seg_pos<S>(j - 1)];
+                    xn = make_double2(gj.x - hz[j - 1] * xn.x, gj.y - hz[j - 1] * xn.y);
+                    base[seg_pos<S>(j - 1)] = xn;
+                }
             }
-            double xn = gp;
-#pragma unroll 4
-            for (int j = M - 1; j >= 1; --j) {
-                const int e = (j - 1) * YS_L + l;
-                xn = d[2 * e] - ht[e] * xn;
-                d[2 * e] = xn;
-            }
+        } else {
+            PoisCoef cf{g.amph, g.acph, g.apph, (-g.ak1[kx] / 1.0 - g.ak3[kz])};
+            double2 d[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) d[k] = base[lane * (S + 1) + k];
+            warp_tdma_c<S>(d, cf, lane);
+#pragma unroll
+            for (int k = 0; k < S; ++k) base[lane * (S + 1) + k] = d[k];
         }
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < YS_L * M; p += YS2_NT) {
-        const int l = p % YS_L, j = p / YS_L;
+    for (int p = threadIdx.x; p < YW_L * M; p += YW_NT) {
+        const int l = p % YW_L, j = p / YW_L;
         if (l < nq) {
             const long long q = q0 + l;
             const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-            SP[kx + (long long)LH * (j + (long long)M * kz)] = tile[p];
+            SP[kx + (long long)LH * (j + (long long)M * kz)] = smc[l * LS + seg_pos<S>(j)];
         }
     }
 }

@@ -378,3 +378,111 @@ __device__ __forceinline__ void warp_tdma_apply_smem(R* base, const R* __restric
 #pragma unroll
     for (int k = 0; k < S; ++k) base[lane * (S + 1) + k] = d[k];
 }
+
+// ---------------------------------------------------------------------------
+// warp_tdma (non-cyclic) with a complex right-hand side: the real and
+// imaginary parts share the real coefficients, as in the per-wavenumber
+// y-solves of the pressure Poisson equation.
+__device__ __forceinline__ double2 c_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+__device__ __forceinline__ double2 c_sub_scaled(double2 a, double s, double2 b) {  // a - s*b
+    return make_double2(a.x - s * b.x, a.y - s * b.y);
+}
+
+template <int S, class Coef>
+__device__ __forceinline__ void warp_tdma_c(double2 (&d)[S], const Coef& cf, int lane) {
+    const int r0 = lane * S;
+    double A0, B0, C0, A1, B1, C1;
+    double2 D0, D1;
+    double ap[S > 2 ? S : 1], cq[S > 2 ? S : 1];
+    if constexpr (S == 1) {
+        A0 = cf.A(r0); B0 = cf.B(r0); C0 = cf.C(r0); D0 = d[0];
+        A1 = B1 = C1 = 0.0; D1 = make_double2(0.0, 0.0);
+    } else if constexpr (S == 2) {
+        A0 = cf.A(r0); B0 = cf.B(r0); C0 = cf.C(r0); D0 = d[0];
+        A1 = cf.A(r0 + 1); B1 = cf.B(r0 + 1); C1 = cf.C(r0 + 1); D1 = d[1];
+    } else {
+        {
+            const double r = 1.0 / cf.B(r0 + 1);
+            ap[1] = cf.A(r0 + 1) * r;
+            cq[1] = cf.C(r0 + 1) * r;
+            d[1] = c_scale(d[1], r);
+        }
+#pragma unroll
+        for (int k = 2; k <= S - 2; ++k) {
+            const double ak = cf.A(r0 + k);
+            const double r = 1.0 / (cf.B(r0 + k) - ak * cq[k - 1]);
+            d[k] = c_scale(c_sub_scaled(d[k], ak, d[k - 1]), r);
+            ap[k] = -ak * ap[k - 1] * r;
+            cq[k] = cf.C(r0 + k) * r;
+        }
+#pragma unroll
+        for (int k = S - 3; k >= 1; --k) {
+            d[k] = c_sub_scaled(d[k], cq[k], d[k + 1]);
+            ap[k] = ap[k] - cq[k] * ap[k + 1];
+            cq[k] = -cq[k] * cq[k + 1];
+        }
+        const double c0 = cf.C(r0);
+        A0 = cf.A(r0);
+        B0 = cf.B(r0) - c0 * ap[1];
+        C0 = -c0 * cq[1];
+        D0 = c_sub_scaled(d[0], c0, d[1]);
+        const double aL = cf.A(r0 + S - 1);
+        A1 = -aL * ap[S - 2];
+        B1 = cf.B(r0 + S - 1) - aL * cq[S - 2];
+        C1 = cf.C(r0 + S - 1);
+        D1 = c_sub_scaled(d[S - 1], aL, d[S - 2]);
+    }
+    if (lane == 0) A0 = 0.0;
+    if (lane == 31) { if constexpr (S == 1) C0 = 0.0; else C1 = 0.0; }
+    double al, be, ga;
+    double2 de;
+    if constexpr (S == 1) {
+        al = A0; be = B0; ga = C0; de = D0;
+    } else {
+        const int nx = (lane + 1) & 31;
+        const double A0n = __shfl_sync(0xffffffffu, A0, nx);
+        const double B0n = __shfl_sync(0xffffffffu, B0, nx);
+        const double C0n = __shfl_sync(0xffffffffu, C0, nx);
+        const double2 D0n = make_double2(__shfl_sync(0xffffffffu, D0.x, nx), __shfl_sync(0xffffffffu, D0.y, nx));
+        const double iB0 = 1.0 / B0, iB0n = 1.0 / B0n;
+        al = -A1 * A0 * iB0;
+        be = B1 - A1 * C0 * iB0 - C1 * A0n * iB0n;
+        ga = -C1 * C0n * iB0n;
+        de = c_sub_scaled(c_sub_scaled(D1, A1 * iB0, D0), C1 * iB0n, D0n);
+    }
+#pragma unroll
+    for (int s = 1; s <= 16; s <<= 1) {
+        const int lo = (lane - s) & 31, hi = (lane + s) & 31;
+        const double lal = __shfl_sync(0xffffffffu, al, lo), lbe = __shfl_sync(0xffffffffu, be, lo);
+        const double lga = __shfl_sync(0xffffffffu, ga, lo);
+        const double hal = __shfl_sync(0xffffffffu, al, hi), hbe = __shfl_sync(0xffffffffu, be, hi);
+        const double hga = __shfl_sync(0xffffffffu, ga, hi);
+        const double2 lde = make_double2(__shfl_sync(0xffffffffu, de.x, lo), __shfl_sync(0xffffffffu, de.y, lo));
+        const double2 hde = make_double2(__shfl_sync(0xffffffffu, de.x, hi), __shfl_sync(0xffffffffu, de.y, hi));
+        const bool hasl = lane - s >= 0, hash = lane + s <= 31;
+        const double k1 = hasl ? al / lbe : 0.0;
+        const double k2 = hash ? ga / hbe : 0.0;
+        const double nal = hasl ? -k1 * lal : 0.0;
+        const double nga = hash ? -k2 * hga : 0.0;
+        be = be - (hasl ? k1 * lga : 0.0) - (hash ? k2 * hal : 0.0);
+        if (hasl) de = c_sub_scaled(de, k1, lde);
+        if (hash) de = c_sub_scaled(de, k2, hde);
+        al = nal;
+        ga = nga;
+    }
+    const double2 u = c_scale(de, 1.0 / be);
+    if constexpr (S == 1) {
+        d[0] = u;
+    } else {
+        const int pv = (lane - 1) & 31;
+        const double2 up = make_double2(__shfl_sync(0xffffffffu, u.x, pv), __shfl_sync(0xffffffffu, u.y, pv));
+        const double iB0 = 1.0 / B0;
+        const double2 y0 = c_scale(c_sub_scaled(c_sub_scaled(D0, A0, up), C0, u), iB0);  // A0 == 0 on lane 0
+        d[0] = y0;
+        d[S - 1] = u;
+        if constexpr (S > 2) {
+#pragma unroll
+            for (int k = 1; k <= S - 2; ++k) d[k] = c_sub_scaled(c_sub_scaled(d[k], ap[k], y0), cq[k], u);
+        }
+    }
+}
