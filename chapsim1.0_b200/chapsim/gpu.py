@@ -32,7 +32,8 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_download_io_fields", "chapsim_rk_substep_io", "chapsim_cfl_io", "chapsim_profile_steps",
             "chapsim_get_stream",
             "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step", "chapsim_tdma_lines_noalloc",
-            "chapsim_prop_table_init", "chapsim_therm_prop_update_points"]
+            "chapsim_prop_table_init", "chapsim_therm_prop_update_points", "chapsim_thermal_init",
+            "chapsim_download_thermal_fields"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
@@ -105,6 +106,8 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_tdmaijj_noncyc.argtypes = [_dp, _dp, _dp, _dp, _dp, ctypes.c_int32, ctypes.c_int32]
     L.chapsim_prop_table_init.argtypes = [vp, ctypes.POINTER(PropTableC)]
     L.chapsim_therm_prop_update_points.argtypes = [vp, ctypes.c_int64] + [_dp] * 7
+    L.chapsim_thermal_init.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.chapsim_download_thermal_fields.argtypes = [vp] + [_dp] * 7
     L.chapsim_tdma_lines_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_int32, vp]
     L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
@@ -377,3 +380,20 @@ class ChannelIO(ChannelTG):
         v = ctypes.c_double()
         self._check(self.lib.chapsim_cfl_io(self.h, ctypes.byref(v)))
         return v.value
+
+    # -- thermal solver (SOLVERRK3_ENG_io with table-search properties) ----------
+    def thermal_init(self, table, DH, qw_bot, qw_top, cthecd, fix_swap=False):
+        """Uploads the property table (chapsim.thermo.SplineTable) and starts the
+        energy equation from the padded rho*h field DH (N, M+2, L)."""
+        self.prop_table_init(table, fix_swap=fix_swap)
+        DH = np.ascontiguousarray(DH, np.float64)
+        if DH.shape != self.field_shape():
+            raise ValueError("DH shape mismatch")
+        self._check(self.lib.chapsim_thermal_init(self.h, _ptr(DH), float(qw_bot), float(qw_top), float(cthecd)))
+
+    def download_thermal(self):
+        """dict DH, H, T, D, M, K, CP of padded fields."""
+        names = ["DH", "H", "T", "D", "M", "K", "CP"]
+        out = {k: np.empty(self.field_shape()) for k in names}
+        self._check(self.lib.chapsim_download_thermal_fields(self.h, *[_ptr(out[k]) for k in names]))
+        return out

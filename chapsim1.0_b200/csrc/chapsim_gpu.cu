@@ -17,6 +17,7 @@
 #include "tdma.cuh"
 #include "io.cuh"
 #include "thermo.cuh"
+#include "thermal.cuh"
 
 // x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
 __global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
@@ -161,6 +162,11 @@ struct chapsim_ctx {
     PropStatus* pstat = nullptr;
     double* pbuf = nullptr;       // staging of the host-array entry (7 doubles per point)
     long long pbuf_pts = 0;
+    // thermal solver of the IO domain (chapsim_thermal_init)
+    bool thermal = false;
+    double* DEN = nullptr;        // DENSITY (io.RHO then holds DENSITY0)
+    ThermoFields tf{};
+    ThermoParams tp{};
     std::string err;
 };
 
@@ -387,7 +393,40 @@ int mixed_to_staging(chapsim_ctx* ctx, bool q, bool pr, bool h0) {
 IoFields io_fields(chapsim_ctx* ctx) {
     IoFields f = ctx->io;
     f.Q = ctx->Q; f.PR = ctx->PR; f.RHS = ctx->RHS;
+    f.DEN = ctx->thermal ? ctx->DEN : f.RHO;
     return f;
+}
+
+int prop_grid(const chapsim_ctx* ctx, long long npts);
+size_t prop_smem(int n);
+
+// SOLVERRK3_ENG_io(NS), DENSITY_TIME_DERIVATION, DENSITY_Staggered,
+// MU_Staggered, then G0 = G and VELOCITY_CALC_io of SOLVERRK3_MOM_io
+void launch_thermal_substep(chapsim_ctx* ctx, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    IoFields f = io_fields(ctx);
+    k_eng_rhs<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ctx->tp, ctx->st, ns);
+    prof_mark(ctx);
+    const size_t sm = prop_smem(ctx->tab.n);
+    const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
+    if (sm) {
+        k_eng_props<true><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        prof_mark(ctx);
+        k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    } else {
+        k_eng_props<false><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        prof_mark(ctx);
+        k_eng_bc<false><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    }
+    prof_mark(ctx);
+    k_drhodt<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ns);
+    prof_mark(ctx);
+    k_io_props<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    prof_mark(ctx);
+    k_g0_velocity<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf.G0);
+    prof_mark(ctx);
+    ctx->launches += 6;
 }
 
 void launch_io_step_start(chapsim_ctx* ctx) {
@@ -401,6 +440,7 @@ void launch_io_step_start(chapsim_ctx* ctx) {
 void launch_io_substep(chapsim_ctx* ctx, int ns) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
+    if (ctx->thermal) launch_thermal_substep(ctx, ns);
     IoFields f = io_fields(ctx);
     k_io_divu<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     prof_mark(ctx);
@@ -409,7 +449,8 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     k_io_massflux<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
     prof_mark(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    k_io_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP, ctx->st, ns);
+    k_io_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP, ctx->st, ns,
+                                                 ctx->thermal ? ctx->tf.DRHO : nullptr);
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
@@ -436,6 +477,8 @@ int check_device_error(chapsim_ctx* ctx) {
         CK(cudaStreamSynchronize(ctx->stream));
         if (e & CHS_EBIT_NAN) return fail(ctx, CHAPSIM_ERR_NAN, "non-finite velocity or time step on the device");
         if (e & CHS_EBIT_DT_COLLAPSE) return fail(ctx, CHAPSIM_ERR_DT_COLLAPSE, "DT/DT0 < 0.01 (time step collapse)");
+        if (e & CHS_EBIT_TABLE)
+            return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, "rho*h (or h) left the property table during the energy update");
     }
     return CHAPSIM_OK;
 }
@@ -648,6 +691,8 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
+    cudaFree(ctx->DEN); cudaFree(ctx->tf.DH); cudaFree(ctx->tf.ENTH); cudaFree(ctx->tf.TEMP); cudaFree(ctx->tf.KAP);
+    cudaFree(ctx->tf.HCP); cudaFree(ctx->tf.RHSE0); cudaFree(ctx->tf.G0); cudaFree(ctx->tf.DRHO);
     cudaFree(ctx->Qf); cudaFree(ctx->PRf); cudaFree(ctx->H0f); cudaFree(ctx->RHSf); cudaFree(ctx->RHSLLf); cudaFree(ctx->facf);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -820,6 +865,7 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
     // nsteps steps (slot 0 is timed from an event recorded before it).
     const int per = 2 + 3 * 9;
     if (!ctx || !ms || nslots < per || nsteps < 1) return CHAPSIM_ERR_BADARG;
+    if (ctx->thermal) return fail(ctx, CHAPSIM_ERR_BADARG, "per-kernel profiling covers the flow-only step");
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
     if (rc) return rc;
@@ -928,7 +974,7 @@ int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count) {
 
 int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count) {
     if (!ctx || !count) return CHAPSIM_ERR_BADARG;
-    int per = 2 + 3 * 9;
+    int per = 2 + 3 * (ctx->thermal ? 15 : 9);
     *count = per;
     return CHAPSIM_OK;
 }
@@ -1082,6 +1128,8 @@ extern "C" int chapsim_prop_table_init(chapsim_ctx_t* ctx, const chapsim_prop_ta
     if (sm) {
         CK(set_smem(k_prop_points<true>, sm));
         CK(set_smem(k_prop_fields<true>, sm));
+        CK(set_smem(k_eng_props<true>, sm));
+        CK(set_smem(k_eng_bc<true>, sm));
     }
     return CHAPSIM_OK;
 }
@@ -1126,6 +1174,75 @@ extern "C" int chapsim_therm_prop_update_points(chapsim_ctx_t* ctx, int64_t npts
                  ps.nbad, (long long)npts, ps.first_bad, dh[ps.first_bad]);
         return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, msg);
     }
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, double qw_top, double cthecd) {
+    if (!ctx || !dh) return fail(ctx, CHAPSIM_ERR_BADARG, "null argument");
+    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver runs in the main (IO) domain");
+    if (!ctx->ptab) return fail(ctx, CHAPSIM_ERR_BADARG, "no property table (call chapsim_prop_table_init first)");
+    if (!(cthecd > 0.0)) return fail(ctx, CHAPSIM_ERR_BADARG, "CTHECD must be positive");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    const size_t fb = (size_t)g.FS * sizeof(double);
+    if (!ctx->thermal) {
+        double** arrs[] = {&ctx->DEN, &ctx->tf.DH, &ctx->tf.ENTH, &ctx->tf.TEMP, &ctx->tf.KAP, &ctx->tf.HCP,
+                           &ctx->tf.RHSE0, &ctx->tf.DRHO};
+        for (double** a : arrs) {
+            CK(cudaMalloc(a, fb));
+            CK(cudaMemsetAsync(*a, 0, fb, s));
+        }
+        CK(cudaMalloc(&ctx->tf.G0, 3 * fb));
+    }
+    ctx->tp.wf_bot = qw_bot;
+    ctx->tp.wf_top = -qw_top;
+    ctx->tp.cthecd = cthecd;
+    double lim[2];
+    CK(cudaMemcpy(&lim[0], ctx->tab.xdh + ctx->tab.imin_dh, sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&lim[1], ctx->tab.xdh + ctx->tab.imax_dh, sizeof(double), cudaMemcpyDeviceToHost));
+    ctx->tp.dhmin = lim[0];
+    ctx->tp.dhmax = lim[1];
+    CK(cudaMemcpyAsync(ctx->tf.DH, dh, fb, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(ctx->tf.RHSE0, 0, fb, s));  // RHS_ENERGY0 = 0 (src/SOLVE.f90:40)
+    CK(cudaMemcpyAsync(ctx->DEN, ctx->io.RHO, fb, cudaMemcpyDeviceToDevice, s));
+    ctx->thermal = true;
+    IoFields f = io_fields(ctx);
+    const size_t sm = prop_smem(ctx->tab.n);
+    const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
+    if (sm) {
+        k_eng_props<true><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    } else {
+        k_eng_props<false><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<false><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    }
+    // DENSITY0 = DENSITY, Viscousity0 = Viscousity, G0_io = G_io
+    CK(cudaMemcpyAsync(ctx->io.RHO, ctx->DEN, fb, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->io.MU0, ctx->io.MU, fb, cudaMemcpyDeviceToDevice, s));
+    CK(cudaMemcpyAsync(ctx->tf.G0, ctx->io.G, 3 * fb, cudaMemcpyDeviceToDevice, s));
+    k_io_props<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    k_io_velocity<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    ctx->launches += 4;
+    CK(cudaGetLastError());
+    if (ctx->step_exec) {  // the captured step no longer matches
+        CK(cudaStreamSynchronize(s));
+        cudaGraphExecDestroy(ctx->step_exec);
+        ctx->step_exec = nullptr;
+    }
+    return check_device_error(ctx);
+}
+
+extern "C" int chapsim_download_thermal_fields(chapsim_ctx_t* ctx, double* dh, double* h, double* t, double* d,
+                                               double* m, double* k, double* cp) {
+    if (!ctx || !ctx->thermal) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver is not active on this context");
+    CK(cudaSetDevice(ctx->device));
+    const size_t fb = (size_t)ctx->g.FS * sizeof(double);
+    double* dst[7] = {dh, h, t, d, m, k, cp};
+    const double* src[7] = {ctx->tf.DH, ctx->tf.ENTH, ctx->tf.TEMP, ctx->DEN, ctx->io.MU, ctx->tf.KAP, ctx->tf.HCP};
+    for (int a = 0; a < 7; ++a)
+        if (dst[a]) CK(cudaMemcpyAsync(dst[a], src[a], fb, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return CHAPSIM_OK;
 }
 

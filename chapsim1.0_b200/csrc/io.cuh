@@ -1,7 +1,7 @@
 // Main-domain (IO, x-periodic) substep with explicit viscous terms:
 // SOLVERRK3_MOM_io (src/SOLVERRK3_MOM_IO.f90:11-120, iVisScheme = 0) for a
 // flow whose property fields (DENSITY0, Viscousity0, Viscousity) are given
-// and held fixed (thermal solver not active; DrhoDtP = 0).
+// and held fixed unless the thermal solver (thermal.cuh) updates them.
 //
 //   k_io_props     DENSITY_Staggered + MU_Staggered (src/MASSFLUX_CALC_IO.f90:155-329), once per upload
 //   k_io_divu      DIVG_U_io (src/DIVG.f90:140-246): DivU = div(u)/3
@@ -24,8 +24,10 @@
 
 #define IO_NT 256
 
+// RHO is DENSITY0 and DEN is DENSITY (the same array while the thermal
+// solver is off); MU0 is Viscousity0 and MU is Viscousity.
 struct IoFields {
-    double *G, *Q, *PR, *EX0, *RHS, *RHO, *MU0, *MU, *DST, *MST, *DIVU;
+    double *G, *Q, *PR, *EX0, *RHS, *RHO, *MU0, *MU, *DST, *MST, *DIVU, *DEN;
 };
 
 __device__ __forceinline__ void io_decode(const Geo& g, long long t, int& i, int& j, int& k) {
@@ -286,8 +288,10 @@ __global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const 
 }
 
 // DIVG_io + forward x transform (same tiling as k_div_fftx)
+// DRHO: DrhoDtP of the thermal solver, or NULL (zero) while it is off
 __global__ void __launch_bounds__(PX_NT) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
-                                                       double2* __restrict__ SP, const DevState* __restrict__ st, int ns) {
+                                                       double2* __restrict__ SP, const DevState* __restrict__ st, int ns,
+                                                       const double* __restrict__ DRHO) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, N = g.N, LH = g.LH;
     const int j0 = 1 + blockIdx.x * PX_TJ;
@@ -310,7 +314,8 @@ __global__ void __launch_bounds__(PX_NT) k_io_div_fftx(Geo g, const double* __re
             const double w = G[c + 2 * g.FS], wp = G[pidx(g, i, j, kp) + 2 * g.FS];
             const double coe2 = g.dyfi[j] / 1.0;
             const double DIVX = (up - u) * coe1, DIVY = (vp - v) * coe2, DIVZ = (wp - w) * g.dzi;
-            const double DQ = DIVX + DIVY + DIVZ + 0.0;  // + DrhoDtP (zero while the thermal solver is off)
+            const double DTRHO = DRHO ? DRHO[c] / 1.0 : 0.0;
+            const double DQ = DIVX + DIVY + DIVZ + DTRHO;
             val = DQ * coe0;
             RHSLL[iidx(g, i, j, k)] = val;
         }
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFields f, double* __r
         double q = (fabs((Q[c] + Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
                     fabs((Q[c + g.FS] + Q[c + g.FS + L]) * g.dyfi[j] * 1.0) +
                     fabs((Q[c + 2 * g.FS] + Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
-        const double vcf = 2.0 * g.cvisc * (g.dxqi + g.dzqi * 1.0 + g.dyfi[j] * g.dyfi[j]) * f.MU[c] / f.RHO[c];
+        const double vcf = 2.0 * g.cvisc * (g.dxqi + g.dzqi * 1.0 + g.dyfi[j] * g.dyfi[j]) * f.MU[c] / f.DEN[c];
         if (!(q == q) || !(vcf == vcf)) bad = true;
         q = fmax(q, vcf);
         mx = fmax(mx, q);

@@ -232,6 +232,29 @@ int chapsim_prop_table_init(chapsim_ctx_t* ctx, const chapsim_prop_table_t* tabl
 int chapsim_therm_prop_update_points(chapsim_ctx_t* ctx, int64_t npts, const double* dh, double* h, double* t,
                                      double* d, double* m, double* k, double* cp);
 
+/* ---- Thermal solver of the main (IO) domain (iThermoDynamics = 1, table search) ----
+ * Starts SOLVERRK3_ENG_io (src/SOLVERRK3_ENG_IO.f90:11-82) on a context
+ * created with grid.idomain = 2 whose flow fields are uploaded and whose
+ * property table is set.  dh = DH(NCL1, 0:NCL2+1, NCL3) (rows 1..NCL2 used);
+ * ENTHALPY, TEMPERATURE, DENSITY, Viscousity, THERMCONDT and HEATCAP follow
+ * from it by THERM_PROP_UPDATE and, on the wall ghosts, BC_WALL_Isoflux
+ * (src/BC_WALL.f90:541-619).  Both walls carry a constant heat flux:
+ * WALLFLUX = +qw_bot at the bottom and -qw_top at the top (nondimensional
+ * thermalWall_nondim, src/Flow_State.f90:140-175); cthecd = CTHECD =
+ * 1/(REN PRT0) (src/SOLVE.f90:168).  DENSITY0 = DENSITY, Viscousity0 =
+ * Viscousity, RHS_ENERGY0 = 0 and G0_io = G_io at start.  From then on every
+ * IO substep (chapsim_rk_substep_io, chapsim_advance_tg) runs
+ * SOLVERRK3_ENG_io(NS), DENSITY_TIME_DERIVATION(NS), DENSITY_Staggered and
+ * MU_Staggered before SOLVERRK3_MOM_io(NS), as SOLVE does
+ * (src/SOLVE.f90:119-133); a point leaving the table gives
+ * CHAPSIM_ERR_TABLE_RANGE. */
+int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, double qw_top, double cthecd);
+
+/* The thermal fields, each (NCL1, 0:NCL2+1, NCL3); any pointer may be NULL:
+ * DH, ENTHALPY, TEMPERATURE, DENSITY, Viscousity, THERMCONDT, HEATCAP. */
+int chapsim_download_thermal_fields(chapsim_ctx_t* ctx, double* dh, double* h, double* t, double* d, double* m,
+                                    double* k, double* cp);
+
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
  * with a CUDA event after every kernel; ms[slot] receives the summed
  * duration of kernel slot `slot` of a step.  Slot order: k_cfl,

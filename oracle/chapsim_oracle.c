@@ -58,7 +58,14 @@ typedef struct {
     /* IO (main-domain) path, allocated by orc_io_enable */
     int io;
     double *G, *EXPLT0, *RHO, *MU0, *MU, *DSTG, *MUSTG, *DIVU, *DRHODT;
+    double* DEN; /* DENSITY; RHO holds DENSITY0 (equal while the thermal solver is off) */
     double CFLMM_IO;
+    /* thermal solver (orc_thermal_enable): SOLVERRK3_ENG_io with the table-search properties */
+    int thermal;
+    void* tab;
+    double *DH, *ENTH, *TEMP, *KAPPA, *HCP, *RHSE, *RHSE0, *G0;
+    double QW_BOT, QW_TOP, CTHECD, DHMIN, DHMAX;
+    int prop_err;
 } orc_t;
 
 #define FOFF(o, i, j, k) ((size_t)((i) - 1) + (size_t)(o)->L * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
@@ -308,7 +315,8 @@ void orc_destroy(orc_t* o) {
     free(o->Q); free(o->PR); free(o->CONVH0); free(o->QTMP); free(o->DPH); free(o->RHSLLPHI); free(o->RHS);
     free(o->SRe); free(o->SIm);
     free(o->G); free(o->EXPLT0); free(o->RHO); free(o->MU0); free(o->MU); free(o->DSTG); free(o->MUSTG);
-    free(o->DIVU); free(o->DRHODT);
+    free(o->DIVU); free(o->DRHODT); free(o->DEN);
+    free(o->DH); free(o->ENTH); free(o->TEMP); free(o->KAPPA); free(o->HCP); free(o->RHSE); free(o->RHSE0); free(o->G0);
     free(o);
 }
 
@@ -964,6 +972,7 @@ void orc_io_enable(orc_t* o) {
     size_t fs = FSZ(o);
     o->G = dalloc(3 * fs); o->EXPLT0 = dalloc(3 * fs); o->RHO = dalloc(fs); o->MU0 = dalloc(fs); o->MU = dalloc(fs);
     o->DSTG = dalloc(3 * fs); o->MUSTG = dalloc(3 * fs); o->DIVU = dalloc(fs); o->DRHODT = dalloc(fs);
+    o->DEN = dalloc(fs);
     o->io = 1;
 }
 
@@ -1033,6 +1042,7 @@ void orc_io_set_fields(orc_t* o, const double* G, const double* PR, const double
     memcpy(o->G, G, 3 * fs * sizeof(double));
     memcpy(o->PR, PR, fs * sizeof(double));
     memcpy(o->RHO, RHO, fs * sizeof(double));
+    memcpy(o->DEN, RHO, fs * sizeof(double));
     memcpy(o->MU0, MU0, fs * sizeof(double));
     memcpy(o->MU, MU, fs * sizeof(double));
     memset(o->EXPLT0, 0, 3 * fs * sizeof(double));
@@ -1439,6 +1449,7 @@ static void io_prcalc_massflux_update(orc_t* o, int NS) {
 /* changes DPH and PR by an x-z-y constant only.                           */
 int orc_io_substep(orc_t* o, int NS) {
     if (!o->io || NS < 0 || NS > 3) return -1;
+    if (o->thermal) memcpy(o->G0, o->G, 3 * FSZ(o) * sizeof(double));  /* G0_io = G_io (:25) */
     io_velocity_calc(o);
     io_convection_x(o);
     io_convection_y(o);
@@ -1461,6 +1472,215 @@ int orc_io_substep(orc_t* o, int NS) {
     return 0;
 }
 
+
+/* ====================================================================== */
+/* Thermal solver of the IO domain (SOLVE.f90:119-128): SOLVERRK3_ENG_io    */
+/* (src/SOLVERRK3_ENG_IO.f90:11-82) with RHS_ENERGY_EXPLICIT               */
+/* (src/RHS_ENERGY_EXPLICIT.f90:11-155), THERM_PROP_UPDATE(IMAIND) by table */
+/* search, BC_WALL_THERMAL with constant wall heat flux on both walls       */
+/* (BC_WALL_Isoflux, src/BC_WALL.f90:541-619), then DENSITY_TIME_DERIVATION */
+/* (src/DIVG.f90:249-317), DENSITY_Staggered and MU_Staggered.  Plane      */
+/* channel: RCCI1 = RCCI2 = RNDI1 = 1.                                     */
+/* ====================================================================== */
+int orc_prop_point(void* tab, double dh, double* out);
+void orc_table_dh_limits(void* tab, double* out);
+
+static void thermal_point(orc_t* o, int I, int J, int K) {
+    double v[6];
+    if (orc_prop_point(o->tab, F3(o->DH, o, I, J, K), v)) o->prop_err = 1;
+    F3(o->ENTH, o, I, J, K) = v[0];
+    F3(o->TEMP, o, I, J, K) = v[1];
+    F3(o->DEN, o, I, J, K) = v[2];
+    F3(o->MU, o, I, J, K) = v[3];
+    F3(o->KAPPA, o, I, J, K) = v[4];
+    F3(o->HCP, o, I, J, K) = v[5];
+}
+
+/* THERM_PROP_UPDATE(IMAIND): rows 1..M */
+static void thermal_props_interior(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int J = 1; J <= M; ++J)
+        for (int I = 1; I <= L; ++I)
+            for (int K = 1; K <= N; ++K) thermal_point(o, I, J, K);
+}
+
+/* BC_WALL_Isoflux on both walls: ghost rho*h extrapolated, then its properties */
+static void thermal_bc_isoflux(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int I = 1; I <= L; ++I)
+        for (int K = 1; K <= N; ++K) {
+            F3(o->DH, o, I, M + 1, K) = 2.0 * F3(o->DH, o, I, M, K) - o->WFF[M] * F3(o->DH, o, I, M, K) -
+                                        o->WFB[M] * F3(o->DH, o, I, M - 1, K);
+            thermal_point(o, I, M + 1, K);
+        }
+    for (int I = 1; I <= L; ++I)
+        for (int K = 1; K <= N; ++K) {
+            F3(o->DH, o, I, 0, K) = 2.0 * F3(o->DH, o, I, 1, K) - o->WFF[2] * F3(o->DH, o, I, 2, K) -
+                                    o->WFB[2] * F3(o->DH, o, I, 1, K);
+            thermal_point(o, I, 0, K);
+        }
+}
+
+/* RHS_ENERGY_EXPLICIT, constant heat flux on both walls */
+static void rhs_energy_explicit(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    const double XND2CL = 0.5, ZND2CL = 0.5, CTHECD = o->CTHECD;
+    const double COE1 = o->DXI * XND2CL * 0.5;
+    const double COE11 = o->DXQI * XND2CL * CTHECD;
+    const double WF_BOT = o->QW_BOT, WF_TOP = -o->QW_TOP; /* WALLFLUX (src/Flow_State.f90:150-175) */
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1, JM = JC - 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * 1.0 * 0.5;
+        double COE3 = o->DZI * ZND2CL * 1.0 * 0.5;
+        double COE33 = o->DZQI * ZND2CL * 1.0 * CTHECD;
+        double COE22 = o->DYFI[JJ] * 1.0 * CTHECD;
+        double COE221, COE222;
+        if (JJ == 1) {
+            COE221 = o->DYCI[JJP] / 1.0;
+            COE222 = 1.0 / 1.0;
+        } else if (JJ == M) {
+            COE222 = o->DYCI[JJ] / 1.0;
+            COE221 = 1.0 / 1.0;
+        } else {
+            COE221 = o->DYCI[JJP] / 1.0;
+            COE222 = o->DYCI[JJ] / 1.0;
+        }
+        for (int IC = 1; IC <= L; ++IC) {
+            int IP = IPV(o, IC), IM = IMV(o, IC);
+            for (int KC = 1; KC <= N; ++KC) {
+                int KP = KPV(o, KC), KM = KMV(o, KC);
+#define HH(i, j, k) F3(o->ENTH, o, i, j, k)
+#define TT(i, j, k) F3(o->TEMP, o, i, j, k)
+#define KK(i, j, k) F3(o->KAPPA, o, i, j, k)
+                double DX_DHU = (HH(IP, JC, KC) + HH(IC, JC, KC)) * (GV(o, IP, JC, KC, 1) + GV(o, IP, JC, KC, 1)) -
+                                (HH(IC, JC, KC) + HH(IM, JC, KC)) * (GV(o, IC, JC, KC, 1) + GV(o, IC, JC, KC, 1));
+                DX_DHU = DX_DHU * COE1;
+                double DY_DHV = (o->WFF[JJP] * HH(IC, JP, KC) + o->WFB[JJP] * HH(IC, JC, KC)) *
+                                    (GV(o, IC, JP, KC, 2) + GV(o, IC, JP, KC, 2)) -
+                                (o->WFF[JJ] * HH(IC, JC, KC) + o->WFB[JJ] * HH(IC, JM, KC)) *
+                                    (GV(o, IC, JC, KC, 2) + GV(o, IC, JC, KC, 2));
+                DY_DHV = DY_DHV * COE2;
+                double DZ_DHW = (HH(IC, JC, KP) + HH(IC, JC, KC)) * (GV(o, IC, JC, KP, 3) + GV(o, IC, JC, KP, 3)) -
+                                (HH(IC, JC, KC) + HH(IC, JC, KM)) * (GV(o, IC, JC, KC, 3) + GV(o, IC, JC, KC, 3));
+                DZ_DHW = DZ_DHW * COE3;
+                double DX_KDT = (KK(IP, JC, KC) + KK(IC, JC, KC)) * (TT(IP, JC, KC) - TT(IC, JC, KC)) -
+                                (KK(IC, JC, KC) + KK(IM, JC, KC)) * (TT(IC, JC, KC) - TT(IM, JC, KC));
+                DX_KDT = DX_KDT * COE11;
+                double KDTy1 = (o->WFF[JJP] * KK(IC, JP, KC) + o->WFB[JJP] * KK(IC, JC, KC)) *
+                               (TT(IC, JP, KC) - TT(IC, JC, KC)) * COE221;
+                double KDTy2 = (o->WFF[JJ] * KK(IC, JC, KC) + o->WFB[JJ] * KK(IC, JM, KC)) *
+                               (TT(IC, JC, KC) - TT(IC, JM, KC)) * COE222;
+                if (JJ == 1) KDTy2 = -WF_BOT * COE222;
+                else if (JJ == M) KDTy1 = -WF_TOP * COE221;
+                double DY_KDT = (KDTy1 - KDTy2) * COE22;
+                double DZ_KDT = (KK(IC, JC, KP) + KK(IC, JC, KC)) * (TT(IC, JC, KP) - TT(IC, JC, KC)) -
+                                (KK(IC, JC, KM) + KK(IC, JC, KC)) * (TT(IC, JC, KC) - TT(IC, JC, KM));
+                DZ_KDT = DZ_KDT * COE33;
+                F3(o->RHSE, o, IC, JC, KC) = -DX_DHU - DY_DHV - DZ_DHW + DX_KDT + DY_KDT + DZ_KDT;
+#undef HH
+#undef TT
+#undef KK
+            }
+        }
+    }
+}
+
+/* DENSITY_TIME_DERIVATION(NS) */
+static void density_time_derivation(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1, JJ = JC;
+        double COE2 = o->DYFI[JJ] * 1.0, COE3 = o->DZI * 1.0;
+        for (int IC = 1; IC <= L; ++IC) {
+            int IP = IPV(o, IC);
+            for (int KC = 1; KC <= N; ++KC) {
+                int KP = KPV(o, KC);
+                size_t fs = FSZ(o);
+#define G0V(i, j, k, c) (o->G0[FOFF(o, i, j, k) + (size_t)((c) - 1) * fs])
+                double DIVX = (GV(o, IP, JC, KC, 1) - GV(o, IC, JC, KC, 1)) * o->DXI;
+                double DIVX0 = (G0V(IP, JC, KC, 1) - G0V(IC, JC, KC, 1)) * o->DXI;
+                double DIVY = (GV(o, IC, JP, KC, 2) - GV(o, IC, JC, KC, 2)) * COE2;
+                double DIVY0 = (G0V(IC, JP, KC, 2) - G0V(IC, JC, KC, 2)) * COE2;
+                double DIVZ = (GV(o, IC, JC, KP, 3) - GV(o, IC, JC, KC, 3)) * COE3;
+                double DIVZ0 = (G0V(IC, JC, KP, 3) - G0V(IC, JC, KC, 3)) * COE3;
+#undef G0V
+                F3(o->DRHODT, o, IC, JC, KC) = -o->TGAM[NS] * (DIVX + DIVY + DIVZ) - o->TROH[NS] * (DIVX0 + DIVY0 + DIVZ0);
+            }
+        }
+    }
+}
+
+/* Energy part of RK substep NS and the property / density coupling that
+ * precedes SOLVERRK3_MOM_io(NS).  Returns nonzero when a point fell outside
+ * the property table (the reference STOPs there). */
+int orc_thermal_substep(orc_t* o, int NS) {
+    if (!o->thermal || NS < 1 || NS > 3) return -1;
+    int L = o->L, M = o->M, N = o->N;
+    size_t fs = FSZ(o);
+    memcpy(o->MU0, o->MU, fs * sizeof(double));   /* Viscousity0 = Viscousity */
+    memcpy(o->RHO, o->DEN, fs * sizeof(double));  /* DENSITY0 = DENSITY */
+    double COE1 = o->TGAM[NS] * o->DT, COE0 = o->TROH[NS] * o->DT;
+    rhs_energy_explicit(o);
+    const double REALMIN = 1.0e-14;
+    for (int J = 1; J <= M; ++J)
+        for (int I = 1; I <= L; ++I)
+            for (int K = 1; K <= N; ++K) {
+                double d = F3(o->DH, o, I, J, K) + COE1 * F3(o->RHSE, o, I, J, K) + COE0 * F3(o->RHSE0, o, I, J, K);
+                d = fmin(o->DHMAX - REALMIN, d);
+                d = fmax(o->DHMIN + REALMIN, d);
+                F3(o->DH, o, I, J, K) = d;
+                F3(o->RHSE0, o, I, J, K) = F3(o->RHSE, o, I, J, K);
+            }
+    o->prop_err = 0;
+    thermal_props_interior(o);
+    thermal_bc_isoflux(o);
+    density_time_derivation(o, NS);
+    io_staggered_props(o);
+    return o->prop_err;
+}
+
+/* Starts the thermal solver on an IO state set by orc_io_set_fields: DH
+ * (padded field, rows 1..M used) with the table-search properties, constant
+ * nondimensional wall heat fluxes qw_bot, qw_top (WALLFLUX = +qw_bot at the
+ * bottom, -qw_top at the top) and CTHECD = 1 / (REN PRT0).  Properties of
+ * the interior and, through BC_WALL_Isoflux, of the wall ghosts follow from
+ * DH; DENSITY0 = DENSITY, Viscousity0 = Viscousity, RHS_ENERGY0 = 0 (SOLVE.f90:40),
+ * G0_io = G_io; D_STG, MU_STG and the velocity are recomputed. */
+int orc_thermal_enable(orc_t* o, void* tab, const double* DH, double qw_bot, double qw_top, double cthecd) {
+    if (!o->io || !tab) return -1;
+    size_t fs = FSZ(o);
+    if (!o->thermal) {
+        o->DH = dalloc(fs); o->ENTH = dalloc(fs); o->TEMP = dalloc(fs); o->KAPPA = dalloc(fs); o->HCP = dalloc(fs);
+        o->RHSE = dalloc(fs); o->RHSE0 = dalloc(fs); o->G0 = dalloc(3 * fs);
+    }
+    o->thermal = 1;
+    o->tab = tab;
+    o->QW_BOT = qw_bot; o->QW_TOP = qw_top; o->CTHECD = cthecd;
+    double lim[2];
+    orc_table_dh_limits(tab, lim);
+    o->DHMIN = lim[0]; o->DHMAX = lim[1];
+    memcpy(o->DH, DH, fs * sizeof(double));
+    memset(o->RHSE0, 0, fs * sizeof(double));
+    o->prop_err = 0;
+    thermal_props_interior(o);
+    thermal_bc_isoflux(o);
+    memcpy(o->MU0, o->MU, fs * sizeof(double));
+    memcpy(o->RHO, o->DEN, fs * sizeof(double));
+    memcpy(o->G0, o->G, 3 * fs * sizeof(double));
+    io_staggered_props(o);
+    io_velocity_calc(o);
+    return o->prop_err;
+}
+
+/* thermal fields: out = DH, ENTHALPY, TEMPERATURE, DENSITY, Viscousity, THERMCONDT, HEATCAP (7 padded fields) */
+void orc_thermal_get(const orc_t* o, double* out) {
+    size_t fs = FSZ(o);
+    const double* src[7] = {o->DH, o->ENTH, o->TEMP, o->DEN, o->MU, o->KAPPA, o->HCP};
+    for (int a = 0; a < 7; ++a) memcpy(out + a * fs, src[a], fs * sizeof(double));
+}
+
 /* CFL_io (src/CFL.f90:55-107), including the viscous number */
 double orc_io_cfl(orc_t* o) {
     int L = o->L, M = o->M, N = o->N;
@@ -1475,7 +1695,7 @@ double orc_io_cfl(orc_t* o) {
                               fabs((QV(o, I, J, K, 2) + QV(o, I, JP, K, 2)) * o->DYFI[JJ] * 1.0) +
                               fabs((QV(o, I, J, K, 3) + QV(o, I, J, KP, 3)) * o->DZI * 1.0)) * 0.5;
                 double VCF = 2.0 * o->CVISC * (o->DXQI + o->DZQI * 1.0 + o->DYFI[JJ] * o->DYFI[JJ]) * F3(o->MU, o, I, J, K) /
-                             F3(o->RHO, o, I, J, K);
+                             F3(o->DEN, o, I, J, K);
                 QCF = fmax(QCF, VCF);
                 CFLMA = fmax(CFLMA, QCF);
             }
@@ -1494,7 +1714,10 @@ int orc_io_run_steps(orc_t* o, int nsteps, double* cfl_dt) {
         o->DT = dt;
         if (cfl_dt) cfl_dt[s] = c * dt;
         if ((dt / o->DT0) < 0.01) return 1;
-        for (int NS = 1; NS <= 3; ++NS) orc_io_substep(o, NS);
+        for (int NS = 1; NS <= 3; ++NS) {
+            if (o->thermal && orc_thermal_substep(o, NS)) return 2;
+            orc_io_substep(o, NS);
+        }
     }
     return 0;
 }
@@ -1522,7 +1745,7 @@ void orc_io_monitor(orc_t* o, double* out) {
                 G2 += gc2;
                 UG1 += uc1 * gc1;
                 UG2 += uc1 * gc2;
-                D1 += F3(o->RHO, o, I, J, K);
+                D1 += F3(o->DEN, o, I, J, K);
             }
         }
         G1 *= VL1313; G2 *= VL1313; UG1 *= VL1313; UG2 *= VL1313; D1 *= VL1313;

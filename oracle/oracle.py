@@ -72,6 +72,12 @@ def lib():
         L.orc_io_run_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.orc_io_run_steps.restype = ctypes.c_int
         L.orc_io_monitor.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_thermal_enable.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double]
+        L.orc_thermal_enable.restype = ctypes.c_int
+        L.orc_thermal_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_thermal_substep.restype = ctypes.c_int
+        L.orc_thermal_get.argtypes = [ctypes.c_void_p, _dp]
         _ip = ctypes.POINTER(ctypes.c_int)
         L.orc_cubic_spline.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
         L.orc_spline_index.argtypes = [ctypes.c_int, _dp, ctypes.c_double]
@@ -219,6 +225,23 @@ class Oracle:
         out = np.zeros(5)
         self._lib.orc_io_monitor(self._h, _p(out))
         return dict(zip(["Uc", "UUc", "UVc", "Gmaxx", "Gbulk"], out.tolist()))
+
+    # ---- thermal solver of the IO domain (table-search properties) ----
+    def thermal_enable(self, table, DH, qw_bot, qw_top, cthecd):
+        """table: a PropTable; DH: padded (N, M+2, L) rho*h field (rows 1..M used)."""
+        DH = np.ascontiguousarray(DH, np.float64)
+        self._table = table
+        rc = self._lib.orc_thermal_enable(self._h, table._h, _p(DH), float(qw_bot), float(qw_top), float(cthecd))
+        if rc != 0:
+            raise ValueError("thermal start-up failed (DH outside the property table)")
+
+    def thermal_substep(self, ns):
+        return self._lib.orc_thermal_substep(self._h, int(ns))
+
+    def thermal_get(self):
+        out = np.zeros((7,) + self.field_shape())
+        self._lib.orc_thermal_get(self._h, _p(out))
+        return dict(zip(["DH", "H", "T", "D", "M", "K", "CP"], out))
 
     def poisson(self, rhs):
         rhs = np.ascontiguousarray(rhs, np.float64)

@@ -271,3 +271,38 @@ long orc_prop_update(void* p, long npts, const double* dh, double* out, long* fi
     if (first_bad) *first_bad = fb;
     return nbad;
 }
+
+/* One point of THERM_PROP_UPDATE_FROM_DH (table arm): out = H, T, DENSITY,
+ * Viscousity, THERMCONDT, HEATCAP.  Returns nonzero when the point (or its
+ * h) is outside the table, where the reference STOPs. */
+int orc_prop_point(void* p, double dh, double* out) {
+    orc_table* t = (orc_table*)p;
+    const double* H = t->lists;
+    const double* DH = t->lists + 7 * t->n;
+    double h = 0, T = 0, vd = 0, vm = 0, vk = 0, cp = 0, b = 0;
+    int rc = eval_s(t, SP_DHH, DH, t->imin_dh, t->imax_dh, dh, &h);
+    if (!rc) rc |= eval_s(t, SP_HT, H, t->imin_h, t->imax_h, h, &T);
+    if (!rc) {
+        if (t->fix_swap) {
+            rc |= eval_s(t, SP_HD, H, t->imin_h, t->imax_h, h, &vd);
+            rc |= eval_s(t, SP_HM, H, t->imin_h, t->imax_h, h, &vm);
+            rc |= eval_s(t, SP_HK, H, t->imin_h, t->imax_h, h, &vk);
+        } else {
+            rc |= eval_s(t, SP_HM, H, t->imin_h, t->imax_h, h, &vd);
+            rc |= eval_s(t, SP_HK, H, t->imin_h, t->imax_h, h, &vm);
+            rc |= eval_s(t, SP_HD, H, t->imin_h, t->imax_h, h, &vk);
+        }
+        rc |= eval_s(t, SP_HCP, H, t->imin_h, t->imax_h, h, &cp);
+        rc |= eval_s(t, SP_HB, H, t->imin_h, t->imax_h, h, &b);
+    }
+    out[0] = h; out[1] = T; out[2] = vd; out[3] = vm; out[4] = vk; out[5] = cp;
+    return rc;
+}
+
+/* DHmin, DHmax of SPLINE_COEFFICIENTS_FOR_H (:1115-1118): LIST_DH at IMIN_DH, IMAX_DH */
+void orc_table_dh_limits(void* p, double* out) {
+    orc_table* t = (orc_table*)p;
+    const double* DH = t->lists + 7 * t->n;
+    out[0] = DH[t->imin_dh];
+    out[1] = DH[t->imax_dh];
+}
