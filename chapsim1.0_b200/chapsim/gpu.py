@@ -33,7 +33,9 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_get_stream",
             "chapsim_sync", "chapsim_launch_count", "chapsim_kernels_per_step", "chapsim_tdma_lines_noalloc",
             "chapsim_prop_table_init", "chapsim_therm_prop_update_points", "chapsim_thermal_init",
-            "chapsim_download_thermal_fields"]
+            "chapsim_download_thermal_fields", "chapsim_mlp_init", "chapsim_mlp_set_params", "chapsim_mlp_get_params",
+            "chapsim_mlp_gradients", "chapsim_mlp_train", "chapsim_mlp_infer_points", "chapsim_thermal_use_mlp",
+            "chapsim_mlp_judge"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
@@ -108,6 +110,15 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_therm_prop_update_points.argtypes = [vp, ctypes.c_int64] + [_dp] * 7
     L.chapsim_thermal_init.argtypes = [vp, _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     L.chapsim_download_thermal_fields.argtypes = [vp] + [_dp] * 7
+    _fp = ctypes.POINTER(ctypes.c_float)
+    L.chapsim_mlp_init.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_uint64]
+    L.chapsim_mlp_set_params.argtypes = [vp, _fp]
+    L.chapsim_mlp_get_params.argtypes = [vp, _fp, _dp]
+    L.chapsim_mlp_gradients.argtypes = [vp, ctypes.c_int32, _dp, _fp, _dp]
+    L.chapsim_mlp_train.argtypes = [vp, ctypes.c_int32, _dp, ctypes.c_int32, ctypes.c_float, _dp]
+    L.chapsim_mlp_infer_points.argtypes = [vp, ctypes.c_int64] + [_dp] * 7
+    L.chapsim_thermal_use_mlp.argtypes = [vp, ctypes.c_int32]
+    L.chapsim_mlp_judge.argtypes = [vp, _dp]
     L.chapsim_tdma_lines_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_int32, vp]
     L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
@@ -348,6 +359,45 @@ class ChannelTG:
         return outs
 
 
+    # -- learned property model -------------------------------------------------
+    MLP_NPARAM = 4678
+    MLP_FIELDS = ("H", "T", "D", "M", "K", "CP")
+
+    def mlp_init(self, dh_lo, dh_hi, seed=2024):
+        """Random-initialised 1-64-64-6 MLP for rho*h in [dh_lo, dh_hi] (needs the property table)."""
+        self._check(self.lib.chapsim_mlp_init(self.h, float(dh_lo), float(dh_hi), int(seed)))
+
+    def mlp_params(self):
+        p = np.zeros(self.MLP_NPARAM, np.float32)
+        nm = np.zeros(14)
+        self._check(self.lib.chapsim_mlp_get_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _ptr(nm)))
+        return p, nm
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.lib.chapsim_mlp_set_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def mlp_gradients(self, dh):
+        dh = np.ascontiguousarray(dh, np.float64).reshape(-1)
+        g = np.zeros(self.MLP_NPARAM, np.float32)
+        loss = ctypes.c_double()
+        self._check(self.lib.chapsim_mlp_gradients(self.h, dh.size, _ptr(dh), g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                   ctypes.byref(loss)))
+        return g, loss.value
+
+    def mlp_train(self, dh, iters, lr=2e-3):
+        dh = np.ascontiguousarray(dh, np.float64).reshape(-1)
+        loss = ctypes.c_double()
+        self._check(self.lib.chapsim_mlp_train(self.h, dh.size, _ptr(dh), int(iters), float(lr), ctypes.byref(loss)))
+        return loss.value
+
+    def mlp_infer_points(self, dh):
+        dh = np.ascontiguousarray(dh, np.float64)
+        outs = {k: np.empty(dh.shape) for k in self.MLP_FIELDS}
+        self._check(self.lib.chapsim_mlp_infer_points(self.h, dh.size, _ptr(dh), *[_ptr(outs[k]) for k in self.MLP_FIELDS]))
+        return outs
+
+
 class ChannelIO(ChannelTG):
     """Device-resident x-periodic main-domain channel (CHAPSim IO domain) with
     explicit viscous terms and fixed property fields.
@@ -397,3 +447,12 @@ class ChannelIO(ChannelTG):
         out = {k: np.empty(self.field_shape()) for k in names}
         self._check(self.lib.chapsim_download_thermal_fields(self.h, *[_ptr(out[k]) for k in names]))
         return out
+
+    def thermal_use_mlp(self, enable=True):
+        self._check(self.lib.chapsim_thermal_use_mlp(self.h, int(bool(enable))))
+
+    def mlp_judge(self):
+        """Largest |model - table| / max(|table|, output scale) per output over the interior fields."""
+        e = np.zeros(6)
+        self._check(self.lib.chapsim_mlp_judge(self.h, _ptr(e)))
+        return dict(zip(self.MLP_FIELDS, e.tolist()))

@@ -18,6 +18,9 @@
 #include "io.cuh"
 #include "thermo.cuh"
 #include "thermal.cuh"
+#include "mlp.cuh"
+
+#include <algorithm>
 
 // x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
 __global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
@@ -167,6 +170,15 @@ struct chapsim_ctx {
     double* DEN = nullptr;        // DENSITY (io.RHO then holds DENSITY0)
     ThermoFields tf{};
     ThermoParams tp{};
+    // learned property model
+    float *mlp_par = nullptr, *mlp_grad = nullptr, *mlp_m1 = nullptr, *mlp_m2 = nullptr, *mlp_loss = nullptr;
+    __nv_bfloat16 *mlp_w2 = nullptr, *mlp_w2t = nullptr, *mlp_w3 = nullptr;
+    float *mlp_xs = nullptr, *mlp_ys = nullptr;
+    double* mlp_dh = nullptr;
+    int mlp_cap = 0, mlp_step = 0;
+    MlpNorm mlp_norm{};
+    bool mlp_ready = false, use_mlp = false;
+    unsigned int* mlp_judge = nullptr;
     std::string err;
 };
 
@@ -410,7 +422,16 @@ void launch_thermal_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     const size_t sm = prop_smem(ctx->tab.n);
     const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
-    if (sm) {
+    if (ctx->use_mlp) {
+        const long long tiles = (tot + MLP_TILE - 1) / MLP_TILE;
+        MlpOut out{ctx->tf.ENTH, ctx->tf.TEMP, f.DEN, f.MU, ctx->tf.KAP, ctx->tf.HCP, f.RHO, f.MU0};
+        k_mlp_infer<true><<<(int)std::min<long long>(tiles, 4LL * ctx->nsm), MLP_NT, MLP_INF_SMEM, s>>>(
+            ctx->mlp_par, MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t}, ctx->mlp_norm, ctx->tab, g, tot,
+            ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
+        prof_mark(ctx);
+        if (sm) k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        else k_eng_bc<false><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    } else if (sm) {
         k_eng_props<true><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
         prof_mark(ctx);
         k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
@@ -479,6 +500,7 @@ int check_device_error(chapsim_ctx* ctx) {
         if (e & CHS_EBIT_DT_COLLAPSE) return fail(ctx, CHAPSIM_ERR_DT_COLLAPSE, "DT/DT0 < 0.01 (time step collapse)");
         if (e & CHS_EBIT_TABLE)
             return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, "rho*h (or h) left the property table during the energy update");
+        if (e & CHS_EBIT_MMA_TIMEOUT) return fail(ctx, CHAPSIM_ERR_TIMEOUT, "a tensor-core completion wait ran out of time");
     }
     return CHAPSIM_OK;
 }
@@ -691,6 +713,8 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
+    cudaFree(ctx->mlp_par); cudaFree(ctx->mlp_w2); cudaFree(ctx->mlp_xs); cudaFree(ctx->mlp_ys); cudaFree(ctx->mlp_dh);
+    cudaFree(ctx->mlp_judge);
     cudaFree(ctx->DEN); cudaFree(ctx->tf.DH); cudaFree(ctx->tf.ENTH); cudaFree(ctx->tf.TEMP); cudaFree(ctx->tf.KAP);
     cudaFree(ctx->tf.HCP); cudaFree(ctx->tf.RHSE0); cudaFree(ctx->tf.G0); cudaFree(ctx->tf.DRHO);
     cudaFree(ctx->Qf); cudaFree(ctx->PRf); cudaFree(ctx->H0f); cudaFree(ctx->RHSf); cudaFree(ctx->RHSLLf); cudaFree(ctx->facf);
@@ -1243,6 +1267,263 @@ extern "C" int chapsim_download_thermal_fields(chapsim_ctx_t* ctx, double* dh, d
     for (int a = 0; a < 7; ++a)
         if (dst[a]) CK(cudaMemcpyAsync(dst[a], src[a], fb, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+// ------------------------- learned property model -------------------------
+namespace {
+int mlp_targets(chapsim_ctx* ctx, int n, const double* dh_host, const MlpNorm& nm) {
+    CK(cudaSetDevice(ctx->device));
+    if (n > ctx->mlp_cap) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->mlp_xs); cudaFree(ctx->mlp_ys); cudaFree(ctx->mlp_dh);
+        ctx->mlp_xs = nullptr; ctx->mlp_ys = nullptr; ctx->mlp_dh = nullptr; ctx->mlp_cap = 0;
+        CK(cudaMalloc(&ctx->mlp_xs, (size_t)n * sizeof(float)));
+        CK(cudaMalloc(&ctx->mlp_ys, (size_t)n * MLP_OUT * sizeof(float)));
+        CK(cudaMalloc(&ctx->mlp_dh, (size_t)n * sizeof(double)));
+        ctx->mlp_cap = n;
+    }
+    CK(cudaMemcpyAsync(ctx->mlp_dh, dh_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (int rc = prop_reset_status(ctx)) return rc;
+    k_mlp_targets<<<prop_grid(ctx, n), PROP_NT, 0, ctx->stream>>>(ctx->tab, nm, n, ctx->mlp_dh, ctx->mlp_xs, ctx->mlp_ys,
+                                                                  ctx->pstat);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    PropStatus ps{};
+    CK(cudaMemcpyAsync(&ps, ctx->pstat, sizeof(ps), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ps.nbad) return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, "training sample outside the property table");
+    return CHAPSIM_OK;
+}
+
+MlpOperands mlp_ops(const chapsim_ctx* ctx) { return MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t}; }
+
+int mlp_pack(chapsim_ctx* ctx) {
+    k_mlp_adam<<<1, 256, 0, ctx->stream>>>(ctx->mlp_par, ctx->mlp_grad, ctx->mlp_m1, ctx->mlp_m2, 0, 0.f, ctx->mlp_w2,
+                                           ctx->mlp_w3, ctx->mlp_w2t);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+
+int mlp_check_err(chapsim_ctx* ctx) {
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->st_host->err & CHS_EBIT_MMA_TIMEOUT) {
+        unsigned int zero = 0;
+        CK(cudaMemcpy(&ctx->st->err, &zero, sizeof(zero), cudaMemcpyHostToDevice));
+        return fail(ctx, CHAPSIM_ERR_TIMEOUT, "a tensor-core completion wait ran out of time");
+    }
+    return CHAPSIM_OK;
+}
+
+// one pass of k_mlp_train over the current training set; gradients summed into mlp_grad
+int mlp_pass(chapsim_ctx* ctx, int n) {
+    const int tiles = (n + MLP_TILE - 1) / MLP_TILE;
+    k_mlp_train<<<tiles, MLP_NT, MLP_TRN_SMEM, ctx->stream>>>(ctx->mlp_par, mlp_ops(ctx), ctx->mlp_xs, ctx->mlp_ys, n,
+                                                              1.0f / ((float)n * MLP_OUT), ctx->mlp_grad,
+                                                              ctx->mlp_loss, &ctx->st->err);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+}  // namespace
+
+extern "C" int chapsim_mlp_init(chapsim_ctx_t* ctx, double dh_lo, double dh_hi, uint64_t seed) {
+    if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
+    if (!ctx->ptab) return fail(ctx, CHAPSIM_ERR_BADARG, "no property table (call chapsim_prop_table_init first)");
+    if (!(dh_hi > dh_lo)) return fail(ctx, CHAPSIM_ERR_BADARG, "empty trained rho*h range");
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->mlp_par) {
+        CK(cudaMalloc(&ctx->mlp_par, 4 * MLP_NPARAM * sizeof(float) + sizeof(float)));
+        ctx->mlp_grad = ctx->mlp_par + MLP_NPARAM;
+        ctx->mlp_m1 = ctx->mlp_grad + MLP_NPARAM;
+        ctx->mlp_m2 = ctx->mlp_m1 + MLP_NPARAM;
+        ctx->mlp_loss = ctx->mlp_m2 + MLP_NPARAM;
+        CK(cudaMalloc(&ctx->mlp_w2, (64 * 64 * 2 + 16 * 64) * sizeof(__nv_bfloat16)));
+        ctx->mlp_w2t = ctx->mlp_w2 + 64 * 64;
+        ctx->mlp_w3 = ctx->mlp_w2t + 64 * 64;
+        CK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_TRN_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
+    }
+    // output scaling from the table over the trained range
+    const int ns = 4097;
+    std::vector<double> dh(ns);
+    for (int q = 0; q < ns; ++q) dh[q] = dh_lo + (dh_hi - dh_lo) * (double)q / (double)(ns - 1);
+    MlpNorm raw{};
+    raw.x_lo = (float)dh_lo;
+    raw.x_hi = (float)dh_hi;
+    for (int k = 0; k < MLP_OUT; ++k) { raw.off[k] = 0.f; raw.scale[k] = 1.f; }
+    if (int rc = mlp_targets(ctx, ns, dh.data(), raw)) return rc;
+    std::vector<float> ys((size_t)ns * MLP_OUT);
+    CK(cudaMemcpy(ys.data(), ctx->mlp_ys, ys.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    MlpNorm nm = raw;
+    for (int k = 0; k < MLP_OUT; ++k) {
+        float lo = ys[k], hi = ys[k];
+        for (int q = 1; q < ns; ++q) { lo = fminf(lo, ys[(size_t)q * MLP_OUT + k]); hi = fmaxf(hi, ys[(size_t)q * MLP_OUT + k]); }
+        nm.off[k] = 0.5f * (lo + hi);
+        nm.scale[k] = fmaxf(0.5f * (hi - lo), 1e-6f);
+    }
+    ctx->mlp_norm = nm;
+    // Glorot-uniform weights from a SplitMix64 stream, zero biases
+    std::vector<float> p(MLP_NPARAM, 0.f);
+    uint64_t st = seed;
+    auto next = [&]() {
+        uint64_t z = (st += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const double a1 = std::sqrt(6.0 / (1 + MLP_H)), a2 = std::sqrt(6.0 / (2 * MLP_H)), a3 = std::sqrt(6.0 / (MLP_H + MLP_OUT));
+    for (int q = 0; q < MLP_H; ++q) p[MLP_W1 + q] = (float)(a1 * (2 * next() - 1) * 3.0);
+    for (int q = 0; q < MLP_H; ++q) p[MLP_B1 + q] = (float)((2 * next() - 1) * 2.0);
+    for (int q = 0; q < MLP_H * MLP_H; ++q) p[MLP_W2 + q] = (float)(a2 * (2 * next() - 1));
+    for (int q = 0; q < MLP_OUT * MLP_H; ++q) p[MLP_W3 + q] = (float)(a3 * (2 * next() - 1));
+    CK(cudaMemcpy(ctx->mlp_par, p.data(), MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMemset(ctx->mlp_grad, 0, (3 * MLP_NPARAM + 1) * sizeof(float)));
+    CK(cudaMemset(ctx->mlp_w2, 0, (64 * 64 * 2 + 16 * 64) * sizeof(__nv_bfloat16)));
+    ctx->mlp_step = 0;
+    if (int rc = mlp_pack(ctx)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->mlp_ready = true;
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_mlp_set_params(chapsim_ctx_t* ctx, const float* params) {
+    if (!ctx || !params || !ctx->mlp_ready) return fail(ctx, CHAPSIM_ERR_BADARG, "MLP not initialised");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpy(ctx->mlp_par, params, MLP_NPARAM * sizeof(float), cudaMemcpyHostToDevice));
+    if (int rc = mlp_pack(ctx)) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_mlp_get_params(chapsim_ctx_t* ctx, float* params, double* norm) {
+    if (!ctx || !ctx->mlp_ready) return fail(ctx, CHAPSIM_ERR_BADARG, "MLP not initialised");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (params) CK(cudaMemcpy(params, ctx->mlp_par, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    if (norm) {
+        const MlpNorm& nm = ctx->mlp_norm;
+        norm[0] = nm.x_lo; norm[1] = nm.x_hi;
+        for (int k = 0; k < MLP_OUT; ++k) { norm[2 + k] = nm.off[k]; norm[2 + MLP_OUT + k] = nm.scale[k]; }
+    }
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_mlp_gradients(chapsim_ctx_t* ctx, int32_t n, const double* dh, float* grad, double* loss) {
+    if (!ctx || !ctx->mlp_ready || n <= 0 || !dh || !grad) return fail(ctx, CHAPSIM_ERR_BADARG, "bad MLP gradient arguments");
+    if (int rc = mlp_targets(ctx, n, dh, ctx->mlp_norm)) return rc;
+    CK(cudaMemsetAsync(ctx->mlp_grad, 0, MLP_NPARAM * sizeof(float), ctx->stream));
+    CK(cudaMemsetAsync(ctx->mlp_loss, 0, sizeof(float), ctx->stream));
+    if (int rc = mlp_pass(ctx, n)) return rc;
+    float l = 0.f;
+    CK(cudaMemcpyAsync(grad, ctx->mlp_grad, MLP_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&l, ctx->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->mlp_grad, 0, MLP_NPARAM * sizeof(float), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (loss) *loss = l;
+    return mlp_check_err(ctx);
+}
+
+extern "C" int chapsim_mlp_train(chapsim_ctx_t* ctx, int32_t n, const double* dh, int32_t iters, float lr,
+                                 double* final_loss) {
+    if (!ctx || !ctx->mlp_ready || n <= 0 || !dh || iters < 1 || !(lr > 0.f))
+        return fail(ctx, CHAPSIM_ERR_BADARG, "bad MLP training arguments");
+    if (int rc = mlp_targets(ctx, n, dh, ctx->mlp_norm)) return rc;
+    CK(cudaMemsetAsync(ctx->mlp_grad, 0, MLP_NPARAM * sizeof(float), ctx->stream));
+    for (int it = 0; it < iters; ++it) {
+        if (it == iters - 1) CK(cudaMemsetAsync(ctx->mlp_loss, 0, sizeof(float), ctx->stream));
+        if (int rc = mlp_pass(ctx, n)) return rc;
+        ++ctx->mlp_step;
+        k_mlp_adam<<<1, 256, 0, ctx->stream>>>(ctx->mlp_par, ctx->mlp_grad, ctx->mlp_m1, ctx->mlp_m2, ctx->mlp_step, lr,
+                                               ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t);
+        ctx->launches += 1;
+    }
+    CK(cudaGetLastError());
+    float l = 0.f;
+    CK(cudaMemcpyAsync(&l, ctx->mlp_loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (final_loss) *final_loss = l;
+    return mlp_check_err(ctx);
+}
+
+extern "C" int chapsim_mlp_infer_points(chapsim_ctx_t* ctx, int64_t npts, const double* dh, double* h, double* t,
+                                        double* d, double* m, double* k, double* cp) {
+    if (!ctx || !ctx->mlp_ready) return fail(ctx, CHAPSIM_ERR_BADARG, "MLP not initialised");
+    if (npts <= 0 || !dh || !h || !t || !d || !m || !k || !cp) return fail(ctx, CHAPSIM_ERR_BADARG, "bad point arrays");
+    CK(cudaSetDevice(ctx->device));
+    if (npts > ctx->pbuf_pts) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ctx->pbuf);
+        ctx->pbuf = nullptr;
+        ctx->pbuf_pts = 0;
+        CK(cudaMalloc(&ctx->pbuf, (size_t)7 * npts * sizeof(double)));
+        ctx->pbuf_pts = npts;
+    }
+    double* dd = ctx->pbuf;
+    double* o = dd + npts;
+    const size_t b = (size_t)npts * sizeof(double);
+    CK(cudaMemcpyAsync(dd, dh, b, cudaMemcpyHostToDevice, ctx->stream));
+    if (int rc = prop_reset_status(ctx)) return rc;
+    const long long tiles = (npts + MLP_TILE - 1) / MLP_TILE;
+    const int grid = (int)std::min<long long>(tiles, 4LL * ctx->nsm);
+    MlpOut out{o, o + npts, o + 2 * npts, o + 3 * npts, o + 4 * npts, o + 5 * npts, nullptr, nullptr};
+    k_mlp_infer<false><<<grid, MLP_NT, MLP_INF_SMEM, ctx->stream>>>(ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab,
+                                                                   ctx->g, npts, dd, out, ctx->pstat, &ctx->st->err);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    double* outs[6] = {h, t, d, m, k, cp};
+    for (int s = 0; s < 6; ++s) CK(cudaMemcpyAsync(outs[s], o + (size_t)s * npts, b, cudaMemcpyDeviceToHost, ctx->stream));
+    PropStatus ps{};
+    CK(cudaMemcpyAsync(&ps, ctx->pstat, sizeof(ps), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (int rc = mlp_check_err(ctx)) return rc;
+    if (ps.nbad) {
+        char msg[160];
+        snprintf(msg, sizeof msg, "%u of %lld points outside the property table; first at index %llu", ps.nbad,
+                 (long long)npts, ps.first_bad);
+        return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, msg);
+    }
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_thermal_use_mlp(chapsim_ctx_t* ctx, int32_t enable) {
+    if (!ctx || !ctx->thermal) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver is not active on this context");
+    if (enable && !ctx->mlp_ready) return fail(ctx, CHAPSIM_ERR_BADARG, "MLP not initialised");
+    CK(cudaSetDevice(ctx->device));
+    ctx->use_mlp = enable != 0;
+    if (ctx->step_exec) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaGraphExecDestroy(ctx->step_exec);
+        ctx->step_exec = nullptr;
+    }
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err) {
+    if (!ctx || !ctx->thermal || !ctx->mlp_ready || !max_rel_err)
+        return fail(ctx, CHAPSIM_ERR_BADARG, "the judge needs an active thermal solver and an initialised MLP");
+    CK(cudaSetDevice(ctx->device));
+    unsigned int* eb = reinterpret_cast<unsigned int*>(ctx->pstat);  // 6 words of scratch after the status
+    if (!ctx->mlp_judge) CK(cudaMalloc(&ctx->mlp_judge, 8 * sizeof(unsigned int)));
+    eb = ctx->mlp_judge;
+    CK(cudaMemsetAsync(eb, 0, 8 * sizeof(unsigned int), ctx->stream));
+    MlpOut cur{ctx->tf.ENTH, ctx->tf.TEMP, ctx->DEN, ctx->io.MU, ctx->tf.KAP, ctx->tf.HCP, nullptr, nullptr};
+    const long long tot = (long long)ctx->g.L * ctx->g.M * ctx->g.N;
+    k_mlp_judge<<<prop_grid(ctx, tot), PROP_NT, 0, ctx->stream>>>(ctx->tab, ctx->mlp_norm, ctx->g, ctx->tf.DH, cur, eb);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    unsigned int hb[8];
+    CK(cudaMemcpyAsync(hb, eb, sizeof(hb), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int m = 0; m < MLP_OUT; ++m) {
+        float f;
+        memcpy(&f, &hb[m], sizeof(f));
+        max_rel_err[m] = f;
+    }
     return CHAPSIM_OK;
 }
 

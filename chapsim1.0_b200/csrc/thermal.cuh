@@ -21,7 +21,9 @@
 #include "io.cuh"
 #include "thermo.cuh"
 
+#ifndef CHS_EBIT_TABLE
 #define CHS_EBIT_TABLE 4u  // a point (or its h) left the property table
+#endif
 
 struct ThermoFields {
     double *DH, *ENTH, *TEMP, *KAP, *HCP, *RHSE0, *G0, *DRHO;

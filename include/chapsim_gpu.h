@@ -255,6 +255,38 @@ int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, do
 int chapsim_download_thermal_fields(chapsim_ctx_t* ctx, double* dh, double* h, double* t, double* d, double* m,
                                     double* k, double* cp);
 
+/* ---- Learned property model (no counterpart in the reference) ----
+ * A 1 -> 64 -> 64 -> 6 tanh MLP from rho*h to the six outputs of
+ * THERM_PROP_UPDATE_FROM_DH (ENTHALPY, TEMPERATURE, DENSITY, Viscousity,
+ * THERMCONDT, HEATCAP), with BF16 tensor-core (tcgen05) layers and FP32
+ * accumulation, trained on the GPU against the table search, which stays the
+ * fallback outside the trained rho*h range and the judge of its accuracy.
+ * Parameters (4678 floats): w1[64], b1[64], W2[64][64] (out, in), b2[64],
+ * W3[6][64], b3[6]; inputs map [dh_lo, dh_hi] to [-1, 1]; output k is
+ * off[k] + scale[k] * y[k] with off/scale from the table over that range.
+ * The property table must be set first (chapsim_prop_table_init). */
+int chapsim_mlp_init(chapsim_ctx_t* ctx, double dh_lo, double dh_hi, uint64_t seed);
+int chapsim_mlp_set_params(chapsim_ctx_t* ctx, const float* params);
+/* params (4678) and/or norm (14: dh_lo, dh_hi, off[6], scale[6]); either may be NULL */
+int chapsim_mlp_get_params(chapsim_ctx_t* ctx, float* params, double* norm);
+/* Gradient of the mean squared error of the normalised outputs against the
+ * table search over n host samples (one forward/backward pass, no update). */
+int chapsim_mlp_gradients(chapsim_ctx_t* ctx, int32_t n, const double* dh, float* grad, double* loss);
+/* iters full-batch Adam steps (learning rate lr) on n host samples; final_loss
+ * receives the loss of the last pass. */
+int chapsim_mlp_train(chapsim_ctx_t* ctx, int32_t n, const double* dh, int32_t iters, float lr, double* final_loss);
+/* Model evaluation of npts host points (table search outside the trained range). */
+int chapsim_mlp_infer_points(chapsim_ctx_t* ctx, int64_t npts, const double* dh, double* h, double* t, double* d,
+                             double* m, double* k, double* cp);
+/* Thermal step: 1 = the interior property update of every substep uses the
+ * model (wall ghosts and points outside the trained range keep the table
+ * search), 0 = table search everywhere. */
+int chapsim_thermal_use_mlp(chapsim_ctx_t* ctx, int32_t enable);
+/* Judge: max over the interior of |field - table(DH)| / max(|table(DH)|, scale)
+ * for each of the six outputs (max_rel_err[6]); the caller runs it every N
+ * steps and switches back to the table when it exceeds its bound. */
+int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err);
+
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
  * with a CUDA event after every kernel; ms[slot] receives the summed
  * duration of kernel slot `slot` of a step.  Slot order: k_cfl,

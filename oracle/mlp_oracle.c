@@ -1,0 +1,114 @@
+/*
+ * mlp_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU forward and backward pass of the learned property model (1 -> 64 ->
+ * 64 -> 6 tanh MLP from rho*h to the outputs of THERM_PROP_UPDATE_FROM_DH),
+ * the checker of the tensor-core training and inference kernels.  The GPU
+ * rounds the operands of its tensor-core products to BF16 (the weights of
+ * layers 2 and 3, the activations h1 and h2, and the hidden-layer error dz2)
+ * and accumulates in FP32; here the same values are rounded to BF16 (round
+ * to nearest even) and the sums are taken in FP64.  Element-wise steps use
+ * the GPU's FP32 operations (fmaf, tanhf).  Targets come from the table
+ * search of thermo_oracle.c, bitwise equal to the GPU's.
+ *
+ * Parameter layout (FP32): w1[64], b1[64], W2[64][64] (out, in), b2[64],
+ * W3[6][64], b3[6].  norm: x_lo, x_hi, off[6], scale[6].
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#define H 64
+#define NO 6
+#define P_W1 0
+#define P_B1 (P_W1 + H)
+#define P_W2 (P_B1 + H)
+#define P_B2 (P_W2 + H * H)
+#define P_W3 (P_B2 + H)
+#define P_B3 (P_W3 + NO * H)
+#define NPARAM (P_B3 + NO)
+
+int orc_prop_point(void* tab, double dh, double* out);
+
+static float bf16r(float f) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return f;
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+static float xnorm(const double* norm, double dh) {
+    const double lo = (double)(float)norm[0], hi = (double)(float)norm[1];
+    return (float)(2.0 * (dh - lo) / (hi - lo) - 1.0);
+}
+
+static void forward(const float* p, float x, float* h1, float* h2, float* y) {
+    for (int i = 0; i < H; ++i) h1[i] = tanhf(fmaf(p[P_W1 + i], x, p[P_B1 + i]));
+    for (int j = 0; j < H; ++j) {
+        double a = 0.0;
+        for (int i = 0; i < H; ++i) a += (double)bf16r(h1[i]) * (double)bf16r(p[P_W2 + j * H + i]);
+        h2[j] = tanhf((float)a + p[P_B2 + j]);
+    }
+    for (int k = 0; k < NO; ++k) {
+        double a = 0.0;
+        for (int j = 0; j < H; ++j) a += (double)bf16r(h2[j]) * (double)bf16r(p[P_W3 + k * H + j]);
+        y[k] = (float)a + p[P_B3 + k];
+    }
+}
+
+/* Model outputs (denormalised) for n points: out[6n] in the order H, T, D, M, K, CP. */
+void orc_mlp_forward(const float* p, const double* norm, int n, const double* dh, double* out) {
+    float h1[H], h2[H], y[NO];
+    for (int q = 0; q < n; ++q) {
+        forward(p, xnorm(norm, dh[q]), h1, h2, y);
+        for (int k = 0; k < NO; ++k) out[(size_t)k * n + q] = (double)((float)norm[2 + k] + (float)norm[2 + NO + k] * y[k]);
+    }
+}
+
+/* Gradient of the mean squared error over n samples and 6 normalised outputs
+ * (targets from the table search).  grad[NPARAM]; returns the loss, or -1
+ * when a sample lies outside the table. */
+double orc_mlp_gradients(void* tab, const float* p, const double* norm, int n, const double* dh, double* grad) {
+    memset(grad, 0, sizeof(double) * NPARAM);
+    const float inv = 1.0f / ((float)n * NO);
+    double loss = 0.0;
+    static double dW2[H * H];
+    memset(dW2, 0, sizeof(dW2));
+    for (int q = 0; q < n; ++q) {
+        double o[6];
+        if (orc_prop_point(tab, dh[q], o)) return -1.0;
+        const float x = xnorm(norm, dh[q]);
+        float h1[H], h2[H], y[NO], dy[NO], dz2[H];
+        forward(p, x, h1, h2, y);
+        for (int k = 0; k < NO; ++k) {
+            const float t = (float)((o[k] - (double)(float)norm[2 + k]) / (double)(float)norm[2 + NO + k]);
+            const float e = y[k] - t;
+            loss += (double)(e * e * inv);
+            dy[k] = 2.f * e * inv;
+            grad[P_B3 + k] += dy[k];
+        }
+        for (int j = 0; j < H; ++j) {
+            float s = 0.f;
+            for (int k = 0; k < NO; ++k) {
+                s = fmaf(dy[k], p[P_W3 + k * H + j], s);
+                grad[P_W3 + k * H + j] += (double)(dy[k] * h2[j]);
+            }
+            dz2[j] = s * (1.f - h2[j] * h2[j]);
+            grad[P_B2 + j] += dz2[j];
+        }
+        for (int i = 0; i < H; ++i) {
+            double a = 0.0;
+            for (int j = 0; j < H; ++j) a += (double)bf16r(dz2[j]) * (double)bf16r(p[P_W2 + j * H + i]);
+            const float dz1 = (float)a * (1.f - h1[i] * h1[i]);
+            grad[P_W1 + i] += (double)(dz1 * x);
+            grad[P_B1 + i] += dz1;
+        }
+        for (int j = 0; j < H; ++j)
+            for (int i = 0; i < H; ++i) dW2[j * H + i] += (double)bf16r(dz2[j]) * (double)bf16r(h1[i]);
+    }
+    for (int q = 0; q < H * H; ++q) grad[P_W2 + q] = dW2[q];
+    return loss;
+}

@@ -22,7 +22,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 
 def build(force: bool = False) -> str:
     """Compile the oracle with its Makefile (gcc, OpenMP)."""
-    srcs = [os.path.join(_HERE, f) for f in ("chapsim_oracle.c", "thermo_oracle.c")]
+    srcs = [os.path.join(_HERE, f) for f in ("chapsim_oracle.c", "thermo_oracle.c", "mlp_oracle.c")]
     if force or not os.path.exists(_LIB_PATH) or (
         os.path.getmtime(_LIB_PATH) < max(os.path.getmtime(f) for f in srcs)
     ):
@@ -78,6 +78,10 @@ def lib():
         L.orc_thermal_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_thermal_substep.restype = ctypes.c_int
         L.orc_thermal_get.argtypes = [ctypes.c_void_p, _dp]
+        _fp = ctypes.POINTER(ctypes.c_float)
+        L.orc_mlp_forward.argtypes = [_fp, _dp, ctypes.c_int, _dp, _dp]
+        L.orc_mlp_gradients.argtypes = [ctypes.c_void_p, _fp, _dp, ctypes.c_int, _dp, _dp]
+        L.orc_mlp_gradients.restype = ctypes.c_double
         _ip = ctypes.POINTER(ctypes.c_int)
         L.orc_cubic_spline.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
         L.orc_spline_index.argtypes = [ctypes.c_int, _dp, ctypes.c_double]
@@ -336,3 +340,26 @@ class PropTable:
         res = {k: out[i * flat.size:(i + 1) * flat.size].reshape(dh.shape) for i, k in
                enumerate(["H", "T", "D", "M", "K", "CP"])}
         return res, nbad, fb.value
+
+
+# ---- learned property model (mlp_oracle.c) ----
+MLP_NPARAM = 64 + 64 + 64 * 64 + 64 + 6 * 64 + 6
+
+
+def mlp_forward(params, norm, dh):
+    p = np.ascontiguousarray(params, np.float32)
+    nm = np.ascontiguousarray(norm, np.float64)
+    dh = np.ascontiguousarray(dh, np.float64)
+    out = np.zeros(6 * dh.size)
+    lib().orc_mlp_forward(p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _p(nm), dh.size, _p(dh), _p(out))
+    return dict(zip(["H", "T", "D", "M", "K", "CP"], out.reshape(6, dh.size)))
+
+
+def mlp_gradients(table, params, norm, dh):
+    p = np.ascontiguousarray(params, np.float32)
+    nm = np.ascontiguousarray(norm, np.float64)
+    dh = np.ascontiguousarray(dh, np.float64)
+    g = np.zeros(MLP_NPARAM)
+    loss = lib().orc_mlp_gradients(table._h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _p(nm), dh.size,
+                                   _p(dh), _p(g))
+    return g, loss
