@@ -35,7 +35,8 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_prop_table_init", "chapsim_therm_prop_update_points", "chapsim_thermal_init",
             "chapsim_download_thermal_fields", "chapsim_mlp_init", "chapsim_mlp_set_params", "chapsim_mlp_get_params",
             "chapsim_mlp_gradients", "chapsim_mlp_train", "chapsim_mlp_infer_points", "chapsim_thermal_use_mlp",
-            "chapsim_mlp_judge"]
+            "chapsim_mlp_judge", "chapsim_autotune", "chapsim_batch_create", "chapsim_batch_advance",
+            "chapsim_batch_get_stream", "chapsim_batch_destroy"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
@@ -119,6 +120,11 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_mlp_infer_points.argtypes = [vp, ctypes.c_int64] + [_dp] * 7
     L.chapsim_thermal_use_mlp.argtypes = [vp, ctypes.c_int32]
     L.chapsim_mlp_judge.argtypes = [vp, _dp]
+    L.chapsim_autotune.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]
+    L.chapsim_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(vp)]
+    L.chapsim_batch_advance.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+    L.chapsim_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.chapsim_batch_destroy.argtypes = [vp]
     L.chapsim_tdma_lines_noalloc.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_int32, vp]
     L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
@@ -396,6 +402,51 @@ class ChannelTG:
         outs = {k: np.empty(dh.shape) for k in self.MLP_FIELDS}
         self._check(self.lib.chapsim_mlp_infer_points(self.h, dh.size, _ptr(dh), *[_ptr(outs[k]) for k in self.MLP_FIELDS]))
         return outs
+
+
+    def autotune(self, force=-1):
+        """Picks the faster Poisson y-solve for this grid (or forces 0: warp hybrid,
+        1: sequential); returns (choice, {variant: ms})."""
+        ch = ctypes.c_int32()
+        ms = (ctypes.c_float * 2)()
+        self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
+        return ch.value, {"warp_pcr": ms[0], "sequential": ms[1]}
+
+
+class Ensemble:
+    """Independent periodic channels advanced together (one graph per step, one branch per member)."""
+
+    def __init__(self, channels):
+        self.lib = load_library()
+        self.members = list(channels)
+        arr = (ctypes.c_void_p * len(self.members))(*[c.h.value if hasattr(c.h, "value") else c.h
+                                                      for c in self.members])
+        h = ctypes.c_void_p()
+        rc = self.lib.chapsim_batch_create(arr, len(self.members), ctypes.byref(h))
+        if rc != 0:
+            raise ChapsimError(rc, self.lib.chapsim_last_error_string(None).decode())
+        self.h = h
+
+    def advance(self, nsteps, DT0, DTMIN, CFLGV):
+        rc = self.lib.chapsim_batch_advance(self.h, int(nsteps), DT0, DTMIN, CFLGV)
+        if rc != 0:
+            raise ChapsimError(rc, self.lib.chapsim_last_error_string(None).decode())
+
+    def stream_handle(self):
+        v = ctypes.c_void_p()
+        self.lib.chapsim_batch_get_stream(self.h, ctypes.byref(v))
+        return v.value or 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chapsim_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class ChannelIO(ChannelTG):

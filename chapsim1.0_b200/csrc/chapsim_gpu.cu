@@ -135,6 +135,8 @@ struct chapsim_ctx {
     cudaStream_t stream = nullptr;
     Geo g{};
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr;
+    double* HS = nullptr;         // forward factors of the sequential y-solve (allocated when chosen)
+    int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
@@ -245,11 +247,25 @@ size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(doubl
 // forward declaration: DISPATCH_S is defined below
 void launch_ysolve_warp(chapsim_ctx* ctx);
 
-void launch_ysolve(chapsim_ctx* ctx) { launch_ysolve_warp(ctx); }
+void launch_ysolve_seq(chapsim_ctx* ctx);
+void launch_ysolve(chapsim_ctx* ctx);
 
+// Kernel attributes are process-wide and several contexts (of different
+// grids) may share a kernel, so the dynamic shared-memory limit is raised to
+// the device's opt-in maximum rather than set to one context's need, which
+// could lower it below another's.  The limit does not affect occupancy.
 template <typename F>
 cudaError_t set_smem(F* f, size_t bytes) {
-    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return e;
+    const int limit = optin - (int)fa.sharedSizeBytes;  // dynamic + static must fit the opt-in size
+    if ((int)bytes > limit) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
 }
 
 #define DISPATCH_S(S_, KERNEL_CALL)                    \
@@ -265,6 +281,17 @@ cudaError_t set_smem(F* f, size_t bytes) {
     }
 
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
+
+void launch_ysolve_seq(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    const long long nl = (long long)g.LH * g.N;
+    k_ysolve_seq<<<(int)((nl + YQ_NT - 1) / YQ_NT), YQ_NT, 0, ctx->stream>>>(g, ctx->SP, ctx->HS);
+}
+
+void launch_ysolve(chapsim_ctx* ctx) {
+    if (ctx->ysolve_kind == 1 && ctx->HS) launch_ysolve_seq(ctx);
+    else launch_ysolve_warp(ctx);
+}
 
 void launch_ysolve_warp(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
@@ -708,7 +735,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
+    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
@@ -1524,6 +1551,170 @@ extern "C" int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err) {
         memcpy(&f, &hb[m], sizeof(f));
         max_rel_err[m] = f;
     }
+    return CHAPSIM_OK;
+}
+
+// ----------------------------- autotuner -----------------------------------
+// Times the two Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
+// Thomas) on this context's grid and keeps the faster.  The spectral array is
+// scratch between substeps, so it is zeroed and solved in place.
+extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms) {
+    if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    CK(cudaStreamSynchronize(s));
+    const size_t nsp = (size_t)g.LH * g.M * g.N;
+    if (!ctx->HS) CK(cudaMalloc(&ctx->HS, nsp * sizeof(double)));
+    CK(cudaMemsetAsync(ctx->SP, 0, nsp * sizeof(double2), s));
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float t[2] = {0.f, 0.f};
+    const int reps = 5;
+    for (int kind = 0; kind < 2; ++kind) {
+        for (int w = 0; w < 2; ++w) {
+            if (kind == 0) launch_ysolve_warp(ctx); else launch_ysolve_seq(ctx);
+        }
+        CK(cudaEventRecord(e0, s));
+        for (int r = 0; r < reps; ++r) {
+            if (kind == 0) launch_ysolve_warp(ctx); else launch_ysolve_seq(ctx);
+        }
+        CK(cudaEventRecord(e1, s));
+        CK(cudaEventSynchronize(e1));
+        CK(cudaEventElapsedTime(&t[kind], e0, e1));
+        t[kind] /= reps;
+    }
+    ctx->launches += 2 * (2 + reps);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(cudaGetLastError());
+    ctx->ysolve_kind = force == 0 ? 0 : force == 1 ? 1 : (t[1] < t[0] ? 1 : 0);
+    if (ctx->ysolve_kind == 0) {
+        cudaFree(ctx->HS);
+        ctx->HS = nullptr;
+    }
+    if (ctx->step_exec) {
+        cudaGraphExecDestroy(ctx->step_exec);
+        ctx->step_exec = nullptr;
+    }
+    if (choice) *choice = ctx->ysolve_kind;
+    if (ms) { ms[0] = t[0]; ms[1] = t[1]; }
+    return CHAPSIM_OK;
+}
+
+// ------------------------------ ensembles ----------------------------------
+struct chapsim_batch {
+    std::vector<chapsim_ctx*> ctx;
+    int device = 0;
+    cudaStream_t stream = nullptr;     // the ensemble's own stream: the graph forks from and joins to it
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t exec = nullptr;
+    int kernels_per_step = 0;
+    std::string err;
+};
+
+extern "C" int chapsim_batch_create(chapsim_ctx_t* const* ctxs, int32_t n, chapsim_batch_t** out) {
+    if (!ctxs || n < 1 || !out) return fail(nullptr, CHAPSIM_ERR_BADARG, "bad ensemble arguments");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (!ctxs[i]) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context in ensemble");
+        if (ctxs[i]->domain != 1 || ctxs[i]->device != ctxs[0]->device)
+            return fail(nullptr, CHAPSIM_ERR_BADARG, "an ensemble holds periodic (TG) contexts of one device");
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) return fail(nullptr, CHAPSIM_ERR_BADARG, "a context appears twice in the ensemble");
+    }
+    auto* b = new chapsim_batch();
+    b->ctx.assign(ctxs, ctxs + n);
+    b->device = ctxs[0]->device;
+    auto bail = [&](cudaError_t e, const char* what) {
+        std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+        chapsim_batch_destroy(b);
+        return fail(nullptr, CHAPSIM_ERR_CUDA, m);
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(b->device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "stream");
+    if ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+    b->join.resize(n, nullptr);
+    for (int i = 0; i < n; ++i)
+        if ((e = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming)) != cudaSuccess) return bail(e, "event");
+    *out = b;
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_batch_destroy(chapsim_batch_t* b) {
+    if (!b) return CHAPSIM_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->fork) cudaEventDestroy(b->fork);
+    for (cudaEvent_t ev : b->join)
+        if (ev) cudaEventDestroy(ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return CHAPSIM_OK;
+}
+
+namespace {
+// One RK3 step of every member, captured as one graph: the members' kernel
+// chains are parallel branches forked from the ensemble stream.
+int batch_capture(chapsim_batch_t* b) {
+    chapsim_ctx* ctx = b->ctx[0];  // for CK's error reporting
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaEventRecord(b->fork, b->stream);
+    int kernels = 0;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        chapsim_ctx* c = b->ctx[i];
+        cudaStreamWaitEvent(c->stream, b->fork, 0);
+        const unsigned long long before = c->launches;
+        launch_step_start(c);
+        for (int ns = 1; ns <= 3; ++ns) launch_substep(c, ns, false);
+        kernels += (int)(c->launches - before);
+        c->launches = before;
+        cudaEventRecord(b->join[i], c->stream);
+        cudaStreamWaitEvent(b->stream, b->join[i], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+    if (e != cudaSuccess) return fail(ctx, CHAPSIM_ERR_CUDA, std::string("ensemble capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(ctx, CHAPSIM_ERR_CUDA, std::string("ensemble instantiate: ") + cudaGetErrorString(e));
+    b->kernels_per_step = kernels;
+    return CHAPSIM_OK;
+}
+}  // namespace
+
+extern "C" int chapsim_batch_advance(chapsim_batch_t* b, int32_t nsteps, double dt0, double dtmin, double cflgv) {
+    if (!b || nsteps < 0) return fail(nullptr, CHAPSIM_ERR_BADARG, "bad ensemble arguments");
+    if (cudaSetDevice(b->device) != cudaSuccess) return fail(nullptr, CHAPSIM_ERR_CUDA, "cudaSetDevice");
+    for (chapsim_ctx* c : b->ctx) {
+        int rc = set_step_params(c, dt0, dtmin, cflgv);
+        if (rc) return fail(nullptr, rc, c->err);
+    }
+    if (!b->exec) {
+        int rc = batch_capture(b);
+        if (rc) return fail(nullptr, rc, b->ctx[0]->err);
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        cudaError_t e = cudaGraphLaunch(b->exec, b->stream);
+        if (e != cudaSuccess) return fail(nullptr, CHAPSIM_ERR_CUDA, std::string("ensemble launch: ") + cudaGetErrorString(e));
+    }
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return fail(nullptr, CHAPSIM_ERR_CUDA, std::string("ensemble sync: ") + cudaGetErrorString(e));
+    for (chapsim_ctx* c : b->ctx) {
+        c->launches += (unsigned long long)nsteps * (unsigned long long)(b->kernels_per_step / (int)b->ctx.size());
+        int rc = check_device_error(c);
+        if (rc) return fail(nullptr, rc, c->err);
+    }
+    return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_batch_get_stream(chapsim_batch_t* b, void** stream) {
+    if (!b || !stream) return CHAPSIM_ERR_BADARG;
+    *stream = (void*)b->stream;
     return CHAPSIM_OK;
 }
 

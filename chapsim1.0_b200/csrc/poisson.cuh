@@ -201,6 +201,52 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __rest
 }
 
 // ---------------------------------------------------------------------------
+// The other y-solve variant: the reference's sequential Thomas recurrence
+// (TDMAIJJ_nonCYC :95-121, zero mode pinned as above), one thread per (kx, kz)
+// line with both parts, coefficients formed on the fly.  Consecutive threads
+// take consecutive kx, so every row access is coalesced; the forward sweep
+// keeps G in the spectral array and H in HS (LH*M*N doubles).  Fewer
+// operations than the warp hybrid but only one thread per line: the
+// autotuner picks between them per grid.
+#define YQ_NT 128
+__global__ void __launch_bounds__(YQ_NT) k_ysolve_seq(Geo g, double2* __restrict__ SP, double* __restrict__ HS) {
+    const int M = g.M, LH = g.LH;
+    const long long nl = (long long)LH * g.N;
+    const long long q = (long long)blockIdx.x * YQ_NT + threadIdx.x;
+    if (q >= nl) return;
+    const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+    const long long js = LH;
+    double2* s = SP + kx + (long long)LH * (long long)M * kz;
+    double* h = HS + kx + (long long)LH * (long long)M * kz;
+    const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+    const bool zero = (q == 0);
+    const double b = g.acph[1] + shift;
+    const double c = zero ? 0.0 : g.apph[1];
+    double2 r = s[0];
+    if (zero) r = make_double2(0.0, 0.0);
+    double hp = c / b;
+    double2 gp = make_double2(r.x / b, r.y / b);
+    h[0] = hp;
+    s[0] = gp;
+    for (int j = 2; j <= M; ++j) {
+        const double a = g.amph[j];
+        const double pp = 1.0 / ((g.acph[j] + shift) - hp * a);
+        const double2 rj = s[(j - 1) * js];
+        gp = make_double2((rj.x - a * gp.x) * pp, (rj.y - a * gp.y) * pp);
+        hp = j < M ? g.apph[j] * pp : 0.0;
+        h[(j - 1) * js] = hp;
+        s[(j - 1) * js] = gp;
+    }
+    double2 xn = gp;
+    for (int j = M - 1; j >= 1; --j) {
+        const double hj = h[(j - 1) * js];
+        const double2 gj = s[(j - 1) * js];
+        xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
+        s[(j - 1) * js] = xn;
+    }
+}
+
+// ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(PX_NT) k_fftx_inv(Geo g, const double2* __restrict__ SP, double* __restrict__ DPH) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, LH = g.LH;

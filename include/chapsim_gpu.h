@@ -287,6 +287,26 @@ int chapsim_thermal_use_mlp(chapsim_ctx_t* ctx, int32_t enable);
  * steps and switches back to the table when it exceeds its bound. */
 int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err);
 
+/* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
+
+/* Times the two Poisson y-solve variants on this context's grid, the warp
+ * Thomas/PCR hybrid (choice 0) and the reference's sequential Thomas
+ * recurrence, one thread per mode (choice 1), and keeps the faster for the
+ * context's steps (force = -1), or the one forced (0 or 1).  ms[2] (may be
+ * NULL) receives their mean durations. */
+int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
+
+/* An ensemble of independent periodic channels (any grids and precisions, one
+ * device) advanced together: one CUDA graph per step holds every member's
+ * kernels as parallel branches, so small members fill the GPU together.
+ * Members keep their own dt; each step of chapsim_batch_advance is the
+ * members' chapsim_advance_tg step. */
+typedef struct chapsim_batch chapsim_batch_t;
+int chapsim_batch_create(chapsim_ctx_t* const* ctxs, int32_t n, chapsim_batch_t** out);
+int chapsim_batch_advance(chapsim_batch_t* batch, int32_t nsteps, double dt0, double dtmin, double cflgv);
+int chapsim_batch_get_stream(chapsim_batch_t* batch, void** stream);
+int chapsim_batch_destroy(chapsim_batch_t* batch);
+
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
  * with a CUDA event after every kernel; ms[slot] receives the summed
  * duration of kernel slot `slot` of a step.  Slot order: k_cfl,

@@ -1,0 +1,90 @@
+"""Ensembles of uneven periodic channels and the y-solve autotuner.
+
+* Both Poisson y-solve variants (warp Thomas/PCR hybrid, sequential Thomas)
+  solve the FFT99 problem to 1e-12 of the oracle, and the step with either
+  stays within 1e-11 after 10 steps.
+* An ensemble (one graph per step, one branch per member) advances every
+  member exactly as its own graph does: fields bitwise equal.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import Oracle
+from chapsim import gpu
+from chapsim.mesh import channel_setup
+from chapsim.fields import initial_field
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_ysolve_variants_match_oracle(kind):
+    L, M, N = 96, 64, 64
+    s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    o = Oracle(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    c = gpu.ChannelTG(s)
+    choice, ms = c.autotune(force=kind)
+    assert choice == kind and ms["warp_pcr"] > 0 and ms["sequential"] > 0
+    rhs = np.random.default_rng(3).standard_normal((N, M, L))
+    full = np.zeros((N, M + 2, L))
+    full[:, 1:M + 1, :] = rhs
+    ref = o.poisson(full)
+    got = c.FFT99_POIS3D_periodicxz(rhs)
+    assert rel(got[:, 1:M + 1], ref[:, 1:M + 1]) <= 1e-12
+    Q, PR = initial_field(s, 1973, 0.1)
+    o.set_fields(Q, PR)
+    c.upload(Q, PR)
+    o.set_dt(2e-3)
+    c.set_dt(2e-3)
+    o.substep(0)
+    c.SOLVERRK3_MOM_tg(0)
+    o2 = Oracle(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0, DT0=2e-3, threads=8)
+    Qo, PRo, H0o = o.get_fields()
+    o2.set_fields(Qo, PRo, H0o)
+    o2.set_dt(2e-3)
+    o2.run_steps(10)
+    c.advance(10, 2e-3, 1e-6, 0.5)
+    Qg, _ = c.download()
+    Qo, _, _ = o2.get_fields()
+    for i in range(3):
+        assert rel(Qg[i][:, 1:M + 1], Qo[i][:, 1:M + 1]) <= 1e-11
+    c.close()
+
+
+GRIDS = [(64, 64, 64, 2 * math.pi, math.pi, 2800.0), (96, 64, 96, 2 * math.pi, math.pi, 4000.0),
+         (128, 96, 64, 4 * math.pi, 2 * math.pi / 3, 5000.0), (64, 128, 96, 2 * math.pi, math.pi, 6875.0)]
+
+
+def _member(k, g, precision="fp64"):
+    L, M, N, HX, HZ, REN = g
+    s = channel_setup(L, M, N, HX, HZ, 2.0, REN)
+    Q, PR = initial_field(s, 100 + k, 0.1)
+    c = gpu.ChannelTG(s, precision=precision)
+    c.upload(Q, PR)
+    c.set_dt(1e-3)
+    c.SOLVERRK3_MOM_tg(0)
+    return c
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ensemble_equals_individual_runs(precision):
+    solo = [_member(k, g, precision) for k, g in enumerate(GRIDS)]
+    grp = [_member(k, g, precision) for k, g in enumerate(GRIDS)]
+    for c in solo:
+        c.advance(6, 0.02, 1e-6, 0.5)
+    ens = gpu.Ensemble(grp)
+    ens.advance(6, 0.02, 1e-6, 0.5)
+    for a, b in zip(solo, grp):
+        Qa, Pa = a.download()
+        Qb, Pb = b.download()
+        assert np.array_equal(Qa, Qb) and np.array_equal(Pa, Pb)
+        assert a.get_dt() == b.get_dt()
+    ens.close()
+    for c in solo + grp:
+        c.close()
