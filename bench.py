@@ -40,6 +40,27 @@ WORKLOADS = {
     "channel384x256x384_retau395_fp64": (384, 256, 384, 2 * math.pi, math.pi, 2.0, 6875.0, 0.05, 0.5),
 }
 DEFAULT_WORKLOAD = "channel128_retau180_fp64"
+ENSEMBLE_WORKLOAD = "ensemble12_uneven"
+
+
+def ensemble_members(seed=2025, n=12):
+    """Twelve periodic channels of uneven size (64^3 .. 192 x 128 x 192, domain
+    2pi x 2 x pi), Re_tau drawn uniformly from 180-395 and converted to REN by
+    Dean's correlation Re_tau = 0.09 (2 Re_b)^0.88; seeds base + member."""
+    rng = np.random.default_rng(seed)
+    xs, ys = [64, 96, 128, 192], [64, 96, 128]
+    out = []
+    for c in range(n):
+        L, N = int(rng.choice(xs)), int(rng.choice(xs))
+        M = int(rng.choice(ys))
+        if c == 0:
+            L, M, N = 64, 64, 64
+        if c == n - 1:
+            L, M, N = 192, 128, 192
+        re_tau = float(rng.uniform(180.0, 395.0))
+        ren = (re_tau / 0.09) ** (1.0 / 0.88) / 2.0
+        out.append((L, M, N, 2 * math.pi, math.pi, 2.0, ren, seed + c))
+    return out
 L2_BYTES = 126 * 1024 * 1024
 
 # algorithmic FP64 words per grid point moved by one launch of each kernel
@@ -205,6 +226,81 @@ def run_reference(args):
     return 0
 
 
+def run_ensemble(args):
+    """Config 5: the members advanced together (one graph per step, one branch per
+    member) against the same members advanced one after another."""
+    from chapsim import gpu
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    members = ensemble_members(2025 + 100 * rank)
+    DT0, DTMIN, CFLGV = 0.05, 1e-6, 0.5
+
+    def build():
+        chans = []
+        for (L, M, N, HX, HZ, STR2, REN, seed) in members:
+            s = channel_setup(L, M, N, HX, HZ, STR2, REN)
+            Q, PR = initial_field(s, seed, 0.1)
+            c = gpu.ChannelTG(s, device=local, precision=args.precision)
+            c.upload(Q, PR)
+            c.set_dt(1e-3)
+            c.SOLVERRK3_MOM_tg(0)
+            chans.append(c)
+        return chans
+
+    pts = sum(L * M * N for (L, M, N, *_r) in members)
+    # sequential: each member's own graph, one after another
+    seq = build()
+    tune = [c.autotune() for c in seq]
+    for c in seq:
+        c.advance(args.warmup, DT0, DTMIN, CFLGV)
+    torch.cuda.synchronize(local)
+    t0 = time.perf_counter()
+    for c in seq:
+        c.advance(args.steps, DT0, DTMIN, CFLGV)
+    torch.cuda.synchronize(local)
+    t_seq = time.perf_counter() - t0
+    for c in seq:
+        c.close()
+    # batched: one graph per step over all members
+    grp = build()
+    for c, (choice, _ms) in zip(grp, tune):
+        c.autotune(force=choice)
+    ens = gpu.Ensemble(grp)
+    ens.advance(args.warmup, DT0, DTMIN, CFLGV)
+    stream = torch.cuda.ExternalStream(ens.stream_handle(), device=local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(local)
+    launches0 = sum(c.launch_count() for c in grp)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        ens.advance(args.steps, DT0, DTMIN, CFLGV)
+        ev1.record(stream)
+        torch.cuda.synchronize(local)
+    ms = ev0.elapsed_time(ev1)
+    launches = sum(c.launch_count() for c in grp) - launches0
+    value = pts * args.steps / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": ENSEMBLE_WORKLOAD, "members": [[L, M, N, round(REN, 1)] for (L, M, N, _a, _b, _c, REN, _s)
+                                                               in members],
+                   "precision": args.precision, "total_points": pts,
+                   "ysolve_choice": [t[0] for t in tune], "l2": "no flush: members total %.0f MB" % (pts * 8 * 20 / 1e6)},
+        "sequential": {"value": pts * args.steps / t_seq, "unit": UNIT, "ms_per_step": 1000.0 * t_seq / args.steps,
+                       "timing": "wall clock around the members' own graph replays, one member after another"},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    line["speedup_vs_sequential"] = line["value"] / line["sequential"]["value"]
+    print(json.dumps(line), flush=True)
+    ens.close()
+    for c in grp:
+        c.close()
+    return 0
+
+
 def run_b200(args):
     from chapsim import gpu
     ws, rank, local = dist_setup()
@@ -337,7 +433,7 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + [ENSEMBLE_WORKLOAD])
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -345,7 +441,13 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
+        if args.workload == ENSEMBLE_WORKLOAD:
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement is timed on the single-channel "
+                                                                  "workloads only"}))
+            return 0
         return run_reference(args)
+    if args.workload == ENSEMBLE_WORKLOAD:
+        return run_ensemble(args)
     return run_b200(args)
 
 
