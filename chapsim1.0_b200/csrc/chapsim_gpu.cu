@@ -23,9 +23,11 @@
 #include <algorithm>
 
 // x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
-__global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
+template <int N1, int N2>
+__global__ void __launch_bounds__(PX_NT, 2) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, LH = g.LH;
+    const int LD = fft4s_ld(L);
     const int j0 = 1 + blockIdx.x * PX_TJ;
     const int k = blockIdx.y;
     const int nj = min(PX_TJ, M - j0 + 1);
@@ -34,15 +36,14 @@ __global__ void __launch_bounds__(PX_NT) k_fftx_from_rhs(Geo g, const double* __
         const int jl = p / L, i = p - jl * L;
         const int pair = jl >> 1, part = jl & 1;
         const double val = jl < nj ? RHSLL[iidx(g, i, j0 + jl, k)] : 0.0;
-        double2* line = smc + pair * L;
-        const int pos = g.permx[i];
-        if (part == 0) line[pos].x = val; else line[pos].y = val;
+        double2* line = smc + pair * LD;
+        if (part == 0) line[i].x = val; else line[i].y = val;
     }
-    block_fft<-1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    block_fft4s<N1, N2, -1>(smc, np, LD, g.twx);
     const double sc = 0.5 / (double)L;
     for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
         const int pair = p / LH, kx = p - pair * LH;
-        const double2* line = smc + pair * L;
+        const double2* line = smc + pair * LD;
         const double2 z = line[kx];
         const double2 zc = line[kx == 0 ? 0 : L - kx];
         const int ja = j0 + 2 * pair;
@@ -151,7 +152,6 @@ struct chapsim_ctx {
     DevState* st_host = nullptr;  // pinned mirror for readback
     double* ybuf = nullptr;       // device copies of y-arrays and wavenumbers
     double2* tw = nullptr;
-    int* perm = nullptr;
     int domain = 1;               // 1: periodic TG channel, 2: main domain (IO)
     IoFields io{};                // IO-path arrays (domain 2)
     int io_grid = 0;              // blocks of the IO point-wise kernels
@@ -201,31 +201,6 @@ int fail(chapsim_ctx* c, int code, const std::string& msg) {
             return fail(ctx, CHAPSIM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-bool factor23(int n, std::vector<int>& rad) {
-    rad.clear();
-    int m = n;
-    while (m % 4 == 0) { rad.push_back(4); m /= 4; }
-    while (m % 2 == 0) { rad.push_back(2); m /= 2; }
-    while (m % 3 == 0) { rad.push_back(3); m /= 3; }
-    return m == 1 && rad.size() <= 8;
-}
-
-// position of input element j for the in-place DIT with pass order rad[0..]
-std::vector<int> dit_perm(int n, const std::vector<int>& rad) {
-    std::vector<int> perm(n);
-    for (int j = 0; j < n; ++j) {
-        int rem = j, mult = n, p = 0;
-        for (int i = (int)rad.size() - 1; i >= 0; --i) {
-            int t = rem % rad[i];
-            rem /= rad[i];
-            mult /= rad[i];
-            p += t * mult;
-        }
-        perm[j] = p;
-    }
-    return perm;
-}
-
 std::vector<double2> twiddles(int n) {
     std::vector<double2> w(n);
     const long double pi = 3.141592653589793238462643383279502884L;
@@ -240,8 +215,28 @@ std::vector<double2> twiddles(int n) {
 template <typename R> size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(R); }
 template <typename R> size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(R); }
 template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
-size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * g.L) * sizeof(double2); }
-size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * (g.N + 1)) * sizeof(double2); }
+size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * fft4s_ld(g.L)) * sizeof(double2); }
+size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(double2); }
+
+// twiddles of the small DFTs inside the four-step FFT (constant memory, shared by all contexts)
+cudaError_t upload_small_twiddles() {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    double2 w[24];
+    const int sizes[4] = {8, 12, 16, 24};
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < 4 && e == cudaSuccess; ++s) {
+        const int P = sizes[s];
+        for (int q = 0; q < P; ++q) {
+            const long double a = 2.0L * pi * (long double)q / (long double)P;
+            w[q] = make_double2((double)cosl(a), (double)(-sinl(a)));
+        }
+        if (P == 8) e = cudaMemcpyToSymbol(c_w8, w, sizeof(double2) * 8);
+        if (P == 12) e = cudaMemcpyToSymbol(c_w12, w, sizeof(double2) * 12);
+        if (P == 16) e = cudaMemcpyToSymbol(c_w16, w, sizeof(double2) * 16);
+        if (P == 24) e = cudaMemcpyToSymbol(c_w24, w, sizeof(double2) * 24);
+    }
+    return e;
+}
 size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(double2) + (size_t)g.M * sizeof(double); }
 
 // forward declaration: DISPATCH_S is defined below
@@ -315,7 +310,7 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R>, smem_rhs<R>(g))));
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R>, smem_z<R>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
-    CK(set_smem(k_div_fftx<R>, smem_px(g)));
+    DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px(g))));
     return CHAPSIM_OK;
 }
 
@@ -323,10 +318,12 @@ int configure_kernels(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     int rc = ctx->prec == CHAPSIM_PREC_MIXED ? configure_momentum<float>(ctx) : configure_momentum<double>(ctx);
     if (rc) return rc;
-    CK(set_smem(k_fftx_inv, smem_px(g)));
+    DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2>, smem_px(g))));
+    DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
+    DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S>, smem_yw(g))));
-    CK(set_smem(k_fftz<-1>, smem_fz(g)));
-    CK(set_smem(k_fftz<+1>, smem_fz(g)));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2>, smem_fz(g))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2>, smem_fz(g))));
     return CHAPSIM_OK;
 }
 
@@ -383,17 +380,17 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     DISPATCH_S(g.M / 32, (k_ysweep<S, R><<<gry, SWEEP_NT, smem_y<R>(g), s>>>(g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    k_div_fftx<R><<<grp, PX_NT, smem_px(g), s>>>(g, f.Q, f.RHSLL, ctx->SP, ctx->st, ns);
+    DISPATCH_FFT(g.L, (k_div_fftx<R, FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, f.Q, f.RHSLL, ctx->SP, ctx->st, ns)));
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     prof_mark(ctx);
     launch_ysolve(ctx);
     prof_mark(ctx);
-    k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     prof_mark(ctx);
-    k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     prof_mark(ctx);
     const long long tot = (long long)g.L * g.M * g.N;
     k_correct<R><<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
@@ -497,18 +494,19 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     k_io_massflux<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
     prof_mark(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    k_io_div_fftx<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP, ctx->st, ns,
-                                                 ctx->thermal ? ctx->tf.DRHO : nullptr);
+    DISPATCH_FFT(g.L, (k_io_div_fftx<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP,
+                                                                            ctx->st, ns,
+                                                                            ctx->thermal ? ctx->tf.DRHO : nullptr)));
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     prof_mark(ctx);
     launch_ysolve(ctx);
     prof_mark(ctx);
-    k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     prof_mark(ctx);
-    k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     prof_mark(ctx);
     k_io_correct<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns);
     prof_mark(ctx);
@@ -571,9 +569,9 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     if (L < 32 || M < 32 || N < 32 || L % 32 || M % 32 || N % 32 || !valid_S(L / 32) || !valid_S(M / 32) ||
         !valid_S(N / 32))
         return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");
-    std::vector<int> radx, radz;
-    if (!factor23(L, radx) || !factor23(N, radz))
-        return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1 and NCL3 must factor into 2s and 3s");
+    int n1_, n2_;
+    if (!fft4s_split(L, n1_, n2_) || !fft4s_split(N, n1_, n2_))
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1 and NCL3 must be one of 32, 64, 96, 128, 192, 256, 384");
     if (!cf->dyfi || !cf->dyci || !cf->ycl2nd_wff || !cf->ycl2nd_wfb || !cf->amph || !cf->acph || !cf->apph ||
         !cf->amvr || !cf->acvr || !cf->apvr || !cf->ak1 || !cf->ak3)
         return fail(nullptr, CHAPSIM_ERR_BADARG, "missing coefficient array");
@@ -647,19 +645,11 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     g.ak1 = yd + 13 * YS; g.ak3 = yd + 13 * YS + L;
     // FFT plans
     std::vector<double2> twx = twiddles(L), twz = twiddles(N);
-    std::vector<int> px = dit_perm(L, radx), pz = dit_perm(N, radz);
+    INIT_CK(upload_small_twiddles());
     INIT_CK(cudaMalloc(&ctx->tw, (size_t)(L + N) * sizeof(double2)));
     INIT_CK(cudaMemcpy(ctx->tw, twx.data(), L * sizeof(double2), cudaMemcpyHostToDevice));
     INIT_CK(cudaMemcpy(ctx->tw + L, twz.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
-    INIT_CK(cudaMalloc(&ctx->perm, (size_t)(L + N) * sizeof(int)));
-    INIT_CK(cudaMemcpy(ctx->perm, px.data(), L * sizeof(int), cudaMemcpyHostToDevice));
-    INIT_CK(cudaMemcpy(ctx->perm + L, pz.data(), N * sizeof(int), cudaMemcpyHostToDevice));
-    g.twx = ctx->tw; g.twz = ctx->tw + L; g.permx = ctx->perm; g.permz = ctx->perm + L;
-    g.nradx = (int)radx.size(); g.nradz = (int)radz.size();
-    for (int i = 0; i < 8; ++i) {
-        g.radx[i] = i < g.nradx ? radx[i] : 0;
-        g.radz[i] = i < g.nradz ? radz[i] : 0;
-    }
+    g.twx = ctx->tw; g.twz = ctx->tw + L;
     // fields
     INIT_CK(cudaMalloc(&ctx->Q, (size_t)(3 * g.FS) * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->PR, (size_t)g.FS * sizeof(double)));
@@ -736,7 +726,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
     cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
-    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->perm);
+    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
@@ -895,13 +885,13 @@ int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph) {
     // copy of the x-transform path that reads it instead of Q
     CK(cudaMemcpyAsync(ctx->RHSLL, rhs, (size_t)g.FI * sizeof(double), cudaMemcpyHostToDevice, s));
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    k_fftx_from_rhs<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->RHSLL, ctx->SP);
+    DISPATCH_FFT(g.L, (k_fftx_from_rhs<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->RHSLL, ctx->SP)));
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    k_fftz<-1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     launch_ysolve(ctx);
-    k_fftz<+1><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP);
-    k_fftx_inv<<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH);
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     ctx->launches += 5;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dph, ctx->DPH, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -56,13 +56,9 @@ struct Geo {
     const double* ak1;   // [L]  modified wavenumbers in x, 0-based kx
     const double* ak3;   // [N]  modified wavenumbers in z, 0-based kz
     double tgam[4], troh[4], talp[4];
-    // FFT plans
+    // FFT twiddles
     const double2* twx;  // [L] exp(-2 pi i e / L)
     const double2* twz;  // [N]
-    const int* permx;    // [L] digit-reversal permutation for the in-place DIT
-    const int* permz;    // [N]
-    int radx[8], nradx;
-    int radz[8], nradz;
 };
 
 __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {

@@ -289,11 +289,13 @@ __global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const 
 
 // DIVG_io + forward x transform (same tiling as k_div_fftx)
 // DRHO: DrhoDtP of the thermal solver, or NULL (zero) while it is off
-__global__ void __launch_bounds__(PX_NT) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
+template <int N1, int N2>
+__global__ void __launch_bounds__(PX_NT, 2) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
                                                        double2* __restrict__ SP, const DevState* __restrict__ st, int ns,
                                                        const double* __restrict__ DRHO) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, N = g.N, LH = g.LH;
+    const int LD = fft4s_ld(L);
     const int j0 = 1 + blockIdx.x * PX_TJ;
     const int k = blockIdx.y;
     const int nj = min(PX_TJ, M - j0 + 1);
@@ -319,15 +321,14 @@ __global__ void __launch_bounds__(PX_NT) k_io_div_fftx(Geo g, const double* __re
             val = DQ * coe0;
             RHSLL[iidx(g, i, j, k)] = val;
         }
-        double2* line = smc + pair * L;
-        const int pos = g.permx[i];
-        if (part == 0) line[pos].x = val; else line[pos].y = val;
+        double2* line = smc + pair * LD;
+        if (part == 0) line[i].x = val; else line[i].y = val;
     }
-    block_fft<-1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    block_fft4s<N1, N2, -1>(smc, np, LD, g.twx);
     const double sc = 0.5 / (double)L;
     for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
         const int pair = p / LH, kx = p - pair * LH;
-        const double2* line = smc + pair * L;
+        const double2* line = smc + pair * LD;
         const double2 z = line[kx];
         const double2 zc = line[kx == 0 ? 0 : L - kx];
         const int ja = j0 + 2 * pair;

@@ -31,11 +31,12 @@
 // ---------------------------------------------------------------------------
 // R is the stored type of Q, PR and RHSLLPHI (double, or float in the mixed-
 // precision step); divergence, transforms and correction are FP64 throughout.
-template <typename R>
-__global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
+template <typename R, int N1, int N2>
+__global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                     double2* __restrict__ SP, const DevState* __restrict__ st, int ns) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, N = g.N, LH = g.LH;
+    const int LD = fft4s_ld(L);
     const int j0 = 1 + blockIdx.x * PX_TJ;
     const int k = blockIdx.y;
     const int nj = min(PX_TJ, M - j0 + 1);
@@ -62,16 +63,15 @@ __global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const R* __restrict__
             val = dv * coe0;
             RHSLL[iidx(g, i, j, k)] = (R)val;
         }
-        double2* line = smc + pair * L;
-        const int pos = g.permx[i];
-        if (part == 0) line[pos].x = val; else line[pos].y = val;
+        double2* line = smc + pair * LD;
+        if (part == 0) line[i].x = val; else line[i].y = val;
     }
-    block_fft<-1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    block_fft4s<N1, N2, -1>(smc, np, LD, g.twx);
     // unpack: A_k = (Z_k + conj Z_{L-k}) / 2, B_k = (Z_k - conj Z_{L-k}) / (2i), both times 1/L
     const double sc = 0.5 / (double)L;
     for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
         const int pair = p / LH, kx = p - pair * LH;
-        const double2* line = smc + pair * L;
+        const double2* line = smc + pair * LD;
         const double2 z = line[kx];
         const double2 zc = line[kx == 0 ? 0 : L - kx];
         const double2 a = make_double2((z.x + zc.x) * sc, (z.y - zc.y) * sc);
@@ -84,24 +84,25 @@ __global__ void __launch_bounds__(PX_NT) k_div_fftx(Geo g, const R* __restrict__
 
 // ---------------------------------------------------------------------------
 // complex z transform of FZ_TQ consecutive (kx, j) lines (index q = kx + LH*(j-1))
-template <int SIGN>
-__global__ void __launch_bounds__(FZ_NT) k_fftz(Geo g, double2* __restrict__ SP) {
+template <int SIGN, int N1, int N2>
+__global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, double2* __restrict__ SP) {
     extern __shared__ double2 smc[];
     const int N = g.N;
+    const int LD = fft4s_ld(N);
     const long long Q = (long long)g.LH * g.M;
     const long long q0 = (long long)blockIdx.x * FZ_TQ;
     const int nq = (int)min((long long)FZ_TQ, Q - q0);
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
         const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
-        if (ql < nq) cp_async16(smc + ql * (N + 1) + g.permz[kz], SP + q0 + ql + Q * kz);
+        if (ql < nq) cp_async16(smc + ql * LD + kz, SP + q0 + ql + Q * kz);
     }
     cp_async_wait_all();
-    block_fft<SIGN>(smc, N, nq, N + 1, g.twz, g.radz, g.nradz);
+    block_fft4s<N1, N2, SIGN>(smc, nq, LD, g.twz);
     const double sc = SIGN < 0 ? 1.0 / (double)N : 1.0;
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
         const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
         if (ql < nq) {
-            double2 v = smc[ql * (N + 1) + kz];
+            double2 v = smc[ql * LD + kz];
             if (SIGN < 0) { v.x = v.x * sc; v.y = v.y * sc; }
             SP[q0 + ql + Q * kz] = v;
         }
@@ -247,9 +248,11 @@ __global__ void __launch_bounds__(YQ_NT) k_ysolve_seq(Geo g, double2* __restrict
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(PX_NT) k_fftx_inv(Geo g, const double2* __restrict__ SP, double* __restrict__ DPH) {
+template <int N1, int N2>
+__global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const double2* __restrict__ SP, double* __restrict__ DPH) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, LH = g.LH;
+    const int LD = fft4s_ld(L);
     const int j0 = 1 + blockIdx.x * PX_TJ;
     const int k = blockIdx.y;
     const int nj = min(PX_TJ, M - j0 + 1);
@@ -265,13 +268,13 @@ __global__ void __launch_bounds__(PX_NT) k_fftx_inv(Geo g, const double2* __rest
         double2 b = hasb ? SP[ks + (long long)LH * ((ja) + (long long)M * k)] : make_double2(0.0, 0.0);
         if (ks == 0 || 2 * ks == L) { a.y = 0.0; b.y = 0.0; }
         if (kk > L / 2) { a.y = -a.y; b.y = -b.y; }
-        smc[pair * L + g.permx[kk]] = make_double2(a.x - b.y, a.y + b.x);
+        smc[pair * LD + kk] = make_double2(a.x - b.y, a.y + b.x);
     }
-    block_fft<+1>(smc, L, np, L, g.twx, g.radx, g.nradx);
+    block_fft4s<N1, N2, +1>(smc, np, LD, g.twx);
     for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
         const int jl = p / L, i = p - jl * L;
         if (jl >= nj) continue;
-        const double2 z = smc[(jl >> 1) * L + i];
+        const double2 z = smc[(jl >> 1) * LD + i];
         DPH[pidx(g, i, j0 + jl, k)] = (jl & 1) ? z.y : z.x;
     }
 }

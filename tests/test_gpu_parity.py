@@ -87,7 +87,7 @@ def test_tdmaijj_noncyc_with_bc(n):
 
 
 # ----------------------------------------------------------------- Poisson
-@pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 192), (128, 96, 64), (32, 32, 32)])
+@pytest.mark.parametrize("shape", [(64, 64, 64), (96, 64, 192), (128, 96, 64), (32, 32, 32), (256, 32, 384), (384, 64, 256)])
 def test_fft99_poisson(shape):
     L, M, N = shape
     s = channel_setup(L, M, N, 4 * math.pi, 4 * math.pi / 3, 2.0, 2800.0)
