@@ -405,12 +405,14 @@ class ChannelTG:
 
 
     def autotune(self, force=-1):
-        """Picks the faster Poisson y-solve for this grid (or forces 0: warp hybrid,
-        1: sequential); returns (choice, {variant: ms})."""
+        """Keeps the faster y-solve and right-hand-side variants for this grid, or
+        forces them (bit 0: sequential y-solve, bit 1: split right-hand sides);
+        returns (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 2)()
+        ms = (ctypes.c_float * 4)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
-        return ch.value, {"warp_pcr": ms[0], "sequential": ms[1]}
+        return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
+                          "rhs_split": ms[3]}
 
 
 class Ensemble:

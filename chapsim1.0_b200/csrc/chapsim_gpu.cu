@@ -138,6 +138,7 @@ struct chapsim_ctx {
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr;
     double* HS = nullptr;         // forward factors of the sequential y-solve (allocated when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
+    int k1_split = 0;             // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep (chapsim_autotune)
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
@@ -215,6 +216,16 @@ std::vector<double2> twiddles(int n) {
 template <typename R> size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(R); }
 template <typename R> size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(R); }
 template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
+template <typename R> size_t smem_xs(const Geo& g) { return (size_t)((XS_NT / 32) * (g.L + 33)) * sizeof(R); }
+template <typename R> size_t smem_rt() { return (size_t)(RT_SLOTS * RT_SLOT) * sizeof(R); }
+// planes per k-chunk of the 2.5D right-hand-side kernel: enough blocks to fill
+// the GPU, at least 16 planes per chunk where N allows; always divides N
+int rt_chunk(const Geo& g) {
+    const int tiles = (g.L / RT_I) * (g.M / RT_J);
+    int chunk = g.N;
+    while (chunk % 2 == 0 && chunk / 2 >= 16 && tiles * (g.N / chunk) < 4 * 148) chunk /= 2;
+    return chunk;
+}
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * fft4s_ld(g.L)) * sizeof(double2); }
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(double2); }
 
@@ -310,6 +321,8 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R>, smem_rhs<R>(g))));
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R>, smem_z<R>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
+    DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
+    CK(set_smem(k_rhs_point<R>, smem_rt<R>()));
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px(g))));
     return CHAPSIM_OK;
 }
@@ -358,6 +371,26 @@ void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
     ctx->launches += 2;
 }
 
+// explicit right-hand sides and the x sweep, fused or split
+template <typename R>
+void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    if (ctx->k1_split) {
+        dim3 grt(g.L / RT_I, g.M / RT_J, g.N / rt_chunk(g));
+        k_rhs_point<R><<<grt, RP_NT, smem_rt<R>(), s>>>(g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, ns,
+                                                         rt_chunk(g));
+        const long long nl = 3LL * g.M * g.N;
+        const int nbx = (int)((nl + XS_NT / 32 - 1) / (XS_NT / 32));
+        DISPATCH_S(g.L / 32, (k_xsweep<S, R><<<nbx, XS_NT, smem_xs<R>(g), s>>>(g, f.RHS, fac)));
+        ctx->launches += 1;
+    } else {
+        const int grx = g.M * g.N / RHS_WPB;
+        DISPATCH_S(g.L / 32, (k_rhs_xsweep<S, R><<<grx, RHS_WPB * 32, smem_rhs<R>(g), s>>>(g, f.Q, f.PR, f.H0, f.RHS,
+                                                                                             ctx->part_rhs, ctx->st, fac, ns)));
+    }
+}
+
 template <typename R>
 void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     const Geo& g = ctx->g;
@@ -369,9 +402,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
         prof_mark(ctx);
         ctx->launches += 1;
     }
-    const int grx = g.M * g.N / RHS_WPB;
-    DISPATCH_S(g.L / 32, (k_rhs_xsweep<S, R><<<grx, RHS_WPB * 32, smem_rhs<R>(g), s>>>(g, f.Q, f.PR, f.H0, f.RHS,
-                                                                                         ctx->part_rhs, ctx->st, fac, ns)));
+    launch_rhs_x<R>(ctx, f, fac, ns);
     prof_mark(ctx);
     dim3 grz(g.L / 32, g.M, 3);
     DISPATCH_S(g.N / 32, (k_zsweep<S, R><<<grz, SWEEP_NT, smem_z<R>(g), s>>>(g, f.RHS, fac)));
@@ -1015,7 +1046,7 @@ int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count) {
 
 int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count) {
     if (!ctx || !count) return CHAPSIM_ERR_BADARG;
-    int per = 2 + 3 * (ctx->thermal ? 15 : 9);
+    int per = 2 + 3 * (ctx->thermal ? 15 : 9 + ctx->k1_split);
     *count = per;
     return CHAPSIM_OK;
 }
@@ -1576,10 +1607,45 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         t[kind] /= reps;
     }
     ctx->launches += 2 * (2 + reps);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     CK(cudaGetLastError());
-    ctx->ysolve_kind = force == 0 ? 0 : force == 1 ? 1 : (t[1] < t[0] ? 1 : 0);
+    ctx->ysolve_kind = force >= 0 ? (force & 1) : (t[1] < t[0] ? 1 : 0);
+    // explicit right-hand sides + x sweep: fused vs split (periodic channel).
+    // CONVH0 is state: kept in a temporary copy and restored afterwards.
+    float tk[2] = {0.f, 0.f};
+    if (ctx->domain == 1) {
+        const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
+        const size_t hb = (size_t)3 * g.FI * (mixed ? sizeof(float) : sizeof(double));
+        void* hsave = nullptr;
+        CK(cudaMalloc(&hsave, hb));
+        void* h0 = mixed ? (void*)ctx->H0f : (void*)ctx->H0;
+        CK(cudaMemcpyAsync(hsave, h0, hb, cudaMemcpyDeviceToDevice, s));
+        const int keep = ctx->k1_split;
+        for (int kind = 0; kind < 2; ++kind) {
+            ctx->k1_split = kind;
+            auto one = [&]() {
+                if (mixed) {
+                    StepFields<float> f = step_fields<float>(ctx);
+                    launch_rhs_x<float>(ctx, f, f.fac + 5 * FAC_SET, 1);
+                } else {
+                    StepFields<double> f = step_fields<double>(ctx);
+                    launch_rhs_x<double>(ctx, f, f.fac + 5 * FAC_SET, 1);
+                }
+            };
+            one();
+            CK(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; ++r) one();
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&tk[kind], e0, e1));
+            tk[kind] /= reps;
+        }
+        ctx->k1_split = keep;
+        CK(cudaMemcpyAsync(h0, hsave, hb, cudaMemcpyDeviceToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        cudaFree(hsave);
+        CK(cudaGetLastError());
+        ctx->k1_split = force >= 0 ? ((force >> 1) & 1) : (tk[1] < tk[0] ? 1 : 0);
+    }
     if (ctx->ysolve_kind == 0) {
         cudaFree(ctx->HS);
         ctx->HS = nullptr;
@@ -1588,8 +1654,10 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         cudaGraphExecDestroy(ctx->step_exec);
         ctx->step_exec = nullptr;
     }
-    if (choice) *choice = ctx->ysolve_kind;
-    if (ms) { ms[0] = t[0]; ms[1] = t[1]; }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (choice) *choice = ctx->ysolve_kind | (ctx->k1_split << 1);
+    if (ms) { ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; }
     return CHAPSIM_OK;
 }
 

@@ -356,3 +356,210 @@ __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : 3)) k_ysweep(Geo g, R*
         __syncthreads();
     }
 }
+
+// ---------------------------------------------------------------------------
+// Split form of k_rhs_xsweep: k_rhs_point computes the same right-hand sides
+// point by point (one thread per point, i fastest, every load independent and
+// no line-solve phase, so more warps keep loads in flight) and k_xsweep runs
+// the cyclic x sweeps line by line.  It moves 6 more words per point (RHS read
+// and written once more); the autotuner picks it where it is faster.
+constexpr int RP_NT = 256;
+constexpr int RT_I = 32, RT_J = 8;                  // tile of one block: 32 (i) x 8 (j) points per plane
+constexpr int RT_HI = RT_I + 2, RT_HJ = RT_J + 2;   // with its one-point halo
+constexpr int RT_PLANE = RT_HI * RT_HJ;             // values of one field in one plane
+constexpr int RT_SLOT = 4 * RT_PLANE + 3 * RT_I * RT_J;  // U, V, W, PR with halo, then CONVH0 x3 (tile only)
+constexpr int RT_AHEAD = 3;                         // planes in flight ahead of plane k+1
+constexpr int RT_SLOTS = RT_AHEAD + 2;              // planes k-1, k, k+1 in use, k+2 .. k+RT_AHEAD+1 arriving
+
+// 2.5D form: the block keeps planes k-1, k, k+1 of U, V, W and PR (tile +
+// halo) in a shared-memory ring and marches over a chunk of k; the next
+// RT_AHEAD planes are in flight (cp.async, one commit group per plane, empty
+// groups past the chunk end) while plane k is computed.  Every neighbour access
+// is a shared-memory hit and each Q / PR value is read from HBM about once
+// per block (plus the halo and the two extra planes of a chunk).
+template <typename R>
+__device__ __forceinline__ void rt_load_plane(const Geo& g, const R* __restrict__ Q, const R* __restrict__ PR,
+                                              const R* __restrict__ H0, R* slot, int i0, int j0, int k) {
+    for (int p = threadIdx.x; p < 4 * RT_PLANE; p += RP_NT) {
+        const int f = p / RT_PLANE, e = p - f * RT_PLANE;
+        const int jj = e / RT_HI, ii = e - jj * RT_HI;
+        int i = i0 - 1 + ii;
+        i = i < 0 ? i + g.L : (i >= g.L ? i - g.L : i);
+        const R* src = f == 3 ? PR : Q + (long long)f * g.FS;
+        cp_async_el(slot + p, src + pidx(g, i, j0 - 1 + jj, k));
+    }
+    // CONVH0 of the tile (row j = 1 of the v component is never read)
+    for (int p = threadIdx.x; p < 3 * RT_I * RT_J; p += RP_NT) {
+        const int c = p / (RT_I * RT_J), e = p - c * (RT_I * RT_J);
+        const int tj = e / RT_I, ti = e - tj * RT_I;
+        cp_async_el(slot + 4 * RT_PLANE + p, H0 + c * g.FI + iidx(g, i0 + ti, j0 + tj, k));
+    }
+}
+__device__ __forceinline__ void rt_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+
+template <typename R>
+__global__ void __launch_bounds__(RP_NT, sizeof(R) == 4 ? 3 : 2) k_rhs_point(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
+                                                        R* __restrict__ H0, R* __restrict__ RHS,
+                                                        double* __restrict__ partial, DevState* __restrict__ st,
+                                                        int ns, int kchunk) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R* ring = reinterpret_cast<R*>(sm_raw);   // [slot][field][jj][ii]
+    __shared__ double sred[32];
+    __shared__ int is_last;
+    const int L = g.L, M = g.M, N = g.N;
+    const int ti = threadIdx.x % RT_I, tj = threadIdx.x / RT_I;
+    const int i0 = blockIdx.x * RT_I, j0 = 1 + blockIdx.y * RT_J;
+    const int k0 = blockIdx.z * kchunk, k1 = min(N, k0 + kchunk);
+    const int i = i0 + ti, j = j0 + tj;
+    const int jp = j + 1;
+    const R dt = (R)st->dt;
+    const R tg = (R)g.tgam[ns], tr = (R)g.troh[ns], ta = (R)g.talp[ns];
+    const R coev = ta * (R)g.cvisc;
+    const R coep = ta * dt;
+    const R dxi = (R)g.dxi, dzi = (R)g.dzi, dxqi = (R)g.dxqi, dzqi = (R)g.dzqi;
+    const R c1x = (R)(0.5 * 0.5 * g.dxi);
+    const R c3x = (R)(0.5 * 0.5 * g.dzi);
+    const R wffj = (R)g.wff[j], wfbj = (R)g.wfb[j], wffp = (R)g.wff[jp], wfbp = (R)g.wfb[jp];
+    const R dyfij = (R)g.dyfi[j], dycij = (R)g.dyci[j];
+    const double dyj = 1.0 / g.dyfi[j] / 1.0;
+    const R amu = (R)g.amvr[j], acu = (R)g.acvr[j], apu = (R)g.apvr[j];
+    const R amv = (R)g.amvr[(M + 2) + j], acv = (R)g.acvr[(M + 2) + j], apv = (R)g.apvr[(M + 2) + j];
+    const R amw = (R)g.amvr[2 * (M + 2) + j], acw = (R)g.acvr[2 * (M + 2) + j], apw = (R)g.apvr[2 * (M + 2) + j];
+    // plane kk of the march lives in slot (kk - k0 + 1) % RT_SLOTS; planes k0-1 ..
+    // k0+RT_AHEAD go in first, one commit group each
+    auto slot_of = [&](int kk) { return ring + ((kk - k0 + 1) % RT_SLOTS) * RT_SLOT; };
+    for (int kk = k0 - 1; kk <= k0 + RT_AHEAD; ++kk) {
+        if (kk <= k1) rt_load_plane<R>(g, Q, PR, H0, slot_of(kk), i0, j0, (kk % N + N) % N);
+        rt_commit();
+    }
+    const int c = (tj + 1) * RT_HI + (ti + 1);          // this point inside a plane
+    const int cim = c - 1, cip = c + 1, cjm = c - RT_HI, cjp = c + RT_HI;
+    double bulk = 0.0;
+    for (int k = k0; k < k1; ++k) {
+        // planes up to k+1 have landed when at most RT_AHEAD - 1 groups are pending
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(RT_AHEAD - 1) : "memory");
+        __syncthreads();
+        const R* Pm = slot_of(k - 1);   // plane k-1
+        const R* Pc = slot_of(k);       // plane k
+        const R* Pp = slot_of(k + 1);   // plane k+1
+        const R* Uc = Pc; const R* Vc = Pc + RT_PLANE; const R* Wc = Pc + 2 * RT_PLANE; const R* Rc = Pc + 3 * RT_PLANE;
+        const R* Um = Pm; const R* Vm = Pm + RT_PLANE; const R* Wm = Pm + 2 * RT_PLANE; const R* Rm = Pm + 3 * RT_PLANE;
+        const R* Up = Pp; const R* Vp = Pp + RT_PLANE; const R* Wp = Pp + 2 * RT_PLANE;
+        const R u = Uc[c], v = Vc[c], w = Wc[c];
+        const R uip = Uc[cip], uim = Uc[cim];
+        const R ujp = Uc[cjp], ujm = Uc[cjm], ukp = Up[c], ukm = Um[c];
+        const R vip = Vc[cip], vim = Vc[cim];
+        const R vjp = Vc[cjp], vjm = Vc[cjm], vkp = Vp[c], vkm = Vm[c];
+        const R wip = Wc[cip], wim = Wc[cim];
+        const R wjp = Wc[cjp], wjm = Wc[cjm], wkp = Wp[c], wkm = Wm[c];
+        const R pc = Rc[c];
+        const R pim = Rc[cim], pjm = Rc[cjm], pkm = Rm[c];
+        const R vjpim = Vc[cjp - 1], wkpim = Wp[cim];
+        const R ujmip = Uc[cjm + 1], wjmkp = Wp[cjm];
+        const R ukmip = Um[cip], vjpkm = Vm[cjp];
+        const long long ii = iidx(g, i, j, k);
+        const R* Hc = Pc + 4 * RT_PLANE + threadIdx.x;
+        const R h0u = Hc[0];
+        const R h0v = j >= 2 ? Hc[RT_I * RT_J] : R(0);
+        const R h0w = Hc[2 * RT_I * RT_J];
+        R Hu, Hv = R(0), Hw, ru, rv = R(0), rw;
+        {
+            const R H11 = ((uip + u) * (uip + u) - (uim + u) * (uim + u)) * c1x;
+            const R H12 = ((vjp + vjpim) * (wffp * ujp + wfbp * u) - (v + vim) * (wffj * u + wfbj * ujm)) * (dyfij * R(0.5));
+            const R H13 = ((wkp + wkpim) * (ukp + u) - (w + wim) * (u + ukm)) * c3x;
+            Hu = -(H11 + H12 + H13);
+            const R rhsc = tg * Hu + tr * h0u;
+            const R rhsl = coev * ((uip - R(2) * u + uim) * dxqi + (ukp - R(2) * u + ukm) * dzqi +
+                                   (ujp * apu + u * acu + ujm * amu));
+            R rr = (rhsc + rhsl) * dt;
+            ru = rr - (pc - pim) * dxi * coep;
+            bulk += (double)ru * dyj;
+        }
+        if (j >= 2) {
+            const R H21 = ((wffj * uip + wfbj * ujmip) * (vip + v) - (wffj * u + wfbj * ujm) * (v + vim)) * (dxi * R(0.5));
+            const R H22 = ((vjp + v) * (vjp + v) - (v + vjm) * (v + vjm)) * (dycij * R(0.5) * R(0.5));
+            const R H23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v) - (wffj * w + wfbj * wjm) * (v + vkm)) * (dzi * R(0.5));
+            Hv = -(H21 + H22 + H23);
+            const R rhsc = tg * Hv + tr * h0v;
+            const R rhsl = coev * ((vip - R(2) * v + vim) * dxqi + (vkp - R(2) * v + vkm) * dzqi +
+                                   (vjp * apv + v * acv + vjm * amv));
+            R rr = (rhsc + rhsl) * dt;
+            rv = rr - (pc - pjm) * dycij * coep;
+        }
+        {
+            const R H31 = ((uip + ukmip) * (wip + w) - (u + ukm) * (w + wim)) * c1x;
+            const R H32 = ((vjp + vjpkm) * (wffp * wjp + wfbp * w) - (v + vkm) * (wffj * w + wfbj * wjm)) * (dyfij * R(0.5));
+            const R H33 = ((wkp + w) * (wkp + w) - (w + wkm) * (w + wkm)) * c3x;
+            Hw = -(H31 + H32 + H33);
+            const R rhsc = tg * Hw + tr * h0w;
+            const R rhsl = coev * ((wip - R(2) * w + wim) * dxqi + (wkp - R(2) * w + wkm) * dzqi +
+                                   (wjp * apw + w * acw + wjm * amw));
+            R rr = (rhsc + rhsl) * dt;
+            rw = rr - (pc - pkm) * dzi * coep;
+        }
+        H0[ii] = Hu;
+        H0[ii + 2 * g.FI] = Hw;
+        RHS[ii] = ru;
+        RHS[ii + 2 * g.FI] = rw;
+        if (j >= 2) {
+            H0[ii + g.FI] = Hv;
+            RHS[ii + g.FI] = rv;
+        }
+        __syncthreads();   // plane k-1's slot is free: plane k+RT_AHEAD+1 goes there
+        const int kn = k + RT_AHEAD + 1;
+        if (kn <= k1) rt_load_plane<R>(g, Q, PR, H0, slot_of(kn), i0, j0, kn % N);
+        rt_commit();
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // grid sum of the bulk-flux integrand: block partials, last block in index order
+    bulk = block_sum<RP_NT>(bulk, sred);
+    const int nblk = gridDim.x * gridDim.y * gridDim.z;
+    const int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    if (threadIdx.x == 0) {
+        partial[bid] = bulk;
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->ctr, 1u);
+        is_last = (prev == (unsigned)nblk - 1);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        double sum = 0.0;
+        for (int t = threadIdx.x; t < nblk; t += RP_NT) sum += __ldcg(partial + t);
+        sum = block_sum<RP_NT>(sum, sred);
+        if (threadIdx.x == 0) {
+            st->bulksum = sum;
+            st->ctr = 0u;
+        }
+    }
+}
+
+// cyclic x sweeps (MOMFA1_X_tg): one warp per (component, j, k) line, staged
+// in segment-padded shared memory with coalesced loads and stores
+constexpr int XS_NT = 256;
+template <int S, typename R>
+__global__ void __launch_bounds__(XS_NT) k_xsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
+    R* sm = reinterpret_cast<R*>(sm_raw);
+    const int L = 32 * S, M = g.M;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long line = (long long)blockIdx.x * (XS_NT / 32) + warp;
+    const long long nlines = 3LL * M * g.N;
+    if (line >= nlines) return;
+    const int comp = (int)(line / ((long long)M * g.N));
+    const long long r = line - (long long)comp * M * g.N;
+    const int j = 1 + (int)(r % M), k = (int)(r / M);
+    if (comp == 1 && j == 1) return;  // MOMFA1_X_tg starts at N2I = 2 for v
+    R* base = RHS + comp * g.FI + iidx(g, 0, j, k);
+    R* sl = sm + warp * (L + 33);
+    R v[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) v[q] = base[lane + 32 * q];
+#pragma unroll
+    for (int q = 0; q < S; ++q) sl[seg_pos<S>(lane + 32 * q)] = v[q];
+    __syncwarp();
+    warp_tdma_apply_smem<S, true>(sl, fac + FSET_X * FAC_SET, lane);
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < S; ++q) base[lane + 32 * q] = sl[seg_pos<S>(lane + 32 * q)];
+}

@@ -289,11 +289,16 @@ int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err);
 
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
-/* Times the two Poisson y-solve variants on this context's grid, the warp
- * Thomas/PCR hybrid (choice 0) and the reference's sequential Thomas
- * recurrence, one thread per mode (choice 1), and keeps the faster for the
- * context's steps (force = -1), or the one forced (0 or 1).  ms[2] (may be
- * NULL) receives their mean durations. */
+/* Times the alternative kernels of the step on this context's grid and keeps
+ * the faster of each pair (force = -1), or the ones forced (force = 0..3):
+ *   bit 0: Poisson y-solve, 0 = warp Thomas/PCR hybrid, 1 = the reference's
+ *          sequential Thomas recurrence, one thread per mode;
+ *   bit 1: explicit right-hand sides + x sweep, 0 = fused (one warp per x
+ *          line), 1 = split into a point-wise kernel and a line-sweep kernel
+ *          (periodic channel only).
+ * choice receives the kept setting in the same bit form; ms[4] (may be NULL)
+ * the mean durations of y-solve (hybrid, sequential) and right-hand sides
+ * (fused, split).  CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 
 /* An ensemble of independent periodic channels (any grids and precisions, one
