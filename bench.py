@@ -251,7 +251,7 @@ def run_ensemble(args):
     pts = sum(L * M * N for (L, M, N, *_r) in members)
     # sequential: each member's own graph, one after another
     seq = build()
-    tune = [c.autotune() for c in seq]
+    tune = [c.autotune(force=args.tune) for c in seq]
     for c in seq:
         c.advance(args.warmup, DT0, DTMIN, CFLGV)
     torch.cuda.synchronize(local)
@@ -323,7 +323,8 @@ def run_b200(args):
     ch.upload(Q0, PR0)
     ch.set_dt(DT0)
     ch.SOLVERRK3_MOM_tg(0)
-    tuned, tune_ms = ch.autotune()  # keeps the faster y-solve and right-hand-side variants for this grid
+    # keeps the faster y-solve and right-hand-side variants for this grid; --tune pins them instead
+    tuned, tune_ms = ch.autotune(force=args.tune)
     # warm-up (also captures the step graph)
     ch.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)
     stream = torch.cuda.ExternalStream(ch.stream_handle(), device=local)
@@ -415,6 +416,33 @@ def run_b200(args):
         "kernel_ms_per_step": {k: kms[k] / prof_steps for k in sorted(kms)},
         "clocks": clk.summary(),
     }
+    if args.precision == "fp64" and not args.no_variants:
+        # the same workload in mixed precision (FP32 stencils / CN sweeps, FP64 Poisson and projection)
+        ch.close()
+        chm = gpu.ChannelTG(s, device=local, precision="mixed")
+        chm.upload(Q0, PR0)
+        chm.set_dt(DT0)
+        chm.SOLVERRK3_MOM_tg(0)
+        mt, _ = chm.autotune(force=args.tune)
+        chm.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)
+        sm_ = torch.cuda.ExternalStream(chm.stream_handle(), device=local)
+        barrier()
+        ev0.record(sm_)
+        chm.advance(args.steps, DT0, DTMIN, CFLGV)
+        ev1.record(sm_)
+        torch.cuda.synchronize(local)
+        msm = ev0.elapsed_time(ev1)
+        if dist is not None:
+            t = torch.tensor([msm], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            msm = float(t.item())
+        vm = pts * args.steps * ws / (msm / 1000.0)
+        line["variants"] = {"mixed": {"value": vm, "unit": UNIT, "ms_per_step": msm / args.steps,
+                                      "speedup_vs_fp64": vm / value, "max_div": chm.DIVGCK_tg(),
+                                      "autotuned_choice_bits": mt,
+                                      "precision": "FP32 storage, stencils and CN sweeps; FP64 Poisson, projection, "
+                                                   "bulk sums"}}
+        ch = chm
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, n, dt = cpu_reference_rate(wl, 1000, float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)
@@ -439,6 +467,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-variants", action="store_true", help="skip the mixed-precision comparison of an FP64 run")
+    ap.add_argument("--tune", type=int, default=-1,
+                    help="kernel variant bits instead of timing them (bit 0: sequential y-solve, bit 1: split "
+                         "right-hand side); -1 times both variants and keeps the faster")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
