@@ -60,7 +60,7 @@ class Coefs(ctypes.Structure):
                 ("dyfi", _dp), ("dyci", _dp), ("ycl2nd_wff", _dp), ("ycl2nd_wfb", _dp), ("amph", _dp),
                 ("acph", _dp), ("apph", _dp), ("amvr", _dp), ("acvr", _dp), ("apvr", _dp), ("ak1", _dp),
                 ("ak3", _dp), ("tgam", ctypes.c_double * 4), ("troh", ctypes.c_double * 4),
-                ("talp", ctypes.c_double * 4)]
+                ("talp", ctypes.c_double * 4), ("amvr1", ctypes.c_double), ("apvrn", ctypes.c_double)]
 
 
 class PropTableC(ctypes.Structure):
@@ -75,7 +75,10 @@ PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("fix_v_wall_row", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 5)]
+                ("ivisscheme", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+
+
+VIS_EXPLICIT, VIS_IMPLICIT = 0, 1
 
 
 _lib = None
@@ -191,10 +194,12 @@ class ChannelTG:
 
     IDOMAIN = 1
 
-    def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False, precision: str = "fp64"):
+    def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False, precision: str = "fp64",
+                 ivisscheme: int = VIS_EXPLICIT):
         """precision: "fp64" (every field and operation in FP64) or "mixed" (FP32
         velocity/pressure storage, stencils and CN sweeps; FP64 Poisson solve,
-        projection and bulk-flux sums)."""
+        projection and bulk-flux sums).  ivisscheme: iVisScheme of the main
+        domain (0 explicit, 1 Crank-Nicolson); the TG domain accepts 0 only."""
         self.lib = load_library()
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
@@ -221,9 +226,9 @@ class ChannelTG:
                    setup.iFlowDriven, 0, _ptr(k["dyfi"]), _ptr(k["dyci"]), _ptr(k["wff"]), _ptr(k["wfb"]),
                    _ptr(k["amph"]), _ptr(k["acph"]), _ptr(k["apph"]), _ptr(k["amvr"]), _ptr(k["acvr"]),
                    _ptr(k["apvr"]), _ptr(k["ak1"]), _ptr(k["ak3"]), (ctypes.c_double * 4)(*setup.TGAM),
-                   (ctypes.c_double * 4)(*setup.TROH), (ctypes.c_double * 4)(*setup.TALP))
+                   (ctypes.c_double * 4)(*setup.TROH), (ctypes.c_double * 4)(*setup.TALP), setup.AMVR1, setup.APVRN)
         g = Grid(L, M, N, 1, self.IDOMAIN)
-        o = Opts(device, int(bool(fix_v_wall_row)), PRECISIONS[precision])
+        o = Opts(device, int(bool(fix_v_wall_row)), PRECISIONS[precision], int(ivisscheme))
         h = ctypes.c_void_p()
         rc = self.lib.chapsim_gpu_init(ctypes.byref(g), ctypes.byref(cf), ctypes.byref(o), ctypes.byref(h))
         if rc != 0:
@@ -453,7 +458,8 @@ class Ensemble:
 
 class ChannelIO(ChannelTG):
     """Device-resident x-periodic main-domain channel (CHAPSim IO domain) with
-    explicit viscous terms and fixed property fields.
+    explicit (``ivisscheme=0``) or Crank-Nicolson (``ivisscheme=1``) viscous
+    terms; property fields fixed, or updated by the thermal solver.
 
     ``G`` is numpy (3, N, M+2, L) = Fortran ``G_io(L, 0:M+1, N, 3)`` (rho*u);
     ``RHO``, ``MU0``, ``MU`` are (N, M+2, L) = ``DENSITY0``, ``Viscousity0``,

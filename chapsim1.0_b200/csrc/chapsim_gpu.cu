@@ -16,6 +16,7 @@
 #include "poisson.cuh"
 #include "tdma.cuh"
 #include "io.cuh"
+#include "io_cn.cuh"
 #include "thermo.cuh"
 #include "thermal.cuh"
 #include "mlp.cuh"
@@ -154,6 +155,7 @@ struct chapsim_ctx {
     double* ybuf = nullptr;       // device copies of y-arrays and wavenumbers
     double2* tw = nullptr;
     int domain = 1;               // 1: periodic TG channel, 2: main domain (IO)
+    int ivis = 0;                 // main domain: 0 explicit viscous terms, 1 Crank-Nicolson (iVisScheme)
     IoFields io{};                // IO-path arrays (domain 2)
     int io_grid = 0;              // blocks of the IO point-wise kernels
     cudaGraphExec_t step_exec = nullptr;
@@ -337,6 +339,11 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S>, smem_yw(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2>, smem_fz(g))));
+    if (ctx->domain == 2 && ctx->ivis) {
+        DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S>, smem_cn(g.L))));
+        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S>, smem_cn(g.N))));
+        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S>, smem_cn(g.M))));
+    }
     return CHAPSIM_OK;
 }
 
@@ -518,12 +525,26 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     cudaStream_t s = ctx->stream;
     if (ctx->thermal) launch_thermal_substep(ctx, ns);
     IoFields f = io_fields(ctx);
-    k_io_divu<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
-    prof_mark(ctx);
-    k_io_rhs<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
-    prof_mark(ctx);
-    k_io_massflux<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
-    prof_mark(ctx);
+    if (!ctx->ivis) {
+        k_io_divu<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+        prof_mark(ctx);
+        k_io_rhs<false><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
+        prof_mark(ctx);
+        k_io_massflux<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
+        prof_mark(ctx);
+    } else {
+        // VISCOUS_PAR_EXPLT_* + RHS_MOM_EXPLICIT_io, then MOMFA_io's sweeps for all components
+        k_io_rhs<true><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
+        prof_mark(ctx);
+        dim3 gx((unsigned)((g.M * (long long)g.N + CN_LINES - 1) / CN_LINES), 3);
+        DISPATCH_S(g.L / 32, (k_io_cn_xsweep<S><<<gx, CN_NT, smem_cn(g.L), s>>>(g, f, ctx->st, ns)));
+        prof_mark(ctx);
+        dim3 gz(g.L / CN_LINES, g.M, 3), gy(g.L / CN_LINES, g.N, 3);
+        DISPATCH_S(g.N / 32, (k_io_cn_zsweep<S><<<gz, CN_NT, smem_cn(g.N), s>>>(g, f, ctx->st, ns)));
+        DISPATCH_S(g.M / 32, (k_io_cn_ysweep<S><<<gy, CN_NT, smem_cn(g.M), s>>>(g, f, ctx->st, ns)));
+        prof_mark(ctx);
+        ctx->launches += 1;
+    }
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
     DISPATCH_FFT(g.L, (k_io_div_fftx<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP,
                                                                             ctx->st, ns,
@@ -539,7 +560,7 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     prof_mark(ctx);
-    k_io_correct<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns);
+    k_io_correct<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, ctx->ivis ? ctx->RHSLL : nullptr);
     prof_mark(ctx);
     ctx->launches += 9;
 }
@@ -613,10 +634,20 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         return fail(nullptr, CHAPSIM_ERR_BADARG, "precision must be CHAPSIM_PREC_FP64 or CHAPSIM_PREC_MIXED");
     if (prec == CHAPSIM_PREC_MIXED && grid->idomain != 1)
         return fail(nullptr, CHAPSIM_ERR_BADARG, "the mixed-precision step is available for the periodic TG domain only");
+    const int ivis = opts ? opts->ivisscheme : CHAPSIM_VIS_EXPLICIT;
+    if (ivis != CHAPSIM_VIS_EXPLICIT && ivis != CHAPSIM_VIS_IMPLICIT)
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "ivisscheme must be CHAPSIM_VIS_EXPLICIT or CHAPSIM_VIS_IMPLICIT");
+    if (ivis == CHAPSIM_VIS_IMPLICIT && grid->idomain != 2)
+        return fail(nullptr, CHAPSIM_ERR_BADARG,
+                    "ivisscheme selects the main-domain (iDomain = 2) scheme; the TG domain is always Crank-Nicolson");
+    if (ivis == CHAPSIM_VIS_IMPLICIT && !(cf->amvr1 > 0.0 && cf->apvrn > 0.0 && std::isfinite(cf->amvr1) &&
+                                          std::isfinite(cf->apvrn)))
+        return fail(nullptr, CHAPSIM_ERR_BADARG, "the Crank-Nicolson main domain needs AMVR1 and APVRN (TDMA_COEF)");
     ctx = new chapsim_ctx();
     ctx->device = opts ? opts->device : 0;
     ctx->domain = grid->idomain;
     ctx->prec = prec;
+    ctx->ivis = ivis;
     int rc;
 #define INIT_CK(call)                                  \
     do {                                               \
@@ -639,6 +670,8 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     g.cvisc = cf->cvisc; g.volm = cf->volm; g.cf_given = cf->cf_given; g.iflowdriven = cf->iflowdriven;
     g.fix_v_wall_row = opts ? opts->fix_v_wall_row : 0;
     for (int s = 0; s < 4; ++s) { g.tgam[s] = cf->tgam[s]; g.troh[s] = cf->troh[s]; g.talp[s] = cf->talp[s]; }
+    g.amvr1 = ivis == CHAPSIM_VIS_IMPLICIT ? cf->amvr1 : 0.0;
+    g.apvrn = ivis == CHAPSIM_VIS_IMPLICIT ? cf->apvrn : 0.0;
     // y arrays with the reference's 1-based index (entry 0 unused)
     const int YS = M + 2;
     std::vector<double> yb((size_t)YS * 13 + L + N, 0.0);

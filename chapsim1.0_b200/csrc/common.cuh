@@ -56,6 +56,7 @@ struct Geo {
     const double* ak1;   // [L]  modified wavenumbers in x, 0-based kx
     const double* ak3;   // [N]  modified wavenumbers in z, 0-based kz
     double tgam[4], troh[4], talp[4];
+    double amvr1, apvrn;  // wall-row factors of the Crank-Nicolson y sweep of the main domain
     // FFT twiddles
     const double2* twx;  // [L] exp(-2 pi i e / L)
     const double2* twz;  // [N]

@@ -1,11 +1,12 @@
-// Main-domain (IO, x-periodic) substep with explicit viscous terms:
-// SOLVERRK3_MOM_io (src/SOLVERRK3_MOM_IO.f90:11-120, iVisScheme = 0) for a
+// Main-domain (IO, x-periodic) substep, SOLVERRK3_MOM_io
+// (src/SOLVERRK3_MOM_IO.f90:11-120) with explicit (iVisScheme = 0) or
+// Crank-Nicolson (iVisScheme = 1, sweeps in io_cn.cuh) viscous terms, for a
 // flow whose property fields (DENSITY0, Viscousity0, Viscousity) are given
 // and held fixed unless the thermal solver (thermal.cuh) updates them.
 //
 //   k_io_props     DENSITY_Staggered + MU_Staggered (src/MASSFLUX_CALC_IO.f90:155-329), once per upload
 //   k_io_divu      DIVG_U_io (src/DIVG.f90:140-246): DivU = div(u)/3
-//   k_io_rhs       CONVECTION_X/Y/Z_io, VISCOUS_ALL_EXPLT_X/Y/Z_io, RHS_MOM_EXPLICIT_io
+//   k_io_rhs<CN>   CONVECTION_X/Y/Z_io, VISCOUS_ALL_EXPLT_X/Y/Z_io (or VISCOUS_PAR_EXPLT_*), RHS_MOM_EXPLICIT_io
 //                  (RK combination, EXPLT0 update, pressure gradient, grid sum of the
 //                  bulk-forcing integrand), one thread per point and all components
 //   k_io_massflux  bulk forcing subtraction + MASSFLUX_CALC_io (G += RHS)
@@ -14,7 +15,7 @@
 //                  discrete problem of FISHPACK_POIS3D_SIMPLE (same AMPH/ACPH/APPH operator
 //                  and x/z eigenvalues); its singular kx = kz = 0 mode is fixed at
 //                  phi_hat(y_1) = 0, which shifts DPH and PR by a constant only
-//   k_io_correct   PRCALC_io (explicit: PR += DPH), MASSFLUX_UPDATE_io
+//   k_io_correct   PRCALC_io (PR += DPH, minus BE*RHSLLPHI under CN), MASSFLUX_UPDATE_io
 //                  (src/VELO_CORRECTION.f90:103-179), VELOCITY_CALC_io (Q = G/D_STG)
 //   k_io_cfl       CFL_io (src/CFL.f90:55-107), including the viscous number
 #pragma once
@@ -102,6 +103,22 @@ __global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFields f) {
 }
 
 // ---------------------------------------------------------------------------
+// CONVECTION_X/Y/Z_io + the viscous terms + RHS_MOM_EXPLICIT_io, all three
+// components per point.
+//   CN = false (VisExplicit): VISCOUS_ALL_EXPLT_X/Y/Z_io, RHS = RK combination.
+//   CN = true  (VisImplicit): VISCOUS_PAR_EXPLT_X/Y/Z_io
+//     (src/VISCOUS_X_EXPLICIT_io.f90:131-293, VISCOUS_Y_EXPLICIT_io.f90:278-443,
+//     VISCOUS_Z_EXPLICIT_io.f90:300-465): the explicit part joins the
+//     convection term, the implicit part enters with alpha*dt
+//     (RHS_MOM_EXPLICIT_io.f90:87-99).  The density-correction part
+//     (DIVU_io, weight alpha*dt/2) is identically zero: it differentiates
+//     G * DRHOI_STG, and DRHOI_STG = 1/D_STG - 1/(the same average of
+//     DENSITY0) is 0 in every entry because DENSITY_IMPLICIT_add runs right
+//     after DENSITY_Staggered on the same DENSITY0 (src/SOLVE.f90:123-127,
+//     src/MASSFLUX_CALC_IO.f90:332-416), and 0 before that (MEMALLOCT.f90:209).
+//     It is therefore not computed.  The v row j = 1 is left unwritten; the
+//     Crank-Nicolson sweeps treat it as zero.
+template <bool CN>
 __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st,
                                                   int ns) {
     __shared__ double sred[32];
@@ -114,6 +131,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __r
     const double* G = f.G;
     const double* Q = f.Q;
     const double* U0 = f.MU0;
+    const double* U = f.MU;
     const double* MS = f.MST;
     const double* DV = f.DIVU;
     const double* PR = f.PR;
@@ -129,8 +147,8 @@ __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __r
         const long long ckp = pidx(g, i, j, kp), ckm = pidx(g, i, j, km);
         const double wffj = g.wff[j], wfbj = g.wfb[j], wffp = g.wff[jp], wfbp = g.wfb[jp];
         const double dyfij = g.dyfi[j], dycij = g.dyci[j], dycip = g.dyci[jp];
-        // -------- x momentum: CONVECTION_X_io + VISCOUS_ALL_EXPLT_X_io --------
-        double ex1, ex2 = 0.0, ex3;
+        // -------- x momentum: CONVECTION_X_io + viscous terms --------
+        double ex1, ex2 = 0.0, ex3, im1 = 0.0, im2 = 0.0, im3 = 0.0;
         {
             const double H11F = (G[cip] + G[c]) * (Q[cip] + Q[c]);
             const double H11B = (G[c] + G[cim]) * (Q[c] + Q[cim]);
@@ -141,27 +159,61 @@ __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __r
             const double H13F = (G[ckp + 2 * FS] + G[pidx(g, im, j, kp) + 2 * FS]) * (Q[ckp] + Q[c]);
             const double H13B = (G[c + 2 * FS] + G[cim + 2 * FS]) * (Q[c] + Q[ckm]);
             const double H13 = (H13F - H13B) * ((g.dzi * 0.5 * 0.5) * 1.0);
-            double DUDX = (Q[cip] - Q[c]) * g.dxi;
-            const double T11F = 0.5 * (U0[c] + U0[c]) * (DUDX - DV[c]);
-            DUDX = (Q[c] - Q[cim]) * g.dxi;
-            const double T11B = 0.5 * (U0[cim] + U0[cim]) * (DUDX - DV[cim]);
-            const double D11 = (T11F - T11B) * (2.0 * g.dxi * cv);
-            double DUDY = (Q[cjp] - Q[c]) * dycip / 1.0;
-            double DVDX = (Q[cjp + FS] - Q[pidx(g, im, jp, k) + FS]) * g.dxi;
-            const double T12F = MS[cjp] * (DUDY + DVDX);
-            DUDY = (Q[c] - Q[cjm]) * dycij / 1.0;
-            DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
-            const double T12B = MS[c] * (DUDY + DVDX);
-            const double D12 = (T12F - T12B) * (dyfij * cv * 1.0);
-            double DUDZ = (Q[ckp] - Q[c]) * g.dzi;
-            double DWDX = (Q[ckp + 2 * FS] - Q[pidx(g, im, j, kp) + 2 * FS]) * g.dxi;
-            const double T13F = MS[ckp + FS] * (DUDZ + DWDX);
-            DUDZ = (Q[c] - Q[ckm]) * g.dzi;
-            DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
-            const double T13B = MS[c + FS] * (DUDZ + DWDX);
-            const double D13 = (T13F - T13B) * ((g.dzi * cv) * 1.0);
             ex1 = -(H11 + H12 + H13);
-            ex1 = ex1 + D11 + D12 + D13;
+            if constexpr (!CN) {
+                double DUDX = (Q[cip] - Q[c]) * g.dxi;
+                const double T11F = 0.5 * (U0[c] + U0[c]) * (DUDX - DV[c]);
+                DUDX = (Q[c] - Q[cim]) * g.dxi;
+                const double T11B = 0.5 * (U0[cim] + U0[cim]) * (DUDX - DV[cim]);
+                const double D11 = (T11F - T11B) * (2.0 * g.dxi * cv);
+                double DUDY = (Q[cjp] - Q[c]) * dycip / 1.0;
+                double DVDX = (Q[cjp + FS] - Q[pidx(g, im, jp, k) + FS]) * g.dxi;
+                const double T12F = MS[cjp] * (DUDY + DVDX);
+                DUDY = (Q[c] - Q[cjm]) * dycij / 1.0;
+                DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
+                const double T12B = MS[c] * (DUDY + DVDX);
+                const double D12 = (T12F - T12B) * (dyfij * cv * 1.0);
+                double DUDZ = (Q[ckp] - Q[c]) * g.dzi;
+                double DWDX = (Q[ckp + 2 * FS] - Q[pidx(g, im, j, kp) + 2 * FS]) * g.dxi;
+                const double T13F = MS[ckp + FS] * (DUDZ + DWDX);
+                DUDZ = (Q[c] - Q[ckm]) * g.dzi;
+                DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
+                const double T13B = MS[c + FS] * (DUDZ + DWDX);
+                const double D13 = (T13F - T13B) * ((g.dzi * cv) * 1.0);
+                ex1 = ex1 + D11 + D12 + D13;
+            } else {
+                const double coe1 = -2.0 / 3.0 * g.dxi * cv;
+                double DUDX = (Q[cip] - Q[c]) * g.dxi;
+                double DVDY = (Q[cjp + FS] - Q[c + FS]) * dyfij * 1.0;
+                double DWDZ = (Q[ckp + 2 * FS] - Q[c + 2 * FS]) * g.dzi * 1.0;
+                const double F_EX11 = U[c] * (DVDY + DWDZ), F_IM11 = U[c] * DUDX;
+                DUDX = (Q[c] - Q[cim]) * g.dxi;
+                DVDY = (Q[pidx(g, im, jp, k) + FS] - Q[cim + FS]) * dyfij * 1.0;
+                DWDZ = (Q[pidx(g, im, j, kp) + 2 * FS] - Q[cim + 2 * FS]) * g.dzi * 1.0;
+                const double B_EX11 = U[cim] * (DVDY + DWDZ), B_IM11 = U[cim] * DUDX;
+                const double D11_EX = (F_EX11 - B_EX11) * coe1;
+                const double D11_IM = (F_IM11 - B_IM11) * coe1 * (-2.0);
+                const double coe2 = dyfij * cv * 1.0;
+                double DVDX = (Q[cjp + FS] - Q[pidx(g, im, jp, k) + FS]) * g.dxi;
+                double DUDY = (Q[cjp] - Q[c]) * dycip / 1.0;
+                const double F_EX12 = MS[cjp] * DVDX, F_IM12 = MS[cjp] * DUDY;
+                DUDY = (Q[c] - Q[cjm]) * dycij / 1.0;
+                DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
+                const double B_EX12 = MS[c] * DVDX, B_IM12 = MS[c] * DUDY;
+                const double D12_EX = (F_EX12 - B_EX12) * coe2;
+                const double D12_IM = (F_IM12 - B_IM12) * coe2;
+                const double coe32 = (g.dzi * cv) * 1.0;
+                double DUDZ = (Q[ckp] - Q[c]) * g.dzi;
+                double DWDX = (Q[ckp + 2 * FS] - Q[pidx(g, im, j, kp) + 2 * FS]) * g.dxi;
+                const double F_EX13 = MS[ckp + FS] * DWDX, F_IM13 = MS[ckp + FS] * DUDZ;
+                DUDZ = (Q[c] - Q[ckm]) * g.dzi;
+                DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
+                const double B_EX13 = MS[c + FS] * DWDX, B_IM13 = MS[c + FS] * DUDZ;
+                const double D13_EX = (F_EX13 - B_EX13) * coe32;
+                const double D13_IM = (F_IM13 - B_IM13) * coe32;
+                ex1 = D11_EX + D12_EX + D13_EX + ex1;
+                im1 = D11_IM + D12_IM + D13_IM;
+            }
         }
         // -------- y momentum (j >= 2) --------
         if (j >= 2) {
@@ -174,27 +226,61 @@ __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __r
             const double H23F = (wffj * G[ckp + 2 * FS] * 1.0 + wfbj * G[pidx(g, i, jm, kp) + 2 * FS] * 1.0) * (Q[ckp + FS] + Q[c + FS]);
             const double H23B = (wffj * G[c + 2 * FS] * 1.0 + wfbj * G[cjm + 2 * FS] * 1.0) * (Q[c + FS] + Q[ckm + FS]);
             const double H23 = (H23F - H23B) * ((g.dzi * 0.5) * 1.0);
-            double DVDY = (Q[cjp + FS] - Q[c + FS]) * dyfij;
-            const double T22F = 0.5 * (U0[c] + U0[c]) * (DVDY - DV[c]);
-            DVDY = (Q[c + FS] - Q[cjm + FS]) * g.dyfi[jm];
-            const double T22B = 0.5 * (U0[cjm] + U0[cjm]) * (DVDY - DV[cjm]);
-            const double D22 = (T22F - T22B) * (2.0 * dycij * cv);
-            double DVDX = (Q[cip + FS] - Q[c + FS]) * g.dxi;
-            double DUDY = (Q[cip] - Q[pidx(g, ip, jm, k)]) * dycij;
-            const double T21F = MS[cip] * (DVDX + DUDY);
-            DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
-            DUDY = (Q[c] - Q[cjm]) * dycij;
-            const double T21B = MS[c] * (DVDX + DUDY);
-            const double D21 = (T21F - T21B) * (g.dxi * cv);
-            double DVDZ = (Q[ckp + FS] - Q[c + FS]) * g.dzi;
-            double DWDY = (Q[ckp + 2 * FS] - Q[pidx(g, i, jm, kp) + 2 * FS]) * dycij;
-            const double T23F = MS[ckp + 2 * FS] * (DVDZ + DWDY);
-            DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
-            DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
-            const double T23B = MS[c + 2 * FS] * (DVDZ + DWDY);
-            const double D23 = (T23F - T23B) * (g.dzi * cv);
             ex2 = -(H21 + H22 + H23);
-            ex2 = ex2 + D21 + D22 + D23;
+            if constexpr (!CN) {
+                double DVDY = (Q[cjp + FS] - Q[c + FS]) * dyfij;
+                const double T22F = 0.5 * (U0[c] + U0[c]) * (DVDY - DV[c]);
+                DVDY = (Q[c + FS] - Q[cjm + FS]) * g.dyfi[jm];
+                const double T22B = 0.5 * (U0[cjm] + U0[cjm]) * (DVDY - DV[cjm]);
+                const double D22 = (T22F - T22B) * (2.0 * dycij * cv);
+                double DVDX = (Q[cip + FS] - Q[c + FS]) * g.dxi;
+                double DUDY = (Q[cip] - Q[pidx(g, ip, jm, k)]) * dycij;
+                const double T21F = MS[cip] * (DVDX + DUDY);
+                DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
+                DUDY = (Q[c] - Q[cjm]) * dycij;
+                const double T21B = MS[c] * (DVDX + DUDY);
+                const double D21 = (T21F - T21B) * (g.dxi * cv);
+                double DVDZ = (Q[ckp + FS] - Q[c + FS]) * g.dzi;
+                double DWDY = (Q[ckp + 2 * FS] - Q[pidx(g, i, jm, kp) + 2 * FS]) * dycij;
+                const double T23F = MS[ckp + 2 * FS] * (DVDZ + DWDY);
+                DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
+                DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
+                const double T23B = MS[c + 2 * FS] * (DVDZ + DWDY);
+                const double D23 = (T23F - T23B) * (g.dzi * cv);
+                ex2 = ex2 + D21 + D22 + D23;
+            } else {
+                const double coe2 = -2.0 / 3.0 * dycij * cv;
+                double DUDX = (Q[cip] - Q[c]) * g.dxi;
+                double DVDY = (Q[cjp + FS] - Q[c + FS]) * dyfij;
+                double DWDZ = (Q[ckp + 2 * FS] - Q[c + 2 * FS]) * g.dzi;
+                const double F_EX22 = U[c] * (DUDX + DWDZ), F_IM22 = U[c] * DVDY;
+                DUDX = (Q[pidx(g, ip, jm, k)] - Q[cjm]) * g.dxi;
+                DVDY = (Q[c + FS] - Q[cjm + FS]) * g.dyfi[jm];
+                DWDZ = (Q[pidx(g, i, jm, kp) + 2 * FS] - Q[cjm + 2 * FS]) * g.dzi;
+                const double B_EX22 = U[cjm] * (DUDX + DWDZ), B_IM22 = U[cjm] * DVDY;
+                const double D22_EX = (F_EX22 - B_EX22) * coe2;
+                const double D22_IM = (F_IM22 - B_IM22) * coe2 * (-2.0);
+                const double coe1 = g.dxi * cv;
+                double DVDX = (Q[cip + FS] - Q[c + FS]) * g.dxi;
+                double DUDY = (Q[cip] - Q[pidx(g, ip, jm, k)]) * dycij;
+                const double F_EX21 = MS[cip] * DUDY, F_IM21 = MS[cip] * DVDX;
+                DVDX = (Q[c + FS] - Q[cim + FS]) * g.dxi;
+                DUDY = (Q[c] - Q[cjm]) * dycij;
+                const double B_EX21 = MS[c] * DUDY, B_IM21 = MS[c] * DVDX;
+                const double D21_EX = (F_EX21 - B_EX21) * coe1;
+                const double D21_IM = (F_IM21 - B_IM21) * coe1;
+                const double coe3 = g.dzi * cv;
+                double DVDZ = (Q[ckp + FS] - Q[c + FS]) * g.dzi;
+                double DWDY = (Q[ckp + 2 * FS] - Q[pidx(g, i, jm, kp) + 2 * FS]) * dycij;
+                const double F_EX23 = MS[ckp + 2 * FS] * DWDY, F_IM23 = MS[ckp + 2 * FS] * DVDZ;
+                DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
+                DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
+                const double B_EX23 = MS[c + 2 * FS] * DWDY, B_IM23 = MS[c + 2 * FS] * DVDZ;
+                const double D23_EX = (F_EX23 - B_EX23) * coe3;
+                const double D23_IM = (F_IM23 - B_IM23) * coe3;
+                ex2 = D21_EX + D22_EX + D23_EX + ex2;
+                im2 = D21_IM + D22_IM + D23_IM;
+            }
         }
         // -------- z momentum --------
         {
@@ -207,35 +293,72 @@ __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __r
             const double H33F = (G[ckp + 2 * FS] + G[c + 2 * FS]) * (Q[ckp + 2 * FS] + Q[c + 2 * FS]);
             const double H33B = (G[c + 2 * FS] + G[ckm + 2 * FS]) * (Q[c + 2 * FS] + Q[ckm + 2 * FS]);
             const double H33 = (H33F - H33B) * ((g.dzi * 0.5 * 0.5) * 1.0);
-            double DWDZ = (Q[ckp + 2 * FS] - Q[c + 2 * FS]) * g.dzi;
-            const double T33F = 0.5 * (U0[c] + U0[c]) * (DWDZ - DV[c]);
-            DWDZ = (Q[c + 2 * FS] - Q[ckm + 2 * FS]) * g.dzi;
-            const double T33B = 0.5 * (U0[ckm] + U0[ckm]) * (DWDZ - DV[ckm]);
-            const double D33 = (T33F - T33B) * (2.0 * g.dzi * cv);
-            double DWDX = (Q[cip + 2 * FS] - Q[c + 2 * FS]) * g.dxi;
-            double DUDZ = (Q[cip] - Q[pidx(g, ip, j, km)]) * g.dzi;
-            const double T31F = MS[cip + FS] * (DWDX + DUDZ);
-            DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
-            DUDZ = (Q[c] - Q[ckm]) * g.dzi;
-            const double T31B = MS[c + FS] * (DWDX + DUDZ);
-            const double D31 = (T31F - T31B) * (g.dxi * cv);
-            double DWDY = (Q[cjp + 2 * FS] - Q[c + 2 * FS]) * dycip;
-            double DVDZ = (Q[cjp + FS] - Q[pidx(g, i, jp, km) + FS]) * g.dzi;
-            const double T32F = MS[cjp + 2 * FS] * (DWDY + DVDZ);
-            DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
-            DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
-            const double T32B = MS[c + 2 * FS] * (DWDY + DVDZ);
-            const double D32 = (T32F - T32B) * (dyfij * cv);
             ex3 = -(H31 + H32 + H33);
-            ex3 = ex3 + D31 + D32 + D33;
+            if constexpr (!CN) {
+                double DWDZ = (Q[ckp + 2 * FS] - Q[c + 2 * FS]) * g.dzi;
+                const double T33F = 0.5 * (U0[c] + U0[c]) * (DWDZ - DV[c]);
+                DWDZ = (Q[c + 2 * FS] - Q[ckm + 2 * FS]) * g.dzi;
+                const double T33B = 0.5 * (U0[ckm] + U0[ckm]) * (DWDZ - DV[ckm]);
+                const double D33 = (T33F - T33B) * (2.0 * g.dzi * cv);
+                double DWDX = (Q[cip + 2 * FS] - Q[c + 2 * FS]) * g.dxi;
+                double DUDZ = (Q[cip] - Q[pidx(g, ip, j, km)]) * g.dzi;
+                const double T31F = MS[cip + FS] * (DWDX + DUDZ);
+                DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
+                DUDZ = (Q[c] - Q[ckm]) * g.dzi;
+                const double T31B = MS[c + FS] * (DWDX + DUDZ);
+                const double D31 = (T31F - T31B) * (g.dxi * cv);
+                double DWDY = (Q[cjp + 2 * FS] - Q[c + 2 * FS]) * dycip;
+                double DVDZ = (Q[cjp + FS] - Q[pidx(g, i, jp, km) + FS]) * g.dzi;
+                const double T32F = MS[cjp + 2 * FS] * (DWDY + DVDZ);
+                DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
+                DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
+                const double T32B = MS[c + 2 * FS] * (DWDY + DVDZ);
+                const double D32 = (T32F - T32B) * (dyfij * cv);
+                ex3 = ex3 + D31 + D32 + D33;
+            } else {
+                const double coe3 = -2.0 / 3.0 * g.dzi * cv;
+                double DUDX = (Q[cip] - Q[c]) * g.dxi;
+                double DVDY = (Q[cjp + FS] - Q[c + FS]) * dyfij;
+                double DWDZ = (Q[ckp + 2 * FS] - Q[c + 2 * FS]) * g.dzi;
+                const double F_EX33 = U[c] * (DUDX + DVDY), F_IM33 = U[c] * DWDZ;
+                DUDX = (Q[pidx(g, ip, j, km)] - Q[ckm]) * g.dxi;
+                DVDY = (Q[pidx(g, i, jp, km) + FS] - Q[ckm + FS]) * dyfij;
+                DWDZ = (Q[c + 2 * FS] - Q[ckm + 2 * FS]) * g.dzi;
+                const double B_EX33 = U[ckm] * (DUDX + DVDY), B_IM33 = U[ckm] * DWDZ;
+                const double D33_EX = (F_EX33 - B_EX33) * coe3;
+                const double D33_IM = (F_IM33 - B_IM33) * coe3 * (-2.0);
+                const double coe1 = g.dxi * cv;
+                double DWDX = (Q[cip + 2 * FS] - Q[c + 2 * FS]) * g.dxi;
+                double DUDZ = (Q[cip] - Q[pidx(g, ip, j, km)]) * g.dzi;
+                const double F_EX31 = MS[cip + FS] * DUDZ, F_IM31 = MS[cip + FS] * DWDX;
+                DWDX = (Q[c + 2 * FS] - Q[cim + 2 * FS]) * g.dxi;
+                DUDZ = (Q[c] - Q[ckm]) * g.dzi;
+                const double B_EX31 = MS[c + FS] * DUDZ, B_IM31 = MS[c + FS] * DWDX;
+                const double D31_EX = (F_EX31 - B_EX31) * coe1;
+                const double D31_IM = (F_IM31 - B_IM31) * coe1;
+                const double coe2 = dyfij * cv;
+                double DWDY = (Q[cjp + 2 * FS] - Q[c + 2 * FS]) * dycip;
+                double DVDZ = (Q[cjp + FS] - Q[pidx(g, i, jp, km) + FS]) * g.dzi;
+                const double F_EX32 = MS[cjp + 2 * FS] * DVDZ, F_IM32 = MS[cjp + 2 * FS] * DWDY;
+                DWDY = (Q[c + 2 * FS] - Q[cjm + 2 * FS]) * dycij;
+                DVDZ = (Q[c + FS] - Q[ckm + FS]) * g.dzi;
+                const double B_EX32 = MS[c + 2 * FS] * DVDZ, B_IM32 = MS[c + 2 * FS] * DWDY;
+                const double D32_EX = (F_EX32 - B_EX32) * coe2;
+                const double D32_IM = (F_IM32 - B_IM32) * coe2;
+                ex3 = D31_EX + D32_EX + D33_EX + ex3;
+                im3 = D31_IM + D32_IM + D33_IM;
+            }
         }
         // -------- RHS_MOM_EXPLICIT_io --------
         const long long ii = iidx(g, i, j, k);
         const double e01 = f.EX0[ii], e02 = f.EX0[ii + g.FI], e03 = f.EX0[ii + 2 * g.FI];
         const double pc = PR[c], pim = PR[cim], pjm = PR[cjm], pkm = PR[ckm];
+        const double coa = ta * dt;
         double r1 = (tg * ex1 + tr * e01) * dt;
+        if constexpr (CN) r1 = r1 + coa * im1;
         r1 = r1 - (pc - pim) * (ta * dt * g.dxi);
         double r3 = (tg * ex3 + tr * e03) * dt;
+        if constexpr (CN) r3 = r3 + coa * im3;
         r3 = r3 - (pc - pkm) * (ta * dt * g.dzi);
         f.EX0[ii] = ex1;
         f.EX0[ii + 2 * g.FI] = ex3;
@@ -243,6 +366,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __r
         f.RHS[ii + 2 * g.FI] = r3;
         if (j >= 2) {
             double r2 = (tg * ex2 + tr * e02) * dt;
+            if constexpr (CN) r2 = r2 + coa * im2;
             r2 = r2 - (pc - pjm) * (ta * dt * dycij / 1.0);
             f.EX0[ii + g.FI] = ex2;
             f.RHS[ii + g.FI] = r2;
@@ -338,12 +462,16 @@ __global__ void __launch_bounds__(PX_NT, 2) k_io_div_fftx(Geo g, const double* _
     }
 }
 
-// PRCALC_io (explicit) + MASSFLUX_UPDATE_io + VELOCITY_CALC_io
+// PRCALC_io + MASSFLUX_UPDATE_io + VELOCITY_CALC_io.  RHSLL == NULL: the
+// explicit scheme's PR += DPH; otherwise the Crank-Nicolson scheme's
+// PR += DPH - BE * RHSLLPHI_io, BE = alpha*dt/(2 Re) (src/PRESSURE_CORRECTION.f90:113-123).
 __global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFields f, const double* __restrict__ DPH,
-                                                      const DevState* __restrict__ st, int ns) {
+                                                      const DevState* __restrict__ st, int ns,
+                                                      const double* __restrict__ RHSLL) {
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
     const double dt = st->dt, ta = g.talp[ns];
+    const double be = 0.50 * ta * dt * g.cvisc;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
@@ -354,7 +482,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFields f, const d
         const double phjm = j >= 2 ? DPH[pidx(g, i, j - 1, k)] : 0.0;
         const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS], pr = f.PR[c];
         const double d1 = f.DST[c], d2 = f.DST[c + g.FS], d3 = f.DST[c + 2 * g.FS];
-        const double pn = pr + ph;
+        const double pn = RHSLL ? pr + ph - be * RHSLL[iidx(g, i, j, k)] : pr + ph;
         f.PR[c] = pn;
         if (j == 1) f.PR[pidx(g, i, 0, k)] = pn;
         if (j == M) f.PR[pidx(g, i, M + 1, k)] = pn;

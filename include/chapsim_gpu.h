@@ -67,6 +67,9 @@ typedef struct {
     const double* ak1;           /* AK1(1:NCL1) (src/possion3d_FFT99.f90:180-198)*/
     const double* ak3;           /* AK3(1:NCL3)                                  */
     double tgam[4], troh[4], talp[4]; /* CONS_RKCOEF (src/CONS_RKCOEF.f90:25-51) */
+    double amvr1, apvrn;         /* AMVR1, APVRN wall-row factors of TDMA_COEF
+                                    (src/TDMA_COEF.f90:79-87); read only when
+                                    ivisscheme = CHAPSIM_VIS_IMPLICIT          */
 } chapsim_coefs_t;
 
 #define CHAPSIM_PREC_FP64 0  /* every field and operation in FP64 (the reference's precision) */
@@ -79,8 +82,14 @@ typedef struct {
     int32_t fix_v_wall_row;  /* 0: keep the reference's v-sweep row-1 input (the u increment of
                                 the same substep, MOMFA3_Y_tg); 1: zero it                      */
     int32_t precision;       /* CHAPSIM_PREC_FP64 (default) or CHAPSIM_PREC_MIXED (TG domain)  */
-    int32_t reserved[5];
+    int32_t ivisscheme;      /* iVisScheme of the main domain (iDomain = 2):
+                                CHAPSIM_VIS_EXPLICIT (default) or CHAPSIM_VIS_IMPLICIT          */
+    int32_t reserved[4];
 } chapsim_opts_t;
+
+#define CHAPSIM_VIS_EXPLICIT 0 /* VisExplicit: VISCOUS_ALL_EXPLT_* + MASSFLUX_CALC_io */
+#define CHAPSIM_VIS_IMPLICIT 1 /* VisImplicit: VISCOUS_PAR_EXPLT_* + MOMFA_io (Crank-Nicolson
+                                  sweeps with per-point coefficients) + PRCALC_io's CN form */
 
 /* Allocates the device fields and uploads coefficients.  Hooks in after
  * FFT99_POIS3D_INIT (src/DNS_THERMAL.f90:118-130). */
@@ -188,7 +197,8 @@ int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* g, const double* 
                              const double* mu0, const double* mu);
 /* g = G_io, q = Q_io (velocity), pr = PR_io; any may be NULL. */
 int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* g, double* q, double* pr);
-/* SOLVERRK3_MOM_io(NS) with the device-resident DT. */
+/* SOLVERRK3_MOM_io(NS) with the device-resident DT, in the viscous scheme
+ * chosen by chapsim_opts_t.ivisscheme (src/SOLVERRK3_MOM_IO.f90:43-79). */
 int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns);
 /* CFL_io (src/CFL.f90:55-107): CFLMM_io including the viscous number. */
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm);

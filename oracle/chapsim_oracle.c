@@ -59,6 +59,8 @@ typedef struct {
     int io;
     double *G, *EXPLT0, *RHO, *MU0, *MU, *DSTG, *MUSTG, *DIVU, *DRHODT;
     double* DEN; /* DENSITY; RHO holds DENSITY0 (equal while the thermal solver is off) */
+    int ivis;       /* iVisScheme: 0 explicit (VisExplicit), 1 Crank-Nicolson (VisImplicit) */
+    double* DRHOI;  /* DRHOI_STG(:,:,:,1:3) of DENSITY_IMPLICIT_add */
     double CFLMM_IO;
     /* thermal solver (orc_thermal_enable): SOLVERRK3_ENG_io with the table-search properties */
     int thermal;
@@ -315,7 +317,7 @@ void orc_destroy(orc_t* o) {
     free(o->Q); free(o->PR); free(o->CONVH0); free(o->QTMP); free(o->DPH); free(o->RHSLLPHI); free(o->RHS);
     free(o->SRe); free(o->SIm);
     free(o->G); free(o->EXPLT0); free(o->RHO); free(o->MU0); free(o->MU); free(o->DSTG); free(o->MUSTG);
-    free(o->DIVU); free(o->DRHODT); free(o->DEN);
+    free(o->DIVU); free(o->DRHODT); free(o->DEN); free(o->DRHOI);
     free(o->DH); free(o->ENTH); free(o->TEMP); free(o->KAPPA); free(o->HCP); free(o->RHSE); free(o->RHSE0); free(o->G0);
     free(o);
 }
@@ -973,6 +975,7 @@ void orc_io_enable(orc_t* o) {
     o->G = dalloc(3 * fs); o->EXPLT0 = dalloc(3 * fs); o->RHO = dalloc(fs); o->MU0 = dalloc(fs); o->MU = dalloc(fs);
     o->DSTG = dalloc(3 * fs); o->MUSTG = dalloc(3 * fs); o->DIVU = dalloc(fs); o->DRHODT = dalloc(fs);
     o->DEN = dalloc(fs);
+    o->DRHOI = dalloc(3 * fs);
     o->io = 1;
 }
 
@@ -1303,16 +1306,31 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
     int NYI = (IDR == 2) ? 2 : 1;
     double* EX = IDR == 1 ? o->QTMP : IDR == 2 ? o->DPH : o->RHSLLPHI;
     double DT = o->DT;
-    memset(o->RHS, 0, FSZ(o) * sizeof(double));
+    if (!o->ivis) {
+        memset(o->RHS, 0, FSZ(o) * sizeof(double));
 #pragma omp parallel for schedule(static)
-    for (int KC = 1; KC <= N; ++KC)
-        for (int JC = NYI; JC <= M; ++JC)
-            for (int IC = 1; IC <= L; ++IC) {
-                double RHSC = F3(EX, o, IC, JC, KC);
-                double RHSL = E0V(o, IC, JC, KC, IDR);
-                F3(o->RHS, o, IC, JC, KC) = (o->TGAM[NS] * RHSC + o->TROH[NS] * RHSL) * DT;
-                E0V(o, IC, JC, KC, IDR) = RHSC;
-            }
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = NYI; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    double RHSC = F3(EX, o, IC, JC, KC);
+                    double RHSL = E0V(o, IC, JC, KC, IDR);
+                    F3(o->RHS, o, IC, JC, KC) = (o->TGAM[NS] * RHSC + o->TROH[NS] * RHSL) * DT;
+                    E0V(o, IC, JC, KC, IDR) = RHSC;
+                }
+    } else {
+        /* VisImplicit (:87-99): RHS holds the implicit viscous part, DIVU the density correction */
+        double COE2 = o->TALP[NS] * DT;
+#pragma omp parallel for schedule(static)
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = NYI; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    double RHSC = F3(EX, o, IC, JC, KC);
+                    double RHSL = E0V(o, IC, JC, KC, IDR);
+                    F3(o->RHS, o, IC, JC, KC) = (o->TGAM[NS] * RHSC + o->TROH[NS] * RHSL) * DT +
+                                                COE2 * F3(o->RHS, o, IC, JC, KC) + 0.5 * COE2 * F3(o->DIVU, o, IC, JC, KC);
+                    E0V(o, IC, JC, KC, IDR) = RHSC;
+                }
+    }
     if (IDR == 1) {
         double COE2 = o->TALP[NS] * DT * o->DXI;
 #pragma omp parallel for schedule(static)
@@ -1360,6 +1378,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
             for (int JC = 1; JC <= M; ++JC)
                 for (int IC = 1; IC <= L; ++IC) F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - DPGRNS;
     }
+    if (o->ivis) return;  /* the save-back (:267-301) is the explicit scheme's */
 #pragma omp parallel for schedule(static)
     for (int KC = 1; KC <= N; ++KC)
         for (int JC = NYI; JC <= M; ++JC)
@@ -1407,10 +1426,21 @@ static void io_divg(orc_t* o, int NS) {
 /* MASSFLUX_UPDATE_io (src/VELO_CORRECTION.f90:103-179)                   */
 static void io_prcalc_massflux_update(orc_t* o, int NS) {
     int L = o->L, M = o->M, N = o->N;
+    if (o->ivis) {
+        double BE = 0.50 * o->TALP[NS] * o->DT * o->CVISC;  /* VisImplicit (:113-123) */
 #pragma omp parallel for schedule(static)
-    for (int KC = 1; KC <= N; ++KC)
-        for (int JC = 1; JC <= M; ++JC)
-            for (int IC = 1; IC <= L; ++IC) F3(o->PR, o, IC, JC, KC) = F3(o->PR, o, IC, JC, KC) + F3(o->DPH, o, IC, JC, KC);
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = 1; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    double LLphi = F3(o->RHSLLPHI, o, IC, JC, KC);
+                    F3(o->PR, o, IC, JC, KC) = F3(o->PR, o, IC, JC, KC) + F3(o->DPH, o, IC, JC, KC) - BE * LLphi;
+                }
+    } else {
+#pragma omp parallel for schedule(static)
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = 1; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) F3(o->PR, o, IC, JC, KC) = F3(o->PR, o, IC, JC, KC) + F3(o->DPH, o, IC, JC, KC);
+    }
     bc_wall_scalar(o, o->PR);
     double COE1 = o->DT * o->TALP[NS] * o->DXI;
 #pragma omp parallel for schedule(static)
@@ -1442,7 +1472,421 @@ static void io_prcalc_massflux_update(orc_t* o, int NS) {
     io_bc_wall_g(o);
 }
 
-/* SOLVERRK3_MOM_io(NS) (src/SOLVERRK3_MOM_IO.f90:11-120), explicit scheme. */
+/* ---------------------------------------------------------------------- */
+/* Crank-Nicolson form of the main-domain momentum step (iVisScheme = 1,  */
+/* VisImplicit): the viscous split after Nicoud (2000) into an explicit   */
+/* part (added to the convection term), an implicit part (RK weight       */
+/* alpha*dt) and a density-correction part, then MOMFA_io's approximate   */
+/* factorisation with per-point coefficients from Viscousity, MU_STG and  */
+/* D_STG.  Plane channel: RCCI1 = RCCI2 = RNDI1 = RNDI2 = 1 (kept as the  */
+/* factors 1.0 where the reference multiplies or divides by them).        */
+/* ---------------------------------------------------------------------- */
+#define DRV(o, i, j, k, c) ((o)->DRHOI[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
+
+void orc_io_set_vis_scheme(orc_t* o, int ivis) { o->ivis = ivis ? 1 : 0; }
+
+/* max |DRHOI_STG| over the interior and the v wall rows (0 by construction) */
+double orc_io_drhoi_maxabs(const orc_t* o) {
+    double m = 0.0;
+    size_t n = 3 * FSZ(o);
+    for (size_t q = 0; q < n; ++q) m = fmax(m, fabs(o->DRHOI[q]));
+    return m;
+}
+
+/* DENSITY_IMPLICIT_add (src/MASSFLUX_CALC_IO.f90:332-416): 1/D_STG minus */
+/* 1/(the same average of DENSITY0); SOLVE.f90:123-127 calls it right     */
+/* after DENSITY_Staggered, so every entry is 1/x - 1/x = 0.              */
+static void io_density_implicit_add(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    for (int I = 1; I <= L; ++I) {
+        int IM = IMV(o, I);
+        for (int J = 1; J <= M; ++J)
+            for (int K = 1; K <= N; ++K) {
+                double DEN_STG = (F3(o->RHO, o, I, J, K) + F3(o->RHO, o, IM, J, K)) * 0.5;
+                DRV(o, I, J, K, 1) = 1.0 / DSV(o, I, J, K, 1) - 1.0 / DEN_STG;
+            }
+    }
+    for (int K = 1; K <= N; ++K) {
+        int KM = KMV(o, K);
+        for (int J = 1; J <= M; ++J)
+            for (int I = 1; I <= L; ++I) {
+                double DEN_STG = (F3(o->RHO, o, I, J, K) + F3(o->RHO, o, I, J, KM)) * 0.5;
+                DRV(o, I, J, K, 3) = 1.0 / DSV(o, I, J, K, 3) - 1.0 / DEN_STG;
+            }
+    }
+    for (int J = 2; J <= M; ++J)
+        for (int K = 1; K <= N; ++K)
+            for (int I = 1; I <= L; ++I) {
+                double DEN_STG = o->WFF[J] * F3(o->RHO, o, I, J, K) + o->WFB[J] * F3(o->RHO, o, I, J - 1, K);
+                DRV(o, I, J, K, 2) = 1.0 / DSV(o, I, J, K, 2) - 1.0 / DEN_STG;
+            }
+    for (int K = 1; K <= N; ++K)
+        for (int I = 1; I <= L; ++I) {
+            DRV(o, I, 1, K, 2) = 0.0;
+            DRV(o, I, M + 1, K, 2) = 0.0;
+        }
+}
+
+/* VISCOUS_PAR_EXPLT_X_io (src/VISCOUS_X_EXPLICIT_io.f90:131-293):          */
+/* QTMP += explicit part, RHS = implicit part, DIVU = density correction.  */
+/* The tau13 correction takes Q_io (not G_io) times DRHOI_STG, as there.  */
+static void io_viscous_par_x(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->RHS, 0, FSZ(o) * sizeof(double));
+    double COE1 = -2.0 / 3.0 * o->DXI * o->CVISC, COE3 = o->DZI * o->CVISC;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * o->CVISC * 1.0, COE32 = COE3 * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double DUDX = (QV(o, IP, JC, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DXI;
+                double DVDY = (QV(o, IC, JP, KC, 2) - QV(o, IC, JC, KC, 2)) * o->DYFI[JJ] * 1.0;
+                double DWDZ = (QV(o, IC, JC, KP, 3) - QV(o, IC, JC, KC, 3)) * o->DZI * 1.0;
+                double T11F_EX = F3(o->MU, o, IC, JC, KC) * (DVDY + DWDZ);
+                double T11F_IM = F3(o->MU, o, IC, JC, KC) * DUDX;
+                DUDX = (GV(o, IP, JC, KC, 1) * DRV(o, IP, JC, KC, 1) - GV(o, IC, JC, KC, 1) * DRV(o, IC, JC, KC, 1)) * o->DXI;
+                double T11F_AD = F3(o->MU, o, IC, JC, KC) * DUDX;
+                DUDX = (QV(o, IC, JC, KC, 1) - QV(o, IM, JC, KC, 1)) * o->DXI;
+                DVDY = (QV(o, IM, JP, KC, 2) - QV(o, IM, JC, KC, 2)) * o->DYFI[JJ] * 1.0;
+                DWDZ = (QV(o, IM, JC, KP, 3) - QV(o, IM, JC, KC, 3)) * o->DZI * 1.0;
+                double T11B_EX = F3(o->MU, o, IM, JC, KC) * (DVDY + DWDZ);
+                double T11B_IM = F3(o->MU, o, IM, JC, KC) * DUDX;
+                DUDX = (GV(o, IC, JC, KC, 1) * DRV(o, IC, JC, KC, 1) - GV(o, IM, JC, KC, 1) * DRV(o, IM, JC, KC, 1)) * o->DXI;
+                double T11B_AD = F3(o->MU, o, IM, JC, KC) * DUDX;
+                double D11_EX = (T11F_EX - T11B_EX) * COE1;
+                double D11_IM = (T11F_IM - T11B_IM) * COE1 * (-2.0);
+                double D11_AD = (T11F_AD - T11B_AD) * COE1 * (-2.0);
+
+                double VIS12P = MSV(o, IC, JP, KC, 1);
+                double DVDX = (QV(o, IC, JP, KC, 2) - QV(o, IM, JP, KC, 2)) * o->DXI;
+                double DUDY = (QV(o, IC, JP, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DYCI[JJP] / 1.0;
+                double T12F_EX = VIS12P * DVDX, T12F_IM = VIS12P * DUDY;
+                DUDY = (GV(o, IC, JP, KC, 1) * DRV(o, IC, JP, KC, 1) - GV(o, IC, JC, KC, 1) * DRV(o, IC, JC, KC, 1)) * o->DYCI[JJP] / 1.0;
+                double T12F_AD = VIS12P * DUDY;
+                double VIS12C = MSV(o, IC, JC, KC, 1);
+                DUDY = (QV(o, IC, JC, KC, 1) - QV(o, IC, JM, KC, 1)) * o->DYCI[JJ] / 1.0;
+                DVDX = (QV(o, IC, JC, KC, 2) - QV(o, IM, JC, KC, 2)) * o->DXI;
+                double T12B_EX = VIS12C * DVDX, T12B_IM = VIS12C * DUDY;
+                DUDY = (GV(o, IC, JC, KC, 1) * DRV(o, IC, JC, KC, 1) - GV(o, IC, JM, KC, 1) * DRV(o, IC, JM, KC, 1)) * o->DYCI[JJ] / 1.0;
+                double T12B_AD = VIS12C * DUDY;
+                double D12_EX = (T12F_EX - T12B_EX) * COE2;
+                double D12_IM = (T12F_IM - T12B_IM) * COE2;
+                double D12_AD = (T12F_AD - T12B_AD) * COE2;
+
+                double VIS13P = MSV(o, IC, JC, KP, 2);
+                double DUDZ = (QV(o, IC, JC, KP, 1) - QV(o, IC, JC, KC, 1)) * o->DZI;
+                double DWDX = (QV(o, IC, JC, KP, 3) - QV(o, IM, JC, KP, 3)) * o->DXI;
+                double T13F_EX = VIS13P * DWDX, T13F_IM = VIS13P * DUDZ;
+                DUDZ = (QV(o, IC, JC, KP, 1) * DRV(o, IC, JC, KP, 1) - QV(o, IC, JC, KC, 1) * DRV(o, IC, JC, KC, 1)) * o->DZI;
+                double T13F_AD = VIS13P * DUDZ;
+                double VIS13C = MSV(o, IC, JC, KC, 2);
+                DUDZ = (QV(o, IC, JC, KC, 1) - QV(o, IC, JC, KM, 1)) * o->DZI;
+                DWDX = (QV(o, IC, JC, KC, 3) - QV(o, IM, JC, KC, 3)) * o->DXI;
+                double T13B_EX = VIS13C * DWDX, T13B_IM = VIS13C * DUDZ;
+                DUDZ = (QV(o, IC, JC, KC, 1) * DRV(o, IC, JC, KC, 1) - QV(o, IC, JC, KM, 1) * DRV(o, IC, JC, KM, 1)) * o->DZI;
+                double T13B_AD = VIS13C * DUDZ;
+                double D13_EX = (T13F_EX - T13B_EX) * COE32;
+                double D13_IM = (T13F_IM - T13B_IM) * COE32;
+                double D13_AD = (T13F_AD - T13B_AD) * COE32;
+
+                F3(o->QTMP, o, IC, JC, KC) = D11_EX + D12_EX + D13_EX + F3(o->QTMP, o, IC, JC, KC);
+                F3(o->RHS, o, IC, JC, KC) = D11_IM + D12_IM + D13_IM;
+                F3(o->DIVU, o, IC, JC, KC) = D11_AD + D12_AD + D13_AD;
+            }
+        }
+    }
+}
+
+/* VISCOUS_PAR_EXPLT_Y_io (src/VISCOUS_Y_EXPLICIT_io.f90:278-443), channel: */
+/* rows 2..M (the wall face j = 1 keeps RHS = 0).                          */
+static void io_viscous_par_y(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->RHS, 0, FSZ(o) * sizeof(double));
+    double COE1 = o->DXI * o->CVISC, COE3 = o->DZI * o->CVISC;
+#pragma omp parallel for schedule(static)
+    for (int JC = 2; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJM = JJ - 1;
+        double COE2 = -2.0 / 3.0 * o->DYCI[JJ] * o->CVISC;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double DUDX = (QV(o, IP, JC, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DXI;
+                double DVDY = (QV(o, IC, JP, KC, 2) - QV(o, IC, JC, KC, 2)) * o->DYFI[JJ];
+                double DWDZ = (QV(o, IC, JC, KP, 3) - QV(o, IC, JC, KC, 3)) * o->DZI;
+                double T22F_EX = F3(o->MU, o, IC, JC, KC) * (DUDX + DWDZ);
+                double T22F_IM = F3(o->MU, o, IC, JC, KC) * DVDY;
+                DVDY = (GV(o, IC, JP, KC, 2) * DRV(o, IC, JP, KC, 2) - GV(o, IC, JC, KC, 2) * DRV(o, IC, JC, KC, 2)) * o->DYFI[JJ];
+                double T22F_AD = F3(o->MU, o, IC, JC, KC) * DVDY;
+                DUDX = (QV(o, IP, JM, KC, 1) - QV(o, IC, JM, KC, 1)) * o->DXI;
+                DVDY = (QV(o, IC, JC, KC, 2) - QV(o, IC, JM, KC, 2)) * o->DYFI[JJM];
+                DWDZ = (QV(o, IC, JM, KP, 3) - QV(o, IC, JM, KC, 3)) * o->DZI;
+                double T22B_EX = F3(o->MU, o, IC, JM, KC) * (DUDX + DWDZ);
+                double T22B_IM = F3(o->MU, o, IC, JM, KC) * DVDY;
+                DVDY = (GV(o, IC, JC, KC, 2) * DRV(o, IC, JC, KC, 2) - GV(o, IC, JM, KC, 2) * DRV(o, IC, JM, KC, 2)) * o->DYFI[JJM];
+                double T22B_AD = F3(o->MU, o, IC, JM, KC) * DVDY;
+                double D22_EX = (T22F_EX - T22B_EX) * COE2;
+                double D22_IM = (T22F_IM - T22B_IM) * COE2 * (-2.0);
+                double D22_AD = (T22F_AD - T22B_AD) * COE2 * (-2.0);
+
+                double VIS21P = MSV(o, IP, JC, KC, 1);
+                double DVDX = (QV(o, IP, JC, KC, 2) - QV(o, IC, JC, KC, 2)) * o->DXI;
+                double DUDY = (QV(o, IP, JC, KC, 1) - QV(o, IP, JM, KC, 1)) * o->DYCI[JJ];
+                double T21F_EX = VIS21P * DUDY, T21F_IM = VIS21P * DVDX;
+                DVDX = (GV(o, IP, JC, KC, 2) * DRV(o, IP, JC, KC, 2) - GV(o, IC, JC, KC, 2) * DRV(o, IC, JC, KC, 2)) * o->DXI;
+                double T21F_AD = VIS21P * DVDX;
+                double VIS21C = MSV(o, IC, JC, KC, 1);
+                DVDX = (QV(o, IC, JC, KC, 2) - QV(o, IM, JC, KC, 2)) * o->DXI;
+                DUDY = (QV(o, IC, JC, KC, 1) - QV(o, IC, JM, KC, 1)) * o->DYCI[JJ];
+                double T21B_EX = VIS21C * DUDY, T21B_IM = VIS21C * DVDX;
+                DVDX = (GV(o, IC, JC, KC, 2) * DRV(o, IC, JC, KC, 2) - GV(o, IM, JC, KC, 2) * DRV(o, IM, JC, KC, 2)) * o->DXI;
+                double T21B_AD = VIS21C * DVDX;
+                double D21_EX = (T21F_EX - T21B_EX) * COE1;
+                double D21_IM = (T21F_IM - T21B_IM) * COE1;
+                double D21_AD = (T21F_AD - T21B_AD) * COE1;
+
+                double VIS23P = MSV(o, IC, JC, KP, 3);
+                double DVDZ = (QV(o, IC, JC, KP, 2) - QV(o, IC, JC, KC, 2)) * o->DZI;
+                double DWDY = (QV(o, IC, JC, KP, 3) - QV(o, IC, JM, KP, 3)) * o->DYCI[JJ];
+                double T23F_EX = VIS23P * DWDY, T23F_IM = VIS23P * DVDZ;
+                DVDZ = (GV(o, IC, JC, KP, 2) * DRV(o, IC, JC, KP, 2) - GV(o, IC, JC, KC, 2) * DRV(o, IC, JC, KC, 2)) * o->DZI;
+                double T23F_AD = VIS23P * DVDZ;
+                double VIS23C = MSV(o, IC, JC, KC, 3);
+                DVDZ = (QV(o, IC, JC, KC, 2) - QV(o, IC, JC, KM, 2)) * o->DZI;
+                DWDY = (QV(o, IC, JC, KC, 3) - QV(o, IC, JM, KC, 3)) * o->DYCI[JJ];
+                double T23B_EX = VIS23C * DWDY, T23B_IM = VIS23C * DVDZ;
+                DVDZ = (GV(o, IC, JC, KC, 2) * DRV(o, IC, JC, KC, 2) - GV(o, IC, JC, KM, 2) * DRV(o, IC, JC, KM, 2)) * o->DZI;
+                double T23B_AD = VIS23C * DVDZ;
+                double D23_EX = (T23F_EX - T23B_EX) * COE3;
+                double D23_IM = (T23F_IM - T23B_IM) * COE3;
+                double D23_AD = (T23F_AD - T23B_AD) * COE3;
+
+                F3(o->DPH, o, IC, JC, KC) = D21_EX + D22_EX + D23_EX + F3(o->DPH, o, IC, JC, KC);
+                F3(o->RHS, o, IC, JC, KC) = D21_IM + D22_IM + D23_IM;
+                F3(o->DIVU, o, IC, JC, KC) = D21_AD + D22_AD + D23_AD;
+            }
+        }
+    }
+}
+
+/* VISCOUS_PAR_EXPLT_Z_io (src/VISCOUS_Z_EXPLICIT_io.f90:300-465), channel */
+static void io_viscous_par_z(orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    memset(o->RHS, 0, FSZ(o) * sizeof(double));
+    double COE1 = o->DXI * o->CVISC, COE3 = -2.0 / 3.0 * o->DZI * o->CVISC;
+#pragma omp parallel for schedule(static)
+    for (int JC = 1; JC <= M; ++JC) {
+        int JM = JC - 1, JP = JC + 1, JJ = JC, JJP = JJ + 1;
+        double COE2 = o->DYFI[JJ] * o->CVISC;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KM = KMV(o, KC), KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC), IM = IMV(o, IC);
+                double DUDX = (QV(o, IP, JC, KC, 1) - QV(o, IC, JC, KC, 1)) * o->DXI;
+                double DVDY = (QV(o, IC, JP, KC, 2) - QV(o, IC, JC, KC, 2)) * o->DYFI[JJ];
+                double DWDZ = (QV(o, IC, JC, KP, 3) - QV(o, IC, JC, KC, 3)) * o->DZI;
+                double T33F_EX = F3(o->MU, o, IC, JC, KC) * (DUDX + DVDY);
+                double T33F_IM = F3(o->MU, o, IC, JC, KC) * DWDZ;
+                DWDZ = (GV(o, IC, JC, KP, 3) * DRV(o, IC, JC, KP, 3) - GV(o, IC, JC, KC, 3) * DRV(o, IC, JC, KC, 3)) * o->DZI;
+                double T33F_AD = F3(o->MU, o, IC, JC, KC) * DWDZ;
+                DUDX = (QV(o, IP, JC, KM, 1) - QV(o, IC, JC, KM, 1)) * o->DXI;
+                DVDY = (QV(o, IC, JP, KM, 2) - QV(o, IC, JC, KM, 2)) * o->DYFI[JJ];
+                DWDZ = (QV(o, IC, JC, KC, 3) - QV(o, IC, JC, KM, 3)) * o->DZI;
+                double T33B_EX = F3(o->MU, o, IC, JC, KM) * (DUDX + DVDY);
+                double T33B_IM = F3(o->MU, o, IC, JC, KM) * DWDZ;
+                DWDZ = (GV(o, IC, JC, KC, 3) * DRV(o, IC, JC, KC, 3) - GV(o, IC, JC, KM, 3) * DRV(o, IC, JC, KM, 3)) * o->DZI;
+                double T33B_AD = F3(o->MU, o, IC, JC, KM) * DWDZ;
+                double D33_EX = (T33F_EX - T33B_EX) * COE3;
+                double D33_IM = (T33F_IM - T33B_IM) * COE3 * (-2.0);
+                double D33_AD = (T33F_AD - T33B_AD) * COE3 * (-2.0);
+
+                double VIS31P = MSV(o, IP, JC, KC, 2);
+                double DWDX = (QV(o, IP, JC, KC, 3) - QV(o, IC, JC, KC, 3)) * o->DXI;
+                double DUDZ = (QV(o, IP, JC, KC, 1) - QV(o, IP, JC, KM, 1)) * o->DZI;
+                double T31F_EX = VIS31P * DUDZ, T31F_IM = VIS31P * DWDX;
+                DWDX = (GV(o, IP, JC, KC, 3) * DRV(o, IP, JC, KC, 3) - GV(o, IC, JC, KC, 3) * DRV(o, IC, JC, KC, 3)) * o->DXI;
+                double T31F_AD = VIS31P * DWDX;
+                double VIS31C = MSV(o, IC, JC, KC, 2);
+                DWDX = (QV(o, IC, JC, KC, 3) - QV(o, IM, JC, KC, 3)) * o->DXI;
+                DUDZ = (QV(o, IC, JC, KC, 1) - QV(o, IC, JC, KM, 1)) * o->DZI;
+                double T31B_EX = VIS31C * DUDZ, T31B_IM = VIS31C * DWDX;
+                DWDX = (GV(o, IC, JC, KC, 3) * DRV(o, IC, JC, KC, 3) - GV(o, IM, JC, KC, 3) * DRV(o, IM, JC, KC, 3)) * o->DXI;
+                double T31B_AD = VIS31C * DWDX;
+                double D31_EX = (T31F_EX - T31B_EX) * COE1;
+                double D31_IM = (T31F_IM - T31B_IM) * COE1;
+                double D31_AD = (T31F_AD - T31B_AD) * COE1;
+
+                double VIS32P = MSV(o, IC, JP, KC, 3);
+                double DWDY = (QV(o, IC, JP, KC, 3) - QV(o, IC, JC, KC, 3)) * o->DYCI[JJP];
+                double DVDZ = (QV(o, IC, JP, KC, 2) - QV(o, IC, JP, KM, 2)) * o->DZI;
+                double T32F_EX = VIS32P * DVDZ, T32F_IM = VIS32P * DWDY;
+                DWDY = (GV(o, IC, JP, KC, 3) * DRV(o, IC, JP, KC, 3) - GV(o, IC, JC, KC, 3) * DRV(o, IC, JC, KC, 3)) * o->DYCI[JJP];
+                double T32F_AD = VIS32P * DWDY;
+                double VIS32C = MSV(o, IC, JC, KC, 3);
+                DWDY = (QV(o, IC, JC, KC, 3) - QV(o, IC, JM, KC, 3)) * o->DYCI[JJ];
+                DVDZ = (QV(o, IC, JC, KC, 2) - QV(o, IC, JC, KM, 2)) * o->DZI;
+                double T32B_EX = VIS32C * DVDZ, T32B_IM = VIS32C * DWDY;
+                DWDY = (GV(o, IC, JC, KC, 3) * DRV(o, IC, JC, KC, 3) - GV(o, IC, JM, KC, 3) * DRV(o, IC, JM, KC, 3)) * o->DYCI[JJ];
+                double T32B_AD = VIS32C * DWDY;
+                double D32_EX = (T32F_EX - T32B_EX) * COE2;
+                double D32_IM = (T32F_IM - T32B_IM) * COE2;
+                double D32_AD = (T32F_AD - T32B_AD) * COE2;
+
+                F3(o->RHSLLPHI, o, IC, JC, KC) = D31_EX + D32_EX + D33_EX + F3(o->RHSLLPHI, o, IC, JC, KC);
+                F3(o->RHS, o, IC, JC, KC) = D31_IM + D32_IM + D33_IM;
+                F3(o->DIVU, o, IC, JC, KC) = D31_AD + D32_AD + D33_AD;
+            }
+        }
+    }
+}
+
+/* MOMFA_io(NS, IDR) (src/MOMFA_io.f90:18-76): x sweep MOMFA1_X_io (:79-172,  */
+/* cyclic), z sweep MOMFA2_Z_io (:175-261, cyclic), y sweep MOMFA3_Y_io       */
+/* (:264-406, TDMAIJJ_nonCYC with BCJ = 0), then G += RHS for j >= N2I.       */
+/* The y-sweep row 1 of the v equation has AMVR(1,2) = APVR(1,2) = 0, so its */
+/* coefficients are (0, 1, 0) whatever the densities it divides by; the     */
+/* ghost D_STG(:,0,:,2) it reads is taken as the y-periodic halo value      */
+/* D_STG(:,M,:,2) that INTFC_VARS3 leaves there in a run of two or more     */
+/* ranks.  The v rows use D_STG(j) for the j+1 coupling, as the reference.  */
+static void io_momfa(orc_t* o, int NS, int IDR) {
+    int L = o->L, M = o->M, N = o->N;
+    double FACOE = 0.50 * o->TALP[NS] * o->DT * o->CVISC;
+    int N2I = (IDR == 2) ? 2 : 1;
+    /* ---- x ---- */
+    {
+        double COE1 = FACOE * 4.0 / 3.0 * o->DXQI, COE2 = FACOE * o->DXQI;
+#pragma omp parallel
+        {
+            double *A = dalloc(L), *B = dalloc(L), *C = dalloc(L), *R = dalloc(L), *w = dalloc(3 * (size_t)L);
+#pragma omp for schedule(static) collapse(2)
+            for (int KC = 1; KC <= N; ++KC)
+                for (int JC = N2I; JC <= M; ++JC) {
+                    for (int IC = 1; IC <= L; ++IC) {
+                        int IM = IMV(o, IC), IP = IPV(o, IC);
+                        double AMU, APU;
+                        if (IDR == 1) {
+                            AMU = -COE1 * F3(o->MU, o, IM, JC, KC);
+                            APU = -COE1 * F3(o->MU, o, IC, JC, KC);
+                        } else if (IDR == 2) {
+                            AMU = -COE2 * MSV(o, IC, JC, KC, 1);
+                            APU = -COE2 * MSV(o, IP, JC, KC, 1);
+                        } else {
+                            AMU = -COE2 * MSV(o, IC, JC, KC, 2);
+                            APU = -COE2 * MSV(o, IP, JC, KC, 2);
+                        }
+                        A[IC - 1] = AMU / DSV(o, IM, JC, KC, IDR);
+                        C[IC - 1] = APU / DSV(o, IP, JC, KC, IDR);
+                        B[IC - 1] = 1.0 - (AMU + APU) / DSV(o, IC, JC, KC, IDR);
+                        R[IC - 1] = F3(o->RHS, o, IC, JC, KC);
+                    }
+                    tdma_cyc_line(L, A, B, C, R, w);
+                    for (int IC = 1; IC <= L; ++IC) F3(o->RHS, o, IC, JC, KC) = R[IC - 1];
+                }
+            free(A); free(B); free(C); free(R); free(w);
+        }
+    }
+    /* ---- z ---- */
+    {
+        double COE1 = FACOE * 4.0 / 3.0 * o->DZQI, COE2 = FACOE * o->DZQI;
+#pragma omp parallel
+        {
+            double *A = dalloc(N), *B = dalloc(N), *C = dalloc(N), *R = dalloc(N), *w = dalloc(3 * (size_t)N);
+#pragma omp for schedule(static) collapse(2)
+            for (int JC = N2I; JC <= M; ++JC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    for (int KC = 1; KC <= N; ++KC) {
+                        int KM = KMV(o, KC), KP = KPV(o, KC);
+                        double AMU, APU;
+                        if (IDR == 1) {
+                            AMU = -COE2 * MSV(o, IC, JC, KC, 2) * 1.0;
+                            APU = -COE2 * MSV(o, IC, JC, KP, 2) * 1.0;
+                        } else if (IDR == 2) {
+                            AMU = -COE2 * MSV(o, IC, JC, KC, 3) * 1.0;
+                            APU = -COE2 * MSV(o, IC, JC, KP, 3) * 1.0;
+                        } else {
+                            AMU = -COE1 * F3(o->MU, o, IC, JC, KM) * 1.0;
+                            APU = -COE1 * F3(o->MU, o, IC, JC, KC) * 1.0;
+                        }
+                        A[KC - 1] = AMU / DSV(o, IC, JC, KM, IDR);
+                        C[KC - 1] = APU / DSV(o, IC, JC, KP, IDR);
+                        B[KC - 1] = 1.0 - (AMU + APU) / DSV(o, IC, JC, KC, IDR);
+                        R[KC - 1] = F3(o->RHS, o, IC, JC, KC);
+                    }
+                    tdma_cyc_line(N, A, B, C, R, w);
+                    for (int KC = 1; KC <= N; ++KC) F3(o->RHS, o, IC, JC, KC) = R[KC - 1];
+                }
+            free(A); free(B); free(C); free(R); free(w);
+        }
+    }
+    /* ---- y ---- */
+    {
+        double COE1 = FACOE * 4.0 / 3.0, COE2 = FACOE;
+        const double* AMV = o->AMVR[IDR];
+        const double* APV = o->APVR[IDR];
+#pragma omp parallel
+        {
+            double *A = dalloc(M), *B = dalloc(M), *C = dalloc(M), *R = dalloc(M), *w = dalloc(2 * (size_t)M);
+#pragma omp for schedule(static) collapse(2)
+            for (int KC = 1; KC <= N; ++KC)
+                for (int IC = 1; IC <= L; ++IC) {
+                    for (int JC = 1; JC <= M; ++JC) {
+                        int JM = JC - 1, JP = JC + 1;
+                        double AMU, APU, AJ, CJ, BJ;
+                        if (IDR == 1 || IDR == 3) {
+                            if (JC == 1) {
+                                double MUQT = (F3(o->MU, o, IC, JC, KC) + F3(o->MU, o, IC, JM, KC)) * 0.5;
+                                AMU = -COE2 * o->AMVR1 * MUQT;
+                                APU = -COE2 * APV[JC] * MSV(o, IC, JP, KC, IDR);
+                                AJ = 0.0;
+                                CJ = APU / DSV(o, IC, JP, KC, IDR);
+                            } else if (JC == M) {
+                                double MUQT = (F3(o->MU, o, IC, M, KC) + F3(o->MU, o, IC, M + 1, KC)) * 0.5;
+                                AMU = -COE2 * AMV[JC] * MSV(o, IC, JC, KC, IDR);
+                                APU = -COE2 * o->APVRN * MUQT;
+                                AJ = AMU / DSV(o, IC, JM, KC, IDR);
+                                CJ = 0.0;
+                            } else {
+                                AMU = -COE2 * AMV[JC] * MSV(o, IC, JC, KC, IDR);
+                                APU = -COE2 * APV[JC] * MSV(o, IC, JP, KC, IDR);
+                                AJ = AMU / DSV(o, IC, JM, KC, IDR);
+                                CJ = APU / DSV(o, IC, JP, KC, IDR);
+                            }
+                            BJ = 1.0 - (AMU + APU) / DSV(o, IC, JC, KC, IDR);
+                        } else {
+                            if (JC == 1) {
+                                AMU = -COE1 * AMV[JC] * F3(o->MU, o, IC, JM, KC);
+                                APU = -COE1 * APV[JC] * F3(o->MU, o, IC, JC, KC);
+                                AJ = AMU / DSV(o, IC, M, KC, 2);  /* D_STG(:,0,:,2): y-periodic halo */
+                                CJ = APU / DSV(o, IC, JP, KC, 2);
+                                BJ = 1.0 - (AMU + APU) / DSV(o, IC, JC, KC, 2);
+                            } else {
+                                AMU = -COE1 * AMV[JC] * F3(o->MU, o, IC, JM, KC);
+                                APU = -COE1 * APV[JC] * F3(o->MU, o, IC, JC, KC);
+                                AJ = AMU / DSV(o, IC, JM, KC, 2);
+                                CJ = APU / DSV(o, IC, JC, KC, 2);
+                                BJ = 1.0 - (AMU + APU) / DSV(o, IC, JC, KC, 2);
+                            }
+                        }
+                        A[JC - 1] = AJ; B[JC - 1] = BJ; C[JC - 1] = CJ;
+                        R[JC - 1] = F3(o->RHS, o, IC, JC, KC);
+                    }
+                    tdma_noncyc_line(M, A, B, C, R, w);
+                    for (int JC = 1; JC <= M; ++JC) F3(o->RHS, o, IC, JC, KC) = R[JC - 1];
+                }
+            free(A); free(B); free(C); free(R); free(w);
+        }
+    }
+#pragma omp parallel for schedule(static)
+    for (int K = 1; K <= N; ++K)
+        for (int J = N2I; J <= M; ++J)
+            for (int I = 1; I <= L; ++I) GV(o, I, J, K, IDR) = F3(o->RHS, o, I, J, K) + GV(o, I, J, K, IDR);
+}
+
+/* SOLVERRK3_MOM_io(NS) (src/SOLVERRK3_MOM_IO.f90:11-120), explicit or      */
+/* Crank-Nicolson viscous scheme (orc_io_set_vis_scheme).                  */
 /* The pressure Poisson equation is the one FISHPACK_POIS3D_SIMPLE solves */
 /* (same AMPH/ACPH/APPH operator and x/z eigenvalues); its singular       */
 /* kx = kz = 0 mode is fixed here as in FFT99 (phi_hat(y_1) = 0), which    */
@@ -1454,14 +1898,26 @@ int orc_io_substep(orc_t* o, int NS) {
     io_convection_x(o);
     io_convection_y(o);
     io_convection_z(o);
-    io_divg_u(o);
-    io_viscous_x(o);
-    io_rhs_mom_explicit(o, NS, 1);
-    io_viscous_y(o);
-    io_rhs_mom_explicit(o, NS, 2);
-    io_viscous_z(o);
-    io_rhs_mom_explicit(o, NS, 3);
-    io_massflux_calc(o);
+    if (!o->ivis) {
+        io_divg_u(o);
+        io_viscous_x(o);
+        io_rhs_mom_explicit(o, NS, 1);
+        io_viscous_y(o);
+        io_rhs_mom_explicit(o, NS, 2);
+        io_viscous_z(o);
+        io_rhs_mom_explicit(o, NS, 3);
+        io_massflux_calc(o);
+    } else {
+        io_viscous_par_x(o);
+        io_rhs_mom_explicit(o, NS, 1);
+        io_momfa(o, NS, 1);
+        io_viscous_par_y(o);
+        io_rhs_mom_explicit(o, NS, 2);
+        io_momfa(o, NS, 2);
+        io_viscous_par_z(o);
+        io_rhs_mom_explicit(o, NS, 3);
+        io_momfa(o, NS, 3);
+    }
     io_bc_wall_g(o);
     io_divg(o, NS);
     memset(o->DPH, 0, FSZ(o) * sizeof(double));
@@ -1638,6 +2094,7 @@ int orc_thermal_substep(orc_t* o, int NS) {
     thermal_bc_isoflux(o);
     density_time_derivation(o, NS);
     io_staggered_props(o);
+    if (o->ivis) io_density_implicit_add(o);
     return o->prop_err;
 }
 

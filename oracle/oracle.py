@@ -72,6 +72,9 @@ def lib():
         L.orc_io_run_steps.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         L.orc_io_run_steps.restype = ctypes.c_int
         L.orc_io_monitor.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_io_set_vis_scheme.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_io_drhoi_maxabs.argtypes = [ctypes.c_void_p]
+        L.orc_io_drhoi_maxabs.restype = ctypes.c_double
         L.orc_thermal_enable.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double]
         L.orc_thermal_enable.restype = ctypes.c_int
@@ -200,7 +203,13 @@ class Oracle:
     def divgck(self):
         return self._lib.orc_divgck(self._h)
 
-    # ---- IO (main-domain) path, explicit viscous terms ----
+    # ---- IO (main-domain) path, explicit (iVisScheme 0) or Crank-Nicolson (1) viscous terms ----
+    def io_set_vis_scheme(self, ivis):
+        self._lib.orc_io_set_vis_scheme(self._h, int(ivis))
+
+    def io_drhoi_maxabs(self):
+        return self._lib.orc_io_drhoi_maxabs(self._h)
+
     def io_set_fields(self, G, PR, RHO, MU0, MU):
         arrs = [np.ascontiguousarray(a, np.float64) for a in (G, PR, RHO, MU0, MU)]
         assert arrs[0].shape == (3,) + self.field_shape()
