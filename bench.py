@@ -66,6 +66,238 @@ L2_BYTES = 126 * 1024 * 1024
 # algorithmic FP64 words per grid point moved by one launch of each kernel
 # (reads + writes of the arrays the reference's algorithm needs; the
 # spectral arrays hold (L/2+1)/L complex values per point)
+HEATED_WORKLOAD = "heated256x192x128_retau180_cn"
+# heated main-domain channel: grid, domain, REN, DT0, CFLGV, wall heat flux, rho*h perturbation
+HEATED = {"L": 256, "M": 192, "N": 128, "HX": 4 * math.pi, "HZ": 4 * math.pi / 3, "STR2": 2.0, "REN": 2800.0,
+          "DT0": 1e-3, "CFLGV": 0.5, "qw": 0.5, "dh_amp": 1e-3}
+# training schedule of the learned property model: (Adam iterations, learning rate)
+MLP_SCHEDULE = [(8000, 3e-3), (8000, 1e-3), (8000, 3e-4), (4000, 1e-4)]
+MLP_BOUND = 2e-2  # stated max error of each model output: |model - table| / max(|table|, output scale)
+
+
+def heated_case():
+    """Seeded heated channel: perturbed Poiseuille G, rho*h = table origin +
+    a seeded perturbation, the 2048-row synthetic property table."""
+    from chapsim import thermo
+    h = HEATED
+    s = channel_setup(h["L"], h["M"], h["N"], h["HX"], h["HZ"], h["STR2"], h["REN"])
+    Q, PR = initial_field(s, 1973, 0.1)
+    rows, T0 = thermo.synthetic_table()
+    tab = thermo.SplineTable.from_rows(rows, T0)
+    cthecd = 1.0 / h["REN"] / (tab.ref["M0"] * tab.ref["CP0"] / tab.ref["K0"])
+    DH = np.zeros((h["N"], h["M"] + 2, h["L"]))
+    DH[:, 1:h["M"] + 1, :] = h["dh_amp"] * np.random.default_rng(5).uniform(-1.0, 1.0, (h["N"], h["M"], h["L"]))
+    return s, Q, PR, tab, cthecd, DH
+
+
+def heated_kernel_words(L, M):
+    """Algorithmic FP64 words per grid point per launch of the heated main-domain
+    step (Crank-Nicolson momentum, thermal solver on)."""
+    spec = 2.0 * (L // 2 + 1) / L
+    return {
+        "k_io_cfl": 5.0, "k_dt": 0.0,                 # Q x3, Viscousity, DENSITY
+        "k_eng_rhs": 10.0,                            # H, T, kappa, G x3, DH, RHS_E0 in; DH, RHS_E0 out
+        "k_eng_props": 11.0, "k_mlp_infer": 11.0,     # DH, DENSITY, Viscousity in; 8 property fields out
+        "k_eng_bc": 22.0 / M,                         # the two ghost planes
+        "k_drhodt": 7.0,                              # G x3, G0 x3 in; DrhoDt out
+        "k_io_props": 8.0,                            # DENSITY0, Viscousity0 in; D_STG x3, MU_STG x3 out
+        "k_g0_velocity": 12.0,                        # G, D_STG in; G0, Q out (x3 each)
+        "k_io_rhs_cn": 20.0,                          # G, Q, MU_STG, EXPLT0 (x3), Viscousity, PR in; EXPLT0, RHS out
+        "k_io_cn_xsweep": 12.0,                       # RHS x3 in/out; 2 coefficient fields per component
+        "k_io_cn_zysweep": 27.0,                      # z: as x; y: coefficients, RHS in, G in/out
+        "k_io_div_fftx": 5.0 + spec,                  # G x3, DrhoDt in; RHSLLPHI, spectrum out
+        "k_fftz_fwd": 2.0 * spec, "k_ysolve": 2.0 * spec, "k_fftz_inv": 2.0 * spec,
+        "k_fftx_inv": spec + 1.0,                     # spectrum in; DPH out
+        "k_io_correct": 16.0,                         # DPH, G, PR, D_STG, RHSLLPHI in; PR, G, Q out
+    }
+
+
+def heated_cpu_rate(time_budget_s, threads):
+    """The heated step on the CPU FP64 restatement (table search, Crank-Nicolson), bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    from oracle import Oracle
+    h = HEATED
+    s, Q, PR, tab, cthecd, DH = heated_case()
+    ones = np.ones_like(PR)
+    o = Oracle(h["L"], h["M"], h["N"], h["HX"], h["HZ"], h["STR2"], h["REN"], DT0=h["DT0"], DTMIN=1e-6,
+               CFLGV=h["CFLGV"], threads=threads)
+    o.io_set_fields(Q, PR, ones, ones, ones)
+    o.io_set_vis_scheme(1)
+    ot = orc.PropTable(tab.lists)
+    o.thermal_enable(ot, DH, h["qw"], h["qw"], cthecd)
+    o.set_dt(h["DT0"])
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        o.io_run_steps(1)
+        n += 1
+        if time.perf_counter() - t0 > time_budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return h["L"] * h["M"] * h["N"] * n / dt, n, dt
+
+
+def run_heated(args):
+    """Config 4: heated main-domain channel, Crank-Nicolson momentum, energy
+    equation and property update every substep; properties by the table
+    search (the plain method) and by the learned model (trained here on the
+    table and on rho*h samples of the running field, judged against the
+    table search)."""
+    from chapsim import gpu
+    import torch
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    h = HEATED
+    L, M, N, DT0, CFLGV, DTMIN = h["L"], h["M"], h["N"], h["DT0"], h["CFLGV"], 1e-6
+    s, Q, PR, tab, cthecd, DH = heated_case()
+    ones = np.ones_like(PR)
+    ch = gpu.ChannelIO(s, device=local, ivisscheme=gpu.VIS_IMPLICIT)
+    ch.upload_io(Q, PR, ones, ones, ones)
+    ch.set_dt(DT0)
+    ch.thermal_init(tab, DH, h["qw"], h["qw"], cthecd)
+    stream = torch.cuda.ExternalStream(ch.stream_handle(), device=local)
+    pts = L * M * N
+
+    def timed(nsteps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ch.launch_count()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        with ClockSampler(local) as clk:
+            ev0.record(stream)
+            ch.advance(nsteps, DT0, DTMIN, CFLGV)
+            ev1.record(stream)
+            torch.cuda.synchronize(local)
+        ms = ev0.elapsed_time(ev1)
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, ch.launch_count() - l0, clk.summary()
+
+    def kernel_profile():
+        n = max(1, min(10, args.steps))
+        kms = ch.profile_steps(n, DT0, DTMIN, CFLGV)
+        return {k: v / n for k, v in kms.items()}
+
+    # ---- plain method: table search ----
+    ch.advance(args.warmup, DT0, DTMIN, CFLGV)
+    ms_t, launches, clk = timed(args.steps)
+    v_table = pts * args.steps * ws / (ms_t / 1000.0)
+    k_table = kernel_profile()
+
+    # ---- end to end through the public API with host buffers (table search) ----
+    try:
+        pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+        gh, ph, dhh = pin((3,) + PR.shape), pin(PR.shape), pin(PR.shape)
+        rh, mh, qh = pin(PR.shape), pin(PR.shape), pin((3,) + PR.shape)
+    except Exception:
+        gh, ph, dhh = np.empty((3,) + PR.shape), np.empty(PR.shape), np.empty(PR.shape)
+        rh, mh, qh = np.empty(PR.shape), np.empty(PR.shape), np.empty((3,) + PR.shape)
+    G0, _, P0 = ch.download_io()
+    th = ch.download_thermal()
+    gh[...], ph[...], dhh[...], rh[...], mh[...] = G0, P0, th["DH"], th["D"], th["M"]
+    ne = max(1, min(args.steps, args.e2e_steps))
+    ch.sync()
+    t0 = time.perf_counter()
+    for _ in range(ne):
+        # H2D: the flow and rho*h state of a restart; the properties follow from rho*h
+        ch.lib.chapsim_upload_io_fields(ch.h, gpu._ptr(gh), gpu._ptr(ph), gpu._ptr(rh), gpu._ptr(mh), gpu._ptr(mh))
+        ch.lib.chapsim_thermal_init(ch.h, gpu._ptr(dhh), h["qw"], h["qw"], cthecd)
+        ch.advance(1, DT0, DTMIN, CFLGV)
+        # D2H: the step's result
+        ch.lib.chapsim_download_io_fields(ch.h, gpu._ptr(gh), gpu._ptr(qh), gpu._ptr(ph))
+        ch.lib.chapsim_download_thermal_fields(ch.h, gpu._ptr(dhh), None, None, None, None, None, None)
+    ch.sync()
+    te = time.perf_counter() - t0
+    e2e = pts * ne * ws / te
+    h2d = int(gh.nbytes + ph.nbytes + rh.nbytes + 2 * mh.nbytes + dhh.nbytes)
+    d2h = int(gh.nbytes + qh.nbytes + ph.nbytes + dhh.nbytes)
+
+    # ---- learned property model: trained on the table and the running field ----
+    dh_list = tab.lists["DH"]
+    lo = float(dh_list[0] + 0.02 * (dh_list[-1] - dh_list[0]))
+    hi = float(dh_list[-1] - 0.02 * (dh_list[-1] - dh_list[0]))
+    field = ch.download_thermal()["DH"][:, 1:M + 1].reshape(-1)
+    rng = np.random.default_rng(6)
+    knots = dh_list[(dh_list >= lo) & (dh_list <= hi)]
+    train = np.concatenate([knots, rng.choice(field, 4000, replace=False), rng.uniform(lo, hi, 2000)])
+    ch.mlp_init(lo, hi, seed=11)
+    t0 = time.perf_counter()
+    loss = None
+    for it, lr in MLP_SCHEDULE:
+        loss = ch.mlp_train(train, it, lr=lr)
+    t_train = time.perf_counter() - t0
+    ch.thermal_use_mlp(True)
+    ch.advance(args.warmup, DT0, DTMIN, CFLGV)
+    ms_m, launches_m, clk_m = timed(args.steps)
+    v_mlp = pts * args.steps * ws / (ms_m / 1000.0)
+    judge = ch.mlp_judge()
+    k_mlp = kernel_profile()
+
+    # ---- roofline of the dominant kernel (table-search step) ----
+    words = heated_kernel_words(L, M)
+    per_step = {k: (1 if k in ("k_io_cfl", "k_dt") else 3) for k in k_table}
+    peak, peak_kind = load_peaks()
+    dom = max(k_table, key=lambda k: k_table[k])
+    per_launch_ms = k_table[dom] / per_step[dom]
+    dom_bytes = words[dom] * 8.0 * pts
+    achieved = dom_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic = load_traffic(HEATED_WORKLOAD).get(dom)
+    step_bytes = sum(words[k] * 8.0 * pts * per_step[k] for k in k_table)
+    step_ms = ms_t / args.steps
+    line = {
+        "metric": METRIC, "value": v_table, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": HEATED_WORKLOAD, "grid": [L, M, N], "domain": "4pi x 2 x 4pi/3", "REN": h["REN"],
+                   "STR2": h["STR2"], "iVisScheme": 1, "thermal": "constant wall heat flux %.2f, table of 2048 rows"
+                   % h["qw"], "properties": "table search", "cuda_graph": True,
+                   "parallelism": "replicas" if ws > 1 else "single",
+                   "l2": "no flush: per-step working set %.1f GB > 126 MB L2" % (40 * 8.0 * (M + 2) * L * N / 1e9)},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": ne,
+                "api": "chapsim_upload_io_fields + chapsim_thermal_init + chapsim_advance_tg(1) + "
+                       "chapsim_download_io_fields + chapsim_download_thermal_fields"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": dom_bytes, "share_of_step": k_table[dom] / sum(k_table.values())},
+        "step_roofline": {"bytes_per_point_step": step_bytes / pts,
+                          "achieved_gbs": step_bytes / (step_ms / 1000) / 1e9,
+                          "frac": step_bytes / (step_ms / 1000) / 1e9 / peak},
+        "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(k_table.items())},
+        "clocks": clk,
+        "variants": {"learned_properties": {
+            "value": v_mlp, "unit": UNIT, "ms_per_step": ms_m / args.steps, "speedup_vs_table": v_mlp / v_table,
+            "judge_max_rel_err": judge, "bound": MLP_BOUND, "within_bound": max(judge.values()) <= MLP_BOUND,
+            "training": {"samples": int(train.size), "iterations": sum(i for i, _ in MLP_SCHEDULE),
+                         "seconds": t_train, "final_loss": loss},
+            "property_update_ms_per_step": {"table": k_table.get("k_eng_props"), "model": k_mlp.get("k_mlp_infer")},
+            "gpu_launches": int(launches_m), "clocks": clk_m}},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt = heated_cpu_rate(float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n} RK3 steps of {HEATED_WORKLOAD} on the CPU FP64 restatement (OpenMP)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ch.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def kernel_bytes(L, precision="fp64"):
     """Algorithmic bytes per grid point per launch.  FP64: 8 bytes per word of
     kernel_words.  Mixed: Q, PR, CONVH0, RHS and RHSLLPHI are 4-byte words;
@@ -211,8 +443,12 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     budget = float(os.environ.get("CHAPSIM_REF_BUDGET_S", "60"))
-    rate, n, dt = cpu_reference_rate(wl, max(args.steps, 1), budget, threads)
-    L, M, N = WORKLOADS[wl][:3]
+    if wl == HEATED_WORKLOAD:
+        rate, n, dt = heated_cpu_rate(budget, threads)
+        L, M, N = HEATED["L"], HEATED["M"], HEATED["N"]
+    else:
+        rate, n, dt = cpu_reference_rate(wl, max(args.steps, 1), budget, threads)
+        L, M, N = WORKLOADS[wl][:3]
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dt / n, "higher_is_better": True,
@@ -463,7 +699,8 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS) + [ENSEMBLE_WORKLOAD])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD,
+                    choices=sorted(WORKLOADS) + [ENSEMBLE_WORKLOAD, HEATED_WORKLOAD])
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -482,6 +719,8 @@ def main():
         return run_reference(args)
     if args.workload == ENSEMBLE_WORKLOAD:
         return run_ensemble(args)
+    if args.workload == HEATED_WORKLOAD:
+        return run_heated(args)
     return run_b200(args)
 
 

@@ -318,13 +318,18 @@ class ChannelTG:
                                                 ctypes.byref(cfl)))
         return dt.value, cfl.value
 
+    def kernel_slots(self):
+        """Names of the kernel slots of one step, in the order chapsim_profile_steps reports them."""
+        return KERNEL_SLOTS
+
     def profile_steps(self, nsteps, DT0, DTMIN, CFLGV):
         """Per-kernel durations (ms, summed over nsteps) keyed by kernel name."""
-        n = len(KERNEL_SLOTS)
+        slots = self.kernel_slots()
+        n = len(slots)
         buf = (ctypes.c_float * n)()
         self._check(self.lib.chapsim_profile_steps(self.h, int(nsteps), DT0, DTMIN, CFLGV, buf, n))
         out = {}
-        for name, v in zip(KERNEL_SLOTS, buf):
+        for name, v in zip(slots, buf):
             out[name] = out.get(name, 0.0) + float(v)
         return out
 
@@ -469,6 +474,20 @@ class ChannelIO(ChannelTG):
 
     IDOMAIN = 2
 
+    def __init__(self, setup, device: int = 0, ivisscheme: int = VIS_EXPLICIT, **kw):
+        super().__init__(setup, device=device, ivisscheme=ivisscheme, **kw)
+        self.ivisscheme = int(ivisscheme)
+        self.thermal = False
+        self.use_mlp = False
+
+    def kernel_slots(self):
+        mom = (["k_io_rhs_cn", "k_io_cn_xsweep", "k_io_cn_zysweep"] if self.ivisscheme
+               else ["k_io_divu", "k_io_rhs", "k_io_massflux"])
+        eng = (["k_eng_rhs", "k_mlp_infer" if self.use_mlp else "k_eng_props", "k_eng_bc", "k_drhodt", "k_io_props",
+                "k_g0_velocity"] if self.thermal else [])
+        sub = eng + mom + ["k_io_div_fftx", "k_fftz_fwd", "k_ysolve", "k_fftz_inv", "k_fftx_inv", "k_io_correct"]
+        return ["k_io_cfl", "k_dt"] + sub * 3
+
     def upload_io(self, G, PR, RHO, MU0, MU):
         arrs = [np.ascontiguousarray(a, np.float64) for a in (G, PR, RHO, MU0, MU)]
         if arrs[0].shape != (3,) + self.field_shape() or any(a.shape != self.field_shape() for a in arrs[1:]):
@@ -499,6 +518,7 @@ class ChannelIO(ChannelTG):
         if DH.shape != self.field_shape():
             raise ValueError("DH shape mismatch")
         self._check(self.lib.chapsim_thermal_init(self.h, _ptr(DH), float(qw_bot), float(qw_top), float(cthecd)))
+        self.thermal = True
 
     def download_thermal(self):
         """dict DH, H, T, D, M, K, CP of padded fields."""
@@ -509,6 +529,7 @@ class ChannelIO(ChannelTG):
 
     def thermal_use_mlp(self, enable=True):
         self._check(self.lib.chapsim_thermal_use_mlp(self.h, int(bool(enable))))
+        self.use_mlp = bool(enable)
 
     def mlp_judge(self):
         """Largest |model - table| / max(|table|, output scale) per output over the interior fields."""

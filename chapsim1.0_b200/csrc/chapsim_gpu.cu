@@ -965,12 +965,14 @@ int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph) {
 
 int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, float* ms,
                           int32_t nslots) {
-    // One step = 2 + 3*9 kernels launched individually with an event after
-    // each; ms[slot] accumulates the duration of kernel slot `slot` over the
-    // nsteps steps (slot 0 is timed from an event recorded before it).
-    const int per = 2 + 3 * 9;
-    if (!ctx || !ms || nslots < per || nsteps < 1) return CHAPSIM_ERR_BADARG;
-    if (ctx->thermal) return fail(ctx, CHAPSIM_ERR_BADARG, "per-kernel profiling covers the flow-only step");
+    // One step = 2 + 3*9 kernel slots (2 + 3*15 with the thermal solver of the
+    // main domain), launched individually with an event after each; ms[slot]
+    // accumulates the duration of slot `slot` over the nsteps steps (slot 0 is
+    // timed from an event recorded before it).
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    const int per = 2 + 3 * (9 + (ctx->thermal ? 6 : 0));
+    if (!ms || nslots < per || nsteps < 1)
+        return fail(ctx, CHAPSIM_ERR_BADARG, "ms must hold " + std::to_string(per) + " slots and nsteps >= 1");
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
     if (rc) return rc;

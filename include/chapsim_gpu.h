@@ -323,11 +323,17 @@ int chapsim_batch_get_stream(chapsim_batch_t* batch, void** stream);
 int chapsim_batch_destroy(chapsim_batch_t* batch);
 
 /* Profiling: runs nsteps steps (as chapsim_advance_tg, without the graph)
- * with a CUDA event after every kernel; ms[slot] receives the summed
- * duration of kernel slot `slot` of a step.  Slot order: k_cfl,
- * k_dt_factors, then for each substep k_rhs_xsweep, k_zsweep, k_ysweep,
- * k_div_fftx, k_fftz_fwd, k_ysolve, k_fftz_inv, k_fftx_inv, k_correct
- * (nslots >= 29). */
+ * with a CUDA event after every kernel slot; ms[slot] receives the summed
+ * duration of slot `slot` of a step.  Periodic channel: k_cfl, k_dt_factors,
+ * then for each substep k_rhs_xsweep, k_zsweep, k_ysweep, k_div_fftx,
+ * k_fftz_fwd, k_ysolve, k_fftz_inv, k_fftx_inv, k_correct (29 slots).
+ * Main domain: k_io_cfl, k_dt, then for each substep (with the thermal
+ * solver) k_eng_rhs, the property update (table search or model), k_eng_bc,
+ * k_drhodt, k_io_props, k_g0_velocity, then the momentum step's three
+ * slots (explicit: k_io_divu, k_io_rhs, k_io_massflux; Crank-Nicolson:
+ * k_io_rhs, the x sweep, the z and y sweeps) and k_io_div_fftx, k_fftz_fwd,
+ * k_ysolve, k_fftz_inv, k_fftx_inv, k_io_correct (29 slots, 47 with the
+ * thermal solver). */
 int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dtmin, double cflgv, float* ms,
                           int32_t nslots);
 
