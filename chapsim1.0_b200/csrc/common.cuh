@@ -68,6 +68,17 @@ __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {
 __device__ __forceinline__ long long iidx(const Geo& g, int i, int j, int k) {
     return (long long)i + (long long)g.L * ((long long)(j - 1) + (long long)g.M * (long long)k);
 }
+// Point index t = i + L*((j-1) + M*k) of the interior to (i, j, k).  Grids
+// have at most 384^3 < 2^31 points, so 32-bit unsigned division is exact
+// (and an order of magnitude cheaper than 64-bit division on the GPU).
+__device__ __forceinline__ void io_decode(const Geo& g, long long t, int& i, int& j, int& k) {
+    const unsigned u = (unsigned)t, L = (unsigned)g.L, M = (unsigned)g.M;
+    const unsigned r = u / L;
+    i = (int)(u - r * L);
+    const unsigned kk = r / M;
+    j = 1 + (int)(r - kk * M);
+    k = (int)kk;
+}
 __device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
 __device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
 
@@ -100,6 +111,9 @@ __device__ __forceinline__ double block_max(double v, double* sbuf) {
     }
     return r;
 }
+
+// Hint that a cache line is about to be read (no register or completion cost).
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // 8-byte asynchronous global -> shared copy (no register staging).
 __device__ __forceinline__ void cp_async8(double* smem_dst, const double* gsrc) {

@@ -31,12 +31,6 @@ struct IoFields {
     double *G, *Q, *PR, *EX0, *RHS, *RHO, *MU0, *MU, *DST, *MST, *DIVU, *DEN;
 };
 
-__device__ __forceinline__ void io_decode(const Geo& g, long long t, int& i, int& j, int& k) {
-    i = (int)(t % g.L);
-    const long long r = t / g.L;
-    j = 1 + (int)(r % g.M);
-    k = (int)(r / g.M);
-}
 
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFields f) {

@@ -180,6 +180,17 @@ struct MlpOut {
 
 constexpr int MLP_INF_SMEM = 1024 + 64 * 64 * 2 + 16 * 64 * 2 + 128 * 64 * 2;
 
+// Hardware tanh (PTX tanh.approx.f32, one MUFU operation; maximum relative
+// error about 2^-11).  Inference uses it: every hidden activation is rounded
+// to BF16 (relative 2^-9) right after, so the approximation sits below the
+// precision the tensor-core layers carry.  Training keeps tanhf, the
+// activation of the CPU oracle's gradient check.
+__device__ __forceinline__ float tanh_mufu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 template <bool FIELD>
 __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ par, MlpOperands ops, MlpNorm nm, PropTab tb,
                                                       Geo g, long long npts, const double* __restrict__ dh, MlpOut out,
@@ -217,17 +228,14 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
         long long idx = p;
         if (FIELD && p < npts) {
             int i, j, k;
-            i = (int)(p % g.L);
-            const long long r = p / g.L;
-            j = 1 + (int)(r % g.M);
-            k = (int)(r / g.M);
+            io_decode(g, p, i, j, k);
             idx = pidx(g, i, j, k);
         }
         const double v = p < npts ? dh[idx] : (double)nm.x_lo;
         const float x = mlp_x(nm, v);
         float h[MLP_H];
 #pragma unroll
-        for (int i = 0; i < MLP_H; ++i) h[i] = tanhf(fmaf(sw1[i], x, sb1[i]));
+        for (int i = 0; i < MLP_H; ++i) h[i] = tanh_mufu(fmaf(sw1[i], x, sb1[i]));
         put_row64(sA, MLP_TILE, tid, h);
         fence_async_smem();
         tc_fence_before();
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
             tmem_ld16(tmem + lane_base + 16 * q, acc);
             tmem_ld_wait();
 #pragma unroll
-            for (int c = 0; c < 16; ++c) h[16 * q + c] = tanhf(acc[c] + sb2[16 * q + c]);
+            for (int c = 0; c < 16; ++c) h[16 * q + c] = tanh_mufu(acc[c] + sb2[16 * q + c]);
         }
         put_row64(sA, MLP_TILE, tid, h);
         fence_async_smem();
@@ -560,9 +568,8 @@ __global__ void __launch_bounds__(PROP_NT) k_mlp_judge(PropTab tb, MlpNorm nm, G
     const long long tot = (long long)g.L * g.M * g.N;
     float e[MLP_OUT] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(q % g.L);
-        const long long r = q / g.L;
-        const int j = 1 + (int)(r % g.M), k = (int)(r / g.M);
+        int i, j, k;
+        io_decode(g, q, i, j, k);
         const long long idx = pidx(g, i, j, k);
         double o[6];
         prop_point(tb, tb.xdh, tb.xh, DH[idx], o);

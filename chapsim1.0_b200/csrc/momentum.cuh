@@ -36,9 +36,11 @@
 #include "tdma.cuh"
 
 #define RHS_WPB 4       // x lines (warps) per block
-#ifndef RHS_MINB
-#define RHS_MINB 4      // resident blocks per SM the register budget is sized for
-#endif
+// Resident blocks per SM the register budget of k_rhs_xsweep is sized for:
+// FP64 at 3 (about 168 registers, no spills) ran 5 % faster at 128^3 and 19 %
+// at 384 x 256 x 384 than at 4 (128 registers with spills); FP32 is fastest
+// at 4.
+#define RHS_MINB(R) (sizeof(R) == 8 ? 3 : 4)
 #define SWEEP_NT 256
 #define FAC_SET (TF_NF(12) * 32)   // doubles per factor table
 
@@ -100,7 +102,7 @@ __global__ void __launch_bounds__(32) k_factors(Geo g, T* __restrict__ fac, cons
 
 // ---------------------------------------------------------------------------
 template <int S, typename R>
-__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
+__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
                                                              R* __restrict__ H0, R* __restrict__ RHS,
                                                              double* __restrict__ partial, DevState* __restrict__ st,
                                                              const R* __restrict__ fac, int ns) {
@@ -136,6 +138,21 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB) k_rhs_xsweep(Geo g, co
     const long long rowkp = pidx(g, 0, j, kp), rowkm = pidx(g, 0, j, km);
     const long long rowjpkm = pidx(g, 0, jp, km), rowjmkp = pidx(g, 0, jm, kp);
     const long long irow = iidx(g, 0, j, k);
+    // The line's own rows (Q, PR, CONVH0 at (j, k)) are what this kernel reads
+    // from DRAM; the neighbour rows are other lines' own rows, fetched by their
+    // warps at about the same time.  Requesting the later segments up front
+    // keeps DRAM busy while the first segment is computed.
+#pragma unroll
+    for (int kk = 1; kk < S; ++kk) {
+        const int i = lane + 32 * kk;
+        prefetch_l2(U + rowc + i);
+        prefetch_l2(V + rowc + i);
+        prefetch_l2(W + rowc + i);
+        prefetch_l2(PR + rowc + i);
+        prefetch_l2(H0 + irow + i);
+        prefetch_l2(H0 + irow + i + g.FI);
+        prefetch_l2(H0 + irow + i + 2 * g.FI);
+    }
     double bulk = 0.0;
 #pragma unroll 1
     for (int kk = 0; kk < S; ++kk) {

@@ -135,13 +135,10 @@ __global__ void __launch_bounds__(PROP_NT) k_prop_fields(PropTab tb, Geo g, cons
         xdh = keys;
         xh = keys + tb.n;
     }
-    const long long LM = (long long)g.L * g.M;
-    const long long tot = LM * g.N;
+    const long long tot = (long long)g.L * g.M * g.N;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(q / LM);
-        const long long r = q - k * LM;
-        const int j = 1 + (int)(r / g.L);
-        const int i = (int)(r - (long long)(j - 1) * g.L);
+        int i, j, k;
+        io_decode(g, q, i, j, k);
         const long long p = pidx(g, i, j, k);
         double o[6];
         if (!prop_point(tb, xdh, xh, __ldg(dh + p), o)) prop_flag(st, (unsigned long long)p);

@@ -3,8 +3,10 @@ against the CPU oracle of the same network, and against the table search it
 replaces.
 
 * forward: model outputs for the same parameters agree with the oracle to
-  2e-3 of each output's scale (the GPU rounds h1, h2 to BF16 after FP32
-  tanhf; a one-ulp difference in tanhf can move a BF16 rounding);
+  5e-3 of each output's scale.  Inference takes the hardware tanh
+  (tanh.approx.f32, relative error up to about 2^-11) where the oracle takes
+  libm's tanhf, and both round h1, h2 to BF16 (2^-9) after it; a layout or
+  indexing fault would show as errors of order 1;
 * gradients of one pass agree with the oracle to 1e-2 of the largest entry
   of each parameter group (FP32 atomics and accumulation order vs FP64);
 * outside the trained range the result is the table search, bitwise;
@@ -46,7 +48,7 @@ def test_forward_matches_oracle(setup):
     for m, k in enumerate(FIELDS):
         err = np.abs(got[k] - want[k]).max() / nm[8 + m]
         print(k, err)
-        assert err <= 2e-3, (k, err)
+        assert err <= 5e-3, (k, err)
 
 
 def test_gradients_match_oracle(setup):
