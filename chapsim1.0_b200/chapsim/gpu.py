@@ -36,7 +36,13 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_download_thermal_fields", "chapsim_mlp_init", "chapsim_mlp_set_params", "chapsim_mlp_get_params",
             "chapsim_mlp_gradients", "chapsim_mlp_train", "chapsim_mlp_infer_points", "chapsim_thermal_use_mlp",
             "chapsim_mlp_judge", "chapsim_autotune", "chapsim_batch_create", "chapsim_batch_advance",
-            "chapsim_batch_get_stream", "chapsim_batch_destroy"]
+            "chapsim_batch_get_stream", "chapsim_batch_destroy", "chapsim_pp_mean_zx_tg", "chapsim_pp_mean_t_tg",
+            "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg"]
+
+# the arrays of one set of x-z means (postprocess_info), their widths per y row
+PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
+PP_MONITOR = ["U1c", "U1c_t", "U2c", "U2c_t", "U3c", "U3c_t", "uu", "uu_t", "uv", "uv_t", "vv", "vv_t", "ww", "ww_t",
+              "Cf_bottom", "Cf_bottom_t", "Cf_top", "Cf_top_t", "U1mean", "U1maxx"]
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
@@ -124,6 +130,11 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_thermal_use_mlp.argtypes = [vp, ctypes.c_int32]
     L.chapsim_mlp_judge.argtypes = [vp, _dp]
     L.chapsim_autotune.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]
+    L.chapsim_pp_mean_zx_tg.argtypes = [vp]
+    L.chapsim_pp_mean_t_tg.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
+    L.chapsim_pp_monitor_tg.argtypes = [vp, ctypes.c_double, _dp]
+    L.chapsim_download_pp_means_tg.argtypes = [vp, ctypes.c_int32] + [_dp] * 7 + [ctypes.POINTER(ctypes.c_int32)]
+    L.chapsim_upload_pp_means_tg.argtypes = [vp, ctypes.c_int32] + [_dp] * 7
     L.chapsim_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(vp)]
     L.chapsim_batch_advance.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     L.chapsim_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -317,6 +328,40 @@ class ChannelTG:
         self._check(self.lib.chapsim_advance_tg(self.h, int(nsteps), DT0, DTMIN, CFLGV, ctypes.byref(dt),
                                                 ctypes.byref(cfl)))
         return dt.value, cfl.value
+
+    # -- statistics (POSTPROCESS_TG) -----------------------------------------------
+    def PP_MEAN_ZX_FLOW_TG(self):
+        self._check(self.lib.chapsim_pp_mean_zx_tg(self.h))
+
+    def PP_MEAN_T_TG(self, TP=1, pp_instn_sz=1):
+        self._check(self.lib.chapsim_pp_mean_t_tg(self.h, int(TP), int(pp_instn_sz)))
+
+    def PP_MONITOR_TG(self, REN):
+        """dict of the monitor quantities (instantaneous and time-averaged, at j = NCL2/2), Cf and U1mean."""
+        mon = np.zeros(20)
+        self._check(self.lib.chapsim_pp_monitor_tg(self.h, float(REN), _ptr(mon)))
+        return dict(zip(PP_MONITOR, mon.tolist()))
+
+    def download_pp_means(self, averaged=False):
+        """(flat set of 122*M doubles in the order of PP_ARRAYS, NSTATIS_TG)"""
+        M = self.M
+        flat = np.zeros(122 * M)
+        ptrs, o = [], 0
+        for _, w in PP_ARRAYS:
+            ptrs.append(_ptr(flat[o * M:(o + w) * M]))
+            o += w
+        n = ctypes.c_int32()
+        self._check(self.lib.chapsim_download_pp_means_tg(self.h, int(bool(averaged)), *ptrs, ctypes.byref(n)))
+        return flat, n.value
+
+    @staticmethod
+    def pp_split(flat, M):
+        """dict name -> numpy array of the Fortran shape (M, w) given as (w, M) (j fastest)."""
+        out, o = {}, 0
+        for name, w in PP_ARRAYS:
+            out[name] = flat[o * M:(o + w) * M].reshape(w, M)
+            o += w
+        return out
 
     def kernel_slots(self):
         """Names of the kernel slots of one step, in the order chapsim_profile_steps reports them."""

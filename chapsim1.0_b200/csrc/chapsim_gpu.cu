@@ -17,6 +17,7 @@
 #include "tdma.cuh"
 #include "io.cuh"
 #include "io_cn.cuh"
+#include "stats.cuh"
 #include "thermo.cuh"
 #include "thermal.cuh"
 #include "mlp.cuh"
@@ -138,6 +139,7 @@ struct chapsim_ctx {
     Geo g{};
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr;
     double* HS = nullptr;         // forward factors of the sequential y-solve (allocated when chosen)
+    double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
     int k1_split = 0;             // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep (chapsim_autotune)
     double2* SP = nullptr;
@@ -156,6 +158,10 @@ struct chapsim_ctx {
     double2* tw = nullptr;
     int domain = 1;               // 1: periodic TG channel, 2: main domain (IO)
     int ivis = 0;                 // main domain: 0 explicit viscous terms, 1 Crank-Nicolson (iVisScheme)
+    // statistics of the periodic channel (stats.cuh), allocated by the first call
+    double *pp_inst = nullptr, *pp_avg = nullptr, *pp_part = nullptr, *pp_mon = nullptr;
+    int pp_nchunk = 0;
+    int nstatis = 0;              // NSTATIS_TG
     IoFields io{};                // IO-path arrays (domain 2)
     int io_grid = 0;              // blocks of the IO point-wise kernels
     cudaGraphExec_t step_exec = nullptr;
@@ -250,7 +256,7 @@ cudaError_t upload_small_twiddles() {
     }
     return e;
 }
-size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(double2) + (size_t)g.M * sizeof(double); }
+size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(double2); }
 
 // forward declaration: DISPATCH_S is defined below
 void launch_ysolve_warp(chapsim_ctx* ctx);
@@ -670,6 +676,9 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     g.cvisc = cf->cvisc; g.volm = cf->volm; g.cf_given = cf->cf_given; g.iflowdriven = cf->iflowdriven;
     g.fix_v_wall_row = opts ? opts->fix_v_wall_row : 0;
     for (int s = 0; s < 4; ++s) { g.tgam[s] = cf->tgam[s]; g.troh[s] = cf->troh[s]; g.talp[s] = cf->talp[s]; }
+    g.area_inlet = 0.0;  // COORDJR's loop order (RCCI1 = 1)
+    for (int jc = 0; jc < M; ++jc)
+        for (int kc = 0; kc < N; ++kc) g.area_inlet = g.area_inlet + 1.0 / 1.0 / cf->dyfi[jc] / cf->dzi;
     g.amvr1 = ivis == CHAPSIM_VIS_IMPLICIT ? cf->amvr1 : 0.0;
     g.apvrn = ivis == CHAPSIM_VIS_IMPLICIT ? cf->apvrn : 0.0;
     // y arrays with the reference's 1-based index (entry 0 unused)
@@ -714,6 +723,10 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaMemcpy(ctx->tw, twx.data(), L * sizeof(double2), cudaMemcpyHostToDevice));
     INIT_CK(cudaMemcpy(ctx->tw + L, twz.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
     g.twx = ctx->tw; g.twz = ctx->tw + L;
+    INIT_CK(cudaMalloc(&ctx->yz, (size_t)2 * M * sizeof(double)));
+    g.yz = ctx->yz;
+    k_ysolve_zero_factors<<<1, 32, 0, ctx->stream>>>(g, ctx->yz);
+    INIT_CK(cudaGetLastError());
     // fields
     INIT_CK(cudaMalloc(&ctx->Q, (size_t)(3 * g.FS) * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->PR, (size_t)g.FS * sizeof(double)));
@@ -790,7 +803,8 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
     cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
-    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw);
+    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->yz);
+    cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
@@ -937,6 +951,120 @@ int chapsim_divgck_tg(chapsim_ctx_t* ctx, double* maxdiv) {
     CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     *maxdiv = ctx->st_host->maxdiv;
+    return CHAPSIM_OK;
+}
+
+// ---- statistics of the periodic channel ----
+namespace {
+int pp_ensure(chapsim_ctx* ctx) {
+    if (ctx->domain != 1) return fail(ctx, CHAPSIM_ERR_BADARG, "the x-z statistics cover the periodic TG domain");
+    if (ctx->pp_inst) return CHAPSIM_OK;
+    const Geo& g = ctx->g;
+    const size_t nset = (size_t)PP_PER_ROW * g.M;
+    int nchunk = (4 * ctx->nsm + g.M - 1) / g.M;
+    nchunk = std::max(1, std::min(nchunk, g.L * g.N / PP_NT));
+    ctx->pp_nchunk = nchunk;
+    CK(cudaMalloc(&ctx->pp_inst, nset * sizeof(double)));
+    CK(cudaMalloc(&ctx->pp_avg, nset * sizeof(double)));
+    CK(cudaMalloc(&ctx->pp_part, (size_t)g.M * nchunk * PP_NACC * sizeof(double)));
+    CK(cudaMalloc(&ctx->pp_mon, 20 * sizeof(double)));
+    CK(cudaMemsetAsync(ctx->pp_inst, 0, nset * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(ctx->pp_avg, 0, nset * sizeof(double), ctx->stream));
+    ctx->nstatis = 0;
+    return CHAPSIM_OK;
+}
+// the seven arrays of one set, in storage order, with their widths
+const int pp_width[7] = {4, 3, 6, 10, 9, 9, 81};
+const int pp_off[7] = {PP_U1, PP_UP, PP_U2, PP_U3, PP_D1, PP_DP, PP_D2};
+}  // namespace
+
+int chapsim_pp_mean_zx_tg(chapsim_ctx_t* ctx) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = pp_ensure(ctx);
+    if (rc) return rc;
+    const Geo& g = ctx->g;
+    dim3 grid(ctx->pp_nchunk, g.M);
+    if (ctx->prec == CHAPSIM_PREC_MIXED)
+        k_pp_mean_zx<float><<<grid, PP_NT, 0, ctx->stream>>>(g, ctx->Qf, ctx->PRf, ctx->pp_part);
+    else
+        k_pp_mean_zx<double><<<grid, PP_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->PR, ctx->pp_part);
+    k_pp_finish<<<g.M, PP_NT, 0, ctx->stream>>>(g, ctx->pp_part, ctx->pp_nchunk, ctx->pp_inst);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+
+int chapsim_pp_mean_t_tg(chapsim_ctx_t* ctx, int32_t tp, int32_t pp_instn_sz) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (tp != 1 && tp != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "TP must be T_Asymptotic_Average (1) or T_Summing_average (2)");
+    if (tp == 2 && pp_instn_sz < 1) return fail(ctx, CHAPSIM_ERR_BADARG, "pp_instn_sz must be >= 1");
+    CK(cudaSetDevice(ctx->device));
+    int rc = pp_ensure(ctx);
+    if (rc) return rc;
+    ctx->nstatis += 1;
+    double coe2, coe3;
+    if (tp == 1) {
+        coe2 = 1.0 / (double)ctx->nstatis;
+        coe3 = (double)(ctx->nstatis - 1) / (double)ctx->nstatis;
+    } else {
+        coe2 = 1.0 / (double)pp_instn_sz;
+        coe3 = 1.0;
+    }
+    const long long n = (long long)PP_PER_ROW * ctx->g.M;
+    k_pp_time_average<<<(int)std::min<long long>((n + 255) / 256, 4LL * ctx->nsm), 256, 0, ctx->stream>>>(
+        ctx->pp_avg, ctx->pp_inst, n, coe2, coe3);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+
+int chapsim_pp_monitor_tg(chapsim_ctx_t* ctx, double ren, double* mon) {
+    if (!ctx || !mon || !(ren > 0.0)) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = pp_ensure(ctx);
+    if (rc) return rc;
+    k_pp_monitor<<<1, 32, 0, ctx->stream>>>(ctx->g, ctx->pp_inst, ctx->pp_avg, ren, ctx->pp_mon);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(mon, ctx->pp_mon, 20 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+int chapsim_download_pp_means_tg(chapsim_ctx_t* ctx, int32_t averaged, double* u1, double* up, double* u2,
+                                 double* u3, double* dvdl1, double* dvdlp, double* dvdl2, int32_t* nstatis) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = pp_ensure(ctx);
+    if (rc) return rc;
+    const double* src = averaged ? ctx->pp_avg : ctx->pp_inst;
+    double* dst[7] = {u1, up, u2, u3, dvdl1, dvdlp, dvdl2};
+    const size_t M = (size_t)ctx->g.M;
+    for (int a = 0; a < 7; ++a)
+        if (dst[a])
+            CK(cudaMemcpyAsync(dst[a], src + pp_off[a] * M, pp_width[a] * M * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (nstatis) *nstatis = ctx->nstatis;
+    return CHAPSIM_OK;
+}
+
+int chapsim_upload_pp_means_tg(chapsim_ctx_t* ctx, int32_t nstatis, const double* u1, const double* up,
+                               const double* u2, const double* u3, const double* dvdl1, const double* dvdlp,
+                               const double* dvdl2) {
+    if (!ctx || nstatis < 0) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    int rc = pp_ensure(ctx);
+    if (rc) return rc;
+    const double* src[7] = {u1, up, u2, u3, dvdl1, dvdlp, dvdl2};
+    const size_t M = (size_t)ctx->g.M;
+    for (int a = 0; a < 7; ++a)
+        if (src[a])
+            CK(cudaMemcpyAsync(ctx->pp_avg + pp_off[a] * M, src[a], pp_width[a] * M * sizeof(double),
+                               cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->nstatis = nstatis;
     return CHAPSIM_OK;
 }
 

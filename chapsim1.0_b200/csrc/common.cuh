@@ -57,9 +57,11 @@ struct Geo {
     const double* ak3;   // [N]  modified wavenumbers in z, 0-based kz
     double tgam[4], troh[4], talp[4];
     double amvr1, apvrn;  // wall-row factors of the Crank-Nicolson y sweep of the main domain
+    double area_inlet;    // Area_inlet (src/COORDJR.f90:367-373)
     // FFT twiddles
     const double2* twx;  // [L] exp(-2 pi i e / L)
     const double2* twz;  // [N]
+    const double* yz;    // [2M] factors of the zero-mode y recurrence (k_ysolve_zero_factors)
 };
 
 __device__ __forceinline__ long long pidx(const Geo& g, int i, int j, int k) {

@@ -132,21 +132,44 @@ struct PoisCoef {
     __device__ __forceinline__ double C(int r) const { return ap[r + 1]; }
 };
 
+// Factors of the zero-mode recurrence (kx = kz = 0, phi(y_1) pinned): the
+// forward sweep's pivots pp[j-1] = 1/((ACPH(j) + shift) - H(j-1) AMPH(j)) and
+// multipliers hz[j-1] = H(j).  They depend on the operator only (not on dt or
+// the right-hand side), so they are formed once, by the expression the
+// sweep itself would evaluate, and the per-substep zero-mode solve is a chain
+// of multiply-adds.  zf[0..M) = pp, zf[M..2M) = hz.
+__global__ void k_ysolve_zero_factors(Geo g, double* __restrict__ zf) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int M = g.M;
+    const double shift = (-g.ak1[0] / 1.0 - g.ak3[0]);
+    const double b = g.acph[1] + shift;
+    double hp = 0.0 / b;
+    zf[0] = 1.0 / b;
+    zf[M] = hp;
+    for (int j = 2; j <= M; ++j) {
+        const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
+        hp = j < M ? g.apph[j] * pp : 0.0;
+        zf[j - 1] = pp;
+        zf[M + j - 1] = hp;
+    }
+}
+
 template <int S>
 __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __restrict__ SP) {
     extern __shared__ double2 smc[];
+    static_assert(YW_NT % YW_L == 0, "a thread keeps one line in the staging loops");
     const int M = 32 * S, LH = g.LH;
     const int LS = M + 33;
     const long long nl = (long long)LH * g.N;
     const long long q0 = (long long)blockIdx.x * YW_L;
     const int nq = (int)min((long long)YW_L, nl - q0);
-    for (int p = threadIdx.x; p < YW_L * M; p += YW_NT) {
-        const int l = p % YW_L, j = p / YW_L;
-        if (l < nq) {
-            const long long q = q0 + l;
-            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-            cp_async16(smc + l * LS + seg_pos<S>(j), SP + kx + (long long)LH * (j + (long long)M * kz));
-        }
+    // the staging loops: thread t moves line t % YW_L, rows t / YW_L + (YW_NT / YW_L) * it
+    const int ls = threadIdx.x % YW_L, js = threadIdx.x / YW_L;
+    const long long qs = q0 + ls;
+    const int kzs = (int)(qs / LH), kxs = (int)(qs - (long long)kzs * LH);
+    double2* const gsrc = SP + kxs + (long long)LH * ((long long)M * kzs);
+    if (ls < nq) {
+        for (int j = js; j < M; j += YW_NT / YW_L) cp_async16(smc + ls * LS + seg_pos<S>(j), gsrc + (long long)LH * j);
     }
     cp_async_wait_all();
     __syncthreads();
@@ -158,25 +181,23 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __rest
         if (q == 0) {
             // zero mode: phi(y_1) = 0 and the reference's forward/backward recurrence
             if (lane == 0) {
-                double* hz = reinterpret_cast<double*>(smc + YW_L * LS);  // M doubles
-                const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-                const double b = g.acph[1] + shift;
-                double hp = 0.0 / b;
-                double2 gp = make_double2(0.0 / b, 0.0 / b);
-                hz[0] = hp;
+                const double* pp = g.yz;
+                const double* hz = g.yz + M;
+                double2 gp = make_double2(0.0 * pp[0], 0.0 * pp[0]);
                 base[seg_pos<S>(0)] = gp;
+#pragma unroll 4
                 for (int j = 2; j <= M; ++j) {
-                    const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
                     const double2 rj = base[seg_pos<S>(j - 1)];
-                    gp = make_double2((rj.x - g.amph[j] * gp.x) * pp, (rj.y - g.amph[j] * gp.y) * pp);
-                    hp = j < M ? g.apph[j] * pp : 0.0;
-                    hz[j - 1] = hp;
+                    const double am = g.amph[j], p = pp[j - 1];
+                    gp = make_double2((rj.x - am * gp.x) * p, (rj.y - am * gp.y) * p);
                     base[seg_pos<S>(j - 1)] = gp;
                 }
                 double2 xn = gp;
+#pragma unroll 4
                 for (int j = M - 1; j >= 1; --j) {
                     const double2 gj = base[seg_pos<S>(j - 1)];
-                    xn = make_double2(gj.x - hz[j - 1] * xn.x, gj.y - hz[j - 1] * xn.y);
+                    const double h = hz[j - 1];
+                    xn = make_double2(gj.x - h * xn.x, gj.y - h * xn.y);
                     base[seg_pos<S>(j - 1)] = xn;
                 }
             }
@@ -191,13 +212,8 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __rest
         }
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < YW_L * M; p += YW_NT) {
-        const int l = p % YW_L, j = p / YW_L;
-        if (l < nq) {
-            const long long q = q0 + l;
-            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-            SP[kx + (long long)LH * (j + (long long)M * kz)] = smc[l * LS + seg_pos<S>(j)];
-        }
+    if (ls < nq) {
+        for (int j = js; j < M; j += YW_NT / YW_L) gsrc[(long long)LH * j] = smc[ls * LS + seg_pos<S>(j)];
     }
 }
 

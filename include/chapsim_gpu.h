@@ -297,6 +297,33 @@ int chapsim_thermal_use_mlp(chapsim_ctx_t* ctx, int32_t enable);
  * steps and switches back to the table when it exceeds its bound. */
 int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err);
 
+/* ---- Statistics of the periodic channel (POSTPROCESS_TG, src/processing/POSTPROESS.f90:11-51) ----
+ * Computed on the device from the resident fields, so the driver needs no
+ * per-step download of Q.  Arrays are the postprocess_info module arrays in
+ * Fortran order, M = NCL2: U1xzL_tg(M, 4), UPxzL_tg(M, 3), U2xzL_tg(M, 6),
+ * U3xzL_tg(M, 10), DVDL1xzL_tg(M, 3, 3), DVDLPxzL_tg(M, 3, 3), DVDL2xzL_tg(M, 9, 9);
+ * the time averages (U1xztL_tg ...) have the same shapes.  Sums over the x-z
+ * plane are taken in a fixed tree order instead of the reference's I, K loop. */
+/* PP_MEAN_ZX_FLOW_TG (src/processing/PP_MEAN_ZX.f90:14-307): instantaneous means. */
+int chapsim_pp_mean_zx_tg(chapsim_ctx_t* ctx);
+/* PP_MEAN_T_TG(TP) (src/processing/PP_MEAN_T.f90:343-392): NSTATIS_TG += 1 and
+ * avg = COE3 avg + COE2 inst; tp = 1 (T_Asymptotic_Average) or 2
+ * (T_Summing_average, with pp_instn_sz). */
+int chapsim_pp_mean_t_tg(chapsim_ctx_t* ctx, int32_t tp, int32_t pp_instn_sz);
+/* PP_MONITOR_TG (src/processing/PP_SCN_MONITOR.f90:147-251) quantities from the
+ * current instantaneous and averaged means: mon[20] = U1_XZT(1:6), UU_XZT(1:8),
+ * CF_XZT(1:4), U1mean_WORK_tg, U1maxx_WORK_tg (the last two of
+ * PP_MEAN_ZX_FLOW_TG :294-305).  ren = REN. */
+int chapsim_pp_monitor_tg(chapsim_ctx_t* ctx, double ren, double* mon);
+/* Downloads the instantaneous (averaged = 0) or time-averaged (1) means; any
+ * pointer may be NULL; nstatis receives NSTATIS_TG. */
+int chapsim_download_pp_means_tg(chapsim_ctx_t* ctx, int32_t averaged, double* u1, double* up, double* u2,
+                                 double* u3, double* dvdl1, double* dvdlp, double* dvdl2, int32_t* nstatis);
+/* Restart of the time averages (the reader of the averaged-statistics file). */
+int chapsim_upload_pp_means_tg(chapsim_ctx_t* ctx, int32_t nstatis, const double* u1, const double* up,
+                               const double* u2, const double* u3, const double* dvdl1, const double* dvdlp,
+                               const double* dvdl2);
+
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps

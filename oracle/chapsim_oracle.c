@@ -2218,3 +2218,149 @@ void orc_io_monitor(orc_t* o, double* out) {
     (void)g1c; (void)dc;
     out[0] = uc; out[1] = uu; out[2] = uv; out[3] = gmax; out[4] = rate / 2.0;
 }
+
+
+/* ====================================================================== */
+/* Statistics of the periodic channel (POSTPROCESS_TG).  The means of one  */
+/* set are stored as out[122*M]: U1xzL(M,4) | UPxzL(M,3) | U2xzL(M,6) |    */
+/* U3xzL(M,10) | DVDL1xzL(M,3,3) | DVDLPxzL(M,3,3) | DVDL2xzL(M,9,9),      */
+/* Fortran order (j fastest).  Plane channel: RCCI1 = RNDI1 = 1.           */
+/* ====================================================================== */
+#define PPA(arr, off, J, c) (arr)[(size_t)((off) + (c)) * M + (size_t)((J) - 1)]
+
+/* PP_MEAN_ZX_FLOW_TG (src/processing/PP_MEAN_ZX.f90:14-307), loop order J, I, K */
+void orc_pp_mean_zx_tg(const orc_t* o, double* out) {
+    const int L = o->L, M = o->M, N = o->N;
+    const double VL = 1.0 / (double)(L * N);
+    const double COE0 = VL, COE1 = VL * 0.5, COE2 = VL * (0.5 * 0.5), COE3 = VL * (0.5 * 0.5 * 0.5);
+    double COG1[3][3] = {{VL * o->DXI, VL * 0.25, VL * 0.25 * o->DZI},
+                         {VL * 0.25 * o->DXI, VL, VL * 0.25 * o->DZI},
+                         {VL * 0.25 * o->DXI, VL * 0.25, VL * o->DZI}};
+#pragma omp parallel for schedule(static)
+    for (int J = 1; J <= M; ++J) {
+        const int JP = J + 1, JM = J - 1, JJ = J, JJP = J + 1;
+        double U1[4] = {0}, UP[3] = {0}, U2[6] = {0}, U3[10] = {0}, D1[3][3] = {{0}}, DP[3][3] = {{0}};
+        double D2[9][9];
+        memset(D2, 0, sizeof(D2));
+        for (int I = 1; I <= L; ++I) {
+            const int IP = IPV(o, I), IM = IMV(o, I);
+            for (int K = 1; K <= N; ++K) {
+                const int KP = KPV(o, K), KM = KMV(o, K);
+                double U[3], UJP[3], UJM[3], UKP[3], UKM[3], UIP[3], UIM[3];
+                U[0] = QV(o, I, J, K, 1) + QV(o, IP, J, K, 1);
+                UJP[0] = QV(o, I, JP, K, 1) + QV(o, IP, JP, K, 1);
+                UJM[0] = QV(o, I, JM, K, 1) + QV(o, IP, JM, K, 1);
+                UKP[0] = QV(o, I, J, KP, 1) + QV(o, IP, J, KP, 1);
+                UKM[0] = QV(o, I, J, KM, 1) + QV(o, IP, J, KM, 1);
+                U[2] = (QV(o, I, J, K, 3) + QV(o, I, J, KP, 3)) * 1.0;
+                UIP[2] = (QV(o, IP, J, K, 3) + QV(o, IP, J, KP, 3)) * 1.0;
+                UIM[2] = (QV(o, IM, J, K, 3) + QV(o, IM, J, KP, 3)) * 1.0;
+                UJP[2] = (QV(o, I, JP, K, 3) + QV(o, I, JP, KP, 3)) * 1.0;
+                UJM[2] = (QV(o, I, JM, K, 3) + QV(o, I, JM, KP, 3)) * 1.0;
+                U[1] = (QV(o, I, J, K, 2) + QV(o, I, JP, K, 2)) * 1.0;
+                UIP[1] = (QV(o, IP, J, K, 2) + QV(o, IP, JP, K, 2)) * 1.0;
+                UIM[1] = (QV(o, IM, J, K, 2) + QV(o, IM, JP, K, 2)) * 1.0;
+                UKP[1] = (QV(o, I, J, KP, 2) + QV(o, I, JP, KP, 2)) * 1.0;
+                UKM[1] = (QV(o, I, J, KM, 2) + QV(o, I, JP, KM, 2)) * 1.0;
+                const double P = F3(o->PR, o, I, J, K);
+                for (int m = 0; m < 3; ++m) {
+                    U1[m] = U1[m] + U[m];
+                    UP[m] = UP[m] + U[m] * P;
+                }
+                U1[3] = U1[3] + P;
+                for (int m = 1; m <= 3; ++m)
+                    for (int n = m; n <= 3; ++n) {
+                        int l = (m * (7 - m)) / 2 + n - 3;
+                        U2[l - 1] = U2[l - 1] + U[m - 1] * U[n - 1];
+                    }
+                for (int m = 1; m <= 3; ++m)
+                    for (int n = m; n <= 3; ++n)
+                        for (int h = n; h <= 3; ++h) {
+                            int l = m * (6 - m) + (n * (7 - n)) / 2 + h - 8;
+                            U3[l - 1] = U3[l - 1] + U[m - 1] * U[n - 1] * U[h - 1];
+                        }
+                double D[3][3];
+                D[0][0] = QV(o, IP, J, K, 1) - QV(o, I, J, K, 1);
+                D[0][1] = (UJP[0] - U[0]) * o->DYCI[JJP] + (U[0] - UJM[0]) * o->DYCI[JJ];
+                D[0][2] = UKP[0] - UKM[0];
+                D[1][0] = UIP[1] - UIM[1];
+                D[1][1] = (QV(o, I, JP, K, 2) * 1.0 - QV(o, I, J, K, 2) * 1.0) * o->DYFI[JJ];
+                D[1][2] = UKP[1] - UKM[1];
+                D[2][0] = UIP[2] - UIM[2];
+                D[2][1] = (UJP[2] - U[2]) * o->DYCI[JJP] + (U[2] - UJM[2]) * o->DYCI[JJ];
+                D[2][2] = QV(o, I, J, KP, 3) * 1.0 - QV(o, I, J, K, 3) * 1.0;
+                for (int m = 0; m < 3; ++m)
+                    for (int n = 0; n < 3; ++n) {
+                        D1[m][n] = D1[m][n] + D[m][n];
+                        DP[m][n] = DP[m][n] + D[m][n] * P;
+                    }
+                for (int m = 0; m < 3; ++m)
+                    for (int h = 0; h < 3; ++h)
+                        for (int n = 0; n < 3; ++n)
+                            for (int p = 0; p < 3; ++p) D2[m * 3 + h][n * 3 + p] = D2[m * 3 + h][n * 3 + p] + D[m][h] * D[n][p];
+            }
+        }
+        PPA(out, 0, J, 3) = U1[3] * COE0;
+        for (int m = 0; m < 3; ++m) PPA(out, 0, J, m) = U1[m] * COE1;
+        for (int m = 0; m < 3; ++m) PPA(out, 4, J, m) = UP[m] * COE1;
+        for (int l = 0; l < 6; ++l) PPA(out, 7, J, l) = U2[l] * COE2;
+        for (int l = 0; l < 10; ++l) PPA(out, 13, J, l) = U3[l] * COE3;
+        for (int m = 0; m < 3; ++m)
+            for (int n = 0; n < 3; ++n) {
+                PPA(out, 23, J, m + 3 * n) = D1[m][n] * COG1[m][n];
+                PPA(out, 32, J, m + 3 * n) = DP[m][n] * COG1[m][n];
+            }
+        for (int l1 = 0; l1 < 9; ++l1)
+            for (int l2 = 0; l2 < 9; ++l2)
+                PPA(out, 41, J, l1 + 9 * l2) = D2[l1][l2] * (COG1[l1 / 3][l1 % 3] * COG1[l2 / 3][l2 % 3]);
+    }
+}
+
+/* PP_MEAN_T_TG(TP) (src/processing/PP_MEAN_T.f90:343-392) on a set of means */
+void orc_pp_mean_t_tg(int M, int tp, int pp_instn_sz, const double* inst, double* avg, int* nstatis) {
+    *nstatis = *nstatis + 1;
+    double COE2, COE3;
+    if (tp == 1) {
+        COE2 = 1.0 / (double)(*nstatis);
+        COE3 = (double)(*nstatis - 1) / (double)(*nstatis);
+    } else {
+        COE2 = 1.0 / (double)pp_instn_sz;
+        COE3 = 1.0;
+    }
+    for (size_t q = 0; q < (size_t)122 * M; ++q) avg[q] = COE3 * avg[q] + COE2 * inst[q];
+}
+
+/* PP_MONITOR_TG quantities (src/processing/PP_SCN_MONITOR.f90:165-226) and
+ * U1mean_WORK_tg, U1maxx_WORK_tg (PP_MEAN_ZX.f90:294-305); mon[20] */
+void orc_pp_monitor_tg(const orc_t* o, const double* inst, const double* avg, double REN, double* mon) {
+    const int M = o->M;
+    double mean = 0.0, mx = 0.0;
+    for (int J = 1; J <= M; ++J) {
+        mean = mean + PPA(inst, 0, J, 0) / o->DYFI[J] / 1.0;
+        mx = fmax(mx, fabs(PPA(inst, 0, J, 0)));
+    }
+    mean = mean / o->DZI * (double)o->N / o->Area_inlet;
+    const int JS = M / 2;
+    mon[0] = PPA(inst, 0, JS, 0); mon[1] = PPA(avg, 0, JS, 0);
+    mon[2] = PPA(inst, 0, JS, 1); mon[3] = PPA(avg, 0, JS, 1);
+    mon[4] = PPA(inst, 0, JS, 2); mon[5] = PPA(avg, 0, JS, 2);
+    mon[6] = PPA(inst, 7, JS, 0) - PPA(inst, 0, JS, 0) * PPA(inst, 0, JS, 0);
+    mon[7] = PPA(avg, 7, JS, 0) - PPA(avg, 0, JS, 0) * PPA(avg, 0, JS, 0);
+    mon[8] = PPA(inst, 7, JS, 1) - PPA(inst, 0, JS, 0) * PPA(inst, 0, JS, 1);
+    mon[9] = PPA(avg, 7, JS, 1) - PPA(avg, 0, JS, 0) * PPA(avg, 0, JS, 1);
+    mon[10] = PPA(inst, 7, JS, 3) - PPA(inst, 0, JS, 1) * PPA(inst, 0, JS, 1);
+    mon[11] = PPA(avg, 7, JS, 3) - PPA(avg, 0, JS, 1) * PPA(avg, 0, JS, 1);
+    mon[12] = PPA(inst, 7, JS, 5) - PPA(inst, 0, JS, 2) * PPA(inst, 0, JS, 2);
+    mon[13] = PPA(avg, 7, JS, 5) - PPA(avg, 0, JS, 2) * PPA(avg, 0, JS, 2);
+    double DUDY = (PPA(inst, 0, 1, 0) - 0.0) * o->DYFI[1] * 2.0;
+    mon[14] = DUDY * 2.0 / REN;
+    DUDY = (PPA(avg, 0, 1, 0) - 0.0) * o->DYFI[1] * 2.0;
+    mon[15] = DUDY * 2.0 / REN;
+    DUDY = (PPA(inst, 0, M, 0) - 0.0) * o->DYFI[M] * 2.0;
+    mon[16] = DUDY * 2.0 / REN;
+    DUDY = (PPA(avg, 0, M, 0) - 0.0) * o->DYFI[M] * 2.0;
+    mon[17] = DUDY * 2.0 / REN;
+    mon[18] = mean;
+    mon[19] = mx;
+}
+#undef PPA

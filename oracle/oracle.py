@@ -58,6 +58,10 @@ def lib():
         L.orc_run_steps.restype = ctypes.c_int
         L.orc_divgck.argtypes = [ctypes.c_void_p]
         L.orc_divgck.restype = ctypes.c_double
+        L.orc_pp_mean_zx_tg.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_pp_mean_t_tg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                       ctypes.POINTER(ctypes.c_int)]
+        L.orc_pp_monitor_tg.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, _dp]
         L.orc_poisson.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_fft_complex.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_tdma_cyc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
@@ -202,6 +206,25 @@ class Oracle:
 
     def divgck(self):
         return self._lib.orc_divgck(self._h)
+
+    # ---- statistics of the periodic channel (POSTPROCESS_TG) ----
+    # A set of x-z means is a flat array of 122*M doubles: U1xzL(M,4), UPxzL(M,3),
+    # U2xzL(M,6), U3xzL(M,10), DVDL1xzL(M,3,3), DVDLPxzL(M,3,3), DVDL2xzL(M,9,9) (Fortran order).
+    def pp_mean_zx_tg(self):
+        out = np.zeros(122 * self.M)
+        self._lib.orc_pp_mean_zx_tg(self._h, _p(out))
+        return out
+
+    def pp_mean_t_tg(self, tp, inst, avg, nstatis, pp_instn_sz=1):
+        """PP_MEAN_T_TG: updates avg in place; returns the new NSTATIS."""
+        n = ctypes.c_int(int(nstatis))
+        self._lib.orc_pp_mean_t_tg(self.M, int(tp), int(pp_instn_sz), _p(inst), _p(avg), ctypes.byref(n))
+        return n.value
+
+    def pp_monitor_tg(self, inst, avg, ren):
+        mon = np.zeros(20)
+        self._lib.orc_pp_monitor_tg(self._h, _p(inst), _p(avg), float(ren), _p(mon))
+        return mon
 
     # ---- IO (main-domain) path, explicit (iVisScheme 0) or Crank-Nicolson (1) viscous terms ----
     def io_set_vis_scheme(self, ivis):
