@@ -140,12 +140,7 @@ def heated_cpu_rate(time_budget_s, threads):
 
 
 def run_heated(args):
-    """Config 4: heated main-domain channel, Crank-Nicolson momentum, energy
-    equation and property update every substep; properties by the table
-    search (the plain method) and by the learned model (trained here on the
-    table and on rho*h samples of the running field, judged against the
-    table search)."""
-    from chapsim import gpu
+    """Config 4 as its own bench line (--workload heated256x192x128_retau180_cn)."""
     import torch
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
@@ -155,6 +150,28 @@ def run_heated(args):
         import torch.distributed as tdist
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
+    line = heated_measure(args, local, dist, ws, args.steps)
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, n, dt = heated_cpu_rate(float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n} RK3 steps of {HEATED_WORKLOAD} on the CPU FP64 restatement (OpenMP)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def heated_measure(args, local, dist, ws, steps):
+    """Config 4: heated main-domain channel, Crank-Nicolson momentum, energy
+    equation and property update every substep; properties by the table
+    search (the plain method) and by the learned model (trained here on the
+    table and on rho*h samples of the running field, judged against the
+    table search).  Returns the bench line (without the CPU baseline)."""
+    from chapsim import gpu
+    import torch
     h = HEATED
     L, M, N, DT0, CFLGV, DTMIN = h["L"], h["M"], h["N"], h["DT0"], h["CFLGV"], 1e-6
     s, Q, PR, tab, cthecd, DH = heated_case()
@@ -185,14 +202,14 @@ def run_heated(args):
         return ms, ch.launch_count() - l0, clk.summary()
 
     def kernel_profile():
-        n = max(1, min(10, args.steps))
+        n = max(1, min(10, steps))
         kms = ch.profile_steps(n, DT0, DTMIN, CFLGV)
         return {k: v / n for k, v in kms.items()}
 
     # ---- plain method: table search ----
     ch.advance(args.warmup, DT0, DTMIN, CFLGV)
-    ms_t, launches, clk = timed(args.steps)
-    v_table = pts * args.steps * ws / (ms_t / 1000.0)
+    ms_t, launches, clk = timed(steps)
+    v_table = pts * steps * ws / (ms_t / 1000.0)
     k_table = kernel_profile()
 
     # ---- end to end through the public API with host buffers (table search) ----
@@ -206,7 +223,7 @@ def run_heated(args):
     G0, _, P0 = ch.download_io()
     th = ch.download_thermal()
     gh[...], ph[...], dhh[...], rh[...], mh[...] = G0, P0, th["DH"], th["D"], th["M"]
-    ne = max(1, min(args.steps, args.e2e_steps))
+    ne = max(1, min(steps, args.e2e_steps))
     ch.sync()
     t0 = time.perf_counter()
     for _ in range(ne):
@@ -239,8 +256,8 @@ def run_heated(args):
     t_train = time.perf_counter() - t0
     ch.thermal_use_mlp(True)
     ch.advance(args.warmup, DT0, DTMIN, CFLGV)
-    ms_m, launches_m, clk_m = timed(args.steps)
-    v_mlp = pts * args.steps * ws / (ms_m / 1000.0)
+    ms_m, launches_m, clk_m = timed(steps)
+    v_mlp = pts * steps * ws / (ms_m / 1000.0)
     judge = ch.mlp_judge()
     k_mlp = kernel_profile()
 
@@ -254,9 +271,9 @@ def run_heated(args):
     achieved = dom_bytes / (per_launch_ms / 1000.0) / 1e9
     traffic = load_traffic(HEATED_WORKLOAD).get(dom)
     step_bytes = sum(words[k] * 8.0 * pts * per_step[k] for k in k_table)
-    step_ms = ms_t / args.steps
+    step_ms = ms_t / steps
     line = {
-        "metric": METRIC, "value": v_table, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC, "value": v_table, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": HEATED_WORKLOAD, "grid": [L, M, N], "domain": "4pi x 2 x 4pi/3", "REN": h["REN"],
@@ -277,25 +294,15 @@ def run_heated(args):
         "kernel_ms_per_step": {k: round(v, 5) for k, v in sorted(k_table.items())},
         "clocks": clk,
         "variants": {"learned_properties": {
-            "value": v_mlp, "unit": UNIT, "ms_per_step": ms_m / args.steps, "speedup_vs_table": v_mlp / v_table,
+            "value": v_mlp, "unit": UNIT, "ms_per_step": ms_m / steps, "speedup_vs_table": v_mlp / v_table,
             "judge_max_rel_err": judge, "bound": MLP_BOUND, "within_bound": max(judge.values()) <= MLP_BOUND,
             "training": {"samples": int(train.size), "iterations": sum(i for i, _ in MLP_SCHEDULE),
                          "seconds": t_train, "final_loss": loss},
             "property_update_ms_per_step": {"table": k_table.get("k_eng_props"), "model": k_mlp.get("k_mlp_infer")},
             "gpu_launches": int(launches_m), "clocks": clk_m}},
     }
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        rate, n, dt = heated_cpu_rate(float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{n} RK3 steps of {HEATED_WORKLOAD} on the CPU FP64 restatement (OpenMP)"}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     ch.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+    return line
 
 
 def kernel_bytes(L, precision="fp64"):
@@ -679,6 +686,19 @@ def run_b200(args):
                                       "precision": "FP32 storage, stencils and CN sweeps; FP64 Poisson, projection, "
                                                    "bulk sums"}}
         ch = chm
+        # config 4: heated main domain, table search against the learned property model
+        hl = heated_measure(args, local, dist, ws, min(args.steps, 100))
+        lv = hl["variants"]["learned_properties"]
+        line["variants"]["heated_learned"] = {
+            "workload": HEATED_WORKLOAD, "grid": hl["config"]["grid"], "steps": hl["steps"],
+            "value_table": hl["value"], "value_learned": lv["value"], "unit": UNIT,
+            "ms_per_step_table": hl["ms_per_step"], "ms_per_step_learned": lv["ms_per_step"],
+            "speedup_learned_vs_table": lv["speedup_vs_table"],
+            "property_update_ms_per_step": lv["property_update_ms_per_step"],
+            "judge_max_rel_err": lv["judge_max_rel_err"], "bound": lv["bound"], "within_bound": lv["within_bound"],
+            "step_roofline_frac": hl["step_roofline"]["frac"],
+            "note": "main domain (Crank-Nicolson momentum, energy equation, property update every substep), FP64; "
+                    "the full line: --workload " + HEATED_WORKLOAD}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, n, dt = cpu_reference_rate(wl, 1000, float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)

@@ -138,8 +138,8 @@ struct chapsim_ctx {
     cudaStream_t stream = nullptr;
     Geo g{};
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr;
-    double* HS = nullptr;         // forward factors of the sequential y-solve (allocated when chosen)
     double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
+    double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
     int k1_split = 0;             // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep (chapsim_autotune)
     double2* SP = nullptr;
@@ -222,7 +222,7 @@ std::vector<double2> twiddles(int n) {
 }
 
 template <typename R> size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(R); }
-template <typename R> size_t smem_z(const Geo& g) { return (size_t)(32 * (g.N + 33)) * sizeof(R); }
+template <typename R> size_t smem_z(const Geo& g) { return (size_t)(2 * 32 * (g.N + 33)) * sizeof(R); }
 template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
 template <typename R> size_t smem_xs(const Geo& g) { return (size_t)((XS_NT / 32) * (g.L + 33)) * sizeof(R); }
 template <typename R> size_t smem_rt() { return (size_t)(RT_SLOTS * RT_SLOT) * sizeof(R); }
@@ -296,14 +296,22 @@ cudaError_t set_smem(F* f, size_t bytes) {
 
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
 
+// lines per block of k_ysolve_seq: up to 32, a multiple of 8 that fits the shared memory
+int ysolve_seq_lines(int M) {
+    int nt = 32;
+    while (nt > 8 && smem_ysolve_seq(M, nt) > 227 * 1024) nt -= 8;
+    return nt;
+}
+
 void launch_ysolve_seq(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
-    k_ysolve_seq<<<(int)((nl + YQ_NT - 1) / YQ_NT), YQ_NT, 0, ctx->stream>>>(g, ctx->SP, ctx->HS);
+    const int nt = ysolve_seq_lines(g.M);
+    k_ysolve_seq<<<(int)((nl + nt - 1) / nt), nt, smem_ysolve_seq(g.M, nt), ctx->stream>>>(g, ctx->SP, ctx->YF);
 }
 
 void launch_ysolve(chapsim_ctx* ctx) {
-    if (ctx->ysolve_kind == 1 && ctx->HS) launch_ysolve_seq(ctx);
+    if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq(ctx);
     else launch_ysolve_warp(ctx);
 }
 
@@ -343,6 +351,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S>, smem_yw(g))));
+    CK(set_smem(k_ysolve_seq, smem_ysolve_seq(g.M, ysolve_seq_lines(g.M))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2>, smem_fz(g))));
     if (ctx->domain == 2 && ctx->ivis) {
@@ -417,8 +426,9 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     }
     launch_rhs_x<R>(ctx, f, fac, ns);
     prof_mark(ctx);
-    dim3 grz(g.L / 32, g.M, 3);
-    DISPATCH_S(g.N / 32, (k_zsweep<S, R><<<grz, SWEEP_NT, smem_z<R>(g), s>>>(g, f.RHS, fac)));
+    // persistent: as many blocks as fit at once (two per SM where the two tile buffers allow)
+    const int nz = std::min((g.L / 32) * (3 * g.M - 1), (smem_z<R>(g) <= 113 * 1024 ? 2 : 1) * ctx->nsm);
+    DISPATCH_S(g.N / 32, (k_zsweep<S, R><<<nz, SWEEP_NT, smem_z<R>(g), s>>>(g, f.RHS, fac)));
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N);
     DISPATCH_S(g.M / 32, (k_ysweep<S, R><<<gry, SWEEP_NT, smem_y<R>(g), s>>>(g, f.Q, f.RHS, ctx->st, fac, ns)));
@@ -802,7 +812,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->HS); cudaFree(ctx->SP); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
+    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->yz);
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
@@ -1749,7 +1759,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     cudaStream_t s = ctx->stream;
     CK(cudaStreamSynchronize(s));
     const size_t nsp = (size_t)g.LH * g.M * g.N;
-    if (!ctx->HS) CK(cudaMalloc(&ctx->HS, nsp * sizeof(double)));
+    if (!ctx->YF) {
+        CK(cudaMalloc(&ctx->YF, 2 * nsp * sizeof(double)));
+        k_ysolve_seq_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF);
+        CK(cudaGetLastError());
+    }
     CK(cudaMemsetAsync(ctx->SP, 0, nsp * sizeof(double2), s));
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -1772,6 +1786,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     ctx->launches += 2 * (2 + reps);
     CK(cudaGetLastError());
     ctx->ysolve_kind = force >= 0 ? (force & 1) : (t[1] < t[0] ? 1 : 0);
+    if (ctx->ysolve_kind == 0) {  // the factor table is only read by the sequential variant
+        CK(cudaStreamSynchronize(s));
+        cudaFree(ctx->YF);
+        ctx->YF = nullptr;
+    }
     // explicit right-hand sides + x sweep: fused vs split (periodic channel).
     // CONVH0 is state: kept in a temporary copy and restored afterwards.
     float tk[2] = {0.f, 0.f};
@@ -1808,10 +1827,6 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         cudaFree(hsave);
         CK(cudaGetLastError());
         ctx->k1_split = force >= 0 ? ((force >> 1) & 1) : (tk[1] < tk[0] ? 1 : 0);
-    }
-    if (ctx->ysolve_kind == 0) {
-        cudaFree(ctx->HS);
-        ctx->HS = nullptr;
     }
     if (ctx->step_exec) {
         cudaGraphExecDestroy(ctx->step_exec);

@@ -22,10 +22,8 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, d
     double mx = 0.0;
     bool bad = false;
     for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
-        const int i = (int)(t % L);
-        const long long r = t / L;
-        const int j = 1 + (int)(r % M);
-        const int k = (int)(r / M);
+        int i, j, k;
+        io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
         const double q = (fabs(((double)Q[c] + (double)Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
                           fabs(((double)Q[c + g.FS] + (double)Q[c + g.FS + g.L]) * g.dyfi[j] * 1.0) +
@@ -64,10 +62,8 @@ __global__ void __launch_bounds__(DG_NT) k_divgck(Geo g, const R* __restrict__ Q
     const long long tot = (long long)L * M * N;
     double mx = 0.0;
     for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
-        const int i = (int)(t % L);
-        const long long r = t / L;
-        const int j = 1 + (int)(r % M);
-        const int k = (int)(r / M);
+        int i, j, k;
+        io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
         const double d = ((double)Q[pidx(g, wrapp(i, L), j, k)] - (double)Q[c]) * g.dxi +
                          ((double)Q[c + g.FS + g.L] - (double)Q[c + g.FS]) * g.dyfi[j] * 1.0 +

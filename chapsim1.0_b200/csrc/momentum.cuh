@@ -271,37 +271,63 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
 }
 
 // ---------------------------------------------------------------------------
-// cyclic z sweep: block = 32 consecutive i at fixed j, all k, one component
+// cyclic z sweep.  A tile is 32 consecutive i at fixed j, all k, one
+// component; tiles of v at j = 1 are skipped (MOMFA2_Z_tg starts at N2I = 2
+// for v).  Blocks are persistent and take tiles in a stride loop with two
+// shared-memory buffers: the next tile's right-hand sides load (cp.async)
+// while the current tile's 32 lines are solved and stored.
 template <int S, typename R>
-__global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : 3)) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
+__global__ void __launch_bounds__(SWEEP_NT, 2) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    R* sm = reinterpret_cast<R*>(sm_raw);
-    const int N = g.N;
-    const int i0 = blockIdx.x * 32;
-    const int j = 1 + blockIdx.y;
-    const int comp = blockIdx.z;
-    if (comp == 1 && j == 1) return;  // MOMFA2_Z_tg starts at N2I = 2 for v
+    R* smb = reinterpret_cast<R*>(sm_raw);
+    const int N = g.N, M = g.M;
     const int LS = N + 33;
-    R* Rz = RHS + comp * g.FI + iidx(g, i0, j, 0);
+    const int TS = 32 * LS;
+    const int nx = g.L / 32;
+    const int nwork = nx * (3 * M - 1);
     const long long ks = g.PI_;
     constexpr int NIT = 4 * S;  // 32*N / SWEEP_NT
+    auto tile_base = [&](int t) -> R* {
+        int comp, j;
+        if (t < nx * M) { comp = 0; j = 1 + t / nx; }
+        else if (t < nx * (2 * M - 1)) { comp = 1; j = 2 + (t - nx * M) / nx; }
+        else { comp = 2; j = 1 + (t - nx * (2 * M - 1)) / nx; }
+        const int i0 = 32 * (t % nx);
+        return RHS + comp * g.FI + iidx(g, i0, j, 0);
+    };
+    auto load = [&](int t, R* buf) {
+        const R* Rz = tile_base(t);
 #pragma unroll 4
-    for (int it = 0; it < NIT; ++it) {
-        const int p = threadIdx.x + SWEEP_NT * it;
-        cp_async_el(sm + (p & 31) * LS + seg_pos<S>(p >> 5), Rz + (p & 31) + ks * (p >> 5));
-    }
-    cp_async_wait_all();
-    __syncthreads();
+        for (int it = 0; it < NIT; ++it) {
+            const int p = threadIdx.x + SWEEP_NT * it;
+            cp_async_el(buf + (p & 31) * LS + seg_pos<S>(p >> 5), Rz + (p & 31) + ks * (p >> 5));
+        }
+    };
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const R* fz = fac + FSET_Z * FAC_SET;
+    int t = blockIdx.x, b = 0;
+    if (t < nwork) load(t, smb);
+    cp_async_commit();
+    for (; t < nwork; t += gridDim.x) {
+        R* cur = smb + b * TS;
+        const int tn = t + gridDim.x;
+        if (tn < nwork) load(tn, smb + (b ^ 1) * TS);
+        cp_async_commit();
+        cp_async_wait_group<1>();
+        __syncthreads();
 #pragma unroll 1
-    for (int il = warp; il < 32; il += SWEEP_NT / 32) warp_tdma_apply_smem<S, true>(sm + il * LS, fz, lane);
-    __syncthreads();
+        for (int il = warp; il < 32; il += SWEEP_NT / 32) warp_tdma_apply_smem<S, true>(cur + il * LS, fz, lane);
+        __syncthreads();
+        R* Rz = tile_base(t);
 #pragma unroll 4
-    for (int it = 0; it < NIT; ++it) {
-        const int p = threadIdx.x + SWEEP_NT * it;
-        Rz[(p & 31) + ks * (p >> 5)] = sm[(p & 31) * LS + seg_pos<S>(p >> 5)];
+        for (int it = 0; it < NIT; ++it) {
+            const int p = threadIdx.x + SWEEP_NT * it;
+            Rz[(p & 31) + ks * (p >> 5)] = cur[(p & 31) * LS + seg_pos<S>(p >> 5)];
+        }
+        __syncthreads();  // cur is the load target two tiles on
+        b ^= 1;
     }
+    cp_async_wait_all();
 }
 
 // ---------------------------------------------------------------------------

@@ -219,47 +219,80 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __rest
 
 // ---------------------------------------------------------------------------
 // The other y-solve variant: the reference's sequential Thomas recurrence
-// (TDMAIJJ_nonCYC :95-121, zero mode pinned as above), one thread per (kx, kz)
-// line with both parts, coefficients formed on the fly.  Consecutive threads
-// take consecutive kx, so every row access is coalesced; the forward sweep
-// keeps G in the spectral array and H in HS (LH*M*N doubles).  Fewer
-// operations than the warp hybrid but only one thread per line: the
-// autotuner picks between them per grid.
-#define YQ_NT 128
-__global__ void __launch_bounds__(YQ_NT) k_ysolve_seq(Geo g, double2* __restrict__ SP, double* __restrict__ HS) {
+// (TDMAIJJ_nonCYC :95-121, zero mode pinned as above), one thread per
+// (kx, kz) line.  The coefficient part of the recurrence (the pivots
+// PP_j = 1/(B_j - H_{j-1} A_j) and multipliers H_j) depends on the operator
+// only, not on dt or the right-hand side, so k_ysolve_seq_factors runs it
+// once per line and keeps PP and H (2 M doubles per line, row-major over the
+// lines: PP_j of line q at F[j*nl + q], H_j at F[(M+j)*nl + q]; row 1 keeps
+// B_1 itself, which the first row divides by).  The per-substep solve is
+// then two chains of multiply-adds.  A block stages its nt consecutive lines
+// (consecutive kx: every row access is coalesced) and their factors in
+// shared memory with cp.async; the autotuner picks between this variant
+// and the warp hybrid per grid.
+inline size_t smem_ysolve_seq(int M, int nt) { return (size_t)nt * (M + 1) * (sizeof(double2) + 2 * sizeof(double)); }
+
+__global__ void k_ysolve_seq_factors(Geo g, double* __restrict__ F) {
     const int M = g.M, LH = g.LH;
     const long long nl = (long long)LH * g.N;
-    const long long q = (long long)blockIdx.x * YQ_NT + threadIdx.x;
-    if (q >= nl) return;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nl; q += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+        const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+        const double b = g.acph[1] + shift;
+        const double c = q == 0 ? 0.0 : g.apph[1];
+        double hp = c / b;
+        F[q] = b;
+        F[(long long)M * nl + q] = hp;
+        for (int j = 2; j <= M; ++j) {
+            const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
+            hp = j < M ? g.apph[j] * pp : 0.0;
+            F[(long long)(j - 1) * nl + q] = pp;
+            F[(long long)(M + j - 1) * nl + q] = hp;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(32) k_ysolve_seq(Geo g, double2* __restrict__ SP, const double* __restrict__ F) {
+    extern __shared__ double2 sm2[];
+    const int M = g.M, LH = g.LH, nt = blockDim.x;
+    const int LS = M + 1;
+    double2* sr = sm2;
+    double* sp = reinterpret_cast<double*>(sm2 + (size_t)nt * LS);
+    double* sh = sp + (size_t)nt * LS;
+    const long long nl = (long long)LH * g.N;
+    const long long q = (long long)blockIdx.x * nt + threadIdx.x;
+    if (q >= nl) return;  // no block barrier below
     const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-    const long long js = LH;
     double2* s = SP + kx + (long long)LH * (long long)M * kz;
-    double* h = HS + kx + (long long)LH * (long long)M * kz;
-    const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-    const bool zero = (q == 0);
-    const double b = g.acph[1] + shift;
-    const double c = zero ? 0.0 : g.apph[1];
-    double2 r = s[0];
-    if (zero) r = make_double2(0.0, 0.0);
-    double hp = c / b;
-    double2 gp = make_double2(r.x / b, r.y / b);
-    h[0] = hp;
-    s[0] = gp;
+    double2* r = sr + threadIdx.x * LS;
+    double* pp = sp + threadIdx.x * LS;
+    double* h = sh + threadIdx.x * LS;
+    for (int j = 0; j < M; ++j) {
+        cp_async16(r + j, s + (long long)LH * j);
+        cp_async8(pp + j, F + (long long)j * nl + q);
+        cp_async8(h + j, F + (long long)(M + j) * nl + q);
+    }
+    cp_async_wait_all();
+    double2 r0 = r[0];
+    if (q == 0) r0 = make_double2(0.0, 0.0);
+    const double b = pp[0];
+    double2 gp = make_double2(r0.x / b, r0.y / b);
+    r[0] = gp;
+#pragma unroll 4
     for (int j = 2; j <= M; ++j) {
-        const double a = g.amph[j];
-        const double pp = 1.0 / ((g.acph[j] + shift) - hp * a);
-        const double2 rj = s[(j - 1) * js];
-        gp = make_double2((rj.x - a * gp.x) * pp, (rj.y - a * gp.y) * pp);
-        hp = j < M ? g.apph[j] * pp : 0.0;
-        h[(j - 1) * js] = hp;
-        s[(j - 1) * js] = gp;
+        const double a = g.amph[j], p = pp[j - 1];
+        const double2 rj = r[j - 1];
+        gp = make_double2((rj.x - a * gp.x) * p, (rj.y - a * gp.y) * p);
+        r[j - 1] = gp;
     }
     double2 xn = gp;
+    s[(long long)LH * (M - 1)] = xn;
+#pragma unroll 4
     for (int j = M - 1; j >= 1; --j) {
-        const double hj = h[(j - 1) * js];
-        const double2 gj = s[(j - 1) * js];
+        const double hj = h[j - 1];
+        const double2 gj = r[j - 1];
         xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
-        s[(j - 1) * js] = xn;
+        s[(long long)LH * (j - 1)] = xn;
     }
 }
 
@@ -305,10 +338,8 @@ __global__ void __launch_bounds__(CR_NT) k_correct(Geo g, R* __restrict__ Q, R* 
     const long long tot = (long long)L * M * N;
     const long long t = (long long)blockIdx.x * CR_NT + threadIdx.x;
     if (t >= tot) return;
-    const int i = (int)(t % L);
-    const long long r = t / L;
-    const int j = 1 + (int)(r % M);
-    const int k = (int)(r / M);
+    int i, j, k;
+    io_decode(g, t, i, j, k);
     const double dt = st->dt, ta = g.talp[ns];
     const long long c = pidx(g, i, j, k);
     // all loads first: Q is read and written through one pointer
