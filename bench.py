@@ -194,11 +194,7 @@ def heated_measure(args, local, dist, ws, steps):
             ch.advance(nsteps, DT0, DTMIN, CFLGV)
             ev1.record(stream)
             torch.cuda.synchronize(local)
-        ms = ev0.elapsed_time(ev1)
-        if dist is not None:
-            t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
         return ms, ch.launch_count() - l0, clk.summary()
 
     def kernel_profile():
@@ -420,6 +416,26 @@ def dist_setup():
     return ws, rank, local
 
 
+def replica_seed(rank):
+    """Seed of the channel rank `rank` advances: replicas are independent channels, one per GPU."""
+    return 1973 + rank
+
+
+def max_over_ranks(x, dist, device):
+    """The largest x over all ranks (a job's time is its slowest rank's); x itself when not distributed."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(points, steps, ws, ms):
+    """Whole-job grid-pt*RK3-steps/s: each of the ws ranks advanced points x steps in at most ms."""
+    return points * steps * ws / (ms / 1000.0)
+
+
 def cpu_reference_rate(wl, steps_cap, time_budget_s, threads):
     """Timed CPU restatement of the step (oracle port, all host threads)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -476,6 +492,12 @@ def run_ensemble(args):
     import torch
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:  # replicas: every rank advances its own ensemble (other seeds)
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
     members = ensemble_members(2025 + 100 * rank)
     DT0, DTMIN, CFLGV = 0.05, 1e-6, 0.5
 
@@ -498,11 +520,13 @@ def run_ensemble(args):
     for c in seq:
         c.advance(args.warmup, DT0, DTMIN, CFLGV)
     torch.cuda.synchronize(local)
+    if dist is not None:
+        dist.barrier()
     t0 = time.perf_counter()
     for c in seq:
         c.advance(args.steps, DT0, DTMIN, CFLGV)
     torch.cuda.synchronize(local)
-    t_seq = time.perf_counter() - t0
+    t_seq = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     for c in seq:
         c.close()
     # batched: one graph per step over all members
@@ -514,33 +538,39 @@ def run_ensemble(args):
     stream = torch.cuda.ExternalStream(ens.stream_handle(), device=local)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(local)
+    if dist is not None:
+        dist.barrier()
     launches0 = sum(c.launch_count() for c in grp)
     with ClockSampler(local) as clk:
         ev0.record(stream)
         ens.advance(args.steps, DT0, DTMIN, CFLGV)
         ev1.record(stream)
         torch.cuda.synchronize(local)
-    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
     launches = sum(c.launch_count() for c in grp) - launches0
-    value = pts * args.steps / (ms / 1000.0)
+    value = aggregate_rate(pts, args.steps, ws, ms)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": ENSEMBLE_WORKLOAD, "members": [[L, M, N, round(REN, 1)] for (L, M, N, _a, _b, _c, REN, _s)
                                                                in members],
                    "precision": args.precision, "total_points": pts,
                    "autotuned_choice_bits": [t[0] for t in tune], "l2": "no flush: members total %.0f MB" % (pts * 8 * 20 / 1e6)},
-        "sequential": {"value": pts * args.steps / t_seq, "unit": UNIT, "ms_per_step": 1000.0 * t_seq / args.steps,
+        "sequential": {"value": pts * args.steps * ws / t_seq, "unit": UNIT, "ms_per_step": 1000.0 * t_seq / args.steps,
                        "timing": "wall clock around the members' own graph replays, one member after another"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
     line["speedup_vs_sequential"] = line["value"] / line["sequential"]["value"]
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     ens.close()
     for c in grp:
         c.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
@@ -561,7 +591,7 @@ def run_b200(args):
     L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = WORKLOADS[wl]
     DTMIN = 1e-6
     s = channel_setup(L, M, N, HX, HZ, STR2, REN)
-    Q0, PR0 = initial_field(s, 1973 + rank, 0.1)
+    Q0, PR0 = initial_field(s, replica_seed(rank), 0.1)
     ch = gpu.ChannelTG(s, device=local, precision=args.precision)
     ch.upload(Q0, PR0)
     ch.set_dt(DT0)
@@ -588,13 +618,9 @@ def run_b200(args):
         torch.cuda.synchronize(local)
     barrier()
     launches = ch.launch_count() - launches0
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
     pts = L * M * N
-    value = pts * args.steps * ws / (ms / 1000.0)
+    value = aggregate_rate(pts, args.steps, ws, ms)
     maxdiv = ch.DIVGCK_tg()
 
     # ---- end to end through the public API with host buffers ----
@@ -612,11 +638,7 @@ def run_b200(args):
         ch.advance(1, DT0, DTMIN, CFLGV)
         ch.lib.chapsim_download_fields(ch.h, gpu._ptr(qh), gpu._ptr(ph), None)  # D2H: the step's result
     ch.sync()
-    te = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([te], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        te = float(t.item())
+    te = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
     e2e = pts * ne * ws / te
     hbytes = int(qh.nbytes + ph.nbytes)
 
@@ -674,12 +696,8 @@ def run_b200(args):
         chm.advance(args.steps, DT0, DTMIN, CFLGV)
         ev1.record(sm_)
         torch.cuda.synchronize(local)
-        msm = ev0.elapsed_time(ev1)
-        if dist is not None:
-            t = torch.tensor([msm], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            msm = float(t.item())
-        vm = pts * args.steps * ws / (msm / 1000.0)
+        msm = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
+        vm = aggregate_rate(pts, args.steps, ws, msm)
         line["variants"] = {"mixed": {"value": vm, "unit": UNIT, "ms_per_step": msm / args.steps,
                                       "speedup_vs_fp64": vm / value, "max_div": chm.DIVGCK_tg(),
                                       "autotuned_choice_bits": mt,
@@ -726,8 +744,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--no-variants", action="store_true", help="skip the mixed-precision comparison of an FP64 run")
     ap.add_argument("--tune", type=int, default=-1,
-                    help="kernel variant bits instead of timing them (bit 0: sequential y-solve, bit 1: split "
-                         "right-hand side); -1 times both variants and keeps the faster")
+                    help="kernel variant bits instead of timing them (bit 0: sequential y-solve; bits 1-2: "
+                         "right-hand side 0 fused, 1 split, 2 fused with bulk-copy staging); -1 times the "
+                         "variants and keeps the fastest")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -460,14 +460,14 @@ class ChannelTG:
 
 
     def autotune(self, force=-1):
-        """Keeps the faster y-solve and right-hand-side variants for this grid, or
-        forces them (bit 0: sequential y-solve, bit 1: split right-hand sides);
-        returns (choice bits, {variant: ms})."""
+        """Keeps the fastest y-solve and right-hand-side variants for this grid, or
+        forces them (bit 0: sequential y-solve; bits 1-2: right-hand sides 0 fused,
+        1 split, 2 fused with bulk-copy staging); returns (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 4)()
+        ms = (ctypes.c_float * 5)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
-                          "rhs_split": ms[3]}
+                          "rhs_split": ms[3], "rhs_bulk": ms[4]}
 
 
 class Ensemble:

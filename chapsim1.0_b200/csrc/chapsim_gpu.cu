@@ -18,6 +18,7 @@
 #include "io.cuh"
 #include "io_cn.cuh"
 #include "stats.cuh"
+#include "rhs_bulk.cuh"
 #include "thermo.cuh"
 #include "thermal.cuh"
 #include "mlp.cuh"
@@ -141,7 +142,7 @@ struct chapsim_ctx {
     double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
     double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
-    int k1_split = 0;             // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep (chapsim_autotune)
+    int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     double2* SP = nullptr;
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
@@ -335,6 +336,7 @@ template <typename R>
 int configure_momentum(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R>, smem_rhs<R>(g))));
+    if (rb_warps<R>(g.L) > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_warps<R>(g.L) * rb_warp_bytes<R>(g.L))));
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R>, smem_z<R>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
     DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
@@ -398,7 +400,12 @@ template <typename R>
 void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    if (ctx->k1_split) {
+    const int nwb = rb_warps<R>(g.L);
+    if (ctx->k1_kind == 2 && nwb > 0) {
+        const int grb = std::min(ctx->nsm, (g.M * g.N + nwb - 1) / nwb);
+        DISPATCH_S(g.L / 32, (k_rhs_xsweep_bulk<S, R><<<grb, nwb * 32, nwb * rb_warp_bytes<R>(g.L), s>>>(
+                                 g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
+    } else if (ctx->k1_kind == 1) {
         dim3 grt(g.L / RT_I, g.M / RT_J, g.N / rt_chunk(g));
         k_rhs_point<R><<<grt, RP_NT, smem_rt<R>(), s>>>(g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, ns,
                                                          rt_chunk(g));
@@ -593,7 +600,8 @@ int check_device_error(chapsim_ctx* ctx) {
         if (e & CHS_EBIT_DT_COLLAPSE) return fail(ctx, CHAPSIM_ERR_DT_COLLAPSE, "DT/DT0 < 0.01 (time step collapse)");
         if (e & CHS_EBIT_TABLE)
             return fail(ctx, CHAPSIM_ERR_TABLE_RANGE, "rho*h (or h) left the property table during the energy update");
-        if (e & CHS_EBIT_MMA_TIMEOUT) return fail(ctx, CHAPSIM_ERR_TIMEOUT, "a tensor-core completion wait ran out of time");
+        if (e & CHS_EBIT_MMA_TIMEOUT)
+            return fail(ctx, CHAPSIM_ERR_TIMEOUT, "a bounded device wait (tensor-core commit or bulk copy) ran out of time");
     }
     return CHAPSIM_OK;
 }
@@ -1219,7 +1227,7 @@ int chapsim_launch_count(const chapsim_ctx_t* ctx, uint64_t* count) {
 
 int chapsim_kernels_per_step(const chapsim_ctx_t* ctx, int32_t* count) {
     if (!ctx || !count) return CHAPSIM_ERR_BADARG;
-    int per = 2 + 3 * (ctx->thermal ? 15 : 9 + ctx->k1_split);
+    int per = 2 + 3 * (ctx->thermal ? 15 : 9 + (ctx->k1_kind == 1 ? 1 : 0));
     *count = per;
     return CHAPSIM_OK;
 }
@@ -1791,9 +1799,10 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         cudaFree(ctx->YF);
         ctx->YF = nullptr;
     }
-    // explicit right-hand sides + x sweep: fused vs split (periodic channel).
-    // CONVH0 is state: kept in a temporary copy and restored afterwards.
-    float tk[2] = {0.f, 0.f};
+    // explicit right-hand sides + x sweep: fused, split, or fused with bulk-copy
+    // staging (periodic channel).  CONVH0 is state: kept in a temporary copy
+    // and restored afterwards.
+    float tk[3] = {0.f, 0.f, 0.f};
     if (ctx->domain == 1) {
         const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
         const size_t hb = (size_t)3 * g.FI * (mixed ? sizeof(float) : sizeof(double));
@@ -1801,9 +1810,14 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaMalloc(&hsave, hb));
         void* h0 = mixed ? (void*)ctx->H0f : (void*)ctx->H0;
         CK(cudaMemcpyAsync(hsave, h0, hb, cudaMemcpyDeviceToDevice, s));
-        const int keep = ctx->k1_split;
-        for (int kind = 0; kind < 2; ++kind) {
-            ctx->k1_split = kind;
+        const int keep = ctx->k1_kind;
+        const bool bulk_fits = mixed ? rb_warps<float>(g.L) > 0 : rb_warps<double>(g.L) > 0;
+        for (int kind = 0; kind < 3; ++kind) {
+            if (kind == 2 && !bulk_fits) {
+                tk[2] = 1e30f;
+                continue;
+            }
+            ctx->k1_kind = kind;
             auto one = [&]() {
                 if (mixed) {
                     StepFields<float> f = step_fields<float>(ctx);
@@ -1821,12 +1835,15 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             CK(cudaEventElapsedTime(&tk[kind], e0, e1));
             tk[kind] /= reps;
         }
-        ctx->k1_split = keep;
+        ctx->k1_kind = keep;
         CK(cudaMemcpyAsync(h0, hsave, hb, cudaMemcpyDeviceToDevice, s));
         CK(cudaStreamSynchronize(s));
         cudaFree(hsave);
         CK(cudaGetLastError());
-        ctx->k1_split = force >= 0 ? ((force >> 1) & 1) : (tk[1] < tk[0] ? 1 : 0);
+        int best = 0;
+        for (int kind = 1; kind < 3; ++kind)
+            if (tk[kind] < tk[best]) best = kind;
+        ctx->k1_kind = force >= 0 ? std::min((force >> 1) & 3, bulk_fits ? 2 : 1) : best;
     }
     if (ctx->step_exec) {
         cudaGraphExecDestroy(ctx->step_exec);
@@ -1834,8 +1851,8 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (choice) *choice = ctx->ysolve_kind | (ctx->k1_split << 1);
-    if (ms) { ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; }
+    if (choice) *choice = ctx->ysolve_kind | (ctx->k1_kind << 1);
+    if (ms) { ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2]; }
     return CHAPSIM_OK;
 }
 

@@ -18,6 +18,7 @@
 // error bits written by kernels into DevState::err
 #define CHS_EBIT_NAN 1u
 #define CHS_EBIT_DT_COLLAPSE 2u
+#define CHS_EBIT_MMA_TIMEOUT 8u  // a bounded device wait (tensor-core commit or bulk copy) ran out
 
 struct DevState {
     double dt;       // current DT (BCAST_COMM_STEP)
@@ -112,6 +113,46 @@ __device__ __forceinline__ double block_max(double v, double* sbuf) {
         for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_down_sync(0xffffffffu, r, o));
     }
     return r;
+}
+
+// ---- shared-memory barriers and the bulk-copy (TMA) engine ----
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// orders this thread's generic-proxy shared-memory accesses before later async-proxy ones
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Waits for phase `parity` of the mbarrier, for at most ~2^31 clocks; returns
+// false (and sets the error bit) when the budget runs out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, unsigned int* err) {
+    const long long t0 = clock64();
+    uint32_t done = 0;
+    while (true) {
+        asm volatile(
+            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t}" : "=r"(done) : "r"(smem_u32(mbar)), "r"(parity) : "memory");
+        if (done) return true;
+        if (clock64() - t0 > (1ll << 31)) {
+            atomicOr(err, CHS_EBIT_MMA_TIMEOUT);
+            return false;
+        }
+    }
+}
+
+// one arrival that also announces `bytes` of bulk-copy traffic on the mbarrier
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");
+}
+
+// Bulk copy (no tensor map, no multicast) of `bytes` (a multiple of 16, both
+// addresses 16-byte aligned) from global to this CTA's shared memory,
+// completing on the mbarrier.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(mbar)) : "memory");
 }
 
 // Hint that a cache line is about to be read (no register or completion cost).

@@ -32,7 +32,6 @@
 #define MLP_NP 16       // output layer padded to the MMA N granule
 #define MLP_TILE 128    // points per tile (MMA M)
 #define MLP_NT 128      // threads per CTA (4 warps: one TMEM lane quarter each)
-#define CHS_EBIT_MMA_TIMEOUT 8u
 #ifndef CHS_EBIT_TABLE
 #define CHS_EBIT_TABLE 4u
 #endif
@@ -62,7 +61,6 @@ __host__ __device__ __forceinline__ int umma_off(int R, int r, int k) {
     return ((((k >> 4) * 2 + ((k >> 3) & 1)) * (R >> 3) + (r >> 3)) * 8 + (r & 7)) * 16 + (k & 7) * 2;
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ uint64_t umma_desc(const void* base, int R, int s) {
     const uint32_t a = smem_u32(base) + (uint32_t)(s * R * 32);
@@ -91,29 +89,6 @@ __device__ __forceinline__ void umma_commit(uint64_t* mbar) {
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-// Waits for phase `parity` of the mbarrier, for at most ~2^31 clocks; returns
-// false (and sets the error bit) when the budget runs out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, unsigned int* err) {
-    const long long t0 = clock64();
-    uint32_t done = 0;
-    while (true) {
-        asm volatile(
-            "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, P1;\n\t}" : "=r"(done) : "r"(smem_u32(mbar)), "r"(parity) : "memory");
-        if (done) return true;
-        if (clock64() - t0 > (1ll << 31)) {
-            atomicOr(err, CHS_EBIT_MMA_TIMEOUT);
-            return false;
-        }
-    }
-}
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),

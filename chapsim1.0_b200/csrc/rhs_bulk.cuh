@@ -1,0 +1,244 @@
+// Fused right-hand sides + x sweep (the work of k_rhs_xsweep, momentum.cuh)
+// with every row the stencil reads staged in shared memory by the bulk-copy
+// (TMA) engine instead of per-thread loads.
+//
+// A warp owns x lines (j, k) in a stride loop over the grid.  For a line it
+// needs 23 rows of length L: u, v, w at (j,k), (j+1,k), (j-1,k), (j,k+1),
+// (j,k-1), v at (j+1,k-1), w at (j-1,k+1), PR at (j,k), (j-1,k), (j,k-1), and
+// the three CONVH0 rows.  Lane 0 issues them as 23 cp.async.bulk copies that
+// complete on the warp's mbarrier into the warp's stage; as soon as the warp
+// has read a line's rows it issues the copies of its next line, which then
+// arrive while it runs the x sweep and while the block's other warps compute.
+// (One stage per warp and up to 8 warps per block measured faster than two
+// stages and 4 warps: the arithmetic needs the extra warps to hide its
+// latency, and the shared memory holds one 23-row stage per warp.)  The stencils,
+// the RK combination, the viscous and pressure terms and the bulk-forcing
+// partial sums are those of k_rhs_xsweep, read from shared memory; the x
+// sweep runs on the line in segment-padded shared memory as there.
+//
+// Rows start at multiples of L elements (L >= 32), so every bulk copy is
+// 16-byte aligned with a multiple-of-16 size.  The copies read Q, PR and
+// CONVH0; the kernel writes CONVH0 only in the row of its own line, after
+// that line's copy has completed, and writes RHS, which it does not read.
+// mbarrier waits are clock-bounded (error bit, then the warp stops issuing
+// and waits, bounded again, for its copies still in flight).
+#pragma once
+#include "common.cuh"
+#include "momentum.cuh"
+#include "tdma.cuh"
+
+#define RB_ROWS 23
+#define RB_WMAX 8  // warps per block at most
+
+// Shared memory of one warp: one stage of RB_ROWS rows, then the line buffer
+// of the x sweep; the region is rounded up to 32 elements so that every
+// warp's stage (a bulk-copy destination) starts on a 128-byte boundary.
+__host__ __device__ inline int rb_warp_elems(int L) { return ((1 * RB_ROWS * L + 3 * (L + 33) + 31) / 32) * 32; }
+template <typename R>
+__host__ __device__ inline size_t rb_warp_bytes(int L) {
+    return (size_t)rb_warp_elems(L) * sizeof(R);
+}
+template <typename R>
+inline int rb_warps(int L) {
+    const size_t per = rb_warp_bytes<R>(L);
+    int w = (int)((size_t)(227 * 1024 - 2048) / per);  // the opt-in limit less the static shared memory
+    return w < 1 ? 0 : (w > RB_WMAX ? RB_WMAX : w);
+}
+
+template <typename R>
+__device__ __forceinline__ void rb_issue(const Geo& g, const R* Q, const R* PR, const R* H0, int line, R* stage,
+                                         uint64_t* bar) {
+    const int L = g.L, M = g.M, N = g.N;
+    const int j = 1 + line % M, k = line / M;
+    const int jp = j + 1, jm = j - 1, kp = wrapp(k, N), km = wrapm(k, N);
+    const R* U = Q;
+    const R* V = Q + g.FS;
+    const R* W = Q + 2 * g.FS;
+    const long long c = pidx(g, 0, j, k), cjp = pidx(g, 0, jp, k), cjm = pidx(g, 0, jm, k);
+    const long long ckp = pidx(g, 0, j, kp), ckm = pidx(g, 0, j, km);
+    const long long ii = iidx(g, 0, j, k);
+    const R* src[RB_ROWS] = {U + c, U + cjp, U + cjm, U + ckp, U + ckm,
+                             V + c, V + cjp, V + cjm, V + ckp, V + ckm, V + pidx(g, 0, jp, km),
+                             W + c, W + cjp, W + cjm, W + ckp, W + ckm, W + pidx(g, 0, jm, kp),
+                             PR + c, PR + cjm, PR + ckm,
+                             H0 + ii, H0 + ii + g.FI, H0 + ii + 2 * g.FI};
+    const uint32_t rb = (uint32_t)(L * sizeof(R));
+    mbar_arrive_expect_tx(bar, RB_ROWS * rb);
+#pragma unroll
+    for (int r = 0; r < RB_ROWS; ++r) bulk_g2s(stage + r * L, src[r], rb, bar);
+}
+
+template <int S, typename R>
+__global__ void __launch_bounds__(RB_WMAX * 32, 1) k_rhs_xsweep_bulk(Geo g, const R* __restrict__ Q,
+                                                                     const R* __restrict__ PR, R* __restrict__ H0,
+                                                                     R* __restrict__ RHS, double* __restrict__ partial,
+                                                                     DevState* __restrict__ st,
+                                                                     const R* __restrict__ fac, int ns) {
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    __shared__ uint64_t bars[RB_WMAX];
+    __shared__ double sred[RB_WMAX];
+    __shared__ int is_last;
+    constexpr int L = 32 * S;
+    const int M = g.M;
+    const int nw = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int LS = L + 33;
+    R* wbase = reinterpret_cast<R*>(sm_raw) + (size_t)warp * rb_warp_elems(L);
+    R* const sg = wbase;
+    R* sl = wbase + RB_ROWS * L;
+    uint64_t* bar = &bars[warp];
+    if (lane == 0) mbar_init(bar, 1);
+    __syncwarp();
+    const int nlines = M * g.N;
+    const int stride = gridDim.x * nw;
+    const int first = blockIdx.x * nw + warp;
+    if (lane == 0) {
+        if (first < nlines) rb_issue<R>(g, Q, PR, H0, first, sg, bar);
+    }
+    const R dt = (R)st->dt;
+    const R tg = (R)g.tgam[ns], tr = (R)g.troh[ns], ta = (R)g.talp[ns];
+    const R coev = ta * (R)g.cvisc;
+    const R coep = ta * dt;
+    const R dxi = (R)g.dxi, dzi = (R)g.dzi, dxqi = (R)g.dxqi, dzqi = (R)g.dzqi;
+    const R c1x = (R)(0.5 * 0.5 * g.dxi);
+    const R c3x = (R)(0.5 * 0.5 * g.dzi);
+    const R* fx = fac + FSET_X * FAC_SET;
+    double bulk = 0.0;
+    uint32_t phase = 0u;
+    bool pending = first < nlines;  // a copy issued and not yet consumed
+    bool ok = true;
+#pragma unroll 1
+    for (int line = first; line < nlines; line += stride) {
+        ok = mbar_wait(bar, phase, &st->err);
+        if (!ok) break;  // the copy never completed: stop issuing
+        phase ^= 1u;
+        pending = false;
+        const int j = 1 + line % M, k = line / M;
+        const int jp = j + 1;
+        const R wffj = (R)g.wff[j], wfbj = (R)g.wfb[j], wffp = (R)g.wff[jp], wfbp = (R)g.wfb[jp];
+        const R dyfij = (R)g.dyfi[j], dycij = (R)g.dyci[j];
+        const double dyj = 1.0 / g.dyfi[j] / 1.0;
+        const R amu = (R)g.amvr[j], acu = (R)g.acvr[j], apu = (R)g.apvr[j];
+        const R amv = (R)g.amvr[(M + 2) + j], acv = (R)g.acvr[(M + 2) + j], apv = (R)g.apvr[(M + 2) + j];
+        const R amw = (R)g.amvr[2 * (M + 2) + j], acw = (R)g.acvr[2 * (M + 2) + j], apw = (R)g.apvr[2 * (M + 2) + j];
+        const R* sU = sg;          // c, jp, jm, kp, km
+        const R* sV = sg + 5 * L;  // c, jp, jm, kp, km, (jp, km)
+        const R* sW = sg + 11 * L; // c, jp, jm, kp, km, (jm, kp)
+        const R* sP = sg + 17 * L; // c, jm, km
+        const R* sH = sg + 20 * L; // u, v, w
+        R* H0l = H0 + iidx(g, 0, j, k);
+#pragma unroll 1
+        for (int kk = 0; kk < S; ++kk) {
+            const int i = lane + 32 * kk;
+            const int ip = i + 1 == L ? 0 : i + 1, im = i == 0 ? L - 1 : i - 1;
+            const R u = sU[i], uip = sU[ip], uim = sU[im];
+            const R ujp = sU[L + i], ujm = sU[2 * L + i], ukp = sU[3 * L + i], ukm = sU[4 * L + i];
+            const R v = sV[i], vip = sV[ip], vim = sV[im];
+            const R vjp = sV[L + i], vjm = sV[2 * L + i], vkp = sV[3 * L + i], vkm = sV[4 * L + i];
+            const R w = sW[i], wip = sW[ip], wim = sW[im];
+            const R wjp = sW[L + i], wjm = sW[2 * L + i], wkp = sW[3 * L + i], wkm = sW[4 * L + i];
+            const R pc = sP[i], pim = sP[im], pjm = sP[L + i], pkm = sP[2 * L + i];
+            const R vjpim = sV[L + im], wkpim = sW[3 * L + im];
+            const R ujmip = sU[2 * L + ip], wjmkp = sW[5 * L + i];
+            const R ukmip = sU[4 * L + ip], vjpkm = sV[5 * L + i];
+            const R h0u = sH[i], h0v = j >= 2 ? sH[L + i] : R(0), h0w = sH[2 * L + i];
+            const int pos = seg_pos<S>(i);
+            R Hu, Hv = R(0), Hw, ru, rv = R(0), rw;
+            {
+                const R H11 = ((uip + u) * (uip + u) - (uim + u) * (uim + u)) * c1x;
+                const R coe2 = dyfij * R(0.5);
+                const R H12 = ((vjp + vjpim) * (wffp * ujp + wfbp * u) - (v + vim) * (wffj * u + wfbj * ujm)) * coe2;
+                const R coe3 = c3x;
+                const R H13 = ((wkp + wkpim) * (ukp + u) - (w + wim) * (u + ukm)) * coe3;
+                Hu = -(H11 + H12 + H13);
+                const R rhsc = tg * Hu + tr * h0u;
+                const R rhsl = coev * ((uip - R(2) * u + uim) * dxqi + (ukp - R(2) * u + ukm) * dzqi +
+                                       (ujp * apu + u * acu + ujm * amu));
+                R r = (rhsc + rhsl) * dt;
+                ru = r - (pc - pim) * dxi * coep;
+                bulk += (double)ru * dyj;
+            }
+            if (j >= 2) {
+                const R coe1 = dxi * R(0.5);
+                const R H21 = ((wffj * uip + wfbj * ujmip) * (vip + v) - (wffj * u + wfbj * ujm) * (v + vim)) * coe1;
+                const R coe2 = dycij * R(0.5) * R(0.5);
+                const R H22 = ((vjp + v) * (vjp + v) - (v + vjm) * (v + vjm)) * coe2;
+                const R coe31 = dzi * R(0.5);
+                const R H23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v) - (wffj * w + wfbj * wjm) * (v + vkm)) * coe31;
+                Hv = -(H21 + H22 + H23);
+                const R rhsc = tg * Hv + tr * h0v;
+                const R rhsl = coev * ((vip - R(2) * v + vim) * dxqi + (vkp - R(2) * v + vkm) * dzqi +
+                                       (vjp * apv + v * acv + vjm * amv));
+                R r = (rhsc + rhsl) * dt;
+                rv = r - (pc - pjm) * dycij * coep;
+            }
+            {
+                const R H31 = ((uip + ukmip) * (wip + w) - (u + ukm) * (w + wim)) * c1x;
+                const R coe2 = dyfij * R(0.5);
+                const R H32 = ((vjp + vjpkm) * (wffp * wjp + wfbp * w) - (v + vkm) * (wffj * w + wfbj * wjm)) * coe2;
+                const R H33 = ((wkp + w) * (wkp + w) - (w + wkm) * (w + wkm)) * c3x;
+                Hw = -(H31 + H32 + H33);
+                const R rhsc = tg * Hw + tr * h0w;
+                const R rhsl = coev * ((wip - R(2) * w + wim) * dxqi + (wkp - R(2) * w + wkm) * dzqi +
+                                       (wjp * apw + w * acw + wjm * amw));
+                R r = (rhsc + rhsl) * dt;
+                rw = r - (pc - pkm) * dzi * coep;
+            }
+            H0l[i] = Hu;
+            if (j >= 2) H0l[i + g.FI] = Hv;
+            H0l[i + 2 * g.FI] = Hw;
+            sl[pos] = ru;
+            if (j >= 2) sl[LS + pos] = rv;
+            sl[2 * LS + pos] = rw;
+        }
+        // the stage is read: refill it with this warp's next line
+        __syncwarp();
+        fence_async_smem();
+        if (line + stride < nlines) {
+            if (lane == 0) rb_issue<R>(g, Q, PR, H0, line + stride, sg, bar);
+            pending = true;
+        }
+        // cyclic x sweeps of this line's three components (MOMFA1_X_tg starts at N2I = 2 for v)
+#pragma unroll 1
+        for (int c = 0; c < 3; ++c)
+            if (c != 1 || j >= 2) warp_tdma_apply_smem<S, true>(sl + c * LS, fx, lane);
+        __syncwarp();
+        R* Rl = RHS + iidx(g, 0, j, k);
+#pragma unroll
+        for (int kk = 0; kk < S; ++kk) {
+            const int i = lane + 32 * kk;
+            const int pos = seg_pos<S>(i);
+            Rl[i] = sl[pos];
+            if (j >= 2) Rl[i + g.FI] = sl[LS + pos];
+            Rl[i + 2 * g.FI] = sl[2 * LS + pos];
+        }
+        __syncwarp();
+    }
+    if (!ok) {
+        // the warp's copy may still be in flight: wait for it (bounded) before the block exits
+        if (pending) mbar_wait(bar, phase, &st->err);
+    }
+    // grid sum of the bulk-flux integrand: warp, block (warp order), then the
+    // last block adds the block partials in index order (deterministic)
+    for (int o = 16; o > 0; o >>= 1) bulk += __shfl_down_sync(0xffffffffu, bulk, o);
+    if (lane == 0) sred[warp] = bulk;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w2 = 0; w2 < nw; ++w2) s += sred[w2];
+        partial[blockIdx.x] = s;
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->ctr, 1u);
+        is_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (is_last) {
+        __threadfence();
+        if (threadIdx.x == 0) {
+            double s = 0.0;
+            for (int t = 0; t < (int)gridDim.x; ++t) s += __ldcg(partial + t);
+            st->bulksum = s;
+            st->ctr = 0u;
+        }
+    }
+}

@@ -327,15 +327,16 @@ int chapsim_upload_pp_means_tg(chapsim_ctx_t* ctx, int32_t nstatis, const double
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the faster of each pair (force = -1), or the ones forced (force = 0..3):
+ * the fastest of each group (force = -1), or the ones forced (force = 0..5):
  *   bit 0: Poisson y-solve, 0 = warp Thomas/PCR hybrid, 1 = the reference's
  *          sequential Thomas recurrence, one thread per mode;
- *   bit 1: explicit right-hand sides + x sweep, 0 = fused (one warp per x
- *          line), 1 = split into a point-wise kernel and a line-sweep kernel
- *          (periodic channel only).
- * choice receives the kept setting in the same bit form; ms[4] (may be NULL)
+ *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
+ *          0 = fused (one warp per x line, per-thread loads), 1 = split into
+ *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
+ *          stencil rows staged in shared memory by bulk copies.
+ * choice receives the kept setting in the same bit form; ms[5] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential) and right-hand sides
- * (fused, split).  CONVH0 is restored after the trial launches. */
+ * (fused, split, bulk-staged).  CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 
 /* An ensemble of independent periodic channels (any grids and precisions, one

@@ -1,9 +1,12 @@
 """Ensembles of uneven periodic channels and the y-solve autotuner.
 
 * Both Poisson y-solve variants (warp Thomas/PCR hybrid, sequential Thomas)
-  and both forms of the right-hand-side / x-sweep stage (fused, split)
-  solve the FFT99 problem to 1e-12 of the oracle, and the step with any
-  combination stays within 1e-11 after 10 steps.
+  and the three forms of the right-hand-side / x-sweep stage (fused, split,
+  fused with bulk-copy staging) solve the FFT99 problem to 1e-12 of the
+  oracle, and the step with any combination stays within 1e-11 after 10
+  steps.  The bulk-staged form computes the same per-point arithmetic as the
+  fused one (only the bulk-flux sum is added in another order), checked at
+  other line lengths and in mixed precision.
 * An ensemble (one graph per step, one branch per member) advances every
   member exactly as its own graph does: fields bitwise equal.
 """
@@ -24,7 +27,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5])
 def test_ysolve_variants_match_oracle(kind):
     L, M, N = 96, 64, 64
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
@@ -56,6 +59,28 @@ def test_ysolve_variants_match_oracle(kind):
     for i in range(3):
         assert rel(Qg[i][:, 1:M + 1], Qo[i][:, 1:M + 1]) <= 1e-11
     c.close()
+
+
+@pytest.mark.parametrize("shape,precision,tol", [((384, 32, 32), "fp64", 1e-12), ((128, 64, 32), "fp64", 1e-12),
+                                                 ((32, 32, 32), "fp64", 1e-12), ((256, 64, 32), "mixed", 1e-5)])
+def test_bulk_staged_rhs_matches_fused(shape, precision, tol):
+    L, M, N = shape
+    s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    Q, PR = initial_field(s, 77, 0.1)
+    out = []
+    for kind in (0, 4):
+        c = gpu.ChannelTG(s, precision=precision)
+        choice, _ = c.autotune(force=kind)
+        assert choice == kind
+        c.upload(Q, PR)
+        c.set_dt(2e-3)
+        c.SOLVERRK3_MOM_tg(0)
+        c.advance(5, 2e-3, 1e-6, 0.5)
+        out.append(c.download()[0])
+        c.close()
+    for i in range(3):
+        e = rel(out[1][i][:, 1:M + 1], out[0][i][:, 1:M + 1])
+        assert e <= tol, (i, e)
 
 
 GRIDS = [(64, 64, 64, 2 * math.pi, math.pi, 2800.0), (96, 64, 96, 2 * math.pi, math.pi, 4000.0),
