@@ -37,7 +37,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_mlp_gradients", "chapsim_mlp_train", "chapsim_mlp_infer_points", "chapsim_thermal_use_mlp",
             "chapsim_mlp_judge", "chapsim_autotune", "chapsim_batch_create", "chapsim_batch_advance",
             "chapsim_batch_get_stream", "chapsim_batch_destroy", "chapsim_pp_mean_zx_tg", "chapsim_pp_mean_t_tg",
-            "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg"]
+            "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
 PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
@@ -130,6 +130,7 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_thermal_use_mlp.argtypes = [vp, ctypes.c_int32]
     L.chapsim_mlp_judge.argtypes = [vp, _dp]
     L.chapsim_autotune.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]
+    L.chapsim_divgck_io.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
     L.chapsim_pp_mean_zx_tg.argtypes = [vp]
     L.chapsim_pp_mean_t_tg.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
     L.chapsim_pp_monitor_tg.argtypes = [vp, ctypes.c_double, _dp]
@@ -552,6 +553,12 @@ class ChannelIO(ChannelTG):
     def CFL_io(self):
         v = ctypes.c_double()
         self._check(self.lib.chapsim_cfl_io(self.h, ctypes.byref(v)))
+        return v.value
+
+    def DIVGCK_io(self):
+        """MAXDIVGV_io: max |div G + DrhoDtP| over the interior."""
+        v = ctypes.c_double()
+        self._check(self.lib.chapsim_divgck_io(self.h, ctypes.byref(v)))
         return v.value
 
     # -- thermal solver (SOLVERRK3_ENG_io with table-search properties) ----------

@@ -1206,6 +1206,21 @@ int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {
     return rc;
 }
 
+int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv) {
+    if (!ctx || !maxdiv) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    CK(cudaSetDevice(ctx->device));
+    k_io_divgck<<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, ctx->io.G, ctx->thermal ? ctx->tf.DRHO : nullptr,
+                                                           ctx->part_red);
+    k_maxdiv_final<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st);
+    ctx->launches += 2;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *maxdiv = ctx->st_host->maxdiv;
+    return CHAPSIM_OK;
+}
+
 int chapsim_get_stream(chapsim_ctx_t* ctx, void** stream) {
     if (!ctx || !stream) return CHAPSIM_ERR_BADARG;
     *stream = (void*)ctx->stream;

@@ -518,3 +518,28 @@ __global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFields f, double* __r
     double r = block_max<IO_NT>(mx, sred);
     if (threadIdx.x == 0) partial[blockIdx.x] = r;
 }
+
+// DIVGCK_io (src/DIVGCK.f90:60-121 with DIVGCK_Comm_io :125-184), x-periodic
+// main domain: max over the interior of |div G + DrhoDtP| (all three ranges of
+// MAXDIVGV_io coincide).  Per-block maxima; k_maxdiv_final reduces them.  DRHO
+// is NULL while the thermal solver is off (DrhoDtP = 0).
+__global__ void __launch_bounds__(IO_NT) k_io_divgck(Geo g, const double* __restrict__ G,
+                                                     const double* __restrict__ DRHO, double* __restrict__ partial) {
+    __shared__ double sred[32];
+    const int L = g.L, N = g.N;
+    const long long tot = (long long)L * g.M * N;
+    double mx = 0.0;
+    for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
+        int i, j, k;
+        io_decode(g, t, i, j, k);
+        const long long c = pidx(g, i, j, k);
+        const double DIVX = (G[pidx(g, wrapp(i, L), j, k)] - G[c]) * g.dxi;
+        const double DIVY = (G[c + g.FS + L] - G[c + g.FS]) * (g.dyfi[j] * 1.0);
+        const double DIVZ = (G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - G[c + 2 * g.FS]) * (g.dzi * 1.0);
+        const double DTRHO = DRHO ? DRHO[c] : 0.0;
+        const double DQCAP = DIVX + DIVY + DIVZ + DTRHO;
+        mx = fmax(fabs(DQCAP), mx);
+    }
+    const double r = block_max<IO_NT>(mx, sred);
+    if (threadIdx.x == 0) partial[blockIdx.x] = r;
+}

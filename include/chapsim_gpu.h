@@ -202,6 +202,9 @@ int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* g, double* q, double*
 int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns);
 /* CFL_io (src/CFL.f90:55-107): CFLMM_io including the viscous number. */
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm);
+/* DIVGCK_io (src/DIVGCK.f90:60-184), x-periodic main domain: MAXDIVGV_io, the
+ * max over the interior of |div G + DrhoDtP| (the three ranges coincide). */
+int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv);
 
 /* ---- Thermophysical properties by table search ----
  * The nondimensional table and spline coefficients of the thermal_info module

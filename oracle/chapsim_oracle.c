@@ -2138,6 +2138,30 @@ void orc_thermal_get(const orc_t* o, double* out) {
     for (int a = 0; a < 7; ++a) memcpy(out + a * fs, src[a], fs * sizeof(double));
 }
 
+/* DIVGCK_io (src/DIVGCK.f90:60-121) via DIVGCK_Comm_io (:125-184), x-periodic:
+ * max |div G + DrhoDtP|, loop order JC, KC, IC. */
+double orc_io_divgck(const orc_t* o) {
+    int L = o->L, M = o->M, N = o->N;
+    double DIVMAX = 0.0;
+    for (int JC = 1; JC <= M; ++JC) {
+        int JP = JC + 1, JJ = JC;
+        double COE2 = o->DYFI[JJ] * 1.0, COE3 = o->DZI * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KP = KPV(o, KC);
+            for (int IC = 1; IC <= L; ++IC) {
+                int IP = IPV(o, IC);
+                double DIVX = (GV(o, IP, JC, KC, 1) - GV(o, IC, JC, KC, 1)) * o->DXI;
+                double DIVY = (GV(o, IC, JP, KC, 2) - GV(o, IC, JC, KC, 2)) * COE2;
+                double DIVZ = (GV(o, IC, JC, KP, 3) - GV(o, IC, JC, KC, 3)) * COE3;
+                double DTRHO = F3(o->DRHODT, o, IC, JC, KC);
+                double DQCAP = DIVX + DIVY + DIVZ + DTRHO;
+                DIVMAX = fmax(fabs(DQCAP), DIVMAX);
+            }
+        }
+    }
+    return DIVMAX;
+}
+
 /* CFL_io (src/CFL.f90:55-107), including the viscous number */
 double orc_io_cfl(orc_t* o) {
     int L = o->L, M = o->M, N = o->N;

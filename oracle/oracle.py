@@ -77,6 +77,8 @@ def lib():
         L.orc_io_run_steps.restype = ctypes.c_int
         L.orc_io_monitor.argtypes = [ctypes.c_void_p, _dp]
         L.orc_io_set_vis_scheme.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_io_divgck.argtypes = [ctypes.c_void_p]
+        L.orc_io_divgck.restype = ctypes.c_double
         L.orc_io_drhoi_maxabs.argtypes = [ctypes.c_void_p]
         L.orc_io_drhoi_maxabs.restype = ctypes.c_double
         L.orc_thermal_enable.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_double,
@@ -248,6 +250,9 @@ class Oracle:
     def io_substep(self, ns):
         if self._lib.orc_io_substep(self._h, int(ns)) != 0:
             raise ValueError("bad substep or IO path not enabled")
+
+    def io_divgck(self):
+        return self._lib.orc_io_divgck(self._h)
 
     def io_cfl(self):
         return self._lib.orc_io_cfl(self._h)

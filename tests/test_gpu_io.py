@@ -82,6 +82,8 @@ def test_io_tc8_reproduces_reference_monitor_on_gpu(tc8):
             ref = r[cols.index(name)]
             assert abs(m[name] - ref) <= 0.5 * 10.0 ** (math.floor(math.log10(abs(ref))) - 5) * 1.0001, (step, name)
         assert abs(m["Gmaxx"] - r[cols.index("Gmaxx")]) <= 0.5e-5 * 1.0001
+        # DIVGCK_io: round-off, within twice the reference's logged MaxDiv of the row
+        assert ch.DIVGCK_io() <= 2.0 * r[cols.index("MaxDiv")], (step, ch.DIVGCK_io())
     Go, Qo, Po = o.io_get_fields()
     for comp in range(3):
         assert rel(Gg[comp], Go[comp]) <= TOL_STEP

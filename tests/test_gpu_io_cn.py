@@ -173,6 +173,10 @@ def test_cn_heated_channel_matches_oracle():
     tg, to = ch.download_thermal(), o.thermal_get()
     for k in ("DH", "T", "D", "M"):
         assert rel(tg[k], to[k]) <= 1e-10, k
+    # DIVGCK_io: the projection leaves div G + DrhoDtP at round-off, on both sides
+    dg, do = ch.DIVGCK_io(), o.io_divgck()
+    print("max |div G + drho/dt|", dg, do)
+    assert dg <= 1e-11 and do <= 1e-11
 
 
 def test_cn_option_rejected_outside_main_domain():

@@ -6,7 +6,9 @@ advanced 19 steps.  The monitor columns that follow from the instantaneous
 fields (CFL, centreline mean u, u'u', u'v', max of the mean mass-flux
 profile) must equal the reference's log rows 101-119 to every printed digit
 (monitor.io.2020.1217.1640.log, written by PP_MONITOR_Xperiodic_io,
-src/processing/PP_SCN_MONITOR.f90:610-613)."""
+src/processing/PP_SCN_MONITOR.f90:610-613).  The MaxDiv column (DIVGCK_io) is
+round-off, 1.1e-14 to 1.4e-14 in the log; the oracle's must stay within twice
+the logged value of each row."""
 import json
 import os
 
@@ -62,4 +64,5 @@ def test_tc8_restart_reproduces_monitor_rows_101_119(tc8):
             ref = r[cols.index(name)]
             assert abs(val - ref) <= _half_ulp(ref, kind), (step, name, val, ref)
             checked += 1
+        assert o.io_divgck() <= 2.0 * r[cols.index("MaxDiv")], (step, o.io_divgck())
     assert checked == 19 * 5
