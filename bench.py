@@ -303,8 +303,8 @@ def heated_measure(args, local, dist, ws, steps):
 
 def kernel_bytes(L, precision="fp64"):
     """Algorithmic bytes per grid point per launch.  FP64: 8 bytes per word of
-    kernel_words.  Mixed: Q, PR, CONVH0, RHS and RHSLLPHI are 4-byte words;
-    the spectrum and DPH stay FP64."""
+    kernel_words.  Mixed: Q, PR, CONVH0, RHS, RHSLLPHI and the spectrum are
+    4-byte words; DPH stays FP64."""
     if precision == "fp64":
         return {k: 8.0 * v for k, v in kernel_words(L).items()}
     spec = 2.0 * (L // 2 + 1) / L
@@ -313,9 +313,9 @@ def kernel_bytes(L, precision="fp64"):
         "k_rhs_xsweep": 13 * 4.0,
         "k_zsweep": 6 * 4.0,
         "k_ysweep": 9 * 4.0,
-        "k_div_fftx": 4 * 4.0 + 8.0 * spec,
-        "k_fftz_fwd": 16.0 * spec, "k_fftz_inv": 16.0 * spec, "k_ysolve": 16.0 * spec,
-        "k_fftx_inv": 8.0 * spec + 8.0,
+        "k_div_fftx": 4 * 4.0 + 4.0 * spec,
+        "k_fftz_fwd": 8.0 * spec, "k_fftz_inv": 8.0 * spec, "k_ysolve": 8.0 * spec,
+        "k_fftx_inv": 4.0 * spec + 8.0,
         "k_correct": 8.0 + 6 * 4.0 + 2 * 4.0 + 4.0,   # DPH; Q x3 in/out; PR in/out; RHSLLPHI
     }
 
@@ -701,8 +701,8 @@ def run_b200(args):
         line["variants"] = {"mixed": {"value": vm, "unit": UNIT, "ms_per_step": msm / args.steps,
                                       "speedup_vs_fp64": vm / value, "max_div": chm.DIVGCK_tg(),
                                       "autotuned_choice_bits": mt,
-                                      "precision": "FP32 storage, stencils and CN sweeps; FP64 Poisson, projection, "
-                                                   "bulk sums"}}
+                                      "precision": "FP32 storage, stencils, CN sweeps and x/z transforms; FP64 "
+                                                   "y-solve, divergence, projection, bulk sums"}}
         ch = chm
         # config 4: heated main domain, table search against the learned property model
         hl = heated_measure(args, local, dist, ws, min(args.steps, 100))

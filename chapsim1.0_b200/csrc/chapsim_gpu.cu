@@ -144,6 +144,7 @@ struct chapsim_ctx {
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     double2* SP = nullptr;
+    float2* SPf = nullptr;       // FP32 spectral array of the mixed-precision step
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
     // mixed precision (CHAPSIM_PREC_MIXED): FP32 copies of the momentum-stage
@@ -157,6 +158,7 @@ struct chapsim_ctx {
     DevState* st_host = nullptr;  // pinned mirror for readback
     double* ybuf = nullptr;       // device copies of y-arrays and wavenumbers
     double2* tw = nullptr;
+    float2* twf = nullptr;        // FP32 copies of tw
     int domain = 1;               // 1: periodic TG channel, 2: main domain (IO)
     int ivis = 0;                 // main domain: 0 explicit viscous terms, 1 Crank-Nicolson (iVisScheme)
     // statistics of the periodic channel (stats.cuh), allocated by the first call
@@ -235,13 +237,20 @@ int rt_chunk(const Geo& g) {
     while (chunk % 2 == 0 && chunk / 2 >= 16 && tiles * (g.N / chunk) < 4 * 148) chunk /= 2;
     return chunk;
 }
-size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * fft4s_ld(g.L)) * sizeof(double2); }
-size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(double2); }
+template <typename C = double2>
+size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * fft4s_ld(g.L)) * sizeof(C); }
+template <typename C = double2>
+size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(C); }
+// the context's spectral array of element type C
+template <typename C> C* spec(chapsim_ctx* c);
+template <> double2* spec<double2>(chapsim_ctx* c) { return c->SP; }
+template <> float2* spec<float2>(chapsim_ctx* c) { return c->SPf; }
 
 // twiddles of the small DFTs inside the four-step FFT (constant memory, shared by all contexts)
 cudaError_t upload_small_twiddles() {
     const long double pi = 3.141592653589793238462643383279502884L;
     double2 w[24];
+    float2 wf[24];
     const int sizes[4] = {8, 12, 16, 24};
     cudaError_t e = cudaSuccess;
     for (int s = 0; s < 4 && e == cudaSuccess; ++s) {
@@ -249,21 +258,26 @@ cudaError_t upload_small_twiddles() {
         for (int q = 0; q < P; ++q) {
             const long double a = 2.0L * pi * (long double)q / (long double)P;
             w[q] = make_double2((double)cosl(a), (double)(-sinl(a)));
+            wf[q] = make_float2((float)cosl(a), (float)(-sinl(a)));
         }
         if (P == 8) e = cudaMemcpyToSymbol(c_w8, w, sizeof(double2) * 8);
         if (P == 12) e = cudaMemcpyToSymbol(c_w12, w, sizeof(double2) * 12);
         if (P == 16) e = cudaMemcpyToSymbol(c_w16, w, sizeof(double2) * 16);
         if (P == 24) e = cudaMemcpyToSymbol(c_w24, w, sizeof(double2) * 24);
+        if (e != cudaSuccess) break;
+        if (P == 8) e = cudaMemcpyToSymbol(c_w8f, wf, sizeof(float2) * 8);
+        if (P == 12) e = cudaMemcpyToSymbol(c_w12f, wf, sizeof(float2) * 12);
+        if (P == 16) e = cudaMemcpyToSymbol(c_w16f, wf, sizeof(float2) * 16);
+        if (P == 24) e = cudaMemcpyToSymbol(c_w24f, wf, sizeof(float2) * 24);
     }
     return e;
 }
 size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(double2); }
 
 // forward declaration: DISPATCH_S is defined below
-void launch_ysolve_warp(chapsim_ctx* ctx);
-
-void launch_ysolve_seq(chapsim_ctx* ctx);
-void launch_ysolve(chapsim_ctx* ctx);
+template <typename C = double2> void launch_ysolve_warp(chapsim_ctx* ctx);
+template <typename C = double2> void launch_ysolve_seq(chapsim_ctx* ctx);
+template <typename C = double2> void launch_ysolve(chapsim_ctx* ctx);
 
 // Kernel attributes are process-wide and several contexts (of different
 // grids) may share a kernel, so the dynamic shared-memory limit is raised to
@@ -304,23 +318,26 @@ int ysolve_seq_lines(int M) {
     return nt;
 }
 
+template <typename C>
 void launch_ysolve_seq(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
     const int nt = ysolve_seq_lines(g.M);
-    k_ysolve_seq<<<(int)((nl + nt - 1) / nt), nt, smem_ysolve_seq(g.M, nt), ctx->stream>>>(g, ctx->SP, ctx->YF);
+    k_ysolve_seq<C><<<(int)((nl + nt - 1) / nt), nt, smem_ysolve_seq(g.M, nt), ctx->stream>>>(g, spec<C>(ctx), ctx->YF);
 }
 
+template <typename C>
 void launch_ysolve(chapsim_ctx* ctx) {
-    if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq(ctx);
-    else launch_ysolve_warp(ctx);
+    if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx);
+    else launch_ysolve_warp<C>(ctx);
 }
 
+template <typename C>
 void launch_ysolve_warp(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
     const int nb = (int)((nl + YW_L - 1) / YW_L);
-    DISPATCH_S(g.M / 32, (k_ysolve_warp<S><<<nb, YW_NT, smem_yw(g), ctx->stream>>>(g, ctx->SP)));
+    DISPATCH_S(g.M / 32, (k_ysolve_warp<S, C><<<nb, YW_NT, smem_yw(g), ctx->stream>>>(g, spec<C>(ctx))));
 }
 
 // Momentum-stage arrays of the context in the real type R of its precision.
@@ -341,7 +358,13 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
     DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
     CK(set_smem(k_rhs_point<R>, smem_rt<R>()));
-    DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px(g))));
+    using C = SpecT<R>;
+    DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
+    DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
+    CK(set_smem(k_ysolve_seq<C>, smem_ysolve_seq(g.M, ysolve_seq_lines(g.M))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, C>, smem_fz<C>(g))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, C>, smem_fz<C>(g))));
     return CHAPSIM_OK;
 }
 
@@ -349,13 +372,14 @@ int configure_kernels(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     int rc = ctx->prec == CHAPSIM_PREC_MIXED ? configure_momentum<float>(ctx) : configure_momentum<double>(ctx);
     if (rc) return rc;
-    DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2>, smem_px(g))));
+    // the FP64 spectral stage serves the standalone Poisson solve and the main domain in every precision
+    DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, double2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq, smem_ysolve_seq(g.M, ysolve_seq_lines(g.M))));
-    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2>, smem_fz(g))));
-    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2>, smem_fz(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw(g))));
+    CK(set_smem(k_ysolve_seq<double2>, smem_ysolve_seq(g.M, ysolve_seq_lines(g.M))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));
     if (ctx->domain == 2 && ctx->ivis) {
         DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S>, smem_cn(g.L))));
         DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S>, smem_cn(g.N))));
@@ -440,18 +464,20 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     dim3 gry(g.L / 32, g.N);
     DISPATCH_S(g.M / 32, (k_ysweep<S, R><<<gry, SWEEP_NT, smem_y<R>(g), s>>>(g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
+    using C = SpecT<R>;
+    C* sp = spec<C>(ctx);
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    DISPATCH_FFT(g.L, (k_div_fftx<R, FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, f.Q, f.RHSLL, ctx->SP, ctx->st, ns)));
+    DISPATCH_FFT(g.L, (k_div_fftx<R, FN1, FN2><<<grp, PX_NT, smem_px<C>(g), s>>>(g, f.Q, f.RHSLL, sp, ctx->st, ns)));
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
     prof_mark(ctx);
-    launch_ysolve(ctx);
+    launch_ysolve<C>(ctx);
     prof_mark(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
     prof_mark(ctx);
-    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, C><<<grp, PX_NT, smem_px<C>(g), s>>>(g, sp, ctx->DPH)));
     prof_mark(ctx);
     const long long tot = (long long)g.L * g.M * g.N;
     k_correct<R><<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
@@ -575,13 +601,13 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     prof_mark(ctx);
-    launch_ysolve(ctx);
+    launch_ysolve<double2>(ctx);
     prof_mark(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
     prof_mark(ctx);
-    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, double2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     prof_mark(ctx);
     k_io_correct<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, ctx->ivis ? ctx->RHSLL : nullptr);
     prof_mark(ctx);
@@ -741,6 +767,14 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaMemcpy(ctx->tw, twx.data(), L * sizeof(double2), cudaMemcpyHostToDevice));
     INIT_CK(cudaMemcpy(ctx->tw + L, twz.data(), N * sizeof(double2), cudaMemcpyHostToDevice));
     g.twx = ctx->tw; g.twz = ctx->tw + L;
+    {
+        std::vector<float2> twf((size_t)(L + N));
+        for (int i = 0; i < L; ++i) twf[i] = make_float2((float)twx[i].x, (float)twx[i].y);
+        for (int k = 0; k < N; ++k) twf[L + k] = make_float2((float)twz[k].x, (float)twz[k].y);
+        INIT_CK(cudaMalloc(&ctx->twf, (size_t)(L + N) * sizeof(float2)));
+        INIT_CK(cudaMemcpy(ctx->twf, twf.data(), (L + N) * sizeof(float2), cudaMemcpyHostToDevice));
+        g.twxf = ctx->twf; g.twzf = ctx->twf + L;
+    }
     INIT_CK(cudaMalloc(&ctx->yz, (size_t)2 * M * sizeof(double)));
     g.yz = ctx->yz;
     k_ysolve_zero_factors<<<1, 32, 0, ctx->stream>>>(g, ctx->yz);
@@ -791,6 +825,7 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         INIT_CK(cudaMemset(ctx->RHSf, 0, (size_t)(3 * g.FI) * sizeof(float)));
         INIT_CK(cudaMemset(ctx->RHSLLf, 0, (size_t)g.FI * sizeof(float)));
         INIT_CK(cudaMemset(ctx->facf, 0, (size_t)4 * 5 * FAC_SET * sizeof(float)));
+        INIT_CK(cudaMalloc(&ctx->SPf, (size_t)g.LH * M * N * sizeof(float2)));
     }
     INIT_CK(cudaMalloc(&ctx->st, sizeof(DevState)));
     INIT_CK(cudaMallocHost(&ctx->st_host, sizeof(DevState)));
@@ -821,7 +856,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
     cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
-    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->yz);
+    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->twf); cudaFree(ctx->yz); cudaFree(ctx->SPf);
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
@@ -1098,10 +1133,10 @@ int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph) {
     DISPATCH_FFT(g.L, (k_fftx_from_rhs<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->RHSLL, ctx->SP)));
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
-    launch_ysolve(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
-    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    launch_ysolve<double2>(ctx);
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, double2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     ctx->launches += 5;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(dph, ctx->DPH, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1787,20 +1822,23 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         k_ysolve_seq_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF);
         CK(cudaGetLastError());
     }
-    CK(cudaMemsetAsync(ctx->SP, 0, nsp * sizeof(double2), s));
+    // the variants are timed on the spectral array the time step uses (FP32 in the mixed-precision step)
+    const bool spf = ctx->SPf != nullptr;
+    if (spf) CK(cudaMemsetAsync(ctx->SPf, 0, nsp * sizeof(float2), s));
+    else CK(cudaMemsetAsync(ctx->SP, 0, nsp * sizeof(double2), s));
+    auto run_y = [&](int kind) {
+        if (spf) { if (kind == 0) launch_ysolve_warp<float2>(ctx); else launch_ysolve_seq<float2>(ctx); }
+        else { if (kind == 0) launch_ysolve_warp<double2>(ctx); else launch_ysolve_seq<double2>(ctx); }
+    };
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float t[2] = {0.f, 0.f};
     const int reps = 5;
     for (int kind = 0; kind < 2; ++kind) {
-        for (int w = 0; w < 2; ++w) {
-            if (kind == 0) launch_ysolve_warp(ctx); else launch_ysolve_seq(ctx);
-        }
+        for (int w = 0; w < 2; ++w) run_y(kind);
         CK(cudaEventRecord(e0, s));
-        for (int r = 0; r < reps; ++r) {
-            if (kind == 0) launch_ysolve_warp(ctx); else launch_ysolve_seq(ctx);
-        }
+        for (int r = 0; r < reps; ++r) run_y(kind);
         CK(cudaEventRecord(e1, s));
         CK(cudaEventSynchronize(e1));
         CK(cudaEventElapsedTime(&t[kind], e0, e1));

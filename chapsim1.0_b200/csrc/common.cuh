@@ -62,6 +62,8 @@ struct Geo {
     // FFT twiddles
     const double2* twx;  // [L] exp(-2 pi i e / L)
     const double2* twz;  // [N]
+    const float2* twxf;  // FP32 copies (spectral stage of the mixed-precision step)
+    const float2* twzf;
     const double* yz;    // [2M] factors of the zero-mode y recurrence (k_ysolve_zero_factors)
 };
 

@@ -22,6 +22,24 @@
 #include "fft.cuh"
 #include "tdma.cuh"
 
+#include <type_traits>
+
+// Spectral element type of a step whose fields are stored as R: double2 in the
+// FP64 step, float2 in the mixed-precision step (whose x and z transforms run
+// in FP32; the y-solve converts to FP64 and back).
+template <typename R> using SpecT = typename std::conditional<std::is_same<R, float>::value, float2, double2>::type;
+template <typename C> __device__ __forceinline__ const C* twx_of(const Geo& g);
+template <> __device__ __forceinline__ const double2* twx_of<double2>(const Geo& g) { return g.twx; }
+template <> __device__ __forceinline__ const float2* twx_of<float2>(const Geo& g) { return g.twxf; }
+template <typename C> __device__ __forceinline__ const C* twz_of(const Geo& g);
+template <> __device__ __forceinline__ const double2* twz_of<double2>(const Geo& g) { return g.twz; }
+template <> __device__ __forceinline__ const float2* twz_of<float2>(const Geo& g) { return g.twzf; }
+__device__ __forceinline__ double2 to_d2(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d2(float2 a) { return make_double2((double)a.x, (double)a.y); }
+template <typename C> __device__ __forceinline__ C from_d2(double2 a);
+template <> __device__ __forceinline__ double2 from_d2<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+
 #define PX_TJ 32  // x-lines per block (16 packed pairs)
 #define PX_NT 256
 #define FZ_TQ 16  // z-lines per block
@@ -33,8 +51,11 @@
 // precision step); divergence, transforms and correction are FP64 throughout.
 template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
-                                                    double2* __restrict__ SP, const DevState* __restrict__ st, int ns) {
-    extern __shared__ double2 smc[];
+                                                    SpecT<R>* __restrict__ SP, const DevState* __restrict__ st, int ns) {
+    using C = SpecT<R>;
+    using T = typename CReal<C>::T;
+    extern __shared__ __align__(16) unsigned char smp_raw[];
+    C* smc = reinterpret_cast<C*>(smp_raw);
     const int L = g.L, M = g.M, N = g.N, LH = g.LH;
     const int LD = fft4s_ld(L);
     const int j0 = 1 + blockIdx.x * PX_TJ;
@@ -63,19 +84,19 @@ __global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restric
             val = dv * coe0;
             RHSLL[iidx(g, i, j, k)] = (R)val;
         }
-        double2* line = smc + pair * LD;
-        if (part == 0) line[i].x = val; else line[i].y = val;
+        C* line = smc + pair * LD;
+        if (part == 0) line[i].x = (T)val; else line[i].y = (T)val;
     }
-    block_fft4s<N1, N2, -1>(smc, np, LD, g.twx);
+    block_fft4s<N1, N2, -1>(smc, np, LD, twx_of<C>(g));
     // unpack: A_k = (Z_k + conj Z_{L-k}) / 2, B_k = (Z_k - conj Z_{L-k}) / (2i), both times 1/L
-    const double sc = 0.5 / (double)L;
+    const T sc = (T)(0.5 / (double)L);
     for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
         const int pair = p / LH, kx = p - pair * LH;
-        const double2* line = smc + pair * LD;
-        const double2 z = line[kx];
-        const double2 zc = line[kx == 0 ? 0 : L - kx];
-        const double2 a = make_double2((z.x + zc.x) * sc, (z.y - zc.y) * sc);
-        const double2 b = make_double2((z.y + zc.y) * sc, (zc.x - z.x) * sc);
+        const C* line = smc + pair * LD;
+        const C z = line[kx];
+        const C zc = line[kx == 0 ? 0 : L - kx];
+        const C a = mkc((z.x + zc.x) * sc, (z.y - zc.y) * sc);
+        const C b = mkc((z.y + zc.y) * sc, (zc.x - z.x) * sc);
         const int ja = j0 + 2 * pair;
         SP[kx + (long long)LH * ((ja - 1) + (long long)M * k)] = a;
         if (2 * pair + 1 < nj) SP[kx + (long long)LH * ((ja) + (long long)M * k)] = b;
@@ -84,9 +105,11 @@ __global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restric
 
 // ---------------------------------------------------------------------------
 // complex z transform of FZ_TQ consecutive (kx, j) lines (index q = kx + LH*(j-1))
-template <int SIGN, int N1, int N2>
-__global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, double2* __restrict__ SP) {
-    extern __shared__ double2 smc[];
+template <int SIGN, int N1, int N2, typename C>
+__global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, C* __restrict__ SP) {
+    using T = typename CReal<C>::T;
+    extern __shared__ __align__(16) unsigned char smp_raw[];
+    C* smc = reinterpret_cast<C*>(smp_raw);
     const int N = g.N;
     const int LD = fft4s_ld(N);
     const long long Q = (long long)g.LH * g.M;
@@ -94,15 +117,18 @@ __global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, double2* __restrict__ 
     const int nq = (int)min((long long)FZ_TQ, Q - q0);
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
         const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
-        if (ql < nq) cp_async16(smc + ql * LD + kz, SP + q0 + ql + Q * kz);
+        if (ql < nq) {
+            if constexpr (sizeof(C) == 16) cp_async16(smc + ql * LD + kz, SP + q0 + ql + Q * kz);
+            else cp_async8(reinterpret_cast<double*>(smc + ql * LD + kz), reinterpret_cast<const double*>(SP + q0 + ql + Q * kz));
+        }
     }
     cp_async_wait_all();
-    block_fft4s<N1, N2, SIGN>(smc, nq, LD, g.twz);
-    const double sc = SIGN < 0 ? 1.0 / (double)N : 1.0;
+    block_fft4s<N1, N2, SIGN>(smc, nq, LD, twz_of<C>(g));
+    const T sc = SIGN < 0 ? (T)(1.0 / (double)N) : (T)1.0;
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
         const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
         if (ql < nq) {
-            double2 v = smc[ql * LD + kz];
+            C v = smc[ql * LD + kz];
             if (SIGN < 0) { v.x = v.x * sc; v.y = v.y * sc; }
             SP[q0 + ql + Q * kz] = v;
         }
@@ -154,8 +180,8 @@ __global__ void k_ysolve_zero_factors(Geo g, double* __restrict__ zf) {
     }
 }
 
-template <int S>
-__global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __restrict__ SP) {
+template <int S, typename C>
+__global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, C* __restrict__ SP) {
     extern __shared__ double2 smc[];
     static_assert(YW_NT % YW_L == 0, "a thread keeps one line in the staging loops");
     const int M = 32 * S, LH = g.LH;
@@ -167,9 +193,12 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __rest
     const int ls = threadIdx.x % YW_L, js = threadIdx.x / YW_L;
     const long long qs = q0 + ls;
     const int kzs = (int)(qs / LH), kxs = (int)(qs - (long long)kzs * LH);
-    double2* const gsrc = SP + kxs + (long long)LH * ((long long)M * kzs);
+    C* const gsrc = SP + kxs + (long long)LH * ((long long)M * kzs);
     if (ls < nq) {
-        for (int j = js; j < M; j += YW_NT / YW_L) cp_async16(smc + ls * LS + seg_pos<S>(j), gsrc + (long long)LH * j);
+        for (int j = js; j < M; j += YW_NT / YW_L) {
+            if constexpr (sizeof(C) == 16) cp_async16(smc + ls * LS + seg_pos<S>(j), gsrc + (long long)LH * j);
+            else smc[ls * LS + seg_pos<S>(j)] = to_d2(gsrc[(long long)LH * j]);
+        }
     }
     cp_async_wait_all();
     __syncthreads();
@@ -213,7 +242,7 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, double2* __rest
     }
     __syncthreads();
     if (ls < nq) {
-        for (int j = js; j < M; j += YW_NT / YW_L) gsrc[(long long)LH * j] = smc[ls * LS + seg_pos<S>(j)];
+        for (int j = js; j < M; j += YW_NT / YW_L) gsrc[(long long)LH * j] = from_d2<C>(smc[ls * LS + seg_pos<S>(j)]);
     }
 }
 
@@ -252,7 +281,8 @@ __global__ void k_ysolve_seq_factors(Geo g, double* __restrict__ F) {
     }
 }
 
-__global__ void __launch_bounds__(32) k_ysolve_seq(Geo g, double2* __restrict__ SP, const double* __restrict__ F) {
+template <typename C>
+__global__ void __launch_bounds__(32) k_ysolve_seq(Geo g, C* __restrict__ SP, const double* __restrict__ F) {
     extern __shared__ double2 sm2[];
     const int M = g.M, LH = g.LH, nt = blockDim.x;
     const int LS = M + 1;
@@ -263,12 +293,13 @@ __global__ void __launch_bounds__(32) k_ysolve_seq(Geo g, double2* __restrict__ 
     const long long q = (long long)blockIdx.x * nt + threadIdx.x;
     if (q >= nl) return;  // no block barrier below
     const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-    double2* s = SP + kx + (long long)LH * (long long)M * kz;
+    C* s = SP + kx + (long long)LH * (long long)M * kz;
     double2* r = sr + threadIdx.x * LS;
     double* pp = sp + threadIdx.x * LS;
     double* h = sh + threadIdx.x * LS;
     for (int j = 0; j < M; ++j) {
-        cp_async16(r + j, s + (long long)LH * j);
+        if constexpr (sizeof(C) == 16) cp_async16(r + j, s + (long long)LH * j);
+        else r[j] = to_d2(s[(long long)LH * j]);
         cp_async8(pp + j, F + (long long)j * nl + q);
         cp_async8(h + j, F + (long long)(M + j) * nl + q);
     }
@@ -286,20 +317,22 @@ __global__ void __launch_bounds__(32) k_ysolve_seq(Geo g, double2* __restrict__ 
         r[j - 1] = gp;
     }
     double2 xn = gp;
-    s[(long long)LH * (M - 1)] = xn;
+    s[(long long)LH * (M - 1)] = from_d2<C>(xn);
 #pragma unroll 4
     for (int j = M - 1; j >= 1; --j) {
         const double hj = h[j - 1];
         const double2 gj = r[j - 1];
         xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
-        s[(long long)LH * (j - 1)] = xn;
+        s[(long long)LH * (j - 1)] = from_d2<C>(xn);
     }
 }
 
 // ---------------------------------------------------------------------------
-template <int N1, int N2>
-__global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const double2* __restrict__ SP, double* __restrict__ DPH) {
-    extern __shared__ double2 smc[];
+template <int N1, int N2, typename C>
+__global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restrict__ SP, double* __restrict__ DPH) {
+    using T = typename CReal<C>::T;
+    extern __shared__ __align__(16) unsigned char smp_raw[];
+    C* smc = reinterpret_cast<C*>(smp_raw);
     const int L = g.L, M = g.M, LH = g.LH;
     const int LD = fft4s_ld(L);
     const int j0 = 1 + blockIdx.x * PX_TJ;
@@ -313,18 +346,18 @@ __global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const double2* __r
         const int ja = j0 + 2 * pair;
         const bool hasb = 2 * pair + 1 < nj;
         const int ks = kk <= L / 2 ? kk : L - kk;
-        double2 a = SP[ks + (long long)LH * ((ja - 1) + (long long)M * k)];
-        double2 b = hasb ? SP[ks + (long long)LH * ((ja) + (long long)M * k)] : make_double2(0.0, 0.0);
-        if (ks == 0 || 2 * ks == L) { a.y = 0.0; b.y = 0.0; }
+        C a = SP[ks + (long long)LH * ((ja - 1) + (long long)M * k)];
+        C b = hasb ? SP[ks + (long long)LH * ((ja) + (long long)M * k)] : mkc((T)0, (T)0);
+        if (ks == 0 || 2 * ks == L) { a.y = (T)0; b.y = (T)0; }
         if (kk > L / 2) { a.y = -a.y; b.y = -b.y; }
-        smc[pair * LD + kk] = make_double2(a.x - b.y, a.y + b.x);
+        smc[pair * LD + kk] = mkc(a.x - b.y, a.y + b.x);
     }
-    block_fft4s<N1, N2, +1>(smc, np, LD, g.twx);
+    block_fft4s<N1, N2, +1>(smc, np, LD, twx_of<C>(g));
     for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
         const int jl = p / L, i = p - jl * L;
         if (jl >= nj) continue;
-        const double2 z = smc[(jl >> 1) * LD + i];
-        DPH[pidx(g, i, j0 + jl, k)] = (jl & 1) ? z.y : z.x;
+        const C z = smc[(jl >> 1) * LD + i];
+        DPH[pidx(g, i, j0 + jl, k)] = (double)((jl & 1) ? z.y : z.x);
     }
 }
 

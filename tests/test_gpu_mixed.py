@@ -1,5 +1,6 @@
 """Mixed-precision periodic-channel step (FP32 storage and stencils / CN
-sweeps; FP64 Poisson solve, projection and bulk-flux sums) against the FP64
+sweeps, FP32 spectrum with FP32 x and z transforms; FP64 y-solve of the
+Poisson modes, divergence, projection and bulk-flux sums) against the FP64
 oracle and the FP64 GPU step.
 
 Tolerances, stated against FP64:
