@@ -311,19 +311,13 @@ cudaError_t set_smem(F* f, size_t bytes) {
 
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
 
-// lines per block of k_ysolve_seq: up to 32, a multiple of 8 that fits the shared memory
-int ysolve_seq_lines(int M) {
-    int nt = 32;
-    while (nt > 8 && smem_ysolve_seq(M, nt) > 227 * 1024) nt -= 8;
-    return nt;
-}
-
 template <typename C>
 void launch_ysolve_seq(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
-    const int nt = ysolve_seq_lines(g.M);
-    k_ysolve_seq<C><<<(int)((nl + nt - 1) / nt), nt, smem_ysolve_seq(g.M, nt), ctx->stream>>>(g, spec<C>(ctx), ctx->YF);
+    // the forward chain's FP64 intermediate: in place in an FP64 spectrum, else in the FP64 array as scratch
+    k_ysolve_seq<C><<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, smem_ysolve_seq(), ctx->stream>>>(g, spec<C>(ctx), ctx->SP,
+                                                                                           ctx->YF);
 }
 
 template <typename C>
@@ -362,7 +356,7 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq<C>, smem_ysolve_seq(g.M, ysolve_seq_lines(g.M))));
+    CK(set_smem(k_ysolve_seq<C>, smem_ysolve_seq()));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, C>, smem_fz<C>(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, C>, smem_fz<C>(g))));
     return CHAPSIM_OK;
@@ -377,7 +371,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq<double2>, smem_ysolve_seq(g.M, ysolve_seq_lines(g.M))));
+    CK(set_smem(k_ysolve_seq<double2>, smem_ysolve_seq()));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));
     if (ctx->domain == 2 && ctx->ivis) {

@@ -255,11 +255,22 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, C* __restrict__
 // once per line and keeps PP and H (2 M doubles per line, row-major over the
 // lines: PP_j of line q at F[j*nl + q], H_j at F[(M+j)*nl + q]; row 1 keeps
 // B_1 itself, which the first row divides by).  The per-substep solve is
-// then two chains of multiply-adds.  A block stages its nt consecutive lines
-// (consecutive kx: every row access is coalesced) and their factors in
-// shared memory with cp.async; the autotuner picks between this variant
-// and the warp hybrid per grid.
-inline size_t smem_ysolve_seq(int M, int nt) { return (size_t)nt * (M + 1) * (sizeof(double2) + 2 * sizeof(double)); }
+// then two chains of multiply-adds.
+//
+// There are only LH * N lines (8320 at 128^3), so the solve is one thread per
+// line, and what bounds it is the latency of its row loads.  Each thread
+// keeps a ring of YS_G * YS_NG rows in shared memory, filled by cp.async in
+// groups of YS_G rows (every row access is coalesced across the consecutive
+// kx of a warp): while the chain consumes one group, the next YS_NG - 1 are
+// in flight.  The forward chain leaves g_j in G (FP64; the spectral array
+// itself when it is FP64, the FP64 array as scratch when the spectrum is
+// FP32), which the backward chain streams back through the same ring.  No
+// thread reads another's ring slots, so there is no block barrier.  The
+// autotuner picks between this variant and the warp hybrid per grid.
+#define YS_G 8
+#define YS_NG 8
+#define YS_NT 32
+constexpr size_t smem_ysolve_seq() { return (size_t)YS_G * YS_NG * YS_NT * (sizeof(double2) + sizeof(double)); }
 
 __global__ void k_ysolve_seq_factors(Geo g, double* __restrict__ F) {
     const int M = g.M, LH = g.LH;
@@ -282,49 +293,101 @@ __global__ void k_ysolve_seq_factors(Geo g, double* __restrict__ F) {
 }
 
 template <typename C>
-__global__ void __launch_bounds__(32) k_ysolve_seq(Geo g, C* __restrict__ SP, const double* __restrict__ F) {
-    extern __shared__ double2 sm2[];
-    const int M = g.M, LH = g.LH, nt = blockDim.x;
-    const int LS = M + 1;
-    double2* sr = sm2;
-    double* sp = reinterpret_cast<double*>(sm2 + (size_t)nt * LS);
-    double* sh = sp + (size_t)nt * LS;
+__device__ __forceinline__ void cp_async_row(C* dst, const C* src) {
+    if constexpr (sizeof(C) == 16) cp_async16(dst, src);
+    else cp_async8(reinterpret_cast<double*>(dst), reinterpret_cast<const double*>(src));
+}
+
+template <typename C>
+__global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, const double* __restrict__ F) {
+    extern __shared__ __align__(16) unsigned char ys_raw[];
+    constexpr int NR = YS_G * YS_NG;
+    double2* const ringg = reinterpret_cast<double2*>(ys_raw);  // [NR][YS_NT] rows of G (backward)
+    C* const ringc = reinterpret_cast<C*>(ys_raw);              // [NR][YS_NT] rows of the spectrum (forward)
+    double* const ringf = reinterpret_cast<double*>(ys_raw + (size_t)NR * YS_NT * sizeof(double2));  // factors
+    const int M = g.M, LH = g.LH, th = threadIdx.x;
     const long long nl = (long long)LH * g.N;
-    const long long q = (long long)blockIdx.x * nt + threadIdx.x;
+    const long long q = (long long)blockIdx.x * YS_NT + th;
     if (q >= nl) return;  // no block barrier below
     const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-    C* s = SP + kx + (long long)LH * (long long)M * kz;
-    double2* r = sr + threadIdx.x * LS;
-    double* pp = sp + threadIdx.x * LS;
-    double* h = sh + threadIdx.x * LS;
-    for (int j = 0; j < M; ++j) {
-        if constexpr (sizeof(C) == 16) cp_async16(r + j, s + (long long)LH * j);
-        else r[j] = to_d2(s[(long long)LH * j]);
-        cp_async8(pp + j, F + (long long)j * nl + q);
-        cp_async8(h + j, F + (long long)(M + j) * nl + q);
+    const long long base = kx + (long long)LH * M * kz;
+    C* const s = SP + base;
+    double2* const gs = G + base;
+    const double* const PP = F + q;
+    const double* const HH = F + (long long)M * nl + q;
+    const long long rs = LH;  // row stride of the spectrum
+    // forward: g_1 = r_1 / B_1 (r_1 = 0 on the zero mode), g_t = (r_t - A_t g_{t-1}) PP_t
+    const int nb = M / YS_G;
+    auto issue_f = [&](int b) {
+        if (b < nb) {
+#pragma unroll
+            for (int u = 0; u < YS_G; ++u) {
+                const int row = b * YS_G + u, slot = (b % YS_NG) * YS_G + u;
+                cp_async_row(ringc + slot * YS_NT + th, s + rs * row);
+                cp_async8(ringf + slot * YS_NT + th, PP + (long long)row * nl);
+            }
+        }
+        cp_async_commit();  // an empty group past the end keeps the group count uniform
+    };
+#pragma unroll 1
+    for (int b = 0; b < YS_NG - 1; ++b) issue_f(b);
+    double2 gp = make_double2(0.0, 0.0);
+#pragma unroll 1
+    for (int b = 0; b < nb; ++b) {
+        issue_f(b + YS_NG - 1);
+        cp_async_wait_group<YS_NG - 1>();  // group b has landed
+#pragma unroll
+        for (int u = 0; u < YS_G; ++u) {
+            const int t = b * YS_G + u, slot = (b % YS_NG) * YS_G + u;
+            const double2 r = to_d2(ringc[slot * YS_NT + th]);
+            const double p = ringf[slot * YS_NT + th];
+            if (t == 0) {
+                const double2 r0 = q == 0 ? make_double2(0.0, 0.0) : r;
+                gp = make_double2(r0.x / p, r0.y / p);
+            } else {
+                const double a = g.amph[t + 1];
+                gp = make_double2((r.x - a * gp.x) * p, (r.y - a * gp.y) * p);
+            }
+            if (t < M - 1) gs[rs * t] = gp;
+        }
     }
-    cp_async_wait_all();
-    double2 r0 = r[0];
-    if (q == 0) r0 = make_double2(0.0, 0.0);
-    const double b = pp[0];
-    double2 gp = make_double2(r0.x / b, r0.y / b);
-    r[0] = gp;
-#pragma unroll 4
-    for (int j = 2; j <= M; ++j) {
-        const double a = g.amph[j], p = pp[j - 1];
-        const double2 rj = r[j - 1];
-        gp = make_double2((rj.x - a * gp.x) * p, (rj.y - a * gp.y) * p);
-        r[j - 1] = gp;
-    }
+    cp_async_wait_group<0>();
+    __threadfence();  // the G rows written above, before the cp.async reads below
+    // backward: x_M = g_M, x_t = g_t - H_t x_{t+1}, t = M-1 .. 1 (rows t-1 = M-2 .. 0)
     double2 xn = gp;
-    s[(long long)LH * (M - 1)] = from_d2<C>(xn);
-#pragma unroll 4
-    for (int j = M - 1; j >= 1; --j) {
-        const double hj = h[j - 1];
-        const double2 gj = r[j - 1];
-        xn = make_double2(gj.x - hj * xn.x, gj.y - hj * xn.y);
-        s[(long long)LH * (j - 1)] = from_d2<C>(xn);
+    s[rs * (M - 1)] = from_d2<C>(xn);
+    const int nbb = (M - 1 + YS_G - 1) / YS_G;
+    auto issue_b = [&](int b) {
+        if (b < nbb) {
+#pragma unroll
+            for (int u = 0; u < YS_G; ++u) {
+                const int t = M - 2 - b * YS_G - u, slot = (b % YS_NG) * YS_G + u;
+                if (t >= 0) {
+                    cp_async16(ringg + slot * YS_NT + th, gs + rs * t);
+                    cp_async8(ringf + slot * YS_NT + th, HH + (long long)t * nl);
+                }
+            }
+        }
+        cp_async_commit();
+    };
+#pragma unroll 1
+    for (int b = 0; b < YS_NG - 1; ++b) issue_b(b);
+#pragma unroll 1
+    for (int b = 0; b < nbb; ++b) {
+        issue_b(b + YS_NG - 1);
+        cp_async_wait_group<YS_NG - 1>();
+#pragma unroll
+        for (int u = 0; u < YS_G; ++u) {
+            const int t = M - 2 - b * YS_G - u, slot = (b % YS_NG) * YS_G + u;
+            if (t >= 0) {
+                const double2 gt = ringg[slot * YS_NT + th];
+                const double h = ringf[slot * YS_NT + th];
+                xn = make_double2(gt.x - h * xn.x, gt.y - h * xn.y);
+                s[rs * t] = from_d2<C>(xn);
+            }
+        }
     }
+    cp_async_wait_group<0>();
 }
 
 // ---------------------------------------------------------------------------
