@@ -19,6 +19,7 @@
 #include "io_cn.cuh"
 #include "stats.cuh"
 #include "rhs_bulk.cuh"
+#include "plane_fft.cuh"
 #include "thermo.cuh"
 #include "thermal.cuh"
 #include "mlp.cuh"
@@ -143,6 +144,7 @@ struct chapsim_ctx {
     double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
+    int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     double2* SP = nullptr;
     float2* SPf = nullptr;       // FP32 spectral array of the mixed-precision step
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
@@ -245,6 +247,11 @@ size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(C
 template <typename C> C* spec(chapsim_ctx* c);
 template <> double2* spec<double2>(chapsim_ctx* c) { return c->SP; }
 template <> float2* spec<float2>(chapsim_ctx* c) { return c->SPf; }
+// fused plane transforms: built for the shape, and the plane fits one block's shared memory
+template <typename C>
+size_t smem_p2(const Geo& g) { return (size_t)plane_fft_words(g.L, g.N) * sizeof(C); }
+template <typename C>
+bool plane_fft_ok(const Geo& g) { return plane_fft_shape(g.L, g.N) && smem_p2<C>(g) <= 220 * 1024; }
 
 // twiddles of the small DFTs inside the four-step FFT (constant memory, shared by all contexts)
 cudaError_t upload_small_twiddles() {
@@ -293,6 +300,19 @@ cudaError_t set_smem(F* f, size_t bytes) {
     e = cudaFuncGetAttributes(&fa, f);
     if (e != cudaSuccess) return e;
     const int limit = optin - (int)fa.sharedSizeBytes;  // dynamic + static must fit the opt-in size
+    if ((int)bytes > limit) return cudaErrorInvalidValue;
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+}
+
+cudaError_t set_smem_void(const void* f, size_t bytes) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa{};
+    e = cudaFuncGetAttributes(&fa, f);
+    if (e != cudaSuccess) return e;
+    const int limit = optin - (int)fa.sharedSizeBytes;
     if ((int)bytes > limit) return cudaErrorInvalidValue;
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
 }
@@ -357,6 +377,8 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
     CK(set_smem(k_ysolve_seq<C>, smem_ysolve_seq()));
+    if (ctx->domain == 1 && plane_fft_ok<C>(g))
+        P2_DISPATCH(g.L, g.N, CK((plane_fft_attrs<R, XN1, XN2, ZN1, ZN2>(set_smem_void, smem_p2<C>(g)))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, C>, smem_fz<C>(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, C>, smem_fz<C>(g))));
     return CHAPSIM_OK;
@@ -438,6 +460,43 @@ void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns
     }
 }
 
+// DIVG_tg + FFT99_POIS3D_periodicxz up to DPH: chained transforms, or the
+// fused plane transforms (one block per y row) where chosen.  Both record the
+// same profiling slots (the fused form leaves the two z-transform slots empty).
+template <typename R>
+void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    using C = SpecT<R>;
+    C* sp = spec<C>(ctx);
+    if (ctx->plane_kind == 1) {
+        P2_DISPATCH(g.L, g.N, (plane_fft_fwd<R, XN1, XN2, ZN1, ZN2>(g, f.Q, f.RHSLL, sp, ctx->st, ns, smem_p2<C>(g), s)));
+        prof_mark(ctx);
+        prof_mark(ctx);
+        launch_ysolve<C>(ctx);
+        prof_mark(ctx);
+        prof_mark(ctx);
+        P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(g, sp, ctx->DPH, smem_p2<C>(g), s)));
+        prof_mark(ctx);
+        ctx->launches += 3;
+        return;
+    }
+    dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
+    DISPATCH_FFT(g.L, (k_div_fftx<R, FN1, FN2><<<grp, PX_NT, smem_px<C>(g), s>>>(g, f.Q, f.RHSLL, sp, ctx->st, ns)));
+    prof_mark(ctx);
+    const long long nq = (long long)g.LH * g.M;
+    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
+    prof_mark(ctx);
+    launch_ysolve<C>(ctx);
+    prof_mark(ctx);
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
+    prof_mark(ctx);
+    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, C><<<grp, PX_NT, smem_px<C>(g), s>>>(g, sp, ctx->DPH)));
+    prof_mark(ctx);
+    ctx->launches += 5;
+}
+
 template <typename R>
 void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     const Geo& g = ctx->g;
@@ -458,25 +517,11 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     dim3 gry(g.L / 32, g.N);
     DISPATCH_S(g.M / 32, (k_ysweep<S, R><<<gry, SWEEP_NT, smem_y<R>(g), s>>>(g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
-    using C = SpecT<R>;
-    C* sp = spec<C>(ctx);
-    dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    DISPATCH_FFT(g.L, (k_div_fftx<R, FN1, FN2><<<grp, PX_NT, smem_px<C>(g), s>>>(g, f.Q, f.RHSLL, sp, ctx->st, ns)));
-    prof_mark(ctx);
-    const long long nq = (long long)g.LH * g.M;
-    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
-    prof_mark(ctx);
-    launch_ysolve<C>(ctx);
-    prof_mark(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
-    prof_mark(ctx);
-    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, C><<<grp, PX_NT, smem_px<C>(g), s>>>(g, sp, ctx->DPH)));
-    prof_mark(ctx);
+    launch_pressure<R>(ctx, f, ns);
     const long long tot = (long long)g.L * g.M * g.N;
     k_correct<R><<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
     prof_mark(ctx);
-    ctx->launches += 9;
+    ctx->launches += 4;
 }
 void launch_substep(chapsim_ctx* ctx, int ns, bool factors = true) {
     if (ctx->prec == CHAPSIM_PREC_MIXED) launch_substep_t<float>(ctx, ns, factors);
@@ -1892,14 +1937,41 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             if (tk[kind] < tk[best]) best = kind;
         ctx->k1_kind = force >= 0 ? std::min((force >> 1) & 3, bulk_fits ? 2 : 1) : best;
     }
+    // pressure stage up to DPH: chained x/z transforms or the fused plane
+    // transforms (periodic channel, planes that fit one block).  It writes
+    // only scratch (RHSLLPHI, the spectrum, DPH), which every substep rewrites.
+    float tp[2] = {0.f, 1e30f};
+    if (ctx->domain == 1) {
+        const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
+        const bool p2 = mixed ? plane_fft_ok<float2>(g) : plane_fft_ok<double2>(g);
+        for (int kind = 0; kind < (p2 ? 2 : 1); ++kind) {
+            ctx->plane_kind = kind;
+            auto one = [&]() {
+                if (mixed) launch_pressure<float>(ctx, step_fields<float>(ctx), 1);
+                else launch_pressure<double>(ctx, step_fields<double>(ctx), 1);
+            };
+            one();
+            CK(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; ++r) one();
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&tp[kind], e0, e1));
+            tp[kind] /= reps;
+        }
+        CK(cudaGetLastError());
+        ctx->plane_kind = force >= 0 ? (p2 ? (force >> 3) & 1 : 0) : (p2 && tp[1] < tp[0] ? 1 : 0);
+    }
     if (ctx->step_exec) {
         cudaGraphExecDestroy(ctx->step_exec);
         ctx->step_exec = nullptr;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (choice) *choice = ctx->ysolve_kind | (ctx->k1_kind << 1);
-    if (ms) { ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2]; }
+    if (choice) *choice = ctx->ysolve_kind | (ctx->k1_kind << 1) | (ctx->plane_kind << 3);
+    if (ms) {
+        ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
+        ms[5] = tp[0]; ms[6] = tp[1];
+    }
     return CHAPSIM_OK;
 }
 

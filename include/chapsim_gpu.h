@@ -330,16 +330,22 @@ int chapsim_upload_pp_means_tg(chapsim_ctx_t* ctx, int32_t nstatis, const double
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the fastest of each group (force = -1), or the ones forced (force = 0..5):
+ * the fastest of each group (force = -1), or the ones forced (force = 0..13):
  *   bit 0: Poisson y-solve, 0 = warp Thomas/PCR hybrid, 1 = the reference's
  *          sequential Thomas recurrence, one thread per mode;
  *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
  *          0 = fused (one warp per x line, per-thread loads), 1 = split into
  *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
- *          stencil rows staged in shared memory by bulk copies.
- * choice receives the kept setting in the same bit form; ms[5] (may be NULL)
- * the mean durations of y-solve (hybrid, sequential) and right-hand sides
- * (fused, split, bulk-staged).  CONVH0 is restored after the trial launches. */
+ *          stencil rows staged in shared memory by bulk copies;
+ *   bit 3: pressure stage (periodic channel only), 0 = chained x and z
+ *          transforms, 1 = fused plane transforms, one block per y row (only
+ *          where the row's half spectrum fits one block's shared memory;
+ *          otherwise 0 is kept whatever is forced).
+ * choice receives the kept setting in the same bit form; ms[7] (may be NULL)
+ * the mean durations of y-solve (hybrid, sequential), right-hand sides
+ * (fused, split, bulk-staged) and pressure stage up to DPH (chained, fused;
+ * 1e30 where a variant does not apply).  CONVH0 is restored after the trial
+ * launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 
 /* An ensemble of independent periodic channels (any grids and precisions, one

@@ -3,8 +3,8 @@
 * Both Poisson y-solve variants (warp Thomas/PCR hybrid, sequential Thomas)
   and the three forms of the right-hand-side / x-sweep stage (fused, split,
   fused with bulk-copy staging) solve the FFT99 problem to 1e-12 of the
-  oracle, and the step with any combination stays within 1e-11 after 10
-  steps.  The bulk-staged form computes the same per-point arithmetic as the
+  oracle, and the step with any combination, with chained or fused plane
+  transforms, stays within 1e-11 after 10 steps.  The bulk-staged form computes the same per-point arithmetic as the
   fused one (only the bulk-flux sum is added in another order), checked at
   other line lengths and in mixed precision.
 * An ensemble (one graph per step, one branch per member) advances every
@@ -27,7 +27,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5, 8, 9, 12, 13])
 def test_ysolve_variants_match_oracle(kind):
     L, M, N = 96, 64, 64
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
@@ -81,6 +81,46 @@ def test_bulk_staged_rhs_matches_fused(shape, precision, tol):
     for i in range(3):
         e = rel(out[1][i][:, 1:M + 1], out[0][i][:, 1:M + 1])
         assert e <= tol, (i, e)
+
+
+@pytest.mark.parametrize("shape,precision,tol", [((128, 128, 128), "fp64", 1e-12), ((64, 64, 64), "fp64", 1e-12),
+                                                 ((192, 32, 128), "fp64", 1e-12), ((96, 64, 192), "fp64", 1e-12),
+                                                 ((128, 64, 192), "mixed", 1e-5), ((192, 32, 192), "mixed", 1e-5)])
+def test_plane_transforms_match_chained(shape, precision, tol):
+    """The fused plane transforms (one block per y row: divergence, x and z
+    transforms, and their inverses) advance the channel as the chained
+    transforms do, to round-off (only the pairing of real lines differs)."""
+    L, M, N = shape
+    s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    Q, PR = initial_field(s, 91, 0.1)
+    out = []
+    for kind in (0, 8):
+        c = gpu.ChannelTG(s, precision=precision)
+        choice, ms = c.autotune(force=kind)
+        assert choice == kind and ms["pressure_plane"] < 1e29
+        c.upload(Q, PR)
+        c.set_dt(2e-3)
+        c.SOLVERRK3_MOM_tg(0)
+        c.advance(5, 2e-3, 1e-6, 0.5)
+        out.append(c.download())
+        c.close()
+    for i in range(3):
+        e = rel(out[1][0][i][:, 1:M + 1], out[0][0][i][:, 1:M + 1])
+        assert e <= tol, (i, e)
+    pa = out[1][1][:, 1:M + 1] - out[1][1][:, 1:M + 1].mean()
+    pb = out[0][1][:, 1:M + 1] - out[0][1][:, 1:M + 1].mean()
+    assert rel(pa, pb) <= (1e-11 if precision == "fp64" else 1e-3)
+
+
+def test_plane_transforms_refused_where_the_plane_does_not_fit():
+    """A 192 x 192 FP64 plane (97 z lines of 205 complex words, 318 KB)
+    exceeds one block's shared memory: forcing bit 3 keeps the chained
+    transforms (in mixed precision the same plane, 159 KB, fits)."""
+    s = channel_setup(192, 32, 192, 2 * math.pi, math.pi, 2.0, 2800.0)
+    c = gpu.ChannelTG(s)
+    choice, ms = c.autotune(force=8)
+    assert choice == 0 and ms["pressure_plane"] >= 1e29
+    c.close()
 
 
 GRIDS = [(64, 64, 64, 2 * math.pi, math.pi, 2800.0), (96, 64, 96, 2 * math.pi, math.pi, 4000.0),
