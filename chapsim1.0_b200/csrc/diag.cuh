@@ -18,18 +18,28 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, d
                                                DevState* __restrict__ st) {
     __shared__ double sred[32];
     const int L = g.L, M = g.M, N = g.N;
-    const long long tot = (long long)L * M * N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nlines = M * N;
     double mx = 0.0;
     bool bad = false;
-    for (long long t = (long long)blockIdx.x * DG_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * DG_NT) {
-        int i, j, k;
-        io_decode(g, t, i, j, k);
-        const long long c = pidx(g, i, j, k);
-        const double q = (fabs(((double)Q[c] + (double)Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
-                          fabs(((double)Q[c + g.FS] + (double)Q[c + g.FS + g.L]) * g.dyfi[j] * 1.0) +
-                          fabs(((double)Q[c + 2 * g.FS] + (double)Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
-        if (!(q == q)) bad = true;
-        mx = fmax(mx, q);
+    // one warp per x line (j, k): the line's indices are decoded once and every load is contiguous
+    for (int line = blockIdx.x * (DG_NT / 32) + warp; line < nlines; line += gridDim.x * (DG_NT / 32)) {
+        const int j = 1 + line % M, k = line / M;
+        const long long c0 = pidx(g, 0, j, k);
+        const R* U = Q + c0;
+        const R* V = Q + g.FS + c0;
+        const R* W = Q + 2 * g.FS + c0;
+        const R* Wkp = Q + 2 * g.FS + pidx(g, 0, j, wrapp(k, N));
+        const double cy = g.dyfi[j];
+#pragma unroll 4
+        for (int i = lane; i < L; i += 32) {
+            const int ip = i + 1 == L ? 0 : i + 1;
+            const double q = (fabs(((double)U[i] + (double)U[ip]) * g.dxi) +
+                              fabs(((double)V[i] + (double)V[i + L]) * cy * 1.0) +
+                              fabs(((double)W[i] + (double)Wkp[i]) * g.dzi * 1.0)) * 0.5;
+            if (!(q == q)) bad = true;
+            mx = fmax(mx, q);
+        }
     }
     if (bad) atomicOr(&st->err, CHS_EBIT_NAN);
     if (blockIdx.x == 0 && threadIdx.x == 0) st->dtprev = st->dt;
@@ -106,8 +116,18 @@ template <typename T>
 __global__ void __launch_bounds__(32) k_dt_factors(Geo g, const double* __restrict__ partial, int np,
                                                    DevState* __restrict__ st, T* __restrict__ fac) {
     const int lane = threadIdx.x;
-    double mx = 0.0;
-    for (int t = lane; t < np; t += 32) mx = fmax(mx, partial[t]);
+    // four independent maxima, so that the partials' loads are in flight together
+    double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+    int t = lane;
+#pragma unroll 2
+    for (; t + 96 < np; t += 128) {
+        m0 = fmax(m0, partial[t]);
+        m1 = fmax(m1, partial[t + 32]);
+        m2 = fmax(m2, partial[t + 64]);
+        m3 = fmax(m3, partial[t + 96]);
+    }
+    for (; t < np; t += 32) m0 = fmax(m0, partial[t]);
+    double mx = fmax(fmax(m0, m1), fmax(m2, m3));
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
     const double c = mx;
     double dt = fmin(fmin(st->dt0, 5.0 * st->dtprev), st->cflgv / c);

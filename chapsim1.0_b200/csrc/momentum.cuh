@@ -231,9 +231,7 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
     __syncwarp();
     // cyclic x sweeps of this warp's three lines (MOMFA1_X_tg starts at N2I = 2 for v)
     const R* fx = fac + FSET_X * FAC_SET;
-#pragma unroll 1
-    for (int c = 0; c < 3; ++c)
-        if (c != 1 || j >= 2) warp_tdma_apply_smem<S, true>(sl + c * LS, fx, lane);
+    warp_tdma_apply_smem3<S, true>(sl, LS, j >= 2, fx, lane);  // the three components together
     __syncwarp();
 #pragma unroll
     for (int kk = 0; kk < S; ++kk) {
@@ -315,8 +313,22 @@ __global__ void __launch_bounds__(SWEEP_NT, 2) k_zsweep(Geo g, R* __restrict__ R
         cp_async_commit();
         cp_async_wait_group<1>();
         __syncthreads();
+        // lines up to 128: two per pass (il, il + 8), their chains interleaved and the factor
+        // loads shared (longer lines would spill)
+        constexpr int NRZ = S <= 4 ? 2 : 1;
 #pragma unroll 1
-        for (int il = warp; il < 32; il += SWEEP_NT / 32) warp_tdma_apply_smem<S, true>(cur + il * LS, fz, lane);
+        for (int il = warp; il < 32; il += NRZ * (SWEEP_NT / 32)) {
+            R d[NRZ][S];
+#pragma unroll
+            for (int r = 0; r < NRZ; ++r)
+#pragma unroll
+                for (int q = 0; q < S; ++q) d[r][q] = cur[(il + r * (SWEEP_NT / 32)) * LS + lane * (S + 1) + q];
+            warp_tdma_apply_n<S, true, NRZ>(d, fz, lane);
+#pragma unroll
+            for (int r = 0; r < NRZ; ++r)
+#pragma unroll
+                for (int q = 0; q < S; ++q) cur[(il + r * (SWEEP_NT / 32)) * LS + lane * (S + 1) + q] = d[r][q];
+        }
         __syncthreads();
         R* Rz = tile_base(t);
 #pragma unroll 4

@@ -199,9 +199,7 @@ __global__ void __launch_bounds__(RB_WMAX * 32, 1) k_rhs_xsweep_bulk(Geo g, cons
             pending = true;
         }
         // cyclic x sweeps of this line's three components (MOMFA1_X_tg starts at N2I = 2 for v)
-#pragma unroll 1
-        for (int c = 0; c < 3; ++c)
-            if (c != 1 || j >= 2) warp_tdma_apply_smem<S, true>(sl + c * LS, fx, lane);
+        warp_tdma_apply_smem3<S, true>(sl, LS, j >= 2, fx, lane);  // the three components together
         __syncwarp();
         R* Rl = RHS + iidx(g, 0, j, k);
 #pragma unroll

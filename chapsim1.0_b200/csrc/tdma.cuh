@@ -369,6 +369,125 @@ __device__ __forceinline__ void warp_tdma_apply(R (&d)[S], const R* __restrict__
     }
 }
 
+// warp_tdma_apply for NR right-hand sides that share one factor table (the
+// three components of an x line, or several lines of one z or y sweep): each
+// factor is loaded once and the NR dependency chains interleave, which is
+// what the latency-bound sweeps need.  Per right-hand side the arithmetic is
+// exactly that of warp_tdma_apply.
+template <int S, bool CYCLIC, int NR, typename R>
+__device__ __forceinline__ void warp_tdma_apply_n(R (&d)[NR][S], const R* __restrict__ fac, int lane) {
+    const R* f = fac + lane;
+    const int b = 5 * S;
+    R D0[NR], D1[NR];
+    if constexpr (S >= 3) {
+        const R f01 = f[(0 * S + 1) * 32];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) d[r][1] *= f01;
+#pragma unroll
+        for (int k = 2; k <= S - 2; ++k) {
+            const R fa = f[(1 * S + k) * 32], fr = f[(0 * S + k) * 32];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) d[r][k] = (d[r][k] - fa * d[r][k - 1]) * fr;
+        }
+#pragma unroll
+        for (int k = S - 3; k >= 1; --k) {
+            const R fc = f[(2 * S + k) * 32];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) d[r][k] = d[r][k] - fc * d[r][k + 1];
+        }
+        const R g0 = f[(b + 0) * 32], g1 = f[(b + 1) * 32];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            D0[r] = d[r][0] - g0 * d[r][1];
+            D1[r] = d[r][S - 1] - g1 * d[r][S - 2];
+        }
+    } else if constexpr (S == 2) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) { D0[r] = d[r][0]; D1[r] = d[r][1]; }
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) { D0[r] = d[r][0]; D1[r] = R(0); }
+    }
+    R de[NR];
+    if constexpr (S == 1) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) de[r] = D0[r];
+    } else {
+        const R f5 = f[(b + 5) * 32], f6 = f[(b + 6) * 32];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const R D0n = __shfl_sync(0xffffffffu, D0[r], (lane + 1) & 31);
+            de[r] = D1[r] - f5 * D0[r] - f6 * D0n;
+        }
+    }
+    const int nsteps = CYCLIC ? 4 : 5;
+#pragma unroll
+    for (int st = 0; st < 5; ++st) {
+        if (st >= nsteps) break;
+        const int s = 1 << st;
+        const R k1 = f[(b + 7 + st) * 32], k2 = f[(b + 12 + st) * 32];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const R lo = __shfl_sync(0xffffffffu, de[r], (lane - s) & 31);
+            const R hi = __shfl_sync(0xffffffffu, de[r], (lane + s) & 31);
+            de[r] = de[r] - k1 * lo - k2 * hi;
+        }
+    }
+    R u[NR];
+    const R f17 = f[(b + 17) * 32];
+    if constexpr (CYCLIC) {
+        const R f18 = f[(b + 18) * 32];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const R pd = __shfl_sync(0xffffffffu, de[r], lane ^ 16);
+            u[r] = de[r] * f17 + pd * f18;
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) u[r] = de[r] * f17;
+    }
+    if constexpr (S == 1) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) d[r][0] = u[r];
+    } else {
+        const R f2 = f[(b + 2) * 32], f3 = f[(b + 3) * 32], f4 = f[(b + 4) * 32];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            const R up = __shfl_sync(0xffffffffu, u[r], (lane - 1) & 31);
+            const R y0 = (D0[r] - f2 * up - f3 * u[r]) * f4;
+            d[r][0] = y0;
+            d[r][S - 1] = u[r];
+        }
+        if constexpr (S > 2) {
+#pragma unroll
+            for (int k = 1; k <= S - 2; ++k) {
+                const R fy0 = f[(3 * S + k) * 32], fu = f[(4 * S + k) * 32];
+#pragma unroll
+                for (int r = 0; r < NR; ++r) d[r][k] = d[r][k] - fy0 * d[r][0] - fu * u[r];
+            }
+        }
+    }
+}
+
+// The three x lines of one (j, k) in segment-padded shared memory at base,
+// base + ls, base + 2 ls; line 1 (v) is solved but written back only when
+// keep1 (MOMFA1_X_tg starts at N2I = 2 for v).
+template <int S, bool CYCLIC, typename R>
+__device__ __forceinline__ void warp_tdma_apply_smem3(R* base, int ls, bool keep1, const R* __restrict__ fac, int lane) {
+    R d[3][S];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int k = 0; k < S; ++k) d[c][k] = base[c * ls + lane * (S + 1) + k];
+    warp_tdma_apply_n<S, CYCLIC, 3>(d, fac, lane);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (c == 1 && !keep1) continue;
+#pragma unroll
+        for (int k = 0; k < S; ++k) base[c * ls + lane * (S + 1) + k] = d[c][k];
+    }
+}
+
 template <int S, bool CYCLIC, typename R>
 __device__ __forceinline__ void warp_tdma_apply_smem(R* base, const R* __restrict__ fac, int lane) {
     R d[S];
