@@ -37,7 +37,8 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_mlp_gradients", "chapsim_mlp_train", "chapsim_mlp_infer_points", "chapsim_thermal_use_mlp",
             "chapsim_mlp_judge", "chapsim_autotune", "chapsim_batch_create", "chapsim_batch_advance",
             "chapsim_batch_get_stream", "chapsim_batch_destroy", "chapsim_pp_mean_zx_tg", "chapsim_pp_mean_t_tg",
-            "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io"]
+            "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
+            "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
 PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
@@ -131,6 +132,12 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_mlp_judge.argtypes = [vp, _dp]
     L.chapsim_autotune.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_float)]
     L.chapsim_divgck_io.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+    i32 = ctypes.c_int32
+    L.chapsim_write_dfile.argtypes = [ctypes.c_char_p, i32, i32, i32, i32, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, _dp]
+    L.chapsim_read_dfile.argtypes = [ctypes.c_char_p, ctypes.POINTER(i32), _dp, _dp, ctypes.c_int64]
+    L.chapsim_dump_begin.argtypes = [vp]
+    L.chapsim_dump_write.argtypes = [vp, ctypes.c_char_p, i32, ctypes.c_double, ctypes.c_double, _dp]
     L.chapsim_pp_mean_zx_tg.argtypes = [vp]
     L.chapsim_pp_mean_t_tg.argtypes = [vp, ctypes.c_int32, ctypes.c_int32]
     L.chapsim_pp_monitor_tg.argtypes = [vp, ctypes.c_double, _dp]
@@ -172,6 +179,37 @@ def _check_global(rc):
     if rc != 0:
         lib = load_library()
         raise ChapsimError(rc, lib.chapsim_last_error_string(None).decode())
+
+
+DUMP_FLOW = ["U", "V", "W", "P"]
+DUMP_THERMAL = ["T", "D", "H", "M", "K"]   # TEMPERATURE, DENSITY, ENTHALPY, Viscousity, THERMCONDT
+DFILE_PREFIX = "DNS_perixz_INSTANT_T"
+
+
+def es15_9(t):
+    """PhyTIME as the reference's file names print it (Fortran ES15.9)."""
+    return "%.9E" % float(t)
+
+
+def write_dfile(path, field_nml, iterg, time, ren, dt):
+    """Native .D writer (WRT_INSTANT_VARS_*): field given (N, M, L) C-order, i.e. Fortran (L, M, N)."""
+    f = np.ascontiguousarray(field_nml, np.float64)
+    N, M, L = f.shape
+    _check_global(load_library().chapsim_write_dfile(str(path).encode(), L, M, N, int(iterg), float(time),
+                                                     float(ren), float(dt), _ptr(f)))
+
+
+def read_dfile(path):
+    """Native .D reader: returns (field (N, M, L), header dict)."""
+    lib = load_library()
+    dims = (ctypes.c_int32 * 4)()
+    reals = np.zeros(3)
+    _check_global(lib.chapsim_read_dfile(str(path).encode(), dims, _ptr(reals), None, 0))
+    L, M, N, it = list(dims)
+    f = np.empty((N, M, L))
+    _check_global(lib.chapsim_read_dfile(str(path).encode(), dims, _ptr(reals), _ptr(f), f.size))
+    return f, {"L": L, "M": M, "N": N, "ITERG": it, "time": float(reals[0]), "REN": float(reals[1]),
+               "DT": float(reals[2])}
 
 
 def tdmaiji_cyc(A, B, C, R):
@@ -383,6 +421,46 @@ class ChannelTG:
         v = ctypes.c_void_p()
         self._check(self.lib.chapsim_get_stream(self.h, ctypes.byref(v)))
         return v.value or 0
+
+    def dump_begin(self):
+        """Snapshot U, V, W, P (and the thermal fields) now; the copy to the host
+        overlaps the steps launched next (chapsim_dump_begin)."""
+        self._check(self.lib.chapsim_dump_begin(self.h))
+
+    def dump_write(self, path_prefix, iterg, time, ren):
+        """Writes the snapshot as .D files <path_prefix><time ES15.9>_X.D; returns the
+        snapshot's dt (chapsim_dump_write)."""
+        dt = ctypes.c_double()
+        self._check(self.lib.chapsim_dump_write(self.h, str(path_prefix).encode(), int(iterg), float(time),
+                                                float(ren), ctypes.byref(dt)))
+        return dt.value
+
+    def WRT_INSTANT_VARS(self, file_path, iterg, time, ren, prefix=DFILE_PREFIX):
+        """WRT_INSTANT_VARS_TG / _FLOW_IO (+ _THERMAL_IO): dump and write now; returns the file stem."""
+        self.dump_begin()
+        self.dump_write(str(file_path) + prefix, iterg, time, ren)
+        return str(file_path) + prefix + es15_9(time)
+
+    def restart_from_dfiles(self, stem):
+        """ReStart_INSTANT_VARS_TG: reads <stem>_U.D, _V.D, _W.D, _P.D, uploads the
+        fields (ghost planes zero, then the wall conditions of the upload) and the
+        files' DT; returns the header of the U file."""
+        M = self.M
+        Q = np.zeros((3,) + self.field_shape())
+        PR = np.zeros(self.field_shape())
+        hdr = None
+        for c, x in enumerate(DUMP_FLOW):
+            f, h = read_dfile(f"{stem}_{x}.D")
+            if (h["L"], h["M"], h["N"]) != (self.L, self.M, self.N):
+                raise ValueError(f"{stem}_{x}.D: grid {h['L']}x{h['M']}x{h['N']} is not this context's")
+            if c < 3:
+                Q[c, :, 1:M + 1, :] = f
+            else:
+                PR[:, 1:M + 1, :] = f
+            hdr = hdr or h
+        self.upload(Q, PR)
+        self.set_dt(hdr["DT"])
+        return hdr
 
     def DIVGCK_tg(self):
         v = ctypes.c_double()

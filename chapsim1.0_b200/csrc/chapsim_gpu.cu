@@ -195,6 +195,14 @@ struct chapsim_ctx {
     MlpNorm mlp_norm{};
     bool mlp_ready = false, use_mlp = false;
     unsigned int* mlp_judge = nullptr;
+    // asynchronous field dumps (chapsim_dump_begin / chapsim_dump_write)
+    double* dump_dev = nullptr;   // packed interiors of the dumped fields, then dt
+    double* dump_host = nullptr;  // pinned copy of dump_dev
+    size_t dump_words = 0;
+    int dump_nf = 0;
+    bool dump_pending = false;
+    cudaStream_t dump_stream = nullptr;
+    cudaEvent_t dump_snap = nullptr, dump_done = nullptr;
     std::string err;
 };
 
@@ -906,6 +914,12 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->tf.HCP); cudaFree(ctx->tf.RHSE0); cudaFree(ctx->tf.G0); cudaFree(ctx->tf.DRHO);
     cudaFree(ctx->Qf); cudaFree(ctx->PRf); cudaFree(ctx->H0f); cudaFree(ctx->RHSf); cudaFree(ctx->RHSLLf); cudaFree(ctx->facf);
     if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    if (ctx->dump_stream) cudaStreamSynchronize(ctx->dump_stream);
+    cudaFree(ctx->dump_dev);
+    if (ctx->dump_host) cudaFreeHost(ctx->dump_host);
+    if (ctx->dump_snap) cudaEventDestroy(ctx->dump_snap);
+    if (ctx->dump_done) cudaEventDestroy(ctx->dump_done);
+    if (ctx->dump_stream) cudaStreamDestroy(ctx->dump_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -2192,3 +2206,5 @@ extern "C" int chapsim_tdma_lines_noalloc(const double* a, const double* b, cons
                                                   " lines have a non-finite solution");
     return CHAPSIM_OK;
 }
+
+#include "field_dump.cuh"

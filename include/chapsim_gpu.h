@@ -327,6 +327,29 @@ int chapsim_upload_pp_means_tg(chapsim_ctx_t* ctx, int32_t nstatis, const double
                                const double* u2, const double* u3, const double* dvdl1, const double* dvdlp,
                                const double* dvdl2);
 
+/* ---- Field files (.D) and asynchronous dumps ----
+ * Replace WRT_INSTANT_VARS_TG (src/processing/WRT_VARS_TG.f90:13-100),
+ * WRT_INSTANT_VARS_FLOW_IO / _THERMAL_IO (src/processing/WRT_VARS_IO.f90:24-227)
+ * and the readers of ReStart_INSTANT_VARS_TG (src/processing/RESTART_tg.f90:11-56).
+ * A .D file: int32[4] {NCL1, NCL2, NCL3, ITERG}, float64[3] {PhyTIME, REN, DT},
+ * then float64 (NCL1, NCL2, NCL3) in Fortran order, no ghost planes. */
+int chapsim_write_dfile(const char* path, int32_t L, int32_t M, int32_t N, int32_t iterg, double time, double ren,
+                        double dt, const double* field);
+/* dims4 = {L, M, N, ITERG}, reals3 = {PhyTIME, REN, DT}; field (capacity in
+ * doubles) may be NULL to read the header only.  A payload whose size does not
+ * match the header is CHAPSIM_ERR_BADARG. */
+int chapsim_read_dfile(const char* path, int32_t* dims4, double* reals3, double* field, int64_t capacity);
+/* Snapshot U, V, W, P (and T, D, H, M, K with the thermal solver) and the
+ * device dt in stream order, then copy the snapshot to pinned host memory on
+ * a stream of the context's own, overlapping the steps launched next. */
+int chapsim_dump_begin(chapsim_ctx_t* ctx);
+/* Waits for the dump's copy and writes <path_prefix><PhyTIME as ES15.9>_U.D,
+ * _V.D, _W.D, _P.D (and _T.D, _D.D, _H.D, _M.D, _K.D); the DT in the headers
+ * is the device dt at the snapshot, returned in dt_out (may be NULL).  The
+ * reference's prefix is <FilePath1>DNS_perixz_INSTANT_T. */
+int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iterg, double time, double ren,
+                       double* dt_out);
+
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
