@@ -592,7 +592,7 @@ def run_b200(args):
     DTMIN = 1e-6
     s = channel_setup(L, M, N, HX, HZ, STR2, REN)
     Q0, PR0 = initial_field(s, replica_seed(rank), 0.1)
-    ch = gpu.ChannelTG(s, device=local, precision=args.precision)
+    ch = gpu.ChannelTG(s, device=local, precision=args.precision, pdl=not args.no_pdl)
     ch.upload(Q0, PR0)
     ch.set_dt(DT0)
     ch.SOLVERRK3_MOM_tg(0)
@@ -664,6 +664,7 @@ def run_b200(args):
         "config": {"workload": wl, "grid": [L, M, N], "domain": "4pi x 2 x 4pi/3" if L == 128 else None,
                    "REN": REN, "STR2": STR2, "CFLGV": CFLGV, "precision": args.precision,
                    "parallelism": "replicas" if ws > 1 else "single", "cuda_graph": True,
+                   "programmatic_dependent_launch": not args.no_pdl,
                    "l2": "no flush: per-step working set %.0f MB > 126 MB L2" % (
                        (12 * 8 * (M + 2) * L * N + 4 * 8 * L * M * N + 24 * (L // 2 + 1) * M * N) / 1e6),
                    "final_dt": dt_last, "final_cfl": cfl_last, "max_div": maxdiv,
@@ -745,8 +746,10 @@ def main():
     ap.add_argument("--no-variants", action="store_true", help="skip the mixed-precision comparison of an FP64 run")
     ap.add_argument("--tune", type=int, default=-1,
                     help="kernel variant bits instead of timing them (bit 0: sequential y-solve; bits 1-2: "
-                         "right-hand side 0 fused, 1 split, 2 fused with bulk-copy staging); -1 times the "
-                         "variants and keeps the fastest")
+                         "right-hand side 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane "
+                         "transforms); -1 times the variants and keeps the fastest")
+    ap.add_argument("--no-pdl", action="store_true",
+                    help="launch the step's kernels without programmatic dependent launch")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -82,7 +82,7 @@ PRECISIONS = {"fp64": PREC_FP64, "mixed": PREC_MIXED}
 
 class Opts(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("fix_v_wall_row", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("ivisscheme", ctypes.c_int32), ("reserved", ctypes.c_int32 * 4)]
+                ("ivisscheme", ctypes.c_int32), ("no_pdl", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
 
 VIS_EXPLICIT, VIS_IMPLICIT = 0, 1
@@ -245,11 +245,12 @@ class ChannelTG:
     IDOMAIN = 1
 
     def __init__(self, setup: ChannelSetup, device: int = 0, fix_v_wall_row: bool = False, precision: str = "fp64",
-                 ivisscheme: int = VIS_EXPLICIT):
+                 ivisscheme: int = VIS_EXPLICIT, pdl: bool = True):
         """precision: "fp64" (every field and operation in FP64) or "mixed" (FP32
         velocity/pressure storage, stencils and CN sweeps; FP64 Poisson solve,
         projection and bulk-flux sums).  ivisscheme: iVisScheme of the main
-        domain (0 explicit, 1 Crank-Nicolson); the TG domain accepts 0 only."""
+        domain (0 explicit, 1 Crank-Nicolson); the TG domain accepts 0 only.
+        pdl: launch the step's kernels with programmatic dependent launch."""
         self.lib = load_library()
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
@@ -278,7 +279,7 @@ class ChannelTG:
                    _ptr(k["apvr"]), _ptr(k["ak1"]), _ptr(k["ak3"]), (ctypes.c_double * 4)(*setup.TGAM),
                    (ctypes.c_double * 4)(*setup.TROH), (ctypes.c_double * 4)(*setup.TALP), setup.AMVR1, setup.APVRN)
         g = Grid(L, M, N, 1, self.IDOMAIN)
-        o = Opts(device, int(bool(fix_v_wall_row)), PRECISIONS[precision], int(ivisscheme))
+        o = Opts(device, int(bool(fix_v_wall_row)), PRECISIONS[precision], int(ivisscheme), int(not pdl))
         h = ctypes.c_void_p()
         rc = self.lib.chapsim_gpu_init(ctypes.byref(g), ctypes.byref(cf), ctypes.byref(o), ctypes.byref(h))
         if rc != 0:

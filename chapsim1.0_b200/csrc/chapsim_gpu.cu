@@ -145,6 +145,7 @@ struct chapsim_ctx {
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
+    bool pdl = true;              // step kernels launched with programmatic dependent launch
     double2* SP = nullptr;
     float2* SPf = nullptr;       // FP32 spectral array of the mixed-precision step
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
@@ -344,7 +345,7 @@ void launch_ysolve_seq(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
     // the forward chain's FP64 intermediate: in place in an FP64 spectrum, else in the FP64 array as scratch
-    k_ysolve_seq<C><<<(int)((nl + YS_NT - 1) / YS_NT), YS_NT, smem_ysolve_seq(), ctx->stream>>>(g, spec<C>(ctx), ctx->SP,
+    launch_pdl(ctx->pdl, k_ysolve_seq<C>, (int)((nl + YS_NT - 1) / YS_NT), YS_NT, smem_ysolve_seq(), ctx->stream, g, spec<C>(ctx), ctx->SP,
                                                                                            ctx->YF);
 }
 
@@ -359,7 +360,7 @@ void launch_ysolve_warp(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
     const int nb = (int)((nl + YW_L - 1) / YW_L);
-    DISPATCH_S(g.M / 32, (k_ysolve_warp<S, C><<<nb, YW_NT, smem_yw(g), ctx->stream>>>(g, spec<C>(ctx))));
+    DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_warp<S, C>, nb, YW_NT, smem_yw(g), ctx->stream, g, spec<C>(ctx))));
 }
 
 // Momentum-stage arrays of the context in the real type R of its precision.
@@ -422,9 +423,9 @@ template <typename R>
 void launch_step_start_t(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     StepFields<R> f = step_fields<R>(ctx);
-    k_cfl<R><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, f.Q, ctx->part_red, ctx->st);
+    launch_pdl(ctx->pdl, k_cfl<R>, ctx->npart_red, DG_NT, 0, ctx->stream, g, f.Q, ctx->part_red, ctx->st);
     prof_mark(ctx);
-    k_dt_factors<R><<<15, 32, 0, ctx->stream>>>(g, ctx->part_red, ctx->npart_red, ctx->st, f.fac);
+    launch_pdl(ctx->pdl, k_dt_factors<R>, 15, 32, 0, ctx->stream, g, ctx->part_red, ctx->npart_red, ctx->st, f.fac);
     prof_mark(ctx);
     ctx->launches += 2;
 }
@@ -435,10 +436,10 @@ void launch_step_start(chapsim_ctx* ctx) {
 
 void launch_cfl_dt(chapsim_ctx* ctx, int update_dt) {
     const Geo& g = ctx->g;
-    if (ctx->prec == CHAPSIM_PREC_MIXED) k_cfl<float><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Qf, ctx->part_red, ctx->st);
-    else k_cfl<double><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->part_red, ctx->st);
+    if (ctx->prec == CHAPSIM_PREC_MIXED) launch_pdl(ctx->pdl, k_cfl<float>, ctx->npart_red, DG_NT, 0, ctx->stream, g, ctx->Qf, ctx->part_red, ctx->st);
+    else launch_pdl(ctx->pdl, k_cfl<double>, ctx->npart_red, DG_NT, 0, ctx->stream, g, ctx->Q, ctx->part_red, ctx->st);
     prof_mark(ctx);
-    k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, update_dt);
+    launch_pdl(ctx->pdl, k_dt, 1, DG_NT, 0, ctx->stream, ctx->part_red, ctx->npart_red, ctx->st, update_dt);
     prof_mark(ctx);
     ctx->launches += 2;
 }
@@ -451,19 +452,19 @@ void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns
     const int nwb = rb_warps<R>(g.L);
     if (ctx->k1_kind == 2 && nwb > 0) {
         const int grb = std::min(ctx->nsm, (g.M * g.N + nwb - 1) / nwb);
-        DISPATCH_S(g.L / 32, (k_rhs_xsweep_bulk<S, R><<<grb, nwb * 32, nwb * rb_warp_bytes<R>(g.L), s>>>(
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep_bulk<S, R>, grb, nwb * 32, nwb * rb_warp_bytes<R>(g.L), s, 
                                  g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
     } else if (ctx->k1_kind == 1) {
         dim3 grt(g.L / RT_I, g.M / RT_J, g.N / rt_chunk(g));
-        k_rhs_point<R><<<grt, RP_NT, smem_rt<R>(), s>>>(g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, ns,
+        launch_pdl(ctx->pdl, k_rhs_point<R>, grt, RP_NT, smem_rt<R>(), s, g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, ns,
                                                          rt_chunk(g));
         const long long nl = 3LL * g.M * g.N;
         const int nbx = (int)((nl + XS_NT / 32 - 1) / (XS_NT / 32));
-        DISPATCH_S(g.L / 32, (k_xsweep<S, R><<<nbx, XS_NT, smem_xs<R>(g), s>>>(g, f.RHS, fac)));
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_xsweep<S, R>, nbx, XS_NT, smem_xs<R>(g), s, g, f.RHS, fac)));
         ctx->launches += 1;
     } else {
         const int grx = g.M * g.N / RHS_WPB;
-        DISPATCH_S(g.L / 32, (k_rhs_xsweep<S, R><<<grx, RHS_WPB * 32, smem_rhs<R>(g), s>>>(g, f.Q, f.PR, f.H0, f.RHS,
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g, f.Q, f.PR, f.H0, f.RHS,
                                                                                              ctx->part_rhs, ctx->st, fac, ns)));
     }
 }
@@ -478,29 +479,29 @@ void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
     using C = SpecT<R>;
     C* sp = spec<C>(ctx);
     if (ctx->plane_kind == 1) {
-        P2_DISPATCH(g.L, g.N, (plane_fft_fwd<R, XN1, XN2, ZN1, ZN2>(g, f.Q, f.RHSLL, sp, ctx->st, ns, smem_p2<C>(g), s)));
+        P2_DISPATCH(g.L, g.N, (plane_fft_fwd<R, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, f.Q, f.RHSLL, sp, ctx->st, ns, smem_p2<C>(g), s)));
         prof_mark(ctx);
         prof_mark(ctx);
         launch_ysolve<C>(ctx);
         prof_mark(ctx);
         prof_mark(ctx);
-        P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(g, sp, ctx->DPH, smem_p2<C>(g), s)));
+        P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, sp, ctx->DPH, smem_p2<C>(g), s)));
         prof_mark(ctx);
         ctx->launches += 3;
         return;
     }
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    DISPATCH_FFT(g.L, (k_div_fftx<R, FN1, FN2><<<grp, PX_NT, smem_px<C>(g), s>>>(g, f.Q, f.RHSLL, sp, ctx->st, ns)));
+    DISPATCH_FFT(g.L, (launch_pdl(ctx->pdl, k_div_fftx<R, FN1, FN2>, grp, PX_NT, smem_px<C>(g), s, g, f.Q, f.RHSLL, sp, ctx->st, ns)));
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
+    DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<-1, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), s, g, sp)));
     prof_mark(ctx);
     launch_ysolve<C>(ctx);
     prof_mark(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, C><<<gfz, FZ_NT, smem_fz<C>(g), s>>>(g, sp)));
+    DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<+1, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), s, g, sp)));
     prof_mark(ctx);
-    DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, C><<<grp, PX_NT, smem_px<C>(g), s>>>(g, sp, ctx->DPH)));
+    DISPATCH_FFT(g.L, (launch_pdl(ctx->pdl, k_fftx_inv<FN1, FN2, C>, grp, PX_NT, smem_px<C>(g), s, g, sp, ctx->DPH)));
     prof_mark(ctx);
     ctx->launches += 5;
 }
@@ -512,7 +513,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     StepFields<R> f = step_fields<R>(ctx);
     R* fac = f.fac + (long long)ns * 5 * FAC_SET;
     if (factors) {
-        k_factors<R><<<5, 32, 0, s>>>(g, fac, ctx->st, ns);
+        launch_pdl(ctx->pdl, k_factors<R>, 5, 32, 0, s, g, fac, ctx->st, ns);
         prof_mark(ctx);
         ctx->launches += 1;
     }
@@ -520,14 +521,14 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     prof_mark(ctx);
     // persistent: as many blocks as fit at once (two per SM where the two tile buffers allow)
     const int nz = std::min((g.L / 32) * (3 * g.M - 1), (smem_z<R>(g) <= 113 * 1024 ? 2 : 1) * ctx->nsm);
-    DISPATCH_S(g.N / 32, (k_zsweep<S, R><<<nz, SWEEP_NT, smem_z<R>(g), s>>>(g, f.RHS, fac)));
+    DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R>, nz, SWEEP_NT, smem_z<R>(g), s, g, f.RHS, fac)));
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N);
-    DISPATCH_S(g.M / 32, (k_ysweep<S, R><<<gry, SWEEP_NT, smem_y<R>(g), s>>>(g, f.Q, f.RHS, ctx->st, fac, ns)));
+    DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R>, gry, SWEEP_NT, smem_y<R>(g), s, g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
     launch_pressure<R>(ctx, f, ns);
     const long long tot = (long long)g.L * g.M * g.N;
-    k_correct<R><<<(int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s>>>(g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
+    launch_pdl(ctx->pdl, k_correct<R>, (int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s, g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
     prof_mark(ctx);
     ctx->launches += 4;
 }
@@ -744,6 +745,7 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     ctx->device = opts ? opts->device : 0;
     ctx->domain = grid->idomain;
     ctx->prec = prec;
+    ctx->pdl = !(opts && opts->no_pdl);
     ctx->ivis = ivis;
     int rc;
 #define INIT_CK(call)                                  \

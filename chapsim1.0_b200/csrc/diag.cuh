@@ -16,6 +16,7 @@
 template <typename R>
 __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, double* __restrict__ partial,
                                                DevState* __restrict__ st) {
+    pdl_wait();
     __shared__ double sred[32];
     const int L = g.L, M = g.M, N = g.N;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -49,6 +50,7 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, d
 
 __global__ void __launch_bounds__(DG_NT) k_dt(const double* __restrict__ partial, int np, DevState* __restrict__ st,
                                               int update_dt) {
+    pdl_wait();
     __shared__ double sred[32];
     double mx = 0.0;
     for (int t = threadIdx.x; t < np; t += DG_NT) mx = fmax(mx, partial[t]);
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(DG_NT) k_bc_fields(Geo g, R* __restrict__ Q, R
 template <typename T>
 __global__ void __launch_bounds__(32) k_dt_factors(Geo g, const double* __restrict__ partial, int np,
                                                    DevState* __restrict__ st, T* __restrict__ fac) {
+    pdl_wait();
     const int lane = threadIdx.x;
     // four independent maxima, so that the partials' loads are in flight together
     double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;

@@ -97,6 +97,7 @@ __device__ __forceinline__ void factor_set(const Geo& g, double dt, int ns, int 
 // sweep, 2..4 y sweep of u, v, w) for the device-resident DT.
 template <typename T>
 __global__ void __launch_bounds__(32) k_factors(Geo g, T* __restrict__ fac, const DevState* __restrict__ st, int ns) {
+    pdl_wait();
     factor_set(g, st->dt, ns, blockIdx.x, fac + (long long)blockIdx.x * FAC_SET, threadIdx.x);
 }
 
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
                                                              R* __restrict__ H0, R* __restrict__ RHS,
                                                              double* __restrict__ partial, DevState* __restrict__ st,
                                                              const R* __restrict__ fac, int ns) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* sm = reinterpret_cast<R*>(sm_raw);
     __shared__ double sred[32];
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
 // while the current tile's 32 lines are solved and stored.
 template <int S, typename R>
 __global__ void __launch_bounds__(SWEEP_NT, 2) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* smb = reinterpret_cast<R*>(sm_raw);
     const int N = g.N, M = g.M;
@@ -348,6 +351,7 @@ template <int S, typename R>
 __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : 3)) k_ysweep(Geo g, R* __restrict__ Q, const R* __restrict__ RHS,
                                                      const DevState* __restrict__ st, const R* __restrict__ fac,
                                                      int ns) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* sm = reinterpret_cast<R*>(sm_raw);
     __shared__ R sdu[32];  // u increment at j = 1
@@ -457,6 +461,7 @@ __global__ void __launch_bounds__(RP_NT, sizeof(R) == 4 ? 3 : 2) k_rhs_point(Geo
                                                         R* __restrict__ H0, R* __restrict__ RHS,
                                                         double* __restrict__ partial, DevState* __restrict__ st,
                                                         int ns, int kchunk) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* ring = reinterpret_cast<R*>(sm_raw);   // [slot][field][jj][ii]
     __shared__ double sred[32];
@@ -594,6 +599,7 @@ __global__ void __launch_bounds__(RP_NT, sizeof(R) == 4 ? 3 : 2) k_rhs_point(Geo
 constexpr int XS_NT = 256;
 template <int S, typename R>
 __global__ void __launch_bounds__(XS_NT) k_xsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* sm = reinterpret_cast<R*>(sm_raw);
     const int L = 32 * S, M = g.M;

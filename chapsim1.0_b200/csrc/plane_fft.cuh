@@ -39,6 +39,7 @@ template <typename R, int NX1, int NX2, int NZ1, int NZ2>
 __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                        SpecT<R>* __restrict__ SP, const DevState* __restrict__ st,
                                                        int ns) {
+    pdl_wait();
     using C = SpecT<R>;
     using T = typename CReal<C>::T;
     constexpr int L = NX1 * NX2, N = NZ1 * NZ2, LH = L / 2 + 1, NP = N / 2;
@@ -110,6 +111,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
 
 template <int NX1, int NX2, int NZ1, int NZ2, typename C>
 __global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restrict__ SP, double* __restrict__ DPH) {
+    pdl_wait();
     using T = typename CReal<C>::T;
     constexpr int L = NX1 * NX2, N = NZ1 * NZ2, LH = L / 2 + 1, NP = N / 2;
     constexpr int LDX = L + NX2 + 1, LDZ = N + NZ2 + 1;
@@ -199,15 +201,15 @@ cudaError_t plane_fft_attrs(cudaError_t (*set)(const void*, size_t), size_t byte
     return cudaErrorInvalidValue;
 }
 template <typename R, int XN1, int XN2, int ZN1, int ZN2>
-void plane_fft_fwd(const Geo& g, const R* Q, R* RHSLL, SpecT<R>* SP, const DevState* st, int ns, size_t smem,
-                   cudaStream_t s) {
+void plane_fft_fwd(bool pdl, const Geo& g, const R* Q, R* RHSLL, SpecT<R>* SP, const DevState* st, int ns,
+                   size_t smem, cudaStream_t s) {
     if constexpr (plane_fft_fits<SpecT<R>, XN1, XN2, ZN1, ZN2>())
-        k_div_fft2<R, XN1, XN2, ZN1, ZN2><<<g.M, P2_NT, smem, s>>>(g, Q, RHSLL, SP, st, ns);
+        launch_pdl(pdl, k_div_fft2<R, XN1, XN2, ZN1, ZN2>, g.M, P2_NT, smem, s, g, Q, RHSLL, SP, st, ns);
 }
 template <typename C, int XN1, int XN2, int ZN1, int ZN2>
-void plane_fft_inv(const Geo& g, const C* SP, double* DPH, size_t smem, cudaStream_t s) {
+void plane_fft_inv(bool pdl, const Geo& g, const C* SP, double* DPH, size_t smem, cudaStream_t s) {
     if constexpr (plane_fft_fits<C, XN1, XN2, ZN1, ZN2>())
-        k_fft2_inv<XN1, XN2, ZN1, ZN2, C><<<g.M, P2_NT, smem, s>>>(g, SP, DPH);
+        launch_pdl(pdl, k_fft2_inv<XN1, XN2, ZN1, ZN2, C>, g.M, P2_NT, smem, s, g, SP, DPH);
 }
 inline bool plane_fft_shape(int L, int N) {
     return (L == 64 || L == 96 || L == 128 || L == 192) && (N == 64 || N == 96 || N == 128 || N == 192);

@@ -52,6 +52,7 @@ template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { retur
 template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                     SpecT<R>* __restrict__ SP, const DevState* __restrict__ st, int ns) {
+    pdl_wait();
     using C = SpecT<R>;
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
@@ -107,6 +108,7 @@ __global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restric
 // complex z transform of FZ_TQ consecutive (kx, j) lines (index q = kx + LH*(j-1))
 template <int SIGN, int N1, int N2, typename C>
 __global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, C* __restrict__ SP) {
+    pdl_wait();
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
     C* smc = reinterpret_cast<C*>(smp_raw);
@@ -182,6 +184,7 @@ __global__ void k_ysolve_zero_factors(Geo g, double* __restrict__ zf) {
 
 template <int S, typename C>
 __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, C* __restrict__ SP) {
+    pdl_wait();
     extern __shared__ double2 smc[];
     static_assert(YW_NT % YW_L == 0, "a thread keeps one line in the staging loops");
     const int M = 32 * S, LH = g.LH;
@@ -300,6 +303,7 @@ __device__ __forceinline__ void cp_async_row(C* dst, const C* src) {
 
 template <typename C>
 __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, const double* __restrict__ F) {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char ys_raw[];
     constexpr int NR = YS_G * YS_NG;
     double2* const ringg = reinterpret_cast<double2*>(ys_raw);  // [NR][YS_NT] rows of G (backward)
@@ -393,6 +397,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
 // ---------------------------------------------------------------------------
 template <int N1, int N2, typename C>
 __global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restrict__ SP, double* __restrict__ DPH) {
+    pdl_wait();
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
     C* smc = reinterpret_cast<C*>(smp_raw);
@@ -430,6 +435,7 @@ template <typename R>
 __global__ void __launch_bounds__(CR_NT) k_correct(Geo g, R* __restrict__ Q, R* __restrict__ PR,
                                                    const double* __restrict__ DPH, const R* __restrict__ RHSLL,
                                                    const DevState* __restrict__ st, int ns) {
+    pdl_wait();
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
     const long long t = (long long)blockIdx.x * CR_NT + threadIdx.x;

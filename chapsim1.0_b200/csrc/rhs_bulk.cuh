@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(RB_WMAX * 32, 1) k_rhs_xsweep_bulk(Geo g, cons
                                                                      R* __restrict__ RHS, double* __restrict__ partial,
                                                                      DevState* __restrict__ st,
                                                                      const R* __restrict__ fac, int ns) {
+    pdl_wait();
     extern __shared__ __align__(128) unsigned char sm_raw[];
     __shared__ uint64_t bars[RB_WMAX];
     __shared__ double sred[RB_WMAX];

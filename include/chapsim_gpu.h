@@ -84,7 +84,10 @@ typedef struct {
     int32_t precision;       /* CHAPSIM_PREC_FP64 (default) or CHAPSIM_PREC_MIXED (TG domain)  */
     int32_t ivisscheme;      /* iVisScheme of the main domain (iDomain = 2):
                                 CHAPSIM_VIS_EXPLICIT (default) or CHAPSIM_VIS_IMPLICIT          */
-    int32_t reserved[4];
+    int32_t no_pdl;          /* 0 (default): the step's kernels are launched with programmatic
+                                dependent launch (each kernel's blocks are scheduled while its
+                                predecessor drains); 1: plain launches                         */
+    int32_t reserved[3];
 } chapsim_opts_t;
 
 #define CHAPSIM_VIS_EXPLICIT 0 /* VisExplicit: VISCOUS_ALL_EXPLT_* + MASSFLUX_CALC_io */
