@@ -747,7 +747,7 @@ def main():
     ap.add_argument("--tune", type=int, default=-1,
                     help="kernel variant bits instead of timing them (bit 0: sequential y-solve; bits 1-2: "
                          "right-hand side 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane "
-                         "transforms); -1 times the variants and keeps the fastest")
+                         "transforms; bit 4: two-way y-solve); -1 times the variants and keeps the fastest")
     ap.add_argument("--no-pdl", action="store_true",
                     help="launch the step's kernels without programmatic dependent launch")
     args = ap.parse_args()

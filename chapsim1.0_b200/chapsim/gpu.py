@@ -543,13 +543,13 @@ class ChannelTG:
         """Keeps the fastest y-solve, right-hand-side and pressure-stage variants for
         this grid, or forces them (bit 0: sequential y-solve; bits 1-2: right-hand
         sides 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane
-        transforms); returns (choice bits, {variant: ms})."""
+        transforms; bit 4: two-way y-solve); returns (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 7)()
+        ms = (ctypes.c_float * 8)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
-                          "pressure_plane": ms[6]}
+                          "pressure_plane": ms[6], "ysolve_two_way": ms[7]}
 
 
 class Ensemble:

@@ -142,7 +142,8 @@ struct chapsim_ctx {
     double *Q = nullptr, *PR = nullptr, *H0 = nullptr, *RHS = nullptr, *RHSLL = nullptr, *DPH = nullptr;
     double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
     double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
-    int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas (chapsim_autotune)
+    double* YF2 = nullptr;        // factors of the two-way y-solve, 2 M doubles per line (when chosen)
+    int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     bool pdl = true;              // step kernels launched with programmatic dependent launch
@@ -350,8 +351,17 @@ void launch_ysolve_seq(chapsim_ctx* ctx) {
 }
 
 template <typename C>
+void launch_ysolve_2w(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    const long long nt = 2 * (long long)g.LH * g.N;  // two threads per mode line
+    launch_pdl(ctx->pdl, k_ysolve_2w<C>, (int)((nt + YS_NT - 1) / YS_NT), YS_NT, smem_ysolve_seq(), ctx->stream, g,
+               spec<C>(ctx), ctx->SP, ctx->YF2);
+}
+
+template <typename C>
 void launch_ysolve(chapsim_ctx* ctx) {
     if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx);
+    else if (ctx->ysolve_kind == 2 && ctx->YF2) launch_ysolve_2w<C>(ctx);
     else launch_ysolve_warp<C>(ctx);
 }
 
@@ -386,6 +396,7 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
     CK(set_smem(k_ysolve_seq<C>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
     if (ctx->domain == 1 && plane_fft_ok<C>(g))
         P2_DISPATCH(g.L, g.N, CK((plane_fft_attrs<R, XN1, XN2, ZN1, ZN2>(set_smem_void, smem_p2<C>(g)))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, C>, smem_fz<C>(g))));
@@ -403,6 +414,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw(g))));
     CK(set_smem(k_ysolve_seq<double2>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));
     if (ctx->domain == 2 && ctx->ivis) {
@@ -904,7 +916,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
+    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->YF2); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->twf); cudaFree(ctx->yz); cudaFree(ctx->SPf);
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
@@ -1877,20 +1889,32 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         k_ysolve_seq_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF);
         CK(cudaGetLastError());
     }
+    if (!ctx->YF2) {
+        CK(cudaMalloc(&ctx->YF2, 2 * nsp * sizeof(double)));
+        k_ysolve_2w_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF2);
+        CK(cudaGetLastError());
+    }
     // the variants are timed on the spectral array the time step uses (FP32 in the mixed-precision step)
     const bool spf = ctx->SPf != nullptr;
     if (spf) CK(cudaMemsetAsync(ctx->SPf, 0, nsp * sizeof(float2), s));
     else CK(cudaMemsetAsync(ctx->SP, 0, nsp * sizeof(double2), s));
     auto run_y = [&](int kind) {
-        if (spf) { if (kind == 0) launch_ysolve_warp<float2>(ctx); else launch_ysolve_seq<float2>(ctx); }
-        else { if (kind == 0) launch_ysolve_warp<double2>(ctx); else launch_ysolve_seq<double2>(ctx); }
+        if (spf) {
+            if (kind == 0) launch_ysolve_warp<float2>(ctx);
+            else if (kind == 1) launch_ysolve_seq<float2>(ctx);
+            else launch_ysolve_2w<float2>(ctx);
+        } else {
+            if (kind == 0) launch_ysolve_warp<double2>(ctx);
+            else if (kind == 1) launch_ysolve_seq<double2>(ctx);
+            else launch_ysolve_2w<double2>(ctx);
+        }
     };
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    float t[2] = {0.f, 0.f};
+    float t[3] = {0.f, 0.f, 0.f};
     const int reps = 5;
-    for (int kind = 0; kind < 2; ++kind) {
+    for (int kind = 0; kind < 3; ++kind) {
         for (int w = 0; w < 2; ++w) run_y(kind);
         CK(cudaEventRecord(e0, s));
         for (int r = 0; r < reps; ++r) run_y(kind);
@@ -1899,13 +1923,24 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaEventElapsedTime(&t[kind], e0, e1));
         t[kind] /= reps;
     }
-    ctx->launches += 2 * (2 + reps);
+    ctx->launches += 3 * (2 + reps);
     CK(cudaGetLastError());
-    ctx->ysolve_kind = force >= 0 ? (force & 1) : (t[1] < t[0] ? 1 : 0);
-    if (ctx->ysolve_kind == 0) {  // the factor table is only read by the sequential variant
-        CK(cudaStreamSynchronize(s));
+    if (force >= 0) {
+        ctx->ysolve_kind = (force & 1) ? 1 : ((force & 16) ? 2 : 0);
+    } else {
+        int best = 0;
+        for (int kind = 1; kind < 3; ++kind)
+            if (t[kind] < t[best]) best = kind;
+        ctx->ysolve_kind = best;
+    }
+    CK(cudaStreamSynchronize(s));
+    if (ctx->ysolve_kind != 1) {  // each factor table is read by its own variant only
         cudaFree(ctx->YF);
         ctx->YF = nullptr;
+    }
+    if (ctx->ysolve_kind != 2) {
+        cudaFree(ctx->YF2);
+        ctx->YF2 = nullptr;
     }
     // explicit right-hand sides + x sweep: fused, split, or fused with bulk-copy
     // staging (periodic channel).  CONVH0 is state: kept in a temporary copy
@@ -1983,10 +2018,12 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (choice) *choice = ctx->ysolve_kind | (ctx->k1_kind << 1) | (ctx->plane_kind << 3);
+    if (choice)
+        *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
+                  (ctx->ysolve_kind == 2 ? 16 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
-        ms[5] = tp[0]; ms[6] = tp[1];
+        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2];
     }
     return CHAPSIM_OK;
 }

@@ -356,9 +356,11 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the fastest of each group (force = -1), or the ones forced (force = 0..13):
- *   bit 0: Poisson y-solve, 0 = warp Thomas/PCR hybrid, 1 = the reference's
- *          sequential Thomas recurrence, one thread per mode;
+ * the fastest of each group (force = -1), or the ones forced (force = 0..29):
+ *   bits 0 and 4: Poisson y-solve, both 0 = warp Thomas/PCR hybrid, bit 0 =
+ *          the reference's sequential Thomas recurrence, one thread per mode,
+ *          bit 4 = two-way elimination, two threads per mode (bit 0 wins
+ *          when both are set);
  *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
  *          0 = fused (one warp per x line, per-thread loads), 1 = split into
  *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
@@ -367,10 +369,10 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *          transforms, 1 = fused plane transforms, one block per y row (only
  *          where the row's half spectrum fits one block's shared memory;
  *          otherwise 0 is kept whatever is forced).
- * choice receives the kept setting in the same bit form; ms[7] (may be NULL)
+ * choice receives the kept setting in the same bit form; ms[8] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
- * (fused, split, bulk-staged) and pressure stage up to DPH (chained, fused;
- * 1e30 where a variant does not apply).  CONVH0 is restored after the trial
+ * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
+ * 1e30 where a variant does not apply) and the two-way y-solve.  CONVH0 is restored after the trial
  * launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 

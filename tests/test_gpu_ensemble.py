@@ -1,6 +1,7 @@
 """Ensembles of uneven periodic channels and the y-solve autotuner.
 
-* Both Poisson y-solve variants (warp Thomas/PCR hybrid, sequential Thomas)
+* The three Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
+  Thomas, two-way elimination)
   and the three forms of the right-hand-side / x-sweep stage (fused, split,
   fused with bulk-copy staging) solve the FFT99 problem to 1e-12 of the
   oracle, and the step with any combination, with chained or fused plane
@@ -27,7 +28,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5, 8, 9, 12, 13])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5, 8, 9, 12, 13, 16, 20, 24, 28])
 def test_ysolve_variants_match_oracle(kind):
     L, M, N = 96, 64, 64
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
@@ -81,6 +82,40 @@ def test_bulk_staged_rhs_matches_fused(shape, precision, tol):
     for i in range(3):
         e = rel(out[1][i][:, 1:M + 1], out[0][i][:, 1:M + 1])
         assert e <= tol, (i, e)
+
+
+@pytest.mark.parametrize("shape", [(64, 32, 64), (128, 128, 128), (32, 256, 32)])
+def test_two_way_ysolve_matches_oracle(shape):
+    """The two-way y-solve (two threads per mode line meeting at the middle
+    row) solves the FFT99 problem to 1e-12 of the oracle for line lengths
+    32, 128 and 256, the zero mode included; in the mixed-precision step it
+    gives the sequential variant's fields to the FP32 bound."""
+    L, M, N = shape
+    s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    o = Oracle(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    c = gpu.ChannelTG(s)
+    choice, ms = c.autotune(force=16)
+    assert choice == 16 and ms["ysolve_two_way"] > 0
+    rhs = np.random.default_rng(7).standard_normal((N, M, L))
+    full = np.zeros((N, M + 2, L))
+    full[:, 1:M + 1, :] = rhs
+    ref = o.poisson(full)
+    got = c.FFT99_POIS3D_periodicxz(rhs)
+    assert rel(got[:, 1:M + 1], ref[:, 1:M + 1]) <= 1e-12
+    c.close()
+    Q, PR = initial_field(s, 5, 0.1)
+    out = []
+    for force in (1, 16):
+        c = gpu.ChannelTG(s, precision="mixed")
+        assert c.autotune(force=force)[0] == force
+        c.upload(Q, PR)
+        c.set_dt(2e-3)
+        c.SOLVERRK3_MOM_tg(0)
+        c.advance(5, 2e-3, 1e-6, 0.5)
+        out.append(c.download()[0])
+        c.close()
+    for i in range(3):
+        assert rel(out[1][i][:, 1:M + 1], out[0][i][:, 1:M + 1]) <= 1e-5
 
 
 @pytest.mark.parametrize("shape,precision,tol", [((128, 128, 128), "fp64", 1e-12), ((64, 64, 64), "fp64", 1e-12),
