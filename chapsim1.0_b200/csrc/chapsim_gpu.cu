@@ -535,7 +535,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     const int nz = std::min((g.L / 32) * (3 * g.M - 1), (smem_z<R>(g) <= 113 * 1024 ? 2 : 1) * ctx->nsm);
     DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R>, nz, SWEEP_NT, smem_z<R>(g), s, g, f.RHS, fac)));
     prof_mark(ctx);
-    dim3 gry(g.L / 32, g.N);
+    dim3 gry(g.L / 32, g.N, 2);  // layer 0: u then v, layer 1: w
     DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R>, gry, SWEEP_NT, smem_y<R>(g), s, g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
     launch_pressure<R>(ctx, f, ns);

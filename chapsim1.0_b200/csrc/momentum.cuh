@@ -346,7 +346,12 @@ __global__ void __launch_bounds__(SWEEP_NT, 2) k_zsweep(Geo g, R* __restrict__ R
 }
 
 // ---------------------------------------------------------------------------
-// y sweep + Q update: block = 32 consecutive i at fixed k, all j, u then v then w
+// y sweep + Q update: block = 32 consecutive i at fixed k, all j; blocks of
+// the grid's first z layer take u then v (v's row 1 reads the u increment of
+// the same tile), those of the second layer w.  Splitting w off balances the
+// waves: at 128^3 the 512 three-component blocks filled 444 resident slots
+// and left a second wave of 68, where the two-plus-one split packs the same
+// work into about four component times instead of six.
 template <int S, typename R>
 __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : 3)) k_ysweep(Geo g, R* __restrict__ Q, const R* __restrict__ RHS,
                                                      const DevState* __restrict__ st, const R* __restrict__ fac,
@@ -368,8 +373,9 @@ __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : 3)) k_ysweep(Geo g, R*
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int NIT = 4 * S;  // 32*M / SWEEP_NT
     const long long js = g.L;   // stride between y rows (interior and padded fields alike)
+    const int comp_lo = blockIdx.z == 0 ? 0 : 2, comp_hi = blockIdx.z == 0 ? 2 : 3;
 #pragma unroll 1
-    for (int comp = 0; comp < 3; ++comp) {
+    for (int comp = comp_lo; comp < comp_hi; ++comp) {
         const R* Ry = RHS + comp * g.FI + iidx(g, i0, 1, k);
 #pragma unroll 4
         for (int it = 0; it < NIT; ++it) {
