@@ -341,13 +341,21 @@ cudaError_t set_smem_void(const void* f, size_t bytes) {
 
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
 
+inline bool ysolve_seq_kg(const Geo& g) { return smem_ysolve_seq(g.M, true) <= (size_t)113 * 1024; }
+
 template <typename C>
 void launch_ysolve_seq(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
-    // the forward chain's FP64 intermediate: in place in an FP64 spectrum, else in the FP64 array as scratch
-    launch_pdl(ctx->pdl, k_ysolve_seq<C>, (int)((nl + YS_NT - 1) / YS_NT), YS_NT, smem_ysolve_seq(), ctx->stream, g, spec<C>(ctx), ctx->SP,
-                                                                                           ctx->YF);
+    // the forward chain's FP64 intermediate: in shared memory where two blocks per SM still fit, else in
+    // place in an FP64 spectrum, else in the FP64 array as scratch
+    const int nb = (int)((nl + YS_NT - 1) / YS_NT);
+    if (ysolve_seq_kg(g))
+        launch_pdl(ctx->pdl, k_ysolve_seq<C, true>, nb, YS_NT, smem_ysolve_seq(g.M, true), ctx->stream, g, spec<C>(ctx),
+                   ctx->SP, ctx->YF);
+    else
+        launch_pdl(ctx->pdl, k_ysolve_seq<C, false>, nb, YS_NT, smem_ysolve_seq(), ctx->stream, g, spec<C>(ctx), ctx->SP,
+                   ctx->YF);
 }
 
 template <typename C>
@@ -395,7 +403,8 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq<C>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
     CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
     if (ctx->domain == 1 && plane_fft_ok<C>(g))
         P2_DISPATCH(g.L, g.N, CK((plane_fft_attrs<R, XN1, XN2, ZN1, ZN2>(set_smem_void, smem_p2<C>(g)))));
@@ -413,7 +422,8 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq<double2>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
     CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));

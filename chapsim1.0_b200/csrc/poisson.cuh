@@ -273,7 +273,12 @@ __global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, C* __restrict__
 #define YS_G 8
 #define YS_NG 8
 #define YS_NT 32
-constexpr size_t smem_ysolve_seq() { return (size_t)YS_G * YS_NG * YS_NT * (sizeof(double2) + sizeof(double)); }
+__host__ __device__ constexpr size_t smem_ysolve_seq() { return (size_t)YS_G * YS_NG * YS_NT * (sizeof(double2) + sizeof(double)); }
+// With kg, the forward intermediate g of the block's lines stays in shared
+// memory ([M][YS_NT] double2 after the ring) instead of making a round trip
+// through global memory, and only the multipliers stream through the ring on
+// the way back: 64 KB more at M = 128, chosen where two blocks still fit an SM.
+inline size_t smem_ysolve_seq(int M, bool kg) { return smem_ysolve_seq() + (kg ? (size_t)M * YS_NT * sizeof(double2) : 0); }
 
 __global__ void k_ysolve_seq_factors(Geo g, double* __restrict__ F) {
     const int M = g.M, LH = g.LH;
@@ -301,7 +306,7 @@ __device__ __forceinline__ void cp_async_row(C* dst, const C* src) {
     else cp_async8(reinterpret_cast<double*>(dst), reinterpret_cast<const double*>(src));
 }
 
-template <typename C>
+template <typename C, bool KG>
 __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, const double* __restrict__ F) {
     pdl_wait();
     extern __shared__ __align__(16) unsigned char ys_raw[];
@@ -309,6 +314,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
     double2* const ringg = reinterpret_cast<double2*>(ys_raw);  // [NR][YS_NT] rows of G (backward)
     C* const ringc = reinterpret_cast<C*>(ys_raw);              // [NR][YS_NT] rows of the spectrum (forward)
     double* const ringf = reinterpret_cast<double*>(ys_raw + (size_t)NR * YS_NT * sizeof(double2));  // factors
+    double2* const gsm = reinterpret_cast<double2*>(ys_raw + smem_ysolve_seq());  // [M][YS_NT] g (KG)
     const int M = g.M, LH = g.LH, th = threadIdx.x;
     const long long nl = (long long)LH * g.N;
     const long long q = (long long)blockIdx.x * YS_NT + th;
@@ -352,11 +358,14 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
                 const double a = g.amph[t + 1];
                 gp = make_double2((r.x - a * gp.x) * p, (r.y - a * gp.y) * p);
             }
-            if (t < M - 1) gs[rs * t] = gp;
+            if (t < M - 1) {
+                if constexpr (KG) gsm[t * YS_NT + th] = gp;
+                else gs[rs * t] = gp;
+            }
         }
     }
     cp_async_wait_group<0>();
-    __threadfence();  // the G rows written above, before the cp.async reads below
+    if constexpr (!KG) __threadfence();  // the G rows written above, before the cp.async reads below
     // backward: x_M = g_M, x_t = g_t - H_t x_{t+1}, t = M-1 .. 1 (rows t-1 = M-2 .. 0)
     double2 xn = gp;
     s[rs * (M - 1)] = from_d2<C>(xn);
@@ -367,7 +376,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
             for (int u = 0; u < YS_G; ++u) {
                 const int t = M - 2 - b * YS_G - u, slot = (b % YS_NG) * YS_G + u;
                 if (t >= 0) {
-                    cp_async16(ringg + slot * YS_NT + th, gs + rs * t);
+                    if constexpr (!KG) cp_async16(ringg + slot * YS_NT + th, gs + rs * t);
                     cp_async8(ringf + slot * YS_NT + th, HH + (long long)t * nl);
                 }
             }
@@ -384,7 +393,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
         for (int u = 0; u < YS_G; ++u) {
             const int t = M - 2 - b * YS_G - u, slot = (b % YS_NG) * YS_G + u;
             if (t >= 0) {
-                const double2 gt = ringg[slot * YS_NT + th];
+                const double2 gt = KG ? gsm[t * YS_NT + th] : ringg[slot * YS_NT + th];
                 const double h = ringf[slot * YS_NT + th];
                 xn = make_double2(gt.x - h * xn.x, gt.y - h * xn.y);
                 s[rs * t] = from_d2<C>(xn);
