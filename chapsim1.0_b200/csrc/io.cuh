@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFields f) {
 //     It is therefore not computed.  The v row j = 1 is left unwritten; the
 //     Crank-Nicolson sweeps treat it as zero.
 template <bool CN>
-__global__ void __launch_bounds__(IO_NT) k_io_rhs(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st,
+__global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st,
                                                   int ns) {
     __shared__ double sred[32];
     __shared__ int is_last;

@@ -42,8 +42,12 @@ struct SegCoef {  // coefficients stored at the segment-padded positions of tdma
     __device__ __forceinline__ double C(int r) const { return c[seg_pos<S>(r)]; }
 };
 
-// one block: CN_LINES lines x (a, b, c, d) x 32 (S+1) doubles
-inline size_t smem_cn(int n) { return (size_t)CN_LINES * 4 * 32 * (n / 32 + 1) * sizeof(double); }
+// One block: CN_LINES lines x (a, b, c, d) x 32 (S+1) doubles, each line's
+// region padded by 2 doubles (stride 4 SEG + 2): the z and y loads write row
+// r of the block's 8 lines from consecutive threads, and an unpadded stride
+// (a multiple of 32 words) put all 8 on one bank.
+__host__ __device__ constexpr int cn_line_stride(int seg) { return 4 * seg + 2; }
+inline size_t smem_cn(int n) { return (size_t)CN_LINES * cn_line_stride(32 * (n / 32 + 1)) * sizeof(double); }
 
 // DPGRNS of RHS_MOM_EXPLICIT_io (:231-263)
 __device__ __forceinline__ double cn_dpgrns(const Geo& g, const DevState* st, int ns) {
@@ -54,7 +58,7 @@ __device__ __forceinline__ double cn_dpgrns(const Geo& g, const DevState* st, in
 
 // x lines (j, k); component blockIdx.y (0 u, 1 v, 2 w)
 template <int S>
-__global__ void __launch_bounds__(CN_NT) k_io_cn_xsweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+__global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smx[];
     constexpr int SEG = 32 * (S + 1);
     const int L = g.L, M = g.M;
@@ -64,7 +68,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_xsweep(Geo g, IoFields f, const
     if (line >= (long long)M * g.N) return;  // whole warp; no block barrier below
     const int j = 1 + (int)(line % M), k = (int)(line / M);
     if (comp == 1 && j == 1) return;
-    double* a = smx + (size_t)warp * 4 * SEG;
+    double* a = smx + (size_t)warp * cn_line_stride(SEG);
     double* b = a + SEG;
     double* c = b + SEG;
     double* d = c + SEG;
@@ -99,7 +103,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_xsweep(Geo g, IoFields f, const
 
 // z lines (i0 .. i0+CN_LINES-1, j); component blockIdx.z
 template <int S>
-__global__ void __launch_bounds__(CN_NT) k_io_cn_zsweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+__global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smz[];
     constexpr int SEG = 32 * (S + 1);
     constexpr int RSTEP = CN_NT / CN_LINES;
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_zsweep(Geo g, IoFields f, const
     const double* D = f.DST + comp * g.FS;
     const double* ms = f.MST + (comp == 0 ? g.FS : 2 * g.FS);
     double* R = f.RHS + comp * g.FI;
-    double* base = smz + (size_t)l * 4 * SEG;
+    double* base = smz + (size_t)l * cn_line_stride(SEG);
     for (int k = r0; k < N; k += RSTEP) {
         const int km = wrapm(k, N), kp = wrapp(k, N);
         const long long p = pidx(g, i, j, k), pm = pidx(g, i, j, km), pp = pidx(g, i, j, kp);
@@ -135,7 +139,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_zsweep(Geo g, IoFields f, const
     __syncthreads();
     {
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        double* bw = smz + (size_t)w * 4 * SEG;
+        double* bw = smz + (size_t)w * cn_line_stride(SEG);
         warp_tdma_smem<S, true>(bw + 3 * SEG, SegCoef<S>{bw, bw + SEG, bw + 2 * SEG}, lane);
     }
     __syncthreads();
@@ -159,7 +163,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const
     const double* amv = g.amvr + comp * (M + 2);
     const double* apv = g.apvr + comp * (M + 2);
     const double* R = f.RHS + comp * g.FI;
-    double* base = smy + (size_t)l * 4 * SEG;
+    double* base = smy + (size_t)l * cn_line_stride(SEG);
     for (int j = 1 + r0; j <= M; j += RSTEP) {
         double A, B, C, amu, apu;
         if (comp != 1) {
@@ -201,7 +205,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const
     __syncthreads();
     {
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        double* bw = smy + (size_t)w * 4 * SEG;
+        double* bw = smy + (size_t)w * cn_line_stride(SEG);
         warp_tdma_smem<S, false>(bw + 3 * SEG, SegCoef<S>{bw, bw + SEG, bw + 2 * SEG}, lane);
     }
     __syncthreads();

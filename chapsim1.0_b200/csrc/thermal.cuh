@@ -34,7 +34,7 @@ struct ThermoParams {
     double dhmin, dhmax;    // LIST_DH at IMIN_DH, IMAX_DH
 };
 
-__global__ void __launch_bounds__(IO_NT) k_eng_rhs(Geo g, IoFields f, ThermoFields t, ThermoParams tp,
+__global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFields f, ThermoFields t, ThermoParams tp,
                                                    const DevState* __restrict__ st, int ns) {
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
