@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFields f, co
     const double* D = f.DST + comp * g.FS;
     const double* ms = f.MST + (comp == 1 ? 0 : g.FS);
     double* R = f.RHS + comp * g.FI;
+#pragma unroll 4  // several rows' coefficient loads in flight
     for (int i = lane; i < L; i += 32) {
         const int im = wrapm(i, L), ip = wrapp(i, L);
         const long long p = pidx(g, i, j, k), pm = pidx(g, im, j, k), pp = pidx(g, ip, j, k);
@@ -119,6 +120,7 @@ __global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFields f, co
     const double* ms = f.MST + (comp == 0 ? g.FS : 2 * g.FS);
     double* R = f.RHS + comp * g.FI;
     double* base = smz + (size_t)l * cn_line_stride(SEG);
+#pragma unroll 4  // several rows' coefficient loads in flight
     for (int k = r0; k < N; k += RSTEP) {
         const int km = wrapm(k, N), kp = wrapp(k, N);
         const long long p = pidx(g, i, j, k), pm = pidx(g, i, j, km), pp = pidx(g, i, j, kp);
@@ -164,6 +166,7 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const
     const double* apv = g.apvr + comp * (M + 2);
     const double* R = f.RHS + comp * g.FI;
     double* base = smy + (size_t)l * cn_line_stride(SEG);
+#pragma unroll 3  // several rows' coefficient loads in flight
     for (int j = 1 + r0; j <= M; j += RSTEP) {
         double A, B, C, amu, apu;
         if (comp != 1) {
