@@ -28,7 +28,11 @@
 #include "tdma.cuh"
 
 #define RB_ROWS 23
-#define RB_WMAX 8  // warps per block at most
+#define RB_WMAX 12  // warps per block at most (FP32; see rb_wmax)
+// Warps per block at most: 8 for FP64 (184 registers: 8 x 32 x 184 fills the
+// register file), 12 for FP32, whose stages are half the size and whose
+// 153 registers leave room for 12 warps.
+template <typename R> __host__ __device__ constexpr int rb_wmax() { return sizeof(R) == 8 ? 8 : RB_WMAX; }
 
 // Shared memory of one warp: one stage of RB_ROWS rows, then the line buffer
 // of the x sweep; the region is rounded up to 32 elements so that every
@@ -42,7 +46,7 @@ template <typename R>
 inline int rb_warps(int L) {
     const size_t per = rb_warp_bytes<R>(L);
     int w = (int)((size_t)(227 * 1024 - 2048) / per);  // the opt-in limit less the static shared memory
-    return w < 1 ? 0 : (w > RB_WMAX ? RB_WMAX : w);
+    return w < 1 ? 0 : (w > rb_wmax<R>() ? rb_wmax<R>() : w);
 }
 
 template <typename R>
@@ -69,7 +73,7 @@ __device__ __forceinline__ void rb_issue(const Geo& g, const R* Q, const R* PR, 
 }
 
 template <int S, typename R>
-__global__ void __launch_bounds__(RB_WMAX * 32, 1) k_rhs_xsweep_bulk(Geo g, const R* __restrict__ Q,
+__global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g, const R* __restrict__ Q,
                                                                      const R* __restrict__ PR, R* __restrict__ H0,
                                                                      R* __restrict__ RHS, double* __restrict__ partial,
                                                                      DevState* __restrict__ st,
