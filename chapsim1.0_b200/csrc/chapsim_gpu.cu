@@ -542,7 +542,9 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     launch_rhs_x<R>(ctx, f, fac, ns);
     prof_mark(ctx);
     // persistent: as many blocks as fit at once (two per SM where the two tile buffers allow)
-    const int nz = std::min((g.L / 32) * (3 * g.M - 1), (smem_z<R>(g) <= 113 * 1024 ? 2 : 1) * ctx->nsm);
+    const int zb_want = sizeof(R) == 4 && g.N / 32 <= 4 ? 3 : 2;  // zsweep_blocks<R, S>
+    const int zb = smem_z<R>(g) * zb_want <= 226 * 1024 ? zb_want : (smem_z<R>(g) <= 113 * 1024 ? 2 : 1);
+    const int nz = std::min((g.L / 32) * (3 * g.M - 1), zb * ctx->nsm);
     DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R>, nz, SWEEP_NT, smem_z<R>(g), s, g, f.RHS, fac)));
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N, 2);  // layer 0: u then v, layer 1: w

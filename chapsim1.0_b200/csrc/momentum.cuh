@@ -270,6 +270,12 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
     }
 }
 
+// Resident blocks per SM of the persistent z sweep: 3 for FP32 lines up to
+// 128 (80 registers; the two tile buffers take 41 KB), else 2 (128
+// registers; longer FP32 lines would spill under the tighter budget, and
+// their buffers leave room for two blocks only).
+template <typename R, int S> __host__ __device__ constexpr int zsweep_blocks() { return sizeof(R) == 4 && S <= 4 ? 3 : 2; }
+
 // ---------------------------------------------------------------------------
 // cyclic z sweep.  A tile is 32 consecutive i at fixed j, all k, one
 // component; tiles of v at j = 1 are skipped (MOMFA2_Z_tg starts at N2I = 2
@@ -277,7 +283,7 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
 // shared-memory buffers: the next tile's right-hand sides load (cp.async)
 // while the current tile's 32 lines are solved and stored.
 template <int S, typename R>
-__global__ void __launch_bounds__(SWEEP_NT, 2) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
+__global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
     pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* smb = reinterpret_cast<R*>(sm_raw);
@@ -353,7 +359,7 @@ __global__ void __launch_bounds__(SWEEP_NT, 2) k_zsweep(Geo g, R* __restrict__ R
 // and left a second wave of 68, where the two-plus-one split packs the same
 // work into about four component times instead of six.
 template <int S, typename R>
-__global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : 3)) k_ysweep(Geo g, R* __restrict__ Q, const R* __restrict__ RHS,
+__global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : (sizeof(R) == 4 ? 4 : 3))) k_ysweep(Geo g, R* __restrict__ Q, const R* __restrict__ RHS,
                                                      const DevState* __restrict__ st, const R* __restrict__ fac,
                                                      int ns) {
     pdl_wait();
