@@ -702,8 +702,8 @@ def run_b200(args):
         line["variants"] = {"mixed": {"value": vm, "unit": UNIT, "ms_per_step": msm / args.steps,
                                       "speedup_vs_fp64": vm / value, "max_div": chm.DIVGCK_tg(),
                                       "autotuned_choice_bits": mt,
-                                      "precision": "FP32 storage, stencils, CN sweeps and x/z transforms; FP64 "
-                                                   "y-solve, divergence, projection, bulk sums"}}
+                                      "precision": "FP32 storage, stencils, CN sweeps, x/z transforms and pressure "
+                                                   "increment; FP64 y-solve, divergence, projection, bulk sums"}}
         ch = chm
         # config 4: heated main domain, table search against the learned property model
         hl = heated_measure(args, local, dist, ws, min(args.steps, 100))

@@ -149,6 +149,7 @@ struct chapsim_ctx {
     bool pdl = true;              // step kernels launched with programmatic dependent launch
     double2* SP = nullptr;
     float2* SPf = nullptr;       // FP32 spectral array of the mixed-precision step
+    float* DPHf = nullptr;       // FP32 pressure increment of the mixed-precision step
     double* part_rhs = nullptr;  // per-block bulk-flux partial sums
     double* fac = nullptr;       // factor tables of the x, z, y sweeps, [substep][set]
     // mixed precision (CHAPSIM_PREC_MIXED): FP32 copies of the momentum-stage
@@ -253,6 +254,10 @@ template <typename C = double2>
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * fft4s_ld(g.L)) * sizeof(C); }
 template <typename C = double2>
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(C); }
+// the context's pressure increment DPH in the step's real type
+template <typename R> R* dph(chapsim_ctx* c);
+template <> double* dph<double>(chapsim_ctx* c) { return c->DPH; }
+template <> float* dph<float>(chapsim_ctx* c) { return c->DPHf; }
 // the context's spectral array of element type C
 template <typename C> C* spec(chapsim_ctx* c);
 template <> double2* spec<double2>(chapsim_ctx* c) { return c->SP; }
@@ -507,7 +512,7 @@ void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
         launch_ysolve<C>(ctx);
         prof_mark(ctx);
         prof_mark(ctx);
-        P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, sp, ctx->DPH, smem_p2<C>(g), s)));
+        P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, sp, dph<R>(ctx), smem_p2<C>(g), s)));
         prof_mark(ctx);
         ctx->launches += 3;
         return;
@@ -523,7 +528,7 @@ void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
     prof_mark(ctx);
     DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<+1, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), s, g, sp)));
     prof_mark(ctx);
-    DISPATCH_FFT(g.L, (launch_pdl(ctx->pdl, k_fftx_inv<FN1, FN2, C>, grp, PX_NT, smem_px<C>(g), s, g, sp, ctx->DPH)));
+    DISPATCH_FFT(g.L, (launch_pdl(ctx->pdl, k_fftx_inv<FN1, FN2, C>, grp, PX_NT, smem_px<C>(g), s, g, sp, dph<R>(ctx))));
     prof_mark(ctx);
     ctx->launches += 5;
 }
@@ -552,7 +557,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     prof_mark(ctx);
     launch_pressure<R>(ctx, f, ns);
     const long long tot = (long long)g.L * g.M * g.N;
-    launch_pdl(ctx->pdl, k_correct<R>, (int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s, g, f.Q, f.PR, ctx->DPH, f.RHSLL, ctx->st, ns);
+    launch_pdl(ctx->pdl, k_correct<R>, (int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s, g, f.Q, f.PR, dph<R>(ctx), f.RHSLL, ctx->st, ns);
     prof_mark(ctx);
     ctx->launches += 4;
 }
@@ -899,6 +904,8 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         INIT_CK(cudaMemset(ctx->RHSLLf, 0, (size_t)g.FI * sizeof(float)));
         INIT_CK(cudaMemset(ctx->facf, 0, (size_t)4 * 5 * FAC_SET * sizeof(float)));
         INIT_CK(cudaMalloc(&ctx->SPf, (size_t)g.LH * M * N * sizeof(float2)));
+        INIT_CK(cudaMalloc(&ctx->DPHf, (size_t)g.FS * sizeof(float)));
+        INIT_CK(cudaMemset(ctx->DPHf, 0, (size_t)g.FS * sizeof(float)));
     }
     INIT_CK(cudaMalloc(&ctx->st, sizeof(DevState)));
     INIT_CK(cudaMallocHost(&ctx->st_host, sizeof(DevState)));
@@ -929,7 +936,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
     cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->YF2); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
-    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->twf); cudaFree(ctx->yz); cudaFree(ctx->SPf);
+    cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->twf); cudaFree(ctx->yz); cudaFree(ctx->SPf); cudaFree(ctx->DPHf);
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);

@@ -110,7 +110,8 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
 }
 
 template <int NX1, int NX2, int NZ1, int NZ2, typename C>
-__global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restrict__ SP, double* __restrict__ DPH) {
+__global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restrict__ SP,
+                                                       typename CReal<C>::T* __restrict__ DPH) {
     pdl_wait();
     using T = typename CReal<C>::T;
     constexpr int L = NX1 * NX2, N = NZ1 * NZ2, LH = L / 2 + 1, NP = N / 2;
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restric
     for (int p = threadIdx.x; p < N * L; p += P2_NT) {
         const int k = p / L, i = p - k * L;
         const C z = smc[(k >> 1) * LDX + i];
-        DPH[pidx(g, i, j, k)] = (double)((k & 1) ? z.y : z.x);
+        DPH[pidx(g, i, j, k)] = (k & 1) ? z.y : z.x;
     }
 }
 
@@ -207,7 +208,7 @@ void plane_fft_fwd(bool pdl, const Geo& g, const R* Q, R* RHSLL, SpecT<R>* SP, c
         launch_pdl(pdl, k_div_fft2<R, XN1, XN2, ZN1, ZN2>, g.M, P2_NT, smem, s, g, Q, RHSLL, SP, st, ns);
 }
 template <typename C, int XN1, int XN2, int ZN1, int ZN2>
-void plane_fft_inv(bool pdl, const Geo& g, const C* SP, double* DPH, size_t smem, cudaStream_t s) {
+void plane_fft_inv(bool pdl, const Geo& g, const C* SP, typename CReal<C>::T* DPH, size_t smem, cudaStream_t s) {
     if constexpr (plane_fft_fits<C, XN1, XN2, ZN1, ZN2>())
         launch_pdl(pdl, k_fft2_inv<XN1, XN2, ZN1, ZN2, C>, g.M, P2_NT, smem, s, g, SP, DPH);
 }

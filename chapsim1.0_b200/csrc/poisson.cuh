@@ -47,8 +47,9 @@ template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { retur
 #define CR_NT 256
 
 // ---------------------------------------------------------------------------
-// R is the stored type of Q, PR and RHSLLPHI (double, or float in the mixed-
-// precision step); divergence, transforms and correction are FP64 throughout.
+// R is the stored type of Q, PR, RHSLLPHI and DPH (double, or float in the
+// mixed-precision step, whose x and z transforms also run in FP32); the
+// divergence and the correction are evaluated in FP64.
 template <typename R, int N1, int N2>
 __global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                     SpecT<R>* __restrict__ SP, const DevState* __restrict__ st, int ns) {
@@ -570,7 +571,8 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_2w(Geo g, C* SP, double2* G, c
 
 // ---------------------------------------------------------------------------
 template <int N1, int N2, typename C>
-__global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restrict__ SP, double* __restrict__ DPH) {
+__global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restrict__ SP,
+                                                    typename CReal<C>::T* __restrict__ DPH) {
     pdl_wait();
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
@@ -599,7 +601,7 @@ __global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restric
         const int jl = p / L, i = p - jl * L;
         if (jl >= nj) continue;
         const C z = smc[(jl >> 1) * LD + i];
-        DPH[pidx(g, i, j0 + jl, k)] = (double)((jl & 1) ? z.y : z.x);
+        DPH[pidx(g, i, j0 + jl, k)] = (jl & 1) ? z.y : z.x;
     }
 }
 
@@ -607,7 +609,7 @@ __global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restric
 // VELOUPDT_tg + PRCALC_tg + BC_WALL_PR_tg (Q walls are never written)
 template <typename R>
 __global__ void __launch_bounds__(CR_NT) k_correct(Geo g, R* __restrict__ Q, R* __restrict__ PR,
-                                                   const double* __restrict__ DPH, const R* __restrict__ RHSLL,
+                                                   const R* __restrict__ DPH, const R* __restrict__ RHSLL,
                                                    const DevState* __restrict__ st, int ns) {
     pdl_wait();
     const int L = g.L, M = g.M, N = g.N;
