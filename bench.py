@@ -303,8 +303,8 @@ def heated_measure(args, local, dist, ws, steps):
 
 def kernel_bytes(L, precision="fp64"):
     """Algorithmic bytes per grid point per launch.  FP64: 8 bytes per word of
-    kernel_words.  Mixed: Q, PR, CONVH0, RHS, RHSLLPHI and the spectrum are
-    4-byte words; DPH stays FP64."""
+    kernel_words.  Mixed: Q, PR, CONVH0, RHS, RHSLLPHI, the spectrum and DPH
+    are 4-byte words."""
     if precision == "fp64":
         return {k: 8.0 * v for k, v in kernel_words(L).items()}
     spec = 2.0 * (L // 2 + 1) / L
@@ -315,8 +315,8 @@ def kernel_bytes(L, precision="fp64"):
         "k_ysweep": 9 * 4.0,
         "k_div_fftx": 4 * 4.0 + 4.0 * spec,
         "k_fftz_fwd": 8.0 * spec, "k_fftz_inv": 8.0 * spec, "k_ysolve": 8.0 * spec,
-        "k_fftx_inv": 4.0 * spec + 8.0,
-        "k_correct": 8.0 + 6 * 4.0 + 2 * 4.0 + 4.0,   # DPH; Q x3 in/out; PR in/out; RHSLLPHI
+        "k_fftx_inv": 4.0 * spec + 4.0,
+        "k_correct": 4.0 + 6 * 4.0 + 2 * 4.0 + 4.0,   # DPH; Q x3 in/out; PR in/out; RHSLLPHI
     }
 
 
