@@ -27,6 +27,14 @@
 #include "poisson.cuh"
 
 #define P2_NT 512
+// threads per block: 512 in FP64 (the transforms need ~128 registers), 1024
+// in FP32 (within 64 registers): twice the warps to hide the latency of the
+// one block per row (fused pressure stage 52 -> 51 us, mixed 128^3 step
+// 0.489 -> 0.483-0.486 ms over two runs).  The FP32
+// 192 x 192 plane keeps 512: within 64 registers it would spill ~500 B.
+template <typename C, int LN> __host__ __device__ constexpr int p2_nt() {
+    return sizeof(C) == 8 && LN < 192 * 192 ? 1024 : P2_NT;
+}
 
 // complex words of shared memory: the packed x lines (N/2 pairs of stride
 // fft4s_ld(L)) and the z lines (L/2+1 of stride fft4s_ld(N)) share one buffer
@@ -36,15 +44,16 @@ __host__ __device__ inline int plane_fft_words(int L, int N) {
 }
 
 template <typename R, int NX1, int NX2, int NZ1, int NZ2>
-__global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
+__global__ void __launch_bounds__((p2_nt<SpecT<R>, NX1 * NX2 * NZ1 * NZ2>()), 1) k_div_fft2(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                        SpecT<R>* __restrict__ SP, const DevState* __restrict__ st,
                                                        int ns) {
     pdl_wait();
     using C = SpecT<R>;
     using T = typename CReal<C>::T;
+    constexpr int NT = p2_nt<C, NX1 * NX2 * NZ1 * NZ2>();
     constexpr int L = NX1 * NX2, N = NZ1 * NZ2, LH = L / 2 + 1, NP = N / 2;
     constexpr int LDX = L + NX2 + 1, LDZ = N + NZ2 + 1;
-    constexpr int NTASK = NP * LH, TPT = (NTASK + P2_NT - 1) / P2_NT;
+    constexpr int NTASK = NP * LH, TPT = (NTASK + NT - 1) / NT;
     extern __shared__ __align__(16) unsigned char smp_raw[];
     C* smc = reinterpret_cast<C*>(smp_raw);
     const int M = g.M;
@@ -57,7 +66,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
     const R* W = Q + 2 * g.FS;
     // 1. divergence of row j; pair p holds k = 2p (real part) and k = 2p + 1 (imaginary part)
 #pragma unroll 4
-    for (int p = threadIdx.x; p < N * L; p += P2_NT) {
+    for (int p = threadIdx.x; p < N * L; p += NT) {
         const int k = p / L, i = p - k * L;
         const long long c = pidx(g, i, j, k);
         const double u = U[c], up = U[pidx(g, wrapp(i, L), j, k)];
@@ -77,7 +86,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
     C av[TPT], bv[TPT];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-        const int t = threadIdx.x + u * P2_NT;
+        const int t = threadIdx.x + u * NT;
         if (t < NTASK) {
             const int pair = t / LH, kx = t - pair * LH;
             const C* line = smc + pair * LDX;
@@ -90,7 +99,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-        const int t = threadIdx.x + u * P2_NT;
+        const int t = threadIdx.x + u * NT;
         if (t < NTASK) {
             const int pair = t / LH, kx = t - pair * LH;
             smc[kx * LDZ + 2 * pair] = av[u];
@@ -100,7 +109,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
     block_fft4s<NZ1, NZ2, -1>(smc, LH, LDZ, twz_of<C>(g));
     // 3. spectrum of row j, scaled by 1/N: SP[kx + LH*((j-1) + M*kz)]
     const T sz = (T)(1.0 / (double)N);
-    for (int p = threadIdx.x; p < LH * N; p += P2_NT) {
+    for (int p = threadIdx.x; p < LH * N; p += NT) {
         const int kz = p / LH, kx = p - kz * LH;
         C v = smc[kx * LDZ + kz];
         v.x = v.x * sz;
@@ -110,19 +119,20 @@ __global__ void __launch_bounds__(P2_NT, 1) k_div_fft2(Geo g, const R* __restric
 }
 
 template <int NX1, int NX2, int NZ1, int NZ2, typename C>
-__global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restrict__ SP,
+__global__ void __launch_bounds__((p2_nt<C, NX1 * NX2 * NZ1 * NZ2>()), 1) k_fft2_inv(Geo g, const C* __restrict__ SP,
                                                        typename CReal<C>::T* __restrict__ DPH) {
     pdl_wait();
     using T = typename CReal<C>::T;
+    constexpr int NT = p2_nt<C, NX1 * NX2 * NZ1 * NZ2>();
     constexpr int L = NX1 * NX2, N = NZ1 * NZ2, LH = L / 2 + 1, NP = N / 2;
     constexpr int LDX = L + NX2 + 1, LDZ = N + NZ2 + 1;
-    constexpr int NTASK = NP * LH, TPT = (NTASK + P2_NT - 1) / P2_NT;
+    constexpr int NTASK = NP * LH, TPT = (NTASK + NT - 1) / NT;
     extern __shared__ __align__(16) unsigned char smp_raw[];
     C* smc = reinterpret_cast<C*>(smp_raw);
     const int M = g.M;
     const int j = 1 + blockIdx.x;
     // 1. row j of the spectrum into z lines (line kx at kx * LDZ)
-    for (int p = threadIdx.x; p < LH * N; p += P2_NT) {
+    for (int p = threadIdx.x; p < LH * N; p += NT) {
         const int kz = p / LH, kx = p - kz * LH;
         const C* src = SP + kx + (long long)LH * ((j - 1) + (long long)M * kz);
         if constexpr (sizeof(C) == 16) cp_async16(smc + kx * LDZ + kz, src);
@@ -135,7 +145,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restric
     C xa[TPT], xb[TPT];
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-        const int t = threadIdx.x + u * P2_NT;
+        const int t = threadIdx.x + u * NT;
         if (t < NTASK) {
             const int pair = t / LH, ks = t - pair * LH;
             C a = smc[ks * LDZ + 2 * pair];
@@ -148,7 +158,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restric
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < TPT; ++u) {
-        const int t = threadIdx.x + u * P2_NT;
+        const int t = threadIdx.x + u * NT;
         if (t < NTASK) {
             const int pair = t / LH, ks = t - pair * LH;
             const C a = xa[u], b = xb[u];
@@ -158,7 +168,7 @@ __global__ void __launch_bounds__(P2_NT, 1) k_fft2_inv(Geo g, const C* __restric
     }
     block_fft4s<NX1, NX2, +1>(smc, NP, LDX, twx_of<C>(g));
     // 3. DPH of row j: pair p gives k = 2p (real part) and 2p + 1 (imaginary part)
-    for (int p = threadIdx.x; p < N * L; p += P2_NT) {
+    for (int p = threadIdx.x; p < N * L; p += NT) {
         const int k = p / L, i = p - k * L;
         const C z = smc[(k >> 1) * LDX + i];
         DPH[pidx(g, i, j, k)] = (k & 1) ? z.y : z.x;
@@ -205,12 +215,12 @@ template <typename R, int XN1, int XN2, int ZN1, int ZN2>
 void plane_fft_fwd(bool pdl, const Geo& g, const R* Q, R* RHSLL, SpecT<R>* SP, const DevState* st, int ns,
                    size_t smem, cudaStream_t s) {
     if constexpr (plane_fft_fits<SpecT<R>, XN1, XN2, ZN1, ZN2>())
-        launch_pdl(pdl, k_div_fft2<R, XN1, XN2, ZN1, ZN2>, g.M, P2_NT, smem, s, g, Q, RHSLL, SP, st, ns);
+        launch_pdl(pdl, k_div_fft2<R, XN1, XN2, ZN1, ZN2>, g.M, (p2_nt<SpecT<R>, XN1 * XN2 * ZN1 * ZN2>()), smem, s, g, Q, RHSLL, SP, st, ns);
 }
 template <typename C, int XN1, int XN2, int ZN1, int ZN2>
 void plane_fft_inv(bool pdl, const Geo& g, const C* SP, typename CReal<C>::T* DPH, size_t smem, cudaStream_t s) {
     if constexpr (plane_fft_fits<C, XN1, XN2, ZN1, ZN2>())
-        launch_pdl(pdl, k_fft2_inv<XN1, XN2, ZN1, ZN2, C>, g.M, P2_NT, smem, s, g, SP, DPH);
+        launch_pdl(pdl, k_fft2_inv<XN1, XN2, ZN1, ZN2, C>, g.M, (p2_nt<C, XN1 * XN2 * ZN1 * ZN2>()), smem, s, g, SP, DPH);
 }
 inline bool plane_fft_shape(int L, int N) {
     return (L == 64 || L == 96 || L == 128 || L == 192) && (N == 64 || N == 96 || N == 128 || N == 192);
