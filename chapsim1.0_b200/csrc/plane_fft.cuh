@@ -27,11 +27,11 @@
 #include "poisson.cuh"
 
 #define P2_NT 512
-// threads per block: 512 in FP64 (the transforms need ~128 registers), 1024
-// in FP32 (within 64 registers): twice the warps to hide the latency of the
-// one block per row (fused pressure stage 52 -> 51 us, mixed 128^3 step
-// 0.489 -> 0.483-0.486 ms over two runs).  The FP32
-// 192 x 192 plane keeps 512: within 64 registers it would spill ~500 B.
+// Threads per block: 512 in FP64 (the transforms need ~128 registers), 1024
+// in FP32 (within 64 registers), twice the warps to hide the latency of the
+// one block per row: the fused pressure stage 52 -> 51 us, the mixed 128^3
+// step 0.489 -> 0.483-0.486 ms over two runs.  The FP32 192 x 192 plane
+// keeps 512 threads: within 64 registers it would spill ~500 B.
 template <typename C, int LN> __host__ __device__ constexpr int p2_nt() {
     return sizeof(C) == 8 && LN < 192 * 192 ? 1024 : P2_NT;
 }
