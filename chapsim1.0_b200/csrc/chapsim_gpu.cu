@@ -359,7 +359,7 @@ void launch_ysolve_seq(chapsim_ctx* ctx) {
         launch_pdl(ctx->pdl, k_ysolve_seq<C, true>, nb, YS_NT, smem_ysolve_seq(g.M, true), ctx->stream, g, spec<C>(ctx),
                    ctx->SP, ctx->YF);
     else
-        launch_pdl(ctx->pdl, k_ysolve_seq<C, false>, nb, YS_NT, smem_ysolve_seq(), ctx->stream, g, spec<C>(ctx), ctx->SP,
+        launch_pdl(ctx->pdl, k_ysolve_seq<C, false>, nb, YS_NT, smem_ysolve_seq(g.M, false), ctx->stream, g, spec<C>(ctx), ctx->SP,
                    ctx->YF);
 }
 
@@ -408,7 +408,7 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
     CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
     if (ctx->domain == 1 && plane_fft_ok<C>(g))
@@ -427,7 +427,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw(g))));
-    CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq()));
+    CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
     CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));

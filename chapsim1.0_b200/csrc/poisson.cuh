@@ -279,7 +279,12 @@ __host__ __device__ constexpr size_t smem_ysolve_seq() { return (size_t)YS_G * Y
 // memory ([M][YS_NT] double2 after the ring) instead of making a round trip
 // through global memory, and only the multipliers stream through the ring on
 // the way back: 64 KB more at M = 128, chosen where two blocks still fit an SM.
-inline size_t smem_ysolve_seq(int M, bool kg) { return smem_ysolve_seq() + (kg ? (size_t)M * YS_NT * sizeof(double2) : 0); }
+// The M values of AMPH follow (the chain reads one per row; with the ring
+// and g filling the shared memory the L1 is small, and the factor copies
+// evicted them: every read went to L2).
+inline size_t smem_ysolve_seq(int M, bool kg) {
+    return smem_ysolve_seq() + (kg ? (size_t)M * YS_NT * sizeof(double2) : 0) + (size_t)M * sizeof(double);
+}
 
 __global__ void k_ysolve_seq_factors(Geo g, double* __restrict__ F) {
     const int M = g.M, LH = g.LH;
@@ -317,6 +322,10 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
     double* const ringf = reinterpret_cast<double*>(ys_raw + (size_t)NR * YS_NT * sizeof(double2));  // factors
     double2* const gsm = reinterpret_cast<double2*>(ys_raw + smem_ysolve_seq());  // [M][YS_NT] g (KG)
     const int M = g.M, LH = g.LH, th = threadIdx.x;
+    double* const sam = reinterpret_cast<double*>(ys_raw + smem_ysolve_seq() +
+                                                  (KG ? (size_t)M * YS_NT * sizeof(double2) : 0));  // AMPH(t+1)
+    for (int t = th; t < M; t += YS_NT) sam[t] = g.amph[t + 1];
+    __syncthreads();
     const long long nl = (long long)LH * g.N;
     const long long q = (long long)blockIdx.x * YS_NT + th;
     if (q >= nl) return;  // no block barrier below
@@ -356,7 +365,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_seq(Geo g, C* SP, double2* G, 
                 const double2 r0 = q == 0 ? make_double2(0.0, 0.0) : r;
                 gp = make_double2(r0.x / p, r0.y / p);
             } else {
-                const double a = g.amph[t + 1];
+                const double a = sam[t];
                 gp = make_double2((r.x - a * gp.x) * p, (r.y - a * gp.y) * p);
             }
             if (t < M - 1) {
