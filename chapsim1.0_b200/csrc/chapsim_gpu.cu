@@ -146,6 +146,7 @@ struct chapsim_ctx {
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
+    int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
     bool pdl = true;              // step kernels launched with programmatic dependent launch
     double2* SP = nullptr;
     float2* SPf = nullptr;       // FP32 spectral array of the mixed-precision step
@@ -332,6 +333,18 @@ cudaError_t set_smem_void(const void* f, size_t bytes) {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
 }
 
+// a block's dynamic shared-memory limit for kernel f: the device's opt-in
+// maximum less f's static shared memory (0 when it cannot be queried)
+template <typename F>
+long long bulk_smem_limit(F* f) {
+    int dev = 0, optin = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, f) != cudaSuccess) return 0;
+    return (long long)optin - (long long)fa.sharedSizeBytes;
+}
+
 #define DISPATCH_S(S_, KERNEL_CALL)                    \
     switch (S_) {                                      \
         case 1: { constexpr int S = 1; KERNEL_CALL; } break;  \
@@ -399,7 +412,9 @@ template <typename R>
 int configure_momentum(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R>, smem_rhs<R>(g))));
-    if (rb_warps<R>(g.L) > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_warps<R>(g.L) * rb_warp_bytes<R>(g.L))));
+    ctx->rb_nw = 0;
+    DISPATCH_S(g.L / 32, ctx->rb_nw = rb_warps<R>(g.L, bulk_smem_limit(k_rhs_xsweep_bulk<S, R>)));
+    if (ctx->rb_nw > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_smem<R>(g.L, ctx->rb_nw))));
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R>, smem_z<R>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
     DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
@@ -476,10 +491,10 @@ template <typename R>
 void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    const int nwb = rb_warps<R>(g.L);
+    const int nwb = ctx->rb_nw;
     if (ctx->k1_kind == 2 && nwb > 0) {
         const int grb = std::min(ctx->nsm, (g.M * g.N + nwb - 1) / nwb);
-        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep_bulk<S, R>, grb, nwb * 32, nwb * rb_warp_bytes<R>(g.L), s, 
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep_bulk<S, R>, grb, nwb * 32, rb_smem<R>(g.L, nwb), s, 
                                  g, f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
     } else if (ctx->k1_kind == 1) {
         dim3 grt(g.L / RT_I, g.M / RT_J, g.N / rt_chunk(g));
@@ -1973,7 +1988,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         void* h0 = mixed ? (void*)ctx->H0f : (void*)ctx->H0;
         CK(cudaMemcpyAsync(hsave, h0, hb, cudaMemcpyDeviceToDevice, s));
         const int keep = ctx->k1_kind;
-        const bool bulk_fits = mixed ? rb_warps<float>(g.L) > 0 : rb_warps<double>(g.L) > 0;
+        const bool bulk_fits = ctx->rb_nw > 0;
         for (int kind = 0; kind < 3; ++kind) {
             if (kind == 2 && !bulk_fits) {
                 tk[2] = 1e30f;

@@ -42,12 +42,23 @@ template <typename R>
 __host__ __device__ inline size_t rb_warp_bytes(int L) {
     return (size_t)rb_warp_elems(L) * sizeof(R);
 }
+// After the warps' regions, the block keeps the x sweep's factor table: its
+// 5S+20 values per lane are read in every line's solve, and with the stages
+// filling the shared memory the L1 is too small to hold them (they came from
+// L2, inside the sweep's dependency chain).
 template <typename R>
-inline int rb_warps(int L) {
+__host__ __device__ inline size_t rb_fac_bytes(int L) { return (size_t)TF_NF(L / 32) * 32 * sizeof(R); }
+// warps per block that fit beside the factor table, given the block's
+// shared-memory limit less the kernel's static shared memory
+template <typename R>
+inline int rb_warps(int L, long long limit) {
     const size_t per = rb_warp_bytes<R>(L);
-    int w = (int)((size_t)(227 * 1024 - 2048) / per);  // the opt-in limit less the static shared memory
+    const long long avail = limit - (long long)rb_fac_bytes<R>(L);
+    int w = avail > 0 ? (int)(avail / (long long)per) : 0;
     return w < 1 ? 0 : (w > rb_wmax<R>() ? rb_wmax<R>() : w);
 }
+template <typename R>
+inline size_t rb_smem(int L, int nw) { return (size_t)nw * rb_warp_bytes<R>(L) + rb_fac_bytes<R>(L); }
 
 template <typename R>
 __device__ __forceinline__ void rb_issue(const Geo& g, const R* Q, const R* PR, const R* H0, int line, R* stage,
@@ -107,7 +118,13 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
     const R dxi = (R)g.dxi, dzi = (R)g.dzi, dxqi = (R)g.dxqi, dzqi = (R)g.dzqi;
     const R c1x = (R)(0.5 * 0.5 * g.dxi);
     const R c3x = (R)(0.5 * 0.5 * g.dzi);
-    const R* fx = fac + FSET_X * FAC_SET;
+    // the x sweep's factor table, staged once per block
+    R* const sfx = reinterpret_cast<R*>(sm_raw) + (size_t)nw * rb_warp_elems(L);
+    {
+        const R* fx = fac + FSET_X * FAC_SET;
+        for (int t = threadIdx.x; t < TF_NF(S) * 32; t += blockDim.x) sfx[t] = fx[t];
+    }
+    __syncthreads();
     double bulk = 0.0;
     uint32_t phase = 0u;
     bool pending = first < nlines;  // a copy issued and not yet consumed
@@ -204,7 +221,7 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
             pending = true;
         }
         // cyclic x sweeps of this line's three components (MOMFA1_X_tg starts at N2I = 2 for v)
-        warp_tdma_apply_smem3<S, true>(sl, LS, j >= 2, fx, lane);  // the three components together
+        warp_tdma_apply_smem3<S, true>(sl, LS, j >= 2, sfx, lane);  // the three components together
         __syncwarp();
         R* Rl = RHS + iidx(g, 0, j, k);
 #pragma unroll
