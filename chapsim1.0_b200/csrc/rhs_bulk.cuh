@@ -83,6 +83,28 @@ __device__ __forceinline__ void rb_issue(const Geo& g, const R* Q, const R* PR, 
     for (int r = 0; r < RB_ROWS; ++r) bulk_g2s(stage + r * L, src[r], rb, bar);
 }
 
+// The y-dependent coefficients of a line (j): interpolation weights at j and
+// j+1, metrics, and the viscous y coefficients of the three components.  With
+// the stages and the factor table filling the shared memory the L1 is too
+// small to keep them, so each line's set comes from L2: the kernel loads the
+// next line's set into registers while it solves the current line.
+struct RbGeo {
+    double wffj, wfbj, wffp, wfbp, dyfi, dyci, am[3], ac[3], ap[3];
+};
+__device__ __forceinline__ RbGeo rb_geo(const Geo& g, int j) {
+    RbGeo r;
+    const int M2 = g.M + 2;
+    r.wffj = g.wff[j]; r.wfbj = g.wfb[j]; r.wffp = g.wff[j + 1]; r.wfbp = g.wfb[j + 1];
+    r.dyfi = g.dyfi[j]; r.dyci = g.dyci[j];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        r.am[c] = g.amvr[c * M2 + j];
+        r.ac[c] = g.acvr[c * M2 + j];
+        r.ap[c] = g.apvr[c * M2 + j];
+    }
+    return r;
+}
+
 template <int S, typename R>
 __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g, const R* __restrict__ Q,
                                                                      const R* __restrict__ PR, R* __restrict__ H0,
@@ -129,6 +151,7 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
     uint32_t phase = 0u;
     bool pending = first < nlines;  // a copy issued and not yet consumed
     bool ok = true;
+    RbGeo gn = rb_geo(g, first < nlines ? 1 + first % M : 1);
 #pragma unroll 1
     for (int line = first; line < nlines; line += stride) {
         ok = mbar_wait(bar, phase, &st->err);
@@ -136,13 +159,13 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
         phase ^= 1u;
         pending = false;
         const int j = 1 + line % M, k = line / M;
-        const int jp = j + 1;
-        const R wffj = (R)g.wff[j], wfbj = (R)g.wfb[j], wffp = (R)g.wff[jp], wfbp = (R)g.wfb[jp];
-        const R dyfij = (R)g.dyfi[j], dycij = (R)g.dyci[j];
-        const double dyj = 1.0 / g.dyfi[j] / 1.0;
-        const R amu = (R)g.amvr[j], acu = (R)g.acvr[j], apu = (R)g.apvr[j];
-        const R amv = (R)g.amvr[(M + 2) + j], acv = (R)g.acvr[(M + 2) + j], apv = (R)g.apvr[(M + 2) + j];
-        const R amw = (R)g.amvr[2 * (M + 2) + j], acw = (R)g.acvr[2 * (M + 2) + j], apw = (R)g.apvr[2 * (M + 2) + j];
+        const RbGeo gc = gn;
+        const R wffj = (R)gc.wffj, wfbj = (R)gc.wfbj, wffp = (R)gc.wffp, wfbp = (R)gc.wfbp;
+        const R dyfij = (R)gc.dyfi, dycij = (R)gc.dyci;
+        const double dyj = 1.0 / gc.dyfi / 1.0;
+        const R amu = (R)gc.am[0], acu = (R)gc.ac[0], apu = (R)gc.ap[0];
+        const R amv = (R)gc.am[1], acv = (R)gc.ac[1], apv = (R)gc.ap[1];
+        const R amw = (R)gc.am[2], acw = (R)gc.ac[2], apw = (R)gc.ap[2];
         const R* sU = sg;          // c, jp, jm, kp, km
         const R* sV = sg + 5 * L;  // c, jp, jm, kp, km, (jp, km)
         const R* sW = sg + 11 * L; // c, jp, jm, kp, km, (jm, kp)
@@ -219,6 +242,7 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
         if (line + stride < nlines) {
             if (lane == 0) rb_issue<R>(g, Q, PR, H0, line + stride, sg, bar);
             pending = true;
+            gn = rb_geo(g, 1 + (line + stride) % M);  // arrives during this line's x sweep
         }
         // cyclic x sweeps of this line's three components (MOMFA1_X_tg starts at N2I = 2 for v)
         warp_tdma_apply_smem3<S, true>(sl, LS, j >= 2, sfx, lane);  // the three components together
