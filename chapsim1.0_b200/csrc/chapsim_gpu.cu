@@ -28,7 +28,7 @@
 
 // x transform reading RHSLLPHI directly (used by chapsim_fft99_pois3d)
 template <int N1, int N2>
-__global__ void __launch_bounds__(PX_NT, 2) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
+__global__ void __launch_bounds__(PX_NT, PX_MINB) k_fftx_from_rhs(Geo g, const double* __restrict__ RHSLL, double2* __restrict__ SP) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, LH = g.LH;
     const int LD = fft4s_ld(L);

@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const 
 // DIVG_io + forward x transform (same tiling as k_div_fftx)
 // DRHO: DrhoDtP of the thermal solver, or NULL (zero) while it is off
 template <int N1, int N2>
-__global__ void __launch_bounds__(PX_NT, 2) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
+__global__ void __launch_bounds__(PX_NT, PX_MINB) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
                                                        double2* __restrict__ SP, const DevState* __restrict__ st, int ns,
                                                        const double* __restrict__ DRHO) {
     extern __shared__ double2 smc[];

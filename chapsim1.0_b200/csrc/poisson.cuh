@@ -40,8 +40,14 @@ template <typename C> __device__ __forceinline__ C from_d2(double2 a);
 template <> __device__ __forceinline__ double2 from_d2<double2>(double2 a) { return a; }
 template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
 
-#define PX_TJ 32  // x-lines per block (16 packed pairs)
-#define PX_NT 256
+// x-line transforms: PX_TJ x lines per block (PX_TJ / 2 packed pairs), PX_NT
+// threads, PX_MINB blocks per SM in the register budget (128 registers).  The
+// block loads its lines, transforms them in shared memory and stores them,
+// one phase after the other; four small blocks per SM overlap those phases
+// better than two blocks of twice the size.
+#define PX_TJ 16
+#define PX_NT 128
+#define PX_MINB 4
 #define FZ_TQ 16  // z-lines per block
 #define FZ_NT 256
 #define CR_NT 256
@@ -51,7 +57,7 @@ template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { retur
 // mixed-precision step, whose x and z transforms also run in FP32); the
 // divergence and the correction are evaluated in FP64.
 template <typename R, int N1, int N2>
-__global__ void __launch_bounds__(PX_NT, 2) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
+__global__ void __launch_bounds__(PX_NT, PX_MINB) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                     SpecT<R>* __restrict__ SP, const DevState* __restrict__ st, int ns) {
     pdl_wait();
     using C = SpecT<R>;
@@ -580,7 +586,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_2w(Geo g, C* SP, double2* G, c
 
 // ---------------------------------------------------------------------------
 template <int N1, int N2, typename C>
-__global__ void __launch_bounds__(PX_NT, 2) k_fftx_inv(Geo g, const C* __restrict__ SP,
+__global__ void __launch_bounds__(PX_NT, PX_MINB) k_fftx_inv(Geo g, const C* __restrict__ SP,
                                                     typename CReal<C>::T* __restrict__ DPH) {
     pdl_wait();
     using T = typename CReal<C>::T;
