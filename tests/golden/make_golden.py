@@ -1,8 +1,8 @@
 """Extract golden vectors from the reference's shipped outputs into small fixtures.
 
-Run in a container where the reference checkout is mounted (default
-``/root/reference``; override with ``CHAPSIM_REFERENCE``).  The GPU tests never
-read the reference tree: they read only the fixtures this script writes.
+Run where a reference checkout exists, with its path in the environment
+variable ``CHAPSIM_REFERENCE``.  The tests never read the reference tree: they
+read only the fixtures this script writes.
 
 Sources (all produced by the reference solver itself):
   test_cases_template/TC8_Channel_IO_thermal_LiquidWater/0_log_monitors/
@@ -13,6 +13,10 @@ Sources (all produced by the reference solver itself):
     CHK_COORD_XND/ZND.dat  -- COORDJR (src/COORDJR.f90:269-328)
     monitor.io.2020.1217.1640.log -- per-step monitor rows (PP_SCN_MONITOR)
   test_cases_template/TC8_.../readdata.ini -- the case parameters
+  test_cases_template/TC4_Channel_IO_thermal_ScpWater/NIST_WATER_23.5MP.DAT
+                         -- the property table read by the table path
+                            (src/thermo_properties_table_searching.f90:1261),
+                            every 6th row kept (nist_water_rows.npz)
 """
 import json
 import os
@@ -20,10 +24,23 @@ import re
 
 import numpy as np
 
-REF = os.environ.get("CHAPSIM_REFERENCE", "/root/reference")
+REF = os.environ.get("CHAPSIM_REFERENCE", "")
 TC8 = os.path.join(REF, "test_cases_template", "TC8_Channel_IO_thermal_LiquidWater")
 MON = os.path.join(TC8, "0_log_monitors")
+NIST = os.path.join(REF, "test_cases_template", "TC4_Channel_IO_thermal_ScpWater", "NIST_WATER_23.5MP.DAT")
 OUT = os.path.dirname(os.path.abspath(__file__))
+NIST_STRIDE = 6
+
+
+def write_nist():
+    """Every NIST_STRIDE-th row of the reference's NIST water table (file order), float64."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(OUT)), "chapsim1.0_b200"))
+    from chapsim import thermo
+    rows = thermo.read_table(NIST)
+    np.savez_compressed(os.path.join(OUT, "nist_water_rows.npz"), rows=rows[::NIST_STRIDE],
+                        n_full=np.int64(rows.shape[0]), stride=np.int64(NIST_STRIDE))
+    print("wrote", os.path.join(OUT, "nist_water_rows.npz"))
 
 
 def _rows(path, ncols=None):
@@ -52,6 +69,9 @@ def _blocks_tdma(path):
 
 
 def main():
+    if not REF or not os.path.isdir(REF):
+        raise SystemExit("set CHAPSIM_REFERENCE to the reference checkout")
+    write_nist()
     fx = {}
     # CHK_COORD_YND: first block JND YND 1/DYCI YND+ ; second block JCL YCC 1/DYFI DYC+
     lines = open(os.path.join(MON, "CHK_COORD_YND.dat")).read().split("# JCL")

@@ -15,7 +15,8 @@ import pytest
 import oracle
 from chapsim import thermo
 
-NIST = os.path.join("/root/reference/test_cases_template/TC4_Channel_IO_thermal_ScpWater/NIST_WATER_23.5MP.DAT")
+# every 6th row of the reference's NIST_WATER_23.5MP.DAT (TC4), written by tests/golden/make_golden.py
+NIST = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "nist_water_rows.npz")
 
 
 @pytest.fixture(scope="module")
@@ -122,10 +123,10 @@ def test_update_interpolates_smoothly(synth):
         assert np.max(np.abs(res[k] - lin)) < 1e-3 * scale, k
 
 
-@pytest.mark.skipif(not os.path.exists(NIST), reason="reference table not present")
 def test_nist_table_setup_equals_oracle():
-    rows = thermo.read_table(NIST)
-    assert rows.shape == (11998, 8)
+    fx = np.load(NIST)
+    rows = fx["rows"]
+    assert int(fx["n_full"]) == 11998 and rows.shape == (2000, 8)
     tab = thermo.SplineTable.from_rows(rows, 680.15)
     lists, ref = oracle.table_nondim(rows, 680.15)
     for k in thermo.LIST_NAMES:
