@@ -1,10 +1,14 @@
 """Benchmark of the CHAPSim periodic-channel time step on B200.
 
 Workload (one "step" = one RK3 time step: CFL/dt + 3 substeps, the CpuT
-boundary of src/SOLVE.f90:76,137): periodic plane channel at Re_tau ~ 180
-(REN = 2800), domain 4pi x 2 x 4pi/3, grid 128 x 128 x 128, tanh-stretched y
+boundary of src/SOLVE.f90:76,137): periodic plane channel at Re_tau ~ 395
+(REN = 6875), domain 2pi x 2 x pi, grid 384 x 256 x 384, tanh-stretched y
 (STR2 = 2), FP64 throughout, seeded perturbed-Poiseuille start projected by
 the NS = 0 substep, CFL 0.5.  Metric: grid-point * RK3-steps per second.
+The line's variants are the same grid in mixed precision (FP32 stencils and
+CN sweeps, FP64 Poisson y-solve and projection), the 128^3 channel at
+Re_tau ~ 180 in both precisions, and the heated main-domain channel with
+table-search and with learned properties.
 
   python bench.py [--gpus N --steps K --warmup W]        # B200 arm
   python bench.py --impl reference [...]                 # CPU reference arm
@@ -39,7 +43,7 @@ WORKLOADS = {
     "channel64_retau180_fp64": (64, 64, 64, 2 * math.pi, math.pi, 2.0, 2800.0, 0.05, 0.5),
     "channel384x256x384_retau395_fp64": (384, 256, 384, 2 * math.pi, math.pi, 2.0, 6875.0, 0.05, 0.5),
 }
-DEFAULT_WORKLOAD = "channel128_retau180_fp64"
+DEFAULT_WORKLOAD = "channel384x256x384_retau395_fp64"
 ENSEMBLE_WORKLOAD = "ensemble12_uneven"
 
 
@@ -302,36 +306,33 @@ def heated_measure(args, local, dist, ws, steps):
 
 
 def kernel_bytes(L, precision="fp64"):
-    """Algorithmic bytes per grid point per launch.  FP64: 8 bytes per word of
-    kernel_words.  Mixed: Q, PR, CONVH0, RHS, RHSLLPHI, the spectrum and DPH
-    are 4-byte words."""
-    if precision == "fp64":
-        return {k: 8.0 * v for k, v in kernel_words(L).items()}
-    spec = 2.0 * (L // 2 + 1) / L
+    """Algorithmic bytes per grid point moved by one launch of each periodic-
+    channel kernel, keyed by the kernel names profile_steps reports: reads +
+    writes of the arrays the reference's algorithm needs.  The spectrum holds
+    (L/2+1)/L complex values per point.  FP64: 8-byte words.  Mixed: Q, PR,
+    CONVH0, RHS, RHSLLPHI, the spectrum and DPH are stored in 4-byte words."""
+    w = 8.0 if precision == "fp64" else 4.0
+    spec = 2.0 * (L // 2 + 1) / L * w  # complex spectrum, bytes per point
     return {
-        "k_cfl": 3 * 4.0, "k_dt_factors": 0.0,
-        "k_rhs_xsweep": 13 * 4.0,
-        "k_zsweep": 6 * 4.0,
-        "k_ysweep": 9 * 4.0,
-        "k_div_fftx": 4 * 4.0 + 4.0 * spec,
-        "k_fftz_fwd": 8.0 * spec, "k_fftz_inv": 8.0 * spec, "k_ysolve": 8.0 * spec,
-        "k_fftx_inv": 4.0 * spec + 4.0,
-        "k_correct": 4.0 + 6 * 4.0 + 2 * 4.0 + 4.0,   # DPH; Q x3 in/out; PR in/out; RHSLLPHI
+        "k_cfl": 3 * w, "k_dt_factors": 0.0,
+        "k_rhs_xsweep": 13 * w,            # Q x3, PR, H0 x3 in; H0 x3, RHS x3 out (x sweep in registers)
+        "k_rhs_xsweep_bulk": 13 * w,       # the same, rows staged by bulk copies
+        "k_rhs_point+k_xsweep": 19 * w,    # the same, plus the RHS round trip of the separate x sweep
+        "k_zsweep": 6 * w,                 # RHS x3 in/out
+        "k_ysweep": 9 * w,                 # RHS x3, Q x3 in; Q x3 out
+        "k_div_fftx": 4 * w + spec,        # Q x3 in; RHSLLPHI, spectrum out
+        "k_div_fft2": 4 * w + spec,        # the same with the z transforms of the plane
+        "k_fftz_fwd": 2 * spec, "k_fftz_inv": 2 * spec,
+        "k_ysolve_warp": 2 * spec, "k_ysolve_seq": 2 * spec, "k_ysolve_2w": 2 * spec,
+        "k_fftx_inv": spec + w,            # spectrum in; DPH out
+        "k_fft2_inv": spec + w,            # the same with the inverse z transforms of the plane
+        "k_correct": 10 * w,               # DPH, Q x3, PR, RHSLLPHI in; Q x3, PR out
     }
 
 
-def kernel_words(L):
-    spec = 2.0 * (L // 2 + 1) / L  # complex spectrum, words per point
-    return {
-        "k_cfl": 3.0, "k_dt_factors": 0.0,
-        "k_rhs_xsweep": 13.0,          # Q x3, PR, H0 x3 in; H0 x3, RHS x3 out
-        "k_zsweep": 6.0,               # RHS x3 in/out
-        "k_ysweep": 9.0,               # RHS x3, Q x3 in; Q x3 out
-        "k_div_fftx": 4.0 + spec,      # Q x3 in; RHSLLPHI, spectrum out
-        "k_fftz_fwd": 2.0 * spec, "k_fftz_inv": 2.0 * spec, "k_ysolve": 2.0 * spec,
-        "k_fftx_inv": spec + 1.0,      # spectrum in; DPH out
-        "k_correct": 10.0,             # DPH, Q x3, PR, RHSLLPHI in; Q x3, PR out
-    }
+def step_launches(name):
+    """Launches of kernel `name` per RK3 step (CFL and the dt rule run once, the rest per substep)."""
+    return 1 if name in ("k_cfl", "k_dt_factors") else 3
 
 
 def load_peaks():
@@ -574,6 +575,88 @@ def run_ensemble(args):
     return 0
 
 
+def channel_roofline(ch, L, precision, pts, prof_steps, DT0, DTMIN, CFLGV, ms_per_step, traffic_key):
+    """Per-kernel CUDA-event durations of the step (the kernels of the variants in
+    use), the roofline of the kernel with the largest share and of the whole step."""
+    kms = ch.profile_steps(prof_steps, DT0, DTMIN, CFLGV)
+    kb = kernel_bytes(L, precision)
+    peak, peak_kind = load_peaks()
+    total_ms = sum(kms.values())
+    dom = max(kms, key=lambda k: kms[k])
+    per_launch_ms = kms[dom] / (prof_steps * step_launches(dom))
+    dom_bytes = kb[dom] * pts
+    achieved = dom_bytes / (per_launch_ms / 1000.0) / 1e9
+    traffic = load_traffic(traffic_key).get(dom)
+    step_bytes = sum(kb[k] * pts * step_launches(k) for k in kms)
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+            "algorithmic_bytes_per_launch": dom_bytes, "launch_ms": per_launch_ms,
+            "share_of_step": kms[dom] / total_ms}
+    step = {"bytes_per_point_step": step_bytes / pts, "achieved_gbs": step_bytes / (ms_per_step / 1000) / 1e9,
+            "frac": step_bytes / (ms_per_step / 1000) / 1e9 / peak,
+            "survey_model_1344B_frac": (1344.0 if precision == "fp64" else 672.0) * pts / (ms_per_step / 1000) / 1e9
+            / peak}
+    per_kernel = {k: {"ms_per_step": kms[k] / prof_steps, "launch_ms": kms[k] / (prof_steps * step_launches(k)),
+                      "frac": kb[k] * pts / (kms[k] / (prof_steps * step_launches(k)) / 1000.0) / 1e9 / peak}
+                  for k in sorted(kms)}
+    return roof, step, per_kernel
+
+
+def channel_measure(args, wl, precision, local, dist, ws, seed, steps, keep=False):
+    """One periodic-channel workload on this rank's GPU: autotune, warm-up, K
+    graph replays timed with CUDA events on the library's stream (max over
+    ranks), then the per-kernel profile.  Returns the measurement and, with
+    keep, the open context."""
+    from chapsim import gpu
+    import torch
+    L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = WORKLOADS[wl]
+    DTMIN = 1e-6
+    s = channel_setup(L, M, N, HX, HZ, STR2, REN)
+    Q0, PR0 = initial_field(s, seed, 0.1)
+    ch = gpu.ChannelTG(s, device=local, precision=precision, pdl=not args.no_pdl)
+    ch.upload(Q0, PR0)
+    ch.set_dt(DT0)
+    ch.SOLVERRK3_MOM_tg(0)
+    # keeps the fastest y-solve, right-hand-side and pressure-stage variants for this grid; --tune pins them instead
+    tuned, tune_ms = ch.autotune(force=args.tune)
+    stream = torch.cuda.ExternalStream(ch.stream_handle(), device=local)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    # the clock sampler runs over the warm-up and the timed region (a window of several 100 ms samples)
+    with ClockSampler(local) as clk:
+        ch.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)  # warm-up (also captures the step graph)
+        launches0 = ch.launch_count()
+        barrier()
+        ev0.record(stream)
+        dt_last, cfl_last = ch.advance(steps, DT0, DTMIN, CFLGV)
+        ev1.record(stream)
+        torch.cuda.synchronize(local)
+    barrier()
+    launches = ch.launch_count() - launches0
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
+    pts = L * M * N
+    value = aggregate_rate(pts, steps, ws, ms)
+    prof_steps = max(1, min(20, steps))
+    roof, step, per_kernel = channel_roofline(ch, L, precision, pts, prof_steps, DT0, DTMIN, CFLGV, ms / steps,
+                                              wl if precision == "fp64" else wl + "_mixed")
+    out = {"value": value, "ms": ms, "ms_per_step": ms / steps, "launches": launches, "clocks": clk.summary(),
+           "choice": tuned, "tune_ms": {k: round(v, 4) for k, v in tune_ms.items()}, "roofline": roof,
+           "step_roofline": step, "kernels": per_kernel, "max_div": ch.DIVGCK_tg(), "final_dt": dt_last,
+           "final_cfl": cfl_last, "grid": [L, M, N], "REN": REN, "STR2": STR2, "CFLGV": CFLGV,
+           "Q0": Q0, "PR0": PR0, "pts": pts, "DT0": DT0, "DTMIN": DTMIN}
+    if keep:
+        out["ch"] = ch
+    else:
+        ch.close()
+    return out
+
+
 def run_b200(args):
     from chapsim import gpu
     ws, rank, local = dist_setup()
@@ -588,42 +671,18 @@ def run_b200(args):
     import torch
     torch.cuda.set_device(local)
     wl = args.workload
-    L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = WORKLOADS[wl]
-    DTMIN = 1e-6
-    s = channel_setup(L, M, N, HX, HZ, STR2, REN)
-    Q0, PR0 = initial_field(s, replica_seed(rank), 0.1)
-    ch = gpu.ChannelTG(s, device=local, precision=args.precision, pdl=not args.no_pdl)
-    ch.upload(Q0, PR0)
-    ch.set_dt(DT0)
-    ch.SOLVERRK3_MOM_tg(0)
-    # keeps the faster y-solve and right-hand-side variants for this grid; --tune pins them instead
-    tuned, tune_ms = ch.autotune(force=args.tune)
-    # warm-up (also captures the step graph)
-    ch.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)
-    stream = torch.cuda.ExternalStream(ch.stream_handle(), device=local)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    m = channel_measure(args, wl, args.precision, local, dist, ws, replica_seed(rank), args.steps, keep=True)
+    ch = m["ch"]
+    L, M, N = m["grid"]
+    pts, DT0, DTMIN, CFLGV = m["pts"], m["DT0"], m["DTMIN"], WORKLOADS[wl][8]
+    Q0, PR0 = m["Q0"], m["PR0"]
 
+    # ---- end to end through the public API with host buffers ----
     def barrier():
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize(local)
 
-    launches0 = ch.launch_count()
-    barrier()
-    with ClockSampler(local) as clk:
-        ev0.record(stream)
-        dt_last, cfl_last = ch.advance(args.steps, DT0, DTMIN, CFLGV)
-        ev1.record(stream)
-        torch.cuda.synchronize(local)
-    barrier()
-    launches = ch.launch_count() - launches0
-    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
-    pts = L * M * N
-    value = aggregate_rate(pts, args.steps, ws, ms)
-    maxdiv = ch.DIVGCK_tg()
-
-    # ---- end to end through the public API with host buffers ----
     try:
         qh = torch.empty(Q0.shape, dtype=torch.float64, pin_memory=True).numpy()
         ph = torch.empty(PR0.shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -639,76 +698,60 @@ def run_b200(args):
         ch.lib.chapsim_download_fields(ch.h, gpu._ptr(qh), gpu._ptr(ph), None)  # D2H: the step's result
     ch.sync()
     te = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+    ch.close()
     e2e = pts * ne * ws / te
     hbytes = int(qh.nbytes + ph.nbytes)
+    del qh, ph
 
-    # ---- per-kernel durations (CUDA events on the library stream) ----
-    prof_steps = max(1, min(20, args.steps))
-    kms = ch.profile_steps(prof_steps, DT0, DTMIN, CFLGV)
-    launches_per_step = {k: (1 if k in ("k_cfl", "k_dt_factors") else 3) for k in kms}
-    kb = kernel_bytes(L, args.precision)
-    peak, peak_kind = load_peaks()
-    per_launch = {k: kms[k] / (prof_steps * launches_per_step[k]) for k in kms}
-    total_ms = sum(kms.values())
-    dom = max(kms, key=lambda k: kms[k])
-    dom_bytes = kb[dom] * pts
-    achieved = dom_bytes / (per_launch[dom] / 1000.0) / 1e9
-    traffic = load_traffic(wl if args.precision == "fp64" else wl + "_mixed").get(dom)
-    step_bytes = sum(kb[k] * pts * launches_per_step[k] for k in kb)
-    step_ms = 1000.0 * 1.0 / (value / ws / pts)
-
+    grid_desc = {128: "4pi x 2 x 4pi/3", 64: "2pi x 2 x pi", 384: "2pi x 2 x pi"}.get(L)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-        "config": {"workload": wl, "grid": [L, M, N], "domain": "4pi x 2 x 4pi/3" if L == 128 else None,
-                   "REN": REN, "STR2": STR2, "CFLGV": CFLGV, "precision": args.precision,
+        "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": wl, "grid": [L, M, N], "domain": grid_desc, "REN": m["REN"], "STR2": m["STR2"],
+                   "CFLGV": CFLGV, "precision": args.precision,
                    "parallelism": "replicas" if ws > 1 else "single", "cuda_graph": True,
                    "programmatic_dependent_launch": not args.no_pdl,
                    "l2": "no flush: per-step working set %.0f MB > 126 MB L2" % (
                        (12 * 8 * (M + 2) * L * N + 4 * 8 * L * M * N + 24 * (L // 2 + 1) * M * N) / 1e6),
-                   "final_dt": dt_last, "final_cfl": cfl_last, "max_div": maxdiv,
-                   "autotuned": {"choice_bits": tuned, "ms": {k: round(v, 4) for k, v in tune_ms.items()}}},
+                   "final_dt": m["final_dt"], "final_cfl": m["final_cfl"], "max_div": m["max_div"],
+                   "autotuned": {"choice_bits": m["choice"], "kernels": sorted(m["kernels"]), "ms": m["tune_ms"]}},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": hbytes, "d2h_bytes_per_step": hbytes,
                 "steps": ne, "api": "chapsim_upload_fields + chapsim_advance_tg(1) + chapsim_download_fields"},
-        "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": dom_bytes,
-                     "share_of_step": kms[dom] / total_ms},
-        "step_roofline": {"bytes_per_point_step": step_bytes / pts, "achieved_gbs": step_bytes / (step_ms / 1000) / 1e9,
-                          "frac": step_bytes / (step_ms / 1000) / 1e9 / peak,
-                          "survey_model_1344B_frac": 1344.0 * pts / (step_ms / 1000) / 1e9 / peak},
-        "kernel_ms_per_step": {k: kms[k] / prof_steps for k in sorted(kms)},
-        "clocks": clk.summary(),
+        "gpu_launches": int(m["launches"]),
+        "roofline": m["roofline"],
+        "step_roofline": m["step_roofline"],
+        "kernels": m["kernels"],
+        "clocks": m["clocks"],
     }
     if args.precision == "fp64" and not args.no_variants:
+        variants = {}
         # the same workload in mixed precision (FP32 stencils / CN sweeps, FP64 Poisson and projection)
-        ch.close()
-        chm = gpu.ChannelTG(s, device=local, precision="mixed")
-        chm.upload(Q0, PR0)
-        chm.set_dt(DT0)
-        chm.SOLVERRK3_MOM_tg(0)
-        mt, _ = chm.autotune(force=args.tune)
-        chm.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)
-        sm_ = torch.cuda.ExternalStream(chm.stream_handle(), device=local)
-        barrier()
-        ev0.record(sm_)
-        chm.advance(args.steps, DT0, DTMIN, CFLGV)
-        ev1.record(sm_)
-        torch.cuda.synchronize(local)
-        msm = max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
-        vm = aggregate_rate(pts, args.steps, ws, msm)
-        line["variants"] = {"mixed": {"value": vm, "unit": UNIT, "ms_per_step": msm / args.steps,
-                                      "speedup_vs_fp64": vm / value, "max_div": chm.DIVGCK_tg(),
-                                      "autotuned_choice_bits": mt,
-                                      "precision": "FP32 storage, stencils, CN sweeps, x/z transforms and pressure "
-                                                   "increment; FP64 y-solve, divergence, projection, bulk sums"}}
-        ch = chm
+        mm = channel_measure(args, wl, "mixed", local, dist, ws, replica_seed(rank), args.steps)
+        variants["mixed"] = {
+            "value": mm["value"], "unit": UNIT, "ms_per_step": mm["ms_per_step"],
+            "speedup_vs_fp64": mm["value"] / m["value"], "max_div": mm["max_div"],
+            "autotuned_choice_bits": mm["choice"], "roofline": mm["roofline"], "step_roofline": mm["step_roofline"],
+            "kernels": mm["kernels"], "gpu_launches": int(mm["launches"]), "clocks": mm["clocks"],
+            "precision": "FP32 storage, stencils, CN sweeps, x/z transforms and pressure increment; "
+                         "FP64 y-solve, divergence, projection, bulk sums"}
+        # the 128^3 channel as a variant when the line is another grid
+        small = "channel128_retau180_fp64"
+        if wl != small:
+            s64 = channel_measure(args, small, "fp64", local, dist, ws, replica_seed(rank), args.steps)
+            s32 = channel_measure(args, small, "mixed", local, dist, ws, replica_seed(rank), args.steps)
+            variants["channel128"] = {
+                "workload": small, "grid": s64["grid"], "value_fp64": s64["value"], "value_mixed": s32["value"],
+                "unit": UNIT, "ms_per_step_fp64": s64["ms_per_step"], "ms_per_step_mixed": s32["ms_per_step"],
+                "speedup_mixed_vs_fp64": s32["value"] / s64["value"],
+                "choice_bits": {"fp64": s64["choice"], "mixed": s32["choice"]},
+                "roofline_fp64": s64["roofline"], "roofline_mixed": s32["roofline"],
+                "step_roofline_fp64": s64["step_roofline"], "step_roofline_mixed": s32["step_roofline"],
+                "kernels_fp64": s64["kernels"], "kernels_mixed": s32["kernels"]}
         # config 4: heated main domain, table search against the learned property model
         hl = heated_measure(args, local, dist, ws, min(args.steps, 100))
         lv = hl["variants"]["learned_properties"]
-        line["variants"]["heated_learned"] = {
+        variants["heated_learned"] = {
             "workload": HEATED_WORKLOAD, "grid": hl["config"]["grid"], "steps": hl["steps"],
             "value_table": hl["value"], "value_learned": lv["value"], "unit": UNIT,
             "ms_per_step_table": hl["ms_per_step"], "ms_per_step_learned": lv["ms_per_step"],
@@ -718,14 +761,15 @@ def run_b200(args):
             "step_roofline_frac": hl["step_roofline"]["frac"],
             "note": "main domain (Crank-Nicolson momentum, energy equation, property update every substep), FP64; "
                     "the full line: --workload " + HEATED_WORKLOAD}
+        line["variants"] = variants
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         rate, n, dt = cpu_reference_rate(wl, 1000, float(os.environ.get("CHAPSIM_CPU_SAMPLE_S", "15")), threads)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{n} RK3 steps of {wl} on the CPU FP64 restatement (OpenMP)"}
+                                "sample": f"{n} RK3 steps of {wl} on the CPU FP64 restatement (OpenMP), after the "
+                                          f"NS = 0 projection and one untimed step"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    ch.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()

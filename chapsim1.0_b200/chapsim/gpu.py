@@ -36,6 +36,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_download_thermal_fields", "chapsim_mlp_init", "chapsim_mlp_set_params", "chapsim_mlp_get_params",
             "chapsim_mlp_gradients", "chapsim_mlp_train", "chapsim_mlp_infer_points", "chapsim_thermal_use_mlp",
             "chapsim_mlp_judge", "chapsim_autotune", "chapsim_batch_create", "chapsim_batch_advance",
+            "chapsim_set_buoyancy", "chapsim_upload_weighted_pressure",
             "chapsim_batch_get_stream", "chapsim_batch_destroy", "chapsim_pp_mean_zx_tg", "chapsim_pp_mean_t_tg",
             "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
             "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write"]
@@ -47,6 +48,20 @@ PP_MONITOR = ["U1c", "U1c_t", "U2c", "U2c_t", "U3c", "U3c_t", "uu", "uu_t", "uv"
 
 KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_ysweep", "k_div_fftx", "k_fftz_fwd", "k_ysolve",
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
+
+
+def step_kernel_slots(choice: int = 0):
+    """Names of the kernels in the profiling slots of one periodic-channel step
+    for the variant bits `choice` of chapsim_autotune.  The split right-hand
+    side times k_rhs_point and k_xsweep in one slot; with the fused plane
+    transforms the two z-transform slots stay empty and are named None."""
+    rhs = {0: "k_rhs_xsweep", 1: "k_rhs_point+k_xsweep", 2: "k_rhs_xsweep_bulk"}[(choice >> 1) & 3]
+    ys = "k_ysolve_seq" if choice & 1 else ("k_ysolve_2w" if choice & 16 else "k_ysolve_warp")
+    if choice & 8:
+        pre = ["k_div_fft2", None, ys, None, "k_fft2_inv"]
+    else:
+        pre = ["k_div_fftx", "k_fftz_fwd", ys, "k_fftz_inv", "k_fftx_inv"]
+    return ["k_cfl", "k_dt_factors"] + ([rhs, "k_zsweep", "k_ysweep"] + pre + ["k_correct"]) * 3
 
 
 class ChapsimError(RuntimeError):
@@ -153,6 +168,8 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_download_io_fields.argtypes = [vp, _dp, _dp, _dp]
     L.chapsim_rk_substep_io.argtypes = [vp, ctypes.c_int32]
     L.chapsim_cfl_io.argtypes = [vp, _dp]
+    L.chapsim_set_buoyancy.argtypes = [vp, ctypes.c_int32, ctypes.c_double]
+    L.chapsim_upload_weighted_pressure.argtypes = [vp, _dp, _dp]
     L.chapsim_profile_steps.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_float), ctypes.c_int32]
     L.chapsim_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
@@ -252,6 +269,7 @@ class ChannelTG:
         domain (0 explicit, 1 Crank-Nicolson); the TG domain accepts 0 only.
         pdl: launch the step's kernels with programmatic dependent launch."""
         self.lib = load_library()
+        self.choice = 0  # variant bits in use (chapsim_autotune); the library starts with all zero
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.precision = precision
@@ -404,18 +422,21 @@ class ChannelTG:
         return out
 
     def kernel_slots(self):
-        """Names of the kernel slots of one step, in the order chapsim_profile_steps reports them."""
-        return KERNEL_SLOTS
+        """Names of the kernels in the slots of one step, in the order
+        chapsim_profile_steps reports them, for the variants in use."""
+        return step_kernel_slots(self.choice)
 
     def profile_steps(self, nsteps, DT0, DTMIN, CFLGV):
-        """Per-kernel durations (ms, summed over nsteps) keyed by kernel name."""
+        """Per-kernel durations (ms, summed over nsteps) keyed by the name of the
+        kernel that ran (empty slots are left out)."""
         slots = self.kernel_slots()
         n = len(slots)
         buf = (ctypes.c_float * n)()
         self._check(self.lib.chapsim_profile_steps(self.h, int(nsteps), DT0, DTMIN, CFLGV, buf, n))
         out = {}
         for name, v in zip(slots, buf):
-            out[name] = out.get(name, 0.0) + float(v)
+            if name is not None:
+                out[name] = out.get(name, 0.0) + float(v)
         return out
 
     def stream_handle(self):
@@ -547,6 +568,7 @@ class ChannelTG:
         ch = ctypes.c_int32()
         ms = (ctypes.c_float * 8)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
+        self.choice = ch.value
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
                           "pressure_plane": ms[6], "ysolve_two_way": ms[7]}
@@ -630,6 +652,22 @@ class ChannelIO(ChannelTG):
 
     def SOLVERRK3_MOM_io(self, NS):
         self._check(self.lib.chapsim_rk_substep_io(self.h, int(NS)))
+
+    def set_buoyancy(self, iGravity, F_A):
+        """thermal_gravity / RHS_MOM_EXPLICIT_io buoyancy: D_STG * TALP*DT*F_A on component |iGravity|."""
+        self._check(self.lib.chapsim_set_buoyancy(self.h, int(iGravity), float(F_A)))
+
+    def set_weighted_pressure(self, PR0_1=None, PR0_2=None):
+        """iWeightedPre = 1 with the two PR0_io layers ((N, M+2, L), the second defaults to the first);
+        None turns it off."""
+        if PR0_1 is None:
+            self._check(self.lib.chapsim_upload_weighted_pressure(self.h, None, None))
+            return
+        a = np.ascontiguousarray(PR0_1, np.float64)
+        b = np.ascontiguousarray(PR0_2 if PR0_2 is not None else PR0_1, np.float64)
+        if a.shape != self.field_shape() or b.shape != self.field_shape():
+            raise ValueError("PR0 layers must have the padded field shape")
+        self._check(self.lib.chapsim_upload_weighted_pressure(self.h, _ptr(a), _ptr(b)))
 
     def CFL_io(self):
         v = ctypes.c_double()

@@ -689,7 +689,8 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
     DISPATCH_FFT(g.L, (k_io_div_fftx<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP,
                                                                             ctx->st, ns,
-                                                                            ctx->thermal ? ctx->tf.DRHO : nullptr)));
+                                                                            ctx->thermal ? ctx->tf.DRHO : nullptr,
+                                                                            ctx->io.PR0A ? 0.25 + IO_PRES_EPSLON : 1.0)));
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
@@ -955,6 +956,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
+    cudaFree(const_cast<double*>(ctx->io.PR0A));
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
     cudaFree(ctx->mlp_par); cudaFree(ctx->mlp_w2); cudaFree(ctx->mlp_xs); cudaFree(ctx->mlp_ys); cudaFree(ctx->mlp_dh);
     cudaFree(ctx->mlp_judge);
@@ -1328,6 +1330,51 @@ int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns) {
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     return CHAPSIM_OK;
+}
+
+// the captured step graph holds the kernels' arguments: a new setting needs a new capture
+static int drop_step_graph(chapsim_ctx* ctx) {
+    if (ctx->step_exec) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaGraphExecDestroy(ctx->step_exec);
+        ctx->step_exec = nullptr;
+    }
+    return CHAPSIM_OK;
+}
+
+int chapsim_set_buoyancy(chapsim_ctx_t* ctx, int32_t igravity, double f_a) {
+    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (igravity < -3 || igravity > 3 || !std::isfinite(f_a))
+        return fail(ctx, CHAPSIM_ERR_BADARG, "iGravity must be in -3..3 and F_A finite");
+    CK(cudaSetDevice(ctx->device));
+    ctx->io.igrav = igravity;
+    ctx->io.fa = igravity ? f_a : 0.0;
+    return drop_step_graph(ctx);
+}
+
+int chapsim_upload_weighted_pressure(chapsim_ctx_t* ctx, const double* pr0_1, const double* pr0_2) {
+    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if ((pr0_1 == nullptr) != (pr0_2 == nullptr))
+        return fail(ctx, CHAPSIM_ERR_BADARG, "give both PR0_io layers, or neither to turn iWeightedPre off");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    const size_t fb = (size_t)g.FS * sizeof(double);
+    if (!pr0_1) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(const_cast<double*>(ctx->io.PR0A));
+        ctx->io.PR0A = ctx->io.PR0B = nullptr;
+        return drop_step_graph(ctx);
+    }
+    if (!ctx->io.PR0A) {  // the two layers in one allocation
+        double* p = nullptr;
+        CK(cudaMalloc(&p, 2 * fb));
+        ctx->io.PR0A = p;
+        ctx->io.PR0B = p + g.FS;
+    }
+    CK(cudaMemcpyAsync(const_cast<double*>(ctx->io.PR0A), pr0_1, fb, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(const_cast<double*>(ctx->io.PR0B), pr0_2, fb, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return drop_step_graph(ctx);
 }
 
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {

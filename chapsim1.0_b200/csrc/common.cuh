@@ -145,6 +145,13 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, unsig
     }
 }
 
+// mbar_wait by every lane of a warp, with one outcome for the whole warp: the
+// lanes leave the wait together, so a warp-collective instruction after it
+// (tcgen05.ld, shuffles) never sees a split warp, even when a budget ran out
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* mbar, uint32_t parity, unsigned int* err) {
+    return __all_sync(0xffffffffu, mbar_wait(mbar, parity, err));
+}
+
 // one arrival that also announces `bytes` of bulk-copy traffic on the mbarrier
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* mbar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)), "r"(bytes) : "memory");

@@ -27,9 +27,28 @@
 
 // RHO is DENSITY0 and DEN is DENSITY (the same array while the thermal
 // solver is off); MU0 is Viscousity0 and MU is Viscousity.
+// PR0A/PR0B: PR0_io(:,:,:,1) and PR0_io(:,:,:,2) of iWeightedPre = 1 (NULL when
+// off).  igrav/fa: iGravity and F_A of thermal_gravity (src/Flow_State.f90:95-125).
 struct IoFields {
     double *G, *Q, *PR, *EX0, *RHS, *RHO, *MU0, *MU, *DST, *MST, *DIVU, *DEN;
+    const double *PR0A = nullptr, *PR0B = nullptr;
+    double fa = 0.0;
+    int igrav = 0;
 };
+
+// iWeightedPre: pres_epslon (src/modules.f90:483)
+#define IO_PRES_EPSLON 0.001
+
+// PGM of RHS_MOM_EXPLICIT_io (src/RHS_MOM_EXPLICIT_io.f90:103-159): the
+// pressure difference between point c and its lower neighbour cm times coe,
+// blended with the two PR0_io layers when iWeightedPre = 1
+__device__ __forceinline__ double io_pgm(const IoFields& f, long long c, long long cm, double pc, double pm,
+                                         double coe) {
+    if (f.PR0A)
+        return ((f.PR0B[c] - f.PR0B[cm]) * (0.25 - IO_PRES_EPSLON) + (f.PR0A[c] - f.PR0A[cm]) * 0.5 +
+                (pc - pm) * (0.25 + IO_PRES_EPSLON)) * coe;
+    return (pc - pm) * coe;
+}
 
 
 // ---------------------------------------------------------------------------
@@ -348,12 +367,17 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* 
         const double e01 = f.EX0[ii], e02 = f.EX0[ii + g.FI], e03 = f.EX0[ii + 2 * g.FI];
         const double pc = PR[c], pim = PR[cim], pjm = PR[cjm], pkm = PR[ckm];
         const double coa = ta * dt;
+        // buoyancy (:161-226): D_STG * TALP*DT*F_A on the component |iGravity| (1/RNDI1 = 1/RCCI1 = 1)
+        const int ig = f.igrav < 0 ? -f.igrav : f.igrav;
+        const double cob = ta * dt * f.fa;
         double r1 = (tg * ex1 + tr * e01) * dt;
         if constexpr (CN) r1 = r1 + coa * im1;
-        r1 = r1 - (pc - pim) * (ta * dt * g.dxi);
+        r1 = r1 - io_pgm(f, c, cim, pc, pim, ta * dt * g.dxi);
+        if (ig == 1) r1 = r1 + f.DST[c] * cob;
         double r3 = (tg * ex3 + tr * e03) * dt;
         if constexpr (CN) r3 = r3 + coa * im3;
-        r3 = r3 - (pc - pkm) * (ta * dt * g.dzi);
+        r3 = r3 - io_pgm(f, c, ckm, pc, pkm, ta * dt * g.dzi);
+        if (ig == 3) r3 = r3 + f.DST[c + 2 * FS] * (cob / 1.0);
         f.EX0[ii] = ex1;
         f.EX0[ii + 2 * g.FI] = ex3;
         f.RHS[ii] = r1;
@@ -361,7 +385,8 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* 
         if (j >= 2) {
             double r2 = (tg * ex2 + tr * e02) * dt;
             if constexpr (CN) r2 = r2 + coa * im2;
-            r2 = r2 - (pc - pjm) * (ta * dt * dycij / 1.0);
+            r2 = r2 - io_pgm(f, c, cjm, pc, pjm, ta * dt * dycij / 1.0);
+            if (ig == 2) r2 = r2 + f.DST[c + FS] * (cob / 1.0);
             f.EX0[ii + g.FI] = ex2;
             f.RHS[ii + g.FI] = r2;
         }
@@ -406,11 +431,12 @@ __global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const 
 }
 
 // DIVG_io + forward x transform (same tiling as k_div_fftx)
-// DRHO: DrhoDtP of the thermal solver, or NULL (zero) while it is off
+// DRHO: DrhoDtP of the thermal solver, or NULL (zero) while it is off;
+// the divergence is divided by wdiv (DIVG.f90:78-82)
 template <int N1, int N2>
 __global__ void __launch_bounds__(PX_NT, PX_MINB) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
                                                        double2* __restrict__ SP, const DevState* __restrict__ st, int ns,
-                                                       const double* __restrict__ DRHO) {
+                                                       const double* __restrict__ DRHO, double wdiv) {
     extern __shared__ double2 smc[];
     const int L = g.L, M = g.M, N = g.N, LH = g.LH;
     const int LD = fft4s_ld(L);
@@ -419,7 +445,8 @@ __global__ void __launch_bounds__(PX_NT, PX_MINB) k_io_div_fftx(Geo g, const dou
     const int nj = min(PX_TJ, M - j0 + 1);
     const int np = (nj + 1) >> 1;
     const int kp = wrapp(k, N);
-    const double coe0 = 1.0 / st->dt / g.talp[ns];
+    // wdiv: 0.25 + pres_epslon with iWeightedPre = 1, else 1 (an exact division)
+    const double coe0 = 1.0 / st->dt / g.talp[ns] / wdiv;
     const double coe1 = g.dxi / 1.0;
 #pragma unroll 4
     for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {

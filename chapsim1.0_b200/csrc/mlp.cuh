@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
                 umma_bf16(tmem, umma_desc(sA, 128, s), umma_desc(sW2, 64, s), umma_idesc(128, 64), s > 0);
             umma_commit(&mbar);
         }
-        ok = mbar_wait(&mbar, phase, err) && ok;
+        ok = mbar_wait_warp(&mbar, phase, err) && ok;
         phase ^= 1;
         tc_fence_after();
         float acc[16];
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
                 umma_bf16(tmem + 64, umma_desc(sA, 128, s), umma_desc(sW3, 16, s), umma_idesc(128, 16), s > 0);
             umma_commit(&mbar);
         }
-        ok = mbar_wait(&mbar, phase, err) && ok;
+        ok = mbar_wait_warp(&mbar, phase, err) && ok;
         phase ^= 1;
         tc_fence_after();
         tmem_ld16(tmem + lane_base + 64, acc);
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
         for (int s = 0; s < 4; ++s) umma_bf16(tmem, umma_desc(sH1, 128, s), umma_desc(sW2, 64, s), umma_idesc(128, 64), s > 0);
         umma_commit(&mbar);
     }
-    mbar_wait(&mbar, phase, err);
+    mbar_wait_warp(&mbar, phase, err);
     phase ^= 1;
     tc_fence_after();
 #pragma unroll
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
             umma_bf16(tmem + 64, umma_desc(sH2, 128, s), umma_desc(sW3, 16, s), umma_idesc(128, 16), s > 0);
         umma_commit(&mbar);
     }
-    mbar_wait(&mbar, phase, err);
+    mbar_wait_warp(&mbar, phase, err);
     phase ^= 1;
     tc_fence_after();
     tmem_ld16(tmem + lane_base + 64, acc);
@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
             umma_bf16(tmem + 192, umma_desc(sDZT, 128, s), umma_desc(sH1T, 64, s), umma_idesc(128, 64), s > 0);
         umma_commit(&mbar);
     }
-    mbar_wait(&mbar, phase, err);
+    mbar_wait_warp(&mbar, phase, err);
     phase ^= 1;
     tc_fence_after();
     // dL/dh1 -> first layer (per-sample dz1 staged, then column sums)

@@ -154,7 +154,8 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
     RbGeo gn = rb_geo(g, first < nlines ? 1 + first % M : 1);
 #pragma unroll 1
     for (int line = first; line < nlines; line += stride) {
-        ok = mbar_wait(bar, phase, &st->err);
+        // every lane waits; the warp leaves together if any lane's budget ran out
+        ok = mbar_wait_warp(bar, phase, &st->err);
         if (!ok) break;  // the copy never completed: stop issuing
         phase ^= 1u;
         pending = false;
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
     }
     if (!ok) {
         // the warp's copy may still be in flight: wait for it (bounded) before the block exits
-        if (pending) mbar_wait(bar, phase, &st->err);
+        if (pending) (void)mbar_wait_warp(bar, phase, &st->err);
     }
     // grid sum of the bulk-flux integrand: warp, block (warp order), then the
     // last block adds the block partials in index order (deterministic)

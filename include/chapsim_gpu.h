@@ -176,7 +176,9 @@ int chapsim_tdmaijj_noncyc(const double* a, const double* b, const double* c, do
  * gives CHAPSIM_ERR_NAN.
  * Set-up: the first call on each device (the one current in the calling
  * thread) looks up the array's address with cudaGetSymbolAddress and keeps
- * it; make that first call before any stream capture begins.
+ * it; make that first call before any stream capture begins.  The address is
+ * kept for the life of the process: a cudaDeviceReset of that device after
+ * its first call is not supported (later calls would use a stale address).
  * Sharing: all calls on a device use the same array, which keeps the last
  * call's contents (the call clears its status counter itself).  Calls that
  * overlap in time on one device, e.g. from two host threads, race on it and
@@ -205,6 +207,21 @@ int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* g, double* q, double*
 int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns);
 /* CFL_io (src/CFL.f90:55-107): CFLMM_io including the viscous number. */
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm);
+/* Buoyancy of RHS_MOM_EXPLICIT_io (src/RHS_MOM_EXPLICIT_io.f90:161-226), set up
+ * as thermal_gravity does (src/Flow_State.f90:95-125): component |igravity| of
+ * the momentum right-hand side (1 x, 2 y, 3 z; 0 none) takes
+ * D_STG * TALP(NS)*DT*F_A, before the bulk-forcing sum.  f_a is the host's
+ * F_A (+-L0/U0^2 * 9.80665 for iGravity = +-1, -2, 3; 0 otherwise).  Main
+ * domain only; CHAPSIM_ERR_BADARG for |igravity| > 3 or a non-finite f_a. */
+int chapsim_set_buoyancy(chapsim_ctx_t* ctx, int32_t igravity, double f_a);
+/* iWeightedPre = 1 (src/RHS_MOM_EXPLICIT_io.f90:103-159, src/DIVG.f90:78-82):
+ * pr0_1 = PR0_io(:,:,:,1), pr0_2 = PR0_io(:,:,:,2), each (NCL1, 0:NCL2+1,
+ * NCL3) host arrays (the reference sets both to PR_io at the start,
+ * src/FLOWSTART.f90:83-85, and keeps them).  The pressure gradient becomes
+ * ((PR0_2 diff)(1/4 - eps) + (PR0_1 diff)/2 + (PR diff)(1/4 + eps)) and DIVG_io
+ * divides by (1/4 + eps), eps = pres_epslon = 0.001.  Both NULL turns it off;
+ * one NULL is CHAPSIM_ERR_BADARG.  Main domain only. */
+int chapsim_upload_weighted_pressure(chapsim_ctx_t* ctx, const double* pr0_1, const double* pr0_2);
 /* DIVGCK_io (src/DIVGCK.f90:60-184), x-periodic main domain: MAXDIVGV_io, the
  * max over the interior of |div G + DrhoDtP| (the three ranges coincide). */
 int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv);

@@ -68,6 +68,11 @@ typedef struct {
     double *DH, *ENTH, *TEMP, *KAPPA, *HCP, *RHSE, *RHSE0, *G0;
     double QW_BOT, QW_TOP, CTHECD, DHMIN, DHMAX;
     int prop_err;
+    /* buoyancy (thermal_gravity, src/Flow_State.f90:95-125): iGravity and F_A */
+    int igrav;
+    double F_A;
+    /* iWeightedPre = 1: PR0_io(:,:,:,1:2) (src/FLOWSTART.f90:83-85), NULL when off */
+    double *PR0A, *PR0B;
 } orc_t;
 
 #define FOFF(o, i, j, k) ((size_t)((i) - 1) + (size_t)(o)->L * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
@@ -316,6 +321,7 @@ void orc_destroy(orc_t* o) {
     free(o->Vini); free(o->AK1); free(o->AK3);
     free(o->Q); free(o->PR); free(o->CONVH0); free(o->QTMP); free(o->DPH); free(o->RHSLLPHI); free(o->RHS);
     free(o->SRe); free(o->SIm);
+    free(o->PR0A); free(o->PR0B);
     free(o->G); free(o->EXPLT0); free(o->RHO); free(o->MU0); free(o->MU); free(o->DSTG); free(o->MUSTG);
     free(o->DIVU); free(o->DRHODT); free(o->DEN); free(o->DRHOI);
     free(o->DH); free(o->ENTH); free(o->TEMP); free(o->KAPPA); free(o->HCP); free(o->RHSE); free(o->RHSE0); free(o->G0);
@@ -1299,8 +1305,22 @@ static void io_viscous_z(orc_t* o) {
     }
 }
 
-/* RHS_MOM_EXPLICIT_io(NS, IDR) (src/RHS_MOM_EXPLICIT_io.f90:11-304),      */
-/* explicit scheme, no gravity, no weighted pressure.                     */
+/* iWeightedPre: pres_epslon (src/modules.f90:483) */
+#define PRES_EPSLON 0.001
+
+/* Pressure-gradient term PGM of RHS_MOM_EXPLICIT_io (:103-159) between the */
+/* points a and b (b the lower neighbour), with the weighted-pressure blend  */
+/* of PR0_io(:,:,:,2), PR0_io(:,:,:,1) and PR_io when iWeightedPre = 1.      */
+static inline double io_pgm(const orc_t* o, size_t a, size_t b, double COE2) {
+    if (o->PR0A)
+        return ((o->PR0B[a] - o->PR0B[b]) * (0.25 - PRES_EPSLON) + (o->PR0A[a] - o->PR0A[b]) * 0.5 +
+                (o->PR[a] - o->PR[b]) * (0.25 + PRES_EPSLON)) * COE2;
+    return (o->PR[a] - o->PR[b]) * COE2;
+}
+
+/* RHS_MOM_EXPLICIT_io(NS, IDR) (src/RHS_MOM_EXPLICIT_io.f90:11-304), plane */
+/* channel (RNDI1 = RCCI1 = 1): RK combination, pressure gradient (weighted  */
+/* or not), buoyancy, bulk forcing, save-back.                               */
 static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
     int L = o->L, M = o->M, N = o->N;
     int NYI = (IDR == 2) ? 2 : 1;
@@ -1337,7 +1357,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
         for (int KC = 1; KC <= N; ++KC)
             for (int JC = 1; JC <= M; ++JC)
                 for (int IC = 1; IC <= L; ++IC) {
-                    double PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IMV(o, IC), JC, KC)) * COE2;
+                    double PGM = io_pgm(o, FOFF(o, IC, JC, KC), FOFF(o, IMV(o, IC), JC, KC), COE2);
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
                 }
     } else if (IDR == 2) {
@@ -1346,7 +1366,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
             double COE2 = o->TALP[NS] * DT * o->DYCI[JC] / 1.0;
             for (int KC = 1; KC <= N; ++KC)
                 for (int IC = 1; IC <= L; ++IC) {
-                    double PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IC, JC - 1, KC)) * COE2;
+                    double PGM = io_pgm(o, FOFF(o, IC, JC, KC), FOFF(o, IC, JC - 1, KC), COE2);
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
                 }
         }
@@ -1357,10 +1377,23 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
             int KM = KMV(o, KC);
             for (int JC = 1; JC <= M; ++JC)
                 for (int IC = 1; IC <= L; ++IC) {
-                    double PGM = (F3(o->PR, o, IC, JC, KC) - F3(o->PR, o, IC, JC, KM)) * COE2;
+                    double PGM = io_pgm(o, FOFF(o, IC, JC, KC), FOFF(o, IC, JC, KM), COE2);
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
                 }
         }
+    }
+    /* buoyancy (:161-226): D_STG(:,:,:,IDR) * TALP*DT*F_A on the component |iGravity| */
+    /* (the 1/RNDI1, 1/RCCI1 factors of the y and z directions are 1 in the channel)   */
+    if (abs(o->igrav) == IDR) {
+        double COE2 = o->TALP[NS] * DT * o->F_A;
+        int JS = IDR == 2 ? 2 : 1;
+#pragma omp parallel for schedule(static)
+        for (int KC = 1; KC <= N; ++KC)
+            for (int JC = JS; JC <= M; ++JC) {
+                double C2 = IDR == 1 ? COE2 : COE2 / 1.0;
+                for (int IC = 1; IC <= L; ++IC)
+                    F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) + DSV(o, IC, JC, KC, IDR) * C2;
+            }
     }
     if (IDR == 1) {
         double DPGRNS = 0.0;
@@ -1398,10 +1431,10 @@ static void io_massflux_calc(orc_t* o) {
             }
 }
 
-/* DIVG_io (src/DIVG.f90:54-137), iWeightedPre = 0 */
+/* DIVG_io (src/DIVG.f90:54-137) */
 static void io_divg(orc_t* o, int NS) {
     int L = o->L, M = o->M, N = o->N;
-    double COE0 = 1.0 / o->DT / o->TALP[NS];
+    double COE0 = o->PR0A ? 1.0 / o->DT / o->TALP[NS] / (0.25 + PRES_EPSLON) : 1.0 / o->DT / o->TALP[NS];
     memset(o->RHSLLPHI, 0, FSZ(o) * sizeof(double));
 #pragma omp parallel for schedule(static)
     for (int JC = 1; JC <= M; ++JC) {
@@ -1484,6 +1517,26 @@ static void io_prcalc_massflux_update(orc_t* o, int NS) {
 #define DRV(o, i, j, k, c) ((o)->DRHOI[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
 
 void orc_io_set_vis_scheme(orc_t* o, int ivis) { o->ivis = ivis ? 1 : 0; }
+
+/* thermal_gravity (src/Flow_State.f90:95-125): iGravity selects the momentum */
+/* component that takes the buoyancy term, F_A its coefficient.              */
+void orc_io_set_buoyancy(orc_t* o, int igravity, double f_a) {
+    o->igrav = igravity;
+    o->F_A = f_a;
+}
+
+/* iWeightedPre = 1 with PR0_io(:,:,:,1) = pr0_1 and PR0_io(:,:,:,2) = pr0_2  */
+/* (padded layout); NULL turns it off.                                       */
+void orc_io_set_weighted_pressure(orc_t* o, const double* pr0_1, const double* pr0_2) {
+    free(o->PR0A);
+    free(o->PR0B);
+    o->PR0A = o->PR0B = NULL;
+    if (!pr0_1 || !pr0_2) return;
+    o->PR0A = dalloc(FSZ(o));
+    o->PR0B = dalloc(FSZ(o));
+    memcpy(o->PR0A, pr0_1, FSZ(o) * sizeof(double));
+    memcpy(o->PR0B, pr0_2, FSZ(o) * sizeof(double));
+}
 
 /* max |DRHOI_STG| over the interior and the v wall rows (0 by construction) */
 double orc_io_drhoi_maxabs(const orc_t* o) {

@@ -77,6 +77,8 @@ def lib():
         L.orc_io_run_steps.restype = ctypes.c_int
         L.orc_io_monitor.argtypes = [ctypes.c_void_p, _dp]
         L.orc_io_set_vis_scheme.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_io_set_buoyancy.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
+        L.orc_io_set_weighted_pressure.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_io_divgck.argtypes = [ctypes.c_void_p]
         L.orc_io_divgck.restype = ctypes.c_double
         L.orc_io_drhoi_maxabs.argtypes = [ctypes.c_void_p]
@@ -231,6 +233,20 @@ class Oracle:
     # ---- IO (main-domain) path, explicit (iVisScheme 0) or Crank-Nicolson (1) viscous terms ----
     def io_set_vis_scheme(self, ivis):
         self._lib.orc_io_set_vis_scheme(self._h, int(ivis))
+
+    def io_set_buoyancy(self, igravity, f_a):
+        """thermal_gravity: the buoyancy term D_STG * TALP*DT*F_A on component |iGravity|."""
+        self._lib.orc_io_set_buoyancy(self._h, int(igravity), float(f_a))
+
+    def io_set_weighted_pressure(self, pr0_1=None, pr0_2=None):
+        """iWeightedPre = 1 with the two PR0_io layers (padded (N, M+2, L)); None turns it off."""
+        if pr0_1 is None:
+            self._lib.orc_io_set_weighted_pressure(self._h, None, None)
+            return
+        a = np.ascontiguousarray(pr0_1, np.float64)
+        b = np.ascontiguousarray(pr0_2 if pr0_2 is not None else pr0_1, np.float64)
+        assert a.shape == self.field_shape() and b.shape == self.field_shape()
+        self._lib.orc_io_set_weighted_pressure(self._h, _p(a), _p(b))
 
     def io_drhoi_maxabs(self):
         return self._lib.orc_io_drhoi_maxabs(self._h)

@@ -1,0 +1,208 @@
+"""Parity of the kernel sets the bench times, at the grids it times them on.
+
+The autotuner picks, per grid and precision, one of three Poisson y-solves
+(warp Thomas/PCR hybrid, sequential Thomas, two-way elimination), one of
+three right-hand-side + x-sweep forms (fused, split, fused with bulk-copy
+staging) and one of two pressure stages (chained x/z transforms, fused plane
+transforms where a plane fits one block).  Every combination it can select
+is run here on the bench's own workloads, with the bench's DT0 and CFL
+(dt follows the CFL rule of CFL_tg / BCAST_COMM_STEP, src/CFL.f90:13-52,
+src/SOLVE.f90:154-211), and compared with the FP64 oracle run once per grid:
+
+* 128^3, 4pi x 2 x 4pi/3, REN 2800: the NS = 0 projection and 10 RK3 steps;
+  U, V, W, P and CONVH0 within 1e-11 relative (max-norm of the difference
+  over the max-norm of the oracle field), dt within 1e-13, max|div u| <= 1e-12.
+* 384 x 256 x 384, 2pi x 2 x pi, REN 6875: the projection and 2 steps, same
+  bounds (max|div u| <= 1e-11 at this grid, whose 1/dy is 4x larger).
+* Mixed precision with the tuner's choice at both grids against the same
+  FP64 oracle: u, v, w within 1e-5, P (modulo its mean) within 3e-3.
+* The heated main domain of the bench (256 x 192 x 128, Crank-Nicolson
+  momentum, energy equation, table-search properties): 2 steps, every flow
+  and thermal field within 1e-10, P modulo its mean.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle as orc
+from oracle import Oracle
+from chapsim import gpu
+from chapsim.mesh import channel_setup
+from chapsim.fields import initial_field
+import bench
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-11
+THREADS = os.cpu_count() or 8
+DTMIN = 1e-6
+
+# every selectable combination: y-solve (warp 0, sequential 1, two-way 16),
+# right-hand side (fused 0, split 2, bulk-staged 4), pressure (chained 0, plane 8)
+COMBOS = [y | r | p for y in (0, 1, 16) for r in (0, 2, 4) for p in (0, 8)]
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _workload(name):
+    L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = bench.WORKLOADS[name]
+    return dict(L=L, M=M, N=N, HX=HX, HZ=HZ, STR2=STR2, REN=REN, DT0=DT0, CFLGV=CFLGV)
+
+
+def _oracle_run(w, nsteps):
+    s = channel_setup(w["L"], w["M"], w["N"], w["HX"], w["HZ"], w["STR2"], w["REN"])
+    Q, PR = initial_field(s, 1973, 0.1)
+    o = Oracle(w["L"], w["M"], w["N"], w["HX"], w["HZ"], w["STR2"], w["REN"], DT0=w["DT0"], DTMIN=DTMIN,
+               CFLGV=w["CFLGV"], threads=THREADS)
+    o.set_fields(Q, PR)
+    o.set_dt(w["DT0"])
+    o.substep(0)
+    rc, dts = o.run_steps(nsteps)
+    assert rc == 0
+    Qo, PRo, H0o = o.get_fields()
+    div = o.divgck()
+    o.close()
+    return {"s": s, "Q0": Q, "PR0": PR, "Q": Qo, "PR": PRo, "H0": H0o, "dt": float(dts[-1]), "div": div}
+
+
+def _gpu_run(w, ref, nsteps, force, precision="fp64"):
+    c = gpu.ChannelTG(ref["s"], precision=precision)
+    c.upload(ref["Q0"], ref["PR0"])
+    c.set_dt(w["DT0"])
+    c.SOLVERRK3_MOM_tg(0)
+    choice, _ = c.autotune(force=force)
+    dt, _ = c.advance(nsteps, w["DT0"], DTMIN, w["CFLGV"])
+    Qg, PRg, H0g = c.download(want_h0=True)
+    div = c.DIVGCK_tg()
+    c.close()
+    return choice, dt, Qg, PRg, H0g, div
+
+
+def _check_fp64(ref, got, tol, divtol):
+    choice, dt, Qg, PRg, H0g, div = got
+    M = ref["s"].M
+    errs = {"U": rel(Qg[0], ref["Q"][0]), "V": rel(Qg[1], ref["Q"][1]), "W": rel(Qg[2], ref["Q"][2]),
+            "P": rel(PRg[:, 1:M + 1], ref["PR"][:, 1:M + 1]),
+            "H0": rel(H0g, ref["H0"][:, :, 1:M + 1, :])}
+    print("choice", choice, "errors", errs, "dt", dt, "max div", div)
+    for k, v in errs.items():
+        assert v <= tol, (choice, k, v, errs)
+    assert abs(dt - ref["dt"]) <= 1e-13 * ref["dt"], (dt, ref["dt"])
+    assert div <= divtol
+
+
+def _check_mixed(ref, got):
+    choice, dt, Qg, PRg, _h0, div = got
+    M = ref["s"].M
+    errs = {n: rel(Qg[i][:, 1:M + 1], ref["Q"][i][:, 1:M + 1]) for i, n in enumerate("uvw")}
+    pg = PRg[:, 1:M + 1] - PRg[:, 1:M + 1].mean()
+    po = ref["PR"][:, 1:M + 1] - ref["PR"][:, 1:M + 1].mean()
+    errs["p"] = rel(pg, po)
+    print("mixed choice", choice, "errors vs FP64 oracle", errs, "max div", div)
+    for k in "uvw":
+        assert errs[k] <= 1e-5, (k, errs)
+    assert errs["p"] <= 3e-3
+    assert abs(dt - ref["dt"]) <= 1e-4 * ref["dt"]
+    assert div <= 1e-5
+
+
+# ------------------------------------------------------------------ 128^3
+C2 = "channel128_retau180_fp64"
+
+
+@pytest.fixture(scope="module")
+def c2_ref():
+    return _oracle_run(_workload(C2), 10)
+
+
+def test_c2_oracle_is_divergence_free(c2_ref):
+    assert c2_ref["div"] <= 1e-12
+
+
+@pytest.mark.parametrize("force", COMBOS)
+def test_c2_every_variant_ten_steps(c2_ref, force):
+    w = _workload(C2)
+    got = _gpu_run(w, c2_ref, 10, force)
+    exp = force if (force & 8) == 0 or got[0] & 8 else force & ~8
+    assert got[0] == exp, (got[0], force)
+    _check_fp64(c2_ref, got, TOL_STEP, 1e-12)
+
+
+def test_c2_tuner_choice_ten_steps(c2_ref):
+    w = _workload(C2)
+    _check_fp64(c2_ref, _gpu_run(w, c2_ref, 10, -1), TOL_STEP, 1e-12)
+
+
+def test_c2_mixed_tuner_choice_ten_steps(c2_ref):
+    w = _workload(C2)
+    _check_mixed(c2_ref, _gpu_run(w, c2_ref, 10, -1, precision="mixed"))
+
+
+# ------------------------------------------------------------------ 384 x 256 x 384
+C3 = "channel384x256x384_retau395_fp64"
+
+
+@pytest.fixture(scope="module")
+def c3_ref():
+    return _oracle_run(_workload(C3), 2)
+
+
+@pytest.mark.parametrize("force", sorted({c & ~8 for c in COMBOS}) + [-1])
+def test_c3_variants_two_steps(c3_ref, force):
+    w = _workload(C3)
+    got = _gpu_run(w, c3_ref, 2, force)
+    if force >= 0:
+        # the bulk-staged form falls back to the split one where its stages do not fit
+        assert got[0] == force or ((force & 6) == 4 and got[0] == (force & ~6) | 2), (got[0], force)
+    _check_fp64(c3_ref, got, TOL_STEP, 1e-11)
+
+
+def test_c3_mixed_tuner_choice_two_steps(c3_ref):
+    w = _workload(C3)
+    _check_mixed(c3_ref, _gpu_run(w, c3_ref, 2, -1, precision="mixed"))
+
+
+# ------------------------------------------------------------------ heated main domain
+def test_heated_bench_grid_two_steps():
+    h = bench.HEATED
+    L, M, N = h["L"], h["M"], h["N"]
+    s, Q, PR, tab, cthecd, DH = bench.heated_case()
+    ones = np.ones_like(PR)
+    o = Oracle(L, M, N, h["HX"], h["HZ"], h["STR2"], h["REN"], DT0=h["DT0"], DTMIN=DTMIN, CFLGV=h["CFLGV"],
+               threads=THREADS)
+    o.io_set_fields(Q, PR, ones, ones, ones)
+    o.io_set_vis_scheme(1)
+    ot = orc.PropTable(tab.lists)
+    o.thermal_enable(ot, DH, h["qw"], h["qw"], cthecd)
+    o.set_dt(h["DT0"])
+    rc, _ = o.io_run_steps(2)
+    assert rc == 0
+    Go, Qo, Po = o.io_get_fields()
+    to = o.thermal_get()
+    o.close()
+    ch = gpu.ChannelIO(s, ivisscheme=gpu.VIS_IMPLICIT)
+    ch.upload_io(Q, PR, ones, ones, ones)
+    ch.set_dt(h["DT0"])
+    ch.thermal_init(tab, DH, h["qw"], h["qw"], cthecd)
+    ch.advance(2, h["DT0"], DTMIN, h["CFLGV"])
+    Gg, Qg, Pg = ch.download_io()
+    tg = ch.download_thermal()
+    dg = ch.DIVGCK_io()
+    ch.close()
+    errs = {}
+    for comp in range(3):
+        errs["G%d" % comp] = rel(Gg[comp][:, 1:M + 1], Go[comp][:, 1:M + 1])
+        errs["Q%d" % comp] = rel(Qg[comp][:, 1:M + 1], Qo[comp][:, 1:M + 1])
+    pg = Pg[:, 1:M + 1] - Pg[:, 1:M + 1].mean()
+    po = Po[:, 1:M + 1] - Po[:, 1:M + 1].mean()
+    errs["P"] = rel(pg, po)
+    for k in ("DH", "T", "D", "M"):
+        errs[k] = rel(tg[k], to[k])
+    print("heated 256x192x128 errors after 2 steps", errs, "max|div G + drho/dt|", dg)
+    for k, v in errs.items():
+        assert v <= 1e-10, (k, v, errs)
+    assert dg <= 1e-11

@@ -55,10 +55,12 @@ def test_ysolve_variants_match_oracle(kind):
     o2.set_dt(2e-3)
     o2.run_steps(10)
     c.advance(10, 2e-3, 1e-6, 0.5)
-    Qg, _ = c.download()
-    Qo, _, _ = o2.get_fields()
+    Qg, PRg, H0g = c.download(want_h0=True)
+    Qo, PRo, H0o = o2.get_fields()
     for i in range(3):
         assert rel(Qg[i][:, 1:M + 1], Qo[i][:, 1:M + 1]) <= 1e-11
+    assert rel(PRg[:, 1:M + 1], PRo[:, 1:M + 1]) <= 1e-11
+    assert rel(H0g, H0o[:, :, 1:M + 1, :]) <= 1e-11
     c.close()
 
 

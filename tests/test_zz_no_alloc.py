@@ -113,3 +113,52 @@ def test_noalloc_status_counter_is_cleared_between_calls():
     rc, out = _noalloc(A, B, C, R, None, cyclic=False)
     assert rc == 0, _err()
     assert _close(out, ref)
+
+
+def test_noalloc_strided_subblock_against_oracle():
+    """Lines inside a larger caller-owned device array, with padded strides:
+    rows of a (48, 80) block with line_stride 80 > n, and every other column
+    of it (line_stride 2, elem_stride 80, neither 1 nor the line count).
+    The solution matches the oracle's recurrences (TDMAIJI_CYC,
+    src/TDMAIJI_CYC.f90:67-157; TDMAIJJ_nonCYC, src/TDMAIJJ_nonCYC.f90:67-123)
+    and no entry outside the lines is read or written: the coefficient
+    padding holds NaN and the right-hand side's padding a sentinel."""
+    import torch
+    import oracle as orc
+    rng = np.random.default_rng(31)
+    rows, cols = 48, 80
+    cases = [
+        # (first offset, nlines, line_stride, elem_stride, n, cyclic)
+        (3 * cols + 5, 40, cols, 1, 60, True),
+        (2 * cols + 1, 30, 2, cols, 45, False),
+    ]
+    for off, nl, ls, es, n, cyc in cases:
+        idx = off + np.arange(nl)[:, None] * ls + np.arange(n)[None, :] * es
+        assert idx.max() < rows * cols and len(np.unique(idx)) == idx.size
+        coef = []
+        for lo, hi in ((-1.0, 0.0), (2.5, 3.5), (-1.0, 0.0)):
+            x = np.full(rows * cols, np.nan)
+            x[idx] = rng.uniform(lo, hi, idx.shape)
+            coef.append(x)
+        r = np.full(rows * cols, 12345.0)
+        r[idx] = rng.standard_normal(idx.shape)
+        dA, dB, dC, dR = (_dev(x) for x in (*coef, r))
+        torch.cuda.synchronize()
+        rc = _lib().chapsim_tdma_lines_noalloc(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), dR.data_ptr(), None,
+                                               nl, ls, es, n, 1 if cyc else 0,
+                                               torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert rc == 0, _err()
+        out = dR.cpu().numpy()
+        pad = np.ones(rows * cols, bool)
+        pad[idx] = False
+        assert np.all(out[pad] == 12345.0)
+        for l in range(nl):
+            a, b, c, rr = (x[idx[l]].copy() for x in (*coef, r))
+            if cyc:
+                ref = orc.tdma_cyc(a, b, c, rr)
+            else:
+                a[0] = 0.0
+                c[-1] = 0.0
+                ref = orc.tdma_noncyc(a, b, c, rr)
+            assert _close(out[idx[l]], ref), (l, cyc)
