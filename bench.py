@@ -322,10 +322,12 @@ def kernel_bytes(L, precision="fp64"):
         "k_ysweep": 9 * w,                 # RHS x3, Q x3 in; Q x3 out
         "k_div_fftx": 4 * w + spec,        # Q x3 in; RHSLLPHI, spectrum out
         "k_div_fft2": 4 * w + spec,        # the same with the z transforms of the plane
+        "k_div_fft2c": 4 * w + spec,       # the same, the plane split over a thread-block cluster
         "k_fftz_fwd": 2 * spec, "k_fftz_inv": 2 * spec,
         "k_ysolve_warp": 2 * spec, "k_ysolve_seq": 2 * spec, "k_ysolve_2w": 2 * spec,
         "k_fftx_inv": spec + w,            # spectrum in; DPH out
         "k_fft2_inv": spec + w,            # the same with the inverse z transforms of the plane
+        "k_fft2c_inv": spec + w,           # the same, the plane split over a thread-block cluster
         "k_correct": 10 * w,               # DPH, Q x3, PR, RHSLLPHI in; Q x3, PR out
     }
 
@@ -523,11 +525,17 @@ def run_ensemble(args):
     torch.cuda.synchronize(local)
     if dist is not None:
         dist.barrier()
-    t0 = time.perf_counter()
+    # each member's K steps timed with CUDA events on its own stream, one member after another
+    ms_seq = 0.0
     for c in seq:
+        st_c = torch.cuda.ExternalStream(c.stream_handle(), device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st_c)
         c.advance(args.steps, DT0, DTMIN, CFLGV)
-    torch.cuda.synchronize(local)
-    t_seq = max_over_ranks(time.perf_counter() - t0, dist, f"cuda:{local}")
+        e1.record(st_c)
+        torch.cuda.synchronize(local)
+        ms_seq += e0.elapsed_time(e1)
+    t_seq = max_over_ranks(ms_seq / 1000.0, dist, f"cuda:{local}")
     for c in seq:
         c.close()
     # batched: one graph per step over all members
@@ -559,7 +567,9 @@ def run_ensemble(args):
                    "precision": args.precision, "total_points": pts,
                    "autotuned_choice_bits": [t[0] for t in tune], "l2": "no flush: members total %.0f MB" % (pts * 8 * 20 / 1e6)},
         "sequential": {"value": pts * args.steps * ws / t_seq, "unit": UNIT, "ms_per_step": 1000.0 * t_seq / args.steps,
-                       "timing": "wall clock around the members' own graph replays, one member after another"},
+                       "timing": "sum over the members of CUDA-event time around each member's own K graph "
+                                 "replays on its stream, one member after another (the batched leg is timed "
+                                 "with CUDA events on the ensemble stream)"},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }

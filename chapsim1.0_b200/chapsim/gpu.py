@@ -50,14 +50,31 @@ KERNEL_SLOTS = ["k_cfl", "k_dt_factors"] + ["k_rhs_xsweep", "k_zsweep", "k_yswee
                                     "k_fftz_inv", "k_fftx_inv", "k_correct"] * 3
 
 
-def step_kernel_slots(choice: int = 0):
+# (n1, n2) split of the supported FFT lengths (csrc/fft.cuh: fft4s_split)
+FFT_SPLIT = {32: (4, 8), 64: (8, 8), 96: (12, 8), 128: (16, 8), 192: (16, 12), 256: (16, 16), 384: (16, 24)}
+
+
+def plane_in_one_block(L, N, precision="fp64"):
+    """True when the fused plane transforms of an (L, N) plane run as one block
+    (k_div_fft2 / k_fft2_inv), False when they run as a thread-block cluster
+    (k_div_fft2c / k_fft2c_inv): the rule of plane_fft_ok in csrc/chapsim_gpu.cu."""
+    if L not in (64, 96, 128, 192) or N not in (64, 96, 128, 192):
+        return False
+    words = max((N // 2) * (L + FFT_SPLIT[L][1] + 1), (L // 2 + 1) * (N + FFT_SPLIT[N][1] + 1))
+    return words * (16 if precision == "fp64" else 8) <= 220 * 1024
+
+
+def step_kernel_slots(choice: int = 0, plane_cluster: bool = False):
     """Names of the kernels in the profiling slots of one periodic-channel step
     for the variant bits `choice` of chapsim_autotune.  The split right-hand
     side times k_rhs_point and k_xsweep in one slot; with the fused plane
-    transforms the two z-transform slots stay empty and are named None."""
+    transforms (one block per row, or a cluster per row when plane_cluster)
+    the two z-transform slots stay empty and are named None."""
     rhs = {0: "k_rhs_xsweep", 1: "k_rhs_point+k_xsweep", 2: "k_rhs_xsweep_bulk"}[(choice >> 1) & 3]
     ys = "k_ysolve_seq" if choice & 1 else ("k_ysolve_2w" if choice & 16 else "k_ysolve_warp")
-    if choice & 8:
+    if choice & 8 and plane_cluster:
+        pre = ["k_div_fft2c", None, ys, None, "k_fft2c_inv"]
+    elif choice & 8:
         pre = ["k_div_fft2", None, ys, None, "k_fft2_inv"]
     else:
         pre = ["k_div_fftx", "k_fftz_fwd", ys, "k_fftz_inv", "k_fftx_inv"]
@@ -424,7 +441,7 @@ class ChannelTG:
     def kernel_slots(self):
         """Names of the kernels in the slots of one step, in the order
         chapsim_profile_steps reports them, for the variants in use."""
-        return step_kernel_slots(self.choice)
+        return step_kernel_slots(self.choice, not plane_in_one_block(self.L, self.N, self.precision))
 
     def profile_steps(self, nsteps, DT0, DTMIN, CFLGV):
         """Per-kernel durations (ms, summed over nsteps) keyed by the name of the

@@ -20,6 +20,7 @@
 #include "stats.cuh"
 #include "rhs_bulk.cuh"
 #include "plane_fft.cuh"
+#include "plane_fft_cluster.cuh"
 #include "thermo.cuh"
 #include "thermal.cuh"
 #include "mlp.cuh"
@@ -146,6 +147,7 @@ struct chapsim_ctx {
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
+    bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
     int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
     bool pdl = true;              // step kernels launched with programmatic dependent launch
     double2* SP = nullptr;
@@ -295,7 +297,10 @@ cudaError_t upload_small_twiddles() {
     }
     return e;
 }
-size_t smem_yw(const Geo& g) { return (size_t)(YW_L * (g.M + 33)) * sizeof(double2); }
+template <typename C>
+size_t smem_yw(const Geo& g) {
+    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (sizeof(C) == 16 ? 0 : (size_t)g.M * sizeof(double2));
+}
 
 // forward declaration: DISPATCH_S is defined below
 template <typename C = double2> void launch_ysolve_warp(chapsim_ctx* ctx);
@@ -395,8 +400,8 @@ template <typename C>
 void launch_ysolve_warp(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
-    const int nb = (int)((nl + YW_L - 1) / YW_L);
-    DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_warp<S, C>, nb, YW_NT, smem_yw(g), ctx->stream, g, spec<C>(ctx))));
+    const int nb = (int)std::min<long long>((nl + YW_L - 1) / YW_L, ctx->nsm);  // persistent: one block per SM
+    DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_warp<S, C>, nb, YW_NT, smem_yw<C>(g), ctx->stream, g, spec<C>(ctx))));
 }
 
 // Momentum-stage arrays of the context in the real type R of its precision.
@@ -422,12 +427,16 @@ int configure_momentum(chapsim_ctx* ctx) {
     using C = SpecT<R>;
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw<C>(g))));
     CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
     CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
     if (ctx->domain == 1 && plane_fft_ok<C>(g))
         P2_DISPATCH(g.L, g.N, CK((plane_fft_attrs<R, XN1, XN2, ZN1, ZN2>(set_smem_void, smem_p2<C>(g)))));
+    // planes too large for one block: the cluster form, where the device can hold one of its clusters
+    ctx->p2c = false;
+    if (ctx->domain == 1 && !plane_fft_ok<C>(g) && plane_fft_cluster_shape(g.L, g.N))
+        P2C_DISPATCH(g.L, g.N, (ctx->p2c = plane_fft_cluster_setup<R, XN1, XN2, ZN1, ZN2>(g)));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, C>, smem_fz<C>(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, C>, smem_fz<C>(g))));
     return CHAPSIM_OK;
@@ -441,7 +450,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, double2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw<double2>(g))));
     CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
     CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
@@ -521,13 +530,21 @@ void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
     using C = SpecT<R>;
     C* sp = spec<C>(ctx);
     if (ctx->plane_kind == 1) {
-        P2_DISPATCH(g.L, g.N, (plane_fft_fwd<R, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, f.Q, f.RHSLL, sp, ctx->st, ns, smem_p2<C>(g), s)));
+        if (ctx->p2c) {
+            P2C_DISPATCH(g.L, g.N, (plane_fft_cluster_fwd<R, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, f.Q, f.RHSLL, sp, ctx->st, ns, s)));
+        } else {
+            P2_DISPATCH(g.L, g.N, (plane_fft_fwd<R, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, f.Q, f.RHSLL, sp, ctx->st, ns, smem_p2<C>(g), s)));
+        }
         prof_mark(ctx);
         prof_mark(ctx);
         launch_ysolve<C>(ctx);
         prof_mark(ctx);
         prof_mark(ctx);
-        P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, sp, dph<R>(ctx), smem_p2<C>(g), s)));
+        if (ctx->p2c) {
+            P2C_DISPATCH(g.L, g.N, (plane_fft_cluster_inv<C, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, sp, dph<R>(ctx), s)));
+        } else {
+            P2_DISPATCH(g.L, g.N, (plane_fft_inv<C, XN1, XN2, ZN1, ZN2>(ctx->pdl, g, sp, dph<R>(ctx), smem_p2<C>(g), s)));
+        }
         prof_mark(ctx);
         ctx->launches += 3;
         return;
@@ -571,7 +588,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R>, gry, SWEEP_NT, smem_y<R>(g), s, g, f.Q, f.RHS, ctx->st, fac, ns)));
     prof_mark(ctx);
     launch_pressure<R>(ctx, f, ns);
-    const long long tot = (long long)g.L * g.M * g.N;
+    const long long tot = (long long)g.L * g.M * g.N / V16<R>::W;  // one thread per 16-byte group of an x line
     launch_pdl(ctx->pdl, k_correct<R>, (int)((tot + CR_NT - 1) / CR_NT), CR_NT, 0, s, g, f.Q, f.PR, dph<R>(ctx), f.RHSLL, ctx->st, ns);
     prof_mark(ctx);
     ctx->launches += 4;
@@ -2075,7 +2092,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     float tp[2] = {0.f, 1e30f};
     if (ctx->domain == 1) {
         const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
-        const bool p2 = mixed ? plane_fft_ok<float2>(g) : plane_fft_ok<double2>(g);
+        bool p2 = (mixed ? plane_fft_ok<float2>(g) : plane_fft_ok<double2>(g)) || ctx->p2c;
         for (int kind = 0; kind < (p2 ? 2 : 1); ++kind) {
             ctx->plane_kind = kind;
             auto one = [&]() {
@@ -2083,6 +2100,13 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
                 else launch_pressure<double>(ctx, step_fields<double>(ctx), 1);
             };
             one();
+            if (kind == 1 && ctx->p2c && cudaGetLastError() != cudaSuccess) {
+                // the cluster launch was refused (configuration): keep the chained transforms
+                ctx->p2c = false;
+                p2 = false;
+                tp[1] = 1e30f;
+                break;
+            }
             CK(cudaEventRecord(e0, s));
             for (int r = 0; r < reps; ++r) one();
             CK(cudaEventRecord(e1, s));

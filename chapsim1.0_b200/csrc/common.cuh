@@ -85,6 +85,24 @@ __device__ __forceinline__ void io_decode(const Geo& g, long long t, int& i, int
     j = 1 + (int)(r - kk * M);
     k = (int)kk;
 }
+// 16-byte vector access of W = 16 / sizeof(R) consecutive elements (float4 or
+// double2); p must be 16-byte aligned
+template <typename R> struct V16 { static constexpr int W = 16 / (int)sizeof(R); };
+__device__ __forceinline__ void ld16(const float* p, float (&a)[4]) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+__device__ __forceinline__ void ld16(const double* p, double (&a)[2]) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    a[0] = v.x; a[1] = v.y;
+}
+__device__ __forceinline__ void st16(float* p, const float (&a)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
+}
+__device__ __forceinline__ void st16(double* p, const double (&a)[2]) {
+    *reinterpret_cast<double2*>(p) = make_double2(a[0], a[1]);
+}
+
 __device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
 __device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
 

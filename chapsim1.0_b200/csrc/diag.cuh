@@ -23,7 +23,9 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, d
     const int nlines = M * N;
     double mx = 0.0;
     bool bad = false;
-    // one warp per x line (j, k): the line's indices are decoded once and every load is contiguous
+    // one warp per x line (j, k): the line's indices are decoded once; each lane
+    // reads VW consecutive points of every row with 16-byte loads
+    constexpr int VW = V16<R>::W;
     for (int line = blockIdx.x * (DG_NT / 32) + warp; line < nlines; line += gridDim.x * (DG_NT / 32)) {
         const int j = 1 + line % M, k = line / M;
         const long long c0 = pidx(g, 0, j, k);
@@ -32,14 +34,24 @@ __global__ void __launch_bounds__(DG_NT) k_cfl(Geo g, const R* __restrict__ Q, d
         const R* W = Q + 2 * g.FS + c0;
         const R* Wkp = Q + 2 * g.FS + pidx(g, 0, j, wrapp(k, N));
         const double cy = g.dyfi[j];
-#pragma unroll 4
-        for (int i = lane; i < L; i += 32) {
-            const int ip = i + 1 == L ? 0 : i + 1;
-            const double q = (fabs(((double)U[i] + (double)U[ip]) * g.dxi) +
-                              fabs(((double)V[i] + (double)V[i + L]) * cy * 1.0) +
-                              fabs(((double)W[i] + (double)Wkp[i]) * g.dzi * 1.0)) * 0.5;
-            if (!(q == q)) bad = true;
-            mx = fmax(mx, q);
+#pragma unroll 2
+        for (int i0 = lane * VW; i0 < L; i0 += 32 * VW) {
+            R u[VW], v[VW], vp[VW], w[VW], wp[VW];
+            ld16(U + i0, u);
+            ld16(V + i0, v);
+            ld16(V + i0 + L, vp);
+            ld16(W + i0, w);
+            ld16(Wkp + i0, wp);
+            const double un = U[i0 + VW == L ? 0 : i0 + VW];
+#pragma unroll
+            for (int e = 0; e < VW; ++e) {
+                const double up = e + 1 < VW ? (double)u[e + 1] : un;
+                const double q = (fabs(((double)u[e] + up) * g.dxi) +
+                                  fabs(((double)v[e] + (double)vp[e]) * cy * 1.0) +
+                                  fabs(((double)w[e] + (double)wp[e]) * g.dzi * 1.0)) * 0.5;
+                if (!(q == q)) bad = true;
+                mx = fmax(mx, q);
+            }
         }
     }
     if (bad) atomicOr(&st->err, CHS_EBIT_NAN);

@@ -155,15 +155,22 @@ struct MlpOut {
 
 constexpr int MLP_INF_SMEM = 1024 + 64 * 64 * 2 + 16 * 64 * 2 + 128 * 64 * 2;
 
-// Hardware tanh (PTX tanh.approx.f32, one MUFU operation; maximum relative
-// error about 2^-11).  Inference uses it: every hidden activation is rounded
-// to BF16 (relative 2^-9) right after, so the approximation sits below the
-// precision the tensor-core layers carry.  Training keeps tanhf, the
-// activation of the CPU oracle's gradient check.
-__device__ __forceinline__ float tanh_mufu(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
+// Hardware tanh for inference, two activations per MUFU operation (PTX
+// tanh.approx.f16x2): the pre-activations are rounded to FP16 (relative
+// 2^-11), the tanh is evaluated on the pair (maximum relative error about
+// 2^-11), and the results are widened again.  These roundings sit below the
+// BF16 rounding (2^-9) that every activation takes right after, as the
+// tensor-core operand; the pair costs one MUFU operation instead of two.
+// Training keeps tanhf, the activation of the CPU oracle's gradient check.
+__device__ __forceinline__ void tanh2_mufu(float a, float b, float& ta, float& tb) {
+    uint32_t in, out;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(in) : "f"(b), "f"(a));  // upper half b, lower half a
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(out) : "r"(in));
+    float lo, hi;
+    asm("{\n\t.reg .f16 l, h;\n\tmov.b32 {l, h}, %2;\n\tcvt.f32.f16 %0, l;\n\tcvt.f32.f16 %1, h;\n\t}"
+        : "=f"(lo), "=f"(hi) : "r"(out));
+    ta = lo;
+    tb = hi;
 }
 
 template <bool FIELD>
@@ -210,7 +217,8 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
         const float x = mlp_x(nm, v);
         float h[MLP_H];
 #pragma unroll
-        for (int i = 0; i < MLP_H; ++i) h[i] = tanh_mufu(fmaf(sw1[i], x, sb1[i]));
+        for (int i = 0; i < MLP_H; i += 2)
+            tanh2_mufu(fmaf(sw1[i], x, sb1[i]), fmaf(sw1[i + 1], x, sb1[i + 1]), h[i], h[i + 1]);
         put_row64(sA, MLP_TILE, tid, h);
         fence_async_smem();
         tc_fence_before();
@@ -231,7 +239,8 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
             tmem_ld16(tmem + lane_base + 16 * q, acc);
             tmem_ld_wait();
 #pragma unroll
-            for (int c = 0; c < 16; ++c) h[16 * q + c] = tanh_mufu(acc[c] + sb2[16 * q + c]);
+            for (int c = 0; c < 16; c += 2)
+                tanh2_mufu(acc[c] + sb2[16 * q + c], acc[c + 1] + sb2[16 * q + c + 1], h[16 * q + c], h[16 * q + c + 1]);
         }
         put_row64(sA, MLP_TILE, tid, h);
         fence_async_smem();

@@ -74,26 +74,48 @@ __global__ void __launch_bounds__(PX_NT, PX_MINB) k_div_fftx(Geo g, const R* __r
     const double coe0 = 1.0 / (st->dt * g.talp[ns]);
     const R* U = Q;
     const R* V = Q + g.FS;
-    const R* W = Q + 2 * g.FS;
+    const R* Wf = Q + 2 * g.FS;
     const double coe1 = g.dxi / 1.0;
-#pragma unroll 4
-    for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
-        const int jl = p / L, i = p - jl * L;
-        const int pair = jl >> 1, part = jl & 1;
-        double val = 0.0;
-        if (jl < nj) {
-            const int j = j0 + jl;
-            const long long c = pidx(g, i, j, k);
-            const double u = U[c], up = U[pidx(g, wrapp(i, L), j, k)];
-            const double v = V[c], vp = V[c + L];
-            const double w = W[c], wp = W[pidx(g, i, j, kp)];
-            const double coe2 = g.dyfi[j] / 1.0;
-            const double dv = (up - u) * coe1 + (vp - v) * coe2 + (wp - w) * g.dzi;
-            val = dv * coe0;
-            RHSLL[iidx(g, i, j, k)] = (R)val;
+    // one item = VW consecutive points of both rows of a packed pair, read with
+    // 16-byte loads; the pair's complex values are stored to shared memory together
+    constexpr int VW = V16<R>::W;
+    const int LV = L / VW;
+#pragma unroll 2
+    for (int p = threadIdx.x; p < np * LV; p += PX_NT) {
+        const int pair = p / LV, i0 = (p - pair * LV) * VW;
+        T val[2][VW];
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {
+            const int jl = 2 * pair + part;
+            if (jl < nj) {
+                const int j = j0 + jl;
+                const long long c = pidx(g, i0, j, k);
+                R u[VW], v[VW], vp[VW], w[VW], wp[VW], out[VW];
+                ld16(U + c, u);
+                ld16(V + c, v);
+                ld16(V + c + L, vp);
+                ld16(Wf + c, w);
+                ld16(Wf + pidx(g, i0, j, kp), wp);
+                const double un = U[pidx(g, i0 + VW == L ? 0 : i0 + VW, j, k)];  // u at i0 + VW (periodic)
+                const double coe2 = g.dyfi[j] / 1.0;
+#pragma unroll
+                for (int e = 0; e < VW; ++e) {
+                    const double uc = u[e], up = e + 1 < VW ? (double)u[e + 1] : un;
+                    const double dv = (up - uc) * coe1 + ((double)vp[e] - (double)v[e]) * coe2 +
+                                      ((double)wp[e] - (double)w[e]) * g.dzi;
+                    const double x = dv * coe0;
+                    out[e] = (R)x;
+                    val[part][e] = (T)x;
+                }
+                st16(RHSLL + iidx(g, i0, j, k), out);
+            } else {
+#pragma unroll
+                for (int e = 0; e < VW; ++e) val[part][e] = (T)0;
+            }
         }
-        C* line = smc + pair * LD;
-        if (part == 0) line[i].x = (T)val; else line[i].y = (T)val;
+        C* line = smc + pair * LD + i0;
+#pragma unroll
+        for (int e = 0; e < VW; ++e) line[e] = mkc(val[0][e], val[1][e]);
     }
     block_fft4s<N1, N2, -1>(smc, np, LD, twx_of<C>(g));
     // unpack: A_k = (Z_k + conj Z_{L-k}) / 2, B_k = (Z_k - conj Z_{L-k}) / (2i), both times 1/L
@@ -155,9 +177,11 @@ __global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, C* __restrict__ SP) {
 // its pinned first row (TDMA_PHI_COEF :225-231, :341-344, :387-389), run by
 // one lane.  Lines are staged in shared memory, line l at l*LS with row r at
 // seg_pos<S>(r), LS = M + 33: conflict-free both for the coalesced tile load
-// (16 lines per row) and for the per-lane segment access.
+// (16 lines per row) and for the per-lane segment access.  Shared memory:
+// two stages of YW_L such lines in the spectrum's type, plus M FP64 complex
+// values for the zero mode's forward sweep when that type is float2.
 #define YW_L 16
-#define YW_NT 256
+#define YW_NT 512
 
 struct PoisCoef {
     const double *am, *ac, *ap;
@@ -189,71 +213,121 @@ __global__ void k_ysolve_zero_factors(Geo g, double* __restrict__ zf) {
     }
 }
 
+// Persistent and double-buffered: each block owns every gridDim.x-th group of
+// YW_L lines.  The copies of its next group go out (cp.async into the other
+// stage) before the current group is solved and written back, so the loads
+// overlap the warps' solves and the stores.  One warp per line of a group.
+// The stage holds the spectrum's own type (float2 in the mixed-precision
+// step); a warp widens its segment to FP64 for the solve.
 template <int S, typename C>
-__global__ void __launch_bounds__(YW_NT, 2) k_ysolve_warp(Geo g, C* __restrict__ SP) {
+__global__ void __launch_bounds__(YW_NT, 1) k_ysolve_warp(Geo g, C* __restrict__ SP) {
     pdl_wait();
-    extern __shared__ double2 smc[];
-    static_assert(YW_NT % YW_L == 0, "a thread keeps one line in the staging loops");
+    extern __shared__ __align__(16) unsigned char yw_raw[];
+    static_assert(YW_NT == 32 * YW_L, "one warp per line of a group");
     const int M = 32 * S, LH = g.LH;
     const int LS = M + 33;
+    C* const stage[2] = {reinterpret_cast<C*>(yw_raw), reinterpret_cast<C*>(yw_raw) + YW_L * LS};
     const long long nl = (long long)LH * g.N;
-    const long long q0 = (long long)blockIdx.x * YW_L;
-    const int nq = (int)min((long long)YW_L, nl - q0);
+    const long long ngr = (nl + YW_L - 1) / YW_L;
     // the staging loops: thread t moves line t % YW_L, rows t / YW_L + (YW_NT / YW_L) * it
     const int ls = threadIdx.x % YW_L, js = threadIdx.x / YW_L;
-    const long long qs = q0 + ls;
-    const int kzs = (int)(qs / LH), kxs = (int)(qs - (long long)kzs * LH);
-    C* const gsrc = SP + kxs + (long long)LH * ((long long)M * kzs);
-    if (ls < nq) {
-        for (int j = js; j < M; j += YW_NT / YW_L) {
-            if constexpr (sizeof(C) == 16) cp_async16(smc + ls * LS + seg_pos<S>(j), gsrc + (long long)LH * j);
-            else smc[ls * LS + seg_pos<S>(j)] = to_d2(gsrc[(long long)LH * j]);
-        }
-    }
-    cp_async_wait_all();
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int l = warp; l < nq; l += YW_NT / 32) {
-        const long long q = q0 + l;
+    constexpr int RS = YW_NT / YW_L;  // rows per staging step
+    auto line_ptr = [&](long long q) {
         const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-        double2* base = smc + l * LS;
-        if (q == 0) {
-            // zero mode: phi(y_1) = 0 and the reference's forward/backward recurrence
-            if (lane == 0) {
-                const double* pp = g.yz;
-                const double* hz = g.yz + M;
-                double2 gp = make_double2(0.0 * pp[0], 0.0 * pp[0]);
-                base[seg_pos<S>(0)] = gp;
-#pragma unroll 4
-                for (int j = 2; j <= M; ++j) {
-                    const double2 rj = base[seg_pos<S>(j - 1)];
-                    const double am = g.amph[j], p = pp[j - 1];
-                    gp = make_double2((rj.x - am * gp.x) * p, (rj.y - am * gp.y) * p);
-                    base[seg_pos<S>(j - 1)] = gp;
-                }
-                double2 xn = gp;
-#pragma unroll 4
-                for (int j = M - 1; j >= 1; --j) {
-                    const double2 gj = base[seg_pos<S>(j - 1)];
-                    const double h = hz[j - 1];
-                    xn = make_double2(gj.x - h * xn.x, gj.y - h * xn.y);
-                    base[seg_pos<S>(j - 1)] = xn;
-                }
+        return SP + kx + (long long)LH * ((long long)M * kz);
+    };
+    auto issue = [&](long long gr, C* st) {
+        if (gr < ngr) {
+            const long long q = gr * YW_L + ls;
+            if (q < nl) {
+                const C* src = line_ptr(q);
+                for (int j = js; j < M; j += RS) cp_async_row(st + ls * LS + seg_pos<S>(j), src + (long long)LH * j);
             }
-        } else {
-            PoisCoef cf{g.amph, g.acph, g.apph, (-g.ak1[kx] / 1.0 - g.ak3[kz])};
-            double2 d[S];
-#pragma unroll
-            for (int k = 0; k < S; ++k) d[k] = base[lane * (S + 1) + k];
-            warp_tdma_c<S>(d, cf, lane);
-#pragma unroll
-            for (int k = 0; k < S; ++k) base[lane * (S + 1) + k] = d[k];
         }
+        cp_async_commit();  // an empty group past the end keeps the group count uniform
+    };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    issue(blockIdx.x, stage[0]);
+    int cur = 0;
+#pragma unroll 1
+    for (long long gr = blockIdx.x; gr < ngr; gr += gridDim.x, cur ^= 1) {
+        issue(gr + gridDim.x, stage[cur ^ 1]);
+        cp_async_wait_group<1>();  // this group's copies (all but the newest group) have landed
+        __syncthreads();
+        C* const st = stage[cur];
+        const long long q = gr * YW_L + warp;
+        if (q < nl) {
+            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+            C* base = st + warp * LS;
+            if (q == 0) {
+                // zero mode: phi(y_1) = 0 and the reference's forward/backward recurrence
+                if (lane == 0) {
+                    const double* pp = g.yz;
+                    const double* hz = g.yz + M;
+                    double2 gp = make_double2(0.0 * pp[0], 0.0 * pp[0]);
+                    base[seg_pos<S>(0)] = from_d2<C>(gp);
+                    // the forward intermediate g stays FP64: kept in the stage when C is
+                    // double2; for a float2 stage the chain runs in a second pass below
+                    if constexpr (sizeof(C) == 16) {
+#pragma unroll 4
+                        for (int j = 2; j <= M; ++j) {
+                            const double2 rj = to_d2(base[seg_pos<S>(j - 1)]);
+                            const double am = g.amph[j], p = pp[j - 1];
+                            gp = make_double2((rj.x - am * gp.x) * p, (rj.y - am * gp.y) * p);
+                            base[seg_pos<S>(j - 1)] = from_d2<C>(gp);
+                        }
+                        double2 xn = gp;
+#pragma unroll 4
+                        for (int j = M - 1; j >= 1; --j) {
+                            const double2 gj = to_d2(base[seg_pos<S>(j - 1)]);
+                            const double h = hz[j - 1];
+                            xn = make_double2(gj.x - h * xn.x, gj.y - h * xn.y);
+                            base[seg_pos<S>(j - 1)] = from_d2<C>(xn);
+                        }
+                    } else {
+                        // FP32 stage: the FP64 forward values go to the FP64 scratch row of
+                        // this block (after both stages), then the backward sweep
+                        double2* gsc = reinterpret_cast<double2*>(reinterpret_cast<C*>(yw_raw) + 2 * YW_L * LS);
+                        gsc[0] = gp;
+#pragma unroll 4
+                        for (int j = 2; j <= M; ++j) {
+                            const double2 rj = to_d2(base[seg_pos<S>(j - 1)]);
+                            const double am = g.amph[j], p = pp[j - 1];
+                            gp = make_double2((rj.x - am * gp.x) * p, (rj.y - am * gp.y) * p);
+                            gsc[j - 1] = gp;
+                        }
+                        double2 xn = gp;
+                        base[seg_pos<S>(M - 1)] = from_d2<C>(xn);
+#pragma unroll 4
+                        for (int j = M - 1; j >= 1; --j) {
+                            const double2 gj = gsc[j - 1];
+                            const double h = hz[j - 1];
+                            xn = make_double2(gj.x - h * xn.x, gj.y - h * xn.y);
+                            base[seg_pos<S>(j - 1)] = from_d2<C>(xn);
+                        }
+                    }
+                }
+            } else {
+                PoisCoef cf{g.amph, g.acph, g.apph, (-g.ak1[kx] / 1.0 - g.ak3[kz])};
+                double2 d[S];
+#pragma unroll
+                for (int k = 0; k < S; ++k) d[k] = to_d2(base[lane * (S + 1) + k]);
+                warp_tdma_c<S>(d, cf, lane);
+#pragma unroll
+                for (int k = 0; k < S; ++k) base[lane * (S + 1) + k] = from_d2<C>(d[k]);
+            }
+        }
+        __syncthreads();
+        {
+            const long long qs = gr * YW_L + ls;
+            if (qs < nl) {
+                C* dst = line_ptr(qs);
+                for (int j = js; j < M; j += RS) dst[(long long)LH * j] = st[ls * LS + seg_pos<S>(j)];
+            }
+        }
+        __syncthreads();  // the stage is free for the copies issued in the next iteration but one
     }
-    __syncthreads();
-    if (ls < nq) {
-        for (int j = js; j < M; j += YW_NT / YW_L) gsrc[(long long)LH * j] = from_d2<C>(smc[ls * LS + seg_pos<S>(j)]);
-    }
+    cp_async_wait_group<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -600,6 +674,7 @@ __global__ void __launch_bounds__(PX_NT, PX_MINB) k_fftx_inv(Geo g, const C* __r
     const int np = (nj + 1) >> 1;
     // Z_k = A_k + i B_k with A_{L-k} = conj A_k; imaginary parts of the k = 0 and
     // k = L/2 coefficients are dropped, as FFT99 does for ISIGN = +1.
+#pragma unroll 4
     for (int p = threadIdx.x; p < np * L; p += PX_NT) {
         const int pair = p / L, kk = p - pair * L;
         const int ja = j0 + 2 * pair;
@@ -621,33 +696,51 @@ __global__ void __launch_bounds__(PX_NT, PX_MINB) k_fftx_inv(Geo g, const C* __r
 }
 
 // ---------------------------------------------------------------------------
-// VELOUPDT_tg + PRCALC_tg + BC_WALL_PR_tg (Q walls are never written)
+// VELOUPDT_tg + PRCALC_tg + BC_WALL_PR_tg (Q walls are never written).
+// Each thread updates W = 16 / sizeof(R) consecutive points of an x line with
+// 16-byte loads and stores (L is a multiple of 4); the per-point arithmetic
+// is FP64, in the same order for every point.
 template <typename R>
 __global__ void __launch_bounds__(CR_NT) k_correct(Geo g, R* __restrict__ Q, R* __restrict__ PR,
                                                    const R* __restrict__ DPH, const R* __restrict__ RHSLL,
                                                    const DevState* __restrict__ st, int ns) {
     pdl_wait();
+    constexpr int W = V16<R>::W;
     const int L = g.L, M = g.M, N = g.N;
-    const long long tot = (long long)L * M * N;
+    const unsigned LV = (unsigned)(L / W);
+    const long long tot = (long long)LV * M * N;
     const long long t = (long long)blockIdx.x * CR_NT + threadIdx.x;
     if (t >= tot) return;
-    int i, j, k;
-    io_decode(g, t, i, j, k);
+    const unsigned u = (unsigned)t, r = u / LV, kk = r / (unsigned)M;
+    const int i0 = (int)(u - r * LV) * W, j = 1 + (int)(r - kk * (unsigned)M), k = (int)kk;
     const double dt = st->dt, ta = g.talp[ns];
-    const long long c = pidx(g, i, j, k);
+    const long long c = pidx(g, i0, j, k);
     // all loads first: Q is read and written through one pointer
-    const double ph = DPH[c];
-    const double phim = DPH[pidx(g, wrapm(i, L), j, k)];
-    const double phkm = DPH[pidx(g, i, j, wrapm(k, N))];
-    const double phjm = j >= 2 ? DPH[pidx(g, i, j - 1, k)] : 0.0;
-    const double u = Q[c], v = Q[c + g.FS], w = Q[c + 2 * g.FS];
-    const double pr = PR[c], ll = RHSLL[iidx(g, i, j, k)];
-    Q[c] = (R)(u - (ph - phim) * (dt * ta * g.dxi));
-    Q[c + 2 * g.FS] = (R)(w - (ph - phkm) * (dt * ta * g.dzi));
-    if (j >= 2) Q[c + g.FS] = (R)(v - (ph - phjm) * (dt * ta * g.dyci[j] / 1.0));
+    R ph[W], phk[W], phj[W], uu[W], vv[W], ww[W], pr[W], ll[W];
+    ld16(DPH + c, ph);
+    ld16(DPH + pidx(g, i0, j, wrapm(k, N)), phk);
+    if (j >= 2) ld16(DPH + c - L, phj);
+    ld16(Q + c, uu);
+    ld16(Q + c + g.FS, vv);
+    ld16(Q + c + 2 * g.FS, ww);
+    ld16(PR + c, pr);
+    ld16(RHSLL + iidx(g, i0, j, k), ll);
+    const double phim0 = DPH[pidx(g, wrapm(i0, L), j, k)];
+    const double cx = dt * ta * g.dxi, cz = dt * ta * g.dzi, cy = dt * ta * g.dyci[j] / 1.0;
     const double be = 0.5 * ta * dt * g.cvisc * 1.0 / 1.0;
-    const R pn = (R)(pr + ph - be * ll);
-    PR[c] = pn;
-    if (j == 1) PR[pidx(g, i, 0, k)] = pn;
-    if (j == M) PR[pidx(g, i, M + 1, k)] = pn;
+    R uo[W], vo[W], wo[W], pn[W];
+#pragma unroll
+    for (int e = 0; e < W; ++e) {
+        const double p = ph[e], pim = e == 0 ? phim0 : (double)ph[e - 1];
+        uo[e] = (R)(uu[e] - (p - pim) * cx);
+        wo[e] = (R)(ww[e] - (p - (double)phk[e]) * cz);
+        vo[e] = j >= 2 ? (R)(vv[e] - (p - (double)phj[e]) * cy) : vv[e];
+        pn[e] = (R)(pr[e] + p - be * ll[e]);
+    }
+    st16(Q + c, uo);
+    st16(Q + c + 2 * g.FS, wo);
+    if (j >= 2) st16(Q + c + g.FS, vo);
+    st16(PR + c, pn);
+    if (j == 1) st16(PR + pidx(g, i0, 0, k), pn);
+    if (j == M) st16(PR + pidx(g, i0, M + 1, k), pn);
 }

@@ -122,10 +122,14 @@ def test_two_way_ysolve_matches_oracle(shape):
 
 @pytest.mark.parametrize("shape,precision,tol", [((128, 128, 128), "fp64", 1e-12), ((64, 64, 64), "fp64", 1e-12),
                                                  ((192, 32, 128), "fp64", 1e-12), ((96, 64, 192), "fp64", 1e-12),
-                                                 ((128, 64, 192), "mixed", 1e-5), ((192, 32, 192), "mixed", 1e-5)])
+                                                 ((128, 64, 192), "mixed", 1e-5), ((192, 32, 192), "mixed", 1e-5),
+                                                 ((384, 32, 384), "fp64", 1e-12), ((384, 32, 384), "mixed", 1e-5),
+                                                 ((256, 64, 384), "fp64", 1e-12), ((384, 32, 256), "mixed", 1e-5),
+                                                 ((256, 32, 256), "fp64", 1e-12)])
 def test_plane_transforms_match_chained(shape, precision, tol):
-    """The fused plane transforms (one block per y row: divergence, x and z
-    transforms, and their inverses) advance the channel as the chained
+    """The fused plane transforms (one block per y row, or a thread-block
+    cluster per row where the plane does not fit one block: divergence, x
+    and z transforms, and their inverses) advance the channel as the chained
     transforms do, to round-off (only the pairing of real lines differs)."""
     L, M, N = shape
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)

@@ -1,0 +1,105 @@
+"""Long-run statistics acceptance of the mixed-precision step against the
+FP64 step: the chaotic-flow bound of the periodic channel.
+
+The two runs start from the same seeded field on the 128^3 channel
+(4pi x 2 x 4pi/3, Re_tau ~ 180, CFL 0.5), spin up through transition to
+turbulence, and then average the x-z means on the device every few steps
+(PP_MEAN_ZX_FLOW_TG + PP_MEAN_T_TG with the asymptotic average,
+src/processing/PP_MEAN_ZX.f90:14-307, src/processing/PP_MEAN_T.f90:343-392).
+By then the instantaneous fields of the two runs have decorrelated (the
+correlation of their u' fields is reported and must be small), so the runs
+are compared as statistics, not as trajectories:
+* mean U+ (U / u_tau, u_tau from the mean wall shear of each run),
+* u', v', w' rms,
+* the Reynolds shear stress -u'v',
+each within 1 % of the FP64 run's peak value of that profile.  The profiles
+are folded about the centreline (the channel's two halves are statistically
+the same flow; -u'v' changes sign), which halves their sampling noise.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from chapsim import gpu
+from chapsim.mesh import channel_setup
+from chapsim.fields import initial_field
+import bench
+
+pytestmark = pytest.mark.gpu
+
+WL = "channel128_retau180_fp64"
+AMP = 0.3            # amplitude of the seeded perturbation (times U_b)
+SPIN = 30000         # RK3 steps before the averaging window
+AVG = 30000          # RK3 steps in the averaging window
+EVERY = 20           # steps between samples
+BOUND = 1e-2
+
+
+def _run(precision):
+    L, M, N, HX, HZ, STR2, REN, DT0, CFLGV = bench.WORKLOADS[WL]
+    s = channel_setup(L, M, N, HX, HZ, STR2, REN)
+    Q, PR = initial_field(s, 1973, AMP)
+    c = gpu.ChannelTG(s, precision=precision)
+    c.upload(Q, PR)
+    c.set_dt(DT0)
+    c.SOLVERRK3_MOM_tg(0)
+    c.autotune()
+    t = 0.0
+    for _ in range(SPIN // 1000):
+        dt, _ = c.advance(1000, DT0, 1e-6, CFLGV)
+        t += 1000 * dt
+    t_spin = t
+    for _ in range(AVG // EVERY):
+        dt, _ = c.advance(EVERY, DT0, 1e-6, CFLGV)
+        t += EVERY * dt
+        c.PP_MEAN_ZX_FLOW_TG()
+        c.PP_MEAN_T_TG(TP=1)
+    flat, nst = c.download_pp_means(averaged=True)
+    c.PP_MEAN_ZX_FLOW_TG()
+    mon = c.PP_MONITOR_TG(REN)
+    Qf, _ = c.download()
+    c.close()
+    return s, gpu.ChannelTG.pp_split(flat, M), nst, Qf, mon, t_spin, t
+
+
+def _profiles(s, pp):
+    M = s.M
+    U, V, W = pp["U1xzL"][0], pp["U1xzL"][1], pp["U1xzL"][2]
+    u2 = pp["U2xzL"]  # uu, uv, uw, vv, vw, ww
+    urms = np.sqrt(np.maximum(u2[0] - U * U, 0.0))
+    vrms = np.sqrt(np.maximum(u2[3] - V * V, 0.0))
+    wrms = np.sqrt(np.maximum(u2[5] - W * W, 0.0))
+    uv = -(u2[1] - U * V)
+    nu = 1.0 / s.REN
+    ycc, ynd = s.YCC[1:M + 1], s.YND[1:M + 2]
+    tau = 0.5 * (nu * U[0] / (ycc[0] - ynd[0]) + nu * U[-1] / (ynd[-1] - ycc[-1]))
+    utau = math.sqrt(tau)
+
+    def fold(f, sign=1.0):
+        return 0.5 * (f + sign * f[::-1])[: M // 2]
+
+    return {"U+": fold(U / utau), "u_rms": fold(urms), "v_rms": fold(vrms), "w_rms": fold(wrms),
+            "-u'v'": fold(uv, -1.0)}, utau
+
+
+def test_mixed_statistics_match_fp64_after_decorrelation():
+    s, p64, n64, q64, m64, ts64, t64 = _run("fp64")
+    _, p32, n32, q32, m32, ts32, t32 = _run("mixed")
+    assert n64 == n32 == AVG // EVERY
+    f64, ut64 = _profiles(s, p64)
+    f32, ut32 = _profiles(s, p32)
+    M = s.M
+    ua = q64[0][:, 1:M + 1] - q64[0][:, 1:M + 1].mean(axis=(0, 2), keepdims=True)
+    ub = q32[0][:, 1:M + 1] - q32[0][:, 1:M + 1].mean(axis=(0, 2), keepdims=True)
+    corr = float((ua * ub).mean() / math.sqrt((ua * ua).mean() * (ub * ub).mean()))
+    print("time: spin-up %.1f, end %.1f (FP64) / %.1f, %.1f (mixed)" % (ts64, t64, ts32, t32))
+    print("u_tau FP64 %.5f mixed %.5f; Cf bottom %.5f / %.5f" % (ut64, ut32, m64["Cf_bottom"], m32["Cf_bottom"]))
+    print("correlation of the final u' fields: %.3f" % corr)
+    # the flow is turbulent: the wall shear is well above the laminar value (Cf = 6 / REN)
+    assert m64["Cf_bottom"] > 2.0 * 6.0 / s.REN
+    assert abs(corr) < 0.5
+    for k in f64:
+        d = float(np.abs(f32[k] - f64[k]).max() / np.abs(f64[k]).max())
+        print("%-6s peak %.4f  max diff / peak %.4f" % (k, float(np.abs(f64[k]).max()), d))
+        assert d <= BOUND, (k, d)

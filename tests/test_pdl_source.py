@@ -29,6 +29,8 @@ def _pdl_kernels(src):
     names = set()
     for text in src.values():
         names.update(re.findall(r"launch_pdl\(\s*[^,()]+,\s*(k_\w+)", text))
+        # launch_cluster(pdl, cluster size, kernel, ...): the cluster launches of the plane transforms
+        names.update(re.findall(r"launch_cluster\(\s*[^,()]+,\s*[^,()]+,\s*(k_\w+)", text))
     return names
 
 
