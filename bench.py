@@ -261,6 +261,36 @@ def heated_measure(args, local, dist, ws, steps):
     judge = ch.mlp_judge()
     k_mlp = kernel_profile()
 
+    # ---- the same channel in mixed precision (FP32 flow fields, FP64 properties, thermal
+    #      fields and Poisson solve), with the table search and with the trained model ----
+    params, _norm = ch.mlp_params()
+    chm = gpu.ChannelIO(s, device=local, ivisscheme=gpu.VIS_IMPLICIT, precision="mixed")
+    chm.upload_io(Q, PR, ones, ones, ones)
+    chm.set_dt(DT0)
+    chm.thermal_init(tab, DH, h["qw"], h["qw"], cthecd)
+    stream_m = torch.cuda.ExternalStream(chm.stream_handle(), device=local)
+
+    def timed_m(nsteps):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+        ev0.record(stream_m)
+        chm.advance(nsteps, DT0, DTMIN, CFLGV)
+        ev1.record(stream_m)
+        torch.cuda.synchronize(local)
+        return max_over_ranks(ev0.elapsed_time(ev1), dist, f"cuda:{local}")
+
+    chm.advance(args.warmup, DT0, DTMIN, CFLGV)
+    ms_mt = timed_m(steps)
+    chm.mlp_init(lo, hi, seed=11)
+    chm.mlp_set_params(params)
+    chm.thermal_use_mlp(True)
+    chm.advance(args.warmup, DT0, DTMIN, CFLGV)
+    ms_ml = timed_m(steps)
+    judge_m = chm.mlp_judge()
+    chm.close()
+
     # ---- roofline of the dominant kernel (table-search step) ----
     words = heated_kernel_words(L, M)
     per_step = {k: (1 if k in ("k_io_cfl", "k_dt") else 3) for k in k_table}
@@ -299,7 +329,14 @@ def heated_measure(args, local, dist, ws, steps):
             "training": {"samples": int(train.size), "iterations": sum(i for i, _ in MLP_SCHEDULE),
                          "seconds": t_train, "final_loss": loss},
             "property_update_ms_per_step": {"table": k_table.get("k_eng_props"), "model": k_mlp.get("k_mlp_infer")},
-            "gpu_launches": int(launches_m), "clocks": clk_m}},
+            "gpu_launches": int(launches_m), "clocks": clk_m},
+            "mixed": {"value_table": pts * steps * ws / (ms_mt / 1000.0),
+                      "value_learned": pts * steps * ws / (ms_ml / 1000.0), "unit": UNIT,
+                      "ms_per_step_table": ms_mt / steps, "ms_per_step_learned": ms_ml / steps,
+                      "speedup_vs_fp64_table": ms_t / ms_mt, "speedup_learned_vs_fp64_table": ms_t / ms_ml,
+                      "judge_max_rel_err": judge_m,
+                      "precision": "FP32 flow fields (G, Q, PR, EXPLT0, RHS, D_STG, MU_STG, DivU); FP64 "
+                                   "properties, thermal fields, Poisson solve and projection"}},
     }
     ch.close()
     return line
@@ -768,6 +805,7 @@ def run_b200(args):
             "speedup_learned_vs_table": lv["speedup_vs_table"],
             "property_update_ms_per_step": lv["property_update_ms_per_step"],
             "judge_max_rel_err": lv["judge_max_rel_err"], "bound": lv["bound"], "within_bound": lv["within_bound"],
+            "mixed": hl["variants"]["mixed"],
             "step_roofline_frac": hl["step_roofline"]["frac"],
             "note": "main domain (Crank-Nicolson momentum, energy equation, property update every substep), FP64; "
                     "the full line: --workload " + HEATED_WORKLOAD}

@@ -173,7 +173,8 @@ struct chapsim_ctx {
     double *pp_inst = nullptr, *pp_avg = nullptr, *pp_part = nullptr, *pp_mon = nullptr;
     int pp_nchunk = 0;
     int nstatis = 0;              // NSTATIS_TG
-    IoFields io{};                // IO-path arrays (domain 2)
+    IoFields io{};                // IO-path arrays (domain 2); FP64 staging of G in the mixed-precision step
+    IoFieldsT<float> iof{};       // FP32 flow fields of the mixed-precision main-domain step (Q, PR, RHS: Qf, PRf, RHSf)
     int io_grid = 0;              // blocks of the IO point-wise kernels
     cudaGraphExec_t step_exec = nullptr;
     cudaEvent_t* prof_ev = nullptr;  // when set, an event is recorded after every kernel
@@ -449,7 +450,8 @@ int configure_kernels(chapsim_ctx* ctx) {
     // the FP64 spectral stage serves the standalone Poisson solve and the main domain in every precision
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, double2>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_from_rhs<FN1, FN2>, smem_px(g))));
-    DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2>, smem_px(g))));
+    DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, double>, smem_px(g))));
+    DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, float>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw<double2>(g))));
     CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
@@ -457,9 +459,12 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));
     if (ctx->domain == 2 && ctx->ivis) {
-        DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S>, smem_cn(g.L))));
-        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S>, smem_cn(g.N))));
-        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S>, smem_cn(g.M))));
+        DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S, double>, smem_cn(g.L))));
+        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S, double>, smem_cn(g.N))));
+        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S, double>, smem_cn(g.M))));
+        DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S, float>, smem_cn(g.L))));
+        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S, float>, smem_cn(g.N))));
+        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S, float>, smem_cn(g.M))));
     }
     return CHAPSIM_OK;
 }
@@ -622,23 +627,39 @@ int mixed_to_staging(chapsim_ctx* ctx, bool q, bool pr, bool h0) {
 }
 
 // ----------------------------- IO path -----------------------------------
-IoFields io_fields(chapsim_ctx* ctx) {
+// The main-domain fields in the storage type F of the context's precision:
+// FP64 (ctx->io, Q, PR, RHS) or the FP32 flow fields of the mixed step
+// (ctx->iof, Qf, PRf, RHSf); the property fields, the buoyancy and the
+// weighted-pressure settings are shared.
+template <typename F> IoFieldsT<F> io_fields_t(chapsim_ctx* ctx);
+template <> IoFieldsT<double> io_fields_t<double>(chapsim_ctx* ctx) {
     IoFields f = ctx->io;
     f.Q = ctx->Q; f.PR = ctx->PR; f.RHS = ctx->RHS;
     f.DEN = ctx->thermal ? ctx->DEN : f.RHO;
     return f;
 }
+template <> IoFieldsT<float> io_fields_t<float>(chapsim_ctx* ctx) {
+    IoFieldsT<float> f = ctx->iof;
+    f.Q = ctx->Qf; f.PR = ctx->PRf; f.RHS = ctx->RHSf;
+    f.RHO = ctx->io.RHO; f.MU0 = ctx->io.MU0; f.MU = ctx->io.MU;
+    f.DEN = ctx->thermal ? ctx->DEN : f.RHO;
+    f.PR0A = ctx->io.PR0A; f.PR0B = ctx->io.PR0B; f.fa = ctx->io.fa; f.igrav = ctx->io.igrav;
+    return f;
+}
+IoFields io_fields(chapsim_ctx* ctx) { return io_fields_t<double>(ctx); }
+inline bool io_mixed(const chapsim_ctx* ctx) { return ctx->prec == CHAPSIM_PREC_MIXED; }
 
 int prop_grid(const chapsim_ctx* ctx, long long npts);
 size_t prop_smem(int n);
 
 // SOLVERRK3_ENG_io(NS), DENSITY_TIME_DERIVATION, DENSITY_Staggered,
 // MU_Staggered, then G0 = G and VELOCITY_CALC_io of SOLVERRK3_MOM_io
-void launch_thermal_substep(chapsim_ctx* ctx, int ns) {
+template <typename F>
+void launch_thermal_substep_t(chapsim_ctx* ctx, int ns) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    IoFields f = io_fields(ctx);
-    k_eng_rhs<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ctx->tp, ctx->st, ns);
+    IoFieldsT<F> f = io_fields_t<F>(ctx);
+    k_eng_rhs<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ctx->tp, ctx->st, ns);
     prof_mark(ctx);
     const size_t sm = prop_smem(ctx->tab.n);
     const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
@@ -649,65 +670,68 @@ void launch_thermal_substep(chapsim_ctx* ctx, int ns) {
             ctx->mlp_par, MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t}, ctx->mlp_norm, ctx->tab, g, tot,
             ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
         prof_mark(ctx);
-        if (sm) k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        else k_eng_bc<false><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
     } else if (sm) {
-        k_eng_props<true><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
         prof_mark(ctx);
-        k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
     } else {
-        k_eng_props<false><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
         prof_mark(ctx);
-        k_eng_bc<false><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
     }
     prof_mark(ctx);
-    k_drhodt<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ns);
+    k_drhodt<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ns);
     prof_mark(ctx);
-    k_io_props<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    k_io_props<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     prof_mark(ctx);
-    k_g0_velocity<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf.G0);
+    k_g0_velocity<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf.G0);
     prof_mark(ctx);
     ctx->launches += 6;
 }
 
 void launch_io_step_start(chapsim_ctx* ctx) {
-    k_io_cfl<<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields(ctx), ctx->part_red, ctx->st);
+    if (io_mixed(ctx)) k_io_cfl<float><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields_t<float>(ctx), ctx->part_red, ctx->st);
+    else k_io_cfl<double><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields_t<double>(ctx), ctx->part_red, ctx->st);
     prof_mark(ctx);
     k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, 1);
     prof_mark(ctx);
     ctx->launches += 2;
 }
 
-void launch_io_substep(chapsim_ctx* ctx, int ns) {
+template <typename F>
+void launch_io_substep_t(chapsim_ctx* ctx, int ns) {
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;
-    if (ctx->thermal) launch_thermal_substep(ctx, ns);
-    IoFields f = io_fields(ctx);
+    if (ctx->thermal) launch_thermal_substep_t<F>(ctx, ns);
+    IoFieldsT<F> f = io_fields_t<F>(ctx);
     if (!ctx->ivis) {
-        k_io_divu<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+        k_io_divu<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
         prof_mark(ctx);
-        k_io_rhs<false><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
+        k_io_rhs<false, F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
         prof_mark(ctx);
-        k_io_massflux<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
+        k_io_massflux<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
         prof_mark(ctx);
     } else {
         // VISCOUS_PAR_EXPLT_* + RHS_MOM_EXPLICIT_io, then MOMFA_io's sweeps for all components
-        k_io_rhs<true><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
+        k_io_rhs<true, F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
         prof_mark(ctx);
         dim3 gx((unsigned)((g.M * (long long)g.N + CN_LINES - 1) / CN_LINES), 3);
-        DISPATCH_S(g.L / 32, (k_io_cn_xsweep<S><<<gx, CN_NT, smem_cn(g.L), s>>>(g, f, ctx->st, ns)));
+        DISPATCH_S(g.L / 32, (k_io_cn_xsweep<S, F><<<gx, CN_NT, smem_cn(g.L), s>>>(g, f, ctx->st, ns)));
         prof_mark(ctx);
         dim3 gz(g.L / CN_LINES, g.M, 3), gy(g.L / CN_LINES, g.N, 3);
-        DISPATCH_S(g.N / 32, (k_io_cn_zsweep<S><<<gz, CN_NT, smem_cn(g.N), s>>>(g, f, ctx->st, ns)));
-        DISPATCH_S(g.M / 32, (k_io_cn_ysweep<S><<<gy, CN_NT, smem_cn(g.M), s>>>(g, f, ctx->st, ns)));
+        DISPATCH_S(g.N / 32, (k_io_cn_zsweep<S, F><<<gz, CN_NT, smem_cn(g.N), s>>>(g, f, ctx->st, ns)));
+        DISPATCH_S(g.M / 32, (k_io_cn_ysweep<S, F><<<gy, CN_NT, smem_cn(g.M), s>>>(g, f, ctx->st, ns)));
         prof_mark(ctx);
         ctx->launches += 1;
     }
+    // the Poisson stage is FP64 in both precisions
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
-    DISPATCH_FFT(g.L, (k_io_div_fftx<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->io.G, ctx->RHSLL, ctx->SP,
-                                                                            ctx->st, ns,
-                                                                            ctx->thermal ? ctx->tf.DRHO : nullptr,
-                                                                            ctx->io.PR0A ? 0.25 + IO_PRES_EPSLON : 1.0)));
+    DISPATCH_FFT(g.L, (k_io_div_fftx<FN1, FN2, F><<<grp, PX_NT, smem_px(g), s>>>(g, f.G, ctx->RHSLL, ctx->SP,
+                                                                               ctx->st, ns,
+                                                                               ctx->thermal ? ctx->tf.DRHO : nullptr,
+                                                                               ctx->io.PR0A ? 0.25 + IO_PRES_EPSLON : 1.0)));
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
@@ -719,9 +743,13 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, double2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     prof_mark(ctx);
-    k_io_correct<<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, ctx->ivis ? ctx->RHSLL : nullptr);
+    k_io_correct<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, ctx->ivis ? ctx->RHSLL : nullptr);
     prof_mark(ctx);
     ctx->launches += 9;
+}
+void launch_io_substep(chapsim_ctx* ctx, int ns) {
+    if (io_mixed(ctx)) launch_io_substep_t<float>(ctx, ns);
+    else launch_io_substep_t<double>(ctx, ns);
 }
 
 int check_device_error(chapsim_ctx* ctx) {
@@ -792,8 +820,6 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     const int prec = opts ? opts->precision : CHAPSIM_PREC_FP64;
     if (prec != CHAPSIM_PREC_FP64 && prec != CHAPSIM_PREC_MIXED)
         return fail(nullptr, CHAPSIM_ERR_BADARG, "precision must be CHAPSIM_PREC_FP64 or CHAPSIM_PREC_MIXED");
-    if (prec == CHAPSIM_PREC_MIXED && grid->idomain != 1)
-        return fail(nullptr, CHAPSIM_ERR_BADARG, "the mixed-precision step is available for the periodic TG domain only");
     const int ivis = opts ? opts->ivisscheme : CHAPSIM_VIS_EXPLICIT;
     if (ivis != CHAPSIM_VIS_EXPLICIT && ivis != CHAPSIM_VIS_IMPLICIT)
         return fail(nullptr, CHAPSIM_ERR_BADARG, "ivisscheme must be CHAPSIM_VIS_EXPLICIT or CHAPSIM_VIS_IMPLICIT");
@@ -939,6 +965,17 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         INIT_CK(cudaMalloc(&ctx->SPf, (size_t)g.LH * M * N * sizeof(float2)));
         INIT_CK(cudaMalloc(&ctx->DPHf, (size_t)g.FS * sizeof(float)));
         INIT_CK(cudaMemset(ctx->DPHf, 0, (size_t)g.FS * sizeof(float)));
+        if (ctx->domain == 2) {  // FP32 flow fields of the main domain (Q, PR and RHS are Qf, PRf, RHSf)
+            IoFieldsT<float>& f = ctx->iof;
+            INIT_CK(cudaMalloc(&f.G, (size_t)(3 * g.FS) * sizeof(float)));
+            INIT_CK(cudaMalloc(&f.EX0, (size_t)(3 * g.FI) * sizeof(float)));
+            INIT_CK(cudaMalloc(&f.DST, (size_t)(3 * g.FS) * sizeof(float)));
+            INIT_CK(cudaMalloc(&f.MST, (size_t)(3 * g.FS) * sizeof(float)));
+            INIT_CK(cudaMalloc(&f.DIVU, (size_t)g.FS * sizeof(float)));
+            INIT_CK(cudaMemset(f.G, 0, (size_t)(3 * g.FS) * sizeof(float)));
+            INIT_CK(cudaMemset(f.EX0, 0, (size_t)(3 * g.FI) * sizeof(float)));
+            INIT_CK(cudaMemset(f.DIVU, 0, (size_t)g.FS * sizeof(float)));
+        }
     }
     INIT_CK(cudaMalloc(&ctx->st, sizeof(DevState)));
     INIT_CK(cudaMallocHost(&ctx->st_host, sizeof(DevState)));
@@ -973,6 +1010,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
+    cudaFree(ctx->iof.G); cudaFree(ctx->iof.EX0); cudaFree(ctx->iof.DST); cudaFree(ctx->iof.MST); cudaFree(ctx->iof.DIVU);
     cudaFree(const_cast<double*>(ctx->io.PR0A));
     cudaFree(ctx->ptab); cudaFree(ctx->pstat); cudaFree(ctx->pbuf);
     cudaFree(ctx->mlp_par); cudaFree(ctx->mlp_w2); cudaFree(ctx->mlp_xs); cudaFree(ctx->mlp_ys); cudaFree(ctx->mlp_dh);
@@ -1318,11 +1356,25 @@ int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* gq, const double*
     CK(cudaMemcpyAsync(f.MU0, mu0, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(f.MU, mu, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(f.EX0, 0, (size_t)(3 * g.FI) * sizeof(double), s));
-    k_bc_fields<<<ctx->npart_red, DG_NT, 0, s>>>(g, f.G, ctx->PR);     // BC_WALL_G_io, BC_WALL_PR_io
-    k_io_props<<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));       // DENSITY_Staggered, MU_Staggered
-    k_io_velocity<<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));    // VELOCITY_CALC_io
-    k_bc_fields<<<ctx->npart_red, DG_NT, 0, s>>>(g, ctx->Q, ctx->PR);   // BC_WALL_Q_io
-    ctx->launches += 4;
+    if (io_mixed(ctx)) {
+        // the FP64 host fields rounded once into the FP32 flow fields
+        const int nb = 4 * ctx->nsm;
+        IoFieldsT<float> ff = io_fields_t<float>(ctx);
+        k_convert<float, double><<<nb, DG_NT, 0, s>>>(ff.G, f.G, 3 * g.FS);
+        k_convert<float, double><<<nb, DG_NT, 0, s>>>(ctx->PRf, ctx->PR, g.FS);
+        CK(cudaMemsetAsync(ff.EX0, 0, (size_t)(3 * g.FI) * sizeof(float), s));
+        k_bc_fields<float><<<ctx->npart_red, DG_NT, 0, s>>>(g, ff.G, ctx->PRf);
+        k_io_props<float><<<ctx->io_grid, IO_NT, 0, s>>>(g, ff);
+        k_io_velocity<float><<<ctx->io_grid, IO_NT, 0, s>>>(g, ff);
+        k_bc_fields<float><<<ctx->npart_red, DG_NT, 0, s>>>(g, ctx->Qf, ctx->PRf);
+        ctx->launches += 6;
+    } else {
+        k_bc_fields<double><<<ctx->npart_red, DG_NT, 0, s>>>(g, f.G, ctx->PR);  // BC_WALL_G_io, BC_WALL_PR_io
+        k_io_props<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));   // DENSITY_Staggered, MU_Staggered
+        k_io_velocity<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));  // VELOCITY_CALC_io
+        k_bc_fields<double><<<ctx->npart_red, DG_NT, 0, s>>>(g, ctx->Q, ctx->PR);  // BC_WALL_Q_io
+        ctx->launches += 4;
+    }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
     return CHAPSIM_OK;
@@ -1332,6 +1384,13 @@ int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* gq, double* q, double
     if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
     const Geo& g = ctx->g;
+    if (io_mixed(ctx)) {  // widen the FP32 flow fields into the FP64 staging arrays first
+        const int nb = 4 * ctx->nsm;
+        if (gq) k_convert<double, float><<<nb, DG_NT, 0, ctx->stream>>>(ctx->io.G, ctx->iof.G, 3 * g.FS);
+        if (q) k_convert<double, float><<<nb, DG_NT, 0, ctx->stream>>>(ctx->Q, ctx->Qf, 3 * g.FS);
+        if (pr) k_convert<double, float><<<nb, DG_NT, 0, ctx->stream>>>(ctx->PR, ctx->PRf, g.FS);
+        CK(cudaGetLastError());
+    }
     if (gq) CK(cudaMemcpyAsync(gq, ctx->io.G, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (q) CK(cudaMemcpyAsync(q, ctx->Q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (pr) CK(cudaMemcpyAsync(pr, ctx->PR, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1397,7 +1456,8 @@ int chapsim_upload_weighted_pressure(chapsim_ctx_t* ctx, const double* pr0_1, co
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {
     if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
-    k_io_cfl<<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields(ctx), ctx->part_red, ctx->st);
+    if (io_mixed(ctx)) k_io_cfl<float><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields_t<float>(ctx), ctx->part_red, ctx->st);
+    else k_io_cfl<double><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields(ctx), ctx->part_red, ctx->st);
     k_dt<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st, 0);
     ctx->launches += 2;
     CK(cudaGetLastError());
@@ -1410,8 +1470,12 @@ int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv) {
     if (!ctx || !maxdiv) return CHAPSIM_ERR_BADARG;
     if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
-    k_io_divgck<<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, ctx->io.G, ctx->thermal ? ctx->tf.DRHO : nullptr,
-                                                           ctx->part_red);
+    if (io_mixed(ctx))
+        k_io_divgck<float><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, ctx->iof.G,
+                                                                      ctx->thermal ? ctx->tf.DRHO : nullptr, ctx->part_red);
+    else
+        k_io_divgck<double><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, ctx->io.G,
+                                                                       ctx->thermal ? ctx->tf.DRHO : nullptr, ctx->part_red);
     k_maxdiv_final<<<1, DG_NT, 0, ctx->stream>>>(ctx->part_red, ctx->npart_red, ctx->st);
     ctx->launches += 2;
     CK(cudaGetLastError());
@@ -1596,8 +1660,10 @@ extern "C" int chapsim_prop_table_init(chapsim_ctx_t* ctx, const chapsim_prop_ta
     if (sm) {
         CK(set_smem(k_prop_points<true>, sm));
         CK(set_smem(k_prop_fields<true>, sm));
-        CK(set_smem(k_eng_props<true>, sm));
-        CK(set_smem(k_eng_bc<true>, sm));
+        CK(set_smem(k_eng_props<true, double>, sm));
+        CK(set_smem(k_eng_bc<true, double>, sm));
+        CK(set_smem(k_eng_props<true, float>, sm));
+        CK(set_smem(k_eng_bc<true, float>, sm));
     }
     return CHAPSIM_OK;
 }
@@ -1645,6 +1711,32 @@ extern "C" int chapsim_therm_prop_update_points(chapsim_ctx_t* ctx, int64_t npts
     return CHAPSIM_OK;
 }
 
+// First properties of the thermal solver: THERM_PROP_UPDATE on the interior and
+// the wall ghosts, DENSITY0 = DENSITY, Viscousity0 = Viscousity, G0_io = G_io,
+// DENSITY_Staggered, MU_Staggered and VELOCITY_CALC_io
+template <typename F>
+void thermal_start(chapsim_ctx* ctx, size_t fb) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    IoFieldsT<F> f = io_fields_t<F>(ctx);
+    const size_t sm = prop_smem(ctx->tab.n);
+    const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
+    if (sm) {
+        k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    } else {
+        k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    }
+    cudaMemcpyAsync(ctx->io.RHO, ctx->DEN, fb, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(ctx->io.MU0, ctx->io.MU, fb, cudaMemcpyDeviceToDevice, s);
+    if constexpr (sizeof(F) == 8) cudaMemcpyAsync(ctx->tf.G0, f.G, 3 * fb, cudaMemcpyDeviceToDevice, s);
+    else k_convert<double, float><<<4 * ctx->nsm, DG_NT, 0, s>>>(ctx->tf.G0, f.G, 3 * g.FS);
+    k_io_props<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    k_io_velocity<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    ctx->launches += 5;
+}
+
 extern "C" int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, double qw_top, double cthecd) {
     if (!ctx || !dh) return fail(ctx, CHAPSIM_ERR_BADARG, "null argument");
     if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver runs in the main (IO) domain");
@@ -1675,23 +1767,8 @@ extern "C" int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double
     CK(cudaMemsetAsync(ctx->tf.RHSE0, 0, fb, s));  // RHS_ENERGY0 = 0 (src/SOLVE.f90:40)
     CK(cudaMemcpyAsync(ctx->DEN, ctx->io.RHO, fb, cudaMemcpyDeviceToDevice, s));
     ctx->thermal = true;
-    IoFields f = io_fields(ctx);
-    const size_t sm = prop_smem(ctx->tab.n);
-    const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
-    if (sm) {
-        k_eng_props<true><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        k_eng_bc<true><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-    } else {
-        k_eng_props<false><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        k_eng_bc<false><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-    }
-    // DENSITY0 = DENSITY, Viscousity0 = Viscousity, G0_io = G_io
-    CK(cudaMemcpyAsync(ctx->io.RHO, ctx->DEN, fb, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->io.MU0, ctx->io.MU, fb, cudaMemcpyDeviceToDevice, s));
-    CK(cudaMemcpyAsync(ctx->tf.G0, ctx->io.G, 3 * fb, cudaMemcpyDeviceToDevice, s));
-    k_io_props<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
-    k_io_velocity<<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
-    ctx->launches += 4;
+    if (io_mixed(ctx)) thermal_start<float>(ctx, fb);
+    else thermal_start<double>(ctx, fb);
     CK(cudaGetLastError());
     if (ctx->step_exec) {  // the captured step no longer matches
         CK(cudaStreamSynchronize(s));

@@ -29,12 +29,21 @@
 // solver is off); MU0 is Viscousity0 and MU is Viscousity.
 // PR0A/PR0B: PR0_io(:,:,:,1) and PR0_io(:,:,:,2) of iWeightedPre = 1 (NULL when
 // off).  igrav/fa: iGravity and F_A of thermal_gravity (src/Flow_State.f90:95-125).
-struct IoFields {
-    double *G, *Q, *PR, *EX0, *RHS, *RHO, *MU0, *MU, *DST, *MST, *DIVU, *DEN;
+// F is the storage type of the flow fields G, Q, PR, EXPLT0, RHS, D_STG, MU_STG
+// and DivU: double, or float in the mixed-precision step.  The property
+// fields (DENSITY, DENSITY0, Viscousity, Viscousity0) stay FP64 (they come
+// from the FP64 property update), and the kernels evaluate in FP64.
+template <typename F>
+struct IoFieldsT {
+    F *G, *Q, *PR, *EX0, *RHS;
+    double *RHO, *MU0, *MU;
+    F *DST, *MST, *DIVU;
+    double* DEN;
     const double *PR0A = nullptr, *PR0B = nullptr;
     double fa = 0.0;
     int igrav = 0;
 };
+using IoFields = IoFieldsT<double>;
 
 // iWeightedPre: pres_epslon (src/modules.f90:483)
 #define IO_PRES_EPSLON 0.001
@@ -42,7 +51,8 @@ struct IoFields {
 // PGM of RHS_MOM_EXPLICIT_io (src/RHS_MOM_EXPLICIT_io.f90:103-159): the
 // pressure difference between point c and its lower neighbour cm times coe,
 // blended with the two PR0_io layers when iWeightedPre = 1
-__device__ __forceinline__ double io_pgm(const IoFields& f, long long c, long long cm, double pc, double pm,
+template <typename F>
+__device__ __forceinline__ double io_pgm(const IoFieldsT<F>& f, long long c, long long cm, double pc, double pm,
                                          double coe) {
     if (f.PR0A)
         return ((f.PR0B[c] - f.PR0B[cm]) * (0.25 - IO_PRES_EPSLON) + (f.PR0A[c] - f.PR0A[cm]) * 0.5 +
@@ -52,7 +62,8 @@ __device__ __forceinline__ double io_pgm(const IoFields& f, long long c, long lo
 
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFields f) {
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFieldsT<F> f) {
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
@@ -62,56 +73,58 @@ __global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFields f) {
         const long long c = pidx(g, i, j, k);
         const double* R = f.RHO;
         const double* U0 = f.MU0;
-        f.DST[c] = (R[c] + R[pidx(g, im, j, k)]) * 0.5;
-        f.DST[c + 2 * g.FS] = (R[c] + R[pidx(g, i, j, km)]) * 0.5;
-        f.DST[c + g.FS] = j >= 2 ? g.wff[j] * R[c] + g.wfb[j] * R[pidx(g, i, j - 1, k)] : R[pidx(g, i, 0, k)];
+        f.DST[c] = (F)((R[c] + R[pidx(g, im, j, k)]) * 0.5);
+        f.DST[c + 2 * g.FS] = (F)((R[c] + R[pidx(g, i, j, km)]) * 0.5);
+        f.DST[c + g.FS] = (F)(j >= 2 ? g.wff[j] * R[c] + g.wfb[j] * R[pidx(g, i, j - 1, k)] : R[pidx(g, i, 0, k)]);
         if (j >= 2) {
-            f.MST[c] = ((U0[c] + U0[pidx(g, im, j, k)]) * g.wff[j] + (U0[pidx(g, i, j - 1, k)] + U0[pidx(g, im, j - 1, k)]) * g.wfb[j]) * 0.5;
-            f.MST[c + 2 * g.FS] = ((U0[pidx(g, i, j, km)] + U0[c]) * g.wff[j] +
-                                   (U0[pidx(g, i, j - 1, km)] + U0[pidx(g, i, j - 1, k)]) * g.wfb[j]) * 0.5;
+            f.MST[c] = (F)(((U0[c] + U0[pidx(g, im, j, k)]) * g.wff[j] + (U0[pidx(g, i, j - 1, k)] + U0[pidx(g, im, j - 1, k)]) * g.wfb[j]) * 0.5);
+            f.MST[c + 2 * g.FS] = (F)(((U0[pidx(g, i, j, km)] + U0[c]) * g.wff[j] +
+                                   (U0[pidx(g, i, j - 1, km)] + U0[pidx(g, i, j - 1, k)]) * g.wfb[j]) * 0.5);
         } else {
-            f.MST[c] = U0[pidx(g, i, 0, k)];
-            f.MST[c + 2 * g.FS] = U0[pidx(g, i, 0, k)];
+            f.MST[c] = (F)U0[pidx(g, i, 0, k)];
+            f.MST[c + 2 * g.FS] = (F)U0[pidx(g, i, 0, k)];
         }
-        f.MST[c + g.FS] = (U0[c] + U0[pidx(g, im, j, k)] + U0[pidx(g, i, j, km)] + U0[pidx(g, im, j, km)]) * 0.5 * 0.5;
+        f.MST[c + g.FS] = (F)((U0[c] + U0[pidx(g, im, j, k)] + U0[pidx(g, i, j, km)] + U0[pidx(g, im, j, km)]) * 0.5 * 0.5);
         if (j == M) {
             const long long ct = pidx(g, i, M + 1, k);
-            f.DST[ct + g.FS] = R[ct];
-            f.MST[ct] = U0[ct];
-            f.MST[ct + 2 * g.FS] = U0[ct];
+            f.DST[ct + g.FS] = (F)R[ct];
+            f.MST[ct] = (F)U0[ct];
+            f.MST[ct + 2 * g.FS] = (F)U0[ct];
         }
     }
 }
 
 // DIVG_U_io; also VELOCITY_CALC_io of the upload (Q = G / D_STG) when vel != 0
-__global__ void __launch_bounds__(IO_NT) k_io_velocity(Geo g, IoFields f) {
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_velocity(Geo g, IoFieldsT<F> f) {
     const long long tot = (long long)g.L * g.M * g.N;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
         const double g1 = f.G[c], g3 = f.G[c + 2 * g.FS], d1 = f.DST[c], d3 = f.DST[c + 2 * g.FS];
-        f.Q[c] = g1 / d1;
-        f.Q[c + 2 * g.FS] = g3 / d3;
-        if (j >= 2) f.Q[c + g.FS] = f.G[c + g.FS] / f.DST[c + g.FS];
+        f.Q[c] = (F)(g1 / d1);
+        f.Q[c + 2 * g.FS] = (F)(g3 / d3);
+        if (j >= 2) f.Q[c + g.FS] = (F)((double)f.G[c + g.FS] / (double)f.DST[c + g.FS]);
     }
 }
 
-__global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFields f) {
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFieldsT<F> f) {
     const int L = g.L, N = g.N;
     const long long tot = (long long)L * g.M * N;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
-        const double* Q = f.Q;
+        const F* Q = f.Q;
         const double u = Q[c], up = Q[pidx(g, wrapp(i, L), j, k)];
         const double v = Q[c + g.FS], vp = Q[c + g.FS + L];
         const double w = Q[c + 2 * g.FS], wp = Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS];
         const double DIVX = (up - u) * g.dxi;
         const double DIVY = (vp - v) * (g.dyfi[j] * 1.0);
         const double DIVZ = (wp - w) * (g.dzi * 1.0);
-        f.DIVU[c] = (DIVX + DIVY + DIVZ) / 3.0;
+        f.DIVU[c] = (F)((DIVX + DIVY + DIVZ) / 3.0);
     }
 }
 
@@ -131,8 +144,8 @@ __global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFields f) {
 //     src/MASSFLUX_CALC_IO.f90:332-416), and 0 before that (MEMALLOCT.f90:209).
 //     It is therefore not computed.  The v row j = 1 is left unwritten; the
 //     Crank-Nicolson sweeps treat it as zero.
-template <bool CN>
-__global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st,
+template <bool CN, typename F>
+__global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, double* __restrict__ partial, DevState* __restrict__ st,
                                                   int ns) {
     __shared__ double sred[32];
     __shared__ int is_last;
@@ -141,13 +154,13 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* 
     const long long FS = g.FS;
     const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns], ta = g.talp[ns];
     const double cv = g.cvisc;
-    const double* G = f.G;
-    const double* Q = f.Q;
+    const F* G = f.G;
+    const F* Q = f.Q;
     const double* U0 = f.MU0;
     const double* U = f.MU;
-    const double* MS = f.MST;
-    const double* DV = f.DIVU;
-    const double* PR = f.PR;
+    const F* MS = f.MST;
+    const F* DV = f.DIVU;
+    const F* PR = f.PR;
     double bulk = 0.0;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
@@ -378,17 +391,17 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* 
         if constexpr (CN) r3 = r3 + coa * im3;
         r3 = r3 - io_pgm(f, c, ckm, pc, pkm, ta * dt * g.dzi);
         if (ig == 3) r3 = r3 + f.DST[c + 2 * FS] * (cob / 1.0);
-        f.EX0[ii] = ex1;
-        f.EX0[ii + 2 * g.FI] = ex3;
-        f.RHS[ii] = r1;
-        f.RHS[ii + 2 * g.FI] = r3;
+        f.EX0[ii] = (F)ex1;
+        f.EX0[ii + 2 * g.FI] = (F)ex3;
+        f.RHS[ii] = (F)r1;
+        f.RHS[ii + 2 * g.FI] = (F)r3;
         if (j >= 2) {
             double r2 = (tg * ex2 + tr * e02) * dt;
             if constexpr (CN) r2 = r2 + coa * im2;
             r2 = r2 - io_pgm(f, c, cjm, pc, pjm, ta * dt * dycij / 1.0);
             if (ig == 2) r2 = r2 + f.DST[c + FS] * (cob / 1.0);
-            f.EX0[ii + g.FI] = ex2;
-            f.RHS[ii + g.FI] = r2;
+            f.EX0[ii + g.FI] = (F)ex2;
+            f.RHS[ii + g.FI] = (F)r2;
         }
         bulk += r1 / dyfij / 1.0;
     }
@@ -413,7 +426,8 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFields f, double* 
 }
 
 // bulk forcing (RHS_MOM_EXPLICIT_io :228-265) + MASSFLUX_CALC_io
-__global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
     const long long tot = (long long)g.L * g.M * g.N;
     double dpg = 0.0;
     if (g.iflowdriven == 1) dpg = st->bulksum / g.volm;
@@ -424,17 +438,17 @@ __global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFields f, const 
         const long long c = pidx(g, i, j, k), ii = iidx(g, i, j, k);
         const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS];
         const double r1 = f.RHS[ii] - dpg, r3 = f.RHS[ii + 2 * g.FI];
-        f.G[c] = g1 + r1;
-        f.G[c + 2 * g.FS] = g3 + r3;
-        if (j >= 2) f.G[c + g.FS] = g2 + f.RHS[ii + g.FI];
+        f.G[c] = (F)(g1 + r1);
+        f.G[c + 2 * g.FS] = (F)(g3 + r3);
+        if (j >= 2) f.G[c + g.FS] = (F)(g2 + (double)f.RHS[ii + g.FI]);
     }
 }
 
 // DIVG_io + forward x transform (same tiling as k_div_fftx)
 // DRHO: DrhoDtP of the thermal solver, or NULL (zero) while it is off;
 // the divergence is divided by wdiv (DIVG.f90:78-82)
-template <int N1, int N2>
-__global__ void __launch_bounds__(PX_NT, PX_MINB) k_io_div_fftx(Geo g, const double* __restrict__ G, double* __restrict__ RHSLL,
+template <int N1, int N2, typename F>
+__global__ void __launch_bounds__(PX_NT, PX_MINB) k_io_div_fftx(Geo g, const F* __restrict__ G, double* __restrict__ RHSLL,
                                                        double2* __restrict__ SP, const DevState* __restrict__ st, int ns,
                                                        const double* __restrict__ DRHO, double wdiv) {
     extern __shared__ double2 smc[];
@@ -486,7 +500,8 @@ __global__ void __launch_bounds__(PX_NT, PX_MINB) k_io_div_fftx(Geo g, const dou
 // PRCALC_io + MASSFLUX_UPDATE_io + VELOCITY_CALC_io.  RHSLL == NULL: the
 // explicit scheme's PR += DPH; otherwise the Crank-Nicolson scheme's
 // PR += DPH - BE * RHSLLPHI_io, BE = alpha*dt/(2 Re) (src/PRESSURE_CORRECTION.f90:113-123).
-__global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFields f, const double* __restrict__ DPH,
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFieldsT<F> f, const double* __restrict__ DPH,
                                                       const DevState* __restrict__ st, int ns,
                                                       const double* __restrict__ RHSLL) {
     const int L = g.L, M = g.M, N = g.N;
@@ -504,24 +519,25 @@ __global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFields f, const d
         const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS], pr = f.PR[c];
         const double d1 = f.DST[c], d2 = f.DST[c + g.FS], d3 = f.DST[c + 2 * g.FS];
         const double pn = RHSLL ? pr + ph - be * RHSLL[iidx(g, i, j, k)] : pr + ph;
-        f.PR[c] = pn;
-        if (j == 1) f.PR[pidx(g, i, 0, k)] = pn;
-        if (j == M) f.PR[pidx(g, i, M + 1, k)] = pn;
+        f.PR[c] = (F)pn;
+        if (j == 1) f.PR[pidx(g, i, 0, k)] = (F)pn;
+        if (j == M) f.PR[pidx(g, i, M + 1, k)] = (F)pn;
         const double n1 = g1 - (ph - phim) * (dt * ta * g.dxi);
         const double n3 = g3 - (ph - phkm) * (dt * ta * g.dzi);
-        f.G[c] = n1;
-        f.G[c + 2 * g.FS] = n3;
-        f.Q[c] = n1 / d1;
-        f.Q[c + 2 * g.FS] = n3 / d3;
+        f.G[c] = (F)n1;
+        f.G[c + 2 * g.FS] = (F)n3;
+        f.Q[c] = (F)(n1 / d1);
+        f.Q[c + 2 * g.FS] = (F)(n3 / d3);
         if (j >= 2) {
             const double n2 = g2 - (ph - phjm) * (dt * ta * g.dyci[j] / 1.0);
-            f.G[c + g.FS] = n2;
-            f.Q[c + g.FS] = n2 / d2;
+            f.G[c + g.FS] = (F)n2;
+            f.Q[c + g.FS] = (F)(n2 / d2);
         }
     }
 }
 
-__global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFields f, double* __restrict__ partial, DevState* __restrict__ st) {
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFieldsT<F> f, double* __restrict__ partial, DevState* __restrict__ st) {
     __shared__ double sred[32];
     const int L = g.L, N = g.N;
     const long long tot = (long long)L * g.M * N;
@@ -531,10 +547,10 @@ __global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFields f, double* __r
         int i, j, k;
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
-        const double* Q = f.Q;
-        double q = (fabs((Q[c] + Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
-                    fabs((Q[c + g.FS] + Q[c + g.FS + L]) * g.dyfi[j] * 1.0) +
-                    fabs((Q[c + 2 * g.FS] + Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
+        const F* Q = f.Q;
+        double q = (fabs(((double)Q[c] + (double)Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
+                    fabs(((double)Q[c + g.FS] + (double)Q[c + g.FS + L]) * g.dyfi[j] * 1.0) +
+                    fabs(((double)Q[c + 2 * g.FS] + (double)Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
         const double vcf = 2.0 * g.cvisc * (g.dxqi + g.dzqi * 1.0 + g.dyfi[j] * g.dyfi[j]) * f.MU[c] / f.DEN[c];
         if (!(q == q) || !(vcf == vcf)) bad = true;
         q = fmax(q, vcf);
@@ -550,7 +566,8 @@ __global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFields f, double* __r
 // main domain: max over the interior of |div G + DrhoDtP| (all three ranges of
 // MAXDIVGV_io coincide).  Per-block maxima; k_maxdiv_final reduces them.  DRHO
 // is NULL while the thermal solver is off (DrhoDtP = 0).
-__global__ void __launch_bounds__(IO_NT) k_io_divgck(Geo g, const double* __restrict__ G,
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_io_divgck(Geo g, const F* __restrict__ G,
                                                      const double* __restrict__ DRHO, double* __restrict__ partial) {
     __shared__ double sred[32];
     const int L = g.L, N = g.N;
@@ -560,9 +577,9 @@ __global__ void __launch_bounds__(IO_NT) k_io_divgck(Geo g, const double* __rest
         int i, j, k;
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
-        const double DIVX = (G[pidx(g, wrapp(i, L), j, k)] - G[c]) * g.dxi;
-        const double DIVY = (G[c + g.FS + L] - G[c + g.FS]) * (g.dyfi[j] * 1.0);
-        const double DIVZ = (G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - G[c + 2 * g.FS]) * (g.dzi * 1.0);
+        const double DIVX = ((double)G[pidx(g, wrapp(i, L), j, k)] - (double)G[c]) * g.dxi;
+        const double DIVY = ((double)G[c + g.FS + L] - (double)G[c + g.FS]) * (g.dyfi[j] * 1.0);
+        const double DIVZ = ((double)G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - (double)G[c + 2 * g.FS]) * (g.dzi * 1.0);
         const double DTRHO = DRHO ? DRHO[c] : 0.0;
         const double DQCAP = DIVX + DIVY + DIVZ + DTRHO;
         mx = fmax(fabs(DQCAP), mx);

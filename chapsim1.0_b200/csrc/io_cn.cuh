@@ -57,8 +57,8 @@ __device__ __forceinline__ double cn_dpgrns(const Geo& g, const DevState* st, in
 }
 
 // x lines (j, k); component blockIdx.y (0 u, 1 v, 2 w)
-template <int S>
-__global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+template <int S, typename F>
+__global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smx[];
     constexpr int SEG = 32 * (S + 1);
     const int L = g.L, M = g.M;
@@ -75,9 +75,9 @@ __global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFields f, co
     const double fac = 0.50 * g.talp[ns] * st->dt * g.cvisc;
     const double coe1 = fac * 4.0 / 3.0 * g.dxqi, coe2 = fac * g.dxqi;
     const double dpg = comp == 0 ? cn_dpgrns(g, st, ns) : 0.0;
-    const double* D = f.DST + comp * g.FS;
-    const double* ms = f.MST + (comp == 1 ? 0 : g.FS);
-    double* R = f.RHS + comp * g.FI;
+    const F* D = f.DST + comp * g.FS;
+    const F* ms = f.MST + (comp == 1 ? 0 : g.FS);
+    F* R = f.RHS + comp * g.FI;
 #pragma unroll 4  // several rows' coefficient loads in flight
     for (int i = lane; i < L; i += 32) {
         const int im = wrapm(i, L), ip = wrapp(i, L);
@@ -91,20 +91,20 @@ __global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFields f, co
             apu = -coe2 * ms[pp];
         }
         const int s = seg_pos<S>(i);
-        a[s] = amu / D[pm];
-        c[s] = apu / D[pp];
-        b[s] = 1.0 - (amu + apu) / D[p];
-        d[s] = comp == 0 ? R[iidx(g, i, j, k)] - dpg : R[iidx(g, i, j, k)];
+        a[s] = amu / (double)D[pm];
+        c[s] = apu / (double)D[pp];
+        b[s] = 1.0 - (amu + apu) / (double)D[p];
+        d[s] = comp == 0 ? (double)R[iidx(g, i, j, k)] - dpg : (double)R[iidx(g, i, j, k)];
     }
     __syncwarp();
     warp_tdma_smem<S, true>(d, SegCoef<S>{a, b, c}, lane);
     __syncwarp();
-    for (int i = lane; i < L; i += 32) R[iidx(g, i, j, k)] = d[seg_pos<S>(i)];
+    for (int i = lane; i < L; i += 32) R[iidx(g, i, j, k)] = (F)d[seg_pos<S>(i)];
 }
 
 // z lines (i0 .. i0+CN_LINES-1, j); component blockIdx.z
-template <int S>
-__global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+template <int S, typename F>
+__global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smz[];
     constexpr int SEG = 32 * (S + 1);
     constexpr int RSTEP = CN_NT / CN_LINES;
@@ -116,9 +116,9 @@ __global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFields f, co
     const int i = blockIdx.x * CN_LINES + l;
     const double fac = 0.50 * g.talp[ns] * st->dt * g.cvisc;
     const double coe1 = fac * 4.0 / 3.0 * g.dzqi, coe2 = fac * g.dzqi;
-    const double* D = f.DST + comp * g.FS;
-    const double* ms = f.MST + (comp == 0 ? g.FS : 2 * g.FS);
-    double* R = f.RHS + comp * g.FI;
+    const F* D = f.DST + comp * g.FS;
+    const F* ms = f.MST + (comp == 0 ? g.FS : 2 * g.FS);
+    F* R = f.RHS + comp * g.FI;
     double* base = smz + (size_t)l * cn_line_stride(SEG);
 #pragma unroll 4  // several rows' coefficient loads in flight
     for (int k = r0; k < N; k += RSTEP) {
@@ -133,9 +133,9 @@ __global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFields f, co
             apu = -coe2 * ms[pp] * 1.0;
         }
         const int s = seg_pos<S>(k);
-        base[s] = amu / D[pm];
-        base[SEG + s] = 1.0 - (amu + apu) / D[p];
-        base[2 * SEG + s] = apu / D[pp];
+        base[s] = amu / (double)D[pm];
+        base[SEG + s] = 1.0 - (amu + apu) / (double)D[p];
+        base[2 * SEG + s] = apu / (double)D[pp];
         base[3 * SEG + s] = R[iidx(g, i, j, k)];
     }
     __syncthreads();
@@ -145,12 +145,12 @@ __global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFields f, co
         warp_tdma_smem<S, true>(bw + 3 * SEG, SegCoef<S>{bw, bw + SEG, bw + 2 * SEG}, lane);
     }
     __syncthreads();
-    for (int k = r0; k < N; k += RSTEP) R[iidx(g, i, j, k)] = base[3 * SEG + seg_pos<S>(k)];
+    for (int k = r0; k < N; k += RSTEP) R[iidx(g, i, j, k)] = (F)base[3 * SEG + seg_pos<S>(k)];
 }
 
 // y lines (i0 .. i0+CN_LINES-1, k); component blockIdx.z; then G += solution
-template <int S>
-__global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const DevState* __restrict__ st, int ns) {
+template <int S, typename F>
+__global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smy[];
     constexpr int SEG = 32 * (S + 1);
     constexpr int RSTEP = CN_NT / CN_LINES;
@@ -161,33 +161,33 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const
     const int i = blockIdx.x * CN_LINES + l;
     const double fac = 0.50 * g.talp[ns] * st->dt * g.cvisc;
     const double coe1 = fac * 4.0 / 3.0, coe2 = fac;
-    const double* D = f.DST + comp * g.FS;
+    const F* D = f.DST + comp * g.FS;
     const double* amv = g.amvr + comp * (M + 2);
     const double* apv = g.apvr + comp * (M + 2);
-    const double* R = f.RHS + comp * g.FI;
+    const F* R = f.RHS + comp * g.FI;
     double* base = smy + (size_t)l * cn_line_stride(SEG);
 #pragma unroll 3  // several rows' coefficient loads in flight
     for (int j = 1 + r0; j <= M; j += RSTEP) {
         double A, B, C, amu, apu;
         if (comp != 1) {
-            const double* ms = f.MST + (comp == 0 ? 0 : 2 * g.FS);
+            const F* ms = f.MST + (comp == 0 ? 0 : 2 * g.FS);
             if (j == 1) {
                 const double muqt = (f.MU[pidx(g, i, 1, k)] + f.MU[pidx(g, i, 0, k)]) * 0.5;
                 amu = -coe2 * g.amvr1 * muqt;
                 apu = -coe2 * apv[1] * ms[pidx(g, i, 2, k)];
                 A = 0.0;
-                C = apu / D[pidx(g, i, 2, k)];
+                C = apu / (double)D[pidx(g, i, 2, k)];
             } else if (j == M) {
                 const double muqt = (f.MU[pidx(g, i, M, k)] + f.MU[pidx(g, i, M + 1, k)]) * 0.5;
                 amu = -coe2 * amv[M] * ms[pidx(g, i, M, k)];
                 apu = -coe2 * g.apvrn * muqt;
-                A = amu / D[pidx(g, i, M - 1, k)];
+                A = amu / (double)D[pidx(g, i, M - 1, k)];
                 C = 0.0;
             } else {
                 amu = -coe2 * amv[j] * ms[pidx(g, i, j, k)];
                 apu = -coe2 * apv[j] * ms[pidx(g, i, j + 1, k)];
-                A = amu / D[pidx(g, i, j - 1, k)];
-                C = apu / D[pidx(g, i, j + 1, k)];
+                A = amu / (double)D[pidx(g, i, j - 1, k)];
+                C = apu / (double)D[pidx(g, i, j + 1, k)];
             }
         } else {
             amu = -coe1 * amv[j] * f.MU[pidx(g, i, j - 1, k)];
@@ -195,10 +195,10 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const
             // j = 1: the ghost D_STG(:,0,:,2) is the y-periodic halo D_STG(:,M,:,2)
             // of a run on two or more ranks; amu is zero there, so only its
             // finiteness matters.
-            A = amu / D[pidx(g, i, j == 1 ? M : j - 1, k)];
-            C = apu / D[pidx(g, i, j == 1 ? 2 : j, k)];
+            A = amu / (double)D[pidx(g, i, j == 1 ? M : j - 1, k)];
+            C = apu / (double)D[pidx(g, i, j == 1 ? 2 : j, k)];
         }
-        B = 1.0 - (amu + apu) / D[pidx(g, i, j, k)];
+        B = 1.0 - (amu + apu) / (double)D[pidx(g, i, j, k)];
         const int s = seg_pos<S>(j - 1);
         base[s] = A;
         base[SEG + s] = B;
@@ -212,10 +212,10 @@ __global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFields f, const
         warp_tdma_smem<S, false>(bw + 3 * SEG, SegCoef<S>{bw, bw + SEG, bw + 2 * SEG}, lane);
     }
     __syncthreads();
-    double* Gc = f.G + comp * g.FS;
+    F* Gc = f.G + comp * g.FS;
     for (int j = 1 + r0; j <= M; j += RSTEP) {
         if (comp == 1 && j == 1) continue;
         const long long p = pidx(g, i, j, k);
-        Gc[p] = base[3 * SEG + seg_pos<S>(j - 1)] + Gc[p];
+        Gc[p] = (F)(base[3 * SEG + seg_pos<S>(j - 1)] + (double)Gc[p]);
     }
 }

@@ -34,7 +34,8 @@ struct ThermoParams {
     double dhmin, dhmax;    // LIST_DH at IMIN_DH, IMAX_DH
 };
 
-__global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFields f, ThermoFields t, ThermoParams tp,
+template <typename F>
+__global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFieldsT<F> f, ThermoFields t, ThermoParams tp,
                                                    const DevState* __restrict__ st, int ns) {
     const int L = g.L, M = g.M, N = g.N;
     const long long tot = (long long)L * M * N;
@@ -46,9 +47,9 @@ __global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFields f, ThermoF
     const double* Hh = t.ENTH;
     const double* T = t.TEMP;
     const double* K = t.KAP;
-    const double* G1 = f.G;
-    const double* G2 = f.G + g.FS;
-    const double* G3 = f.G + 2 * g.FS;
+    const F* G1 = f.G;
+    const F* G2 = f.G + g.FS;
+    const F* G3 = f.G + 2 * g.FS;
     for (long long q = (long long)blockIdx.x * IO_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, q, i, j, k);
@@ -101,7 +102,8 @@ __global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFields f, ThermoF
 
 // Properties of one padded point from its rho*h; the old DENSITY and
 // Viscousity are kept in DENSITY0 (f.RHO) and Viscousity0 (f.MU0) first.
-__device__ __forceinline__ void eng_point(const PropTab& tb, const double* xdh, const double* xh, const IoFields& f,
+template <typename F>
+__device__ __forceinline__ void eng_point(const PropTab& tb, const double* xdh, const double* xh, const IoFieldsT<F>& f,
                                           const ThermoFields& t, long long p, DevState* st) {
     f.RHO[p] = f.DEN[p];
     f.MU0[p] = f.MU[p];
@@ -125,8 +127,8 @@ __device__ __forceinline__ void stage_keys(const PropTab& tb, double* keys, cons
     xh = keys + tb.n;
 }
 
-template <bool SMEM>
-__global__ void __launch_bounds__(PROP_NT) k_eng_props(PropTab tb, Geo g, IoFields f, ThermoFields t, DevState* st) {
+template <bool SMEM, typename F>
+__global__ void __launch_bounds__(PROP_NT) k_eng_props(PropTab tb, Geo g, IoFieldsT<F> f, ThermoFields t, DevState* st) {
     extern __shared__ double keys[];
     const double* xdh = tb.xdh;
     const double* xh = tb.xh;
@@ -140,8 +142,8 @@ __global__ void __launch_bounds__(PROP_NT) k_eng_props(PropTab tb, Geo g, IoFiel
 }
 
 // ghost rows j = 0 (bottom) and j = M+1 (top), every i and k
-template <bool SMEM>
-__global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFields f, ThermoFields t, DevState* st) {
+template <bool SMEM, typename F>
+__global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFieldsT<F> f, ThermoFields t, DevState* st) {
     extern __shared__ double keys[];
     const double* xdh = tb.xdh;
     const double* xh = tb.xh;
@@ -164,11 +166,12 @@ __global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFields 
     }
 }
 
-__global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFields f, ThermoFields t, int ns) {
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFieldsT<F> f, ThermoFields t, int ns) {
     const int L = g.L, N = g.N;
     const long long tot = (long long)L * g.M * N;
     const double tgam = g.tgam[ns], troh = g.troh[ns];
-    const double* G = f.G;
+    const F* G = f.G;
     const double* G0 = t.G0;
     for (long long q = (long long)blockIdx.x * IO_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * IO_NT) {
         int i, j, k;
@@ -176,18 +179,20 @@ __global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFields f, ThermoField
         const long long c = pidx(g, i, j, k);
         const long long cip = pidx(g, wrapp(i, L), j, k), ckp = pidx(g, i, j, wrapp(k, N)), cjp = pidx(g, i, j + 1, k);
         const double COE2 = g.dyfi[j] * 1.0, COE3 = g.dzi * 1.0;
-        const double DIVX = (G[cip] - G[c]) * g.dxi;
+        const double DIVX = ((double)G[cip] - (double)G[c]) * g.dxi;
         const double DIVX0 = (G0[cip] - G0[c]) * g.dxi;
-        const double DIVY = (G[cjp + g.FS] - G[c + g.FS]) * COE2;
+        const double DIVY = ((double)G[cjp + g.FS] - (double)G[c + g.FS]) * COE2;
         const double DIVY0 = (G0[cjp + g.FS] - G0[c + g.FS]) * COE2;
-        const double DIVZ = (G[ckp + 2 * g.FS] - G[c + 2 * g.FS]) * COE3;
+        const double DIVZ = ((double)G[ckp + 2 * g.FS] - (double)G[c + 2 * g.FS]) * COE3;
         const double DIVZ0 = (G0[ckp + 2 * g.FS] - G0[c + 2 * g.FS]) * COE3;
         t.DRHO[c] = -tgam * (DIVX + DIVY + DIVZ) - troh * (DIVX0 + DIVY0 + DIVZ0);
     }
 }
 
-// G0_io = G_io (interior; the wall values of G never change) and VELOCITY_CALC_io
-__global__ void __launch_bounds__(IO_NT) k_g0_velocity(Geo g, IoFields f, double* __restrict__ G0) {
+// G0_io = G_io (interior; the wall values of G never change) and VELOCITY_CALC_io.
+// G0 is FP64 in both precisions (a copy of the FP32 G in the mixed step).
+template <typename F>
+__global__ void __launch_bounds__(IO_NT) k_g0_velocity(Geo g, IoFieldsT<F> f, double* __restrict__ G0) {
     const long long tot = (long long)g.L * g.M * g.N;
     for (long long q = (long long)blockIdx.x * IO_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * IO_NT) {
         int i, j, k;
@@ -197,8 +202,8 @@ __global__ void __launch_bounds__(IO_NT) k_g0_velocity(Geo g, IoFields f, double
         G0[c] = g1;
         G0[c + g.FS] = g2;
         G0[c + 2 * g.FS] = g3;
-        f.Q[c] = g1 / f.DST[c];
-        f.Q[c + 2 * g.FS] = g3 / f.DST[c + 2 * g.FS];
-        if (j >= 2) f.Q[c + g.FS] = g2 / f.DST[c + g.FS];
+        f.Q[c] = (F)(g1 / (double)f.DST[c]);
+        f.Q[c + 2 * g.FS] = (F)(g3 / (double)f.DST[c + 2 * g.FS]);
+        if (j >= 2) f.Q[c + g.FS] = (F)(g2 / (double)f.DST[c + g.FS]);
     }
 }

@@ -1,4 +1,4 @@
-"""Mixed-precision periodic-channel step (FP32 storage and stencils / CN
+"""Mixed-precision periodic-channel and main-domain steps (FP32 storage and stencils / CN
 sweeps, FP32 spectrum with FP32 x and z transforms; FP64 y-solve of the
 Poisson modes, divergence, projection and bulk-flux sums) against the FP64
 oracle and the FP64 GPU step.
@@ -115,8 +115,89 @@ def test_mixed_statistics_track_fp64_200_steps():
     assert max(drms) <= 1e-2
 
 
-def test_mixed_rejected_for_io_domain():
-    s, _, _ = _setup()
-    with pytest.raises(gpu.ChapsimError) as e:
-        gpu.ChannelIO(s, precision="mixed")
-    assert e.value.code == -6
+# ---------------------------------------------------------------- main (IO) domain
+# Mixed precision of the main-domain step: FP32 storage of the flow fields G,
+# Q, PR, EXPLT0, RHS, D_STG, MU_STG, DivU (stencils and Crank-Nicolson sweeps
+# evaluated from them); FP64 properties, thermal fields, Poisson solve and
+# projection.  Bounds against the FP64 oracle as for the periodic channel:
+# G, Q within 1e-5, P (modulo its mean) within 3e-3, the thermal fields within
+# 1e-5.
+
+def _io_errs(o, c, M):
+    Gg, Qg, Pg = c.download_io()
+    Go, Qo, Po = o.io_get_fields()
+    errs = {}
+    for i, n in enumerate("uvw"):
+        errs["G" + n] = rel(Gg[i][:, 1:M + 1], Go[i][:, 1:M + 1])
+        errs["Q" + n] = rel(Qg[i][:, 1:M + 1], Qo[i][:, 1:M + 1])
+    pg = Pg[:, 1:M + 1] - Pg[:, 1:M + 1].mean()
+    po = Po[:, 1:M + 1] - Po[:, 1:M + 1].mean()
+    errs["P"] = rel(pg, po)
+    return errs
+
+
+@pytest.mark.parametrize("ivis", [0, 1])
+def test_mixed_main_domain_tc8_five_steps(golden_dir, ivis):
+    """From the reference's TC8 step-100 fields with non-uniform properties."""
+    import json
+    import os
+    d = np.load(os.path.join(golden_dir, "tc8_step100_fields.npz"))
+    cs = json.load(open(os.path.join(golden_dir, "tc8_setup.json")))["case"]
+    L, M, N = cs["NCL1"], cs["NCL2"], cs["NCL3"]
+    G = np.zeros((3, N, M + 2, L))
+    PR = np.zeros((N, M + 2, L))
+    for comp, name in enumerate(("G1", "G2", "G3")):
+        G[comp, :, 1:M + 1, :] = d[name].astype(np.float64)
+    PR[:, 1:M + 1, :] = d["P"].astype(np.float64)
+    k, j, i = np.meshgrid(np.arange(N), np.arange(M + 2), np.arange(L), indexing="ij")
+    rho = 1.0 + 0.05 * np.sin(2 * np.pi * i / L) * np.cos(2 * np.pi * k / N) + 0.02 * np.cos(np.pi * j / (M + 2))
+    mu = 1.0 + 0.1 * np.cos(2 * np.pi * i / L + 0.3) * np.sin(np.pi * j / (M + 2))
+    o = Oracle(L, M, N, cs["HX"], cs["HZ"], cs["STR2"], cs["REN"], iFlowDriven=cs["iFlowDriven"],
+               Cf_Given=cs["Cf_Given"], DT0=cs["DT"], DTMIN=1e-6, CFLGV=cs["CFLGV"], threads=8)
+    o.io_set_fields(G, PR, rho, mu, mu)
+    o.io_set_vis_scheme(ivis)
+    s = channel_setup(L, M, N, cs["HX"], cs["HZ"], cs["STR2"], cs["REN"], cs["iFlowDriven"], cs["Cf_Given"])
+    c = gpu.ChannelIO(s, ivisscheme=ivis, precision="mixed")
+    c.upload_io(G, PR, rho, mu, mu)
+    c.set_dt(cs["DT"])
+    assert o.io_run_steps(5)[0] == 0
+    c.advance(5, cs["DT"], 1e-6, cs["CFLGV"])
+    errs = _io_errs(o, c, M)
+    print("mixed main domain (TC8, iVisScheme %d) vs FP64 oracle:" % ivis, errs)
+    for k2, v in errs.items():
+        assert v <= (3e-3 if k2 == "P" else 1e-5), (k2, v)
+    assert c.DIVGCK_io() <= 1e-4
+
+
+def test_mixed_heated_channel_cn_five_steps():
+    import oracle as orc
+    from chapsim import thermo
+    L, M, N, qw = 64, 64, 32, 0.5
+    HX, HZ, STR2, REN = 2 * np.pi, np.pi, 2.0, 2800.0
+    s = channel_setup(L, M, N, HX, HZ, STR2, REN)
+    Q, PR = initial_field(s, 1973, 0.1)
+    rows, T0 = thermo.synthetic_table()
+    tab = thermo.SplineTable.from_rows(rows, T0)
+    cthecd = 1.0 / REN / (tab.ref["M0"] * tab.ref["CP0"] / tab.ref["K0"])
+    DH = np.zeros((N, M + 2, L))
+    DH[:, 1:M + 1, :] = 1e-2 * np.random.default_rng(5).uniform(-1.0, 1.0, (N, M, L))
+    ones = np.ones((N, M + 2, L))
+    o = Oracle(L, M, N, HX, HZ, STR2, REN, DT0=1e-3, DTMIN=1e-6, CFLGV=0.5, threads=8)
+    o.io_set_fields(Q, PR, ones, ones, ones)
+    o.io_set_vis_scheme(1)
+    o.thermal_enable(orc.PropTable(tab.lists), DH, qw, qw, cthecd)
+    o.set_dt(1e-3)
+    c = gpu.ChannelIO(s, ivisscheme=1, precision="mixed")
+    c.upload_io(Q, PR, ones, ones, ones)
+    c.thermal_init(tab, DH, qw, qw, cthecd)
+    c.set_dt(1e-3)
+    assert o.io_run_steps(5)[0] == 0
+    c.advance(5, 1e-3, 1e-6, 0.5)
+    errs = _io_errs(o, c, M)
+    tg, to = c.download_thermal(), o.thermal_get()
+    for k2 in ("DH", "T", "D", "M"):
+        errs[k2] = rel(tg[k2], to[k2])
+    print("mixed heated channel (CN) vs FP64 oracle:", errs)
+    for k2, v in errs.items():
+        assert v <= (3e-3 if k2 == "P" else 1e-5), (k2, v)
+
