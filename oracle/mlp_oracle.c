@@ -8,7 +8,9 @@
  * layers 2 and 3, the activations h1 and h2, and the hidden-layer error dz2)
  * and accumulates in FP32; here the same values are rounded to BF16 (round
  * to nearest even) and the sums are taken in FP64.  Element-wise steps use
- * the GPU's FP32 operations (fmaf, tanhf).  Targets come from the table
+ * the GPU's FP32 operations (fmaf, tanhf); the inference form also rounds each
+ * hidden activation's input and result to FP16, as the GPU's paired
+ * activation does.  Targets come from the table
  * search of thermo_oracle.c, bitwise equal to the GPU's.
  *
  * Parameter layout (FP32): w1[64], b1[64], W2[64][64] (out, in), b2[64],
@@ -40,6 +42,11 @@ static float bf16r(float f) {
     return f;
 }
 
+/* Round to FP16 (round to nearest even) and back: inference evaluates each
+ * hidden activation as a pair instruction on FP16 operands (the GPU's
+ * tanh.approx.f16x2), so its input and its result are FP16 values. */
+static float f16r(float f) { return (float)(_Float16)f; }
+
 static float xnorm(const double* norm, double dh) {
     const double lo = (double)(float)norm[0], hi = (double)(float)norm[1];
     return (float)(2.0 * (dh - lo) / (hi - lo) - 1.0);
@@ -59,11 +66,29 @@ static void forward(const float* p, float x, float* h1, float* h2, float* y) {
     }
 }
 
-/* Model outputs (denormalised) for n points: out[6n] in the order H, T, D, M, K, CP. */
+/* The inference form of forward(): the FP16 rounding of every hidden
+ * activation's input and result, with the exact tanh in between (the GPU's
+ * hardware tanh adds its own approximation, about 2^-11 relative). */
+static void forward_inf(const float* p, float x, float* h1, float* h2, float* y) {
+    for (int i = 0; i < H; ++i) h1[i] = f16r(tanhf(f16r(fmaf(p[P_W1 + i], x, p[P_B1 + i]))));
+    for (int j = 0; j < H; ++j) {
+        double a = 0.0;
+        for (int i = 0; i < H; ++i) a += (double)bf16r(h1[i]) * (double)bf16r(p[P_W2 + j * H + i]);
+        h2[j] = f16r(tanhf(f16r((float)a + p[P_B2 + j])));
+    }
+    for (int k = 0; k < NO; ++k) {
+        double a = 0.0;
+        for (int j = 0; j < H; ++j) a += (double)bf16r(h2[j]) * (double)bf16r(p[P_W3 + k * H + j]);
+        y[k] = (float)a + p[P_B3 + k];
+    }
+}
+
+/* Model outputs (denormalised) for n points, as inference evaluates them:
+ * out[6n] in the order H, T, D, M, K, CP. */
 void orc_mlp_forward(const float* p, const double* norm, int n, const double* dh, double* out) {
     float h1[H], h2[H], y[NO];
     for (int q = 0; q < n; ++q) {
-        forward(p, xnorm(norm, dh[q]), h1, h2, y);
+        forward_inf(p, xnorm(norm, dh[q]), h1, h2, y);
         for (int k = 0; k < NO; ++k) out[(size_t)k * n + q] = (double)((float)norm[2 + k] + (float)norm[2 + NO + k] * y[k]);
     }
 }

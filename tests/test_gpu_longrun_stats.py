@@ -2,8 +2,10 @@
 FP64 step: the chaotic-flow bound of the periodic channel.
 
 The two runs start from the same seeded field on the 128^3 channel
-(4pi x 2 x 4pi/3, Re_tau ~ 180, CFL 0.5), spin up through transition to
-turbulence, and then average the x-z means on the device every few steps
+(4pi x 2 x 4pi/3, Re_tau ~ 180, CFL 0.5; perturbation amplitude 0.3 U_b,
+which transitions, where 0.1 U_b relaminarises), spin up through transition
+to turbulence (Cf settles near 8.7e-3, u_tau near 0.066, Re_tau near 185),
+and then average the x-z means on the device every few steps
 (PP_MEAN_ZX_FLOW_TG + PP_MEAN_T_TG with the asymptotic average,
 src/processing/PP_MEAN_ZX.f90:14-307, src/processing/PP_MEAN_T.f90:343-392).
 By then the instantaneous fields of the two runs have decorrelated (the
@@ -30,8 +32,10 @@ pytestmark = pytest.mark.gpu
 
 WL = "channel128_retau180_fp64"
 AMP = 0.3            # amplitude of the seeded perturbation (times U_b)
-SPIN = 30000         # RK3 steps before the averaging window
-AVG = 30000          # RK3 steps in the averaging window
+SPIN = 30000         # RK3 steps before the averaging window (about 400 time units h/U_b)
+AVG = 60000          # RK3 steps in the averaging window (about 800 time units)
+CHOICE = 13          # kernel variants pinned (sequential y-solve, bulk-staged right-hand side, plane
+                     # transforms), so that every run follows the same trajectory
 EVERY = 20           # steps between samples
 BOUND = 1e-2
 
@@ -44,7 +48,7 @@ def _run(precision):
     c.upload(Q, PR)
     c.set_dt(DT0)
     c.SOLVERRK3_MOM_tg(0)
-    c.autotune()
+    assert c.autotune(force=CHOICE)[0] == CHOICE
     t = 0.0
     for _ in range(SPIN // 1000):
         dt, _ = c.advance(1000, DT0, 1e-6, CFLGV)

@@ -3,9 +3,10 @@ against the CPU oracle of the same network, and against the table search it
 replaces.
 
 * forward: model outputs for the same parameters agree with the oracle to
-  5e-3 of each output's scale.  Inference takes the hardware tanh
-  (tanh.approx.f32, relative error up to about 2^-11) where the oracle takes
-  libm's tanhf, and both round h1, h2 to BF16 (2^-9) after it; a layout or
+  5e-3 of each output's scale.  Inference takes the hardware tanh on FP16
+  pairs (tanh.approx.f16x2, relative error up to about 2^-11) where the oracle
+  takes libm's tanhf between the same FP16 roundings of the activation's input
+  and result, and both round h1, h2 to BF16 (2^-9) after it; a layout or
   indexing fault would show as errors of order 1;
 * gradients of one pass agree with the oracle to 1e-2 of the largest entry
   of each parameter group (FP32 atomics and accumulation order vs FP64);

@@ -144,8 +144,9 @@ def test_noalloc_strided_subblock_against_oracle():
         r[idx] = rng.standard_normal(idx.shape)
         dA, dB, dC, dR = (_dev(x) for x in (*coef, r))
         torch.cuda.synchronize()
-        rc = _lib().chapsim_tdma_lines_noalloc(dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), dR.data_ptr(), None,
-                                               nl, ls, es, n, 1 if cyc else 0,
+        o8 = 8 * off  # the sub-block starts `off` doubles into each array
+        rc = _lib().chapsim_tdma_lines_noalloc(dA.data_ptr() + o8, dB.data_ptr() + o8, dC.data_ptr() + o8,
+                                               dR.data_ptr() + o8, None, nl, ls, es, n, 1 if cyc else 0,
                                                torch.cuda.current_stream().cuda_stream)
         torch.cuda.synchronize()
         assert rc == 0, _err()
