@@ -144,7 +144,8 @@ struct chapsim_ctx {
     double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
     double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
     double* YF2 = nullptr;        // factors of the two-way y-solve, 2 M doubles per line (when chosen)
-    int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way (chapsim_autotune)
+    int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way, 3: sequential with
+                                  // the forward intermediate in shared memory at one block per SM (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
@@ -305,7 +306,7 @@ size_t smem_yw(const Geo& g) {
 
 // forward declaration: DISPATCH_S is defined below
 template <typename C = double2> void launch_ysolve_warp(chapsim_ctx* ctx);
-template <typename C = double2> void launch_ysolve_seq(chapsim_ctx* ctx);
+template <typename C = double2> void launch_ysolve_seq(chapsim_ctx* ctx, bool kg1);
 template <typename C = double2> void launch_ysolve(chapsim_ctx* ctx);
 
 // Kernel attributes are process-wide and several contexts (of different
@@ -366,15 +367,20 @@ long long bulk_smem_limit(F* f) {
 bool valid_S(int s) { return s == 1 || s == 2 || s == 3 || s == 4 || s == 6 || s == 8 || s == 12; }
 
 inline bool ysolve_seq_kg(const Geo& g) { return smem_ysolve_seq(g.M, true) <= (size_t)113 * 1024; }
+// the fourth y-solve variant: the sequential recurrence with its forward
+// intermediate in shared memory at one block per SM, for lines too long for two
+inline bool ysolve_seq_kg1(const Geo& g) {
+    return !ysolve_seq_kg(g) && smem_ysolve_seq(g.M, true) <= (size_t)227 * 1024;
+}
 
 template <typename C>
-void launch_ysolve_seq(chapsim_ctx* ctx) {
+void launch_ysolve_seq(chapsim_ctx* ctx, bool kg1) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
-    // the forward chain's FP64 intermediate: in shared memory where two blocks per SM still fit, else in
-    // place in an FP64 spectrum, else in the FP64 array as scratch
+    // the forward chain's FP64 intermediate: in shared memory where two blocks per SM still fit (or at one
+    // block per SM, kg1), else in place in an FP64 spectrum, else in the FP64 array as scratch
     const int nb = (int)((nl + YS_NT - 1) / YS_NT);
-    if (ysolve_seq_kg(g))
+    if (ysolve_seq_kg(g) || (kg1 && ysolve_seq_kg1(g)))
         launch_pdl(ctx->pdl, k_ysolve_seq<C, true>, nb, YS_NT, smem_ysolve_seq(g.M, true), ctx->stream, g, spec<C>(ctx),
                    ctx->SP, ctx->YF);
     else
@@ -392,7 +398,8 @@ void launch_ysolve_2w(chapsim_ctx* ctx) {
 
 template <typename C>
 void launch_ysolve(chapsim_ctx* ctx) {
-    if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx);
+    if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx, false);
+    else if (ctx->ysolve_kind == 3 && ctx->YF) launch_ysolve_seq<C>(ctx, true);
     else if (ctx->ysolve_kind == 2 && ctx->YF2) launch_ysolve_2w<C>(ctx);
     else launch_ysolve_warp<C>(ctx);
 }
@@ -430,7 +437,7 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw<C>(g))));
     CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq(g.M, false)));
-    CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
+    CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g) || ysolve_seq_kg1(g))));
     CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
     if (ctx->domain == 1 && plane_fft_ok<C>(g))
         P2_DISPATCH(g.L, g.N, CK((plane_fft_attrs<R, XN1, XN2, ZN1, ZN2>(set_smem_void, smem_p2<C>(g)))));
@@ -454,7 +461,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, float>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw<double2>(g))));
     CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq(g.M, false)));
-    CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g))));
+    CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g) || ysolve_seq_kg1(g))));
     CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, double2>, smem_fz(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));
@@ -2076,20 +2083,23 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     auto run_y = [&](int kind) {
         if (spf) {
             if (kind == 0) launch_ysolve_warp<float2>(ctx);
-            else if (kind == 1) launch_ysolve_seq<float2>(ctx);
+            else if (kind == 1) launch_ysolve_seq<float2>(ctx, false);
+            else if (kind == 3) launch_ysolve_seq<float2>(ctx, true);
             else launch_ysolve_2w<float2>(ctx);
         } else {
             if (kind == 0) launch_ysolve_warp<double2>(ctx);
-            else if (kind == 1) launch_ysolve_seq<double2>(ctx);
+            else if (kind == 1) launch_ysolve_seq<double2>(ctx, false);
+            else if (kind == 3) launch_ysolve_seq<double2>(ctx, true);
             else launch_ysolve_2w<double2>(ctx);
         }
     };
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    float t[3] = {0.f, 0.f, 0.f};
+    const bool kg1 = ysolve_seq_kg1(g);
+    float t[4] = {0.f, 0.f, 0.f, 1e30f};
     const int reps = 5;
-    for (int kind = 0; kind < 3; ++kind) {
+    for (int kind = 0; kind < (kg1 ? 4 : 3); ++kind) {
         for (int w = 0; w < 2; ++w) run_y(kind);
         CK(cudaEventRecord(e0, s));
         for (int r = 0; r < reps; ++r) run_y(kind);
@@ -2101,15 +2111,15 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     ctx->launches += 3 * (2 + reps);
     CK(cudaGetLastError());
     if (force >= 0) {
-        ctx->ysolve_kind = (force & 1) ? 1 : ((force & 16) ? 2 : 0);
+        ctx->ysolve_kind = (force & 1) ? 1 : ((force & 16) ? 2 : ((force & 32) ? (kg1 ? 3 : 1) : 0));
     } else {
         int best = 0;
-        for (int kind = 1; kind < 3; ++kind)
+        for (int kind = 1; kind < 4; ++kind)
             if (t[kind] < t[best]) best = kind;
         ctx->ysolve_kind = best;
     }
     CK(cudaStreamSynchronize(s));
-    if (ctx->ysolve_kind != 1) {  // each factor table is read by its own variant only
+    if (ctx->ysolve_kind != 1 && ctx->ysolve_kind != 3) {  // each factor table is read by its own variant only
         cudaFree(ctx->YF);
         ctx->YF = nullptr;
     }
@@ -2202,10 +2212,10 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     cudaEventDestroy(e1);
     if (choice)
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
-                  (ctx->ysolve_kind == 2 ? 16 : 0);
+                  (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
-        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2];
+        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3];
     }
     return CHAPSIM_OK;
 }

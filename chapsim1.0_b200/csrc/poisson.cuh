@@ -48,6 +48,9 @@ template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { retur
 #define PX_TJ 16
 #define PX_NT 128
 #define PX_MINB 4
+// FP32 transforms: eight blocks per SM within 64 registers (twice the warps to
+// hide the latency of the load, transform and store phases)
+template <typename C> __host__ __device__ constexpr int px_minb() { return sizeof(C) == 8 ? 8 : PX_MINB; }
 #define FZ_TQ 16  // z-lines per block
 #define FZ_NT 256
 #define CR_NT 256
@@ -57,7 +60,7 @@ template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { retur
 // mixed-precision step, whose x and z transforms also run in FP32); the
 // divergence and the correction are evaluated in FP64.
 template <typename R, int N1, int N2>
-__global__ void __launch_bounds__(PX_NT, PX_MINB) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
+__global__ void __launch_bounds__(PX_NT, px_minb<SpecT<R>>()) k_div_fftx(Geo g, const R* __restrict__ Q, R* __restrict__ RHSLL,
                                                     SpecT<R>* __restrict__ SP, const DevState* __restrict__ st, int ns) {
     pdl_wait();
     using C = SpecT<R>;
@@ -660,7 +663,7 @@ __global__ void __launch_bounds__(YS_NT) k_ysolve_2w(Geo g, C* SP, double2* G, c
 
 // ---------------------------------------------------------------------------
 template <int N1, int N2, typename C>
-__global__ void __launch_bounds__(PX_NT, PX_MINB) k_fftx_inv(Geo g, const C* __restrict__ SP,
+__global__ void __launch_bounds__(PX_NT, px_minb<C>()) k_fftx_inv(Geo g, const C* __restrict__ SP,
                                                     typename CReal<C>::T* __restrict__ DPH) {
     pdl_wait();
     using T = typename CReal<C>::T;

@@ -376,21 +376,26 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  * the fastest of each group (force = -1), or the ones forced (force = 0..29):
  *   bits 0 and 4: Poisson y-solve, both 0 = warp Thomas/PCR hybrid, bit 0 =
  *          the reference's sequential Thomas recurrence, one thread per mode,
- *          bit 4 = two-way elimination, two threads per mode (bit 0 wins
- *          when both are set);
+ *          bit 4 = two-way elimination, two threads per mode, bit 5 = the
+ *          sequential recurrence with its forward intermediate in shared
+ *          memory at one block per SM (lines longer than two blocks per SM
+ *          allow; elsewhere it means bit 0); the lowest set bit wins;
  *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
  *          0 = fused (one warp per x line, per-thread loads), 1 = split into
  *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
  *          stencil rows staged in shared memory by bulk copies;
  *   bit 3: pressure stage (periodic channel only), 0 = chained x and z
- *          transforms, 1 = fused plane transforms, one block per y row (only
- *          where the row's half spectrum fits one block's shared memory;
- *          otherwise 0 is kept whatever is forced).
- * choice receives the kept setting in the same bit form; ms[8] (may be NULL)
+ *          transforms, 1 = fused plane transforms: one block per y row where
+ *          the row's half spectrum fits one block's shared memory, one
+ *          thread-block cluster per row (the x-z transpose in distributed
+ *          shared memory) for 256- and 384-point planes; otherwise 0 is kept
+ *          whatever is forced.
+ * choice receives the kept setting in the same bit form; ms[9] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
  * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
- * 1e30 where a variant does not apply) and the two-way y-solve.  CONVH0 is restored after the trial
- * launches. */
+ * 1e30 where a variant does not apply), the two-way y-solve and the
+ * sequential y-solve at one block per SM (1e30 where it does not apply).
+ * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 
 /* An ensemble of independent periodic channels (any grids and precisions, one

@@ -162,7 +162,11 @@ def c3_ref():
     return _oracle_run(_workload(C3), 2)
 
 
-@pytest.mark.parametrize("force", COMBOS + [-1])
+# at M = 256 the sequential y-solve can also keep its forward intermediate in shared memory at one block per SM
+COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4) for p in (0, 8)]
+
+
+@pytest.mark.parametrize("force", COMBOS_C3 + [-1])
 def test_c3_variants_two_steps(c3_ref, force):
     """every combination, the fused plane transforms included (a thread-block
     cluster per row at this plane size)"""

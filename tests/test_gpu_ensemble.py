@@ -86,6 +86,41 @@ def test_bulk_staged_rhs_matches_fused(shape, precision, tol):
         assert e <= tol, (i, e)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sequential_ysolve_in_shared_memory_at_one_block(precision):
+    """Lines of 256 rows: the sequential y-solve's forward intermediate does
+    not fit two blocks per SM, so the fourth variant (bit 5) keeps it in
+    shared memory at one block per SM.  The same recurrence as the sequential
+    variant with the intermediate in global memory: bitwise equal fields, and
+    the Poisson solve within 1e-12 of the oracle."""
+    L, M, N = 64, 256, 64
+    s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    if precision == "fp64":
+        o = Oracle(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+        c = gpu.ChannelTG(s)
+        choice, ms = c.autotune(force=32)
+        assert choice == 32 and ms["ysolve_sequential_smem"] < 1e29
+        rhs = np.random.default_rng(9).standard_normal((N, M, L))
+        full = np.zeros((N, M + 2, L))
+        full[:, 1:M + 1, :] = rhs
+        ref = o.poisson(full)
+        got = c.FFT99_POIS3D_periodicxz(rhs)
+        assert rel(got[:, 1:M + 1], ref[:, 1:M + 1]) <= 1e-12
+        c.close()
+    Q, PR = initial_field(s, 13, 0.1)
+    out = []
+    for force in (1, 32):
+        c = gpu.ChannelTG(s, precision=precision)
+        assert c.autotune(force=force)[0] == force
+        c.upload(Q, PR)
+        c.set_dt(2e-3)
+        c.SOLVERRK3_MOM_tg(0)
+        c.advance(3, 2e-3, 1e-6, 0.5)
+        out.append(c.download())
+        c.close()
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+
+
 @pytest.mark.parametrize("shape", [(64, 32, 64), (128, 128, 128), (32, 256, 32)])
 def test_two_way_ysolve_matches_oracle(shape):
     """The two-way y-solve (two threads per mode line meeting at the middle
