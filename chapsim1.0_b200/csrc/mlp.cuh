@@ -205,15 +205,37 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
     uint32_t phase = 0;
     bool ok = true;
     const long long ntiles = (npts + MLP_TILE - 1) / MLP_TILE;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long p = tile * MLP_TILE + tid;
-        long long idx = p;
+    // The global reads of a tile (rho*h, and in field mode the DENSITY and
+    // Viscousity that become DENSITY0 and Viscousity0) are issued one tile
+    // ahead, so their latency overlaps the current tile's layers.
+    auto point_index = [&](long long p) -> long long {
         if (FIELD && p < npts) {
             int i, j, k;
             io_decode(g, p, i, j, k);
-            idx = pidx(g, i, j, k);
+            return pidx(g, i, j, k);
         }
-        const double v = p < npts ? dh[idx] : (double)nm.x_lo;
+        return p;
+    };
+    long long p_nx = (long long)blockIdx.x * MLP_TILE + tid;
+    long long idx_nx = point_index(p_nx);
+    double v_nx = p_nx < npts ? dh[idx_nx] : (double)nm.x_lo;
+    double d_nx = 0.0, m_nx = 0.0;
+    if (FIELD && p_nx < npts) {
+        d_nx = out.D[idx_nx];
+        m_nx = out.M[idx_nx];
+    }
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long p = p_nx, idx = idx_nx;
+        const double v = v_nx, dold = d_nx, mold = m_nx;
+        p_nx = (tile + gridDim.x) * MLP_TILE + tid;
+        if (tile + gridDim.x < ntiles) {
+            idx_nx = point_index(p_nx);
+            v_nx = p_nx < npts ? dh[idx_nx] : (double)nm.x_lo;
+            if (FIELD && p_nx < npts) {
+                d_nx = out.D[idx_nx];
+                m_nx = out.M[idx_nx];
+            }
+        }
         const float x = mlp_x(nm, v);
         float h[MLP_H];
 #pragma unroll
@@ -274,8 +296,8 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
                 for (int k = 0; k < MLP_OUT; ++k) o[k] = (double)(nm.off[k] + nm.scale[k] * (acc[k] + sb3[k]));
             }
             if (FIELD) {
-                out.D0[idx] = out.D[idx];
-                out.M0[idx] = out.M[idx];
+                out.D0[idx] = dold;
+                out.M0[idx] = mold;
             }
             out.H[idx] = o[0]; out.T[idx] = o[1]; out.D[idx] = o[2];
             out.M[idx] = o[3]; out.K[idx] = o[4]; out.CP[idx] = o[5];

@@ -49,7 +49,8 @@ template <> __device__ __forceinline__ float2 from_d2<float2>(double2 a) { retur
 #define PX_NT 128
 #define PX_MINB 4
 // FP32 transforms: eight blocks per SM within 64 registers (twice the warps to
-// hide the latency of the load, transform and store phases)
+// hide the latency of the load, transform and store phases); the z transform
+// likewise runs four FP32 blocks of FZ_NT threads per SM instead of two
 template <typename C> __host__ __device__ constexpr int px_minb() { return sizeof(C) == 8 ? 8 : PX_MINB; }
 #define FZ_TQ 16  // z-lines per block
 #define FZ_NT 256
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(PX_NT, px_minb<SpecT<R>>()) k_div_fftx(Geo g, 
 // ---------------------------------------------------------------------------
 // complex z transform of FZ_TQ consecutive (kx, j) lines (index q = kx + LH*(j-1))
 template <int SIGN, int N1, int N2, typename C>
-__global__ void __launch_bounds__(FZ_NT, 2) k_fftz(Geo g, C* __restrict__ SP) {
+__global__ void __launch_bounds__(FZ_NT, sizeof(C) == 8 ? 4 : 2) k_fftz(Geo g, C* __restrict__ SP) {
     pdl_wait();
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
