@@ -362,6 +362,7 @@ def kernel_bytes(L, precision="fp64"):
         "k_div_fft2c": 4 * w + spec,       # the same, the plane split over a thread-block cluster
         "k_fftz_fwd": 2 * spec, "k_fftz_inv": 2 * spec,
         "k_ysolve_warp": 2 * spec, "k_ysolve_seq": 2 * spec, "k_ysolve_2w": 2 * spec,
+        "k_ysolve_scan": 2 * spec,         # the factors it reads are not algorithmic bytes
         "k_fftx_inv": spec + w,            # spectrum in; DPH out
         "k_fft2_inv": spec + w,            # the same with the inverse z transforms of the plane
         "k_fft2c_inv": spec + w,           # the same, the plane split over a thread-block cluster

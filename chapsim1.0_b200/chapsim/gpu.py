@@ -71,7 +71,16 @@ def step_kernel_slots(choice: int = 0, plane_cluster: bool = False):
     transforms (one block per row, or a cluster per row when plane_cluster)
     the two z-transform slots stay empty and are named None."""
     rhs = {0: "k_rhs_xsweep", 1: "k_rhs_point+k_xsweep", 2: "k_rhs_xsweep_bulk"}[(choice >> 1) & 3]
-    ys = "k_ysolve_seq" if choice & 33 else ("k_ysolve_2w" if choice & 16 else "k_ysolve_warp")
+    if choice & 1:
+        ys = "k_ysolve_seq"
+    elif choice & 16:
+        ys = "k_ysolve_2w"
+    elif choice & 32:
+        ys = "k_ysolve_seq"
+    elif choice & 192:
+        ys = "k_ysolve_scan"
+    else:
+        ys = "k_ysolve_warp"
     if choice & 8 and plane_cluster:
         pre = ["k_div_fft2c", None, ys, None, "k_fft2c_inv"]
     elif choice & 8:
@@ -582,15 +591,18 @@ class ChannelTG:
         this grid, or forces them (bit 0: sequential y-solve; bits 1-2: right-hand
         sides 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane
         transforms; bit 4: two-way y-solve; bit 5: sequential y-solve with its
-        forward intermediate in shared memory at one block per SM); returns
+        forward intermediate in shared memory at one block per SM; bit 6: warp
+        affine scans over the sequential factors; bit 7: the same with the
+        factors formed in the kernel); returns
         (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 9)()
+        ms = (ctypes.c_float * 11)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         self.choice = ch.value
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
-                          "pressure_plane": ms[6], "ysolve_two_way": ms[7], "ysolve_sequential_smem": ms[8]}
+                          "pressure_plane": ms[6], "ysolve_two_way": ms[7], "ysolve_sequential_smem": ms[8],
+                          "ysolve_scan": ms[9], "ysolve_scan_otf": ms[10]}
 
 
 class Ensemble:

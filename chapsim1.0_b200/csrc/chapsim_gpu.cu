@@ -144,8 +144,11 @@ struct chapsim_ctx {
     double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
     double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
     double* YF2 = nullptr;        // factors of the two-way y-solve, 2 M doubles per line (when chosen)
+    double* YF3 = nullptr;        // factors of the scan y-solve, 2 M doubles per line, line by line (when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way, 3: sequential with
-                                  // the forward intermediate in shared memory at one block per SM (chapsim_autotune)
+                                  // the forward intermediate in shared memory at one block per SM, 4: warp affine
+                                  // scans over the sequential factors, 5: the same with the factors formed by a
+                                  // scan in the kernel (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
@@ -197,6 +200,7 @@ struct chapsim_ctx {
     // learned property model
     float *mlp_par = nullptr, *mlp_grad = nullptr, *mlp_m1 = nullptr, *mlp_m2 = nullptr, *mlp_loss = nullptr;
     __nv_bfloat16 *mlp_w2 = nullptr, *mlp_w2t = nullptr, *mlp_w3 = nullptr;
+    __half *mlp_w2h = nullptr, *mlp_w3h = nullptr;  // FP16 images for inference (in the same allocation)
     float *mlp_xs = nullptr, *mlp_ys = nullptr;
     double* mlp_dh = nullptr;
     int mlp_cap = 0, mlp_step = 0;
@@ -397,8 +401,29 @@ void launch_ysolve_2w(chapsim_ctx* ctx) {
 }
 
 template <typename C>
+size_t smem_ysc(const Geo& g, bool otf) {
+    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)(otf ? 3 : 1) * g.M * sizeof(double);
+}
+
+template <typename C>
+void launch_ysolve_scan(chapsim_ctx* ctx, bool otf) {
+    const Geo& g = ctx->g;
+    const long long nl = (long long)g.LH * g.N;
+    const int nb = (int)std::min<long long>((nl + YW_L - 1) / YW_L, ctx->nsm);  // persistent: one block per SM
+    if (otf) {
+        DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_scan<S, C, true>, nb, YW_NT, smem_ysc<C>(g, true), ctx->stream,
+                                         g, spec<C>(ctx), (const double*)nullptr)));
+    } else {
+        DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_scan<S, C, false>, nb, YW_NT, smem_ysc<C>(g, false),
+                                         ctx->stream, g, spec<C>(ctx), (const double*)ctx->YF3)));
+    }
+}
+
+template <typename C>
 void launch_ysolve(chapsim_ctx* ctx) {
-    if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx, false);
+    if (ctx->ysolve_kind == 5) launch_ysolve_scan<C>(ctx, true);
+    else if (ctx->ysolve_kind == 4 && ctx->YF3) launch_ysolve_scan<C>(ctx, false);
+    else if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx, false);
     else if (ctx->ysolve_kind == 3 && ctx->YF) launch_ysolve_seq<C>(ctx, true);
     else if (ctx->ysolve_kind == 2 && ctx->YF2) launch_ysolve_2w<C>(ctx);
     else launch_ysolve_warp<C>(ctx);
@@ -436,6 +461,8 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw<C>(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, C, false>, smem_ysc<C>(g, false))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, C, true>, smem_ysc<C>(g, true))));
     CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g) || ysolve_seq_kg1(g))));
     CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
@@ -460,6 +487,8 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, double>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, float>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw<double2>(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, double2, false>, smem_ysc<double2>(g, false))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, double2, true>, smem_ysc<double2>(g, true))));
     CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g) || ysolve_seq_kg1(g))));
     CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
@@ -659,6 +688,10 @@ inline bool io_mixed(const chapsim_ctx* ctx) { return ctx->prec == CHAPSIM_PREC_
 int prop_grid(const chapsim_ctx* ctx, long long npts);
 size_t prop_smem(int n);
 
+MlpOperands mlp_ops(const chapsim_ctx* ctx) {
+    return MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t, ctx->mlp_w2h, ctx->mlp_w3h};
+}
+
 // SOLVERRK3_ENG_io(NS), DENSITY_TIME_DERIVATION, DENSITY_Staggered,
 // MU_Staggered, then G0 = G and VELOCITY_CALC_io of SOLVERRK3_MOM_io
 template <typename F>
@@ -674,7 +707,7 @@ void launch_thermal_substep_t(chapsim_ctx* ctx, int ns) {
         const long long tiles = (tot + MLP_TILE - 1) / MLP_TILE;
         MlpOut out{ctx->tf.ENTH, ctx->tf.TEMP, f.DEN, f.MU, ctx->tf.KAP, ctx->tf.HCP, f.RHO, f.MU0};
         k_mlp_infer<true><<<(int)std::min<long long>(tiles, 4LL * ctx->nsm), MLP_NT, MLP_INF_SMEM, s>>>(
-            ctx->mlp_par, MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t}, ctx->mlp_norm, ctx->tab, g, tot,
+            ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, g, tot,
             ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
         prof_mark(ctx);
         if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
@@ -1012,7 +1045,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->step_exec) cudaGraphExecDestroy(ctx->step_exec);
     cudaFree(ctx->Q); cudaFree(ctx->PR); cudaFree(ctx->H0); cudaFree(ctx->RHS); cudaFree(ctx->RHSLL);
-    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->YF2); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
+    cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->YF2); cudaFree(ctx->YF3); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->twf); cudaFree(ctx->yz); cudaFree(ctx->SPf); cudaFree(ctx->DPHf);
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
@@ -1824,11 +1857,9 @@ int mlp_targets(chapsim_ctx* ctx, int n, const double* dh_host, const MlpNorm& n
     return CHAPSIM_OK;
 }
 
-MlpOperands mlp_ops(const chapsim_ctx* ctx) { return MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t}; }
-
 int mlp_pack(chapsim_ctx* ctx) {
     k_mlp_adam<<<1, 256, 0, ctx->stream>>>(ctx->mlp_par, ctx->mlp_grad, ctx->mlp_m1, ctx->mlp_m2, 0, 0.f, ctx->mlp_w2,
-                                           ctx->mlp_w3, ctx->mlp_w2t);
+                                           ctx->mlp_w3, ctx->mlp_w2t, ctx->mlp_w2h, ctx->mlp_w3h);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return CHAPSIM_OK;
@@ -1868,9 +1899,11 @@ extern "C" int chapsim_mlp_init(chapsim_ctx_t* ctx, double dh_lo, double dh_hi, 
         ctx->mlp_m1 = ctx->mlp_grad + MLP_NPARAM;
         ctx->mlp_m2 = ctx->mlp_m1 + MLP_NPARAM;
         ctx->mlp_loss = ctx->mlp_m2 + MLP_NPARAM;
-        CK(cudaMalloc(&ctx->mlp_w2, (64 * 64 * 2 + 16 * 64) * sizeof(__nv_bfloat16)));
+        CK(cudaMalloc(&ctx->mlp_w2, 2 * (64 * 64 * 2 + 16 * 64) * sizeof(__nv_bfloat16)));
         ctx->mlp_w2t = ctx->mlp_w2 + 64 * 64;
         ctx->mlp_w3 = ctx->mlp_w2t + 64 * 64;
+        ctx->mlp_w2h = reinterpret_cast<__half*>(ctx->mlp_w3 + 16 * 64);
+        ctx->mlp_w3h = ctx->mlp_w2h + 64 * 64;
         CK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_TRN_SMEM));
         CK(cudaFuncSetAttribute(k_mlp_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
         CK(cudaFuncSetAttribute(k_mlp_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
@@ -1967,7 +2000,7 @@ extern "C" int chapsim_mlp_train(chapsim_ctx_t* ctx, int32_t n, const double* dh
         if (int rc = mlp_pass(ctx, n)) return rc;
         ++ctx->mlp_step;
         k_mlp_adam<<<1, 256, 0, ctx->stream>>>(ctx->mlp_par, ctx->mlp_grad, ctx->mlp_m1, ctx->mlp_m2, ctx->mlp_step, lr,
-                                               ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t);
+                                               ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t, ctx->mlp_w2h, ctx->mlp_w3h);
         ctx->launches += 1;
     }
     CK(cudaGetLastError());
@@ -2056,9 +2089,11 @@ extern "C" int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err) {
 }
 
 // ----------------------------- autotuner -----------------------------------
-// Times the two Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
-// Thomas) on this context's grid and keeps the faster.  The spectral array is
-// scratch between substeps, so it is zeroed and solved in place.
+// Times the Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
+// Thomas, two-way, sequential at one block per SM, warp scans over read or
+// in-kernel factors) on this
+// context's grid and keeps the fastest.  The spectral array is scratch
+// between substeps, so it is zeroed and solved in place.
 extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms) {
     if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
     CK(cudaSetDevice(ctx->device));
@@ -2076,6 +2111,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         k_ysolve_2w_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF2);
         CK(cudaGetLastError());
     }
+    if (!ctx->YF3) {
+        CK(cudaMalloc(&ctx->YF3, 2 * nsp * sizeof(double)));
+        k_ysolve_scan_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF3);
+        CK(cudaGetLastError());
+    }
     // the variants are timed on the spectral array the time step uses (FP32 in the mixed-precision step)
     const bool spf = ctx->SPf != nullptr;
     if (spf) CK(cudaMemsetAsync(ctx->SPf, 0, nsp * sizeof(float2), s));
@@ -2085,11 +2125,15 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             if (kind == 0) launch_ysolve_warp<float2>(ctx);
             else if (kind == 1) launch_ysolve_seq<float2>(ctx, false);
             else if (kind == 3) launch_ysolve_seq<float2>(ctx, true);
+            else if (kind == 4) launch_ysolve_scan<float2>(ctx, false);
+            else if (kind == 5) launch_ysolve_scan<float2>(ctx, true);
             else launch_ysolve_2w<float2>(ctx);
         } else {
             if (kind == 0) launch_ysolve_warp<double2>(ctx);
             else if (kind == 1) launch_ysolve_seq<double2>(ctx, false);
             else if (kind == 3) launch_ysolve_seq<double2>(ctx, true);
+            else if (kind == 4) launch_ysolve_scan<double2>(ctx, false);
+            else if (kind == 5) launch_ysolve_scan<double2>(ctx, true);
             else launch_ysolve_2w<double2>(ctx);
         }
     };
@@ -2097,9 +2141,10 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     const bool kg1 = ysolve_seq_kg1(g);
-    float t[4] = {0.f, 0.f, 0.f, 1e30f};
+    float t[6] = {0.f, 0.f, 0.f, 1e30f, 0.f, 0.f};
     const int reps = 5;
-    for (int kind = 0; kind < (kg1 ? 4 : 3); ++kind) {
+    for (int kind = 0; kind < 6; ++kind) {
+        if (kind == 3 && !kg1) continue;
         for (int w = 0; w < 2; ++w) run_y(kind);
         CK(cudaEventRecord(e0, s));
         for (int r = 0; r < reps; ++r) run_y(kind);
@@ -2108,13 +2153,15 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaEventElapsedTime(&t[kind], e0, e1));
         t[kind] /= reps;
     }
-    ctx->launches += 3 * (2 + reps);
+    ctx->launches += (kg1 ? 6 : 5) * (2 + reps);
     CK(cudaGetLastError());
     if (force >= 0) {
-        ctx->ysolve_kind = (force & 1) ? 1 : ((force & 16) ? 2 : ((force & 32) ? (kg1 ? 3 : 1) : 0));
+        ctx->ysolve_kind =
+            (force & 1) ? 1
+                        : ((force & 16) ? 2 : ((force & 32) ? (kg1 ? 3 : 1) : ((force & 64) ? 4 : ((force & 128) ? 5 : 0))));
     } else {
         int best = 0;
-        for (int kind = 1; kind < 4; ++kind)
+        for (int kind = 1; kind < 6; ++kind)
             if (t[kind] < t[best]) best = kind;
         ctx->ysolve_kind = best;
     }
@@ -2126,6 +2173,10 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     if (ctx->ysolve_kind != 2) {
         cudaFree(ctx->YF2);
         ctx->YF2 = nullptr;
+    }
+    if (ctx->ysolve_kind != 4) {
+        cudaFree(ctx->YF3);
+        ctx->YF3 = nullptr;
     }
     // explicit right-hand sides + x sweep: fused, split, or fused with bulk-copy
     // staging (periodic channel).  CONVH0 is state: kept in a temporary copy
@@ -2212,10 +2263,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     cudaEventDestroy(e1);
     if (choice)
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
-                  (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0);
+                  (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0) | (ctx->ysolve_kind == 4 ? 64 : 0) |
+                  (ctx->ysolve_kind == 5 ? 128 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
-        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3];
+        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4]; ms[10] = t[5];
     }
     return CHAPSIM_OK;
 }

@@ -5,9 +5,12 @@
 // judge of its accuracy.
 //
 // Tensor cores: the 64 x 64 hidden layer and the output layer (6 outputs
-// padded to N = 16) of 128-point tiles run as tcgen05.mma kind::f16 with BF16
-// operands in shared memory and FP32 accumulators in tensor memory (TMEM), one
-// elected thread issuing and committing to an mbarrier.  Training uses the
+// padded to N = 16) of 128-point tiles run as tcgen05.mma kind::f16 with
+// 16-bit operands in shared memory and FP32 accumulators in tensor memory
+// (TMEM), one elected thread issuing and committing to an mbarrier.  Training
+// takes BF16 operands; inference takes FP16 ones (weights and activations),
+// because its paired hardware tanh produces FP16 activations that go to the
+// operand tile as they are.  Training uses the
 // same forward pass and two more tcgen05 GEMMs for the backward pass
 // (dL/dh1 = dz2 W2 and dL/dW2 = dz2^T h1); the rank-1 first layer, the small
 // output-layer gradients and the optimiser run on the CUDA cores in FP32.
@@ -24,6 +27,7 @@
 // ends.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include "common.cuh"
 #include "thermo.cuh"
 
@@ -50,11 +54,14 @@ struct MlpNorm {
     float off[MLP_OUT], scale[MLP_OUT];  // output k = off[k] + scale[k] * y[k]
 };
 
-// BF16 operand images in the canonical layout, rebuilt by the optimiser
+// 16-bit operand images in the canonical layout, rebuilt by the optimiser:
+// BF16 for training, FP16 for inference (A and B of one MMA always share the type)
 struct MlpOperands {
     const __nv_bfloat16* w2;   // B of layer 2: rows j (64) x K i (64)
     const __nv_bfloat16* w3;   // B of layer 3: rows k (16, 6 used) x K j (64)
     const __nv_bfloat16* w2t;  // B of dL/dh1: rows i (64) x K j (64) = W2^T
+    const __half* w2h;         // FP16 copies of w2 and w3 for inference
+    const __half* w3h;
 };
 
 __host__ __device__ __forceinline__ int umma_off(int R, int r, int k) {
@@ -72,6 +79,10 @@ __device__ __forceinline__ uint64_t umma_desc(const void* base, int R, int s) {
 // kind::f16 instruction descriptor: BF16 A and B (K-major), FP32 D, M x N
 __host__ __device__ constexpr uint32_t umma_idesc(int M, int N) {
     return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+// the same with FP16 A and B (formats 0)
+__host__ __device__ constexpr uint32_t umma_idesc_f16(int M, int N) {
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
@@ -112,6 +123,25 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int c = 0; c < 16; ++c) v[c] = __uint_as_float(r[c]);
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// The same load without its wait, into raw registers: several loads can be in flight, and
+// their registers hold the data only after tmem_ld_wait().  tmem_tie16() after the wait
+// passes the registers through an (empty) volatile asm, so no use of them can be
+// scheduled above the wait: volatile asm statements keep their order, and every use
+// depends on the tie's outputs.
+__device__ __forceinline__ void tmem_ld16_raw(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_tie16(uint32_t* r) {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]));
+}
 
 // Row r of an R x 64 K-major operand from 64 floats (rounded to BF16), written
 // as eight 16-byte chunks.
@@ -156,27 +186,29 @@ struct MlpOut {
 constexpr int MLP_INF_SMEM = 1024 + 64 * 64 * 2 + 16 * 64 * 2 + 128 * 64 * 2;
 
 // Hardware tanh for inference, two activations per MUFU operation (PTX
-// tanh.approx.f16x2): the pre-activations are rounded to FP16 (relative
-// 2^-11), the tanh is evaluated on the pair (maximum relative error about
-// 2^-11), and the results are widened again.  These roundings sit below the
-// BF16 rounding (2^-9) that every activation takes right after, as the
-// tensor-core operand; the pair costs one MUFU operation instead of two.
+// tanh.approx.f16x2): the FP32 pre-activations are rounded to FP16 (relative
+// 2^-11) and the tanh is evaluated on the pair (maximum relative error about
+// 2^-11).  The FP16 pair is the next layer's operand as it stands: inference
+// multiplies FP16 activations by FP16 weights (a finer rounding than the BF16
+// operands of training, 2^-9), so no conversion follows the activation.
 // Training keeps tanhf, the activation of the CPU oracle's gradient check.
-__device__ __forceinline__ void tanh2_mufu(float a, float b, float& ta, float& tb) {
+__device__ __forceinline__ uint32_t tanh2_f16(float a, float b) {
     uint32_t in, out;
     asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(in) : "f"(b), "f"(a));  // upper half b, lower half a
     asm("tanh.approx.f16x2 %0, %1;" : "=r"(out) : "r"(in));
-    float lo, hi;
-    asm("{\n\t.reg .f16 l, h;\n\tmov.b32 {l, h}, %2;\n\tcvt.f32.f16 %0, l;\n\tcvt.f32.f16 %1, h;\n\t}"
-        : "=f"(lo), "=f"(hi) : "r"(out));
-    ta = lo;
-    tb = hi;
+    return out;
+}
+
+// 16-byte chunk c (k = 8c .. 8c+7) of row r of an R x 64 K-major operand
+__device__ __forceinline__ void put_chunk(unsigned char* base, int R, int r, int c, uint32_t a, uint32_t b, uint32_t d,
+                                          uint32_t e) {
+    *reinterpret_cast<uint4*>(base + umma_off(R, r, 8 * c)) = make_uint4(a, b, d, e);
 }
 
 template <bool FIELD>
-__global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ par, MlpOperands ops, MlpNorm nm, PropTab tb,
-                                                      Geo g, long long npts, const double* __restrict__ dh, MlpOut out,
-                                                      PropStatus* ps, unsigned int* err) {
+__global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict__ par, MlpOperands ops, MlpNorm nm,
+                                                         PropTab tb, Geo g, long long npts, const double* __restrict__ dh,
+                                                         MlpOut out, PropStatus* ps, unsigned int* err) {
     extern __shared__ __align__(1024) unsigned char smraw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smraw) + 1023) & ~uintptr_t(1023));
     unsigned char* sW2 = sm;                  // 8 KB
@@ -184,15 +216,17 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
     unsigned char* sA = sW3 + 16 * 64 * 2;    // 16 KB
     __shared__ uint64_t mbar;
     __shared__ uint32_t taddr_s;
-    __shared__ float sw1[MLP_H], sb1[MLP_H], sb2[MLP_H], sb3[MLP_OUT];
+    // first-layer weights and biases interleaved (w1[i], b1[i], w1[i+1], b1[i+1]), second-layer
+    // biases by fours: every thread reads the same values, in 16-byte loads
+    __shared__ float4 swb1[MLP_H / 2], sb2[MLP_H / 4];
+    __shared__ float sb3[MLP_OUT];
     const int tid = threadIdx.x, warp = tid >> 5;
-    copy_smem16(sW2, ops.w2, 64 * 64 * 2);
-    copy_smem16(sW3, ops.w3, 16 * 64 * 2);
-    for (int q = tid; q < MLP_H; q += MLP_NT) {
-        sw1[q] = par[MLP_W1 + q];
-        sb1[q] = par[MLP_B1 + q];
-        sb2[q] = par[MLP_B2 + q];
-    }
+    copy_smem16(sW2, ops.w2h, 64 * 64 * 2);
+    copy_smem16(sW3, ops.w3h, 16 * 64 * 2);
+    for (int q = tid; q < MLP_H / 2; q += MLP_NT)
+        swb1[q] = make_float4(par[MLP_W1 + 2 * q], par[MLP_B1 + 2 * q], par[MLP_W1 + 2 * q + 1], par[MLP_B1 + 2 * q + 1]);
+    for (int q = tid; q < MLP_H / 4; q += MLP_NT)
+        sb2[q] = make_float4(par[MLP_B2 + 4 * q], par[MLP_B2 + 4 * q + 1], par[MLP_B2 + 4 * q + 2], par[MLP_B2 + 4 * q + 3]);
     if (tid < MLP_OUT) sb3[tid] = par[MLP_B3 + tid];
     if (warp == 0) tmem_alloc(&taddr_s, 128);
     if (tid == 0) mbar_init(&mbar, 1);
@@ -237,11 +271,17 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
             }
         }
         const float x = mlp_x(nm, v);
-        float h[MLP_H];
+        // layer 1 (rank one, CUDA cores): h1 = tanh(w1 x + b1), straight into the FP16 operand row
 #pragma unroll
-        for (int i = 0; i < MLP_H; i += 2)
-            tanh2_mufu(fmaf(sw1[i], x, sb1[i]), fmaf(sw1[i + 1], x, sb1[i + 1]), h[i], h[i + 1]);
-        put_row64(sA, MLP_TILE, tid, h);
+        for (int c = 0; c < 8; ++c) {
+            uint32_t hv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float4 wb = swb1[4 * c + u];
+                hv[u] = tanh2_f16(fmaf(wb.x, x, wb.y), fmaf(wb.z, x, wb.w));
+            }
+            put_chunk(sA, MLP_TILE, tid, c, hv[0], hv[1], hv[2], hv[3]);
+        }
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
@@ -249,37 +289,43 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
             tc_fence_after();
 #pragma unroll
             for (int s = 0; s < 4; ++s)
-                umma_bf16(tmem, umma_desc(sA, 128, s), umma_desc(sW2, 64, s), umma_idesc(128, 64), s > 0);
+                umma_bf16(tmem, umma_desc(sA, 128, s), umma_desc(sW2, 64, s), umma_idesc_f16(128, 64), s > 0);
             umma_commit(&mbar);
         }
         ok = mbar_wait_warp(&mbar, phase, err) && ok;
         phase ^= 1;
         tc_fence_after();
-        float acc[16];
+        // layer 2 epilogue: the row's 64 accumulators in four loads and one wait, + b2, tanh, FP16 row
+        uint32_t acc[64];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            tmem_ld16(tmem + lane_base + 16 * q, acc);
-            tmem_ld_wait();
-#pragma unroll
-            for (int c = 0; c < 16; c += 2)
-                tanh2_mufu(acc[c] + sb2[16 * q + c], acc[c + 1] + sb2[16 * q + c + 1], h[16 * q + c], h[16 * q + c + 1]);
-        }
-        put_row64(sA, MLP_TILE, tid, h);
-        fence_async_smem();
-        tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
-            tc_fence_after();
-#pragma unroll
-            for (int s = 0; s < 4; ++s)
-                umma_bf16(tmem + 64, umma_desc(sA, 128, s), umma_desc(sW3, 16, s), umma_idesc(128, 16), s > 0);
-            umma_commit(&mbar);
-        }
-        ok = mbar_wait_warp(&mbar, phase, err) && ok;
-        phase ^= 1;
-        tc_fence_after();
-        tmem_ld16(tmem + lane_base + 64, acc);
+        for (int q = 0; q < 4; ++q) tmem_ld16_raw(tmem + lane_base + 16 * q, acc + 16 * q);
         tmem_ld_wait();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) tmem_tie16(acc + 16 * q);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float4 b0 = sb2[2 * c], b1 = sb2[2 * c + 1];
+            const uint32_t* a = acc + 8 * c;
+            auto f = [&](int e) { return __uint_as_float(a[e]); };
+            put_chunk(sA, MLP_TILE, tid, c, tanh2_f16(f(0) + b0.x, f(1) + b0.y), tanh2_f16(f(2) + b0.z, f(3) + b0.w),
+                      tanh2_f16(f(4) + b1.x, f(5) + b1.y), tanh2_f16(f(6) + b1.z, f(7) + b1.w));
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                umma_bf16(tmem + 64, umma_desc(sA, 128, s), umma_desc(sW3, 16, s), umma_idesc_f16(128, 16), s > 0);
+            umma_commit(&mbar);
+        }
+        ok = mbar_wait_warp(&mbar, phase, err) && ok;
+        phase ^= 1;
+        tc_fence_after();
+        tmem_ld16_raw(tmem + lane_base + 64, acc);
+        tmem_ld_wait();
+        tmem_tie16(acc);
         if (p < npts) {
             double o[6];
             if (v < (double)nm.x_lo || v > (double)nm.x_hi) {
@@ -293,7 +339,8 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_infer(const float* __restrict__ 
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < MLP_OUT; ++k) o[k] = (double)(nm.off[k] + nm.scale[k] * (acc[k] + sb3[k]));
+                for (int k = 0; k < MLP_OUT; ++k)
+                    o[k] = (double)(nm.off[k] + nm.scale[k] * (__uint_as_float(acc[k]) + sb3[k]));
             }
             if (FIELD) {
                 out.D0[idx] = dold;
@@ -520,13 +567,15 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
     if (warp == 0) tmem_dealloc(tmem, 256);
 }
 
-// Adam step on the FP32 master parameters, then the BF16 operand images.
-// grad is cleared for the next pass.  One block of 256 threads.
-// With step == 0 only the BF16 images are rebuilt (after new parameters).
+// Adam step on the FP32 master parameters, then the 16-bit operand images
+// (BF16 for training, FP16 for inference).  grad is cleared for the next
+// pass.  One block of 256 threads.  With step == 0 only the images are
+// rebuilt (after new parameters).
 __global__ void __launch_bounds__(256) k_mlp_adam(float* __restrict__ par, float* __restrict__ grad,
                                                   float* __restrict__ m1, float* __restrict__ m2, int step, float lr,
                                                   __nv_bfloat16* __restrict__ w2, __nv_bfloat16* __restrict__ w3,
-                                                  __nv_bfloat16* __restrict__ w2t) {
+                                                  __nv_bfloat16* __restrict__ w2t, __half* __restrict__ w2h,
+                                                  __half* __restrict__ w3h) {
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const float c1 = 1.f - powf(b1, (float)step), c2 = 1.f - powf(b2, (float)step);
     for (int q = threadIdx.x; step > 0 && q < MLP_NPARAM; q += blockDim.x) {
@@ -544,12 +593,15 @@ __global__ void __launch_bounds__(256) k_mlp_adam(float* __restrict__ par, float
         const __nv_bfloat16 v = __float2bfloat16_rn(par[MLP_W2 + q]);
         *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(w2) + umma_off(64, j, i)) = v;
         *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(w2t) + umma_off(64, i, j)) = v;
+        *reinterpret_cast<__half*>(reinterpret_cast<unsigned char*>(w2h) + umma_off(64, j, i)) =
+            __float2half_rn(par[MLP_W2 + q]);
     }
     for (int q = threadIdx.x; q < MLP_NP * MLP_H; q += blockDim.x) {
         const int k = q / MLP_H, j = q % MLP_H;
         const float v = k < MLP_OUT ? par[MLP_W3 + k * MLP_H + j] : 0.f;
         *reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<unsigned char*>(w3) + umma_off(16, k, j)) =
             __float2bfloat16_rn(v);
+        *reinterpret_cast<__half*>(reinterpret_cast<unsigned char*>(w3h) + umma_off(16, k, j)) = __float2half_rn(v);
     }
 }
 

@@ -102,6 +102,118 @@ __global__ void __launch_bounds__(32) k_factors(Geo g, T* __restrict__ fac, cons
 }
 
 // ---------------------------------------------------------------------------
+// The per-point arithmetic of the explicit right-hand sides, shared by the
+// fused, split and bulk-staged kernels: convection (CONVECTION_X_tg :13-64,
+// CONVECTION_Y_tg :13-114, CONVECTION_Z_tg :13-103), the RK combination with
+// CONVH0, the viscous and pressure-gradient terms (RHS_CvLpGpS_tg :97-161),
+// and the point's bulk-flux integrand.  RhsStencil holds the values a point
+// reads: the three components at the point and its x, y and z neighbours,
+// the cross terms, PR at the point and its -x, -y and -z neighbours, and the
+// three CONVH0 values; RhsLine the coefficients of its (j, substep).
+template <typename R>
+struct RhsStencil {
+    R u, uip, uim, ujp, ujm, ukp, ukm;
+    R v, vip, vim, vjp, vjm, vkp, vkm;
+    R w, wip, wim, wjp, wjm, wkp, wkm;
+    R pc, pim, pjm, pkm;
+    R vjpim, wkpim, ujmip, wjmkp, ukmip, vjpkm;
+    R h0u, h0v, h0w;
+};
+template <typename R>
+struct RhsLine {
+    R dt, tg, tr, coev, coep, dxi, dzi, dxqi, dzqi, c1x, c3x;
+    R wffj, wfbj, wffp, wfbp, dyfij, dycij;
+    R amu, acu, apu, amv, acv, apv, amw, acw, apw;
+    double dyj;
+};
+// v has no increment on row j = 1 (RHS_CvLpGpS_tg starts v at N2I = 2): vrow = j >= 2
+template <typename R>
+__device__ __forceinline__ void rhs_point(const RhsLine<R>& c, const RhsStencil<R>& s, bool vrow, R& Hu, R& Hv, R& Hw,
+                                          R& ru, R& rv, R& rw, double& bulk) {
+    const R u = s.u, uip = s.uip, uim = s.uim, ujp = s.ujp, ujm = s.ujm, ukp = s.ukp, ukm = s.ukm;
+    const R v = s.v, vip = s.vip, vim = s.vim, vjp = s.vjp, vjm = s.vjm, vkp = s.vkp, vkm = s.vkm;
+    const R w = s.w, wip = s.wip, wim = s.wim, wjp = s.wjp, wjm = s.wjm, wkp = s.wkp, wkm = s.wkm;
+    const R pc = s.pc;
+    // ---------------- u (CONVECTION_X_tg) ----------------
+    {
+        const R H11 = ((uip + u) * (uip + u) - (uim + u) * (uim + u)) * c.c1x;
+        const R coe2 = c.dyfij * R(0.5);
+        const R H12 = ((vjp + s.vjpim) * (c.wffp * ujp + c.wfbp * u) - (v + vim) * (c.wffj * u + c.wfbj * ujm)) * coe2;
+        const R coe3 = c.c3x;
+        const R H13 = ((wkp + s.wkpim) * (ukp + u) - (w + wim) * (u + ukm)) * coe3;
+        Hu = -(H11 + H12 + H13);
+        const R rhsc = c.tg * Hu + c.tr * s.h0u;
+        const R rhsl = c.coev * ((uip - R(2) * u + uim) * c.dxqi + (ukp - R(2) * u + ukm) * c.dzqi +
+                                 (ujp * c.apu + u * c.acu + ujm * c.amu));
+        R r = (rhsc + rhsl) * c.dt;
+        ru = r - (pc - s.pim) * c.dxi * c.coep;
+        bulk += (double)ru * c.dyj;
+    }
+    // ---------------- v (CONVECTION_Y_tg), j >= 2 ----------------
+    Hv = R(0);
+    rv = R(0);
+    if (vrow) {
+        const R coe1 = c.dxi * R(0.5);
+        const R H21 = ((c.wffj * uip + c.wfbj * s.ujmip) * (vip + v) - (c.wffj * u + c.wfbj * ujm) * (v + vim)) * coe1;
+        const R coe2 = c.dycij * R(0.5) * R(0.5);
+        const R H22 = ((vjp + v) * (vjp + v) - (v + vjm) * (v + vjm)) * coe2;
+        const R coe31 = c.dzi * R(0.5);
+        const R H23 = ((c.wffj * wkp + c.wfbj * s.wjmkp) * (vkp + v) - (c.wffj * w + c.wfbj * wjm) * (v + vkm)) * coe31;
+        Hv = -(H21 + H22 + H23);
+        const R rhsc = c.tg * Hv + c.tr * s.h0v;
+        const R rhsl = c.coev * ((vip - R(2) * v + vim) * c.dxqi + (vkp - R(2) * v + vkm) * c.dzqi +
+                                 (vjp * c.apv + v * c.acv + vjm * c.amv));
+        R r = (rhsc + rhsl) * c.dt;
+        rv = r - (pc - s.pjm) * c.dycij * c.coep;
+    }
+    // ---------------- w (CONVECTION_Z_tg) ----------------
+    {
+        const R H31 = ((uip + s.ukmip) * (wip + w) - (u + ukm) * (w + wim)) * c.c1x;
+        const R coe2 = c.dyfij * R(0.5);
+        const R H32 = ((vjp + s.vjpkm) * (c.wffp * wjp + c.wfbp * w) - (v + vkm) * (c.wffj * w + c.wfbj * wjm)) * coe2;
+        const R H33 = ((wkp + w) * (wkp + w) - (w + wkm) * (w + wkm)) * c.c3x;
+        Hw = -(H31 + H32 + H33);
+        const R rhsc = c.tg * Hw + c.tr * s.h0w;
+        const R rhsl = c.coev * ((wip - R(2) * w + wim) * c.dxqi + (wkp - R(2) * w + wkm) * c.dzqi +
+                                 (wjp * c.apw + w * c.acw + wjm * c.amw));
+        R r = (rhsc + rhsl) * c.dt;
+        rw = r - (pc - s.pkm) * c.dzi * c.coep;
+    }
+}
+
+// The line coefficients of (j, substep ns) in the real type R.
+template <typename R>
+__device__ __forceinline__ RhsLine<R> rhs_line(const Geo& g, double dt, int ns, double wffj, double wfbj, double wffp,
+                                               double wfbp, double dyfi, double dyci, const double* am, const double* ac,
+                                               const double* ap) {
+    RhsLine<R> c;
+    c.dt = (R)dt;
+    c.tg = (R)g.tgam[ns];
+    c.tr = (R)g.troh[ns];
+    const R ta = (R)g.talp[ns];
+    c.coev = ta * (R)g.cvisc;  // COE1 of RHS_CvLpGpS_tg
+    c.coep = ta * c.dt;        // COE2 (pressure gradient)
+    c.dxi = (R)g.dxi; c.dzi = (R)g.dzi; c.dxqi = (R)g.dxqi; c.dzqi = (R)g.dzqi;
+    c.c1x = (R)(0.5 * 0.5 * g.dxi);  // XND2CL*XND2CL*DXI
+    c.c3x = (R)(0.5 * 0.5 * g.dzi);
+    c.wffj = (R)wffj; c.wfbj = (R)wfbj; c.wffp = (R)wffp; c.wfbp = (R)wfbp;
+    c.dyfij = (R)dyfi; c.dycij = (R)dyci;
+    c.amu = (R)am[0]; c.acu = (R)ac[0]; c.apu = (R)ap[0];
+    c.amv = (R)am[1]; c.acv = (R)ac[1]; c.apv = (R)ap[1];
+    c.amw = (R)am[2]; c.acw = (R)ac[2]; c.apw = (R)ap[2];
+    c.dyj = 1.0 / dyfi / 1.0;  // cell height in the bulk-flux integrand
+    return c;
+}
+template <typename R>
+__device__ __forceinline__ RhsLine<R> rhs_line(const Geo& g, double dt, int ns, int j) {
+    const int M2 = g.M + 2;
+    const double am[3] = {g.amvr[j], g.amvr[M2 + j], g.amvr[2 * M2 + j]};
+    const double ac[3] = {g.acvr[j], g.acvr[M2 + j], g.acvr[2 * M2 + j]};
+    const double ap[3] = {g.apvr[j], g.apvr[M2 + j], g.apvr[2 * M2 + j]};
+    return rhs_line<R>(g, dt, ns, g.wff[j], g.wfb[j], g.wff[j + 1], g.wfb[j + 1], g.dyfi[j], g.dyci[j], am, ac, ap);
+}
+
+// ---------------------------------------------------------------------------
 template <int S, typename R>
 __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
                                                              R* __restrict__ H0, R* __restrict__ RHS,
@@ -118,28 +230,17 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
     const int line = blockIdx.x * RHS_WPB + warp;
     const int j = 1 + line % M, k = line / M;
     const int jp = j + 1, jm = j - 1;
-    const R dt = (R)st->dt;
-    const R tg = (R)g.tgam[ns], tr = (R)g.troh[ns], ta = (R)g.talp[ns];
-    const R coev = ta * (R)g.cvisc;  // COE1 of RHS_CvLpGpS_tg
-    const R coep = ta * dt;          // COE2 (pressure gradient)
-    const R dxi = (R)g.dxi, dzi = (R)g.dzi, dxqi = (R)g.dxqi, dzqi = (R)g.dzqi;
+    const RhsLine<R> cl = rhs_line<R>(g, st->dt, ns, j);
     const int kp = wrapp(k, N), km = wrapm(k, N);
     const R* U = Q;
     const R* V = Q + g.FS;
     const R* W = Q + 2 * g.FS;
     R* sl = sm + warp * 3 * LS;
-    const R c1x = (R)(0.5 * 0.5 * g.dxi);  // XND2CL*XND2CL*DXI
-    const R c3x = (R)(0.5 * 0.5 * g.dzi);
-    const R wffj = (R)g.wff[j], wfbj = (R)g.wfb[j], wffp = (R)g.wff[jp], wfbp = (R)g.wfb[jp];
-    const R dyfij = (R)g.dyfi[j], dycij = (R)g.dyci[j];
-    const double dyj = 1.0 / g.dyfi[j] / 1.0;  // cell height in the bulk-flux integrand
-    const R amu = (R)g.amvr[j], acu = (R)g.acvr[j], apu = (R)g.apvr[j];
-    const R amv = (R)g.amvr[(M + 2) + j], acv = (R)g.acvr[(M + 2) + j], apv = (R)g.apvr[(M + 2) + j];
-    const R amw = (R)g.amvr[2 * (M + 2) + j], acw = (R)g.acvr[2 * (M + 2) + j], apw = (R)g.apvr[2 * (M + 2) + j];
     const long long rowc = pidx(g, 0, j, k), rowjp = pidx(g, 0, jp, k), rowjm = pidx(g, 0, jm, k);
     const long long rowkp = pidx(g, 0, j, kp), rowkm = pidx(g, 0, j, km);
     const long long rowjpkm = pidx(g, 0, jp, km), rowjmkp = pidx(g, 0, jm, kp);
     const long long irow = iidx(g, 0, j, k);
+    const bool vrow = j >= 2;
     // The line's own rows (Q, PR, CONVH0 at (j, k)) are what this kernel reads
     // from DRAM; the neighbour rows are other lines' own rows, fetched by their
     // warps at about the same time.  Requesting the later segments up front
@@ -156,79 +257,88 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
         prefetch_l2(H0 + irow + i + 2 * g.FI);
     }
     double bulk = 0.0;
+    if constexpr (sizeof(R) == 4 && S % 2 == 0) {
+        // FP32: each lane takes two adjacent points (i, i+1) per iteration with 8-byte loads, so
+        // a warp request moves 256 bytes as in FP64 (twice the bytes in flight per load of the
+        // one-point form); the x neighbours outside the pair are single loads.  Rows start at
+        // multiples of L (even), so every pair is 8-byte aligned.
 #pragma unroll 1
-    for (int kk = 0; kk < S; ++kk) {
-        const int i = lane + 32 * kk;
-        const int ip = wrapp(i, L), im = wrapm(i, L);
-        const R u = U[rowc + i], v = V[rowc + i], w = W[rowc + i];
-        const R uip = U[rowc + ip], uim = U[rowc + im];
-        const R ujp = U[rowjp + i], ujm = U[rowjm + i], ukp = U[rowkp + i], ukm = U[rowkm + i];
-        const R vip = V[rowc + ip], vim = V[rowc + im];
-        const R vjp = V[rowjp + i], vjm = V[rowjm + i], vkp = V[rowkp + i], vkm = V[rowkm + i];
-        const R wip = W[rowc + ip], wim = W[rowc + im];
-        const R wjp = W[rowjp + i], wjm = W[rowjm + i], wkp = W[rowkp + i], wkm = W[rowkm + i];
-        const R pc = PR[rowc + i];
-        // every load of the iteration is issued before any store: H0 is read
-        // and written through one pointer, which the compiler cannot reorder
-        const R pim = PR[rowc + im], pjm = PR[rowjm + i], pkm = PR[rowkm + i];
-        const R vjpim = V[rowjp + im], wkpim = W[rowkp + im];
-        const R ujmip = U[rowjm + ip], wjmkp = W[rowjmkp + i];
-        const R ukmip = U[rowkm + ip], vjpkm = V[rowjpkm + i];
-        const long long ii = irow + i;
-        const R h0u = H0[ii];
-        const R h0v = j >= 2 ? H0[ii + g.FI] : R(0);
-        const R h0w = H0[ii + 2 * g.FI];
-        const int pos = seg_pos<S>(i);
-        R Hu, Hv = R(0), Hw, ru, rv = R(0), rw;
-        // ---------------- u (CONVECTION_X_tg) ----------------
-        {
-            const R H11 = ((uip + u) * (uip + u) - (uim + u) * (uim + u)) * c1x;
-            const R coe2 = dyfij * R(0.5);
-            const R H12 = ((vjp + vjpim) * (wffp * ujp + wfbp * u) - (v + vim) * (wffj * u + wfbj * ujm)) * coe2;
-            const R coe3 = c3x;
-            const R H13 = ((wkp + wkpim) * (ukp + u) - (w + wim) * (u + ukm)) * coe3;
-            Hu = -(H11 + H12 + H13);
-            const R rhsc = tg * Hu + tr * h0u;
-            const R rhsl = coev * ((uip - R(2) * u + uim) * dxqi + (ukp - R(2) * u + ukm) * dzqi +
-                                   (ujp * apu + u * acu + ujm * amu));
-            R r = (rhsc + rhsl) * dt;
-            ru = r - (pc - pim) * dxi * coep;
-            bulk += (double)ru * dyj;
+        for (int kk = 0; kk < S / 2; ++kk) {
+            const int i = 2 * lane + 64 * kk;
+            const int il = i == 0 ? L - 1 : i - 1, ir = i + 2 == L ? 0 : i + 2;
+            auto ld2 = [&](const R* b, long long row) { return *reinterpret_cast<const float2*>(b + row + i); };
+            const float2 u2 = ld2(U, rowc), v2 = ld2(V, rowc), w2 = ld2(W, rowc);
+            const float2 ujp = ld2(U, rowjp), ujm = ld2(U, rowjm), ukp = ld2(U, rowkp), ukm = ld2(U, rowkm);
+            const float2 vjp = ld2(V, rowjp), vjm = ld2(V, rowjm), vkp = ld2(V, rowkp), vkm = ld2(V, rowkm);
+            const float2 wjp = ld2(W, rowjp), wjm = ld2(W, rowjm), wkp = ld2(W, rowkp), wkm = ld2(W, rowkm);
+            const float2 pc = ld2(PR, rowc), pjm = ld2(PR, rowjm), pkm = ld2(PR, rowkm);
+            const float2 wjmkp = ld2(W, rowjmkp), vjpkm = ld2(V, rowjpkm);
+            const R ul = U[rowc + il], ur = U[rowc + ir], vl = V[rowc + il], vr = V[rowc + ir];
+            const R wl = W[rowc + il], wr = W[rowc + ir], pl = PR[rowc + il];
+            const R vjpl = V[rowjp + il], wkpl = W[rowkp + il], ujmr = U[rowjm + ir], ukmr = U[rowkm + ir];
+            // every load of the iteration is issued before any store: H0 is read
+            // and written through one pointer, which the compiler cannot reorder
+            const long long ii = irow + i;
+            const float2 h0u = *reinterpret_cast<const float2*>(H0 + ii);
+            const float2 h0v = vrow ? *reinterpret_cast<const float2*>(H0 + ii + g.FI) : make_float2(0.f, 0.f);
+            const float2 h0w = *reinterpret_cast<const float2*>(H0 + ii + 2 * g.FI);
+            const RhsStencil<R> s0{u2.x, u2.y, ul, ujp.x, ujm.x, ukp.x, ukm.x,
+                                   v2.x, v2.y, vl, vjp.x, vjm.x, vkp.x, vkm.x,
+                                   w2.x, w2.y, wl, wjp.x, wjm.x, wkp.x, wkm.x,
+                                   pc.x, pl, pjm.x, pkm.x,
+                                   vjpl, wkpl, ujm.y, wjmkp.x, ukm.y, vjpkm.x,
+                                   h0u.x, h0v.x, h0w.x};
+            const RhsStencil<R> s1{u2.y, ur, u2.x, ujp.y, ujm.y, ukp.y, ukm.y,
+                                   v2.y, vr, v2.x, vjp.y, vjm.y, vkp.y, vkm.y,
+                                   w2.y, wr, w2.x, wjp.y, wjm.y, wkp.y, wkm.y,
+                                   pc.y, pc.x, pjm.y, pkm.y,
+                                   vjp.x, wkp.x, ujmr, wjmkp.y, ukmr, vjpkm.y,
+                                   h0u.y, h0v.y, h0w.y};
+            float2 Hu, Hv, Hw, ru, rv, rw;
+            rhs_point(cl, s0, vrow, Hu.x, Hv.x, Hw.x, ru.x, rv.x, rw.x, bulk);
+            rhs_point(cl, s1, vrow, Hu.y, Hv.y, Hw.y, ru.y, rv.y, rw.y, bulk);
+            *reinterpret_cast<float2*>(H0 + ii) = Hu;
+            if (vrow) *reinterpret_cast<float2*>(H0 + ii + g.FI) = Hv;
+            *reinterpret_cast<float2*>(H0 + ii + 2 * g.FI) = Hw;
+            const int pos = seg_pos<S>(i);  // i + 1 is the next position of the same segment (S even)
+            sl[pos] = ru.x; sl[pos + 1] = ru.y;
+            if (vrow) { sl[LS + pos] = rv.x; sl[LS + pos + 1] = rv.y; }
+            sl[2 * LS + pos] = rw.x; sl[2 * LS + pos + 1] = rw.y;
         }
-        // ---------------- v (CONVECTION_Y_tg), j >= 2 ----------------
-        if (j >= 2) {
-            const R coe1 = dxi * R(0.5);
-            const R H21 = ((wffj * uip + wfbj * ujmip) * (vip + v) - (wffj * u + wfbj * ujm) * (v + vim)) * coe1;
-            const R coe2 = dycij * R(0.5) * R(0.5);
-            const R H22 = ((vjp + v) * (vjp + v) - (v + vjm) * (v + vjm)) * coe2;
-            const R coe31 = dzi * R(0.5);
-            const R H23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v) - (wffj * w + wfbj * wjm) * (v + vkm)) * coe31;
-            Hv = -(H21 + H22 + H23);
-            const R rhsc = tg * Hv + tr * h0v;
-            const R rhsl = coev * ((vip - R(2) * v + vim) * dxqi + (vkp - R(2) * v + vkm) * dzqi +
-                                   (vjp * apv + v * acv + vjm * amv));
-            R r = (rhsc + rhsl) * dt;
-            rv = r - (pc - pjm) * dycij * coep;
+    } else {
+#pragma unroll 1
+        for (int kk = 0; kk < S; ++kk) {
+            const int i = lane + 32 * kk;
+            const int ip = wrapp(i, L), im = wrapm(i, L);
+            RhsStencil<R> sp;
+            sp.u = U[rowc + i]; sp.v = V[rowc + i]; sp.w = W[rowc + i];
+            sp.uip = U[rowc + ip]; sp.uim = U[rowc + im];
+            sp.ujp = U[rowjp + i]; sp.ujm = U[rowjm + i]; sp.ukp = U[rowkp + i]; sp.ukm = U[rowkm + i];
+            sp.vip = V[rowc + ip]; sp.vim = V[rowc + im];
+            sp.vjp = V[rowjp + i]; sp.vjm = V[rowjm + i]; sp.vkp = V[rowkp + i]; sp.vkm = V[rowkm + i];
+            sp.wip = W[rowc + ip]; sp.wim = W[rowc + im];
+            sp.wjp = W[rowjp + i]; sp.wjm = W[rowjm + i]; sp.wkp = W[rowkp + i]; sp.wkm = W[rowkm + i];
+            sp.pc = PR[rowc + i];
+            // every load of the iteration is issued before any store: H0 is read
+            // and written through one pointer, which the compiler cannot reorder
+            sp.pim = PR[rowc + im]; sp.pjm = PR[rowjm + i]; sp.pkm = PR[rowkm + i];
+            sp.vjpim = V[rowjp + im]; sp.wkpim = W[rowkp + im];
+            sp.ujmip = U[rowjm + ip]; sp.wjmkp = W[rowjmkp + i];
+            sp.ukmip = U[rowkm + ip]; sp.vjpkm = V[rowjpkm + i];
+            const long long ii = irow + i;
+            sp.h0u = H0[ii];
+            sp.h0v = vrow ? H0[ii + g.FI] : R(0);
+            sp.h0w = H0[ii + 2 * g.FI];
+            const int pos = seg_pos<S>(i);
+            R Hu, Hv, Hw, ru, rv, rw;
+            rhs_point(cl, sp, vrow, Hu, Hv, Hw, ru, rv, rw, bulk);
+            H0[ii] = Hu;
+            if (vrow) H0[ii + g.FI] = Hv;
+            H0[ii + 2 * g.FI] = Hw;
+            sl[pos] = ru;
+            if (vrow) sl[LS + pos] = rv;
+            sl[2 * LS + pos] = rw;
         }
-        // ---------------- w (CONVECTION_Z_tg) ----------------
-        {
-            const R H31 = ((uip + ukmip) * (wip + w) - (u + ukm) * (w + wim)) * c1x;
-            const R coe2 = dyfij * R(0.5);
-            const R H32 = ((vjp + vjpkm) * (wffp * wjp + wfbp * w) - (v + vkm) * (wffj * w + wfbj * wjm)) * coe2;
-            const R H33 = ((wkp + w) * (wkp + w) - (w + wkm) * (w + wkm)) * c3x;
-            Hw = -(H31 + H32 + H33);
-            const R rhsc = tg * Hw + tr * h0w;
-            const R rhsl = coev * ((wip - R(2) * w + wim) * dxqi + (wkp - R(2) * w + wkm) * dzqi +
-                                   (wjp * apw + w * acw + wjm * amw));
-            R r = (rhsc + rhsl) * dt;
-            rw = r - (pc - pkm) * dzi * coep;
-        }
-        H0[ii] = Hu;
-        if (j >= 2) H0[ii + g.FI] = Hv;
-        H0[ii + 2 * g.FI] = Hw;
-        sl[pos] = ru;
-        if (j >= 2) sl[LS + pos] = rv;
-        sl[2 * LS + pos] = rw;
     }
     __syncwarp();
     // cyclic x sweeps of this warp's three lines (MOMFA1_X_tg starts at N2I = 2 for v)
@@ -483,20 +593,7 @@ __global__ void __launch_bounds__(RP_NT, sizeof(R) == 4 ? 3 : 2) k_rhs_point(Geo
     const int i0 = blockIdx.x * RT_I, j0 = 1 + blockIdx.y * RT_J;
     const int k0 = blockIdx.z * kchunk, k1 = min(N, k0 + kchunk);
     const int i = i0 + ti, j = j0 + tj;
-    const int jp = j + 1;
-    const R dt = (R)st->dt;
-    const R tg = (R)g.tgam[ns], tr = (R)g.troh[ns], ta = (R)g.talp[ns];
-    const R coev = ta * (R)g.cvisc;
-    const R coep = ta * dt;
-    const R dxi = (R)g.dxi, dzi = (R)g.dzi, dxqi = (R)g.dxqi, dzqi = (R)g.dzqi;
-    const R c1x = (R)(0.5 * 0.5 * g.dxi);
-    const R c3x = (R)(0.5 * 0.5 * g.dzi);
-    const R wffj = (R)g.wff[j], wfbj = (R)g.wfb[j], wffp = (R)g.wff[jp], wfbp = (R)g.wfb[jp];
-    const R dyfij = (R)g.dyfi[j], dycij = (R)g.dyci[j];
-    const double dyj = 1.0 / g.dyfi[j] / 1.0;
-    const R amu = (R)g.amvr[j], acu = (R)g.acvr[j], apu = (R)g.apvr[j];
-    const R amv = (R)g.amvr[(M + 2) + j], acv = (R)g.acvr[(M + 2) + j], apv = (R)g.apvr[(M + 2) + j];
-    const R amw = (R)g.amvr[2 * (M + 2) + j], acw = (R)g.acvr[2 * (M + 2) + j], apw = (R)g.apvr[2 * (M + 2) + j];
+    const RhsLine<R> cl = rhs_line<R>(g, st->dt, ns, j);
     // plane kk of the march lives in slot (kk - k0 + 1) % RT_SLOTS; planes k0-1 ..
     // k0+RT_AHEAD go in first, one commit group each
     auto slot_of = [&](int kk) { return ring + ((kk - k0 + 1) % RT_SLOTS) * RT_SLOT; };
@@ -517,58 +614,26 @@ __global__ void __launch_bounds__(RP_NT, sizeof(R) == 4 ? 3 : 2) k_rhs_point(Geo
         const R* Uc = Pc; const R* Vc = Pc + RT_PLANE; const R* Wc = Pc + 2 * RT_PLANE; const R* Rc = Pc + 3 * RT_PLANE;
         const R* Um = Pm; const R* Vm = Pm + RT_PLANE; const R* Wm = Pm + 2 * RT_PLANE; const R* Rm = Pm + 3 * RT_PLANE;
         const R* Up = Pp; const R* Vp = Pp + RT_PLANE; const R* Wp = Pp + 2 * RT_PLANE;
-        const R u = Uc[c], v = Vc[c], w = Wc[c];
-        const R uip = Uc[cip], uim = Uc[cim];
-        const R ujp = Uc[cjp], ujm = Uc[cjm], ukp = Up[c], ukm = Um[c];
-        const R vip = Vc[cip], vim = Vc[cim];
-        const R vjp = Vc[cjp], vjm = Vc[cjm], vkp = Vp[c], vkm = Vm[c];
-        const R wip = Wc[cip], wim = Wc[cim];
-        const R wjp = Wc[cjp], wjm = Wc[cjm], wkp = Wp[c], wkm = Wm[c];
-        const R pc = Rc[c];
-        const R pim = Rc[cim], pjm = Rc[cjm], pkm = Rm[c];
-        const R vjpim = Vc[cjp - 1], wkpim = Wp[cim];
-        const R ujmip = Uc[cjm + 1], wjmkp = Wp[cjm];
-        const R ukmip = Um[cip], vjpkm = Vm[cjp];
+        RhsStencil<R> sp;
+        sp.u = Uc[c]; sp.v = Vc[c]; sp.w = Wc[c];
+        sp.uip = Uc[cip]; sp.uim = Uc[cim];
+        sp.ujp = Uc[cjp]; sp.ujm = Uc[cjm]; sp.ukp = Up[c]; sp.ukm = Um[c];
+        sp.vip = Vc[cip]; sp.vim = Vc[cim];
+        sp.vjp = Vc[cjp]; sp.vjm = Vc[cjm]; sp.vkp = Vp[c]; sp.vkm = Vm[c];
+        sp.wip = Wc[cip]; sp.wim = Wc[cim];
+        sp.wjp = Wc[cjp]; sp.wjm = Wc[cjm]; sp.wkp = Wp[c]; sp.wkm = Wm[c];
+        sp.pc = Rc[c];
+        sp.pim = Rc[cim]; sp.pjm = Rc[cjm]; sp.pkm = Rm[c];
+        sp.vjpim = Vc[cjp - 1]; sp.wkpim = Wp[cim];
+        sp.ujmip = Uc[cjm + 1]; sp.wjmkp = Wp[cjm];
+        sp.ukmip = Um[cip]; sp.vjpkm = Vm[cjp];
         const long long ii = iidx(g, i, j, k);
         const R* Hc = Pc + 4 * RT_PLANE + threadIdx.x;
-        const R h0u = Hc[0];
-        const R h0v = j >= 2 ? Hc[RT_I * RT_J] : R(0);
-        const R h0w = Hc[2 * RT_I * RT_J];
-        R Hu, Hv = R(0), Hw, ru, rv = R(0), rw;
-        {
-            const R H11 = ((uip + u) * (uip + u) - (uim + u) * (uim + u)) * c1x;
-            const R H12 = ((vjp + vjpim) * (wffp * ujp + wfbp * u) - (v + vim) * (wffj * u + wfbj * ujm)) * (dyfij * R(0.5));
-            const R H13 = ((wkp + wkpim) * (ukp + u) - (w + wim) * (u + ukm)) * c3x;
-            Hu = -(H11 + H12 + H13);
-            const R rhsc = tg * Hu + tr * h0u;
-            const R rhsl = coev * ((uip - R(2) * u + uim) * dxqi + (ukp - R(2) * u + ukm) * dzqi +
-                                   (ujp * apu + u * acu + ujm * amu));
-            R rr = (rhsc + rhsl) * dt;
-            ru = rr - (pc - pim) * dxi * coep;
-            bulk += (double)ru * dyj;
-        }
-        if (j >= 2) {
-            const R H21 = ((wffj * uip + wfbj * ujmip) * (vip + v) - (wffj * u + wfbj * ujm) * (v + vim)) * (dxi * R(0.5));
-            const R H22 = ((vjp + v) * (vjp + v) - (v + vjm) * (v + vjm)) * (dycij * R(0.5) * R(0.5));
-            const R H23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v) - (wffj * w + wfbj * wjm) * (v + vkm)) * (dzi * R(0.5));
-            Hv = -(H21 + H22 + H23);
-            const R rhsc = tg * Hv + tr * h0v;
-            const R rhsl = coev * ((vip - R(2) * v + vim) * dxqi + (vkp - R(2) * v + vkm) * dzqi +
-                                   (vjp * apv + v * acv + vjm * amv));
-            R rr = (rhsc + rhsl) * dt;
-            rv = rr - (pc - pjm) * dycij * coep;
-        }
-        {
-            const R H31 = ((uip + ukmip) * (wip + w) - (u + ukm) * (w + wim)) * c1x;
-            const R H32 = ((vjp + vjpkm) * (wffp * wjp + wfbp * w) - (v + vkm) * (wffj * w + wfbj * wjm)) * (dyfij * R(0.5));
-            const R H33 = ((wkp + w) * (wkp + w) - (w + wkm) * (w + wkm)) * c3x;
-            Hw = -(H31 + H32 + H33);
-            const R rhsc = tg * Hw + tr * h0w;
-            const R rhsl = coev * ((wip - R(2) * w + wim) * dxqi + (wkp - R(2) * w + wkm) * dzqi +
-                                   (wjp * apw + w * acw + wjm * amw));
-            R rr = (rhsc + rhsl) * dt;
-            rw = rr - (pc - pkm) * dzi * coep;
-        }
+        sp.h0u = Hc[0];
+        sp.h0v = j >= 2 ? Hc[RT_I * RT_J] : R(0);
+        sp.h0w = Hc[2 * RT_I * RT_J];
+        R Hu, Hv, Hw, ru, rv, rw;
+        rhs_point(cl, sp, j >= 2, Hu, Hv, Hw, ru, rv, rw, bulk);
         H0[ii] = Hu;
         H0[ii + 2 * g.FI] = Hw;
         RHS[ii] = ru;

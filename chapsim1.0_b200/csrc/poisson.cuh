@@ -335,6 +335,269 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_warp(Geo g, C* __restrict__
 }
 
 // ---------------------------------------------------------------------------
+// Fifth y-solve variant: the sequential recurrence's factors (k_ysolve_scan_
+// factors: the same pivots PP and multipliers H as k_ysolve_seq_factors, laid
+// out line by line, F[q*2M + t] = PP_t, F[q*2M + M + t] = H_t) turn both sweeps
+// into first-order linear recurrences,
+//   forward   g_t = (r_t - A_t g_{t-1}) PP_t      (g_0 = r_0 / PP_0, r_0 = 0 on the zero mode)
+//   backward  x_t = g_t - H_t x_{t+1}             (H_{M-1} = 0),
+// which one warp per line evaluates as affine scans: lane l owns rows
+// lS .. lS+S-1, composes its rows' maps, the 32 lane maps are combined by a
+// shuffle scan (5 steps), and each lane then runs its rows' recurrence
+// sequentially from its incoming value, in the reference's operation order.
+// Only the spectrum is read and written (plus the factors): the forward
+// intermediate stays in registers, where the sequential variant moves it
+// through memory.  Lines are staged as in k_ysolve_warp (persistent,
+// double-buffered groups of YW_L lines, one warp per line).  The lane maps are
+// combined in tree order, so the result agrees with the sequential recurrence
+// to rounding (1e-12 of the oracle on the Poisson problem).
+//
+// With OTF the factors are not read but formed in the kernel, by a scan too:
+// the multipliers follow the continued fraction H_t = C_t / (B_t - A_t H_{t-1})
+// (H_0 = C_0 / B_0, C_0 = 0 on the zero mode, C_{M-1} = 0), a Moebius map of
+// H_{t-1} with the matrix [[0, C_t], [-A_t, B_t]] acting on (H, 1).  Each lane
+// multiplies its rows' matrices, the lane products are combined by a shuffle
+// scan (rescaled by powers of two after every product: a map is unchanged by
+// scaling its matrix), the incoming H of a lane is the ratio of its prefix's
+// right column (row 0's matrix has a zero left column, so every prefix is a
+// constant map), and the lane forms its rows' PP_t = 1 / (B_t - H_{t-1} A_t)
+// and H_t = C_t PP_t sequentially, with the expressions of
+// k_ysolve_scan_factors.  Only the spectrum then moves through HBM; the
+// operator's rows (AMPH, ACPH, APPH) are staged in shared memory.
+__device__ __forceinline__ double pow2_scale_of(double m) {
+    // 2^-e for m = 2^e * f, 1 <= f < 2 (m finite and not zero)
+    const int be = (__double2hiint(m) >> 20) & 0x7ff;
+    return __hiloint2double((2046 - be) << 20, 0);
+}
+struct Mob {
+    double p00, p01, p10, p11;
+};
+// x * y (the map y first, then x), rescaled by a power of two
+__device__ __forceinline__ Mob mob_mul(const Mob& x, const Mob& y) {
+    Mob r{x.p00 * y.p00 + x.p01 * y.p10, x.p00 * y.p01 + x.p01 * y.p11, x.p10 * y.p00 + x.p11 * y.p10,
+          x.p10 * y.p01 + x.p11 * y.p11};
+    const double m = fmax(fmax(fabs(r.p00), fabs(r.p01)), fmax(fabs(r.p10), fabs(r.p11)));
+    if (m > 0.0) {
+        const double sc = pow2_scale_of(m);
+        r.p00 *= sc; r.p01 *= sc; r.p10 *= sc; r.p11 *= sc;
+    }
+    return r;
+}
+
+__global__ void k_ysolve_scan_factors(Geo g, double* __restrict__ F) {
+    const int M = g.M, LH = g.LH;
+    const long long nl = (long long)LH * g.N;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nl; q += (long long)gridDim.x * blockDim.x) {
+        const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+        const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+        const double b = g.acph[1] + shift;
+        const double c = q == 0 ? 0.0 : g.apph[1];
+        double hp = c / b;
+        double* f = F + q * 2LL * M;
+        f[0] = b;
+        f[M] = hp;
+        for (int j = 2; j <= M; ++j) {
+            const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
+            hp = j < M ? g.apph[j] * pp : 0.0;
+            f[j - 1] = pp;
+            f[M + j - 1] = hp;
+        }
+    }
+}
+
+template <int S, typename C, bool OTF>
+__global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__ SP, const double* __restrict__ F) {
+    pdl_wait();
+    extern __shared__ __align__(16) unsigned char ysc_raw[];
+    static_assert(YW_NT == 32 * YW_L, "one warp per line of a group");
+    const int M = 32 * S, LH = g.LH;
+    const int LS = M + 33;
+    C* const stage[2] = {reinterpret_cast<C*>(ysc_raw), reinterpret_cast<C*>(ysc_raw) + YW_L * LS};
+    double* const sam = reinterpret_cast<double*>(reinterpret_cast<C*>(ysc_raw) + 2 * YW_L * LS);  // AMPH(t+1)
+    double* const sac = sam + M;  // ACPH(t+1), APPH(t+1) (OTF)
+    double* const sap = sac + M;
+    for (int t = threadIdx.x; t < M; t += YW_NT) {
+        sam[t] = g.amph[t + 1];
+        if (OTF) {
+            sac[t] = g.acph[t + 1];
+            sap[t] = g.apph[t + 1];
+        }
+    }
+    const long long nl = (long long)LH * g.N;
+    const long long ngr = (nl + YW_L - 1) / YW_L;
+    const int ls = threadIdx.x % YW_L, js = threadIdx.x / YW_L;
+    constexpr int RS = YW_NT / YW_L;
+    auto line_ptr = [&](long long q) {
+        const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+        return SP + kx + (long long)LH * ((long long)M * kz);
+    };
+    auto issue = [&](long long gr, C* st) {
+        if (gr < ngr) {
+            const long long q = gr * YW_L + ls;
+            if (q < nl) {
+                const C* src = line_ptr(q);
+                for (int j = js; j < M; j += RS) cp_async_row(st + ls * LS + seg_pos<S>(j), src + (long long)LH * j);
+            }
+        }
+        cp_async_commit();
+    };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = lane * S;
+    issue(blockIdx.x, stage[0]);
+    int cur = 0;
+#pragma unroll 1
+    for (long long gr = blockIdx.x; gr < ngr; gr += gridDim.x, cur ^= 1) {
+        issue(gr + gridDim.x, stage[cur ^ 1]);
+        // this warp's line factors (coalesced: the warp reads 2 x 32 S contiguous doubles)
+        const long long q = gr * YW_L + warp;
+        double pp[S], hh[S];
+        if (!OTF && q < nl) {
+            const double* f = F + q * 2LL * M + r0;
+            if constexpr (S % 2 == 0) {
+#pragma unroll
+                for (int k = 0; k < S; k += 2) {
+                    const double2 a = __ldg(reinterpret_cast<const double2*>(f + k));
+                    const double2 b = __ldg(reinterpret_cast<const double2*>(f + M + k));
+                    pp[k] = a.x; pp[k + 1] = a.y;
+                    hh[k] = b.x; hh[k + 1] = b.y;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < S; ++k) {
+                    pp[k] = __ldg(f + k);
+                    hh[k] = __ldg(f + M + k);
+                }
+            }
+        }
+        cp_async_wait_group<1>();
+        __syncthreads();
+        C* const st = stage[cur];
+        if (OTF && q < nl) {
+            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
+            const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
+            auto cof = [&](int t) { return t == M - 1 || (t == 0 && q == 0) ? 0.0 : sap[t]; };
+            // the lane's product of its rows' maps (row 0: [[0, C_0], [0, B_0]])
+            Mob P{1.0, 0.0, 0.0, 1.0};
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int t = r0 + k;
+                const double a = t == 0 ? 0.0 : sam[t], b = sac[t] + shift, c = cof(t);
+                P = Mob{c * P.p10, c * P.p11, b * P.p10 - a * P.p00, b * P.p11 - a * P.p01};
+            }
+            P = mob_mul(P, Mob{1.0, 0.0, 0.0, 1.0});  // rescale
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                Mob Q;
+                Q.p00 = __shfl_up_sync(0xffffffffu, P.p00, o);
+                Q.p01 = __shfl_up_sync(0xffffffffu, P.p01, o);
+                Q.p10 = __shfl_up_sync(0xffffffffu, P.p10, o);
+                Q.p11 = __shfl_up_sync(0xffffffffu, P.p11, o);
+                if (lane >= o) P = mob_mul(P, Q);
+            }
+            const double num = __shfl_up_sync(0xffffffffu, P.p01, 1), den = __shfl_up_sync(0xffffffffu, P.p11, 1);
+            double hp = lane == 0 ? 0.0 : num / den;  // H of the row before the lane's first
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int t = r0 + k;
+                const double b = sac[t] + shift;
+                if (t == 0) {
+                    hp = cof(0) / b;
+                    pp[k] = b;
+                } else {
+                    const double p = 1.0 / (b - hp * sam[t]);
+                    hp = t < M - 1 ? sap[t] * p : 0.0;
+                    pp[k] = p;
+                }
+                hh[k] = hp;
+            }
+        }
+        if (q < nl) {
+            C* base = st + warp * LS + lane * (S + 1);
+            double2 d[S];
+#pragma unroll
+            for (int k = 0; k < S; ++k) d[k] = to_d2(base[k]);
+            if (q == 0 && lane == 0) d[0] = make_double2(0.0, 0.0);  // the zero mode's pinned first row
+            // forward: the lane's map g_out = A g_in + B over its rows (row 0 ignores g_in)
+            double A = 1.0;
+            double2 B = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int t = r0 + k;
+                if (t == 0) {
+                    A = 0.0;
+                    B = make_double2(d[k].x / pp[k], d[k].y / pp[k]);
+                } else {
+                    const double al = -sam[t] * pp[k];
+                    B = make_double2(al * B.x + d[k].x * pp[k], al * B.y + d[k].y * pp[k]);
+                    A = al * A;
+                }
+            }
+            // inclusive scan over the lanes (lane 0's map first)
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double Ap = __shfl_up_sync(0xffffffffu, A, o);
+                const double Bx = __shfl_up_sync(0xffffffffu, B.x, o), By = __shfl_up_sync(0xffffffffu, B.y, o);
+                if (lane >= o) {
+                    B = make_double2(A * Bx + B.x, A * By + B.y);
+                    A = A * Ap;
+                }
+            }
+            double2 gp = make_double2(__shfl_up_sync(0xffffffffu, B.x, 1), __shfl_up_sync(0xffffffffu, B.y, 1));
+            if (lane == 0) gp = make_double2(0.0, 0.0);
+            // the lane's rows from its incoming value, in the reference's order
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int t = r0 + k;
+                if (t == 0) {
+                    gp = make_double2(d[k].x / pp[k], d[k].y / pp[k]);
+                } else {
+                    const double a = sam[t];
+                    gp = make_double2((d[k].x - a * gp.x) * pp[k], (d[k].y - a * gp.y) * pp[k]);
+                }
+                d[k] = gp;
+            }
+            // backward: x_t = g_t - H_t x_{t+1}; the lane's map gives its first row's x from the next lane's
+            // first row's (x_in): x = A x_in + B, composed from the lane's last row down
+            A = 1.0;
+            B = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int k = S - 1; k >= 0; --k) {
+                const double ga = -hh[k];
+                B = make_double2(ga * B.x + d[k].x, ga * B.y + d[k].y);
+                A = ga * A;
+            }
+            // inclusive scan over the lanes from lane 31 down
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double Ap = __shfl_down_sync(0xffffffffu, A, o);
+                const double Bx = __shfl_down_sync(0xffffffffu, B.x, o), By = __shfl_down_sync(0xffffffffu, B.y, o);
+                if (lane + o < 32) {
+                    B = make_double2(A * Bx + B.x, A * By + B.y);
+                    A = A * Ap;
+                }
+            }
+            double2 xn = make_double2(__shfl_down_sync(0xffffffffu, B.x, 1), __shfl_down_sync(0xffffffffu, B.y, 1));
+            if (lane == 31) xn = make_double2(0.0, 0.0);  // H_{M-1} = 0: the top row is its own g
+#pragma unroll
+            for (int k = S - 1; k >= 0; --k) {
+                xn = make_double2(d[k].x - hh[k] * xn.x, d[k].y - hh[k] * xn.y);
+                base[k] = from_d2<C>(xn);
+            }
+        }
+        __syncthreads();
+        {
+            const long long qs = gr * YW_L + ls;
+            if (qs < nl) {
+                C* dst = line_ptr(qs);
+                for (int j = js; j < M; j += RS) dst[(long long)LH * j] = st[ls * LS + seg_pos<S>(j)];
+            }
+        }
+        __syncthreads();
+    }
+    cp_async_wait_group<0>();
+}
+
+// ---------------------------------------------------------------------------
 // The other y-solve variant: the reference's sequential Thomas recurrence
 // (TDMAIJJ_nonCYC :95-121, zero mode pinned as above), one thread per
 // (kx, kz) line.  The coefficient part of the recurrence (the pivots

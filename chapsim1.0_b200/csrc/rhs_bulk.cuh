@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
                                                                      DevState* __restrict__ st,
                                                                      const R* __restrict__ fac, int ns) {
     pdl_wait();
-    extern __shared__ __align__(128) unsigned char sm_raw[];
+    extern __shared__ __align__(128) unsigned char rb_raw[];
     __shared__ uint64_t bars[RB_WMAX];
     __shared__ double sred[RB_WMAX];
     __shared__ int is_last;
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
     const int nw = blockDim.x >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int LS = L + 33;
-    R* wbase = reinterpret_cast<R*>(sm_raw) + (size_t)warp * rb_warp_elems(L);
+    R* wbase = reinterpret_cast<R*>(rb_raw) + (size_t)warp * rb_warp_elems(L);
     R* const sg = wbase;
     R* sl = wbase + RB_ROWS * L;
     uint64_t* bar = &bars[warp];
@@ -133,15 +133,9 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
     if (lane == 0) {
         if (first < nlines) rb_issue<R>(g, Q, PR, H0, first, sg, bar);
     }
-    const R dt = (R)st->dt;
-    const R tg = (R)g.tgam[ns], tr = (R)g.troh[ns], ta = (R)g.talp[ns];
-    const R coev = ta * (R)g.cvisc;
-    const R coep = ta * dt;
-    const R dxi = (R)g.dxi, dzi = (R)g.dzi, dxqi = (R)g.dxqi, dzqi = (R)g.dzqi;
-    const R c1x = (R)(0.5 * 0.5 * g.dxi);
-    const R c3x = (R)(0.5 * 0.5 * g.dzi);
+    const double dts = st->dt;
     // the x sweep's factor table, staged once per block
-    R* const sfx = reinterpret_cast<R*>(sm_raw) + (size_t)nw * rb_warp_elems(L);
+    R* const sfx = reinterpret_cast<R*>(rb_raw) + (size_t)nw * rb_warp_elems(L);
     {
         const R* fx = fac + FSET_X * FAC_SET;
         for (int t = threadIdx.x; t < TF_NF(S) * 32; t += blockDim.x) sfx[t] = fx[t];
@@ -161,12 +155,8 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
         pending = false;
         const int j = 1 + line % M, k = line / M;
         const RbGeo gc = gn;
-        const R wffj = (R)gc.wffj, wfbj = (R)gc.wfbj, wffp = (R)gc.wffp, wfbp = (R)gc.wfbp;
-        const R dyfij = (R)gc.dyfi, dycij = (R)gc.dyci;
-        const double dyj = 1.0 / gc.dyfi / 1.0;
-        const R amu = (R)gc.am[0], acu = (R)gc.ac[0], apu = (R)gc.ap[0];
-        const R amv = (R)gc.am[1], acv = (R)gc.ac[1], apv = (R)gc.ap[1];
-        const R amw = (R)gc.am[2], acw = (R)gc.ac[2], apw = (R)gc.ap[2];
+        const RhsLine<R> cl = rhs_line<R>(g, dts, ns, gc.wffj, gc.wfbj, gc.wffp, gc.wfbp, gc.dyfi, gc.dyci, gc.am, gc.ac,
+                                          gc.ap);
         const R* sU = sg;          // c, jp, jm, kp, km
         const R* sV = sg + 5 * L;  // c, jp, jm, kp, km, (jp, km)
         const R* sW = sg + 11 * L; // c, jp, jm, kp, km, (jm, kp)
@@ -177,59 +167,21 @@ __global__ void __launch_bounds__(rb_wmax<R>() * 32, 1) k_rhs_xsweep_bulk(Geo g,
         for (int kk = 0; kk < S; ++kk) {
             const int i = lane + 32 * kk;
             const int ip = i + 1 == L ? 0 : i + 1, im = i == 0 ? L - 1 : i - 1;
-            const R u = sU[i], uip = sU[ip], uim = sU[im];
-            const R ujp = sU[L + i], ujm = sU[2 * L + i], ukp = sU[3 * L + i], ukm = sU[4 * L + i];
-            const R v = sV[i], vip = sV[ip], vim = sV[im];
-            const R vjp = sV[L + i], vjm = sV[2 * L + i], vkp = sV[3 * L + i], vkm = sV[4 * L + i];
-            const R w = sW[i], wip = sW[ip], wim = sW[im];
-            const R wjp = sW[L + i], wjm = sW[2 * L + i], wkp = sW[3 * L + i], wkm = sW[4 * L + i];
-            const R pc = sP[i], pim = sP[im], pjm = sP[L + i], pkm = sP[2 * L + i];
-            const R vjpim = sV[L + im], wkpim = sW[3 * L + im];
-            const R ujmip = sU[2 * L + ip], wjmkp = sW[5 * L + i];
-            const R ukmip = sU[4 * L + ip], vjpkm = sV[5 * L + i];
-            const R h0u = sH[i], h0v = j >= 2 ? sH[L + i] : R(0), h0w = sH[2 * L + i];
+            RhsStencil<R> sp;
+            sp.u = sU[i]; sp.uip = sU[ip]; sp.uim = sU[im];
+            sp.ujp = sU[L + i]; sp.ujm = sU[2 * L + i]; sp.ukp = sU[3 * L + i]; sp.ukm = sU[4 * L + i];
+            sp.v = sV[i]; sp.vip = sV[ip]; sp.vim = sV[im];
+            sp.vjp = sV[L + i]; sp.vjm = sV[2 * L + i]; sp.vkp = sV[3 * L + i]; sp.vkm = sV[4 * L + i];
+            sp.w = sW[i]; sp.wip = sW[ip]; sp.wim = sW[im];
+            sp.wjp = sW[L + i]; sp.wjm = sW[2 * L + i]; sp.wkp = sW[3 * L + i]; sp.wkm = sW[4 * L + i];
+            sp.pc = sP[i]; sp.pim = sP[im]; sp.pjm = sP[L + i]; sp.pkm = sP[2 * L + i];
+            sp.vjpim = sV[L + im]; sp.wkpim = sW[3 * L + im];
+            sp.ujmip = sU[2 * L + ip]; sp.wjmkp = sW[5 * L + i];
+            sp.ukmip = sU[4 * L + ip]; sp.vjpkm = sV[5 * L + i];
+            sp.h0u = sH[i]; sp.h0v = j >= 2 ? sH[L + i] : R(0); sp.h0w = sH[2 * L + i];
             const int pos = seg_pos<S>(i);
-            R Hu, Hv = R(0), Hw, ru, rv = R(0), rw;
-            {
-                const R H11 = ((uip + u) * (uip + u) - (uim + u) * (uim + u)) * c1x;
-                const R coe2 = dyfij * R(0.5);
-                const R H12 = ((vjp + vjpim) * (wffp * ujp + wfbp * u) - (v + vim) * (wffj * u + wfbj * ujm)) * coe2;
-                const R coe3 = c3x;
-                const R H13 = ((wkp + wkpim) * (ukp + u) - (w + wim) * (u + ukm)) * coe3;
-                Hu = -(H11 + H12 + H13);
-                const R rhsc = tg * Hu + tr * h0u;
-                const R rhsl = coev * ((uip - R(2) * u + uim) * dxqi + (ukp - R(2) * u + ukm) * dzqi +
-                                       (ujp * apu + u * acu + ujm * amu));
-                R r = (rhsc + rhsl) * dt;
-                ru = r - (pc - pim) * dxi * coep;
-                bulk += (double)ru * dyj;
-            }
-            if (j >= 2) {
-                const R coe1 = dxi * R(0.5);
-                const R H21 = ((wffj * uip + wfbj * ujmip) * (vip + v) - (wffj * u + wfbj * ujm) * (v + vim)) * coe1;
-                const R coe2 = dycij * R(0.5) * R(0.5);
-                const R H22 = ((vjp + v) * (vjp + v) - (v + vjm) * (v + vjm)) * coe2;
-                const R coe31 = dzi * R(0.5);
-                const R H23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v) - (wffj * w + wfbj * wjm) * (v + vkm)) * coe31;
-                Hv = -(H21 + H22 + H23);
-                const R rhsc = tg * Hv + tr * h0v;
-                const R rhsl = coev * ((vip - R(2) * v + vim) * dxqi + (vkp - R(2) * v + vkm) * dzqi +
-                                       (vjp * apv + v * acv + vjm * amv));
-                R r = (rhsc + rhsl) * dt;
-                rv = r - (pc - pjm) * dycij * coep;
-            }
-            {
-                const R H31 = ((uip + ukmip) * (wip + w) - (u + ukm) * (w + wim)) * c1x;
-                const R coe2 = dyfij * R(0.5);
-                const R H32 = ((vjp + vjpkm) * (wffp * wjp + wfbp * w) - (v + vkm) * (wffj * w + wfbj * wjm)) * coe2;
-                const R H33 = ((wkp + w) * (wkp + w) - (w + wkm) * (w + wkm)) * c3x;
-                Hw = -(H31 + H32 + H33);
-                const R rhsc = tg * Hw + tr * h0w;
-                const R rhsl = coev * ((wip - R(2) * w + wim) * dxqi + (wkp - R(2) * w + wkm) * dzqi +
-                                       (wjp * apw + w * acw + wjm * amw));
-                R r = (rhsc + rhsl) * dt;
-                rw = r - (pc - pkm) * dzi * coep;
-            }
+            R Hu, Hv, Hw, ru, rv, rw;
+            rhs_point(cl, sp, j >= 2, Hu, Hv, Hw, ru, rv, rw, bulk);
             H0l[i] = Hu;
             if (j >= 2) H0l[i + g.FI] = Hv;
             H0l[i + 2 * g.FI] = Hw;

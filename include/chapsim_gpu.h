@@ -291,8 +291,9 @@ int chapsim_download_thermal_fields(chapsim_ctx_t* ctx, double* dh, double* h, d
 /* ---- Learned property model (no counterpart in the reference) ----
  * A 1 -> 64 -> 64 -> 6 tanh MLP from rho*h to the six outputs of
  * THERM_PROP_UPDATE_FROM_DH (ENTHALPY, TEMPERATURE, DENSITY, Viscousity,
- * THERMCONDT, HEATCAP), with BF16 tensor-core (tcgen05) layers and FP32
- * accumulation, trained on the GPU against the table search, which stays the
+ * THERMCONDT, HEATCAP), with tensor-core (tcgen05) layers on 16-bit operands
+ * (BF16 in training, FP16 in inference) and FP32 accumulation, trained on the
+ * GPU against the table search, which stays the
  * fallback outside the trained rho*h range and the judge of its accuracy.
  * Parameters (4678 floats): w1[64], b1[64], W2[64][64] (out, in), b2[64],
  * W3[6][64], b3[6]; inputs map [dh_lo, dh_hi] to [-1, 1]; output k is
@@ -373,13 +374,17 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the fastest of each group (force = -1), or the ones forced (force = 0..29):
- *   bits 0 and 4: Poisson y-solve, both 0 = warp Thomas/PCR hybrid, bit 0 =
- *          the reference's sequential Thomas recurrence, one thread per mode,
- *          bit 4 = two-way elimination, two threads per mode, bit 5 = the
- *          sequential recurrence with its forward intermediate in shared
- *          memory at one block per SM (lines longer than two blocks per SM
- *          allow; elsewhere it means bit 0); the lowest set bit wins;
+ * the fastest of each group (force = -1), or the ones forced (force = 0..255):
+ *   bits 0, 4, 5, 6 and 7: Poisson y-solve, all 0 = warp Thomas/PCR hybrid,
+ *          bit 0 = the reference's sequential Thomas recurrence, one thread
+ *          per mode, bit 4 = two-way elimination, two threads per mode,
+ *          bit 5 = the sequential recurrence with its forward intermediate in
+ *          shared memory at one block per SM (lines longer than two blocks
+ *          per SM allow; elsewhere it means bit 0), bit 6 = one warp per mode
+ *          line evaluating the sequential recurrence's two sweeps as affine
+ *          scans over its precomputed factors, bit 7 = the same with the
+ *          factors formed in the kernel by a scan of the continued fraction
+ *          (no factor array); the lowest set bit wins;
  *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
  *          0 = fused (one warp per x line, per-thread loads), 1 = split into
  *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
@@ -390,11 +395,12 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *          thread-block cluster per row (the x-z transpose in distributed
  *          shared memory) for 256- and 384-point planes; otherwise 0 is kept
  *          whatever is forced.
- * choice receives the kept setting in the same bit form; ms[9] (may be NULL)
+ * choice receives the kept setting in the same bit form; ms[11] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
  * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
- * 1e30 where a variant does not apply), the two-way y-solve and the
- * sequential y-solve at one block per SM (1e30 where it does not apply).
+ * 1e30 where a variant does not apply), the two-way y-solve, the
+ * sequential y-solve at one block per SM (1e30 where it does not apply) and
+ * the scan y-solve over read and over in-kernel factors.
  * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 

@@ -8,9 +8,10 @@
  * layers 2 and 3, the activations h1 and h2, and the hidden-layer error dz2)
  * and accumulates in FP32; here the same values are rounded to BF16 (round
  * to nearest even) and the sums are taken in FP64.  Element-wise steps use
- * the GPU's FP32 operations (fmaf, tanhf); the inference form also rounds each
+ * the GPU's FP32 operations (fmaf, tanhf).  The inference form rounds each
  * hidden activation's input and result to FP16, as the GPU's paired
- * activation does.  Targets come from the table
+ * activation does, and its tensor-core operands are FP16 (the activations as
+ * they come out of the activation, the weights rounded to FP16).  Targets come from the table
  * search of thermo_oracle.c, bitwise equal to the GPU's.
  *
  * Parameter layout (FP32): w1[64], b1[64], W2[64][64] (out, in), b2[64],
@@ -68,17 +69,19 @@ static void forward(const float* p, float x, float* h1, float* h2, float* y) {
 
 /* The inference form of forward(): the FP16 rounding of every hidden
  * activation's input and result, with the exact tanh in between (the GPU's
- * hardware tanh adds its own approximation, about 2^-11 relative). */
+ * hardware tanh adds its own approximation, about 2^-11 relative), and FP16
+ * operands of the two tensor-core products (h1 and h2 are FP16 values
+ * already; W2 and W3 are rounded to FP16). */
 static void forward_inf(const float* p, float x, float* h1, float* h2, float* y) {
     for (int i = 0; i < H; ++i) h1[i] = f16r(tanhf(f16r(fmaf(p[P_W1 + i], x, p[P_B1 + i]))));
     for (int j = 0; j < H; ++j) {
         double a = 0.0;
-        for (int i = 0; i < H; ++i) a += (double)bf16r(h1[i]) * (double)bf16r(p[P_W2 + j * H + i]);
+        for (int i = 0; i < H; ++i) a += (double)h1[i] * (double)f16r(p[P_W2 + j * H + i]);
         h2[j] = f16r(tanhf(f16r((float)a + p[P_B2 + j])));
     }
     for (int k = 0; k < NO; ++k) {
         double a = 0.0;
-        for (int j = 0; j < H; ++j) a += (double)bf16r(h2[j]) * (double)bf16r(p[P_W3 + k * H + j]);
+        for (int j = 0; j < H; ++j) a += (double)h2[j] * (double)f16r(p[P_W3 + k * H + j]);
         y[k] = (float)a + p[P_B3 + k];
     }
 }

@@ -41,9 +41,10 @@ TOL_STEP = 1e-11
 THREADS = os.cpu_count() or 8
 DTMIN = 1e-6
 
-# every selectable combination: y-solve (warp 0, sequential 1, two-way 16),
-# right-hand side (fused 0, split 2, bulk-staged 4), pressure (chained 0, plane 8)
-COMBOS = [y | r | p for y in (0, 1, 16) for r in (0, 2, 4) for p in (0, 8)]
+# every selectable combination: y-solve (warp 0, sequential 1, two-way 16, scans over read
+# factors 64, scans with in-kernel factors 128), right-hand side (fused 0, split 2,
+# bulk-staged 4), pressure (chained 0, plane 8)
+COMBOS = [y | r | p for y in (0, 1, 16, 64, 128) for r in (0, 2, 4) for p in (0, 8)]
 
 
 def rel(a, b):

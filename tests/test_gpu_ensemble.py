@@ -1,7 +1,7 @@
 """Ensembles of uneven periodic channels and the y-solve autotuner.
 
-* The three Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
-  Thomas, two-way elimination)
+* The Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
+  Thomas, two-way elimination, warp affine scans over the sequential factors)
   and the three forms of the right-hand-side / x-sweep stage (fused, split,
   fused with bulk-copy staging) solve the FFT99 problem to 1e-12 of the
   oracle, and the step with any combination, with chained or fused plane
@@ -28,7 +28,7 @@ def rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5, 8, 9, 12, 13, 16, 20, 24, 28])
+@pytest.mark.parametrize("kind", [0, 1, 2, 3, 4, 5, 8, 9, 12, 13, 16, 20, 24, 28, 64, 68, 72, 128, 132, 136])
 def test_ysolve_variants_match_oracle(kind):
     L, M, N = 96, 64, 64
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
@@ -230,3 +230,42 @@ def test_ensemble_equals_individual_runs(precision):
     ens.close()
     for c in solo + grp:
         c.close()
+
+
+@pytest.mark.parametrize("bit", [64, 128])
+@pytest.mark.parametrize("shape", [(64, 32, 64), (96, 96, 64), (32, 256, 32), (32, 384, 32), (64, 64, 96)])
+def test_scan_ysolve_matches_oracle(shape, bit):
+    """The scan y-solve (one warp per mode line; the sequential recurrence's
+    forward and backward sweeps as affine maps composed over the lanes, then
+    each lane's rows recomputed in the reference's order from its incoming
+    value) solves the FFT99 problem to 1e-12 of the oracle for line lengths
+    32 to 384 (one to twelve rows per lane), the pinned zero mode included,
+    with the factors read (bit 6) or formed in the kernel by the scan of
+    their continued fraction (bit 7); in the mixed-precision step it gives
+    the sequential variant's fields to the FP32 bound."""
+    L, M, N = shape
+    s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    o = Oracle(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
+    c = gpu.ChannelTG(s)
+    choice, ms = c.autotune(force=bit)
+    assert choice == bit and 0 < ms["ysolve_scan" if bit == 64 else "ysolve_scan_otf"] < 1e29
+    rhs = np.random.default_rng(17).standard_normal((N, M, L))
+    full = np.zeros((N, M + 2, L))
+    full[:, 1:M + 1, :] = rhs
+    ref = o.poisson(full)
+    got = c.FFT99_POIS3D_periodicxz(rhs)
+    assert rel(got[:, 1:M + 1], ref[:, 1:M + 1]) <= 1e-12
+    c.close()
+    Q, PR = initial_field(s, 23, 0.1)
+    out = []
+    for force in (1, bit):
+        c = gpu.ChannelTG(s, precision="mixed")
+        assert c.autotune(force=force)[0] == force
+        c.upload(Q, PR)
+        c.set_dt(2e-3)
+        c.SOLVERRK3_MOM_tg(0)
+        c.advance(5, 2e-3, 1e-6, 0.5)
+        out.append(c.download()[0])
+        c.close()
+    for i in range(3):
+        assert rel(out[1][i][:, 1:M + 1], out[0][i][:, 1:M + 1]) <= 1e-5

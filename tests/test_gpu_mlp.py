@@ -1,15 +1,16 @@
-"""Learned property model on the GPU (tcgen05 BF16 layers, FP32 accumulation)
-against the CPU oracle of the same network, and against the table search it
-replaces.
+"""Learned property model on the GPU (tcgen05 layers with 16-bit operands,
+FP32 accumulation) against the CPU oracle of the same network, and against
+the table search it replaces.
 
 * forward: model outputs for the same parameters agree with the oracle to
   1e-2 of each output's scale.  Inference takes the hardware tanh on FP16
   pairs (tanh.approx.f16x2) where the oracle takes libm's tanhf between the
-  same FP16 roundings of the activation's input and result, and both round
-  h1, h2 to BF16 (2^-9) after it; the hardware approximation of the
-  untrained network's 128 activations per point adds up to about 6e-3 of an
-  output's scale (measured); a layout or indexing fault would show as errors
-  of order 1.  The trained model's accuracy is held to its own bound below;
+  same FP16 roundings of the activation's input and result; both multiply
+  the FP16 activations by the FP16-rounded weights.  The hardware
+  approximation of the untrained network's 128 activations per point adds
+  up to a few 1e-3 of an output's scale (6e-3 measured with BF16 operands);
+  a layout or indexing fault would show as errors of order 1.  The trained
+  model's accuracy is held to its own bound below;
 * gradients of one pass agree with the oracle to 1e-2 of the largest entry
   of each parameter group (FP32 atomics and accumulation order vs FP64);
 * outside the trained range the result is the table search, bitwise;
