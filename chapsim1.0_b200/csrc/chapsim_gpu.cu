@@ -247,7 +247,8 @@ std::vector<double2> twiddles(int n) {
 }
 
 template <typename R> size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(R); }
-template <typename R> size_t smem_z(const Geo& g) { return (size_t)(2 * 32 * (g.N + 33)) * sizeof(R); }
+template <typename R> int zs_tw(const Geo& g) { return sizeof(R) == 8 && g.N / 32 >= 6 ? 16 : 32; }  // zsweep_tw<R, S>
+template <typename R> size_t smem_z(const Geo& g) { return (size_t)(2 * zs_tw<R>(g) * (g.N + 33)) * sizeof(R); }
 template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
 template <typename R> size_t smem_xs(const Geo& g) { return (size_t)((XS_NT / 32) * (g.L + 33)) * sizeof(R); }
 template <typename R> size_t smem_rt() { return (size_t)(RT_SLOTS * RT_SLOT) * sizeof(R); }
@@ -402,7 +403,7 @@ void launch_ysolve_2w(chapsim_ctx* ctx) {
 
 template <typename C>
 size_t smem_ysc(const Geo& g, bool otf) {
-    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)(otf ? 3 : 1) * g.M * sizeof(double);
+    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)(otf ? 3 : 1) * (g.M + 32) * sizeof(double);
 }
 
 template <typename C>
@@ -622,7 +623,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     // persistent: as many blocks as fit at once (two per SM where the two tile buffers allow)
     const int zb_want = sizeof(R) == 4 && g.N / 32 <= 4 ? 3 : 2;  // zsweep_blocks<R, S>
     const int zb = smem_z<R>(g) * zb_want <= 226 * 1024 ? zb_want : (smem_z<R>(g) <= 113 * 1024 ? 2 : 1);
-    const int nz = std::min((g.L / 32) * (3 * g.M - 1), zb * ctx->nsm);
+    const int nz = std::min((g.L / zs_tw<R>(g)) * (3 * g.M - 1), zb * ctx->nsm);
     DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R>, nz, SWEEP_NT, smem_z<R>(g), s, g, f.RHS, fac)));
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N, 2);  // layer 0: u then v, layer 1: w

@@ -198,6 +198,17 @@ __device__ __forceinline__ uint32_t tanh2_f16(float a, float b) {
     asm("tanh.approx.f16x2 %0, %1;" : "=r"(out) : "r"(in));
     return out;
 }
+__device__ __forceinline__ uint32_t tanh2_f16(__half2 pre) {
+    uint32_t out;
+    asm("tanh.approx.f16x2 %0, %1;" : "=r"(out) : "r"(*reinterpret_cast<uint32_t*>(&pre)));
+    return out;
+}
+// The first layer's pre-activations w1 x + b1 in FP16 pair arithmetic (on the
+// FMA pipe; the packing conversion of the FP32 form shares the MUFU unit with
+// the tanh): x = xh + xl split into two FP16 parts (x - xh is exact in FP32),
+// then fma(w1, xh, fma(w1, xl, b1)), each fma rounded once to FP16, with w1 and
+// b1 rounded to FP16.  The input's own rounding would otherwise be 2^-12 of the
+// trained range, a visible shift in the steep part of the property curves.
 
 // 16-byte chunk c (k = 8c .. 8c+7) of row r of an R x 64 K-major operand
 __device__ __forceinline__ void put_chunk(unsigned char* base, int R, int r, int c, uint32_t a, uint32_t b, uint32_t d,
@@ -216,15 +227,20 @@ __global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict
     unsigned char* sA = sW3 + 16 * 64 * 2;    // 16 KB
     __shared__ uint64_t mbar;
     __shared__ uint32_t taddr_s;
-    // first-layer weights and biases interleaved (w1[i], b1[i], w1[i+1], b1[i+1]), second-layer
-    // biases by fours: every thread reads the same values, in 16-byte loads
-    __shared__ float4 swb1[MLP_H / 2], sb2[MLP_H / 4];
+    // first-layer weights and biases as FP16 pairs (w1[i], w1[i+1]) and (b1[i], b1[i+1]), four pairs
+    // of each per 16-byte load; second-layer biases by fours: every thread reads the same values
+    __shared__ uint4 sw1h[MLP_H / 8], sb1h[MLP_H / 8];
+    __shared__ float4 sb2[MLP_H / 4];
     __shared__ float sb3[MLP_OUT];
     const int tid = threadIdx.x, warp = tid >> 5;
     copy_smem16(sW2, ops.w2h, 64 * 64 * 2);
     copy_smem16(sW3, ops.w3h, 16 * 64 * 2);
-    for (int q = tid; q < MLP_H / 2; q += MLP_NT)
-        swb1[q] = make_float4(par[MLP_W1 + 2 * q], par[MLP_B1 + 2 * q], par[MLP_W1 + 2 * q + 1], par[MLP_B1 + 2 * q + 1]);
+    if (tid < MLP_H / 2) {
+        const __half2 w = __floats2half2_rn(par[MLP_W1 + 2 * tid], par[MLP_W1 + 2 * tid + 1]);
+        const __half2 b = __floats2half2_rn(par[MLP_B1 + 2 * tid], par[MLP_B1 + 2 * tid + 1]);
+        reinterpret_cast<__half2*>(sw1h)[tid] = w;
+        reinterpret_cast<__half2*>(sb1h)[tid] = b;
+    }
     for (int q = tid; q < MLP_H / 4; q += MLP_NT)
         sb2[q] = make_float4(par[MLP_B2 + 4 * q], par[MLP_B2 + 4 * q + 1], par[MLP_B2 + 4 * q + 2], par[MLP_B2 + 4 * q + 3]);
     if (tid < MLP_OUT) sb3[tid] = par[MLP_B3 + tid];
@@ -271,14 +287,20 @@ __global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict
             }
         }
         const float x = mlp_x(nm, v);
+        const __half xh = __float2half_rn(x);
+        const __half xl = __float2half_rn(x - __half2float(xh));
+        const __half2 xh2 = __halves2half2(xh, xh), xl2 = __halves2half2(xl, xl);
         // layer 1 (rank one, CUDA cores): h1 = tanh(w1 x + b1), straight into the FP16 operand row
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
+            const uint4 wq = sw1h[c], bq = sb1h[c];
+            const uint32_t wv[4] = {wq.x, wq.y, wq.z, wq.w}, bv[4] = {bq.x, bq.y, bq.z, bq.w};
             uint32_t hv[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const float4 wb = swb1[4 * c + u];
-                hv[u] = tanh2_f16(fmaf(wb.x, x, wb.y), fmaf(wb.z, x, wb.w));
+                const __half2 w = *reinterpret_cast<const __half2*>(&wv[u]);
+                const __half2 b = *reinterpret_cast<const __half2*>(&bv[u]);
+                hv[u] = tanh2_f16(__hfma2(w, xh2, __hfma2(w, xl2, b)));
             }
             put_chunk(sA, MLP_TILE, tid, c, hv[0], hv[1], hv[2], hv[3]);
         }

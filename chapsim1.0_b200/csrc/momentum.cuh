@@ -385,11 +385,15 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
 // registers; longer FP32 lines would spill under the tighter budget, and
 // their buffers leave room for two blocks only).
 template <typename R, int S> __host__ __device__ constexpr int zsweep_blocks() { return sizeof(R) == 4 && S <= 4 ? 3 : 2; }
+// Lines (consecutive i) per tile: 32, or 16 for FP64 lines of 192 points and more, whose 32-line
+// tile buffers (2 x 32 x (N + 33) doubles, 213 KB at N = 384) leave room for one block per SM;
+// 16 doubles are still one 128-byte row segment per z position.
+template <typename R, int S> __host__ __device__ constexpr int zsweep_tw() { return sizeof(R) == 8 && S >= 6 ? 16 : 32; }
 
 // ---------------------------------------------------------------------------
-// cyclic z sweep.  A tile is 32 consecutive i at fixed j, all k, one
-// component; tiles of v at j = 1 are skipped (MOMFA2_Z_tg starts at N2I = 2
-// for v).  Blocks are persistent and take tiles in a stride loop with two
+// cyclic z sweep.  A tile is TW (32 or 16, zsweep_tw) consecutive i at
+// fixed j, all k, one component; tiles of v at j = 1 are skipped (MOMFA2_Z_tg
+// starts at N2I = 2 for v).  Blocks are persistent and take tiles in a stride loop with two
 // shared-memory buffers: the next tile's right-hand sides load (cp.async)
 // while the current tile's 32 lines are solved and stored.
 template <int S, typename R>
@@ -397,19 +401,20 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
     pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* smb = reinterpret_cast<R*>(sm_raw);
+    constexpr int TW = zsweep_tw<R, S>();
     const int N = g.N, M = g.M;
     const int LS = N + 33;
-    const int TS = 32 * LS;
-    const int nx = g.L / 32;
+    const int TS = TW * LS;
+    const int nx = g.L / TW;
     const int nwork = nx * (3 * M - 1);
     const long long ks = g.PI_;
-    constexpr int NIT = 4 * S;  // 32*N / SWEEP_NT
+    constexpr int NIT = TW * S / 8;  // TW*N / SWEEP_NT
     auto tile_base = [&](int t) -> R* {
         int comp, j;
         if (t < nx * M) { comp = 0; j = 1 + t / nx; }
         else if (t < nx * (2 * M - 1)) { comp = 1; j = 2 + (t - nx * M) / nx; }
         else { comp = 2; j = 1 + (t - nx * (2 * M - 1)) / nx; }
-        const int i0 = 32 * (t % nx);
+        const int i0 = TW * (t % nx);
         return RHS + comp * g.FI + iidx(g, i0, j, 0);
     };
     auto load = [&](int t, R* buf) {
@@ -417,7 +422,7 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
 #pragma unroll 4
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            cp_async_el(buf + (p & 31) * LS + seg_pos<S>(p >> 5), Rz + (p & 31) + ks * (p >> 5));
+            cp_async_el(buf + (p % TW) * LS + seg_pos<S>(p / TW), Rz + (p % TW) + ks * (p / TW));
         }
     };
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -436,7 +441,7 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
         // loads shared (longer lines would spill)
         constexpr int NRZ = S <= 4 ? 2 : 1;
 #pragma unroll 1
-        for (int il = warp; il < 32; il += NRZ * (SWEEP_NT / 32)) {
+        for (int il = warp; il < TW; il += NRZ * (SWEEP_NT / 32)) {
             R d[NRZ][S];
 #pragma unroll
             for (int r = 0; r < NRZ; ++r)
@@ -453,7 +458,7 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
 #pragma unroll 4
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            Rz[(p & 31) + ks * (p >> 5)] = cur[(p & 31) * LS + seg_pos<S>(p >> 5)];
+            Rz[(p % TW) + ks * (p / TW)] = cur[(p % TW) * LS + seg_pos<S>(p / TW)];
         }
         __syncthreads();  // cur is the load target two tiles on
         b ^= 1;

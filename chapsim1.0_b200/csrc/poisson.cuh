@@ -363,7 +363,9 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_warp(Geo g, C* __restrict__
 // constant map), and the lane forms its rows' PP_t = 1 / (B_t - H_{t-1} A_t)
 // and H_t = C_t PP_t sequentially, with the expressions of
 // k_ysolve_scan_factors.  Only the spectrum then moves through HBM; the
-// operator's rows (AMPH, ACPH, APPH) are staged in shared memory.
+// operator's rows (AMPH, ACPH, APPH) are staged in shared memory.  The
+// singular kx = kz = 0 line, whose weakly dominant system the composed maps
+// solve only to about 1e-11, takes the factors of k_ysolve_zero_factors.
 __device__ __forceinline__ double pow2_scale_of(double m) {
     // 2^-e for m = 2^e * f, 1 <= f < 2 (m finite and not zero)
     const int be = (__double2hiint(m) >> 20) & 0x7ff;
@@ -413,14 +415,16 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
     const int M = 32 * S, LH = g.LH;
     const int LS = M + 33;
     C* const stage[2] = {reinterpret_cast<C*>(ysc_raw), reinterpret_cast<C*>(ysc_raw) + YW_L * LS};
-    double* const sam = reinterpret_cast<double*>(reinterpret_cast<C*>(ysc_raw) + 2 * YW_L * LS);  // AMPH(t+1)
-    double* const sac = sam + M;  // ACPH(t+1), APPH(t+1) (OTF)
-    double* const sap = sac + M;
+    // AMPH(t+1) (and ACPH(t+1), APPH(t+1) with OTF) at t + t / S: a lane reads rows lS .. lS+S-1,
+    // and the pad after every S rows puts the lanes' rows on different banks
+    double* const sam = reinterpret_cast<double*>(reinterpret_cast<C*>(ysc_raw) + 2 * YW_L * LS);
+    double* const sac = sam + (M + 32);
+    double* const sap = sac + (M + 32);
     for (int t = threadIdx.x; t < M; t += YW_NT) {
-        sam[t] = g.amph[t + 1];
+        sam[t + t / S] = g.amph[t + 1];
         if (OTF) {
-            sac[t] = g.acph[t + 1];
-            sap[t] = g.apph[t + 1];
+            sac[t + t / S] = g.acph[t + 1];
+            sap[t + t / S] = g.apph[t + 1];
         }
     }
     const long long nl = (long long)LH * g.N;
@@ -442,7 +446,7 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
         cp_async_commit();
     };
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int r0 = lane * S;
+    const int r0 = lane * S, s0 = lane * (S + 1);  // the lane's first row and its operator-row slot
     issue(blockIdx.x, stage[0]);
     int cur = 0;
 #pragma unroll 1
@@ -472,16 +476,26 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
         cp_async_wait_group<1>();
         __syncthreads();
         C* const st = stage[cur];
-        if (OTF && q < nl) {
+        if (OTF && q == 0) {
+            // the singular mode's system is only weakly dominant (Neumann operator with its first
+            // row pinned), where the composed maps lose digits: its factors come from the
+            // sequential recurrence of k_ysolve_zero_factors (PP_0 only divides r_0 = 0)
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int t = r0 + k;
+                pp[k] = t == 0 ? 1.0 : g.yz[t];
+                hh[k] = g.yz[M + t];
+            }
+        } else if (OTF && q < nl) {
             const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
             const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-            auto cof = [&](int t) { return t == M - 1 || (t == 0 && q == 0) ? 0.0 : sap[t]; };
+            auto cof = [&](int t, int k) { return t == M - 1 || (t == 0 && q == 0) ? 0.0 : sap[s0 + k]; };
             // the lane's product of its rows' maps (row 0: [[0, C_0], [0, B_0]])
             Mob P{1.0, 0.0, 0.0, 1.0};
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 const int t = r0 + k;
-                const double a = t == 0 ? 0.0 : sam[t], b = sac[t] + shift, c = cof(t);
+                const double a = t == 0 ? 0.0 : sam[s0 + k], b = sac[s0 + k] + shift, c = cof(t, k);
                 P = Mob{c * P.p10, c * P.p11, b * P.p10 - a * P.p00, b * P.p11 - a * P.p01};
             }
             P = mob_mul(P, Mob{1.0, 0.0, 0.0, 1.0});  // rescale
@@ -499,13 +513,13 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
 #pragma unroll
             for (int k = 0; k < S; ++k) {
                 const int t = r0 + k;
-                const double b = sac[t] + shift;
+                const double b = sac[s0 + k] + shift;
                 if (t == 0) {
-                    hp = cof(0) / b;
+                    hp = cof(0, 0) / b;
                     pp[k] = b;
                 } else {
-                    const double p = 1.0 / (b - hp * sam[t]);
-                    hp = t < M - 1 ? sap[t] * p : 0.0;
+                    const double p = 1.0 / (b - hp * sam[s0 + k]);
+                    hp = t < M - 1 ? sap[s0 + k] * p : 0.0;
                     pp[k] = p;
                 }
                 hh[k] = hp;
@@ -527,7 +541,7 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
                     A = 0.0;
                     B = make_double2(d[k].x / pp[k], d[k].y / pp[k]);
                 } else {
-                    const double al = -sam[t] * pp[k];
+                    const double al = -sam[s0 + k] * pp[k];
                     B = make_double2(al * B.x + d[k].x * pp[k], al * B.y + d[k].y * pp[k]);
                     A = al * A;
                 }
@@ -551,7 +565,7 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
                 if (t == 0) {
                     gp = make_double2(d[k].x / pp[k], d[k].y / pp[k]);
                 } else {
-                    const double a = sam[t];
+                    const double a = sam[s0 + k];
                     gp = make_double2((d[k].x - a * gp.x) * pp[k], (d[k].y - a * gp.y) * pp[k]);
                 }
                 d[k] = gp;

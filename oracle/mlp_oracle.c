@@ -69,11 +69,20 @@ static void forward(const float* p, float x, float* h1, float* h2, float* y) {
 
 /* The inference form of forward(): the FP16 rounding of every hidden
  * activation's input and result, with the exact tanh in between (the GPU's
- * hardware tanh adds its own approximation, about 2^-11 relative), and FP16
- * operands of the two tensor-core products (h1 and h2 are FP16 values
- * already; W2 and W3 are rounded to FP16). */
+ * hardware tanh adds its own approximation, about 2^-11 relative), the first
+ * layer's pre-activation in FP16 fused multiply-adds, and FP16 operands of the
+ * two tensor-core products (h1 and h2 are FP16 values already; W2 and W3 are
+ * rounded to FP16). */
 static void forward_inf(const float* p, float x, float* h1, float* h2, float* y) {
-    for (int i = 0; i < H; ++i) h1[i] = f16r(tanhf(f16r(fmaf(p[P_W1 + i], x, p[P_B1 + i]))));
+    /* first layer in FP16 arithmetic: x = xh + xl, pre = fma(w1, xh, fma(w1, xl, b1)), each fma
+     * rounded once to FP16 (the products and sums of FP16 values are exact in FP64) */
+    const float xh = f16r(x), xl = f16r(x - xh);
+    for (int i = 0; i < H; ++i) {
+        const double w = (double)f16r(p[P_W1 + i]), b = (double)f16r(p[P_B1 + i]);
+        const double inner = (double)(_Float16)(w * (double)xl + b);
+        const float pre = (float)(_Float16)(w * (double)xh + inner);
+        h1[i] = f16r(tanhf(pre));
+    }
     for (int j = 0; j < H; ++j) {
         double a = 0.0;
         for (int i = 0; i < H; ++i) a += (double)h1[i] * (double)f16r(p[P_W2 + j * H + i]);
