@@ -779,7 +779,8 @@ def run_b200(args):
         variants["mixed"] = {
             "value": mm["value"], "unit": UNIT, "ms_per_step": mm["ms_per_step"],
             "speedup_vs_fp64": mm["value"] / m["value"], "max_div": mm["max_div"],
-            "autotuned_choice_bits": mm["choice"], "roofline": mm["roofline"], "step_roofline": mm["step_roofline"],
+            "autotuned_choice_bits": mm["choice"], "autotuned_ms": {k: round(v, 4) for k, v in mm["tune_ms"].items()},
+            "roofline": mm["roofline"], "step_roofline": mm["step_roofline"],
             "kernels": mm["kernels"], "gpu_launches": int(mm["launches"]), "clocks": mm["clocks"],
             "precision": "FP32 storage, stencils, CN sweeps, x/z transforms and pressure increment; "
                          "FP64 y-solve, divergence, projection, bulk sums"}

@@ -77,7 +77,7 @@ def step_kernel_slots(choice: int = 0, plane_cluster: bool = False):
         ys = "k_ysolve_2w"
     elif choice & 32:
         ys = "k_ysolve_seq"
-    elif choice & 192:
+    elif choice & 64:
         ys = "k_ysolve_scan"
     else:
         ys = "k_ysolve_warp"
@@ -592,17 +592,17 @@ class ChannelTG:
         sides 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane
         transforms; bit 4: two-way y-solve; bit 5: sequential y-solve with its
         forward intermediate in shared memory at one block per SM; bit 6: warp
-        affine scans over the sequential factors; bit 7: the same with the
-        factors formed in the kernel); returns
+        affine scans over the sequential factors; bit 8: z-sweep tiles of 16
+        lines instead of 32); returns
         (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 11)()
+        ms = (ctypes.c_float * 12)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         self.choice = ch.value
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
                           "pressure_plane": ms[6], "ysolve_two_way": ms[7], "ysolve_sequential_smem": ms[8],
-                          "ysolve_scan": ms[9], "ysolve_scan_otf": ms[10]}
+                          "ysolve_scan": ms[9], "zsweep_tile32": ms[10], "zsweep_tile16": ms[11]}
 
 
 class Ensemble:

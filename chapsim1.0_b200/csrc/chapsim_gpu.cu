@@ -147,10 +147,10 @@ struct chapsim_ctx {
     double* YF3 = nullptr;        // factors of the scan y-solve, 2 M doubles per line, line by line (when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way, 3: sequential with
                                   // the forward intermediate in shared memory at one block per SM, 4: warp affine
-                                  // scans over the sequential factors, 5: the same with the factors formed by a
-                                  // scan in the kernel (chapsim_autotune)
+                                  // scans over the sequential factors (chapsim_autotune)
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
+    int zs_tw = 32;               // lines per tile of the z sweep, 32 or 16 (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
     int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
     bool pdl = true;              // step kernels launched with programmatic dependent launch
@@ -247,8 +247,7 @@ std::vector<double2> twiddles(int n) {
 }
 
 template <typename R> size_t smem_rhs(const Geo& g) { return (size_t)(RHS_WPB * 3 * (g.L + 33)) * sizeof(R); }
-template <typename R> int zs_tw(const Geo& g) { return sizeof(R) == 8 && g.N / 32 >= 6 ? 16 : 32; }  // zsweep_tw<R, S>
-template <typename R> size_t smem_z(const Geo& g) { return (size_t)(2 * zs_tw<R>(g) * (g.N + 33)) * sizeof(R); }
+template <typename R> size_t smem_z(const Geo& g, int tw) { return (size_t)(2 * tw * (g.N + 33)) * sizeof(R); }
 template <typename R> size_t smem_y(const Geo& g) { return (size_t)(32 * (g.M + 33)) * sizeof(R); }
 template <typename R> size_t smem_xs(const Geo& g) { return (size_t)((XS_NT / 32) * (g.L + 33)) * sizeof(R); }
 template <typename R> size_t smem_rt() { return (size_t)(RT_SLOTS * RT_SLOT) * sizeof(R); }
@@ -402,28 +401,22 @@ void launch_ysolve_2w(chapsim_ctx* ctx) {
 }
 
 template <typename C>
-size_t smem_ysc(const Geo& g, bool otf) {
-    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)(otf ? 3 : 1) * (g.M + 32) * sizeof(double);
+size_t smem_ysc(const Geo& g) {
+    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)(g.M + 32) * sizeof(double);
 }
 
 template <typename C>
-void launch_ysolve_scan(chapsim_ctx* ctx, bool otf) {
+void launch_ysolve_scan(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
     const long long nl = (long long)g.LH * g.N;
     const int nb = (int)std::min<long long>((nl + YW_L - 1) / YW_L, ctx->nsm);  // persistent: one block per SM
-    if (otf) {
-        DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_scan<S, C, true>, nb, YW_NT, smem_ysc<C>(g, true), ctx->stream,
-                                         g, spec<C>(ctx), (const double*)nullptr)));
-    } else {
-        DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_scan<S, C, false>, nb, YW_NT, smem_ysc<C>(g, false),
-                                         ctx->stream, g, spec<C>(ctx), (const double*)ctx->YF3)));
-    }
+    DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysolve_scan<S, C>, nb, YW_NT, smem_ysc<C>(g), ctx->stream, g,
+                                     spec<C>(ctx), (const double*)ctx->YF3)));
 }
 
 template <typename C>
 void launch_ysolve(chapsim_ctx* ctx) {
-    if (ctx->ysolve_kind == 5) launch_ysolve_scan<C>(ctx, true);
-    else if (ctx->ysolve_kind == 4 && ctx->YF3) launch_ysolve_scan<C>(ctx, false);
+    if (ctx->ysolve_kind == 4 && ctx->YF3) launch_ysolve_scan<C>(ctx);
     else if (ctx->ysolve_kind == 1 && ctx->YF) launch_ysolve_seq<C>(ctx, false);
     else if (ctx->ysolve_kind == 3 && ctx->YF) launch_ysolve_seq<C>(ctx, true);
     else if (ctx->ysolve_kind == 2 && ctx->YF2) launch_ysolve_2w<C>(ctx);
@@ -454,7 +447,8 @@ int configure_momentum(chapsim_ctx* ctx) {
     ctx->rb_nw = 0;
     DISPATCH_S(g.L / 32, ctx->rb_nw = rb_warps<R>(g.L, bulk_smem_limit(k_rhs_xsweep_bulk<S, R>)));
     if (ctx->rb_nw > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_smem<R>(g.L, ctx->rb_nw))));
-    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R>, smem_z<R>(g))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 32>, smem_z<R>(g, 32))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 16>, smem_z<R>(g, 16))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
     DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
     CK(set_smem(k_rhs_point<R>, smem_rt<R>()));
@@ -462,8 +456,7 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_div_fftx<R, FN1, FN2>, smem_px<C>(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_fftx_inv<FN1, FN2, C>, smem_px<C>(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, C>, smem_yw<C>(g))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, C, false>, smem_ysc<C>(g, false))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, C, true>, smem_ysc<C>(g, true))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, C>, smem_ysc<C>(g))));
     CK(set_smem(k_ysolve_seq<C, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<C, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g) || ysolve_seq_kg1(g))));
     CK(set_smem(k_ysolve_2w<C>, smem_ysolve_seq()));
@@ -480,6 +473,8 @@ int configure_momentum(chapsim_ctx* ctx) {
 
 int configure_kernels(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
+    // z-sweep tiles before any tuning: 16 lines where 32-line FP64 tiles leave one block per SM
+    ctx->zs_tw = ctx->prec != CHAPSIM_PREC_MIXED && g.N / 32 >= 6 ? 16 : 32;
     int rc = ctx->prec == CHAPSIM_PREC_MIXED ? configure_momentum<float>(ctx) : configure_momentum<double>(ctx);
     if (rc) return rc;
     // the FP64 spectral stage serves the standalone Poisson solve and the main domain in every precision
@@ -488,8 +483,7 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, double>, smem_px(g))));
     DISPATCH_FFT(g.L, CK(set_smem(k_io_div_fftx<FN1, FN2, float>, smem_px(g))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_warp<S, double2>, smem_yw<double2>(g))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, double2, false>, smem_ysc<double2>(g, false))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, double2, true>, smem_ysc<double2>(g, true))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysolve_scan<S, double2>, smem_ysc<double2>(g))));
     CK(set_smem(k_ysolve_seq<double2, false>, smem_ysolve_seq(g.M, false)));
     CK(set_smem(k_ysolve_seq<double2, true>, smem_ysolve_seq(g.M, ysolve_seq_kg(g) || ysolve_seq_kg1(g))));
     CK(set_smem(k_ysolve_2w<double2>, smem_ysolve_seq()));
@@ -607,6 +601,23 @@ void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
     ctx->launches += 5;
 }
 
+// cyclic z sweep, persistent: as many blocks as fit at once (two per SM where the two tile
+// buffers allow); tiles of ctx->zs_tw lines
+template <typename R>
+void launch_zsweep(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac) {
+    const Geo& g = ctx->g;
+    const int tw = ctx->zs_tw;
+    const size_t sz = smem_z<R>(g, tw);
+    const int zb_want = sizeof(R) == 4 && g.N / 32 <= 4 ? 3 : 2;  // zsweep_blocks<R, S>
+    const int zb = sz * zb_want <= 226 * 1024 ? zb_want : (sz <= 113 * 1024 ? 2 : 1);
+    const int nz = std::min((g.L / tw) * (3 * g.M - 1), zb * ctx->nsm);
+    if (tw == 16) {
+        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 16>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
+    } else {
+        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 32>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
+    }
+}
+
 template <typename R>
 void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     const Geo& g = ctx->g;
@@ -620,11 +631,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     }
     launch_rhs_x<R>(ctx, f, fac, ns);
     prof_mark(ctx);
-    // persistent: as many blocks as fit at once (two per SM where the two tile buffers allow)
-    const int zb_want = sizeof(R) == 4 && g.N / 32 <= 4 ? 3 : 2;  // zsweep_blocks<R, S>
-    const int zb = smem_z<R>(g) * zb_want <= 226 * 1024 ? zb_want : (smem_z<R>(g) <= 113 * 1024 ? 2 : 1);
-    const int nz = std::min((g.L / zs_tw<R>(g)) * (3 * g.M - 1), zb * ctx->nsm);
-    DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R>, nz, SWEEP_NT, smem_z<R>(g), s, g, f.RHS, fac)));
+    launch_zsweep<R>(ctx, f, fac);
     prof_mark(ctx);
     dim3 gry(g.L / 32, g.N, 2);  // layer 0: u then v, layer 1: w
     DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R>, gry, SWEEP_NT, smem_y<R>(g), s, g, f.Q, f.RHS, ctx->st, fac, ns)));
@@ -2091,8 +2098,7 @@ extern "C" int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err) {
 
 // ----------------------------- autotuner -----------------------------------
 // Times the Poisson y-solve variants (warp Thomas/PCR hybrid, sequential
-// Thomas, two-way, sequential at one block per SM, warp scans over read or
-// in-kernel factors) on this
+// Thomas, two-way, sequential at one block per SM, warp scans) on this
 // context's grid and keeps the fastest.  The spectral array is scratch
 // between substeps, so it is zeroed and solved in place.
 extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms) {
@@ -2126,15 +2132,13 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             if (kind == 0) launch_ysolve_warp<float2>(ctx);
             else if (kind == 1) launch_ysolve_seq<float2>(ctx, false);
             else if (kind == 3) launch_ysolve_seq<float2>(ctx, true);
-            else if (kind == 4) launch_ysolve_scan<float2>(ctx, false);
-            else if (kind == 5) launch_ysolve_scan<float2>(ctx, true);
+            else if (kind == 4) launch_ysolve_scan<float2>(ctx);
             else launch_ysolve_2w<float2>(ctx);
         } else {
             if (kind == 0) launch_ysolve_warp<double2>(ctx);
             else if (kind == 1) launch_ysolve_seq<double2>(ctx, false);
             else if (kind == 3) launch_ysolve_seq<double2>(ctx, true);
-            else if (kind == 4) launch_ysolve_scan<double2>(ctx, false);
-            else if (kind == 5) launch_ysolve_scan<double2>(ctx, true);
+            else if (kind == 4) launch_ysolve_scan<double2>(ctx);
             else launch_ysolve_2w<double2>(ctx);
         }
     };
@@ -2142,9 +2146,9 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     const bool kg1 = ysolve_seq_kg1(g);
-    float t[6] = {0.f, 0.f, 0.f, 1e30f, 0.f, 0.f};
+    float t[5] = {0.f, 0.f, 0.f, 1e30f, 0.f};
     const int reps = 5;
-    for (int kind = 0; kind < 6; ++kind) {
+    for (int kind = 0; kind < 5; ++kind) {
         if (kind == 3 && !kg1) continue;
         for (int w = 0; w < 2; ++w) run_y(kind);
         CK(cudaEventRecord(e0, s));
@@ -2154,15 +2158,14 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaEventElapsedTime(&t[kind], e0, e1));
         t[kind] /= reps;
     }
-    ctx->launches += (kg1 ? 6 : 5) * (2 + reps);
+    ctx->launches += (kg1 ? 5 : 4) * (2 + reps);
     CK(cudaGetLastError());
     if (force >= 0) {
         ctx->ysolve_kind =
-            (force & 1) ? 1
-                        : ((force & 16) ? 2 : ((force & 32) ? (kg1 ? 3 : 1) : ((force & 64) ? 4 : ((force & 128) ? 5 : 0))));
+            (force & 1) ? 1 : ((force & 16) ? 2 : ((force & 32) ? (kg1 ? 3 : 1) : ((force & 64) ? 4 : 0)));
     } else {
         int best = 0;
-        for (int kind = 1; kind < 6; ++kind)
+        for (int kind = 1; kind < 5; ++kind)
             if (t[kind] < t[best]) best = kind;
         ctx->ysolve_kind = best;
     }
@@ -2225,6 +2228,34 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             if (tk[kind] < tk[best]) best = kind;
         ctx->k1_kind = force >= 0 ? std::min((force >> 1) & 3, bulk_fits ? 2 : 1) : best;
     }
+    // tile shape of the z sweep: 32 or 16 lines per tile (it rewrites RHS in place, which every
+    // substep's right-hand-side kernel rewrites before reading)
+    float tz[2] = {0.f, 0.f};
+    if (ctx->domain == 1) {
+        const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
+        for (int v = 0; v < 2; ++v) {
+            ctx->zs_tw = v == 0 ? 32 : 16;
+            auto one = [&]() {
+                if (mixed) {
+                    StepFields<float> f = step_fields<float>(ctx);
+                    launch_zsweep<float>(ctx, f, f.fac + 5 * FAC_SET);
+                } else {
+                    StepFields<double> f = step_fields<double>(ctx);
+                    launch_zsweep<double>(ctx, f, f.fac + 5 * FAC_SET);
+                }
+            };
+            one();
+            CK(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; ++r) one();
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&tz[v], e0, e1));
+            tz[v] /= reps;
+        }
+        ctx->launches += 2 * (1 + reps);
+        CK(cudaGetLastError());
+        ctx->zs_tw = force >= 0 ? ((force & 256) ? 16 : 32) : (tz[1] < tz[0] ? 16 : 32);
+    }
     // pressure stage up to DPH: chained x/z transforms or the fused plane
     // transforms (periodic channel, planes that fit one block).  It writes
     // only scratch (RHSLLPHI, the spectrum, DPH), which every substep rewrites.
@@ -2265,10 +2296,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     if (choice)
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
                   (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0) | (ctx->ysolve_kind == 4 ? 64 : 0) |
-                  (ctx->ysolve_kind == 5 ? 128 : 0);
+                  (ctx->zs_tw == 16 ? 256 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
-        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4]; ms[10] = t[5];
+        ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4];
+        ms[10] = tz[0]; ms[11] = tz[1];
     }
     return CHAPSIM_OK;
 }

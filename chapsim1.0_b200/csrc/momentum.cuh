@@ -385,23 +385,22 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
 // registers; longer FP32 lines would spill under the tighter budget, and
 // their buffers leave room for two blocks only).
 template <typename R, int S> __host__ __device__ constexpr int zsweep_blocks() { return sizeof(R) == 4 && S <= 4 ? 3 : 2; }
-// Lines (consecutive i) per tile: 32, or 16 for FP64 lines of 192 points and more, whose 32-line
-// tile buffers (2 x 32 x (N + 33) doubles, 213 KB at N = 384) leave room for one block per SM;
-// 16 doubles are still one 128-byte row segment per z position.
-template <typename R, int S> __host__ __device__ constexpr int zsweep_tw() { return sizeof(R) == 8 && S >= 6 ? 16 : 32; }
+// Lines (consecutive i) per tile, TW: 32 or 16 (autotuned, chapsim_autotune bit 8).  16 halves the
+// two tile buffers (2 x 32 x (N + 33) doubles are 213 KB at N = 384: one block per SM) and each z
+// position of a tile still reads whole 32-byte sectors (64 or 128 bytes per row segment).
 
 // ---------------------------------------------------------------------------
-// cyclic z sweep.  A tile is TW (32 or 16, zsweep_tw) consecutive i at
-// fixed j, all k, one component; tiles of v at j = 1 are skipped (MOMFA2_Z_tg
+// cyclic z sweep.  A tile is TW (32 or 16) consecutive i at fixed j, all
+// k, one component; tiles of v at j = 1 are skipped (MOMFA2_Z_tg
 // starts at N2I = 2 for v).  Blocks are persistent and take tiles in a stride loop with two
 // shared-memory buffers: the next tile's right-hand sides load (cp.async)
 // while the current tile's 32 lines are solved and stored.
-template <int S, typename R>
+template <int S, typename R, int TW>
 __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
     pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* smb = reinterpret_cast<R*>(sm_raw);
-    constexpr int TW = zsweep_tw<R, S>();
+    static_assert(TW == 16 || TW == 32, "tile width");
     const int N = g.N, M = g.M;
     const int LS = N + 33;
     const int TS = TW * LS;

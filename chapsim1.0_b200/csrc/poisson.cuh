@@ -351,40 +351,6 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_warp(Geo g, C* __restrict__
 // double-buffered groups of YW_L lines, one warp per line).  The lane maps are
 // combined in tree order, so the result agrees with the sequential recurrence
 // to rounding (1e-12 of the oracle on the Poisson problem).
-//
-// With OTF the factors are not read but formed in the kernel, by a scan too:
-// the multipliers follow the continued fraction H_t = C_t / (B_t - A_t H_{t-1})
-// (H_0 = C_0 / B_0, C_0 = 0 on the zero mode, C_{M-1} = 0), a Moebius map of
-// H_{t-1} with the matrix [[0, C_t], [-A_t, B_t]] acting on (H, 1).  Each lane
-// multiplies its rows' matrices, the lane products are combined by a shuffle
-// scan (rescaled by powers of two after every product: a map is unchanged by
-// scaling its matrix), the incoming H of a lane is the ratio of its prefix's
-// right column (row 0's matrix has a zero left column, so every prefix is a
-// constant map), and the lane forms its rows' PP_t = 1 / (B_t - H_{t-1} A_t)
-// and H_t = C_t PP_t sequentially, with the expressions of
-// k_ysolve_scan_factors.  Only the spectrum then moves through HBM; the
-// operator's rows (AMPH, ACPH, APPH) are staged in shared memory.  The
-// singular kx = kz = 0 line, whose weakly dominant system the composed maps
-// solve only to about 1e-11, takes the factors of k_ysolve_zero_factors.
-__device__ __forceinline__ double pow2_scale_of(double m) {
-    // 2^-e for m = 2^e * f, 1 <= f < 2 (m finite and not zero)
-    const int be = (__double2hiint(m) >> 20) & 0x7ff;
-    return __hiloint2double((2046 - be) << 20, 0);
-}
-struct Mob {
-    double p00, p01, p10, p11;
-};
-// x * y (the map y first, then x), rescaled by a power of two
-__device__ __forceinline__ Mob mob_mul(const Mob& x, const Mob& y) {
-    Mob r{x.p00 * y.p00 + x.p01 * y.p10, x.p00 * y.p01 + x.p01 * y.p11, x.p10 * y.p00 + x.p11 * y.p10,
-          x.p10 * y.p01 + x.p11 * y.p11};
-    const double m = fmax(fmax(fabs(r.p00), fabs(r.p01)), fmax(fabs(r.p10), fabs(r.p11)));
-    if (m > 0.0) {
-        const double sc = pow2_scale_of(m);
-        r.p00 *= sc; r.p01 *= sc; r.p10 *= sc; r.p11 *= sc;
-    }
-    return r;
-}
 
 __global__ void k_ysolve_scan_factors(Geo g, double* __restrict__ F) {
     const int M = g.M, LH = g.LH;
@@ -407,7 +373,7 @@ __global__ void k_ysolve_scan_factors(Geo g, double* __restrict__ F) {
     }
 }
 
-template <int S, typename C, bool OTF>
+template <int S, typename C>
 __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__ SP, const double* __restrict__ F) {
     pdl_wait();
     extern __shared__ __align__(16) unsigned char ysc_raw[];
@@ -415,18 +381,11 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
     const int M = 32 * S, LH = g.LH;
     const int LS = M + 33;
     C* const stage[2] = {reinterpret_cast<C*>(ysc_raw), reinterpret_cast<C*>(ysc_raw) + YW_L * LS};
-    // AMPH(t+1) (and ACPH(t+1), APPH(t+1) with OTF) at t + t / S: a lane reads rows lS .. lS+S-1,
-    // and the pad after every S rows puts the lanes' rows on different banks
+    // AMPH(t+1) at t + t / S: a lane reads rows lS .. lS+S-1, and the pad after every S rows
+    // puts the lanes' rows on different banks (lane-strided reads of the unpadded rows made
+    // 36 M bank conflicts per launch at 384 x 256 x 384)
     double* const sam = reinterpret_cast<double*>(reinterpret_cast<C*>(ysc_raw) + 2 * YW_L * LS);
-    double* const sac = sam + (M + 32);
-    double* const sap = sac + (M + 32);
-    for (int t = threadIdx.x; t < M; t += YW_NT) {
-        sam[t + t / S] = g.amph[t + 1];
-        if (OTF) {
-            sac[t + t / S] = g.acph[t + 1];
-            sap[t + t / S] = g.apph[t + 1];
-        }
-    }
+    for (int t = threadIdx.x; t < M; t += YW_NT) sam[t + t / S] = g.amph[t + 1];
     const long long nl = (long long)LH * g.N;
     const long long ngr = (nl + YW_L - 1) / YW_L;
     const int ls = threadIdx.x % YW_L, js = threadIdx.x / YW_L;
@@ -455,7 +414,7 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
         // this warp's line factors (coalesced: the warp reads 2 x 32 S contiguous doubles)
         const long long q = gr * YW_L + warp;
         double pp[S], hh[S];
-        if (!OTF && q < nl) {
+        if (q < nl) {
             const double* f = F + q * 2LL * M + r0;
             if constexpr (S % 2 == 0) {
 #pragma unroll
@@ -476,55 +435,6 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
         cp_async_wait_group<1>();
         __syncthreads();
         C* const st = stage[cur];
-        if (OTF && q == 0) {
-            // the singular mode's system is only weakly dominant (Neumann operator with its first
-            // row pinned), where the composed maps lose digits: its factors come from the
-            // sequential recurrence of k_ysolve_zero_factors (PP_0 only divides r_0 = 0)
-#pragma unroll
-            for (int k = 0; k < S; ++k) {
-                const int t = r0 + k;
-                pp[k] = t == 0 ? 1.0 : g.yz[t];
-                hh[k] = g.yz[M + t];
-            }
-        } else if (OTF && q < nl) {
-            const int kz = (int)(q / LH), kx = (int)(q - (long long)kz * LH);
-            const double shift = (-g.ak1[kx] / 1.0 - g.ak3[kz]);
-            auto cof = [&](int t, int k) { return t == M - 1 || (t == 0 && q == 0) ? 0.0 : sap[s0 + k]; };
-            // the lane's product of its rows' maps (row 0: [[0, C_0], [0, B_0]])
-            Mob P{1.0, 0.0, 0.0, 1.0};
-#pragma unroll
-            for (int k = 0; k < S; ++k) {
-                const int t = r0 + k;
-                const double a = t == 0 ? 0.0 : sam[s0 + k], b = sac[s0 + k] + shift, c = cof(t, k);
-                P = Mob{c * P.p10, c * P.p11, b * P.p10 - a * P.p00, b * P.p11 - a * P.p01};
-            }
-            P = mob_mul(P, Mob{1.0, 0.0, 0.0, 1.0});  // rescale
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                Mob Q;
-                Q.p00 = __shfl_up_sync(0xffffffffu, P.p00, o);
-                Q.p01 = __shfl_up_sync(0xffffffffu, P.p01, o);
-                Q.p10 = __shfl_up_sync(0xffffffffu, P.p10, o);
-                Q.p11 = __shfl_up_sync(0xffffffffu, P.p11, o);
-                if (lane >= o) P = mob_mul(P, Q);
-            }
-            const double num = __shfl_up_sync(0xffffffffu, P.p01, 1), den = __shfl_up_sync(0xffffffffu, P.p11, 1);
-            double hp = lane == 0 ? 0.0 : num / den;  // H of the row before the lane's first
-#pragma unroll
-            for (int k = 0; k < S; ++k) {
-                const int t = r0 + k;
-                const double b = sac[s0 + k] + shift;
-                if (t == 0) {
-                    hp = cof(0, 0) / b;
-                    pp[k] = b;
-                } else {
-                    const double p = 1.0 / (b - hp * sam[s0 + k]);
-                    hp = t < M - 1 ? sap[s0 + k] * p : 0.0;
-                    pp[k] = p;
-                }
-                hh[k] = hp;
-            }
-        }
         if (q < nl) {
             C* base = st + warp * LS + lane * (S + 1);
             double2 d[S];

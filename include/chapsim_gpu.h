@@ -374,17 +374,15 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the fastest of each group (force = -1), or the ones forced (force = 0..255):
- *   bits 0, 4, 5, 6 and 7: Poisson y-solve, all 0 = warp Thomas/PCR hybrid,
+ * the fastest of each group (force = -1), or the ones forced (force = 0..511):
+ *   bits 0, 4, 5 and 6: Poisson y-solve, all 0 = warp Thomas/PCR hybrid,
  *          bit 0 = the reference's sequential Thomas recurrence, one thread
  *          per mode, bit 4 = two-way elimination, two threads per mode,
  *          bit 5 = the sequential recurrence with its forward intermediate in
  *          shared memory at one block per SM (lines longer than two blocks
  *          per SM allow; elsewhere it means bit 0), bit 6 = one warp per mode
  *          line evaluating the sequential recurrence's two sweeps as affine
- *          scans over its precomputed factors, bit 7 = the same with the
- *          factors formed in the kernel by a scan of the continued fraction
- *          (no factor array); the lowest set bit wins;
+ *          scans over its precomputed factors; the lowest set bit wins;
  *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
  *          0 = fused (one warp per x line, per-thread loads), 1 = split into
  *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
@@ -394,13 +392,16 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *          the row's half spectrum fits one block's shared memory, one
  *          thread-block cluster per row (the x-z transpose in distributed
  *          shared memory) for 256- and 384-point planes; otherwise 0 is kept
- *          whatever is forced.
- * choice receives the kept setting in the same bit form; ms[11] (may be NULL)
+ *          whatever is forced;
+ *   bit 8: tile shape of the z sweep (periodic channel only), 0 = 32
+ *          consecutive x lines per tile, 1 = 16.
+ * choice receives the kept setting in the same bit form; ms[12] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
  * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
  * 1e30 where a variant does not apply), the two-way y-solve, the
  * sequential y-solve at one block per SM (1e30 where it does not apply) and
- * the scan y-solve over read and over in-kernel factors.
+ * the scan y-solve, and the z sweep with 32- and with 16-line tiles (0 where
+ * it does not apply).
  * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 

@@ -41,10 +41,9 @@ TOL_STEP = 1e-11
 THREADS = os.cpu_count() or 8
 DTMIN = 1e-6
 
-# every selectable combination: y-solve (warp 0, sequential 1, two-way 16, scans over read
-# factors 64, scans with in-kernel factors 128), right-hand side (fused 0, split 2,
-# bulk-staged 4), pressure (chained 0, plane 8)
-COMBOS = [y | r | p for y in (0, 1, 16, 64, 128) for r in (0, 2, 4) for p in (0, 8)]
+# every selectable combination: y-solve (warp 0, sequential 1, two-way 16, scans 64),
+# right-hand side (fused 0, split 2, bulk-staged 4), pressure (chained 0, plane 8)
+COMBOS = [y | r | p for y in (0, 1, 16, 64) for r in (0, 2, 4) for p in (0, 8)]
 
 
 def rel(a, b):
@@ -163,8 +162,9 @@ def c3_ref():
     return _oracle_run(_workload(C3), 2)
 
 
-# at M = 256 the sequential y-solve can also keep its forward intermediate in shared memory at one block per SM
-COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4) for p in (0, 8)]
+# at M = 256 the sequential y-solve can also keep its forward intermediate in shared memory at one block per SM;
+# the z sweep in 16-line tiles (bit 8) with the tuner's usual y-solves
+COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4) for p in (0, 8)] + [256 | y for y in (1, 64)]
 
 
 @pytest.mark.parametrize("force", COMBOS_C3 + [-1])
