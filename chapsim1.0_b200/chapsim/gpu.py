@@ -593,16 +593,18 @@ class ChannelTG:
         transforms; bit 4: two-way y-solve; bit 5: sequential y-solve with its
         forward intermediate in shared memory at one block per SM; bit 6: warp
         affine scans over the sequential factors; bit 8: z-sweep tiles of 16
-        lines instead of 32); returns
+        lines instead of 32; bit 9: double-buffered persistent z transforms);
+        returns
         (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 12)()
+        ms = (ctypes.c_float * 13)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         self.choice = ch.value
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
                           "pressure_plane": ms[6], "ysolve_two_way": ms[7], "ysolve_sequential_smem": ms[8],
-                          "ysolve_scan": ms[9], "zsweep_tile32": ms[10], "zsweep_tile16": ms[11]}
+                          "ysolve_scan": ms[9], "zsweep_tile32": ms[10], "zsweep_tile16": ms[11],
+                          "pressure_chained_zpipe": ms[12]}
 
 
 class Ensemble:

@@ -151,6 +151,7 @@ struct chapsim_ctx {
     int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     int zs_tw = 32;               // lines per tile of the z sweep, 32 or 16 (chapsim_autotune)
+    bool fz_pipe = false;         // persistent double-buffered z transforms (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
     int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
     bool pdl = true;              // step kernels launched with programmatic dependent launch
@@ -263,6 +264,8 @@ template <typename C = double2>
 size_t smem_px(const Geo& g) { return (size_t)((PX_TJ / 2) * fft4s_ld(g.L)) * sizeof(C); }
 template <typename C = double2>
 size_t smem_fz(const Geo& g) { return (size_t)(FZ_TQ * fft4s_ld(g.N)) * sizeof(C); }
+template <typename C>
+size_t smem_fzp(const Geo& g) { return (size_t)(2 * fzp_tq<C>() * fft4s_ld(g.N)) * sizeof(C); }
 // the context's pressure increment DPH in the step's real type
 template <typename R> R* dph(chapsim_ctx* c);
 template <> double* dph<double>(chapsim_ctx* c) { return c->DPH; }
@@ -468,6 +471,8 @@ int configure_momentum(chapsim_ctx* ctx) {
         P2C_DISPATCH(g.L, g.N, (ctx->p2c = plane_fft_cluster_setup<R, XN1, XN2, ZN1, ZN2>(g)));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<-1, FN1, FN2, C>, smem_fz<C>(g))));
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, C>, smem_fz<C>(g))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz_pipe<-1, FN1, FN2, C>, smem_fzp<C>(g))));
+    DISPATCH_FFT(g.N, CK(set_smem(k_fftz_pipe<+1, FN1, FN2, C>, smem_fzp<C>(g))));
     return CHAPSIM_OK;
 }
 
@@ -559,6 +564,22 @@ void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns
 // DIVG_tg + FFT99_POIS3D_periodicxz up to DPH: chained transforms, or the
 // fused plane transforms (one block per y row) where chosen.  Both record the
 // same profiling slots (the fused form leaves the two z-transform slots empty).
+// z transforms of the periodic channel's spectrum: one tile per block (k_fftz), or the
+// persistent double-buffered form (ctx->fz_pipe, chapsim_autotune bit 9)
+template <int SIGN, typename C>
+void launch_fftz(chapsim_ctx* ctx, C* sp) {
+    const Geo& g = ctx->g;
+    const long long nq = (long long)g.LH * g.M;
+    if (ctx->fz_pipe) {
+        const long long nt = (nq + fzp_tq<C>() - 1) / fzp_tq<C>();
+        const int nb = (int)std::min<long long>(nt, (long long)fzp_minb<C>() * ctx->nsm);
+        DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz_pipe<SIGN, FN1, FN2, C>, nb, FZ_NT, smem_fzp<C>(g), ctx->stream, g, sp)));
+    } else {
+        const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
+        DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<SIGN, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), ctx->stream, g, sp)));
+    }
+}
+
 template <typename R>
 void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
     const Geo& g = ctx->g;
@@ -588,13 +609,11 @@ void launch_pressure(chapsim_ctx* ctx, const StepFields<R>& f, int ns) {
     dim3 grp((g.M + PX_TJ - 1) / PX_TJ, g.N);
     DISPATCH_FFT(g.L, (launch_pdl(ctx->pdl, k_div_fftx<R, FN1, FN2>, grp, PX_NT, smem_px<C>(g), s, g, f.Q, f.RHSLL, sp, ctx->st, ns)));
     prof_mark(ctx);
-    const long long nq = (long long)g.LH * g.M;
-    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<-1, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), s, g, sp)));
+    launch_fftz<-1, C>(ctx, sp);
     prof_mark(ctx);
     launch_ysolve<C>(ctx);
     prof_mark(ctx);
-    DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<+1, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), s, g, sp)));
+    launch_fftz<+1, C>(ctx, sp);
     prof_mark(ctx);
     DISPATCH_FFT(g.L, (launch_pdl(ctx->pdl, k_fftx_inv<FN1, FN2, C>, grp, PX_NT, smem_px<C>(g), s, g, sp, dph<R>(ctx))));
     prof_mark(ctx);
@@ -2259,12 +2278,16 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     // pressure stage up to DPH: chained x/z transforms or the fused plane
     // transforms (periodic channel, planes that fit one block).  It writes
     // only scratch (RHSLLPHI, the spectrum, DPH), which every substep rewrites.
-    float tp[2] = {0.f, 1e30f};
+    // (kind 0: chained transforms, 1: fused plane transforms, 2: chained with the persistent
+    // double-buffered z transforms)
+    float tp[3] = {0.f, 1e30f, 0.f};
     if (ctx->domain == 1) {
         const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
         bool p2 = (mixed ? plane_fft_ok<float2>(g) : plane_fft_ok<double2>(g)) || ctx->p2c;
-        for (int kind = 0; kind < (p2 ? 2 : 1); ++kind) {
-            ctx->plane_kind = kind;
+        for (int kind = 0; kind < 3; ++kind) {
+            if (kind == 1 && !p2) continue;
+            ctx->plane_kind = kind == 1 ? 1 : 0;
+            ctx->fz_pipe = kind == 2;
             auto one = [&]() {
                 if (mixed) launch_pressure<float>(ctx, step_fields<float>(ctx), 1);
                 else launch_pressure<double>(ctx, step_fields<double>(ctx), 1);
@@ -2275,7 +2298,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
                 ctx->p2c = false;
                 p2 = false;
                 tp[1] = 1e30f;
-                break;
+                continue;
             }
             CK(cudaEventRecord(e0, s));
             for (int r = 0; r < reps; ++r) one();
@@ -2285,7 +2308,16 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             tp[kind] /= reps;
         }
         CK(cudaGetLastError());
-        ctx->plane_kind = force >= 0 ? (p2 ? (force >> 3) & 1 : 0) : (p2 && tp[1] < tp[0] ? 1 : 0);
+        if (force >= 0) {
+            ctx->plane_kind = p2 ? (force >> 3) & 1 : 0;
+            ctx->fz_pipe = (force & 512) != 0;
+        } else {
+            int best = 0;
+            for (int kind = 1; kind < 3; ++kind)
+                if (tp[kind] < tp[best]) best = kind;
+            ctx->plane_kind = best == 1 ? 1 : 0;
+            ctx->fz_pipe = best == 2;
+        }
     }
     if (ctx->step_exec) {
         cudaGraphExecDestroy(ctx->step_exec);
@@ -2296,11 +2328,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     if (choice)
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
                   (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0) | (ctx->ysolve_kind == 4 ? 64 : 0) |
-                  (ctx->zs_tw == 16 ? 256 : 0);
+                  (ctx->zs_tw == 16 ? 256 : 0) | (ctx->fz_pipe ? 512 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
         ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4];
-        ms[10] = tz[0]; ms[11] = tz[1];
+        ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2];
     }
     return CHAPSIM_OK;
 }

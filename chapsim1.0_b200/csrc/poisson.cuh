@@ -170,6 +170,69 @@ __global__ void __launch_bounds__(FZ_NT, sizeof(C) == 8 ? 4 : 2) k_fftz(Geo g, C
     }
 }
 
+// Persistent, double-buffered form of k_fftz (autotuned alternative): a block
+// owns every gridDim.x-th tile of TQ = 16 lines and issues the copies of its
+// next tile (cp.async into the other buffer) before it transforms and stores
+// the current one, so the loads overlap the transform and the stores, where
+// the one-tile blocks of k_fftz overlap them only across blocks.  The
+// arithmetic is k_fftz's: the fields are bitwise equal.
+template <typename C> __host__ __device__ constexpr int fzp_tq() { return 16; }
+// Blocks per SM: one in FP64 (two 105 KB buffers at N = 384; inside the persistent tile loop
+// the FP64 transform of 384-point lines spilled 700 bytes under a two-block register budget,
+// where the one-tile kernel spills none), two in FP32.
+template <typename C> __host__ __device__ constexpr int fzp_minb() { return sizeof(C) == 16 ? 1 : 2; }
+
+template <int SIGN, int N1, int N2, typename C>
+__global__ void __launch_bounds__(FZ_NT, fzp_minb<C>()) k_fftz_pipe(Geo g, C* __restrict__ SP) {
+    pdl_wait();
+    constexpr int TQ = fzp_tq<C>();
+    using T = typename CReal<C>::T;
+    extern __shared__ __align__(16) unsigned char smp_raw[];
+    const int N = g.N;
+    const int LD = fft4s_ld(N);
+    C* const buf0 = reinterpret_cast<C*>(smp_raw);
+    const long long Q = (long long)g.LH * g.M;
+    const long long ntile = (Q + TQ - 1) / TQ;
+    auto issue = [&](long long tile, C* b) {
+        if (tile < ntile) {
+            const long long q0 = tile * TQ;
+            const int nq = (int)min((long long)TQ, Q - q0);
+#pragma unroll 1
+            for (int p = threadIdx.x; p < TQ * N; p += FZ_NT) {
+                const int kz = p / TQ, ql = p - kz * TQ;
+                if (ql < nq) {
+                    if constexpr (sizeof(C) == 16) cp_async16(b + ql * LD + kz, SP + q0 + ql + Q * kz);
+                    else cp_async8(reinterpret_cast<double*>(b + ql * LD + kz), reinterpret_cast<const double*>(SP + q0 + ql + Q * kz));
+                }
+            }
+        }
+        cp_async_commit();  // an empty group past the end keeps the group count uniform
+    };
+    const T sc = SIGN < 0 ? (T)(1.0 / (double)N) : (T)1.0;
+    issue(blockIdx.x, buf0);
+    int cur = 0;
+#pragma unroll 1
+    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x, cur ^= 1) {
+        C* const bc = buf0 + cur * (TQ * LD);
+        issue(tile + gridDim.x, buf0 + (cur ^ 1) * (TQ * LD));
+        cp_async_wait_group<1>();  // this tile's copies (all but the newest group) have landed
+        const long long q0 = tile * TQ;
+        const int nq = (int)min((long long)TQ, Q - q0);
+        block_fft4s<N1, N2, SIGN>(bc, nq, LD, twz_of<C>(g));  // starts and ends with a block barrier
+#pragma unroll 1
+        for (int p = threadIdx.x; p < TQ * N; p += FZ_NT) {
+            const int kz = p / TQ, ql = p - kz * TQ;
+            if (ql < nq) {
+                C v = bc[ql * LD + kz];
+                if (SIGN < 0) { v.x = v.x * sc; v.y = v.y * sc; }
+                SP[q0 + ql + Q * kz] = v;
+            }
+        }
+        __syncthreads();  // the buffer is the copy target of the iteration after next
+    }
+    cp_async_wait_group<0>();
+}
+
 // ---------------------------------------------------------------------------
 // y solve of YW_L consecutive lines q = kx + LH*kz per block, one warp per
 // line, by the warp Thomas/PCR hybrid with a complex right-hand side

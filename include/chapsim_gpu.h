@@ -374,7 +374,7 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the fastest of each group (force = -1), or the ones forced (force = 0..511):
+ * the fastest of each group (force = -1), or the ones forced (force = 0..1023):
  *   bits 0, 4, 5 and 6: Poisson y-solve, all 0 = warp Thomas/PCR hybrid,
  *          bit 0 = the reference's sequential Thomas recurrence, one thread
  *          per mode, bit 4 = two-way elimination, two threads per mode,
@@ -394,14 +394,18 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *          shared memory) for 256- and 384-point planes; otherwise 0 is kept
  *          whatever is forced;
  *   bit 8: tile shape of the z sweep (periodic channel only), 0 = 32
- *          consecutive x lines per tile, 1 = 16.
- * choice receives the kept setting in the same bit form; ms[12] (may be NULL)
+ *          consecutive x lines per tile, 1 = 16;
+ *   bit 9: with the chained transforms, the z transforms as persistent
+ *          blocks that load their next tile while transforming the current
+ *          one (periodic channel only; timed as a third pressure-stage form).
+ * choice receives the kept setting in the same bit form; ms[13] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
  * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
  * 1e30 where a variant does not apply), the two-way y-solve, the
  * sequential y-solve at one block per SM (1e30 where it does not apply) and
- * the scan y-solve, and the z sweep with 32- and with 16-line tiles (0 where
- * it does not apply).
+ * the scan y-solve, the z sweep with 32- and with 16-line tiles (0 where it
+ * does not apply), and the pressure stage with the double-buffered z
+ * transforms.
  * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 
