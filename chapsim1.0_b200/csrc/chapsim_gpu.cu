@@ -144,7 +144,7 @@ struct chapsim_ctx {
     double* yz = nullptr;         // zero-mode factors of the warp y-solve (Geo::yz)
     double* YF = nullptr;         // factors of the sequential y-solve, 2 M doubles per line (when chosen)
     double* YF2 = nullptr;        // factors of the two-way y-solve, 2 M doubles per line (when chosen)
-    double* YF3 = nullptr;        // factors of the scan y-solve, 2 M doubles per line, line by line (when chosen)
+    double* YF3 = nullptr;        // pivots of the scan y-solve, M doubles per line, line by line (when chosen)
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way, 3: sequential with
                                   // the forward intermediate in shared memory at one block per SM, 4: warp affine
                                   // scans over the sequential factors (chapsim_autotune)
@@ -405,7 +405,7 @@ void launch_ysolve_2w(chapsim_ctx* ctx) {
 
 template <typename C>
 size_t smem_ysc(const Geo& g) {
-    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)(g.M + 32) * sizeof(double);
+    return (size_t)(2 * YW_L * (g.M + 33)) * sizeof(C) + (size_t)2 * (g.M + 32) * sizeof(double);
 }
 
 template <typename C>
@@ -2138,7 +2138,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaGetLastError());
     }
     if (!ctx->YF3) {
-        CK(cudaMalloc(&ctx->YF3, 2 * nsp * sizeof(double)));
+        CK(cudaMalloc(&ctx->YF3, nsp * sizeof(double)));
         k_ysolve_scan_factors<<<4 * ctx->nsm, 128, 0, s>>>(g, ctx->YF3);
         CK(cudaGetLastError());
     }

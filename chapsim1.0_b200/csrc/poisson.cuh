@@ -398,9 +398,11 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_warp(Geo g, C* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Fifth y-solve variant: the sequential recurrence's factors (k_ysolve_scan_
-// factors: the same pivots PP and multipliers H as k_ysolve_seq_factors, laid
-// out line by line, F[q*2M + t] = PP_t, F[q*2M + M + t] = H_t) turn both sweeps
+// Fifth y-solve variant: the sequential recurrence's factors (the same pivots
+// PP and multipliers H as k_ysolve_seq_factors; k_ysolve_scan_factors stores
+// the pivots line by line, F[q*M + t] = PP_t, and the kernel forms each
+// H_t = APPH(t+1) PP_t, H_0 = C_0 / PP_0, H_{M-1} = 0, with the factor
+// kernel's own operations, so only half the factor bytes are read) turn both sweeps
 // into first-order linear recurrences,
 //   forward   g_t = (r_t - A_t g_{t-1}) PP_t      (g_0 = r_0 / PP_0, r_0 = 0 on the zero mode)
 //   backward  x_t = g_t - H_t x_{t+1}             (H_{M-1} = 0),
@@ -424,14 +426,12 @@ __global__ void k_ysolve_scan_factors(Geo g, double* __restrict__ F) {
         const double b = g.acph[1] + shift;
         const double c = q == 0 ? 0.0 : g.apph[1];
         double hp = c / b;
-        double* f = F + q * 2LL * M;
+        double* f = F + q * M;
         f[0] = b;
-        f[M] = hp;
         for (int j = 2; j <= M; ++j) {
             const double pp = 1.0 / ((g.acph[j] + shift) - hp * g.amph[j]);
             hp = j < M ? g.apph[j] * pp : 0.0;
             f[j - 1] = pp;
-            f[M + j - 1] = hp;
         }
     }
 }
@@ -448,7 +448,11 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
     // puts the lanes' rows on different banks (lane-strided reads of the unpadded rows made
     // 36 M bank conflicts per launch at 384 x 256 x 384)
     double* const sam = reinterpret_cast<double*>(reinterpret_cast<C*>(ysc_raw) + 2 * YW_L * LS);
-    for (int t = threadIdx.x; t < M; t += YW_NT) sam[t + t / S] = g.amph[t + 1];
+    double* const sap = sam + (M + 32);  // APPH(t+1), the same layout
+    for (int t = threadIdx.x; t < M; t += YW_NT) {
+        sam[t + t / S] = g.amph[t + 1];
+        sap[t + t / S] = g.apph[t + 1];
+    }
     const long long nl = (long long)LH * g.N;
     const long long ngr = (nl + YW_L - 1) / YW_L;
     const int ls = threadIdx.x % YW_L, js = threadIdx.x / YW_L;
@@ -474,29 +478,32 @@ __global__ void __launch_bounds__(YW_NT, 1) k_ysolve_scan(Geo g, C* __restrict__
 #pragma unroll 1
     for (long long gr = blockIdx.x; gr < ngr; gr += gridDim.x, cur ^= 1) {
         issue(gr + gridDim.x, stage[cur ^ 1]);
-        // this warp's line factors (coalesced: the warp reads 2 x 32 S contiguous doubles)
+        // this warp's line pivots (coalesced: the warp reads 32 S contiguous doubles)
         const long long q = gr * YW_L + warp;
         double pp[S], hh[S];
         if (q < nl) {
-            const double* f = F + q * 2LL * M + r0;
+            const double* f = F + q * M + r0;
             if constexpr (S % 2 == 0) {
 #pragma unroll
                 for (int k = 0; k < S; k += 2) {
                     const double2 a = __ldg(reinterpret_cast<const double2*>(f + k));
-                    const double2 b = __ldg(reinterpret_cast<const double2*>(f + M + k));
                     pp[k] = a.x; pp[k + 1] = a.y;
-                    hh[k] = b.x; hh[k + 1] = b.y;
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < S; ++k) {
-                    pp[k] = __ldg(f + k);
-                    hh[k] = __ldg(f + M + k);
-                }
+                for (int k = 0; k < S; ++k) pp[k] = __ldg(f + k);
             }
         }
         cp_async_wait_group<1>();
-        __syncthreads();
+        __syncthreads();  // (also the first iteration's barrier for sam and sap)
+        if (q < nl) {
+#pragma unroll
+            for (int k = 0; k < S; ++k) {
+                const int t = r0 + k;
+                if (t == 0) hh[k] = (q == 0 ? 0.0 : sap[0]) / pp[0];
+                else hh[k] = t < M - 1 ? sap[s0 + k] * pp[k] : 0.0;
+            }
+        }
         C* const st = stage[cur];
         if (q < nl) {
             C* base = st + warp * LS + lane * (S + 1);
