@@ -70,7 +70,7 @@ def step_kernel_slots(choice: int = 0, plane_cluster: bool = False):
     side times k_rhs_point and k_xsweep in one slot; with the fused plane
     transforms (one block per row, or a cluster per row when plane_cluster)
     the two z-transform slots stay empty and are named None."""
-    rhs = {0: "k_rhs_xsweep", 1: "k_rhs_point+k_xsweep", 2: "k_rhs_xsweep_bulk"}[(choice >> 1) & 3]
+    rhs = {0: "k_rhs_xsweep", 1: "k_rhs_point+k_xsweep", 2: "k_rhs_xsweep_bulk", 3: "k_rhs_xsweep"}[(choice >> 1) & 3]
     if choice & 1:
         ys = "k_ysolve_seq"
     elif choice & 16:
@@ -589,7 +589,8 @@ class ChannelTG:
     def autotune(self, force=-1):
         """Keeps the fastest y-solve, right-hand-side and pressure-stage variants for
         this grid, or forces them (bit 0: sequential y-solve; bits 1-2: right-hand
-        sides 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane
+        sides 0 fused, 1 split, 2 fused with bulk-copy staging, 3 fused with two
+        points per lane in FP64; bit 3: fused plane
         transforms; bit 4: two-way y-solve; bit 5: sequential y-solve with its
         forward intermediate in shared memory at one block per SM; bit 6: warp
         affine scans over the sequential factors; bit 8: z-sweep tiles of 16
@@ -597,14 +598,14 @@ class ChannelTG:
         returns
         (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 13)()
+        ms = (ctypes.c_float * 14)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         self.choice = ch.value
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
                           "pressure_plane": ms[6], "ysolve_two_way": ms[7], "ysolve_sequential_smem": ms[8],
                           "ysolve_scan": ms[9], "zsweep_tile32": ms[10], "zsweep_tile16": ms[11],
-                          "pressure_chained_zpipe": ms[12]}
+                          "pressure_chained_zpipe": ms[12], "rhs_fused_paired": ms[13]}
 
 
 class Ensemble:

@@ -148,7 +148,8 @@ struct chapsim_ctx {
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way, 3: sequential with
                                   // the forward intermediate in shared memory at one block per SM, 4: warp affine
                                   // scans over the sequential factors (chapsim_autotune)
-    int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk (chapsim_autotune)
+    int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk, 3: fused with
+                                  // two points per lane in FP64 (FP32 always pairs) (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     int zs_tw = 32;               // lines per tile of the z sweep, 32 or 16 (chapsim_autotune)
     bool fz_pipe = false;         // persistent double-buffered z transforms (chapsim_autotune)
@@ -446,7 +447,8 @@ template <> StepFields<float> step_fields<float>(chapsim_ctx* c) { return {c->Qf
 template <typename R>
 int configure_momentum(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
-    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R>, smem_rhs<R>(g))));
+    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R, sizeof(R) == 4>, smem_rhs<R>(g))));
+    if (sizeof(R) == 8) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R, true>, smem_rhs<R>(g))));
     ctx->rb_nw = 0;
     DISPATCH_S(g.L / 32, ctx->rb_nw = rb_warps<R>(g.L, bulk_smem_limit(k_rhs_xsweep_bulk<S, R>)));
     if (ctx->rb_nw > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_smem<R>(g.L, ctx->rb_nw))));
@@ -554,10 +556,14 @@ void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns
         const int nbx = (int)((nl + XS_NT / 32 - 1) / (XS_NT / 32));
         DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_xsweep<S, R>, nbx, XS_NT, smem_xs<R>(g), s, g, f.RHS, fac)));
         ctx->launches += 1;
+    } else if (ctx->k1_kind == 3 && sizeof(R) == 8) {
+        const int grx = g.M * g.N / RHS_WPB;
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R, true>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g, f.Q, f.PR,
+                                         f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
     } else {
         const int grx = g.M * g.N / RHS_WPB;
-        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g, f.Q, f.PR, f.H0, f.RHS,
-                                                                                             ctx->part_rhs, ctx->st, fac, ns)));
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R, sizeof(R) == 4>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g, f.Q,
+                                         f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
     }
 }
 
@@ -2204,7 +2210,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     // explicit right-hand sides + x sweep: fused, split, or fused with bulk-copy
     // staging (periodic channel).  CONVH0 is state: kept in a temporary copy
     // and restored afterwards.
-    float tk[3] = {0.f, 0.f, 0.f};
+    float tk[4] = {0.f, 0.f, 0.f, 1e30f};
     if (ctx->domain == 1) {
         const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
         const size_t hb = (size_t)3 * g.FI * (mixed ? sizeof(float) : sizeof(double));
@@ -2214,9 +2220,10 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaMemcpyAsync(hsave, h0, hb, cudaMemcpyDeviceToDevice, s));
         const int keep = ctx->k1_kind;
         const bool bulk_fits = ctx->rb_nw > 0;
-        for (int kind = 0; kind < 3; ++kind) {
-            if (kind == 2 && !bulk_fits) {
-                tk[2] = 1e30f;
+        const bool pair_ok = !mixed && (g.L / 32) % 2 == 0;  // kind 3: the FP64 paired form
+        for (int kind = 0; kind < 4; ++kind) {
+            if ((kind == 2 && !bulk_fits) || (kind == 3 && !pair_ok)) {
+                tk[kind] = 1e30f;
                 continue;
             }
             ctx->k1_kind = kind;
@@ -2243,9 +2250,12 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         cudaFree(hsave);
         CK(cudaGetLastError());
         int best = 0;
-        for (int kind = 1; kind < 3; ++kind)
+        for (int kind = 1; kind < 4; ++kind)
             if (tk[kind] < tk[best]) best = kind;
-        ctx->k1_kind = force >= 0 ? std::min((force >> 1) & 3, bulk_fits ? 2 : 1) : best;
+        int fk = (force >> 1) & 3;
+        if (fk == 2 && !bulk_fits) fk = 1;
+        if (fk == 3 && !pair_ok) fk = 0;
+        ctx->k1_kind = force >= 0 ? fk : best;
     }
     // tile shape of the z sweep: 32 or 16 lines per tile (it rewrites RHS in place, which every
     // substep's right-hand-side kernel rewrites before reading)
@@ -2332,7 +2342,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
         ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4];
-        ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2];
+        ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2]; ms[13] = tk[3];
     }
     return CHAPSIM_OK;
 }

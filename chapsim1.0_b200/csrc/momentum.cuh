@@ -41,6 +41,12 @@
 // at 384 x 256 x 384 than at 4 (128 registers with spills); FP32 is fastest
 // at 4.
 #define RHS_MINB(R) (sizeof(R) == 8 ? 3 : 4)
+// The paired form (two adjacent points per lane, 2-element vector loads) in FP64 holds twice the
+// loaded values: a two-block budget (up to 255 registers).
+#define RHS_MINB_P(R, PAIR) ((PAIR) && sizeof(R) == 8 ? 2 : RHS_MINB(R))
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
 #define SWEEP_NT 256
 #define FAC_SET (TF_NF(12) * 32)   // doubles per factor table
 
@@ -214,8 +220,8 @@ __device__ __forceinline__ RhsLine<R> rhs_line(const Geo& g, double dt, int ns, 
 }
 
 // ---------------------------------------------------------------------------
-template <int S, typename R>
-__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
+template <int S, typename R, bool PAIR>
+__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB_P(R, PAIR)) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
                                                              R* __restrict__ H0, R* __restrict__ RHS,
                                                              double* __restrict__ partial, DevState* __restrict__ st,
                                                              const R* __restrict__ fac, int ns) {
@@ -257,31 +263,35 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
         prefetch_l2(H0 + irow + i + 2 * g.FI);
     }
     double bulk = 0.0;
-    if constexpr (sizeof(R) == 4 && S % 2 == 0) {
-        // FP32: each lane takes two adjacent points (i, i+1) per iteration with 8-byte loads, so
-        // a warp request moves 256 bytes as in FP64 (twice the bytes in flight per load of the
-        // one-point form); the x neighbours outside the pair are single loads.  Rows start at
-        // multiples of L (even), so every pair is 8-byte aligned.
+    if constexpr (PAIR && S % 2 == 0) {
+        // Paired form (always in FP32; an autotuned alternative in FP64): each lane takes two
+        // adjacent points (i, i+1) per iteration with 2-element vector loads, so a warp request
+        // moves twice the bytes of the one-point form (in FP32 as many as one FP64 request); the
+        // x neighbours outside the pair are single loads.  Rows start at multiples of L (even),
+        // so every pair is aligned to its vector size.
+        using R2 = typename Vec2<R>::T;
 #pragma unroll 1
         for (int kk = 0; kk < S / 2; ++kk) {
             const int i = 2 * lane + 64 * kk;
             const int il = i == 0 ? L - 1 : i - 1, ir = i + 2 == L ? 0 : i + 2;
-            auto ld2 = [&](const R* b, long long row) { return *reinterpret_cast<const float2*>(b + row + i); };
-            const float2 u2 = ld2(U, rowc), v2 = ld2(V, rowc), w2 = ld2(W, rowc);
-            const float2 ujp = ld2(U, rowjp), ujm = ld2(U, rowjm), ukp = ld2(U, rowkp), ukm = ld2(U, rowkm);
-            const float2 vjp = ld2(V, rowjp), vjm = ld2(V, rowjm), vkp = ld2(V, rowkp), vkm = ld2(V, rowkm);
-            const float2 wjp = ld2(W, rowjp), wjm = ld2(W, rowjm), wkp = ld2(W, rowkp), wkm = ld2(W, rowkm);
-            const float2 pc = ld2(PR, rowc), pjm = ld2(PR, rowjm), pkm = ld2(PR, rowkm);
-            const float2 wjmkp = ld2(W, rowjmkp), vjpkm = ld2(V, rowjpkm);
+            auto ld2 = [&](const R* b, long long row) { return *reinterpret_cast<const R2*>(b + row + i); };
+            const R2 u2 = ld2(U, rowc), v2 = ld2(V, rowc), w2 = ld2(W, rowc);
+            const R2 ujp = ld2(U, rowjp), ujm = ld2(U, rowjm), ukp = ld2(U, rowkp), ukm = ld2(U, rowkm);
+            const R2 vjp = ld2(V, rowjp), vjm = ld2(V, rowjm), vkp = ld2(V, rowkp), vkm = ld2(V, rowkm);
+            const R2 wjp = ld2(W, rowjp), wjm = ld2(W, rowjm), wkp = ld2(W, rowkp), wkm = ld2(W, rowkm);
+            const R2 pc = ld2(PR, rowc), pjm = ld2(PR, rowjm), pkm = ld2(PR, rowkm);
+            const R2 wjmkp = ld2(W, rowjmkp), vjpkm = ld2(V, rowjpkm);
             const R ul = U[rowc + il], ur = U[rowc + ir], vl = V[rowc + il], vr = V[rowc + ir];
             const R wl = W[rowc + il], wr = W[rowc + ir], pl = PR[rowc + il];
             const R vjpl = V[rowjp + il], wkpl = W[rowkp + il], ujmr = U[rowjm + ir], ukmr = U[rowkm + ir];
             // every load of the iteration is issued before any store: H0 is read
             // and written through one pointer, which the compiler cannot reorder
             const long long ii = irow + i;
-            const float2 h0u = *reinterpret_cast<const float2*>(H0 + ii);
-            const float2 h0v = vrow ? *reinterpret_cast<const float2*>(H0 + ii + g.FI) : make_float2(0.f, 0.f);
-            const float2 h0w = *reinterpret_cast<const float2*>(H0 + ii + 2 * g.FI);
+            const R2 h0u = *reinterpret_cast<const R2*>(H0 + ii);
+            R2 h0v;
+            if (vrow) h0v = *reinterpret_cast<const R2*>(H0 + ii + g.FI);
+            else h0v.x = h0v.y = R(0);
+            const R2 h0w = *reinterpret_cast<const R2*>(H0 + ii + 2 * g.FI);
             const RhsStencil<R> s0{u2.x, u2.y, ul, ujp.x, ujm.x, ukp.x, ukm.x,
                                    v2.x, v2.y, vl, vjp.x, vjm.x, vkp.x, vkm.x,
                                    w2.x, w2.y, wl, wjp.x, wjm.x, wkp.x, wkm.x,
@@ -294,12 +304,12 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB(R)) k_rhs_xsweep(Geo g,
                                    pc.y, pc.x, pjm.y, pkm.y,
                                    vjp.x, wkp.x, ujmr, wjmkp.y, ukmr, vjpkm.y,
                                    h0u.y, h0v.y, h0w.y};
-            float2 Hu, Hv, Hw, ru, rv, rw;
+            R2 Hu, Hv, Hw, ru, rv, rw;
             rhs_point(cl, s0, vrow, Hu.x, Hv.x, Hw.x, ru.x, rv.x, rw.x, bulk);
             rhs_point(cl, s1, vrow, Hu.y, Hv.y, Hw.y, ru.y, rv.y, rw.y, bulk);
-            *reinterpret_cast<float2*>(H0 + ii) = Hu;
-            if (vrow) *reinterpret_cast<float2*>(H0 + ii + g.FI) = Hv;
-            *reinterpret_cast<float2*>(H0 + ii + 2 * g.FI) = Hw;
+            *reinterpret_cast<R2*>(H0 + ii) = Hu;
+            if (vrow) *reinterpret_cast<R2*>(H0 + ii + g.FI) = Hv;
+            *reinterpret_cast<R2*>(H0 + ii + 2 * g.FI) = Hw;
             const int pos = seg_pos<S>(i);  // i + 1 is the next position of the same segment (S even)
             sl[pos] = ru.x; sl[pos + 1] = ru.y;
             if (vrow) { sl[LS + pos] = rv.x; sl[LS + pos + 1] = rv.y; }

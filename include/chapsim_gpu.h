@@ -384,9 +384,11 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *          line evaluating the sequential recurrence's two sweeps as affine
  *          scans over its precomputed factors; the lowest set bit wins;
  *   bits 1-2: explicit right-hand sides + x sweep (periodic channel only),
- *          0 = fused (one warp per x line, per-thread loads), 1 = split into
- *          a point-wise kernel and a line-sweep kernel, 2 = fused with the
- *          stencil rows staged in shared memory by bulk copies;
+ *          0 = fused (one warp per x line, per-thread loads; two adjacent
+ *          points per lane in FP32), 1 = split into a point-wise kernel and
+ *          a line-sweep kernel, 2 = fused with the stencil rows staged in
+ *          shared memory by bulk copies, 3 = fused with two adjacent points
+ *          per lane in FP64 (even L / 32; elsewhere it means 0);
  *   bit 3: pressure stage (periodic channel only), 0 = chained x and z
  *          transforms, 1 = fused plane transforms: one block per y row where
  *          the row's half spectrum fits one block's shared memory, one
@@ -398,14 +400,15 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *   bit 9: with the chained transforms, the z transforms as persistent
  *          blocks that load their next tile while transforming the current
  *          one (periodic channel only; timed as a third pressure-stage form).
- * choice receives the kept setting in the same bit form; ms[13] (may be NULL)
+ * choice receives the kept setting in the same bit form; ms[14] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
  * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
  * 1e30 where a variant does not apply), the two-way y-solve, the
  * sequential y-solve at one block per SM (1e30 where it does not apply) and
  * the scan y-solve, the z sweep with 32- and with 16-line tiles (0 where it
- * does not apply), and the pressure stage with the double-buffered z
- * transforms.
+ * does not apply), the pressure stage with the double-buffered z
+ * transforms, and the FP64 paired right-hand side (1e30 where it does not
+ * apply).
  * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 

@@ -42,8 +42,9 @@ THREADS = os.cpu_count() or 8
 DTMIN = 1e-6
 
 # every selectable combination: y-solve (warp 0, sequential 1, two-way 16, scans 64),
-# right-hand side (fused 0, split 2, bulk-staged 4), pressure (chained 0, plane 8)
-COMBOS = [y | r | p for y in (0, 1, 16, 64) for r in (0, 2, 4) for p in (0, 8)]
+# right-hand side (fused 0, split 2, bulk-staged 4, fused with two points per lane in FP64 6),
+# pressure (chained 0, plane 8)
+COMBOS = [y | r | p for y in (0, 1, 16, 64) for r in (0, 2, 4, 6) for p in (0, 8)]
 
 
 def rel(a, b):
@@ -164,7 +165,7 @@ def c3_ref():
 
 # at M = 256 the sequential y-solve can also keep its forward intermediate in shared memory at one block per SM;
 # the z sweep in 16-line tiles (bit 8) and the double-buffered z transforms (bit 9) with the tuner's usual y-solves
-COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4) for p in (0, 8)] + [256 | y for y in (1, 64)] + [512 | y for y in (1, 64)]
+COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4, 6) for p in (0, 8)] + [256 | y for y in (1, 64)] + [512 | y for y in (1, 64)]
 
 
 @pytest.mark.parametrize("force", COMBOS_C3 + [-1])
