@@ -39,6 +39,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_set_buoyancy", "chapsim_upload_weighted_pressure",
             "chapsim_batch_get_stream", "chapsim_batch_destroy", "chapsim_pp_mean_zx_tg", "chapsim_pp_mean_t_tg",
             "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
+            "chapsim_pp_mean_zx_io", "chapsim_download_pp_means_io",
             "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
@@ -184,6 +185,8 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_pp_monitor_tg.argtypes = [vp, ctypes.c_double, _dp]
     L.chapsim_download_pp_means_tg.argtypes = [vp, ctypes.c_int32] + [_dp] * 7 + [ctypes.POINTER(ctypes.c_int32)]
     L.chapsim_upload_pp_means_tg.argtypes = [vp, ctypes.c_int32] + [_dp] * 7
+    L.chapsim_pp_mean_zx_io.argtypes = [vp]
+    L.chapsim_download_pp_means_io.argtypes = [vp, _dp, ctypes.POINTER(ctypes.c_int32)]
     L.chapsim_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(vp)]
     L.chapsim_batch_advance.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double]
     L.chapsim_batch_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -690,6 +693,17 @@ class ChannelIO(ChannelTG):
     def set_buoyancy(self, iGravity, F_A):
         """thermal_gravity / RHS_MOM_EXPLICIT_io buoyancy: D_STG * TALP*DT*F_A on component |iGravity|."""
         self._check(self.lib.chapsim_set_buoyancy(self.h, int(iGravity), float(F_A)))
+
+    def PP_MEAN_ZX_FLOW_Xperiodic_io(self):
+        """Instantaneous x-z means of the main domain on the device; returns the set as a flat
+        array of per_row * M doubles (141 per row, 360 with the thermal solver) in the module
+        arrays' order (Fortran order, j fastest)."""
+        self._check(self.lib.chapsim_pp_mean_zx_io(self.h))
+        n = ctypes.c_int32()
+        self._check(self.lib.chapsim_download_pp_means_io(self.h, None, ctypes.byref(n)))
+        out = np.zeros(n.value * self.M)
+        self._check(self.lib.chapsim_download_pp_means_io(self.h, _ptr(out), ctypes.byref(n)))
+        return out
 
     def set_weighted_pressure(self, PR0_1=None, PR0_2=None):
         """iWeightedPre = 1 with the two PR0_io layers ((N, M+2, L), the second defaults to the first);

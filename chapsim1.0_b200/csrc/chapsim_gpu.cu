@@ -18,6 +18,7 @@
 #include "io.cuh"
 #include "io_cn.cuh"
 #include "stats.cuh"
+#include "stats_io.cuh"
 #include "rhs_bulk.cuh"
 #include "plane_fft.cuh"
 #include "plane_fft_cluster.cuh"
@@ -178,6 +179,7 @@ struct chapsim_ctx {
     // statistics of the periodic channel (stats.cuh), allocated by the first call
     double *pp_inst = nullptr, *pp_avg = nullptr, *pp_part = nullptr, *pp_mon = nullptr;
     int pp_nchunk = 0;
+    double *ppio_set = nullptr, *ppio_part = nullptr;  // main-domain means (PPIO_ALL per row) and chunk partials
     int nstatis = 0;              // NSTATIS_TG
     IoFields io{};                // IO-path arrays (domain 2); FP64 staging of G in the mixed-precision step
     IoFieldsT<float> iof{};       // FP32 flow fields of the mixed-precision main-domain step (Q, PR, RHS: Qf, PRf, RHSf)
@@ -1081,6 +1083,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->DPH); cudaFree(ctx->SP); cudaFree(ctx->YF); cudaFree(ctx->YF2); cudaFree(ctx->YF3); cudaFree(ctx->part_rhs); cudaFree(ctx->part_red); cudaFree(ctx->fac);
     cudaFree(ctx->st); cudaFree(ctx->ybuf); cudaFree(ctx->tw); cudaFree(ctx->twf); cudaFree(ctx->yz); cudaFree(ctx->SPf); cudaFree(ctx->DPHf);
     cudaFree(ctx->pp_inst); cudaFree(ctx->pp_avg); cudaFree(ctx->pp_part); cudaFree(ctx->pp_mon);
+    cudaFree(ctx->ppio_set); cudaFree(ctx->ppio_part);
     cudaFree(ctx->io.G); cudaFree(ctx->io.EX0); cudaFree(ctx->io.RHO); cudaFree(ctx->io.MU0); cudaFree(ctx->io.MU);
     cudaFree(ctx->io.DST); cudaFree(ctx->io.MST); cudaFree(ctx->io.DIVU);
     cudaFree(ctx->iof.G); cudaFree(ctx->iof.EX0); cudaFree(ctx->iof.DST); cudaFree(ctx->iof.MST); cudaFree(ctx->iof.DIVU);
@@ -1260,6 +1263,34 @@ int pp_ensure(chapsim_ctx* ctx) {
 // the seven arrays of one set, in storage order, with their widths
 const int pp_width[7] = {4, 3, 6, 10, 9, 9, 81};
 const int pp_off[7] = {PP_U1, PP_UP, PP_U2, PP_U3, PP_D1, PP_DP, PP_D2};
+extern "C++" {  // a template, inside the C-linkage block of the ABI
+// the seven sum groups of the main-domain means (stats_io.cuh), for the field type F
+template <typename F>
+void pp_io_launch(chapsim_ctx* ctx, IoFieldsT<F> f, int ngroups) {
+    const Geo& g = ctx->g;
+    dim3 grid(ctx->pp_nchunk, g.M);
+    cudaStream_t s = ctx->stream;
+    const int nc = ctx->pp_nchunk;
+    k_pp_io<0, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+    k_pp_io_finish<0><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+    k_pp_io<1, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+    k_pp_io_finish<1><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+    if (ngroups > 2) {
+        k_pp_io<2, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+        k_pp_io_finish<2><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+        k_pp_io<3, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+        k_pp_io_finish<3><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+        k_pp_io<4, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+        k_pp_io_finish<4><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+        k_pp_io<5, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+        k_pp_io_finish<5><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+        k_pp_io<6, F><<<grid, PP_NT, 0, s>>>(g, f, ctx->tf, ctx->ppio_part);
+        k_pp_io_finish<6><<<g.M, PP_NT, 0, s>>>(g, ctx->ppio_part, nc, ctx->ppio_set);
+    }
+    ctx->launches += 2 * ngroups;
+}
+
+}  // extern "C++"
 }  // namespace
 
 int chapsim_pp_mean_zx_tg(chapsim_ctx_t* ctx) {
@@ -1276,6 +1307,41 @@ int chapsim_pp_mean_zx_tg(chapsim_ctx_t* ctx) {
     k_pp_finish<<<g.M, PP_NT, 0, ctx->stream>>>(g, ctx->pp_part, ctx->pp_nchunk, ctx->pp_inst);
     ctx->launches += 2;
     CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+
+int chapsim_pp_mean_zx_io(chapsim_ctx_t* ctx) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "the main-domain statistics need a main-domain context");
+    CK(cudaSetDevice(ctx->device));
+    const Geo& g = ctx->g;
+    if (!ctx->ppio_set) {
+        int nchunk = (4 * ctx->nsm + g.M - 1) / g.M;
+        nchunk = std::max(1, std::min(nchunk, g.L * g.N / PP_NT));
+        ctx->pp_nchunk = ctx->pp_nchunk ? ctx->pp_nchunk : nchunk;
+        CK(cudaMalloc(&ctx->ppio_set, (size_t)PPIO_ALL * g.M * sizeof(double)));
+        CK(cudaMalloc(&ctx->ppio_part, (size_t)g.M * ctx->pp_nchunk * 60 * sizeof(double)));
+        CK(cudaMemsetAsync(ctx->ppio_set, 0, (size_t)PPIO_ALL * g.M * sizeof(double), ctx->stream));
+    }
+    const int ngroups = ctx->thermal ? 7 : 2;
+    if (ctx->prec == CHAPSIM_PREC_MIXED) pp_io_launch<float>(ctx, io_fields_t<float>(ctx), ngroups);
+    else pp_io_launch<double>(ctx, io_fields_t<double>(ctx), ngroups);
+    CK(cudaGetLastError());
+    return CHAPSIM_OK;
+}
+
+int chapsim_download_pp_means_io(chapsim_ctx_t* ctx, double* out, int32_t* per_row) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "the main-domain statistics need a main-domain context");
+    if (!ctx->ppio_set) return fail(ctx, CHAPSIM_ERR_BADARG, "no main-domain means yet (call chapsim_pp_mean_zx_io)");
+    CK(cudaSetDevice(ctx->device));
+    const int nr = ctx->thermal ? PPIO_ALL : PPIO_FLOW;
+    if (per_row) *per_row = nr;
+    if (out) {
+        CK(cudaMemcpyAsync(out, ctx->ppio_set, (size_t)nr * ctx->g.M * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
     return CHAPSIM_OK;
 }
 

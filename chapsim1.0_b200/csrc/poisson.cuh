@@ -934,25 +934,35 @@ __global__ void __launch_bounds__(PX_NT, px_minb<C>()) k_fftx_inv(Geo g, const C
     const int nj = min(PX_TJ, M - j0 + 1);
     const int np = (nj + 1) >> 1;
     // Z_k = A_k + i B_k with A_{L-k} = conj A_k; imaginary parts of the k = 0 and
-    // k = L/2 coefficients are dropped, as FFT99 does for ISIGN = +1.
-#pragma unroll 4
-    for (int p = threadIdx.x; p < np * L; p += PX_NT) {
-        const int pair = p / L, kk = p - pair * L;
+    // k = L/2 coefficients are dropped, as FFT99 does for ISIGN = +1.  Each
+    // stored coefficient is read once and gives Z at k and at L - k.
+#pragma unroll 2
+    for (int p = threadIdx.x; p < np * LH; p += PX_NT) {
+        const int pair = p / LH, ks = p - pair * LH;
         const int ja = j0 + 2 * pair;
         const bool hasb = 2 * pair + 1 < nj;
-        const int ks = kk <= L / 2 ? kk : L - kk;
         C a = SP[ks + (long long)LH * ((ja - 1) + (long long)M * k)];
         C b = hasb ? SP[ks + (long long)LH * ((ja) + (long long)M * k)] : mkc((T)0, (T)0);
-        if (ks == 0 || 2 * ks == L) { a.y = (T)0; b.y = (T)0; }
-        if (kk > L / 2) { a.y = -a.y; b.y = -b.y; }
-        smc[pair * LD + kk] = mkc(a.x - b.y, a.y + b.x);
+        C* line = smc + pair * LD;
+        if (ks == 0 || 2 * ks == L) {
+            a.y = (T)0;
+            b.y = (T)0;
+        } else {
+            line[L - ks] = mkc(a.x - (-b.y), (-a.y) + b.x);
+        }
+        line[ks] = mkc(a.x - b.y, a.y + b.x);
     }
     block_fft4s<N1, N2, +1>(smc, np, LD, twx_of<C>(g));
-    for (int p = threadIdx.x; p < 2 * np * L; p += PX_NT) {
-        const int jl = p / L, i = p - jl * L;
-        if (jl >= nj) continue;
-        const C z = smc[(jl >> 1) * LD + i];
-        DPH[pidx(g, i, j0 + jl, k)] = (jl & 1) ? z.y : z.x;
+    // DPH rows with 16-byte stores (W consecutive points per thread; L is a multiple of 4)
+    constexpr int W = V16<T>::W;
+    const int LV = L / W;
+    for (int p = threadIdx.x; p < nj * LV; p += PX_NT) {
+        const int jl = p / LV, i0 = (p - jl * LV) * W;
+        const C* z = smc + (jl >> 1) * LD + i0;
+        T v[W];
+#pragma unroll
+        for (int e = 0; e < W; ++e) v[e] = (jl & 1) ? z[e].y : z[e].x;
+        st16(DPH + pidx(g, i0, j0 + jl, k), v);
     }
 }
 

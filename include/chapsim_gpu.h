@@ -343,6 +343,25 @@ int chapsim_pp_monitor_tg(chapsim_ctx_t* ctx, double ren, double* mon);
  * pointer may be NULL; nstatis receives NSTATIS_TG. */
 int chapsim_download_pp_means_tg(chapsim_ctx_t* ctx, int32_t averaged, double* u1, double* up, double* u2,
                                  double* u3, double* dvdl1, double* dvdlp, double* dvdl2, int32_t* nstatis);
+/* ---- Statistics of the main domain (POSTPROCESS_io's PP_MEAN_ZX_FLOW_Xperiodic_io,
+ * src/processing/PP_MEAN_ZX.f90:311-796; plane channel) ----
+ * chapsim_pp_mean_zx_io computes the instantaneous x-z means of a main-domain
+ * context on the device from its resident fields (G, Q, PR and, with the
+ * thermal solver, TEMPERATURE, DENSITY, ENTHALPY, Viscousity, THERMCONDT).
+ * One set holds per_row * M doubles, per_row = 141 (flow) or 360 (with the
+ * thermal solver), the module arrays in the order the reference zeroes them
+ * (Fortran order, j fastest): U1xzL_io(M,4), G1xzL_io(M,3), UPxzL_io(M,3),
+ * U2xzL_io(M,6), UGxzL_io(M,6), U3xzL_io(M,10), UGUxzL_io(M,10),
+ * DVDL1xzL_io(M,3,3), DVDLPxzL_io(M,3,3), DVDL2xzL_io(M,9,9), then T1, D1, H1,
+ * M1, T2, D2, H2, DH, PHxzL_io(M), DVDL1MxzL_io(M,3,3), DVDL1MHxzL_io(M,3,3),
+ * DVDL1MUxzL_io(M,3,3,3), DVDL2MxzL_io(M,9,9), UHxzL_io(M,3), GHxzL_io(M,3),
+ * U2DHxzL_io(M,6), DhDL1xzL_io(M,3), DhDLPxzL_io(M,3), DTDLKxzL_io(M,3),
+ * DTDLKUxzL_io(M,3,3), DTDLKDVDLxzL_io(M,3,3,3), DHDLMDVDLxzL_io(M,3,3,3).
+ * Plane sums are taken in a fixed tree order.  A periodic-domain context
+ * gives CHAPSIM_ERR_BADARG. */
+int chapsim_pp_mean_zx_io(chapsim_ctx_t* ctx);
+/* Downloads the last set (out may be NULL); per_row (may be NULL) receives 141 or 360. */
+int chapsim_download_pp_means_io(chapsim_ctx_t* ctx, double* out, int32_t* per_row);
 /* Restart of the time averages (the reader of the averaged-statistics file). */
 int chapsim_upload_pp_means_tg(chapsim_ctx_t* ctx, int32_t nstatis, const double* u1, const double* up,
                                const double* u2, const double* u3, const double* dvdl1, const double* dvdlp,

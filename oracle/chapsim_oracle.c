@@ -2393,6 +2393,187 @@ void orc_pp_mean_zx_tg(const orc_t* o, double* out) {
     }
 }
 
+/* ====================================================================== */
+/* Statistics of the main domain: PP_MEAN_ZX_FLOW_Xperiodic_io           */
+/* (src/processing/PP_MEAN_ZX.f90:311-796), plane channel (RCCI1 = RNDI1 */
+/* = 1, no pipe-centre branch).  One set is out[NIO*M], Fortran order     */
+/* with j fastest, the module arrays in the order the reference zeroes    */
+/* them: U1xzL_io(M,4) | G1xzL_io(M,3) | UPxzL_io(M,3) | U2xzL_io(M,6) |   */
+/* UGxzL_io(M,6) | U3xzL_io(M,10) | UGUxzL_io(M,10) | DVDL1xzL_io(M,3,3) | */
+/* DVDLPxzL_io(M,3,3) | DVDL2xzL_io(M,9,9)  (141 per row), then with the  */
+/* thermal solver: T1 | D1 | H1 | M1 | T2 | D2 | H2 | DH | PH (M each) |  */
+/* DVDL1MxzL_io(M,3,3) | DVDL1MHxzL_io(M,3,3) | DVDL1MUxzL_io(M,3,3,3) |   */
+/* DVDL2MxzL_io(M,9,9) | UHxzL_io(M,3) | GHxzL_io(M,3) | U2DHxzL_io(M,6) | */
+/* DhDL1xzL_io(M,3) | DhDLPxzL_io(M,3) | DTDLKxzL_io(M,3) |               */
+/* DTDLKUxzL_io(M,3,3) | DTDLKDVDLxzL_io(M,3,3,3) | DHDLMDVDLxzL_io(M,3,3,3) */
+/* (219 more).  Loop order J, I, K as the reference; every product in its */
+/* left-to-right order.                                                   */
+/* ====================================================================== */
+int orc_pp_io_per_row(const orc_t* o) { return o->thermal ? 360 : 141; }
+
+void orc_pp_mean_zx_io(const orc_t* o, double* out) {
+    const int L = o->L, M = o->M, N = o->N;
+    const double VL = 1.0 / (double)(L * N);  /* VL1313_io */
+    const int th = o->thermal;
+#pragma omp parallel for schedule(static)
+    for (int J = 1; J <= M; ++J) {
+        const int JP = J + 1, JM = J - 1, JJ = J, JJP = J + 1;
+        double U1[4] = {0}, G1[3] = {0}, UP[3] = {0}, U2[6] = {0}, UG[6] = {0}, U3[10] = {0}, UGU[10] = {0};
+        double D1[3][3] = {{0}}, DP[3][3] = {{0}}, D2[9][9];
+        double T1 = 0, Dn1 = 0, H1 = 0, M1 = 0, T2 = 0, Dn2 = 0, H2 = 0, DHs = 0, PHs = 0;
+        double D1M[3][3] = {{0}}, D1MH[3][3] = {{0}}, D1MU[3][3][3], D2M[9][9];
+        double UH[3] = {0}, GH[3] = {0}, U2DH[6] = {0}, HD1[3] = {0}, HDP[3] = {0}, TK[3] = {0}, TKU[3][3] = {{0}};
+        double TKD[3][3][3], HMD[3][3][3];
+        memset(D2, 0, sizeof(D2)); memset(D2M, 0, sizeof(D2M)); memset(D1MU, 0, sizeof(D1MU));
+        memset(TKD, 0, sizeof(TKD)); memset(HMD, 0, sizeof(HMD));
+        for (int I = 1; I <= L; ++I) {
+            const int IP = IPV(o, I), IM = IMV(o, I);
+            for (int K = 1; K <= N; ++K) {
+                const int KP = KPV(o, K), KM = KMV(o, K);
+                double G[3], U[3], UJP[3], UJM[3], UKP[3], UKM[3], UIP[3], UIM[3];
+                G[0] = (GV(o, I, J, K, 1) + GV(o, IP, J, K, 1)) * 0.5;
+                U[0] = (QV(o, I, J, K, 1) + QV(o, IP, J, K, 1)) * 0.5;
+                UJP[0] = (QV(o, I, JP, K, 1) + QV(o, IP, JP, K, 1)) * 0.5;
+                UJM[0] = (QV(o, I, JM, K, 1) + QV(o, IP, JM, K, 1)) * 0.5;
+                UKP[0] = (QV(o, I, J, KP, 1) + QV(o, IP, J, KP, 1)) * 0.5;
+                UKM[0] = (QV(o, I, J, KM, 1) + QV(o, IP, J, KM, 1)) * 0.5;
+                G[2] = ((GV(o, I, J, K, 3) + GV(o, I, J, KP, 3)) * 1.0) * 0.5;
+                U[2] = ((QV(o, I, J, K, 3) + QV(o, I, J, KP, 3)) * 1.0) * 0.5;
+                UIP[2] = ((QV(o, IP, J, K, 3) + QV(o, IP, J, KP, 3)) * 1.0) * 0.5;
+                UIM[2] = ((QV(o, IM, J, K, 3) + QV(o, IM, J, KP, 3)) * 1.0) * 0.5;
+                UJP[2] = ((QV(o, I, JP, K, 3) + QV(o, I, JP, KP, 3)) * 1.0) * 0.5;
+                UJM[2] = ((QV(o, I, JM, K, 3) + QV(o, I, JM, KP, 3)) * 1.0) * 0.5;
+                G[1] = ((GV(o, I, J, K, 2) + GV(o, I, JP, K, 2)) * 1.0) * 0.5;
+                U[1] = ((QV(o, I, J, K, 2) + QV(o, I, JP, K, 2)) * 1.0) * 0.5;
+                UIP[1] = ((QV(o, IP, J, K, 2) + QV(o, IP, JP, K, 2)) * 1.0) * 0.5;
+                UIM[1] = ((QV(o, IM, J, K, 2) + QV(o, IM, JP, K, 2)) * 1.0) * 0.5;
+                UKP[1] = ((QV(o, I, J, KP, 2) + QV(o, I, JP, KP, 2)) * 1.0) * 0.5;
+                UKM[1] = ((QV(o, I, J, KM, 2) + QV(o, I, JP, KM, 2)) * 1.0) * 0.5;
+                const double P = F3(o->PR, o, I, J, K);
+                for (int m = 0; m < 3; ++m) {
+                    U1[m] = U1[m] + U[m];
+                    G1[m] = G1[m] + G[m];
+                    UP[m] = UP[m] + U[m] * P;
+                }
+                U1[3] = U1[3] + P;
+                for (int m = 1; m <= 3; ++m)
+                    for (int n = m; n <= 3; ++n) {
+                        const int l = (m * (7 - m)) / 2 + n - 3;
+                        UG[l - 1] = UG[l - 1] + U[m - 1] * G[n - 1];
+                        U2[l - 1] = U2[l - 1] + U[m - 1] * U[n - 1];
+                    }
+                for (int m = 1; m <= 3; ++m)
+                    for (int n = m; n <= 3; ++n)
+                        for (int h = n; h <= 3; ++h) {
+                            const int l = m * (6 - m) + (n * (7 - n)) / 2 + h - 8;
+                            UGU[l - 1] = UGU[l - 1] + U[m - 1] * G[n - 1] * U[h - 1];
+                        }
+                for (int m = 1; m <= 3; ++m)
+                    for (int n = m; n <= 3; ++n)
+                        for (int h = n; h <= 3; ++h) {
+                            const int l = m * (6 - m) + (n * (7 - n)) / 2 + h - 8;
+                            U3[l - 1] = U3[l - 1] + U[m - 1] * U[n - 1] * U[h - 1];
+                        }
+                double D[3][3];
+                D[0][0] = (QV(o, IP, J, K, 1) - QV(o, I, J, K, 1)) * o->DXI;
+                D[0][2] = (UKP[0] - UKM[0]) * o->DZI * 0.5;
+                D[0][1] = ((UJP[0] - U[0]) * o->DYCI[JJP] + (U[0] - UJM[0]) * o->DYCI[JJ]) * 0.5;
+                D[1][0] = (UIP[1] - UIM[1]) * o->DXI * 0.5;
+                D[1][2] = (UKP[1] - UKM[1]) * o->DZI * 0.5;
+                D[1][1] = (QV(o, I, JP, K, 2) * 1.0 - QV(o, I, J, K, 2) * 1.0) * o->DYFI[JJ];
+                D[2][2] = (QV(o, I, J, KP, 3) * 1.0 - QV(o, I, J, K, 3) * 1.0) * o->DZI;
+                D[2][0] = (UIP[2] - UIM[2]) * o->DXI * 0.5;
+                D[2][1] = ((UJP[2] - U[2]) * o->DYCI[JJP] + (U[2] - UJM[2]) * o->DYCI[JJ]) * 0.5;
+                for (int m = 0; m < 3; ++m)
+                    for (int n = 0; n < 3; ++n) {
+                        D1[m][n] = D1[m][n] + D[m][n];
+                        DP[m][n] = DP[m][n] + D[m][n] * P;
+                    }
+                for (int m = 0; m < 3; ++m)
+                    for (int h = 0; h < 3; ++h)
+                        for (int n = 0; n < 3; ++n)
+                            for (int p = 0; p < 3; ++p) D2[m * 3 + h][n * 3 + p] = D2[m * 3 + h][n * 3 + p] + D[m][h] * D[n][p];
+                if (!th) continue;
+                const double Tc = F3(o->TEMP, o, I, J, K), Dc = F3(o->DEN, o, I, J, K);
+                const double Hc = F3(o->ENTH, o, I, J, K), MUc = F3(o->MU, o, I, J, K);
+                const double Kc = F3(o->KAPPA, o, I, J, K);
+                T1 = T1 + Tc; Dn1 = Dn1 + Dc; H1 = H1 + Hc; M1 = M1 + MUc;
+                T2 = T2 + Tc * Tc; Dn2 = Dn2 + Dc * Dc; H2 = H2 + Hc * Hc;
+                DHs = DHs + Hc * Dc;
+                PHs = PHs + Hc * P;
+                double HDL[3], TDL[3];
+                HDL[0] = (F3(o->ENTH, o, IP, J, K) - F3(o->ENTH, o, IM, J, K)) * o->DXI * 0.5;
+                HDL[2] = (F3(o->ENTH, o, I, J, KP) - F3(o->ENTH, o, I, J, KM)) * o->DZI * 0.5;
+                HDL[1] = ((F3(o->ENTH, o, I, JP, K) - F3(o->ENTH, o, I, J, K)) * o->DYCI[JJP] +
+                          (F3(o->ENTH, o, I, J, K) - F3(o->ENTH, o, I, JM, K)) * o->DYCI[JJ]) * 0.5;
+                TDL[0] = (F3(o->TEMP, o, IP, J, K) - F3(o->TEMP, o, IM, J, K)) * o->DXI * 0.5;
+                TDL[2] = (F3(o->TEMP, o, I, J, KP) - F3(o->TEMP, o, I, J, KM)) * o->DZI * 0.5;
+                TDL[1] = ((F3(o->TEMP, o, I, JP, K) - F3(o->TEMP, o, I, J, K)) * o->DYCI[JJP] +
+                          (F3(o->TEMP, o, I, J, K) - F3(o->TEMP, o, I, JM, K)) * o->DYCI[JJ]) * 0.5;
+                for (int m = 0; m < 3; ++m)
+                    for (int n = 0; n < 3; ++n) {
+                        D1M[m][n] = D1M[m][n] + D[m][n] * MUc;
+                        D1MH[m][n] = D1MH[m][n] + D[m][n] * MUc * Hc;
+                        for (int h = 0; h < 3; ++h) D1MU[m][n][h] = D1MU[m][n][h] + D[m][n] * MUc * U[h];
+                    }
+                for (int m = 0; m < 3; ++m)
+                    for (int h = 0; h < 3; ++h)
+                        for (int n = 0; n < 3; ++n)
+                            for (int p = 0; p < 3; ++p)
+                                D2M[m * 3 + h][n * 3 + p] = D2M[m * 3 + h][n * 3 + p] + D[m][h] * D[n][p] * MUc;
+                for (int m = 0; m < 3; ++m) {
+                    UH[m] = UH[m] + Hc * U[m];
+                    GH[m] = GH[m] + Hc * G[m];
+                    HD1[m] = HD1[m] + HDL[m];
+                    HDP[m] = HDP[m] + HDL[m] * P;
+                    TK[m] = TK[m] + TDL[m] * Kc;
+                    for (int n = 0; n < 3; ++n) {
+                        TKU[m][n] = TKU[m][n] + TDL[m] * Kc * U[n];
+                        for (int h = 0; h < 3; ++h) {
+                            TKD[m][n][h] = TKD[m][n][h] + TDL[m] * Kc * D[n][h];
+                            HMD[m][n][h] = HMD[m][n][h] + HDL[m] * MUc * D[n][h];
+                        }
+                    }
+                }
+                for (int m = 1; m <= 3; ++m)
+                    for (int n = m; n <= 3; ++n) {
+                        const int l = (m * (7 - m)) / 2 + n - 3;
+                        U2DH[l - 1] = U2DH[l - 1] + Dc * Hc * U[m - 1] * U[n - 1];
+                    }
+            }
+        }
+        int off = 0;
+#define PUT(v) (out[(size_t)(off++) * M + (size_t)(J - 1)] = (v) * VL)
+        for (int m = 0; m < 4; ++m) PUT(U1[m]);
+        for (int m = 0; m < 3; ++m) PUT(G1[m]);
+        for (int m = 0; m < 3; ++m) PUT(UP[m]);
+        for (int l = 0; l < 6; ++l) PUT(U2[l]);
+        for (int l = 0; l < 6; ++l) PUT(UG[l]);
+        for (int l = 0; l < 10; ++l) PUT(U3[l]);
+        for (int l = 0; l < 10; ++l) PUT(UGU[l]);
+        for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(D1[m][n]);
+        for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(DP[m][n]);
+        for (int l2 = 0; l2 < 9; ++l2) for (int l1 = 0; l1 < 9; ++l1) PUT(D2[l1][l2]);
+        if (th) {
+            PUT(T1); PUT(Dn1); PUT(H1); PUT(M1); PUT(T2); PUT(Dn2); PUT(H2); PUT(DHs); PUT(PHs);
+            for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(D1M[m][n]);
+            for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(D1MH[m][n]);
+            for (int h = 0; h < 3; ++h) for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(D1MU[m][n][h]);
+            for (int l2 = 0; l2 < 9; ++l2) for (int l1 = 0; l1 < 9; ++l1) PUT(D2M[l1][l2]);
+            for (int m = 0; m < 3; ++m) PUT(UH[m]);
+            for (int m = 0; m < 3; ++m) PUT(GH[m]);
+            for (int l = 0; l < 6; ++l) PUT(U2DH[l]);
+            for (int m = 0; m < 3; ++m) PUT(HD1[m]);
+            for (int m = 0; m < 3; ++m) PUT(HDP[m]);
+            for (int m = 0; m < 3; ++m) PUT(TK[m]);
+            for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(TKU[m][n]);
+            for (int h = 0; h < 3; ++h) for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(TKD[m][n][h]);
+            for (int h = 0; h < 3; ++h) for (int n = 0; n < 3; ++n) for (int m = 0; m < 3; ++m) PUT(HMD[m][n][h]);
+        }
+#undef PUT
+    }
+}
+
 /* PP_MEAN_T_TG(TP) (src/processing/PP_MEAN_T.f90:343-392) on a set of means */
 void orc_pp_mean_t_tg(int M, int tp, int pp_instn_sz, const double* inst, double* avg, int* nstatis) {
     *nstatis = *nstatis + 1;

@@ -62,6 +62,9 @@ def lib():
         L.orc_pp_mean_t_tg.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp,
                                        ctypes.POINTER(ctypes.c_int)]
         L.orc_pp_monitor_tg.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double, _dp]
+        L.orc_pp_io_per_row.argtypes = [ctypes.c_void_p]
+        L.orc_pp_io_per_row.restype = ctypes.c_int
+        L.orc_pp_mean_zx_io.argtypes = [ctypes.c_void_p, _dp]
         L.orc_poisson.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_fft_complex.argtypes = [ctypes.c_int, _dp, _dp, ctypes.c_int]
         L.orc_tdma_cyc.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
@@ -224,6 +227,14 @@ class Oracle:
         n = ctypes.c_int(int(nstatis))
         self._lib.orc_pp_mean_t_tg(self.M, int(tp), int(pp_instn_sz), _p(inst), _p(avg), ctypes.byref(n))
         return n.value
+
+    # ---- statistics of the main domain (PP_MEAN_ZX_FLOW_Xperiodic_io) ----
+    # One set is a flat array of 141*M doubles (flow) or 360*M (with the thermal solver), the
+    # module arrays in the order the reference zeroes them (Fortran order, j fastest).
+    def pp_mean_zx_io(self):
+        out = np.zeros(self._lib.orc_pp_io_per_row(self._h) * self.M)
+        self._lib.orc_pp_mean_zx_io(self._h, _p(out))
+        return out
 
     def pp_monitor_tg(self, inst, avg, ren):
         mon = np.zeros(20)
