@@ -592,8 +592,8 @@ class ChannelTG:
     def autotune(self, force=-1):
         """Keeps the fastest y-solve, right-hand-side and pressure-stage variants for
         this grid, or forces them (bit 0: sequential y-solve; bits 1-2: right-hand
-        sides 0 fused, 1 split, 2 fused with bulk-copy staging, 3 fused with two
-        points per lane in FP64; bit 3: fused plane
+        sides 0 fused, 1 split, 2 fused with bulk-copy staging, 3 the wide fused
+        form (16-byte loads: two points per lane in FP64, four in FP32); bit 3: fused plane
         transforms; bit 4: two-way y-solve; bit 5: sequential y-solve with its
         forward intermediate in shared memory at one block per SM; bit 6: warp
         affine scans over the sequential factors; bit 8: z-sweep tiles of 16
@@ -608,7 +608,7 @@ class ChannelTG:
                           "rhs_split": ms[3], "rhs_bulk": ms[4], "pressure_chained": ms[5],
                           "pressure_plane": ms[6], "ysolve_two_way": ms[7], "ysolve_sequential_smem": ms[8],
                           "ysolve_scan": ms[9], "zsweep_tile32": ms[10], "zsweep_tile16": ms[11],
-                          "pressure_chained_zpipe": ms[12], "rhs_fused_paired": ms[13]}
+                          "pressure_chained_zpipe": ms[12], "rhs_fused_wide": ms[13]}
 
 
 class Ensemble:

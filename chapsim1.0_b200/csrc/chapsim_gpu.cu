@@ -149,8 +149,8 @@ struct chapsim_ctx {
     int ysolve_kind = 0;          // 0: warp Thomas/PCR hybrid, 1: sequential Thomas, 2: two-way, 3: sequential with
                                   // the forward intermediate in shared memory at one block per SM, 4: warp affine
                                   // scans over the sequential factors (chapsim_autotune)
-    int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk, 3: fused with
-                                  // two points per lane in FP64 (FP32 always pairs) (chapsim_autotune)
+    int k1_kind = 0;              // 0: fused k_rhs_xsweep, 1: k_rhs_point + k_xsweep, 2: k_rhs_xsweep_bulk, 3: the wide
+                                  // fused form, 16-byte loads (rhs_pv) (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     int zs_tw = 32;               // lines per tile of the z sweep, 32 or 16 (chapsim_autotune)
     bool fz_pipe = false;         // persistent double-buffered z transforms (chapsim_autotune)
@@ -449,8 +449,8 @@ template <> StepFields<float> step_fields<float>(chapsim_ctx* c) { return {c->Qf
 template <typename R>
 int configure_momentum(chapsim_ctx* ctx) {
     const Geo& g = ctx->g;
-    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R, sizeof(R) == 4>, smem_rhs<R>(g))));
-    if (sizeof(R) == 8) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R, true>, smem_rhs<R>(g))));
+    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R, rhs_pv<R>(false)>, smem_rhs<R>(g))));
+    DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep<S, R, rhs_pv<R>(true)>, smem_rhs<R>(g))));
     ctx->rb_nw = 0;
     DISPATCH_S(g.L / 32, ctx->rb_nw = rb_warps<R>(g.L, bulk_smem_limit(k_rhs_xsweep_bulk<S, R>)));
     if (ctx->rb_nw > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_smem<R>(g.L, ctx->rb_nw))));
@@ -558,14 +558,14 @@ void launch_rhs_x(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns
         const int nbx = (int)((nl + XS_NT / 32 - 1) / (XS_NT / 32));
         DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_xsweep<S, R>, nbx, XS_NT, smem_xs<R>(g), s, g, f.RHS, fac)));
         ctx->launches += 1;
-    } else if (ctx->k1_kind == 3 && sizeof(R) == 8) {
+    } else if (ctx->k1_kind == 3) {
         const int grx = g.M * g.N / RHS_WPB;
-        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R, true>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g, f.Q, f.PR,
-                                         f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R, rhs_pv<R>(true)>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g,
+                                         f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
     } else {
         const int grx = g.M * g.N / RHS_WPB;
-        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R, sizeof(R) == 4>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g, f.Q,
-                                         f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
+        DISPATCH_S(g.L / 32, (launch_pdl(ctx->pdl, k_rhs_xsweep<S, R, rhs_pv<R>(false)>, grx, RHS_WPB * 32, smem_rhs<R>(g), s, g,
+                                         f.Q, f.PR, f.H0, f.RHS, ctx->part_rhs, ctx->st, fac, ns)));
     }
 }
 
@@ -2286,7 +2286,7 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         CK(cudaMemcpyAsync(hsave, h0, hb, cudaMemcpyDeviceToDevice, s));
         const int keep = ctx->k1_kind;
         const bool bulk_fits = ctx->rb_nw > 0;
-        const bool pair_ok = !mixed && (g.L / 32) % 2 == 0;  // kind 3: the FP64 paired form
+        const bool pair_ok = (g.L / 32) % (mixed ? 4 : 2) == 0;  // kind 3: the wide form
         for (int kind = 0; kind < 4; ++kind) {
             if ((kind == 2 && !bulk_fits) || (kind == 3 && !pair_ok)) {
                 tk[kind] = 1e30f;

@@ -41,12 +41,40 @@
 // at 384 x 256 x 384 than at 4 (128 registers with spills); FP32 is fastest
 // at 4.
 #define RHS_MINB(R) (sizeof(R) == 8 ? 3 : 4)
-// The paired form (two adjacent points per lane, 2-element vector loads) in FP64 holds twice the
-// loaded values: a two-block budget (up to 255 registers).
-#define RHS_MINB_P(R, PAIR) ((PAIR) && sizeof(R) == 8 ? 2 : RHS_MINB(R))
-template <typename R> struct Vec2;
-template <> struct Vec2<float> { using T = float2; };
-template <> struct Vec2<double> { using T = double2; };
+// The vector forms (PV adjacent points per lane) with 16-byte vectors hold two or four times the
+// loaded values of the one-point form: a two-block budget (up to 255 registers).
+#define RHS_MINB_P(R, PV) ((PV) * sizeof(R) > 8 ? 2 : RHS_MINB(R))
+// points per lane of the fused right-hand side: the default form (1 in FP64, 2 in FP32) and
+// the wide form, autotuned kind 3 (2 in FP64, 4 in FP32: 16-byte loads)
+template <typename R> __host__ __device__ constexpr int rhs_pv(bool wide) {
+    return sizeof(R) == 8 ? (wide ? 2 : 1) : (wide ? 4 : 2);
+}
+// PV consecutive elements through one vector access (PV * sizeof(R) = 8 or 16 bytes, aligned)
+template <int PV, typename R>
+__device__ __forceinline__ void ldvec(const R* p, R (&o)[PV]) {
+    if constexpr (PV * sizeof(R) == 16) {
+        if constexpr (sizeof(R) == 4) {
+            const float4 v = *reinterpret_cast<const float4*>(p);
+            o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+        } else {
+            const double2 v = *reinterpret_cast<const double2*>(p);
+            o[0] = v.x; o[1] = v.y;
+        }
+    } else {
+        static_assert(PV * sizeof(R) == 8, "8- or 16-byte vectors");
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        o[0] = v.x; o[1] = v.y;
+    }
+}
+template <int PV, typename R>
+__device__ __forceinline__ void stvec(R* p, const R (&a)[PV]) {
+    if constexpr (PV * sizeof(R) == 16) {
+        if constexpr (sizeof(R) == 4) *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
+        else *reinterpret_cast<double2*>(p) = make_double2(a[0], a[1]);
+    } else {
+        *reinterpret_cast<float2*>(p) = make_float2(a[0], a[1]);
+    }
+}
 #define SWEEP_NT 256
 #define FAC_SET (TF_NF(12) * 32)   // doubles per factor table
 
@@ -220,8 +248,8 @@ __device__ __forceinline__ RhsLine<R> rhs_line(const Geo& g, double dt, int ns, 
 }
 
 // ---------------------------------------------------------------------------
-template <int S, typename R, bool PAIR>
-__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB_P(R, PAIR)) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
+template <int S, typename R, int PV>
+__global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB_P(R, PV)) k_rhs_xsweep(Geo g, const R* __restrict__ Q, const R* __restrict__ PR,
                                                              R* __restrict__ H0, R* __restrict__ RHS,
                                                              double* __restrict__ partial, DevState* __restrict__ st,
                                                              const R* __restrict__ fac, int ns) {
@@ -263,57 +291,65 @@ __global__ void __launch_bounds__(RHS_WPB * 32, RHS_MINB_P(R, PAIR)) k_rhs_xswee
         prefetch_l2(H0 + irow + i + 2 * g.FI);
     }
     double bulk = 0.0;
-    if constexpr (PAIR && S % 2 == 0) {
-        // Paired form (always in FP32; an autotuned alternative in FP64): each lane takes two
-        // adjacent points (i, i+1) per iteration with 2-element vector loads, so a warp request
-        // moves twice the bytes of the one-point form (in FP32 as many as one FP64 request); the
-        // x neighbours outside the pair are single loads.  Rows start at multiples of L (even),
-        // so every pair is aligned to its vector size.
-        using R2 = typename Vec2<R>::T;
+    if constexpr (PV > 1 && S % PV == 0) {
+        // Vector form (PV = 2 in FP32 always; PV = 2 in FP64 and 4 in FP32 as the autotuned
+        // wide form): each lane takes PV adjacent points (i .. i+PV-1, one segment of the
+        // x sweep's layout) per iteration with PV-element vector loads, so a warp request moves
+        // PV times the bytes of the one-point form; the x neighbours outside the group are
+        // single loads.  Rows start at multiples of L (a multiple of 32), so every group is
+        // aligned to its vector size.
 #pragma unroll 1
-        for (int kk = 0; kk < S / 2; ++kk) {
-            const int i = 2 * lane + 64 * kk;
-            const int il = i == 0 ? L - 1 : i - 1, ir = i + 2 == L ? 0 : i + 2;
-            auto ld2 = [&](const R* b, long long row) { return *reinterpret_cast<const R2*>(b + row + i); };
-            const R2 u2 = ld2(U, rowc), v2 = ld2(V, rowc), w2 = ld2(W, rowc);
-            const R2 ujp = ld2(U, rowjp), ujm = ld2(U, rowjm), ukp = ld2(U, rowkp), ukm = ld2(U, rowkm);
-            const R2 vjp = ld2(V, rowjp), vjm = ld2(V, rowjm), vkp = ld2(V, rowkp), vkm = ld2(V, rowkm);
-            const R2 wjp = ld2(W, rowjp), wjm = ld2(W, rowjm), wkp = ld2(W, rowkp), wkm = ld2(W, rowkm);
-            const R2 pc = ld2(PR, rowc), pjm = ld2(PR, rowjm), pkm = ld2(PR, rowkm);
-            const R2 wjmkp = ld2(W, rowjmkp), vjpkm = ld2(V, rowjpkm);
+        for (int kk = 0; kk < S / PV; ++kk) {
+            const int i = PV * lane + 32 * PV * kk;
+            const int il = i == 0 ? L - 1 : i - 1, ir = i + PV == L ? 0 : i + PV;
+            auto ldv = [&](const R* b, long long row, R (&o)[PV]) { ldvec<PV>(b + row + i, o); };
+            R uc[PV], vc[PV], wc[PV], ujp[PV], ujm[PV], ukp[PV], ukm[PV], vjp[PV], vjm[PV], vkp[PV], vkm[PV];
+            R wjp[PV], wjm[PV], wkp[PV], wkm[PV], pc[PV], pjm[PV], pkm[PV], wjmkp[PV], vjpkm[PV];
+            ldv(U, rowc, uc); ldv(V, rowc, vc); ldv(W, rowc, wc);
+            ldv(U, rowjp, ujp); ldv(U, rowjm, ujm); ldv(U, rowkp, ukp); ldv(U, rowkm, ukm);
+            ldv(V, rowjp, vjp); ldv(V, rowjm, vjm); ldv(V, rowkp, vkp); ldv(V, rowkm, vkm);
+            ldv(W, rowjp, wjp); ldv(W, rowjm, wjm); ldv(W, rowkp, wkp); ldv(W, rowkm, wkm);
+            ldv(PR, rowc, pc); ldv(PR, rowjm, pjm); ldv(PR, rowkm, pkm);
+            ldv(W, rowjmkp, wjmkp); ldv(V, rowjpkm, vjpkm);
             const R ul = U[rowc + il], ur = U[rowc + ir], vl = V[rowc + il], vr = V[rowc + ir];
             const R wl = W[rowc + il], wr = W[rowc + ir], pl = PR[rowc + il];
             const R vjpl = V[rowjp + il], wkpl = W[rowkp + il], ujmr = U[rowjm + ir], ukmr = U[rowkm + ir];
             // every load of the iteration is issued before any store: H0 is read
             // and written through one pointer, which the compiler cannot reorder
             const long long ii = irow + i;
-            const R2 h0u = *reinterpret_cast<const R2*>(H0 + ii);
-            R2 h0v;
-            if (vrow) h0v = *reinterpret_cast<const R2*>(H0 + ii + g.FI);
-            else h0v.x = h0v.y = R(0);
-            const R2 h0w = *reinterpret_cast<const R2*>(H0 + ii + 2 * g.FI);
-            const RhsStencil<R> s0{u2.x, u2.y, ul, ujp.x, ujm.x, ukp.x, ukm.x,
-                                   v2.x, v2.y, vl, vjp.x, vjm.x, vkp.x, vkm.x,
-                                   w2.x, w2.y, wl, wjp.x, wjm.x, wkp.x, wkm.x,
-                                   pc.x, pl, pjm.x, pkm.x,
-                                   vjpl, wkpl, ujm.y, wjmkp.x, ukm.y, vjpkm.x,
-                                   h0u.x, h0v.x, h0w.x};
-            const RhsStencil<R> s1{u2.y, ur, u2.x, ujp.y, ujm.y, ukp.y, ukm.y,
-                                   v2.y, vr, v2.x, vjp.y, vjm.y, vkp.y, vkm.y,
-                                   w2.y, wr, w2.x, wjp.y, wjm.y, wkp.y, wkm.y,
-                                   pc.y, pc.x, pjm.y, pkm.y,
-                                   vjp.x, wkp.x, ujmr, wjmkp.y, ukmr, vjpkm.y,
-                                   h0u.y, h0v.y, h0w.y};
-            R2 Hu, Hv, Hw, ru, rv, rw;
-            rhs_point(cl, s0, vrow, Hu.x, Hv.x, Hw.x, ru.x, rv.x, rw.x, bulk);
-            rhs_point(cl, s1, vrow, Hu.y, Hv.y, Hw.y, ru.y, rv.y, rw.y, bulk);
-            *reinterpret_cast<R2*>(H0 + ii) = Hu;
-            if (vrow) *reinterpret_cast<R2*>(H0 + ii + g.FI) = Hv;
-            *reinterpret_cast<R2*>(H0 + ii + 2 * g.FI) = Hw;
-            const int pos = seg_pos<S>(i);  // i + 1 is the next position of the same segment (S even)
-            sl[pos] = ru.x; sl[pos + 1] = ru.y;
-            if (vrow) { sl[LS + pos] = rv.x; sl[LS + pos + 1] = rv.y; }
-            sl[2 * LS + pos] = rw.x; sl[2 * LS + pos + 1] = rw.y;
+            R h0u[PV], h0v[PV], h0w[PV];
+            ldvec<PV>(H0 + ii, h0u);
+            if (vrow) ldvec<PV>(H0 + ii + g.FI, h0v);
+            else
+#pragma unroll
+                for (int e = 0; e < PV; ++e) h0v[e] = R(0);
+            ldvec<PV>(H0 + ii + 2 * g.FI, h0w);
+            R Hu[PV], Hv[PV], Hw[PV], ru[PV], rv[PV], rw[PV];
+#pragma unroll
+            for (int e = 0; e < PV; ++e) {
+                const bool lo = e == 0, hi = e == PV - 1;
+                const RhsStencil<R> sp{uc[e], hi ? ur : uc[hi ? e : e + 1], lo ? ul : uc[lo ? e : e - 1],
+                                       ujp[e], ujm[e], ukp[e], ukm[e],
+                                       vc[e], hi ? vr : vc[hi ? e : e + 1], lo ? vl : vc[lo ? e : e - 1],
+                                       vjp[e], vjm[e], vkp[e], vkm[e],
+                                       wc[e], hi ? wr : wc[hi ? e : e + 1], lo ? wl : wc[lo ? e : e - 1],
+                                       wjp[e], wjm[e], wkp[e], wkm[e],
+                                       pc[e], lo ? pl : pc[lo ? e : e - 1], pjm[e], pkm[e],
+                                       lo ? vjpl : vjp[lo ? e : e - 1], lo ? wkpl : wkp[lo ? e : e - 1],
+                                       hi ? ujmr : ujm[hi ? e : e + 1], wjmkp[e], hi ? ukmr : ukm[hi ? e : e + 1],
+                                       vjpkm[e], h0u[e], h0v[e], h0w[e]};
+                rhs_point(cl, sp, vrow, Hu[e], Hv[e], Hw[e], ru[e], rv[e], rw[e], bulk);
+            }
+            stvec<PV>(H0 + ii, Hu);
+            if (vrow) stvec<PV>(H0 + ii + g.FI, Hv);
+            stvec<PV>(H0 + ii + 2 * g.FI, Hw);
+            const int pos = seg_pos<S>(i);  // the group's points are consecutive positions of one segment
+#pragma unroll
+            for (int e = 0; e < PV; ++e) {
+                sl[pos + e] = ru[e];
+                if (vrow) sl[LS + pos + e] = rv[e];
+                sl[2 * LS + pos + e] = rw[e];
+            }
         }
     } else {
 #pragma unroll 1

@@ -406,8 +406,9 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *          0 = fused (one warp per x line, per-thread loads; two adjacent
  *          points per lane in FP32), 1 = split into a point-wise kernel and
  *          a line-sweep kernel, 2 = fused with the stencil rows staged in
- *          shared memory by bulk copies, 3 = fused with two adjacent points
- *          per lane in FP64 (even L / 32; elsewhere it means 0);
+ *          shared memory by bulk copies, 3 = the wide fused form, 16-byte
+ *          loads of two adjacent points per lane in FP64 or four in FP32
+ *          (L / 32 a multiple of 2 or 4; elsewhere it means 0);
  *   bit 3: pressure stage (periodic channel only), 0 = chained x and z
  *          transforms, 1 = fused plane transforms: one block per y row where
  *          the row's half spectrum fits one block's shared memory, one
@@ -426,8 +427,7 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  * sequential y-solve at one block per SM (1e30 where it does not apply) and
  * the scan y-solve, the z sweep with 32- and with 16-line tiles (0 where it
  * does not apply), the pressure stage with the double-buffered z
- * transforms, and the FP64 paired right-hand side (1e30 where it does not
- * apply).
+ * transforms, and the wide right-hand side (1e30 where it does not apply).
  * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 

@@ -154,6 +154,16 @@ def test_c2_mixed_tuner_choice_ten_steps(c2_ref):
     _check_mixed(c2_ref, _gpu_run(w, c2_ref, 10, -1, precision="mixed"))
 
 
+@pytest.mark.parametrize("force", [0, 6, 6 | 64, 2, 4])
+def test_c2_mixed_rhs_forms_ten_steps(c2_ref, force):
+    """every right-hand-side form in mixed precision (two points per lane, the wide
+    form with four, split, bulk-staged) against the FP64 oracle"""
+    w = _workload(C2)
+    got = _gpu_run(w, c2_ref, 10, force, precision="mixed")
+    assert got[0] == force, (got[0], force)
+    _check_mixed(c2_ref, got)
+
+
 # ------------------------------------------------------------------ 384 x 256 x 384
 C3 = "channel384x256x384_retau395_fp64"
 
@@ -180,9 +190,13 @@ def test_c3_variants_two_steps(c3_ref, force):
     _check_fp64(c3_ref, got, TOL_STEP, 1e-11)
 
 
-def test_c3_mixed_tuner_choice_two_steps(c3_ref):
+@pytest.mark.parametrize("force", [-1, 6 | 64])
+def test_c3_mixed_two_steps(c3_ref, force):
     w = _workload(C3)
-    _check_mixed(c3_ref, _gpu_run(w, c3_ref, 2, -1, precision="mixed"))
+    got = _gpu_run(w, c3_ref, 2, force, precision="mixed")
+    if force >= 0:
+        assert got[0] == force, (got[0], force)
+    _check_mixed(c3_ref, got)
 
 
 # ------------------------------------------------------------------ heated main domain

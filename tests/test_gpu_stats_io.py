@@ -53,7 +53,7 @@ def _compare(got, ref, M, arrays, tol, skip=()):
         assert v <= tol, (k, v)
 
 
-def _flow_case(L=64, M=48, N=32):
+def _flow_case(L=64, M=64, N=32):
     HX, HZ, STR2, REN = 2 * math.pi, math.pi, 2.0, 2800.0
     s = channel_setup(L, M, N, HX, HZ, STR2, REN)
     G, PR = initial_field(s, 41, 0.2)  # the momentum rho u
@@ -69,7 +69,7 @@ def _flow_case(L=64, M=48, N=32):
     return s, o, c
 
 
-def _thermal_case(L=64, M=48, N=32, qw=0.5):
+def _thermal_case(L=64, M=64, N=32, qw=0.5):
     HX, HZ, STR2, REN = 2 * math.pi, math.pi, 2.0, 2800.0
     s = channel_setup(L, M, N, HX, HZ, STR2, REN)
     Q, PR = initial_field(s, 1973, 0.1)
