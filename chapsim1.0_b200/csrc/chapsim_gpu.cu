@@ -153,6 +153,7 @@ struct chapsim_ctx {
                                   // fused form, 16-byte loads (rhs_pv) (chapsim_autotune)
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     int zs_tw = 32;               // lines per tile of the z sweep, 32 or 16 (chapsim_autotune)
+    int zs_il = 1;                // z-sweep tile layout: 1 line-contiguous, 2 lines interleaved in pairs (chapsim_autotune)
     bool fz_pipe = false;         // persistent double-buffered z transforms (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
     int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
@@ -454,8 +455,10 @@ int configure_momentum(chapsim_ctx* ctx) {
     ctx->rb_nw = 0;
     DISPATCH_S(g.L / 32, ctx->rb_nw = rb_warps<R>(g.L, bulk_smem_limit(k_rhs_xsweep_bulk<S, R>)));
     if (ctx->rb_nw > 0) DISPATCH_S(g.L / 32, CK(set_smem(k_rhs_xsweep_bulk<S, R>, rb_smem<R>(g.L, ctx->rb_nw))));
-    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 32>, smem_z<R>(g, 32))));
-    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 16>, smem_z<R>(g, 16))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 32, 1>, smem_z<R>(g, 32))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 16, 1>, smem_z<R>(g, 16))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 32, 2>, smem_z<R>(g, 32))));
+    DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 16, 2>, smem_z<R>(g, 16))));
     DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
     DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
     CK(set_smem(k_rhs_point<R>, smem_rt<R>()));
@@ -638,10 +641,14 @@ void launch_zsweep(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac) {
     const int zb_want = sizeof(R) == 4 && g.N / 32 <= 4 ? 3 : 2;  // zsweep_blocks<R, S>
     const int zb = sz * zb_want <= 226 * 1024 ? zb_want : (sz <= 113 * 1024 ? 2 : 1);
     const int nz = std::min((g.L / tw) * (3 * g.M - 1), zb * ctx->nsm);
-    if (tw == 16) {
-        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 16>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
+    if (tw == 16 && ctx->zs_il == 2) {
+        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 16, 2>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
+    } else if (tw == 16) {
+        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 16, 1>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
+    } else if (ctx->zs_il == 2) {
+        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 32, 2>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
     } else {
-        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 32>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
+        DISPATCH_S(g.N / 32, (launch_pdl(ctx->pdl, k_zsweep<S, R, 32, 1>, nz, SWEEP_NT, sz, ctx->stream, g, f.RHS, fac)));
     }
 }
 
@@ -2323,13 +2330,15 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         if (fk == 3 && !pair_ok) fk = 0;
         ctx->k1_kind = force >= 0 ? fk : best;
     }
-    // tile shape of the z sweep: 32 or 16 lines per tile (it rewrites RHS in place, which every
-    // substep's right-hand-side kernel rewrites before reading)
-    float tz[2] = {0.f, 0.f};
+    // tile shape of the z sweep: 32 or 16 lines per tile, line-contiguous or pair-interleaved
+    // (v = tile16 + 2 interleaved; it rewrites RHS in place, which every substep's
+    // right-hand-side kernel rewrites before reading)
+    float tz[4] = {0.f, 0.f, 0.f, 0.f};
     if (ctx->domain == 1) {
         const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
-        for (int v = 0; v < 2; ++v) {
-            ctx->zs_tw = v == 0 ? 32 : 16;
+        for (int v = 0; v < 4; ++v) {
+            ctx->zs_tw = (v & 1) ? 16 : 32;
+            ctx->zs_il = (v & 2) ? 2 : 1;
             auto one = [&]() {
                 if (mixed) {
                     StepFields<float> f = step_fields<float>(ctx);
@@ -2347,9 +2356,14 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
             CK(cudaEventElapsedTime(&tz[v], e0, e1));
             tz[v] /= reps;
         }
-        ctx->launches += 2 * (1 + reps);
+        ctx->launches += 4 * (1 + reps);
         CK(cudaGetLastError());
-        ctx->zs_tw = force >= 0 ? ((force & 256) ? 16 : 32) : (tz[1] < tz[0] ? 16 : 32);
+        int bz = 0;
+        for (int v = 1; v < 4; ++v)
+            if (tz[v] < tz[bz]) bz = v;
+        if (force >= 0) bz = ((force & 256) ? 1 : 0) | ((force & 1024) ? 2 : 0);
+        ctx->zs_tw = (bz & 1) ? 16 : 32;
+        ctx->zs_il = (bz & 2) ? 2 : 1;
     }
     // pressure stage up to DPH: chained x/z transforms or the fused plane
     // transforms (periodic channel, planes that fit one block).  It writes
@@ -2404,11 +2418,11 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     if (choice)
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
                   (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0) | (ctx->ysolve_kind == 4 ? 64 : 0) |
-                  (ctx->zs_tw == 16 ? 256 : 0) | (ctx->fz_pipe ? 512 : 0);
+                  (ctx->zs_tw == 16 ? 256 : 0) | (ctx->fz_pipe ? 512 : 0) | (ctx->zs_il == 2 ? 1024 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
         ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4];
-        ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2]; ms[13] = tk[3];
+        ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2]; ms[13] = tk[3]; ms[14] = tz[2]; ms[15] = tz[3];
     }
     return CHAPSIM_OK;
 }

@@ -441,19 +441,29 @@ template <typename R, int S> __host__ __device__ constexpr int zsweep_blocks() {
 // starts at N2I = 2 for v).  Blocks are persistent and take tiles in a stride loop with two
 // shared-memory buffers: the next tile's right-hand sides load (cp.async)
 // while the current tile's 32 lines are solved and stored.
-template <int S, typename R, int TW>
+// Shared-memory layout of a tile: IL = 1 keeps each line contiguous (segment
+// padded, LS = N + 33 elements per line); IL = 2 interleaves the lines in
+// pairs, element z of line il at (il / 2) * 2 LS + 2 seg_pos(z) + il % 2, so
+// that one cp.async of two consecutive x points (8 bytes in FP32, 16 in FP64)
+// fills both lines of a pair: half the copy instructions, for 2-way bank
+// conflicts in the solve's segment reads (the lane stride is 2 (S + 1)).
+template <int IL> __device__ __forceinline__ int zs_line(int il, int LS) { return IL == 1 ? il * LS : (il >> 1) * 2 * LS + (il & 1); }
+
+template <int S, typename R, int TW, int IL>
 __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Geo g, R* __restrict__ RHS, const R* __restrict__ fac) {
     pdl_wait();
     extern __shared__ __align__(16) unsigned char sm_raw[];
     R* smb = reinterpret_cast<R*>(sm_raw);
     static_assert(TW == 16 || TW == 32, "tile width");
+    static_assert(IL == 1 || IL == 2, "line interleave");
     const int N = g.N, M = g.M;
     const int LS = N + 33;
     const int TS = TW * LS;
     const int nx = g.L / TW;
     const int nwork = nx * (3 * M - 1);
     const long long ks = g.PI_;
-    constexpr int NIT = TW * S / 8;  // TW*N / SWEEP_NT
+    constexpr int NIT = TW * S / 8 / IL;  // TW*N / (SWEEP_NT*IL) copies per thread
+    constexpr int TP = TW / IL;           // copies per z row of a tile
     auto tile_base = [&](int t) -> R* {
         int comp, j;
         if (t < nx * M) { comp = 0; j = 1 + t / nx; }
@@ -467,7 +477,15 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
 #pragma unroll 4
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            cp_async_el(buf + (p % TW) * LS + seg_pos<S>(p / TW), Rz + (p % TW) + ks * (p / TW));
+            const int c = p % TP, z = p / TP;
+            if constexpr (IL == 1) {
+                cp_async_el(buf + c * LS + seg_pos<S>(z), Rz + c + ks * z);
+            } else {
+                R* dst = buf + c * 2 * LS + 2 * seg_pos<S>(z);
+                const R* src = Rz + 2 * c + ks * z;
+                if constexpr (sizeof(R) == 8) cp_async16(dst, src);
+                else cp_async8(reinterpret_cast<double*>(dst), reinterpret_cast<const double*>(src));
+            }
         }
     };
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -491,19 +509,28 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
 #pragma unroll
             for (int r = 0; r < NRZ; ++r)
 #pragma unroll
-                for (int q = 0; q < S; ++q) d[r][q] = cur[(il + r * (SWEEP_NT / 32)) * LS + lane * (S + 1) + q];
+                for (int q = 0; q < S; ++q)
+                    d[r][q] = cur[zs_line<IL>(il + r * (SWEEP_NT / 32), LS) + IL * (lane * (S + 1) + q)];
             warp_tdma_apply_n<S, true, NRZ>(d, fz, lane);
 #pragma unroll
             for (int r = 0; r < NRZ; ++r)
 #pragma unroll
-                for (int q = 0; q < S; ++q) cur[(il + r * (SWEEP_NT / 32)) * LS + lane * (S + 1) + q] = d[r][q];
+                for (int q = 0; q < S; ++q)
+                    cur[zs_line<IL>(il + r * (SWEEP_NT / 32), LS) + IL * (lane * (S + 1) + q)] = d[r][q];
         }
         __syncthreads();
         R* Rz = tile_base(t);
 #pragma unroll 4
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            Rz[(p % TW) + ks * (p / TW)] = cur[(p % TW) * LS + seg_pos<S>(p / TW)];
+            const int c = p % TP, z = p / TP;
+            if constexpr (IL == 1) {
+                Rz[c + ks * z] = cur[c * LS + seg_pos<S>(z)];
+            } else {
+                const R* src = cur + c * 2 * LS + 2 * seg_pos<S>(z);
+                R v[2] = {src[0], src[1]};
+                stvec<2>(Rz + 2 * c + ks * z, v);
+            }
         }
         __syncthreads();  // cur is the load target two tiles on
         b ^= 1;

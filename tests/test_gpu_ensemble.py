@@ -272,24 +272,27 @@ def test_scan_ysolve_matches_oracle(shape):
 @pytest.mark.parametrize("shape,precision", [((64, 32, 192), "fp64"), ((64, 32, 384), "fp64"),
                                              ((64, 64, 128), "mixed"), ((32, 32, 384), "mixed")])
 def test_zsweep_tile_widths_bitwise(shape, precision):
-    """The z sweep's tile shape (32 or 16 x lines per tile, bit 8) changes only
-    which block solves a line: the fields after 3 steps are bitwise equal,
-    and the tuner times both shapes."""
+    """The z sweep's tile shape (32 or 16 x lines per tile, bit 8) and layout
+    (lines contiguous or interleaved in pairs, bit 10) change only which block
+    solves a line and where it is staged: the fields after 3 steps are
+    bitwise equal, and the tuner times all four."""
     L, M, N = shape
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
     Q, PR = initial_field(s, 29, 0.1)
     out = []
-    for force in (0, 256):
+    for force in (0, 256, 1024, 1280):
         c = gpu.ChannelTG(s, precision=precision)
         choice, ms = c.autotune(force=force)
-        assert choice == force and ms["zsweep_tile32"] > 0 and ms["zsweep_tile16"] > 0
+        assert choice == force and min(ms[k] for k in ("zsweep_tile32", "zsweep_tile16", "zsweep_tile32_pairs",
+                                                       "zsweep_tile16_pairs")) > 0
         c.upload(Q, PR)
         c.set_dt(2e-3)
         c.SOLVERRK3_MOM_tg(0)
         c.advance(3, 2e-3, 1e-6, 0.5)
         out.append(c.download())
         c.close()
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
 
 
 @pytest.mark.parametrize("shape,precision", [((64, 32, 384), "fp64"), ((64, 64, 256), "fp64"), ((96, 32, 96), "fp64"),
