@@ -154,6 +154,7 @@ struct chapsim_ctx {
     int plane_kind = 0;           // 0: chained x/z transforms, 1: fused plane transforms k_div_fft2/k_fft2_inv (chapsim_autotune)
     int zs_tw = 32;               // lines per tile of the z sweep, 32 or 16 (chapsim_autotune)
     int zs_il = 1;                // z-sweep tile layout: 1 line-contiguous, 2 lines interleaved in pairs (chapsim_autotune)
+    int ys_il = 1;                // the same for the y sweep (chapsim_autotune)
     bool fz_pipe = false;         // persistent double-buffered z transforms (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
     int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
@@ -459,7 +460,8 @@ int configure_momentum(chapsim_ctx* ctx) {
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 16, 1>, smem_z<R>(g, 16))));
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 32, 2>, smem_z<R>(g, 32))));
     DISPATCH_S(g.N / 32, CK(set_smem(k_zsweep<S, R, 16, 2>, smem_z<R>(g, 16))));
-    DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R>, smem_y<R>(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R, 1>, smem_y<R>(g))));
+    DISPATCH_S(g.M / 32, CK(set_smem(k_ysweep<S, R, 2>, smem_y<R>(g))));
     DISPATCH_S(g.L / 32, CK(set_smem(k_xsweep<S, R>, smem_xs<R>(g))));
     CK(set_smem(k_rhs_point<R>, smem_rt<R>()));
     using C = SpecT<R>;
@@ -652,6 +654,20 @@ void launch_zsweep(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac) {
     }
 }
 
+// y sweep + update, the tile layout ctx->ys_il (chapsim_autotune bit 11)
+template <typename R>
+void launch_ysweep(chapsim_ctx* ctx, const StepFields<R>& f, const R* fac, int ns) {
+    const Geo& g = ctx->g;
+    dim3 gry(g.L / 32, g.N, 2);  // layer 0: u then v, layer 1: w
+    if (ctx->ys_il == 2) {
+        DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R, 2>, gry, SWEEP_NT, smem_y<R>(g), ctx->stream, g, f.Q, f.RHS,
+                                         ctx->st, fac, ns)));
+    } else {
+        DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R, 1>, gry, SWEEP_NT, smem_y<R>(g), ctx->stream, g, f.Q, f.RHS,
+                                         ctx->st, fac, ns)));
+    }
+}
+
 template <typename R>
 void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     const Geo& g = ctx->g;
@@ -667,8 +683,7 @@ void launch_substep_t(chapsim_ctx* ctx, int ns, bool factors) {
     prof_mark(ctx);
     launch_zsweep<R>(ctx, f, fac);
     prof_mark(ctx);
-    dim3 gry(g.L / 32, g.N, 2);  // layer 0: u then v, layer 1: w
-    DISPATCH_S(g.M / 32, (launch_pdl(ctx->pdl, k_ysweep<S, R>, gry, SWEEP_NT, smem_y<R>(g), s, g, f.Q, f.RHS, ctx->st, fac, ns)));
+    launch_ysweep<R>(ctx, f, fac, ns);
     prof_mark(ctx);
     launch_pressure<R>(ctx, f, ns);
     const long long tot = (long long)g.L * g.M * g.N / V16<R>::W;  // one thread per 16-byte group of an x line
@@ -2365,6 +2380,42 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         ctx->zs_tw = (bz & 1) ? 16 : 32;
         ctx->zs_il = (bz & 2) ? 2 : 1;
     }
+    // tile layout of the y sweep; it adds the increments to Q, which is state: Q is kept in a
+    // temporary copy and restored afterwards
+    float ty[2] = {0.f, 0.f};
+    if (ctx->domain == 1) {
+        const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
+        const size_t qb = (size_t)3 * g.FS * (mixed ? sizeof(float) : sizeof(double));
+        void* qsave = nullptr;
+        CK(cudaMalloc(&qsave, qb));
+        void* q0 = mixed ? (void*)ctx->Qf : (void*)ctx->Q;
+        CK(cudaMemcpyAsync(qsave, q0, qb, cudaMemcpyDeviceToDevice, s));
+        for (int v = 0; v < 2; ++v) {
+            ctx->ys_il = v + 1;
+            auto one = [&]() {
+                if (mixed) {
+                    StepFields<float> f = step_fields<float>(ctx);
+                    launch_ysweep<float>(ctx, f, f.fac + 5 * FAC_SET, 1);
+                } else {
+                    StepFields<double> f = step_fields<double>(ctx);
+                    launch_ysweep<double>(ctx, f, f.fac + 5 * FAC_SET, 1);
+                }
+            };
+            one();
+            CK(cudaEventRecord(e0, s));
+            for (int r = 0; r < reps; ++r) one();
+            CK(cudaEventRecord(e1, s));
+            CK(cudaEventSynchronize(e1));
+            CK(cudaEventElapsedTime(&ty[v], e0, e1));
+            ty[v] /= reps;
+        }
+        ctx->launches += 2 * (1 + reps);
+        CK(cudaMemcpyAsync(q0, qsave, qb, cudaMemcpyDeviceToDevice, s));
+        CK(cudaStreamSynchronize(s));
+        cudaFree(qsave);
+        CK(cudaGetLastError());
+        ctx->ys_il = force >= 0 ? ((force & 2048) ? 2 : 1) : (ty[1] < ty[0] ? 2 : 1);
+    }
     // pressure stage up to DPH: chained x/z transforms or the fused plane
     // transforms (periodic channel, planes that fit one block).  It writes
     // only scratch (RHSLLPHI, the spectrum, DPH), which every substep rewrites.
@@ -2418,11 +2469,13 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     if (choice)
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
                   (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0) | (ctx->ysolve_kind == 4 ? 64 : 0) |
-                  (ctx->zs_tw == 16 ? 256 : 0) | (ctx->fz_pipe ? 512 : 0) | (ctx->zs_il == 2 ? 1024 : 0);
+                  (ctx->zs_tw == 16 ? 256 : 0) | (ctx->fz_pipe ? 512 : 0) | (ctx->zs_il == 2 ? 1024 : 0) |
+                  (ctx->ys_il == 2 ? 2048 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
         ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4];
         ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2]; ms[13] = tk[3]; ms[14] = tz[2]; ms[15] = tz[3];
+        ms[16] = ty[0]; ms[17] = ty[1];
     }
     return CHAPSIM_OK;
 }

@@ -545,7 +545,9 @@ __global__ void __launch_bounds__(SWEEP_NT, (zsweep_blocks<R, S>())) k_zsweep(Ge
 // waves: at 128^3 the 512 three-component blocks filled 444 resident slots
 // and left a second wave of 68, where the two-plus-one split packs the same
 // work into about four component times instead of six.
-template <int S, typename R>
+// IL: the tile layout of k_zsweep (1 lines contiguous, 2 interleaved in pairs: one copy and one
+// vector access of Q per two x points).
+template <int S, typename R, int IL>
 __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : (sizeof(R) == 4 ? 4 : 3))) k_ysweep(Geo g, R* __restrict__ Q, const R* __restrict__ RHS,
                                                      const DevState* __restrict__ st, const R* __restrict__ fac,
                                                      int ns) {
@@ -564,8 +566,9 @@ __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : (sizeof(R) == 4 ? 4 : 
     else if (g.iflowdriven == 2) dpg64 = -0.5 * g.cf_given * (g.talp[ns] * dt / 1.0);
     const R dpg = (R)dpg64;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int NIT = 4 * S;  // 32*M / SWEEP_NT
-    const long long js = g.L;   // stride between y rows (interior and padded fields alike)
+    constexpr int NIT = 4 * S / IL;  // 32*M / (SWEEP_NT*IL) copies per thread
+    constexpr int TP = 32 / IL;      // copies per y row of the tile
+    const long long js = g.L;        // stride between y rows (interior and padded fields alike)
     const int comp_lo = blockIdx.z == 0 ? 0 : 2, comp_hi = blockIdx.z == 0 ? 2 : 3;
 #pragma unroll 1
     for (int comp = comp_lo; comp < comp_hi; ++comp) {
@@ -573,17 +576,25 @@ __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : (sizeof(R) == 4 ? 4 : 
 #pragma unroll 4
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            cp_async_el(sm + (p & 31) * LS + seg_pos<S>(p >> 5), Ry + (p & 31) + js * (p >> 5));
+            const int c = p % TP, jl = p / TP;
+            if constexpr (IL == 1) {
+                cp_async_el(sm + c * LS + seg_pos<S>(jl), Ry + c + js * jl);
+            } else {
+                R* dst = sm + c * 2 * LS + 2 * seg_pos<S>(jl);
+                const R* src = Ry + 2 * c + js * jl;
+                if constexpr (sizeof(R) == 8) cp_async16(dst, src);
+                else cp_async8(reinterpret_cast<double*>(dst), reinterpret_cast<const double*>(src));
+            }
         }
         cp_async_wait_all();
         __syncthreads();
         const R* fy = fac + (FSET_Y + comp) * FAC_SET;
 #pragma unroll 1
         for (int il = warp; il < 32; il += SWEEP_NT / 32) {
-            R* base = sm + il * LS;
+            R* base = sm + zs_line<IL>(il, LS);
             R d[S];
 #pragma unroll
-            for (int q = 0; q < S; ++q) d[q] = base[lane * (S + 1) + q];
+            for (int q = 0; q < S; ++q) d[q] = base[IL * (lane * (S + 1) + q)];
             if (comp == 0) {
 #pragma unroll
                 for (int q = 0; q < S; ++q) d[q] = d[q] - dpg;
@@ -592,24 +603,39 @@ __global__ void __launch_bounds__(SWEEP_NT, (S >= 6 ? 2 : (sizeof(R) == 4 ? 4 : 
             }
             warp_tdma_apply<S, false>(d, fy, lane);
 #pragma unroll
-            for (int q = 0; q < S; ++q) base[lane * (S + 1) + q] = d[q];
+            for (int q = 0; q < S; ++q) base[IL * (lane * (S + 1) + q)] = d[q];
         }
         __syncthreads();
         R* Qc = Q + comp * g.FS + pidx(g, i0, 1, k);
         const int n2i = comp == 1 ? 2 : 1;
-        R qv[NIT];
+        R qv[NIT][IL];
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            qv[it] = Qc[(p & 31) + js * (p >> 5)];
+            const int c = p % TP, jl = p / TP;
+            if constexpr (IL == 1) qv[it][0] = Qc[c + js * jl];
+            else ldvec<2>(Qc + 2 * c + js * jl, qv[it]);
         }
 #pragma unroll
         for (int it = 0; it < NIT; ++it) {
             const int p = threadIdx.x + SWEEP_NT * it;
-            const int jl = p >> 5, il = p & 31;
-            const R x = sm[il * LS + seg_pos<S>(jl)];
-            if (comp == 0 && jl == 0) sdu[il] = x;
-            if (jl + 1 >= n2i) Qc[il + js * jl] = x + qv[it];
+            const int c = p % TP, jl = p / TP;
+            if constexpr (IL == 1) {
+                const R x = sm[c * LS + seg_pos<S>(jl)];
+                if (comp == 0 && jl == 0) sdu[c] = x;
+                if (jl + 1 >= n2i) Qc[c + js * jl] = x + qv[it][0];
+            } else {
+                const R* sx = sm + c * 2 * LS + 2 * seg_pos<S>(jl);
+                const R x0 = sx[0], x1 = sx[1];
+                if (comp == 0 && jl == 0) {
+                    sdu[2 * c] = x0;
+                    sdu[2 * c + 1] = x1;
+                }
+                if (jl + 1 >= n2i) {
+                    const R o[2] = {x0 + qv[it][0], x1 + qv[it][1]};
+                    stvec<2>(Qc + 2 * c + js * jl, o);
+                }
+            }
         }
         __syncthreads();
     }

@@ -175,7 +175,7 @@ def c3_ref():
 
 # at M = 256 the sequential y-solve can also keep its forward intermediate in shared memory at one block per SM;
 # the z sweep in 16-line tiles (bit 8) and the double-buffered z transforms (bit 9) with the tuner's usual y-solves
-COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4, 6) for p in (0, 8)] + [256 | y for y in (1, 64)] + [512 | y for y in (1, 64)] + [1024 | y for y in (1, 64)]
+COMBOS_C3 = COMBOS + [32 | r | p for r in (0, 2, 4, 6) for p in (0, 8)] + [256 | y for y in (1, 64)] + [512 | y for y in (1, 64)] + [1024 | y for y in (1, 64)] + [2048 | y for y in (1, 64)]
 
 
 @pytest.mark.parametrize("force", COMBOS_C3 + [-1])

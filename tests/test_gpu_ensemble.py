@@ -273,18 +273,19 @@ def test_scan_ysolve_matches_oracle(shape):
                                              ((64, 64, 128), "mixed"), ((32, 32, 384), "mixed")])
 def test_zsweep_tile_widths_bitwise(shape, precision):
     """The z sweep's tile shape (32 or 16 x lines per tile, bit 8) and layout
-    (lines contiguous or interleaved in pairs, bit 10) change only which block
-    solves a line and where it is staged: the fields after 3 steps are
-    bitwise equal, and the tuner times all four."""
+    (lines contiguous or interleaved in pairs, bit 10), and the y sweep's
+    layout (bit 11) change only which block solves a line and where it is
+    staged: the fields after 3 steps are bitwise equal, and the tuner times
+    every form (restoring Q after the y-sweep trials)."""
     L, M, N = shape
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
     Q, PR = initial_field(s, 29, 0.1)
     out = []
-    for force in (0, 256, 1024, 1280):
+    for force in (0, 256, 1024, 1280, 2048, 3328):
         c = gpu.ChannelTG(s, precision=precision)
         choice, ms = c.autotune(force=force)
         assert choice == force and min(ms[k] for k in ("zsweep_tile32", "zsweep_tile16", "zsweep_tile32_pairs",
-                                                       "zsweep_tile16_pairs")) > 0
+                                                       "zsweep_tile16_pairs", "ysweep_lines", "ysweep_pairs")) > 0
         c.upload(Q, PR)
         c.set_dt(2e-3)
         c.SOLVERRK3_MOM_tg(0)
