@@ -598,11 +598,12 @@ class ChannelTG:
         forward intermediate in shared memory at one block per SM; bit 6: warp
         affine scans over the sequential factors; bit 8: z-sweep tiles of 16
         lines instead of 32; bit 9: double-buffered persistent z transforms; bit 10:
-        z-sweep tiles with the lines interleaved in pairs; bit 11: the same for the y sweep);
+        z-sweep tiles with the lines interleaved in pairs; bit 11: the same for the y sweep;
+        bit 12: z transforms that request the next wave's tiles into L2);
         returns
         (choice bits, {variant: ms})."""
         ch = ctypes.c_int32()
-        ms = (ctypes.c_float * 18)()
+        ms = (ctypes.c_float * 19)()
         self._check(self.lib.chapsim_autotune(self.h, int(force), ctypes.byref(ch), ms))
         self.choice = ch.value
         return ch.value, {"ysolve_warp_pcr": ms[0], "ysolve_sequential": ms[1], "rhs_fused": ms[2],
@@ -611,7 +612,7 @@ class ChannelTG:
                           "ysolve_scan": ms[9], "zsweep_tile32": ms[10], "zsweep_tile16": ms[11],
                           "pressure_chained_zpipe": ms[12], "rhs_fused_wide": ms[13],
                           "zsweep_tile32_pairs": ms[14], "zsweep_tile16_pairs": ms[15],
-                          "ysweep_lines": ms[16], "ysweep_pairs": ms[17]}
+                          "ysweep_lines": ms[16], "ysweep_pairs": ms[17], "pressure_chained_zprefetch": ms[18]}
 
 
 class Ensemble:

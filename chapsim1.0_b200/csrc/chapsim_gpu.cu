@@ -156,6 +156,7 @@ struct chapsim_ctx {
     int zs_il = 1;                // z-sweep tile layout: 1 line-contiguous, 2 lines interleaved in pairs (chapsim_autotune)
     int ys_il = 1;                // the same for the y sweep (chapsim_autotune)
     bool fz_pipe = false;         // persistent double-buffered z transforms (chapsim_autotune)
+    bool fz_prefetch = false;     // one-tile z transforms request the tile one wave ahead into L2 (chapsim_autotune)
     bool p2c = false;             // the fused plane transforms run as a thread-block cluster (k_div_fft2c/k_fft2c_inv)
     int rb_nw = 0;                // warps per block of k_rhs_xsweep_bulk (0: the stages do not fit)
     bool pdl = true;              // step kernels launched with programmatic dependent launch
@@ -589,7 +590,10 @@ void launch_fftz(chapsim_ctx* ctx, C* sp) {
         DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz_pipe<SIGN, FN1, FN2, C>, nb, FZ_NT, smem_fzp<C>(g), ctx->stream, g, sp)));
     } else {
         const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-        DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<SIGN, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), ctx->stream, g, sp)));
+        // prefetch distance: one wave of resident blocks (by the shared memory of a tile)
+        const int bps = std::max(1, std::min(sizeof(C) == 8 ? 4 : 2, (int)((227 * 1024) / smem_fz<C>(g))));
+        const int ahead = ctx->fz_prefetch ? bps * ctx->nsm : 0;
+        DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz<SIGN, FN1, FN2, C>, gfz, FZ_NT, smem_fz<C>(g), ctx->stream, g, sp, ahead)));
     }
 }
 
@@ -832,11 +836,11 @@ void launch_io_substep_t(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
     prof_mark(ctx);
     launch_ysolve<double2>(ctx);
     prof_mark(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
     prof_mark(ctx);
     DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, double2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     prof_mark(ctx);
@@ -1452,9 +1456,9 @@ int chapsim_fft99_pois3d(chapsim_ctx_t* ctx, const double* rhs, double* dph) {
     DISPATCH_FFT(g.L, (k_fftx_from_rhs<FN1, FN2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->RHSLL, ctx->SP)));
     const long long nq = (long long)g.LH * g.M;
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
-    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
     launch_ysolve<double2>(ctx);
-    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP)));
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
     DISPATCH_FFT(g.L, (k_fftx_inv<FN1, FN2, double2><<<grp, PX_NT, smem_px(g), s>>>(g, ctx->SP, ctx->DPH)));
     ctx->launches += 5;
     CK(cudaGetLastError());
@@ -2420,15 +2424,16 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
     // transforms (periodic channel, planes that fit one block).  It writes
     // only scratch (RHSLLPHI, the spectrum, DPH), which every substep rewrites.
     // (kind 0: chained transforms, 1: fused plane transforms, 2: chained with the persistent
-    // double-buffered z transforms)
-    float tp[3] = {0.f, 1e30f, 0.f};
+    // double-buffered z transforms, 3: chained with the z transforms' wave-ahead L2 requests)
+    float tp[4] = {0.f, 1e30f, 0.f, 0.f};
     if (ctx->domain == 1) {
         const bool mixed = ctx->prec == CHAPSIM_PREC_MIXED;
         bool p2 = (mixed ? plane_fft_ok<float2>(g) : plane_fft_ok<double2>(g)) || ctx->p2c;
-        for (int kind = 0; kind < 3; ++kind) {
+        for (int kind = 0; kind < 4; ++kind) {
             if (kind == 1 && !p2) continue;
             ctx->plane_kind = kind == 1 ? 1 : 0;
             ctx->fz_pipe = kind == 2;
+            ctx->fz_prefetch = kind == 3;
             auto one = [&]() {
                 if (mixed) launch_pressure<float>(ctx, step_fields<float>(ctx), 1);
                 else launch_pressure<double>(ctx, step_fields<double>(ctx), 1);
@@ -2452,12 +2457,14 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         if (force >= 0) {
             ctx->plane_kind = p2 ? (force >> 3) & 1 : 0;
             ctx->fz_pipe = (force & 512) != 0;
+            ctx->fz_prefetch = (force & 4096) != 0;
         } else {
             int best = 0;
-            for (int kind = 1; kind < 3; ++kind)
+            for (int kind = 1; kind < 4; ++kind)
                 if (tp[kind] < tp[best]) best = kind;
             ctx->plane_kind = best == 1 ? 1 : 0;
             ctx->fz_pipe = best == 2;
+            ctx->fz_prefetch = best == 3;
         }
     }
     if (ctx->step_exec) {
@@ -2470,12 +2477,12 @@ extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choi
         *choice = (ctx->ysolve_kind == 1 ? 1 : 0) | (ctx->k1_kind << 1) | (ctx->plane_kind << 3) |
                   (ctx->ysolve_kind == 2 ? 16 : 0) | (ctx->ysolve_kind == 3 ? 32 : 0) | (ctx->ysolve_kind == 4 ? 64 : 0) |
                   (ctx->zs_tw == 16 ? 256 : 0) | (ctx->fz_pipe ? 512 : 0) | (ctx->zs_il == 2 ? 1024 : 0) |
-                  (ctx->ys_il == 2 ? 2048 : 0);
+                  (ctx->ys_il == 2 ? 2048 : 0) | (ctx->fz_prefetch ? 4096 : 0);
     if (ms) {
         ms[0] = t[0]; ms[1] = t[1]; ms[2] = tk[0]; ms[3] = tk[1]; ms[4] = tk[2];
         ms[5] = tp[0]; ms[6] = tp[1]; ms[7] = t[2]; ms[8] = t[3]; ms[9] = t[4];
         ms[10] = tz[0]; ms[11] = tz[1]; ms[12] = tp[2]; ms[13] = tk[3]; ms[14] = tz[2]; ms[15] = tz[3];
-        ms[16] = ty[0]; ms[17] = ty[1];
+        ms[16] = ty[0]; ms[17] = ty[1]; ms[18] = tp[3];
     }
     return CHAPSIM_OK;
 }

@@ -42,8 +42,9 @@
 // at 4.
 #define RHS_MINB(R) (sizeof(R) == 8 ? 3 : 4)
 // The vector forms (PV adjacent points per lane) with 16-byte vectors hold two or four times the
-// loaded values of the one-point form: a two-block budget (up to 255 registers).
-#define RHS_MINB_P(R, PV) ((PV) * sizeof(R) > 8 ? 2 : RHS_MINB(R))
+// loaded values of the one-point form: a two-block budget in FP64 (234 registers), three in FP32
+// (168, no spills).
+#define RHS_MINB_P(R, PV) ((PV) * sizeof(R) > 8 ? (sizeof(R) == 4 ? 3 : 2) : RHS_MINB(R))
 // points per lane of the fused right-hand side: the default form (1 in FP64, 2 in FP32) and
 // the wide form, autotuned kind 3 (2 in FP64, 4 in FP32: 16-byte loads)
 template <typename R> __host__ __device__ constexpr int rhs_pv(bool wide) {

@@ -139,8 +139,10 @@ __global__ void __launch_bounds__(PX_NT, px_minb<SpecT<R>>()) k_div_fftx(Geo g, 
 
 // ---------------------------------------------------------------------------
 // complex z transform of FZ_TQ consecutive (kx, j) lines (index q = kx + LH*(j-1))
+// pf_ahead > 0: the block also requests into L2 the tile of block blockIdx.x + pf_ahead (about
+// one wave of resident blocks later), whose copies then find their rows there.
 template <int SIGN, int N1, int N2, typename C>
-__global__ void __launch_bounds__(FZ_NT, sizeof(C) == 8 ? 4 : 2) k_fftz(Geo g, C* __restrict__ SP) {
+__global__ void __launch_bounds__(FZ_NT, sizeof(C) == 8 ? 4 : 2) k_fftz(Geo g, C* __restrict__ SP, int pf_ahead) {
     pdl_wait();
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
@@ -150,6 +152,16 @@ __global__ void __launch_bounds__(FZ_NT, sizeof(C) == 8 ? 4 : 2) k_fftz(Geo g, C
     const long long Q = (long long)g.LH * g.M;
     const long long q0 = (long long)blockIdx.x * FZ_TQ;
     const int nq = (int)min((long long)FZ_TQ, Q - q0);
+    if (pf_ahead > 0) {
+        const long long qa = q0 + (long long)pf_ahead * FZ_TQ;
+        if (qa + FZ_TQ <= Q) {
+            constexpr int LPR = (FZ_TQ * (int)sizeof(C) + 127) / 128;  // 128-byte lines per kz row of a tile
+            for (int t = threadIdx.x; t < N * LPR; t += FZ_NT) {
+                const int kz = t / LPR, c = t - kz * LPR;
+                prefetch_l2(reinterpret_cast<const char*>(SP + qa + Q * kz) + 128 * c);
+            }
+        }
+    }
     for (int p = threadIdx.x; p < FZ_TQ * N; p += FZ_NT) {
         const int kz = p / FZ_TQ, ql = p - kz * FZ_TQ;
         if (ql < nq) {

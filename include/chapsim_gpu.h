@@ -393,7 +393,7 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
 /* ---- Autotuner and ensembles (no counterpart in the reference) ---- */
 
 /* Times the alternative kernels of the step on this context's grid and keeps
- * the fastest of each group (force = -1), or the ones forced (force = 0..4095):
+ * the fastest of each group (force = -1), or the ones forced (force = 0..8191):
  *   bits 0, 4, 5 and 6: Poisson y-solve, all 0 = warp Thomas/PCR hybrid,
  *          bit 0 = the reference's sequential Thomas recurrence, one thread
  *          per mode, bit 4 = two-way elimination, two threads per mode,
@@ -423,8 +423,11 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  *   bit 10: z-sweep tile layout (periodic channel only), 0 = each x line
  *          contiguous in shared memory, 1 = lines interleaved in pairs (one
  *          copy instruction per two points);
- *   bit 11: the same for the y sweep (Q is restored after its trials).
- * choice receives the kept setting in the same bit form; ms[18] (may be NULL)
+ *   bit 11: the same for the y sweep (Q is restored after its trials);
+ *   bit 12: with the chained transforms, each z-transform block also
+ *          requests into L2 the tile of the block one wave later (timed as a
+ *          fourth pressure-stage form).
+ * choice receives the kept setting in the same bit form; ms[19] (may be NULL)
  * the mean durations of y-solve (hybrid, sequential), right-hand sides
  * (fused, split, bulk-staged), pressure stage up to DPH (chained, fused;
  * 1e30 where a variant does not apply), the two-way y-solve, the
@@ -432,8 +435,9 @@ int chapsim_dump_write(chapsim_ctx_t* ctx, const char* path_prefix, int32_t iter
  * the scan y-solve, the z sweep with 32- and with 16-line tiles (0 where it
  * does not apply), the pressure stage with the double-buffered z
  * transforms, the wide right-hand side (1e30 where it does not apply), and
- * the z sweep with pair-interleaved 32- and 16-line tiles, and the y sweep
- * with line-contiguous and pair-interleaved tiles.
+ * the z sweep with pair-interleaved 32- and 16-line tiles, the y sweep with
+ * line-contiguous and pair-interleaved tiles, and the pressure stage with
+ * the z transforms' wave-ahead requests.
  * CONVH0 is restored after the trial launches. */
 int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms);
 

@@ -299,20 +299,22 @@ def test_zsweep_tile_widths_bitwise(shape, precision):
 @pytest.mark.parametrize("shape,precision", [((64, 32, 384), "fp64"), ((64, 64, 256), "fp64"), ((96, 32, 96), "fp64"),
                                              ((64, 32, 384), "mixed"), ((64, 64, 128), "mixed")])
 def test_pipelined_z_transforms_bitwise(shape, precision):
-    """The persistent double-buffered z transforms (bit 9) compute each line as
-    the one-tile kernel does: fields bitwise equal after 3 steps."""
+    """The persistent double-buffered z transforms (bit 9) and the z transforms
+    with wave-ahead L2 requests (bit 12) compute each line as the one-tile
+    kernel does: fields bitwise equal after 3 steps."""
     L, M, N = shape
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
     Q, PR = initial_field(s, 31, 0.1)
     out = []
-    for force in (1, 513):
+    for force in (1, 513, 4097):
         c = gpu.ChannelTG(s, precision=precision)
         choice, ms = c.autotune(force=force)
-        assert choice == force and ms["pressure_chained_zpipe"] > 0
+        assert choice == force and ms["pressure_chained_zpipe"] > 0 and ms["pressure_chained_zprefetch"] > 0
         c.upload(Q, PR)
         c.set_dt(2e-3)
         c.SOLVERRK3_MOM_tg(0)
         c.advance(3, 2e-3, 1e-6, 0.5)
         out.append(c.download())
         c.close()
-    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0]) and np.array_equal(out[0][1], o[1])
