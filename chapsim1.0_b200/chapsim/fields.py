@@ -106,3 +106,16 @@ def read_dfile(path):
         raise ValueError(f"{path}: header dims {L}x{M}x{N} do not match the payload")
     f = np.frombuffer(b[40:], dtype="<f8").reshape(N, M, L).copy()
     return f, {"L": L, "M": M, "N": N, "ITERG": it, "time": t, "REN": ren, "DT": dt}
+
+
+def xinout_fields_from_tg(Q_tg, L_io: int):
+    """Start fields of an inflow/outflow main domain (iDomain = 3) of L_io cells from a
+    periodic TG velocity field (3, N, M+2, L_tg): the TG field repeated along x, with the
+    ghost columns 0 and L_io + 1 (NCL1S:NCL1E) filled the same way.  Returns G of shape
+    (3, N, M+2, L_io+2) (rho u with unit density) and a zero pressure (N, M+2, L_io+2).
+    """
+    Q_tg = np.asarray(Q_tg, np.float64)
+    _, N, M2, LT = Q_tg.shape
+    idx = [(i - 1) % LT for i in range(L_io + 2)]
+    G = np.ascontiguousarray(Q_tg[:, :, :, idx])
+    return G, np.zeros((N, M2, L_io + 2))

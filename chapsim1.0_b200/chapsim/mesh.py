@@ -13,6 +13,8 @@ that a Python caller can drive the library without the Fortran host:
   LAMPOISLPROF        src/LAMPOISLPROF.f90:17-60   Vini (Poiseuille profile)
   CONS_RKCOEF         src/CONS_RKCOEF.f90:25-51    TGAM, TROH, TALP
   FFT99_ROOT          src/possion3d_FFT99.f90:140-202  AK1, AK3
+  FFTPACK_ROOT        src/possion3d_fishpack.f90:48-137 XRT, YRT of the inflow/outflow
+                      main domain (xinout_setup)
 
 Arrays are returned 1-based as in Fortran (index 0 unused) unless noted.
 """
@@ -183,4 +185,24 @@ def channel_setup(L, M, N, HX, HZ, STR2, REN, iFlowDriven=1, Cf_Given=8.18e-3) -
     s.AMPH, s.ACPH, s.APPH = AMPH, ACPH, APPH
     s.AMVR, s.ACVR, s.APVR = AMVR, ACVR, APVR
     s.Vini, s.TGAM, s.TROH, s.TALP, s.AK1, s.AK3 = Vini, TGAM, TROH, TALP, AK1, AK3
+    return s
+
+
+def xinout_setup(L, M, N, HX, HZ, STR2, REN) -> ChannelSetup:
+    """Set-up of the main domain of a TG + main-domain run (iDomain = 3): the channel
+    set-up with no bulk forcing (RHS_MOM_EXPLICIT_io applies it only to the x-periodic
+    flow, src/RHS_MOM_EXPLICIT_io.f90:229) and the FISHPACK roots of BCX_io = (2, 1),
+    LPEROD = 4, and the periodic z direction (FFTPACK_ROOT, src/possion3d_fishpack.f90:
+    48-137), stored as the positive AK1/AK3 the Poisson y-solve subtracts from ACPH:
+
+      AK1[m]  = -XRT(m+1) = 4 DXQI sin^2((m + 1/2) pi / (2 L)),  m = 0..L-1
+      AK3[kz] = -YRT      = 4 DZQI sin^2(pi min(kz, N-kz) / N)   (the RFFTF pair of
+                            wavenumber min(kz, N-kz) shares one root)
+    """
+    s = channel_setup(L, M, N, HX, HZ, STR2, REN, iFlowDriven=0, Cf_Given=0.0)
+    PI = 2.0 * math.asin(1.0)
+    DX = PI / (2.0 * float(L))
+    s.AK1 = np.array([4.0 * s.DXQI * (math.sin((float(I) - 0.5) * DX) ** 2) for I in range(1, L + 1)])
+    DY = PI / (2.0 * float(N))
+    s.AK3 = np.array([4.0 * s.DZQI * (math.sin(float(2 * min(k, N - k)) * DY) ** 2) for k in range(N)])
     return s

@@ -29,6 +29,8 @@
 
 typedef struct {
     int L, M, N, NND2;
+    int xo, LS;  /* x offset and x stride: 0, L (x-periodic); 1, L+2 (inflow/outflow main domain, ghost
+                    columns i = 0 and L+1, NCL1S:NCL1E of src/READINI.f90:597-605) */
     double HX, HZ, STR2, REN, CVISC;
     int iFlowDriven;
     double Cf_Given;
@@ -73,10 +75,14 @@ typedef struct {
     double F_A;
     /* iWeightedPre = 1: PR0_io(:,:,:,1:2) (src/FLOWSTART.f90:83-85), NULL when off */
     double *PR0A, *PR0B;
+    /* inflow/outflow main domain (iDomain = 3): BC_CONV0 (src/MEMALLOCT.f90:172), the
+       FISHPACK x roots -XRT (LPEROD = 4), U_OUTLET and CHK_Mass_CONSV0_SCALING of the last step */
+    double *BCCONV0, *AKX;
+    double U_OUTLET, MASS_SCALING;
 } orc_t;
 
-#define FOFF(o, i, j, k) ((size_t)((i) - 1) + (size_t)(o)->L * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
-#define FSZ(o) ((size_t)(o)->L * (size_t)((o)->M + 2) * (size_t)(o)->N)
+#define FOFF(o, i, j, k) ((size_t)((i) - 1 + (o)->xo) + (size_t)(o)->LS * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
+#define FSZ(o) ((size_t)(o)->LS * (size_t)((o)->M + 2) * (size_t)(o)->N)
 #define QV(o, i, j, k, c) ((o)->Q[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
 #define F3(a, o, i, j, k) ((a)[FOFF(o, i, j, k)])
 #define H0V(o, i, j, k, c) ((o)->CONVH0[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
@@ -85,8 +91,10 @@ typedef struct {
 #define DSV(o, i, j, k, c) ((o)->DSTG[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
 #define MSV(o, i, j, k, c) ((o)->MUSTG[FOFF(o, i, j, k) + (size_t)((c) - 1) * FSZ(o)])
 
-static inline int IPV(const orc_t* o, int i) { return i == o->L ? 1 : i + 1; }
-static inline int IMV(const orc_t* o, int i) { return i == 1 ? o->L : i - 1; }
+/* IPV_io / IMV_io (src/INDEXSET.f90:26-52): cyclic in x-periodic domains, the ghost columns */
+/* 0 and L+1 in the inflow/outflow main domain                                              */
+static inline int IPV(const orc_t* o, int i) { return (i == o->L && !o->xo) ? 1 : i + 1; }
+static inline int IMV(const orc_t* o, int i) { return (i == 1 && !o->xo) ? o->L : i - 1; }
 static inline int KPV(const orc_t* o, int k) { return k == o->N ? 1 : k + 1; }
 static inline int KMV(const orc_t* o, int k) { return k == 1 ? o->N : k - 1; }
 
@@ -288,11 +296,12 @@ static void setup(orc_t* o) {
     }
 }
 
-orc_t* orc_create(int L, int M, int N, double HX, double HZ, double STR2, double REN, int iFlowDriven,
-                  double Cf_Given, double DT0, double DTMIN, double CFLGV) {
+static orc_t* create_impl(int L, int M, int N, double HX, double HZ, double STR2, double REN, int iFlowDriven,
+                          double Cf_Given, double DT0, double DTMIN, double CFLGV, int xo) {
     if (L < 4 || M < 4 || N < 4 || (L % 2) || (N % 2)) return NULL;
     orc_t* o = (orc_t*)calloc(1, sizeof(orc_t));
     o->L = L; o->M = M; o->N = N; o->NND2 = M + 1;
+    o->xo = xo; o->LS = L + 2 * xo;
     o->HX = HX; o->HZ = HZ; o->STR2 = STR2; o->REN = REN;
     o->iFlowDriven = iFlowDriven; o->Cf_Given = Cf_Given;
     o->DT0 = DT0; o->DT = DT0; o->DTMIN = DTMIN; o->CFLGV = CFLGV;
@@ -307,10 +316,33 @@ orc_t* orc_create(int L, int M, int N, double HX, double HZ, double STR2, double
     size_t fs = FSZ(o);
     o->Q = dalloc(3 * fs); o->PR = dalloc(fs); o->CONVH0 = dalloc(3 * fs);
     o->QTMP = dalloc(fs); o->DPH = dalloc(fs); o->RHSLLPHI = dalloc(fs); o->RHS = dalloc(fs);
-    size_t LH = (size_t)L / 2 + 1;
+    size_t LH = xo ? (size_t)L : (size_t)L / 2 + 1;  /* the cosine transform keeps L x modes */
     o->SRe = dalloc(LH * (size_t)M * (size_t)N); o->SIm = dalloc(LH * (size_t)M * (size_t)N);
     setup(o);
+    if (xo) {
+        /* FFTPACK_ROOT with LP = 5 (src/possion3d_fishpack.f90:65-111): XRT(I) =                  */
+        /* -4 DXQI sin^2((I - 1/2) pi / (2 L)); AKX holds -XRT (the AK1 of the cosine modes)      */
+        double PI = 2.0 * asin(1.0), DX = PI / (2.0 * (double)L);
+        o->AKX = dalloc((size_t)L + 1);
+        for (int I = 1; I <= L; ++I) {
+            double sn = sin(((double)I - 0.5) * DX);
+            o->AKX[I] = 4.0 * o->DXQI * (sn * sn);
+        }
+        o->BCCONV0 = dalloc(3 * (size_t)M * (size_t)N);
+    }
     return o;
+}
+
+orc_t* orc_create(int L, int M, int N, double HX, double HZ, double STR2, double REN, int iFlowDriven,
+                  double Cf_Given, double DT0, double DTMIN, double CFLGV) {
+    return create_impl(L, M, N, HX, HZ, STR2, REN, iFlowDriven, Cf_Given, DT0, DTMIN, CFLGV, 0);
+}
+
+/* The main domain of iDomain = 3 (TgFlowFlg and IoFlowFlg): x runs over NCL1S:NCL1E = 0:L+1 with */
+/* the inlet ghost column 0 fed by a periodic TG domain and the convective outlet column L+1.     */
+orc_t* orc_create_xinout(int L, int M, int N, double HX, double HZ, double STR2, double REN, double DT0,
+                         double DTMIN, double CFLGV) {
+    return create_impl(L, M, N, HX, HZ, STR2, REN, 0, 0.0, DT0, DTMIN, CFLGV, 1);
 }
 
 void orc_destroy(orc_t* o) {
@@ -325,6 +357,7 @@ void orc_destroy(orc_t* o) {
     free(o->G); free(o->EXPLT0); free(o->RHO); free(o->MU0); free(o->MU); free(o->DSTG); free(o->MUSTG);
     free(o->DIVU); free(o->DRHODT); free(o->DEN); free(o->DRHOI);
     free(o->DH); free(o->ENTH); free(o->TEMP); free(o->KAPPA); free(o->HCP); free(o->RHSE); free(o->RHSE0); free(o->G0);
+    free(o->BCCONV0); free(o->AKX);
     free(o);
 }
 
@@ -697,7 +730,7 @@ static void momfa(orc_t* o, int NS, int IDR) {
 static void bc_wall_q(orc_t* o) {
     int L = o->L, M = o->M, N = o->N;
     for (int K = 1; K <= N; ++K)
-        for (int I = 1; I <= L; ++I) {
+        for (int I = 1 - o->xo; I <= L + o->xo; ++I) {
             QV(o, I, M + 1, K, 1) = 0.0; QV(o, I, M + 1, K, 3) = 0.0; QV(o, I, M + 1, K, 2) = 0.0;
             QV(o, I, 0, K, 1) = 0.0; QV(o, I, 0, K, 3) = 0.0; QV(o, I, 1, K, 2) = 0.0; QV(o, I, 0, K, 2) = 0.0;
         }
@@ -705,7 +738,7 @@ static void bc_wall_q(orc_t* o) {
 static void bc_wall_scalar(orc_t* o, double* F) {
     int L = o->L, M = o->M, N = o->N;
     for (int K = 1; K <= N; ++K)
-        for (int I = 1; I <= L; ++I) {
+        for (int I = 1 - o->xo; I <= L + o->xo; ++I) {
             F3(F, o, I, M + 1, K) = F3(F, o, I, M, K);
             F3(F, o, I, 0, K) = F3(F, o, I, 1, K);
         }
@@ -982,6 +1015,9 @@ void orc_io_enable(orc_t* o) {
     o->DSTG = dalloc(3 * fs); o->MUSTG = dalloc(3 * fs); o->DIVU = dalloc(fs); o->DRHODT = dalloc(fs);
     o->DEN = dalloc(fs);
     o->DRHOI = dalloc(3 * fs);
+    /* D_STG and MU_STG start at 1 (src/MEMALLOCT.f90:200-201); DENSITY_Staggered and MU_Staggered */
+    /* fill the interior, the ghost columns of the inflow/outflow domain keep it                  */
+    for (size_t e = 0; e < 3 * fs; ++e) { o->DSTG[e] = 1.0; o->MUSTG[e] = 1.0; }
     o->io = 1;
 }
 
@@ -1021,7 +1057,7 @@ static void io_staggered_props(orc_t* o) {
 static void io_bc_wall_g(orc_t* o) {
     int L = o->L, M = o->M, N = o->N;
     for (int K = 1; K <= N; ++K)
-        for (int I = 1; I <= L; ++I) {
+        for (int I = 1 - o->xo; I <= L + o->xo; ++I) {
             GV(o, I, 0, K, 1) = 0.0; GV(o, I, 0, K, 3) = 0.0; GV(o, I, 1, K, 2) = 0.0; GV(o, I, 0, K, 2) = 0.0;
             GV(o, I, M + 1, K, 1) = 0.0; GV(o, I, M + 1, K, 3) = 0.0; GV(o, I, M + 1, K, 2) = 0.0;
         }
@@ -1080,7 +1116,7 @@ static void io_convection_x(orc_t* o) {
         double COE2 = o->DYFI[JJ] * 0.5 * 1.0, COE32 = COE3 * 1.0;
         for (int KC = 1; KC <= N; ++KC) {
             int KM = KMV(o, KC), KP = KPV(o, KC);
-            for (int IC = 1; IC <= L; ++IC) {
+            for (int IC = 1 + o->xo; IC <= L; ++IC) {  /* NXI = 2 with TgFlowFlg (:92) */
                 int IP = IPV(o, IC), IM = IMV(o, IC);
                 double H11F = (GV(o, IP, JC, KC, 1) + GV(o, IC, JC, KC, 1)) * (QV(o, IP, JC, KC, 1) + QV(o, IC, JC, KC, 1));
                 double H11B = (GV(o, IC, JC, KC, 1) + GV(o, IM, JC, KC, 1)) * (QV(o, IC, JC, KC, 1) + QV(o, IM, JC, KC, 1));
@@ -1324,6 +1360,7 @@ static inline double io_pgm(const orc_t* o, size_t a, size_t b, double COE2) {
 static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
     int L = o->L, M = o->M, N = o->N;
     int NYI = (IDR == 2) ? 2 : 1;
+    int NXI = (o->xo && IDR == 1) ? 2 : 1;  /* TgFlowFlg: the inlet face u(1) is a boundary value (:35) */
     double* EX = IDR == 1 ? o->QTMP : IDR == 2 ? o->DPH : o->RHSLLPHI;
     double DT = o->DT;
     if (!o->ivis) {
@@ -1331,7 +1368,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
 #pragma omp parallel for schedule(static)
         for (int KC = 1; KC <= N; ++KC)
             for (int JC = NYI; JC <= M; ++JC)
-                for (int IC = 1; IC <= L; ++IC) {
+                for (int IC = NXI; IC <= L; ++IC) {
                     double RHSC = F3(EX, o, IC, JC, KC);
                     double RHSL = E0V(o, IC, JC, KC, IDR);
                     F3(o->RHS, o, IC, JC, KC) = (o->TGAM[NS] * RHSC + o->TROH[NS] * RHSL) * DT;
@@ -1343,7 +1380,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
 #pragma omp parallel for schedule(static)
         for (int KC = 1; KC <= N; ++KC)
             for (int JC = NYI; JC <= M; ++JC)
-                for (int IC = 1; IC <= L; ++IC) {
+                for (int IC = NXI; IC <= L; ++IC) {
                     double RHSC = F3(EX, o, IC, JC, KC);
                     double RHSL = E0V(o, IC, JC, KC, IDR);
                     F3(o->RHS, o, IC, JC, KC) = (o->TGAM[NS] * RHSC + o->TROH[NS] * RHSL) * DT +
@@ -1356,7 +1393,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
 #pragma omp parallel for schedule(static)
         for (int KC = 1; KC <= N; ++KC)
             for (int JC = 1; JC <= M; ++JC)
-                for (int IC = 1; IC <= L; ++IC) {
+                for (int IC = NXI; IC <= L; ++IC) {
                     double PGM = io_pgm(o, FOFF(o, IC, JC, KC), FOFF(o, IMV(o, IC), JC, KC), COE2);
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
                 }
@@ -1365,7 +1402,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
         for (int JC = 2; JC <= M; ++JC) {
             double COE2 = o->TALP[NS] * DT * o->DYCI[JC] / 1.0;
             for (int KC = 1; KC <= N; ++KC)
-                for (int IC = 1; IC <= L; ++IC) {
+                for (int IC = NXI; IC <= L; ++IC) {
                     double PGM = io_pgm(o, FOFF(o, IC, JC, KC), FOFF(o, IC, JC - 1, KC), COE2);
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
                 }
@@ -1376,7 +1413,7 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
         for (int KC = 1; KC <= N; ++KC) {
             int KM = KMV(o, KC);
             for (int JC = 1; JC <= M; ++JC)
-                for (int IC = 1; IC <= L; ++IC) {
+                for (int IC = NXI; IC <= L; ++IC) {
                     double PGM = io_pgm(o, FOFF(o, IC, JC, KC), FOFF(o, IC, JC, KM), COE2);
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - PGM;
                 }
@@ -1391,16 +1428,16 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
         for (int KC = 1; KC <= N; ++KC)
             for (int JC = JS; JC <= M; ++JC) {
                 double C2 = IDR == 1 ? COE2 : COE2 / 1.0;
-                for (int IC = 1; IC <= L; ++IC)
+                for (int IC = NXI; IC <= L; ++IC)
                     F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) + DSV(o, IC, JC, KC, IDR) * C2;
             }
     }
-    if (IDR == 1) {
+    if (IDR == 1 && !o->xo) {  /* bulk forcing of the streamwise-periodic flow only (:229) */
         double DPGRNS = 0.0;
         if (o->iFlowDriven == 1) {
             double INTGRHSY = 0.0;  /* loop order JC, IC, KC */
             for (int JC = 1; JC <= M; ++JC)
-                for (int IC = 1; IC <= L; ++IC)
+                for (int IC = NXI; IC <= L; ++IC)
                     for (int KC = 1; KC <= N; ++KC) INTGRHSY = INTGRHSY + F3(o->RHS, o, IC, JC, KC) / o->DYFI[JC] / 1.0;
             DPGRNS = INTGRHSY / o->VOLM;
         } else if (o->iFlowDriven == 2) {
@@ -1409,13 +1446,13 @@ static void io_rhs_mom_explicit(orc_t* o, int NS, int IDR) {
 #pragma omp parallel for schedule(static)
         for (int KC = 1; KC <= N; ++KC)
             for (int JC = 1; JC <= M; ++JC)
-                for (int IC = 1; IC <= L; ++IC) F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - DPGRNS;
+                for (int IC = NXI; IC <= L; ++IC) F3(o->RHS, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC) - DPGRNS;
     }
     if (o->ivis) return;  /* the save-back (:267-301) is the explicit scheme's */
 #pragma omp parallel for schedule(static)
     for (int KC = 1; KC <= N; ++KC)
         for (int JC = NYI; JC <= M; ++JC)
-            for (int IC = 1; IC <= L; ++IC) F3(EX, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC);
+            for (int IC = NXI; IC <= L; ++IC) F3(EX, o, IC, JC, KC) = F3(o->RHS, o, IC, JC, KC);
 }
 
 /* MASSFLUX_CALC_io (src/MASSFLUX_CALC_IO.f90:15-93): G += explicit RHS */
@@ -1425,7 +1462,7 @@ static void io_massflux_calc(orc_t* o) {
     for (int KC = 1; KC <= N; ++KC)
         for (int JC = 1; JC <= M; ++JC)
             for (int IC = 1; IC <= L; ++IC) {
-                GV(o, IC, JC, KC, 1) = GV(o, IC, JC, KC, 1) + F3(o->QTMP, o, IC, JC, KC);
+                if (IC > o->xo) GV(o, IC, JC, KC, 1) = GV(o, IC, JC, KC, 1) + F3(o->QTMP, o, IC, JC, KC);  /* NXI */
                 GV(o, IC, JC, KC, 3) = GV(o, IC, JC, KC, 3) + F3(o->RHSLLPHI, o, IC, JC, KC);
                 if (JC >= 2) GV(o, IC, JC, KC, 2) = GV(o, IC, JC, KC, 2) + F3(o->DPH, o, IC, JC, KC);
             }
@@ -1476,10 +1513,11 @@ static void io_prcalc_massflux_update(orc_t* o, int NS) {
     }
     bc_wall_scalar(o, o->PR);
     double COE1 = o->DT * o->TALP[NS] * o->DXI;
+    /* u faces NXI..NXE: 1..L, or 2..L+1 with TgFlowFlg (the outlet face included, :121-127) */
 #pragma omp parallel for schedule(static)
     for (int KC = 1; KC <= N; ++KC)
         for (int JC = 1; JC <= M; ++JC)
-            for (int IC = 1; IC <= L; ++IC) {
+            for (int IC = 1 + o->xo; IC <= L + o->xo; ++IC) {
                 double DFX11 = F3(o->DPH, o, IC, JC, KC) - F3(o->DPH, o, IMV(o, IC), JC, KC);
                 GV(o, IC, JC, KC, 1) = GV(o, IC, JC, KC, 1) - DFX11 * COE1;
             }
@@ -2254,6 +2292,296 @@ int orc_io_run_steps(orc_t* o, int nsteps, double* cfl_dt) {
         }
     }
     return 0;
+}
+
+/* ====================================================================== */
+/* Main domain with inflow and outflow (iDomain = 3: TgFlowFlg and        */
+/* IoFlowFlg), flow only (iThermoDynamics = 0 or before timeThermoStart),  */
+/* explicit viscous terms.  x runs over 0..L+1: the inlet ghost column 0   */
+/* and the inlet face u(1) come from the periodic TG domain each substep  */
+/* (BC_TINLET_FLOW), the outlet column L+1 takes a convective update      */
+/* (BC_COUTLET_MOM_RK3), and the pressure Poisson equation is FISHPACK's  */
+/* with BCX_io = (2, 1).                                                    */
+/* ====================================================================== */
+
+/* BC_TINLET_FLOW (src/BC_INLET.f90:12-61), rows J = 0..M+1 */
+static void xio_inlet(orc_t* o, const orc_t* tg) {
+    int M = o->M, N = o->N, LT = tg->L;
+    for (int J = 0; J <= M + 1; ++J)
+        for (int K = 1; K <= N; ++K) {
+            double D0 = F3(o->RHO, o, 0, J, K);
+            QV(o, 0, J, K, 1) = QV(tg, LT, J, K, 1);
+            QV(o, 1, J, K, 1) = QV(tg, 1, J, K, 1);
+            GV(o, 0, J, K, 1) = QV(o, 0, J, K, 1) * D0;
+            GV(o, 1, J, K, 1) = QV(o, 1, J, K, 1) * D0;
+            QV(o, 0, J, K, 2) = QV(tg, LT, J, K, 2);
+            GV(o, 0, J, K, 2) = QV(o, 0, J, K, 2) * D0;
+            QV(o, 0, J, K, 3) = QV(tg, LT, J, K, 3);
+            GV(o, 0, J, K, 3) = QV(o, 0, J, K, 3) * D0;
+            F3(o->PR, o, 0, J, K) = F3(tg->PR, tg, LT, J, K);
+        }
+    for (int J = 0; J <= M + 1; ++J)
+        for (int K = 1; K <= N; ++K) F3(o->DPH, o, 0, J, K) = 0.0;
+}
+
+#define BCV(o, j, k, c) ((o)->BCCONV0[(size_t)((j) - 1) + (size_t)(o)->M * ((size_t)((k) - 1) + (size_t)(o)->N * (size_t)((c) - 1))])
+
+/* BC_COUTLET_MOM_RK3(NS) (src/BC_COUTLET_MOM_RK3.f90:16-112) with U_OUTLET of CONVCTION_OUTLET_U  */
+/* (:115-192, method two: the mean of the largest and smallest outlet u) and the outflow scaling */
+/* of CHK_MassConsv_io (src/processing/CHK_conservation.f90:11-79, method 1).                   */
+static void xio_outlet(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+    double UxMax = -1.0E20, UxMin = 1.0E20;
+    for (int K = 1; K <= N; ++K)
+        for (int J = 1; J <= M; ++J) {
+            double UCC = (QV(o, L, J, K, 1) + QV(o, L + 1, J, K, 1)) * 0.5;
+            if (UCC > UxMax) UxMax = UCC;
+            if (UCC < UxMin) UxMin = UCC;
+        }
+    o->U_OUTLET = 0.5 * (UxMax + UxMin);
+    double COE1 = o->DXI * o->U_OUTLET;
+    for (int IDR = 1; IDR <= 3; ++IDR) {
+        int N2I = IDR == 2 ? 2 : 1;
+        for (int K = 1; K <= N; ++K)
+            for (int J = N2I; J <= M; ++J) {
+                double BC_CONV = -(GV(o, L + 1, J, K, IDR) - GV(o, L, J, K, IDR)) * COE1;
+                double BC_RHS = o->TGAM[NS] * BC_CONV + o->TROH[NS] * BCV(o, J, K, IDR);
+                BCV(o, J, K, IDR) = BC_CONV;
+                GV(o, L + 1, J, K, IDR) = GV(o, L + 1, J, K, IDR) + o->DT * BC_RHS;
+                double RHO = (F3(o->RHO, o, L, J, K) + F3(o->RHO, o, L + 1, J, K)) * 0.5;
+                QV(o, L + 1, J, K, IDR) = GV(o, L + 1, J, K, IDR) / RHO;
+            }
+    }
+    /* CHK_MassConsv_io: inlet and outlet (NCL1E = L+1) fluxes, and the mass rate of the interior */
+    double FluxIntg_INL = 0.0, FluxIntg_OUT = 0.0, MASS_RATE_INTG = 0.0;
+    for (int JC = 1; JC <= M; ++JC) {
+        double COE2 = 1.0 / o->DYFI[JC] / 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            FluxIntg_INL = FluxIntg_INL + GV(o, 1, JC, KC, 1) * COE2;
+            FluxIntg_OUT = FluxIntg_OUT + GV(o, L + 1, JC, KC, 1) * COE2;
+        }
+    }
+    FluxIntg_INL = FluxIntg_INL / o->DZI;
+    FluxIntg_OUT = FluxIntg_OUT / o->DZI;
+    for (int JC = 1; JC <= M; ++JC) {
+        double COE2 = 1.0 / o->DYFI[JC] / 1.0;
+        for (int KC = 1; KC <= N; ++KC)
+            for (int IC = 1; IC <= L; ++IC) MASS_RATE_INTG = F3(o->DRHODT, o, IC, JC, KC) * COE2 + MASS_RATE_INTG;
+    }
+    MASS_RATE_INTG = MASS_RATE_INTG / o->DZI / o->DXI;
+    o->MASS_SCALING = (FluxIntg_INL - MASS_RATE_INTG) / FluxIntg_OUT;
+    for (int J = 1; J <= M; ++J)
+        for (int K = 1; K <= N; ++K) {
+            GV(o, L + 1, J, K, 1) = GV(o, L + 1, J, K, 1) * (o->MASS_SCALING - 1.0) + GV(o, L + 1, J, K, 1);
+            double RHO = (F3(o->RHO, o, L, J, K) + F3(o->RHO, o, L + 1, J, K)) * 0.5;
+            QV(o, L + 1, J, K, 1) = GV(o, L + 1, J, K, 1) / RHO;
+        }
+    io_bc_wall_g(o);
+    bc_wall_q(o);
+}
+
+/* The x and z eigenvalues of the FISHPACK solve as positive numbers: AKX(I) = -XRT(I) (LP = 5),   */
+/* and -YRT of the periodic z direction (MP = 1): 4 DZQI sin^2(pi kz / N) for the complex mode kz */
+/* (the RFFTF half-complex pair of wavenumber min(kz, N-kz) shares one root, :118-124).            */
+static double xio_akz(const orc_t* o, int kz) {
+    int kk = kz <= o->N - kz ? kz : o->N - kz;
+    double PI = 2.0 * asin(1.0), DY = PI / (2.0 * (double)o->N);
+    double sn = sin((double)(2 * kk) * DY);
+    return 4.0 * o->DZQI * (sn * sn);
+}
+double orc_xio_akz(const orc_t* o, int kz) { return xio_akz(o, kz); }
+double orc_xio_akx(const orc_t* o, int I) { return o->AKX ? o->AKX[I] : 0.0; }
+
+/* FISHPACK_POIS3D_SIMPLE (src/possion3d_fishpack.f90:344-460) with LPEROD = 4 (BCX_io = (2, 1):  */
+/* x(0) = x(2), x(L+1) = 0) and MPEROD = 0 (periodic z).  The transforms are written as the sums  */
+/* FFTPACK defines them by:                                                                       */
+/*   COSQF  X(m) = x(1) + sum_{p=2..L} 2 x(p) cos((2m-1)(p-1) pi / (2L))                          */
+/*   COSQB  x(p) = sum_{m=1..L} 4 X(m) cos((2m-1)(p-1) pi / (2L))                                 */
+/* and the z pair RFFTF/RFFTB as the complex DFT of the real line (its half-complex half).  TRID0 */
+/* (:309-340) solves each (m, kz) line with BB = ACPH + XRT(m)/RCCI2 + YRT(kz); no x mode is       */
+/* singular (XRT < 0), so its zero-pivot branch is not taken.  The result is scaled by            */
+/* 1/(SCALX*SCALY) = 1/(4 L N) (1/N applied after the forward z transform).                        */
+static void poisson_xinout(orc_t* o, const double* src, double* dst) {
+    int L = o->L, M = o->M, N = o->N;
+    double UN3M = 1.0 / (double)N;
+    double PI = 2.0 * asin(1.0);
+    int Q4 = 4 * L;
+    double* cq = dalloc((size_t)Q4);
+    for (int q = 0; q < Q4; ++q) cq[q] = cos((double)q * PI / (double)(2 * L));
+    cplx* wfz = fft_table(N, -1);
+    cplx* wbz = fft_table(N, +1);
+    double* SRe = o->SRe;
+    double* SIm = o->SIm;
+#define SXM(I, J, K) ((size_t)((I) - 1) + (size_t)L * ((size_t)((J) - 1) + (size_t)M * (size_t)((K) - 1)))
+#pragma omp parallel
+    {
+        int nmax = L > N ? L : N;
+        cplx* a = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+        cplx* b = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+#pragma omp for schedule(static)
+        for (int J = 1; J <= M; ++J) {
+            for (int K = 1; K <= N; ++K)
+                for (int m = 1; m <= L; ++m) {
+                    double X = F3(src, o, 1, J, K);
+                    for (int p = 2; p <= L; ++p) X = X + 2.0 * F3(src, o, p, J, K) * cq[((2 * m - 1) * (p - 1)) % Q4];
+                    SRe[SXM(m, J, K)] = X;
+                }
+            for (int m = 1; m <= L; ++m) {
+                for (int K = 1; K <= N; ++K) { a[K - 1].re = SRe[SXM(m, J, K)]; a[K - 1].im = 0.0; }
+                fft_rec(N, a, 1, b, -1, wfz, 1);
+                for (int K = 1; K <= N; ++K) {
+                    SRe[SXM(m, J, K)] = b[K - 1].re * UN3M;
+                    SIm[SXM(m, J, K)] = b[K - 1].im * UN3M;
+                }
+            }
+        }
+        free(a); free(b);
+    }
+#pragma omp parallel
+    {
+        double* D = dalloc((size_t)M);
+        double* T = dalloc((size_t)M);
+        double* BB = dalloc((size_t)M);
+#pragma omp for schedule(static)
+        for (int K = 1; K <= N; ++K) {
+            double YRT = -xio_akz(o, K - 1);
+            for (int m = 1; m <= L; ++m) {
+                double XRT = -o->AKX[m];
+                for (int J = 1; J <= M; ++J) BB[J - 1] = o->ACPH[J] + XRT / 1.0 + YRT;
+                for (int part = 0; part < 2; ++part) {
+                    double* S = part ? SIm : SRe;
+                    for (int J = 1; J <= M; ++J) T[J - 1] = S[SXM(m, J, K)];
+                    /* TRID0 */
+                    int NR = M, MM1 = NR - 1;
+                    double Z = 1.0 / BB[0];
+                    D[0] = o->APPH[1] * Z;
+                    T[0] = T[0] * Z;
+                    for (int I = 2; I <= MM1; ++I) {
+                        Z = 1.0 / (BB[I - 1] - o->AMPH[I] * D[I - 2]);
+                        D[I - 1] = o->APPH[I] * Z;
+                        T[I - 1] = (T[I - 1] - o->AMPH[I] * T[I - 2]) * Z;
+                    }
+                    Z = BB[NR - 1] - o->AMPH[NR] * D[MM1 - 1];
+                    if (fabs(Z) > 1.0E-14) T[NR - 1] = (T[NR - 1] - o->AMPH[NR] * T[MM1 - 1]) / Z;
+                    else T[NR - 1] = 0.0;
+                    for (int IP = 1; IP <= MM1; ++IP) {
+                        int I = NR - IP;
+                        T[I - 1] = T[I - 1] - D[I - 1] * T[I];
+                    }
+                    for (int J = 1; J <= M; ++J) S[SXM(m, J, K)] = T[J - 1];
+                }
+            }
+        }
+        free(D); free(T); free(BB);
+    }
+#pragma omp parallel
+    {
+        int nmax = L > N ? L : N;
+        cplx* a = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+        cplx* b = (cplx*)malloc(sizeof(cplx) * (size_t)nmax);
+#pragma omp for schedule(static)
+        for (int J = 1; J <= M; ++J) {
+            for (int m = 1; m <= L; ++m) {
+                for (int K = 1; K <= N; ++K) { a[K - 1].re = SRe[SXM(m, J, K)]; a[K - 1].im = SIm[SXM(m, J, K)]; }
+                fft_rec(N, a, 1, b, +1, wbz, 1);
+                for (int K = 1; K <= N; ++K) SRe[SXM(m, J, K)] = b[K - 1].re;
+            }
+            for (int K = 1; K <= N; ++K)
+                for (int p = 1; p <= L; ++p) {
+                    double x = 0.0;
+                    for (int m = 1; m <= L; ++m) x = x + 4.0 * SRe[SXM(m, J, K)] * cq[((2 * m - 1) * (p - 1)) % Q4];
+                    F3(dst, o, p, J, K) = x / (double)Q4;
+                }
+        }
+        free(a); free(b);
+    }
+#undef SXM
+    free(cq); free(wfz); free(wbz);
+}
+
+/* SOLVERRK3_MOM_io(NS) with TgFlowFlg (src/SOLVERRK3_MOM_IO.f90:11-120), iVisScheme = 0 */
+int orc_xio_substep(orc_t* o, const orc_t* tg, int NS) {
+    if (!o->io || !o->xo || tg->xo || tg->M != o->M || tg->N != o->N || NS < 1 || NS > 3 || o->ivis || o->thermal)
+        return -1;
+    io_velocity_calc(o);
+    xio_inlet(o, tg);
+    xio_outlet(o, NS);
+    io_convection_x(o);
+    io_convection_y(o);
+    io_convection_z(o);
+    io_divg_u(o);
+    io_viscous_x(o);
+    io_rhs_mom_explicit(o, NS, 1);
+    io_viscous_y(o);
+    io_rhs_mom_explicit(o, NS, 2);
+    io_viscous_z(o);
+    io_rhs_mom_explicit(o, NS, 3);
+    io_massflux_calc(o);
+    io_bc_wall_g(o);
+    io_divg(o, NS);
+    memset(o->DPH, 0, FSZ(o) * sizeof(double));
+    poisson_xinout(o, o->RHSLLPHI, o->DPH);
+    bc_wall_scalar(o, o->DPH);
+    io_prcalc_massflux_update(o, NS);
+    io_velocity_calc(o);
+    return 0;
+}
+
+/* The SOLVE loop of a TG + main-domain run (src/SOLVE.f90:75-134): CFL_tg and CFL_io, DT from  */
+/* CFLMM = max of the two (the dt rule of BCAST_COMM_STEP, :154-211), then per NS the TG substep */
+/* and the main-domain substep.  cfl_dt[s] = CFLMM * DT of step s.                               */
+int orc_xio_run_steps(orc_t* o, orc_t* tg, int nsteps, double* cfl_dt) {
+    for (int s = 0; s < nsteps; ++s) {
+        double ctg = orc_cfl(tg), cio = orc_io_cfl(o);
+        double c = fmax(ctg, cio);
+        double dt = fmin(fmin(o->DT0, 5.0 * o->DT), o->CFLGV / c);
+        dt = fmax(dt, o->DTMIN);
+        o->DT = dt;
+        tg->DT = dt;
+        if (cfl_dt) cfl_dt[s] = c * dt;
+        if ((dt / o->DT0) < 0.01) return 1;
+        for (int NS = 1; NS <= 3; ++NS) {
+            orc_substep(tg, NS);
+            if (orc_xio_substep(o, tg, NS)) return 2;
+        }
+    }
+    return 0;
+}
+
+/* DIVGCK_io with TgFlowFlg (src/DIVGCK.f90:60-100): MAXDIVGV_io(1:3) over the cells 2..L-1, */
+/* 0..1 and L of DIVGCK_Comm_io (|div G + DrhoDtP|).                                         */
+static double xio_divmax(const orc_t* o, int I0, int I1) {
+    int M = o->M, N = o->N;
+    double DIVMAX = 0.0;
+    for (int JC = 1; JC <= M; ++JC) {
+        double COE2 = o->DYFI[JC] * 1.0;
+        for (int KC = 1; KC <= N; ++KC) {
+            int KP = KPV(o, KC);
+            for (int IC = I0; IC <= I1; ++IC) {
+                int IP = IC + 1;
+                double DIVX = (GV(o, IP, JC, KC, 1) - GV(o, IC, JC, KC, 1)) * o->DXI;
+                double DIVY = (GV(o, IC, JC + 1, KC, 2) - GV(o, IC, JC, KC, 2)) * COE2;
+                double DIVZ = (GV(o, IC, JC, KP, 3) - GV(o, IC, JC, KC, 3)) * o->DZI;
+                double DQCAP = DIVX + DIVY + DIVZ + F3(o->DRHODT, o, IC, JC, KC);
+                DIVMAX = fmax(fabs(DQCAP), DIVMAX);
+            }
+        }
+    }
+    return DIVMAX;
+}
+void orc_xio_divgck(const orc_t* o, double* out) {
+    out[0] = xio_divmax(o, 2, o->L - 1);
+    out[1] = xio_divmax(o, 0, 1);
+    out[2] = xio_divmax(o, o->L, o->L);
+}
+void orc_xio_outlet_state(const orc_t* o, double* out) {
+    out[0] = o->U_OUTLET;
+    out[1] = o->MASS_SCALING;
+}
+/* Poisson solve alone (tests): rhs and dph are (0:L+1, 0:M+1, N) fields, interior rows used. */
+void orc_xio_poisson(orc_t* o, const double* rhs, double* dph) {
+    memset(dph, 0, FSZ(o) * sizeof(double));
+    poisson_xinout(o, rhs, dph);
 }
 
 /* Monitor quantities of PP_MONITOR_Xperiodic_io (src/processing/

@@ -111,6 +111,19 @@ def lib():
         L.orc_table_extrema.argtypes = [ctypes.c_void_p, _ip]
         L.orc_prop_update.argtypes = [ctypes.c_void_p, ctypes.c_long, _dp, _dp, ctypes.POINTER(ctypes.c_long)]
         L.orc_prop_update.restype = ctypes.c_long
+        L.orc_create_xinout.restype = ctypes.c_void_p
+        L.orc_create_xinout.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 7
+        L.orc_xio_substep.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+        L.orc_xio_substep.restype = ctypes.c_int
+        L.orc_xio_run_steps.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_xio_run_steps.restype = ctypes.c_int
+        L.orc_xio_divgck.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_xio_outlet_state.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_xio_poisson.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_xio_akx.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_xio_akx.restype = ctypes.c_double
+        L.orc_xio_akz.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_xio_akz.restype = ctypes.c_double
         _lib = L
     return _lib
 
@@ -316,6 +329,59 @@ class Oracle:
         out = np.zeros(self.field_shape())
         self._lib.orc_poisson(self._h, _p(rhs), _p(out))
         return out
+
+
+class OracleXinout(Oracle):
+    """Main domain of a TG + main-domain run (iDomain = 3) with inflow from a periodic TG
+    domain and a convective outlet; flow only, explicit viscous terms.
+
+    Fields carry the x ghost columns: shape (N, M+2, L+2) = Fortran (0:L+1, 0:M+1, N), i.e.
+    ``NCL1S:NCL1E``.  The TG domain is an :class:`Oracle` with the same M, N and y mesh.
+    """
+
+    def __init__(self, L, M, N, HX, HZ, STR2, REN, DT0=1e-3, DTMIN=1e-6, CFLGV=0.5, threads=1):
+        self.L, self.M, self.N = L, M, N
+        self._lib = lib()
+        self._h = self._lib.orc_create_xinout(L, M, N, HX, HZ, STR2, REN, DT0, DTMIN, CFLGV)
+        if not self._h:
+            raise ValueError("invalid oracle grid")
+        self._lib.orc_set_threads(self._h, int(threads))
+
+    def field_shape(self):
+        return (self.N, self.M + 2, self.L + 2)
+
+    def xio_substep(self, tg: Oracle, ns):
+        if self._lib.orc_xio_substep(self._h, tg._h, int(ns)) != 0:
+            raise ValueError("bad substep, TG domain mismatch or fields not set")
+
+    def xio_run_steps(self, tg: Oracle, n):
+        out = np.zeros(max(n, 1))
+        rc = self._lib.orc_xio_run_steps(self._h, tg._h, int(n), _p(out))
+        return rc, out[:n]
+
+    def xio_divgck(self):
+        out = np.zeros(3)
+        self._lib.orc_xio_divgck(self._h, _p(out))
+        return out
+
+    def xio_outlet_state(self):
+        """(U_OUTLET, CHK_Mass_CONSV0_SCALING) of the last substep."""
+        out = np.zeros(2)
+        self._lib.orc_xio_outlet_state(self._h, _p(out))
+        return tuple(out.tolist())
+
+    def xio_poisson(self, rhs):
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        assert rhs.shape == self.field_shape()
+        out = np.zeros(self.field_shape())
+        self._lib.orc_xio_poisson(self._h, _p(rhs), _p(out))
+        return out
+
+    def akx(self):
+        return np.array([self._lib.orc_xio_akx(self._h, i) for i in range(1, self.L + 1)])
+
+    def akz(self):
+        return np.array([self._lib.orc_xio_akz(self._h, k) for k in range(self.N)])
 
 
 def fft_complex(x: np.ndarray, sign: int) -> np.ndarray:
