@@ -40,7 +40,8 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_batch_get_stream", "chapsim_batch_destroy", "chapsim_pp_mean_zx_tg", "chapsim_pp_mean_t_tg",
             "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
             "chapsim_pp_mean_zx_io", "chapsim_download_pp_means_io",
-            "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write"]
+            "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write",
+            "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
 PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
@@ -196,6 +197,11 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_upload_io_fields.argtypes = [vp, _dp, _dp, _dp, _dp, _dp]
     L.chapsim_download_io_fields.argtypes = [vp, _dp, _dp, _dp]
     L.chapsim_rk_substep_io.argtypes = [vp, ctypes.c_int32]
+    L.chapsim_xinout_attach.argtypes = [vp, vp]
+    L.chapsim_advance_xinout.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp,
+                                         _dp]
+    L.chapsim_divgck_xinout.argtypes = [vp, _dp]
+    L.chapsim_xinout_outlet_state.argtypes = [vp, _dp]
     L.chapsim_cfl_io.argtypes = [vp, _dp]
     L.chapsim_set_buoyancy.argtypes = [vp, ctypes.c_int32, ctypes.c_double]
     L.chapsim_upload_weighted_pressure.argtypes = [vp, _dp, _dp]
@@ -759,3 +765,54 @@ class ChannelIO(ChannelTG):
         e = np.zeros(6)
         self._check(self.lib.chapsim_mlp_judge(self.h, _ptr(e)))
         return dict(zip(self.MLP_FIELDS, e.tolist()))
+
+
+class ChannelXinout(ChannelIO):
+    """Main domain of a TG + main-domain run (CHAPSim iDomain = 3): inflow from a periodic
+    :class:`ChannelTG` context (BC_TINLET_FLOW), a convective outlet (BC_COUTLET_MOM_RK3) and
+    FISHPACK's x-cosine Poisson solve; flow only, explicit viscous terms, FP64.
+
+    ``setup`` comes from :func:`chapsim.mesh.xinout_setup`.  Fields carry the x ghost
+    columns: ``G`` is (3, N, M+2, L+2) = Fortran ``G_io(0:L+1, 0:M+1, N, 3)``, ``PR``, ``RHO``,
+    ``MU0``, ``MU`` are (N, M+2, L+2).  ``attach(tg)`` names the TG context that feeds the
+    inlet; ``advance`` runs both domains' steps with their common DT.
+    """
+
+    IDOMAIN = 3
+
+    def __init__(self, setup, tg: ChannelTG = None, device: int = 0, **kw):
+        super().__init__(setup, device=device, ivisscheme=VIS_EXPLICIT, **kw)
+        self.tg = None
+        if tg is not None:
+            self.attach(tg)
+
+    def field_shape(self):
+        return (self.N, self.M + 2, self.L + 2)
+
+    def attach(self, tg: ChannelTG):
+        self._check(self.lib.chapsim_xinout_attach(self.h, tg.h))
+        self.tg = tg
+
+    def kernel_slots(self):
+        sub = ["k_xio_inlet", "k_xio_outlet", "k_io_divu", "k_io_rhs", "k_io_massflux", "k_xio_div_dctx", "k_fftz_fwd",
+               "k_xio_ysolve", "k_fftz_inv", "k_xio_dctx_inv", "k_io_correct"]
+        return ["k_io_cfl", "k_dt", "k_dt_pair"] + sub * 3
+
+    def advance(self, nsteps, DT0, DTMIN, CFLGV):
+        """nsteps steps of the TG + main-domain loop; returns (DT, CFLMM) of the last step."""
+        dt, cfl = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.chapsim_advance_xinout(self.h, int(nsteps), DT0, DTMIN, CFLGV, ctypes.byref(dt),
+                                                    ctypes.byref(cfl)))
+        return dt.value, cfl.value
+
+    def DIVGCK_io(self):
+        """MAXDIVGV_io(1:3): max |div G| over the cells 2..L-1, 0..1 and L."""
+        out = np.zeros(3)
+        self._check(self.lib.chapsim_divgck_xinout(self.h, _ptr(out)))
+        return out
+
+    def outlet_state(self):
+        """(U_OUTLET, CHK_Mass_CONSV0_SCALING) of the last substep."""
+        out = np.zeros(2)
+        self._check(self.lib.chapsim_xinout_outlet_state(self.h, _ptr(out)))
+        return float(out[0]), float(out[1])

@@ -17,6 +17,7 @@
 #include "tdma.cuh"
 #include "io.cuh"
 #include "io_cn.cuh"
+#include "io_xinout.cuh"
 #include "stats.cuh"
 #include "stats_io.cuh"
 #include "rhs_bulk.cuh"
@@ -177,7 +178,8 @@ struct chapsim_ctx {
     double* ybuf = nullptr;       // device copies of y-arrays and wavenumbers
     double2* tw = nullptr;
     float2* twf = nullptr;        // FP32 copies of tw
-    int domain = 1;               // 1: periodic TG channel, 2: main domain (IO)
+    int domain = 1;               // 1: periodic TG channel, 2: main domain (IO), 3: main domain with inflow from
+                                  // a periodic TG context and a convective outlet (iDomain = 3)
     int ivis = 0;                 // main domain: 0 explicit viscous terms, 1 Crank-Nicolson (iVisScheme)
     // statistics of the periodic channel (stats.cuh), allocated by the first call
     double *pp_inst = nullptr, *pp_avg = nullptr, *pp_part = nullptr, *pp_mon = nullptr;
@@ -222,6 +224,14 @@ struct chapsim_ctx {
     bool dump_pending = false;
     cudaStream_t dump_stream = nullptr;
     cudaEvent_t dump_snap = nullptr, dump_done = nullptr;
+    // inflow/outflow main domain (domain 3)
+    chapsim_ctx* tg_in = nullptr;  // the periodic TG context whose fields feed the inlet
+    double* xio_cq = nullptr;      // cos(q pi / (2 L)), q < 4 L
+    double* xio_bc0 = nullptr;     // BC_CONV0 (3 M N)
+    double* xio_yd = nullptr;      // forward factors of the Poisson y-solve (L N M)
+    double* xio_state = nullptr;   // U_OUTLET, CHK_Mass_CONSV0_SCALING of the last substep
+    double* xio_part = nullptr;    // block maxima of the three divergence ranges
+    cudaEvent_t xev[2] = {nullptr, nullptr};
     std::string err;
 };
 
@@ -853,6 +863,75 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
     else launch_io_substep_t<double>(ctx, ns);
 }
 
+// ------------------------- inflow/outflow main domain ------------------------
+size_t smem_xd(const Geo& g) { return (size_t)(4 + XD_R) * g.LI * sizeof(double); }
+
+// SOLVERRK3_MOM_io(NS) with TgFlowFlg (src/SOLVERRK3_MOM_IO.f90:11-120), explicit viscous
+// terms: BC_TINLET_FLOW from the attached TG context (its substep NS must have run; the
+// caller orders the two streams), BC_COUTLET_MOM_RK3, the momentum step of io.cuh (which
+// leaves the inlet face u(1) alone and adds no bulk forcing), DIVG_io and FISHPACK's
+// cosine/z/y solve, PRCALC_io + MASSFLUX_UPDATE_io + VELOCITY_CALC_io.
+void launch_xio_substep(chapsim_ctx* ctx, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    IoFields f = io_fields(ctx);
+    const chapsim_ctx* tg = ctx->tg_in;
+    const int gin = (int)std::min<long long>(4LL * ctx->nsm, ((long long)(g.M + 2) * g.N + XIO_NT - 1) / XIO_NT);
+    k_xio_inlet<<<gin, XIO_NT, 0, s>>>(g, f, tg->Q, tg->PR, tg->g.L, tg->g.FS);
+    prof_mark(ctx);
+    k_xio_outlet<<<1, XIO_OUT_NT, 0, s>>>(g, f, ctx->xio_bc0, ctx->xio_state, ctx->st, ns);
+    prof_mark(ctx);
+    k_io_divu<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
+    prof_mark(ctx);
+    k_io_rhs<false, double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->part_rhs, ctx->st, ns);
+    prof_mark(ctx);
+    k_io_massflux<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
+    prof_mark(ctx);
+    const int nrb = (int)(((long long)g.M * g.N + XD_R - 1) / XD_R);
+    k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cq, ctx->SP, ctx->st, ns, 1.0);
+    prof_mark(ctx);
+    const long long nq = (long long)g.LH * g.M;  // LH = LI x modes
+    const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
+    DISPATCH_FFT(g.N, (k_fftz<-1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
+    prof_mark(ctx);
+    k_xio_ysolve<<<(int)(((long long)g.LI * g.N + XIO_NT - 1) / XIO_NT), XIO_NT, 0, s>>>(g, ctx->SP, ctx->xio_yd);
+    prof_mark(ctx);
+    DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
+    prof_mark(ctx);
+    k_xio_dctx_inv<<<nrb, XIO_NT, smem_xd(g), s>>>(g, ctx->SP, ctx->xio_cq, ctx->DPH);
+    prof_mark(ctx);
+    k_io_correct<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, nullptr);
+    prof_mark(ctx);
+    ctx->launches += 11;
+}
+
+// CFL_tg and CFL_io of one TG + main-domain step, then CFLMM = max of the two and the dt rule
+// (src/SOLVE.f90:79-94), DT in both states.  The TG stream waits for the DT.
+void launch_xio_step_start(chapsim_ctx* io) {
+    chapsim_ctx* tg = io->tg_in;
+    launch_cfl_dt(tg, 0);
+    cudaEventRecord(io->xev[0], tg->stream);
+    k_io_cfl<double><<<io->npart_red, IO_NT, 0, io->stream>>>(io->g, io_fields(io), io->part_red, io->st);
+    k_dt<<<1, DG_NT, 0, io->stream>>>(io->part_red, io->npart_red, io->st, 0);
+    cudaStreamWaitEvent(io->stream, io->xev[0], 0);
+    k_dt_pair<<<1, 32, 0, io->stream>>>(tg->st, io->st);
+    cudaEventRecord(io->xev[1], io->stream);
+    cudaStreamWaitEvent(tg->stream, io->xev[1], 0);
+    io->launches += 3;
+}
+
+// one TG substep, then the main-domain substep that reads the TG fields; the next TG launch
+// waits for that read
+void launch_xio_pair_substep(chapsim_ctx* io, int ns) {
+    chapsim_ctx* tg = io->tg_in;
+    launch_substep(tg, ns, true);
+    cudaEventRecord(io->xev[0], tg->stream);
+    cudaStreamWaitEvent(io->stream, io->xev[0], 0);
+    launch_xio_substep(io, ns);
+    cudaEventRecord(io->xev[1], io->stream);
+    cudaStreamWaitEvent(tg->stream, io->xev[1], 0);
+}
+
 int check_device_error(chapsim_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
@@ -904,14 +983,20 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     if (!grid || !cf || !out) return fail(nullptr, CHAPSIM_ERR_BADARG, "null argument");
     *out = nullptr;
     const int L = grid->ncl1, M = grid->ncl2, N = grid->ncl3;
-    if (grid->icase != 1 || (grid->idomain != 1 && grid->idomain != 2))
+    if (grid->icase != 1 || grid->idomain < 1 || grid->idomain > 3)
         return fail(nullptr, CHAPSIM_ERR_BADARG,
-                    "only the plane channel (iCase=1) with a periodic TG (iDomain=1) or main (iDomain=2) domain is supported");
-    if (L < 32 || M < 32 || N < 32 || L % 32 || M % 32 || N % 32 || !valid_S(L / 32) || !valid_S(M / 32) ||
-        !valid_S(N / 32))
+                    "only the plane channel (iCase=1) with a periodic TG (iDomain=1), x-periodic main (2) or inflow/outflow "
+                    "main (3) domain is supported");
+    const bool xio = grid->idomain == 3;
+    // the inflow/outflow main domain has no x FFT and no x sweep: any even NCL1_io from 4 to 1024
+    if (xio ? (L < 4 || L > 1024 || L % 2) : (L < 32 || L % 32 || !valid_S(L / 32)))
+        return fail(nullptr, CHAPSIM_ERR_BADARG,
+                    xio ? "NCL1_io of the inflow/outflow domain must be even, 4..1024"
+                        : "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");
+    if (M < 32 || N < 32 || M % 32 || N % 32 || !valid_S(M / 32) || !valid_S(N / 32))
         return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");
     int n1_, n2_;
-    if (!fft4s_split(L, n1_, n2_) || !fft4s_split(N, n1_, n2_))
+    if ((!xio && !fft4s_split(L, n1_, n2_)) || !fft4s_split(N, n1_, n2_))
         return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1 and NCL3 must be one of 32, 64, 96, 128, 192, 256, 384");
     if (!cf->dyfi || !cf->dyci || !cf->ycl2nd_wff || !cf->ycl2nd_wfb || !cf->amph || !cf->acph || !cf->apph ||
         !cf->amvr || !cf->acvr || !cf->apvr || !cf->ak1 || !cf->ak3)
@@ -924,9 +1009,12 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     const int ivis = opts ? opts->ivisscheme : CHAPSIM_VIS_EXPLICIT;
     if (ivis != CHAPSIM_VIS_EXPLICIT && ivis != CHAPSIM_VIS_IMPLICIT)
         return fail(nullptr, CHAPSIM_ERR_BADARG, "ivisscheme must be CHAPSIM_VIS_EXPLICIT or CHAPSIM_VIS_IMPLICIT");
-    if (ivis == CHAPSIM_VIS_IMPLICIT && grid->idomain != 2)
+    if (ivis == CHAPSIM_VIS_IMPLICIT && grid->idomain == 1)
         return fail(nullptr, CHAPSIM_ERR_BADARG,
                     "ivisscheme selects the main-domain (iDomain = 2) scheme; the TG domain is always Crank-Nicolson");
+    if (xio && (ivis != CHAPSIM_VIS_EXPLICIT || prec != CHAPSIM_PREC_FP64))
+        return fail(nullptr, CHAPSIM_ERR_BADARG,
+                    "the inflow/outflow main domain (iDomain = 3) runs the explicit viscous scheme in FP64");
     if (ivis == CHAPSIM_VIS_IMPLICIT && !(cf->amvr1 > 0.0 && cf->apvrn > 0.0 && std::isfinite(cf->amvr1) &&
                                           std::isfinite(cf->apvrn)))
         return fail(nullptr, CHAPSIM_ERR_BADARG, "the Crank-Nicolson main domain needs AMVR1 and APVRN (TDMA_COEF)");
@@ -949,13 +1037,16 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaSetDevice(ctx->device));
     INIT_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
     Geo& g = ctx->g;
-    g.L = L; g.M = M; g.N = N; g.LH = L / 2 + 1;
-    g.P = (long long)L * (M + 2);
+    const int LS = xio ? L + 2 : L;  // row stride: the ghost columns 0 and L+1 with inflow/outflow
+    g.L = LS; g.M = M; g.N = N; g.LH = xio ? L : L / 2 + 1;
+    g.LI = L; g.xo = xio ? 1 : 0;
+    g.P = (long long)LS * (M + 2);
     g.FS = g.P * N;
     g.PI_ = (long long)L * M;
     g.FI = g.PI_ * N;
     g.dxi = cf->dxi; g.dzi = cf->dzi; g.dxqi = cf->dxqi; g.dzqi = cf->dzqi;
     g.cvisc = cf->cvisc; g.volm = cf->volm; g.cf_given = cf->cf_given; g.iflowdriven = cf->iflowdriven;
+    if (xio) g.iflowdriven = 0;  // no bulk forcing with inflow (src/RHS_MOM_EXPLICIT_io.f90:229)
     g.fix_v_wall_row = opts ? opts->fix_v_wall_row : 0;
     for (int s = 0; s < 4; ++s) { g.tgam[s] = cf->tgam[s]; g.troh[s] = cf->troh[s]; g.talp[s] = cf->talp[s]; }
     g.area_inlet = 0.0;  // COORDJR's loop order (RCCI1 = 1)
@@ -1021,6 +1112,7 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     INIT_CK(cudaMalloc(&ctx->Q, (size_t)(3 * g.FS) * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->PR, (size_t)g.FS * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->DPH, (size_t)g.FS * sizeof(double)));
+    INIT_CK(cudaMemset(ctx->DPH, 0, (size_t)g.FS * sizeof(double)));  // the inflow/outflow ghost columns stay 0
     INIT_CK(cudaMalloc(&ctx->H0, (size_t)(3 * g.FI) * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->RHS, (size_t)(3 * g.FI) * sizeof(double)));
     INIT_CK(cudaMalloc(&ctx->RHSLL, (size_t)g.FI * sizeof(double)));
@@ -1035,7 +1127,7 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
     ctx->nsm = nsm;
     ctx->npart_red = 4 * nsm;
     INIT_CK(cudaMalloc(&ctx->part_red, (size_t)ctx->npart_red * sizeof(double)));
-    if (ctx->domain == 2) {
+    if (ctx->domain >= 2) {
         IoFields& f = ctx->io;
         INIT_CK(cudaMalloc(&f.G, (size_t)(3 * g.FS) * sizeof(double)));
         INIT_CK(cudaMalloc(&f.EX0, (size_t)(3 * g.FI) * sizeof(double)));
@@ -1048,7 +1140,29 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         INIT_CK(cudaMemset(f.G, 0, (size_t)(3 * g.FS) * sizeof(double)));
         INIT_CK(cudaMemset(f.EX0, 0, (size_t)(3 * g.FI) * sizeof(double)));
         INIT_CK(cudaMemset(f.DIVU, 0, (size_t)g.FS * sizeof(double)));
+        k_fill<<<4 * nsm, XIO_NT, 0, ctx->stream>>>(f.DST, 3 * g.FS, 1.0);  // src/MEMALLOCT.f90:200-201
+        k_fill<<<4 * nsm, XIO_NT, 0, ctx->stream>>>(f.MST, 3 * g.FS, 1.0);
+        INIT_CK(cudaGetLastError());
         ctx->io_grid = ctx->npart_rhs < 8 * nsm ? ctx->npart_rhs : 8 * nsm;
+    }
+    if (xio) {
+        std::vector<double> cq((size_t)4 * L);
+        const double pi = 2.0 * std::asin(1.0);
+        for (int q = 0; q < 4 * L; ++q) cq[q] = std::cos((double)q * pi / (double)(2 * L));
+        INIT_CK(cudaMalloc(&ctx->xio_cq, cq.size() * sizeof(double)));
+        INIT_CK(cudaMemcpy(ctx->xio_cq, cq.data(), cq.size() * sizeof(double), cudaMemcpyHostToDevice));
+        INIT_CK(cudaMalloc(&ctx->xio_bc0, (size_t)3 * M * N * sizeof(double)));
+        INIT_CK(cudaMemset(ctx->xio_bc0, 0, (size_t)3 * M * N * sizeof(double)));
+        INIT_CK(cudaMalloc(&ctx->xio_yd, (size_t)L * M * N * sizeof(double)));
+        INIT_CK(cudaMalloc(&ctx->xio_state, 2 * sizeof(double)));
+        INIT_CK(cudaMemset(ctx->xio_state, 0, 2 * sizeof(double)));
+        INIT_CK(cudaMalloc(&ctx->xio_part, (size_t)3 * ctx->npart_red * sizeof(double)));
+        INIT_CK(cudaEventCreateWithFlags(&ctx->xev[0], cudaEventDisableTiming));
+        INIT_CK(cudaEventCreateWithFlags(&ctx->xev[1], cudaEventDisableTiming));
+        if (smem_xd(g) > 48 * 1024) {
+            INIT_CK(set_smem(k_xio_div_dctx, smem_xd(g)));
+            INIT_CK(set_smem(k_xio_dctx_inv, smem_xd(g)));
+        }
     }
     if (ctx->prec == CHAPSIM_PREC_MIXED) {
         INIT_CK(cudaMalloc(&ctx->Qf, (size_t)(3 * g.FS) * sizeof(float)));
@@ -1127,6 +1241,9 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->dump_snap) cudaEventDestroy(ctx->dump_snap);
     if (ctx->dump_done) cudaEventDestroy(ctx->dump_done);
     if (ctx->dump_stream) cudaStreamDestroy(ctx->dump_stream);
+    cudaFree(ctx->xio_cq); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
+    for (auto& e : ctx->xev)
+        if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1213,7 +1330,7 @@ int chapsim_step_begin(chapsim_ctx_t* ctx, double dt0, double dtmin, double cflg
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
     if (rc) return rc;
-    if (ctx->domain == 2) launch_io_step_start(ctx);
+    if (ctx->domain >= 2) launch_io_step_start(ctx);
     else launch_cfl_dt(ctx, 1);
     CK(cudaGetLastError());
     rc = check_device_error(ctx);
@@ -1237,6 +1354,8 @@ int chapsim_advance_tg(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dt
                        double* cfl_out) {
     if (!ctx) return CHAPSIM_ERR_BADARG;
     if (nsteps < 0) return fail(ctx, CHAPSIM_ERR_BADARG, "nsteps < 0");
+    if (ctx->domain == 3)
+        return fail(ctx, CHAPSIM_ERR_BADARG, "the inflow/outflow main domain steps with its TG domain: chapsim_advance_xinout");
     CK(cudaSetDevice(ctx->device));
     int rc = set_step_params(ctx, dt0, dtmin, cflgv);
     if (rc) return rc;
@@ -1474,6 +1593,7 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
     // accumulates the duration of slot `slot` over the nsteps steps (slot 0 is
     // timed from an event recorded before it).
     if (!ctx) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain == 3) return fail(ctx, CHAPSIM_ERR_BADARG, "profile the inflow/outflow main domain's kernels with ncu");
     const int per = 2 + 3 * (9 + (ctx->thermal ? 6 : 0));
     if (!ms || nslots < per || nsteps < 1)
         return fail(ctx, CHAPSIM_ERR_BADARG, "ms must hold " + std::to_string(per) + " slots and nsteps >= 1");
@@ -1510,7 +1630,7 @@ int chapsim_profile_steps(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double
 int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* gq, const double* pr, const double* rho,
                              const double* mu0, const double* mu) {
     if (!ctx || !gq || !pr || !rho || !mu0 || !mu) return fail(ctx, CHAPSIM_ERR_BADARG, "null field");
-    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
     const Geo& g = ctx->g;
     IoFields& f = ctx->io;
@@ -1539,6 +1659,12 @@ int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* gq, const double*
         k_io_velocity<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, io_fields(ctx));  // VELOCITY_CALC_io
         k_bc_fields<double><<<ctx->npart_red, DG_NT, 0, s>>>(g, ctx->Q, ctx->PR);  // BC_WALL_Q_io
         ctx->launches += 4;
+        if (ctx->domain == 3) {
+            k_xio_ghost_velocity<<<4 * ctx->nsm, XIO_NT, 0, s>>>(g, io_fields(ctx));
+            k_bc_fields<double><<<ctx->npart_red, DG_NT, 0, s>>>(g, ctx->Q, ctx->PR);
+            CK(cudaMemsetAsync(ctx->xio_bc0, 0, (size_t)3 * g.M * g.N * sizeof(double), s));
+            ctx->launches += 2;
+        }
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(s));
@@ -1546,7 +1672,7 @@ int chapsim_upload_io_fields(chapsim_ctx_t* ctx, const double* gq, const double*
 }
 
 int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* gq, double* q, double* pr) {
-    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (!ctx || ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
     const Geo& g = ctx->g;
     if (io_mixed(ctx)) {  // widen the FP32 flow fields into the FP64 staging arrays first
@@ -1564,9 +1690,18 @@ int chapsim_download_io_fields(chapsim_ctx_t* ctx, double* gq, double* q, double
 }
 
 int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns) {
-    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (!ctx || ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     if (ns < 0 || ns > 3) return fail(ctx, CHAPSIM_ERR_BADARG, "NS must be 0..3");
     CK(cudaSetDevice(ctx->device));
+    if (ctx->domain == 3) {
+        if (!ctx->tg_in) return fail(ctx, CHAPSIM_ERR_BADARG, "no TG context attached (chapsim_xinout_attach)");
+        if (ns < 1) return fail(ctx, CHAPSIM_ERR_BADARG, "the inflow/outflow main domain has substeps NS = 1..3");
+        CK(cudaStreamSynchronize(ctx->tg_in->stream));  // the TG substep NS feeds the inlet
+        launch_xio_substep(ctx, ns);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->stream));
+        return check_device_error(ctx);
+    }
     launch_io_substep(ctx, ns);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
@@ -1584,7 +1719,7 @@ static int drop_step_graph(chapsim_ctx* ctx) {
 }
 
 int chapsim_set_buoyancy(chapsim_ctx_t* ctx, int32_t igravity, double f_a) {
-    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (!ctx || ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     if (igravity < -3 || igravity > 3 || !std::isfinite(f_a))
         return fail(ctx, CHAPSIM_ERR_BADARG, "iGravity must be in -3..3 and F_A finite");
     CK(cudaSetDevice(ctx->device));
@@ -1619,7 +1754,7 @@ int chapsim_upload_weighted_pressure(chapsim_ctx_t* ctx, const double* pr0_1, co
 }
 
 int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {
-    if (!ctx || ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (!ctx || ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
     if (io_mixed(ctx)) k_io_cfl<float><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields_t<float>(ctx), ctx->part_red, ctx->st);
     else k_io_cfl<double><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, io_fields(ctx), ctx->part_red, ctx->st);
@@ -1631,9 +1766,75 @@ int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {
     return rc;
 }
 
+int chapsim_xinout_attach(chapsim_ctx_t* io, chapsim_ctx_t* tg) {
+    if (!io || !tg) return fail(io, CHAPSIM_ERR_BADARG, "null context");
+    if (io->domain != 3) return fail(io, CHAPSIM_ERR_BADARG, "context was not created for the inflow/outflow main domain");
+    if (tg->domain != 1 || tg->prec != CHAPSIM_PREC_FP64)
+        return fail(io, CHAPSIM_ERR_BADARG, "the inlet is fed by an FP64 periodic TG context");
+    if (tg->device != io->device || tg->g.M != io->g.M || tg->g.N != io->g.N)
+        return fail(io, CHAPSIM_ERR_BADARG, "the TG context must be on the same device with the same NCL2, NCL3");
+    io->tg_in = tg;
+    return CHAPSIM_OK;
+}
+
+int chapsim_advance_xinout(chapsim_ctx_t* io, int32_t nsteps, double dt0, double dtmin, double cflgv, double* dt_out,
+                           double* cfl_out) {
+    if (!io) return CHAPSIM_ERR_BADARG;
+    if (io->domain != 3) return fail(io, CHAPSIM_ERR_BADARG, "context was not created for the inflow/outflow main domain");
+    if (!io->tg_in) return fail(io, CHAPSIM_ERR_BADARG, "no TG context attached (chapsim_xinout_attach)");
+    if (nsteps < 0) return fail(io, CHAPSIM_ERR_BADARG, "nsteps < 0");
+    chapsim_ctx* tg = io->tg_in;
+    chapsim_ctx* ctx = io;  // for CK
+    CK(cudaSetDevice(io->device));
+    int rc = set_step_params(io, dt0, dtmin, cflgv);
+    if (rc) return rc;
+    rc = set_step_params(tg, dt0, dtmin, cflgv);
+    if (rc) return fail(io, rc, tg->err);
+    for (int s = 0; s < nsteps; ++s) {
+        launch_xio_step_start(io);
+        for (int ns = 1; ns <= 3; ++ns) launch_xio_pair_substep(io, ns);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(tg->stream));
+    rc = check_device_error(tg);
+    if (rc) return fail(io, rc, "TG domain: " + tg->err);
+    rc = check_device_error(io);
+    if (dt_out) *dt_out = io->st_host->dt;
+    if (cfl_out) *cfl_out = io->st_host->cflmm;
+    return rc;
+}
+
+int chapsim_divgck_xinout(chapsim_ctx_t* ctx, double* maxdiv3) {
+    if (!ctx || !maxdiv3) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 3) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the inflow/outflow main domain");
+    CK(cudaSetDevice(ctx->device));
+    const int nb = ctx->npart_red;
+    k_xio_divgck<<<nb, XIO_NT, 0, ctx->stream>>>(ctx->g, ctx->io.G, ctx->xio_part);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    std::vector<double> part((size_t)3 * nb);
+    CK(cudaMemcpyAsync(part.data(), ctx->xio_part, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int r = 0; r < 3; ++r) {
+        double m = 0.0;
+        for (int b = 0; b < nb; ++b) m = std::max(m, part[(size_t)3 * b + r]);
+        maxdiv3[r] = m;
+    }
+    return CHAPSIM_OK;
+}
+
+int chapsim_xinout_outlet_state(chapsim_ctx_t* ctx, double* state2) {
+    if (!ctx || !state2) return CHAPSIM_ERR_BADARG;
+    if (ctx->domain != 3) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the inflow/outflow main domain");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(state2, ctx->xio_state, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
 int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv) {
     if (!ctx || !maxdiv) return CHAPSIM_ERR_BADARG;
-    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
+    if (ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the main (IO) domain");
     CK(cudaSetDevice(ctx->device));
     if (io_mixed(ctx))
         k_io_divgck<float><<<ctx->npart_red, IO_NT, 0, ctx->stream>>>(ctx->g, ctx->iof.G,
@@ -2220,6 +2421,7 @@ extern "C" int chapsim_mlp_judge(chapsim_ctx_t* ctx, double* max_rel_err) {
 // between substeps, so it is zeroed and solved in place.
 extern "C" int chapsim_autotune(chapsim_ctx_t* ctx, int32_t force, int32_t* choice, float* ms) {
     if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
+    if (ctx->domain == 3) return fail(ctx, CHAPSIM_ERR_BADARG, "the inflow/outflow main domain has no tuned variants");
     CK(cudaSetDevice(ctx->device));
     const Geo& g = ctx->g;
     cudaStream_t s = ctx->stream;

@@ -37,6 +37,10 @@ struct DevState {
 // Geometry and constant coefficients of one channel (passed by value).
 struct Geo {
     int L, M, N, LH;
+    // x layout: LI interior columns; xo = 0 in the x-periodic domains (L = LI), xo = 1 in the
+    // main domain with inflow and outflow, whose rows hold the ghost columns 0 and LI + 1 of
+    // NCL1S:NCL1E (L = LI + 2 is then the row stride and LH = LI the count of x modes)
+    int LI, xo;
     long long P;    // L*(M+2): k-plane stride of padded fields
     long long FS;   // P*N: size of one padded field
     long long PI_;  // L*M: k-plane stride of interior fields
@@ -77,14 +81,27 @@ __device__ __forceinline__ long long iidx(const Geo& g, int i, int j, int k) {
 // Point index t = i + L*((j-1) + M*k) of the interior to (i, j, k).  Grids
 // have at most 384^3 < 2^31 points, so 32-bit unsigned division is exact
 // (and an order of magnitude cheaper than 64-bit division on the GPU).
+// In the inflow/outflow main domain t runs over the LI interior columns and i is the
+// storage column 1..LI.
 __device__ __forceinline__ void io_decode(const Geo& g, long long t, int& i, int& j, int& k) {
-    const unsigned u = (unsigned)t, L = (unsigned)g.L, M = (unsigned)g.M;
+    const unsigned u = (unsigned)t, L = (unsigned)g.LI, M = (unsigned)g.M;
     const unsigned r = u / L;
-    i = (int)(u - r * L);
+    i = (int)(u - r * L) + g.xo;
     const unsigned kk = r / M;
     j = 1 + (int)(r - kk * M);
     k = (int)kk;
 }
+// x neighbours of storage column i in the main-domain kernels: cyclic in the x-periodic
+// domains, the ghost columns 0 and LI + 1 with inflow and outflow (IPV_io / IMV_io,
+// src/INDEXSET.f90:26-52)
+__device__ __forceinline__ int xpn(const Geo& g, int i) { return g.xo ? i + 1 : (i + 1 == g.L ? 0 : i + 1); }
+__device__ __forceinline__ int xmn(const Geo& g, int i) { return g.xo ? i - 1 : (i == 0 ? g.L - 1 : i - 1); }
+// interior-array index (RHS, EXPLT0, RHSLLPHI) of storage point (i, j, k)
+__device__ __forceinline__ long long io_iidx(const Geo& g, int i, int j, int k) {
+    return (long long)(i - g.xo) + (long long)g.LI * ((long long)(j - 1) + (long long)g.M * (long long)k);
+}
+// number of interior points
+__device__ __forceinline__ long long io_points(const Geo& g) { return (long long)g.LI * g.M * g.N; }
 // 16-byte vector access of W = 16 / sizeof(R) consecutive elements (float4 or
 // double2); p must be 16-byte aligned
 template <typename R> struct V16 { static constexpr int W = 16 / (int)sizeof(R); };

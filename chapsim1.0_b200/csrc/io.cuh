@@ -64,12 +64,12 @@ __device__ __forceinline__ double io_pgm(const IoFieldsT<F>& f, long long c, lon
 // ---------------------------------------------------------------------------
 template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFieldsT<F> f) {
-    const int L = g.L, M = g.M, N = g.N;
-    const long long tot = (long long)L * M * N;
+    const int M = g.M, N = g.N;
+    const long long tot = io_points(g);
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
-        const int im = wrapm(i, L), km = wrapm(k, N);
+        const int im = xmn(g, i), km = wrapm(k, N);
         const long long c = pidx(g, i, j, k);
         const double* R = f.RHO;
         const double* U0 = f.MU0;
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_props(Geo g, IoFieldsT<F> f) {
 // DIVG_U_io; also VELOCITY_CALC_io of the upload (Q = G / D_STG) when vel != 0
 template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_velocity(Geo g, IoFieldsT<F> f) {
-    const long long tot = (long long)g.L * g.M * g.N;
+    const long long tot = io_points(g);
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
@@ -111,14 +111,14 @@ __global__ void __launch_bounds__(IO_NT) k_io_velocity(Geo g, IoFieldsT<F> f) {
 
 template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_divu(Geo g, IoFieldsT<F> f) {
-    const int L = g.L, N = g.N;
-    const long long tot = (long long)L * g.M * N;
+    const int L = g.L, N = g.N;  // L: row stride
+    const long long tot = io_points(g);
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
         const F* Q = f.Q;
-        const double u = Q[c], up = Q[pidx(g, wrapp(i, L), j, k)];
+        const double u = Q[c], up = Q[pidx(g, xpn(g, i), j, k)];
         const double v = Q[c + g.FS], vp = Q[c + g.FS + L];
         const double w = Q[c + 2 * g.FS], wp = Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS];
         const double DIVX = (up - u) * g.dxi;
@@ -149,8 +149,8 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, doub
                                                   int ns) {
     __shared__ double sred[32];
     __shared__ int is_last;
-    const int L = g.L, M = g.M, N = g.N;
-    const long long tot = (long long)L * M * N;
+    const int N = g.N;
+    const long long tot = io_points(g);
     const long long FS = g.FS;
     const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns], ta = g.talp[ns];
     const double cv = g.cvisc;
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, doub
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
-        const int ip = wrapp(i, L), im = wrapm(i, L), kp = wrapp(k, N), km = wrapm(k, N);
+        const int ip = xpn(g, i), im = xmn(g, i), kp = wrapp(k, N), km = wrapm(k, N);
         const int jp = j + 1, jm = j - 1;
         const long long c = pidx(g, i, j, k);
         const long long cip = pidx(g, ip, j, k), cim = pidx(g, im, j, k);
@@ -376,7 +376,10 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, doub
             }
         }
         // -------- RHS_MOM_EXPLICIT_io --------
-        const long long ii = iidx(g, i, j, k);
+        const long long ii = io_iidx(g, i, j, k);
+        // with inflow the inlet face u(1) is a boundary value: its x-momentum RHS, EXPLT0 and
+        // G are left alone (NXI = 2, src/RHS_MOM_EXPLICIT_io.f90:35)
+        const bool ux = !(g.xo && i == 1);
         const double e01 = f.EX0[ii], e02 = f.EX0[ii + g.FI], e03 = f.EX0[ii + 2 * g.FI];
         const double pc = PR[c], pim = PR[cim], pjm = PR[cjm], pkm = PR[ckm];
         const double coa = ta * dt;
@@ -391,9 +394,11 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, doub
         if constexpr (CN) r3 = r3 + coa * im3;
         r3 = r3 - io_pgm(f, c, ckm, pc, pkm, ta * dt * g.dzi);
         if (ig == 3) r3 = r3 + f.DST[c + 2 * FS] * (cob / 1.0);
-        f.EX0[ii] = (F)ex1;
+        if (ux) {
+            f.EX0[ii] = (F)ex1;
+            f.RHS[ii] = (F)r1;
+        }
         f.EX0[ii + 2 * g.FI] = (F)ex3;
-        f.RHS[ii] = (F)r1;
         f.RHS[ii + 2 * g.FI] = (F)r3;
         if (j >= 2) {
             double r2 = (tg * ex2 + tr * e02) * dt;
@@ -403,7 +408,7 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, doub
             f.EX0[ii + g.FI] = (F)ex2;
             f.RHS[ii + g.FI] = (F)r2;
         }
-        bulk += r1 / dyfij / 1.0;
+        if (ux) bulk += r1 / dyfij / 1.0;
     }
     double s = block_sum<IO_NT>(bulk, sred);
     if (threadIdx.x == 0) {
@@ -428,17 +433,17 @@ __global__ void __launch_bounds__(IO_NT, 2) k_io_rhs(Geo g, IoFieldsT<F> f, doub
 // bulk forcing (RHS_MOM_EXPLICIT_io :228-265) + MASSFLUX_CALC_io
 template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_massflux(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
-    const long long tot = (long long)g.L * g.M * g.N;
+    const long long tot = io_points(g);
     double dpg = 0.0;
     if (g.iflowdriven == 1) dpg = st->bulksum / g.volm;
     else if (g.iflowdriven == 2) dpg = -0.5 * g.cf_given * (g.talp[ns] * st->dt);
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
-        const long long c = pidx(g, i, j, k), ii = iidx(g, i, j, k);
+        const long long c = pidx(g, i, j, k), ii = io_iidx(g, i, j, k);
         const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS];
         const double r1 = f.RHS[ii] - dpg, r3 = f.RHS[ii + 2 * g.FI];
-        f.G[c] = (F)(g1 + r1);
+        if (!(g.xo && i == 1)) f.G[c] = (F)(g1 + r1);  // NXI = 2 with inflow
         f.G[c + 2 * g.FS] = (F)(g3 + r3);
         if (j >= 2) f.G[c + g.FS] = (F)(g2 + (double)f.RHS[ii + g.FI]);
     }
@@ -504,8 +509,8 @@ template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFieldsT<F> f, const double* __restrict__ DPH,
                                                       const DevState* __restrict__ st, int ns,
                                                       const double* __restrict__ RHSLL) {
-    const int L = g.L, M = g.M, N = g.N;
-    const long long tot = (long long)L * M * N;
+    const int M = g.M, N = g.N;
+    const long long tot = io_points(g);
     const double dt = st->dt, ta = g.talp[ns];
     const double be = 0.50 * ta * dt * g.cvisc;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
@@ -513,18 +518,24 @@ __global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFieldsT<F> f, con
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
         const double ph = DPH[c];
-        const double phim = DPH[pidx(g, wrapm(i, L), j, k)];
+        const double phim = DPH[pidx(g, xmn(g, i), j, k)];
         const double phkm = DPH[pidx(g, i, j, wrapm(k, N))];
         const double phjm = j >= 2 ? DPH[pidx(g, i, j - 1, k)] : 0.0;
         const double g1 = f.G[c], g2 = f.G[c + g.FS], g3 = f.G[c + 2 * g.FS], pr = f.PR[c];
         const double d1 = f.DST[c], d2 = f.DST[c + g.FS], d3 = f.DST[c + 2 * g.FS];
-        const double pn = RHSLL ? pr + ph - be * RHSLL[iidx(g, i, j, k)] : pr + ph;
+        const double pn = RHSLL ? pr + ph - be * RHSLL[io_iidx(g, i, j, k)] : pr + ph;
         f.PR[c] = (F)pn;
         if (j == 1) f.PR[pidx(g, i, 0, k)] = (F)pn;
         if (j == M) f.PR[pidx(g, i, M + 1, k)] = (F)pn;
-        const double n1 = g1 - (ph - phim) * (dt * ta * g.dxi);
+        // u faces NXI..NXE: 1..L, or 2..L+1 with inflow (MASSFLUX_UPDATE_io, src/VELO_CORRECTION.f90:121-137);
+        // VELOCITY_CALC_io still divides the fixed inlet face, and leaves the outlet face's Q alone
+        const double n1 = (g.xo && i == 1) ? g1 : g1 - (ph - phim) * (dt * ta * g.dxi);
         const double n3 = g3 - (ph - phkm) * (dt * ta * g.dzi);
         f.G[c] = (F)n1;
+        if (g.xo && i == g.LI) {
+            const double go = f.G[c + 1];
+            f.G[c + 1] = (F)(go - (DPH[c + 1] - ph) * (dt * ta * g.dxi));
+        }
         f.G[c + 2 * g.FS] = (F)n3;
         f.Q[c] = (F)(n1 / d1);
         f.Q[c + 2 * g.FS] = (F)(n3 / d3);
@@ -539,8 +550,8 @@ __global__ void __launch_bounds__(IO_NT) k_io_correct(Geo g, IoFieldsT<F> f, con
 template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFieldsT<F> f, double* __restrict__ partial, DevState* __restrict__ st) {
     __shared__ double sred[32];
-    const int L = g.L, N = g.N;
-    const long long tot = (long long)L * g.M * N;
+    const int L = g.L, N = g.N;  // L: row stride
+    const long long tot = io_points(g);
     double mx = 0.0;
     bool bad = false;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
@@ -548,7 +559,7 @@ __global__ void __launch_bounds__(IO_NT) k_io_cfl(Geo g, IoFieldsT<F> f, double*
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
         const F* Q = f.Q;
-        double q = (fabs(((double)Q[c] + (double)Q[pidx(g, wrapp(i, L), j, k)]) * g.dxi) +
+        double q = (fabs(((double)Q[c] + (double)Q[pidx(g, xpn(g, i), j, k)]) * g.dxi) +
                     fabs(((double)Q[c + g.FS] + (double)Q[c + g.FS + L]) * g.dyfi[j] * 1.0) +
                     fabs(((double)Q[c + 2 * g.FS] + (double)Q[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS]) * g.dzi * 1.0)) * 0.5;
         const double vcf = 2.0 * g.cvisc * (g.dxqi + g.dzqi * 1.0 + g.dyfi[j] * g.dyfi[j]) * f.MU[c] / f.DEN[c];
@@ -570,14 +581,14 @@ template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_io_divgck(Geo g, const F* __restrict__ G,
                                                      const double* __restrict__ DRHO, double* __restrict__ partial) {
     __shared__ double sred[32];
-    const int L = g.L, N = g.N;
-    const long long tot = (long long)L * g.M * N;
+    const int L = g.L, N = g.N;  // L: row stride
+    const long long tot = io_points(g);
     double mx = 0.0;
     for (long long t = (long long)blockIdx.x * IO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, t, i, j, k);
         const long long c = pidx(g, i, j, k);
-        const double DIVX = ((double)G[pidx(g, wrapp(i, L), j, k)] - (double)G[c]) * g.dxi;
+        const double DIVX = ((double)G[pidx(g, xpn(g, i), j, k)] - (double)G[c]) * g.dxi;
         const double DIVY = ((double)G[c + g.FS + L] - (double)G[c + g.FS]) * (g.dyfi[j] * 1.0);
         const double DIVZ = ((double)G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - (double)G[c + 2 * g.FS]) * (g.dzi * 1.0);
         const double DTRHO = DRHO ? DRHO[c] : 0.0;

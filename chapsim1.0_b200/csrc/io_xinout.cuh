@@ -1,0 +1,330 @@
+// Main domain with inflow and outflow (iDomain = 3: TgFlowFlg and IoFlowFlg), flow
+// only, explicit viscous terms: SOLVERRK3_MOM_io with TgFlowFlg
+// (src/SOLVERRK3_MOM_IO.f90:11-120).  The rows of every field hold the ghost
+// columns 0 and LI + 1 (NCL1S:NCL1E, Geo::xo = 1); the momentum, correction and
+// CFL kernels of io.cuh run unchanged on that layout (their x neighbours are the
+// ghost columns, and the inlet face u(1) is left alone).  This file holds what is
+// specific to the inflow/outflow domain:
+//
+//   k_xio_inlet      BC_TINLET_FLOW (src/BC_INLET.f90:12-61): the inlet ghost column from
+//                    the periodic TG domain's last column, the inlet face u(1) from its first
+//   k_xio_outlet     BC_COUTLET_MOM_RK3(NS) (src/BC_COUTLET_MOM_RK3.f90:16-112): U_OUTLET of
+//                    CONVCTION_OUTLET_U (:115-192), the convective update of the outlet
+//                    column, and the outflow scaling of CHK_MassConsv_io
+//                    (src/processing/CHK_conservation.f90:11-79); one block
+//   k_xio_div_dctx   DIVG_io (src/DIVG.f90:54-137) and FISHPACK's x transform COSQF
+//   k_xio_ysolve     TRID0 (src/possion3d_fishpack.f90:309-340) per (x mode, kz)
+//   k_xio_dctx_inv   COSQB and the 1/(SCALX SCALY) scaling -> DPH (interior; the ghost
+//                    columns of DPH stay zero)
+//   k_xio_divgck     DIVGCK_io with TgFlowFlg (src/DIVGCK.f90:80-84): the three cell ranges
+//   k_dt_pair        CFLMM = max(CFLMM_tg, CFLMM_io) and the dt rule (src/SOLVE.f90:79-94)
+//
+// FISHPACK_POIS3D_SIMPLE with BCX_io = (2, 1) is LPEROD = 4: x(0) = x(2) at the inlet,
+// x(L+1) = 0 at the outlet (src/possion3d_fishpack.f90:148-152).  Its x transforms are the
+// quarter-wave cosine pair, written here as the sums FFTPACK defines them by
+//   COSQF  X(m) = x(1) + sum_{p=2..L} 2 x(p) cos((2m-1)(p-1) pi / (2L))
+//   COSQB  x(p) = sum_{m=1..L} 4 X(m) cos((2m-1)(p-1) pi / (2L))
+// (one block computes them for a set of rows from a cosine table in shared memory: L^2
+// multiply-adds per row, well under the bytes a row moves at these lengths).  The z pair
+// RFFTF/RFFTB is k_fftz on the real lines held as complex values.  With LPEROD = 4 no x
+// root is zero, so no mode is singular and TRID0's zero-pivot branch is not taken.
+#pragma once
+#include "common.cuh"
+#include "io.cuh"
+
+#define XIO_NT 256
+#define XIO_OUT_NT 1024
+#define XD_R 8  // rows (j, k) per block of the cosine transforms
+
+// ---------------------------------------------------------------------------
+// BC_TINLET_FLOW: rows j = 0..M+1 of the TG domain's last column (LT - 1) and first
+// u face (column 0).  QT, PRT: the TG fields (row stride LT, field size FST).
+__global__ void __launch_bounds__(XIO_NT) k_xio_inlet(Geo g, IoFields f, const double* __restrict__ QT,
+                                                      const double* __restrict__ PRT, int LT, long long FST) {
+    const int M = g.M;
+    const long long tot = (long long)(M + 2) * g.N;
+    for (long long t = (long long)blockIdx.x * XIO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * XIO_NT) {
+        const int j = (int)(t % (M + 2)), k = (int)(t / (M + 2));
+        const long long rt = (long long)LT * ((long long)j + (long long)(M + 2) * k);
+        const long long cl = rt + LT - 1;
+        const long long c0 = pidx(g, 0, j, k), c1 = c0 + 1;
+        const double d0 = f.RHO[c0];
+        const double u0 = QT[cl], u1 = QT[rt];
+        const double v0 = QT[cl + FST], w0 = QT[cl + 2 * FST];
+        f.Q[c0] = u0;
+        f.Q[c1] = u1;
+        f.G[c0] = u0 * d0;
+        f.G[c1] = u1 * d0;
+        f.Q[c0 + g.FS] = v0;
+        f.G[c0 + g.FS] = v0 * d0;
+        f.Q[c0 + 2 * g.FS] = w0;
+        f.G[c0 + 2 * g.FS] = w0 * d0;
+        f.PR[c0] = PRT[cl];
+    }
+}
+
+// Velocity of the ghost columns at upload: G over the x average of DENSITY0 of the column and
+// its interior neighbour (what BC_COUTLET_MOM_RK3 divides the outlet column by), all rows.
+__global__ void __launch_bounds__(XIO_NT) k_xio_ghost_velocity(Geo g, IoFields f) {
+    const int M = g.M, LI = g.LI;
+    const long long tot = 2LL * (M + 2) * g.N;
+    for (long long t = (long long)blockIdx.x * XIO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * XIO_NT) {
+        const int side = (int)(t & 1);
+        const long long r = t >> 1;
+        const int j = (int)(r % (M + 2)), k = (int)(r / (M + 2));
+        const int ig = side ? LI + 1 : 0, in = side ? LI : 1;
+        const long long c = pidx(g, ig, j, k);
+        const double rho = (f.RHO[pidx(g, in, j, k)] + f.RHO[c]) * 0.5;
+        for (int d = 0; d < 3; ++d) f.Q[c + d * g.FS] = f.G[c + d * g.FS] / rho;
+    }
+}
+
+// Fill a buffer with a constant (D_STG and MU_STG start at 1, src/MEMALLOCT.f90:200-201)
+__global__ void __launch_bounds__(XIO_NT) k_fill(double* __restrict__ p, long long n, double v) {
+    for (long long t = (long long)blockIdx.x * XIO_NT + threadIdx.x; t < n; t += (long long)gridDim.x * XIO_NT) p[t] = v;
+}
+
+// ---------------------------------------------------------------------------
+// BC_COUTLET_MOM_RK3(NS).  BC0: BC_CONV0(J, K, IDR) as [IDR][K][J] (M*N per component);
+// state[0] = U_OUTLET, state[1] = CHK_Mass_CONSV0_SCALING of this substep.  One block: the
+// outlet plane is M*N points, and the three phases (extremes of the outlet u, the update, the
+// fluxes) each need the whole plane.  The mass rate of the interior is zero (flow only).
+__global__ void __launch_bounds__(XIO_OUT_NT) k_xio_outlet(Geo g, IoFields f, double* __restrict__ BC0,
+                                                           double* __restrict__ state, DevState* __restrict__ st,
+                                                           int ns) {
+    __shared__ double sred[32];
+    const int M = g.M, N = g.N, L = g.LI;
+    const int np = M * N;
+    // CONVCTION_OUTLET_U: UCC = (u(L) + u(L+1)) / 2 over the outlet plane, U_OUTLET = (max + min) / 2
+    double mx = -1.0E20, mn = 1.0E20;
+    for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
+        const int j = 1 + p % M, k = p / M;
+        const long long c = pidx(g, L, j, k);
+        const double ucc = (f.Q[c] + f.Q[c + 1]) * 0.5;
+        mx = fmax(mx, ucc);
+        mn = fmin(mn, ucc);
+    }
+    const double umax = block_max<XIO_OUT_NT>(mx, sred);
+    const double umin = -block_max<XIO_OUT_NT>(-mn, sred);
+    const double uout = 0.5 * (umax + umin);
+    const double coe1 = g.dxi * uout;
+    const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns];
+    for (int idr = 0; idr < 3; ++idr) {
+        const int n2i = idr == 1 ? 2 : 1;
+        for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
+            const int j = 1 + p % M, k = p / M;
+            if (j < n2i) continue;
+            const long long c = pidx(g, L, j, k) + idr * g.FS;
+            const long long b = (long long)idr * np + (long long)(j - 1) + (long long)M * k;
+            const double bc_conv = -(f.G[c + 1] - f.G[c]) * coe1;
+            const double bc_rhs = tg * bc_conv + tr * BC0[b];
+            BC0[b] = bc_conv;
+            const double gn = f.G[c + 1] + dt * bc_rhs;
+            f.G[c + 1] = gn;
+            const long long cr = pidx(g, L, j, k);
+            const double rho = (f.RHO[cr] + f.RHO[cr + 1]) * 0.5;
+            f.Q[c + 1] = gn / rho;
+        }
+    }
+    __syncthreads();
+    // CHK_MassConsv_io: inlet (u face 1) and outlet (u face L+1) fluxes
+    double fin = 0.0, fout = 0.0;
+    for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
+        const int j = 1 + p % M, k = p / M;
+        const double coe2 = 1.0 / g.dyfi[j] / 1.0;
+        fin += f.G[pidx(g, 1, j, k)] * coe2;
+        fout += f.G[pidx(g, L + 1, j, k)] * coe2;
+    }
+    const double flux_in = block_sum<XIO_OUT_NT>(fin, sred) / g.dzi;
+    const double flux_out = block_sum<XIO_OUT_NT>(fout, sred) / g.dzi;
+    const double mass_rate = 0.0;
+    const double scaling = (flux_in - mass_rate) / flux_out;
+    for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
+        const int j = 1 + p % M, k = p / M;
+        const long long c = pidx(g, L + 1, j, k);
+        const double go = f.G[c];
+        const double gn = go * (scaling - 1.0) + go;
+        f.G[c] = gn;
+        f.Q[c] = gn / ((f.RHO[c - 1] + f.RHO[c]) * 0.5);
+    }
+    if (threadIdx.x == 0) {
+        state[0] = uout;
+        state[1] = scaling;
+        if (!(scaling == scaling) || !(uout == uout)) atomicOr(&st->err, CHS_EBIT_NAN);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// DIVG_io + COSQF.  Block: XD_R rows q = (j - 1) + M k; the row's divergence times
+// 1/(alpha dt) (and 1/wdiv, DIVG.f90:78-82) goes to shared memory, then each thread forms
+// whole modes X(m) = x(1) + sum_p 2 x(p) cos(...) in the sum's own order.  The cosine table
+// cq[q] = cos(q pi / (2 L)), q < 4 L, comes from the host.  SP[m + L ((j-1) + M k)] = (X(m), 0).
+__global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __restrict__ G, const double* __restrict__ cq,
+                                                         double2* __restrict__ SP, const DevState* __restrict__ st,
+                                                         int ns, double wdiv) {
+    extern __shared__ double xsm[];
+    const int L = g.LI, M = g.M, N = g.N, Q4 = 4 * L;
+    double* tab = xsm;           // 4 L
+    double* row = xsm + Q4;      // XD_R x L
+    const long long nrows = (long long)M * N;
+    const long long q0 = (long long)blockIdx.x * XD_R;
+    const int nr = (int)min((long long)XD_R, nrows - q0);
+    for (int t = threadIdx.x; t < Q4; t += XIO_NT) tab[t] = cq[t];
+    const double coe0 = 1.0 / st->dt / g.talp[ns] / wdiv;
+    const double coe1 = g.dxi / 1.0;
+    for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
+        const int r = p / L, i = 1 + (p - r * L);
+        const long long q = q0 + r;
+        const int j = 1 + (int)(q % M), k = (int)(q / M);
+        const long long c = pidx(g, i, j, k);
+        const double u = G[c], up = G[c + 1];
+        const double v = G[c + g.FS], vp = G[c + g.FS + g.L];
+        const double w = G[c + 2 * g.FS], wp = G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS];
+        const double coe2 = g.dyfi[j] / 1.0;
+        const double DIVX = (up - u) * coe1, DIVY = (vp - v) * coe2, DIVZ = (wp - w) * g.dzi;
+        const double DQ = DIVX + DIVY + DIVZ + 0.0;
+        row[r * L + (i - 1)] = DQ * coe0;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
+        const int r = p / L, m = p - r * L;
+        const double* x = row + r * L;
+        const int a = 2 * m + 1;
+        double X = x[0];
+        int e = 0;
+        for (int pp = 1; pp < L; ++pp) {
+            e += a;
+            if (e >= Q4) e -= Q4;
+            X = X + 2.0 * x[pp] * tab[e];
+        }
+        const long long q = q0 + r;
+        SP[m + (long long)L * q] = make_double2(X, 0.0);
+    }
+}
+
+// TRID0 for every (x mode m, kz) line: BB(j) = ACPH(j) + XRT(m) + YRT(kz) with XRT = -ak1[m],
+// YRT = -ak3[kz]; A = AMPH, C = APPH.  D holds the forward factors (M per line, line-major
+// across threads).  Complex right-hand side: the real and imaginary lines share D.
+__global__ void __launch_bounds__(XIO_NT) k_xio_ysolve(Geo g, double2* __restrict__ SP, double* __restrict__ D) {
+    const int L = g.LI, M = g.M, N = g.N;
+    const long long nl = (long long)L * N;
+    const long long ln = (long long)blockIdx.x * XIO_NT + threadIdx.x;
+    if (ln >= nl) return;
+    const int m = (int)(ln % L), kz = (int)(ln / L);
+    const double xrt = -g.ak1[m], yrt = -g.ak3[kz];
+    const long long stride = L;  // element j of the line: m + L ((j - 1) + M kz)
+    double2* S = SP + m + (long long)L * M * kz;
+    double* Dl = D + ln;          // element j - 1 at Dl[(j - 1) * nl]
+    double bb = g.acph[1] + xrt / 1.0 + yrt;
+    double z = 1.0 / bb;
+    double d = g.apph[1] * z;
+    Dl[0] = d;
+    double2 t = S[0];
+    t.x = t.x * z;
+    t.y = t.y * z;
+    S[0] = t;
+    for (int j = 2; j <= M - 1; ++j) {
+        bb = g.acph[j] + xrt / 1.0 + yrt;
+        z = 1.0 / (bb - g.amph[j] * d);
+        d = g.apph[j] * z;
+        Dl[(long long)(j - 1) * nl] = d;
+        double2 r = S[(long long)(j - 1) * stride];
+        r.x = (r.x - g.amph[j] * t.x) * z;
+        r.y = (r.y - g.amph[j] * t.y) * z;
+        S[(long long)(j - 1) * stride] = r;
+        t = r;
+    }
+    bb = g.acph[M] + xrt / 1.0 + yrt;
+    z = bb - g.amph[M] * d;
+    double2 r = S[(long long)(M - 1) * stride];
+    if (fabs(z) > 1.0E-14) {
+        r.x = (r.x - g.amph[M] * t.x) / z;
+        r.y = (r.y - g.amph[M] * t.y) / z;
+    } else {
+        r = make_double2(0.0, 0.0);
+    }
+    S[(long long)(M - 1) * stride] = r;
+    for (int j = M - 1; j >= 1; --j) {
+        const double dj = Dl[(long long)(j - 1) * nl];
+        double2 s = S[(long long)(j - 1) * stride];
+        s.x = s.x - dj * r.x;
+        s.y = s.y - dj * r.y;
+        S[(long long)(j - 1) * stride] = s;
+        r = s;
+    }
+}
+
+// COSQB of the real parts and the scaling 1/(4 L) (the 1/N is the forward z transform's):
+// DPH(p, j, k) for the interior columns p = 1..L.
+__global__ void __launch_bounds__(XIO_NT) k_xio_dctx_inv(Geo g, const double2* __restrict__ SP, const double* __restrict__ cq,
+                                                         double* __restrict__ DPH) {
+    extern __shared__ double xsm[];
+    const int L = g.LI, M = g.M, N = g.N, Q4 = 4 * L;
+    double* tab = xsm;
+    double* row = xsm + Q4;
+    const long long nrows = (long long)M * N;
+    const long long q0 = (long long)blockIdx.x * XD_R;
+    const int nr = (int)min((long long)XD_R, nrows - q0);
+    for (int t = threadIdx.x; t < Q4; t += XIO_NT) tab[t] = cq[t];
+    for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
+        const int r = p / L, m = p - r * L;
+        row[r * L + m] = SP[m + (long long)L * (q0 + r)].x;
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
+        const int r = p / L, pp = p - r * L;
+        const double* X = row + r * L;
+        double x = 0.0;
+        int e = pp;  // ((2m + 1) pp) mod 4L for m = 0
+        const int step = 2 * pp;
+        for (int m = 0; m < L; ++m) {
+            x = x + 4.0 * X[m] * tab[e];
+            e += step;
+            while (e >= Q4) e -= Q4;
+        }
+        const long long q = q0 + r;
+        const int j = 1 + (int)(q % M), k = (int)(q / M);
+        DPH[pidx(g, pp + 1, j, k)] = x / (double)Q4;
+    }
+}
+
+// DIVGCK_io with TgFlowFlg: max |div G| over the cells 2..L-1, 0..1 and L (DrhoDtP = 0).
+// partial[3 b + r] holds block b's maximum of range r.
+__global__ void __launch_bounds__(XIO_NT) k_xio_divgck(Geo g, const double* __restrict__ G, double* __restrict__ partial) {
+    __shared__ double sred[32];
+    const int L = g.LI, M = g.M, N = g.N;
+    const long long tot = (long long)(L + 1) * M * N;  // cells i = 0..L
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (long long t = (long long)blockIdx.x * XIO_NT + threadIdx.x; t < tot; t += (long long)gridDim.x * XIO_NT) {
+        const int i = (int)(t % (L + 1));
+        const long long rq = t / (L + 1);
+        const int j = 1 + (int)(rq % M), k = (int)(rq / M);
+        const long long c = pidx(g, i, j, k);
+        const double DIVX = (G[c + 1] - G[c]) * g.dxi;
+        const double DIVY = (G[c + g.FS + g.L] - G[c + g.FS]) * (g.dyfi[j] * 1.0);
+        const double DIVZ = (G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - G[c + 2 * g.FS]) * (g.dzi * 1.0);
+        const double a = fabs(DIVX + DIVY + DIVZ + 0.0);
+        const int r = (i >= 2 && i <= L - 1) ? 0 : (i <= 1 ? 1 : 2);
+        mx[r] = fmax(mx[r], a);
+    }
+    for (int r = 0; r < 3; ++r) {
+        const double b = block_max<XIO_NT>(mx[r], sred);
+        if (threadIdx.x == 0) partial[3 * blockIdx.x + r] = b;
+    }
+}
+
+// The dt of a TG + main-domain step: CFLMM = max(CFLMM_tg, CFLMM_io) (src/SOLVE.f90:79-86),
+// then BCAST_COMM_STEP's rule on the main domain's DT0, DTMIN, CFLGV; DT goes to both states.
+__global__ void k_dt_pair(DevState* __restrict__ tg, DevState* __restrict__ io) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const double c = fmax(tg->cflmm, io->cflmm);
+    double dt = fmin(fmin(io->dt0, 5.0 * io->dt), io->cflgv / c);
+    dt = fmax(dt, io->dtmin);
+    io->cflmm = c;
+    io->dtprev = io->dt;
+    tg->dtprev = tg->dt;
+    io->dt = dt;
+    tg->dt = dt;
+    if ((dt / io->dt0) < 0.01) atomicOr(&io->err, CHS_EBIT_DT_COLLAPSE);
+    if (!(dt == dt)) atomicOr(&io->err, CHS_EBIT_NAN);
+}

@@ -34,15 +34,19 @@ typedef struct chapsim_ctx chapsim_ctx_t;
 
 /* Grid: NCL1 (NCL1_tg or NCL1_io), NCL2, NCL3 of src/modules.f90 (mesh_info).
  * Only the plane channel (iCase = 1) is accepted, in the periodic TG domain
- * (iDomain = 1) or the x-periodic main domain (iDomain = 2).
+ * (iDomain = 1), the x-periodic main domain (iDomain = 2), or the main domain of
+ * a TG + main-domain run with inflow and outflow (idomain = 3; the TG domain is a
+ * separate idomain = 1 context, see chapsim_xinout_attach).
  * L and N must factor into 2s and 3s (FFT lengths), L, M, N must be
- * multiples of 32 between 32 and 384. */
+ * multiples of 32 between 32 and 384; with idomain = 3, L = NCL1_io is any even
+ * number from 4 to 1024. */
 typedef struct {
     int32_t ncl1;   /* L */
     int32_t ncl2;   /* M */
     int32_t ncl3;   /* N */
     int32_t icase;  /* must be 1 (ICHANL) */
-    int32_t idomain;/* 1 (ITG) or 2 (IIO, x-periodic main domain) */
+    int32_t idomain;/* 1 (ITG), 2 (IIO, x-periodic main domain) or 3 (main domain with inflow
+                       from a TG context and a convective outlet, TgFlowFlg)               */
 } chapsim_grid_t;
 
 /* Coefficients computed by the host's set-up routines, passed unchanged.
@@ -64,8 +68,12 @@ typedef struct {
     const double* amvr;          /* AMVR(1:NND2, 1:3), Fortran order             */
     const double* acvr;          /* ACVR(1:NND2, 1:3)                            */
     const double* apvr;          /* APVR(1:NND2, 1:3)                            */
-    const double* ak1;           /* AK1(1:NCL1) (src/possion3d_FFT99.f90:180-198)*/
-    const double* ak3;           /* AK3(1:NCL3)                                  */
+    const double* ak1;           /* AK1(1:NCL1) (src/possion3d_FFT99.f90:180-198);
+                                    idomain 3: -XRT(1:NCL1) of FFTPACK_ROOT with
+                                    LP = 5 (src/possion3d_fishpack.f90:65-111),
+                                    4 DXQI sin^2((I-1/2) pi/(2 NCL1))           */
+    const double* ak3;           /* AK3(1:NCL3); idomain 3: -YRT, 4 DZQI
+                                    sin^2(pi min(k, NCL3-k)/NCL3), k = 0..NCL3-1 */
     double tgam[4], troh[4], talp[4]; /* CONS_RKCOEF (src/CONS_RKCOEF.f90:25-51) */
     double amvr1, apvrn;         /* AMVR1, APVRN wall-row factors of TDMA_COEF
                                     (src/TDMA_COEF.f90:79-87); read only when
@@ -225,6 +233,44 @@ int chapsim_upload_weighted_pressure(chapsim_ctx_t* ctx, const double* pr0_1, co
 /* DIVGCK_io (src/DIVGCK.f90:60-184), x-periodic main domain: MAXDIVGV_io, the
  * max over the interior of |div G + DrhoDtP| (the three ranges coincide). */
 int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv);
+
+/* ---- Main domain with inflow and outflow (grid.idomain = 3): the IO part of a
+ * TG + main-domain run (iDomain = 3, TgFlowFlg and IoFlowFlg), flow only
+ * (iThermoDynamics = 0, or before timeThermoStart), explicit viscous terms, FP64.
+ * Fields carry the x ghost columns NCL1S:NCL1E = 0:NCL1+1: chapsim_upload_io_fields /
+ * chapsim_download_io_fields take (0:NCL1+1, 0:NCL2+1, NCL3) arrays (and G_io(..., 3));
+ * the upload also sets the ghost columns' velocity to G over the x average of DENSITY0
+ * of the column and its interior neighbour, and zeroes BC_CONV0.  No bulk forcing
+ * (src/RHS_MOM_EXPLICIT_io.f90:229); chapsim_set_buoyancy, chapsim_cfl_io and
+ * chapsim_divgck_io (max over the cells 1..NCL1) apply; the thermal solver, iWeightedPre,
+ * the main-domain statistics, chapsim_advance_tg, chapsim_autotune and
+ * chapsim_profile_steps do not (CHAPSIM_ERR_BADARG). */
+
+/* The periodic TG context whose fields feed BC_TINLET_FLOW (src/BC_INLET.f90:12-61):
+ * FP64, same device, same NCL2, NCL3 and y mesh (the x spacing must match, as
+ * CONSPARA checks, src/CONSPARA.f90:44-52).  The TG context must outlive its use. */
+int chapsim_xinout_attach(chapsim_ctx_t* io, chapsim_ctx_t* tg);
+/* chapsim_rk_substep_io(io, NS), NS = 1..3, on an idomain 3 context runs
+ * SOLVERRK3_MOM_io(NS) with TgFlowFlg (src/SOLVERRK3_MOM_IO.f90:11-120): BC_TINLET_FLOW
+ * from the attached TG context's resident fields (run its substep NS first),
+ * BC_COUTLET_MOM_RK3(NS) (src/BC_COUTLET_MOM_RK3.f90:16-192 with CHK_MassConsv_io,
+ * src/processing/CHK_conservation.f90:11-79), the momentum step with the inlet face u(1)
+ * fixed, DIVG_io, FISHPACK_POIS3D_SIMPLE with BCX_io = (2, 1) (LPEROD = 4,
+ * src/possion3d_fishpack.f90:344-460), PRCALC_io and MASSFLUX_UPDATE_io over the u faces
+ * 2..NCL1+1 (src/VELO_CORRECTION.f90:121-137). */
+
+/* nsteps iterations of the SOLVE loop of a TG + main-domain run (src/SOLVE.f90:75-134):
+ * CFL_tg and CFL_io, DT from CFLMM = max(CFLMM_tg, CFLMM_io) by the dt rule, then per NS
+ * SOLVERRK3_MOM_tg(NS) on the attached TG context and SOLVERRK3_MOM_io(NS) here.  Both
+ * contexts' DT follow; dt_out / cfl_out (may be NULL) receive DT and CFLMM of the last step.
+ * CHAPSIM_ERR_DT_COLLAPSE as chapsim_advance_tg. */
+int chapsim_advance_xinout(chapsim_ctx_t* io, int32_t nsteps, double dt0, double dtmin, double cflgv, double* dt_out,
+                           double* cfl_out);
+/* DIVGCK_io with TgFlowFlg (src/DIVGCK.f90:80-84): MAXDIVGV_io(1:3), the max |div G| over
+ * the cells 2..NCL1-1, 0..1 and NCL1 (DrhoDtP = 0). */
+int chapsim_divgck_xinout(chapsim_ctx_t* ctx, double* maxdiv3);
+/* U_OUTLET (CONVCTION_OUTLET_U) and CHK_Mass_CONSV0_SCALING of the last substep. */
+int chapsim_xinout_outlet_state(chapsim_ctx_t* ctx, double* state2);
 
 /* ---- Thermophysical properties by table search ----
  * The nondimensional table and spline coefficients of the thermal_info module

@@ -1096,6 +1096,19 @@ void orc_io_set_fields(orc_t* o, const double* G, const double* PR, const double
     bc_wall_scalar(o, o->PR);
     io_staggered_props(o);
     io_velocity_calc(o);
+    if (o->xo) {
+        /* the ghost columns' velocity: G over the x average of DENSITY0 of the column and its */
+        /* interior neighbour (the division BC_COUTLET_MOM_RK3 applies to the outlet column)    */
+        int L = o->L, M = o->M, N = o->N;
+        for (int K = 1; K <= N; ++K)
+            for (int J = 0; J <= M + 1; ++J)
+                for (int side = 0; side < 2; ++side) {
+                    int IG = side ? L + 1 : 0, IN = side ? L : 1;
+                    double RHO = (F3(o->RHO, o, IN, J, K) + F3(o->RHO, o, IG, J, K)) * 0.5;
+                    for (int c = 1; c <= 3; ++c) QV(o, IG, J, K, c) = GV(o, IG, J, K, c) / RHO;
+                }
+        memset(o->BCCONV0, 0, 3 * (size_t)M * (size_t)N * sizeof(double));
+    }
 }
 
 void orc_io_get_fields(const orc_t* o, double* G, double* Q, double* PR) {
