@@ -84,6 +84,28 @@ __global__ void __launch_bounds__(XIO_NT) k_fill(double* __restrict__ p, long lo
     for (long long t = (long long)blockIdx.x * XIO_NT + threadIdx.x; t < n; t += (long long)gridDim.x * XIO_NT) p[t] = v;
 }
 
+// block_sum / block_max leave the result in thread 0; these hand it to every thread
+template <int NT>
+__device__ __forceinline__ double block_sum_all(double v, double* sbuf) {
+    __shared__ double bcast;
+    const double r = block_sum<NT>(v, sbuf);
+    if (threadIdx.x == 0) bcast = r;
+    __syncthreads();
+    const double a = bcast;
+    __syncthreads();
+    return a;
+}
+template <int NT>
+__device__ __forceinline__ double block_max_all(double v, double* sbuf) {
+    __shared__ double bcast;
+    const double r = block_max<NT>(v, sbuf);
+    if (threadIdx.x == 0) bcast = r;
+    __syncthreads();
+    const double a = bcast;
+    __syncthreads();
+    return a;
+}
+
 // ---------------------------------------------------------------------------
 // BC_COUTLET_MOM_RK3(NS).  BC0: BC_CONV0(J, K, IDR) as [IDR][K][J] (M*N per component);
 // state[0] = U_OUTLET, state[1] = CHK_Mass_CONSV0_SCALING of this substep.  One block: the
@@ -104,8 +126,8 @@ __global__ void __launch_bounds__(XIO_OUT_NT) k_xio_outlet(Geo g, IoFields f, do
         mx = fmax(mx, ucc);
         mn = fmin(mn, ucc);
     }
-    const double umax = block_max<XIO_OUT_NT>(mx, sred);
-    const double umin = -block_max<XIO_OUT_NT>(-mn, sred);
+    const double umax = block_max_all<XIO_OUT_NT>(mx, sred);
+    const double umin = -block_max_all<XIO_OUT_NT>(-mn, sred);
     const double uout = 0.5 * (umax + umin);
     const double coe1 = g.dxi * uout;
     const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns];
@@ -135,8 +157,8 @@ __global__ void __launch_bounds__(XIO_OUT_NT) k_xio_outlet(Geo g, IoFields f, do
         fin += f.G[pidx(g, 1, j, k)] * coe2;
         fout += f.G[pidx(g, L + 1, j, k)] * coe2;
     }
-    const double flux_in = block_sum<XIO_OUT_NT>(fin, sred) / g.dzi;
-    const double flux_out = block_sum<XIO_OUT_NT>(fout, sred) / g.dzi;
+    const double flux_in = block_sum_all<XIO_OUT_NT>(fin, sred) / g.dzi;
+    const double flux_out = block_sum_all<XIO_OUT_NT>(fout, sred) / g.dzi;
     const double mass_rate = 0.0;
     const double scaling = (flux_in - mass_rate) / flux_out;
     for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
