@@ -342,6 +342,58 @@ def heated_measure(args, local, dist, ws, steps):
     return line
 
 
+# TG + main-domain run with inflow and outflow (iDomain = 3): a 128^3 periodic TG channel (4 pi x 2 x 4 pi/3)
+# feeding a main domain twice its length
+XINOUT = {"LT": 128, "L": 256, "M": 128, "N": 128, "HXT": 4 * math.pi, "HZ": 4 * math.pi / 3, "STR2": 2.0,
+          "REN": 2800.0, "DT0": 0.01, "CFLGV": 0.5}
+
+
+def xinout_measure(args, local, steps):
+    """The coupled TG + inflow/outflow step (chapsim_advance_xinout), timed with CUDA events from the TG
+    stream's first launch to the main-domain stream's last (the two streams join every substep)."""
+    import torch
+    from chapsim import gpu
+    from chapsim.mesh import xinout_setup
+    from chapsim.fields import xinout_fields_from_tg
+    c = XINOUT
+    dx = c["HXT"] / c["LT"]
+    st = channel_setup(c["LT"], c["M"], c["N"], c["HXT"], c["HZ"], c["STR2"], c["REN"])
+    Q, PR = initial_field(st, 7, 0.2)
+    tg = gpu.ChannelTG(st)
+    tg.upload(Q, PR)
+    tg.set_dt(c["DT0"])
+    tg.SOLVERRK3_MOM_tg(0)
+    Qt, _ = tg.download()
+    io = gpu.ChannelXinout(xinout_setup(c["L"], c["M"], c["N"], c["L"] * dx, c["HZ"], c["STR2"], c["REN"]), tg=tg)
+    G, P = xinout_fields_from_tg(Qt, c["L"])
+    ones = np.ones(io.field_shape())
+    io.upload_io(G, P, ones, ones, ones)
+    io.set_dt(c["DT0"])
+    io.advance(args.warmup, c["DT0"], 1e-6, c["CFLGV"])
+    s_tg = torch.cuda.ExternalStream(tg.stream_handle(), device=local)
+    s_io = torch.cuda.ExternalStream(io.stream_handle(), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(local)
+    l0 = io.launch_count() + tg.launch_count()
+    e0.record(s_tg)
+    dt, cfl = io.advance(steps, c["DT0"], 1e-6, c["CFLGV"])
+    e1.record(s_io)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = io.launch_count() + tg.launch_count() - l0
+    div = io.DIVGCK_io()
+    u_out, scaling = io.outlet_state()
+    pts = (c["LT"] + c["L"]) * c["M"] * c["N"]
+    io.close()
+    tg.close()
+    return {"grids": {"tg": [c["LT"], c["M"], c["N"]], "main": [c["L"], c["M"], c["N"]]},
+            "value": pts * 1e3 / ms, "unit": UNIT, "ms_per_step": ms, "steps": steps, "gpu_launches": int(launches),
+            "final_dt": dt, "final_cfl": cfl, "maxdiv_ranges": [float(x) for x in div], "u_outlet": u_out,
+            "outflow_scaling": scaling,
+            "note": "TG + main domain with inflow/outflow (iDomain = 3), explicit viscous main domain, FP64; "
+                    "value counts the points of both domains"}
+
+
 def kernel_bytes(L, precision="fp64"):
     """Algorithmic bytes per grid point moved by one launch of each periodic-
     channel kernel, keyed by the kernel names profile_steps reports: reads +
@@ -811,6 +863,7 @@ def run_b200(args):
             "step_roofline_frac": hl["step_roofline"]["frac"],
             "note": "main domain (Crank-Nicolson momentum, energy equation, property update every substep), FP64; "
                     "the full line: --workload " + HEATED_WORKLOAD}
+        variants["developing"] = xinout_measure(args, local, min(args.steps, 100))
         line["variants"] = variants
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -226,7 +226,8 @@ struct chapsim_ctx {
     cudaEvent_t dump_snap = nullptr, dump_done = nullptr;
     // inflow/outflow main domain (domain 3)
     chapsim_ctx* tg_in = nullptr;  // the periodic TG context whose fields feed the inlet
-    double* xio_cq = nullptr;      // cos(q pi / (2 L)), q < 4 L
+    double* xio_cf = nullptr;      // COSQF matrix w_p cos((2m+1) p pi / (2L)), [p][m]; then the COSQB matrix
+                                   // 4 cos((2m+1) p pi / (2L)), [m][p] (one allocation, 2 L^2)
     double* xio_bc0 = nullptr;     // BC_CONV0 (3 M N)
     double* xio_yd = nullptr;      // forward factors of the Poisson y-solve (L N M)
     double* xio_state = nullptr;   // U_OUTLET, CHK_Mass_CONSV0_SCALING of the last substep
@@ -864,7 +865,7 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
 }
 
 // ------------------------- inflow/outflow main domain ------------------------
-size_t smem_xd(const Geo& g) { return (size_t)(4 + XD_R) * g.LI * sizeof(double); }
+size_t smem_xd(const Geo& g) { return (size_t)XD_R * g.LI * sizeof(double); }
 
 // SOLVERRK3_MOM_io(NS) with TgFlowFlg (src/SOLVERRK3_MOM_IO.f90:11-120), explicit viscous
 // terms: BC_TINLET_FLOW from the attached TG context (its substep NS must have run; the
@@ -888,7 +889,7 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     k_io_massflux<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
     prof_mark(ctx);
     const int nrb = (int)(((long long)g.M * g.N + XD_R - 1) / XD_R);
-    k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cq, ctx->SP, ctx->st, ns, 1.0);
+    k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cf, ctx->SP, ctx->st, ns, 1.0);
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;  // LH = LI x modes
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
@@ -898,7 +899,7 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
     prof_mark(ctx);
-    k_xio_dctx_inv<<<nrb, XIO_NT, smem_xd(g), s>>>(g, ctx->SP, ctx->xio_cq, ctx->DPH);
+    k_xio_dctx_inv<<<nrb, XIO_NT, smem_xd(g), s>>>(g, ctx->SP, ctx->xio_cf + (size_t)g.LI * g.LI, ctx->DPH);
     prof_mark(ctx);
     k_io_correct<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, nullptr);
     prof_mark(ctx);
@@ -1146,11 +1147,17 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         ctx->io_grid = ctx->npart_rhs < 8 * nsm ? ctx->npart_rhs : 8 * nsm;
     }
     if (xio) {
-        std::vector<double> cq((size_t)4 * L);
+        std::vector<double> cq((size_t)4 * L), cm((size_t)2 * L * L);
         const double pi = 2.0 * std::asin(1.0);
         for (int q = 0; q < 4 * L; ++q) cq[q] = std::cos((double)q * pi / (double)(2 * L));
-        INIT_CK(cudaMalloc(&ctx->xio_cq, cq.size() * sizeof(double)));
-        INIT_CK(cudaMemcpy(ctx->xio_cq, cq.data(), cq.size() * sizeof(double), cudaMemcpyHostToDevice));
+        for (int p = 0; p < L; ++p)
+            for (int m = 0; m < L; ++m) {
+                const double c = cq[(size_t)(((long long)(2 * m + 1) * p) % (4 * L))];
+                cm[(size_t)p * L + m] = p == 0 ? 1.0 : 2.0 * c;       // COSQF
+                cm[(size_t)L * L + (size_t)m * L + p] = 4.0 * c;      // COSQB
+            }
+        INIT_CK(cudaMalloc(&ctx->xio_cf, cm.size() * sizeof(double)));
+        INIT_CK(cudaMemcpy(ctx->xio_cf, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice));
         INIT_CK(cudaMalloc(&ctx->xio_bc0, (size_t)3 * M * N * sizeof(double)));
         INIT_CK(cudaMemset(ctx->xio_bc0, 0, (size_t)3 * M * N * sizeof(double)));
         INIT_CK(cudaMalloc(&ctx->xio_yd, (size_t)L * M * N * sizeof(double)));
@@ -1241,7 +1248,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->dump_snap) cudaEventDestroy(ctx->dump_snap);
     if (ctx->dump_done) cudaEventDestroy(ctx->dump_done);
     if (ctx->dump_stream) cudaStreamDestroy(ctx->dump_stream);
-    cudaFree(ctx->xio_cq); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
+    cudaFree(ctx->xio_cf); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
     for (auto& e : ctx->xev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -24,8 +24,8 @@
 // quarter-wave cosine pair, written here as the sums FFTPACK defines them by
 //   COSQF  X(m) = x(1) + sum_{p=2..L} 2 x(p) cos((2m-1)(p-1) pi / (2L))
 //   COSQB  x(p) = sum_{m=1..L} 4 X(m) cos((2m-1)(p-1) pi / (2L))
-// (one block computes them for a set of rows from a cosine table in shared memory: L^2
-// multiply-adds per row, well under the bytes a row moves at these lengths).  The z pair
+// (a block of rows times the L x L transform matrix, register-tiled: L^2 multiply-adds per
+// row).  The z pair
 // RFFTF/RFFTB is k_fftz on the real lines held as complex values.  With LPEROD = 4 no x
 // root is zero, so no mode is singular and TRID0's zero-pivot branch is not taken.
 #pragma once
@@ -34,7 +34,9 @@
 
 #define XIO_NT 256
 #define XIO_OUT_NT 1024
-#define XD_R 8  // rows (j, k) per block of the cosine transforms
+#define XD_R 16  // rows (j, k) per block of the cosine transforms
+#define XD_RT 4  // rows per thread
+#define XD_MT 4  // modes (or points) per thread in one pass
 
 // ---------------------------------------------------------------------------
 // BC_TINLET_FLOW: rows j = 0..M+1 of the TG domain's last column (LT - 1) and first
@@ -177,21 +179,52 @@ __global__ void __launch_bounds__(XIO_OUT_NT) k_xio_outlet(Geo g, IoFields f, do
 }
 
 // ---------------------------------------------------------------------------
-// DIVG_io + COSQF.  Block: XD_R rows q = (j - 1) + M k; the row's divergence times
-// 1/(alpha dt) (and 1/wdiv, DIVG.f90:78-82) goes to shared memory, then each thread forms
-// whole modes X(m) = x(1) + sum_p 2 x(p) cos(...) in the sum's own order.  The cosine table
-// cq[q] = cos(q pi / (2 L)), q < 4 L, comes from the host.  SP[m + L ((j-1) + M k)] = (X(m), 0).
-__global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __restrict__ G, const double* __restrict__ cq,
+// The cosine transforms are products of a block of rows with one L x L matrix, so a block
+// takes XD_R rows (q = (j - 1) + M k) into shared memory and each thread accumulates
+// XD_RT rows x XD_MT modes in registers, in the sum's order over p; the matrix entries
+// come from global memory (L2-resident: L^2 doubles) and serve the XD_R / XD_RT thread
+// groups of the block that share a mode.
+//   CF[p L + m] = w_p cos((2m+1) p pi / (2L)), w_0 = 1, w_p = 2     (COSQF: sum over p)
+//   CB[m L + p] = 4 cos((2m+1) p pi / (2L))                         (COSQB: sum over m)
+// Both are stored summed-index-major, so C[s L + o] pairs summed index s with output index o.
+#define XD_MG (XIO_NT / (XD_R / XD_RT))  // threads per row group: 64 consecutive modes each
+
+__device__ __forceinline__ void xd_rows_times_matrix(const double* __restrict__ rows, const double* __restrict__ C,
+                                                     int L, int nr, double (&acc)[XD_RT][XD_MT], int m0, int tm, int tr) {
+#pragma unroll
+    for (int r = 0; r < XD_RT; ++r)
+#pragma unroll
+        for (int u = 0; u < XD_MT; ++u) acc[r][u] = 0.0;
+    for (int p = 0; p < L; ++p) {
+        double x[XD_RT], c[XD_MT];
+#pragma unroll
+        for (int r = 0; r < XD_RT; ++r) {
+            const int rr = tr + r * (XD_R / XD_RT);
+            x[r] = rr < nr ? rows[rr * L + p] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < XD_MT; ++u) {
+            const int m = m0 + tm + u * XD_MG;
+            c[u] = m < L ? __ldg(C + (long long)p * L + m) : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < XD_RT; ++r)
+#pragma unroll
+            for (int u = 0; u < XD_MT; ++u) acc[r][u] = acc[r][u] + x[r] * c[u];
+    }
+}
+
+// DIVG_io + COSQF: the row's divergence times 1/(alpha dt) (and 1/wdiv, DIVG.f90:78-82) goes
+// to shared memory, then SP[m + L ((j-1) + M k)] = (X(m), 0).
+__global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __restrict__ G, const double* __restrict__ CF,
                                                          double2* __restrict__ SP, const DevState* __restrict__ st,
                                                          int ns, double wdiv) {
     extern __shared__ double xsm[];
-    const int L = g.LI, M = g.M, N = g.N, Q4 = 4 * L;
-    double* tab = xsm;           // 4 L
-    double* row = xsm + Q4;      // XD_R x L
+    const int L = g.LI, M = g.M, N = g.N;
+    double* row = xsm;  // XD_R x L
     const long long nrows = (long long)M * N;
     const long long q0 = (long long)blockIdx.x * XD_R;
     const int nr = (int)min((long long)XD_R, nrows - q0);
-    for (int t = threadIdx.x; t < Q4; t += XIO_NT) tab[t] = cq[t];
     const double coe0 = 1.0 / st->dt / g.talp[ns] / wdiv;
     const double coe1 = g.dxi / 1.0;
     for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
@@ -208,19 +241,20 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __
         row[r * L + (i - 1)] = DQ * coe0;
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
-        const int r = p / L, m = p - r * L;
-        const double* x = row + r * L;
-        const int a = 2 * m + 1;
-        double X = x[0];
-        int e = 0;
-        for (int pp = 1; pp < L; ++pp) {
-            e += a;
-            if (e >= Q4) e -= Q4;
-            X = X + 2.0 * x[pp] * tab[e];
+    const int tm = threadIdx.x % XD_MG, tr = threadIdx.x / XD_MG;
+    for (int m0 = 0; m0 < L; m0 += XD_MT * XD_MG) {
+        double acc[XD_RT][XD_MT];
+        xd_rows_times_matrix(row, CF, L, nr, acc, m0, tm, tr);
+#pragma unroll
+        for (int r = 0; r < XD_RT; ++r) {
+            const int rr = tr + r * (XD_R / XD_RT);
+            if (rr >= nr) continue;
+#pragma unroll
+            for (int u = 0; u < XD_MT; ++u) {
+                const int m = m0 + tm + u * XD_MG;
+                if (m < L) SP[m + (long long)L * (q0 + rr)] = make_double2(acc[r][u], 0.0);
+            }
         }
-        const long long q = q0 + r;
-        SP[m + (long long)L * q] = make_double2(X, 0.0);
     }
 }
 
@@ -278,36 +312,38 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_ysolve(Geo g, double2* __restric
 
 // COSQB of the real parts and the scaling 1/(4 L) (the 1/N is the forward z transform's):
 // DPH(p, j, k) for the interior columns p = 1..L.
-__global__ void __launch_bounds__(XIO_NT) k_xio_dctx_inv(Geo g, const double2* __restrict__ SP, const double* __restrict__ cq,
+__global__ void __launch_bounds__(XIO_NT) k_xio_dctx_inv(Geo g, const double2* __restrict__ SP, const double* __restrict__ CB,
                                                          double* __restrict__ DPH) {
     extern __shared__ double xsm[];
-    const int L = g.LI, M = g.M, N = g.N, Q4 = 4 * L;
-    double* tab = xsm;
-    double* row = xsm + Q4;
+    const int L = g.LI, M = g.M, N = g.N;
+    double* row = xsm;  // XD_R x L
     const long long nrows = (long long)M * N;
     const long long q0 = (long long)blockIdx.x * XD_R;
     const int nr = (int)min((long long)XD_R, nrows - q0);
-    for (int t = threadIdx.x; t < Q4; t += XIO_NT) tab[t] = cq[t];
     for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
         const int r = p / L, m = p - r * L;
         row[r * L + m] = SP[m + (long long)L * (q0 + r)].x;
     }
     __syncthreads();
-    for (int p = threadIdx.x; p < nr * L; p += XIO_NT) {
-        const int r = p / L, pp = p - r * L;
-        const double* X = row + r * L;
-        double x = 0.0;
-        int e = pp;  // ((2m + 1) pp) mod 4L for m = 0
-        const int step = 2 * pp;
-        for (int m = 0; m < L; ++m) {
-            x = x + 4.0 * X[m] * tab[e];
-            e += step;
-            while (e >= Q4) e -= Q4;
+    const int tm = threadIdx.x % XD_MG, tr = threadIdx.x / XD_MG;
+    const double q4 = (double)(4 * L);
+    for (int p0 = 0; p0 < L; p0 += XD_MT * XD_MG) {
+        double acc[XD_RT][XD_MT];
+        xd_rows_times_matrix(row, CB, L, nr, acc, p0, tm, tr);
+#pragma unroll
+        for (int r = 0; r < XD_RT; ++r) {
+            const int rr = tr + r * (XD_R / XD_RT);
+            if (rr >= nr) continue;
+            const long long q = q0 + rr;
+            const int j = 1 + (int)(q % M), k = (int)(q / M);
+#pragma unroll
+            for (int u = 0; u < XD_MT; ++u) {
+                const int pp = p0 + tm + u * XD_MG;
+                if (pp < L) DPH[pidx(g, pp + 1, j, k)] = acc[r][u] / q4;
+            }
         }
-        const long long q = q0 + r;
-        const int j = 1 + (int)(q % M), k = (int)(q / M);
-        DPH[pidx(g, pp + 1, j, k)] = x / (double)Q4;
     }
+    (void)N;
 }
 
 // DIVGCK_io with TgFlowFlg: max |div G| over the cells 2..L-1, 0..1 and L (DrhoDtP = 0).
