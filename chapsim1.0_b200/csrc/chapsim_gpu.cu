@@ -866,6 +866,13 @@ void launch_io_substep(chapsim_ctx* ctx, int ns) {
 
 // ------------------------- inflow/outflow main domain ------------------------
 size_t smem_xd(const Geo& g) { return (size_t)XD_R * g.LI * sizeof(double); }
+// blocks of the outlet passes: one thread per outlet point, at most npart_red blocks (the
+// partials buffer holds 3 doubles per block of npart_red: 2 for pass a, 2 for pass b fit in 4 per
+// block of half as many)
+int xio_outlet_blocks(const chapsim_ctx* ctx) {
+    const int want = (int)(((long long)ctx->g.M * ctx->g.N + XIO_NT - 1) / XIO_NT);
+    return std::max(1, std::min(want, (3 * ctx->npart_red) / 4));
+}
 
 // SOLVERRK3_MOM_io(NS) with TgFlowFlg (src/SOLVERRK3_MOM_IO.f90:11-120), explicit viscous
 // terms: BC_TINLET_FLOW from the attached TG context (its substep NS must have run; the
@@ -880,7 +887,11 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     const int gin = (int)std::min<long long>(4LL * ctx->nsm, ((long long)(g.M + 2) * g.N + XIO_NT - 1) / XIO_NT);
     k_xio_inlet<<<gin, XIO_NT, 0, s>>>(g, f, tg->Q, tg->PR, tg->g.L, tg->g.FS);
     prof_mark(ctx);
-    k_xio_outlet<<<1, XIO_OUT_NT, 0, s>>>(g, f, ctx->xio_bc0, ctx->xio_state, ctx->st, ns);
+    const int gout = xio_outlet_blocks(ctx);
+    k_xio_outlet_a<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_part);
+    k_xio_outlet_b<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_bc0, ctx->xio_part, ctx->xio_part + 2 * gout, ctx->xio_state,
+                                           ctx->st, ns);
+    k_xio_outlet_c<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_part + 2 * gout, ctx->xio_state, ctx->st);
     prof_mark(ctx);
     k_io_divu<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     prof_mark(ctx);
@@ -903,7 +914,7 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     k_io_correct<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, nullptr);
     prof_mark(ctx);
-    ctx->launches += 11;
+    ctx->launches += 13;
 }
 
 // CFL_tg and CFL_io of one TG + main-domain step, then CFLMM = max of the two and the dt rule
@@ -989,10 +1000,11 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
                     "only the plane channel (iCase=1) with a periodic TG (iDomain=1), x-periodic main (2) or inflow/outflow "
                     "main (3) domain is supported");
     const bool xio = grid->idomain == 3;
-    // the inflow/outflow main domain has no x FFT and no x sweep: any even NCL1_io from 4 to 1024
-    if (xio ? (L < 4 || L > 1024 || L % 2) : (L < 32 || L % 32 || !valid_S(L / 32)))
+    // the inflow/outflow main domain has no x FFT and no x sweep: any even NCL1_io from 4 to 768 (the
+    // cosine transforms hold 32 rows of it in shared memory)
+    if (xio ? (L < 4 || L > 768 || L % 2) : (L < 32 || L % 32 || !valid_S(L / 32)))
         return fail(nullptr, CHAPSIM_ERR_BADARG,
-                    xio ? "NCL1_io of the inflow/outflow domain must be even, 4..1024"
+                    xio ? "NCL1_io of the inflow/outflow domain must be even, 4..768"
                         : "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");
     if (M < 32 || N < 32 || M % 32 || N % 32 || !valid_S(M / 32) || !valid_S(N / 32))
         return fail(nullptr, CHAPSIM_ERR_BADARG, "NCL1, NCL2, NCL3 must be 32*S with S in {1,2,3,4,6,8,12}");

@@ -8,10 +8,10 @@
 //
 //   k_xio_inlet      BC_TINLET_FLOW (src/BC_INLET.f90:12-61): the inlet ghost column from
 //                    the periodic TG domain's last column, the inlet face u(1) from its first
-//   k_xio_outlet     BC_COUTLET_MOM_RK3(NS) (src/BC_COUTLET_MOM_RK3.f90:16-112): U_OUTLET of
+//   k_xio_outlet_a/b/c  BC_COUTLET_MOM_RK3(NS) (src/BC_COUTLET_MOM_RK3.f90:16-112): U_OUTLET of
 //                    CONVCTION_OUTLET_U (:115-192), the convective update of the outlet
 //                    column, and the outflow scaling of CHK_MassConsv_io
-//                    (src/processing/CHK_conservation.f90:11-79); one block
+//                    (src/processing/CHK_conservation.f90:11-79)
 //   k_xio_div_dctx   DIVG_io (src/DIVG.f90:54-137) and FISHPACK's x transform COSQF
 //   k_xio_ysolve     TRID0 (src/possion3d_fishpack.f90:309-340) per (x mode, kz)
 //   k_xio_dctx_inv   COSQB and the 1/(SCALX SCALY) scaling -> DPH (interior; the ghost
@@ -33,10 +33,9 @@
 #include "io.cuh"
 
 #define XIO_NT 256
-#define XIO_OUT_NT 1024
-#define XD_R 16  // rows (j, k) per block of the cosine transforms
-#define XD_RT 4  // rows per thread
-#define XD_MT 4  // modes (or points) per thread in one pass
+#define XD_R 32  // rows (j, k) per block of the cosine transforms
+#define XD_RT 8  // rows per thread
+#define XD_MT 4  // modes (or points) per thread in one pass: two adjacent pairs
 
 // ---------------------------------------------------------------------------
 // BC_TINLET_FLOW: rows j = 0..M+1 of the TG domain's last column (LT - 1) and first
@@ -86,95 +85,109 @@ __global__ void __launch_bounds__(XIO_NT) k_fill(double* __restrict__ p, long lo
     for (long long t = (long long)blockIdx.x * XIO_NT + threadIdx.x; t < n; t += (long long)gridDim.x * XIO_NT) p[t] = v;
 }
 
-// block_sum / block_max leave the result in thread 0; these hand it to every thread
-template <int NT>
-__device__ __forceinline__ double block_sum_all(double v, double* sbuf) {
-    __shared__ double bcast;
-    const double r = block_sum<NT>(v, sbuf);
-    if (threadIdx.x == 0) bcast = r;
-    __syncthreads();
-    const double a = bcast;
-    __syncthreads();
-    return a;
-}
-template <int NT>
-__device__ __forceinline__ double block_max_all(double v, double* sbuf) {
-    __shared__ double bcast;
-    const double r = block_max<NT>(v, sbuf);
-    if (threadIdx.x == 0) bcast = r;
-    __syncthreads();
-    const double a = bcast;
-    __syncthreads();
-    return a;
-}
-
 // ---------------------------------------------------------------------------
-// BC_COUTLET_MOM_RK3(NS).  BC0: BC_CONV0(J, K, IDR) as [IDR][K][J] (M*N per component);
-// state[0] = U_OUTLET, state[1] = CHK_Mass_CONSV0_SCALING of this substep.  One block: the
-// outlet plane is M*N points, and the three phases (extremes of the outlet u, the update, the
-// fluxes) each need the whole plane.  The mass rate of the interior is zero (flow only).
-__global__ void __launch_bounds__(XIO_OUT_NT) k_xio_outlet(Geo g, IoFields f, double* __restrict__ BC0,
-                                                           double* __restrict__ state, DevState* __restrict__ st,
-                                                           int ns) {
+// BC_COUTLET_MOM_RK3(NS) in three grid-wide passes over the outlet plane (each needs a value
+// the previous one reduces over the whole plane); partial results per block, reduced by every
+// block in block order (deterministic).  BC0: BC_CONV0(J, K, IDR) as [IDR][K][J]; state[0] =
+// U_OUTLET, state[1] = CHK_Mass_CONSV0_SCALING of this substep; part: 2 doubles per block.
+// The interior mass rate is zero (flow only).
+//   a: extremes of UCC = (u(L) + u(L+1)) / 2 (CONVCTION_OUTLET_U, method two)
+//   b: U_OUTLET = (max + min) / 2, the convective update of the outlet column (:36-58), and
+//      the inlet (u face 1) and outlet (u face L+1) fluxes of CHK_MassConsv_io
+//   c: the outflow scaling of u(L+1) (:62-72)
+__global__ void __launch_bounds__(XIO_NT) k_xio_outlet_a(Geo g, IoFields f, double* __restrict__ part) {
     __shared__ double sred[32];
-    const int M = g.M, N = g.N, L = g.LI;
-    const int np = M * N;
-    // CONVCTION_OUTLET_U: UCC = (u(L) + u(L+1)) / 2 over the outlet plane, U_OUTLET = (max + min) / 2
+    const int M = g.M, np = M * g.N, L = g.LI;
     double mx = -1.0E20, mn = 1.0E20;
-    for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
+    for (int p = blockIdx.x * XIO_NT + threadIdx.x; p < np; p += gridDim.x * XIO_NT) {
         const int j = 1 + p % M, k = p / M;
         const long long c = pidx(g, L, j, k);
         const double ucc = (f.Q[c] + f.Q[c + 1]) * 0.5;
         mx = fmax(mx, ucc);
         mn = fmin(mn, ucc);
     }
-    const double umax = block_max_all<XIO_OUT_NT>(mx, sred);
-    const double umin = -block_max_all<XIO_OUT_NT>(-mn, sred);
-    const double uout = 0.5 * (umax + umin);
-    const double coe1 = g.dxi * uout;
+    const double bmax = block_max<XIO_NT>(mx, sred);
+    const double bmin = -block_max<XIO_NT>(-mn, sred);
+    if (threadIdx.x == 0) {
+        part[2 * blockIdx.x] = bmax;
+        part[2 * blockIdx.x + 1] = bmin;
+    }
+}
+
+__global__ void __launch_bounds__(XIO_NT) k_xio_outlet_b(Geo g, IoFields f, double* __restrict__ BC0,
+                                                         const double* __restrict__ parta, double* __restrict__ partb,
+                                                         double* __restrict__ state, const DevState* __restrict__ st,
+                                                         int ns) {
+    __shared__ double sred[32];
+    __shared__ double uo;
+    if (threadIdx.x == 0) {
+        double mx = -1.0E20, mn = 1.0E20;
+        for (int b = 0; b < (int)gridDim.x; ++b) {
+            mx = fmax(mx, parta[2 * b]);
+            mn = fmin(mn, parta[2 * b + 1]);
+        }
+        uo = 0.5 * (mx + mn);
+        if (blockIdx.x == 0) state[0] = uo;
+    }
+    __syncthreads();
+    const int M = g.M, np = M * g.N, L = g.LI;
+    const double coe1 = g.dxi * uo;
     const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns];
-    for (int idr = 0; idr < 3; ++idr) {
-        const int n2i = idr == 1 ? 2 : 1;
-        for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
-            const int j = 1 + p % M, k = p / M;
-            if (j < n2i) continue;
-            const long long c = pidx(g, L, j, k) + idr * g.FS;
+    double fin = 0.0, fout = 0.0;
+    for (int p = blockIdx.x * XIO_NT + threadIdx.x; p < np; p += gridDim.x * XIO_NT) {
+        const int j = 1 + p % M, k = p / M;
+        const long long cr = pidx(g, L, j, k);
+        const double rho = (f.RHO[cr] + f.RHO[cr + 1]) * 0.5;
+        for (int idr = 0; idr < 3; ++idr) {
+            if (idr == 1 && j < 2) continue;  // N2I = 2 for v
+            const long long c = cr + idr * g.FS;
             const long long b = (long long)idr * np + (long long)(j - 1) + (long long)M * k;
             const double bc_conv = -(f.G[c + 1] - f.G[c]) * coe1;
             const double bc_rhs = tg * bc_conv + tr * BC0[b];
             BC0[b] = bc_conv;
             const double gn = f.G[c + 1] + dt * bc_rhs;
             f.G[c + 1] = gn;
-            const long long cr = pidx(g, L, j, k);
-            const double rho = (f.RHO[cr] + f.RHO[cr + 1]) * 0.5;
             f.Q[c + 1] = gn / rho;
+        }
+        const double coe2 = 1.0 / g.dyfi[j] / 1.0;
+        fin += f.G[pidx(g, 1, j, k)] * coe2;
+        fout += f.G[cr + 1] * coe2;
+    }
+    const double bin = block_sum<XIO_NT>(fin, sred);
+    const double bout = block_sum<XIO_NT>(fout, sred);
+    if (threadIdx.x == 0) {
+        partb[2 * blockIdx.x] = bin;
+        partb[2 * blockIdx.x + 1] = bout;
+    }
+}
+
+__global__ void __launch_bounds__(XIO_NT) k_xio_outlet_c(Geo g, IoFields f, const double* __restrict__ partb,
+                                                         double* __restrict__ state, DevState* __restrict__ st) {
+    __shared__ double sc;
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < (int)gridDim.x; ++q) {
+            a += partb[2 * q];
+            b += partb[2 * q + 1];
+        }
+        const double flux_in = a / g.dzi, flux_out = b / g.dzi;
+        const double mass_rate = 0.0;
+        sc = (flux_in - mass_rate) / flux_out;
+        if (blockIdx.x == 0) {
+            state[1] = sc;
+            if (!(sc == sc) || !(state[0] == state[0])) atomicOr(&st->err, CHS_EBIT_NAN);
         }
     }
     __syncthreads();
-    // CHK_MassConsv_io: inlet (u face 1) and outlet (u face L+1) fluxes
-    double fin = 0.0, fout = 0.0;
-    for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
-        const int j = 1 + p % M, k = p / M;
-        const double coe2 = 1.0 / g.dyfi[j] / 1.0;
-        fin += f.G[pidx(g, 1, j, k)] * coe2;
-        fout += f.G[pidx(g, L + 1, j, k)] * coe2;
-    }
-    const double flux_in = block_sum_all<XIO_OUT_NT>(fin, sred) / g.dzi;
-    const double flux_out = block_sum_all<XIO_OUT_NT>(fout, sred) / g.dzi;
-    const double mass_rate = 0.0;
-    const double scaling = (flux_in - mass_rate) / flux_out;
-    for (int p = threadIdx.x; p < np; p += XIO_OUT_NT) {
+    const double scaling = sc;
+    const int M = g.M, np = M * g.N, L = g.LI;
+    for (int p = blockIdx.x * XIO_NT + threadIdx.x; p < np; p += gridDim.x * XIO_NT) {
         const int j = 1 + p % M, k = p / M;
         const long long c = pidx(g, L + 1, j, k);
         const double go = f.G[c];
         const double gn = go * (scaling - 1.0) + go;
         f.G[c] = gn;
         f.Q[c] = gn / ((f.RHO[c - 1] + f.RHO[c]) * 0.5);
-    }
-    if (threadIdx.x == 0) {
-        state[0] = uout;
-        state[1] = scaling;
-        if (!(scaling == scaling) || !(uout == uout)) atomicOr(&st->err, CHS_EBIT_NAN);
     }
 }
 
@@ -187,7 +200,10 @@ __global__ void __launch_bounds__(XIO_OUT_NT) k_xio_outlet(Geo g, IoFields f, do
 //   CF[p L + m] = w_p cos((2m+1) p pi / (2L)), w_0 = 1, w_p = 2     (COSQF: sum over p)
 //   CB[m L + p] = 4 cos((2m+1) p pi / (2L))                         (COSQB: sum over m)
 // Both are stored summed-index-major, so C[s L + o] pairs summed index s with output index o.
-#define XD_MG (XIO_NT / (XD_R / XD_RT))  // threads per row group: 64 consecutive modes each
+#define XD_MG (XIO_NT / (XD_R / XD_RT))  // threads per row group (64): a pass covers 2 * XD_MG * 2 outputs
+// output u (0..3) of thread tm in the pass starting at o0: o0 + 2 tm + (u >> 1) * 2 XD_MG + (u & 1);
+// the pairs are 16-byte loads of the matrix row (L is even)
+__device__ __forceinline__ int xd_out(int o0, int tm, int u) { return o0 + 2 * tm + (u >> 1) * 2 * XD_MG + (u & 1); }
 
 __device__ __forceinline__ void xd_rows_times_matrix(const double* __restrict__ rows, const double* __restrict__ C,
                                                      int L, int nr, double (&acc)[XD_RT][XD_MT], int m0, int tm, int tr) {
@@ -203,9 +219,12 @@ __device__ __forceinline__ void xd_rows_times_matrix(const double* __restrict__ 
             x[r] = rr < nr ? rows[rr * L + p] : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < XD_MT; ++u) {
-            const int m = m0 + tm + u * XD_MG;
-            c[u] = m < L ? __ldg(C + (long long)p * L + m) : 0.0;
+        for (int h = 0; h < XD_MT / 2; ++h) {
+            const int m = xd_out(m0, tm, 2 * h);
+            double2 cc = make_double2(0.0, 0.0);
+            if (m < L) cc = __ldg(reinterpret_cast<const double2*>(C + (long long)p * L + m));
+            c[2 * h] = cc.x;
+            c[2 * h + 1] = cc.y;
         }
 #pragma unroll
         for (int r = 0; r < XD_RT; ++r)
@@ -216,7 +235,7 @@ __device__ __forceinline__ void xd_rows_times_matrix(const double* __restrict__ 
 
 // DIVG_io + COSQF: the row's divergence times 1/(alpha dt) (and 1/wdiv, DIVG.f90:78-82) goes
 // to shared memory, then SP[m + L ((j-1) + M k)] = (X(m), 0).
-__global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __restrict__ G, const double* __restrict__ CF,
+__global__ void __launch_bounds__(XIO_NT, 2) k_xio_div_dctx(Geo g, const double* __restrict__ G, const double* __restrict__ CF,
                                                          double2* __restrict__ SP, const DevState* __restrict__ st,
                                                          int ns, double wdiv) {
     extern __shared__ double xsm[];
@@ -242,7 +261,7 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __
     }
     __syncthreads();
     const int tm = threadIdx.x % XD_MG, tr = threadIdx.x / XD_MG;
-    for (int m0 = 0; m0 < L; m0 += XD_MT * XD_MG) {
+    for (int m0 = 0; m0 < L; m0 += XD_MT * XD_MG) {  // XD_MT * XD_MG = 256 outputs per pass
         double acc[XD_RT][XD_MT];
         xd_rows_times_matrix(row, CF, L, nr, acc, m0, tm, tr);
 #pragma unroll
@@ -251,7 +270,7 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_div_dctx(Geo g, const double* __
             if (rr >= nr) continue;
 #pragma unroll
             for (int u = 0; u < XD_MT; ++u) {
-                const int m = m0 + tm + u * XD_MG;
+                const int m = xd_out(m0, tm, u);
                 if (m < L) SP[m + (long long)L * (q0 + rr)] = make_double2(acc[r][u], 0.0);
             }
         }
@@ -312,7 +331,7 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_ysolve(Geo g, double2* __restric
 
 // COSQB of the real parts and the scaling 1/(4 L) (the 1/N is the forward z transform's):
 // DPH(p, j, k) for the interior columns p = 1..L.
-__global__ void __launch_bounds__(XIO_NT) k_xio_dctx_inv(Geo g, const double2* __restrict__ SP, const double* __restrict__ CB,
+__global__ void __launch_bounds__(XIO_NT, 2) k_xio_dctx_inv(Geo g, const double2* __restrict__ SP, const double* __restrict__ CB,
                                                          double* __restrict__ DPH) {
     extern __shared__ double xsm[];
     const int L = g.LI, M = g.M, N = g.N;
@@ -338,7 +357,7 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_dctx_inv(Geo g, const double2* _
             const int j = 1 + (int)(q % M), k = (int)(q / M);
 #pragma unroll
             for (int u = 0; u < XD_MT; ++u) {
-                const int pp = p0 + tm + u * XD_MG;
+                const int pp = xd_out(p0, tm, u);
                 if (pp < L) DPH[pidx(g, pp + 1, j, k)] = acc[r][u] / q4;
             }
         }

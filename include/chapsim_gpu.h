@@ -39,7 +39,7 @@ typedef struct chapsim_ctx chapsim_ctx_t;
  * separate idomain = 1 context, see chapsim_xinout_attach).
  * L and N must factor into 2s and 3s (FFT lengths), L, M, N must be
  * multiples of 32 between 32 and 384; with idomain = 3, L = NCL1_io is any even
- * number from 4 to 1024. */
+ * number from 4 to 768. */
 typedef struct {
     int32_t ncl1;   /* L */
     int32_t ncl2;   /* M */
