@@ -249,6 +249,8 @@ def heated_measure(args, local, dist, ws, steps):
     knots = dh_list[(dh_list >= lo) & (dh_list <= hi)]
     train = np.concatenate([knots, rng.choice(field, 4000, replace=False), rng.uniform(lo, hi, 2000)])
     ch.mlp_init(lo, hi, seed=11)
+    act = gpu.MLP_CUBIC if args.mlp_activation == "cubic" else gpu.MLP_TANH
+    ch.mlp_set_activation(act)
     t0 = time.perf_counter()
     loss = None
     for it, lr in MLP_SCHEDULE:
@@ -284,6 +286,7 @@ def heated_measure(args, local, dist, ws, steps):
     chm.advance(args.warmup, DT0, DTMIN, CFLGV)
     ms_mt = timed_m(steps)
     chm.mlp_init(lo, hi, seed=11)
+    chm.mlp_set_activation(act)
     chm.mlp_set_params(params)
     chm.thermal_use_mlp(True)
     chm.advance(args.warmup, DT0, DTMIN, CFLGV)
@@ -325,6 +328,7 @@ def heated_measure(args, local, dist, ws, steps):
         "clocks": clk,
         "variants": {"learned_properties": {
             "value": v_mlp, "unit": UNIT, "ms_per_step": ms_m / steps, "speedup_vs_table": v_mlp / v_table,
+            "activation": args.mlp_activation,
             "judge_max_rel_err": judge, "bound": MLP_BOUND, "within_bound": max(judge.values()) <= MLP_BOUND,
             "training": {"samples": int(train.size), "iterations": sum(i for i, _ in MLP_SCHEDULE),
                          "seconds": t_train, "final_loss": loss},
@@ -895,6 +899,9 @@ def main():
                     help="kernel variant bits instead of timing them (bit 0: sequential y-solve; bits 1-2: "
                          "right-hand side 0 fused, 1 split, 2 fused with bulk-copy staging; bit 3: fused plane "
                          "transforms; bit 4: two-way y-solve); -1 times the variants and keeps the fastest")
+    ap.add_argument("--mlp-activation", default="cubic", choices=["cubic", "tanh"],
+                    help="hidden-layer activation of the learned property model (the clamped cubic needs no "
+                         "special-function unit)")
     ap.add_argument("--no-pdl", action="store_true",
                     help="launch the step's kernels without programmatic dependent launch")
     args = ap.parse_args()

@@ -25,6 +25,8 @@ ERR_NAMES = {0: "CHAPSIM_OK", -1: "CHAPSIM_ERR_CUDA", -2: "CHAPSIM_ERR_NAN", -3:
              -4: "CHAPSIM_ERR_TABLE_RANGE", -5: "CHAPSIM_ERR_TIMEOUT", -6: "CHAPSIM_ERR_BADARG",
              -7: "CHAPSIM_ERR_NOMEM"}
 
+MLP_TANH, MLP_CUBIC = 0, 1
+
 EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_string", "chapsim_upload_fields",
             "chapsim_download_fields", "chapsim_set_dt", "chapsim_get_dt", "chapsim_cfl_tg", "chapsim_step_begin",
             "chapsim_rk_substep_tg", "chapsim_advance_tg", "chapsim_divgck_tg", "chapsim_fft99_pois3d",
@@ -41,7 +43,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
             "chapsim_pp_mean_zx_io", "chapsim_download_pp_means_io",
             "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write",
-            "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
+            "chapsim_mlp_set_activation", "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
 PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
@@ -198,6 +200,7 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_download_io_fields.argtypes = [vp, _dp, _dp, _dp]
     L.chapsim_rk_substep_io.argtypes = [vp, ctypes.c_int32]
     L.chapsim_xinout_attach.argtypes = [vp, vp]
+    L.chapsim_mlp_set_activation.argtypes = [vp, ctypes.c_int32]
     L.chapsim_advance_xinout.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp,
                                          _dp]
     L.chapsim_divgck_xinout.argtypes = [vp, _dp]
@@ -563,6 +566,11 @@ class ChannelTG:
     def mlp_init(self, dh_lo, dh_hi, seed=2024):
         """Random-initialised 1-64-64-6 MLP for rho*h in [dh_lo, dh_hi] (needs the property table)."""
         self._check(self.lib.chapsim_mlp_init(self.h, float(dh_lo), float(dh_hi), int(seed)))
+
+    def mlp_set_activation(self, act):
+        """Hidden-layer activation: MLP_TANH (default) or MLP_CUBIC, the clamped cubic
+        c = clamp(z, -1, 1), h = c (3 - c^2) / 2.  Set it before training."""
+        self._check(self.lib.chapsim_mlp_set_activation(self.h, int(act)))
 
     def mlp_params(self):
         p = np.zeros(self.MLP_NPARAM, np.float32)

@@ -215,6 +215,7 @@ struct chapsim_ctx {
     int mlp_cap = 0, mlp_step = 0;
     MlpNorm mlp_norm{};
     bool mlp_ready = false, use_mlp = false;
+    int mlp_act = MLP_ACT_TANH;   // hidden-layer activation (chapsim_mlp_set_activation)
     unsigned int* mlp_judge = nullptr;
     // asynchronous field dumps (chapsim_dump_begin / chapsim_dump_write)
     double* dump_dev = nullptr;   // packed interiors of the dumped fields, then dt
@@ -778,9 +779,13 @@ void launch_thermal_substep_t(chapsim_ctx* ctx, int ns) {
     if (ctx->use_mlp) {
         const long long tiles = (tot + MLP_TILE - 1) / MLP_TILE;
         MlpOut out{ctx->tf.ENTH, ctx->tf.TEMP, f.DEN, f.MU, ctx->tf.KAP, ctx->tf.HCP, f.RHO, f.MU0};
-        k_mlp_infer<true><<<(int)std::min<long long>(tiles, 4LL * ctx->nsm), MLP_NT, MLP_INF_SMEM, s>>>(
-            ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, g, tot,
-            ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
+        const int gi = (int)std::min<long long>(tiles, 4LL * ctx->nsm);
+        if (ctx->mlp_act == MLP_ACT_CUBIC)
+            k_mlp_infer<true, MLP_ACT_CUBIC><<<gi, MLP_NT, MLP_INF_SMEM, s>>>(
+                ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, g, tot, ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
+        else
+            k_mlp_infer<true, MLP_ACT_TANH><<<gi, MLP_NT, MLP_INF_SMEM, s>>>(
+                ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, g, tot, ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
         prof_mark(ctx);
         if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
         else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
@@ -2224,9 +2229,13 @@ int mlp_check_err(chapsim_ctx* ctx) {
 // one pass of k_mlp_train over the current training set; gradients summed into mlp_grad
 int mlp_pass(chapsim_ctx* ctx, int n) {
     const int tiles = (n + MLP_TILE - 1) / MLP_TILE;
-    k_mlp_train<<<tiles, MLP_NT, MLP_TRN_SMEM, ctx->stream>>>(ctx->mlp_par, mlp_ops(ctx), ctx->mlp_xs, ctx->mlp_ys, n,
-                                                              1.0f / ((float)n * MLP_OUT), ctx->mlp_grad,
-                                                              ctx->mlp_loss, &ctx->st->err);
+    const float inv = 1.0f / ((float)n * MLP_OUT);
+    if (ctx->mlp_act == MLP_ACT_CUBIC)
+        k_mlp_train<MLP_ACT_CUBIC><<<tiles, MLP_NT, MLP_TRN_SMEM, ctx->stream>>>(
+            ctx->mlp_par, mlp_ops(ctx), ctx->mlp_xs, ctx->mlp_ys, n, inv, ctx->mlp_grad, ctx->mlp_loss, &ctx->st->err);
+    else
+        k_mlp_train<MLP_ACT_TANH><<<tiles, MLP_NT, MLP_TRN_SMEM, ctx->stream>>>(
+            ctx->mlp_par, mlp_ops(ctx), ctx->mlp_xs, ctx->mlp_ys, n, inv, ctx->mlp_grad, ctx->mlp_loss, &ctx->st->err);
     ctx->launches += 1;
     CK(cudaGetLastError());
     return CHAPSIM_OK;
@@ -2249,9 +2258,12 @@ extern "C" int chapsim_mlp_init(chapsim_ctx_t* ctx, double dh_lo, double dh_hi, 
         ctx->mlp_w3 = ctx->mlp_w2t + 64 * 64;
         ctx->mlp_w2h = reinterpret_cast<__half*>(ctx->mlp_w3 + 16 * 64);
         ctx->mlp_w3h = ctx->mlp_w2h + 64 * 64;
-        CK(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_TRN_SMEM));
-        CK(cudaFuncSetAttribute(k_mlp_infer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
-        CK(cudaFuncSetAttribute(k_mlp_infer<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_train<MLP_ACT_TANH>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_TRN_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_train<MLP_ACT_CUBIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_TRN_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_infer<false, MLP_ACT_TANH>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_infer<true, MLP_ACT_TANH>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_infer<false, MLP_ACT_CUBIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
+        CK(cudaFuncSetAttribute(k_mlp_infer<true, MLP_ACT_CUBIC>, cudaFuncAttributeMaxDynamicSharedMemorySize, MLP_INF_SMEM));
     }
     // output scaling from the table over the trained range
     const int ns = 4097;
@@ -2295,6 +2307,14 @@ extern "C" int chapsim_mlp_init(chapsim_ctx_t* ctx, double dh_lo, double dh_hi, 
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->mlp_ready = true;
     return CHAPSIM_OK;
+}
+
+extern "C" int chapsim_mlp_set_activation(chapsim_ctx_t* ctx, int32_t act) {
+    if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
+    if (act != CHAPSIM_MLP_TANH && act != CHAPSIM_MLP_CUBIC)
+        return fail(ctx, CHAPSIM_ERR_BADARG, "activation must be CHAPSIM_MLP_TANH or CHAPSIM_MLP_CUBIC");
+    ctx->mlp_act = act;
+    return drop_step_graph(ctx);
 }
 
 extern "C" int chapsim_mlp_set_params(chapsim_ctx_t* ctx, const float* params) {
@@ -2377,8 +2397,12 @@ extern "C" int chapsim_mlp_infer_points(chapsim_ctx_t* ctx, int64_t npts, const 
     const long long tiles = (npts + MLP_TILE - 1) / MLP_TILE;
     const int grid = (int)std::min<long long>(tiles, 4LL * ctx->nsm);
     MlpOut out{o, o + npts, o + 2 * npts, o + 3 * npts, o + 4 * npts, o + 5 * npts, nullptr, nullptr};
-    k_mlp_infer<false><<<grid, MLP_NT, MLP_INF_SMEM, ctx->stream>>>(ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab,
-                                                                   ctx->g, npts, dd, out, ctx->pstat, &ctx->st->err);
+    if (ctx->mlp_act == MLP_ACT_CUBIC)
+        k_mlp_infer<false, MLP_ACT_CUBIC><<<grid, MLP_NT, MLP_INF_SMEM, ctx->stream>>>(
+            ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, ctx->g, npts, dd, out, ctx->pstat, &ctx->st->err);
+    else
+        k_mlp_infer<false, MLP_ACT_TANH><<<grid, MLP_NT, MLP_INF_SMEM, ctx->stream>>>(
+            ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, ctx->g, npts, dd, out, ctx->pstat, &ctx->st->err);
     ctx->launches += 1;
     CK(cudaGetLastError());
     double* outs[6] = {h, t, d, m, k, cp};

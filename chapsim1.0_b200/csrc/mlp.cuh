@@ -1,4 +1,5 @@
-// Learned property model: a 1 -> 64 -> 64 -> 6 tanh MLP from rho*h to the
+// Learned property model: a 1 -> 64 -> 64 -> 6 MLP (tanh, or the clamped cubic
+// below) from rho*h to the
 // six outputs of THERM_PROP_UPDATE_FROM_DH (ENTHALPY, TEMPERATURE, DENSITY,
 // Viscousity, THERMCONDT, HEATCAP), used in place of the table search inside
 // its trained range; the table search stays the fallback outside it and the
@@ -25,6 +26,12 @@
 // Every wait is bounded: an mbarrier wait that exceeds its clock budget sets
 // an error bit and returns, and TMEM is always released before the kernel
 // ends.
+//
+// Activations (template ACT): MLP_ACT_TANH, or MLP_ACT_CUBIC, the clamped cubic
+//   c = clamp(z, -1, 1),  h = c (3 - c^2) / 2,  dh/dz = 3 (1 - c^2) / 2  (0 outside [-1, 1]),
+// a C1 saturating activation that takes only min/max and multiply-adds: inference evaluates
+// it on FP16 pairs on the FMA pipe, where tanh needs the special-function unit (one
+// tanh.approx.f16x2 per pair) and bounds the kernel there.
 #pragma once
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -210,13 +217,57 @@ __device__ __forceinline__ uint32_t tanh2_f16(__half2 pre) {
 // b1 rounded to FP16.  The input's own rounding would otherwise be 2^-12 of the
 // trained range, a visible shift in the steep part of the property curves.
 
+#define MLP_ACT_TANH 0
+#define MLP_ACT_CUBIC 1
+// FP32 activation and its derivative (training), in an order the CPU oracle repeats exactly
+template <int ACT>
+__device__ __forceinline__ float act_f(float z) {
+    if constexpr (ACT == MLP_ACT_TANH) {
+        return tanhf(z);
+    } else {
+        const float c = fminf(fmaxf(z, -1.f), 1.f);
+        return __fmul_rn(c, __fsub_rn(1.5f, __fmul_rn(__fmul_rn(0.5f, c), c)));
+    }
+}
+template <int ACT>
+__device__ __forceinline__ float act_d(float z, float h) {
+    if constexpr (ACT == MLP_ACT_TANH) {
+        return 1.f - h * h;
+    } else {
+        const float c = fminf(fmaxf(z, -1.f), 1.f);
+        return __fmul_rn(1.5f, __fsub_rn(1.f, __fmul_rn(c, c)));
+    }
+}
+// The clamped cubic on an FP16 pair: each product rounded to FP16, the multiply-add once
+__device__ __forceinline__ uint32_t cubic2_f16(__half2 pre) {
+    const __half2 c = __hmin2(__hmax2(pre, __float2half2_rn(-1.f)), __float2half2_rn(1.f));
+    const __half2 s = __hfma2(__hmul2(c, c), __float2half2_rn(-0.5f), __float2half2_rn(1.5f));
+    const __half2 h = __hmul2(c, s);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+__device__ __forceinline__ uint32_t cubic2_f16(float a, float b) {
+    uint32_t in;
+    asm("cvt.rn.f16x2.f32 %0, %1, %2;" : "=r"(in) : "f"(b), "f"(a));
+    return cubic2_f16(*reinterpret_cast<const __half2*>(&in));
+}
+template <int ACT>
+__device__ __forceinline__ uint32_t act2_f16(__half2 pre) {
+    if constexpr (ACT == MLP_ACT_TANH) return tanh2_f16(pre);
+    else return cubic2_f16(pre);
+}
+template <int ACT>
+__device__ __forceinline__ uint32_t act2_f16(float a, float b) {
+    if constexpr (ACT == MLP_ACT_TANH) return tanh2_f16(a, b);
+    else return cubic2_f16(a, b);
+}
+
 // 16-byte chunk c (k = 8c .. 8c+7) of row r of an R x 64 K-major operand
 __device__ __forceinline__ void put_chunk(unsigned char* base, int R, int r, int c, uint32_t a, uint32_t b, uint32_t d,
                                           uint32_t e) {
     *reinterpret_cast<uint4*>(base + umma_off(R, r, 8 * c)) = make_uint4(a, b, d, e);
 }
 
-template <bool FIELD>
+template <bool FIELD, int ACT>
 __global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict__ par, MlpOperands ops, MlpNorm nm,
                                                          PropTab tb, Geo g, long long npts, const double* __restrict__ dh,
                                                          MlpOut out, PropStatus* ps, unsigned int* err) {
@@ -300,7 +351,7 @@ __global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict
             for (int u = 0; u < 4; ++u) {
                 const __half2 w = *reinterpret_cast<const __half2*>(&wv[u]);
                 const __half2 b = *reinterpret_cast<const __half2*>(&bv[u]);
-                hv[u] = tanh2_f16(__hfma2(w, xh2, __hfma2(w, xl2, b)));
+                hv[u] = act2_f16<ACT>(__hfma2(w, xh2, __hfma2(w, xl2, b)));
             }
             put_chunk(sA, MLP_TILE, tid, c, hv[0], hv[1], hv[2], hv[3]);
         }
@@ -329,8 +380,9 @@ __global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict
             const float4 b0 = sb2[2 * c], b1 = sb2[2 * c + 1];
             const uint32_t* a = acc + 8 * c;
             auto f = [&](int e) { return __uint_as_float(a[e]); };
-            put_chunk(sA, MLP_TILE, tid, c, tanh2_f16(f(0) + b0.x, f(1) + b0.y), tanh2_f16(f(2) + b0.z, f(3) + b0.w),
-                      tanh2_f16(f(4) + b1.x, f(5) + b1.y), tanh2_f16(f(6) + b1.z, f(7) + b1.w));
+            put_chunk(sA, MLP_TILE, tid, c, act2_f16<ACT>(f(0) + b0.x, f(1) + b0.y),
+                      act2_f16<ACT>(f(2) + b0.z, f(3) + b0.w), act2_f16<ACT>(f(4) + b1.x, f(5) + b1.y),
+                      act2_f16<ACT>(f(6) + b1.z, f(7) + b1.w));
         }
         fence_async_smem();
         tc_fence_before();
@@ -386,6 +438,7 @@ __global__ void __launch_bounds__(MLP_NT, 4) k_mlp_infer(const float* __restrict
 constexpr int MLP_TRN_SMEM = 1024 + 3 * 64 * 64 * 2 + 16 * 64 * 2 + 3 * 128 * 64 * 2 + 128 * 128 * 2 + 64 * 128 * 2 +
                              128 * 64 * 4;
 
+template <int ACT>
 __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ par, MlpOperands ops,
                                                       const float* __restrict__ xs, const float* __restrict__ ys,
                                                       int ntr, float inv_count, float* __restrict__ grad,
@@ -432,8 +485,9 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
     const float x = live ? xs[p] : 0.f;
     // ---- forward ----
     float h1[MLP_H], h2[MLP_H], acc[16];
+    float dz2[MLP_H];  // holds the second layer's activation derivative until the backward pass scales it
 #pragma unroll
-    for (int i = 0; i < MLP_H; ++i) h1[i] = tanhf(fmaf(sw1[i], x, sb1[i]));
+    for (int i = 0; i < MLP_H; ++i) h1[i] = act_f<ACT>(fmaf(sw1[i], x, sb1[i]));
     put_row64(sH1, 128, tid, h1);
     fence_async_smem();
     tc_fence_before();
@@ -452,7 +506,11 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
         tmem_ld16(tmem + lane_base + 16 * q, acc);
         tmem_ld_wait();
 #pragma unroll
-        for (int c = 0; c < 16; ++c) h2[16 * q + c] = tanhf(acc[c] + sb2[16 * q + c]);
+        for (int c = 0; c < 16; ++c) {
+            const float z = acc[c] + sb2[16 * q + c];
+            h2[16 * q + c] = act_f<ACT>(z);
+            dz2[16 * q + c] = act_d<ACT>(z, h2[16 * q + c]);
+        }
     }
     put_row64(sH2, 128, tid, h2);
     fence_async_smem();
@@ -484,13 +542,12 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
     sX[tid] = live ? x : 0.f;
 #pragma unroll
     for (int j = 0; j < MLP_H; ++j) sRed[tid * MLP_H + j] = h2[j];
-    float dz2[MLP_H];
 #pragma unroll
     for (int j = 0; j < MLP_H; ++j) {
         float s = 0.f;
 #pragma unroll
         for (int k = 0; k < MLP_OUT; ++k) s = fmaf(dy[k], sW3f[k * MLP_H + j], s);
-        dz2[j] = s * (1.f - h2[j] * h2[j]);
+        dz2[j] = s * dz2[j];
     }
     __syncthreads();
     // dW3[k][j] = sum_p dy[p][k] h2[p][j], db3, loss: column sums over the tile
@@ -552,7 +609,7 @@ __global__ void __launch_bounds__(MLP_NT) k_mlp_train(const float* __restrict__ 
 #pragma unroll
         for (int c = 0; c < 16; ++c) {
             const int i = 16 * q + c;
-            sRed[tid * MLP_H + i] = live ? acc[c] * (1.f - h1[i] * h1[i]) : 0.f;
+            sRed[tid * MLP_H + i] = live ? acc[c] * act_d<ACT>(fmaf(sw1[i], x, sb1[i]), h1[i]) : 0.f;
         }
     }
     // dL/dW2: TMEM lane j (threads 0..63) holds row j

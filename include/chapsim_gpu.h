@@ -347,6 +347,14 @@ int chapsim_download_thermal_fields(chapsim_ctx_t* ctx, double* dh, double* h, d
  * The property table must be set first (chapsim_prop_table_init). */
 int chapsim_mlp_init(chapsim_ctx_t* ctx, double dh_lo, double dh_hi, uint64_t seed);
 int chapsim_mlp_set_params(chapsim_ctx_t* ctx, const float* params);
+/* Hidden-layer activation of training and inference (default CHAPSIM_MLP_TANH).
+ * CHAPSIM_MLP_CUBIC is the clamped cubic c = clamp(z, -1, 1), h = c (3 - c^2) / 2:
+ * inference evaluates it with multiply-adds on FP16 pairs instead of the
+ * special-function unit's tanh.  Set it before training; parameters trained
+ * with one activation do not carry over to the other. */
+#define CHAPSIM_MLP_TANH 0
+#define CHAPSIM_MLP_CUBIC 1
+int chapsim_mlp_set_activation(chapsim_ctx_t* ctx, int32_t act);
 /* params (4678) and/or norm (14: dh_lo, dh_hi, off[6], scale[6]); either may be NULL */
 int chapsim_mlp_get_params(chapsim_ctx_t* ctx, float* params, double* norm);
 /* Gradient of the mean squared error of the normalised outputs against the

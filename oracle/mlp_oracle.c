@@ -16,6 +16,11 @@
  *
  * Parameter layout (FP32): w1[64], b1[64], W2[64][64] (out, in), b2[64],
  * W3[6][64], b3[6].  norm: x_lo, x_hi, off[6], scale[6].
+ *
+ * Activation (orc_mlp_set_activation): 0 tanh, 1 the clamped cubic
+ * c = clamp(z, -1, 1), h = c (3 - c^2) / 2, h' = 3 (1 - c^2) / 2, evaluated in
+ * the GPU's operation order (FP32 for training; FP16 pair arithmetic for
+ * inference, each product rounded to FP16 and the multiply-add rounded once).
  */
 #include <math.h>
 #include <stdint.h>
@@ -48,17 +53,41 @@ static float bf16r(float f) {
  * tanh.approx.f16x2), so its input and its result are FP16 values. */
 static float f16r(float f) { return (float)(_Float16)f; }
 
+static int g_act = 0;
+void orc_mlp_set_activation(int act) { g_act = act ? 1 : 0; }
+
+static float act_f(float z) {
+    if (!g_act) return tanhf(z);
+    const float c = z < -1.f ? -1.f : (z > 1.f ? 1.f : z);
+    return c * (1.5f - 0.5f * c * c);
+}
+static float act_d(float z, float h) {
+    if (!g_act) return 1.f - h * h;
+    const float c = z < -1.f ? -1.f : (z > 1.f ? 1.f : z);
+    return 1.5f * (1.f - c * c);
+}
+/* inference form on an FP16 pre-activation: the GPU's tanh.approx.f16x2 (emulated by the exact
+ * tanh rounded to FP16) or the clamped cubic in FP16 pair arithmetic */
+static float act_inf(float pre) {
+    if (!g_act) return f16r(tanhf(pre));
+    const float c = pre < -1.f ? -1.f : (pre > 1.f ? 1.f : pre);
+    const float c2 = f16r(c * c);                                   /* exact product, one rounding */
+    const float s = (float)(_Float16)((double)c2 * -0.5 + 1.5);      /* fused: one rounding */
+    return f16r(c * s);
+}
+
 static float xnorm(const double* norm, double dh) {
     const double lo = (double)(float)norm[0], hi = (double)(float)norm[1];
     return (float)(2.0 * (dh - lo) / (hi - lo) - 1.0);
 }
 
-static void forward(const float* p, float x, float* h1, float* h2, float* y) {
-    for (int i = 0; i < H; ++i) h1[i] = tanhf(fmaf(p[P_W1 + i], x, p[P_B1 + i]));
+static void forward(const float* p, float x, float* h1, float* h2, float* z2, float* y) {
+    for (int i = 0; i < H; ++i) h1[i] = act_f(fmaf(p[P_W1 + i], x, p[P_B1 + i]));
     for (int j = 0; j < H; ++j) {
         double a = 0.0;
         for (int i = 0; i < H; ++i) a += (double)bf16r(h1[i]) * (double)bf16r(p[P_W2 + j * H + i]);
-        h2[j] = tanhf((float)a + p[P_B2 + j]);
+        z2[j] = (float)a + p[P_B2 + j];
+        h2[j] = act_f(z2[j]);
     }
     for (int k = 0; k < NO; ++k) {
         double a = 0.0;
@@ -81,12 +110,12 @@ static void forward_inf(const float* p, float x, float* h1, float* h2, float* y)
         const double w = (double)f16r(p[P_W1 + i]), b = (double)f16r(p[P_B1 + i]);
         const double inner = (double)(_Float16)(w * (double)xl + b);
         const float pre = (float)(_Float16)(w * (double)xh + inner);
-        h1[i] = f16r(tanhf(pre));
+        h1[i] = act_inf(pre);
     }
     for (int j = 0; j < H; ++j) {
         double a = 0.0;
         for (int i = 0; i < H; ++i) a += (double)h1[i] * (double)f16r(p[P_W2 + j * H + i]);
-        h2[j] = f16r(tanhf(f16r((float)a + p[P_B2 + j])));
+        h2[j] = act_inf(f16r((float)a + p[P_B2 + j]));
     }
     for (int k = 0; k < NO; ++k) {
         double a = 0.0;
@@ -118,8 +147,8 @@ double orc_mlp_gradients(void* tab, const float* p, const double* norm, int n, c
         double o[6];
         if (orc_prop_point(tab, dh[q], o)) return -1.0;
         const float x = xnorm(norm, dh[q]);
-        float h1[H], h2[H], y[NO], dy[NO], dz2[H];
-        forward(p, x, h1, h2, y);
+        float h1[H], h2[H], z2[H], y[NO], dy[NO], dz2[H];
+        forward(p, x, h1, h2, z2, y);
         for (int k = 0; k < NO; ++k) {
             const float t = (float)((o[k] - (double)(float)norm[2 + k]) / (double)(float)norm[2 + NO + k]);
             const float e = y[k] - t;
@@ -133,13 +162,13 @@ double orc_mlp_gradients(void* tab, const float* p, const double* norm, int n, c
                 s = fmaf(dy[k], p[P_W3 + k * H + j], s);
                 grad[P_W3 + k * H + j] += (double)(dy[k] * h2[j]);
             }
-            dz2[j] = s * (1.f - h2[j] * h2[j]);
+            dz2[j] = s * act_d(z2[j], h2[j]);
             grad[P_B2 + j] += dz2[j];
         }
         for (int i = 0; i < H; ++i) {
             double a = 0.0;
             for (int j = 0; j < H; ++j) a += (double)bf16r(dz2[j]) * (double)bf16r(p[P_W2 + j * H + i]);
-            const float dz1 = (float)a * (1.f - h1[i] * h1[i]);
+            const float dz1 = (float)a * act_d(fmaf(p[P_W1 + i], x, p[P_B1 + i]), h1[i]);
             grad[P_W1 + i] += (double)(dz1 * x);
             grad[P_B1 + i] += dz1;
         }

@@ -96,6 +96,7 @@ def lib():
         L.orc_mlp_forward.argtypes = [_fp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_mlp_gradients.argtypes = [ctypes.c_void_p, _fp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_mlp_gradients.restype = ctypes.c_double
+        L.orc_mlp_set_activation.argtypes = [ctypes.c_int]
         _ip = ctypes.POINTER(ctypes.c_int)
         L.orc_cubic_spline.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp, _dp]
         L.orc_spline_index.argtypes = [ctypes.c_int, _dp, ctypes.c_double]
@@ -474,6 +475,11 @@ class PropTable:
 
 # ---- learned property model (mlp_oracle.c) ----
 MLP_NPARAM = 64 + 64 + 64 * 64 + 64 + 6 * 64 + 6
+
+
+def mlp_set_activation(act):
+    """0: tanh, 1: the clamped cubic (applies to mlp_forward and mlp_gradients)."""
+    lib().orc_mlp_set_activation(int(act))
 
 
 def mlp_forward(params, norm, dh):

@@ -108,3 +108,70 @@ def test_trained_model_accuracy(setup):
         rel = np.abs(got[k] - want[k]) / np.maximum(np.abs(want[k]), nm[8 + m])
         print(k, rel.max())
         assert rel.max() <= 2e-2, (k, rel.max())
+
+
+# ---- the clamped cubic activation (no special-function unit in inference) ----
+
+@pytest.fixture(scope="module")
+def setup_cubic():
+    rows, T0 = thermo.synthetic_table()
+    tab = thermo.SplineTable.from_rows(rows, T0)
+    c = gpu.ChannelTG(channel_setup(32, 32, 32, 6.0, 3.0, 2.0, 2800.0))
+    c.prop_table_init(tab)
+    dh = tab.lists["DH"]
+    lo, hi = float(dh[0] + 0.05 * (dh[-1] - dh[0])), float(dh[-1] - 0.05 * (dh[-1] - dh[0]))
+    c.mlp_init(lo, hi, seed=7)
+    c.mlp_set_activation(gpu.MLP_CUBIC)
+    orc.mlp_set_activation(1)
+    yield c, tab, lo, hi
+    orc.mlp_set_activation(0)
+    c.close()
+
+
+def test_cubic_forward_matches_oracle(setup_cubic):
+    """The FP16 pair arithmetic of the cubic is emulated exactly by the oracle; what is left is
+    the order of the tensor-core sums, which can move an activation by one FP16 rounding."""
+    c, tab, lo, hi = setup_cubic
+    p, nm = c.mlp_params()
+    dh = np.random.default_rng(1).uniform(lo, hi, 5000)
+    got = c.mlp_infer_points(dh)
+    want = orc.mlp_forward(p, nm, dh)
+    for m, k in enumerate(FIELDS):
+        err = np.abs(got[k] - want[k]).max() / nm[8 + m]
+        print(k, err)
+        assert err <= 2e-3, (k, err)
+
+
+def test_cubic_gradients_match_oracle(setup_cubic):
+    c, tab, lo, hi = setup_cubic
+    p, nm = c.mlp_params()
+    dh = np.random.default_rng(2).uniform(lo, hi, 1000)
+    g, loss = c.mlp_gradients(dh)
+    ot = orc.PropTable(tab.lists)
+    go, lo_ = orc.mlp_gradients(ot, p, nm, dh)
+    assert lo_ >= 0 and abs(loss - lo_) <= 1e-3 * lo_
+    for name, (a, b) in GROUPS.items():
+        err = np.abs(g[a:b] - go[a:b]).max() / np.abs(go[a:b]).max()
+        print(name, err)
+        assert err <= 1e-2, (name, err)
+
+
+def test_cubic_trained_model_accuracy(setup_cubic):
+    """The same training and bound as the tanh model (2 % of max(|value|, output scale))."""
+    c, tab, lo, hi = setup_cubic
+    dh = tab.lists["DH"]
+    knots = dh[(dh >= lo) & (dh <= hi)]
+    train = np.concatenate([knots, np.random.default_rng(3).uniform(lo, hi, 6000)])
+    loss0 = c.mlp_train(train, 1, lr=1e-3)
+    for it, lr in TRAIN_SCHEDULE:
+        loss = c.mlp_train(train, it, lr=lr)
+    print("loss", loss0, "->", loss)
+    assert loss < 1e-3 * loss0
+    test = np.random.default_rng(4).uniform(lo, hi, 20000)
+    got = c.mlp_infer_points(test)
+    want, _, _ = orc.PropTable(tab.lists).update(test)
+    p, nm = c.mlp_params()
+    for m, k in enumerate(FIELDS):
+        rel = np.abs(got[k] - want[k]) / np.maximum(np.abs(want[k]), nm[8 + m])
+        print(k, rel.max())
+        assert rel.max() <= 2e-2, (k, rel.max())

@@ -36,7 +36,8 @@ def _channel(s, Q, PR, tab, DH, qw, cthecd):
     return c
 
 
-def test_thermal_step_with_learned_properties():
+@pytest.mark.parametrize("act", [gpu.MLP_TANH, gpu.MLP_CUBIC])
+def test_thermal_step_with_learned_properties(act):
     L, M, N = 64, 64, 32
     s = channel_setup(L, M, N, 2 * math.pi, math.pi, 2.0, 2800.0)
     Q, PR = initial_field(s, 1973, 0.1)
@@ -57,6 +58,7 @@ def test_thermal_step_with_learned_properties():
     lo = float(dh[0] + 0.02 * (dh[-1] - dh[0]))
     hi = float(dh[-1] - 0.02 * (dh[-1] - dh[0]))
     ml.mlp_init(lo, hi, seed=11)
+    ml.mlp_set_activation(act)
     samples = np.random.default_rng(6).choice(field.reshape(-1), 4000, replace=False)
     knots = dh[(dh >= lo) & (dh <= hi)]
     train = np.concatenate([knots, samples, np.random.default_rng(7).uniform(lo, hi, 2000)])
