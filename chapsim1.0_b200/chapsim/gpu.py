@@ -802,8 +802,10 @@ class ChannelXinout(ChannelIO):
         self.tg = tg
 
     def kernel_slots(self):
-        sub = ["k_xio_inlet", "k_xio_outlet_a", "k_xio_outlet_b", "k_xio_outlet_c", "k_io_divu", "k_io_rhs", "k_io_massflux", "k_xio_div_dctx", "k_fftz_fwd",
-               "k_xio_ysolve", "k_fftz_inv", "k_xio_dctx_inv", "k_io_correct"]
+        fft = self.L in (32, 64, 96, 128, 192, 256, 384)  # the cosine transforms through the FFT
+        sub = ["k_xio_inlet", "k_xio_outlet_a", "k_xio_outlet_b", "k_xio_outlet_c", "k_io_divu", "k_io_rhs",
+               "k_io_massflux", "k_xio_div_cosqf" if fft else "k_xio_div_dctx", "k_fftz_fwd", "k_xio_ysolve",
+               "k_fftz_inv", "k_xio_cosqb" if fft else "k_xio_dctx_inv", "k_io_correct"]
         return ["k_io_cfl", "k_dt", "k_dt_pair"] + sub * 3
 
     def advance(self, nsteps, DT0, DTMIN, CFLGV):

@@ -227,6 +227,7 @@ struct chapsim_ctx {
     cudaEvent_t dump_snap = nullptr, dump_done = nullptr;
     // inflow/outflow main domain (domain 3)
     chapsim_ctx* tg_in = nullptr;  // the periodic TG context whose fields feed the inlet
+    double2* xio_tq = nullptr;     // (cos, sin)(pi p / (2L)) of the FFT form of the cosine transforms
     double* xio_cf = nullptr;      // COSQF matrix w_p cos((2m+1) p pi / (2L)), [p][m]; then the COSQB matrix
                                    // 4 cos((2m+1) p pi / (2L)), [m][p] (one allocation, 2 L^2)
     double* xio_bc0 = nullptr;     // BC_CONV0 (3 M N)
@@ -905,7 +906,15 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     k_io_massflux<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->st, ns);
     prof_mark(ctx);
     const int nrb = (int)(((long long)g.M * g.N + XD_R - 1) / XD_R);
-    k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cf, ctx->SP, ctx->st, ns, 1.0);
+    int f1_, f2_;
+    const bool fftx = fft4s_split(g.LI, f1_, f2_);  // an FFT length: the cosine transforms through the FFT
+    dim3 gxf((g.M + XF_TJ - 1) / XF_TJ, g.N);
+    const size_t smf = (size_t)XF_TJ * fft4s_ld(g.LI) * sizeof(double2);
+    if (fftx) {
+        DISPATCH_FFT(g.LI, (k_xio_div_cosqf<FN1, FN2><<<gxf, PX_NT, smf, s>>>(g, f.G, ctx->xio_tq, ctx->SP, ctx->st, ns, 1.0)));
+    } else {
+        k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cf, ctx->SP, ctx->st, ns, 1.0);
+    }
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;  // LH = LI x modes
     const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
@@ -915,7 +924,11 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     DISPATCH_FFT(g.N, (k_fftz<+1, FN1, FN2, double2><<<gfz, FZ_NT, smem_fz(g), s>>>(g, ctx->SP, 0)));
     prof_mark(ctx);
-    k_xio_dctx_inv<<<nrb, XIO_NT, smem_xd(g), s>>>(g, ctx->SP, ctx->xio_cf + (size_t)g.LI * g.LI, ctx->DPH);
+    if (fftx) {
+        DISPATCH_FFT(g.LI, (k_xio_cosqb<FN1, FN2><<<gxf, PX_NT, smf, s>>>(g, ctx->SP, ctx->xio_tq, ctx->DPH)));
+    } else {
+        k_xio_dctx_inv<<<nrb, XIO_NT, smem_xd(g), s>>>(g, ctx->SP, ctx->xio_cf + (size_t)g.LI * g.LI, ctx->DPH);
+    }
     prof_mark(ctx);
     k_io_correct<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->DPH, ctx->st, ns, nullptr);
     prof_mark(ctx);
@@ -1175,6 +1188,11 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
             }
         INIT_CK(cudaMalloc(&ctx->xio_cf, cm.size() * sizeof(double)));
         INIT_CK(cudaMemcpy(ctx->xio_cf, cm.data(), cm.size() * sizeof(double), cudaMemcpyHostToDevice));
+        std::vector<double2> tq((size_t)L);
+        for (int p = 0; p < L; ++p)
+            tq[p] = make_double2(std::cos((double)p * pi / (double)(2 * L)), std::sin((double)p * pi / (double)(2 * L)));
+        INIT_CK(cudaMalloc(&ctx->xio_tq, tq.size() * sizeof(double2)));
+        INIT_CK(cudaMemcpy(ctx->xio_tq, tq.data(), tq.size() * sizeof(double2), cudaMemcpyHostToDevice));
         INIT_CK(cudaMalloc(&ctx->xio_bc0, (size_t)3 * M * N * sizeof(double)));
         INIT_CK(cudaMemset(ctx->xio_bc0, 0, (size_t)3 * M * N * sizeof(double)));
         INIT_CK(cudaMalloc(&ctx->xio_yd, (size_t)L * M * N * sizeof(double)));
@@ -1186,6 +1204,12 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         if (smem_xd(g) > 48 * 1024) {
             INIT_CK(set_smem(k_xio_div_dctx, smem_xd(g)));
             INIT_CK(set_smem(k_xio_dctx_inv, smem_xd(g)));
+        }
+        int f1_, f2_;
+        const size_t smf = (size_t)XF_TJ * fft4s_ld(L) * sizeof(double2);
+        if (fft4s_split(L, f1_, f2_) && smf > 48 * 1024) {
+            DISPATCH_FFT(L, INIT_CK(set_smem(k_xio_div_cosqf<FN1, FN2>, smf)));
+            DISPATCH_FFT(L, INIT_CK(set_smem(k_xio_cosqb<FN1, FN2>, smf)));
         }
     }
     if (ctx->prec == CHAPSIM_PREC_MIXED) {
@@ -1265,7 +1289,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->dump_snap) cudaEventDestroy(ctx->dump_snap);
     if (ctx->dump_done) cudaEventDestroy(ctx->dump_done);
     if (ctx->dump_stream) cudaStreamDestroy(ctx->dump_stream);
-    cudaFree(ctx->xio_cf); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
+    cudaFree(ctx->xio_cf); cudaFree(ctx->xio_tq); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
     for (auto& e : ctx->xev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

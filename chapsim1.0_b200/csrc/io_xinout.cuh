@@ -12,10 +12,12 @@
 //                    CONVCTION_OUTLET_U (:115-192), the convective update of the outlet
 //                    column, and the outflow scaling of CHK_MassConsv_io
 //                    (src/processing/CHK_conservation.f90:11-79)
-//   k_xio_div_dctx   DIVG_io (src/DIVG.f90:54-137) and FISHPACK's x transform COSQF
+//   k_xio_div_cosqf  DIVG_io (src/DIVG.f90:54-137) and FISHPACK's x transform COSQF through one
+//                    complex FFT per row (k_xio_div_dctx: as a matrix product, for L that is no
+//                    FFT length)
 //   k_xio_ysolve     TRID0 (src/possion3d_fishpack.f90:309-340) per (x mode, kz)
-//   k_xio_dctx_inv   COSQB and the 1/(SCALX SCALY) scaling -> DPH (interior; the ghost
-//                    columns of DPH stay zero)
+//   k_xio_cosqb      COSQB and the 1/(SCALX SCALY) scaling -> DPH (interior; the ghost
+//                    columns of DPH stay zero); k_xio_dctx_inv as a matrix product
 //   k_xio_divgck     DIVGCK_io with TgFlowFlg (src/DIVGCK.f90:80-84): the three cell ranges
 //   k_dt_pair        CFLMM = max(CFLMM_tg, CFLMM_io) and the dt rule (src/SOLVE.f90:79-94)
 //
@@ -274,6 +276,79 @@ __global__ void __launch_bounds__(XIO_NT, 2) k_xio_div_dctx(Geo g, const double*
                 if (m < L) SP[m + (long long)L * (q0 + rr)] = make_double2(acc[r][u], 0.0);
             }
         }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The same pair of transforms through one L-point complex FFT per row when L is an FFT length
+// (32, 64, 96, 128, 192, 256, 384), after Makhoul's reordering:
+//   COSQF: with c_p = w_p x_p and u_n = sum_p (c_p e^{i pi p / (2L)}) e^{+2 pi i p n / L},
+//          X(2n) = Re u_n and X(2n+1) = Re u_{L-1-n}, n < L/2
+//          (cos(pi p (4n+1) / (2L)) is the (2m+1) = 4n+1 term; 4(L-1-n)+1 = 4L - (4n+3))
+//   COSQB: with v_n = X(2n), v_{L-1-n} = X(2n+1) and V_p = sum_n v_n e^{-2 pi i n p / L},
+//          x(p) = 4 Re(e^{-i pi p / (2L)} V_p)
+// TQ[p] = (cos, sin)(pi p / (2L)).  XF_TJ rows (j) of one k per block, one FFT line each.
+#define XF_TJ 8
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(PX_NT) k_xio_div_cosqf(Geo g, const double* __restrict__ G, const double2* __restrict__ TQ,
+                                                         double2* __restrict__ SP, const DevState* __restrict__ st,
+                                                         int ns, double wdiv) {
+    extern __shared__ __align__(16) unsigned char xf_raw[];
+    double2* smc = reinterpret_cast<double2*>(xf_raw);
+    const int L = g.LI, M = g.M, N = g.N;
+    const int LD = fft4s_ld(L);
+    const int j0 = 1 + blockIdx.x * XF_TJ, k = blockIdx.y;
+    const int nj = min(XF_TJ, M - j0 + 1);
+    const double coe0 = 1.0 / st->dt / g.talp[ns] / wdiv;
+    const double coe1 = g.dxi / 1.0;
+    const int kp = wrapp(k, N);
+    for (int p = threadIdx.x; p < nj * L; p += PX_NT) {
+        const int jl = p / L, i = p - jl * L;
+        const int j = j0 + jl;
+        const long long c = pidx(g, i + 1, j, k);
+        const double u = G[c], up = G[c + 1];
+        const double v = G[c + g.FS], vp = G[c + g.FS + g.L];
+        const double w = G[c + 2 * g.FS], wp = G[pidx(g, i + 1, j, kp) + 2 * g.FS];
+        const double coe2 = g.dyfi[j] / 1.0;
+        const double DIVX = (up - u) * coe1, DIVY = (vp - v) * coe2, DIVZ = (wp - w) * g.dzi;
+        const double x = (DIVX + DIVY + DIVZ + 0.0) * coe0;
+        const double cw = i == 0 ? x : 2.0 * x;
+        const double2 t = TQ[i];
+        smc[jl * LD + i] = make_double2(cw * t.x, cw * t.y);
+    }
+    block_fft4s<N1, N2, +1>(smc, nj, LD, g.twx);
+    __syncthreads();
+    for (int p = threadIdx.x; p < nj * L; p += PX_NT) {
+        const int jl = p / L, m = p - jl * L;
+        const int n = (m & 1) ? L - 1 - (m >> 1) : (m >> 1);
+        SP[m + (long long)L * ((j0 + jl - 1) + (long long)M * k)] = make_double2(smc[jl * LD + n].x, 0.0);
+    }
+}
+
+template <int N1, int N2>
+__global__ void __launch_bounds__(PX_NT) k_xio_cosqb(Geo g, const double2* __restrict__ SP, const double2* __restrict__ TQ,
+                                                     double* __restrict__ DPH) {
+    extern __shared__ __align__(16) unsigned char xf_raw[];
+    double2* smc = reinterpret_cast<double2*>(xf_raw);
+    const int L = g.LI, M = g.M;
+    const int LD = fft4s_ld(L);
+    const int j0 = 1 + blockIdx.x * XF_TJ, k = blockIdx.y;
+    const int nj = min(XF_TJ, M - j0 + 1);
+    const int LHf = L / 2;
+    for (int p = threadIdx.x; p < nj * L; p += PX_NT) {
+        const int jl = p / L, n = p - jl * L;
+        const int m = n < LHf ? 2 * n : 2 * (L - 1 - n) + 1;
+        smc[jl * LD + n] = make_double2(SP[m + (long long)L * ((j0 + jl - 1) + (long long)M * k)].x, 0.0);
+    }
+    block_fft4s<N1, N2, -1>(smc, nj, LD, g.twx);
+    __syncthreads();
+    const double q4 = (double)(4 * L);
+    for (int p = threadIdx.x; p < nj * L; p += PX_NT) {
+        const int jl = p / L, pp = p - jl * L;
+        const double2 V = smc[jl * LD + pp], t = TQ[pp];
+        const double y = V.x * t.x + V.y * t.y;
+        DPH[pidx(g, pp + 1, j0 + jl, k)] = 4.0 * y / q4;
     }
 }
 
