@@ -354,7 +354,10 @@ __global__ void __launch_bounds__(PX_NT) k_xio_cosqb(Geo g, const double2* __res
 
 // TRID0 for every (x mode m, kz) line: BB(j) = ACPH(j) + XRT(m) + YRT(kz) with XRT = -ak1[m],
 // YRT = -ak3[kz]; A = AMPH, C = APPH.  D holds the forward factors (M per line, line-major
-// across threads).  Complex right-hand side: the real and imaginary lines share D.
+// across threads).  Complex right-hand side: the real and imaginary lines share D.  Each
+// sweep loads XY_U rows ahead of the recurrence (the loads do not wait for the previous
+// row's store), so a line costs one memory latency per XY_U rows.
+#define XY_U 8
 __global__ void __launch_bounds__(XIO_NT) k_xio_ysolve(Geo g, double2* __restrict__ SP, double* __restrict__ D) {
     const int L = g.LI, M = g.M, N = g.N;
     const long long nl = (long long)L * N;
@@ -373,16 +376,25 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_ysolve(Geo g, double2* __restric
     t.x = t.x * z;
     t.y = t.y * z;
     S[0] = t;
-    for (int j = 2; j <= M - 1; ++j) {
-        bb = g.acph[j] + xrt / 1.0 + yrt;
-        z = 1.0 / (bb - g.amph[j] * d);
-        d = g.apph[j] * z;
-        Dl[(long long)(j - 1) * nl] = d;
-        double2 r = S[(long long)(j - 1) * stride];
-        r.x = (r.x - g.amph[j] * t.x) * z;
-        r.y = (r.y - g.amph[j] * t.y) * z;
-        S[(long long)(j - 1) * stride] = r;
-        t = r;
+    for (int j0 = 2; j0 <= M - 1; j0 += XY_U) {
+        double2 rr[XY_U];
+#pragma unroll
+        for (int u = 0; u < XY_U; ++u)
+            if (j0 + u <= M - 1) rr[u] = S[(long long)(j0 + u - 1) * stride];
+#pragma unroll
+        for (int u = 0; u < XY_U; ++u) {
+            const int j = j0 + u;
+            if (j > M - 1) break;
+            bb = g.acph[j] + xrt / 1.0 + yrt;
+            z = 1.0 / (bb - g.amph[j] * d);
+            d = g.apph[j] * z;
+            Dl[(long long)(j - 1) * nl] = d;
+            double2 r = rr[u];
+            r.x = (r.x - g.amph[j] * t.x) * z;
+            r.y = (r.y - g.amph[j] * t.y) * z;
+            S[(long long)(j - 1) * stride] = r;
+            t = r;
+        }
     }
     bb = g.acph[M] + xrt / 1.0 + yrt;
     z = bb - g.amph[M] * d;
@@ -394,13 +406,25 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_ysolve(Geo g, double2* __restric
         r = make_double2(0.0, 0.0);
     }
     S[(long long)(M - 1) * stride] = r;
-    for (int j = M - 1; j >= 1; --j) {
-        const double dj = Dl[(long long)(j - 1) * nl];
-        double2 s = S[(long long)(j - 1) * stride];
-        s.x = s.x - dj * r.x;
-        s.y = s.y - dj * r.y;
-        S[(long long)(j - 1) * stride] = s;
-        r = s;
+    for (int j0 = M - 1; j0 >= 1; j0 -= XY_U) {
+        double2 ss[XY_U];
+        double dd[XY_U];
+#pragma unroll
+        for (int u = 0; u < XY_U; ++u)
+            if (j0 - u >= 1) {
+                ss[u] = S[(long long)(j0 - u - 1) * stride];
+                dd[u] = Dl[(long long)(j0 - u - 1) * nl];
+            }
+#pragma unroll
+        for (int u = 0; u < XY_U; ++u) {
+            const int j = j0 - u;
+            if (j < 1) break;
+            double2 sv = ss[u];
+            sv.x = sv.x - dd[u] * r.x;
+            sv.y = sv.y - dd[u] * r.y;
+            S[(long long)(j - 1) * stride] = sv;
+            r = sv;
+        }
     }
 }
 
