@@ -138,6 +138,16 @@ __global__ void k_tdma_seq(const double* A, const double* B, const double* C, do
 }
 
 
+// Failure-path probe: one warp waits on an mbarrier that nothing arrives at.  The wait is the
+// bounded one every tensor-core and bulk-copy stage uses (about 2^31 clocks), so the kernel gives
+// up, sets the timeout bit of the error word and returns; no fault, and the context stays usable.
+__global__ void k_wait_probe(unsigned int* err) {
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) mbar_init(&mbar, 1);
+    __syncthreads();
+    (void)mbar_wait_warp(&mbar, 0, err);
+}
+
 struct chapsim_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -1812,6 +1822,15 @@ int chapsim_cfl_io(chapsim_ctx_t* ctx, double* cflmm) {
     int rc = check_device_error(ctx);
     if (cflmm) *cflmm = ctx->st_host->cflmm;
     return rc;
+}
+
+int chapsim_probe_wait_timeout(chapsim_ctx_t* ctx) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    k_wait_probe<<<1, 32, 0, ctx->stream>>>(&ctx->st->err);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    return check_device_error(ctx);
 }
 
 int chapsim_xinout_attach(chapsim_ctx_t* io, chapsim_ctx_t* tg) {

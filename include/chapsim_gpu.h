@@ -26,7 +26,7 @@ extern "C" {
 #define CHAPSIM_ERR_NAN (-2)         /* non-finite velocity or dt */
 #define CHAPSIM_ERR_DT_COLLAPSE (-3) /* DT/DT0 < 0.01: src/SOLVE.f90:199-207 dumps and STOPs */
 #define CHAPSIM_ERR_TABLE_RANGE (-4) /* property table out of range: spline_interpolation_* STOP */
-#define CHAPSIM_ERR_TIMEOUT (-5)     /* reserved: bounded device wait expired */
+#define CHAPSIM_ERR_TIMEOUT (-5)     /* a bounded device wait expired */
 #define CHAPSIM_ERR_BADARG (-6)      /* invalid argument or unsupported grid */
 #define CHAPSIM_ERR_NOMEM (-7)       /* device allocation failed */
 
@@ -233,6 +233,12 @@ int chapsim_upload_weighted_pressure(chapsim_ctx_t* ctx, const double* pr0_1, co
 /* DIVGCK_io (src/DIVGCK.f90:60-184), x-periodic main domain: MAXDIVGV_io, the
  * max over the interior of |div G + DrhoDtP| (the three ranges coincide). */
 int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv);
+
+/* No counterpart in the reference: the failure path of the bounded device waits.  One warp
+ * waits on an mbarrier that nothing arrives at, with the clock budget (about 2^31 clocks)
+ * of every tensor-core completion and bulk-copy wait; the call returns CHAPSIM_ERR_TIMEOUT
+ * after about a second, and the context stays usable (the error word is cleared). */
+int chapsim_probe_wait_timeout(chapsim_ctx_t* ctx);
 
 /* ---- Main domain with inflow and outflow (grid.idomain = 3): the IO part of a
  * TG + main-domain run (iDomain = 3, TgFlowFlg and IoFlowFlg), flow only
