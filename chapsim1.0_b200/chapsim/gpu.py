@@ -43,7 +43,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
             "chapsim_pp_mean_zx_io", "chapsim_download_pp_means_io",
             "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write",
-            "chapsim_mlp_set_activation", "chapsim_probe_wait_timeout", "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
+            "chapsim_mlp_set_activation", "chapsim_probe_wait_timeout", "chapsim_thermal_set_isothermal", "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
 PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
@@ -202,6 +202,7 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_xinout_attach.argtypes = [vp, vp]
     L.chapsim_mlp_set_activation.argtypes = [vp, ctypes.c_int32]
     L.chapsim_probe_wait_timeout.argtypes = [vp]
+    L.chapsim_thermal_set_isothermal.argtypes = [vp, ctypes.c_int32, _dp]
     L.chapsim_advance_xinout.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp,
                                          _dp]
     L.chapsim_divgck_xinout.argtypes = [vp, _dp]
@@ -757,6 +758,12 @@ class ChannelIO(ChannelTG):
             raise ValueError("DH shape mismatch")
         self._check(self.lib.chapsim_thermal_init(self.h, _ptr(DH), float(qw_bot), float(qw_top), float(cthecd)))
         self.thermal = True
+
+    def thermal_set_isothermal(self, wall, state=None):
+        """BC_Fixed_Temperature on wall 0 (bottom) or 1 (top): state = (T, H, D, M, K) of the wall;
+        None returns that wall to the constant heat flux."""
+        v = None if state is None else np.ascontiguousarray(state, np.float64)
+        self._check(self.lib.chapsim_thermal_set_isothermal(self.h, int(wall), _ptr(v)))
 
     def download_thermal(self):
         """dict DH, H, T, D, M, K, CP of padded fields."""

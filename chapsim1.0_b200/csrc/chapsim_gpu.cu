@@ -798,16 +798,16 @@ void launch_thermal_substep_t(chapsim_ctx* ctx, int ns) {
             k_mlp_infer<true, MLP_ACT_TANH><<<gi, MLP_NT, MLP_INF_SMEM, s>>>(
                 ctx->mlp_par, mlp_ops(ctx), ctx->mlp_norm, ctx->tab, g, tot, ctx->tf.DH, out, ctx->pstat, &ctx->st->err);
         prof_mark(ctx);
-        if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+        else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     } else if (sm) {
         k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
         prof_mark(ctx);
-        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     } else {
         k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
         prof_mark(ctx);
-        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     }
     prof_mark(ctx);
     k_drhodt<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ns);
@@ -2156,10 +2156,10 @@ void thermal_start(chapsim_ctx* ctx, size_t fb) {
     const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
     if (sm) {
         k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     } else {
         k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     }
     cudaMemcpyAsync(ctx->io.RHO, ctx->DEN, fb, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(ctx->io.MU0, ctx->io.MU, fb, cudaMemcpyDeviceToDevice, s);
@@ -2168,6 +2168,36 @@ void thermal_start(chapsim_ctx* ctx, size_t fb) {
     k_io_props<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     k_io_velocity<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     ctx->launches += 5;
+}
+
+// BC_WALL_THERMAL on its own (the wall rows of every column): after a change of the wall condition
+template <typename F>
+void thermal_walls(chapsim_ctx* ctx) {
+    const Geo& g = ctx->g;
+    IoFieldsT<F> f = io_fields_t<F>(ctx);
+    const size_t sm = prop_smem(ctx->tab.n);
+    const long long plane = 2LL * g.L * g.N;
+    if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, ctx->stream>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+    else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, ctx->stream>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+    ctx->launches += 1;
+}
+
+extern "C" int chapsim_thermal_set_isothermal(chapsim_ctx_t* ctx, int32_t wall, const double* state5) {
+    if (!ctx) return fail(nullptr, CHAPSIM_ERR_BADARG, "null context");
+    if (!ctx->thermal) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver is not initialised (chapsim_thermal_init)");
+    if (wall < 0 || wall > 1) return fail(ctx, CHAPSIM_ERR_BADARG, "wall must be 0 (bottom) or 1 (top)");
+    if (state5)
+        for (int a = 0; a < 5; ++a)
+            if (!std::isfinite(state5[a])) return fail(ctx, CHAPSIM_ERR_BADARG, "non-finite wall state");
+    CK(cudaSetDevice(ctx->device));
+    ctx->tp.iso[wall] = state5 != nullptr;
+    if (state5)
+        for (int a = 0; a < 5; ++a) ctx->tp.wv[wall][a] = state5[a];
+    if (io_mixed(ctx)) thermal_walls<float>(ctx);
+    else thermal_walls<double>(ctx);
+    CK(cudaGetLastError());
+    if (int rc = check_device_error(ctx)) return rc;
+    return drop_step_graph(ctx);
 }
 
 extern "C" int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, double qw_top, double cthecd) {

@@ -32,6 +32,10 @@ struct ThermoParams {
     double wf_bot, wf_top;  // WALLFLUX of the bottom (+q) and top (-q) walls (src/Flow_State.f90:150-175)
     double cthecd;          // 1 / (REN PRT0)
     double dhmin, dhmax;    // LIST_DH at IMIN_DH, IMAX_DH
+    // BC_Fixed_Temperature walls (0 bottom, 1 top): the wall state T, H, D, M, K held in the ghost
+    // row (BC_WALL_IsoTHERMAL, src/BC_WALL.f90:484-538); 0 = constant heat flux
+    int iso[2];
+    double wv[2][5];
 };
 
 template <typename F>
@@ -64,12 +68,12 @@ __global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFieldsT<F> f, The
         const double COE33 = g.dzqi * ZND2CL * 1.0 * tp.cthecd;
         const double COE22 = g.dyfi[j] * 1.0 * tp.cthecd;
         double COE221, COE222;
-        if (j == 1) {
+        if (j == 1) {  // src/RHS_ENERGY_EXPLICIT.f90:50-77: the wall face of an isothermal wall keeps DYCI
             COE221 = g.dyci[jp] / 1.0;
-            COE222 = 1.0 / 1.0;
+            COE222 = tp.iso[0] ? g.dyci[j] / 1.0 : 1.0 / 1.0;
         } else if (j == M) {
             COE222 = g.dyci[j] / 1.0;
-            COE221 = 1.0 / 1.0;
+            COE221 = tp.iso[1] ? g.dyci[jp] / 1.0 : 1.0 / 1.0;
         } else {
             COE221 = g.dyci[jp] / 1.0;
             COE222 = g.dyci[j] / 1.0;
@@ -86,8 +90,8 @@ __global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFieldsT<F> f, The
         DX_KDT = DX_KDT * COE11;
         double KDTy1 = (g.wff[jp] * K[cjp] + g.wfb[jp] * kc) * (T[cjp] - tc) * COE221;
         double KDTy2 = (g.wff[j] * kc + g.wfb[j] * K[cjm]) * (tc - T[cjm]) * COE222;
-        if (j == 1) KDTy2 = -tp.wf_bot * COE222;
-        else if (j == M) KDTy1 = -tp.wf_top * COE221;
+        if (j == 1 && !tp.iso[0]) KDTy2 = -tp.wf_bot * COE222;
+        else if (j == M && !tp.iso[1]) KDTy1 = -tp.wf_top * COE221;
         const double DY_KDT = (KDTy1 - KDTy2) * COE22;
         double DZ_KDT = (K[ckp] + kc) * (T[ckp] - tc) - (K[ckm] + kc) * (tc - T[ckm]);
         DZ_KDT = DZ_KDT * COE33;
@@ -143,7 +147,8 @@ __global__ void __launch_bounds__(PROP_NT) k_eng_props(PropTab tb, Geo g, IoFiel
 
 // ghost rows j = 0 (bottom) and j = M+1 (top), every i and k
 template <bool SMEM, typename F>
-__global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFieldsT<F> f, ThermoFields t, DevState* st) {
+__global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFieldsT<F> f, ThermoFields t, ThermoParams tp,
+                                                  DevState* st) {
     extern __shared__ double keys[];
     const double* xdh = tb.xdh;
     const double* xh = tb.xh;
@@ -155,6 +160,19 @@ __global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFieldsT
         const long long r = top ? q - plane : q;
         const int i = (int)(r % L), k = (int)(r / L);
         long long p;
+        const int w = top ? 1 : 0;
+        if (tp.iso[w]) {  // BC_WALL_IsoTHERMAL: the wall state, DH = H * D (DENSITY0, Viscousity0 keep the old row)
+            p = pidx(g, i, top ? M + 1 : 0, k);
+            f.RHO[p] = f.DEN[p];
+            f.MU0[p] = f.MU[p];
+            t.TEMP[p] = tp.wv[w][0];
+            t.ENTH[p] = tp.wv[w][1];
+            f.DEN[p] = tp.wv[w][2];
+            f.MU[p] = tp.wv[w][3];
+            t.KAP[p] = tp.wv[w][4];
+            t.DH[p] = t.ENTH[p] * f.DEN[p];
+            continue;
+        }
         if (top) {
             p = pidx(g, i, M + 1, k);
             t.DH[p] = 2.0 * t.DH[pidx(g, i, M, k)] - g.wff[M] * t.DH[pidx(g, i, M, k)] - g.wfb[M] * t.DH[pidx(g, i, M - 1, k)];

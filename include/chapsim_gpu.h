@@ -334,6 +334,14 @@ int chapsim_therm_prop_update_points(chapsim_ctx_t* ctx, int64_t npts, const dou
  * (src/SOLVE.f90:119-133); a point leaving the table gives
  * CHAPSIM_ERR_TABLE_RANGE. */
 int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, double qw_top, double cthecd);
+/* BC_Fixed_Temperature (iThermalWallType = 2) on wall 0 (bottom, iBotWall) or 1 (top):
+ * state5 = the wall state T, H, D, M, K of T_WAL_GV, H_WAL_GV, D_WAL_GV, M_WAL_GV,
+ * K_WAL_GV (src/Flow_State.f90:186-230, nondimensional), held in the wall's ghost row
+ * (BC_WALL_IsoTHERMAL, src/BC_WALL.f90:484-538, with DH = H * D), and the wall face of
+ * RHS_ENERGY_EXPLICIT keeps its DYCI conduction term (src/RHS_ENERGY_EXPLICIT.f90:50-77).
+ * NULL returns the wall to the constant heat flux of chapsim_thermal_init.  Call after
+ * chapsim_thermal_init; the ghost row is set at once. */
+int chapsim_thermal_set_isothermal(chapsim_ctx_t* ctx, int32_t wall, const double* state5);
 
 /* The thermal fields, each (NCL1, 0:NCL2+1, NCL3); any pointer may be NULL:
  * DH, ENTHALPY, TEMPERATURE, DENSITY, Viscousity, THERMCONDT, HEATCAP. */

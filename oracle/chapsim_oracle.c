@@ -69,6 +69,10 @@ typedef struct {
     void* tab;
     double *DH, *ENTH, *TEMP, *KAPPA, *HCP, *RHSE, *RHSE0, *G0;
     double QW_BOT, QW_TOP, CTHECD, DHMIN, DHMAX;
+    /* BC_Fixed_Temperature walls (0 bottom, 1 top): the wall state T, H, D, M, K of T_WAL_GV ...
+       (src/Flow_State.f90:186-230), held in the ghost rows (BC_WALL_IsoTHERMAL) */
+    int iso[2];
+    double WV[2][5];
     int prop_err;
     /* buoyancy (thermal_gravity, src/Flow_State.f90:95-125): iGravity and F_A */
     int igrav;
@@ -2064,17 +2068,36 @@ static void thermal_props_interior(orc_t* o) {
             for (int K = 1; K <= N; ++K) thermal_point(o, I, J, K);
 }
 
-/* BC_WALL_Isoflux on both walls: ghost rho*h extrapolated, then its properties */
-static void thermal_bc_isoflux(orc_t* o) {
+/* BC_WALL_IsoTHERMAL (src/BC_WALL.f90:484-538): the ghost row holds the wall state; DH = H * D */
+static void thermal_wall_state(orc_t* o, int w, int I, int J, int K) {
+    F3(o->TEMP, o, I, J, K) = o->WV[w][0];
+    F3(o->ENTH, o, I, J, K) = o->WV[w][1];
+    F3(o->DEN, o, I, J, K) = o->WV[w][2];
+    F3(o->MU, o, I, J, K) = o->WV[w][3];
+    F3(o->KAPPA, o, I, J, K) = o->WV[w][4];
+    F3(o->DH, o, I, J, K) = F3(o->ENTH, o, I, J, K) * F3(o->DEN, o, I, J, K);
+}
+
+/* BC_WALL_THERMAL (src/BC_WALL.f90:622-643): per wall BC_WALL_Isoflux (:541-619, ghost rho*h
+ * extrapolated, then its properties) or BC_WALL_IsoTHERMAL; columns NCL1S..NCL1E */
+static void thermal_bc(orc_t* o) {
     int L = o->L, M = o->M, N = o->N;
-    for (int I = 1; I <= L; ++I)
+    for (int I = 1 - o->xo; I <= L + o->xo; ++I)
         for (int K = 1; K <= N; ++K) {
+            if (o->iso[1]) {
+                thermal_wall_state(o, 1, I, M + 1, K);
+                continue;
+            }
             F3(o->DH, o, I, M + 1, K) = 2.0 * F3(o->DH, o, I, M, K) - o->WFF[M] * F3(o->DH, o, I, M, K) -
                                         o->WFB[M] * F3(o->DH, o, I, M - 1, K);
             thermal_point(o, I, M + 1, K);
         }
-    for (int I = 1; I <= L; ++I)
+    for (int I = 1 - o->xo; I <= L + o->xo; ++I)
         for (int K = 1; K <= N; ++K) {
+            if (o->iso[0]) {
+                thermal_wall_state(o, 0, I, 0, K);
+                continue;
+            }
             F3(o->DH, o, I, 0, K) = 2.0 * F3(o->DH, o, I, 1, K) - o->WFF[2] * F3(o->DH, o, I, 2, K) -
                                     o->WFB[2] * F3(o->DH, o, I, 1, K);
             thermal_point(o, I, 0, K);
@@ -2096,12 +2119,12 @@ static void rhs_energy_explicit(orc_t* o) {
         double COE33 = o->DZQI * ZND2CL * 1.0 * CTHECD;
         double COE22 = o->DYFI[JJ] * 1.0 * CTHECD;
         double COE221, COE222;
-        if (JJ == 1) {
+        if (JJ == 1) {  /* src/RHS_ENERGY_EXPLICIT.f90:50-66 */
             COE221 = o->DYCI[JJP] / 1.0;
-            COE222 = 1.0 / 1.0;
-        } else if (JJ == M) {
+            COE222 = o->iso[0] ? o->DYCI[JJ] / 1.0 : 1.0 / 1.0;
+        } else if (JJ == M) {  /* :68-77 */
             COE222 = o->DYCI[JJ] / 1.0;
-            COE221 = 1.0 / 1.0;
+            COE221 = o->iso[1] ? o->DYCI[JJP] / 1.0 : 1.0 / 1.0;
         } else {
             COE221 = o->DYCI[JJP] / 1.0;
             COE222 = o->DYCI[JJ] / 1.0;
@@ -2131,8 +2154,8 @@ static void rhs_energy_explicit(orc_t* o) {
                                (TT(IC, JP, KC) - TT(IC, JC, KC)) * COE221;
                 double KDTy2 = (o->WFF[JJ] * KK(IC, JC, KC) + o->WFB[JJ] * KK(IC, JM, KC)) *
                                (TT(IC, JC, KC) - TT(IC, JM, KC)) * COE222;
-                if (JJ == 1) KDTy2 = -WF_BOT * COE222;
-                else if (JJ == M) KDTy1 = -WF_TOP * COE221;
+                if (JJ == 1 && !o->iso[0]) KDTy2 = -WF_BOT * COE222;
+                else if (JJ == M && !o->iso[1]) KDTy1 = -WF_TOP * COE221;
                 double DY_KDT = (KDTy1 - KDTy2) * COE22;
                 double DZ_KDT = (KK(IC, JC, KP) + KK(IC, JC, KC)) * (TT(IC, JC, KP) - TT(IC, JC, KC)) -
                                 (KK(IC, JC, KM) + KK(IC, JC, KC)) * (TT(IC, JC, KC) - TT(IC, JC, KM));
@@ -2195,7 +2218,7 @@ int orc_thermal_substep(orc_t* o, int NS) {
             }
     o->prop_err = 0;
     thermal_props_interior(o);
-    thermal_bc_isoflux(o);
+    thermal_bc(o);
     density_time_derivation(o, NS);
     io_staggered_props(o);
     if (o->ivis) io_density_implicit_add(o);
@@ -2226,12 +2249,24 @@ int orc_thermal_enable(orc_t* o, void* tab, const double* DH, double qw_bot, dou
     memset(o->RHSE0, 0, fs * sizeof(double));
     o->prop_err = 0;
     thermal_props_interior(o);
-    thermal_bc_isoflux(o);
+    thermal_bc(o);
     memcpy(o->MU0, o->MU, fs * sizeof(double));
     memcpy(o->RHO, o->DEN, fs * sizeof(double));
     memcpy(o->G0, o->G, 3 * fs * sizeof(double));
     io_staggered_props(o);
     io_velocity_calc(o);
+    return o->prop_err;
+}
+
+/* BC_Fixed_Temperature on wall w (0 bottom, 1 top) with the wall state v = T, H, D, M, K, or the
+ * constant heat flux of orc_thermal_enable again (v NULL); the wall's ghost row is set at once */
+int orc_thermal_set_isothermal(orc_t* o, int w, const double* v) {
+    if (!o->thermal || w < 0 || w > 1) return -1;
+    o->iso[w] = v != NULL;
+    if (v)
+        for (int a = 0; a < 5; ++a) o->WV[w][a] = v[a];
+    o->prop_err = 0;
+    thermal_bc(o);
     return o->prop_err;
 }
 

@@ -92,6 +92,8 @@ def lib():
         L.orc_thermal_substep.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_thermal_substep.restype = ctypes.c_int
         L.orc_thermal_get.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_thermal_set_isothermal.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_thermal_set_isothermal.restype = ctypes.c_int
         _fp = ctypes.POINTER(ctypes.c_float)
         L.orc_mlp_forward.argtypes = [_fp, _dp, ctypes.c_int, _dp, _dp]
         L.orc_mlp_gradients.argtypes = [ctypes.c_void_p, _fp, _dp, ctypes.c_int, _dp, _dp]
@@ -316,6 +318,13 @@ class Oracle:
         rc = self._lib.orc_thermal_enable(self._h, table._h, _p(DH), float(qw_bot), float(qw_top), float(cthecd))
         if rc != 0:
             raise ValueError("thermal start-up failed (DH outside the property table)")
+
+    def thermal_set_isothermal(self, wall, state=None):
+        """BC_Fixed_Temperature on wall 0 (bottom) or 1 (top) with the wall state (T, H, D, M, K);
+        None returns that wall to the constant heat flux."""
+        v = None if state is None else np.ascontiguousarray(state, np.float64)
+        if self._lib.orc_thermal_set_isothermal(self._h, int(wall), None if v is None else _p(v)) != 0:
+            raise ValueError("thermal solver not enabled, bad wall, or a point outside the table")
 
     def thermal_substep(self, ns):
         return self._lib.orc_thermal_substep(self._h, int(ns))

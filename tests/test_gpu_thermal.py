@@ -106,3 +106,38 @@ def test_thermal_substeps_match_oracle_per_call():
         c.SOLVERRK3_MOM_io(ns)
     _compare(s, o, c, TOL)
     c.close()
+
+
+def _wall_state(ot, dh):
+    r, nbad, _ = ot.update(np.array([dh]))
+    assert nbad == 0
+    return [float(r[k][0]) for k in ("T", "H", "D", "M", "K")]
+
+
+def test_isothermal_walls_match_oracle():
+    """BC_Fixed_Temperature on both walls (iThermalWallType = 2, 2 as TC4 and TC6 set them):
+    the wall state from the table at a hotter bottom and a cooler top rho*h, held in the
+    ghost rows; the wall face of the energy equation keeps its conduction term.  Five
+    steps against the oracle at the same tolerance; the wall rows hold the state exactly,
+    and the fluid next to the hot wall heats up."""
+    s, o, ot, c = _case()
+    hot, cold = _wall_state(ot, 2e-3), _wall_state(ot, -2e-3)
+    for w, st in ((0, hot), (1, cold)):
+        o.thermal_set_isothermal(w, st)
+        c.thermal_set_isothermal(w, st)
+    t0 = _compare(s, o, c, 1e-14)["T"][:, 1:s.M + 1].mean(axis=(0, 2))
+    rc, _ = o.io_run_steps(5)
+    assert rc == 0
+    c.advance(5, 1e-3, 1e-6, 0.5)
+    tg = _compare(s, o, c, TOL)
+    M = s.M
+    assert np.all(tg["T"][:, 0] == hot[0]) and np.all(tg["T"][:, M + 1] == cold[0])
+    dt_rows = tg["T"][:, 1:M + 1].mean(axis=(0, 2)) - t0
+    assert dt_rows[0] > 0 > dt_rows[-1]  # the first rows warm at the hot wall and cool at the cold one
+    # back to the constant heat flux on the top wall
+    o.thermal_set_isothermal(1, None)
+    c.thermal_set_isothermal(1, None)
+    o.io_run_steps(2)
+    c.advance(2, 1e-3, 1e-6, 0.5)
+    _compare(s, o, c, TOL)
+    c.close()
