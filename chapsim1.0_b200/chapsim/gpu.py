@@ -43,7 +43,7 @@ EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_stri
             "chapsim_pp_monitor_tg", "chapsim_download_pp_means_tg", "chapsim_upload_pp_means_tg", "chapsim_divgck_io",
             "chapsim_pp_mean_zx_io", "chapsim_download_pp_means_io",
             "chapsim_write_dfile", "chapsim_read_dfile", "chapsim_dump_begin", "chapsim_dump_write",
-            "chapsim_mlp_set_activation", "chapsim_probe_wait_timeout", "chapsim_thermal_set_isothermal", "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
+            "chapsim_mlp_set_activation", "chapsim_probe_wait_timeout", "chapsim_thermal_set_isothermal", "chapsim_xinout_thermal_inlet", "chapsim_xinout_attach", "chapsim_advance_xinout", "chapsim_divgck_xinout", "chapsim_xinout_outlet_state"]
 
 # the arrays of one set of x-z means (postprocess_info), their widths per y row
 PP_ARRAYS = [("U1xzL", 4), ("UPxzL", 3), ("U2xzL", 6), ("U3xzL", 10), ("DVDL1xzL", 9), ("DVDLPxzL", 9), ("DVDL2xzL", 81)]
@@ -203,6 +203,7 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_mlp_set_activation.argtypes = [vp, ctypes.c_int32]
     L.chapsim_probe_wait_timeout.argtypes = [vp]
     L.chapsim_thermal_set_isothermal.argtypes = [vp, ctypes.c_int32, _dp]
+    L.chapsim_xinout_thermal_inlet.argtypes = [vp, _dp]
     L.chapsim_advance_xinout.argtypes = [vp, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp,
                                          _dp]
     L.chapsim_divgck_xinout.argtypes = [vp, _dp]
@@ -828,6 +829,10 @@ class ChannelXinout(ChannelIO):
         out = np.zeros(3)
         self._check(self.lib.chapsim_divgck_xinout(self.h, _ptr(out)))
         return out
+
+    def thermal_inlet(self, state7):
+        """BC_TINLET_THERML's inlet state (T, H, D, M, K, CP, DH) after thermal_init."""
+        self._check(self.lib.chapsim_xinout_thermal_inlet(self.h, _ptr(np.ascontiguousarray(state7, np.float64))))
 
     def outlet_state(self):
         """(U_OUTLET, CHK_Mass_CONSV0_SCALING) of the last substep."""

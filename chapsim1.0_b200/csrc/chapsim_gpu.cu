@@ -244,6 +244,10 @@ struct chapsim_ctx {
     double* xio_yd = nullptr;      // forward factors of the Poisson y-solve (L N M)
     double* xio_state = nullptr;   // U_OUTLET, CHK_Mass_CONSV0_SCALING of the last substep
     double* xio_part = nullptr;    // block maxima of the three divergence ranges
+    double* xio_bc0e = nullptr;    // BC_CONV0_ENG (M N)
+    double* xio_mpart = nullptr;   // block sums of the interior mass rate (io_grid)
+    XioInlet xio_in{};             // inlet state of the thermal solver (chapsim_xinout_thermal_inlet)
+    bool xio_in_set = false;
     cudaEvent_t xev[2] = {nullptr, nullptr};
     std::string err;
 };
@@ -776,6 +780,22 @@ MlpOperands mlp_ops(const chapsim_ctx* ctx) {
     return MlpOperands{ctx->mlp_w2, ctx->mlp_w3, ctx->mlp_w2t, ctx->mlp_w2h, ctx->mlp_w3h};
 }
 
+int xio_outlet_blocks(const chapsim_ctx* ctx);
+// BC_TINLET_THERML and BC_COUTLET_ENEG_RK3(NS) of the inflow/outflow domain (FP64)
+void xio_thermal_columns(chapsim_ctx* ctx, int ns) {
+    const Geo& g = ctx->g;
+    cudaStream_t s = ctx->stream;
+    IoFields f = io_fields(ctx);
+    const int gin = (int)std::min<long long>(4LL * ctx->nsm, ((long long)(g.M + 2) * g.N + XIO_NT - 1) / XIO_NT);
+    k_xio_thermal_inlet<<<gin, XIO_NT, 0, s>>>(g, f, ctx->tf, ctx->xio_in);
+    const int gout = xio_outlet_blocks(ctx);
+    k_xio_outlet_a<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_part);
+    k_xio_energy_outlet<<<gout, PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->xio_part, gout, ctx->xio_bc0e,
+                                                 ctx->st, ns);
+    prof_mark(ctx);
+    ctx->launches += 3;
+}
+
 // SOLVERRK3_ENG_io(NS), DENSITY_TIME_DERIVATION, DENSITY_Staggered,
 // MU_Staggered, then G0 = G and VELOCITY_CALC_io of SOLVERRK3_MOM_io
 template <typename F>
@@ -787,7 +807,15 @@ void launch_thermal_substep_t(chapsim_ctx* ctx, int ns) {
     prof_mark(ctx);
     const size_t sm = prop_smem(ctx->tab.n);
     const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
-    if (ctx->use_mlp) {
+    if (ctx->domain == 3) {
+        // inflow/outflow: props of the interior, then the inlet and outlet columns, then the walls
+        if (sm) k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        else k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+        prof_mark(ctx);
+        xio_thermal_columns(ctx, ns);
+        if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+        else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+    } else if (ctx->use_mlp) {
         const long long tiles = (tot + MLP_TILE - 1) / MLP_TILE;
         MlpOut out{ctx->tf.ENTH, ctx->tf.TEMP, f.DEN, f.MU, ctx->tf.KAP, ctx->tf.HCP, f.RHO, f.MU0};
         const int gi = (int)std::min<long long>(tiles, 4LL * ctx->nsm);
@@ -810,7 +838,7 @@ void launch_thermal_substep_t(chapsim_ctx* ctx, int ns) {
         k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     }
     prof_mark(ctx);
-    k_drhodt<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ns);
+    k_drhodt<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f, ctx->tf, ns, ctx->domain == 3 ? ctx->xio_mpart : nullptr);
     prof_mark(ctx);
     k_io_props<F><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     prof_mark(ctx);
@@ -900,6 +928,8 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     cudaStream_t s = ctx->stream;
     IoFields f = io_fields(ctx);
     const chapsim_ctx* tg = ctx->tg_in;
+    if (ctx->thermal) launch_thermal_substep_t<double>(ctx, ns);
+    const double* drho = ctx->thermal ? ctx->tf.DRHO : nullptr;
     const int gin = (int)std::min<long long>(4LL * ctx->nsm, ((long long)(g.M + 2) * g.N + XIO_NT - 1) / XIO_NT);
     k_xio_inlet<<<gin, XIO_NT, 0, s>>>(g, f, tg->Q, tg->PR, tg->g.L, tg->g.FS);
     prof_mark(ctx);
@@ -907,7 +937,8 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     k_xio_outlet_a<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_part);
     k_xio_outlet_b<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_bc0, ctx->xio_part, ctx->xio_part + 2 * gout, ctx->xio_state,
                                            ctx->st, ns);
-    k_xio_outlet_c<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_part + 2 * gout, ctx->xio_state, ctx->st);
+    k_xio_outlet_c<<<gout, XIO_NT, 0, s>>>(g, f, ctx->xio_part + 2 * gout, ctx->thermal ? ctx->xio_mpart : nullptr,
+                                           ctx->io_grid, ctx->xio_state, ctx->st);
     prof_mark(ctx);
     k_io_divu<double><<<ctx->io_grid, IO_NT, 0, s>>>(g, f);
     prof_mark(ctx);
@@ -921,9 +952,10 @@ void launch_xio_substep(chapsim_ctx* ctx, int ns) {
     dim3 gxf((g.M + XF_TJ - 1) / XF_TJ, g.N);
     const size_t smf = (size_t)XF_TJ * fft4s_ld(g.LI) * sizeof(double2);
     if (fftx) {
-        DISPATCH_FFT(g.LI, (k_xio_div_cosqf<FN1, FN2><<<gxf, PX_NT, smf, s>>>(g, f.G, ctx->xio_tq, ctx->SP, ctx->st, ns, 1.0)));
+        DISPATCH_FFT(g.LI, (k_xio_div_cosqf<FN1, FN2><<<gxf, PX_NT, smf, s>>>(g, f.G, ctx->xio_tq, ctx->SP, ctx->st, ns, 1.0,
+                                                                               drho)));
     } else {
-        k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cf, ctx->SP, ctx->st, ns, 1.0);
+        k_xio_div_dctx<<<nrb, XIO_NT, smem_xd(g), s>>>(g, f.G, ctx->xio_cf, ctx->SP, ctx->st, ns, 1.0, drho);
     }
     prof_mark(ctx);
     const long long nq = (long long)g.LH * g.M;  // LH = LI x modes
@@ -1209,6 +1241,9 @@ int chapsim_gpu_init(const chapsim_grid_t* grid, const chapsim_coefs_t* cf, cons
         INIT_CK(cudaMalloc(&ctx->xio_state, 2 * sizeof(double)));
         INIT_CK(cudaMemset(ctx->xio_state, 0, 2 * sizeof(double)));
         INIT_CK(cudaMalloc(&ctx->xio_part, (size_t)3 * ctx->npart_red * sizeof(double)));
+        INIT_CK(cudaMalloc(&ctx->xio_bc0e, (size_t)M * N * sizeof(double)));
+        INIT_CK(cudaMemset(ctx->xio_bc0e, 0, (size_t)M * N * sizeof(double)));
+        INIT_CK(cudaMalloc(&ctx->xio_mpart, (size_t)ctx->io_grid * sizeof(double)));
         INIT_CK(cudaEventCreateWithFlags(&ctx->xev[0], cudaEventDisableTiming));
         INIT_CK(cudaEventCreateWithFlags(&ctx->xev[1], cudaEventDisableTiming));
         if (smem_xd(g) > 48 * 1024) {
@@ -1299,7 +1334,7 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     if (ctx->dump_snap) cudaEventDestroy(ctx->dump_snap);
     if (ctx->dump_done) cudaEventDestroy(ctx->dump_done);
     if (ctx->dump_stream) cudaStreamDestroy(ctx->dump_stream);
-    cudaFree(ctx->xio_cf); cudaFree(ctx->xio_tq); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
+    cudaFree(ctx->xio_cf); cudaFree(ctx->xio_tq); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_bc0e); cudaFree(ctx->xio_mpart); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
     for (auto& e : ctx->xev)
         if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1754,6 +1789,8 @@ int chapsim_rk_substep_io(chapsim_ctx_t* ctx, int32_t ns) {
     if (ctx->domain == 3) {
         if (!ctx->tg_in) return fail(ctx, CHAPSIM_ERR_BADARG, "no TG context attached (chapsim_xinout_attach)");
         if (ns < 1) return fail(ctx, CHAPSIM_ERR_BADARG, "the inflow/outflow main domain has substeps NS = 1..3");
+        if (ctx->thermal && !ctx->xio_in_set)
+            return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal inflow needs its inlet state (chapsim_xinout_thermal_inlet)");
         CK(cudaStreamSynchronize(ctx->tg_in->stream));  // the TG substep NS feeds the inlet
         launch_xio_substep(ctx, ns);
         CK(cudaGetLastError());
@@ -1850,6 +1887,8 @@ int chapsim_advance_xinout(chapsim_ctx_t* io, int32_t nsteps, double dt0, double
     if (io->domain != 3) return fail(io, CHAPSIM_ERR_BADARG, "context was not created for the inflow/outflow main domain");
     if (!io->tg_in) return fail(io, CHAPSIM_ERR_BADARG, "no TG context attached (chapsim_xinout_attach)");
     if (nsteps < 0) return fail(io, CHAPSIM_ERR_BADARG, "nsteps < 0");
+    if (io->thermal && !io->xio_in_set)
+        return fail(io, CHAPSIM_ERR_BADARG, "the thermal inflow needs its inlet state (chapsim_xinout_thermal_inlet)");
     chapsim_ctx* tg = io->tg_in;
     chapsim_ctx* ctx = io;  // for CK
     CK(cudaSetDevice(io->device));
@@ -1871,12 +1910,30 @@ int chapsim_advance_xinout(chapsim_ctx_t* io, int32_t nsteps, double dt0, double
     return rc;
 }
 
+int chapsim_xinout_thermal_inlet(chapsim_ctx_t* ctx, const double* state7) {
+    if (!ctx || !state7) return fail(ctx, CHAPSIM_ERR_BADARG, "null argument");
+    if (ctx->domain != 3 || !ctx->thermal)
+        return fail(ctx, CHAPSIM_ERR_BADARG, "needs an inflow/outflow main domain with the thermal solver initialised");
+    for (int a = 0; a < 7; ++a)
+        if (!std::isfinite(state7[a])) return fail(ctx, CHAPSIM_ERR_BADARG, "non-finite inlet state");
+    CK(cudaSetDevice(ctx->device));
+    for (int a = 0; a < 7; ++a) ctx->xio_in.v[a] = state7[a];
+    ctx->xio_in_set = true;
+    const Geo& g = ctx->g;
+    const int gin = (int)std::min<long long>(4LL * ctx->nsm, ((long long)(g.M + 2) * g.N + XIO_NT - 1) / XIO_NT);
+    k_xio_thermal_inlet<<<gin, XIO_NT, 0, ctx->stream>>>(g, io_fields(ctx), ctx->tf, ctx->xio_in);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
 int chapsim_divgck_xinout(chapsim_ctx_t* ctx, double* maxdiv3) {
     if (!ctx || !maxdiv3) return CHAPSIM_ERR_BADARG;
     if (ctx->domain != 3) return fail(ctx, CHAPSIM_ERR_BADARG, "context was not created for the inflow/outflow main domain");
     CK(cudaSetDevice(ctx->device));
     const int nb = ctx->npart_red;
-    k_xio_divgck<<<nb, XIO_NT, 0, ctx->stream>>>(ctx->g, ctx->io.G, ctx->xio_part);
+    k_xio_divgck<<<nb, XIO_NT, 0, ctx->stream>>>(ctx->g, ctx->io.G, ctx->thermal ? ctx->tf.DRHO : nullptr, ctx->xio_part);
     ctx->launches += 1;
     CK(cudaGetLastError());
     std::vector<double> part((size_t)3 * nb);
@@ -2154,13 +2211,17 @@ void thermal_start(chapsim_ctx* ctx, size_t fb) {
     IoFieldsT<F> f = io_fields_t<F>(ctx);
     const size_t sm = prop_smem(ctx->tab.n);
     const long long tot = (long long)g.L * g.M * g.N, plane = 2LL * g.L * g.N;
-    if (sm) {
-        k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
-    } else {
-        k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
-        k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+    if (sm) k_eng_props<true, F><<<prop_grid(ctx, tot), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    else k_eng_props<false, F><<<prop_grid(ctx, tot), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+    if constexpr (sizeof(F) == 8) {
+        if (ctx->domain == 3) {  // the inlet and outlet columns from their rho*h
+            k_xio_ghost_props<<<prop_grid(ctx, 2LL * g.M * g.N), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->st);
+            cudaMemsetAsync(ctx->xio_bc0e, 0, (size_t)g.M * g.N * sizeof(double), s);
+            ctx->launches += 1;
+        }
     }
+    if (sm) k_eng_bc<true, F><<<prop_grid(ctx, plane), PROP_NT, sm, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
+    else k_eng_bc<false, F><<<prop_grid(ctx, plane), PROP_NT, 0, s>>>(ctx->tab, g, f, ctx->tf, ctx->tp, ctx->st);
     cudaMemcpyAsync(ctx->io.RHO, ctx->DEN, fb, cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(ctx->io.MU0, ctx->io.MU, fb, cudaMemcpyDeviceToDevice, s);
     if constexpr (sizeof(F) == 8) cudaMemcpyAsync(ctx->tf.G0, f.G, 3 * fb, cudaMemcpyDeviceToDevice, s);
@@ -2202,7 +2263,7 @@ extern "C" int chapsim_thermal_set_isothermal(chapsim_ctx_t* ctx, int32_t wall, 
 
 extern "C" int chapsim_thermal_init(chapsim_ctx_t* ctx, const double* dh, double qw_bot, double qw_top, double cthecd) {
     if (!ctx || !dh) return fail(ctx, CHAPSIM_ERR_BADARG, "null argument");
-    if (ctx->domain != 2) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver runs in the main (IO) domain");
+    if (ctx->domain < 2) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver runs in the main (IO) domain");
     if (!ctx->ptab) return fail(ctx, CHAPSIM_ERR_BADARG, "no property table (call chapsim_prop_table_init first)");
     if (!(cthecd > 0.0)) return fail(ctx, CHAPSIM_ERR_BADARG, "CTHECD must be positive");
     CK(cudaSetDevice(ctx->device));
@@ -2496,6 +2557,8 @@ extern "C" int chapsim_mlp_infer_points(chapsim_ctx_t* ctx, int64_t npts, const 
 extern "C" int chapsim_thermal_use_mlp(chapsim_ctx_t* ctx, int32_t enable) {
     if (!ctx || !ctx->thermal) return fail(ctx, CHAPSIM_ERR_BADARG, "the thermal solver is not active on this context");
     if (enable && !ctx->mlp_ready) return fail(ctx, CHAPSIM_ERR_BADARG, "MLP not initialised");
+    if (enable && ctx->domain == 3)
+        return fail(ctx, CHAPSIM_ERR_BADARG, "the inflow/outflow main domain updates its properties by table search");
     CK(cudaSetDevice(ctx->device));
     ctx->use_mlp = enable != 0;
     if (ctx->step_exec) {

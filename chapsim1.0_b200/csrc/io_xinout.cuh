@@ -33,6 +33,7 @@
 #pragma once
 #include "common.cuh"
 #include "io.cuh"
+#include "thermal.cuh"
 
 #define XIO_NT 256
 #define XD_R 32  // rows (j, k) per block of the cosine transforms
@@ -92,7 +93,8 @@ __global__ void __launch_bounds__(XIO_NT) k_fill(double* __restrict__ p, long lo
 // the previous one reduces over the whole plane); partial results per block, reduced by every
 // block in block order (deterministic).  BC0: BC_CONV0(J, K, IDR) as [IDR][K][J]; state[0] =
 // U_OUTLET, state[1] = CHK_Mass_CONSV0_SCALING of this substep; part: 2 doubles per block.
-// The interior mass rate is zero (flow only).
+// The interior mass rate (sum of DrhoDtP / DYFI) comes from k_drhodt's block sums with the thermal
+// solver on, and is zero without it.
 //   a: extremes of UCC = (u(L) + u(L+1)) / 2 (CONVCTION_OUTLET_U, method two)
 //   b: U_OUTLET = (max + min) / 2, the convective update of the outlet column (:36-58), and
 //      the inlet (u face 1) and outlet (u face L+1) fluxes of CHK_MassConsv_io
@@ -163,17 +165,21 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_outlet_b(Geo g, IoFields f, doub
     }
 }
 
+// mpart, nmp: the per-block sums of DrhoDtP / DYFI of k_drhodt (thermal solver on), else NULL
 __global__ void __launch_bounds__(XIO_NT) k_xio_outlet_c(Geo g, IoFields f, const double* __restrict__ partb,
+                                                         const double* __restrict__ mpart, int nmp,
                                                          double* __restrict__ state, DevState* __restrict__ st) {
     __shared__ double sc;
     if (threadIdx.x == 0) {
-        double a = 0.0, b = 0.0;
+        double a = 0.0, b = 0.0, mr = 0.0;
         for (int q = 0; q < (int)gridDim.x; ++q) {
             a += partb[2 * q];
             b += partb[2 * q + 1];
         }
+        if (mpart)
+            for (int q = 0; q < nmp; ++q) mr += mpart[q];
         const double flux_in = a / g.dzi, flux_out = b / g.dzi;
-        const double mass_rate = 0.0;
+        const double mass_rate = mr / g.dzi / g.dxi;
         sc = (flux_in - mass_rate) / flux_out;
         if (blockIdx.x == 0) {
             state[1] = sc;
@@ -239,7 +245,7 @@ __device__ __forceinline__ void xd_rows_times_matrix(const double* __restrict__ 
 // to shared memory, then SP[m + L ((j-1) + M k)] = (X(m), 0).
 __global__ void __launch_bounds__(XIO_NT, 2) k_xio_div_dctx(Geo g, const double* __restrict__ G, const double* __restrict__ CF,
                                                          double2* __restrict__ SP, const DevState* __restrict__ st,
-                                                         int ns, double wdiv) {
+                                                         int ns, double wdiv, const double* __restrict__ DRHO) {
     extern __shared__ double xsm[];
     const int L = g.LI, M = g.M, N = g.N;
     double* row = xsm;  // XD_R x L
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(XIO_NT, 2) k_xio_div_dctx(Geo g, const double*
         const double w = G[c + 2 * g.FS], wp = G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS];
         const double coe2 = g.dyfi[j] / 1.0;
         const double DIVX = (up - u) * coe1, DIVY = (vp - v) * coe2, DIVZ = (wp - w) * g.dzi;
-        const double DQ = DIVX + DIVY + DIVZ + 0.0;
+        const double DQ = DIVX + DIVY + DIVZ + (DRHO ? DRHO[c] / 1.0 : 0.0);
         row[r * L + (i - 1)] = DQ * coe0;
     }
     __syncthreads();
@@ -293,7 +299,7 @@ __global__ void __launch_bounds__(XIO_NT, 2) k_xio_div_dctx(Geo g, const double*
 template <int N1, int N2>
 __global__ void __launch_bounds__(PX_NT) k_xio_div_cosqf(Geo g, const double* __restrict__ G, const double2* __restrict__ TQ,
                                                          double2* __restrict__ SP, const DevState* __restrict__ st,
-                                                         int ns, double wdiv) {
+                                                         int ns, double wdiv, const double* __restrict__ DRHO) {
     extern __shared__ __align__(16) unsigned char xf_raw[];
     double2* smc = reinterpret_cast<double2*>(xf_raw);
     const int L = g.LI, M = g.M, N = g.N;
@@ -312,7 +318,7 @@ __global__ void __launch_bounds__(PX_NT) k_xio_div_cosqf(Geo g, const double* __
         const double w = G[c + 2 * g.FS], wp = G[pidx(g, i + 1, j, kp) + 2 * g.FS];
         const double coe2 = g.dyfi[j] / 1.0;
         const double DIVX = (up - u) * coe1, DIVY = (vp - v) * coe2, DIVZ = (wp - w) * g.dzi;
-        const double x = (DIVX + DIVY + DIVZ + 0.0) * coe0;
+        const double x = (DIVX + DIVY + DIVZ + (DRHO ? DRHO[c] / 1.0 : 0.0)) * coe0;
         const double cw = i == 0 ? x : 2.0 * x;
         const double2 t = TQ[i];
         smc[jl * LD + i] = make_double2(cw * t.x, cw * t.y);
@@ -464,9 +470,11 @@ __global__ void __launch_bounds__(XIO_NT, 2) k_xio_dctx_inv(Geo g, const double2
     (void)N;
 }
 
-// DIVGCK_io with TgFlowFlg: max |div G| over the cells 2..L-1, 0..1 and L (DrhoDtP = 0).
+// DIVGCK_io with TgFlowFlg: max |div G + DrhoDtP| over the cells 2..L-1, 0..1 and L (DRHO NULL
+// without the thermal solver).
 // partial[3 b + r] holds block b's maximum of range r.
-__global__ void __launch_bounds__(XIO_NT) k_xio_divgck(Geo g, const double* __restrict__ G, double* __restrict__ partial) {
+__global__ void __launch_bounds__(XIO_NT) k_xio_divgck(Geo g, const double* __restrict__ G, const double* __restrict__ DRHO,
+                                                       double* __restrict__ partial) {
     __shared__ double sred[32];
     const int L = g.LI, M = g.M, N = g.N;
     const long long tot = (long long)(L + 1) * M * N;  // cells i = 0..L
@@ -479,7 +487,7 @@ __global__ void __launch_bounds__(XIO_NT) k_xio_divgck(Geo g, const double* __re
         const double DIVX = (G[c + 1] - G[c]) * g.dxi;
         const double DIVY = (G[c + g.FS + g.L] - G[c + g.FS]) * (g.dyfi[j] * 1.0);
         const double DIVZ = (G[pidx(g, i, j, wrapp(k, N)) + 2 * g.FS] - G[c + 2 * g.FS]) * (g.dzi * 1.0);
-        const double a = fabs(DIVX + DIVY + DIVZ + 0.0);
+        const double a = fabs(DIVX + DIVY + DIVZ + (DRHO && i >= 1 ? DRHO[c] : 0.0));  // DrhoDtP of the interior
         const int r = (i >= 2 && i <= L - 1) ? 0 : (i <= 1 ? 1 : 2);
         mx[r] = fmax(mx[r], a);
     }
@@ -503,4 +511,74 @@ __global__ void k_dt_pair(DevState* __restrict__ tg, DevState* __restrict__ io) 
     tg->dt = dt;
     if ((dt / io->dt0) < 0.01) atomicOr(&io->err, CHS_EBIT_DT_COLLAPSE);
     if (!(dt == dt)) atomicOr(&io->err, CHS_EBIT_NAN);
+}
+
+// ---------------------------------------------------------------------------
+// Thermal inflow/outflow.  The inlet state (BC_TINLET_THERML, src/BC_INLET.f90:64-84):
+// v = T, H, D, M, K, CP, DH of the inlet (src/Flow_State.f90:44-50).
+struct XioInlet {
+    double v[7];
+};
+
+// The inlet ghost column, rows 0..M+1 (DENSITY0 and Viscousity0 keep the previous values, the
+// whole-field copies at the top of SOLVERRK3_ENG_io)
+__global__ void __launch_bounds__(XIO_NT) k_xio_thermal_inlet(Geo g, IoFields f, ThermoFields t, XioInlet in) {
+    const long long tot = (long long)(g.M + 2) * g.N;
+    for (long long q = (long long)blockIdx.x * XIO_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * XIO_NT) {
+        const int j = (int)(q % (g.M + 2)), k = (int)(q / (g.M + 2));
+        const long long p = pidx(g, 0, j, k);
+        f.RHO[p] = f.DEN[p];
+        f.MU0[p] = f.MU[p];
+        t.TEMP[p] = in.v[0];
+        t.KAP[p] = in.v[4];
+        f.DEN[p] = in.v[2];
+        f.MU[p] = in.v[3];
+        t.HCP[p] = in.v[5];
+        t.DH[p] = in.v[6];
+        t.ENTH[p] = in.v[1];
+    }
+}
+
+// BC_COUTLET_ENEG_RK3(NS) (src/BC_COUTLET_ENEG_RK3.f90:11-59): U_OUTLET from the extremes of
+// k_xio_outlet_a (on the current velocity), the convective RK3 update of the outlet column's
+// rho*h with BC_CONV0_ENG (BC0E, [K][J]), the table limiter, THERM_PROP_UPDATE(IOULET) on rows
+// 1..M of column L+1
+__global__ void __launch_bounds__(PROP_NT) k_xio_energy_outlet(PropTab tb, Geo g, IoFields f, ThermoFields t,
+                                                               ThermoParams tp, const double* __restrict__ parta,
+                                                               int npa, double* __restrict__ BC0E, DevState* st,
+                                                               int ns) {
+    __shared__ double uo;
+    if (threadIdx.x == 0) {
+        double mx = -1.0E20, mn = 1.0E20;
+        for (int b = 0; b < npa; ++b) {
+            mx = fmax(mx, parta[2 * b]);
+            mn = fmin(mn, parta[2 * b + 1]);
+        }
+        uo = 0.5 * (mx + mn);
+    }
+    __syncthreads();
+    const int M = g.M, np = M * g.N, L = g.LI;
+    const double dt = st->dt, tg = g.tgam[ns], tr = g.troh[ns];
+    for (int p = blockIdx.x * PROP_NT + threadIdx.x; p < np; p += gridDim.x * PROP_NT) {
+        const int j = 1 + p % M, k = p / M;
+        const long long c = pidx(g, L, j, k), co = c + 1;
+        const double bc_conv = -g.dxi * uo * (t.DH[co] - t.DH[c]);
+        const double bc_rhs = tg * bc_conv + tr * BC0E[p];
+        BC0E[p] = bc_conv;
+        double d = t.DH[co] + dt * bc_rhs;
+        d = fmin(tp.dhmax - 1.0e-14, d);
+        d = fmax(tp.dhmin + 1.0e-14, d);
+        t.DH[co] = d;
+        eng_point(tb, tb.xdh, tb.xh, f, t, co, st);
+    }
+}
+
+// Properties of the inlet and outlet columns (rows 1..M) from their rho*h, at the thermal start
+__global__ void __launch_bounds__(PROP_NT) k_xio_ghost_props(PropTab tb, Geo g, IoFields f, ThermoFields t, DevState* st) {
+    const int M = g.M, np = M * g.N;
+    for (int q = blockIdx.x * PROP_NT + threadIdx.x; q < 2 * np; q += gridDim.x * PROP_NT) {
+        const int side = q >= np, p = side ? q - np : q;
+        const int j = 1 + p % M, k = p / M;
+        eng_point(tb, tb.xdh, tb.xh, f, t, pidx(g, side ? g.LI + 1 : 0, j, k), st);
+    }
 }

@@ -41,8 +41,8 @@ struct ThermoParams {
 template <typename F>
 __global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFieldsT<F> f, ThermoFields t, ThermoParams tp,
                                                    const DevState* __restrict__ st, int ns) {
-    const int L = g.L, M = g.M, N = g.N;
-    const long long tot = (long long)L * M * N;
+    const int M = g.M, N = g.N;
+    const long long tot = io_points(g);
     const double dt = st->dt;
     const double coe1n = g.tgam[ns] * dt, coe0n = g.troh[ns] * dt;
     const double XND2CL = 0.5, ZND2CL = 0.5;
@@ -57,7 +57,7 @@ __global__ void __launch_bounds__(IO_NT, 4) k_eng_rhs(Geo g, IoFieldsT<F> f, The
     for (long long q = (long long)blockIdx.x * IO_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, q, i, j, k);
-        const int ip = wrapp(i, L), im = wrapm(i, L), kp = wrapp(k, N), km = wrapm(k, N);
+        const int ip = xpn(g, i), im = xmn(g, i), kp = wrapp(k, N), km = wrapm(k, N);
         const int jp = j + 1, jm = j - 1;
         const long long c = pidx(g, i, j, k);
         const long long cip = pidx(g, ip, j, k), cim = pidx(g, im, j, k);
@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(PROP_NT) k_eng_props(PropTab tb, Geo g, IoFiel
     const double* xdh = tb.xdh;
     const double* xh = tb.xh;
     if (SMEM) stage_keys(tb, keys, xdh, xh);
-    const long long tot = (long long)g.L * g.M * g.N;
+    const long long tot = io_points(g);
     for (long long q = (long long)blockIdx.x * PROP_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * PROP_NT) {
         int i, j, k;
         io_decode(g, q, i, j, k);
@@ -184,10 +184,14 @@ __global__ void __launch_bounds__(PROP_NT) k_eng_bc(PropTab tb, Geo g, IoFieldsT
     }
 }
 
+// mpart (inflow/outflow domain, else NULL): per-block sums of DrhoDtP / DYFI for the interior mass
+// rate of CHK_MassConsv_io (src/processing/CHK_conservation.f90:41-53)
 template <typename F>
-__global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFieldsT<F> f, ThermoFields t, int ns) {
-    const int L = g.L, N = g.N;
-    const long long tot = (long long)L * g.M * N;
+__global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFieldsT<F> f, ThermoFields t, int ns, double* __restrict__ mpart) {
+    __shared__ double sred[32];
+    const int N = g.N;
+    const long long tot = io_points(g);
+    double ms = 0.0;
     const double tgam = g.tgam[ns], troh = g.troh[ns];
     const F* G = f.G;
     const double* G0 = t.G0;
@@ -195,7 +199,7 @@ __global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFieldsT<F> f, ThermoF
         int i, j, k;
         io_decode(g, q, i, j, k);
         const long long c = pidx(g, i, j, k);
-        const long long cip = pidx(g, wrapp(i, L), j, k), ckp = pidx(g, i, j, wrapp(k, N)), cjp = pidx(g, i, j + 1, k);
+        const long long cip = pidx(g, xpn(g, i), j, k), ckp = pidx(g, i, j, wrapp(k, N)), cjp = pidx(g, i, j + 1, k);
         const double COE2 = g.dyfi[j] * 1.0, COE3 = g.dzi * 1.0;
         const double DIVX = ((double)G[cip] - (double)G[c]) * g.dxi;
         const double DIVX0 = (G0[cip] - G0[c]) * g.dxi;
@@ -203,7 +207,13 @@ __global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFieldsT<F> f, ThermoF
         const double DIVY0 = (G0[cjp + g.FS] - G0[c + g.FS]) * COE2;
         const double DIVZ = ((double)G[ckp + 2 * g.FS] - (double)G[c + 2 * g.FS]) * COE3;
         const double DIVZ0 = (G0[ckp + 2 * g.FS] - G0[c + 2 * g.FS]) * COE3;
-        t.DRHO[c] = -tgam * (DIVX + DIVY + DIVZ) - troh * (DIVX0 + DIVY0 + DIVZ0);
+        const double dr = -tgam * (DIVX + DIVY + DIVZ) - troh * (DIVX0 + DIVY0 + DIVZ0);
+        t.DRHO[c] = dr;
+        if (mpart) ms += dr * (1.0 / g.dyfi[j] / 1.0);
+    }
+    if (mpart) {
+        const double b = block_sum<IO_NT>(ms, sred);
+        if (threadIdx.x == 0) mpart[blockIdx.x] = b;
     }
 }
 
@@ -211,7 +221,7 @@ __global__ void __launch_bounds__(IO_NT) k_drhodt(Geo g, IoFieldsT<F> f, ThermoF
 // G0 is FP64 in both precisions (a copy of the FP32 G in the mixed step).
 template <typename F>
 __global__ void __launch_bounds__(IO_NT) k_g0_velocity(Geo g, IoFieldsT<F> f, double* __restrict__ G0) {
-    const long long tot = (long long)g.L * g.M * g.N;
+    const long long tot = io_points(g);
     for (long long q = (long long)blockIdx.x * IO_NT + threadIdx.x; q < tot; q += (long long)gridDim.x * IO_NT) {
         int i, j, k;
         io_decode(g, q, i, j, k);
@@ -220,6 +230,10 @@ __global__ void __launch_bounds__(IO_NT) k_g0_velocity(Geo g, IoFieldsT<F> f, do
         G0[c] = g1;
         G0[c + g.FS] = g2;
         G0[c + 2 * g.FS] = g3;
+        if (g.xo && (i == 1 || i == g.LI)) {  // G0_io = G_io takes the inlet and outlet ghost columns too
+            const long long e = i == 1 ? c - 1 : c + 1;
+            for (int d = 0; d < 3; ++d) G0[e + d * g.FS] = (double)f.G[e + d * g.FS];
+        }
         f.Q[c] = (F)(g1 / (double)f.DST[c]);
         f.Q[c + 2 * g.FS] = (F)(g3 / (double)f.DST[c + 2 * g.FS]);
         if (j >= 2) f.Q[c + g.FS] = (F)(g2 / (double)f.DST[c + g.FS]);

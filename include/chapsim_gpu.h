@@ -241,16 +241,17 @@ int chapsim_divgck_io(chapsim_ctx_t* ctx, double* maxdiv);
 int chapsim_probe_wait_timeout(chapsim_ctx_t* ctx);
 
 /* ---- Main domain with inflow and outflow (grid.idomain = 3): the IO part of a
- * TG + main-domain run (iDomain = 3, TgFlowFlg and IoFlowFlg), flow only
- * (iThermoDynamics = 0, or before timeThermoStart), explicit viscous terms, FP64.
+ * TG + main-domain run (iDomain = 3, TgFlowFlg and IoFlowFlg), explicit viscous terms, FP64,
+ * flow only or with the thermal solver (chapsim_xinout_thermal_inlet).
  * Fields carry the x ghost columns NCL1S:NCL1E = 0:NCL1+1: chapsim_upload_io_fields /
  * chapsim_download_io_fields take (0:NCL1+1, 0:NCL2+1, NCL3) arrays (and G_io(..., 3));
  * the upload also sets the ghost columns' velocity to G over the x average of DENSITY0
  * of the column and its interior neighbour, and zeroes BC_CONV0.  No bulk forcing
- * (src/RHS_MOM_EXPLICIT_io.f90:229); chapsim_set_buoyancy, chapsim_cfl_io and
- * chapsim_divgck_io (max over the cells 1..NCL1) apply; the thermal solver, iWeightedPre,
- * the main-domain statistics, chapsim_advance_tg, chapsim_autotune and
- * chapsim_profile_steps do not (CHAPSIM_ERR_BADARG). */
+ * (src/RHS_MOM_EXPLICIT_io.f90:229); chapsim_set_buoyancy, chapsim_cfl_io,
+ * chapsim_divgck_io (max over the cells 1..NCL1) and the thermal solver (table search; see
+ * chapsim_xinout_thermal_inlet) apply; iWeightedPre, the learned property model, the
+ * main-domain statistics, chapsim_advance_tg, chapsim_autotune and chapsim_profile_steps do
+ * not (CHAPSIM_ERR_BADARG). */
 
 /* The periodic TG context whose fields feed BC_TINLET_FLOW (src/BC_INLET.f90:12-61):
  * FP64, same device, same NCL2, NCL3 and y mesh (the x spacing must match, as
@@ -272,6 +273,15 @@ int chapsim_xinout_attach(chapsim_ctx_t* io, chapsim_ctx_t* tg);
  * CHAPSIM_ERR_DT_COLLAPSE as chapsim_advance_tg. */
 int chapsim_advance_xinout(chapsim_ctx_t* io, int32_t nsteps, double dt0, double dtmin, double cflgv, double* dt_out,
                            double* cfl_out);
+/* Thermal inflow/outflow (iThermoDynamics = 1 with TgFlowFlg): after chapsim_thermal_init on the
+ * idomain = 3 context (DH over 0:NCL1+1; the inlet and outlet columns' properties follow from it),
+ * state7 = T_inlet, H_inlet, D_inlet, M_inlet, K_inlet, CP_inlet, DH_inlet (src/Flow_State.f90:
+ * 44-50).  Each substep then runs SOLVERRK3_ENG_io with BC_TINLET_THERML (src/BC_INLET.f90:64-84:
+ * the inlet column holds that state) and BC_COUTLET_ENEG_RK3 (src/BC_COUTLET_ENEG_RK3.f90:11-59:
+ * convective outflow of rho*h with the table limiter, THERM_PROP_UPDATE(IOULET)), and the outflow
+ * scaling of BC_COUTLET_MOM_RK3 takes the interior mass rate of DrhoDtP.  Table search only
+ * (chapsim_thermal_use_mlp is CHAPSIM_ERR_BADARG here). */
+int chapsim_xinout_thermal_inlet(chapsim_ctx_t* ctx, const double* state7);
 /* DIVGCK_io with TgFlowFlg (src/DIVGCK.f90:80-84): MAXDIVGV_io(1:3), the max |div G| over
  * the cells 2..NCL1-1, 0..1 and NCL1 (DrhoDtP = 0). */
 int chapsim_divgck_xinout(chapsim_ctx_t* ctx, double* maxdiv3);

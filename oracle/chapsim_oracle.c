@@ -83,6 +83,11 @@ typedef struct {
        FISHPACK x roots -XRT (LPEROD = 4), U_OUTLET and CHK_Mass_CONSV0_SCALING of the last step */
     double *BCCONV0, *AKX;
     double U_OUTLET, MASS_SCALING;
+    /* thermal inflow/outflow: BC_CONV0_ENG (src/MEMALLOCT.f90:173) and the inlet state T, H, D, M, K,
+       CP, DH of BC_TINLET_THERML (src/Flow_State.f90:44-50) */
+    double* BCCONV0E;
+    double XIN[7];
+    int xin_set;
 } orc_t;
 
 #define FOFF(o, i, j, k) ((size_t)((i) - 1 + (o)->xo) + (size_t)(o)->LS * ((size_t)(j) + (size_t)((o)->M + 2) * (size_t)((k) - 1)))
@@ -333,6 +338,7 @@ static orc_t* create_impl(int L, int M, int N, double HX, double HZ, double STR2
             o->AKX[I] = 4.0 * o->DXQI * (sn * sn);
         }
         o->BCCONV0 = dalloc(3 * (size_t)M * (size_t)N);
+        o->BCCONV0E = dalloc((size_t)M * (size_t)N);
     }
     return o;
 }
@@ -361,7 +367,7 @@ void orc_destroy(orc_t* o) {
     free(o->G); free(o->EXPLT0); free(o->RHO); free(o->MU0); free(o->MU); free(o->DSTG); free(o->MUSTG);
     free(o->DIVU); free(o->DRHODT); free(o->DEN); free(o->DRHOI);
     free(o->DH); free(o->ENTH); free(o->TEMP); free(o->KAPPA); free(o->HCP); free(o->RHSE); free(o->RHSE0); free(o->G0);
-    free(o->BCCONV0); free(o->AKX);
+    free(o->BCCONV0); free(o->AKX); free(o->BCCONV0E);
     free(o);
 }
 
@@ -2195,6 +2201,63 @@ static void density_time_derivation(orc_t* o, int NS) {
     }
 }
 
+/* BC_TINLET_THERML (src/BC_INLET.f90:64-84): the inlet ghost column holds the inlet state */
+static void xio_thermal_inlet(orc_t* o) {
+    int M = o->M, N = o->N;
+    for (int J = 0; J <= M + 1; ++J)
+        for (int K = 1; K <= N; ++K) {
+            F3(o->TEMP, o, 0, J, K) = o->XIN[0];
+            F3(o->KAPPA, o, 0, J, K) = o->XIN[4];
+            F3(o->DEN, o, 0, J, K) = o->XIN[2];
+            F3(o->MU, o, 0, J, K) = o->XIN[3];
+            F3(o->HCP, o, 0, J, K) = o->XIN[5];
+            F3(o->DH, o, 0, J, K) = o->XIN[6];
+            F3(o->ENTH, o, 0, J, K) = o->XIN[1];
+        }
+}
+
+/* BC_COUTLET_ENEG_RK3(NS) (src/BC_COUTLET_ENEG_RK3.f90:11-59): U_OUTLET of CONVCTION_OUTLET_U on  */
+/* the current velocity, the convective RK3 update of the outlet column's rho*h with BC_CONV0_ENG, */
+/* the table limiter, then THERM_PROP_UPDATE(IOULET) (rows 1..M of column L+1)                    */
+static void xio_energy_outlet(orc_t* o, int NS) {
+    int L = o->L, M = o->M, N = o->N;
+    double UxMax = -1.0E20, UxMin = 1.0E20;
+    for (int K = 1; K <= N; ++K)
+        for (int J = 1; J <= M; ++J) {
+            double UCC = (QV(o, L, J, K, 1) + QV(o, L + 1, J, K, 1)) * 0.5;
+            if (UCC > UxMax) UxMax = UCC;
+            if (UCC < UxMin) UxMin = UCC;
+        }
+    double U_OUTLET = 0.5 * (UxMax + UxMin);
+    const double REALMIN = 1.0e-14;
+    for (int K = 1; K <= N; ++K)
+        for (int J = 1; J <= M; ++J) {
+            double BC_CONV = -o->DXI * U_OUTLET * (F3(o->DH, o, L + 1, J, K) - F3(o->DH, o, L, J, K));
+            double* b0 = o->BCCONV0E + (size_t)(J - 1) + (size_t)M * (size_t)(K - 1);
+            double BC_RHS = o->TGAM[NS] * BC_CONV + o->TROH[NS] * (*b0);
+            *b0 = BC_CONV;
+            F3(o->DH, o, L + 1, J, K) = F3(o->DH, o, L + 1, J, K) + o->DT * BC_RHS;
+        }
+    for (int K = 1; K <= N; ++K)
+        for (int J = 1; J <= M; ++J) {
+            double d = F3(o->DH, o, L + 1, J, K);
+            d = fmin(o->DHMAX - REALMIN, d);
+            d = fmax(o->DHMIN + REALMIN, d);
+            F3(o->DH, o, L + 1, J, K) = d;
+        }
+    for (int J = 1; J <= M; ++J)
+        for (int K = 1; K <= N; ++K) thermal_point(o, L + 1, J, K);
+}
+
+/* The inlet state of a thermal TG + main-domain run: v = T, H, D, M, K, CP, DH (applied at once) */
+int orc_xio_thermal_inlet(orc_t* o, const double* v) {
+    if (!o->xo || !o->thermal) return -1;
+    for (int a = 0; a < 7; ++a) o->XIN[a] = v[a];
+    o->xin_set = 1;
+    xio_thermal_inlet(o);
+    return 0;
+}
+
 /* Energy part of RK substep NS and the property / density coupling that
  * precedes SOLVERRK3_MOM_io(NS).  Returns nonzero when a point fell outside
  * the property table (the reference STOPs there). */
@@ -2218,6 +2281,10 @@ int orc_thermal_substep(orc_t* o, int NS) {
             }
     o->prop_err = 0;
     thermal_props_interior(o);
+    if (o->xo) {
+        xio_thermal_inlet(o);
+        xio_energy_outlet(o, NS);
+    }
     thermal_bc(o);
     density_time_derivation(o, NS);
     io_staggered_props(o);
@@ -2249,6 +2316,14 @@ int orc_thermal_enable(orc_t* o, void* tab, const double* DH, double qw_bot, dou
     memset(o->RHSE0, 0, fs * sizeof(double));
     o->prop_err = 0;
     thermal_props_interior(o);
+    if (o->xo) { /* the inlet and outlet columns from their given rho*h */
+        for (int J = 1; J <= o->M; ++J)
+            for (int K = 1; K <= o->N; ++K) {
+                thermal_point(o, 0, J, K);
+                thermal_point(o, o->L + 1, J, K);
+            }
+        memset(o->BCCONV0E, 0, (size_t)o->M * (size_t)o->N * sizeof(double));
+    }
     thermal_bc(o);
     memcpy(o->MU0, o->MU, fs * sizeof(double));
     memcpy(o->RHO, o->DEN, fs * sizeof(double));
@@ -2549,8 +2624,9 @@ static void poisson_xinout(orc_t* o, const double* src, double* dst) {
 
 /* SOLVERRK3_MOM_io(NS) with TgFlowFlg (src/SOLVERRK3_MOM_IO.f90:11-120), iVisScheme = 0 */
 int orc_xio_substep(orc_t* o, const orc_t* tg, int NS) {
-    if (!o->io || !o->xo || tg->xo || tg->M != o->M || tg->N != o->N || NS < 1 || NS > 3 || o->ivis || o->thermal)
+    if (!o->io || !o->xo || tg->xo || tg->M != o->M || tg->N != o->N || NS < 1 || NS > 3 || o->ivis)
         return -1;
+    if (o->thermal) memcpy(o->G0, o->G, 3 * FSZ(o) * sizeof(double));  /* G0_io = G_io (:25) */
     io_velocity_calc(o);
     xio_inlet(o, tg);
     xio_outlet(o, NS);
@@ -2590,6 +2666,10 @@ int orc_xio_run_steps(orc_t* o, orc_t* tg, int nsteps, double* cfl_dt) {
         if ((dt / o->DT0) < 0.01) return 1;
         for (int NS = 1; NS <= 3; ++NS) {
             orc_substep(tg, NS);
+            if (o->thermal) {
+                if (!o->xin_set) return 3;
+                if (orc_thermal_substep(o, NS)) return 4;
+            }
             if (orc_xio_substep(o, tg, NS)) return 2;
         }
     }

@@ -127,6 +127,8 @@ def lib():
         L.orc_xio_akx.restype = ctypes.c_double
         L.orc_xio_akz.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_xio_akz.restype = ctypes.c_double
+        L.orc_xio_thermal_inlet.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_xio_thermal_inlet.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -386,6 +388,12 @@ class OracleXinout(Oracle):
         out = np.zeros(self.field_shape())
         self._lib.orc_xio_poisson(self._h, _p(rhs), _p(out))
         return out
+
+    def xio_thermal_inlet(self, state7):
+        """BC_TINLET_THERML's inlet state (T, H, D, M, K, CP, DH), applied at once and every substep."""
+        v = np.ascontiguousarray(state7, np.float64)
+        if self._lib.orc_xio_thermal_inlet(self._h, _p(v)) != 0:
+            raise ValueError("thermal solver not enabled")
 
     def akx(self):
         return np.array([self._lib.orc_xio_akx(self._h, i) for i in range(1, self.L + 1)])

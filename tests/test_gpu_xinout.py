@@ -17,6 +17,7 @@ import math
 import numpy as np
 import pytest
 
+import oracle as orc
 from oracle import Oracle, OracleXinout
 from chapsim import gpu
 from chapsim.mesh import channel_setup, xinout_setup
@@ -126,4 +127,46 @@ def test_inflow_outflow_contract_errors():
     with pytest.raises(gpu.ChapsimError):
         gpu.ChannelXinout(s, precision="mixed")
     for h in (io, other, mixed):
+        h.close()
+
+
+def test_thermal_inflow_outflow_matches_oracle():
+    """The same coupled case with the thermal solver on the main domain (TC7's setting: constant
+    wall heat flux, explicit viscous terms): BC_TINLET_THERML, BC_COUTLET_ENEG_RK3, DrhoDtP in
+    DIVG_io and in the outflow scaling.  Flow and thermal fields with their ghost columns within
+    1e-10 after three steps, and U_OUTLET and the scaling to round-off."""
+    from chapsim import thermo
+    LT, L, M, N, qw = 32, 64, 32, 32, 0.5
+    otg, oio, tg, io = _pair(LT, L, M, N)
+    rows, T0 = thermo.synthetic_table()
+    tab = thermo.SplineTable.from_rows(rows, T0)
+    cthecd = 1.0 / REN / (tab.ref["M0"] * tab.ref["CP0"] / tab.ref["K0"])
+    DH = np.zeros(oio.field_shape())
+    DH[:, 1:M + 1, :] = 1e-3 * np.random.default_rng(5).uniform(-1.0, 1.0, (N, M, L + 2))
+    ot = orc.PropTable(tab.lists)
+    oio.thermal_enable(ot, DH, qw, qw, cthecd)
+    io.thermal_init(tab, DH, qw, qw, cthecd)
+    r, nbad, _ = ot.update(np.array([0.0]))
+    st = [float(r[k][0]) for k in ("T", "H", "D", "M", "K", "CP")]
+    inlet = st + [st[2] * st[1]]
+    oio.xio_thermal_inlet(inlet)
+    io.thermal_inlet(inlet)
+    for step in range(3):
+        rc, cfl_dt = oio.xio_run_steps(otg, 1)
+        assert rc == 0
+        dt, cfl = io.advance(1, 1e-3, 1e-6, 0.5)
+        assert abs(dt - oio.dt()) <= 1e-13 * oio.dt()
+        d = _compare(oio, io, M, L)
+        to, tg_ = oio.thermal_get(), io.download_thermal()
+        for k in ("DH", "T", "D", "M", "K"):
+            d[k] = rel(tg_[k][:, 1:M + 1], to[k][:, 1:M + 1])
+        uo, so = oio.xio_outlet_state()
+        ug, sg = io.outlet_state()
+        print(step, d, "U_OUTLET", ug, uo, "scaling", sg, so)
+        assert max(d.values()) <= TOL, d
+        assert abs(ug - uo) <= 1e-11 * abs(uo) and abs(sg - so) <= 1e-12
+    dv_o, dv_g = oio.xio_divgck(), io.DIVGCK_io()
+    print("divergence ranges", dv_g, dv_o)
+    assert dv_g[0] < 1e-11 and dv_g[2] < 1e-11
+    for h in (io, tg, oio, otg):
         h.close()

@@ -15,6 +15,9 @@ checked on the CPU before it is trusted as the checker of the device path.
   cell next to the inlet keeps a residual: FISHPACK's mirror condition
   x(0) = x(2) is not the one-sided condition of the fixed inlet face, and the
   reference has the same residual.
+* With the thermal solver (BC_TINLET_THERML, BC_COUTLET_ENEG_RK3): the inlet
+  column holds the inlet state, the heated walls raise the mean rho*h, and
+  the cells 2..L stay divergence-free against DrhoDtP.
 """
 import math
 
@@ -100,5 +103,46 @@ def test_coupled_run_inlet_outlet_and_projection():
     div = io.xio_divgck()
     assert div[0] < 1e-12 and div[2] < 1e-12, div  # cells 2..L-1 and L
     assert div[1] < 1e-2, div  # cells 0..1: the inlet cell's residual
+    tg.close()
+    io.close()
+
+
+def thermal_case(LT=32, L=64, M=32, N=32, qw=0.5, threads=8):
+    """The coupled flow case plus the thermal solver on the main domain: the seeded synthetic
+    table, rho*h perturbed by 1e-3 (interior and both ghost columns), the inlet state from the
+    table at rho*h = 0, a constant heat flux on both walls."""
+    import oracle as orc
+    from chapsim import thermo
+    tg, io = coupled_case(LT, L, M, N, threads=threads)
+    rows, T0 = thermo.synthetic_table()
+    tab = thermo.SplineTable.from_rows(rows, T0)
+    cthecd = 1.0 / REN / (tab.ref["M0"] * tab.ref["CP0"] / tab.ref["K0"])
+    DH = np.zeros(io.field_shape())
+    DH[:, 1:M + 1, :] = 1e-3 * np.random.default_rng(5).uniform(-1.0, 1.0, (N, M, L + 2))
+    ot = orc.PropTable(tab.lists)
+    io.thermal_enable(ot, DH, qw, qw, cthecd)
+    r, nbad, _ = ot.update(np.array([0.0]))
+    assert nbad == 0
+    st = [float(r[k][0]) for k in ("T", "H", "D", "M", "K", "CP")]
+    inlet = st + [st[2] * st[1]]
+    io.xio_thermal_inlet(inlet)
+    return tg, io, ot, tab, DH, cthecd, inlet
+
+
+def test_thermal_inflow_outflow_oracle_run():
+    """BC_TINLET_THERML holds the inlet column at the inlet state, BC_COUTLET_ENEG_RK3 carries
+    rho*h out, the heated walls raise the mean rho*h, and the interior stays divergence-free
+    against DrhoDtP (DIVGCK_io adds it)."""
+    tg, io, ot, tab, DH, cthecd, inlet = thermal_case()
+    L, M = io.L, io.M
+    rc, _ = io.xio_run_steps(tg, 3)
+    assert rc == 0
+    th = io.thermal_get()
+    # rows 1..M of the inlet column (BC_WALL_THERMAL then re-extrapolates its wall rows)
+    assert np.all(th["DH"][:, 1:M + 1, 0] == inlet[6]) and np.all(th["T"][:, 1:M + 1, 0] == inlet[0])
+    assert np.isfinite(th["DH"]).all()
+    assert th["DH"][:, 1:M + 1, 1:L + 1].mean() > DH[:, 1:M + 1, 1:L + 1].mean()
+    div = io.xio_divgck()
+    assert div[0] < 1e-11 and div[2] < 1e-11, div
     tg.close()
     io.close()
