@@ -533,11 +533,11 @@ int configure_kernels(chapsim_ctx* ctx) {
     DISPATCH_FFT(g.N, CK(set_smem(k_fftz<+1, FN1, FN2, double2>, smem_fz(g))));
     if (ctx->domain == 2 && ctx->ivis) {
         DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S, double>, smem_cn(g.L))));
-        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S, double>, smem_cnz(g.N))));
-        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S, double>, smem_cnz(g.M))));
+        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S, double>, smem_cn(g.N))));
+        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S, double>, smem_cn(g.M))));
         DISPATCH_S(g.L / 32, CK(set_smem(k_io_cn_xsweep<S, float>, smem_cn(g.L))));
-        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S, float>, smem_cnz(g.N))));
-        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S, float>, smem_cnz(g.M))));
+        DISPATCH_S(g.N / 32, CK(set_smem(k_io_cn_zsweep<S, float>, smem_cn(g.N))));
+        DISPATCH_S(g.M / 32, CK(set_smem(k_io_cn_ysweep<S, float>, smem_cn(g.M))));
     }
     return CHAPSIM_OK;
 }
@@ -876,9 +876,9 @@ void launch_io_substep_t(chapsim_ctx* ctx, int ns) {
         dim3 gx((unsigned)((g.M * (long long)g.N + CN_LINES - 1) / CN_LINES), 3);
         DISPATCH_S(g.L / 32, (k_io_cn_xsweep<S, F><<<gx, CN_NT, smem_cn(g.L), s>>>(g, f, ctx->st, ns)));
         prof_mark(ctx);
-        dim3 gz(g.L / CNZ_LINES, g.M, 3), gy(g.L / CNZ_LINES, g.N, 3);
-        DISPATCH_S(g.N / 32, (k_io_cn_zsweep<S, F><<<gz, CNZ_NT, smem_cnz(g.N), s>>>(g, f, ctx->st, ns)));
-        DISPATCH_S(g.M / 32, (k_io_cn_ysweep<S, F><<<gy, CNZ_NT, smem_cnz(g.M), s>>>(g, f, ctx->st, ns)));
+        dim3 gz(g.L / CN_LINES, g.M, 3), gy(g.L / CN_LINES, g.N, 3);
+        DISPATCH_S(g.N / 32, (k_io_cn_zsweep<S, F><<<gz, CN_NT, smem_cn(g.N), s>>>(g, f, ctx->st, ns)));
+        DISPATCH_S(g.M / 32, (k_io_cn_ysweep<S, F><<<gy, CN_NT, smem_cn(g.M), s>>>(g, f, ctx->st, ns)));
         prof_mark(ctx);
         ctx->launches += 1;
     }

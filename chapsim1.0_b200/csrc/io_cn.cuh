@@ -23,9 +23,9 @@
 //
 // One warp solves one line held in shared memory (warp_tdma of tdma.cuh:
 // per-lane Thomas on segments of S rows, PCR over the 32 lanes).  A block
-// holds CN_LINES lines (x) or CNZ_LINES lines (z, y).  x lines are contiguous in memory; for z
-// and y the block's lines are CNZ_LINES consecutive i at one (j) or (k), so each global row
-// access covers CNZ_LINES consecutive values.
+// holds CN_LINES lines.  x lines are contiguous in memory; for z and y the
+// block's lines are CN_LINES consecutive i at one (j) or (k), so each global
+// row access covers CN_LINES consecutive doubles.
 #pragma once
 #include "common.cuh"
 #include "tdma.cuh"
@@ -33,10 +33,6 @@
 
 #define CN_LINES 8
 #define CN_NT (CN_LINES * 32)
-// z and y sweeps: CNZ_LINES consecutive i per block, so a warp's row loads cover 128 contiguous
-// bytes of a field row (8 lines gave 64-byte pieces); one warp still solves one line
-#define CNZ_LINES 16
-#define CNZ_NT (CNZ_LINES * 32)
 
 template <int S>
 struct SegCoef {  // coefficients stored at the segment-padded positions of tdma.cuh
@@ -52,7 +48,6 @@ struct SegCoef {  // coefficients stored at the segment-padded positions of tdma
 // (a multiple of 32 words) put all 8 on one bank.
 __host__ __device__ constexpr int cn_line_stride(int seg) { return 4 * seg + 2; }
 inline size_t smem_cn(int n) { return (size_t)CN_LINES * cn_line_stride(32 * (n / 32 + 1)) * sizeof(double); }
-inline size_t smem_cnz(int n) { return (size_t)CNZ_LINES * cn_line_stride(32 * (n / 32 + 1)) * sizeof(double); }
 
 // DPGRNS of RHS_MOM_EXPLICIT_io (:231-263)
 __device__ __forceinline__ double cn_dpgrns(const Geo& g, const DevState* st, int ns) {
@@ -109,16 +104,16 @@ __global__ void __launch_bounds__(CN_NT, 3) k_io_cn_xsweep(Geo g, IoFieldsT<F> f
 
 // z lines (i0 .. i0+CN_LINES-1, j); component blockIdx.z
 template <int S, typename F>
-__global__ void __launch_bounds__(CNZ_NT, 2) k_io_cn_zsweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
+__global__ void __launch_bounds__(CN_NT, 4) k_io_cn_zsweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smz[];
     constexpr int SEG = 32 * (S + 1);
-    constexpr int RSTEP = CNZ_NT / CNZ_LINES;
+    constexpr int RSTEP = CN_NT / CN_LINES;
     const int N = g.N;
     const int comp = blockIdx.z;
     const int j = 1 + blockIdx.y;
     if (comp == 1 && j == 1) return;  // uniform over the block
-    const int l = threadIdx.x % CNZ_LINES, r0 = threadIdx.x / CNZ_LINES;
-    const int i = blockIdx.x * CNZ_LINES + l;
+    const int l = threadIdx.x % CN_LINES, r0 = threadIdx.x / CN_LINES;
+    const int i = blockIdx.x * CN_LINES + l;
     const double fac = 0.50 * g.talp[ns] * st->dt * g.cvisc;
     const double coe1 = fac * 4.0 / 3.0 * g.dzqi, coe2 = fac * g.dzqi;
     const F* D = f.DST + comp * g.FS;
@@ -155,15 +150,15 @@ __global__ void __launch_bounds__(CNZ_NT, 2) k_io_cn_zsweep(Geo g, IoFieldsT<F> 
 
 // y lines (i0 .. i0+CN_LINES-1, k); component blockIdx.z; then G += solution
 template <int S, typename F>
-__global__ void __launch_bounds__(CNZ_NT, 1) k_io_cn_ysweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
+__global__ void __launch_bounds__(CN_NT) k_io_cn_ysweep(Geo g, IoFieldsT<F> f, const DevState* __restrict__ st, int ns) {
     extern __shared__ double smy[];
     constexpr int SEG = 32 * (S + 1);
-    constexpr int RSTEP = CNZ_NT / CNZ_LINES;
+    constexpr int RSTEP = CN_NT / CN_LINES;
     const int M = g.M;
     const int comp = blockIdx.z;
     const int k = blockIdx.y;
-    const int l = threadIdx.x % CNZ_LINES, r0 = threadIdx.x / CNZ_LINES;
-    const int i = blockIdx.x * CNZ_LINES + l;
+    const int l = threadIdx.x % CN_LINES, r0 = threadIdx.x / CN_LINES;
+    const int i = blockIdx.x * CN_LINES + l;
     const double fac = 0.50 * g.talp[ns] * st->dt * g.cvisc;
     const double coe1 = fac * 4.0 / 3.0, coe2 = fac;
     const F* D = f.DST + comp * g.FS;
