@@ -787,7 +787,8 @@ class ChannelIO(ChannelTG):
 class ChannelXinout(ChannelIO):
     """Main domain of a TG + main-domain run (CHAPSim iDomain = 3): inflow from a periodic
     :class:`ChannelTG` context (BC_TINLET_FLOW), a convective outlet (BC_COUTLET_MOM_RK3) and
-    FISHPACK's x-cosine Poisson solve; flow only, explicit viscous terms, FP64.
+    FISHPACK's x-cosine Poisson solve; explicit viscous terms, FP64; the thermal solver with
+    ``thermal_init`` and ``thermal_inlet`` (BC_TINLET_THERML, BC_COUTLET_ENEG_RK3).
 
     ``setup`` comes from :func:`chapsim.mesh.xinout_setup`.  Fields carry the x ghost
     columns: ``G`` is (3, N, M+2, L+2) = Fortran ``G_io(0:L+1, 0:M+1, N, 3)``, ``PR``, ``RHO``,

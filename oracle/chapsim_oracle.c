@@ -2419,7 +2419,7 @@ int orc_io_run_steps(orc_t* o, int nsteps, double* cfl_dt) {
 
 /* ====================================================================== */
 /* Main domain with inflow and outflow (iDomain = 3: TgFlowFlg and        */
-/* IoFlowFlg), flow only (iThermoDynamics = 0 or before timeThermoStart),  */
+/* IoFlowFlg), flow and (orc_xio_thermal_inlet) the thermal solver,       */
 /* explicit viscous terms.  x runs over 0..L+1: the inlet ghost column 0   */
 /* and the inlet face u(1) come from the periodic TG domain each substep  */
 /* (BC_TINLET_FLOW), the outlet column L+1 takes a convective update      */

@@ -345,7 +345,8 @@ class Oracle:
 
 class OracleXinout(Oracle):
     """Main domain of a TG + main-domain run (iDomain = 3) with inflow from a periodic TG
-    domain and a convective outlet; flow only, explicit viscous terms.
+    domain and a convective outlet; explicit viscous terms; the thermal solver after
+    ``thermal_enable`` and ``xio_thermal_inlet``.
 
     Fields carry the x ghost columns: shape (N, M+2, L+2) = Fortran (0:L+1, 0:M+1, N), i.e.
     ``NCL1S:NCL1E``.  The TG domain is an :class:`Oracle` with the same M, N and y mesh.
