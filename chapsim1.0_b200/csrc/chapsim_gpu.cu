@@ -614,7 +614,7 @@ void launch_fftz(chapsim_ctx* ctx, C* sp) {
     if (ctx->fz_pipe) {
         const long long nt = (nq + fzp_tq<C>() - 1) / fzp_tq<C>();
         const int nb = (int)std::min<long long>(nt, (long long)fzp_minb<C>() * ctx->nsm);
-        DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz_pipe<SIGN, FN1, FN2, C>, nb, FZ_NT, smem_fzp<C>(g), ctx->stream, g, sp)));
+        DISPATCH_FFT(g.N, (launch_pdl(ctx->pdl, k_fftz_pipe<SIGN, FN1, FN2, C>, nb, fzp_nt<C>(), smem_fzp<C>(g), ctx->stream, g, sp)));
     } else {
         const int gfz = (int)((nq + FZ_TQ - 1) / FZ_TQ);
         // prefetch distance: one wave of resident blocks (by the shared memory of a tile)

@@ -183,21 +183,24 @@ __global__ void __launch_bounds__(FZ_NT, sizeof(C) == 8 ? 4 : 2) k_fftz(Geo g, C
 }
 
 // Persistent, double-buffered form of k_fftz (autotuned alternative): a block
-// owns every gridDim.x-th tile of TQ = 16 lines and issues the copies of its
+// owns every gridDim.x-th tile of TQ lines and issues the copies of its
 // next tile (cp.async into the other buffer) before it transforms and stores
 // the current one, so the loads overlap the transform and the stores, where
 // the one-tile blocks of k_fftz overlap them only across blocks.  The
 // arithmetic is k_fftz's: the fields are bitwise equal.
-template <typename C> __host__ __device__ constexpr int fzp_tq() { return 16; }
-// Blocks per SM: one in FP64 (two 105 KB buffers at N = 384; inside the persistent tile loop
-// the FP64 transform of 384-point lines spilled 700 bytes under a two-block register budget,
-// where the one-tile kernel spills none), two in FP32.
-template <typename C> __host__ __device__ constexpr int fzp_minb() { return sizeof(C) == 16 ? 1 : 2; }
+// Two blocks per SM at both precisions.  FP64: tiles of 8 lines (two 51 KB buffers at
+// N = 384) and 128 threads, whose register budget holds the 384-point transform inside the
+// persistent tile loop (at 256 threads and 128 registers it spilled 700 bytes); FP32: tiles
+// of 16 lines and 256 threads.
+template <typename C> __host__ __device__ constexpr int fzp_tq() { return sizeof(C) == 16 ? 8 : 16; }
+template <typename C> __host__ __device__ constexpr int fzp_nt() { return sizeof(C) == 16 ? 128 : 256; }
+template <typename C> __host__ __device__ constexpr int fzp_minb() { return 2; }
 
 template <int SIGN, int N1, int N2, typename C>
-__global__ void __launch_bounds__(FZ_NT, fzp_minb<C>()) k_fftz_pipe(Geo g, C* __restrict__ SP) {
+__global__ void __launch_bounds__(fzp_nt<C>(), fzp_minb<C>()) k_fftz_pipe(Geo g, C* __restrict__ SP) {
     pdl_wait();
     constexpr int TQ = fzp_tq<C>();
+    constexpr int NT = fzp_nt<C>();
     using T = typename CReal<C>::T;
     extern __shared__ __align__(16) unsigned char smp_raw[];
     const int N = g.N;
@@ -210,7 +213,7 @@ __global__ void __launch_bounds__(FZ_NT, fzp_minb<C>()) k_fftz_pipe(Geo g, C* __
             const long long q0 = tile * TQ;
             const int nq = (int)min((long long)TQ, Q - q0);
 #pragma unroll 1
-            for (int p = threadIdx.x; p < TQ * N; p += FZ_NT) {
+            for (int p = threadIdx.x; p < TQ * N; p += NT) {
                 const int kz = p / TQ, ql = p - kz * TQ;
                 if (ql < nq) {
                     if constexpr (sizeof(C) == 16) cp_async16(b + ql * LD + kz, SP + q0 + ql + Q * kz);
@@ -232,7 +235,7 @@ __global__ void __launch_bounds__(FZ_NT, fzp_minb<C>()) k_fftz_pipe(Geo g, C* __
         const int nq = (int)min((long long)TQ, Q - q0);
         block_fft4s<N1, N2, SIGN>(bc, nq, LD, twz_of<C>(g));  // starts and ends with a block barrier
 #pragma unroll 1
-        for (int p = threadIdx.x; p < TQ * N; p += FZ_NT) {
+        for (int p = threadIdx.x; p < TQ * N; p += NT) {
             const int kz = p / TQ, ql = p - kz * TQ;
             if (ql < nq) {
                 C v = bc[ql * LD + kz];
