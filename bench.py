@@ -737,9 +737,13 @@ def channel_measure(args, wl, precision, local, dist, ws, seed, steps, keep=Fals
         ch.advance(max(args.warmup, 1), DT0, DTMIN, CFLGV)  # warm-up (also captures the step graph)
         launches0 = ch.launch_count()
         barrier()
+        # an NVTX range around the timed steps, so that a profiler can select them alone
+        # (ncu --nvtx --nvtx-include "timed_steps/")
+        torch.cuda.nvtx.range_push("timed_steps")
         ev0.record(stream)
         dt_last, cfl_last = ch.advance(steps, DT0, DTMIN, CFLGV)
         ev1.record(stream)
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize(local)
     barrier()
     launches = ch.launch_count() - launches0
