@@ -28,7 +28,7 @@ ERR_NAMES = {0: "CHAPSIM_OK", -1: "CHAPSIM_ERR_CUDA", -2: "CHAPSIM_ERR_NAN", -3:
 MLP_TANH, MLP_CUBIC = 0, 1
 
 EXPORTED = ["chapsim_gpu_init", "chapsim_gpu_finalize", "chapsim_last_error_string", "chapsim_upload_fields",
-            "chapsim_download_fields", "chapsim_set_dt", "chapsim_get_dt", "chapsim_cfl_tg", "chapsim_step_begin",
+            "chapsim_download_fields", "chapsim_upload_fields_async", "chapsim_download_fields_async", "chapsim_io_wait", "chapsim_set_dt", "chapsim_get_dt", "chapsim_cfl_tg", "chapsim_step_begin",
             "chapsim_rk_substep_tg", "chapsim_advance_tg", "chapsim_divgck_tg", "chapsim_fft99_pois3d",
             "chapsim_tdmaiji_cyc", "chapsim_tdmaijj_noncyc", "chapsim_upload_io_fields",
             "chapsim_download_io_fields", "chapsim_rk_substep_io", "chapsim_cfl_io", "chapsim_profile_steps",
@@ -152,6 +152,9 @@ def load_library(path: str = LIB_PATH):
     L.chapsim_last_error_string.restype = ctypes.c_char_p
     L.chapsim_upload_fields.argtypes = [vp, _dp, _dp, _dp]
     L.chapsim_download_fields.argtypes = [vp, _dp, _dp, _dp]
+    L.chapsim_upload_fields_async.argtypes = [vp, _dp, _dp]
+    L.chapsim_download_fields_async.argtypes = [vp, _dp, _dp]
+    L.chapsim_io_wait.argtypes = [vp]
     L.chapsim_set_dt.argtypes = [vp, ctypes.c_double]
     L.chapsim_get_dt.argtypes = [vp, _dp]
     L.chapsim_cfl_tg.argtypes = [vp, _dp]
@@ -386,6 +389,24 @@ class ChannelTG:
         H = np.empty((3, self.N, self.M, self.L)) if want_h0 else None
         self._check(self.lib.chapsim_download_fields(self.h, _ptr(Q), _ptr(PR), _ptr(H)))
         return (Q, PR, H) if want_h0 else (Q, PR)
+
+    def upload_async(self, Q, PR):
+        """Pipelined upload (chapsim_upload_fields_async): Q and PR, C-contiguous float64 arrays of
+        the field shapes, preferably in pinned memory, stay unchanged until io_wait(); the next
+        advance() starts from them."""
+        if Q.shape != (3,) + self.field_shape() or PR.shape != self.field_shape():
+            raise ValueError("field shape mismatch")
+        self._check(self.lib.chapsim_upload_fields_async(self.h, _ptr(Q), _ptr(PR)))
+
+    def download_async(self, Q, PR):
+        """Pipelined download (chapsim_download_fields_async) of the current fields into Q and PR,
+        complete after io_wait()."""
+        if Q.shape != (3,) + self.field_shape() or PR.shape != self.field_shape():
+            raise ValueError("field shape mismatch")
+        self._check(self.lib.chapsim_download_fields_async(self.h, _ptr(Q), _ptr(PR)))
+
+    def io_wait(self):
+        self._check(self.lib.chapsim_io_wait(self.h))
 
     def set_dt(self, dt):
         self._check(self.lib.chapsim_set_dt(self.h, float(dt)))

@@ -235,6 +235,15 @@ struct chapsim_ctx {
     bool dump_pending = false;
     cudaStream_t dump_stream = nullptr;
     cudaEvent_t dump_snap = nullptr, dump_done = nullptr;
+    // pipelined host I/O (chapsim_upload_fields_async / chapsim_download_fields_async): two input and
+    // two output staging slots of Q and PR, an H2D and a D2H copy stream, and per slot the events that
+    // order the copies against the step stream
+    double* pio_in[2] = {nullptr, nullptr};
+    double* pio_out[2] = {nullptr, nullptr};
+    cudaStream_t pio_h2d = nullptr, pio_d2h = nullptr;
+    cudaEvent_t pio_in_ready[2] = {nullptr, nullptr}, pio_in_free[2] = {nullptr, nullptr};
+    cudaEvent_t pio_out_ready[2] = {nullptr, nullptr}, pio_out_free[2] = {nullptr, nullptr};
+    int pio_in_next = 0, pio_in_pending = 0, pio_in_head = 0, pio_out_next = 0;
     // inflow/outflow main domain (domain 3)
     chapsim_ctx* tg_in = nullptr;  // the periodic TG context whose fields feed the inlet
     double2* xio_tq = nullptr;     // (cos, sin)(pi p / (2L)) of the FFT form of the cosine transforms
@@ -1337,6 +1346,15 @@ void chapsim_gpu_finalize(chapsim_ctx_t* ctx) {
     cudaFree(ctx->xio_cf); cudaFree(ctx->xio_tq); cudaFree(ctx->xio_bc0); cudaFree(ctx->xio_bc0e); cudaFree(ctx->xio_mpart); cudaFree(ctx->xio_yd); cudaFree(ctx->xio_state); cudaFree(ctx->xio_part);
     for (auto& e : ctx->xev)
         if (e) cudaEventDestroy(e);
+    if (ctx->pio_h2d) cudaStreamSynchronize(ctx->pio_h2d);
+    if (ctx->pio_d2h) cudaStreamSynchronize(ctx->pio_d2h);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(ctx->pio_in[b]); cudaFree(ctx->pio_out[b]);
+        for (cudaEvent_t e : {ctx->pio_in_ready[b], ctx->pio_in_free[b], ctx->pio_out_ready[b], ctx->pio_out_free[b]})
+            if (e) cudaEventDestroy(e);
+    }
+    if (ctx->pio_h2d) cudaStreamDestroy(ctx->pio_h2d);
+    if (ctx->pio_d2h) cudaStreamDestroy(ctx->pio_d2h);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1378,6 +1396,105 @@ int chapsim_download_fields(chapsim_ctx_t* ctx, double* q, double* pr, double* c
     if (pr) CK(cudaMemcpyAsync(pr, ctx->PR, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     if (convh0)
         CK(cudaMemcpyAsync(convh0, ctx->H0, (size_t)(3 * g.FI) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return CHAPSIM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pipelined host I/O.  The fields of a run that streams them from and to host
+// memory every step pass through two device staging slots in each direction,
+// so that the H2D copy of the next step's input, the D2H copy of the last
+// step's result and the step itself run at the same time (the copy engines of
+// the two directions and the SMs).  Q and PR of a slot are one allocation
+// (3 FS + FS words).
+static int pio_setup(chapsim_ctx* ctx) {
+    if (ctx->pio_h2d) return CHAPSIM_OK;
+    const size_t bytes = (size_t)(4 * ctx->g.FS) * sizeof(double);
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaMalloc(&ctx->pio_in[b], bytes));
+        CK(cudaMalloc(&ctx->pio_out[b], bytes));
+        for (cudaEvent_t* e : {&ctx->pio_in_ready[b], &ctx->pio_in_free[b], &ctx->pio_out_ready[b], &ctx->pio_out_free[b]})
+            CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    CK(cudaStreamCreateWithFlags(&ctx->pio_h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&ctx->pio_d2h, cudaStreamNonBlocking));
+    return CHAPSIM_OK;
+}
+
+// The oldest pending upload becomes the context's fields, on the step stream:
+// the staged Q and PR copied in, CONVH0 zeroed, the wall ghosts set (as
+// chapsim_upload_fields), and in mixed precision the FP32 fields converted.
+static int pio_commit(chapsim_ctx* ctx) {
+    if (ctx->pio_in_pending == 0) return CHAPSIM_OK;
+    const Geo& g = ctx->g;
+    const int b = ctx->pio_in_head;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->pio_in_ready[b], 0));
+    CK(cudaMemcpyAsync(ctx->Q, ctx->pio_in[b], (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->PR, ctx->pio_in[b] + 3 * g.FS, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    CK(cudaEventRecord(ctx->pio_in_free[b], ctx->stream));
+    CK(cudaMemsetAsync(ctx->H0, 0, (size_t)(3 * g.FI) * sizeof(double), ctx->stream));
+    k_bc_fields<double><<<ctx->npart_red, DG_NT, 0, ctx->stream>>>(g, ctx->Q, ctx->PR);
+    ctx->launches += 1;
+    CK(cudaGetLastError());
+    if (ctx->prec == CHAPSIM_PREC_MIXED) {
+        int rc = mixed_from_staging(ctx, true);
+        if (rc) return rc;
+    }
+    ctx->pio_in_head ^= 1;
+    ctx->pio_in_pending -= 1;
+    return CHAPSIM_OK;
+}
+
+int chapsim_upload_fields_async(chapsim_ctx_t* ctx, const double* q, const double* pr) {
+    if (!ctx || !q || !pr) return fail(ctx, CHAPSIM_ERR_BADARG, "null field");
+    if (ctx->domain != 1) return fail(ctx, CHAPSIM_ERR_BADARG, "pipelined host I/O is for the periodic channel (TG)");
+    CK(cudaSetDevice(ctx->device));
+    int rc = pio_setup(ctx);
+    if (rc) return rc;
+    if (ctx->pio_in_pending == 2) rc = pio_commit(ctx);  // both slots hold uploads: the older one goes in first
+    if (rc) return rc;
+    const Geo& g = ctx->g;
+    const int b = ctx->pio_in_next;
+    CK(cudaStreamWaitEvent(ctx->pio_h2d, ctx->pio_in_free[b], 0));  // the slot's last commit has read it
+    CK(cudaMemcpyAsync(ctx->pio_in[b], q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyHostToDevice, ctx->pio_h2d));
+    CK(cudaMemcpyAsync(ctx->pio_in[b] + 3 * g.FS, pr, (size_t)g.FS * sizeof(double), cudaMemcpyHostToDevice, ctx->pio_h2d));
+    CK(cudaEventRecord(ctx->pio_in_ready[b], ctx->pio_h2d));
+    ctx->pio_in_next ^= 1;
+    ctx->pio_in_pending += 1;
+    return CHAPSIM_OK;
+}
+
+int chapsim_download_fields_async(chapsim_ctx_t* ctx, double* q, double* pr) {
+    if (!ctx || !q || !pr) return fail(ctx, CHAPSIM_ERR_BADARG, "null field");
+    if (ctx->domain != 1) return fail(ctx, CHAPSIM_ERR_BADARG, "pipelined host I/O is for the periodic channel (TG)");
+    CK(cudaSetDevice(ctx->device));
+    int rc = pio_setup(ctx);
+    if (rc) return rc;
+    const Geo& g = ctx->g;
+    if (ctx->prec == CHAPSIM_PREC_MIXED) {
+        rc = mixed_to_staging(ctx, true, true, false);
+        if (rc) return rc;
+    }
+    const int b = ctx->pio_out_next;
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->pio_out_free[b], 0));  // the slot's last D2H copy has read it
+    CK(cudaMemcpyAsync(ctx->pio_out[b], ctx->Q, (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->pio_out[b] + 3 * g.FS, ctx->PR, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    CK(cudaEventRecord(ctx->pio_out_ready[b], ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->pio_d2h, ctx->pio_out_ready[b], 0));
+    CK(cudaMemcpyAsync(q, ctx->pio_out[b], (size_t)(3 * g.FS) * sizeof(double), cudaMemcpyDeviceToHost, ctx->pio_d2h));
+    CK(cudaMemcpyAsync(pr, ctx->pio_out[b] + 3 * g.FS, (size_t)g.FS * sizeof(double), cudaMemcpyDeviceToHost, ctx->pio_d2h));
+    CK(cudaEventRecord(ctx->pio_out_free[b], ctx->pio_d2h));
+    ctx->pio_out_next ^= 1;
+    return CHAPSIM_OK;
+}
+
+int chapsim_io_wait(chapsim_ctx_t* ctx) {
+    if (!ctx) return CHAPSIM_ERR_BADARG;
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->pio_h2d) CK(cudaStreamSynchronize(ctx->pio_h2d));
+    if (ctx->pio_d2h) CK(cudaStreamSynchronize(ctx->pio_d2h));
     CK(cudaStreamSynchronize(ctx->stream));
     return CHAPSIM_OK;
 }
@@ -1450,7 +1567,9 @@ int chapsim_advance_tg(chapsim_ctx_t* ctx, int32_t nsteps, double dt0, double dt
     if (ctx->domain == 3)
         return fail(ctx, CHAPSIM_ERR_BADARG, "the inflow/outflow main domain steps with its TG domain: chapsim_advance_xinout");
     CK(cudaSetDevice(ctx->device));
-    int rc = set_step_params(ctx, dt0, dtmin, cflgv);
+    int rc = pio_commit(ctx);  // the oldest fields of chapsim_upload_fields_async, if any wait
+    if (rc) return rc;
+    rc = set_step_params(ctx, dt0, dtmin, cflgv);
     if (rc) return rc;
     rc = build_step_graph(ctx);
     if (rc) return rc;

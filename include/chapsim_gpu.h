@@ -117,6 +117,23 @@ const char* chapsim_last_error_string(const chapsim_ctx_t* ctx);
 int chapsim_upload_fields(chapsim_ctx_t* ctx, const double* q, const double* pr, const double* convh0);
 int chapsim_download_fields(chapsim_ctx_t* ctx, double* q, double* pr, double* convh0);
 
+/* Pipelined field transfer of the periodic channel, for a driver that streams Q and PR from and to host
+ * memory every step (the same transfer points as chapsim_upload_fields / chapsim_download_fields,
+ * src/SOLVE.f90:75-134; the reference's fields stay in host memory, so it has no copy).  Neither call waits:
+ * - chapsim_upload_fields_async starts the H2D copy of q and pr (layouts as above) into one of two device
+ *   staging slots.  The next chapsim_advance_tg makes the oldest staged upload the context's fields first
+ *   (CONVH0 zero, wall ghosts applied: as chapsim_upload_fields).  With both slots full, a third upload
+ *   commits the older one at once.
+ * - chapsim_download_fields_async copies the current Q and PR into one of two staging slots on the step
+ *   stream and starts their D2H copy into q and pr.
+ * - chapsim_io_wait returns when every copy and step issued so far has finished.
+ * The host buffers must stay valid and unchanged (upload) or unread (download) until chapsim_io_wait;
+ * they should be pinned (cudaHostAlloc / cudaHostRegister), or the copies do not overlap.  The staging
+ * slots (4 (3 + 1) FS words of device memory) are allocated by the first call. */
+int chapsim_upload_fields_async(chapsim_ctx_t* ctx, const double* q, const double* pr);
+int chapsim_download_fields_async(chapsim_ctx_t* ctx, double* q, double* pr);
+int chapsim_io_wait(chapsim_ctx_t* ctx);
+
 /* The module variable DT (src/modules.f90 init_info) as seen by the device. */
 int chapsim_set_dt(chapsim_ctx_t* ctx, double dt);
 int chapsim_get_dt(chapsim_ctx_t* ctx, double* dt);
